@@ -1,0 +1,422 @@
+#!/usr/bin/env python
+"""Column unknowns solved per second for the TIE-GCM NG vertical column solves
+on one B200 (or N, one process each, weak scaling).
+
+One step = every system of one column step of the workload: by default the
+2.5 deg global grid, 144 x 72 = 10368 columns x 57 levels, seven scalar
+tridiagonal systems plus one block-tridiagonal system per column.  Inputs are
+seeded synthetic coefficients with the benchmark's value laws, generated on
+the device; each step's inputs (0.24-0.32 GB) exceed the 126 MB L2, so no L2
+flush is needed between steps.
+
+  value   FP32-sweep + FP64-refinement path, device-resident plan, one CUDA
+          graph per step (unknowns/s); the FP64 drop-in path is reported
+          beside it ("fp64") with the ratio.
+  e2e     the same solves through the C-ABI drop-ins with pinned host
+          buffers in the reference's Fortran layout, host<->device copies
+          inside the timed region.
+  roofline  the dominant kernel (scalar solve) against the measured HBM copy
+          bandwidth, algorithmic bytes = 40 B per scalar unknown.
+  cpu_baseline  the oracle port (C, OpenMP, all host threads) on full steps.
+
+--impl reference times the reference algorithm on the host cores (the oracle
+port: the reference is Fortran and no Fortran compiler exists here).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+import __graft_entry__ as ge  # noqa: E402
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--config", type=int, default=1, help="workload index 0..4 (default: 2.5 deg column step)")
+    p.add_argument("--block", type=int, default=2, help="block size of the block system (2: O2/O, 3: O2/O/He)")
+    p.add_argument("--max-sub", type=int, default=None, help="cap nest sub-steps (nested workloads)")
+    p.add_argument("--skip-e2e", action="store_true")
+    p.add_argument("--skip-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=10.0)
+    p.add_argument("--e2e-steps", type=int, default=5)
+    return p.parse_args()
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_from_profiles(kernel, workload):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary, if any
+    (a line 'traffic_bytes_per_launch <kernel> <workload> <bytes>')."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for name in sorted(os.listdir(d)):
+        if not name.endswith((".md", ".txt")):
+            continue
+        with open(os.path.join(d, name)) as fh:
+            for line in fh:
+                parts = line.strip().strip("`").split()
+                if len(parts) == 4 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel and parts[2] == workload:
+                    return float(parts[3])
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons (200 ms)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                p = [v.strip() for v in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax = float(p[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def host_inputs(pkg, wl, grid, seed_offset=0):
+    """numpy (Fortran layout) inputs of one column step of one grid."""
+    scal, blk = pkg.synth.column_step(wl, grid, sub=seed_offset)
+    return scal, blk
+
+
+def cpu_step(orc, scal, blk, nthreads):
+    for (a, b, c, f) in scal:
+        orc.trsolv_ng(a, b, c, f, a.shape[0], nthreads=nthreads)
+    if blk is not None:
+        P, Q, R, f = blk
+        orc.blksolve(P, Q, R, f, f.shape[1], nthreads=nthreads)
+
+
+def cpu_unknowns(scal, blk):
+    n = sum(a.size for (a, _, _, _) in scal)
+    if blk is not None:
+        n += blk[3].size
+    return n
+
+
+def time_cpu(orc, scal, blk, nthreads, steps=None, seconds=None, warmup=1):
+    for _ in range(warmup):
+        cpu_step(orc, scal, blk, nthreads)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        cpu_step(orc, scal, blk, nthreads)
+        n += 1
+        el = time.perf_counter() - t0
+        if steps is not None and n >= steps:
+            break
+        if seconds is not None and el >= seconds:
+            break
+    return el / n, n
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    pkg = ge.load_package()
+    orc = ge.load_oracle()
+    wl = pkg.synth.workload(args.config)
+    if wl.block:
+        wl.block = args.block
+    grid = wl.grids[0]
+    scal, blk = host_inputs(pkg, wl, grid)
+    nthreads = orc.max_threads()
+    dt, n = time_cpu(orc, scal, blk, nthreads, steps=args.steps, warmup=args.warmup)
+    unk = cpu_unknowns(scal, blk)
+    value = unk / dt
+    sample = f"{grid.name}: {grid.ncol} columns x {grid.nk} levels, {len(scal)} scalar + {1 if blk else 0} block(B={wl.block}) systems per step"
+    out = {
+        "impl": "reference", "metric": "column unknowns/s", "value": value, "unit": "unknowns/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl.name, "columns": grid.ncol, "levels": grid.nk, "systems": len(scal) + (1 if blk else 0),
+                   "block": wl.block, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "unknowns/s", "cores": nthreads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "unknowns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference algorithm restated in C (oracle port, -O2 -ffp-contract=off, OpenMP over columns); "
+                "the reference is Fortran and no Fortran compiler is available",
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    pkg = ge.load_package()
+    cs = pkg.colsolve
+    wl = pkg.synth.workload(args.config)
+    if wl.block:
+        wl.block = args.block
+
+    dw = pkg.batch.DeviceWorkload(wl, dev, seed=pkg.synth.SEED_BASE + 7919 * rank, max_sub=args.max_sub)
+    segs = dw.segments()
+    scal_segs = dw.segments((cs.TG_KIND_SCALAR,))
+    blk_segs = [s for s in segs if s["kind"] != cs.TG_KIND_SCALAR]
+    unknowns = dw.unknowns()
+    stream = torch.cuda.Stream(device=dev)
+
+    def make(seglist, prec):
+        p = pkg.Plan(seglist, prec)
+        p.capture_graph(stream)
+        return p
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def time_plan(plan, steps, warmup):
+        for _ in range(warmup):
+            plan.execute(stream)
+        stream.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            plan.execute(stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        barrier()
+        torch.cuda.synchronize()
+        return max_over_ranks(ms)
+
+    results = {}
+    plans = {}
+    for prec, name in ((cs.TG_PREC_F64, "fp64"), (cs.TG_PREC_F32_REFINE, "refine")):
+        plans[name] = make(segs, prec)
+        plans[name + "_scalar"] = make(scal_segs, prec)
+        if blk_segs:
+            plans[name + "_block"] = make(blk_segs, prec)
+
+    # correctness of the refined solution against the FP64 (bit-exact) one
+    plans["fp64"].execute(stream)
+    stream.synchronize()
+    ref = [s["x"].clone() for s in segs]
+    plans["refine"].execute(stream)
+    stream.synchronize()
+    rc_ref, _ = plans["refine"].status()
+    hist = plans["refine"].sweep_histogram(8)
+    max_rel = 0.0
+    for s, r in zip(segs, ref):
+        n = s["ncol"]
+        d = (s["x"][..., :n] - r[..., :n]).abs().max().item()
+        m = r[..., :n].abs().max().item()
+        max_rel = max(max_rel, d / m if m > 0 else d)
+    rc64, _ = plans["fp64"].status()
+    del ref
+
+    clocks = Clocks(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    clocks.start()
+    # untimed pre-heat so that clocks settle and the sampler sees the load
+    t_end = time.time() + 1.0
+    while time.time() < t_end:
+        for _ in range(20):
+            plans["refine"].execute(stream)
+        stream.synchronize()
+    for name in ("refine", "fp64"):
+        results[name] = time_plan(plans[name], args.steps, args.warmup)
+    clk = clocks.stop()
+    for name in ("refine_scalar", "fp64_scalar", "refine_block", "fp64_block"):
+        if name in plans:
+            results[name] = time_plan(plans[name], args.steps, args.warmup)
+
+    peak, peak_kind = measured_peak()
+    bytes_scalar = dw.algorithmic_bytes((cs.TG_KIND_SCALAR,))
+    wl_tag = f"{wl.name}_B{wl.block}"
+
+    def roofline(name, kernel):
+        ms = results[name + "_scalar"]
+        ach = bytes_scalar / (ms * 1e-3) / 1e9
+        tr = traffic_from_profiles(kernel, wl_tag)
+        return {"bound": "hbm", "kernel": kernel, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "traffic": tr, "algorithmic_bytes_per_launch": bytes_scalar, "ms_per_launch": ms,
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s"}
+
+    value = world * unknowns / (results["refine"] * 1e-3)
+    v64 = world * unknowns / (results["fp64"] * 1e-3)
+    launches_per_step = plans["refine"].launches
+
+    # ---- end to end through the host-pointer C ABI (rank-local, pinned buffers)
+    e2e = None
+    cpu = None
+    if not args.skip_e2e or (rank == 0 and not args.skip_cpu):
+        grid = wl.grids[0]
+        scal_np, blk_np = host_inputs(pkg, wl, grid, seed_offset=rank)
+    if not args.skip_e2e:
+        def pinned_like(a):
+            t = torch.empty(a.shape[::-1], dtype=torch.float64, pin_memory=True)
+            v = t.numpy().T
+            v[...] = a
+            return t, v
+        keep = []
+        hs = []
+        for (a, b, c, f) in scal_np:
+            arrs = []
+            for v in (a, b, c, f, np.zeros_like(a, order="F")):
+                t, nv = pinned_like(v)
+                keep.append(t)
+                arrs.append(nv)
+            hs.append(arrs)
+        hb = None
+        if blk_np is not None:
+            hb = []
+            for v in (*blk_np, np.zeros_like(blk_np[3], order="F")):
+                t, nv = pinned_like(v)
+                keep.append(t)
+                hb.append(nv)
+        h2d = sum(4 * a.nbytes for (a, *_r) in hs) + (sum(v.nbytes for v in hb[:4]) if hb else 0)
+        d2h = sum(arr[4].nbytes for arr in hs) + (hb[4].nbytes if hb else 0)
+        cs.set_host_precision(cs.TG_PREC_F32_REFINE)
+
+        def e2e_step():
+            for (a, b, c, f, x) in hs:
+                cs.trsolv_ng(a, b, c, f, x, a.shape[0])
+            if hb:
+                P, Q, R, f, u = hb
+                cs.blksolve(P, Q, R, f, u, f.shape[1])
+        for _ in range(max(1, min(args.warmup, 3))):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        dt = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps)
+        cs.set_host_precision(cs.TG_PREC_F64)
+        e2e_unk = cpu_unknowns([tuple(h[:4]) for h in hs], tuple(hb[:4]) if hb else None)
+        e2e = {"value": world * e2e_unk / dt, "unit": "unknowns/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3, "steps": args.e2e_steps,
+               "path": "tg_trsolv_ng x7 + tg_blksolve, pinned host Fortran-layout arrays, refine precision",
+               "timer": "host wall clock around synchronous C-ABI calls"}
+        del keep
+
+    if rank == 0 and not args.skip_cpu and world == 1:
+        orc = ge.load_oracle()
+        nthr = orc.max_threads()
+        dt, n = time_cpu(orc, scal_np, blk_np, nthr, seconds=args.cpu_seconds)
+        cpu = {"value": cpu_unknowns(scal_np, blk_np) / dt, "unit": "unknowns/s", "cores": nthr, "kind": "port",
+               "sample": f"{n} full column steps ({grid.ncol} columns x {grid.nk} levels, {len(scal_np)} scalar + "
+                         f"{1 if blk_np else 0} block systems), oracle C port, OpenMP"}
+
+    if rank == 0:
+        out = {
+            "metric": "column unknowns/s (FP32+FP64-refine; FP64 beside it)",
+            "value": value, "unit": "unknowns/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": results["refine"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 sweeps + f64 refinement (f64 I/O)", "data": "synthetic (seeded, generated on device)",
+            "config": {"workload": wl.name, "grids": [(g.name, g.nlon, g.nlat, g.nk, g.nsub if args.max_sub is None else min(g.nsub, args.max_sub)) for g in wl.grids],
+                       "systems_per_column": wl.n_scalar + (1 if wl.block else 0), "block": wl.block,
+                       "unknowns_per_step_per_gpu": unknowns, "segments": len(segs),
+                       "l2": f"inputs {dw.input_bytes() / 1e9:.3f} GB per step > 126 MB L2 (no flush needed)",
+                       "parallelism": f"{world} GPU(s), independent column batches per GPU"},
+            "roofline": roofline("refine", "k_scalar_refine"),
+            "fp64": {"value": v64, "ms_per_step": results["fp64"], "roofline": roofline("fp64", "k_scalar_f64"),
+                     "status": cs.STATUS_NAMES[rc64]},
+            "refine": {"value": value, "refine_over_fp64": value / v64, "max_rel_err_vs_fp64": max_rel,
+                       "sweep_histogram": hist, "status": cs.STATUS_NAMES[rc_ref]},
+            "kernel_ms": {k: v for k, v in results.items()},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk,
+            "gpu_launches": args.steps * launches_per_step,
+        }
+        print(json.dumps(out))
+    for p in plans.values():
+        p.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

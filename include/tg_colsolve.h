@@ -1,0 +1,203 @@
+/*
+ * tg_colsolve.h -- C ABI of the B200 vertical column solvers for TIE-GCM NG.
+ *
+ * The library (libtg_colsolve.so) replaces the reference's vertical implicit
+ * column solves:
+ *   - the scalar tridiagonal Thomas solve trsolv / trsolv_ng, used by dt,
+ *     minor (N4S, NO, N2D, Ar), oplus and settei;
+ *   - the block-tridiagonal solves: the 3x3 O2/O/He system inline in
+ *     comp / comp_ng and the 2x2 U/V system blktri in duv.
+ *
+ * Conventions
+ *   - FP64 everywhere in the interface ("real" is promoted to 8 bytes in the
+ *     reference builds).
+ *   - Arrays are the reference's column-major (Fortran) arrays passed by
+ *     address, unless a layout argument says otherwise:
+ *       scalar          (nk, ncol)         element (k,col)     at k + nk*col
+ *       block matrices  (B, B, nk, ncol)   element (i,j,k,col) at i + B*j + B*B*(k + nk*col)
+ *       block vectors   (B, nk, ncol)      element (i,k,col)   at i + B*(k + nk*col)
+ *     Row arguments (k1, k2, lev0, lev1 ...) are 1-based, as in the reference.
+ *   - Host-pointer entry points are synchronous, like the Fortran routines
+ *     they replace.  Device-pointer entry points (suffix _dev) are
+ *     stream-ordered and do not synchronise.
+ *   - Every entry point returns a tg_status.  The reference has no error
+ *     return (a zero pivot silently yields Inf/NaN); the solves here produce
+ *     the same numbers in that case and additionally report TG_EPIVOT.
+ *   - The caller owns all arrays.  The library keeps device mirrors and work
+ *     buffers per device, reused across calls and released by
+ *     tg_release_buffers() or at process exit.  Calls from several host
+ *     threads are serialised per device.
+ *   - Precision: TG_PREC_F64 reproduces the reference's FP64 arithmetic bit
+ *     for bit (same operation order, no FMA contraction, IEEE division).
+ *     TG_PREC_F32_REFINE runs the Thomas sweeps in FP32 and corrects with
+ *     FP64 residuals (iterative refinement) to a relative correction below
+ *     tg_set_refine(); columns that do not converge are re-solved in FP64 on
+ *     the GPU.
+ */
+#ifndef TG_COLSOLVE_H
+#define TG_COLSOLVE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+typedef enum {
+    TG_OK = 0,
+    TG_EINVAL = 1,      /* an argument is out of range or a pointer is NULL   */
+    TG_EPIVOT = 2,      /* a pivot (w1, or a block determinant) was zero or    */
+                        /* non-finite in at least one column                   */
+    TG_ENONFINITE = 3,  /* a solution value is non-finite                      */
+    TG_ENOCONV = 4,     /* FP32 refinement did not converge in the sweep cap   */
+                        /* for some column (that column was re-solved in FP64) */
+    TG_ETIMEOUT = 5,    /* a bounded device wait gave up                       */
+    TG_ECUDA = 6,       /* a CUDA runtime call failed                          */
+    TG_ENOMEM = 7,      /* device or pinned memory allocation failed           */
+    TG_ENODEV = 8       /* no CUDA device is available                         */
+} tg_status;
+
+typedef enum {
+    TG_PREC_F64 = 0,         /* FP64 throughout: the drop-in                  */
+    TG_PREC_F32_REFINE = 1   /* FP32 sweeps + FP64 iterative refinement       */
+} tg_precision;
+
+typedef enum {
+    TG_LAYOUT_COLUMN = 0,    /* Fortran layout: level index fastest           */
+    TG_LAYOUT_LEVEL = 1      /* level-major: column index fastest, column     */
+                             /* stride ld >= ncol (see tg_segment)            */
+} tg_layout;
+
+typedef enum {
+    TG_KIND_SCALAR = 0,      /* tridiagonal, a/b/c/f -> x                      */
+    TG_KIND_BLOCK2 = 2,      /* 2x2 block tridiagonal, P/Q/R/f -> u            */
+    TG_KIND_BLOCK3 = 3       /* 3x3 block tridiagonal, P/Q/R/f -> u            */
+} tg_kind;
+
+/* ---- drop-in replacements, host pointers, synchronous -------------------- */
+
+/* trsolv (src/trsolv.F:2-107): one latitude slab of the global grid.
+ * a,b,c,f,x are (lev0:lev1, lon0:lon1).  Solves rows k1..k2 of every column
+ * except the periodic points 1,2 and lonmax-1,lonmax when the slab touches
+ * them (trsolv.F:32-35).  Elements of x outside rows k1..k2 or in skipped
+ * columns are not written.  The reference reads w1(k1) after initialising
+ * w1(lev0); every caller passes k1 == lev0, and here w1(k1) = b(k1).
+ * The reference's lat and idebug arguments only feed its debug output. */
+int tg_trsolv(const double *a, const double *b, const double *c, const double *f,
+              double *x, int lev0, int lev1, int k1, int k2, int lon0, int lon1,
+              int lonmax);
+
+/* trsolv_ng (src/trsolv_ng.F90:1-28): all ncol = (lond1-lond0+1)*(latd1-latd0+1)
+ * ghost-inclusive columns of a nest level, arrays (nk, ncol).  Rows 1..k2
+ * are solved; rows k2+1..nk of x are not written. */
+int tg_trsolv_ng(const double *a, const double *b, const double *c, const double *f,
+                 double *x, int nk, int k2, int ncol);
+
+/* blktri (src/duv.F:801-908): 2x2 block solve on one slab, a,b,c are
+ * (2,2,lev0:lev1,lon0:lon1) and f,x are (2,lev0:lev1,lon0:lon1).  Solves
+ * rows lev0..lev1-1, skipping the periodic columns as duv.F:102-105 does with
+ * nlonp4.  The reference's beta, gamma and y arguments are work arrays its
+ * callers never read; they are not produced. */
+int tg_blktri(const double *a, const double *b, const double *c, const double *f,
+              double *x, int lev0, int lev1, int lon0, int lon1, int nlonp4);
+
+/* The comp_ng 3x3 O2/O/He block solve (src/comp_ng.F90:166-332), extracted
+ * into a call: P,Q,R are the per-level pk,qk,rk blocks (3,3,nk,ncol) with
+ * the LBC/UBC folds already applied, f is fk (3,nk,ncol).  Rows 1..nk-1 are
+ * solved and row nk is set from the upper boundary as comp_ng.F90:328-332
+ * does:  u(i,nk) = ubc_ratio(i)*u(i,nk-1) + ubc_add(i), with ubc_ratio and
+ * ubc_add (3,ncol) (ubc_add may be NULL for zero).  B = 2 gives the same
+ * solve for 2x2 blocks. */
+int tg_comp_blksolve_ng(int B, const double *P, const double *Q, const double *R,
+                        const double *f, const double *ubc_ratio, const double *ubc_add,
+                        double *u, int nk, int ncol);
+
+/* General host-pointer block solve: P,Q,R (B,B,nk,ncol), f,u (B,nk,ncol),
+ * rows 1..k2 solved; if ubc_ratio (B,ncol) is given (k2 < nk), row k2+1 is
+ * set as in tg_comp_blksolve_ng.  tg_comp_blksolve_ng(B,...,nk,ncol) is
+ * tg_blksolve(B,...,nk,nk-1,ncol), and duv's blktri is the B = 2 case with
+ * k2 = nlev-1. */
+int tg_blksolve(int B, const double *P, const double *Q, const double *R, const double *f,
+                const double *ubc_ratio, const double *ubc_add, double *u, int nk, int k2,
+                int ncol);
+
+/* ---- device-pointer entry points, stream-ordered ----------------------------
+ * Pointers are device memory.  layout selects TG_LAYOUT_COLUMN (ld ignored)
+ * or TG_LAYOUT_LEVEL (ld = column stride in elements, ld >= ncol).  stream is
+ * a cudaStream_t (NULL = legacy default stream).  status_dev, if not NULL,
+ * is a device int that receives TG_OK or the first error status; the call
+ * itself only reports argument and launch errors. */
+int tg_trsolv_dev(const double *a, const double *b, const double *c, const double *f,
+                  double *x, int nk, int k2, int ncol, int layout, long ld,
+                  int precision, int *status_dev, void *stream);
+
+int tg_blksolve_dev(int B, const double *P, const double *Q, const double *R,
+                    const double *f, const double *ubc_ratio, const double *ubc_add,
+                    double *u, int nk, int k2, int ncol, int layout, long ld,
+                    int precision, int *status_dev, void *stream);
+
+/* ---- batched, GPU-resident plans ---------------------------------------------
+ * A plan solves many independent systems ("segments": any mix of grids, nest
+ * levels, sub-steps and species) in one persistent launch per system kind,
+ * driven by a flattened table of column tiles.  Segment arrays are device
+ * memory in TG_LAYOUT_LEVEL with column stride ld:
+ *   scalar  a,b,c,f,x   element (k,col)     at k*ld + col
+ *   block   P,Q,R       element (i,j,k,col) at ((k*B + j)*B + i)*ld + col
+ *           f,u         element (i,k,col)   at (k*B + i)*ld + col
+ *           ubc_ratio, ubc_add (optional)   at i*ld + col
+ * For block segments a,b,c carry P,Q,R and x carries u. */
+typedef struct {
+    int kind;              /* tg_kind                                        */
+    int nk;                /* levels per column (array extent)               */
+    int k2;                /* rows 1..k2 are solved                          */
+    int ncol;              /* columns                                        */
+    long ld;               /* column stride, >= ncol                         */
+    const double *a, *b, *c, *f;
+    double *x;
+    const double *ubc_ratio, *ubc_add;   /* block only; NULL for none        */
+} tg_segment;
+
+typedef struct tg_plan tg_plan;
+
+/* Copies the segment table; the arrays themselves are referenced, not
+ * copied, and must stay valid while the plan is executed. */
+int tg_plan_create(const tg_segment *segs, int nseg, int precision, tg_plan **plan);
+/* Enqueues the solve of every segment on stream (cudaStream_t). */
+int tg_plan_execute(tg_plan *plan, void *stream);
+/* Records one tg_plan_execute into a CUDA graph and replays it from then on
+ * (the stream must be the one used by later executes). */
+int tg_plan_capture_graph(tg_plan *plan, void *stream);
+/* Waits for the plan's work and copies one tg_status per segment. */
+int tg_plan_status(tg_plan *plan, int *per_segment_status);
+/* Number of kernel launches one tg_plan_execute issues. */
+int tg_plan_launches(const tg_plan *plan);
+/* Refinement sweep histogram of the last execute: hist[s] = columns that
+ * needed s sweeps (s = 0..nbins-1; the last bin also counts the FP64
+ * re-solves).  Returns the number of bins written. */
+int tg_plan_sweep_histogram(tg_plan *plan, long *hist, int nbins);
+int tg_plan_destroy(tg_plan *plan);
+
+/* ---- tuning, configuration, housekeeping ------------------------------------ */
+
+/* Mixed-precision refinement: at most max_sweeps FP64 residual sweeps per
+ * column, stopping when max|dx| <= rel_tol * max|x| (defaults 3 and 1e-12). */
+int tg_set_refine(int max_sweeps, double rel_tol);
+/* Precision of the host-pointer drop-ins (tg_trsolv, tg_trsolv_ng, tg_blktri,
+ * tg_comp_blksolve_ng, tg_blksolve), which keep the reference's signatures
+ * and therefore have no precision argument.  Default TG_PREC_F64. */
+int tg_set_host_precision(int precision);
+/* Launch shape of a kind/precision: columns per thread block (32..512, a
+ * multiple of 32) and columns per thread (1 or 2); 0 restores the default. */
+int tg_set_tile(int kind, int precision, int cols_per_block, int cols_per_thread);
+/* Frees the per-device mirrors, work buffers and streams. */
+int tg_release_buffers(void);
+/* Library version, e.g. "tg_colsolve 0.1.0 sm_100a". */
+const char *tg_version(void);
+/* Message of the last failing call on this thread. */
+const char *tg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TG_COLSOLVE_H */

@@ -1,0 +1,131 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py, always as the checker or the timed baseline,
+never by the product library.  Parity of the oracle with the reference is
+unpinned (no Fortran compiler here, no reference tests); it is pinned against
+LAPACK, manufactured solutions and a long-double restatement instead.
+
+Arrays are numpy float64 in the reference's column-major layouts:
+  scalar (nk, ncol), block matrices (B, B, nk, ncol), block vectors (B, nk, ncol),
+stored Fortran-ordered (``order='F'``), i.e. the level index fastest.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build(force=False):
+    """Compile oracle/liboracle.so with its Makefile (gcc, -ffp-contract=off)."""
+    src = os.path.join(_HERE, "tg_oracle.c")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.c_void_p
+        i, l = ctypes.c_int, ctypes.c_long
+        L.oracle_trsolv_ng.argtypes = [P, P, P, P, P, i, i, l, i]
+        L.oracle_trsolv_ng_ld.argtypes = [P, P, P, P, P, i, i, l]
+        L.oracle_trsolv.argtypes = [P, P, P, P, P, i, i, i, i, i, i, i]
+        L.oracle_matinv3.argtypes = [P, P]
+        L.oracle_matinv2.argtypes = [P, P]
+        L.oracle_blksolve.argtypes = [i, P, P, P, P, P, i, i, l, P, P, i]
+        L.oracle_blksolve_ld.argtypes = [i, P, P, P, P, P, i, i, l, P, P]
+        L.oracle_blktri.argtypes = [P, P, P, P, P, i, i, i, i, i]
+        L.oracle_max_threads.restype = i
+        for fn in (L.oracle_trsolv_ng, L.oracle_trsolv_ng_ld, L.oracle_trsolv, L.oracle_matinv3,
+                   L.oracle_matinv2, L.oracle_blksolve, L.oracle_blksolve_ld, L.oracle_blktri):
+            fn.restype = None
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and (a.flags.f_contiguous or a.ndim == 1), "float64 Fortran-ordered array expected"
+    return a.ctypes.data
+
+
+def _fcopy(a):
+    return np.asfortranarray(np.asarray(a, dtype=np.float64))
+
+
+def max_threads():
+    return lib().oracle_max_threads()
+
+
+def trsolv_ng(a, b, c, f, k2, x=None, nthreads=1, long_double=False):
+    """trsolv_ng (src/trsolv_ng.F90) over (nk, ncol) arrays; returns x.
+
+    Rows k2+1..nk of x keep the values of the ``x`` passed in (NaN if none)."""
+    a, b, c, f = (_fcopy(v) for v in (a, b, c, f))
+    nk = a.shape[0]
+    ncol = a.size // nk
+    if x is None:
+        x = np.full(a.shape, np.nan, order="F")
+    else:
+        x = _fcopy(x).copy(order="F")
+    if long_double:
+        lib().oracle_trsolv_ng_ld(_p(a), _p(b), _p(c), _p(f), _p(x), nk, k2, ncol)
+    else:
+        lib().oracle_trsolv_ng(_p(a), _p(b), _p(c), _p(f), _p(x), nk, k2, ncol, nthreads)
+    return x
+
+
+def trsolv(a, b, c, f, x, lev0, lev1, k1, k2, lon0, lon1, lonmax):
+    """trsolv (src/trsolv.F) on one (lev0:lev1, lon0:lon1) slab; returns x."""
+    a, b, c, f = (_fcopy(v) for v in (a, b, c, f))
+    x = _fcopy(x).copy(order="F")
+    lib().oracle_trsolv(_p(a), _p(b), _p(c), _p(f), _p(x), lev0, lev1, k1, k2, lon0, lon1, lonmax)
+    return x
+
+
+def matinv3(A):
+    A = _fcopy(A)
+    B = np.empty((3, 3), order="F")
+    lib().oracle_matinv3(_p(A), _p(B))
+    return B
+
+
+def matinv2(A):
+    A = _fcopy(A)
+    B = np.empty((2, 2), order="F")
+    lib().oracle_matinv2(_p(A), _p(B))
+    return B
+
+
+def blksolve(P, Q, R, f, k2, ubc_ratio=None, ubc_add=None, u=None, nthreads=1, long_double=False):
+    """Block-tridiagonal solve (comp_ng.F90:166-332 / duv.F blktri) over
+    (B,B,nk,ncol) blocks and (B,nk,ncol) vectors; returns u."""
+    P, Q, R, f = (_fcopy(v) for v in (P, Q, R, f))
+    B, nk = f.shape[0], f.shape[1]
+    ncol = f.size // (B * nk)
+    u = np.full(f.shape, np.nan, order="F") if u is None else _fcopy(u).copy(order="F")
+    ur = None if ubc_ratio is None else _fcopy(ubc_ratio)
+    ua = None if ubc_add is None else _fcopy(ubc_add)
+    if long_double:
+        lib().oracle_blksolve_ld(B, _p(P), _p(Q), _p(R), _p(f), _p(u), nk, k2, ncol, _p(ur), _p(ua))
+    else:
+        lib().oracle_blksolve(B, _p(P), _p(Q), _p(R), _p(f), _p(u), nk, k2, ncol, _p(ur), _p(ua), nthreads)
+    return u
+
+
+def blktri(a, b, c, f, x, lev0, lev1, lon0, lon1, nlonp4):
+    """blktri (src/duv.F:801-908) on one slab; returns x."""
+    a, b, c, f = (_fcopy(v) for v in (a, b, c, f))
+    x = _fcopy(x).copy(order="F")
+    lib().oracle_blktri(_p(a), _p(b), _p(c), _p(f), _p(x), lev0, lev1, lon0, lon1, nlonp4)
+    return x

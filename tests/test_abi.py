@@ -1,0 +1,69 @@
+"""The C-ABI library loads and exports every symbol include/tg_colsolve.h
+declares; host-only calls validate their arguments.  No GPU work here."""
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "tg_colsolve.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*)\s*(tg_\w+)\s*\(", txt, re.M)))
+
+
+def test_header_lists_every_export(pkg):
+    assert header_functions() == sorted(pkg.colsolve.EXPORTS)
+
+
+def test_library_exports_all_symbols(pkg):
+    L = pkg.colsolve.lib()
+    for name in header_functions():
+        assert hasattr(L, name), name
+
+
+def test_library_has_sm100a_code(pkg):
+    import subprocess
+    out = subprocess.run(["cuobjdump", "--list-elf", pkg.colsolve.LIB_PATH], capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip("cuobjdump unavailable")
+    assert "sm_100a" in out.stdout
+
+
+def test_version_and_host_validation(pkg):
+    cs = pkg.colsolve
+    assert "sm_100a" in cs.version()
+    with pytest.raises(cs.TgError):
+        cs.set_refine(0, 1e-10)
+    with pytest.raises(cs.TgError):
+        cs.set_refine(3, 2.0)
+    cs.set_refine(3, 1e-11)
+    with pytest.raises(cs.TgError):
+        cs.set_tile(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 48, 1)
+    with pytest.raises(cs.TgError):
+        cs.set_tile(cs.TG_KIND_BLOCK3, cs.TG_PREC_F64, 64, 2)
+    cs.set_tile(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 0, 0)
+
+
+def test_python_argument_checks(pkg):
+    import numpy as np
+    cs = pkg.colsolve
+    a = np.zeros((5, 3))  # C order: rejected before any device call
+    with pytest.raises(TypeError):
+        cs.trsolv_ng(a, a, a, a, a, 5)
+    af = np.zeros((5, 3), order="F")
+    with pytest.raises(ValueError):
+        cs.trsolv_ng(af, af, af, af, np.zeros((4, 3), order="F"), 5)
+
+
+def test_bad_arguments_rejected_without_device(pkg):
+    import ctypes
+    L = pkg.colsolve.lib()
+    # null pointers / k2 > nk are rejected before the library touches CUDA
+    assert L.tg_trsolv_ng(None, None, None, None, None, 5, 5, 3) == pkg.TG_EINVAL
+    buf = (ctypes.c_double * 15)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    assert L.tg_trsolv_ng(p, p, p, p, p, 5, 6, 3) == pkg.TG_EINVAL
+    assert L.tg_comp_blksolve_ng(4, p, p, p, p, None, None, p, 5, 1) == pkg.TG_EINVAL
+    assert L.tg_plan_create(None, 1, 0, None) == pkg.TG_EINVAL

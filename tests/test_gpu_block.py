@@ -1,0 +1,86 @@
+"""Block-tridiagonal solves (3x3 comp_ng O2/O/He, 2x2 blktri) on the GPU
+through the C ABI, against the oracle (bit-exact in FP64)."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("B,nk,ncol", [(3, 57, 1500), (2, 57, 1500), (3, 113, 301), (2, 29, 2592), (3, 2, 7), (3, 3, 33)])
+def test_comp_blksolve_bit_exact(cuda, pkg, orc, B, nk, ncol):
+    P, Q, R, f = pkg.synth.block_system(B, nk, ncol, 14.0 / (nk - 1), 31 + nk)
+    rng = np.random.default_rng(B + nk)
+    ratio = np.asfortranarray(rng.uniform(0.5, 1.5, (B, ncol)))
+    add = np.asfortranarray(rng.uniform(-1e-3, 1e-3, (B, ncol)))
+    u = np.zeros_like(f, order="F")
+    assert pkg.comp_blksolve_ng(P, Q, R, f, u, ratio, add) == pkg.TG_OK
+    assert np.array_equal(u, orc.blksolve(P, Q, R, f, nk - 1, ubc_ratio=ratio, ubc_add=add))
+    u2 = np.full(f.shape, 5.0, order="F")
+    assert pkg.comp_blksolve_ng(P, Q, R, f, u2) == pkg.TG_OK
+    ref = orc.blksolve(P, Q, R, f, nk - 1)
+    assert np.array_equal(u2[:, : nk - 1], ref[:, : nk - 1])
+    assert np.all(u2[:, nk - 1] == 5.0)
+
+
+def test_block_golden(cuda, pkg):
+    g = golden("pin_block3_57.npz")
+    u = np.zeros_like(g["f"], order="F")
+    pkg.comp_blksolve_ng(g["P"], g["Q"], g["R"], g["f"], u, g["ratio"], g["add"])
+    assert np.array_equal(u, g["u"])
+    for B in (2, 3):
+        kat = golden(f"kat_block{B}.npz")
+        for nk in (2, 3, 29):
+            P, Q, R, f, us = (kat[f"nk{nk}_{k}"] for k in ("P", "Q", "R", "f", "u"))
+            # rows 1..nk solved through the device entry (column layout)
+            import torch
+            t = [torch.from_numpy(np.ascontiguousarray(np.ravel(v, order="F"))).cuda() for v in (P, Q, R, f)]
+            tu = torch.zeros_like(t[3])
+            pkg.blksolve_dev(B, *t, tu, nk, nk, f.shape[2], layout=pkg.TG_LAYOUT_COLUMN, ld=0)
+            torch.cuda.synchronize()
+            u = tu.cpu().numpy().reshape(f.shape, order="F")
+            assert np.max(np.abs(u - us)) <= 1e-12 * np.max(np.abs(us))
+
+
+@pytest.mark.parametrize("lon0,lon1", [(1, 40), (3, 30), (5, 40)])
+def test_blktri_slab(cuda, pkg, orc, lon0, lon1):
+    nlonp4, nlev = 40, 29
+    ncol = lon1 - lon0 + 1
+    P, Q, R, f = pkg.synth.block_system(2, nlev, ncol, 0.5, lon0)
+    x = np.full(f.shape, 2.0, order="F")
+    assert pkg.blktri(P, Q, R, f, None, None, None, x, 1, nlev, lon0, lon1, nlonp4) == pkg.TG_OK
+    ref = orc.blktri(P, Q, R, f, np.full(f.shape, 2.0, order="F"), 1, nlev, lon0, lon1, nlonp4)
+    assert np.array_equal(x, ref)
+
+
+@pytest.mark.parametrize("B", [2, 3])
+def test_block_level_layout_and_refine(cuda, pkg, orc, B):
+    torch = cuda
+    nk, ncol, ld = 57, 1200, 1216
+    P, Q, R, f = pkg.synth.block_system(B, nk, ncol, 0.25, 90 + B)
+    ref = orc.blksolve(P, Q, R, f, nk)
+    tP, tQ, tR = (pkg.batch.level_matrix(v, ld, "cuda") for v in (P, Q, R))
+    tf = pkg.batch.level_vector(f, ld, "cuda")
+    for prec in (pkg.TG_PREC_F64, pkg.TG_PREC_F32_REFINE):
+        tu = torch.zeros_like(tf)
+        st = torch.zeros(1, dtype=torch.int32, device="cuda")
+        pkg.blksolve_dev(B, tP, tQ, tR, tf, tu, nk, nk, ncol, layout=pkg.TG_LAYOUT_LEVEL, ld=ld, precision=prec,
+                         status=st)
+        torch.cuda.synchronize()
+        u = pkg.batch.from_level_vector(tu, ncol)
+        if prec == pkg.TG_PREC_F64:
+            assert np.array_equal(u, ref)
+            assert int(st.item()) == pkg.TG_OK
+        else:
+            assert np.max(np.abs(u - ref)) / np.max(np.abs(ref)) <= 1e-10
+            assert int(st.item()) in (pkg.TG_OK, pkg.TG_ENOCONV)
+
+
+def test_singular_block_flagged(cuda, pkg, orc):
+    P, Q, R, f = pkg.synth.block_system(3, 12, 40, 0.5, 5)
+    Q = Q.copy(order="F")
+    Q[:, :, 4, 7] = 0.0
+    u = np.zeros_like(f, order="F")
+    assert pkg.comp_blksolve_ng(P, Q, R, f, u) == pkg.TG_EPIVOT
+    assert np.array_equal(u[:, :11], orc.blksolve(P, Q, R, f, 11)[:, :11], equal_nan=True)

@@ -1,0 +1,128 @@
+"""Batched plans: many segments of mixed kinds and sizes in one persistent
+launch per kind, CUDA-graph replay, per-segment status, refinement."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def make_segments(pkg, torch, specs, seed=0):
+    segs, refs_in = [], []
+    for i, (kind, nk, k2, ncol) in enumerate(specs):
+        ld = pkg.batch.pad_ld(ncol) + (32 if i % 2 else 0)
+        if kind == pkg.TG_KIND_SCALAR:
+            a, b, c, f = pkg.synth.scalar_system(nk, ncol, 14.0 / (nk - 1), seed + i, (1e-4, 1e-1), ("lognormal", -6, 2))
+            t = [pkg.batch.level_scalar(v, ld, "cuda") for v in (a, b, c, f)]
+            x = torch.full((nk, ld), 3.5, dtype=torch.float64, device="cuda")
+        else:
+            a, b, c, f = pkg.synth.block_system(kind, nk, ncol, 14.0 / (nk - 1), seed + i)
+            t = [pkg.batch.level_matrix(v, ld, "cuda") for v in (a, b, c)] + [pkg.batch.level_vector(f, ld, "cuda")]
+            x = torch.full((nk, kind, ld), 3.5, dtype=torch.float64, device="cuda")
+        segs.append(dict(kind=kind, nk=nk, k2=k2, ncol=ncol, ld=ld, a=t[0], b=t[1], c=t[2], f=t[3], x=x))
+        refs_in.append((a, b, c, f))
+    return segs, refs_in
+
+
+def check(pkg, orc, segs, refs_in, exact=True):
+    for s, (a, b, c, f) in zip(segs, refs_in):
+        if s["kind"] == pkg.TG_KIND_SCALAR:
+            x = pkg.batch.from_level_scalar(s["x"], s["ncol"])
+            ref = orc.trsolv_ng(a, b, c, f, s["k2"])
+            got, want = x[: s["k2"]], ref[: s["k2"]]
+            assert np.all(x[s["k2"]:] == 3.5)
+        else:
+            x = pkg.batch.from_level_vector(s["x"], s["ncol"])
+            ref = orc.blksolve(a, b, c, f, s["k2"])
+            got, want = x[:, : s["k2"]], ref[:, : s["k2"]]
+        if exact:
+            assert np.array_equal(got, want)
+        else:
+            assert np.max(np.abs(got - want)) / np.max(np.abs(want)) <= 1e-10
+
+
+SPECS = [(0, 57, 57, 1000), (0, 57, 56, 333), (0, 29, 29, 2592), (0, 113, 113, 100), (2, 57, 57, 500),
+         (3, 57, 57, 700), (3, 29, 29, 64), (0, 57, 57, 1)]
+
+
+def test_mixed_plan_bit_exact(cuda, pkg, orc):
+    torch = cuda
+    segs, refs_in = make_segments(pkg, torch, SPECS)
+    plan = pkg.Plan(segs, pkg.TG_PREC_F64)
+    assert plan.launches == 3
+    plan.execute()
+    rc, per = plan.status()
+    assert rc == pkg.TG_OK and per == [0] * len(SPECS)
+    check(pkg, orc, segs, refs_in)
+    plan.close()
+
+
+def test_graph_replay(cuda, pkg, orc):
+    torch = cuda
+    segs, refs_in = make_segments(pkg, torch, SPECS[:6], seed=50)
+    plan = pkg.Plan(segs, pkg.TG_PREC_F64)
+    stream = torch.cuda.Stream()
+    plan.capture_graph(stream)
+    with torch.cuda.stream(stream):
+        plan.execute(stream)
+    stream.synchronize()
+    check(pkg, orc, segs, refs_in)
+    # new inputs in the same buffers, replay the graph
+    segs2, refs2 = make_segments(pkg, torch, SPECS[:6], seed=90)
+    for s, s2 in zip(segs, segs2):
+        for k in "abcf":
+            s[k].copy_(s2[k])
+        s["x"].fill_(3.5)
+    torch.cuda.synchronize()
+    plan.execute(stream)
+    stream.synchronize()
+    check(pkg, orc, segs, refs2)
+    plan.close()
+
+
+def test_per_segment_status(cuda, pkg, orc):
+    torch = cuda
+    segs, refs_in = make_segments(pkg, torch, SPECS[:4], seed=7)
+    segs[2]["b"][10, 17] = 0.0
+    plan = pkg.Plan(segs, pkg.TG_PREC_F64)
+    plan.execute()
+    rc, per = plan.status()
+    assert rc == pkg.TG_EPIVOT
+    assert per == [pkg.TG_OK, pkg.TG_OK, pkg.TG_EPIVOT, pkg.TG_OK]
+    plan.close()
+
+
+def test_refine_plan(cuda, pkg, orc):
+    torch = cuda
+    segs, refs_in = make_segments(pkg, torch, SPECS, seed=11)
+    plan = pkg.Plan(segs, pkg.TG_PREC_F32_REFINE)
+    plan.execute()
+    rc, per = plan.status()
+    assert rc in (pkg.TG_OK, pkg.TG_ENOCONV)
+    check(pkg, orc, segs, refs_in, exact=False)
+    hist = plan.sweep_histogram(8)
+    assert sum(hist) == sum(s["ncol"] for s in segs)
+    plan.close()
+
+
+def test_device_workload_nested(cuda, pkg, orc):
+    """A scaled-down nested batch: global grid + 3 nests with sub-steps in one
+    plan; sampled columns checked against the oracle."""
+    torch = cuda
+    wl = pkg.synth.workload(3)
+    dw = pkg.batch.DeviceWorkload(wl, "cuda", max_sub=2)
+    plan = pkg.Plan(dw.segments(), pkg.TG_PREC_F64)
+    plan.execute()
+    assert plan.status()[0] == pkg.TG_OK
+    for it in dw.items[:: 5]:
+        n = min(it["ncol"], 64)
+        if it["kind"] == pkg.TG_KIND_SCALAR:
+            a, b, c, f = (np.asfortranarray(it[k][:, :n].cpu().numpy()) for k in "abcf")
+            ref = orc.trsolv_ng(a, b, c, f, it["k2"])
+            assert np.array_equal(it["x"][:, :n].cpu().numpy(), ref)
+        else:
+            B = it["kind"]
+            P, Q, R = (np.asfortranarray(np.transpose(it[k][..., :n].cpu().numpy(), (2, 1, 0, 3))) for k in "abc")
+            f = np.asfortranarray(np.transpose(it["f"][..., :n].cpu().numpy(), (1, 0, 2)))
+            ref = orc.blksolve(P, Q, R, f, it["k2"])
+            assert np.array_equal(pkg.batch.from_level_vector(it["x"], n), ref)
+    plan.close()

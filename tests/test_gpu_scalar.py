@@ -1,0 +1,137 @@
+"""Scalar tridiagonal solves on the GPU through the C ABI, against the oracle.
+
+FP64 results must be bit-identical to the oracle (the reference's arithmetic
+in the reference's order); the FP32+refinement path must be within 1e-10
+relative (normwise per field) of it."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_err(x, ref):
+    return np.max(np.abs(x - ref)) / np.max(np.abs(ref))
+
+
+def system(pkg, cfg, ncol, seed=0):
+    wl = pkg.synth.workload(cfg)
+    g = wl.grids[0]
+    return pkg.synth.scalar_system(g.nk, ncol, g.dz, 100 + seed, wl.d0_range, wl.loss, wl.d_span), g.nk
+
+
+@pytest.mark.parametrize("cfg,ncol", [(0, 2592), (1, 3001), (2, 777)])
+def test_trsolv_ng_bit_exact(cuda, pkg, orc, cfg, ncol):
+    (a, b, c, f), nk = system(pkg, cfg, ncol)
+    x = np.zeros_like(a, order="F")
+    assert pkg.trsolv_ng(a, b, c, f, x, nk) == pkg.TG_OK
+    assert np.array_equal(x, orc.trsolv_ng(a, b, c, f, nk))
+
+
+@pytest.mark.parametrize("nk,k2,ncol", [(1, 1, 5), (2, 2, 1), (3, 3, 31), (3, 2, 33), (57, 56, 1025), (113, 113, 63)])
+def test_trsolv_ng_edges_and_k2(cuda, pkg, orc, nk, k2, ncol):
+    rng = np.random.default_rng(nk * 1000 + ncol)
+    a = np.asfortranarray(-rng.uniform(0.1, 1, (nk, ncol)))
+    c = np.asfortranarray(-rng.uniform(0.1, 1, (nk, ncol)))
+    b = np.asfortranarray(2.5 + rng.uniform(0, 1, (nk, ncol)))
+    f = np.asfortranarray(rng.uniform(-1, 1, (nk, ncol)))
+    x = np.full((nk, ncol), 123.5, order="F")
+    assert pkg.trsolv_ng(a, b, c, f, x, k2) == pkg.TG_OK
+    ref = orc.trsolv_ng(a, b, c, f, k2)
+    assert np.array_equal(x[:k2], ref[:k2])
+    assert np.all(x[k2:] == 123.5)  # rows above k2 are not written
+
+
+def test_trsolv_ng_golden(cuda, pkg):
+    g = golden("pin_trsolv_ng_29.npz")
+    x = np.zeros_like(g["a"], order="F")
+    pkg.trsolv_ng(g["a"], g["b"], g["c"], g["f"], x, 29)
+    assert np.array_equal(x, g["x_nk"])
+    kat = golden("kat_scalar.npz")
+    for nk in (2, 3, 5, 29, 57):
+        a, b, c, f, xs = (kat[f"nk{nk}_{k}"] for k in "abcfx")
+        x = np.zeros_like(a, order="F")
+        pkg.trsolv_ng(a, b, c, f, x, nk)
+        assert np.max(np.abs(x - xs)) <= 1e-13 * np.max(np.abs(xs))
+
+
+@pytest.mark.parametrize("lon0,lon1,k1,k2", [(1, 76, 1, 56), (3, 40, 1, 57), (20, 76, 1, 57), (1, 76, 5, 50)])
+def test_trsolv_slab(cuda, pkg, orc, lon0, lon1, k1, k2):
+    lonmax, nlev = 76, 57
+    (a, b, c, f), _ = system(pkg, 1, lon1 - lon0 + 1, seed=lon0)
+    x = np.full(a.shape, -9.0, order="F")
+    assert pkg.trsolv(a, b, c, f, x, 1, nlev, k1, k2, lon0, lon1, lonmax, 17, 0) == pkg.TG_OK
+    ref = orc.trsolv(a, b, c, f, np.full(a.shape, -9.0, order="F"), 1, nlev, k1, k2, lon0, lon1, lonmax)
+    assert np.array_equal(x, ref)
+
+
+def test_zero_pivot_status_and_values(cuda, pkg, orc):
+    (a, b, c, f), nk = system(pkg, 0, 64)
+    b = b.copy(order="F")
+    b[0, 5] = 0.0          # zero pivot
+    b[3, 9] = np.nan       # non-finite pivot
+    x = np.zeros_like(a, order="F")
+    assert pkg.trsolv_ng(a, b, c, f, x, nk) == pkg.TG_EPIVOT
+    ref = orc.trsolv_ng(a, b, c, f, nk)
+    assert np.array_equal(x, ref, equal_nan=True)
+    # the library stays usable after a flagged call
+    (a, b, c, f), nk = system(pkg, 0, 64, seed=3)
+    assert pkg.trsolv_ng(a, b, c, f, x, nk) == pkg.TG_OK
+    assert np.array_equal(x, orc.trsolv_ng(a, b, c, f, nk))
+
+
+@pytest.mark.parametrize("layout", ["level", "column"])
+def test_device_entry(cuda, pkg, orc, layout):
+    torch = cuda
+    (a, b, c, f), nk = system(pkg, 1, 1000)
+    ref = orc.trsolv_ng(a, b, c, f, nk)
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    if layout == "level":
+        ld = 1000 + 24
+        ta, tb, tc, tf = (pkg.batch.level_scalar(v, ld, "cuda") for v in (a, b, c, f))
+        tx = torch.zeros((nk, ld), dtype=torch.float64, device="cuda")
+        pkg.trsolv_dev(ta, tb, tc, tf, tx, nk, nk, 1000, pkg.TG_LAYOUT_LEVEL, ld, status=st)
+        x = pkg.batch.from_level_scalar(tx, 1000)
+    else:
+        ta, tb, tc, tf = (torch.from_numpy(np.ascontiguousarray(v.T)).cuda() for v in (a, b, c, f))
+        tx = torch.zeros_like(ta)
+        pkg.trsolv_dev(ta, tb, tc, tf, tx, nk, nk, 1000, pkg.TG_LAYOUT_COLUMN, 0, status=st)
+        x = np.asfortranarray(tx.cpu().numpy().T)
+    torch.cuda.synchronize()
+    assert int(st.item()) == pkg.TG_OK
+    assert np.array_equal(x, ref)
+
+
+def test_two_columns_per_thread(cuda, pkg, orc):
+    torch = cuda
+    cs = pkg.colsolve
+    (a, b, c, f), nk = system(pkg, 1, 777)
+    ref = orc.trsolv_ng(a, b, c, f, nk)
+    ld = 800
+    ta, tb, tc, tf = (pkg.batch.level_scalar(v, ld, "cuda") for v in (a, b, c, f))
+    tx = torch.zeros((nk, ld), dtype=torch.float64, device="cuda")
+    cs.set_tile(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 128, 2)
+    try:
+        pkg.trsolv_dev(ta, tb, tc, tf, tx, nk, nk, 777, pkg.TG_LAYOUT_LEVEL, ld)
+        torch.cuda.synchronize()
+    finally:
+        cs.set_tile(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 0, 0)
+    assert np.array_equal(pkg.batch.from_level_scalar(tx, 777), ref)
+    assert torch.all(tx[:, 777:] == 0)  # padding columns are not written
+
+
+@pytest.mark.parametrize("cfg", [0, 1, 2])
+def test_refine_accuracy(cuda, pkg, orc, cfg):
+    torch = cuda
+    (a, b, c, f), nk = system(pkg, cfg, 2000, seed=7)
+    ref = orc.trsolv_ng(a, b, c, f, nk)
+    ld = 2016
+    ta, tb, tc, tf = (pkg.batch.level_scalar(v, ld, "cuda") for v in (a, b, c, f))
+    tx = torch.zeros((nk, ld), dtype=torch.float64, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pkg.trsolv_dev(ta, tb, tc, tf, tx, nk, nk, 2000, pkg.TG_LAYOUT_LEVEL, ld, pkg.TG_PREC_F32_REFINE, status=st)
+    torch.cuda.synchronize()
+    x = pkg.batch.from_level_scalar(tx, 2000)
+    assert rel_err(x, ref) <= 1e-10
+    assert int(st.item()) in (pkg.TG_OK, pkg.TG_ENOCONV)

@@ -1,0 +1,15 @@
+"""B200-native vertical column solvers for TIE-GCM NG.
+
+csrc/        CUDA kernels (sm_100a) and the C ABI, built into libtg_colsolve.so
+colsolve.py  Python mirror of the reference interface (trsolv, trsolv_ng,
+             blktri, the comp_ng block solve) and of the device/plan API
+synth.py     seeded synthetic column systems of the benchmark workloads
+batch.py     builders of the batched (plan) layout for whole workloads
+build.py     nvcc build of libtg_colsolve.so
+"""
+from . import batch, colsolve, synth  # noqa: F401
+from .colsolve import (TG_OK, TG_EINVAL, TG_EPIVOT, TG_ENONFINITE, TG_ENOCONV, TG_ETIMEOUT,  # noqa: F401
+                       TG_ECUDA, TG_ENOMEM, TG_ENODEV, TG_PREC_F64, TG_PREC_F32_REFINE,
+                       TG_LAYOUT_COLUMN, TG_LAYOUT_LEVEL, TG_KIND_SCALAR, TG_KIND_BLOCK2,
+                       TG_KIND_BLOCK3, TgError, Plan, trsolv, trsolv_ng, blktri, comp_blksolve_ng, blksolve,
+                       trsolv_dev, blksolve_dev, set_refine, set_host_precision, set_tile, release_buffers, version)

@@ -1,0 +1,328 @@
+"""Python mirror of the reference's column-solver interface over the C ABI of
+libtg_colsolve.so (include/tg_colsolve.h).
+
+The functions keep the reference's names, argument order and meaning:
+
+  trsolv(a,b,c,f,x,lev0,lev1,k1,k2,lon0,lon1,lonmax,lat,idebug)   src/trsolv.F:2
+  trsolv_ng(a,b,c,f,x,k2,i_ng)                                     src/trsolv_ng.F90:1
+  blktri(a,b,c,f,beta,gamma,y,x,lev0,lev1,lon0,lon1,nlonp4)        src/duv.F:801
+  comp_blksolve_ng(P,Q,R,f,u,ubc_ratio,ubc_add)                    src/comp_ng.F90:166-332
+
+Host arrays are numpy float64 arrays in the reference's Fortran layouts
+(order='F'); x/u are written in place, as the Fortran intent(out) arguments
+are.  Like the reference, a zero pivot does not raise: the numbers come out
+as Inf/NaN exactly as the Fortran would produce them, and the call returns the
+status code (TG_EPIVOT).  Argument and CUDA errors raise TgError.
+
+Device entry points (trsolv_dev, blksolve_dev, Plan) take raw device
+pointers (ints) or torch CUDA tensors.
+
+There is no CPU fallback: if the CUDA library is missing the import of this
+module's functions fails with an error.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+TG_OK, TG_EINVAL, TG_EPIVOT, TG_ENONFINITE, TG_ENOCONV, TG_ETIMEOUT, TG_ECUDA, TG_ENOMEM, TG_ENODEV = range(9)
+STATUS_NAMES = {0: "TG_OK", 1: "TG_EINVAL", 2: "TG_EPIVOT", 3: "TG_ENONFINITE", 4: "TG_ENOCONV",
+                5: "TG_ETIMEOUT", 6: "TG_ECUDA", 7: "TG_ENOMEM", 8: "TG_ENODEV"}
+TG_PREC_F64, TG_PREC_F32_REFINE = 0, 1
+TG_LAYOUT_COLUMN, TG_LAYOUT_LEVEL = 0, 1
+TG_KIND_SCALAR, TG_KIND_BLOCK2, TG_KIND_BLOCK3 = 0, 2, 3
+NUMERIC_STATUS = (TG_OK, TG_EPIVOT, TG_ENONFINITE, TG_ENOCONV)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
+
+# Every symbol include/tg_colsolve.h declares.
+EXPORTS = ("tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
+           "tg_blksolve_dev", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
+           "tg_plan_status", "tg_plan_launches", "tg_plan_sweep_histogram", "tg_plan_destroy",
+           "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_release_buffers", "tg_version", "tg_last_error")
+
+
+class TgError(RuntimeError):
+    def __init__(self, status, where):
+        self.status = status
+        msg = lib().tg_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}: {msg}")
+
+
+class Segment(ctypes.Structure):
+    """tg_segment of include/tg_colsolve.h."""
+    _fields_ = [("kind", ctypes.c_int), ("nk", ctypes.c_int), ("k2", ctypes.c_int), ("ncol", ctypes.c_int),
+                ("ld", ctypes.c_long),
+                ("a", ctypes.c_void_p), ("b", ctypes.c_void_p), ("c", ctypes.c_void_p), ("f", ctypes.c_void_p),
+                ("x", ctypes.c_void_p), ("ubc_ratio", ctypes.c_void_p), ("ubc_add", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libtg_colsolve.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with tiegcm3.0_ng_b200/build.py "
+                              "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, Lg, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_long, ctypes.c_double
+        sig = {
+            "tg_trsolv": [P, P, P, P, P, I, I, I, I, I, I, I],
+            "tg_trsolv_ng": [P, P, P, P, P, I, I, I],
+            "tg_blktri": [P, P, P, P, P, I, I, I, I, I],
+            "tg_comp_blksolve_ng": [I, P, P, P, P, P, P, P, I, I],
+            "tg_blksolve": [I, P, P, P, P, P, P, P, I, I, I],
+            "tg_trsolv_dev": [P, P, P, P, P, I, I, I, I, Lg, I, P, P],
+            "tg_blksolve_dev": [I, P, P, P, P, P, P, P, I, I, I, I, Lg, I, P, P],
+            "tg_plan_create": [ctypes.POINTER(Segment), I, I, ctypes.POINTER(P)],
+            "tg_plan_execute": [P, P],
+            "tg_plan_capture_graph": [P, P],
+            "tg_plan_status": [P, P],
+            "tg_plan_launches": [P],
+            "tg_plan_sweep_histogram": [P, ctypes.POINTER(Lg), I],
+            "tg_plan_destroy": [P],
+            "tg_set_refine": [I, D],
+            "tg_set_host_precision": [I],
+            "tg_set_tile": [I, I, I, I],
+            "tg_release_buffers": [],
+            "tg_version": [],
+            "tg_last_error": [],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = I
+        L.tg_version.restype = ctypes.c_char_p
+        L.tg_last_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def version():
+    return lib().tg_version().decode()
+
+
+def _check(rc, where, numeric_ok=True):
+    if rc == TG_OK or (numeric_ok and rc in NUMERIC_STATUS):
+        return rc
+    raise TgError(rc, where)
+
+
+def _host(a, name):
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not (a.flags.f_contiguous or a.ndim <= 1):
+        raise TypeError(f"{name}: a Fortran-ordered float64 numpy array is required")
+    return a.ctypes.data
+
+
+def _out(x, name):
+    p = _host(x, name)
+    if not x.flags.writeable:
+        raise TypeError(f"{name}: output array is read-only")
+    return p
+
+
+# ---------------------------------------------------------------------------
+# Drop-ins (host arrays, synchronous)
+# ---------------------------------------------------------------------------
+def trsolv(a, b, c, f, x, lev0, lev1, k1, k2, lon0, lon1, lonmax, lat=None, idebug=0):
+    """trsolv (src/trsolv.F): one latitude slab (lev0:lev1, lon0:lon1).
+    lat and idebug only feed the reference's debug output and are ignored."""
+    nlev, nlon = lev1 - lev0 + 1, lon1 - lon0 + 1
+    for v, n in ((a, "a"), (b, "b"), (c, "c"), (f, "f"), (x, "x")):
+        if v.shape != (nlev, nlon):
+            raise ValueError(f"trsolv: {n} must have shape {(nlev, nlon)}")
+    rc = lib().tg_trsolv(_host(a, "a"), _host(b, "b"), _host(c, "c"), _host(f, "f"), _out(x, "x"),
+                         lev0, lev1, k1, k2, lon0, lon1, lonmax)
+    return _check(rc, "tg_trsolv")
+
+
+def trsolv_ng(a, b, c, f, x, k2, i_ng=None):
+    """trsolv_ng (src/trsolv_ng.F90): arrays (nk, lond0:lond1, latd0:latd1)
+    (any trailing shape), all ghost-inclusive columns solved, rows 1..k2."""
+    nk = a.shape[0]
+    ncol = a.size // nk if nk else 0
+    for v, n in ((b, "b"), (c, "c"), (f, "f"), (x, "x")):
+        if v.shape != a.shape:
+            raise ValueError(f"trsolv_ng: {n} must have the shape of a {a.shape}")
+    rc = lib().tg_trsolv_ng(_host(a, "a"), _host(b, "b"), _host(c, "c"), _host(f, "f"), _out(x, "x"),
+                            nk, k2, ncol)
+    return _check(rc, "tg_trsolv_ng")
+
+
+def blktri(a, b, c, f, beta, gamma, y, x, lev0, lev1, lon0, lon1, nlonp4):
+    """blktri (src/duv.F:801): 2x2 blocks (2,2,lev0:lev1,lon0:lon1), vectors
+    (2,lev0:lev1,lon0:lon1).  beta, gamma and y are the reference's work
+    arrays; they are accepted for signature compatibility and not written."""
+    nlev, nlon = lev1 - lev0 + 1, lon1 - lon0 + 1
+    for v, n in ((a, "a"), (b, "b"), (c, "c")):
+        if v.shape != (2, 2, nlev, nlon):
+            raise ValueError(f"blktri: {n} must have shape {(2, 2, nlev, nlon)}")
+    for v, n in ((f, "f"), (x, "x")):
+        if v.shape != (2, nlev, nlon):
+            raise ValueError(f"blktri: {n} must have shape {(2, nlev, nlon)}")
+    rc = lib().tg_blktri(_host(a, "a"), _host(b, "b"), _host(c, "c"), _host(f, "f"), _out(x, "x"),
+                         lev0, lev1, lon0, lon1, nlonp4)
+    return _check(rc, "tg_blktri")
+
+
+def comp_blksolve_ng(P, Q, R, f, u, ubc_ratio=None, ubc_add=None):
+    """The comp_ng block solve (src/comp_ng.F90:166-332): P,Q,R (B,B,nk,ncol),
+    f,u (B,nk,ncol); rows 1..nk-1 solved, row nk from the UBC if ubc_ratio
+    (B,ncol) is given."""
+    B, nk = f.shape[0], f.shape[1]
+    ncol = f.size // (B * nk)
+    for v, n in ((P, "P"), (Q, "Q"), (R, "R")):
+        if v.shape[:3] != (B, B, nk) or v.size != B * B * nk * ncol:
+            raise ValueError(f"comp_blksolve_ng: {n} has the wrong shape")
+    if u.shape != f.shape:
+        raise ValueError("comp_blksolve_ng: u must have the shape of f")
+    ur = None if ubc_ratio is None else _host(ubc_ratio, "ubc_ratio")
+    ua = None if ubc_add is None else _host(ubc_add, "ubc_add")
+    rc = lib().tg_comp_blksolve_ng(B, _host(P, "P"), _host(Q, "Q"), _host(R, "R"), _host(f, "f"), ur, ua,
+                                   _out(u, "u"), nk, ncol)
+    return _check(rc, "tg_comp_blksolve_ng")
+
+
+def blksolve(P, Q, R, f, u, k2, ubc_ratio=None, ubc_add=None):
+    """General block solve on host arrays: rows 1..k2 of (B,B,nk,ncol) blocks;
+    row k2+1 from the UBC if ubc_ratio is given."""
+    B, nk = f.shape[0], f.shape[1]
+    ncol = f.size // (B * nk)
+    for v, n in ((P, "P"), (Q, "Q"), (R, "R")):
+        if v.shape[:3] != (B, B, nk) or v.size != B * B * nk * ncol:
+            raise ValueError(f"blksolve: {n} has the wrong shape")
+    if u.shape != f.shape:
+        raise ValueError("blksolve: u must have the shape of f")
+    ur = None if ubc_ratio is None else _host(ubc_ratio, "ubc_ratio")
+    ua = None if ubc_add is None else _host(ubc_add, "ubc_add")
+    rc = lib().tg_blksolve(B, _host(P, "P"), _host(Q, "Q"), _host(R, "R"), _host(f, "f"), ur, ua,
+                           _out(u, "u"), nk, k2, ncol)
+    return _check(rc, "tg_blksolve")
+
+
+# ---------------------------------------------------------------------------
+# Device entry points
+# ---------------------------------------------------------------------------
+def _dptr(t):
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    if hasattr(t, "data_ptr"):
+        if not t.is_cuda or str(t.dtype) != "torch.float64":
+            raise TypeError("a float64 CUDA tensor is required")
+        return t.data_ptr()
+    raise TypeError("device pointer (int) or torch CUDA tensor expected")
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def trsolv_dev(a, b, c, f, x, nk, k2, ncol, layout=TG_LAYOUT_LEVEL, ld=None, precision=TG_PREC_F64,
+               status=None, stream=None):
+    ld = ncol if ld is None else ld
+    rc = lib().tg_trsolv_dev(_dptr(a), _dptr(b), _dptr(c), _dptr(f), _dptr(x), nk, k2, ncol, layout, ld,
+                             precision, None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_trsolv_dev", numeric_ok=False)
+
+
+def blksolve_dev(B, P, Q, R, f, u, nk, k2, ncol, ubc_ratio=None, ubc_add=None, layout=TG_LAYOUT_LEVEL,
+                 ld=None, precision=TG_PREC_F64, status=None, stream=None):
+    ld = ncol if ld is None else ld
+    rc = lib().tg_blksolve_dev(B, _dptr(P), _dptr(Q), _dptr(R), _dptr(f), _dptr(ubc_ratio), _dptr(ubc_add),
+                               _dptr(u), nk, k2, ncol, layout, ld, precision,
+                               None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_blksolve_dev", numeric_ok=False)
+
+
+def _int_dptr(t):
+    if isinstance(t, int):
+        return t
+    if not t.is_cuda or str(t.dtype) != "torch.int32":
+        raise TypeError("status must be an int32 CUDA tensor")
+    return t.data_ptr()
+
+
+def set_refine(max_sweeps=3, rel_tol=1e-11):
+    return _check(lib().tg_set_refine(max_sweeps, rel_tol), "tg_set_refine", numeric_ok=False)
+
+
+def set_host_precision(precision=TG_PREC_F64):
+    """Precision used by the host-array drop-ins (default FP64)."""
+    return _check(lib().tg_set_host_precision(precision), "tg_set_host_precision", numeric_ok=False)
+
+
+def set_tile(kind, precision, cols_per_block=0, cols_per_thread=0):
+    return _check(lib().tg_set_tile(kind, precision, cols_per_block, cols_per_thread), "tg_set_tile",
+                  numeric_ok=False)
+
+
+def release_buffers():
+    return lib().tg_release_buffers()
+
+
+class Plan:
+    """A batched, GPU-resident solve of many segments (tg_plan_*).
+
+    segments: list of dicts with keys kind, nk, k2, ncol, ld, a, b, c, f, x
+    and optionally ubc_ratio, ubc_add (device pointers or torch tensors, in
+    the level-major plan layout of include/tg_colsolve.h).  The tensors are
+    referenced, not copied; keep them alive while the plan is used."""
+
+    def __init__(self, segments, precision=TG_PREC_F64):
+        arr = (Segment * max(len(segments), 1))()
+        self._keep = []
+        for i, s in enumerate(segments):
+            arr[i] = Segment(s["kind"], s["nk"], s["k2"], s["ncol"], s.get("ld", s["ncol"]),
+                             _dptr(s["a"]), _dptr(s["b"]), _dptr(s["c"]), _dptr(s["f"]), _dptr(s["x"]),
+                             _dptr(s.get("ubc_ratio")), _dptr(s.get("ubc_add")))
+            self._keep.append(s)
+        self.nseg = len(segments)
+        self.precision = precision
+        h = ctypes.c_void_p()
+        rc = lib().tg_plan_create(arr, len(segments), precision, ctypes.byref(h))
+        _check(rc, "tg_plan_create", numeric_ok=False)
+        self._h = h
+
+    def execute(self, stream=None):
+        _check(lib().tg_plan_execute(self._h, _stream(stream)), "tg_plan_execute", numeric_ok=False)
+
+    def capture_graph(self, stream):
+        _check(lib().tg_plan_capture_graph(self._h, _stream(stream)), "tg_plan_capture_graph", numeric_ok=False)
+
+    @property
+    def launches(self):
+        return lib().tg_plan_launches(self._h)
+
+    def status(self):
+        per = (ctypes.c_int * max(self.nseg, 1))()
+        rc = lib().tg_plan_status(self._h, per)
+        _check(rc, "tg_plan_status")
+        return rc, list(per)[: self.nseg]
+
+    def sweep_histogram(self, nbins=8):
+        h = (ctypes.c_long * nbins)()
+        n = lib().tg_plan_sweep_histogram(self._h, h, nbins)
+        if n < 0:
+            raise TgError(-n, "tg_plan_sweep_histogram")
+        return list(h)[:n]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tg_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

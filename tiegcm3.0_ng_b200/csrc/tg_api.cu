@@ -1,0 +1,798 @@
+// C ABI of the column solvers (include/tg_colsolve.h).
+//
+// Host-pointer drop-ins copy the reference's Fortran-layout arrays to the
+// device in column chunks on two streams (host->device copy of chunk j+1
+// overlaps the relayout + solve + device->host copy of chunk j), relayout
+// them to the level-major layout the kernels want, solve, and copy back only
+// the rows the reference writes.  Device-pointer entries and plans run on the
+// caller's stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "tg_internal.h"
+
+using namespace tg;
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+void set_err(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+#define TG_CUDA(call)                                                                             \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return TG_ECUDA;                                                                      \
+        }                                                                                         \
+    } while (0)
+
+Refine g_refine = {3, 1e-11};
+int g_host_precision = TG_PREC_F64;
+
+struct Buf {
+    void *p = nullptr;
+    size_t n = 0;
+};
+
+// Per-device work buffers and streams, created on first use.
+struct DevCtx {
+    int dev = -1;
+    std::mutex mu;
+    cudaStream_t st[2] = {nullptr, nullptr};
+    Buf colbuf[2][5];   // Fortran-layout staging: 4 inputs + output, per stream
+    Buf lvlbuf[2][7];   // level-major arrays: a,b,c,f,x,ubc_ratio,ubc_add, per stream
+    Buf scratch[2];     // block-kernel scratch, per stream
+    unsigned *flags = nullptr;           // device, 2 words (one per stream)
+    unsigned *flags_host = nullptr;      // pinned, 2 words
+    unsigned long long *hist = nullptr;  // device, kMaxSweepBins
+};
+
+constexpr int kMaxDev = 64;
+DevCtx *g_ctx[kMaxDev] = {};
+std::mutex g_ctx_mu;
+
+int get_ctx(DevCtx **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            set_err("no CUDA device available");
+            return TG_ENODEV;
+        }
+        set_err("cudaGetDevice failed: %s", cudaGetErrorString(e));
+        return TG_ECUDA;
+    }
+    if (dev < 0 || dev >= kMaxDev) {
+        set_err("device index %d out of range", dev);
+        return TG_ENODEV;
+    }
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    if (!g_ctx[dev]) {
+        DevCtx *c = new (std::nothrow) DevCtx;
+        if (!c) return TG_ENOMEM;
+        c->dev = dev;
+        for (int i = 0; i < 2; ++i) TG_CUDA(cudaStreamCreateWithFlags(&c->st[i], cudaStreamNonBlocking));
+        TG_CUDA(cudaMalloc(&c->flags, 2 * sizeof(unsigned)));
+        TG_CUDA(cudaMallocHost(&c->flags_host, 2 * sizeof(unsigned)));
+        TG_CUDA(cudaMalloc(&c->hist, kMaxSweepBins * sizeof(unsigned long long)));
+        g_ctx[dev] = c;
+    }
+    *out = g_ctx[dev];
+    return TG_OK;
+}
+
+// Grows a device buffer; the device is synchronised before an old buffer is
+// freed, since queued work may still use it.
+int grow(Buf &b, size_t bytes)
+{
+    if (bytes <= b.n) return TG_OK;
+    if (b.p) {
+        TG_CUDA(cudaDeviceSynchronize());
+        TG_CUDA(cudaFree(b.p));
+        b.p = nullptr;
+        b.n = 0;
+    }
+    bytes = (bytes + 4095) & ~(size_t)4095;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_err("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        return TG_ENOMEM;
+    }
+    b.n = bytes;
+    return TG_OK;
+}
+
+int flags_to_status(unsigned f)
+{
+    if (f & FLAG_PIVOT) return TG_EPIVOT;
+    if (f & FLAG_NONFINITE) return TG_ENONFINITE;
+    if (f & FLAG_NOCONV) return TG_ENOCONV;
+    return TG_OK;
+}
+
+__global__ void k_finish_status(const unsigned *flags, int *out)
+{
+    const unsigned f = *flags;
+    *out = (f & FLAG_PIVOT) ? TG_EPIVOT : (f & FLAG_NONFINITE) ? TG_ENONFINITE : (f & FLAG_NOCONV) ? TG_ENOCONV : TG_OK;
+}
+
+long round_up(long v, long m) { return (v + m - 1) / m * m; }
+
+bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+// One level-major solve of a single segment on stream st.
+int solve_level(DevCtx *c, int slot, int kind, int precision, Seg seg, unsigned *flags, cudaStream_t st)
+{
+    const int B = kind == TG_KIND_SCALAR ? 1 : kind;
+    int cpt = cols_per_thread(kind, precision);
+    if (cpt == 2) {
+        const bool al = (seg.ld % 2 == 0) && aligned16(seg.a) && aligned16(seg.b) && aligned16(seg.c) &&
+                        aligned16(seg.f) && aligned16(seg.x);
+        if (!al) cpt = 1;
+    }
+    const int cpb = cols_per_block(kind, precision);
+    const int threads = cpb / cols_per_thread(kind, precision);
+    const int cpb_eff = threads * cpt;
+    SegTable tab{};
+    tab.segs = nullptr;
+    tab.nseg = 1;
+    tab.ntiles = (int)((seg.ncol + cpb_eff - 1) / cpb_eff);
+    tab.k2max = seg.k2;
+    seg.tile0 = 0;
+    seg.status_idx = 0;
+    tab.one = seg;
+    Shape sh{};
+    cudaError_t e = plan_shape(kind, precision, seg.k2, tab.ntiles, &sh);
+    if (e != cudaSuccess) {
+        set_err("no launch shape for kind %d nk %d: %s", kind, seg.k2, cudaGetErrorString(e));
+        return TG_EINVAL;
+    }
+    sh.cpt = cpt;
+    sh.threads = threads;
+    if (kind == TG_KIND_SCALAR) {
+        sh.smem = scalar_smem_bytes(precision, sh.threads, sh.cpt, seg.k2);
+        TG_CUDA(launch_scalar(tab, precision, sh, g_refine, flags, c->hist, st));
+    } else {
+        const size_t need = block_scratch_bytes(B, precision, (long)sh.blocks * sh.threads, seg.k2);
+        int rc = grow(c->scratch[slot], need);
+        if (rc) return rc;
+        TG_CUDA(launch_block(tab, B, precision, sh, g_refine, (double *)c->scratch[slot].p, flags, c->hist, st));
+    }
+    return TG_OK;
+}
+
+// Host arrays in Fortran layout -> solve -> host x.
+//   B = 1 (scalar) or 2/3 (block); m[3], v (vectors) point at row 0 of the
+//   solve in column 0; colstride = elements between columns of a vector
+//   array (matrices: B*colstride); k2 rows are solved; ubc arrays (B, ncol).
+int host_solve(int kind, const double *const m[3], const double *v, double *x, long colstride, int k2,
+               long ncol, const double *ubc_ratio, const double *ubc_add, int precision)
+{
+    const int B = kind == TG_KIND_SCALAR ? 1 : kind;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long mrows = (long)B * B * k2;         // matrix rows copied per column
+    const long vrows = (long)B * k2;             // vector rows copied per column
+    const long orows = (long)B * (k2 + (ubc_ratio ? 1 : 0));
+    const long mstride = (long)B * colstride;     // matrix column stride (elements)
+    // chunk: ~1/8 of the columns for copy/compute overlap, at most 32 MB/array
+    long chunk = std::max<long>(1024, (ncol + 7) / 8);
+    const long cap = std::max<long>(256, (32l << 20) / (8 * std::max<long>(mrows, 1)));
+    chunk = std::min(chunk, cap);
+    chunk = std::min(chunk, ncol);
+    chunk = round_up(chunk, 32);
+    const long ld = chunk;
+    for (int s = 0; s < 2; ++s) {
+        for (int i = 0; i < 3; ++i)
+            if ((rc = grow(c->colbuf[s][i], sizeof(double) * mrows * chunk))) return rc;
+        if ((rc = grow(c->colbuf[s][3], sizeof(double) * vrows * chunk))) return rc;
+        if ((rc = grow(c->colbuf[s][4], sizeof(double) * orows * chunk))) return rc;
+        for (int i = 0; i < 3; ++i)
+            if ((rc = grow(c->lvlbuf[s][i], sizeof(double) * mrows * ld))) return rc;
+        if ((rc = grow(c->lvlbuf[s][3], sizeof(double) * vrows * ld))) return rc;
+        if ((rc = grow(c->lvlbuf[s][4], sizeof(double) * orows * ld))) return rc;
+        if (ubc_ratio) {
+            if ((rc = grow(c->lvlbuf[s][5], sizeof(double) * B * ld))) return rc;
+            if ((rc = grow(c->lvlbuf[s][6], sizeof(double) * B * ld))) return rc;
+        }
+    }
+    TG_CUDA(cudaMemsetAsync(c->flags, 0, 2 * sizeof(unsigned), c->st[0]));
+    TG_CUDA(cudaMemsetAsync(c->hist, 0, kMaxSweepBins * sizeof(unsigned long long), c->st[0]));
+    TG_CUDA(cudaStreamSynchronize(c->st[0]));
+    int j = 0;
+    for (long c0 = 0; c0 < ncol; c0 += chunk, ++j) {
+        const int s = j & 1;
+        cudaStream_t st = c->st[s];
+        const long nc = std::min(chunk, ncol - c0);
+        double *lv[7];
+        for (int i = 0; i < 7; ++i) lv[i] = (double *)c->lvlbuf[s][i].p;
+        for (int i = 0; i < 3; ++i) {
+            double *cb = (double *)c->colbuf[s][i].p;
+            if (mrows == mstride)
+                TG_CUDA(cudaMemcpyAsync(cb, m[i] + c0 * mstride, sizeof(double) * mrows * nc, cudaMemcpyHostToDevice, st));
+            else
+                TG_CUDA(cudaMemcpy2DAsync(cb, sizeof(double) * mrows, m[i] + c0 * mstride, sizeof(double) * mstride,
+                                          sizeof(double) * mrows, nc, cudaMemcpyHostToDevice, st));
+            TG_CUDA(launch_col_to_level(cb, mrows, lv[i], ld, mrows, nc, st));
+        }
+        {
+            double *cb = (double *)c->colbuf[s][3].p;
+            if (vrows == colstride)
+                TG_CUDA(cudaMemcpyAsync(cb, v + c0 * colstride, sizeof(double) * vrows * nc, cudaMemcpyHostToDevice, st));
+            else
+                TG_CUDA(cudaMemcpy2DAsync(cb, sizeof(double) * vrows, v + c0 * colstride, sizeof(double) * colstride,
+                                          sizeof(double) * vrows, nc, cudaMemcpyHostToDevice, st));
+            TG_CUDA(launch_col_to_level(cb, vrows, lv[3], ld, vrows, nc, st));
+        }
+        if (ubc_ratio) {
+            double *cb = (double *)c->colbuf[s][4].p;
+            TG_CUDA(cudaMemcpyAsync(cb, ubc_ratio + c0 * B, sizeof(double) * B * nc, cudaMemcpyHostToDevice, st));
+            TG_CUDA(launch_col_to_level(cb, B, lv[5], ld, B, nc, st));
+            if (ubc_add) {
+                TG_CUDA(cudaMemcpyAsync(cb, ubc_add + c0 * B, sizeof(double) * B * nc, cudaMemcpyHostToDevice, st));
+                TG_CUDA(launch_col_to_level(cb, B, lv[6], ld, B, nc, st));
+            }
+        }
+        Seg seg{};
+        seg.a = lv[0];
+        seg.b = lv[1];
+        seg.c = lv[2];
+        seg.f = lv[3];
+        seg.x = lv[4];
+        seg.ubc_ratio = ubc_ratio ? lv[5] : nullptr;
+        seg.ubc_add = (ubc_ratio && ubc_add) ? lv[6] : nullptr;
+        seg.ld = ld;
+        seg.nk = k2 + (ubc_ratio ? 1 : 0);
+        seg.k2 = k2;
+        seg.ncol = (int)nc;
+        seg.kind = kind;
+        if ((rc = solve_level(c, s, kind, precision, seg, c->flags + s, st))) return rc;
+        double *ob = (double *)c->colbuf[s][4].p;
+        TG_CUDA(launch_level_to_col(lv[4], ld, ob, orows, orows, nc, st));
+        if (orows == colstride)
+            TG_CUDA(cudaMemcpyAsync(x + c0 * colstride, ob, sizeof(double) * orows * nc, cudaMemcpyDeviceToHost, st));
+        else
+            TG_CUDA(cudaMemcpy2DAsync(x + c0 * colstride, sizeof(double) * colstride, ob, sizeof(double) * orows,
+                                      sizeof(double) * orows, nc, cudaMemcpyDeviceToHost, st));
+    }
+    TG_CUDA(cudaStreamSynchronize(c->st[0]));
+    TG_CUDA(cudaStreamSynchronize(c->st[1]));
+    TG_CUDA(cudaMemcpy(c->flags_host, c->flags, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    return flags_to_status(c->flags_host[0] | c->flags_host[1]);
+}
+
+bool bad_prec(int p) { return p != TG_PREC_F64 && p != TG_PREC_F32_REFINE; }
+
+}  // namespace
+
+// ===========================================================================
+// Public entry points
+// ===========================================================================
+extern "C" {
+
+__attribute__((visibility("default"))) const char *tg_version(void) { return "tg_colsolve 0.1.0 sm_100a"; }
+
+__attribute__((visibility("default"))) const char *tg_last_error(void) { return g_err; }
+
+__attribute__((visibility("default"))) int tg_set_refine(int max_sweeps, double rel_tol)
+{
+    if (max_sweeps < 1 || max_sweeps > kMaxSweepBins - 2 || !(rel_tol > 0.0) || !(rel_tol < 1.0)) {
+        set_err("tg_set_refine: max_sweeps must be 1..%d and 0 < rel_tol < 1", kMaxSweepBins - 2);
+        return TG_EINVAL;
+    }
+    g_refine.max_sweeps = max_sweeps;
+    g_refine.rel_tol = rel_tol;
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_host_precision(int precision)
+{
+    if (bad_prec(precision)) {
+        set_err("tg_set_host_precision: unknown precision %d", precision);
+        return TG_EINVAL;
+    }
+    g_host_precision = precision;
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_tile(int kind, int precision, int cols_per_block_,
+                                                       int cols_per_thread_)
+{
+    if ((kind != TG_KIND_SCALAR && kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) || bad_prec(precision)) {
+        set_err("tg_set_tile: bad kind or precision");
+        return TG_EINVAL;
+    }
+    if (cols_per_block_ != 0 || cols_per_thread_ != 0) {
+        const int cpt = cols_per_thread_ ? cols_per_thread_ : 1;
+        const int maxthr = kind == TG_KIND_SCALAR ? 256 : 128;
+        if ((cpt != 1 && cpt != 2) || (cpt == 2 && (kind != TG_KIND_SCALAR || precision != TG_PREC_F64)) ||
+            cols_per_block_ < 32 || cols_per_block_ > 512 || cols_per_block_ % 32 ||
+            cols_per_block_ / cpt > maxthr || (cols_per_block_ / cpt) % 32) {
+            set_err("tg_set_tile: unsupported shape cpb=%d cpt=%d", cols_per_block_, cols_per_thread_);
+            return TG_EINVAL;
+        }
+    }
+    set_tile(kind, precision, cols_per_block_, cols_per_thread_);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_trsolv_ng(const double *a, const double *b, const double *c,
+                                                        const double *f, double *x, int nk, int k2, int ncol)
+{
+    if (!a || !b || !c || !f || !x || nk < 1 || k2 < 1 || k2 > nk || ncol < 0) {
+        set_err("tg_trsolv_ng: bad arguments (nk=%d k2=%d ncol=%d)", nk, k2, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    const double *m[3] = {a, b, c};
+    return host_solve(TG_KIND_SCALAR, m, f, x, nk, k2, ncol, nullptr, nullptr, g_host_precision);
+}
+
+__attribute__((visibility("default"))) int tg_trsolv(const double *a, const double *b, const double *c,
+                                                     const double *f, double *x, int lev0, int lev1, int k1,
+                                                     int k2, int lon0, int lon1, int lonmax)
+{
+    const int nlev = lev1 - lev0 + 1;
+    if (!a || !b || !c || !f || !x || nlev < 1 || k1 < lev0 || k2 > lev1 || k2 < k1 || lon1 < lon0) {
+        set_err("tg_trsolv: bad arguments");
+        return TG_EINVAL;
+    }
+    const int lonbeg = lon0 == 1 ? 3 : lon0;
+    const int lonend = lon1 == lonmax ? lon1 - 2 : lon1;
+    if (lonend < lonbeg) return TG_OK;
+    const size_t off = (size_t)nlev * (lonbeg - lon0) + (k1 - lev0);
+    const double *m[3] = {a + off, b + off, c + off};
+    return host_solve(TG_KIND_SCALAR, m, f + off, x + off, nlev, k2 - k1 + 1, lonend - lonbeg + 1, nullptr,
+                      nullptr, g_host_precision);
+}
+
+__attribute__((visibility("default"))) int tg_blktri(const double *a, const double *b, const double *c,
+                                                     const double *f, double *x, int lev0, int lev1, int lon0,
+                                                     int lon1, int nlonp4)
+{
+    const int nlev = lev1 - lev0 + 1;
+    if (!a || !b || !c || !f || !x || nlev < 2 || lon1 < lon0) {
+        set_err("tg_blktri: bad arguments");
+        return TG_EINVAL;
+    }
+    const int lonbeg = lon0 == 1 ? 3 : lon0;
+    const int lonend = lon1 == nlonp4 ? nlonp4 - 2 : lon1;
+    if (lonend < lonbeg) return TG_OK;
+    const size_t om = (size_t)4 * nlev * (lonbeg - lon0), ov = (size_t)2 * nlev * (lonbeg - lon0);
+    const double *m[3] = {a + om, b + om, c + om};
+    return host_solve(TG_KIND_BLOCK2, m, f + ov, x + ov, 2l * nlev, nlev - 1, lonend - lonbeg + 1, nullptr,
+                      nullptr, g_host_precision);
+}
+
+__attribute__((visibility("default"))) int tg_blksolve(int B, const double *P, const double *Q,
+                                                       const double *R, const double *f,
+                                                       const double *ubc_ratio, const double *ubc_add, double *u,
+                                                       int nk, int k2, int ncol)
+{
+    if ((B != 2 && B != 3) || !P || !Q || !R || !f || !u || nk < 1 || k2 < 1 || k2 > nk || ncol < 0 ||
+        (ubc_ratio && k2 >= nk)) {
+        set_err("tg_blksolve: bad arguments (B=%d nk=%d k2=%d ncol=%d)", B, nk, k2, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    const double *m[3] = {P, Q, R};
+    return host_solve(B, m, f, u, (long)B * nk, k2, ncol, ubc_ratio, ubc_add, g_host_precision);
+}
+
+__attribute__((visibility("default"))) int tg_comp_blksolve_ng(int B, const double *P, const double *Q,
+                                                               const double *R, const double *f,
+                                                               const double *ubc_ratio, const double *ubc_add,
+                                                               double *u, int nk, int ncol)
+{
+    if (nk < 2) {
+        set_err("tg_comp_blksolve_ng: nk must be >= 2");
+        return TG_EINVAL;
+    }
+    return tg_blksolve(B, P, Q, R, f, ubc_ratio, ubc_add, u, nk, nk - 1, ncol);
+}
+
+static int dev_solve(int kind, const double *a, const double *b, const double *c, const double *f,
+                     const double *ubc_ratio, const double *ubc_add, double *x, int nk, int k2, int ncol,
+                     int layout, long ld, int precision, int *status_dev, void *stream)
+{
+    const int B = kind == TG_KIND_SCALAR ? 1 : kind;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!a || !b || !c || !f || !x || nk < 1 || k2 < 1 || k2 > nk || ncol < 0 || bad_prec(precision) ||
+        (layout != TG_LAYOUT_COLUMN && layout != TG_LAYOUT_LEVEL) || (layout == TG_LAYOUT_LEVEL && ld < ncol) ||
+        (ubc_ratio && k2 >= nk)) {
+        set_err("device solve: bad arguments (nk=%d k2=%d ncol=%d layout=%d ld=%ld)", nk, k2, ncol, layout, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    unsigned *flags = cx->flags;
+    TG_CUDA(cudaMemsetAsync(flags, 0, sizeof(unsigned), st));
+    if (precision != TG_PREC_F64)
+        TG_CUDA(cudaMemsetAsync(cx->hist, 0, kMaxSweepBins * sizeof(unsigned long long), st));
+    if (ncol > 0) {
+        Seg seg{};
+        seg.nk = nk;
+        seg.k2 = k2;
+        seg.ncol = ncol;
+        seg.kind = kind;
+        const long orows = (long)B * (k2 + (ubc_ratio ? 1 : 0));
+        if (layout == TG_LAYOUT_LEVEL) {
+            seg.a = a; seg.b = b; seg.c = c; seg.f = f; seg.x = x;
+            seg.ubc_ratio = ubc_ratio;
+            seg.ubc_add = ubc_ratio ? ubc_add : nullptr;
+            seg.ld = ld;
+            if ((rc = solve_level(cx, 0, kind, precision, seg, flags, st))) return rc;
+        } else {
+            const long mrows = (long)B * B * k2, vrows = (long)B * k2;
+            const long lld = round_up(ncol, 32);
+            for (int i = 0; i < 3; ++i)
+                if ((rc = grow(cx->lvlbuf[0][i], sizeof(double) * mrows * lld))) return rc;
+            if ((rc = grow(cx->lvlbuf[0][3], sizeof(double) * vrows * lld))) return rc;
+            if ((rc = grow(cx->lvlbuf[0][4], sizeof(double) * orows * lld))) return rc;
+            if (ubc_ratio) {
+                if ((rc = grow(cx->lvlbuf[0][5], sizeof(double) * B * lld))) return rc;
+                if ((rc = grow(cx->lvlbuf[0][6], sizeof(double) * B * lld))) return rc;
+            }
+            double *lv[7];
+            for (int i = 0; i < 7; ++i) lv[i] = (double *)cx->lvlbuf[0][i].p;
+            const double *src[3] = {a, b, c};
+            for (int i = 0; i < 3; ++i) TG_CUDA(launch_col_to_level(src[i], (long)B * B * nk, lv[i], lld, mrows, ncol, st));
+            TG_CUDA(launch_col_to_level(f, (long)B * nk, lv[3], lld, vrows, ncol, st));
+            if (ubc_ratio) {
+                TG_CUDA(launch_col_to_level(ubc_ratio, B, lv[5], lld, B, ncol, st));
+                if (ubc_add) TG_CUDA(launch_col_to_level(ubc_add, B, lv[6], lld, B, ncol, st));
+            }
+            seg.a = lv[0]; seg.b = lv[1]; seg.c = lv[2]; seg.f = lv[3]; seg.x = lv[4];
+            seg.ubc_ratio = ubc_ratio ? lv[5] : nullptr;
+            seg.ubc_add = (ubc_ratio && ubc_add) ? lv[6] : nullptr;
+            seg.ld = lld;
+            seg.nk = k2 + (ubc_ratio ? 1 : 0);
+            if ((rc = solve_level(cx, 0, kind, precision, seg, flags, st))) return rc;
+            TG_CUDA(launch_level_to_col(lv[4], lld, x, (long)B * nk, orows, ncol, st));
+        }
+    }
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_trsolv_dev(const double *a, const double *b, const double *c,
+                                                         const double *f, double *x, int nk, int k2, int ncol,
+                                                         int layout, long ld, int precision, int *status_dev,
+                                                         void *stream)
+{
+    return dev_solve(TG_KIND_SCALAR, a, b, c, f, nullptr, nullptr, x, nk, k2, ncol, layout, ld, precision,
+                     status_dev, stream);
+}
+
+__attribute__((visibility("default"))) int tg_blksolve_dev(int B, const double *P, const double *Q,
+                                                           const double *R, const double *f,
+                                                           const double *ubc_ratio, const double *ubc_add,
+                                                           double *u, int nk, int k2, int ncol, int layout,
+                                                           long ld, int precision, int *status_dev, void *stream)
+{
+    if (B != 2 && B != 3) {
+        set_err("tg_blksolve_dev: B must be 2 or 3");
+        return TG_EINVAL;
+    }
+    return dev_solve(B, P, Q, R, f, ubc_ratio, ubc_add, u, nk, k2, ncol, layout, ld, precision, status_dev,
+                     stream);
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Plans
+// ===========================================================================
+struct tg_plan {
+    int dev = 0;
+    int precision = 0;
+    int nseg = 0;
+    struct Group {
+        int kind = 0;
+        int nseg = 0;
+        int ntiles = 0;
+        int k2max = 0;
+        Seg *d_segs = nullptr;
+        Shape shape{};
+        void *scratch = nullptr;
+    } groups[3];
+    unsigned *d_flags = nullptr;
+    int *d_status = nullptr;
+    unsigned long long *d_hist = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    int launches = 0;
+};
+
+namespace {
+int plan_enqueue(tg_plan *p, cudaStream_t st)
+{
+    TG_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(unsigned) * p->nseg, st));
+    if (p->precision != TG_PREC_F64)
+        TG_CUDA(cudaMemsetAsync(p->d_hist, 0, kMaxSweepBins * sizeof(unsigned long long), st));
+    for (auto &g : p->groups) {
+        if (g.nseg == 0) continue;
+        SegTable tab{};
+        tab.segs = g.d_segs;
+        tab.nseg = g.nseg;
+        tab.ntiles = g.ntiles;
+        tab.k2max = g.k2max;
+        if (g.kind == TG_KIND_SCALAR)
+            TG_CUDA(launch_scalar(tab, p->precision, g.shape, g_refine, p->d_flags, p->d_hist, st));
+        else
+            TG_CUDA(launch_block(tab, g.kind, p->precision, g.shape, g_refine, (double *)g.scratch, p->d_flags,
+                                 p->d_hist, st));
+    }
+    return TG_OK;
+}
+
+void plan_free(tg_plan *p)
+{
+    if (!p) return;
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    for (auto &g : p->groups) {
+        if (g.d_segs) cudaFree(g.d_segs);
+        if (g.scratch) cudaFree(g.scratch);
+    }
+    if (p->d_flags) cudaFree(p->d_flags);
+    if (p->d_status) cudaFree(p->d_status);
+    if (p->d_hist) cudaFree(p->d_hist);
+    delete p;
+}
+}  // namespace
+
+extern "C" {
+
+__attribute__((visibility("default"))) int tg_plan_create(const tg_segment *segs, int nseg, int precision,
+                                                          tg_plan **out)
+{
+    if (!out || (!segs && nseg > 0) || nseg < 0 || bad_prec(precision)) {
+        set_err("tg_plan_create: bad arguments");
+        return TG_EINVAL;
+    }
+    *out = nullptr;
+    for (int i = 0; i < nseg; ++i) {
+        const tg_segment &s = segs[i];
+        const bool blk = s.kind == TG_KIND_BLOCK2 || s.kind == TG_KIND_BLOCK3;
+        if ((s.kind != TG_KIND_SCALAR && !blk) || s.nk < 1 || s.k2 < 1 || s.k2 > s.nk || s.ncol < 0 ||
+            s.ld < s.ncol || !s.a || !s.b || !s.c || !s.f || !s.x || (blk && s.ubc_ratio && s.k2 >= s.nk)) {
+            set_err("tg_plan_create: segment %d invalid", i);
+            return TG_EINVAL;
+        }
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    tg_plan *p = new (std::nothrow) tg_plan;
+    if (!p) return TG_ENOMEM;
+    p->dev = cx->dev;
+    p->precision = precision;
+    p->nseg = nseg;
+    const int kinds[3] = {TG_KIND_SCALAR, TG_KIND_BLOCK2, TG_KIND_BLOCK3};
+    for (int gi = 0; gi < 3; ++gi) {
+        auto &g = p->groups[gi];
+        g.kind = kinds[gi];
+        int cpt = cols_per_thread(g.kind, precision);
+        const int cpb0 = cols_per_block(g.kind, precision);
+        const int threads = cpb0 / cols_per_thread(g.kind, precision);
+        std::vector<Seg> hs;
+        for (int i = 0; i < nseg; ++i) {
+            const tg_segment &s = segs[i];
+            if (s.kind != g.kind || s.ncol == 0) continue;
+            Seg d{};
+            d.a = s.a; d.b = s.b; d.c = s.c; d.f = s.f; d.x = s.x;
+            d.ubc_ratio = g.kind == TG_KIND_SCALAR ? nullptr : s.ubc_ratio;
+            d.ubc_add = d.ubc_ratio ? s.ubc_add : nullptr;
+            d.ld = s.ld; d.nk = s.nk; d.k2 = s.k2; d.ncol = s.ncol; d.kind = s.kind;
+            d.status_idx = i;
+            if (cpt == 2 && !((s.ld % 2 == 0) && aligned16(s.a) && aligned16(s.b) && aligned16(s.c) &&
+                              aligned16(s.f) && aligned16(s.x)))
+                cpt = 1;
+            hs.push_back(d);
+            g.k2max = std::max(g.k2max, s.k2);
+        }
+        if (hs.empty()) continue;
+        const int cpb = threads * cpt;
+        long tiles = 0;
+        for (auto &d : hs) {
+            d.tile0 = (int)tiles;
+            tiles += (d.ncol + cpb - 1) / cpb;
+        }
+        if (tiles > 0x7fffffffL) {
+            plan_free(p);
+            set_err("tg_plan_create: too many tiles");
+            return TG_EINVAL;
+        }
+        g.nseg = (int)hs.size();
+        g.ntiles = (int)tiles;
+        cudaError_t e = plan_shape(g.kind, precision, g.k2max, g.ntiles, &g.shape);
+        if (e != cudaSuccess) {
+            plan_free(p);
+            set_err("tg_plan_create: no launch shape: %s", cudaGetErrorString(e));
+            return TG_EINVAL;
+        }
+        g.shape.cpt = cpt;
+        g.shape.threads = threads;
+        if (g.kind == TG_KIND_SCALAR) g.shape.smem = scalar_smem_bytes(precision, threads, cpt, g.k2max);
+        if (cudaMalloc(&g.d_segs, sizeof(Seg) * hs.size()) != cudaSuccess ||
+            cudaMemcpy(g.d_segs, hs.data(), sizeof(Seg) * hs.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaGetLastError();
+            plan_free(p);
+            set_err("tg_plan_create: segment table upload failed");
+            return TG_ENOMEM;
+        }
+        if (g.kind != TG_KIND_SCALAR) {
+            const size_t need = block_scratch_bytes(g.kind, precision, (long)g.shape.blocks * g.shape.threads, g.k2max);
+            if (cudaMalloc(&g.scratch, need) != cudaSuccess) {
+                cudaGetLastError();
+                plan_free(p);
+                set_err("tg_plan_create: scratch allocation failed");
+                return TG_ENOMEM;
+            }
+        }
+        p->launches += 1;
+    }
+    if (cudaMalloc(&p->d_flags, sizeof(unsigned) * std::max(nseg, 1)) != cudaSuccess ||
+        cudaMalloc(&p->d_status, sizeof(int) * std::max(nseg, 1)) != cudaSuccess ||
+        cudaMalloc(&p->d_hist, kMaxSweepBins * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMemset(p->d_flags, 0, sizeof(unsigned) * std::max(nseg, 1)) != cudaSuccess ||
+        cudaMemset(p->d_hist, 0, kMaxSweepBins * sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        plan_free(p);
+        set_err("tg_plan_create: allocation failed");
+        return TG_ENOMEM;
+    }
+    *out = p;
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_plan_execute(tg_plan *p, void *stream)
+{
+    if (!p) {
+        set_err("tg_plan_execute: null plan");
+        return TG_EINVAL;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (p->exec) {
+        TG_CUDA(cudaGraphLaunch(p->exec, st));
+        return TG_OK;
+    }
+    return plan_enqueue(p, st);
+}
+
+__attribute__((visibility("default"))) int tg_plan_capture_graph(tg_plan *p, void *stream)
+{
+    if (!p || !stream) {
+        set_err("tg_plan_capture_graph: needs a plan and a non-default stream");
+        return TG_EINVAL;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (p->exec) {
+        cudaGraphExecDestroy(p->exec);
+        p->exec = nullptr;
+    }
+    if (p->graph) {
+        cudaGraphDestroy(p->graph);
+        p->graph = nullptr;
+    }
+    TG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = plan_enqueue(p, st);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        set_err("graph capture failed: %s", cudaGetErrorString(e));
+        return TG_ECUDA;
+    }
+    p->graph = g;
+    TG_CUDA(cudaGraphInstantiate(&p->exec, g, 0));
+    p->graph_stream = st;
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_plan_status(tg_plan *p, int *per_segment_status)
+{
+    if (!p) {
+        set_err("tg_plan_status: null plan");
+        return TG_EINVAL;
+    }
+    TG_CUDA(cudaDeviceSynchronize());
+    std::vector<unsigned> f(std::max(p->nseg, 1));
+    TG_CUDA(cudaMemcpy(f.data(), p->d_flags, sizeof(unsigned) * p->nseg, cudaMemcpyDeviceToHost));
+    unsigned all = 0;
+    for (int i = 0; i < p->nseg; ++i) {
+        if (per_segment_status) per_segment_status[i] = flags_to_status(f[i]);
+        all |= f[i];
+    }
+    return flags_to_status(all);
+}
+
+__attribute__((visibility("default"))) int tg_plan_launches(const tg_plan *p) { return p ? p->launches : 0; }
+
+__attribute__((visibility("default"))) int tg_plan_sweep_histogram(tg_plan *p, long *hist, int nbins)
+{
+    if (!p || !hist || nbins < 1) {
+        set_err("tg_plan_sweep_histogram: bad arguments");
+        return TG_EINVAL;
+    }
+    unsigned long long h[kMaxSweepBins];
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(h, p->d_hist, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_err("tg_plan_sweep_histogram: copy failed");
+        return -TG_ECUDA;
+    }
+    const int n = std::min(nbins, kMaxSweepBins);
+    for (int i = 0; i < n; ++i) hist[i] = (long)h[i];
+    for (int i = n; i < kMaxSweepBins; ++i) hist[n - 1] += (long)h[i];
+    return n;
+}
+
+__attribute__((visibility("default"))) int tg_plan_destroy(tg_plan *p)
+{
+    if (!p) return TG_OK;
+    cudaDeviceSynchronize();
+    plan_free(p);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_release_buffers(void)
+{
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    for (int d = 0; d < kMaxDev; ++d) {
+        DevCtx *c = g_ctx[d];
+        if (!c) continue;
+        std::lock_guard<std::mutex> lk2(c->mu);
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(d);
+        cudaDeviceSynchronize();
+        for (int s = 0; s < 2; ++s) {
+            for (auto &b : c->colbuf[s])
+                if (b.p) cudaFree(b.p);
+            for (auto &b : c->lvlbuf[s])
+                if (b.p) cudaFree(b.p);
+            if (c->scratch[s].p) cudaFree(c->scratch[s].p);
+            if (c->st[s]) cudaStreamDestroy(c->st[s]);
+        }
+        if (c->flags) cudaFree(c->flags);
+        if (c->flags_host) cudaFreeHost(c->flags_host);
+        if (c->hist) cudaFree(c->hist);
+        cudaSetDevice(cur);
+        delete c;
+        g_ctx[d] = nullptr;
+    }
+    return TG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// Internal declarations shared by the kernels (tg_kernels.cu) and the C ABI
+// (tg_api.cu).  Nothing here is part of the public interface.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tg_colsolve.h"
+
+namespace tg {
+
+// Per-segment status bits written by the kernels (atomicOr into a device word).
+enum : unsigned {
+    FLAG_PIVOT = 1u,      // zero or non-finite pivot / block determinant
+    FLAG_NONFINITE = 2u,  // non-finite solution value
+    FLAG_NOCONV = 4u,     // refinement hit the sweep cap (column re-solved in FP64)
+};
+
+// Maximum refinement sweeps tracked by the histogram (bins 0..kMaxSweepBins-1).
+constexpr int kMaxSweepBins = 8;
+
+// Device-side description of one batch of independent systems in level-major
+// layout (column index fastest, column stride ld).  For block kinds a/b/c
+// hold P/Q/R and x holds u.
+struct Seg {
+    const double *a, *b, *c, *f;
+    double *x;
+    const double *ubc_ratio, *ubc_add;
+    long ld;
+    int nk, k2, ncol, kind;
+    int tile0;        // first tile of this segment in the flattened tile space
+    int status_idx;   // index into the per-segment status array
+};
+
+// Flattened tile table: tile t belongs to the segment s with
+// segs[s].tile0 <= t < segs[s+1].tile0 (tile0 is a prefix sum).  When segs is
+// null the single segment `one` is used.
+struct SegTable {
+    const Seg *segs;
+    int nseg;
+    int ntiles;
+    int k2max;        // largest k2 of any segment (sizes per-thread scratch)
+    Seg one;
+};
+
+struct Refine {
+    int max_sweeps;
+    double rel_tol;
+};
+
+// Launch shape.
+struct Shape {
+    int threads;        // threads per block
+    int cpt;            // columns per thread (1 or 2)
+    int blocks;         // persistent grid size
+    size_t smem;        // dynamic shared memory bytes
+};
+
+int cols_per_block(int kind, int precision);
+int cols_per_thread(int kind, int precision);
+void set_tile(int kind, int precision, int cpb, int cpt);
+
+// Shared memory / scratch needs of a kernel for the largest k2 it will see.
+size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max);
+// Global scratch (bytes) of a block kernel with `slots` resident threads.
+size_t block_scratch_bytes(int B, int precision, long slots, int k2max);
+
+// Computes the persistent grid for a kind/precision/k2max on the current
+// device, limited to ntiles.
+cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, Shape *shape);
+
+// Solve launches (level-major).  status: per-segment device status words.
+// hist: device histogram of refinement sweeps (kMaxSweepBins longs), may be null.
+cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, Refine rf,
+                          unsigned *status, unsigned long long *hist, cudaStream_t st);
+cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape &sh, Refine rf,
+                         double *scratch, unsigned *status, unsigned long long *hist,
+                         cudaStream_t st);
+
+// 2-D relayout between the Fortran column layout and the level-major layout.
+// in(r, col) at in[r + in_ld*col] -> out[r*out_ld + col], r < nrows.
+cudaError_t launch_col_to_level(const double *in, long in_ld, double *out, long out_ld,
+                                long nrows, long ncols, cudaStream_t st);
+// in[r*in_ld + col] -> out(r, col) at out[r + out_ld*col], r < nrows.
+cudaError_t launch_level_to_col(const double *in, long in_ld, double *out, long out_ld,
+                                long nrows, long ncols, cudaStream_t st);
+
+}  // namespace tg

@@ -1,0 +1,220 @@
+"""Seeded synthetic column systems with the shapes and value laws of the
+benchmark workloads (no model data is available offline).
+
+Scalar law, per system and column, levels k = 0..nk-1 (dz the level spacing):
+    D_k = D0 * exp(k*dz) * LogNormal(0, 0.3)
+    a_k = c_k = -D_k / dz**2
+    b_k = 1/dt - a_k - c_k + L_k,   dt = 60 s
+    rhs_k ~ U(0, 1)
+with a Dirichlet bottom row (a=c=0, b=1, rhs=x_bot ~ U(0,1)) and a zero-flux
+top row (a=-1, b=1, c=0, rhs=0).  exp(k*dz) is exp(z_k - z_bot): on the 5 deg
+grid (dz = 0.5) it is exp(0.5k); finer grids keep the same altitude profile
+(14 scale heights between the model's zibot=-7 and zitop=7).
+
+Block law (B = 2 for the O2/O pair, 3 for O2/O/He): the diagonal of P, Q, R
+is the scalar law of each component; every off-diagonal entry (i,j) of P, Q, R
+is U(-0.2, 0.2) times the diagonal entry of row i of the same block; Q_ii is
+then raised by the sum of the absolute off-diagonal couplings of row i so that
+every block row stays strictly diagonally dominant by 1/dt + L_i.
+
+Everything is FP64, seeded from numpy's PCG64.  Arrays come back in the
+reference's Fortran layouts: scalar (nk, ncol), block matrices (B,B,nk,ncol),
+block vectors (B,nk,ncol), all order='F' (level index fastest within a column).
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+DT = 60.0
+SEED_BASE = 20261203
+
+# Species order of the seven scalar systems and the block system of a column.
+SCALAR_SYSTEMS = ("TN", "OPLUS", "N4S", "NO", "N2D", "AR", "HE")
+
+
+@dataclass
+class Grid:
+    """One horizontal grid (global or a nest level) of columns."""
+    name: str
+    nlon: int
+    nlat: int
+    nk: int
+    dz: float
+    nsub: int = 1          # sub-steps of this grid per outer step
+    ghost: int = 0         # ghost halo width on each side (nested grids: 2)
+
+    @property
+    def ncol(self):
+        return (self.nlon + 2 * self.ghost) * (self.nlat + 2 * self.ghost)
+
+
+@dataclass
+class Workload:
+    name: str
+    grids: list
+    n_scalar: int = 7
+    block: int = 2                 # 0: no block system, else block size B
+    d0_range: tuple = (1e-4, 1e-1)
+    loss: tuple = ("lognormal", -6.0, 2.0)
+    d_span: tuple = None           # (Dmin, Dmax): log-uniform bottom->top instead of exp(k dz)
+    notes: str = ""
+    extra: dict = field(default_factory=dict)
+
+    def unknowns_per_step(self):
+        n = 0
+        for g in self.grids:
+            per_col = self.n_scalar * g.nk + (self.block * g.nk if self.block else 0)
+            n += per_col * g.ncol * g.nsub
+        return n
+
+    def bytes_per_step(self):
+        """Algorithmic bytes of the FP64 I/O contract per outer step:
+        scalar 40 B per unknown (a,b,c,f in, x out); B x B block rows
+        (3*B*B + 2*B) * 8 B per block row."""
+        n = 0
+        for g in self.grids:
+            s = self.n_scalar * g.nk * 40
+            if self.block:
+                B = self.block
+                s += (3 * B * B + 2 * B) * 8 * g.nk
+            n += s * g.ncol * g.nsub
+        return n
+
+
+def nest_dims(lat_span, lon_span, dres):
+    """Nest interior size with the reference's truncation rule
+    (src/advance.F:213-216: n = int(span/d + 1))."""
+    return int(lon_span / dres + 1), int(lat_span / dres + 1)
+
+
+def workload(config):
+    """The five benchmark workloads by index (0..4)."""
+    if config == 0:
+        return Workload("5deg_trsolv_72x36x29", [Grid("global5", 72, 36, 29, 0.5)],
+                        n_scalar=1, block=0, d0_range=(1e-3, 1e-2), loss=("uniform", 0.0, 1e-3))
+    if config == 1:
+        return Workload("2.5deg_column_step_144x72x57", [Grid("global2.5", 144, 72, 57, 0.25)])
+    if config == 2:
+        return Workload("1.25deg_144x288x113_widerange", [Grid("global1.25", 288, 144, 113, 0.125)],
+                        d_span=(1e-5, 1e2))
+    if config == 3:
+        g = [Grid("global2.5", 144, 72, 57, 0.25)]
+        sub = 1
+        for i, (la, lo, d, n) in enumerate(((40, 60, 0.625, 4), (15, 20, 0.3125, 8), (5, 8, 0.15625, 16))):
+            sub *= n
+            nlon, nlat = nest_dims(la, lo, d)
+            g.append(Grid(f"nest{i+1}", nlon, nlat, 57, 0.25, nsub=sub, ghost=2))
+        return Workload("2.5deg_global_plus_3_nests", g)
+    if config == 4:
+        nlon, nlat = nest_dims(20, 30, 0.15625)
+        return Workload("0.625deg_576x288x113_plus_nest",
+                        [Grid("global0.625", 576, 288, 113, 0.125),
+                         Grid("nest1", nlon, nlat, 113, 0.125, nsub=4, ghost=2)],
+                        d_span=(1e-5, 1e2))
+    raise ValueError(f"unknown workload {config}")
+
+
+def _rng(seed):
+    return np.random.Generator(np.random.PCG64(seed))
+
+
+def _diffusion(rng, nk, ncol, dz, d0_range, d_span):
+    k = np.arange(nk, dtype=np.float64)[:, None]
+    if d_span is None:
+        d0 = rng.uniform(d0_range[0], d0_range[1], size=(1, ncol))
+        prof = d0 * np.exp(k * dz)
+    else:
+        lo, hi = np.log(d_span[0]), np.log(d_span[1])
+        # log-uniform endpoints per column, bottom to top
+        e0 = rng.uniform(lo, lo + 0.25 * (hi - lo), size=(1, ncol))
+        e1 = rng.uniform(hi - 0.25 * (hi - lo), hi, size=(1, ncol))
+        prof = np.exp(e0 + (e1 - e0) * k / max(nk - 1, 1))
+    return prof * rng.lognormal(0.0, 0.3, size=(nk, ncol))
+
+
+def _loss(rng, shape, loss):
+    kind, p0, p1 = loss
+    if kind == "uniform":
+        return rng.uniform(p0, p1, size=shape)
+    return rng.lognormal(p0, p1, size=shape)
+
+
+def scalar_system(nk, ncol, dz, seed, d0_range=(1e-3, 1e-2), loss=("uniform", 0.0, 1e-3),
+                  d_span=None, top_extra=0.0):
+    """One scalar tridiagonal system per column: returns (a, b, c, f), each
+    (nk, ncol) Fortran-ordered float64."""
+    rng = _rng(seed)
+    D = _diffusion(rng, nk, ncol, dz, d0_range, d_span)
+    L = _loss(rng, (nk, ncol), loss)
+    a = -D / dz**2
+    c = a.copy()
+    b = 1.0 / DT - a - c + L
+    f = rng.uniform(0.0, 1.0, size=(nk, ncol))
+    # Dirichlet bottom row
+    a[0] = 0.0
+    c[0] = 0.0
+    b[0] = 1.0
+    f[0] = rng.uniform(0.0, 1.0, size=ncol)
+    # zero-flux top row
+    a[-1] = -1.0
+    b[-1] = 1.0 + top_extra
+    c[-1] = 0.0
+    f[-1] = 0.0
+    return tuple(np.asfortranarray(v) for v in (a, b, c, f))
+
+
+def block_system(B, nk, ncol, dz, seed, d0_range=(1e-4, 1e-1), loss=("lognormal", -6.0, 2.0),
+                 d_span=None, coupling=0.2):
+    """One B x B block-tridiagonal system per column: returns (P, Q, R, f)
+    with P, Q, R (B,B,nk,ncol) and f (B,nk,ncol), Fortran-ordered float64."""
+    rng = _rng(seed)
+    P = np.zeros((B, B, nk, ncol))
+    Q = np.zeros((B, B, nk, ncol))
+    R = np.zeros((B, B, nk, ncol))
+    for i in range(B):
+        D = _diffusion(rng, nk, ncol, dz, d0_range, d_span)
+        L = _loss(rng, (nk, ncol), loss)
+        a = -D / dz**2
+        P[i, i] = a
+        R[i, i] = a
+        Q[i, i] = 1.0 / DT - 2.0 * a + L
+    for M in (P, Q, R):
+        for i in range(B):
+            for j in range(B):
+                if i != j:
+                    M[i, j] = rng.uniform(-coupling, coupling, size=(nk, ncol)) * M[i, i]
+    off = np.zeros((B, nk, ncol))
+    for i in range(B):
+        s = np.abs(P[i]).sum(axis=0) - np.abs(P[i, i]) + np.abs(R[i]).sum(axis=0) - np.abs(R[i, i])
+        s += np.abs(Q[i]).sum(axis=0) - np.abs(Q[i, i])
+        off[i] = s
+    for i in range(B):
+        Q[i, i] += off[i]
+    f = rng.uniform(0.0, 1.0, size=(B, nk, ncol))
+    # Dirichlet bottom block row, zero-flux top block row
+    P[:, :, 0] = 0.0
+    R[:, :, 0] = 0.0
+    Q[:, :, 0] = 0.0
+    P[:, :, -1] = 0.0
+    Q[:, :, -1] = 0.0
+    R[:, :, -1] = 0.0
+    for i in range(B):
+        Q[i, i, 0] = 1.0
+        P[i, i, -1] = -1.0
+        Q[i, i, -1] = 1.0
+    f[:, -1] = 0.0
+    return tuple(np.asfortranarray(v) for v in (P, Q, R, f))
+
+
+def column_step(wl, grid, sub=0, sys_count=None):
+    """All systems of one grid's sub-step: returns (scalars, block) where
+    scalars is a list of (a,b,c,f) and block is (P,Q,R,f) or None."""
+    gi = [g.name for g in wl.grids].index(grid.name)
+    base = SEED_BASE + 1000 * gi + 97 * sub
+    ns = wl.n_scalar if sys_count is None else min(sys_count, wl.n_scalar)
+    scal = [scalar_system(grid.nk, grid.ncol, grid.dz, base + s, wl.d0_range, wl.loss, wl.d_span)
+            for s in range(ns)]
+    blk = None
+    if wl.block:
+        blk = block_system(wl.block, grid.nk, grid.ncol, grid.dz, base + 50, wl.d0_range, wl.loss, wl.d_span)
+    return scal, blk
