@@ -80,7 +80,7 @@ def test_block_level_layout_and_refine(cuda, pkg, orc, B):
 def test_singular_block_flagged(cuda, pkg, orc):
     P, Q, R, f = pkg.synth.block_system(3, 12, 40, 0.5, 5)
     Q = Q.copy(order="F")
-    Q[:, :, 4, 7] = 0.0
+    Q[:, :, 0, 7] = 0.0   # the first row's pivot block is Q itself
     u = np.zeros_like(f, order="F")
     assert pkg.comp_blksolve_ng(P, Q, R, f, u) == pkg.TG_EPIVOT
     assert np.array_equal(u[:, :11], orc.blksolve(P, Q, R, f, 11)[:, :11], equal_nan=True)

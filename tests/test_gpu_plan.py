@@ -82,7 +82,7 @@ def test_graph_replay(cuda, pkg, orc):
 def test_per_segment_status(cuda, pkg, orc):
     torch = cuda
     segs, refs_in = make_segments(pkg, torch, SPECS[:4], seed=7)
-    segs[2]["b"][10, 17] = 0.0
+    segs[2]["b"][0, 17] = 0.0   # w1(1) = b(1) is the first pivot
     plan = pkg.Plan(segs, pkg.TG_PREC_F64)
     plan.execute()
     rc, per = plan.status()
