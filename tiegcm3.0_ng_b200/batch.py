@@ -185,3 +185,45 @@ class DeviceWorkload:
             for k in ("a", "b", "c", "f"):
                 n += it[k].numel() * 8
         return n
+
+
+# ---- sharding across GPUs -------------------------------------------------------
+def shard_columns(ncols, weights, world, rank):
+    """Contiguous share of the flattened column space for one rank.
+
+    Segment i has ncols[i] columns of weight weights[i] (unknowns per column:
+    B*k2).  The concatenated columns are cut at multiples of total/world in
+    weight, so every column goes to exactly one rank and the ranks' unknowns
+    differ by at most one column's weight.  Returns [(segment, c0, c1), ...]."""
+    total = sum(n * w for n, w in zip(ncols, weights))
+    lo = total * rank // world
+    hi = total * (rank + 1) // world
+    out = []
+    start = 0
+    for i, (n, w) in enumerate(zip(ncols, weights)):
+        seg_lo, seg_hi = start, start + n * w
+        a, b = max(lo, seg_lo), min(hi, seg_hi)
+        if a < b:
+            # a column belongs to the rank whose range holds its first unknown
+            c0 = -(-(a - seg_lo) // w)
+            c1 = -(-(b - seg_lo) // w)
+            if c1 > c0:
+                out.append((i, c0, c1))
+        start = seg_hi
+    return out
+
+
+def shard_segments(segments, world, rank):
+    """Plan segments restricted to this rank's columns (views, no copies)."""
+    ncols = [s["ncol"] for s in segments]
+    weights = [(1 if s["kind"] == TG_KIND_SCALAR else s["kind"]) * s["k2"] for s in segments]
+    out = []
+    for i, c0, c1 in shard_columns(ncols, weights, world, rank):
+        s = dict(segments[i])
+        for k in ("a", "b", "c", "f", "x", "ubc_ratio", "ubc_add"):
+            if s.get(k) is not None:
+                s[k] = s[k][..., c0:c1]
+        s["ncol"] = c1 - c0
+        s["col0"] = c0
+        out.append(s)
+    return out
