@@ -137,6 +137,25 @@ int tg_blksolve_dev(int B, const double *P, const double *Q, const double *R,
                     double *u, int nk, int k2, int ncol, int layout, long ld,
                     int precision, int *status_dev, void *stream);
 
+/* Allocation-free variant of tg_blksolve_dev (no counterpart in the reference).
+ * For callers that cannot allocate device memory: a model that reserves its
+ * whole device-memory budget up front, or a time loop that must not be
+ * stalled by the device synchronisation cudaFree implies.  FP64 only,
+ * TG_LAYOUT_LEVEL only; results are bit-identical to tg_blksolve_dev.
+ * The scratch is a fixed 16 MiB array in the library's device image, held by
+ * every GPU that loads the library until the process exits.  Limit: each
+ * resident thread needs B*B*k2 doubles and one thread block of the block
+ * kernel (64 threads by default) must fit, so k2 <= 3640 for B = 3 and
+ * k2 <= 8192 for B = 2; larger k2 returns TG_EINVAL.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (e.g. on two streams) race and must not be
+ * issued concurrently. */
+int tg_blksolve_dev_noalloc(int B, const double *P, const double *Q, const double *R,
+                            const double *f, const double *ubc_ratio, const double *ubc_add,
+                            double *u, int nk, int k2, int ncol, long ld, int *status_dev,
+                            void *stream);
+
 /* ---- batched, GPU-resident plans ---------------------------------------------
  * A plan solves many independent systems ("segments": any mix of grids, nest
  * levels, sub-steps and species) in one persistent launch per system kind,

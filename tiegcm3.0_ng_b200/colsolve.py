@@ -38,7 +38,7 @@ LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
 EXPORTS = ("tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
-           "tg_blksolve_dev", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
+           "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_release_buffers", "tg_version", "tg_last_error")
 
@@ -78,6 +78,7 @@ def lib():
             "tg_blksolve": [I, P, P, P, P, P, P, P, I, I, I],
             "tg_trsolv_dev": [P, P, P, P, P, I, I, I, I, Lg, I, P, P],
             "tg_blksolve_dev": [I, P, P, P, P, P, P, P, I, I, I, I, Lg, I, P, P],
+            "tg_blksolve_dev_noalloc": [I, P, P, P, P, P, P, P, I, I, I, Lg, P, P],
             "tg_plan_create": [ctypes.POINTER(Segment), I, I, ctypes.POINTER(P)],
             "tg_plan_execute": [P, P],
             "tg_plan_capture_graph": [P, P],
@@ -242,6 +243,17 @@ def blksolve_dev(B, P, Q, R, f, u, nk, k2, ncol, ubc_ratio=None, ubc_add=None, l
                                _dptr(u), nk, k2, ncol, layout, ld, precision,
                                None if status is None else _int_dptr(status), _stream(stream))
     return _check(rc, "tg_blksolve_dev", numeric_ok=False)
+
+
+def blksolve_dev_noalloc(B, P, Q, R, f, u, nk, k2, ncol, ubc_ratio=None, ubc_add=None, ld=None, status=None,
+                         stream=None):
+    """tg_blksolve_dev_noalloc: the FP64 level-major block solve with its
+    scratch in a fixed array of the library (no device allocation)."""
+    ld = ncol if ld is None else ld
+    rc = lib().tg_blksolve_dev_noalloc(B, _dptr(P), _dptr(Q), _dptr(R), _dptr(f), _dptr(ubc_ratio),
+                                       _dptr(ubc_add), _dptr(u), nk, k2, ncol, ld,
+                                       None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_blksolve_dev_noalloc", numeric_ok=False)
 
 
 def _int_dptr(t):

@@ -286,6 +286,8 @@ bool bad_prec(int p) { return p != TG_PREC_F64 && p != TG_PREC_F32_REFINE; }
 
 }  // namespace
 
+void tg::record_error(const char *msg) { set_err("%s", msg); }
+
 // ===========================================================================
 // Public entry points
 // ===========================================================================

@@ -85,4 +85,7 @@ cudaError_t launch_col_to_level(const double *in, long in_ld, double *out, long 
 cudaError_t launch_level_to_col(const double *in, long in_ld, double *out, long out_ld,
                                 long nrows, long ncols, cudaStream_t st);
 
+// Records the message tg_last_error() returns on this thread.
+void record_error(const char *msg);
+
 }  // namespace tg
