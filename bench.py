@@ -9,9 +9,10 @@ seeded synthetic coefficients with the benchmark's value laws, generated on
 the device; each step's inputs (0.24-0.32 GB) exceed the 126 MB L2, so no L2
 flush is needed between steps.
 
-  value   FP32-sweep + FP64-refinement path, device-resident plan, one CUDA
-          graph per step (unknowns/s); the FP64 drop-in path is reported
-          beside it ("fp64") with the ratio.
+  value   FP64 path (bit-identical to the reference arithmetic), device-
+          resident plan, one CUDA graph per step (unknowns/s); the FP32-sweep
+          + FP64-refinement path is reported beside it ("refine") with its
+          ratio to FP64 and its error against the FP64 solution.
   e2e     the same solves through the C-ABI drop-ins with pinned host
           buffers in the reference's Fortran layout, host<->device copies
           inside the timed region.
@@ -53,6 +54,9 @@ def parse():
     p.add_argument("--skip-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--profile", default=None,
+                   help="run only one kind's plan for a profiler: KIND:PREC[:VARIANT], KIND scalar|block, "
+                        "PREC f64|refine, VARIANT reg:CPB:CPT[:PF], regg:CPB:1[:PF] or ring:DEPTH (default: library default)")
     return p.parse_args()
 
 
@@ -194,7 +198,8 @@ def run_reference(args):
     value = unk / dt
     sample = f"{grid.name}: {grid.ncol} columns x {grid.nk} levels, {len(scal)} scalar + {1 if blk else 0} block(B={wl.block}) systems per step"
     out = {
-        "impl": "reference", "metric": "column unknowns/s", "value": value, "unit": "unknowns/s",
+        "impl": "reference", "metric": "column unknowns/s (FP64 path; FP32+FP64-refine path beside it, <=1e-10 rel err)",
+        "value": value, "unit": "unknowns/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": wl.name, "columns": grid.ncol, "levels": grid.nk, "systems": len(scal) + (1 if blk else 0),
@@ -208,10 +213,51 @@ def run_reference(args):
     return 0
 
 
+def run_profile(args):
+    """Executes one kind's plan --warmup + --steps times (for ncu captures)."""
+    import torch
+    pkg = ge.load_package()
+    cs = pkg.colsolve
+    from tiegcm_ng_b200 import autotune
+    parts = args.profile.split(":")
+    wl = pkg.synth.workload(args.config)
+    if wl.block:
+        wl.block = args.block
+    kind = cs.TG_KIND_SCALAR if parts[0] == "scalar" else wl.block
+    prec = cs.TG_PREC_F64 if parts[1] == "f64" else cs.TG_PREC_F32_REFINE
+    if len(parts) > 2:
+        v = parts[2]
+        cand = ("ring", int(parts[3]), 0, 4) if v == "ring" else \
+            (v, int(parts[3]), int(parts[4]), int(parts[5]) if len(parts) > 5 else 4)
+        autotune.apply(kind, prec, cand)
+    dw = pkg.batch.DeviceWorkload(wl, "cuda", max_sub=args.max_sub)
+    segs = dw.segments((kind,))
+    plan = pkg.Plan(segs, prec)
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        plan.execute(stream)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.execute(stream)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    rc, _ = plan.status()
+    print(json.dumps({"profile": args.profile, "workload": wl.name, "block": wl.block, "ms_per_launch": ms,
+                      "algorithmic_bytes": dw.algorithmic_bytes((kind,)), "unknowns": dw.unknowns((kind,)),
+                      "GBps": dw.algorithmic_bytes((kind,)) / ms / 1e6, "status": cs.STATUS_NAMES[rc]}))
+    plan.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile(args)
     import torch
     import torch.distributed as dist
 
@@ -299,9 +345,9 @@ def main():
     t_end = time.time() + 1.0
     while time.time() < t_end:
         for _ in range(20):
-            plans["refine"].execute(stream)
+            plans["fp64"].execute(stream)
         stream.synchronize()
-    for name in ("refine", "fp64"):
+    for name in ("fp64", "refine"):
         results[name] = time_plan(plans[name], args.steps, args.warmup)
     clk = clocks.stop()
     for name in ("refine_scalar", "fp64_scalar", "refine_block", "fp64_block"):
@@ -320,8 +366,8 @@ def main():
                 "traffic": tr, "algorithmic_bytes_per_launch": bytes_scalar, "ms_per_launch": ms,
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s"}
 
-    value = world * unknowns / (results["refine"] * 1e-3)
-    v64 = world * unknowns / (results["fp64"] * 1e-3)
+    vref = world * unknowns / (results["refine"] * 1e-3)
+    value = world * unknowns / (results["fp64"] * 1e-3)
     launches_per_step = plans["refine"].launches
 
     # ---- end to end through the host-pointer C ABI (rank-local, pinned buffers)
@@ -354,8 +400,6 @@ def main():
                 hb.append(nv)
         h2d = sum(4 * a.nbytes for (a, *_r) in hs) + (sum(v.nbytes for v in hb[:4]) if hb else 0)
         d2h = sum(arr[4].nbytes for arr in hs) + (hb[4].nbytes if hb else 0)
-        cs.set_host_precision(cs.TG_PREC_F32_REFINE)
-
         def e2e_step():
             for (a, b, c, f, x) in hs:
                 cs.trsolv_ng(a, b, c, f, x, a.shape[0])
@@ -371,11 +415,10 @@ def main():
             e2e_step()
         torch.cuda.synchronize()
         dt = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps)
-        cs.set_host_precision(cs.TG_PREC_F64)
         e2e_unk = cpu_unknowns([tuple(h[:4]) for h in hs], tuple(hb[:4]) if hb else None)
         e2e = {"value": world * e2e_unk / dt, "unit": "unknowns/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3, "steps": args.e2e_steps,
-               "path": "tg_trsolv_ng x7 + tg_blksolve, pinned host Fortran-layout arrays, refine precision",
+               "path": "tg_trsolv_ng x7 + tg_blksolve, pinned host Fortran-layout arrays, FP64",
                "timer": "host wall clock around synchronous C-ABI calls"}
         del keep
 
@@ -389,20 +432,21 @@ def main():
 
     if rank == 0:
         out = {
-            "metric": "column unknowns/s (FP32+FP64-refine; FP64 beside it)",
+            "metric": "column unknowns/s (FP64 path; FP32+FP64-refine path beside it, <=1e-10 rel err)",
             "value": value, "unit": "unknowns/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": results["refine"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 sweeps + f64 refinement (f64 I/O)", "data": "synthetic (seeded, generated on device)",
+            "ms_per_step": results["fp64"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded, generated on device)",
             "config": {"workload": wl.name, "grids": [(g.name, g.nlon, g.nlat, g.nk, g.nsub if args.max_sub is None else min(g.nsub, args.max_sub)) for g in wl.grids],
                        "systems_per_column": wl.n_scalar + (1 if wl.block else 0), "block": wl.block,
                        "unknowns_per_step_per_gpu": unknowns, "segments": len(segs),
                        "l2": f"inputs {dw.input_bytes() / 1e9:.3f} GB per step > 126 MB L2 (no flush needed)",
                        "parallelism": f"{world} GPU(s), independent column batches per GPU"},
-            "roofline": roofline("refine", "k_scalar_refine"),
-            "fp64": {"value": v64, "ms_per_step": results["fp64"], "roofline": roofline("fp64", "k_scalar_f64"),
-                     "status": cs.STATUS_NAMES[rc64]},
-            "refine": {"value": value, "refine_over_fp64": value / v64, "max_rel_err_vs_fp64": max_rel,
-                       "sweep_histogram": hist, "status": cs.STATUS_NAMES[rc_ref]},
+            "roofline": roofline("fp64", "k_scalar_f64"),
+            "fp64": {"value": value, "ms_per_step": results["fp64"], "status": cs.STATUS_NAMES[rc64]},
+            "refine": {"value": vref, "ms_per_step": results["refine"], "refine_over_fp64": vref / value,
+                       "max_rel_err_vs_fp64": max_rel, "sweep_histogram": hist, "status": cs.STATUS_NAMES[rc_ref],
+                       "dtype": "f32 sweeps + f64 residual/update (f64 I/O)",
+                       "roofline": roofline("refine", "k_scalar_refine")},
             "kernel_ms": {k: v for k, v in results.items()},
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -156,6 +156,35 @@ int tg_blksolve_dev_noalloc(int B, const double *P, const double *Q, const doubl
                             double *u, int nk, int k2, int ncol, long ld, int *status_dev,
                             void *stream);
 
+/* ---- fused column assembly + solve ------------------------------------------
+ * dt_ng's vertical column step (src/dt_ng.F90:57-167): the neutral-
+ * temperature coefficients p, q, r, rhs are assembled per column from the
+ * physical fields and solved (rows 1..nk-1, trsolv_ng), and row nk is set to
+ * tn(nk-1)**2/tn(nk-2).  The horizontal operators stay in the host model:
+ * horadv = advec_ng(tn) and tnsmooth = smooth_ng(tn_nm) are inputs.
+ * tlbc is the previous step's lower-boundary Tn (the routine's tlbc
+ * argument), t_lbc the current one.  3-D fields (nk, ncol); 2-D (ncol);
+ * expz, dift (nk).  nk >= 3.  Results are bit-identical to the reference's
+ * FP64 arithmetic. */
+typedef struct {
+    const double *tn, *tnsmooth, *horadv, *un, *vn, *o1, *mbar, *xnmbar, *scht, *schti, *cp, *kt,
+        *km, *hdt, *qji_tn, *cool_imp, *cool_exp, *w, *qtotal, *rkm12;
+    const double *tlbc, *t_lbc, *ulbc, *vlbc;
+    const double *expz, *dift;
+} tg_dt_fields;
+
+typedef struct {
+    double dz, dtx2inv, expzmid_inv, grav, p0, avo, gask, tsurplus, rmassinv_o1;
+} tg_dt_consts;
+
+/* Host arrays in the Fortran layout, synchronous. */
+int tg_dt_ng(const tg_dt_fields *F, const tg_dt_consts *C, double *tn_upd, int nk, int ncol);
+/* Device arrays, level-major (3-D field (k,col) at k*ld + col).  If
+ * system_out is not NULL it receives the assembled rows 1..nk-1 (after the
+ * lower-boundary fold) as four level-major planes p, q, r, rhs of nk*ld each. */
+int tg_dt_ng_dev(const tg_dt_fields *F, const tg_dt_consts *C, double *tn_upd, int nk, int ncol, long ld,
+                 double *system_out, int *status_dev, void *stream);
+
 /* ---- batched, GPU-resident plans ---------------------------------------------
  * A plan solves many independent systems ("segments": any mix of grids, nest
  * levels, sub-steps and species) in one persistent launch per system kind,
@@ -209,6 +238,28 @@ int tg_set_host_precision(int precision);
 /* Launch shape of a kind/precision: columns per thread block (32..512, a
  * multiple of 32) and columns per thread (1 or 2); 0 restores the default. */
 int tg_set_tile(int kind, int precision, int cols_per_block, int cols_per_thread);
+/* Coefficient staging of the FP64 kernels of a kind: 0 = register-prefetch
+ * kernel (shape from tg_set_tile); 4, 8 or 16 = depth in levels of the
+ * shared-memory ring that bulk asynchronous copies fill ahead of the sweep
+ * (one warp per 32 columns; used when the level-major column stride is a
+ * multiple of 32 and the arrays are 16-byte aligned, otherwise the
+ * register-prefetch kernel runs); -1 restores the default. */
+int tg_set_pipeline(int kind, int precision, int stages);
+/* Depth (levels) of the register prefetch of the scalar kernels' coefficient
+ * loads: 4, 8 or 16 (kind TG_KIND_SCALAR, either precision); -1 restores the
+ * default.  Deeper prefetch keeps more bytes in flight per column at the cost
+ * of registers. */
+int tg_set_prefetch(int kind, int precision, int levels);
+/* Where the scalar FP64 register-prefetch kernel keeps its forward-sweep
+ * quotients w2: 0 = shared memory (limits residency to ~8 B x nk per column
+ * of shared memory), 1 = a library-owned global scratch that stays in L2
+ * (residency then limited only by registers); -1 restores the default.
+ * Only kind TG_KIND_SCALAR with TG_PREC_F64. */
+int tg_set_scratch_global(int kind, int precision, int on);
+/* Test entry: q[i] = a[i]/b[i] (device arrays, n elements) computed by the
+ * kernels' division routine (Markstein's correction of the correctly rounded
+ * reciprocal, IEEE division outside its safe range); must equal IEEE a/b. */
+int tg_selftest_division(const double *a, const double *b, double *q, long n, void *stream);
 /* Frees the per-device mirrors, work buffers and streams. */
 int tg_release_buffers(void);
 /* Library version, e.g. "tg_colsolve 0.1.0 sm_100a". */

@@ -129,3 +129,38 @@ def blktri(a, b, c, f, x, lev0, lev1, lon0, lon1, nlonp4):
     x = _fcopy(x).copy(order="F")
     lib().oracle_blktri(_p(a), _p(b), _p(c), _p(f), _p(x), lev0, lev1, lon0, lon1, nlonp4)
     return x
+
+
+# ---- dt_ng column assembly ----------------------------------------------------
+DT_FIELD_ORDER = ("tn", "tnsmooth", "horadv", "un", "vn", "o1", "mbar", "xnmbar", "scht", "schti", "cp", "kt",
+                  "km", "hdt", "qji_tn", "cool_imp", "cool_exp", "w", "qtotal", "rkm12",
+                  "tlbc", "t_lbc", "ulbc", "vlbc", "expz", "dift")
+DT_CONST_ORDER = ("dz", "dtx2inv", "expzmid_inv", "grav", "p0", "avo", "gask", "tsurplus", "rmassinv_o1")
+
+
+class DtFields(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in DT_FIELD_ORDER]
+
+
+class DtConsts(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in DT_CONST_ORDER]
+
+
+def dt_ng(fields, consts, with_system=False):
+    """dt_ng assembly + solve (src/dt_ng.F90:57-167); returns tn_upd and, if
+    with_system, (p, q, r, rhs) rows 1..nk-1."""
+    L = lib()
+    if not hasattr(L, "_dt_bound"):
+        L.oracle_dt_ng.argtypes = [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), ctypes.c_int,
+                                   ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_dt_ng.restype = None
+        L._dt_bound = True
+    arrs = {k: _fcopy(fields[k]) for k in DT_FIELD_ORDER}
+    nk, ncol = arrs["tn"].shape[0], arrs["tn"].size // arrs["tn"].shape[0]
+    F = DtFields(*[arrs[k].ctypes.data for k in DT_FIELD_ORDER])
+    C = DtConsts(*[float(consts[k]) for k in DT_CONST_ORDER])
+    tn_upd = np.zeros((nk, ncol), order="F")
+    sysarr = [np.zeros((nk, ncol), order="F") for _ in range(4)] if with_system else [None] * 4
+    L.oracle_dt_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(s) for s in sysarr], _p(tn_upd))
+    return (tn_upd, tuple(sysarr)) if with_system else tn_upd

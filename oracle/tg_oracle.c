@@ -407,3 +407,271 @@ ORACLE_API int oracle_max_threads(void)
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------------ */
+/* dt_ng neutral-temperature column assembly + solve (src/dt_ng.F90:57-167). */
+/* Fields are (nk, ncol); 2-D fields (ncol); expz, dift (nk).  The outputs   */
+/* of the horizontal operators (horadv = advec_ng(tn), tnsmooth =            */
+/* smooth_ng(tn_nm)) are inputs.  tlbc is the previous step's lower-boundary  */
+/* Tn (the routine's tlbc argument, dt_ng.F90:126), t_lbc the current one.   */
+/* p, q, r, rhs (may be NULL) receive rows 1..nk-1 of the assembled system  */
+/* after the LBC fold; tn_upd rows 1..nk (row nk from dt_ng.F90:167).        */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    double dz, dtx2inv, expzmid_inv, grav, p0, avo, gask, tsurplus, rmassinv_o1;
+} oracle_dt_consts;
+
+typedef struct {
+    const double *tn, *tnsmooth, *horadv, *un, *vn, *o1, *mbar, *xnmbar, *scht, *schti, *cp, *kt, *km,
+        *hdt, *qji_tn, *cool_imp, *cool_exp, *w, *qtotal, *rkm12;   /* (nk, ncol) */
+    const double *tlbc, *t_lbc, *ulbc, *vlbc;                          /* (ncol)     */
+    const double *expz, *dift;                                         /* (nk)       */
+} oracle_dt_fields;
+
+ORACLE_API void oracle_dt_ng(const oracle_dt_fields *F, const oracle_dt_consts *C, int nk, long ncol,
+                             double *p_out, double *q_out, double *r_out, double *rhs_out, double *tn_upd)
+{
+    double *w = (double *)malloc(sizeof(double) * 17 * (size_t)nk);
+    double *vad = w, *cpi = w + nk, *kmi = w + 2 * nk, *wi = w + 3 * nk, *dudz = w + 4 * nk,
+           *dvdz = w + 5 * nk, *qsolar = w + 6 * nk, *tni = w + 7 * nk, *g = w + 8 * nk, *f = w + 9 * nk,
+           *p = w + 10 * nk, *q = w + 11 * nk, *r = w + 12 * nk, *rhs = w + 13 * nk, *ws = w + 14 * nk;
+    const double dz = C->dz, dtx2inv = C->dtx2inv;
+    long col;
+    int k;
+    for (col = 0; col < ncol; ++col) {
+        const size_t o = (size_t)nk * col;
+        const double *tn = F->tn + o, *ww = F->w + o, *cp = F->cp + o, *km = F->km + o, *un = F->un + o,
+                     *vn = F->vn + o, *qt = F->qtotal + o;
+        /* vertical advection (dt_ng.F90:57-64) */
+        vad[0] = (tn[0] - F->t_lbc[col]) * ww[0] * 2.;
+        vad[nk - 1] = 0.;
+        for (k = 1; k < nk - 1; ++k) vad[k] = (tn[k] - tn[k - 1]) * ww[k];
+        for (k = 0; k < nk - 1; ++k) vad[k] = (vad[k] + vad[k + 1]) * .5;
+        for (k = 0; k < nk; ++k) vad[k] = vad[k] / dz;
+        /* interface averages (:72-79) */
+        for (k = 0; k < nk - 1; ++k) {
+            cpi[k] = .5 * (cp[k] + cp[k + 1]);
+            kmi[k] = .5 * (km[k] + km[k + 1]);
+            wi[k] = .5 * (ww[k] + ww[k + 1]);
+        }
+        cpi[nk - 1] = 1.5 * cp[nk - 1] - .5 * cp[nk - 2];
+        kmi[nk - 1] = 1.5 * km[nk - 1] - .5 * km[nk - 2];
+        wi[nk - 1] = 1.5 * ww[nk - 1] - .5 * ww[nk - 2];
+        /* wind shear (:86-95) */
+        for (k = 1; k < nk - 2; ++k) {
+            dudz[k] = (un[k + 1] - un[k - 1]) / (2. * dz);
+            dvdz[k] = (vn[k + 1] - vn[k - 1]) / (2. * dz);
+        }
+        dudz[0] = (un[0] + 1. / 3. * un[1] - 4. / 3. * F->ulbc[col]) / dz;
+        dvdz[0] = (vn[0] + 1. / 3. * vn[1] - 4. / 3. * F->vlbc[col]) / dz;
+        dudz[nk - 2] = dudz[nk - 3] / 3.;
+        dvdz[nk - 2] = dvdz[nk - 3] / 3.;
+        dudz[nk - 1] = dudz[nk - 2] / 3.;
+        dvdz[nk - 1] = dvdz[nk - 2] / 3.;
+        for (k = 0; k < nk - 1; ++k) qsolar[k] = .5 * (qt[k] + qt[k + 1]);
+        qsolar[nk - 1] = 1.5 * qt[nk - 1] - .5 * qt[nk - 2];
+        /* tni (:120-124), conductivity terms (:126-148) */
+        for (k = 1; k < nk - 1; ++k) tni[k] = .5 * (tn[k - 1] + tn[k]);
+        tni[0] = F->tlbc[col];
+        tni[nk - 1] = tn[nk - 2];
+        for (k = 0; k < nk; ++k) {
+            const double h = F->schti[o + k];
+            double rho = C->p0 * C->expzmid_inv / (h * C->grav);
+            rho = rho * F->expz[k];
+            double gpart = h * h * rho * cp[k];
+            gpart = gpart * F->dift[k];
+            g[k] = C->grav * (F->kt[o + k] + gpart) / (C->p0 * h * (dz * dz));
+            double ff = C->grav * C->grav * (h * h) * rho / (tni[k] * C->p0 * 2. * dz);
+            f[k] = ff * F->dift[k];
+        }
+        for (k = 0; k < nk - 1; ++k) {
+            p[k] = g[k] - f[k];
+            q[k] = -(g[k + 1] - f[k + 1] + g[k] + f[k]);
+            r[k] = g[k + 1] + f[k + 1];
+        }
+        q[nk - 2] = -g[nk - 2] - f[nk - 2];
+        r[nk - 2] = 0.;
+        /* right-hand side and implicit part (:81-84, :97-118, :150-163) */
+        for (k = 0; k < nk - 1; ++k) {
+            const size_t i = o + k;
+            const double advec = F->horadv[i] + vad[k];
+            double cptn = cpi[k] * (advec - dtx2inv * F->tnsmooth[i]);
+            cptn = cptn * F->expz[k];
+            const double x = F->xnmbar[i] * F->o1[i] * C->rmassinv_o1;
+            const double qrecomb = C->tsurplus * F->rkm12[i] * (x * x) * C->avo / F->mbar[i];
+            double qm = C->grav * kmi[k] / (C->p0 * F->scht[i]) * (dudz[k] * dudz[k] + dvdz[k] * dvdz[k]);
+            qm = qm / F->expz[k];
+            const double th = qsolar[k] + F->hdt[i] + qrecomb + F->qji_tn[i] + qm;
+            cptn = cptn - th * F->expz[k];
+            rhs[k] = cptn + F->cool_exp[i];
+            const double qpart = cpi[k] * (dtx2inv + F->cool_imp[i]) + wi[k] * C->gask / F->mbar[i];
+            q[k] = q[k] - qpart * F->expz[k];
+        }
+        q[0] = q[0] - p[0];
+        rhs[0] = rhs[0] - 2. * p[0] * F->t_lbc[col];
+        p[0] = 0.;
+        if (p_out)
+            for (k = 0; k < nk - 1; ++k) {
+                p_out[o + k] = p[k];
+                q_out[o + k] = q[k];
+                r_out[o + k] = r[k];
+                rhs_out[o + k] = rhs[k];
+            }
+        /* trsolv_ng(p,q,r,rhs,tn_upd,nk-1) and the top row (:165-167) */
+        thomas_column(p, q, r, rhs, tn_upd + o, nk - 1, ws);
+        tn_upd[o + nk - 1] = tn_upd[o + nk - 2] * tn_upd[o + nk - 2] / tn_upd[o + nk - 3];
+    }
+    free(w);
+}
+
+/* ------------------------------------------------------------------------ */
+/* minor_ng minor-species column assembly + solve (src/minor_ng.F90:60-200), */
+/* used for N4S, NO, N2D and Ar.  Fields (nk, ncol); 2-D (ncol); expz, difk  */
+/* (nk).  hadvec = advec_ng(fcomp) and ftm1_smooth = smooth_ng(fcomp_tm1)    */
+/* are inputs (horizontal operators), dfactor the latitude factor of         */
+/* minor_ng.F90:146-155 per column.  b (3x3, column-major) and fb (3) are the */
+/* lower-boundary relation of the lbc module.  p,q,r,f (may be NULL) receive */
+/* rows 1..nk after the boundary folds; fcomp_out rows 1..nk (k2 = nk).       */
+/* ------------------------------------------------------------------------ */
+#include <math.h>
+
+typedef struct {
+    const double *tn, *o2, *o1, *he, *mbar, *barm, *xnmbar, *w, *ftm1_smooth, *hadvec, *sloss, *sprod;
+    const double *tlbc, *flbc1, *flbc2, *flbc3, *fubc, *dfactor;
+    const double *expz, *difk;
+} oracle_minor_fields;
+
+typedef struct {
+    double rmx, alfax, phix[4], dzp, dtx2inv, expzmid, expzmid_inv;
+    double rmassinv_o2, rmassinv_o1, rmassinv_n2, rmassinv_he;
+    double rmass_o2, rmass_o1, rmass_he, rmass_n2, p0, grav, avo;
+    double b[9], fb[3];
+} oracle_minor_consts;
+
+/* phi(3,4) and ss(3) of minor_ng.F90:25-28 (column-major phi(i,j) = PHI[i-1][j-1]) */
+static const double MPHI[3][4] = {{0., 1.35, 2.16, 1.11}, {0.673, 0., 1.616, 0.769}, {0.270, 0.404, 0., 0.322}};
+static const double MSS[3] = {1.710, 1.749, 1.718};
+
+ORACLE_API void oracle_minor_ng(const oracle_minor_fields *F, const oracle_minor_consts *C, int nk, long ncol,
+                                double *p_out, double *q_out, double *r_out, double *f_out, double *fcomp_out)
+{
+    const double tau = 1.86e+3, t00 = 273.;
+    const double dzp = C->dzp;
+    double salfax[3];
+    double *w = (double *)malloc(sizeof(double) * 24 * (size_t)nk);
+    double *dmdz = w, *pso1 = w + nk, *pso2 = w + 2 * nk, *pshe = w + 3 * nk, *do1dz = w + 4 * nk,
+           *do2dz = w + 5 * nk, *dhedz = w + 6 * nk, *tni = w + 7 * nk, *sa1 = w + 8 * nk, *sa2 = w + 9 * nk,
+           *sa3 = w + 10 * nk, *ex = w + 11 * nk, *ax = w + 12 * nk, *thdiff = w + 13 * nk, *wi = w + 14 * nk,
+           *p = w + 15 * nk, *q = w + 16 * nk, *r = w + 17 * nk, *f = w + 18 * nk, *ws = w + 19 * nk;
+    long col;
+    int k, n;
+    for (n = 0; n < 3; ++n) salfax[n] = C->phix[n] - C->phix[3];
+    for (col = 0; col < ncol; ++col) {
+        const size_t o = (size_t)nk * col;
+        const double *tn = F->tn + o, *o2 = F->o2 + o, *o1 = F->o1 + o, *he = F->he + o, *mbar = F->mbar + o,
+                     *barm = F->barm + o, *ww = F->w + o;
+        /* lower-boundary mixing ratios (:72-75) */
+        const double bo2 = C->b[0] * o2[0] + C->b[3] * o1[0] + C->b[6] * he[0] + C->fb[0];
+        const double bo1 = C->b[1] * o2[0] + C->b[4] * o1[0] + C->b[7] * he[0] + C->fb[1];
+        const double bhe = C->b[2] * o2[0] + C->b[5] * o1[0] + C->b[8] * he[0] + C->fb[2];
+        const double xmbari = 1. / (bo2 * C->rmassinv_o2 + bo1 * C->rmassinv_o1 +
+                                    (1. - bo2 - bo1 - bhe) * C->rmassinv_n2 + bhe * C->rmassinv_he);
+        /* interface quantities (:77-96) */
+        dmdz[0] = (mbar[0] - xmbari) / dzp;
+        pso1[0] = .5 * (bo1 + o1[0]);
+        pso2[0] = .5 * (bo2 + o2[0]);
+        pshe[0] = .5 * (bhe + he[0]);
+        do1dz[0] = (o1[0] - bo1) / dzp;
+        do2dz[0] = (o2[0] - bo2) / dzp;
+        dhedz[0] = (he[0] - bhe) / dzp;
+        for (k = 1; k < nk; ++k) {
+            dmdz[k] = (mbar[k] - mbar[k - 1]) / dzp;
+            pso1[k] = .5 * (o1[k] + o1[k - 1]);
+            pso2[k] = .5 * (o2[k] + o2[k - 1]);
+            pshe[k] = .5 * (he[k] + he[k - 1]);
+            do1dz[k] = (o1[k] - o1[k - 1]) / dzp;
+            do2dz[k] = (o2[k] - o2[k - 1]) / dzp;
+            dhedz[k] = (he[k] - he[k - 1]) / dzp;
+        }
+        tni[0] = F->tlbc[col];
+        tni[nk - 1] = tn[nk - 2];
+        for (k = 1; k < nk - 1; ++k) tni[k] = .5 * (tn[k] + tn[k - 1]);
+        /* alfa matrix, its inverse, salfax . invalfa(:,n) (:100-133) */
+        for (k = 0; k < nk; ++k) {
+            double df[3], A[9], Ai[9];
+            for (n = 0; n < 3; ++n) df[n] = pow(tni[k] / t00, 1.75 - MSS[n]);
+#define PH(i, j) MPHI[(i) - 1][(j) - 1]
+            M3(A, 1, 1) = -(PH(1, 4) + (PH(1, 2) - PH(1, 4)) * pso1[k] + (df[0] * PH(1, 3) - PH(1, 4)) * pshe[k]);
+            M3(A, 2, 2) = -(PH(2, 4) + (PH(2, 1) - PH(2, 4)) * pso2[k] + (df[1] * PH(2, 3) - PH(2, 4)) * pshe[k]);
+            M3(A, 3, 3) = -(df[2] * PH(3, 4) + (df[0] * PH(3, 1) - df[2] * PH(3, 4)) * pso2[k] +
+                           (df[1] * PH(3, 2) - df[2] * PH(3, 4)) * pso1[k]);
+            M3(A, 1, 2) = (PH(1, 2) - PH(1, 4)) * pso2[k];
+            M3(A, 1, 3) = (df[0] * PH(1, 3) - PH(1, 4)) * pso2[k];
+            M3(A, 2, 1) = (PH(2, 1) - PH(2, 4)) * pso1[k];
+            M3(A, 2, 3) = (df[1] * PH(2, 3) - PH(2, 4)) * pso1[k];
+            M3(A, 3, 1) = (df[0] * PH(3, 1) - df[2] * PH(3, 4)) * pshe[k];
+            M3(A, 3, 2) = (df[1] * PH(3, 2) - df[2] * PH(3, 4)) * pshe[k];
+            oracle_matinv3(A, Ai);
+            sa1[k] = salfax[0] * M3(Ai, 1, 1) + salfax[1] * M3(Ai, 2, 1) + salfax[2] * M3(Ai, 3, 1);
+            sa2[k] = salfax[0] * M3(Ai, 1, 2) + salfax[1] * M3(Ai, 2, 2) + salfax[2] * M3(Ai, 3, 2);
+            sa3[k] = salfax[0] * M3(Ai, 1, 3) + salfax[1] * M3(Ai, 2, 3) + salfax[2] * M3(Ai, 3, 3);
+        }
+        /* ex, ax, thdiff (:135-153) */
+        for (k = 0; k < nk; ++k) {
+            ex[k] = 1. - (C->rmx + dmdz[k]) / barm[k] +
+                    sa1[k] * (do2dz[k] - (1. - (C->rmass_o2 + dmdz[k]) / barm[k]) * pso2[k]) +
+                    sa2[k] * (do1dz[k] - (1. - (C->rmass_o1 + dmdz[k]) / barm[k]) * pso1[k]) +
+                    sa3[k] * (dhedz[k] - (1. - (C->rmass_he + dmdz[k]) / barm[k]) * pshe[k]);
+            dmdz[k] = dmdz[k] / barm[k];
+            ax[k] = -(barm[k] / (tau * C->rmass_n2) * pow(t00 / tni[k], 0.25) /
+                      (C->phix[2] + salfax[0] * pso2[k] + salfax[1] * pso1[k] + salfax[2] * pshe[k]));
+        }
+        for (k = 0; k < nk; ++k) {
+            double dt;
+            if (k == 0) dt = tni[1] - tni[0];
+            else if (k == nk - 1) dt = tni[nk - 1] - tni[nk - 2];
+            else dt = (tni[k + 1] - tni[k - 1]) / 2.;
+            thdiff[k] = ex[k] - C->alfax * dt / (dzp * tni[k]);
+        }
+        for (k = 0; k < nk - 1; ++k) wi[k] = .5 * (ww[k] + ww[k + 1]);
+        wi[nk - 1] = 1.5 * ww[nk - 1] - .5 * ww[nk - 2];
+        /* p, q, r, f (:161-198) */
+        const double dfac = F->dfactor[col];
+        for (k = 0; k < nk - 1; ++k) {
+            const double molp = ax[k] * (1. / dzp + .5 * thdiff[k]);
+            const double molr = ax[k + 1] * (1. / dzp - .5 * thdiff[k + 1]);
+            const double molq = ax[k] * (1. / dzp - .5 * thdiff[k]) + ax[k + 1] * (1. / dzp + .5 * thdiff[k + 1]);
+            const double eddyp = C->expzmid_inv * F->difk[k] * (1. / dzp - .5 * dmdz[k]);
+            const double eddyr = C->expzmid * F->difk[k + 1] * (1. / dzp + .5 * dmdz[k + 1]);
+            const double eddyq = C->expzmid_inv * F->difk[k] * (1. / dzp + .5 * dmdz[k]) +
+                                 C->expzmid * F->difk[k + 1] * (1. / dzp - .5 * dmdz[k + 1]);
+            p[k] = molp / dzp - F->expz[k] * (eddyp * dfac + .5 * wi[k]) / dzp;
+            r[k] = molr / dzp - F->expz[k] * (eddyr * dfac - .5 * wi[k]) / dzp;
+            q[k] = -molq / dzp + F->expz[k] * (eddyq * dfac / dzp + C->dtx2inv - F->sloss[o + k]);
+        }
+        for (k = 0; k < nk; ++k) {
+            const double s0prod = F->sprod[o + k] * C->rmx / F->xnmbar[o + k];
+            f[k] = F->ftm1_smooth[o + k] * C->dtx2inv - F->hadvec[o + k] + s0prod;
+            f[k] = f[k] * F->expz[k];
+        }
+        {
+            const double l1 = F->flbc1[col], l2 = F->flbc2[col], l3 = F->flbc3[col];
+            q[0] = q[0] + p[0] * (l1 + .5 * l2 * dzp) / (l1 - .5 * l2 * dzp);
+            f[0] = f[0] - p[0] * l3 * dzp / (l1 - .5 * l2 * dzp);
+            p[0] = 0.;
+        }
+        p[nk - 1] = 1. + .5 * dzp * thdiff[nk - 1];
+        q[nk - 1] = p[nk - 1] - 2.;
+        r[nk - 1] = 0.;
+        f[nk - 1] = -C->grav * C->rmx * F->fubc[col] * dzp / (C->p0 * ax[nk - 1] * C->avo);
+        if (p_out)
+            for (k = 0; k < nk; ++k) {
+                p_out[o + k] = p[k];
+                q_out[o + k] = q[k];
+                r_out[o + k] = r[k];
+                f_out[o + k] = f[k];
+            }
+        thomas_column(p, q, r, f, fcomp_out + o, nk, ws);
+    }
+    free(w);
+}

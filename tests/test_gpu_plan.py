@@ -126,3 +126,39 @@ def test_device_workload_nested(cuda, pkg, orc):
             ref = orc.blksolve(P, Q, R, f, it["k2"])
             assert np.array_equal(pkg.batch.from_level_vector(it["x"], n), ref)
     plan.close()
+
+
+@pytest.mark.parametrize("kind", [0, 2, 3])
+def test_every_launch_variant_bit_exact(cuda, pkg, orc, kind):
+    """Each launch shape the autotuner may choose (register-prefetch shapes,
+    bulk-copy rings of depth 4/8/16) gives the oracle's bits."""
+    torch = cuda
+    from tiegcm_ng_b200 import autotune
+    specs = [(kind, 57, 57, 1000), (kind, 29, 28, 77), (kind, 113, 113, 40), (kind, 57, 56, 31)]
+    segs, refs_in = make_segments(pkg, torch, specs, seed=300 + kind)
+    try:
+        for cand in autotune.candidates(kind, pkg.TG_PREC_F64):
+            autotune.apply(kind, pkg.TG_PREC_F64, cand)
+            for s in segs:
+                s["x"].fill_(3.5)
+            plan = pkg.Plan(segs, pkg.TG_PREC_F64)
+            plan.execute()
+            rc, per = plan.status()
+            plan.close()
+            assert rc == pkg.TG_OK, cand
+            check(pkg, orc, segs, refs_in)
+    finally:
+        autotune.reset(kind, pkg.TG_PREC_F64)
+
+
+def test_ring_kernel_with_unaligned_stride_falls_back(cuda, pkg, orc):
+    """A column stride that is not a multiple of 32 cannot use the bulk-copy
+    ring; the register-prefetch kernel runs instead, same bits."""
+    torch = cuda
+    a, b, c, f = pkg.synth.scalar_system(57, 1000, 0.25, 5)
+    ld = 1001
+    t = [pkg.batch.level_scalar(v, ld, "cuda") for v in (a, b, c, f)]
+    x = torch.zeros((57, ld), dtype=torch.float64, device="cuda")
+    pkg.trsolv_dev(*t, x, 57, 57, 1000, pkg.TG_LAYOUT_LEVEL, ld)
+    torch.cuda.synchronize()
+    assert np.array_equal(pkg.batch.from_level_scalar(x, 1000), orc.trsolv_ng(a, b, c, f, 57))

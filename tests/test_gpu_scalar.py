@@ -111,12 +111,14 @@ def test_two_columns_per_thread(cuda, pkg, orc):
     ld = 800
     ta, tb, tc, tf = (pkg.batch.level_scalar(v, ld, "cuda") for v in (a, b, c, f))
     tx = torch.zeros((nk, ld), dtype=torch.float64, device="cuda")
+    cs.set_pipeline(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 0)
     cs.set_tile(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 128, 2)
     try:
         pkg.trsolv_dev(ta, tb, tc, tf, tx, nk, nk, 777, pkg.TG_LAYOUT_LEVEL, ld)
         torch.cuda.synchronize()
     finally:
         cs.set_tile(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 0, 0)
+        cs.set_pipeline(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, -1)
     assert np.array_equal(pkg.batch.from_level_scalar(tx, 777), ref)
     assert torch.all(tx[:, 777:] == 0)  # padding columns are not written
 
@@ -135,3 +137,28 @@ def test_refine_accuracy(cuda, pkg, orc, cfg):
     x = pkg.batch.from_level_scalar(tx, 2000)
     assert rel_err(x, ref) <= 1e-10
     assert int(st.item()) in (pkg.TG_OK, pkg.TG_ENOCONV)
+
+
+def test_division_routine_matches_ieee(cuda, pkg):
+    """The kernels divide by a shared correctly rounded reciprocal with
+    Markstein's correction; every quotient must equal IEEE a/b exactly."""
+    torch = cuda
+    rng = np.random.default_rng(99)
+    n = 1 << 21
+    a = rng.standard_normal(n) * np.exp2(rng.integers(-60, 60, n))
+    b = rng.standard_normal(n) * np.exp2(rng.integers(-60, 60, n))
+    # wide exponents, near-equal operands, exact quotients and edge values
+    a[:4096] = rng.uniform(0.5, 1.0, 4096) * np.exp2(rng.integers(-1000, 1000, 4096))
+    b[:4096] = rng.uniform(0.5, 1.0, 4096) * np.exp2(rng.integers(-1000, 1000, 4096))
+    a[4096:8192] = b[4096:8192] * rng.integers(-1000, 1000, 4096)
+    a[8192:8192 + 16] = [0.0, -0.0, np.inf, -np.inf, np.nan, 1e-310, 5e-324, 1e308, 1.0, 3.0, 1.0, -7.0, 2.0, 1e-300, 1e300, 0.0]
+    b[8192:8192 + 16] = [3.0, 3.0, 2.0, 2.0, 1.0, 3.0, 7.0, 1e-10, 0.0, -0.0, np.inf, 1e-310, 5e-324, 1e300, 1e-300, np.nan]
+    ta, tb = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    tq = torch.empty_like(ta)
+    pkg.selftest_division(ta, tb, tq)
+    torch.cuda.synchronize()
+    q = tq.cpu().numpy()
+    with np.errstate(all="ignore"):
+        ref = a / b
+    same = (q.view(np.int64) == ref.view(np.int64)) | (np.isnan(q) & np.isnan(ref))
+    assert same.all(), (a[~same][:5], b[~same][:5], q[~same][:5], ref[~same][:5])

@@ -37,10 +37,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
-EXPORTS = ("tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
+EXPORTS = ("tg_dt_ng", "tg_dt_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_sweep_histogram", "tg_plan_destroy",
-           "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_release_buffers", "tg_version", "tg_last_error")
+           "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
 
 
 class TgError(RuntimeError):
@@ -58,6 +58,22 @@ class Segment(ctypes.Structure):
                 ("x", ctypes.c_void_p), ("ubc_ratio", ctypes.c_void_p), ("ubc_add", ctypes.c_void_p)]
 
 
+DT_FIELDS = ("tn", "tnsmooth", "horadv", "un", "vn", "o1", "mbar", "xnmbar", "scht", "schti", "cp", "kt", "km",
+             "hdt", "qji_tn", "cool_imp", "cool_exp", "w", "qtotal", "rkm12", "tlbc", "t_lbc", "ulbc", "vlbc",
+             "expz", "dift")
+DT_CONSTS = ("dz", "dtx2inv", "expzmid_inv", "grav", "p0", "avo", "gask", "tsurplus", "rmassinv_o1")
+
+
+class DtFields(ctypes.Structure):
+    """tg_dt_fields of include/tg_colsolve.h."""
+    _fields_ = [(n, ctypes.c_void_p) for n in DT_FIELDS]
+
+
+class DtConsts(ctypes.Structure):
+    """tg_dt_consts of include/tg_colsolve.h."""
+    _fields_ = [(n, ctypes.c_double) for n in DT_CONSTS]
+
+
 _lib = None
 
 
@@ -72,6 +88,8 @@ def lib():
         P, I, Lg, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_long, ctypes.c_double
         sig = {
             "tg_trsolv": [P, P, P, P, P, I, I, I, I, I, I, I],
+            "tg_dt_ng": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I],
+            "tg_dt_ng_dev": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I, Lg, P, P, P],
             "tg_trsolv_ng": [P, P, P, P, P, I, I, I],
             "tg_blktri": [P, P, P, P, P, I, I, I, I, I],
             "tg_comp_blksolve_ng": [I, P, P, P, P, P, P, P, I, I],
@@ -89,6 +107,10 @@ def lib():
             "tg_set_refine": [I, D],
             "tg_set_host_precision": [I],
             "tg_set_tile": [I, I, I, I],
+            "tg_set_pipeline": [I, I, I],
+            "tg_set_scratch_global": [I, I, I],
+            "tg_set_prefetch": [I, I, I],
+            "tg_selftest_division": [P, P, P, Lg, P],
             "tg_release_buffers": [],
             "tg_version": [],
             "tg_last_error": [],
@@ -205,6 +227,29 @@ def blksolve(P, Q, R, f, u, k2, ubc_ratio=None, ubc_add=None):
     return _check(rc, "tg_blksolve")
 
 
+def dt_ng(fields, consts, tn_upd):
+    """dt_ng's vertical column step (src/dt_ng.F90:57-167) on host arrays:
+    fields is a dict of the DT_FIELDS arrays (3-D (nk,ncol...) Fortran-ordered,
+    2-D (ncol...), expz/dift (nk)), consts a dict of DT_CONSTS; tn_upd
+    (nk, ...) receives the solution."""
+    nk = tn_upd.shape[0]
+    ncol = tn_upd.size // nk
+    F = DtFields(*[_host(fields[n], n) for n in DT_FIELDS])
+    C = DtConsts(*[float(consts[n]) for n in DT_CONSTS])
+    rc = lib().tg_dt_ng(ctypes.byref(F), ctypes.byref(C), _out(tn_upd, "tn_upd"), nk, ncol)
+    return _check(rc, "tg_dt_ng")
+
+
+def dt_ng_dev(fields, consts, tn_upd, nk, ncol, ld, system_out=None, status=None, stream=None):
+    """Device form of dt_ng: fields are device pointers / CUDA tensors in the
+    level-major layout (3-D (nk, ld)); system_out (4*nk*ld) receives p,q,r,rhs."""
+    F = DtFields(*[_dptr(fields[n]) for n in DT_FIELDS])
+    C = DtConsts(*[float(consts[n]) for n in DT_CONSTS])
+    rc = lib().tg_dt_ng_dev(ctypes.byref(F), ctypes.byref(C), _dptr(tn_upd), nk, ncol, ld, _dptr(system_out),
+                            None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_dt_ng_dev", numeric_ok=False)
+
+
 # ---------------------------------------------------------------------------
 # Device entry points
 # ---------------------------------------------------------------------------
@@ -276,6 +321,28 @@ def set_host_precision(precision=TG_PREC_F64):
 def set_tile(kind, precision, cols_per_block=0, cols_per_thread=0):
     return _check(lib().tg_set_tile(kind, precision, cols_per_block, cols_per_thread), "tg_set_tile",
                   numeric_ok=False)
+
+
+def set_pipeline(kind, precision, stages=-1):
+    """Ring depth of the bulk-copy staged FP64 kernels (0: register prefetch,
+    -1: default)."""
+    return _check(lib().tg_set_pipeline(kind, precision, stages), "tg_set_pipeline", numeric_ok=False)
+
+
+def set_prefetch(kind, precision, levels=-1):
+    """Register prefetch depth (levels) of the scalar kernels: 4, 8, 16; -1 default."""
+    return _check(lib().tg_set_prefetch(kind, precision, levels), "tg_set_prefetch", numeric_ok=False)
+
+
+def set_scratch_global(kind, precision, on=-1):
+    """Scalar FP64 register kernel: w2 in global scratch (1) or shared memory (0)."""
+    return _check(lib().tg_set_scratch_global(kind, precision, on), "tg_set_scratch_global", numeric_ok=False)
+
+
+def selftest_division(a, b, q, stream=None):
+    """q = a/b on the device through the kernels' division routine."""
+    return _check(lib().tg_selftest_division(_dptr(a), _dptr(b), _dptr(q), int(q.numel()), _stream(stream)),
+                  "tg_selftest_division", numeric_ok=False)
 
 
 def release_buffers():

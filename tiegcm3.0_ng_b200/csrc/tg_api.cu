@@ -49,16 +49,19 @@ struct Buf {
     size_t n = 0;
 };
 
-// Per-device work buffers and streams, created on first use.
+// Per-device work buffers and streams, created on first use.  The host
+// drop-ins pipeline column chunks over kSlots streams, each with its own
+// buffers.
+constexpr int kSlots = 3;
 struct DevCtx {
     int dev = -1;
     std::mutex mu;
-    cudaStream_t st[2] = {nullptr, nullptr};
-    Buf colbuf[2][5];   // Fortran-layout staging: 4 inputs + output, per stream
-    Buf lvlbuf[2][7];   // level-major arrays: a,b,c,f,x,ubc_ratio,ubc_add, per stream
-    Buf scratch[2];     // block-kernel scratch, per stream
-    unsigned *flags = nullptr;           // device, 2 words (one per stream)
-    unsigned *flags_host = nullptr;      // pinned, 2 words
+    cudaStream_t st[kSlots] = {};
+    Buf colbuf[kSlots][5];   // Fortran-layout staging: 4 inputs + output, per slot
+    Buf lvlbuf[kSlots][7];   // level-major arrays: a,b,c,f,x,ubc_ratio,ubc_add, per slot
+    Buf scratch[kSlots];     // block-kernel scratch, per slot
+    unsigned *flags = nullptr;           // device, one word per slot
+    unsigned *flags_host = nullptr;      // pinned, one word per slot
     unsigned long long *hist = nullptr;  // device, kMaxSweepBins
 };
 
@@ -88,9 +91,9 @@ int get_ctx(DevCtx **out)
         DevCtx *c = new (std::nothrow) DevCtx;
         if (!c) return TG_ENOMEM;
         c->dev = dev;
-        for (int i = 0; i < 2; ++i) TG_CUDA(cudaStreamCreateWithFlags(&c->st[i], cudaStreamNonBlocking));
-        TG_CUDA(cudaMalloc(&c->flags, 2 * sizeof(unsigned)));
-        TG_CUDA(cudaMallocHost(&c->flags_host, 2 * sizeof(unsigned)));
+        for (int i = 0; i < kSlots; ++i) TG_CUDA(cudaStreamCreateWithFlags(&c->st[i], cudaStreamNonBlocking));
+        TG_CUDA(cudaMalloc(&c->flags, kSlots * sizeof(unsigned)));
+        TG_CUDA(cudaMallocHost(&c->flags_host, kSlots * sizeof(unsigned)));
         TG_CUDA(cudaMalloc(&c->hist, kMaxSweepBins * sizeof(unsigned long long)));
         g_ctx[dev] = c;
     }
@@ -122,6 +125,7 @@ int grow(Buf &b, size_t bytes)
 
 int flags_to_status(unsigned f)
 {
+    if (f & FLAG_TIMEOUT) return TG_ETIMEOUT;
     if (f & FLAG_PIVOT) return TG_EPIVOT;
     if (f & FLAG_NONFINITE) return TG_ENONFINITE;
     if (f & FLAG_NOCONV) return TG_ENOCONV;
@@ -131,7 +135,7 @@ int flags_to_status(unsigned f)
 __global__ void k_finish_status(const unsigned *flags, int *out)
 {
     const unsigned f = *flags;
-    *out = (f & FLAG_PIVOT) ? TG_EPIVOT : (f & FLAG_NONFINITE) ? TG_ENONFINITE : (f & FLAG_NOCONV) ? TG_ENOCONV : TG_OK;
+    *out = (f & FLAG_TIMEOUT) ? TG_ETIMEOUT : (f & FLAG_PIVOT) ? TG_EPIVOT : (f & FLAG_NONFINITE) ? TG_ENONFINITE : (f & FLAG_NOCONV) ? TG_ENOCONV : TG_OK;
 }
 
 long round_up(long v, long m) { return (v + m - 1) / m * m; }
@@ -139,37 +143,46 @@ long round_up(long v, long m) { return (v + m - 1) / m * m; }
 bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 
 // One level-major solve of a single segment on stream st.
+bool ring_ok_seg(const Seg &s)
+{
+    return s.ld % 32 == 0 && aligned16(s.a) && aligned16(s.b) && aligned16(s.c) && aligned16(s.f);
+}
+bool cpt2_ok_seg(const Seg &s)
+{
+    return s.ld % 2 == 0 && aligned16(s.a) && aligned16(s.b) && aligned16(s.c) && aligned16(s.f) && aligned16(s.x);
+}
+
 int solve_level(DevCtx *c, int slot, int kind, int precision, Seg seg, unsigned *flags, cudaStream_t st)
 {
     const int B = kind == TG_KIND_SCALAR ? 1 : kind;
-    int cpt = cols_per_thread(kind, precision);
-    if (cpt == 2) {
-        const bool al = (seg.ld % 2 == 0) && aligned16(seg.a) && aligned16(seg.b) && aligned16(seg.c) &&
-                        aligned16(seg.f) && aligned16(seg.x);
-        if (!al) cpt = 1;
+    int cpb = 0, cpt = 1, stages = 0, w2g = 0;
+    tile_for(kind, precision, ring_ok_seg(seg), &cpb, &cpt, &stages, &w2g);
+    if (cpt == 2 && !cpt2_ok_seg(seg)) {
+        cpb /= 2;
+        cpt = 1;
     }
-    const int cpb = cols_per_block(kind, precision);
-    const int threads = cpb / cols_per_thread(kind, precision);
-    const int cpb_eff = threads * cpt;
     SegTable tab{};
     tab.segs = nullptr;
     tab.nseg = 1;
-    tab.ntiles = (int)((seg.ncol + cpb_eff - 1) / cpb_eff);
+    tab.ntiles = (int)((seg.ncol + cpb - 1) / cpb);
     tab.k2max = seg.k2;
     seg.tile0 = 0;
     seg.status_idx = 0;
     tab.one = seg;
     Shape sh{};
-    cudaError_t e = plan_shape(kind, precision, seg.k2, tab.ntiles, &sh);
+    cudaError_t e = plan_shape(kind, precision, seg.k2, tab.ntiles, cpb, cpt, stages, w2g, &sh);
     if (e != cudaSuccess) {
-        set_err("no launch shape for kind %d nk %d: %s", kind, seg.k2, cudaGetErrorString(e));
+        set_err("no launch shape for kind %d k2 %d: %s", kind, seg.k2, cudaGetErrorString(e));
         return TG_EINVAL;
     }
-    sh.cpt = cpt;
-    sh.threads = threads;
     if (kind == TG_KIND_SCALAR) {
-        sh.smem = scalar_smem_bytes(precision, sh.threads, sh.cpt, seg.k2);
-        TG_CUDA(launch_scalar(tab, precision, sh, g_refine, flags, c->hist, st));
+        double *scr = nullptr;
+        if (sh.w2g) {
+            int rc = grow(c->scratch[slot], scalar_scratch_bytes((long)sh.blocks * sh.threads, seg.k2));
+            if (rc) return rc;
+            scr = (double *)c->scratch[slot].p;
+        }
+        TG_CUDA(launch_scalar(tab, precision, sh, g_refine, scr, flags, c->hist, st));
     } else {
         const size_t need = block_scratch_bytes(B, precision, (long)sh.blocks * sh.threads, seg.k2);
         int rc = grow(c->scratch[slot], need);
@@ -183,6 +196,9 @@ int solve_level(DevCtx *c, int slot, int kind, int precision, Seg seg, unsigned 
 //   B = 1 (scalar) or 2/3 (block); m[3], v (vectors) point at row 0 of the
 //   solve in column 0; colstride = elements between columns of a vector
 //   array (matrices: B*colstride); k2 rows are solved; ubc arrays (B, ncol).
+// Column chunks of about 4 MB of input are pipelined over kSlots streams:
+// while chunk j is relaid, solved and copied back on its stream, the next
+// chunks' host->device copies are already queued on the others.
 int host_solve(int kind, const double *const m[3], const double *v, double *x, long colstride, int k2,
                long ncol, const double *ubc_ratio, const double *ubc_add, int precision)
 {
@@ -196,18 +212,17 @@ int host_solve(int kind, const double *const m[3], const double *v, double *x, l
     const long vrows = (long)B * k2;             // vector rows copied per column
     const long orows = (long)B * (k2 + (ubc_ratio ? 1 : 0));
     const long mstride = (long)B * colstride;     // matrix column stride (elements)
-    // chunk: ~1/8 of the columns for copy/compute overlap, at most 32 MB/array
-    long chunk = std::max<long>(1024, (ncol + 7) / 8);
-    const long cap = std::max<long>(256, (32l << 20) / (8 * std::max<long>(mrows, 1)));
-    chunk = std::min(chunk, cap);
-    chunk = std::min(chunk, ncol);
-    chunk = round_up(chunk, 32);
+    const long in_per_col = (3 * mrows + vrows) * 8;
+    long nchunks = (in_per_col * ncol + (4l << 20) - 1) / (4l << 20);
+    nchunks = std::max<long>(1, std::min<long>(nchunks, 64));
+    const long chunk = round_up((ncol + nchunks - 1) / nchunks, 32);
     const long ld = chunk;
-    for (int s = 0; s < 2; ++s) {
+    const int nslots = (int)std::min<long>(kSlots, (ncol + chunk - 1) / chunk);
+    for (int s = 0; s < nslots; ++s) {
         for (int i = 0; i < 3; ++i)
             if ((rc = grow(c->colbuf[s][i], sizeof(double) * mrows * chunk))) return rc;
         if ((rc = grow(c->colbuf[s][3], sizeof(double) * vrows * chunk))) return rc;
-        if ((rc = grow(c->colbuf[s][4], sizeof(double) * orows * chunk))) return rc;
+        if ((rc = grow(c->colbuf[s][4], sizeof(double) * std::max<long>(orows, 2l * B) * chunk))) return rc;
         for (int i = 0; i < 3; ++i)
             if ((rc = grow(c->lvlbuf[s][i], sizeof(double) * mrows * ld))) return rc;
         if ((rc = grow(c->lvlbuf[s][3], sizeof(double) * vrows * ld))) return rc;
@@ -216,43 +231,54 @@ int host_solve(int kind, const double *const m[3], const double *v, double *x, l
             if ((rc = grow(c->lvlbuf[s][5], sizeof(double) * B * ld))) return rc;
             if ((rc = grow(c->lvlbuf[s][6], sizeof(double) * B * ld))) return rc;
         }
+        TG_CUDA(cudaMemsetAsync(c->flags + s, 0, sizeof(unsigned), c->st[s]));
     }
-    TG_CUDA(cudaMemsetAsync(c->flags, 0, 2 * sizeof(unsigned), c->st[0]));
-    TG_CUDA(cudaMemsetAsync(c->hist, 0, kMaxSweepBins * sizeof(unsigned long long), c->st[0]));
-    TG_CUDA(cudaStreamSynchronize(c->st[0]));
     int j = 0;
     for (long c0 = 0; c0 < ncol; c0 += chunk, ++j) {
-        const int s = j & 1;
+        const int s = j % nslots;
         cudaStream_t st = c->st[s];
         const long nc = std::min(chunk, ncol - c0);
         double *lv[7];
         for (int i = 0; i < 7; ++i) lv[i] = (double *)c->lvlbuf[s][i].p;
-        for (int i = 0; i < 3; ++i) {
+        Relayout r{};
+        r.out_ld = ld;
+        r.ncols = nc;
+        r.n = 4;
+        for (int i = 0; i < 4; ++i) {
             double *cb = (double *)c->colbuf[s][i].p;
-            if (mrows == mstride)
-                TG_CUDA(cudaMemcpyAsync(cb, m[i] + c0 * mstride, sizeof(double) * mrows * nc, cudaMemcpyHostToDevice, st));
+            const double *src = i < 3 ? m[i] : v;
+            const long rows = i < 3 ? mrows : vrows, stride = i < 3 ? mstride : colstride;
+            if (rows == stride)
+                TG_CUDA(cudaMemcpyAsync(cb, src + c0 * stride, sizeof(double) * rows * nc, cudaMemcpyHostToDevice, st));
             else
-                TG_CUDA(cudaMemcpy2DAsync(cb, sizeof(double) * mrows, m[i] + c0 * mstride, sizeof(double) * mstride,
-                                          sizeof(double) * mrows, nc, cudaMemcpyHostToDevice, st));
-            TG_CUDA(launch_col_to_level(cb, mrows, lv[i], ld, mrows, nc, st));
+                TG_CUDA(cudaMemcpy2DAsync(cb, sizeof(double) * rows, src + c0 * stride, sizeof(double) * stride,
+                                          sizeof(double) * rows, nc, cudaMemcpyHostToDevice, st));
+            r.in[i] = cb;
+            r.out[i] = lv[i];
+            r.in_ld[i] = rows;
+            r.nrows[i] = rows;
         }
-        {
-            double *cb = (double *)c->colbuf[s][3].p;
-            if (vrows == colstride)
-                TG_CUDA(cudaMemcpyAsync(cb, v + c0 * colstride, sizeof(double) * vrows * nc, cudaMemcpyHostToDevice, st));
-            else
-                TG_CUDA(cudaMemcpy2DAsync(cb, sizeof(double) * vrows, v + c0 * colstride, sizeof(double) * colstride,
-                                          sizeof(double) * vrows, nc, cudaMemcpyHostToDevice, st));
-            TG_CUDA(launch_col_to_level(cb, vrows, lv[3], ld, vrows, nc, st));
-        }
+        TG_CUDA(launch_col_to_level_multi(r, st));
         if (ubc_ratio) {
             double *cb = (double *)c->colbuf[s][4].p;
+            Relayout u{};
+            u.out_ld = ld;
+            u.ncols = nc;
+            u.n = ubc_add ? 2 : 1;
             TG_CUDA(cudaMemcpyAsync(cb, ubc_ratio + c0 * B, sizeof(double) * B * nc, cudaMemcpyHostToDevice, st));
-            TG_CUDA(launch_col_to_level(cb, B, lv[5], ld, B, nc, st));
+            u.in[0] = cb;
+            u.out[0] = lv[5];
+            u.in_ld[0] = B;
+            u.nrows[0] = B;
             if (ubc_add) {
-                TG_CUDA(cudaMemcpyAsync(cb, ubc_add + c0 * B, sizeof(double) * B * nc, cudaMemcpyHostToDevice, st));
-                TG_CUDA(launch_col_to_level(cb, B, lv[6], ld, B, nc, st));
+                TG_CUDA(cudaMemcpyAsync(cb + B * chunk, ubc_add + c0 * B, sizeof(double) * B * nc,
+                                        cudaMemcpyHostToDevice, st));
+                u.in[1] = cb + B * chunk;
+                u.out[1] = lv[6];
+                u.in_ld[1] = B;
+                u.nrows[1] = B;
             }
+            TG_CUDA(launch_col_to_level_multi(u, st));
         }
         Seg seg{};
         seg.a = lv[0];
@@ -276,10 +302,11 @@ int host_solve(int kind, const double *const m[3], const double *v, double *x, l
             TG_CUDA(cudaMemcpy2DAsync(x + c0 * colstride, sizeof(double) * colstride, ob, sizeof(double) * orows,
                                       sizeof(double) * orows, nc, cudaMemcpyDeviceToHost, st));
     }
-    TG_CUDA(cudaStreamSynchronize(c->st[0]));
-    TG_CUDA(cudaStreamSynchronize(c->st[1]));
-    TG_CUDA(cudaMemcpy(c->flags_host, c->flags, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost));
-    return flags_to_status(c->flags_host[0] | c->flags_host[1]);
+    for (int s = 0; s < nslots; ++s) TG_CUDA(cudaStreamSynchronize(c->st[s]));
+    TG_CUDA(cudaMemcpy(c->flags_host, c->flags, nslots * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    unsigned all = 0;
+    for (int s = 0; s < nslots; ++s) all |= c->flags_host[s];
+    return flags_to_status(all);
 }
 
 bool bad_prec(int p) { return p != TG_PREC_F64 && p != TG_PREC_F32_REFINE; }
@@ -305,6 +332,49 @@ __attribute__((visibility("default"))) int tg_set_refine(int max_sweeps, double 
     }
     g_refine.max_sweeps = max_sweeps;
     g_refine.rel_tol = rel_tol;
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_pipeline(int kind, int precision, int stages)
+{
+    if ((kind != TG_KIND_SCALAR && kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) || bad_prec(precision) ||
+        (stages != -1 && stages != 0 && stages != 4 && stages != 8 && stages != 16) ||
+        (stages > 0 && precision != TG_PREC_F64)) {
+        set_err("tg_set_pipeline: stages must be 0, 4, 8 or 16 (FP64 only), or -1 for the default");
+        return TG_EINVAL;
+    }
+    set_stages(kind, precision, stages);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_prefetch(int kind, int precision, int levels)
+{
+    if (kind != TG_KIND_SCALAR || bad_prec(precision) || (levels != -1 && levels != 4 && levels != 8 && levels != 16)) {
+        set_err("tg_set_prefetch: scalar kind only, levels 4, 8, 16 or -1");
+        return TG_EINVAL;
+    }
+    set_prefetch(kind, precision, levels);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_scratch_global(int kind, int precision, int on)
+{
+    if (kind != TG_KIND_SCALAR || precision != TG_PREC_F64 || on < -1 || on > 1) {
+        set_err("tg_set_scratch_global: only the scalar FP64 kernel, on = 0, 1 or -1");
+        return TG_EINVAL;
+    }
+    set_w2g(kind, precision, on);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_selftest_division(const double *a, const double *b, double *q,
+                                                                long n, void *stream)
+{
+    if (!a || !b || !q || n < 0) {
+        set_err("tg_selftest_division: bad arguments");
+        return TG_EINVAL;
+    }
+    TG_CUDA(launch_selftest_division(a, b, q, n, (cudaStream_t)stream));
     return TG_OK;
 }
 
@@ -483,6 +553,95 @@ static int dev_solve(int kind, const double *a, const double *b, const double *c
     return TG_OK;
 }
 
+__attribute__((visibility("default"))) int tg_dt_ng_dev(const tg_dt_fields *F, const tg_dt_consts *C,
+                                                        double *tn_upd, int nk, int ncol, long ld, double *system_out,
+                                                        int *status_dev, void *stream)
+{
+    if (!F || !C || !tn_upd || nk < 3 || ncol < 0 || ld < ncol) {
+        set_err("tg_dt_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    const double *const ptrs[] = {F->tn, F->tnsmooth, F->horadv, F->un, F->vn, F->o1, F->mbar, F->xnmbar,
+                                  F->scht, F->schti, F->cp, F->kt, F->km, F->hdt, F->qji_tn, F->cool_imp,
+                                  F->cool_exp, F->w, F->qtotal, F->rkm12, F->tlbc, F->t_lbc, F->ulbc, F->vlbc,
+                                  F->expz, F->dift};
+    for (const double *p : ptrs)
+        if (!p) {
+            set_err("tg_dt_ng_dev: a field pointer is NULL");
+            return TG_EINVAL;
+        }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_dt_ng(*F, *C, tn_upd, nk, ncol, ld, system_out, cx->flags, st));
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_dt_ng(const tg_dt_fields *F, const tg_dt_consts *C, double *tn_upd,
+                                                    int nk, int ncol)
+{
+    if (!F || !C || !tn_upd || nk < 3 || ncol < 0) {
+        set_err("tg_dt_ng: bad arguments (nk=%d ncol=%d)", nk, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    const double *const f3[20] = {F->tn, F->tnsmooth, F->horadv, F->un, F->vn, F->o1, F->mbar, F->xnmbar,
+                                  F->scht, F->schti, F->cp, F->kt, F->km, F->hdt, F->qji_tn, F->cool_imp,
+                                  F->cool_exp, F->w, F->qtotal, F->rkm12};
+    const double *const f2[4] = {F->tlbc, F->t_lbc, F->ulbc, F->vlbc};
+    for (const double *p : f3)
+        if (!p) return set_err("tg_dt_ng: a field pointer is NULL"), TG_EINVAL;
+    for (const double *p : f2)
+        if (!p) return set_err("tg_dt_ng: a field pointer is NULL"), TG_EINVAL;
+    if (!F->expz || !F->dift) return set_err("tg_dt_ng: expz/dift NULL"), TG_EINVAL;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ld = round_up(ncol, 32);
+    const size_t lvl = (size_t)nk * ld, colsz = (size_t)nk * ncol;
+    // one buffer: 20 level-major 3-D fields, the output, 4 2-D fields, expz, dift; one staging buffer
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (21 * lvl + 4 * (size_t)ld + 2 * (size_t)nk)))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * colsz))) return rc;
+    double *base = (double *)c->lvlbuf[0][0].p, *stage = (double *)c->colbuf[0][0].p;
+    cudaStream_t st = c->st[0];
+    tg_dt_fields D;
+    const double **dst3[20] = {&D.tn, &D.tnsmooth, &D.horadv, &D.un, &D.vn, &D.o1, &D.mbar, &D.xnmbar, &D.scht,
+                               &D.schti, &D.cp, &D.kt, &D.km, &D.hdt, &D.qji_tn, &D.cool_imp, &D.cool_exp, &D.w,
+                               &D.qtotal, &D.rkm12};
+    for (int i = 0; i < 20; ++i) {
+        double *d = base + i * lvl;
+        TG_CUDA(cudaMemcpyAsync(stage, f3[i], sizeof(double) * colsz, cudaMemcpyHostToDevice, st));
+        TG_CUDA(launch_col_to_level(stage, nk, d, ld, nk, ncol, st));
+        *dst3[i] = d;
+    }
+    double *out = base + 20 * lvl, *two = base + 21 * lvl, *one = two + 4 * ld;
+    const double **dst2[4] = {&D.tlbc, &D.t_lbc, &D.ulbc, &D.vlbc};
+    for (int i = 0; i < 4; ++i) {
+        TG_CUDA(cudaMemcpyAsync(two + i * ld, f2[i], sizeof(double) * ncol, cudaMemcpyHostToDevice, st));
+        *dst2[i] = two + i * ld;
+    }
+    TG_CUDA(cudaMemcpyAsync(one, F->expz, sizeof(double) * nk, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(one + nk, F->dift, sizeof(double) * nk, cudaMemcpyHostToDevice, st));
+    D.expz = one;
+    D.dift = one + nk;
+    TG_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_dt_ng(D, *C, out, nk, ncol, ld, nullptr, c->flags, st));
+    TG_CUDA(launch_level_to_col(out, ld, stage, nk, nk, ncol, st));
+    TG_CUDA(cudaMemcpyAsync(tn_upd, stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    TG_CUDA(cudaMemcpy(c->flags_host, c->flags, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    return flags_to_status(c->flags_host[0]);
+}
+
 __attribute__((visibility("default"))) int tg_trsolv_dev(const double *a, const double *b, const double *c,
                                                          const double *f, double *x, int nk, int k2, int ncol,
                                                          int layout, long ld, int precision, int *status_dev,
@@ -530,28 +689,50 @@ struct tg_plan {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t graph_stream = nullptr;
+    cudaStream_t side = nullptr;            // block kinds run here, beside the scalar kind
+    cudaEvent_t fork = nullptr, join = nullptr;
     int launches = 0;
 };
 
 namespace {
+int plan_launch_group(tg_plan *p, tg_plan::Group &g, cudaStream_t st)
+{
+    SegTable tab{};
+    tab.segs = g.d_segs;
+    tab.nseg = g.nseg;
+    tab.ntiles = g.ntiles;
+    tab.k2max = g.k2max;
+    if (g.kind == TG_KIND_SCALAR)
+        TG_CUDA(launch_scalar(tab, p->precision, g.shape, g_refine, (double *)g.scratch, p->d_flags, p->d_hist, st));
+    else
+        TG_CUDA(launch_block(tab, g.kind, p->precision, g.shape, g_refine, (double *)g.scratch, p->d_flags, p->d_hist,
+                             st));
+    return TG_OK;
+}
+
+// The scalar kind is bandwidth-bound and the block kinds are latency-bound
+// (few columns, long per-level dependency chains), so the block groups run on
+// a side stream forked from st and joined back: in a captured graph they are
+// parallel branches and the two kernels share the GPU.
 int plan_enqueue(tg_plan *p, cudaStream_t st)
 {
     TG_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(unsigned) * p->nseg, st));
     if (p->precision != TG_PREC_F64)
         TG_CUDA(cudaMemsetAsync(p->d_hist, 0, kMaxSweepBins * sizeof(unsigned long long), st));
-    for (auto &g : p->groups) {
-        if (g.nseg == 0) continue;
-        SegTable tab{};
-        tab.segs = g.d_segs;
-        tab.nseg = g.nseg;
-        tab.ntiles = g.ntiles;
-        tab.k2max = g.k2max;
-        if (g.kind == TG_KIND_SCALAR)
-            TG_CUDA(launch_scalar(tab, p->precision, g.shape, g_refine, p->d_flags, p->d_hist, st));
-        else
-            TG_CUDA(launch_block(tab, g.kind, p->precision, g.shape, g_refine, (double *)g.scratch, p->d_flags,
-                                 p->d_hist, st));
+    const bool split = p->groups[0].nseg > 0 && (p->groups[1].nseg > 0 || p->groups[2].nseg > 0);
+    int rc;
+    if (!split) {
+        for (auto &g : p->groups)
+            if (g.nseg > 0 && (rc = plan_launch_group(p, g, st))) return rc;
+        return TG_OK;
     }
+    TG_CUDA(cudaEventRecord(p->fork, st));
+    TG_CUDA(cudaStreamWaitEvent(p->side, p->fork, 0));
+    for (int gi = 1; gi < 3; ++gi)
+        if (p->groups[gi].nseg > 0 && (rc = plan_launch_group(p, p->groups[gi], p->side))) return rc;
+    if ((rc = plan_launch_group(p, p->groups[0], st))) return rc;
+    TG_CUDA(cudaEventRecord(p->join, p->side));
+    TG_CUDA(cudaStreamWaitEvent(st, p->join, 0));
     return TG_OK;
 }
 
@@ -567,6 +748,9 @@ void plan_free(tg_plan *p)
     if (p->d_flags) cudaFree(p->d_flags);
     if (p->d_status) cudaFree(p->d_status);
     if (p->d_hist) cudaFree(p->d_hist);
+    if (p->fork) cudaEventDestroy(p->fork);
+    if (p->join) cudaEventDestroy(p->join);
+    if (p->side) cudaStreamDestroy(p->side);
     delete p;
 }
 }  // namespace
@@ -602,10 +786,8 @@ __attribute__((visibility("default"))) int tg_plan_create(const tg_segment *segs
     for (int gi = 0; gi < 3; ++gi) {
         auto &g = p->groups[gi];
         g.kind = kinds[gi];
-        int cpt = cols_per_thread(g.kind, precision);
-        const int cpb0 = cols_per_block(g.kind, precision);
-        const int threads = cpb0 / cols_per_thread(g.kind, precision);
         std::vector<Seg> hs;
+        bool ring_ok = true, cpt2_ok = true;
         for (int i = 0; i < nseg; ++i) {
             const tg_segment &s = segs[i];
             if (s.kind != g.kind || s.ncol == 0) continue;
@@ -615,14 +797,18 @@ __attribute__((visibility("default"))) int tg_plan_create(const tg_segment *segs
             d.ubc_add = d.ubc_ratio ? s.ubc_add : nullptr;
             d.ld = s.ld; d.nk = s.nk; d.k2 = s.k2; d.ncol = s.ncol; d.kind = s.kind;
             d.status_idx = i;
-            if (cpt == 2 && !((s.ld % 2 == 0) && aligned16(s.a) && aligned16(s.b) && aligned16(s.c) &&
-                              aligned16(s.f) && aligned16(s.x)))
-                cpt = 1;
+            ring_ok = ring_ok && ring_ok_seg(d);
+            cpt2_ok = cpt2_ok && cpt2_ok_seg(d);
             hs.push_back(d);
             g.k2max = std::max(g.k2max, s.k2);
         }
         if (hs.empty()) continue;
-        const int cpb = threads * cpt;
+        int cpb = 0, cpt = 1, stages = 0, w2g = 0;
+        tile_for(g.kind, precision, ring_ok, &cpb, &cpt, &stages, &w2g);
+        if (cpt == 2 && !cpt2_ok) {
+            cpb /= 2;
+            cpt = 1;
+        }
         long tiles = 0;
         for (auto &d : hs) {
             d.tile0 = (int)tiles;
@@ -635,15 +821,12 @@ __attribute__((visibility("default"))) int tg_plan_create(const tg_segment *segs
         }
         g.nseg = (int)hs.size();
         g.ntiles = (int)tiles;
-        cudaError_t e = plan_shape(g.kind, precision, g.k2max, g.ntiles, &g.shape);
+        cudaError_t e = plan_shape(g.kind, precision, g.k2max, g.ntiles, cpb, cpt, stages, w2g, &g.shape);
         if (e != cudaSuccess) {
             plan_free(p);
             set_err("tg_plan_create: no launch shape: %s", cudaGetErrorString(e));
             return TG_EINVAL;
         }
-        g.shape.cpt = cpt;
-        g.shape.threads = threads;
-        if (g.kind == TG_KIND_SCALAR) g.shape.smem = scalar_smem_bytes(precision, threads, cpt, g.k2max);
         if (cudaMalloc(&g.d_segs, sizeof(Seg) * hs.size()) != cudaSuccess ||
             cudaMemcpy(g.d_segs, hs.data(), sizeof(Seg) * hs.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
             cudaGetLastError();
@@ -651,8 +834,10 @@ __attribute__((visibility("default"))) int tg_plan_create(const tg_segment *segs
             set_err("tg_plan_create: segment table upload failed");
             return TG_ENOMEM;
         }
-        if (g.kind != TG_KIND_SCALAR) {
-            const size_t need = block_scratch_bytes(g.kind, precision, (long)g.shape.blocks * g.shape.threads, g.k2max);
+        if (g.kind != TG_KIND_SCALAR || g.shape.w2g) {
+            const long slots = (long)g.shape.blocks * g.shape.threads;
+            const size_t need = g.kind == TG_KIND_SCALAR ? scalar_scratch_bytes(slots, g.k2max)
+                                                         : block_scratch_bytes(g.kind, precision, slots, g.k2max);
             if (cudaMalloc(&g.scratch, need) != cudaSuccess) {
                 cudaGetLastError();
                 plan_free(p);
@@ -662,7 +847,10 @@ __attribute__((visibility("default"))) int tg_plan_create(const tg_segment *segs
         }
         p->launches += 1;
     }
-    if (cudaMalloc(&p->d_flags, sizeof(unsigned) * std::max(nseg, 1)) != cudaSuccess ||
+    if (cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(&p->d_flags, sizeof(unsigned) * std::max(nseg, 1)) != cudaSuccess ||
         cudaMalloc(&p->d_status, sizeof(int) * std::max(nseg, 1)) != cudaSuccess ||
         cudaMalloc(&p->d_hist, kMaxSweepBins * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMemset(p->d_flags, 0, sizeof(unsigned) * std::max(nseg, 1)) != cudaSuccess ||
@@ -779,7 +967,7 @@ __attribute__((visibility("default"))) int tg_release_buffers(void)
         cudaGetDevice(&cur);
         cudaSetDevice(d);
         cudaDeviceSynchronize();
-        for (int s = 0; s < 2; ++s) {
+        for (int s = 0; s < kSlots; ++s) {
             for (auto &b : c->colbuf[s])
                 if (b.p) cudaFree(b.p);
             for (auto &b : c->lvlbuf[s])

@@ -14,6 +14,7 @@ enum : unsigned {
     FLAG_PIVOT = 1u,      // zero or non-finite pivot / block determinant
     FLAG_NONFINITE = 2u,  // non-finite solution value
     FLAG_NOCONV = 4u,     // refinement hit the sweep cap (column re-solved in FP64)
+    FLAG_TIMEOUT = 8u,    // a bounded wait on an asynchronous copy gave up
 };
 
 // Maximum refinement sweeps tracked by the histogram (bins 0..kMaxSweepBins-1).
@@ -53,26 +54,49 @@ struct Shape {
     int threads;        // threads per block
     int cpt;            // columns per thread (1 or 2)
     int blocks;         // persistent grid size
+    int stages;         // bulk-copy ring depth (0: register-prefetch kernel)
+    int w2g;            // scalar register kernel with w2 in global scratch
+    int pf;             // scalar register kernels: prefetch depth in levels
     size_t smem;        // dynamic shared memory bytes
 };
 
+// Register-prefetch kernel shape of a kind/precision (tg_set_tile).
 int cols_per_block(int kind, int precision);
 int cols_per_thread(int kind, int precision);
 void set_tile(int kind, int precision, int cpb, int cpt);
+// Bulk-copy ring depth of a kind/precision (tg_set_pipeline); 0 disables.
+void set_stages(int kind, int precision, int stages);
+// Effective tile of a launch: the ring kernel (32 columns per warp-CTA)
+// when configured and ring_ok (ld % 32 == 0, 16-byte aligned bases), else
+// the register-prefetch kernel.
+void tile_for(int kind, int precision, bool ring_ok, int *cpb, int *cpt, int *stages, int *w2g);
+// Levels of coefficient loads the scalar register kernels keep in flight
+// (4, 8 or 16; 2-column threads at most 8).
+int prefetch_depth(int kind, int precision);
+void set_prefetch(int kind, int precision, int pf);
+// Scalar FP64 register kernel keeps w2 in global scratch (1) or shared
+// memory (0); -1 restores the default.
+void set_w2g(int kind, int precision, int on);
+// Global scratch (bytes) of the scalar kernel with w2 in global memory.
+size_t scalar_scratch_bytes(long slots, int k2max);
 
 // Shared memory / scratch needs of a kernel for the largest k2 it will see.
-size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max);
+size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages);
+size_t block_smem_bytes(int B, int stages);
 // Global scratch (bytes) of a block kernel with `slots` resident threads.
 size_t block_scratch_bytes(int B, int precision, long slots, int k2max);
 
-// Computes the persistent grid for a kind/precision/k2max on the current
-// device, limited to ntiles.
-cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, Shape *shape);
+// Computes the persistent grid for a launch on the current device, limited
+// to ntiles.
+cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, int cpt, int stages, int w2g,
+                       Shape *shape);
 
 // Solve launches (level-major).  status: per-segment device status words.
 // hist: device histogram of refinement sweeps (kMaxSweepBins longs), may be null.
-cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, Refine rf,
+cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, Refine rf, double *scratch,
                           unsigned *status, unsigned long long *hist, cudaStream_t st);
+// q[i] = a[i]/b[i] through the kernels' division (test entry).
+cudaError_t launch_selftest_division(const double *a, const double *b, double *q, long n, cudaStream_t st);
 cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape &sh, Refine rf,
                          double *scratch, unsigned *status, unsigned long long *hist,
                          cudaStream_t st);
@@ -81,9 +105,26 @@ cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape 
 // in(r, col) at in[r + in_ld*col] -> out[r*out_ld + col], r < nrows.
 cudaError_t launch_col_to_level(const double *in, long in_ld, double *out, long out_ld,
                                 long nrows, long ncols, cudaStream_t st);
+// Up to four column->level relayouts in one launch.
+struct Relayout {
+    const double *in[4];
+    double *out[4];
+    long in_ld[4];
+    long nrows[4];
+    long out_ld;
+    long ncols;
+    int n;
+};
+cudaError_t launch_col_to_level_multi(const Relayout &r, cudaStream_t st);
 // in[r*in_ld + col] -> out(r, col) at out[r + out_ld*col], r < nrows.
 cudaError_t launch_level_to_col(const double *in, long in_ld, double *out, long out_ld,
                                 long nrows, long ncols, cudaStream_t st);
+
+// dt_ng fused assembly + solve (tg_assembly.cu).
+typedef tg_dt_fields DtFields;
+typedef tg_dt_consts DtConsts;
+cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, int nk, int ncol, long ld,
+                         double *sys_out, unsigned *status, cudaStream_t st);
 
 // Records the message tg_last_error() returns on this thread.
 void record_error(const char *msg);

@@ -28,6 +28,38 @@ __device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a,
 __device__ __forceinline__ bool finite_nz(double w) { return fabs(w) <= DBL_MAX && w != 0.0; }
 __device__ __forceinline__ bool finite(double w) { return fabs(w) <= DBL_MAX; }
 
+// Correctly rounded quotients that share a divisor.  y = __drcp_rn(b) is the
+// correctly rounded reciprocal; q0 = RN(a*y) is within ~2 ulp of a/b, one
+// FMA correction q1 = RN(q0 + RN(a - b*q0)*y) brings it within 1 ulp, and
+// Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1), 1990; Muller et
+// al., Handbook of Floating-Point Arithmetic, Thm. 5.8) makes the second
+// correction RN(q1 + (a - b*q1)*y) equal to RN(a/b), provided nothing
+// underflows or overflows.  div_safe() keeps a, b (and hence a/b and the
+// residuals) well inside the normal range; other operands, zeros included
+// (whose quotient's sign the correction steps would not keep), take IEEE
+// division.
+// The result is therefore bit-identical to a/b; tg_selftest_division checks
+// it against the hardware division.
+__device__ __forceinline__ bool div_safe(double a, double b)
+{
+    const double lo = 0x1p-500, hi = 0x1p500;
+    const double fa = fabs(a), fb = fabs(b);
+    return fb >= lo && fb <= hi && fa >= lo && fa <= hi;
+}
+__device__ __forceinline__ double div_markstein(double a, double b, double y)
+{
+    double q = __dmul_rn(a, y);
+    double r = __fma_rn(-b, q, a);
+    q = __fma_rn(r, y, q);
+    r = __fma_rn(-b, q, a);
+    return __fma_rn(r, y, q);
+}
+// a/b, correctly rounded, given y = __drcp_rn(b).
+__device__ __forceinline__ double qdiv(double a, double b, double y)
+{
+    return div_safe(a, b) ? div_markstein(a, b, y) : __ddiv_rn(a, b);
+}
+
 // Streaming read of coefficients used once (evict-first in L1/L2).
 template <int N>
 __device__ __forceinline__ void ld_stream(const double *p, double (&v)[N]);
@@ -98,6 +130,97 @@ __device__ __forceinline__ void report(unsigned *status, int idx, unsigned flags
 }
 
 // ---------------------------------------------------------------------------
+// Bulk asynchronous copies global -> shared (the TMA engine, 1-D form) with
+// mbarrier completion.  Each CTA copies only into its own shared memory.
+// Waits are bounded: kWaitLimit polls of mbarrier.try_wait (each poll may
+// suspend the thread for a short hardware-defined time) before giving up.
+// ---------------------------------------------------------------------------
+constexpr unsigned kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned long long *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait of the whole warp; true when every lane saw the phase complete.
+__device__ __forceinline__ bool mbar_wait_warp(unsigned long long *bar, uint32_t parity)
+{
+    bool done = false;
+#pragma unroll 1
+    for (unsigned i = 0; i < kWaitLimit && !done; ++i) done = mbar_try_wait(bar, parity);
+    return __all_sync(0xffffffffu, done);
+}
+
+// Stage ring of a single-warp CTA: level k of NE arrays (32 columns x 8 B =
+// 256 B each) lands in stage (q % D), q the running level counter of the CTA.
+template <int NE, int D>
+struct Ring {
+    double *buf;                 // D * NE * 32 doubles
+    unsigned long long *bar;     // D mbarriers
+    __device__ __forceinline__ void init(int lane)
+    {
+        if (lane == 0) {
+#pragma unroll 1
+            for (int s = 0; s < D; ++s) mbar_init(&bar[s], 1);
+            fence_mbar_init();
+        }
+        __syncwarp();
+    }
+    // All lanes call; lanes e < NE issue entry e from src[e].
+    __device__ __forceinline__ void issue(unsigned q, const double *src_e, int lane)
+    {
+        const int st = (int)(q % D);
+        if (lane == 0) mbar_expect(&bar[st], NE * 256u);
+        __syncwarp();
+        if (lane < NE) bulk_load(buf + (st * NE + lane) * 32, src_e, 256u, &bar[st]);
+    }
+    __device__ __forceinline__ bool wait(unsigned q) { return mbar_wait_warp(&bar[q % D], (q / D) & 1u); }
+    __device__ __forceinline__ double at(unsigned q, int e, int lane) const
+    {
+        return buf[((int)(q % D) * NE + e) * 32 + lane];
+    }
+    // After a timeout: bounded wait for the fills still in flight (q0..q1-1).
+    __device__ __forceinline__ void drain(unsigned q0, unsigned q1)
+    {
+#pragma unroll 1
+        for (unsigned q = q0; q < q1; ++q) mbar_wait_warp(&bar[q % D], (q / D) & 1u);
+    }
+};
+
+// ---------------------------------------------------------------------------
 // Scalar Thomas, FP64, bit-exact (trsolv_ng.F90:14-26).
 //
 // Forward: w2(k-1) = c(k-1)/w1(k-1); w1(k) = b(k)-a(k)*w2(k-1);
@@ -121,7 +244,7 @@ __device__ __forceinline__ unsigned thomas_f64_cols(const Seg &s, long col, doub
     double *__restrict__ px = s.x + col;
 
     bool ok = true;
-    double w1[CPT], w3[CPT], cprev[CPT];
+    double w1[CPT], y1[CPT], w3[CPT], cprev[CPT];   // y1 = RN(1/w1)
     {
         double b0[CPT], f0[CPT];
         ld_stream<CPT>(pb, b0);
@@ -130,7 +253,8 @@ __device__ __forceinline__ unsigned thomas_f64_cols(const Seg &s, long col, doub
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
             w1[j] = b0[j];
-            w3[j] = xdiv(f0[j], w1[j]);
+            y1[j] = __drcp_rn(w1[j]);
+            w3[j] = qdiv(f0[j], w1[j], y1[j]);
             if (j < nvalid) ok = ok && finite_nz(w1[j]);
         }
         st_cols<CPT>(px, w3, nvalid);
@@ -155,9 +279,10 @@ __device__ __forceinline__ unsigned thomas_f64_cols(const Seg &s, long col, doub
                 double w2[CPT];
 #pragma unroll
                 for (int j = 0; j < CPT; ++j) {
-                    w2[j] = xdiv(cprev[j], w1[j]);
+                    w2[j] = qdiv(cprev[j], w1[j], y1[j]);
                     w1[j] = xsub(rb[u][j], xmul(ra[u][j], w2[j]));
-                    w3[j] = xdiv(xsub(rf[u][j], xmul(ra[u][j], w3[j])), w1[j]);
+                    y1[j] = __drcp_rn(w1[j]);
+                    w3[j] = qdiv(xsub(rf[u][j], xmul(ra[u][j], w3[j])), w1[j], y1[j]);
                     if (j < nvalid) ok = ok && finite_nz(w1[j]);
                     cprev[j] = rc[u][j];
                 }
@@ -235,6 +360,109 @@ __global__ void __launch_bounds__(256) k_scalar_f64(SegTable tab, unsigned *stat
     }
 }
 
+// Same sweep with w2 in a global scratch buffer instead of shared memory
+// (element (k, slot) at scratch[k*S + slot], S resident threads): no shared
+// memory limits residency, so a grid of register-limited size keeps every
+// column of a batch in flight at once; the scratch lines stay in L2 between
+// the forward and back sweeps.
+template <int PF>
+__global__ void __launch_bounds__(256) k_scalar_f64_g(SegTable tab, double *scratch, unsigned *status)
+{
+    const long S = (long)gridDim.x * blockDim.x;
+    double *w2s = scratch + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int t = blockIdx.x; t < tab.ntiles; t += gridDim.x) {
+        const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
+        const long col = (long)(t - s.tile0) * blockDim.x + threadIdx.x;
+        if (col < s.ncol) report(status, s.status_idx, thomas_f64_cols<1, PF>(s, col, w2s, (int)S, 1));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Scalar Thomas, FP64, bit-exact, coefficients staged by bulk copies.
+//
+// One warp per CTA solves 32 adjacent columns.  a, b, c, f of level k arrive
+// in a D-stage shared-memory ring (4 x 256 B per level), refilled D levels
+// ahead, so a warp keeps 4*D*256 bytes of loads in flight without spending
+// registers.  w2 goes to shared memory ([k][lane]), w3 is parked in x.
+// Requires ld % 32 == 0 and 16-byte aligned array bases (checked on the host).
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(32) k_scalar_f64_ring(SegTable tab, unsigned *status)
+{
+    constexpr int NE = 4;
+    extern __shared__ __align__(128) double smem_r[];
+    __shared__ __align__(8) unsigned long long bars[D];
+    const int lane = threadIdx.x;
+    Ring<NE, D> ring{smem_r, bars};
+    double *w2s = smem_r + D * NE * 32 + lane;
+    ring.init(lane);
+    unsigned q = 0;
+    for (int t = blockIdx.x; t < tab.ntiles; t += gridDim.x) {
+        const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
+        const long col0 = (long)(t - s.tile0) * 32;
+        const long ld = s.ld;
+        const int k2 = s.k2;
+        const bool valid = col0 + lane < s.ncol;
+        const double *src = (lane == 0 ? s.a : lane == 1 ? s.b : lane == 2 ? s.c : s.f) + col0;
+        double *px = s.x + col0 + lane;
+        const int pre = k2 < D ? k2 : D;
+        for (int j = 0; j < pre; ++j) ring.issue(q + j, src + j * ld, lane);
+        bool ok = true, fin = true;
+        double w1 = 0.0, y1 = 0.0, w3 = 0.0, cprev = 0.0;
+        for (int k = 0; k < k2; ++k) {
+            const unsigned qk = q + k;
+            if (!ring.wait(qk)) {
+                ring.drain(qk, q + (k + D < k2 ? k + D : k2));
+                if (lane == 0) report(status, s.status_idx, FLAG_TIMEOUT);
+                return;
+            }
+            const double ak = ring.at(qk, 0, lane), bk = ring.at(qk, 1, lane), ck = ring.at(qk, 2, lane),
+                         fk = ring.at(qk, 3, lane);
+            __syncwarp();
+            fence_proxy_async();
+            if (k + D < k2) ring.issue(qk + D, src + (k + D) * ld, lane);
+            if (valid) {
+                if (k == 0) {
+                    w1 = bk;
+                    y1 = __drcp_rn(w1);
+                    w3 = qdiv(fk, w1, y1);
+                } else {
+                    const double w2 = qdiv(cprev, w1, y1);
+                    w2s[(k - 1) * 32] = w2;
+                    w1 = xsub(bk, xmul(ak, w2));
+                    y1 = __drcp_rn(w1);
+                    w3 = qdiv(xsub(fk, xmul(ak, w3)), w1, y1);
+                }
+                ok = ok && finite_nz(w1);
+                cprev = ck;
+                px[k * ld] = w3;
+            }
+        }
+        q += k2;
+        if (valid) {
+            double xn = w3;
+            fin = finite(xn);
+            double rw[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k2 - 2 - u >= 0) rw[u] = px[(k2 - 2 - u) * ld];
+            for (int kb = k2 - 2; kb >= 0; kb -= 4) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = kb - u;
+                    if (k >= 0) {
+                        xn = xsub(rw[u], xmul(w2s[k * 32], xn));
+                        fin = fin && finite(xn);
+                        if (k - 4 >= 0) rw[u] = px[(k - 4) * ld];
+                        px[k * ld] = xn;
+                    }
+                }
+            }
+            report(status, s.status_idx, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Scalar Thomas, FP32 sweeps + FP64 iterative refinement.
 //
@@ -246,6 +474,22 @@ __global__ void __launch_bounds__(256) k_scalar_f64(SegTable tab, unsigned *stat
 // slots reused for w2) and flagged FLAG_NOCONV.
 // Shared memory per thread: three float planes (w2, 1/w1, y) of k2 levels.
 // ---------------------------------------------------------------------------
+// Stopping rule of the refinement sweeps.  dmax = max|d| of this sweep's
+// correction, xmax = max|x| after it, dprev = max|d| of the previous sweep
+// (0 before the second sweep).  Each sweep shrinks the error by a factor rho,
+// estimated as dmax/dprev; the error left after applying d is then about
+// dmax*rho/(1-rho).  A column stops when that estimate, or the correction
+// itself, is below rel_tol*xmax.
+__device__ __forceinline__ bool refine_done(double dmax, double xmax, double dprev, double tol)
+{
+    if (dmax <= tol * xmax) return true;
+    if (dprev > 0.0) {
+        const double rho = dmax / dprev;
+        if (rho < 0.5 && dmax * rho <= (1.0 - rho) * tol * xmax) return true;
+    }
+    return false;
+}
+
 template <int PF>
 __device__ __forceinline__ unsigned thomas_refine_col(const Seg &s, long col, float *sw2, float *sri,
                                                       float *sy, int T, Refine rf, int &sweeps)
@@ -313,6 +557,7 @@ __device__ __forceinline__ unsigned thomas_refine_col(const Seg &s, long col, fl
     // ---- refinement sweeps
     bool conv = false;
     int sw = 0;
+    double dprev = 0.0;
     if (ok) {
         for (sw = 1; sw <= rf.max_sweeps; ++sw) {
             double xm1 = 0.0, x0 = px[0];
@@ -362,10 +607,11 @@ __device__ __forceinline__ unsigned thomas_refine_col(const Seg &s, long col, fl
                 xmax = fmax(xmax, fabs(xv));
             }
             if (!(xmax <= DBL_MAX) || !(dmax <= DBL_MAX)) break;
-            if (dmax <= rf.rel_tol * xmax) {
+            if (refine_done(dmax, xmax, dprev, rf.rel_tol)) {
                 conv = true;
                 break;
             }
+            dprev = dmax;
         }
     }
     sweeps = conv ? sw : rf.max_sweeps + 1;
@@ -441,10 +687,11 @@ template <>
 __device__ __forceinline__ bool inv_exact<2>(const double (&A)[4], double (&W)[4])
 {
     const double d = xsub(xmul(A[0], A[3]), xmul(A[2], A[1]));
-    W[0] = xdiv(A[3], d);
-    W[1] = xdiv(-A[1], d);
-    W[2] = xdiv(-A[2], d);
-    W[3] = xdiv(A[0], d);
+    const double y = __drcp_rn(d);
+    W[0] = qdiv(A[3], d, y);
+    W[1] = qdiv(-A[1], d, y);
+    W[2] = qdiv(-A[2], d, y);
+    W[3] = qdiv(A[0], d, y);
     return finite_nz(d);
 }
 
@@ -470,8 +717,9 @@ __device__ __forceinline__ bool inv_exact<3>(const double (&A)[9], double (&W)[9
     w_(3, 3) = xsub(xmul(a_(1, 1), a_(2, 2)), xmul(a_(1, 2), a_(2, 1)));
 #undef a_
 #undef w_
+    const double y = __drcp_rn(d);
 #pragma unroll
-    for (int e = 0; e < 9; ++e) W[e] = xdiv(W[e], d);
+    for (int e = 0; e < 9; ++e) W[e] = qdiv(W[e], d, y);
     return finite_nz(d);
 }
 
@@ -629,6 +877,160 @@ __global__ void __launch_bounds__(128) k_block_f64(SegTable tab, double *scratch
 }
 
 // ---------------------------------------------------------------------------
+// Block-tridiagonal Thomas, FP64, bit-exact, coefficients staged by bulk
+// copies: one warp per CTA, 32 columns; the 3*B*B + B entries of a level
+// (P, Q, R, f) arrive in a D-stage shared-memory ring, one 256-byte copy per
+// entry issued by one lane.  Same arithmetic as blk_f64_col.
+// ---------------------------------------------------------------------------
+template <int B, int D>
+__global__ void __launch_bounds__(32) k_block_f64_ring(SegTable tab, double *scratch, unsigned *status)
+{
+    constexpr int BB = B * B, NE = 3 * BB + B;
+    extern __shared__ __align__(128) double smem_b[];
+    __shared__ __align__(8) unsigned long long bars[D];
+    const int lane = threadIdx.x;
+    Ring<NE, D> ring{smem_b, bars};
+    ring.init(lane);
+    const long gs = (long)gridDim.x * 32;
+    double *gam = scratch + (long)blockIdx.x * 32 + lane;
+    unsigned q = 0;
+    for (int t = blockIdx.x; t < tab.ntiles; t += gridDim.x) {
+        const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
+        const long col0 = (long)(t - s.tile0) * 32;
+        const long ld = s.ld;
+        const int k2 = s.k2;
+        const bool valid = col0 + lane < s.ncol;
+        // entry e of level k: P/Q/R element e at (k*BB + e)*ld, f component at (k*B + i)*ld
+        const double *src = s.a + col0;
+        long lstride = 0;
+        if (lane < BB) {
+            src = s.a + col0 + lane * ld;
+            lstride = BB * ld;
+        } else if (lane < 2 * BB) {
+            src = s.b + col0 + (lane - BB) * ld;
+            lstride = BB * ld;
+        } else if (lane < 3 * BB) {
+            src = s.c + col0 + (lane - 2 * BB) * ld;
+            lstride = BB * ld;
+        } else if (lane < NE) {
+            src = s.f + col0 + (lane - 3 * BB) * ld;
+            lstride = B * ld;
+        }
+        double *pU = s.x + col0 + lane;
+        const int pre = k2 < D ? k2 : D;
+        for (int j = 0; j < pre; ++j) ring.issue(q + j, src + j * lstride, lane);
+        bool ok = true;
+        double G[BB], z[B];
+        for (int k = 0; k < k2; ++k) {
+            const unsigned qk = q + k;
+            if (!ring.wait(qk)) {
+                ring.drain(qk, q + (k + D < k2 ? k + D : k2));
+                if (lane == 0) report(status, s.status_idx, FLAG_TIMEOUT);
+                return;
+            }
+            double P[BB], Q[BB], R[BB], F[B];
+#pragma unroll
+            for (int e = 0; e < BB; ++e) {
+                P[e] = ring.at(qk, e, lane);
+                Q[e] = ring.at(qk, BB + e, lane);
+                R[e] = ring.at(qk, 2 * BB + e, lane);
+            }
+#pragma unroll
+            for (int i = 0; i < B; ++i) F[i] = ring.at(qk, 3 * BB + i, lane);
+            __syncwarp();
+            fence_proxy_async();
+            if (k + D < k2) ring.issue(qk + D, src + (k + D) * lstride, lane);
+            if (!valid) continue;
+            double Qp[BB], W[BB], v[B];
+            if (k == 0) {
+#pragma unroll
+                for (int e = 0; e < BB; ++e) Qp[e] = Q[e];
+#pragma unroll
+                for (int i = 0; i < B; ++i) v[i] = F[i];
+            } else {
+#pragma unroll
+                for (int m = 0; m < B; ++m)
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        double qv = Q[i + B * m];
+#pragma unroll
+                        for (int n = 0; n < B; ++n) qv = xsub(qv, xmul(P[i + B * n], G[n + B * m]));
+                        Qp[i + B * m] = qv;
+                    }
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    double tv = F[i];
+#pragma unroll
+                    for (int m = 0; m < B; ++m) tv = xsub(tv, xmul(P[i + B * m], z[m]));
+                    v[i] = tv;
+                }
+            }
+            ok = inv_exact<B>(Qp, W) && ok;
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                double tv = xmul(W[i], v[0]);
+#pragma unroll
+                for (int m = 1; m < B; ++m) tv = xadd(tv, xmul(W[i + B * m], v[m]));
+                z[i] = tv;
+                pU[((long)k * B + i) * ld] = tv;
+            }
+            if (k < k2 - 1) {
+#pragma unroll
+                for (int m = 0; m < B; ++m)
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        double g = xmul(W[i], R[B * m]);
+#pragma unroll
+                        for (int n = 1; n < B; ++n) g = xadd(g, xmul(W[i + B * n], R[n + B * m]));
+                        G[i + B * m] = g;
+                        gam[((long)k * BB + i + B * m) * gs] = g;
+                    }
+            }
+        }
+        q += k2;
+        if (!valid) continue;
+        bool fin = true;
+        double un[B], top[B];
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            un[i] = z[i];
+            top[i] = z[i];
+            fin = fin && finite(z[i]);
+        }
+        for (int k = k2 - 2; k >= 0; --k) {
+            double zk[B], Gk[BB], nu[B];
+#pragma unroll
+            for (int i = 0; i < B; ++i) zk[i] = pU[((long)k * B + i) * ld];
+#pragma unroll
+            for (int e = 0; e < BB; ++e) Gk[e] = gam[((long)k * BB + e) * gs];
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                double tv = zk[i];
+#pragma unroll
+                for (int m = 0; m < B; ++m) tv = xsub(tv, xmul(Gk[i + B * m], un[m]));
+                nu[i] = tv;
+                fin = fin && finite(tv);
+            }
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                un[i] = nu[i];
+                pU[((long)k * B + i) * ld] = nu[i];
+            }
+        }
+        if (s.ubc_ratio) {
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                double tv = xmul(__ldg(s.ubc_ratio + i * ld + col0 + lane), top[i]);
+                if (s.ubc_add) tv = xadd(tv, __ldg(s.ubc_add + i * ld + col0 + lane));
+                fin = fin && finite(tv);
+                pU[((long)k2 * B + i) * ld] = tv;
+            }
+        }
+        report(status, s.status_idx, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Block-tridiagonal, FP32 Gamma/z sweeps + FP64 iterative refinement.
 // Pivot blocks Q' = Q - P G and their inverses W stay in FP64; W and
 // G_{k+1} = W R are kept in FP32 in the thread's scratch slots together with
@@ -736,6 +1138,7 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
     // ---- refinement sweeps
     bool conv = false;
     int sw = 0;
+    double dprev = 0.0;
     if (ok) {
         for (sw = 1; sw <= rf.max_sweeps; ++sw) {
             double um[B], u0[B];
@@ -821,10 +1224,11 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
                 }
             }
             if (!(xmax <= DBL_MAX) || !(dmax <= DBL_MAX)) break;
-            if (dmax <= rf.rel_tol * xmax) {
+            if (refine_done(dmax, xmax, dprev, rf.rel_tol)) {
                 conv = true;
                 break;
             }
+            dprev = dmax;
         }
     }
     sweeps = conv ? sw : rf.max_sweeps + 1;
@@ -993,20 +1397,110 @@ __global__ void __launch_bounds__(256) k_level_to_col(const double *__restrict__
     }
 }
 
+// Up to four arrays relaid in one launch (blockIdx.y = array), each with its
+// own row count and input column stride; output column stride shared.
+__global__ void __launch_bounds__(256) k_col_to_level_multi(Relayout r)
+{
+    __shared__ double tile[32][33];
+    const int a = blockIdx.y;
+    const double *__restrict__ in = r.in[a];
+    double *__restrict__ out = r.out[a];
+    const long nrows = r.nrows[a], in_ld = r.in_ld[a], out_ld = r.out_ld, ncols = r.ncols;
+    const long nrt = (nrows + 31) / 32, nct = (ncols + 31) / 32;
+    for (long bt = blockIdx.x; bt < nrt * nct; bt += gridDim.x) {
+        const long r0 = (bt % nrt) * 32, c0 = (bt / nrt) * 32;
+        for (int j = threadIdx.y; j < 32; j += 8) {
+            const long c = c0 + j, rr = r0 + threadIdx.x;
+            if (c < ncols && rr < nrows) tile[j][threadIdx.x] = __ldcs(in + rr + in_ld * c);
+        }
+        __syncthreads();
+        for (int j = threadIdx.y; j < 32; j += 8) {
+            const long rr = r0 + j, c = c0 + threadIdx.x;
+            if (rr < nrows && c < ncols) out[rr * out_ld + c] = tile[threadIdx.x][j];
+        }
+        __syncthreads();
+    }
+}
+
+// Division self-test: q[i] = a[i]/b[i] through qdiv (Markstein where safe).
+__global__ void k_selftest_division(const double *a, const double *b, double *q, long n)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        q[i] = qdiv(a[i], b[i], __drcp_rn(b[i]));
+}
+
+cudaError_t launch_selftest_division(const double *a, const double *b, double *q, long n, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    k_selftest_division<<<1184, 256, 0, st>>>(a, b, q, n);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // Launch shapes and launchers
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int kPF = 4;
 struct TileCfg {
-    int cpb, cpt;
+    int cpb, cpt, stages;  // register kernel: columns per block / per thread; ring depth (0: no ring)
+    int w2g;               // scalar register kernel: w2 in global scratch instead of shared memory
+    int pf;                // scalar register kernels: levels of coefficient loads in flight per column
 };
 // [kind index: scalar, block2, block3][precision]
-TileCfg g_tile[3][2] = {{{128, 1}, {128, 1}}, {{64, 1}, {64, 1}}, {{64, 1}, {64, 1}}};
-const TileCfg kDefaultTile[3][2] = {{{128, 1}, {128, 1}}, {{64, 1}, {64, 1}}, {{64, 1}, {64, 1}}};
+// Defaults: the fastest shapes on the 2.5 deg column step (10368 x 57) on a
+// B200 (autotune.py sweep): scalar FP64 register kernel 256x1; 2x2 block
+// ring depth 16; 3x3 block register kernel 128; refinement kernels 128 / 32 / 128.
+const TileCfg kDefaultTile[3][2] = {{{256, 1, 0, 0, 4}, {128, 1, 0, 0, 4}}, {{64, 1, 16, 0, 4}, {32, 1, 0, 0, 4}},
+                                     {{128, 1, 0, 0, 4}, {128, 1, 0, 0, 4}}};
+TileCfg g_tile[3][2] = {{{256, 1, 0, 0, 4}, {128, 1, 0, 0, 4}}, {{64, 1, 16, 0, 4}, {32, 1, 0, 0, 4}},
+                        {{128, 1, 0, 0, 4}, {128, 1, 0, 0, 4}}};
 int kind_index(int kind) { return kind == TG_KIND_SCALAR ? 0 : (kind == TG_KIND_BLOCK2 ? 1 : 2); }
 int g_num_sms = -1;
 int g_smem_optin = -1;
+
+// Register-prefetch scalar kernels by (columns per thread, prefetch depth).
+template <typename F>
+cudaError_t with_scalar_reg(int cpt, int pf, F f)
+{
+    if (cpt == 2) {
+        switch (pf) {
+        case 4: return f(k_scalar_f64<2, 4>);
+        case 8: return f(k_scalar_f64<2, 8>);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (pf) {
+    case 4: return f(k_scalar_f64<1, 4>);
+    case 8: return f(k_scalar_f64<1, 8>);
+    case 16: return f(k_scalar_f64<1, 16>);
+    default: return cudaErrorInvalidValue;
+    }
+}
+template <typename F>
+cudaError_t with_scalar_g(int pf, F f)
+{
+    switch (pf) {
+    case 4: return f(k_scalar_f64_g<4>);
+    case 8: return f(k_scalar_f64_g<8>);
+    case 16: return f(k_scalar_f64_g<16>);
+    default: return cudaErrorInvalidValue;
+    }
+}
+template <typename F>
+cudaError_t with_scalar_refine(int pf, F f)
+{
+    switch (pf) {
+    case 4: return f(k_scalar_refine<4>);
+    case 8: return f(k_scalar_refine<8>);
+    case 16: return f(k_scalar_refine<16>);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename K>
+void allow_smem(K k, int lim)
+{
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
 
 int num_sms()
 {
@@ -1018,9 +1512,20 @@ int num_sms()
         // every kernel that takes dynamic shared memory may use up to the
         // opt-in limit (minus its static shared memory)
         const int lim = g_smem_optin - 1024;
-        cudaFuncSetAttribute(k_scalar_f64<1, kPF>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-        cudaFuncSetAttribute(k_scalar_f64<2, kPF>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-        cudaFuncSetAttribute(k_scalar_refine<kPF>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        for (int pf : {4, 8, 16}) {
+            with_scalar_reg(1, pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+            with_scalar_reg(2, pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+            with_scalar_refine(pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+        }
+        allow_smem(k_scalar_f64_ring<4>, lim);
+        allow_smem(k_scalar_f64_ring<8>, lim);
+        allow_smem(k_scalar_f64_ring<16>, lim);
+        allow_smem(k_block_f64_ring<2, 4>, lim);
+        allow_smem(k_block_f64_ring<2, 8>, lim);
+        allow_smem(k_block_f64_ring<2, 16>, lim);
+        allow_smem(k_block_f64_ring<3, 4>, lim);
+        allow_smem(k_block_f64_ring<3, 8>, lim);
+        allow_smem(k_block_f64_ring<3, 16>, lim);
     }
     return g_num_sms;
 }
@@ -1031,16 +1536,76 @@ cudaError_t occupancy(K kernel, int threads, size_t smem, int *per_sm)
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kernel, threads, smem);
 }
 
+template <typename F>
+cudaError_t with_scalar_ring(int D, F f)
+{
+    switch (D) {
+    case 4: return f(k_scalar_f64_ring<4>);
+    case 8: return f(k_scalar_f64_ring<8>);
+    case 16: return f(k_scalar_f64_ring<16>);
+    default: return cudaErrorInvalidValue;
+    }
+}
+template <typename F>
+cudaError_t with_block_ring(int B, int D, F f)
+{
+    if (B == 2) {
+        switch (D) {
+        case 4: return f(k_block_f64_ring<2, 4>);
+        case 8: return f(k_block_f64_ring<2, 8>);
+        case 16: return f(k_block_f64_ring<2, 16>);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (D) {
+    case 4: return f(k_block_f64_ring<3, 4>);
+    case 8: return f(k_block_f64_ring<3, 8>);
+    case 16: return f(k_block_f64_ring<3, 16>);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 // Resident threads per SM allowed for the block kernels: their Gamma scratch
 // (k2 * B*B doubles per resident thread) should stay well inside L2.
 constexpr double kBlockScratchBudget = 48.0 * 1024 * 1024;
 }  // namespace
 
-int cols_per_block(int kind, int precision)
+int prefetch_depth(int kind, int precision) { return g_tile[kind_index(kind)][precision ? 1 : 0].pf; }
+void set_prefetch(int kind, int precision, int pf)
+{
+    TileCfg &t = g_tile[kind_index(kind)][precision ? 1 : 0];
+    t.pf = pf > 0 ? pf : kDefaultTile[kind_index(kind)][precision ? 1 : 0].pf;
+}
+
+void tile_for(int kind, int precision, bool ring_ok, int *cpb, int *cpt, int *stages, int *w2g)
 {
     const TileCfg &t = g_tile[kind_index(kind)][precision ? 1 : 0];
-    return t.cpb;
+    *w2g = 0;
+    if (precision == TG_PREC_F64 && t.stages > 0 && ring_ok) {
+        *cpb = 32;
+        *cpt = 1;
+        *stages = t.stages;
+    } else {
+        *cpb = t.cpb;
+        *cpt = t.cpt;
+        *stages = 0;
+        if (kind == TG_KIND_SCALAR && precision == TG_PREC_F64 && t.w2g) {
+            *w2g = 1;
+            *cpb = t.cpb / t.cpt;
+            *cpt = 1;
+        }
+    }
 }
+
+void set_w2g(int kind, int precision, int on)
+{
+    TileCfg &t = g_tile[kind_index(kind)][precision ? 1 : 0];
+    t.w2g = on >= 0 ? on : kDefaultTile[kind_index(kind)][precision ? 1 : 0].w2g;
+}
+
+size_t scalar_scratch_bytes(long slots, int k2max) { return (size_t)slots * (size_t)(k2max > 1 ? k2max - 1 : 1) * 8; }
+
+int cols_per_block(int kind, int precision) { return g_tile[kind_index(kind)][precision ? 1 : 0].cpb; }
 int cols_per_thread(int kind, int precision) { return g_tile[kind_index(kind)][precision ? 1 : 0].cpt; }
 void set_tile(int kind, int precision, int cpb, int cpt)
 {
@@ -1050,12 +1615,21 @@ void set_tile(int kind, int precision, int cpb, int cpt)
     t.cpt = cpt > 0 ? cpt : d.cpt;
     if (kind != TG_KIND_SCALAR || precision) t.cpt = 1;
 }
-
-size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max)
+void set_stages(int kind, int precision, int stages)
 {
-    if (precision == TG_PREC_F64) return (size_t)threads * cpt * (size_t)(k2max > 1 ? k2max - 1 : 1) * 8;
+    TileCfg &t = g_tile[kind_index(kind)][precision ? 1 : 0];
+    t.stages = stages >= 0 ? stages : kDefaultTile[kind_index(kind)][precision ? 1 : 0].stages;
+}
+
+size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages)
+{
+    const size_t lev = (size_t)(k2max > 1 ? k2max - 1 : 1);
+    if (stages > 0) return (size_t)stages * 4 * 32 * 8 + 32 * lev * 8;
+    if (precision == TG_PREC_F64) return (size_t)threads * cpt * lev * 8;
     return (size_t)threads * 3 * (size_t)k2max * 4;
 }
+
+size_t block_smem_bytes(int B, int stages) { return stages > 0 ? (size_t)stages * (3 * B * B + B) * 32 * 8 : 0; }
 
 size_t block_scratch_bytes(int B, int precision, long slots, int k2max)
 {
@@ -1063,26 +1637,37 @@ size_t block_scratch_bytes(int B, int precision, long slots, int k2max)
     return (size_t)slots * (2 * B * B + B) * (size_t)k2max * 4;
 }
 
-cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, Shape *sh)
+cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, int cpt, int stages, int w2g,
+                       Shape *sh)
 {
     const int nsm = num_sms();
-    const TileCfg &t = g_tile[kind_index(kind)][precision ? 1 : 0];
     int per_sm = 0;
     cudaError_t e = cudaSuccess;
-    sh->cpt = t.cpt;
-    sh->threads = t.cpb / t.cpt;
+    sh->cpt = cpt;
+    sh->threads = cpb / cpt;
+    sh->stages = stages;
+    sh->w2g = w2g;
+    sh->pf = prefetch_depth(kind, precision);
+    if (kind == TG_KIND_SCALAR && sh->cpt == 2 && sh->pf > 8) sh->pf = 8;
     if (kind == TG_KIND_SCALAR) {
-        sh->smem = scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max);
+        sh->smem = w2g ? 0 : scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max, stages);
         if (sh->smem > (size_t)(g_smem_optin - 1024)) return cudaErrorInvalidConfiguration;
-        if (precision == TG_PREC_F64)
-            e = sh->cpt == 2 ? occupancy(k_scalar_f64<2, kPF>, sh->threads, sh->smem, &per_sm)
-                             : occupancy(k_scalar_f64<1, kPF>, sh->threads, sh->smem, &per_sm);
+        auto occ = [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); };
+        if (w2g)
+            e = with_scalar_g(sh->pf, occ);
+        else if (stages > 0)
+            e = with_scalar_ring(stages, [&](auto k) { return occupancy(k, 32, sh->smem, &per_sm); });
+        else if (precision == TG_PREC_F64)
+            e = with_scalar_reg(sh->cpt, sh->pf, occ);
         else
-            e = occupancy(k_scalar_refine<kPF>, sh->threads, sh->smem, &per_sm);
+            e = with_scalar_refine(sh->pf, occ);
     } else {
         const int B = kind;
-        sh->smem = 0;
-        if (precision == TG_PREC_F64)
+        sh->smem = block_smem_bytes(B, stages);
+        if (sh->smem > (size_t)(g_smem_optin - 1024)) return cudaErrorInvalidConfiguration;
+        if (stages > 0)
+            e = with_block_ring(B, stages, [&](auto k) { return occupancy(k, 32, sh->smem, &per_sm); });
+        else if (precision == TG_PREC_F64)
             e = B == 2 ? occupancy(k_block_f64<2>, sh->threads, 0, &per_sm)
                        : occupancy(k_block_f64<3>, sh->threads, 0, &per_sm);
         else
@@ -1102,18 +1687,33 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, Shape *sh
     return cudaSuccess;
 }
 
-cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, Refine rf,
+cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, Refine rf, double *scratch,
                           unsigned *status, unsigned long long *hist, cudaStream_t st)
 {
     if (tab.ntiles <= 0) return cudaSuccess;
-    if (precision == TG_PREC_F64) {
-        if (sh.cpt == 2)
-            k_scalar_f64<2, kPF><<<sh.blocks, sh.threads, sh.smem, st>>>(tab, status);
-        else
-            k_scalar_f64<1, kPF><<<sh.blocks, sh.threads, sh.smem, st>>>(tab, status);
+    cudaError_t e = cudaSuccess;
+    if (precision == TG_PREC_F64 && sh.w2g) {
+        e = with_scalar_g(sh.pf, [&](auto k) {
+            k<<<sh.blocks, sh.threads, 0, st>>>(tab, scratch, status);
+            return cudaSuccess;
+        });
+    } else if (precision == TG_PREC_F64 && sh.stages > 0) {
+        e = with_scalar_ring(sh.stages, [&](auto k) {
+            k<<<sh.blocks, 32, sh.smem, st>>>(tab, status);
+            return cudaSuccess;
+        });
+    } else if (precision == TG_PREC_F64) {
+        e = with_scalar_reg(sh.cpt, sh.pf, [&](auto k) {
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(tab, status);
+            return cudaSuccess;
+        });
     } else {
-        k_scalar_refine<kPF><<<sh.blocks, sh.threads, sh.smem, st>>>(tab, rf, status, hist);
+        e = with_scalar_refine(sh.pf, [&](auto k) {
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(tab, rf, status, hist);
+            return cudaSuccess;
+        });
     }
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
@@ -1121,7 +1721,13 @@ cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape 
                          double *scratch, unsigned *status, unsigned long long *hist, cudaStream_t st)
 {
     if (tab.ntiles <= 0) return cudaSuccess;
-    if (precision == TG_PREC_F64) {
+    if (precision == TG_PREC_F64 && sh.stages > 0) {
+        cudaError_t e = with_block_ring(B, sh.stages, [&](auto k) {
+            k<<<sh.blocks, 32, sh.smem, st>>>(tab, scratch, status);
+            return cudaSuccess;
+        });
+        if (e != cudaSuccess) return e;
+    } else if (precision == TG_PREC_F64) {
         if (B == 2)
             k_block_f64<2><<<sh.blocks, sh.threads, 0, st>>>(tab, scratch, status);
         else
@@ -1148,6 +1754,20 @@ cudaError_t launch_col_to_level(const double *in, long in_ld, double *out, long 
 {
     if (nrows <= 0 || ncols <= 0) return cudaSuccess;
     k_col_to_level<<<relayout_blocks(nrows, ncols), dim3(32, 8), 0, st>>>(in, in_ld, out, out_ld, nrows, ncols);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_col_to_level_multi(const Relayout &r, cudaStream_t st)
+{
+    long tiles = 0;
+    for (int a = 0; a < r.n; ++a) {
+        const long t = ((r.nrows[a] + 31) / 32) * ((r.ncols + 31) / 32);
+        tiles = t > tiles ? t : tiles;
+    }
+    if (tiles <= 0 || r.n <= 0) return cudaSuccess;
+    const long cap = (long)num_sms() * 4;
+    const int bx = (int)(tiles < cap ? tiles : cap);
+    k_col_to_level_multi<<<dim3(bx, r.n), dim3(32, 8), 0, st>>>(r);
     return cudaGetLastError();
 }
 

@@ -74,7 +74,7 @@ int device_ptrs(DevPtrs *out)
 __global__ void k_noalloc_status(const unsigned *flags, int *out)
 {
     const unsigned f = *flags;
-    *out = (f & tg::FLAG_PIVOT) ? TG_EPIVOT : (f & tg::FLAG_NONFINITE) ? TG_ENONFINITE : TG_OK;
+    *out = (f & tg::FLAG_TIMEOUT) ? TG_ETIMEOUT : (f & tg::FLAG_PIVOT) ? TG_EPIVOT : (f & tg::FLAG_NONFINITE) ? TG_ENONFINITE : TG_OK;
 }
 
 }  // namespace
@@ -128,10 +128,8 @@ extern "C" __attribute__((visibility("default"))) int tg_blksolve_dev_noalloc(
         tab.k2max = k2;
         tab.one = seg;
         tg::Shape sh{};
-        e = tg::plan_shape(B, TG_PREC_F64, k2, tab.ntiles, &sh);
+        e = tg::plan_shape(B, TG_PREC_F64, k2, tab.ntiles, threads, 1, 0, 0, &sh);
         if (e == cudaSuccess) {
-            sh.threads = threads;
-            sh.cpt = 1;
             const long cap_blocks = max_slots / threads;
             if (sh.blocks > cap_blocks) sh.blocks = (int)cap_blocks;
             e = tg::launch_block(tab, B, TG_PREC_F64, sh, tg::Refine{1, 0.5}, p.scratch, p.flags, nullptr, st);

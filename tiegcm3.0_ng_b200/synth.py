@@ -218,3 +218,73 @@ def column_step(wl, grid, sub=0, sys_count=None):
     if wl.block:
         blk = block_system(wl.block, grid.nk, grid.ncol, grid.dz, base + 50, wl.d0_range, wl.loss, wl.d_span)
     return scal, blk
+
+
+# ---------------------------------------------------------------------------
+# Physical inputs of the column assembly (dt_ng)
+# ---------------------------------------------------------------------------
+def level_constants(nk, dz, zibot=-7.0, dif0=5.0e-6, prndtl=1.0):
+    """expz, expzmid, expzmid_inv, difk, dift of one grid, built by the
+    recurrences of src/set_const_fields_ng.F90:50-60 (difk/dift start from the
+    bottom-level background values of src/cons.F:244-249)."""
+    expdz = np.exp(-dz)
+    expz = np.empty(nk)
+    difk = np.empty(nk)
+    dift = np.empty(nk)
+    expz[0] = np.exp(-zibot - .5 * dz)
+    difk[0] = dif0
+    dift[0] = dif0 / prndtl
+    for k in range(1, nk):
+        expz[k] = expz[k - 1] * expdz
+        difk[k] = difk[k - 1] * expdz
+        dift[k] = dift[k - 1] * expdz
+    expzmid = np.exp(-.5 * dz)
+    return dict(expz=expz, expzmid=expzmid, expzmid_inv=1. / expzmid, difk=difk, dift=dift)
+
+
+DT_FIELDS = ("tn", "tnsmooth", "horadv", "un", "vn", "o1", "mbar", "xnmbar", "scht", "schti", "cp", "kt", "km",
+             "hdt", "qji_tn", "cool_imp", "cool_exp", "w", "qtotal", "rkm12")
+DT_2D = ("tlbc", "t_lbc", "ulbc", "vlbc")
+
+
+def dt_inputs(nk, ncol, dz, seed, step=60.0):
+    """Seeded physical fields of the dt_ng column assembly with the model's
+    magnitudes (CGS units, as in the reference): Tn rising from ~200 K to
+    ~1000 K, scale heights of 1e6-6e6 cm, specific heat ~1e7 erg/g/K, and so on.
+    Returns (fields dict of (nk,ncol) / (ncol) / (nk) arrays, constants dict)."""
+    rng = _rng(seed)
+    z = np.linspace(0.0, 1.0, nk)[:, None]
+    U = lambda lo, hi, shape=(nk, ncol): rng.uniform(lo, hi, size=shape)
+    f = {}
+    tn = 200.0 + 800.0 * z ** 0.7 * U(0.9, 1.1)
+    f["tn"] = tn
+    f["tnsmooth"] = tn * U(0.99, 1.01)
+    f["horadv"] = U(-1e-3, 1e-3)
+    f["un"] = U(-5e3, 5e3)
+    f["vn"] = U(-5e3, 5e3)
+    f["o1"] = 0.05 + 0.8 * z * U(0.9, 1.1)
+    f["mbar"] = 28.0 - 12.0 * z * U(0.95, 1.05)
+    f["xnmbar"] = 1e13 * np.exp(-10.0 * z) * U(0.5, 1.5)
+    f["scht"] = 1e6 + 5e6 * z * U(0.9, 1.1)
+    f["schti"] = f["scht"] * U(0.95, 1.05)
+    f["cp"] = 1e7 * (1.0 + 0.5 * z) * U(0.95, 1.05)
+    f["kt"] = 10.0 * tn ** 0.69 * U(0.9, 1.1)
+    f["km"] = 3e-4 * tn ** 0.69 * U(0.9, 1.1)
+    f["hdt"] = U(-1e-2, 1e-2)
+    f["qji_tn"] = U(0.0, 1e-2)
+    f["cool_imp"] = U(1e-6, 1e-4)
+    f["cool_exp"] = U(-1e-3, 1e-3)
+    f["w"] = U(-1e-4, 1e-4)
+    f["qtotal"] = U(0.0, 5e-2) * (1.0 + z)
+    f["rkm12"] = U(1e-33, 1e-32)
+    for k in DT_FIELDS:
+        f[k] = np.asfortranarray(f[k])
+    f["tlbc"] = rng.uniform(190.0, 210.0, ncol)
+    f["t_lbc"] = rng.uniform(190.0, 210.0, ncol)
+    f["ulbc"] = rng.uniform(-1e3, 1e3, ncol)
+    f["vlbc"] = rng.uniform(-1e3, 1e3, ncol)
+    lc = level_constants(nk, dz)
+    f["expz"], f["dift"] = lc["expz"], lc["dift"]
+    c = dict(dz=dz, dtx2inv=1.0 / (2.0 * step), expzmid_inv=lc["expzmid_inv"], grav=870.0, p0=5.0e-4,
+             avo=6.023e23, gask=8.314e7, tsurplus=5.11 * 1.602e-12, rmassinv_o1=1.0 / 16.0)
+    return f, c
