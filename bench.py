@@ -56,7 +56,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--profile", default=None,
                    help="run only one kind's plan for a profiler: KIND:PREC[:VARIANT], KIND scalar|block, "
-                        "PREC f64|refine, VARIANT reg:CPB:CPT[:PF], regg:CPB:1[:PF] or ring:DEPTH (default: library default)")
+                        "PREC f64|refine, VARIANT reg:CPB:CPT[:PF], regg:CPB:1[:PF], ring[g]:DEPTH[:WARPS] "
+                        "(default: library default)")
     return p.parse_args()
 
 
@@ -227,7 +228,7 @@ def run_profile(args):
     prec = cs.TG_PREC_F64 if parts[1] == "f64" else cs.TG_PREC_F32_REFINE
     if len(parts) > 2:
         v = parts[2]
-        cand = ("ring", int(parts[3]), 0, 4) if v == "ring" else \
+        cand = (v, int(parts[3]), int(parts[4]) if len(parts) > 4 else 4, 4) if v in ("ring", "ringg") else \
             (v, int(parts[3]), int(parts[4]), int(parts[5]) if len(parts) > 5 else 4)
         autotune.apply(kind, prec, cand)
     dw = pkg.batch.DeviceWorkload(wl, "cuda", max_sub=args.max_sub)
@@ -400,26 +401,58 @@ def main():
                 hb.append(nv)
         h2d = sum(4 * a.nbytes for (a, *_r) in hs) + (sum(v.nbytes for v in hb[:4]) if hb else 0)
         d2h = sum(arr[4].nbytes for arr in hs) + (hb[4].nbytes if hb else 0)
-        def e2e_step():
+        systems = [dict(kind=cs.TG_KIND_SCALAR, a=a, b=b, c=c, f=f, x=x, k2=a.shape[0]) for (a, b, c, f, x) in hs]
+        if hb:
+            P, Q, R, f, u = hb
+            systems.append(dict(kind=wl.block, a=P, b=Q, c=R, f=f, x=u, k2=f.shape[1]))
+
+        def e2e_step():            # one pipelined C-ABI call for the whole step
+            cs.solve_host(systems)
+
+        def e2e_percall():         # the per-routine drop-ins, one call per system
             for (a, b, c, f, x) in hs:
                 cs.trsolv_ng(a, b, c, f, x, a.shape[0])
             if hb:
                 P, Q, R, f, u = hb
                 cs.blksolve(P, Q, R, f, u, f.shape[1])
-        for _ in range(max(1, min(args.warmup, 3))):
-            e2e_step()
-        torch.cuda.synchronize()
-        barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            e2e_step()
-        torch.cuda.synchronize()
-        dt = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps)
+
+        def time_host(fn):
+            for _ in range(max(1, min(args.warmup, 3))):
+                fn()
+            torch.cuda.synchronize()
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(args.e2e_steps):
+                fn()
+            torch.cuda.synchronize()
+            return max_over_ranks((time.perf_counter() - t0) / args.e2e_steps)
+        dt = time_host(e2e_step)
+        dt_pc = time_host(e2e_percall)
+        # the link this path is bound by: pinned host<->device copy bandwidth
+        hbuf = torch.empty(h2d // 8, dtype=torch.float64, pin_memory=True)
+        dbuf = torch.empty(h2d // 8, dtype=torch.float64, device=dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        cstream = torch.cuda.Stream(device=dev)
+        with torch.cuda.stream(cstream):
+            dbuf.copy_(hbuf, non_blocking=True)
+            ev[0].record(cstream)
+            dbuf.copy_(hbuf, non_blocking=True)
+            ev[1].record(cstream)
+            hbuf.copy_(dbuf, non_blocking=True)
+            ev[2].record(cstream)
+        cstream.synchronize()
+        h2d_gbs = h2d / (ev[0].elapsed_time(ev[1]) * 1e-3) / 1e9
+        d2h_gbs = h2d / (ev[1].elapsed_time(ev[2]) * 1e-3) / 1e9
+        del hbuf, dbuf
         e2e_unk = cpu_unknowns([tuple(h[:4]) for h in hs], tuple(hb[:4]) if hb else None)
         e2e = {"value": world * e2e_unk / dt, "unit": "unknowns/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3, "steps": args.e2e_steps,
-               "path": "tg_trsolv_ng x7 + tg_blksolve, pinned host Fortran-layout arrays, FP64",
-               "timer": "host wall clock around synchronous C-ABI calls"}
+               "path": "tg_solve_host (all systems of the step in one call), pinned host Fortran-layout arrays, FP64",
+               "timer": "host wall clock around synchronous C-ABI calls",
+               "per_call_drop_ins": {"value": world * e2e_unk / dt_pc, "ms_per_step": dt_pc * 1e3,
+                                     "path": "tg_trsolv_ng x7 + tg_blksolve"},
+               "link": {"h2d_GBps": h2d_gbs, "d2h_GBps": d2h_gbs,
+                        "h2d_bound_ms_per_step": h2d / h2d_gbs / 1e6}}
         del keep
 
     if rank == 0 and not args.skip_cpu and world == 1:

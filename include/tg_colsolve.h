@@ -122,6 +122,23 @@ int tg_blksolve(int B, const double *P, const double *Q, const double *R, const 
                 const double *ubc_ratio, const double *ubc_add, double *u, int nk, int k2,
                 int ncol);
 
+/* Many independent systems of one model stage in one call (host arrays,
+ * Fortran layout, synchronous): e.g. the scalar species of a step together
+ * with the major-species block system.  The host<->device copies of all
+ * systems are pipelined together, so the call costs about the transfer time
+ * of its bytes rather than the sum of per-system calls.  Scalar systems take
+ * a,b,c,f,x as in tg_trsolv_ng; block systems (kind 2 or 3) P,Q,R in a,b,c
+ * and u in x, as in tg_blksolve. */
+typedef struct {
+    int kind;               /* tg_kind                                        */
+    int nk, k2, ncol;       /* levels, rows solved, columns                   */
+    const double *a, *b, *c, *f;
+    double *x;
+    const double *ubc_ratio, *ubc_add;   /* block only, optional               */
+} tg_host_system;
+
+int tg_solve_host(const tg_host_system *sys, int nsys);
+
 /* ---- device-pointer entry points, stream-ordered ----------------------------
  * Pointers are device memory.  layout selects TG_LAYOUT_COLUMN (ld ignored)
  * or TG_LAYOUT_LEVEL (ld = column stride in elements, ld >= ncol).  stream is
@@ -241,10 +258,11 @@ int tg_set_tile(int kind, int precision, int cols_per_block, int cols_per_thread
 /* Coefficient staging of the FP64 kernels of a kind: 0 = register-prefetch
  * kernel (shape from tg_set_tile); 4, 8 or 16 = depth in levels of the
  * shared-memory ring that bulk asynchronous copies fill ahead of the sweep
- * (one warp per 32 columns; used when the level-major column stride is a
- * multiple of 32 and the arrays are 16-byte aligned, otherwise the
- * register-prefetch kernel runs); -1 restores the default. */
-int tg_set_pipeline(int kind, int precision, int stages);
+ * (one warp per 32 columns, `warps` independent warps per CTA, 1..8, 0 keeps
+ * the current count; used when the level-major column stride is a multiple
+ * of 32 and the arrays are 16-byte aligned, otherwise the register-prefetch
+ * kernel runs); -1 restores the default. */
+int tg_set_pipeline(int kind, int precision, int stages, int warps);
 /* Depth (levels) of the register prefetch of the scalar kernels' coefficient
  * loads: 4, 8 or 16 (kind TG_KIND_SCALAR, either precision); -1 restores the
  * default.  Deeper prefetch keeps more bytes in flight per column at the cost

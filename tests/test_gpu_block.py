@@ -84,3 +84,26 @@ def test_singular_block_flagged(cuda, pkg, orc):
     u = np.zeros_like(f, order="F")
     assert pkg.comp_blksolve_ng(P, Q, R, f, u) == pkg.TG_EPIVOT
     assert np.array_equal(u[:, :11], orc.blksolve(P, Q, R, f, 11)[:, :11], equal_nan=True)
+
+
+def test_solve_host_mixed_batch(cuda, pkg, orc):
+    """tg_solve_host: scalar and block systems of one stage in one pipelined call."""
+    systems, refs = [], []
+    for i, (nk, ncol) in enumerate(((57, 10368), (57, 3001), (29, 777))):
+        a, b, c, f = pkg.synth.scalar_system(nk, ncol, 14.0 / (nk - 1), 500 + i)
+        x = np.zeros_like(a, order="F")
+        systems.append(dict(kind=pkg.TG_KIND_SCALAR, a=a, b=b, c=c, f=f, x=x, k2=nk - (i % 2)))
+        refs.append(orc.trsolv_ng(a, b, c, f, nk - (i % 2)))
+    for B in (2, 3):
+        P, Q, R, f = pkg.synth.block_system(B, 57, 2000, 0.25, 600 + B)
+        ratio = np.asfortranarray(np.random.default_rng(B).uniform(0.5, 1.5, (B, 2000)))
+        u = np.zeros_like(f, order="F")
+        systems.append(dict(kind=B, a=P, b=Q, c=R, f=f, x=u, k2=56, ubc_ratio=ratio))
+        refs.append(orc.blksolve(P, Q, R, f, 56, ubc_ratio=ratio))
+    assert pkg.solve_host(systems) == pkg.TG_OK
+    for q, ref in zip(systems, refs):
+        k2 = q["k2"]
+        if q["kind"] == pkg.TG_KIND_SCALAR:
+            assert np.array_equal(q["x"][:k2], ref[:k2])
+        else:
+            assert np.array_equal(q["x"][:, :k2 + 1], ref[:, :k2 + 1])

@@ -112,12 +112,14 @@ def test_two_columns_per_thread(cuda, pkg, orc):
     ta, tb, tc, tf = (pkg.batch.level_scalar(v, ld, "cuda") for v in (a, b, c, f))
     tx = torch.zeros((nk, ld), dtype=torch.float64, device="cuda")
     cs.set_pipeline(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 0)
+    cs.set_scratch_global(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 0)
     cs.set_tile(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 128, 2)
     try:
         pkg.trsolv_dev(ta, tb, tc, tf, tx, nk, nk, 777, pkg.TG_LAYOUT_LEVEL, ld)
         torch.cuda.synchronize()
     finally:
         cs.set_tile(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, 0, 0)
+        cs.set_scratch_global(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, -1)
         cs.set_pipeline(cs.TG_KIND_SCALAR, cs.TG_PREC_F64, -1)
     assert np.array_equal(pkg.batch.from_level_scalar(tx, 777), ref)
     assert torch.all(tx[:, 777:] == 0)  # padding columns are not written

@@ -7,7 +7,8 @@ from a CUDA graph, CUDA-event timed) and keeps the fastest:
   FP64      register-prefetch kernel: columns per block x columns per thread x
             prefetch depth, w2 scratch in shared memory ("reg") or global
             memory ("regg")
-            bulk-copy ring kernel: staging depth 4, 8 or 16 levels
+            bulk-copy ring kernel: staging depth 4, 8 or 16 levels, w2 in shared
+            ("ring") or global ("ringg") memory
   FP32+ref  columns per block x prefetch depth
 
 Results are cached in a JSON file keyed by GPU name, kind, precision, level
@@ -25,9 +26,11 @@ CACHE_DEFAULT = os.path.join(os.path.expanduser("~"), ".cache", "tg_colsolve_tun
 SCALAR_F64 = [("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg", 256, 1, 8), ("reg", 64, 1, 16),
               ("reg", 128, 1, 16), ("reg", 128, 2, 4), ("reg", 256, 2, 4), ("reg", 128, 2, 8),
               ("regg", 256, 1, 4), ("regg", 128, 1, 8), ("regg", 128, 1, 16),
-              ("ring", 4, 0, 4), ("ring", 8, 0, 4), ("ring", 16, 0, 4)]
-BLOCK_F64 = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("ring", 4, 0, 4), ("ring", 8, 0, 4),
-             ("ring", 16, 0, 4)]
+              ("ring", 4, 4, 4), ("ring", 8, 4, 4), ("ring", 4, 2, 4),
+              ("ringg", 4, 1, 4), ("ringg", 8, 1, 4), ("ringg", 4, 2, 4), ("ringg", 4, 4, 4), ("ringg", 4, 8, 4)]
+BLOCK_F64 = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 96, 1, 4),
+             ("ring", 4, 4, 4), ("ring", 8, 4, 4), ("ring", 4, 2, 4), ("ring", 8, 2, 4), ("ring", 16, 2, 4),
+             ("ring", 4, 1, 4)]
 SCALAR_REF = [("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg", 64, 1, 8)]
 BLOCK_REF = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4)]
 
@@ -44,19 +47,19 @@ def apply(kind, precision, cand):
     scalar64 = kind == cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64
     if kind == cs.TG_KIND_SCALAR:
         cs.set_prefetch(kind, precision, pf)
-    if v == "ring":
-        cs.set_pipeline(kind, precision, p1)
+    if v in ("ring", "ringg"):
+        cs.set_pipeline(kind, precision, p1, p2)    # ring depth, warps per CTA
     else:
         if precision == cs.TG_PREC_F64:
             cs.set_pipeline(kind, precision, 0)
         cs.set_tile(kind, precision, p1, p2)
     if scalar64:
-        cs.set_scratch_global(kind, precision, 1 if v == "regg" else 0)
+        cs.set_scratch_global(kind, precision, 1 if v in ("regg", "ringg") else 0)
 
 
 def reset(kind, precision):
     cs.set_tile(kind, precision, 0, 0)
-    cs.set_pipeline(kind, precision, -1)
+    cs.set_pipeline(kind, precision, -1, 4)
     if kind == cs.TG_KIND_SCALAR:
         cs.set_prefetch(kind, precision, -1)
     if kind == cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64:

@@ -37,7 +37,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
-EXPORTS = ("tg_dt_ng", "tg_dt_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
+EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
@@ -62,6 +62,13 @@ DT_FIELDS = ("tn", "tnsmooth", "horadv", "un", "vn", "o1", "mbar", "xnmbar", "sc
              "hdt", "qji_tn", "cool_imp", "cool_exp", "w", "qtotal", "rkm12", "tlbc", "t_lbc", "ulbc", "vlbc",
              "expz", "dift")
 DT_CONSTS = ("dz", "dtx2inv", "expzmid_inv", "grav", "p0", "avo", "gask", "tsurplus", "rmassinv_o1")
+
+
+class HostSystem(ctypes.Structure):
+    """tg_host_system of include/tg_colsolve.h."""
+    _fields_ = [("kind", ctypes.c_int), ("nk", ctypes.c_int), ("k2", ctypes.c_int), ("ncol", ctypes.c_int),
+                ("a", ctypes.c_void_p), ("b", ctypes.c_void_p), ("c", ctypes.c_void_p), ("f", ctypes.c_void_p),
+                ("x", ctypes.c_void_p), ("ubc_ratio", ctypes.c_void_p), ("ubc_add", ctypes.c_void_p)]
 
 
 class DtFields(ctypes.Structure):
@@ -89,6 +96,7 @@ def lib():
         sig = {
             "tg_trsolv": [P, P, P, P, P, I, I, I, I, I, I, I],
             "tg_dt_ng": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I],
+            "tg_solve_host": [ctypes.POINTER(HostSystem), I],
             "tg_dt_ng_dev": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I, Lg, P, P, P],
             "tg_trsolv_ng": [P, P, P, P, P, I, I, I],
             "tg_blktri": [P, P, P, P, P, I, I, I, I, I],
@@ -107,7 +115,7 @@ def lib():
             "tg_set_refine": [I, D],
             "tg_set_host_precision": [I],
             "tg_set_tile": [I, I, I, I],
-            "tg_set_pipeline": [I, I, I],
+            "tg_set_pipeline": [I, I, I, I],
             "tg_set_scratch_global": [I, I, I],
             "tg_set_prefetch": [I, I, I],
             "tg_selftest_division": [P, P, P, Lg, P],
@@ -227,6 +235,24 @@ def blksolve(P, Q, R, f, u, k2, ubc_ratio=None, ubc_add=None):
     return _check(rc, "tg_blksolve")
 
 
+def solve_host(systems):
+    """tg_solve_host: systems is a list of dicts with kind and the host arrays
+    a, b, c, f, x (Fortran layout; block kinds P, Q, R in a, b, c), k2, and
+    optionally ubc_ratio / ubc_add; all solved in one pipelined call."""
+    arr = (HostSystem * max(len(systems), 1))()
+    for i, q in enumerate(systems):
+        kind = q["kind"]
+        f = q["f"]
+        nk = f.shape[0] if kind == TG_KIND_SCALAR else f.shape[1]
+        B = 1 if kind == TG_KIND_SCALAR else kind
+        ncol = f.size // (B * nk)
+        arr[i] = HostSystem(kind, nk, q.get("k2", nk), ncol, _host(q["a"], "a"), _host(q["b"], "b"),
+                            _host(q["c"], "c"), _host(f, "f"), _out(q["x"], "x"),
+                            None if q.get("ubc_ratio") is None else _host(q["ubc_ratio"], "ubc_ratio"),
+                            None if q.get("ubc_add") is None else _host(q["ubc_add"], "ubc_add"))
+    return _check(lib().tg_solve_host(arr, len(systems)), "tg_solve_host")
+
+
 def dt_ng(fields, consts, tn_upd):
     """dt_ng's vertical column step (src/dt_ng.F90:57-167) on host arrays:
     fields is a dict of the DT_FIELDS arrays (3-D (nk,ncol...) Fortran-ordered,
@@ -323,10 +349,10 @@ def set_tile(kind, precision, cols_per_block=0, cols_per_thread=0):
                   numeric_ok=False)
 
 
-def set_pipeline(kind, precision, stages=-1):
+def set_pipeline(kind, precision, stages=-1, warps=0):
     """Ring depth of the bulk-copy staged FP64 kernels (0: register prefetch,
-    -1: default)."""
-    return _check(lib().tg_set_pipeline(kind, precision, stages), "tg_set_pipeline", numeric_ok=False)
+    -1: default) and their warps per CTA (0: keep)."""
+    return _check(lib().tg_set_pipeline(kind, precision, stages, warps), "tg_set_pipeline", numeric_ok=False)
 
 
 def set_prefetch(kind, precision, levels=-1):

@@ -192,121 +192,170 @@ int solve_level(DevCtx *c, int slot, int kind, int precision, Seg seg, unsigned 
     return TG_OK;
 }
 
-// Host arrays in Fortran layout -> solve -> host x.
+// Host arrays in Fortran layout -> solve -> host x, for a list of systems.
 //   B = 1 (scalar) or 2/3 (block); m[3], v (vectors) point at row 0 of the
 //   solve in column 0; colstride = elements between columns of a vector
 //   array (matrices: B*colstride); k2 rows are solved; ubc arrays (B, ncol).
-// Column chunks of about 4 MB of input are pipelined over kSlots streams:
-// while chunk j is relaid, solved and copied back on its stream, the next
-// chunks' host->device copies are already queued on the others.
-int host_solve(int kind, const double *const m[3], const double *v, double *x, long colstride, int k2,
-               long ncol, const double *ubc_ratio, const double *ubc_add, int precision)
+// Every system is cut into column chunks of about 4 MB of input, and all
+// chunks of all systems are pipelined over kSlots streams: while a chunk is
+// relaid, solved and copied back on its stream, the next chunks' host->device
+// copies are already queued on the others.  One synchronisation at the end.
+struct HostSys {
+    int kind;
+    const double *m[3];
+    const double *v;
+    double *x;
+    long colstride;
+    int k2;
+    long ncol;
+    const double *ubc_ratio, *ubc_add;
+};
+
+struct HostPlan {
+    int B;
+    long mrows, vrows, orows, mstride, chunk;
+};
+
+HostPlan host_plan(const HostSys &h)
 {
-    const int B = kind == TG_KIND_SCALAR ? 1 : kind;
+    HostPlan p;
+    p.B = h.kind == TG_KIND_SCALAR ? 1 : h.kind;
+    p.mrows = (long)p.B * p.B * h.k2;
+    p.vrows = (long)p.B * h.k2;
+    p.orows = (long)p.B * (h.k2 + (h.ubc_ratio ? 1 : 0));
+    p.mstride = (long)p.B * h.colstride;
+    const long in_per_col = (3 * p.mrows + p.vrows) * 8;
+    long nchunks = (in_per_col * h.ncol + (4l << 20) - 1) / (4l << 20);
+    nchunks = std::max<long>(1, std::min<long>(nchunks, 64));
+    p.chunk = round_up((h.ncol + nchunks - 1) / nchunks, 32);
+    return p;
+}
+
+int host_solve_many(const HostSys *sys, int nsys, int precision)
+{
     DevCtx *c = nullptr;
     int rc = get_ctx(&c);
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
     TG_CUDA(cudaSetDevice(c->dev));
-    const long mrows = (long)B * B * k2;         // matrix rows copied per column
-    const long vrows = (long)B * k2;             // vector rows copied per column
-    const long orows = (long)B * (k2 + (ubc_ratio ? 1 : 0));
-    const long mstride = (long)B * colstride;     // matrix column stride (elements)
-    const long in_per_col = (3 * mrows + vrows) * 8;
-    long nchunks = (in_per_col * ncol + (4l << 20) - 1) / (4l << 20);
-    nchunks = std::max<long>(1, std::min<long>(nchunks, 64));
-    const long chunk = round_up((ncol + nchunks - 1) / nchunks, 32);
-    const long ld = chunk;
-    const int nslots = (int)std::min<long>(kSlots, (ncol + chunk - 1) / chunk);
+    std::vector<HostPlan> plans(nsys);
+    long need_m = 0, need_v = 0, need_o = 0, need_u = 0, total_chunks = 0;
+    for (int i = 0; i < nsys; ++i) {
+        plans[i] = host_plan(sys[i]);
+        const HostPlan &p = plans[i];
+        need_m = std::max(need_m, p.mrows * p.chunk);
+        need_v = std::max(need_v, p.vrows * p.chunk);
+        need_o = std::max(need_o, std::max<long>(p.orows, 2l * p.B) * p.chunk);
+        if (sys[i].ubc_ratio) need_u = std::max(need_u, (long)p.B * p.chunk);
+        total_chunks += (sys[i].ncol + p.chunk - 1) / p.chunk;
+    }
+    if (total_chunks == 0) return TG_OK;
+    const int nslots = (int)std::min<long>(kSlots, total_chunks);
     for (int s = 0; s < nslots; ++s) {
         for (int i = 0; i < 3; ++i)
-            if ((rc = grow(c->colbuf[s][i], sizeof(double) * mrows * chunk))) return rc;
-        if ((rc = grow(c->colbuf[s][3], sizeof(double) * vrows * chunk))) return rc;
-        if ((rc = grow(c->colbuf[s][4], sizeof(double) * std::max<long>(orows, 2l * B) * chunk))) return rc;
+            if ((rc = grow(c->colbuf[s][i], sizeof(double) * need_m))) return rc;
+        if ((rc = grow(c->colbuf[s][3], sizeof(double) * need_v))) return rc;
+        if ((rc = grow(c->colbuf[s][4], sizeof(double) * need_o))) return rc;
         for (int i = 0; i < 3; ++i)
-            if ((rc = grow(c->lvlbuf[s][i], sizeof(double) * mrows * ld))) return rc;
-        if ((rc = grow(c->lvlbuf[s][3], sizeof(double) * vrows * ld))) return rc;
-        if ((rc = grow(c->lvlbuf[s][4], sizeof(double) * orows * ld))) return rc;
-        if (ubc_ratio) {
-            if ((rc = grow(c->lvlbuf[s][5], sizeof(double) * B * ld))) return rc;
-            if ((rc = grow(c->lvlbuf[s][6], sizeof(double) * B * ld))) return rc;
+            if ((rc = grow(c->lvlbuf[s][i], sizeof(double) * need_m))) return rc;
+        if ((rc = grow(c->lvlbuf[s][3], sizeof(double) * need_v))) return rc;
+        if ((rc = grow(c->lvlbuf[s][4], sizeof(double) * need_o))) return rc;
+        if (need_u) {
+            if ((rc = grow(c->lvlbuf[s][5], sizeof(double) * need_u))) return rc;
+            if ((rc = grow(c->lvlbuf[s][6], sizeof(double) * need_u))) return rc;
         }
         TG_CUDA(cudaMemsetAsync(c->flags + s, 0, sizeof(unsigned), c->st[s]));
     }
-    int j = 0;
-    for (long c0 = 0; c0 < ncol; c0 += chunk, ++j) {
-        const int s = j % nslots;
-        cudaStream_t st = c->st[s];
-        const long nc = std::min(chunk, ncol - c0);
-        double *lv[7];
-        for (int i = 0; i < 7; ++i) lv[i] = (double *)c->lvlbuf[s][i].p;
-        Relayout r{};
-        r.out_ld = ld;
-        r.ncols = nc;
-        r.n = 4;
-        for (int i = 0; i < 4; ++i) {
-            double *cb = (double *)c->colbuf[s][i].p;
-            const double *src = i < 3 ? m[i] : v;
-            const long rows = i < 3 ? mrows : vrows, stride = i < 3 ? mstride : colstride;
-            if (rows == stride)
-                TG_CUDA(cudaMemcpyAsync(cb, src + c0 * stride, sizeof(double) * rows * nc, cudaMemcpyHostToDevice, st));
-            else
-                TG_CUDA(cudaMemcpy2DAsync(cb, sizeof(double) * rows, src + c0 * stride, sizeof(double) * stride,
-                                          sizeof(double) * rows, nc, cudaMemcpyHostToDevice, st));
-            r.in[i] = cb;
-            r.out[i] = lv[i];
-            r.in_ld[i] = rows;
-            r.nrows[i] = rows;
-        }
-        TG_CUDA(launch_col_to_level_multi(r, st));
-        if (ubc_ratio) {
-            double *cb = (double *)c->colbuf[s][4].p;
-            Relayout u{};
-            u.out_ld = ld;
-            u.ncols = nc;
-            u.n = ubc_add ? 2 : 1;
-            TG_CUDA(cudaMemcpyAsync(cb, ubc_ratio + c0 * B, sizeof(double) * B * nc, cudaMemcpyHostToDevice, st));
-            u.in[0] = cb;
-            u.out[0] = lv[5];
-            u.in_ld[0] = B;
-            u.nrows[0] = B;
-            if (ubc_add) {
-                TG_CUDA(cudaMemcpyAsync(cb + B * chunk, ubc_add + c0 * B, sizeof(double) * B * nc,
-                                        cudaMemcpyHostToDevice, st));
-                u.in[1] = cb + B * chunk;
-                u.out[1] = lv[6];
-                u.in_ld[1] = B;
-                u.nrows[1] = B;
+    long j = 0;
+    for (int si = 0; si < nsys; ++si) {
+        const HostSys &h = sys[si];
+        const HostPlan &p = plans[si];
+        const int B = p.B;
+        const long ld = p.chunk;
+        for (long c0 = 0; c0 < h.ncol; c0 += p.chunk, ++j) {
+            const int s = (int)(j % nslots);
+            cudaStream_t st = c->st[s];
+            const long nc = std::min(p.chunk, h.ncol - c0);
+            double *lv[7];
+            for (int i = 0; i < 7; ++i) lv[i] = (double *)c->lvlbuf[s][i].p;
+            Relayout r{};
+            r.out_ld = ld;
+            r.ncols = nc;
+            r.n = 4;
+            for (int i = 0; i < 4; ++i) {
+                double *cb = (double *)c->colbuf[s][i].p;
+                const double *src = i < 3 ? h.m[i] : h.v;
+                const long rows = i < 3 ? p.mrows : p.vrows, stride = i < 3 ? p.mstride : h.colstride;
+                if (rows == stride)
+                    TG_CUDA(cudaMemcpyAsync(cb, src + c0 * stride, sizeof(double) * rows * nc, cudaMemcpyHostToDevice,
+                                            st));
+                else
+                    TG_CUDA(cudaMemcpy2DAsync(cb, sizeof(double) * rows, src + c0 * stride, sizeof(double) * stride,
+                                              sizeof(double) * rows, nc, cudaMemcpyHostToDevice, st));
+                r.in[i] = cb;
+                r.out[i] = lv[i];
+                r.in_ld[i] = rows;
+                r.nrows[i] = rows;
             }
-            TG_CUDA(launch_col_to_level_multi(u, st));
+            TG_CUDA(launch_col_to_level_multi(r, st));
+            if (h.ubc_ratio) {
+                double *cb = (double *)c->colbuf[s][4].p;
+                Relayout u{};
+                u.out_ld = ld;
+                u.ncols = nc;
+                u.n = h.ubc_add ? 2 : 1;
+                TG_CUDA(cudaMemcpyAsync(cb, h.ubc_ratio + c0 * B, sizeof(double) * B * nc, cudaMemcpyHostToDevice, st));
+                u.in[0] = cb;
+                u.out[0] = lv[5];
+                u.in_ld[0] = B;
+                u.nrows[0] = B;
+                if (h.ubc_add) {
+                    TG_CUDA(cudaMemcpyAsync(cb + B * p.chunk, h.ubc_add + c0 * B, sizeof(double) * B * nc,
+                                            cudaMemcpyHostToDevice, st));
+                    u.in[1] = cb + B * p.chunk;
+                    u.out[1] = lv[6];
+                    u.in_ld[1] = B;
+                    u.nrows[1] = B;
+                }
+                TG_CUDA(launch_col_to_level_multi(u, st));
+            }
+            Seg seg{};
+            seg.a = lv[0];
+            seg.b = lv[1];
+            seg.c = lv[2];
+            seg.f = lv[3];
+            seg.x = lv[4];
+            seg.ubc_ratio = h.ubc_ratio ? lv[5] : nullptr;
+            seg.ubc_add = (h.ubc_ratio && h.ubc_add) ? lv[6] : nullptr;
+            seg.ld = ld;
+            seg.nk = h.k2 + (h.ubc_ratio ? 1 : 0);
+            seg.k2 = h.k2;
+            seg.ncol = (int)nc;
+            seg.kind = h.kind;
+            if ((rc = solve_level(c, s, h.kind, precision, seg, c->flags + s, st))) return rc;
+            double *ob = (double *)c->colbuf[s][4].p;
+            TG_CUDA(launch_level_to_col(lv[4], ld, ob, p.orows, p.orows, nc, st));
+            if (p.orows == h.colstride)
+                TG_CUDA(cudaMemcpyAsync(h.x + c0 * h.colstride, ob, sizeof(double) * p.orows * nc,
+                                        cudaMemcpyDeviceToHost, st));
+            else
+                TG_CUDA(cudaMemcpy2DAsync(h.x + c0 * h.colstride, sizeof(double) * h.colstride, ob,
+                                          sizeof(double) * p.orows, sizeof(double) * p.orows, nc,
+                                          cudaMemcpyDeviceToHost, st));
         }
-        Seg seg{};
-        seg.a = lv[0];
-        seg.b = lv[1];
-        seg.c = lv[2];
-        seg.f = lv[3];
-        seg.x = lv[4];
-        seg.ubc_ratio = ubc_ratio ? lv[5] : nullptr;
-        seg.ubc_add = (ubc_ratio && ubc_add) ? lv[6] : nullptr;
-        seg.ld = ld;
-        seg.nk = k2 + (ubc_ratio ? 1 : 0);
-        seg.k2 = k2;
-        seg.ncol = (int)nc;
-        seg.kind = kind;
-        if ((rc = solve_level(c, s, kind, precision, seg, c->flags + s, st))) return rc;
-        double *ob = (double *)c->colbuf[s][4].p;
-        TG_CUDA(launch_level_to_col(lv[4], ld, ob, orows, orows, nc, st));
-        if (orows == colstride)
-            TG_CUDA(cudaMemcpyAsync(x + c0 * colstride, ob, sizeof(double) * orows * nc, cudaMemcpyDeviceToHost, st));
-        else
-            TG_CUDA(cudaMemcpy2DAsync(x + c0 * colstride, sizeof(double) * colstride, ob, sizeof(double) * orows,
-                                      sizeof(double) * orows, nc, cudaMemcpyDeviceToHost, st));
     }
     for (int s = 0; s < nslots; ++s) TG_CUDA(cudaStreamSynchronize(c->st[s]));
     TG_CUDA(cudaMemcpy(c->flags_host, c->flags, nslots * sizeof(unsigned), cudaMemcpyDeviceToHost));
     unsigned all = 0;
     for (int s = 0; s < nslots; ++s) all |= c->flags_host[s];
     return flags_to_status(all);
+}
+
+int host_solve(int kind, const double *const m[3], const double *v, double *x, long colstride, int k2,
+               long ncol, const double *ubc_ratio, const double *ubc_add, int precision)
+{
+    HostSys h{kind, {m[0], m[1], m[2]}, v, x, colstride, k2, ncol, ubc_ratio, ubc_add};
+    return host_solve_many(&h, 1, precision);
 }
 
 bool bad_prec(int p) { return p != TG_PREC_F64 && p != TG_PREC_F32_REFINE; }
@@ -335,15 +384,15 @@ __attribute__((visibility("default"))) int tg_set_refine(int max_sweeps, double 
     return TG_OK;
 }
 
-__attribute__((visibility("default"))) int tg_set_pipeline(int kind, int precision, int stages)
+__attribute__((visibility("default"))) int tg_set_pipeline(int kind, int precision, int stages, int warps)
 {
     if ((kind != TG_KIND_SCALAR && kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) || bad_prec(precision) ||
         (stages != -1 && stages != 0 && stages != 4 && stages != 8 && stages != 16) ||
-        (stages > 0 && precision != TG_PREC_F64)) {
-        set_err("tg_set_pipeline: stages must be 0, 4, 8 or 16 (FP64 only), or -1 for the default");
+        (stages > 0 && precision != TG_PREC_F64) || warps < 0 || warps > 8) {
+        set_err("tg_set_pipeline: stages must be 0, 4, 8 or 16 (FP64 only) or -1; warps 0..8");
         return TG_EINVAL;
     }
-    set_stages(kind, precision, stages);
+    set_stages(kind, precision, stages, warps);
     return TG_OK;
 }
 
@@ -407,6 +456,31 @@ __attribute__((visibility("default"))) int tg_set_tile(int kind, int precision, 
     }
     set_tile(kind, precision, cols_per_block_, cols_per_thread_);
     return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_solve_host(const tg_host_system *sys, int nsys)
+{
+    if (nsys < 0 || (nsys > 0 && !sys)) {
+        set_err("tg_solve_host: bad arguments");
+        return TG_EINVAL;
+    }
+    std::vector<HostSys> hs;
+    hs.reserve(nsys);
+    for (int i = 0; i < nsys; ++i) {
+        const tg_host_system &q = sys[i];
+        const bool blk = q.kind == TG_KIND_BLOCK2 || q.kind == TG_KIND_BLOCK3;
+        if ((q.kind != TG_KIND_SCALAR && !blk) || !q.a || !q.b || !q.c || !q.f || !q.x || q.nk < 1 || q.k2 < 1 ||
+            q.k2 > q.nk || q.ncol < 0 || (blk && q.ubc_ratio && q.k2 >= q.nk)) {
+            set_err("tg_solve_host: system %d invalid", i);
+            return TG_EINVAL;
+        }
+        if (q.ncol == 0) continue;
+        const int B = blk ? q.kind : 1;
+        hs.push_back(HostSys{q.kind, {q.a, q.b, q.c}, q.f, q.x, (long)B * q.nk, q.k2, q.ncol,
+                             blk ? q.ubc_ratio : nullptr, blk && q.ubc_ratio ? q.ubc_add : nullptr});
+    }
+    if (hs.empty()) return TG_OK;
+    return host_solve_many(hs.data(), (int)hs.size(), g_host_precision);
 }
 
 __attribute__((visibility("default"))) int tg_trsolv_ng(const double *a, const double *b, const double *c,

@@ -65,7 +65,9 @@ int cols_per_block(int kind, int precision);
 int cols_per_thread(int kind, int precision);
 void set_tile(int kind, int precision, int cpb, int cpt);
 // Bulk-copy ring depth of a kind/precision (tg_set_pipeline); 0 disables.
-void set_stages(int kind, int precision, int stages);
+// wpb: independent warps per CTA of the ring kernels (0 keeps the default).
+void set_stages(int kind, int precision, int stages, int wpb);
+int ring_warps(int kind, int precision);
 // Effective tile of a launch: the ring kernel (32 columns per warp-CTA)
 // when configured and ring_ok (ld % 32 == 0, 16-byte aligned bases), else
 // the register-prefetch kernel.
@@ -81,8 +83,8 @@ void set_w2g(int kind, int precision, int on);
 size_t scalar_scratch_bytes(long slots, int k2max);
 
 // Shared memory / scratch needs of a kernel for the largest k2 it will see.
-size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages);
-size_t block_smem_bytes(int B, int stages);
+size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g);
+size_t block_smem_bytes(int B, int stages, int threads);
 // Global scratch (bytes) of a block kernel with `slots` resident threads.
 size_t block_scratch_bytes(int B, int precision, long slots, int k2max);
 

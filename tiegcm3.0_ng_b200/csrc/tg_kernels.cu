@@ -13,6 +13,7 @@
 // src/matutil.F90:25-27,63-71,116).
 #include <cfloat>
 #include <cstdio>
+#include <mutex>
 
 #include "tg_internal.h"
 
@@ -385,19 +386,26 @@ __global__ void __launch_bounds__(256) k_scalar_f64_g(SegTable tab, double *scra
 // ahead, so a warp keeps 4*D*256 bytes of loads in flight without spending
 // registers.  w2 goes to shared memory ([k][lane]), w3 is parked in x.
 // Requires ld % 32 == 0 and 16-byte aligned array bases (checked on the host).
+// With W2G, w2 goes to a global scratch slot (element k at w2s[k*S], S the
+// resident lanes) instead of shared memory, so shared memory holds only the
+// ring and every column of a batch can be resident at once.
 // ---------------------------------------------------------------------------
-template <int D>
-__global__ void __launch_bounds__(32) k_scalar_f64_ring(SegTable tab, unsigned *status)
+template <int D, bool W2G>
+__global__ void __launch_bounds__(256) k_scalar_f64_ring(SegTable tab, double *scratch, unsigned *status)
 {
     constexpr int NE = 4;
+    __shared__ __align__(8) unsigned long long bars[8 * D];
     extern __shared__ __align__(128) double smem_r[];
-    __shared__ __align__(8) unsigned long long bars[D];
-    const int lane = threadIdx.x;
-    Ring<NE, D> ring{smem_r, bars};
-    double *w2s = smem_r + D * NE * 32 + lane;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    // each warp of the CTA is independent: its own ring, barriers and tiles
+    const long per_warp = (long)D * NE * 32 + (W2G ? 0 : (long)32 * (tab.k2max > 1 ? tab.k2max - 1 : 1));
+    double *mine = smem_r + warp * per_warp;
+    Ring<NE, D> ring{mine, bars + warp * D};
+    const long ws = W2G ? (long)gridDim.x * blockDim.x : 32;
+    double *w2s = W2G ? scratch + (long)blockIdx.x * blockDim.x + threadIdx.x : mine + D * NE * 32 + lane;
     ring.init(lane);
     unsigned q = 0;
-    for (int t = blockIdx.x; t < tab.ntiles; t += gridDim.x) {
+    for (int t = blockIdx.x * nwarps + warp; t < tab.ntiles; t += gridDim.x * nwarps) {
         const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
         const long col0 = (long)(t - s.tile0) * 32;
         const long ld = s.ld;
@@ -428,7 +436,7 @@ __global__ void __launch_bounds__(32) k_scalar_f64_ring(SegTable tab, unsigned *
                     w3 = qdiv(fk, w1, y1);
                 } else {
                     const double w2 = qdiv(cprev, w1, y1);
-                    w2s[(k - 1) * 32] = w2;
+                    w2s[(k - 1) * ws] = w2;
                     w1 = xsub(bk, xmul(ak, w2));
                     y1 = __drcp_rn(w1);
                     w3 = qdiv(xsub(fk, xmul(ak, w3)), w1, y1);
@@ -440,20 +448,27 @@ __global__ void __launch_bounds__(32) k_scalar_f64_ring(SegTable tab, unsigned *
         }
         q += k2;
         if (valid) {
+            // back sweep; w3 (in x) and w2 of the next 4 levels in flight
             double xn = w3;
             fin = finite(xn);
-            double rw[4];
+            double rw[4], r2[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (k2 - 2 - u >= 0) rw[u] = px[(k2 - 2 - u) * ld];
+                if (k2 - 2 - u >= 0) {
+                    rw[u] = px[(k2 - 2 - u) * ld];
+                    r2[u] = w2s[(k2 - 2 - u) * ws];
+                }
             for (int kb = k2 - 2; kb >= 0; kb -= 4) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int k = kb - u;
                     if (k >= 0) {
-                        xn = xsub(rw[u], xmul(w2s[k * 32], xn));
+                        xn = xsub(rw[u], xmul(r2[u], xn));
                         fin = fin && finite(xn);
-                        if (k - 4 >= 0) rw[u] = px[(k - 4) * ld];
+                        if (k - 4 >= 0) {
+                            rw[u] = px[(k - 4) * ld];
+                            r2[u] = w2s[(k - 4) * ws];
+                        }
                         px[k * ld] = xn;
                     }
                 }
@@ -750,6 +765,58 @@ __device__ __forceinline__ void blk_load(const double *pP, const double *pQ, con
 // scratch slots (element (k, e) at gam[(k*B*B + e)*gs]), sized so the
 // resident working set stays in L2.  Back: u_k = z_{k+1} - G_{k+1} u_{k+1}.
 // ---------------------------------------------------------------------------
+// Back sweep u_k = z_{k+1} - Gamma_{k+1} u_{k+1} for k = k2-2..0 (z parked in
+// u, Gamma in the scratch slots), keeping the loads of the next BPF levels in
+// flight: every level's operands come from L2, so an unprefetched sweep would
+// wait a full L2 round trip per level.  un holds u_{k2-1} on entry.
+template <int B>
+__device__ __forceinline__ bool blk_back(double *pU, long ld, const double *gam, long gs, int k2, double (&un)[B])
+{
+    constexpr int BB = B * B, BPF = B == 2 ? 4 : 2;
+    bool fin = true;
+    double rz[BPF][B], rg[BPF][BB];
+#pragma unroll
+    for (int u = 0; u < BPF; ++u) {
+        const int k = k2 - 2 - u;
+        if (k >= 0) {
+#pragma unroll
+            for (int i = 0; i < B; ++i) rz[u][i] = pU[((long)k * B + i) * ld];
+#pragma unroll
+            for (int e = 0; e < BB; ++e) rg[u][e] = gam[((long)k * BB + e) * gs];
+        }
+    }
+    for (int kb = k2 - 2; kb >= 0; kb -= BPF) {
+#pragma unroll
+        for (int u = 0; u < BPF; ++u) {
+            const int k = kb - u;
+            if (k >= 0) {
+                double nu[B];
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    double t = rz[u][i];
+#pragma unroll
+                    for (int m = 0; m < B; ++m) t = xsub(t, xmul(rg[u][i + B * m], un[m]));
+                    nu[i] = t;
+                    fin = fin && finite(t);
+                }
+                const int kn = k - BPF;
+                if (kn >= 0) {
+#pragma unroll
+                    for (int i = 0; i < B; ++i) rz[u][i] = pU[((long)kn * B + i) * ld];
+#pragma unroll
+                    for (int e = 0; e < BB; ++e) rg[u][e] = gam[((long)kn * BB + e) * gs];
+                }
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    un[i] = nu[i];
+                    pU[((long)k * B + i) * ld] = nu[i];
+                }
+            }
+        }
+    }
+    return fin;
+}
+
 template <int B>
 __device__ __forceinline__ unsigned blk_f64_col(const Seg &s, long col, double *gam, long gs)
 {
@@ -832,26 +899,7 @@ __device__ __forceinline__ unsigned blk_f64_col(const Seg &s, long col, double *
         top[i] = z[i];
         fin = fin && finite(z[i]);
     }
-    for (int k = k2 - 2; k >= 0; --k) {
-        double zk[B], Gk[BB], nu[B];
-#pragma unroll
-        for (int i = 0; i < B; ++i) zk[i] = pU[((long)k * B + i) * ld];
-#pragma unroll
-        for (int e = 0; e < BB; ++e) Gk[e] = gam[((long)k * BB + e) * gs];
-#pragma unroll
-        for (int i = 0; i < B; ++i) {
-            double t = zk[i];
-#pragma unroll
-            for (int m = 0; m < B; ++m) t = xsub(t, xmul(Gk[i + B * m], un[m]));
-            nu[i] = t;
-            fin = fin && finite(t);
-        }
-#pragma unroll
-        for (int i = 0; i < B; ++i) {
-            un[i] = nu[i];
-            pU[((long)k * B + i) * ld] = nu[i];
-        }
-    }
+    fin = blk_back<B>(pU, ld, gam, gs, k2, un) && fin;
     if (s.ubc_ratio) {
 #pragma unroll
         for (int i = 0; i < B; ++i) {
@@ -883,18 +931,18 @@ __global__ void __launch_bounds__(128) k_block_f64(SegTable tab, double *scratch
 // entry issued by one lane.  Same arithmetic as blk_f64_col.
 // ---------------------------------------------------------------------------
 template <int B, int D>
-__global__ void __launch_bounds__(32) k_block_f64_ring(SegTable tab, double *scratch, unsigned *status)
+__global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *scratch, unsigned *status)
 {
     constexpr int BB = B * B, NE = 3 * BB + B;
+    __shared__ __align__(8) unsigned long long bars[8 * D];
     extern __shared__ __align__(128) double smem_b[];
-    __shared__ __align__(8) unsigned long long bars[D];
-    const int lane = threadIdx.x;
-    Ring<NE, D> ring{smem_b, bars};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    Ring<NE, D> ring{smem_b + (long)warp * D * NE * 32, bars + warp * D};
     ring.init(lane);
-    const long gs = (long)gridDim.x * 32;
-    double *gam = scratch + (long)blockIdx.x * 32 + lane;
+    const long gs = (long)gridDim.x * blockDim.x;
+    double *gam = scratch + (long)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned q = 0;
-    for (int t = blockIdx.x; t < tab.ntiles; t += gridDim.x) {
+    for (int t = blockIdx.x * nwarps + warp; t < tab.ntiles; t += gridDim.x * nwarps) {
         const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
         const long col0 = (long)(t - s.tile0) * 32;
         const long ld = s.ld;
@@ -997,26 +1045,7 @@ __global__ void __launch_bounds__(32) k_block_f64_ring(SegTable tab, double *scr
             top[i] = z[i];
             fin = fin && finite(z[i]);
         }
-        for (int k = k2 - 2; k >= 0; --k) {
-            double zk[B], Gk[BB], nu[B];
-#pragma unroll
-            for (int i = 0; i < B; ++i) zk[i] = pU[((long)k * B + i) * ld];
-#pragma unroll
-            for (int e = 0; e < BB; ++e) Gk[e] = gam[((long)k * BB + e) * gs];
-#pragma unroll
-            for (int i = 0; i < B; ++i) {
-                double tv = zk[i];
-#pragma unroll
-                for (int m = 0; m < B; ++m) tv = xsub(tv, xmul(Gk[i + B * m], un[m]));
-                nu[i] = tv;
-                fin = fin && finite(tv);
-            }
-#pragma unroll
-            for (int i = 0; i < B; ++i) {
-                un[i] = nu[i];
-                pU[((long)k * B + i) * ld] = nu[i];
-            }
-        }
+        fin = blk_back<B>(pU, ld, gam, gs, k2, un) && fin;
         if (s.ubc_ratio) {
 #pragma unroll
             for (int i = 0; i < B; ++i) {
@@ -1444,15 +1473,20 @@ struct TileCfg {
     int cpb, cpt, stages;  // register kernel: columns per block / per thread; ring depth (0: no ring)
     int w2g;               // scalar register kernel: w2 in global scratch instead of shared memory
     int pf;                // scalar register kernels: levels of coefficient loads in flight per column
+    int wpb;               // ring kernels: independent warps (32-column tiles) per CTA
 };
 // [kind index: scalar, block2, block3][precision]
 // Defaults: the fastest shapes on the 2.5 deg column step (10368 x 57) on a
-// B200 (autotune.py sweep): scalar FP64 register kernel 256x1; 2x2 block
-// ring depth 16; 3x3 block register kernel 128; refinement kernels 128 / 32 / 128.
-const TileCfg kDefaultTile[3][2] = {{{256, 1, 0, 0, 4}, {128, 1, 0, 0, 4}}, {{64, 1, 16, 0, 4}, {32, 1, 0, 0, 4}},
-                                     {{128, 1, 0, 0, 4}, {128, 1, 0, 0, 4}}};
-TileCfg g_tile[3][2] = {{{256, 1, 0, 0, 4}, {128, 1, 0, 0, 4}}, {{64, 1, 16, 0, 4}, {32, 1, 0, 0, 4}},
-                        {{128, 1, 0, 0, 4}, {128, 1, 0, 0, 4}}};
+// B200 (autotune.py sweep): scalar FP64 bulk-copy ring of depth 4, one warp
+// per CTA, w2 in global scratch; 2x2 block ring of depth 4, one warp per CTA;
+// 3x3 block register kernel of 128 threads; refinement kernels 64 threads
+// (scalar, prefetch 8), 64 (2x2) and 128 (3x3).
+const TileCfg kDefaultTile[3][2] = {{{256, 1, 4, 1, 4, 1}, {64, 1, 0, 0, 8, 4}},
+                                     {{64, 1, 4, 0, 4, 1}, {64, 1, 0, 0, 4, 4}},
+                                     {{128, 1, 0, 0, 4, 4}, {128, 1, 0, 0, 4, 4}}};
+TileCfg g_tile[3][2] = {{{256, 1, 4, 1, 4, 1}, {64, 1, 0, 0, 8, 4}},
+                        {{64, 1, 4, 0, 4, 1}, {64, 1, 0, 0, 4, 4}},
+                        {{128, 1, 0, 0, 4, 4}, {128, 1, 0, 0, 4, 4}}};
 int kind_index(int kind) { return kind == TG_KIND_SCALAR ? 0 : (kind == TG_KIND_BLOCK2 ? 1 : 2); }
 int g_num_sms = -1;
 int g_smem_optin = -1;
@@ -1496,53 +1530,21 @@ cudaError_t with_scalar_refine(int pf, F f)
     }
 }
 
-template <typename K>
-void allow_smem(K k, int lim)
-{
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-}
-
-int num_sms()
-{
-    if (g_num_sms < 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        // every kernel that takes dynamic shared memory may use up to the
-        // opt-in limit (minus its static shared memory)
-        const int lim = g_smem_optin - 1024;
-        for (int pf : {4, 8, 16}) {
-            with_scalar_reg(1, pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
-            with_scalar_reg(2, pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
-            with_scalar_refine(pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
-        }
-        allow_smem(k_scalar_f64_ring<4>, lim);
-        allow_smem(k_scalar_f64_ring<8>, lim);
-        allow_smem(k_scalar_f64_ring<16>, lim);
-        allow_smem(k_block_f64_ring<2, 4>, lim);
-        allow_smem(k_block_f64_ring<2, 8>, lim);
-        allow_smem(k_block_f64_ring<2, 16>, lim);
-        allow_smem(k_block_f64_ring<3, 4>, lim);
-        allow_smem(k_block_f64_ring<3, 8>, lim);
-        allow_smem(k_block_f64_ring<3, 16>, lim);
-    }
-    return g_num_sms;
-}
-
-template <typename K>
-cudaError_t occupancy(K kernel, int threads, size_t smem, int *per_sm)
-{
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kernel, threads, smem);
-}
-
 template <typename F>
-cudaError_t with_scalar_ring(int D, F f)
+cudaError_t with_scalar_ring(int D, int w2g, F f)
 {
+    if (w2g) {
+        switch (D) {
+        case 4: return f(k_scalar_f64_ring<4, true>);
+        case 8: return f(k_scalar_f64_ring<8, true>);
+        case 16: return f(k_scalar_f64_ring<16, true>);
+        default: return cudaErrorInvalidValue;
+        }
+    }
     switch (D) {
-    case 4: return f(k_scalar_f64_ring<4>);
-    case 8: return f(k_scalar_f64_ring<8>);
-    case 16: return f(k_scalar_f64_ring<16>);
+    case 4: return f(k_scalar_f64_ring<4, false>);
+    case 8: return f(k_scalar_f64_ring<8, false>);
+    case 16: return f(k_scalar_f64_ring<16, false>);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1565,6 +1567,72 @@ cudaError_t with_block_ring(int B, int D, F f)
     }
 }
 
+template <typename K>
+void allow_smem(K k, int lim)
+{
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
+
+int num_sms()
+{
+    if (g_num_sms < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        // every kernel that takes dynamic shared memory may use up to the
+        // opt-in limit (minus its static shared memory)
+        const int lim = g_smem_optin - 1024;
+        for (int pf : {4, 8, 16}) {
+            with_scalar_reg(1, pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+            with_scalar_reg(2, pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+            with_scalar_refine(pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+        }
+        for (int d : {4, 8, 16})
+            for (int g : {0, 1}) with_scalar_ring(d, g, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+        allow_smem(k_block_f64_ring<2, 4>, lim);
+        allow_smem(k_block_f64_ring<2, 8>, lim);
+        allow_smem(k_block_f64_ring<2, 16>, lim);
+        allow_smem(k_block_f64_ring<3, 4>, lim);
+        allow_smem(k_block_f64_ring<3, 8>, lim);
+        allow_smem(k_block_f64_ring<3, 16>, lim);
+    }
+    return g_num_sms;
+}
+
+// Occupancy queries are cached per (kernel, threads, shared memory): the host
+// drop-ins shape one launch per column chunk, and the query is host time on
+// the path that feeds the copy engines.
+struct OccKey {
+    const void *k;
+    int threads;
+    size_t smem;
+    int per_sm;
+};
+OccKey g_occ[64];
+int g_nocc = 0;
+std::mutex g_occ_mu;
+
+template <typename K>
+cudaError_t occupancy(K kernel, int threads, size_t smem, int *per_sm)
+{
+    const void *kp = reinterpret_cast<const void *>(kernel);
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        for (int i = 0; i < g_nocc; ++i)
+            if (g_occ[i].k == kp && g_occ[i].threads == threads && g_occ[i].smem == smem) {
+                *per_sm = g_occ[i].per_sm;
+                return cudaSuccess;
+            }
+    }
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kernel, threads, smem);
+    if (e == cudaSuccess) {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        if (g_nocc < 64) g_occ[g_nocc++] = OccKey{kp, threads, smem, *per_sm};
+    }
+    return e;
+}
+
 // Resident threads per SM allowed for the block kernels: their Gamma scratch
 // (k2 * B*B doubles per resident thread) should stay well inside L2.
 constexpr double kBlockScratchBudget = 48.0 * 1024 * 1024;
@@ -1585,6 +1653,7 @@ void tile_for(int kind, int precision, bool ring_ok, int *cpb, int *cpt, int *st
         *cpb = 32;
         *cpt = 1;
         *stages = t.stages;
+        *w2g = kind == TG_KIND_SCALAR ? t.w2g : 0;
     } else {
         *cpb = t.cpb;
         *cpt = t.cpt;
@@ -1615,21 +1684,28 @@ void set_tile(int kind, int precision, int cpb, int cpt)
     t.cpt = cpt > 0 ? cpt : d.cpt;
     if (kind != TG_KIND_SCALAR || precision) t.cpt = 1;
 }
-void set_stages(int kind, int precision, int stages)
+void set_stages(int kind, int precision, int stages, int wpb)
 {
     TileCfg &t = g_tile[kind_index(kind)][precision ? 1 : 0];
-    t.stages = stages >= 0 ? stages : kDefaultTile[kind_index(kind)][precision ? 1 : 0].stages;
+    const TileCfg &d = kDefaultTile[kind_index(kind)][precision ? 1 : 0];
+    t.stages = stages >= 0 ? stages : d.stages;
+    t.wpb = wpb > 0 ? wpb : d.wpb;
 }
+int ring_warps(int kind, int precision) { return g_tile[kind_index(kind)][precision ? 1 : 0].wpb; }
 
-size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages)
+size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g)
 {
     const size_t lev = (size_t)(k2max > 1 ? k2max - 1 : 1);
-    if (stages > 0) return (size_t)stages * 4 * 32 * 8 + 32 * lev * 8;
+    if (stages > 0) return (size_t)threads / 32 * ((size_t)stages * 4 * 32 * 8 + (w2g ? 0 : 32 * lev * 8));
+    if (w2g) return 0;
     if (precision == TG_PREC_F64) return (size_t)threads * cpt * lev * 8;
     return (size_t)threads * 3 * (size_t)k2max * 4;
 }
 
-size_t block_smem_bytes(int B, int stages) { return stages > 0 ? (size_t)stages * (3 * B * B + B) * 32 * 8 : 0; }
+size_t block_smem_bytes(int B, int stages, int threads)
+{
+    return stages > 0 ? (size_t)threads / 32 * stages * (3 * B * B + B) * 32 * 8 : 0;
+}
 
 size_t block_scratch_bytes(int B, int precision, long slots, int k2max)
 {
@@ -1644,29 +1720,41 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     int per_sm = 0;
     cudaError_t e = cudaSuccess;
     sh->cpt = cpt;
-    sh->threads = cpb / cpt;
+    sh->threads = stages > 0 ? 32 * ring_warps(kind, precision) : cpb / cpt;
     sh->stages = stages;
     sh->w2g = w2g;
     sh->pf = prefetch_depth(kind, precision);
     if (kind == TG_KIND_SCALAR && sh->cpt == 2 && sh->pf > 8) sh->pf = 8;
+    if (stages > 0) {
+        // a ring that does not fit in shared memory falls back to the
+        // register-prefetch kernel with the same 32-column tile
+        const size_t need = kind == TG_KIND_SCALAR ? scalar_smem_bytes(precision, sh->threads, 1, k2max, stages, w2g)
+                                                   : block_smem_bytes(kind, stages, sh->threads);
+        if (need > (size_t)(g_smem_optin - 1024)) {
+            stages = 0;
+            sh->stages = 0;
+            sh->threads = 32;
+            sh->cpt = 1;
+        }
+    }
     if (kind == TG_KIND_SCALAR) {
-        sh->smem = w2g ? 0 : scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max, stages);
+        sh->smem = scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max, stages, w2g);
         if (sh->smem > (size_t)(g_smem_optin - 1024)) return cudaErrorInvalidConfiguration;
         auto occ = [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); };
-        if (w2g)
+        if (stages > 0)
+            e = with_scalar_ring(stages, w2g, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
+        else if (w2g)
             e = with_scalar_g(sh->pf, occ);
-        else if (stages > 0)
-            e = with_scalar_ring(stages, [&](auto k) { return occupancy(k, 32, sh->smem, &per_sm); });
         else if (precision == TG_PREC_F64)
             e = with_scalar_reg(sh->cpt, sh->pf, occ);
         else
             e = with_scalar_refine(sh->pf, occ);
     } else {
         const int B = kind;
-        sh->smem = block_smem_bytes(B, stages);
+        sh->smem = block_smem_bytes(B, stages, sh->threads);
         if (sh->smem > (size_t)(g_smem_optin - 1024)) return cudaErrorInvalidConfiguration;
         if (stages > 0)
-            e = with_block_ring(B, stages, [&](auto k) { return occupancy(k, 32, sh->smem, &per_sm); });
+            e = with_block_ring(B, stages, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
         else if (precision == TG_PREC_F64)
             e = B == 2 ? occupancy(k_block_f64<2>, sh->threads, 0, &per_sm)
                        : occupancy(k_block_f64<3>, sh->threads, 0, &per_sm);
@@ -1682,7 +1770,8 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     long blocks = (long)per_sm * nsm;
-    if (blocks > ntiles) blocks = ntiles;
+    const long units = stages > 0 ? (ntiles + sh->threads / 32 - 1) / (sh->threads / 32) : ntiles;
+    if (blocks > units) blocks = units;
     sh->blocks = (int)(blocks > 0 ? blocks : 1);
     return cudaSuccess;
 }
@@ -1692,14 +1781,14 @@ cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, R
 {
     if (tab.ntiles <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
-    if (precision == TG_PREC_F64 && sh.w2g) {
-        e = with_scalar_g(sh.pf, [&](auto k) {
-            k<<<sh.blocks, sh.threads, 0, st>>>(tab, scratch, status);
+    if (precision == TG_PREC_F64 && sh.stages > 0) {
+        e = with_scalar_ring(sh.stages, sh.w2g, [&](auto k) {
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(tab, scratch, status);
             return cudaSuccess;
         });
-    } else if (precision == TG_PREC_F64 && sh.stages > 0) {
-        e = with_scalar_ring(sh.stages, [&](auto k) {
-            k<<<sh.blocks, 32, sh.smem, st>>>(tab, status);
+    } else if (precision == TG_PREC_F64 && sh.w2g) {
+        e = with_scalar_g(sh.pf, [&](auto k) {
+            k<<<sh.blocks, sh.threads, 0, st>>>(tab, scratch, status);
             return cudaSuccess;
         });
     } else if (precision == TG_PREC_F64) {
@@ -1723,7 +1812,7 @@ cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape 
     if (tab.ntiles <= 0) return cudaSuccess;
     if (precision == TG_PREC_F64 && sh.stages > 0) {
         cudaError_t e = with_block_ring(B, sh.stages, [&](auto k) {
-            k<<<sh.blocks, 32, sh.smem, st>>>(tab, scratch, status);
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(tab, scratch, status);
             return cudaSuccess;
         });
         if (e != cudaSuccess) return e;
