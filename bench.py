@@ -57,7 +57,8 @@ def parse():
     p.add_argument("--profile", default=None,
                    help="run only one kind's plan for a profiler: KIND:PREC[:VARIANT], KIND scalar|block, "
                         "PREC f64|refine, VARIANT reg:CPB:CPT[:PF], regg:CPB:1[:PF], ring[g]:DEPTH[:WARPS] "
-                        "(default: library default)")
+                        "(default: library default); or 'dt' / 'minor' for the fused assembly+solve kernels")
+    p.add_argument("--skip-assembly", action="store_true")
     return p.parse_args()
 
 
@@ -214,10 +215,64 @@ def run_reference(args):
     return 0
 
 
+ASSEMBLY_REPLICAS = 4    # grid copies per assembly launch: inputs > L2
+
+
+def assembly_setup(pkg, wl, which, dev, replicas=ASSEMBLY_REPLICAS):
+    """Device inputs of one fused assembly+solve routine (dt_ng or minor_ng)
+    over `replicas` copies of the workload's first grid, level-major.
+    Returns (launch(stream), columns, algorithmic bytes per launch)."""
+    import torch
+    grid = wl.grids[0]
+    nk, ncol, dz = grid.nk, grid.ncol * replicas, grid.dz
+    if which == "dt":
+        F, C = pkg.synth.dt_inputs(nk, ncol, dz, 101)
+        one_d, n2d, n3d = ("expz", "dift"), len(pkg.synth.DT_2D), len(pkg.synth.DT_FIELDS)
+    else:
+        F, C = pkg.synth.minor_inputs(nk, ncol, dz, 103)
+        one_d, n2d, n3d = ("expz", "difk"), len(pkg.synth.MINOR_2D), len(pkg.synth.MINOR_FIELDS)
+    ld = pkg.batch.pad_ld(ncol)
+    d = {}
+    for k, v in F.items():
+        if v.ndim == 2:
+            d[k] = pkg.batch.level_scalar(v, ld, dev)
+        elif k in one_d:
+            d[k] = torch.from_numpy(np.ascontiguousarray(v)).to(dev)
+        else:
+            t = torch.zeros(ld, dtype=torch.float64, device=dev)
+            t[:ncol] = torch.from_numpy(v)
+            d[k] = t
+    out = torch.zeros((nk, ld), dtype=torch.float64, device=dev)
+    fn = pkg.dt_ng_dev if which == "dt" else pkg.minor_ng_dev
+    # 3-D fields read + the solution written, 2-D and 1-D inputs read
+    nbytes = 8 * ((n3d + 1) * nk * ncol + n2d * ncol + 2 * nk)
+
+    def launch(stream):
+        fn(d, C, out, nk, ncol, ld, stream=stream)
+    return launch, ncol, nbytes
+
+
 def run_profile(args):
     """Executes one kind's plan --warmup + --steps times (for ncu captures)."""
     import torch
     pkg = ge.load_package()
+    if args.profile in ("dt", "minor"):
+        wl = pkg.synth.workload(args.config)
+        launch, ncol, nbytes = assembly_setup(pkg, wl, args.profile, "cuda")
+        stream = torch.cuda.Stream()
+        for _ in range(args.warmup):
+            launch(stream)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            launch(stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        print(json.dumps({"profile": args.profile, "workload": wl.name, "columns": ncol, "ms_per_launch": ms,
+                          "algorithmic_bytes": nbytes, "GBps": nbytes / ms / 1e6}))
+        return 0
     cs = pkg.colsolve
     from tiegcm_ng_b200 import autotune
     parts = args.profile.split(":")
@@ -234,6 +289,7 @@ def run_profile(args):
     dw = pkg.batch.DeviceWorkload(wl, "cuda", max_sub=args.max_sub)
     segs = dw.segments((kind,))
     plan = pkg.Plan(segs, prec)
+    print(plan.describe(), file=sys.stderr)
     stream = torch.cuda.Stream()
     for _ in range(args.warmup):
         plan.execute(stream)
@@ -355,11 +411,40 @@ def main():
         if name in plans:
             results[name] = time_plan(plans[name], args.steps, args.warmup)
 
+    # ---- fused assembly + solve routines (dt_ng, minor_ng), device-resident
+    assembly = None
+    if not args.skip_assembly:
+        assembly = {}
+        for which, kern in (("dt", "k_dt_ng"), ("minor", "k_minor_ng")):
+            launch, ncol_a, nbytes = assembly_setup(pkg, wl, which, dev)
+            for _ in range(args.warmup):
+                launch(stream)
+            stream.synchronize()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                launch(stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+            pk, _ = measured_peak()
+            ach = nbytes / (ms * 1e-3) / 1e9
+            assembly[which + "_ng"] = {
+                "kernel": kern, "columns": ncol_a, "levels": wl.grids[0].nk, "ms_per_launch": ms,
+                "columns_per_s": world * ncol_a / (ms * 1e-3), "algorithmic_bytes_per_launch": nbytes,
+                "roofline": {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
+                             "traffic": traffic_from_profiles(kern, f"{wl.name}_x{ASSEMBLY_REPLICAS}")},
+                "inputs": f"{ASSEMBLY_REPLICAS} copies of the {wl.grids[0].name} grid, {nbytes / 1e6:.0f} MB > L2"}
+            del launch
+        torch.cuda.empty_cache()
+
     peak, peak_kind = measured_peak()
     bytes_scalar = dw.algorithmic_bytes((cs.TG_KIND_SCALAR,))
     wl_tag = f"{wl.name}_B{wl.block}"
 
     def roofline(name, kernel):
+        kernel = plans[name + "_scalar"].describe().split(" ")[0]
         ms = results[name + "_scalar"]
         ach = bytes_scalar / (ms * 1e-3) / 1e9
         tr = traffic_from_profiles(kernel, wl_tag)
@@ -475,12 +560,14 @@ def main():
                        "l2": f"inputs {dw.input_bytes() / 1e9:.3f} GB per step > 126 MB L2 (no flush needed)",
                        "parallelism": f"{world} GPU(s), independent column batches per GPU"},
             "roofline": roofline("fp64", "k_scalar_f64"),
+            "kernels": {k: plans[k].describe() for k in ("fp64", "refine")},
             "fp64": {"value": value, "ms_per_step": results["fp64"], "status": cs.STATUS_NAMES[rc64]},
             "refine": {"value": vref, "ms_per_step": results["refine"], "refine_over_fp64": vref / value,
                        "max_rel_err_vs_fp64": max_rel, "sweep_histogram": hist, "status": cs.STATUS_NAMES[rc_ref],
                        "dtype": "f32 sweeps + f64 residual/update (f64 I/O)",
                        "roofline": roofline("refine", "k_scalar_refine")},
             "kernel_ms": {k: v for k, v in results.items()},
+            "assembly": assembly,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk,

@@ -202,6 +202,33 @@ int tg_dt_ng(const tg_dt_fields *F, const tg_dt_consts *C, double *tn_upd, int n
 int tg_dt_ng_dev(const tg_dt_fields *F, const tg_dt_consts *C, double *tn_upd, int nk, int ncol, long ld,
                  double *system_out, int *status_dev, void *stream);
 
+/* minor_ng's vertical column step (src/minor_ng.F90:60-200), used for the
+ * minor species N4S, NO, N2D and Ar: the coefficients are assembled per
+ * column (a 3x3 diffusion matrix alfa is inverted per level) and solved for
+ * rows 1..nk.  The horizontal operators stay in the host model: hadvec =
+ * advec_ng(fcomp) and ftm1_smooth = smooth_ng(fcomp_tm1) are inputs, and
+ * dfactor is the per-column latitude factor of minor_ng.F90:146-155.  b (3x3,
+ * column-major) and fb (3) are the lbc module's lower-boundary relation,
+ * phix/alfax/rmx the species parameters.  3-D fields (nk, ncol); 2-D (ncol);
+ * expz, difk (nk).  The fractional powers use the device pow, so results
+ * agree with the reference arithmetic to ~1e-13 relative, not bit for bit. */
+typedef struct {
+    const double *tn, *o2, *o1, *he, *mbar, *barm, *xnmbar, *w, *ftm1_smooth, *hadvec, *sloss, *sprod;
+    const double *tlbc, *flbc1, *flbc2, *flbc3, *fubc, *dfactor;
+    const double *expz, *difk;
+} tg_minor_fields;
+
+typedef struct {
+    double rmx, alfax, phix[4], dzp, dtx2inv, expzmid, expzmid_inv;
+    double rmassinv_o2, rmassinv_o1, rmassinv_n2, rmassinv_he;
+    double rmass_o2, rmass_o1, rmass_he, rmass_n2, p0, grav, avo;
+    double b[9], fb[3];
+} tg_minor_consts;
+
+int tg_minor_ng(const tg_minor_fields *F, const tg_minor_consts *C, double *fcomp_out, int nk, int ncol);
+int tg_minor_ng_dev(const tg_minor_fields *F, const tg_minor_consts *C, double *fcomp_out, int nk, int ncol,
+                    long ld, double *system_out, int *status_dev, void *stream);
+
 /* ---- batched, GPU-resident plans ---------------------------------------------
  * A plan solves many independent systems ("segments": any mix of grids, nest
  * levels, sub-steps and species) in one persistent launch per system kind,
@@ -237,6 +264,10 @@ int tg_plan_capture_graph(tg_plan *plan, void *stream);
 int tg_plan_status(tg_plan *plan, int *per_segment_status);
 /* Number of kernel launches one tg_plan_execute issues. */
 int tg_plan_launches(const tg_plan *plan);
+/* The kernel each group of the plan launches, with its launch shape, as
+ * "k_scalar_f64_ring<4,1> kind=0 threads=32 blocks=...; ..." (for logs and
+ * profiler filters).  TG_EINVAL when n is too small (output truncated). */
+int tg_plan_describe(const tg_plan *plan, char *buf, int n);
 /* Refinement sweep histogram of the last execute: hist[s] = columns that
  * needed s sweeps (s = 0..nbins-1; the last bin also counts the FP64
  * re-solves).  Returns the number of bins written. */

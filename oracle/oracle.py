@@ -164,3 +164,40 @@ def dt_ng(fields, consts, with_system=False):
     sysarr = [np.zeros((nk, ncol), order="F") for _ in range(4)] if with_system else [None] * 4
     L.oracle_dt_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(s) for s in sysarr], _p(tn_upd))
     return (tn_upd, tuple(sysarr)) if with_system else tn_upd
+
+
+MINOR_FIELD_ORDER = ("tn", "o2", "o1", "he", "mbar", "barm", "xnmbar", "w", "ftm1_smooth", "hadvec", "sloss",
+                     "sprod", "tlbc", "flbc1", "flbc2", "flbc3", "fubc", "dfactor", "expz", "difk")
+MINOR_CONST_ORDER = ("dzp", "dtx2inv", "expzmid", "expzmid_inv", "rmassinv_o2", "rmassinv_o1", "rmassinv_n2",
+                     "rmassinv_he", "rmass_o2", "rmass_o1", "rmass_he", "rmass_n2", "p0", "grav", "avo")
+
+
+class MinorFields(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in MINOR_FIELD_ORDER]
+
+
+class MinorConsts(ctypes.Structure):
+    _fields_ = ([("rmx", ctypes.c_double), ("alfax", ctypes.c_double), ("phix", ctypes.c_double * 4)] +
+                [(n, ctypes.c_double) for n in MINOR_CONST_ORDER] +
+                [("b", ctypes.c_double * 9), ("fb", ctypes.c_double * 3)])
+
+
+def minor_ng(fields, consts, with_system=False):
+    """minor_ng assembly + solve (src/minor_ng.F90:60-200); returns fcomp_out
+    (before the max(.,small) clamp) and, if with_system, (p, q, r, f) rows 1..nk."""
+    L = lib()
+    if not hasattr(L, "_minor_bound"):
+        L.oracle_minor_ng.argtypes = [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), ctypes.c_int,
+                                      ctypes.c_long] + [ctypes.c_void_p] * 5
+        L.oracle_minor_ng.restype = None
+        L._minor_bound = True
+    arrs = {k: _fcopy(fields[k]) for k in MINOR_FIELD_ORDER}
+    nk, ncol = arrs["tn"].shape[0], arrs["tn"].size // arrs["tn"].shape[0]
+    F = MinorFields(*[arrs[k].ctypes.data for k in MINOR_FIELD_ORDER])
+    C = MinorConsts(consts["rmx"], consts["alfax"], (ctypes.c_double * 4)(*consts["phix"]),
+                    *[float(consts[k]) for k in MINOR_CONST_ORDER],
+                    (ctypes.c_double * 9)(*np.ravel(consts["b"], order="F")), (ctypes.c_double * 3)(*consts["fb"]))
+    out = np.zeros((nk, ncol), order="F")
+    sysarr = [np.zeros((nk, ncol), order="F") for _ in range(4)] if with_system else [None] * 4
+    L.oracle_minor_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(s) for s in sysarr], _p(out))
+    return (out, tuple(sysarr)) if with_system else out

@@ -37,9 +37,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
-EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
+EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
-           "tg_plan_status", "tg_plan_launches", "tg_plan_sweep_histogram", "tg_plan_destroy",
+           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
 
 
@@ -81,6 +81,30 @@ class DtConsts(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in DT_CONSTS]
 
 
+MINOR_FIELDS = ("tn", "o2", "o1", "he", "mbar", "barm", "xnmbar", "w", "ftm1_smooth", "hadvec", "sloss", "sprod",
+                "tlbc", "flbc1", "flbc2", "flbc3", "fubc", "dfactor", "expz", "difk")
+MINOR_SCALARS = ("rmx", "alfax")
+MINOR_CONSTS2 = ("dzp", "dtx2inv", "expzmid", "expzmid_inv", "rmassinv_o2", "rmassinv_o1", "rmassinv_n2",
+                 "rmassinv_he", "rmass_o2", "rmass_o1", "rmass_he", "rmass_n2", "p0", "grav", "avo")
+
+
+class MinorFields(ctypes.Structure):
+    """tg_minor_fields of include/tg_colsolve.h."""
+    _fields_ = [(n, ctypes.c_void_p) for n in MINOR_FIELDS]
+
+
+class MinorConsts(ctypes.Structure):
+    """tg_minor_consts of include/tg_colsolve.h."""
+    _fields_ = ([("rmx", ctypes.c_double), ("alfax", ctypes.c_double), ("phix", ctypes.c_double * 4)] +
+                [(n, ctypes.c_double) for n in MINOR_CONSTS2] +
+                [("b", ctypes.c_double * 9), ("fb", ctypes.c_double * 3)])
+
+
+def minor_consts(c):
+    return MinorConsts(c["rmx"], c["alfax"], (ctypes.c_double * 4)(*c["phix"]), *[float(c[n]) for n in MINOR_CONSTS2],
+                       (ctypes.c_double * 9)(*np.ravel(c["b"], order="F")), (ctypes.c_double * 3)(*c["fb"]))
+
+
 _lib = None
 
 
@@ -97,6 +121,8 @@ def lib():
             "tg_trsolv": [P, P, P, P, P, I, I, I, I, I, I, I],
             "tg_dt_ng": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I],
             "tg_solve_host": [ctypes.POINTER(HostSystem), I],
+            "tg_minor_ng": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, I, I],
+            "tg_minor_ng_dev": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, I, I, Lg, P, P, P],
             "tg_dt_ng_dev": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I, Lg, P, P, P],
             "tg_trsolv_ng": [P, P, P, P, P, I, I, I],
             "tg_blktri": [P, P, P, P, P, I, I, I, I, I],
@@ -110,6 +136,7 @@ def lib():
             "tg_plan_capture_graph": [P, P],
             "tg_plan_status": [P, P],
             "tg_plan_launches": [P],
+            "tg_plan_describe": [P, ctypes.c_char_p, I],
             "tg_plan_sweep_histogram": [P, ctypes.POINTER(Lg), I],
             "tg_plan_destroy": [P],
             "tg_set_refine": [I, D],
@@ -266,6 +293,26 @@ def dt_ng(fields, consts, tn_upd):
     return _check(rc, "tg_dt_ng")
 
 
+def minor_ng(fields, consts, fcomp_out):
+    """minor_ng's vertical column step (src/minor_ng.F90:60-200) on host
+    arrays (fields: MINOR_FIELDS; consts: rmx, alfax, phix(4), b(3,3), fb(3)
+    and the MINOR_CONSTS2 constants); fcomp_out (nk, ...) receives the solution."""
+    nk = fcomp_out.shape[0]
+    ncol = fcomp_out.size // nk
+    F = MinorFields(*[_host(fields[n], n) for n in MINOR_FIELDS])
+    C = minor_consts(consts)
+    rc = lib().tg_minor_ng(ctypes.byref(F), ctypes.byref(C), _out(fcomp_out, "fcomp_out"), nk, ncol)
+    return _check(rc, "tg_minor_ng")
+
+
+def minor_ng_dev(fields, consts, out, nk, ncol, ld, system_out=None, status=None, stream=None):
+    F = MinorFields(*[_dptr(fields[n]) for n in MINOR_FIELDS])
+    C = minor_consts(consts)
+    rc = lib().tg_minor_ng_dev(ctypes.byref(F), ctypes.byref(C), _dptr(out), nk, ncol, ld, _dptr(system_out),
+                               None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_minor_ng_dev", numeric_ok=False)
+
+
 def dt_ng_dev(fields, consts, tn_upd, nk, ncol, ld, system_out=None, status=None, stream=None):
     """Device form of dt_ng: fields are device pointers / CUDA tensors in the
     level-major layout (3-D (nk, ld)); system_out (4*nk*ld) receives p,q,r,rhs."""
@@ -407,6 +454,12 @@ class Plan:
     @property
     def launches(self):
         return lib().tg_plan_launches(self._h)
+
+    def describe(self):
+        """Kernel and launch shape of each group, e.g. 'k_scalar_f64_ring<4,1> kind=0 ...'."""
+        buf = ctypes.create_string_buffer(1024)
+        _check(lib().tg_plan_describe(self._h, buf, len(buf)), "tg_plan_describe", numeric_ok=False)
+        return buf.value.decode()
 
     def status(self):
         per = (ctypes.c_int * max(self.nseg, 1))()

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <new>
 #include <vector>
 
@@ -716,6 +717,88 @@ __attribute__((visibility("default"))) int tg_dt_ng(const tg_dt_fields *F, const
     return flags_to_status(c->flags_host[0]);
 }
 
+__attribute__((visibility("default"))) int tg_minor_ng_dev(const tg_minor_fields *F, const tg_minor_consts *C,
+                                                           double *out, int nk, int ncol, long ld, double *system_out,
+                                                           int *status_dev, void *stream)
+{
+    if (!F || !C || !out || nk < 3 || ncol < 0 || ld < ncol) {
+        set_err("tg_minor_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    const double *const ptrs[] = {F->tn, F->o2, F->o1, F->he, F->mbar, F->barm, F->xnmbar, F->w, F->ftm1_smooth,
+                                  F->hadvec, F->sloss, F->sprod, F->tlbc, F->flbc1, F->flbc2, F->flbc3, F->fubc,
+                                  F->dfactor, F->expz, F->difk};
+    for (const double *p : ptrs)
+        if (!p) return set_err("tg_minor_ng_dev: a field pointer is NULL"), TG_EINVAL;
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_minor_ng(*F, *C, out, nk, ncol, ld, system_out, cx->flags, st));
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_minor_ng(const tg_minor_fields *F, const tg_minor_consts *C,
+                                                       double *out, int nk, int ncol)
+{
+    if (!F || !C || !out || nk < 3 || ncol < 0) {
+        set_err("tg_minor_ng: bad arguments (nk=%d ncol=%d)", nk, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    const double *const f3[12] = {F->tn, F->o2, F->o1, F->he, F->mbar, F->barm, F->xnmbar, F->w, F->ftm1_smooth,
+                                  F->hadvec, F->sloss, F->sprod};
+    const double *const f2[6] = {F->tlbc, F->flbc1, F->flbc2, F->flbc3, F->fubc, F->dfactor};
+    for (const double *p : f3)
+        if (!p) return set_err("tg_minor_ng: a field pointer is NULL"), TG_EINVAL;
+    for (const double *p : f2)
+        if (!p) return set_err("tg_minor_ng: a field pointer is NULL"), TG_EINVAL;
+    if (!F->expz || !F->difk) return set_err("tg_minor_ng: expz/difk NULL"), TG_EINVAL;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ld = round_up(ncol, 32);
+    const size_t lvl = (size_t)nk * ld, colsz = (size_t)nk * ncol;
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (13 * lvl + 6 * (size_t)ld + 2 * (size_t)nk)))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * colsz))) return rc;
+    double *base = (double *)c->lvlbuf[0][0].p, *stage = (double *)c->colbuf[0][0].p;
+    cudaStream_t st = c->st[0];
+    tg_minor_fields D;
+    const double **dst3[12] = {&D.tn, &D.o2, &D.o1, &D.he, &D.mbar, &D.barm, &D.xnmbar, &D.w, &D.ftm1_smooth,
+                               &D.hadvec, &D.sloss, &D.sprod};
+    for (int i = 0; i < 12; ++i) {
+        double *d = base + i * lvl;
+        TG_CUDA(cudaMemcpyAsync(stage, f3[i], sizeof(double) * colsz, cudaMemcpyHostToDevice, st));
+        TG_CUDA(launch_col_to_level(stage, nk, d, ld, nk, ncol, st));
+        *dst3[i] = d;
+    }
+    double *out_l = base + 12 * lvl, *two = base + 13 * lvl, *one = two + 6 * ld;
+    const double **dst2[6] = {&D.tlbc, &D.flbc1, &D.flbc2, &D.flbc3, &D.fubc, &D.dfactor};
+    for (int i = 0; i < 6; ++i) {
+        TG_CUDA(cudaMemcpyAsync(two + i * ld, f2[i], sizeof(double) * ncol, cudaMemcpyHostToDevice, st));
+        *dst2[i] = two + i * ld;
+    }
+    TG_CUDA(cudaMemcpyAsync(one, F->expz, sizeof(double) * nk, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(one + nk, F->difk, sizeof(double) * nk, cudaMemcpyHostToDevice, st));
+    D.expz = one;
+    D.difk = one + nk;
+    TG_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_minor_ng(D, *C, out_l, nk, ncol, ld, nullptr, c->flags, st));
+    TG_CUDA(launch_level_to_col(out_l, ld, stage, nk, nk, ncol, st));
+    TG_CUDA(cudaMemcpyAsync(out, stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    TG_CUDA(cudaMemcpy(c->flags_host, c->flags, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    return flags_to_status(c->flags_host[0]);
+}
+
 __attribute__((visibility("default"))) int tg_trsolv_dev(const double *a, const double *b, const double *c,
                                                          const double *f, double *x, int nk, int k2, int ncol,
                                                          int layout, long ld, int precision, int *status_dev,
@@ -1003,6 +1086,37 @@ __attribute__((visibility("default"))) int tg_plan_status(tg_plan *p, int *per_s
 }
 
 __attribute__((visibility("default"))) int tg_plan_launches(const tg_plan *p) { return p ? p->launches : 0; }
+
+__attribute__((visibility("default"))) int tg_plan_describe(const tg_plan *p, char *buf, int n)
+{
+    if (!p || !buf || n < 1) {
+        set_err("tg_plan_describe: bad arguments");
+        return TG_EINVAL;
+    }
+    std::string out;
+    const bool f64 = p->precision == TG_PREC_F64;
+    for (const tg_plan::Group &g : p->groups) {
+        if (!g.nseg) continue;
+        const Shape &h = g.shape;
+        char name[96];
+        if (g.kind == TG_KIND_SCALAR) {
+            if (!f64) snprintf(name, sizeof name, "k_scalar_refine<%d>", h.pf);
+            else if (h.stages) snprintf(name, sizeof name, "k_scalar_f64_ring<%d,%d>", h.stages, h.w2g);
+            else if (h.w2g) snprintf(name, sizeof name, "k_scalar_f64_g<%d>", h.pf);
+            else snprintf(name, sizeof name, "k_scalar_f64<%d,%d>", h.cpt, h.pf);
+        } else {
+            if (!f64) snprintf(name, sizeof name, "k_block_refine<%d>", g.kind);
+            else if (h.stages) snprintf(name, sizeof name, "k_block_f64_ring<%d,%d>", g.kind, h.stages);
+            else snprintf(name, sizeof name, "k_block_f64<%d>", g.kind);
+        }
+        char line[256];
+        snprintf(line, sizeof line, "%s%s kind=%d threads=%d blocks=%d smem=%zu tiles=%d k2max=%d",
+                 out.empty() ? "" : "; ", name, g.kind, h.threads, h.blocks, h.smem, g.ntiles, g.k2max);
+        out += line;
+    }
+    snprintf(buf, (size_t)n, "%s", out.c_str());
+    return (int)out.size() < n ? TG_OK : TG_EINVAL;
+}
 
 __attribute__((visibility("default"))) int tg_plan_sweep_histogram(tg_plan *p, long *hist, int nbins)
 {

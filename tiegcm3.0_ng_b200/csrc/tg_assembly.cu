@@ -202,3 +202,259 @@ cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, i
 }
 
 }  // namespace tg
+
+// ===========================================================================
+// minor_ng (N4S, NO, N2D, Ar): src/minor_ng.F90:60-200, fused with the solve.
+// Row k of the system needs the level quantities ax, thdiff and dmdz/barm of
+// levels k and k+1; level j's quantities need tni of j-1..j+1, the interface
+// mixing ratios of levels j-1 and j, and the inverse of the 3x3 matrix alfa of
+// level j.  A thread carries level k's quantities from the previous row and
+// computes level k+1's.  The fractional powers (tni/t00)**(1.75-ss) and
+// (t00/tni)**0.25 use the device pow (within 2 ulp of the host library's), so
+// this kernel matches the CPU restatement to a stated tolerance, not bitwise.
+// ===========================================================================
+namespace tg {
+namespace {
+__device__ __constant__ double kMPhi[3][4] = {{0., 1.35, 2.16, 1.11}, {0.673, 0., 1.616, 0.769}, {0.270, 0.404, 0., 0.322}};
+__device__ __constant__ double kMSs[3] = {1.710, 1.749, 1.718};
+
+__device__ __forceinline__ void inv3_ieee(const double (&A)[9], double (&W)[9])
+{
+    // matdet3 / matadj3 / matinv3 (src/matutil.F90), IEEE division
+#define a_(i, j) A[((i) - 1) + 3 * ((j) - 1)]
+#define w_(i, j) W[((i) - 1) + 3 * ((j) - 1)]
+    double d = xm(xm(a_(1, 1), a_(2, 2)), a_(3, 3));
+    d = xs(d, xm(xm(a_(1, 1), a_(2, 3)), a_(3, 2)));
+    d = xs(d, xm(xm(a_(1, 2), a_(2, 1)), a_(3, 3)));
+    d = xa(d, xm(xm(a_(1, 2), a_(2, 3)), a_(3, 1)));
+    d = xa(d, xm(xm(a_(1, 3), a_(2, 1)), a_(3, 2)));
+    d = xs(d, xm(xm(a_(1, 3), a_(2, 2)), a_(3, 1)));
+    w_(1, 1) = xs(xm(a_(2, 2), a_(3, 3)), xm(a_(2, 3), a_(3, 2)));
+    w_(2, 1) = -xs(xm(a_(2, 1), a_(3, 3)), xm(a_(2, 3), a_(3, 1)));
+    w_(3, 1) = xs(xm(a_(2, 1), a_(3, 2)), xm(a_(2, 2), a_(3, 1)));
+    w_(1, 2) = -xs(xm(a_(1, 2), a_(3, 3)), xm(a_(1, 3), a_(3, 2)));
+    w_(2, 2) = xs(xm(a_(1, 1), a_(3, 3)), xm(a_(1, 3), a_(3, 1)));
+    w_(3, 2) = -xs(xm(a_(1, 1), a_(3, 2)), xm(a_(1, 2), a_(3, 1)));
+    w_(1, 3) = xs(xm(a_(1, 2), a_(2, 3)), xm(a_(1, 3), a_(2, 2)));
+    w_(2, 3) = -xs(xm(a_(1, 1), a_(2, 3)), xm(a_(1, 3), a_(2, 1)));
+    w_(3, 3) = xs(xm(a_(1, 1), a_(2, 2)), xm(a_(1, 2), a_(2, 1)));
+#undef a_
+#undef w_
+#pragma unroll
+    for (int e = 0; e < 9; ++e) W[e] = xd(W[e], d);
+}
+
+struct MinorLevel {
+    double ax, thdiff, dmdzs;   // dmdz/barm
+};
+
+// Raw interface quantities of level j (minor_ng.F90:77-96).
+struct MinorIface {
+    double pso1, pso2, pshe, do1dz, do2dz, dhedz, dmdz;
+};
+
+__device__ __forceinline__ MinorIface minor_iface(const MinorConsts &C, double o1, double o1m, double o2, double o2m,
+                                                  double he, double hem, double mb, double mbm)
+{
+    MinorIface r;
+    r.dmdz = xd(xs(mb, mbm), C.dzp);
+    r.pso1 = xm(0.5, xa(o1, o1m));
+    r.pso2 = xm(0.5, xa(o2, o2m));
+    r.pshe = xm(0.5, xa(he, hem));
+    r.do1dz = xd(xs(o1, o1m), C.dzp);
+    r.do2dz = xd(xs(o2, o2m), C.dzp);
+    r.dhedz = xd(xs(he, hem), C.dzp);
+    return r;
+}
+
+// ax, thdiff, dmdz/barm of level j (minor_ng.F90:100-153).
+__device__ __forceinline__ MinorLevel minor_level(const MinorConsts &C, const MinorIface &I, double barm, double tni,
+                                                  double dtnidz)
+{
+    const double t00 = 273.0, tau = 1.86e+3;
+    double df[3];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) df[n] = pow(xd(tni, t00), xs(1.75, kMSs[n]));
+#define PH(i, j) kMPhi[(i) - 1][(j) - 1]
+    double A[9], W[9];
+    A[0] = -xa(xa(PH(1, 4), xm(xs(PH(1, 2), PH(1, 4)), I.pso1)), xm(xs(xm(df[0], PH(1, 3)), PH(1, 4)), I.pshe));
+    A[4] = -xa(xa(PH(2, 4), xm(xs(PH(2, 1), PH(2, 4)), I.pso2)), xm(xs(xm(df[1], PH(2, 3)), PH(2, 4)), I.pshe));
+    A[8] = -xa(xa(xm(df[2], PH(3, 4)), xm(xs(xm(df[0], PH(3, 1)), xm(df[2], PH(3, 4))), I.pso2)),
+               xm(xs(xm(df[1], PH(3, 2)), xm(df[2], PH(3, 4))), I.pso1));
+    A[3] = xm(xs(PH(1, 2), PH(1, 4)), I.pso2);                          // (1,2)
+    A[6] = xm(xs(xm(df[0], PH(1, 3)), PH(1, 4)), I.pso2);               // (1,3)
+    A[1] = xm(xs(PH(2, 1), PH(2, 4)), I.pso1);                          // (2,1)
+    A[7] = xm(xs(xm(df[1], PH(2, 3)), PH(2, 4)), I.pso1);               // (2,3)
+    A[2] = xm(xs(xm(df[0], PH(3, 1)), xm(df[2], PH(3, 4))), I.pshe);     // (3,1)
+    A[5] = xm(xs(xm(df[1], PH(3, 2)), xm(df[2], PH(3, 4))), I.pshe);     // (3,2)
+#undef PH
+    inv3_ieee(A, W);
+    const double s0 = xs(C.phix[0], C.phix[3]), s1 = xs(C.phix[1], C.phix[3]), s2 = xs(C.phix[2], C.phix[3]);
+    // salfax . invalfa(:,n)
+    const double sa1 = xa(xa(xm(s0, W[0]), xm(s1, W[1])), xm(s2, W[2]));
+    const double sa2 = xa(xa(xm(s0, W[3]), xm(s1, W[4])), xm(s2, W[5]));
+    const double sa3 = xa(xa(xm(s0, W[6]), xm(s1, W[7])), xm(s2, W[8]));
+    double ex = xs(1.0, xd(xa(C.rmx, I.dmdz), barm));
+    ex = xa(ex, xm(sa1, xs(I.do2dz, xm(xs(1.0, xd(xa(C.rmass_o2, I.dmdz), barm)), I.pso2))));
+    ex = xa(ex, xm(sa2, xs(I.do1dz, xm(xs(1.0, xd(xa(C.rmass_o1, I.dmdz), barm)), I.pso1))));
+    ex = xa(ex, xm(sa3, xs(I.dhedz, xm(xs(1.0, xd(xa(C.rmass_he, I.dmdz), barm)), I.pshe))));
+    MinorLevel L;
+    L.dmdzs = xd(I.dmdz, barm);
+    const double den = xa(xa(xa(C.phix[2], xm(s0, I.pso2)), xm(s1, I.pso1)), xm(s2, I.pshe));
+    L.ax = -xd(xm(xd(barm, xm(tau, C.rmass_n2)), pow(xd(t00, tni), 0.25)), den);
+    L.thdiff = xs(ex, xd(xm(C.alfax, dtnidz), xm(C.dzp, tni)));
+    return L;
+}
+}  // namespace
+
+__global__ void __launch_bounds__(128) k_minor_ng(MinorFields F, MinorConsts C, double *out, int nk, int ncol, long ld,
+                                                  double *sys_out, unsigned *status)
+{
+    extern __shared__ double smem_mn[];
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    double *w2s = smem_mn + threadIdx.x;
+    const int T = blockDim.x;
+    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+    const double dzp = C.dzp;
+    // lower-boundary mixing ratios and mean mass (:72-75)
+    const double o2_0 = at(F.o2, 0), o1_0 = at(F.o1, 0), he_0 = at(F.he, 0), mb_0 = at(F.mbar, 0);
+    const double bo2 = xa(xa(xa(xm(C.b[0], o2_0), xm(C.b[3], o1_0)), xm(C.b[6], he_0)), C.fb[0]);
+    const double bo1 = xa(xa(xa(xm(C.b[1], o2_0), xm(C.b[4], o1_0)), xm(C.b[7], he_0)), C.fb[1]);
+    const double bhe = xa(xa(xa(xm(C.b[2], o2_0), xm(C.b[5], o1_0)), xm(C.b[8], he_0)), C.fb[2]);
+    const double xmbari =
+        xd(1.0, xa(xa(xa(xm(bo2, C.rmassinv_o2), xm(bo1, C.rmassinv_o1)),
+                      xm(xs(xs(xs(1.0, bo2), bo1), bhe), C.rmassinv_n2)),
+                   xm(bhe, C.rmassinv_he)));
+    // tni(j) for j = 0..nk-1: tni(0) = tlbc, tni(nk-1) = tn(nk-2), else .5*(tn(j)+tn(j-1))
+    const double tlbc = __ldg(F.tlbc + col);
+    double tn_a = at(F.tn, 0), tn_b = nk > 1 ? at(F.tn, 1) : 0.0;   // tn(j), tn(j+1) while computing tni(j+1)
+    auto tni_of = [&](int j, double tnj, double tnjm1) { return j == 0 ? tlbc : (j == nk - 1 ? tnjm1 : xm(0.5, xa(tnj, tnjm1))); };
+    double tni_m = 0.0, tni_0 = tlbc, tni_p = tni_of(1, tn_b, tn_a);
+    // level 0 interface values
+    MinorIface I0;
+    I0.dmdz = xd(xs(mb_0, xmbari), dzp);
+    I0.pso1 = xm(0.5, xa(bo1, o1_0));
+    I0.pso2 = xm(0.5, xa(bo2, o2_0));
+    I0.pshe = xm(0.5, xa(bhe, he_0));
+    I0.do1dz = xd(xs(o1_0, bo1), dzp);
+    I0.do2dz = xd(xs(o2_0, bo2), dzp);
+    I0.dhedz = xd(xs(he_0, bhe), dzp);
+    auto dtnidz_of = [&](int j, double tm, double t0, double tp) {
+        return j == 0 ? xs(tp, t0) : (j == nk - 1 ? xs(t0, tm) : xd(xs(tp, tm), 2.0));
+    };
+    MinorLevel L0 = minor_level(C, I0, at(F.barm, 0), tni_0, dtnidz_of(0, tni_m, tni_0, tni_p));
+    double o1_p = o1_0, o2_p = o2_0, he_p = he_0, mb_p = mb_0;   // level values of the previous level
+    const double dfac = __ldg(F.dfactor + col);
+    const double rdz = xd(1.0, dzp);
+    bool ok = true;
+    double w1 = 0.0, w3 = 0.0, rprev = 0.0, y0 = 0.0;
+    for (int k = 0; k < nk; ++k) {
+        double p, q, r, f;
+        const double expz = __ldg(F.expz + k);
+        const double sp = xd(xm(at(F.sprod, k), C.rmx), at(F.xnmbar, k));
+        f = xa(xs(xm(at(F.ftm1_smooth, k), C.dtx2inv), at(F.hadvec, k)), sp);
+        f = xm(f, expz);
+        MinorLevel L1 = L0;
+        if (k < nk - 1) {
+            // level k+1 quantities
+            const double o1k = at(F.o1, k + 1), o2k = at(F.o2, k + 1), hek = at(F.he, k + 1), mbk = at(F.mbar, k + 1);
+            const MinorIface I1 = minor_iface(C, o1k, o1_p, o2k, o2_p, hek, he_p, mbk, mb_p);
+            o1_p = o1k; o2_p = o2k; he_p = hek; mb_p = mbk;
+            // tni of k+2 for dtnidz(k+1)
+            double tni_pp = 0.0;
+            if (k + 2 <= nk - 1) {
+                const double tn_c = at(F.tn, k + 2);
+                tni_pp = tni_of(k + 2, tn_c, tn_b);
+                tn_a = tn_b;
+                tn_b = tn_c;
+            }
+            L1 = minor_level(C, I1, at(F.barm, k + 1), tni_p, dtnidz_of(k + 1, tni_0, tni_p, tni_pp));
+            tni_m = tni_0;
+            tni_0 = tni_p;
+            tni_p = tni_pp;
+            // row k (:161-184)
+            const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1);
+            const double molp = xm(L0.ax, xa(rdz, xm(0.5, L0.thdiff)));
+            const double molr = xm(L1.ax, xs(rdz, xm(0.5, L1.thdiff)));
+            const double molq = xa(xm(L0.ax, xs(rdz, xm(0.5, L0.thdiff))), xm(L1.ax, xa(rdz, xm(0.5, L1.thdiff))));
+            const double eddyp = xm(xm(C.expzmid_inv, difk0), xs(rdz, xm(0.5, L0.dmdzs)));
+            const double eddyr = xm(xm(C.expzmid, difk1), xa(rdz, xm(0.5, L1.dmdzs)));
+            const double eddyq = xa(xm(xm(C.expzmid_inv, difk0), xa(rdz, xm(0.5, L0.dmdzs))),
+                                    xm(xm(C.expzmid, difk1), xs(rdz, xm(0.5, L1.dmdzs))));
+            const double wk = at(F.w, k), wk1 = at(F.w, k + 1);
+            const double wi = xm(0.5, xa(wk, wk1));
+            p = xs(xd(molp, dzp), xd(xm(expz, xa(xm(eddyp, dfac), xm(0.5, wi))), dzp));
+            r = xs(xd(molr, dzp), xd(xm(expz, xs(xm(eddyr, dfac), xm(0.5, wi))), dzp));
+            q = xa(-xd(molq, dzp), xm(expz, xs(xa(xd(xm(eddyq, dfac), dzp), C.dtx2inv), at(F.sloss, k))));
+            if (k == 0) {   // lower boundary (:191-193)
+                const double l1 = __ldg(F.flbc1 + col), l2 = __ldg(F.flbc2 + col), l3 = __ldg(F.flbc3 + col);
+                const double den = xs(l1, xm(xm(0.5, l2), dzp));
+                q = xa(q, xd(xm(p, xa(l1, xm(xm(0.5, l2), dzp))), den));
+                f = xs(f, xd(xm(xm(p, l3), dzp), den));
+                p = 0.0;
+            }
+        } else {   // top row (:195-198)
+            p = xa(1.0, xm(xm(0.5, dzp), L0.thdiff));
+            q = xs(p, 2.0);
+            r = 0.0;
+            f = -xd(xm(xm(xm(C.grav, C.rmx), __ldg(F.fubc + col)), dzp), xm(xm(C.p0, L0.ax), C.avo));
+        }
+        if (sys_out) {
+            const long n = (long)nk * ld;
+            sys_out[k * ld + col] = p;
+            sys_out[n + k * ld + col] = q;
+            sys_out[2 * n + k * ld + col] = r;
+            sys_out[3 * n + k * ld + col] = f;
+        }
+        // Thomas forward step
+        if (k == 0) {
+            w1 = q;
+            w3 = xd(f, w1);
+        } else {
+            const double w2 = xd(rprev, w1);
+            w2s[(k - 1) * T] = w2;
+            w1 = xs(q, xm(p, w2));
+            w3 = xd(xs(f, xm(p, w3)), w1);
+        }
+        ok = ok && fin_nz(w1);
+        out[k * ld + col] = w3;
+        rprev = r;
+        L0 = L1;
+    }
+    (void)y0;
+    (void)tn_a;
+    (void)tni_m;
+    double xn = w3;
+    bool fin = fabs(xn) <= DBL_MAX;
+    for (int k = nk - 2; k >= 0; --k) {
+        xn = xs(out[k * ld + col], xm(w2s[k * T], xn));
+        fin = fin && fabs(xn) <= DBL_MAX;
+        out[k * ld + col] = xn;
+    }
+    if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+}
+
+cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *out, int nk, int ncol, long ld,
+                            double *sys_out, unsigned *status, cudaStream_t st)
+{
+    if (ncol <= 0) return cudaSuccess;
+    static int optin = 0;
+    if (!optin) {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        cudaFuncSetAttribute(k_minor_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+        optin = v;
+    }
+    // w2 of the forward sweep lives in shared memory, one column per thread:
+    // shrink the block until the column fits (nk <= ~220 at 128 threads).
+    int T = 128;
+    while (T > 32 && (size_t)T * (nk - 1) * sizeof(double) > (size_t)optin) T /= 2;
+    const size_t smem = (size_t)T * (nk - 1 > 0 ? nk - 1 : 1) * sizeof(double);
+    if (smem > (size_t)optin) return cudaErrorInvalidValue;
+    k_minor_ng<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, out, nk, ncol, ld, sys_out, status);
+    return cudaGetLastError();
+}
+
+}  // namespace tg

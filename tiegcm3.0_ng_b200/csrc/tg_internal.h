@@ -128,6 +128,11 @@ typedef tg_dt_consts DtConsts;
 cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, int nk, int ncol, long ld,
                          double *sys_out, unsigned *status, cudaStream_t st);
 
+typedef tg_minor_fields MinorFields;
+typedef tg_minor_consts MinorConsts;
+cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *out, int nk, int ncol, long ld,
+                            double *sys_out, unsigned *status, cudaStream_t st);
+
 // Records the message tg_last_error() returns on this thread.
 void record_error(const char *msg);
 

@@ -288,3 +288,50 @@ def dt_inputs(nk, ncol, dz, seed, step=60.0):
     c = dict(dz=dz, dtx2inv=1.0 / (2.0 * step), expzmid_inv=lc["expzmid_inv"], grav=870.0, p0=5.0e-4,
              avo=6.023e23, gask=8.314e7, tsurplus=5.11 * 1.602e-12, rmassinv_o1=1.0 / 16.0)
     return f, c
+
+
+MINOR_FIELDS = ("tn", "o2", "o1", "he", "mbar", "barm", "xnmbar", "w", "ftm1_smooth", "hadvec", "sloss", "sprod")
+MINOR_2D = ("tlbc", "flbc1", "flbc2", "flbc3", "fubc", "dfactor")
+
+
+def minor_inputs(nk, ncol, dz, seed, step=60.0, rmx=30.0):
+    """Seeded fields of the minor_ng column assembly with the model's
+    magnitudes (CGS units): major-species mass mixing ratios O2 0.22 -> 0.01,
+    O 0.05 -> 0.8, He 1e-5 -> 0.05, a minor species near 1e-7, and a lower
+    boundary that mixes Robin (flbc1 != 0) and Dirichlet (flbc1 = 0) columns.
+    Returns (fields dict of (nk,ncol) / (ncol) / (nk) arrays, constants dict)."""
+    rng = _rng(seed)
+    z = np.linspace(0.0, 1.0, nk)[:, None]
+    U = lambda lo, hi, shape=(nk, ncol): rng.uniform(lo, hi, size=shape)
+    f = {}
+    f["tn"] = 200.0 + 800.0 * z ** 0.7 * U(0.9, 1.1)
+    f["o2"] = (0.22 - 0.21 * z) * U(0.9, 1.1)
+    f["o1"] = (0.05 + 0.75 * z) * U(0.9, 1.1)
+    f["he"] = (1e-5 + 0.05 * z ** 2) * U(0.9, 1.1)
+    f["mbar"] = 1.0 / (f["o2"] / 32.0 + f["o1"] / 16.0 + f["he"] / 4.0 +
+                       (1.0 - f["o2"] - f["o1"] - f["he"]) / 28.0)
+    f["barm"] = f["mbar"] * U(0.99, 1.01)
+    f["xnmbar"] = 1e13 * np.exp(-10.0 * z) * U(0.5, 1.5)
+    f["w"] = U(-1e-4, 1e-4)
+    f["ftm1_smooth"] = 1e-7 * (1.0 + z) * U(0.5, 1.5)
+    f["hadvec"] = U(-1e-12, 1e-12)
+    f["sloss"] = U(1e-6, 1e-3)
+    f["sprod"] = U(0.0, 1e-10) * f["xnmbar"] / rmx
+    for k in MINOR_FIELDS:
+        f[k] = np.asfortranarray(f[k])
+    f["tlbc"] = rng.uniform(190.0, 210.0, ncol)
+    f["flbc1"] = np.where(rng.uniform(size=ncol) < 0.5, 0.0, rng.uniform(0.5, 1.0, ncol))
+    f["flbc2"] = rng.uniform(0.5, 1.5, ncol)
+    f["flbc3"] = rng.uniform(-1e-7, 0.0, ncol)
+    f["fubc"] = rng.uniform(0.0, 1e8, ncol)
+    f["dfactor"] = rng.uniform(1.0, 2.0, ncol)
+    lc = level_constants(nk, dz)
+    f["expz"], f["difk"] = lc["expz"], lc["difk"]
+    phix = np.array([rng.uniform(0.7, 1.0), rng.uniform(0.7, 1.0), rng.uniform(0.8, 1.1), rng.uniform(0.0, 0.2)])
+    b = np.eye(3) * rng.uniform(0.6, 0.9, 3) + rng.uniform(-0.05, 0.05, (3, 3))
+    c = dict(rmx=rmx, alfax=rng.uniform(-0.4, 0.0), phix=phix, dzp=dz, dtx2inv=1.0 / (2.0 * step),
+             expzmid=lc["expzmid"], expzmid_inv=lc["expzmid_inv"],
+             rmassinv_o2=1.0 / 32.0, rmassinv_o1=1.0 / 16.0, rmassinv_n2=1.0 / 28.0, rmassinv_he=1.0 / 4.0,
+             rmass_o2=32.0, rmass_o1=16.0, rmass_he=4.0, rmass_n2=28.0, p0=5.0e-4, grav=870.0, avo=6.023e23,
+             b=b, fb=rng.uniform(0.0, 0.02, 3))
+    return f, c
