@@ -201,3 +201,75 @@ def minor_ng(fields, consts, with_system=False):
     sysarr = [np.zeros((nk, ncol), order="F") for _ in range(4)] if with_system else [None] * 4
     L.oracle_minor_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(s) for s in sysarr], _p(out))
     return (out, tuple(sysarr)) if with_system else out
+
+
+COMP_FIELD_ORDER = ("tn", "o2", "o1", "he", "w", "mbar", "o2nm_smooth", "o1nm_smooth", "henm_smooth",
+                    "o2_advec", "o1_advec", "he_advec", "hdo2", "hdo1", "hdhe", "fs",
+                    "tlbc", "flx_he", "dfactor", "expz", "difk")
+COMP_CONST_ORDER = ("dz", "dtx2inv", "expzmid", "expzmid_inv", "rmassinv_o2", "rmassinv_o1", "rmassinv_he",
+                    "rmassinv_n2", "rmass_o2", "rmass_o1", "rmass_he", "p0", "grav")
+
+
+class CompFields(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in COMP_FIELD_ORDER]
+
+
+class CompConsts(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_double) for n in COMP_CONST_ORDER] +
+                [("b", ctypes.c_double * 9), ("fb", ctypes.c_double * 3), ("pshelb", ctypes.c_double),
+                 ("calc_helium", ctypes.c_int)])
+
+
+def comp_consts(c, cls=CompConsts):
+    return cls(*[float(c[k]) for k in COMP_CONST_ORDER], (ctypes.c_double * 9)(*np.ravel(c["b"], order="F")),
+               (ctypes.c_double * 3)(*c["fb"]), float(c["pshelb"]), int(c["calc_helium"]))
+
+
+def _bind_comp(L):
+    if not hasattr(L, "_comp_bound"):
+        L.oracle_comp_ng.argtypes = [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), ctypes.c_int,
+                                     ctypes.c_long] + [ctypes.c_void_p] * 8
+        L.oracle_comp_ng.restype = None
+        L.oracle_comp_post_ng.argtypes = [ctypes.c_void_p] * 8 + [ctypes.c_double] * 3 + \
+            [ctypes.c_int, ctypes.c_long] + [ctypes.c_void_p] * 6
+        L.oracle_comp_post_ng.restype = None
+        L._comp_bound = True
+    return L
+
+
+def comp_ng(fields, consts, with_system=False):
+    """comp_ng column step (src/comp_ng.F90:74-332); returns (o2, o1, he)
+    upd arrays (nk, ncol) and, if with_system, (P, Q, R, f, ubc) with P,Q,R
+    (3,3,nk,ncol), f (3,nk,ncol) rows 1..nk-1 and ubc (6,ncol)."""
+    L = _bind_comp(lib())
+    arrs = {k: (np.ascontiguousarray(fields[k]) if k == "fs" else _fcopy(fields[k])) for k in COMP_FIELD_ORDER}
+    nk, ncol = arrs["tn"].shape[0], arrs["tn"].size // arrs["tn"].shape[0]
+    assert arrs["fs"].size == 12 * nk * ncol
+    F = CompFields(*[arrs[k].ctypes.data for k in COMP_FIELD_ORDER])
+    C = comp_consts(consts)
+    upd = [np.zeros((nk, ncol), order="F") for _ in range(3)]
+    if with_system:
+        sysarr = [np.zeros((3, 3, nk, ncol), order="F") for _ in range(3)] + \
+                 [np.zeros((3, nk, ncol), order="F"), np.zeros((6, ncol), order="F")]
+    else:
+        sysarr = [None] * 5
+    L.oracle_comp_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(u) for u in upd], *[_p(s) for s in sysarr])
+    return (tuple(upd), tuple(sysarr)) if with_system else tuple(upd)
+
+
+POST_INPUTS = ("o2", "o1", "he", "o2_nm", "o1_nm", "he_nm", "xnmbar")
+
+
+def comp_post_ng(fields, consts):
+    """comp_ng post-solve steps (src/comp_ng.F90:415-457); returns
+    (o2_upd, o1_upd, he_upd, o2nm_upd, o1nm_upd, henm_upd)."""
+    L = _bind_comp(lib())
+    a = {k: _fcopy(fields[k]) for k in POST_INPUTS}
+    nk, ncol = a["o2"].shape[0], a["o2"].size // a["o2"].shape[0]
+    upd = [_fcopy(fields[k]).copy(order="F") for k in ("o2_upd", "o1_upd", "he_upd")]
+    nm = [np.zeros((nk, ncol), order="F") for _ in range(3)]
+    zp = np.ascontiguousarray(fields["zpmid"], dtype=np.float64)
+    L.oracle_comp_post_ng(*[_p(a[k]) for k in POST_INPUTS], zp.ctypes.data, float(consts["dz"]),
+                          float(consts["dtsmooth"]), float(consts["dtsmooth_div2"]), nk, ncol,
+                          *[_p(u) for u in upd], *[_p(u) for u in nm])
+    return tuple(upd) + tuple(nm)

@@ -675,3 +675,286 @@ ORACLE_API void oracle_minor_ng(const oracle_minor_fields *F, const oracle_minor
     }
     free(w);
 }
+
+/* ------------------------------------------------------------------------ */
+/* comp_ng major-species column step (src/comp_ng.F90:74-332): O2, O and He */
+/* mass mixing ratios from the 3x3 block-tridiagonal diffusion system.      */
+/* Fields (nk, ncol); fs is fs(nk, ncol, 3, 0:3) of the reference, i.e. 12  */
+/* slabs (nk, ncol) with slab index m*3+isp; 2-D (ncol); expz, difk (nk).    */
+/* o2/o1/he_advec = advec_ng(o2/o1/he), o2/o1/henm_smooth = smooth_ng(..nm) */
+/* and hdo2/hdo1/hdhe are inputs (horizontal operators), dfactor the        */
+/* latitude factor of comp_ng.F90:117-126.  Outputs upd (o2, o1, he) rows   */
+/* 1..nk before the time filter (he_upd = pshelb when calc_helium is 0);    */
+/* P,Q,R (3,3,nk,ncol), f (3,nk,ncol) and                                   */
+/* ubc (6,ncol: ratio(3), add(3)) may be NULL and receive the system the    */
+/* block solve sees, rows 1..nk-1, after the boundary folds.                */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    const double *tn, *o2, *o1, *he, *w, *mbar, *o2nm_smooth, *o1nm_smooth, *henm_smooth;
+    const double *o2_advec, *o1_advec, *he_advec, *hdo2, *hdo1, *hdhe, *fs;
+    const double *tlbc, *flx_he, *dfactor;
+    const double *expz, *difk;
+} oracle_comp_fields;
+
+typedef struct {
+    double dz, dtx2inv, expzmid, expzmid_inv;
+    double rmassinv_o2, rmassinv_o1, rmassinv_he, rmassinv_n2;
+    double rmass_o2, rmass_o1, rmass_he, p0, grav;
+    double b[9], fb[3];
+    double pshelb;     /* He mixing ratio held when calc_helium is 0 */
+    int calc_helium;   /* 0: flx_he is taken as 0 and he_upd = pshelb (comp_ng.F90:72,386-389) */
+} oracle_comp_consts;
+
+/* ep, alpha, ak = matinv3(alpha)*wks1 and wks4 of one level (comp_ng.F90:128-166, 176-211) */
+static void comp_level(const oracle_comp_consts *C, double o2i, double o1i, double hei, double embari,
+                       double tni, double dembardz, double dtndz, int he_thermal, double ep[3],
+                       double A[9], double ak[9], double *wks4)
+{
+    const double tau = 1.86e+3, thdiffalpha = -0.38, t00 = 273.;
+    double df[3], Ai[9], wks1;
+    int n, e;
+    for (n = 0; n < 3; ++n) df[n] = pow(tni / t00, 1.75 - MSS[n]);
+    ep[0] = 1. - 1. / embari * (C->rmass_o2 + dembardz);
+    ep[1] = 1. - 1. / embari * (C->rmass_o1 + dembardz);
+    ep[2] = 1. - 1. / embari * (C->rmass_he + dembardz);
+    if (he_thermal) ep[2] = ep[2] - thdiffalpha * dtndz / tni;
+    M3(A, 1, 1) = -(PH(1, 4) + (PH(1, 2) - PH(1, 4)) * o1i + (df[0] * PH(1, 3) - PH(1, 4)) * hei);
+    M3(A, 2, 2) = -(PH(2, 4) + (PH(2, 1) - PH(2, 4)) * o2i + (df[1] * PH(2, 3) - PH(2, 4)) * hei);
+    M3(A, 3, 3) = -(df[2] * PH(3, 4) + (df[0] * PH(3, 1) - df[2] * PH(3, 4)) * o2i +
+                   (df[1] * PH(3, 2) - df[2] * PH(3, 4)) * o1i);
+    M3(A, 1, 2) = (PH(1, 2) - PH(1, 4)) * o2i;
+    M3(A, 1, 3) = (df[0] * PH(1, 3) - PH(1, 4)) * o2i;
+    M3(A, 2, 1) = (PH(2, 1) - PH(2, 4)) * o1i;
+    M3(A, 2, 3) = (df[1] * PH(2, 3) - PH(2, 4)) * o1i;
+    M3(A, 3, 1) = (df[0] * PH(3, 1) - df[2] * PH(3, 4)) * hei;
+    M3(A, 3, 2) = (df[1] * PH(3, 2) - df[2] * PH(3, 4)) * hei;
+    oracle_matinv3(A, Ai);
+    wks1 = embari * C->rmassinv_n2 * pow(t00 / tni, 0.25) / tau;
+    for (e = 0; e < 9; ++e) ak[e] = Ai[e] * wks1;
+    *wks4 = dembardz / (embari * 2.);
+}
+
+ORACLE_API void oracle_comp_ng(const oracle_comp_fields *F, const oracle_comp_consts *C, int nk, long ncol,
+                               double *o2_upd, double *o1_upd, double *he_upd, double *P_out, double *Q_out,
+                               double *R_out, double *f_out, double *ubc_out)
+{
+    const double tau = 1.86e+3, t00 = 273.;
+    const double dz = C->dz;
+    double *w = (double *)malloc(sizeof(double) * (8 + 12 + 3) * (size_t)nk);
+    long col;
+    if (nk < 3) { free(w); return; }
+    for (col = 0; col < ncol; ++col) {
+        const size_t o = (size_t)nk * col, slab = (size_t)nk * ncol;
+        const double *tn = F->tn + o, *o2 = F->o2 + o, *o1 = F->o1 + o, *he = F->he + o, *mbar = F->mbar + o,
+                     *ww = F->w + o;
+        const double *nms[3] = {F->o2nm_smooth + o, F->o1nm_smooth + o, F->henm_smooth + o};
+        const double *adv[3] = {F->o2_advec + o, F->o1_advec + o, F->he_advec + o};
+        const double *hd[3] = {F->hdo2 + o, F->hdo1 + o, F->hdhe + o};
+        double *o2i = w, *o1i = w + nk, *hei = w + 2 * nk, *embari = w + 3 * nk, *tni = w + 4 * nk,
+               *dembardz = w + 5 * nk, *dtndz = w + 6 * nk, *wi = w + 7 * nk, *G = w + 8 * nk;
+        double ps0[3], embar0, ep_km[3], ep_kp[3], A[9], ak_km[9], ak_kp[9], wks3, wks4;
+        double a22 = 0., a33 = 0., a23 = 0., a32 = 0., flx00 = 1.;
+        double upd[3][2];
+        const double flx_he = C->calc_helium ? F->flx_he[col] : 0.;
+        int k, i, m, n;
+        /* lower-boundary mixing ratios and interface quantities (:74-102) */
+        for (i = 0; i < 3; ++i)
+            ps0[i] = C->b[i] * o2[0] + C->b[i + 3] * o1[0] + C->b[i + 6] * he[0] + C->fb[i];
+        embar0 = 1. / (ps0[0] * C->rmassinv_o2 + ps0[1] * C->rmassinv_o1 + ps0[2] * C->rmassinv_he +
+                       (1. - ps0[0] - ps0[1] - ps0[2]) * C->rmassinv_n2);
+        o2i[0] = .5 * (ps0[0] + o2[0]);
+        o1i[0] = .5 * (ps0[1] + o1[0]);
+        hei[0] = .5 * (ps0[2] + he[0]);
+        embari[0] = .5 * (embar0 + mbar[0]);
+        tni[0] = F->tlbc[col];
+        dembardz[0] = mbar[0] - embar0;
+        dtndz[0] = (tn[0] - F->tlbc[col]) * 2;
+        for (k = 1; k < nk; ++k) {
+            o2i[k] = .5 * (o2[k - 1] + o2[k]);
+            o1i[k] = .5 * (o1[k - 1] + o1[k]);
+            hei[k] = .5 * (he[k - 1] + he[k]);
+            embari[k] = .5 * (mbar[k - 1] + mbar[k]);
+            tni[k] = .5 * (tn[k - 1] + tn[k]);
+            dembardz[k] = mbar[k] - mbar[k - 1];
+            dtndz[k] = tn[k] - tn[k - 1];
+        }
+        for (k = 0; k < nk; ++k) {
+            dembardz[k] = dembardz[k] / dz;
+            dtndz[k] = dtndz[k] / dz;
+        }
+        for (k = 0; k < nk - 1; ++k) wi[k] = .5 * (ww[k] + ww[k + 1]);
+        wi[nk - 1] = 1.5 * ww[nk - 1] - .5 * ww[nk - 2];
+        /* level 1 (:128-166) */
+        comp_level(C, o2i[0], o1i[0], hei[0], embari[0], tni[0], dembardz[0], dtndz[0], 1, ep_kp, A, ak_kp, &wks4);
+        for (i = 0; i < 12; ++i) G[i] = 0.;
+        const double dfac = F->dfactor[col];
+        /* rows 1..nk-1: assembly (:176-278) and block forward sweep (:280-314) */
+        for (k = 0; k < nk - 1; ++k) {
+            double Pk[9], Qk[9], Rk[9], fk[3], W[9], v[3];
+            for (i = 0; i < 3; ++i) ep_km[i] = ep_kp[i];
+            for (i = 0; i < 9; ++i) ak_km[i] = ak_kp[i];
+            wks3 = wks4;
+            comp_level(C, o2i[k + 1], o1i[k + 1], hei[k + 1], embari[k + 1], tni[k + 1], dembardz[k + 1],
+                       dtndz[k + 1], k + 1 != nk - 1, ep_kp, A, ak_kp, &wks4);
+            const double eddyp = C->expzmid_inv * F->difk[k] * (1. / dz - wks3);
+            const double eddyr = C->expzmid * F->difk[k + 1] * (1. / dz + wks4);
+            const double eddyq = C->expzmid_inv * F->difk[k] * (1. / dz + wks3) +
+                                 C->expzmid * F->difk[k + 1] * (1. / dz - wks4);
+            const double ez = F->expz[k];
+            for (m = 0; m < 3; ++m)
+                for (i = 0; i < 3; ++i) {
+                    const double delta = i == m ? 1. : 0.;
+                    const double molp = ak_km[i + 3 * m] * (1. / dz + ep_km[m] / 2.);
+                    const double molr = ak_kp[i + 3 * m] * (1. / dz - ep_kp[m] / 2.);
+                    const double molq = ak_km[i + 3 * m] * (1. / dz - ep_km[m] / 2.) +
+                                        ak_kp[i + 3 * m] * (1. / dz + ep_kp[m] / 2.);
+                    Pk[i + 3 * m] = molp / dz - ez * delta / dz * (eddyp * dfac + .5 * wi[k]);
+                    Rk[i + 3 * m] = molr / dz - ez * delta / dz * (eddyr * dfac - .5 * wi[k]);
+                    Qk[i + 3 * m] = -molq / dz + ez * delta * (eddyq * dfac / dz + C->dtx2inv) -
+                                    ez * F->fs[(size_t)(m + 1) * 3 * slab + (size_t)i * slab + o + k];
+                }
+            for (i = 0; i < 3; ++i)
+                fk[i] = ez * (nms[i][k] * C->dtx2inv - (adv[i][k] - F->fs[(size_t)i * slab + o + k]) + hd[i][k]);
+            if (k == 0) {
+                for (m = 0; m < 3; ++m)
+                    for (n = 0; n < 3; ++n)
+                        for (i = 0; i < 3; ++i) Qk[i + 3 * m] = Qk[i + 3 * m] + Pk[i + 3 * n] * C->b[n + 3 * m];
+                for (m = 0; m < 3; ++m)
+                    for (i = 0; i < 3; ++i) fk[i] = fk[i] - Pk[i + 3 * m] * C->fb[m];
+                for (i = 0; i < 9; ++i) Pk[i] = 0.;
+            } else if (k == nk - 2) {
+                for (m = 0; m < 3; ++m)
+                    for (i = 0; i < 3; ++i)
+                        Qk[i + 3 * m] = Qk[i + 3 * m] +
+                                        (1. + .5 * ep_kp[m] * dz) / (1. - .5 * ep_kp[m] * dz) * Rk[i + 3 * m];
+                a22 = M3(A, 2, 2);
+                a33 = M3(A, 3, 3);
+                a23 = M3(A, 2, 3);
+                a32 = M3(A, 3, 2);
+                flx00 = embari[k] * C->rmassinv_n2 * C->p0 * pow(t00 / tn[k], 0.25) / (tau * C->grav);
+                for (i = 0; i < 3; ++i)
+                    fk[i] = fk[i] - Rk[i + 3] * (a23 - a22) * flx_he / (flx00 * (1. / dz - 0.5 * ep_kp[1])) -
+                            Rk[i + 6] * (a33 - a32) * flx_he / (flx00 * (1. / dz - 0.5 * ep_kp[2]));
+                for (i = 0; i < 9; ++i) Rk[i] = 0.;
+            }
+            if (P_out) {
+                const size_t om = (size_t)9 * nk * col + 9 * (size_t)k, ov = (size_t)3 * nk * col + 3 * (size_t)k;
+                for (i = 0; i < 9; ++i) {
+                    P_out[om + i] = Pk[i];
+                    Q_out[om + i] = Qk[i];
+                    R_out[om + i] = Rk[i];
+                }
+                for (i = 0; i < 3; ++i) f_out[ov + i] = fk[i];
+            }
+            {
+                const double *Gk = G + 12 * k;
+                double *Gn = G + 12 * (k + 1);
+                for (m = 0; m < 3; ++m)
+                    for (n = 0; n < 3; ++n)
+                        for (i = 0; i < 3; ++i) Qk[i + 3 * m] = Qk[i + 3 * m] - Pk[i + 3 * n] * Gk[n + 3 * m];
+                oracle_matinv3(Qk, W);
+                for (i = 0; i < 3; ++i) v[i] = fk[i];
+                for (m = 0; m < 3; ++m) {
+                    for (i = 0; i < 3; ++i) v[i] = v[i] - Pk[i + 3 * m] * Gk[9 + m];
+                }
+                for (i = 0; i < 12; ++i) Gn[i] = 0.;
+                for (m = 0; m < 3; ++m)
+                    for (n = 0; n < 3; ++n)
+                        for (i = 0; i < 3; ++i) Gn[i + 3 * m] = Gn[i + 3 * m] + W[i + 3 * n] * Rk[n + 3 * m];
+                for (m = 0; m < 3; ++m)
+                    for (i = 0; i < 3; ++i) Gn[9 + i] = Gn[9 + i] + W[i + 3 * m] * v[m];
+            }
+        }
+        /* back sweep (:317-324) */
+        {
+            double *x[3] = {o2_upd + o, o1_upd + o, he_upd + o};
+            for (i = 0; i < 3; ++i) x[i][nk - 1] = 0.;
+            for (k = nk - 2; k >= 0; --k) {
+                const double *Gn = G + 12 * (k + 1);
+                for (i = 0; i < 3; ++i) upd[i][0] = Gn[9 + i];
+                for (i = 0; i < 3; ++i)
+                    for (m = 0; m < 3; ++m) upd[i][0] = upd[i][0] - Gn[i + 3 * m] * x[m][k + 1];
+                for (i = 0; i < 3; ++i) x[i][k] = upd[i][0];
+            }
+            /* upper boundary (:326-332) */
+            double ratio[3], add[3] = {0., 0., 0.};
+            for (i = 0; i < 3; ++i) {
+                ratio[i] = (1. + .5 * ep_kp[i] * dz) / (1. - .5 * ep_kp[i] * dz);
+                x[i][nk - 1] = ratio[i] * x[i][nk - 2];
+            }
+            add[1] = (a23 - a22) * flx_he / (flx00 * (1. / dz - 0.5 * ep_kp[1]));
+            add[2] = (a33 - a32) * flx_he / (flx00 * (1. / dz - 0.5 * ep_kp[2]));
+            x[1][nk - 1] = x[1][nk - 1] + add[1];
+            x[2][nk - 1] = x[2][nk - 1] + add[2];
+            if (ubc_out)
+                for (i = 0; i < 3; ++i) {
+                    ubc_out[6 * col + i] = ratio[i];
+                    ubc_out[6 * col + 3 + i] = add[i];
+                }
+            if (!C->calc_helium)
+                for (k = 0; k < nk; ++k) x[2][k] = C->pshelb;
+        }
+    }
+    free(w);
+}
+
+/* comp_ng post-solve steps per column (src/comp_ng.F90:415-457): the time  */
+/* filter, N2 = 1 - O2 - O - He with the exponential extrapolation above the */
+/* level where N2 < 0.01, the floor at 1e-9 and the normalisation.  o2/o1/he */
+/* are the fields at the current step (itp), o2/o1/he_nm the previous one;    */
+/* upd arrays (in: solution, lateral-boundary columns already overwritten)   */
+/* receive the final mixing ratios, *nm_upd the filtered ones.  A column    */
+/* whose N2 drops below 0.01 at level 1 is left without extrapolation (the  */
+/* reference would read level 0 there).                                      */
+ORACLE_API void oracle_comp_post_ng(const double *o2, const double *o1, const double *he, const double *o2_nm,
+                                    const double *o1_nm, const double *he_nm, const double *xnmbar,
+                                    const double *zpmid, double dz, double dtsmooth, double dtsmooth_div2,
+                                    int nk, long ncol, double *o2_upd,
+                                    double *o1_upd, double *he_upd, double *o2nm_upd, double *o1nm_upd,
+                                    double *henm_upd)
+{
+    const double small = 1.e-9;
+    double *n2 = (double *)malloc(sizeof(double) * 2 * (size_t)nk), *n2nm = n2 + nk;
+    long col;
+    for (col = 0; col < ncol; ++col) {
+        const size_t o = (size_t)nk * col;
+        int k, ktop;
+        for (k = 0; k < nk; ++k) {
+            o2nm_upd[o + k] = dtsmooth_div2 * (o2_nm[o + k] + o2_upd[o + k]) + dtsmooth * o2[o + k];
+            o1nm_upd[o + k] = dtsmooth_div2 * (o1_nm[o + k] + o1_upd[o + k]) + dtsmooth * o1[o + k];
+            henm_upd[o + k] = dtsmooth_div2 * (he_nm[o + k] + he_upd[o + k]) + dtsmooth * he[o + k];
+        }
+        for (k = 0; k < nk; ++k) {
+            n2[k] = 1. - o2_upd[o + k] - o1_upd[o + k] - he_upd[o + k];
+            n2nm[k] = 1. - o2nm_upd[o + k] - o1nm_upd[o + k] - henm_upd[o + k];
+        }
+        for (ktop = 0; ktop < nk; ++ktop)
+            if (n2[ktop] < 0.01) break;
+        if (ktop < nk - 1 && ktop > 0) {
+            const double zmtop = zpmid[ktop];
+            const double n2top = log(n2[ktop] * xnmbar[o + ktop]);
+            const double n2top1 = log(n2[ktop - 1] * xnmbar[o + ktop - 1]);
+            const double dn2dz = (n2top - n2top1) / dz;
+            for (k = ktop + 1; k < nk; ++k) n2[k] = exp(n2top + dn2dz * (zpmid[k] - zmtop)) / xnmbar[o + k];
+        }
+        for (k = 0; k < nk; ++k) {
+            double a = o2_upd[o + k] > small ? o2_upd[o + k] : small;
+            double b = o1_upd[o + k] > small ? o1_upd[o + k] : small;
+            double c = he_upd[o + k] > small ? he_upd[o + k] : small;
+            double d = n2[k] > small ? n2[k] : small;
+            double s = a + b + c + d;
+            o2_upd[o + k] = a / s;
+            o1_upd[o + k] = b / s;
+            he_upd[o + k] = c / s;
+            a = o2nm_upd[o + k] > small ? o2nm_upd[o + k] : small;
+            b = o1nm_upd[o + k] > small ? o1nm_upd[o + k] : small;
+            c = henm_upd[o + k] > small ? henm_upd[o + k] : small;
+            d = n2nm[k] > small ? n2nm[k] : small;
+            s = a + b + c + d;
+            o2nm_upd[o + k] = a / s;
+            o1nm_upd[o + k] = b / s;
+            henm_upd[o + k] = c / s;
+        }
+    }
+    free(n2);
+}

@@ -335,3 +335,72 @@ def minor_inputs(nk, ncol, dz, seed, step=60.0, rmx=30.0):
              rmass_o2=32.0, rmass_o1=16.0, rmass_he=4.0, rmass_n2=28.0, p0=5.0e-4, grav=870.0, avo=6.023e23,
              b=b, fb=rng.uniform(0.0, 0.02, 3))
     return f, c
+
+
+COMP_FIELDS = ("tn", "o2", "o1", "he", "w", "mbar", "o2nm_smooth", "o1nm_smooth", "henm_smooth",
+               "o2_advec", "o1_advec", "he_advec", "hdo2", "hdo1", "hdhe")
+COMP_2D = ("tlbc", "flx_he", "dfactor")
+
+
+def comp_inputs(nk, ncol, dz, seed, step=60.0, calc_helium=1):
+    """Seeded fields of the comp_ng column step with the model's magnitudes:
+    O2/O/He mass mixing ratios as in minor_inputs, production and a loss
+    matrix fs(nk, ncol, 3, 0:3) (slab m*3+isp of a (12, ncol, nk) array,
+    i.e. the reference's Fortran order), and an upper-boundary He flux.
+    Returns (fields dict, constants dict)."""
+    rng = _rng(seed)
+    z = np.linspace(0.0, 1.0, nk)[:, None]
+    U = lambda lo, hi, shape=(nk, ncol): rng.uniform(lo, hi, size=shape)
+    f = {}
+    f["tn"] = 200.0 + 800.0 * z ** 0.7 * U(0.9, 1.1)
+    f["o2"] = (0.22 - 0.21 * z) * U(0.9, 1.1)
+    f["o1"] = (0.05 + 0.75 * z) * U(0.9, 1.1)
+    f["he"] = (1e-5 + 0.05 * z ** 2) * U(0.9, 1.1)
+    f["mbar"] = 1.0 / (f["o2"] / 32.0 + f["o1"] / 16.0 + f["he"] / 4.0 +
+                       (1.0 - f["o2"] - f["o1"] - f["he"]) / 28.0)
+    f["w"] = U(-1e-4, 1e-4)
+    for s in ("o2", "o1", "he"):
+        f[s + "nm_smooth"] = f[s] * U(0.99, 1.01)
+        f[s + "_advec"] = f[s] * U(-1e-6, 1e-6)
+    f["hdo2"], f["hdo1"], f["hdhe"] = (U(-1e-9, 1e-9) for _ in range(3))
+    for k in COMP_FIELDS:
+        f[k] = np.asfortranarray(f[k])
+    fs = np.empty((12, ncol, nk))
+    fs[0:3] = rng.uniform(0.0, 1e-8, size=(3, ncol, nk))                 # production fs(:,:,isp,0)
+    fs[3:12] = rng.uniform(-1e-6, 1e-6, size=(9, ncol, nk))              # loss fs(:,:,isp,m)
+    for isp in range(3):
+        fs[3 + isp * 3 + isp] = rng.uniform(1e-6, 1e-4, size=(ncol, nk))  # diagonal loss
+    f["fs"] = fs
+    f["tlbc"] = rng.uniform(190.0, 210.0, ncol)
+    f["flx_he"] = rng.uniform(-1e-13, 1e-13, ncol)
+    f["dfactor"] = rng.uniform(1.0, 2.0, ncol)
+    lc = level_constants(nk, dz)
+    f["expz"], f["difk"] = lc["expz"], lc["difk"]
+    b = np.eye(3) * rng.uniform(0.6, 0.9, 3) + rng.uniform(-0.05, 0.05, (3, 3))
+    c = dict(dz=dz, dtx2inv=1.0 / (2.0 * step), expzmid=lc["expzmid"], expzmid_inv=lc["expzmid_inv"],
+             rmassinv_o2=1.0 / 32.0, rmassinv_o1=1.0 / 16.0, rmassinv_he=1.0 / 4.0, rmassinv_n2=1.0 / 28.0,
+             rmass_o2=32.0, rmass_o1=16.0, rmass_he=4.0, p0=5.0e-4, grav=870.0, b=b, fb=rng.uniform(0.0, 0.02, 3),
+             pshelb=0.1154e-5, calc_helium=calc_helium)
+    return f, c
+
+
+def comp_post_inputs(nk, ncol, dz, seed, zibot=-7.0):
+    """Fields of the comp_ng post-solve steps: the current and previous
+    O2/O/He, N2 number-density factors, level midpoints and a solution whose
+    N2 drops below 0.01 in the upper levels of about half the columns."""
+    rng = _rng(seed)
+    z = np.linspace(0.0, 1.0, nk)[:, None]
+    U = lambda lo, hi, shape=(nk, ncol): rng.uniform(lo, hi, size=shape)
+    f = {}
+    for pre in ("", "_nm", "_upd"):
+        # N2 decays from 0.78 to 0.002-0.04 at the top; O2, He and O share the rest
+        n2 = 0.78 * np.exp(-rng.uniform(3.0, 6.0, size=(1, ncol)) * z) * U(0.98, 1.02)
+        rest = 1.0 - n2
+        f["o2" + pre] = rest * (0.28 - 0.27 * z) * U(0.9, 1.1)
+        f["he" + pre] = rest * (1e-5 + 0.1 * z ** 2) * U(0.5, 1.5)
+        f["o1" + pre] = rest - f["o2" + pre] - f["he" + pre]
+    f["xnmbar"] = 1e13 * np.exp(-10.0 * z) * U(0.5, 1.5)
+    for k in list(f):
+        f[k] = np.asfortranarray(f[k])
+    f["zpmid"] = zibot + (np.arange(nk) + 0.5) * dz
+    return f, dict(dz=dz, dtsmooth=0.95, dtsmooth_div2=0.5 * (1.0 - 0.95))
