@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--profile", default=None,
                    help="run only one kind's plan for a profiler: KIND:PREC[:VARIANT], KIND scalar|block, "
                         "PREC f64|refine, VARIANT reg:CPB:CPT[:PF], regg:CPB:1[:PF], ring[g]:DEPTH[:WARPS] "
-                        "(default: library default); or 'dt' / 'minor' for the fused assembly+solve kernels")
+                        "(default: library default); or 'dt' / 'minor' / 'comp' for the fused assembly+solve kernels")
     p.add_argument("--skip-assembly", action="store_true")
     return p.parse_args()
 
@@ -225,16 +225,27 @@ def assembly_setup(pkg, wl, which, dev, replicas=ASSEMBLY_REPLICAS):
     import torch
     grid = wl.grids[0]
     nk, ncol, dz = grid.nk, grid.ncol * replicas, grid.dz
+    nout = 1
     if which == "dt":
         F, C = pkg.synth.dt_inputs(nk, ncol, dz, 101)
         one_d, n2d, n3d = ("expz", "dift"), len(pkg.synth.DT_2D), len(pkg.synth.DT_FIELDS)
-    else:
+    elif which == "minor":
         F, C = pkg.synth.minor_inputs(nk, ncol, dz, 103)
         one_d, n2d, n3d = ("expz", "difk"), len(pkg.synth.MINOR_2D), len(pkg.synth.MINOR_FIELDS)
+    else:
+        F, C = pkg.synth.comp_inputs(nk, ncol, dz, 107)
+        one_d, n2d, n3d = ("expz", "difk"), len(pkg.synth.COMP_2D), len(pkg.synth.COMP_FIELDS) + 12
+        nout = 3
     ld = pkg.batch.pad_ld(ncol)
     d = {}
     for k, v in F.items():
-        if v.ndim == 2:
+        if k == "fs":
+            fs = np.asarray(v).reshape(12, ncol, nk)
+            t = torch.zeros((12, nk, ld), dtype=torch.float64, device=dev)
+            for s_ in range(12):
+                t[s_, :, :ncol] = torch.from_numpy(np.ascontiguousarray(fs[s_].T)).to(dev)
+            d[k] = t
+        elif v.ndim == 2:
             d[k] = pkg.batch.level_scalar(v, ld, dev)
         elif k in one_d:
             d[k] = torch.from_numpy(np.ascontiguousarray(v)).to(dev)
@@ -242,10 +253,10 @@ def assembly_setup(pkg, wl, which, dev, replicas=ASSEMBLY_REPLICAS):
             t = torch.zeros(ld, dtype=torch.float64, device=dev)
             t[:ncol] = torch.from_numpy(v)
             d[k] = t
-    out = torch.zeros((nk, ld), dtype=torch.float64, device=dev)
-    fn = pkg.dt_ng_dev if which == "dt" else pkg.minor_ng_dev
+    out = torch.zeros((nout, nk, ld), dtype=torch.float64, device=dev)
+    fn = {"dt": pkg.dt_ng_dev, "minor": pkg.minor_ng_dev, "comp": pkg.comp_ng_dev}[which]
     # 3-D fields read + the solution written, 2-D and 1-D inputs read
-    nbytes = 8 * ((n3d + 1) * nk * ncol + n2d * ncol + 2 * nk)
+    nbytes = 8 * ((n3d + nout) * nk * ncol + n2d * ncol + 2 * nk)
 
     def launch(stream):
         fn(d, C, out, nk, ncol, ld, stream=stream)
@@ -256,7 +267,7 @@ def run_profile(args):
     """Executes one kind's plan --warmup + --steps times (for ncu captures)."""
     import torch
     pkg = ge.load_package()
-    if args.profile in ("dt", "minor"):
+    if args.profile in ("dt", "minor", "comp"):
         wl = pkg.synth.workload(args.config)
         launch, ncol, nbytes = assembly_setup(pkg, wl, args.profile, "cuda")
         stream = torch.cuda.Stream()
@@ -415,7 +426,7 @@ def main():
     assembly = None
     if not args.skip_assembly:
         assembly = {}
-        for which, kern in (("dt", "k_dt_ng"), ("minor", "k_minor_ng")):
+        for which, kern in (("dt", "k_dt_ng"), ("minor", "k_minor_ng"), ("comp", "k_comp_ng")):
             launch, ncol_a, nbytes = assembly_setup(pkg, wl, which, dev)
             for _ in range(args.warmup):
                 launch(stream)

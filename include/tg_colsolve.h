@@ -229,6 +229,54 @@ int tg_minor_ng(const tg_minor_fields *F, const tg_minor_consts *C, double *fcom
 int tg_minor_ng_dev(const tg_minor_fields *F, const tg_minor_consts *C, double *fcomp_out, int nk, int ncol,
                     long ld, double *system_out, int *status_dev, void *stream);
 
+/* comp_ng's major-species column step (src/comp_ng.F90:74-332): O2, O and He
+ * from the 3x3 block-tridiagonal diffusion system, assembled per column and
+ * solved for rows 1..nk-1, with the top level from the upper boundary (He
+ * escape flux flx_he).  Horizontal operators stay in the host model: the
+ * *_advec fields are advec_ng of the species, *nm_smooth smooth_ng of the
+ * previous step, hdo2/hdo1/hdhe the horizontal diffusion.  fs is the
+ * reference's fs(nk, ncol, 3, 0:3): 12 slabs (nk, ncol), slab m*3+isp, m = 0
+ * production, 1..3 the loss matrix.  b, fb: the lbc module's lower-boundary
+ * relation.  calc_helium = 0 takes flx_he as 0 and returns He = pshelb
+ * (comp_ng.F90:72,386-389).  Outputs o2/o1/he_upd before the time filter;
+ * tg_comp_post_ng applies the post-solve steps (:415-457) after the caller
+ * has written its lateral-boundary columns. */
+typedef struct {
+    const double *tn, *o2, *o1, *he, *w, *mbar, *o2nm_smooth, *o1nm_smooth, *henm_smooth;
+    const double *o2_advec, *o1_advec, *he_advec, *hdo2, *hdo1, *hdhe, *fs;
+    const double *tlbc, *flx_he, *dfactor;
+    const double *expz, *difk;
+} tg_comp_fields;
+
+typedef struct {
+    double dz, dtx2inv, expzmid, expzmid_inv;
+    double rmassinv_o2, rmassinv_o1, rmassinv_he, rmassinv_n2;
+    double rmass_o2, rmass_o1, rmass_he, p0, grav;
+    double b[9], fb[3];
+    double pshelb;
+    int calc_helium;
+} tg_comp_consts;
+
+int tg_comp_ng(const tg_comp_fields *F, const tg_comp_consts *C, double *o2_upd, double *o1_upd, double *he_upd,
+               int nk, int ncol);
+/* Device form: level-major (k*ld + col) fields, fs 12 slabs of nk*ld; out
+ * receives 3 slabs (O2, O, He) of nk*ld; system_out (may be NULL) 30 slabs
+ * of nk*ld: P(i,m) at slab i+3m, Q at 9+i+3m, R at 18+i+3m, f at 27+i. */
+int tg_comp_ng_dev(const tg_comp_fields *F, const tg_comp_consts *C, double *out, int nk, int ncol, long ld,
+                   double *system_out, int *status_dev, void *stream);
+
+/* comp_ng's post-solve steps per column (src/comp_ng.F90:415-457): time
+ * filter, N2 = 1-O2-O-He with the exponential extrapolation above the first
+ * level where N2 < 0.01, the floor at 1e-9 and the normalisation.  o2/o1/he
+ * are the current-step fields, *_nm the previous step; o2/o1/he_upd are
+ * updated in place, *nm_upd receive the filtered fields.  Host arrays (nk,
+ * ncol); zpmid (nk) the level midpoints.  A column whose N2 is below 0.01 at
+ * level 1 is left without extrapolation (the reference reads level 0 there). */
+int tg_comp_post_ng(const double *o2, const double *o1, const double *he, const double *o2_nm, const double *o1_nm,
+                    const double *he_nm, const double *xnmbar, const double *zpmid, double dz, double dtsmooth,
+                    double dtsmooth_div2, int nk, int ncol, double *o2_upd, double *o1_upd, double *he_upd,
+                    double *o2nm_upd, double *o1nm_upd, double *henm_upd);
+
 /* ---- batched, GPU-resident plans ---------------------------------------------
  * A plan solves many independent systems ("segments": any mix of grids, nest
  * levels, sub-steps and species) in one persistent launch per system kind,
@@ -305,6 +353,10 @@ int tg_set_prefetch(int kind, int precision, int levels);
  * (residency then limited only by registers); -1 restores the default.
  * Only kind TG_KIND_SCALAR with TG_PREC_F64. */
 int tg_set_scratch_global(int kind, int precision, int on);
+/* L2 eviction-priority hints of the bulk-copy (ring) kernels: coefficient
+ * streams evict-first, the sweep's scratch and parked w3 evict-last.
+ * on: 1 (default), 0 off, -1 back to the default. */
+int tg_set_cache_hints(int on);
 /* Test entry: q[i] = a[i]/b[i] (device arrays, n elements) computed by the
  * kernels' division routine (Markstein's correction of the correctly rounded
  * reciprocal, IEEE division outside its safe range); must equal IEEE a/b. */

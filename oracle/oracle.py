@@ -273,3 +273,46 @@ def comp_post_ng(fields, consts):
                           float(consts["dtsmooth"]), float(consts["dtsmooth_div2"]), nk, ncol,
                           *[_p(u) for u in upd], *[_p(u) for u in nm])
     return tuple(upd) + tuple(nm)
+
+
+SETTEI_FIELD_ORDER = ("tn", "o2", "o1", "he", "n2", "ne", "te", "ti", "op", "o2p", "nplus", "n2p", "nop", "xnmbar",
+                      "xnmbari", "scht", "schti", "qji_ti", "qop2p", "qop2d", "qo2p", "qop", "qn2p", "qnp", "qnop",
+                      "Q1", "Q2", "t_lbc", "chi", "rlatm", "dipmag", "qteaur")
+SETTEI_CONST_ORDER = ("f107", "dipmin", "dz", "evergs", "avo", "rmass_o1", "rmassinv_o2", "rmassinv_o1",
+                      "rmassinv_he", "rmassinv_n2", "rmassinv_n4s", "rmassinv_no")
+
+
+class SetteiFields(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in SETTEI_FIELD_ORDER]
+
+
+class SetteiConsts(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_double) for n in SETTEI_CONST_ORDER] +
+                [("b", ctypes.c_double * 9), ("fb", ctypes.c_double * 3), ("et", ctypes.c_int),
+                 ("electron_heating", ctypes.c_int)])
+
+
+def settei_consts(c, cls=SetteiConsts):
+    return cls(*[float(c[k]) for k in SETTEI_CONST_ORDER], (ctypes.c_double * 9)(*np.ravel(c["b"], order="F")),
+               (ctypes.c_double * 3)(*c["fb"]), int(c["et"]), int(c["electron_heating"]))
+
+
+def settei_ng(fields, consts, qtotal, with_system=False):
+    """settei_ng column step (src/settei_ng.F90:60-261); returns (te_out,
+    ti_out, qtotal_out) and, if with_system, (p, q, r, rhs) rows 1..nk-1."""
+    L = lib()
+    if not hasattr(L, "_settei_bound"):
+        L.oracle_settei_ng.argtypes = [ctypes.POINTER(SetteiFields), ctypes.POINTER(SetteiConsts), ctypes.c_int,
+                                       ctypes.c_long] + [ctypes.c_void_p] * 7
+        L.oracle_settei_ng.restype = None
+        L._settei_bound = True
+    arrs = {k: _fcopy(fields[k]) for k in SETTEI_FIELD_ORDER}
+    nk, ncol = arrs["tn"].shape[0], arrs["tn"].size // arrs["tn"].shape[0]
+    F = SetteiFields(*[arrs[k].ctypes.data for k in SETTEI_FIELD_ORDER])
+    C = settei_consts(consts)
+    te_out, ti_out = np.zeros((nk, ncol), order="F"), np.zeros((nk, ncol), order="F")
+    qt = _fcopy(qtotal).copy(order="F")
+    sysarr = [np.zeros((nk, ncol), order="F") for _ in range(4)] if with_system else [None] * 4
+    L.oracle_settei_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, _p(te_out), _p(ti_out), _p(qt),
+                       *[_p(s) for s in sysarr])
+    return ((te_out, ti_out, qt), tuple(sysarr)) if with_system else (te_out, ti_out, qt)

@@ -958,3 +958,210 @@ ORACLE_API void oracle_comp_post_ng(const double *o2, const double *o1, const do
     }
     free(n2);
 }
+
+/* ------------------------------------------------------------------------ */
+/* settei_ng electron / ion temperature column step (src/settei_ng.F90:     */
+/* 60-261): the whole routine is column-local.  Fields (nk, ncol), 2-D      */
+/* (ncol).  qtotal is read and updated (qtotal += q_eni_i, :254).  te_out   */
+/* and ti_out receive the new Te and Ti; p,q,r,rhs (may be NULL) the system */
+/* rows 1..nk-1 after the boundary folds.                                   */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    const double *tn, *o2, *o1, *he, *n2, *ne, *te, *ti, *op, *o2p, *nplus, *n2p, *nop, *xnmbar, *xnmbari, *scht,
+        *schti, *qji_ti, *qop2p, *qop2d, *qo2p, *qop, *qn2p, *qnp, *qnop, *Q1, *Q2;
+    const double *t_lbc, *chi, *rlatm, *dipmag, *qteaur;
+} oracle_settei_fields;
+
+typedef struct {
+    double f107, dipmin, dz, evergs, avo, rmass_o1;
+    double rmassinv_o2, rmassinv_o1, rmassinv_he, rmassinv_n2, rmassinv_n4s, rmassinv_no;
+    double b[9], fb[3];
+    int et, electron_heating;
+} oracle_settei_consts;
+
+static double omax(double a, double b) { return a > b ? a : b; }
+static double omin(double a, double b) { return a < b ? a : b; }
+
+ORACLE_API void oracle_settei_ng(const oracle_settei_fields *F, const oracle_settei_consts *C, int nk, long ncol,
+                                 double *te_out, double *ti_out, double *qtotal, double *p_out, double *q_out,
+                                 double *r_out, double *rhs_out)
+{
+    const double fpolar = -3.0e+9, del = 1.e-6, alam = 0.0069, ad = 0.0091, sd = 2.3e-11;
+    const double pi = 4.0 * atan(1.0), rtd = 180.0 / pi, dz = C->dz, ev = C->evergs;
+    const double *b = C->b, *fb = C->fb;
+    double *w = (double *)malloc(sizeof(double) * 21 * (size_t)nk);
+    long col;
+    if (nk < 3) { free(w); return; }
+    for (col = 0; col < ncol; ++col) {
+        const size_t o = (size_t)nk * col;
+        const double *tn = F->tn + o, *o2 = F->o2 + o, *o1 = F->o1 + o, *he = F->he + o, *n2 = F->n2 + o,
+                     *ne = F->ne + o, *te = F->te + o, *ti = F->ti + o, *xnmbar = F->xnmbar + o,
+                     *xnmbari = F->xnmbari + o, *hmid = F->scht + o, *hint = F->schti + o;
+        double *te_int = w, *o2n = w + nk, *o1n = w + 2 * nk, *hen = w + 3 * nk, *n2n = w + 4 * nk,
+               *tn_int = w + 5 * nk, *tek0 = w + 6 * nk, *p = w + 7 * nk, *q = w + 8 * nk, *r = w + 9 * nk,
+               *rhs = w + 10 * nk, *th = w + 11 * nk, *qtot = w + 12 * nk, *rne = w + 13 * nk,
+               *loss_ei = w + 14 * nk, *loss_in = w + 15 * nk, *q_eni = w + 16 * nk, *ws = w + 17 * nk,
+               *x = w + 20 * nk;
+        int k;
+        /* fe: the upper-boundary heat flux (:62-87) */
+        const double f107te = omin(C->f107, 235.);
+        const double arl = fabs(F->rlatm[col]), chi = F->chi[col];
+        double a = 0., fed, fen, fe;
+        if (arl >= pi / 4.5) a = 1.;
+        if (arl < pi / 4.5 && arl > pi / 18) a = .5 * (1. + cos(arl * 6. - pi * 4. / 3.));
+        if (arl <= pi / 18) a = 0.;
+        fed = -9.0e+7 * f107te * a;
+        fen = fed / 2.;
+        fed = fed + F->qteaur[col];
+        fen = fen + F->qteaur[col];
+        fe = chi >= .5 * pi ? fen : fed;
+        if ((chi * rtd - 80.) * (chi * rtd - 100.) >= 0.) fe = fe * ev;
+        else fe = (.5 * (fed + fen) + .5 * (fed - fen) * cos(pi * (chi * rtd - 80.) / 20.)) * ev;
+        if (arl >= pi / 3.) fe = fe + fpolar * ev;
+        /* interface quantities (:89-120) */
+        for (k = 1; k < nk - 1; ++k) {
+            te_int[k] = .5 * (te[k] + te[k - 1]);
+            o2n[k] = .5 * (o2[k] + o2[k - 1]);
+            o1n[k] = .5 * (o1[k] + o1[k - 1]);
+            hen[k] = .5 * (he[k] + he[k - 1]);
+            n2n[k] = .5 * (n2[k] + n2[k - 1]);
+            tn_int[k] = .5 * (tn[k] + tn[k - 1]);
+        }
+        te_int[0] = omax(1.5 * te[0] - .5 * te[1], F->t_lbc[col]);
+        o2n[0] = .5 * (fb[0] + (b[0] + 1.) * o2[0] + b[3] * o1[0] + b[6] * he[0]);
+        o1n[0] = .5 * (fb[0] + b[0] * o2[0] + (b[3] + 1.) * o1[0] + b[6] * he[0]);
+        hen[0] = .5 * (fb[0] + b[0] * o2[0] + b[3] * o1[0] + (b[6] + 1.) * he[0]);
+        n2n[0] = omax(1. - o2n[0] - o1n[0] - hen[0], 0.);
+        tn_int[0] = F->t_lbc[col];
+        te_int[nk - 1] = 1.5 * te[nk - 2] - .5 * te[nk - 3];
+        o2n[nk - 1] = .5 * (o2[nk - 1] + o2[nk - 2]);
+        o1n[nk - 1] = .5 * (o1[nk - 1] + o1[nk - 2]);
+        hen[nk - 1] = .5 * (he[nk - 1] + he[nk - 2]);
+        n2n[nk - 1] = .5 * (n2[nk - 1] + n2[nk - 2]);
+        tn_int[nk - 1] = 1.5 * tn[nk - 2] - .5 * tn[nk - 3];
+        for (k = 0; k < nk; ++k) {
+            n2n[k] = omax(n2n[k], 0.);
+            o2n[k] = xnmbari[k] * o2n[k] * C->rmassinv_o2;
+            o1n[k] = xnmbari[k] * o1n[k] * C->rmassinv_o1;
+            hen[k] = xnmbari[k] * hen[k] * C->rmassinv_he;
+            n2n[k] = xnmbari[k] * n2n[k] * C->rmassinv_n2;
+        }
+        /* thermal conductivity and the conduction rows (:122-155) */
+        {
+            const double sd_ = sin(omax(fabs(F->dipmag[col]), C->dipmin));
+            const double sindip = omax(sd_ * sd_, .10);
+            for (k = 0; k < nk; ++k) {
+                const double rt = sqrt(te_int[k]);
+                tek0[k] = 7.5e5 /
+                          (1. + 3.22e4 * (te_int[k] * te_int[k]) / ne[k] *
+                                    ((2.20e-16 + 7.92e-18 * rt) * o2n[k] + 1.10e-16 * (1. + 5.7e-4 * te_int[k]) * o1n[k] +
+                                     5.60e-16 * hen[k] + (2.82e-17 - 3.41e-21 * te_int[k]) * rt * n2n[k])) *
+                          ev;
+                p[k] = 2. / 7. / (hmid[k] * (dz * dz));
+                p[k] = p[k] * sindip;
+                th[k] = tek0[k] / hint[k];
+            }
+            for (k = 0; k < nk; ++k) {
+                const double th1 = k < nk - 1 ? th[k + 1] : 2. * th[nk - 1] - th[nk - 2];
+                r[k] = p[k] * th1;
+                p[k] = p[k] * th[k];
+                q[k] = -(p[k] + r[k]);
+                rhs[k] = 0.;
+            }
+            q[0] = q[0] - p[0];
+            rhs[0] = rhs[0] - 2. * p[0] * pow(tn_int[0], 3.5);
+            p[0] = 0.;
+            q[nk - 2] = q[nk - 2] + r[nk - 2];
+            rhs[nk - 2] = rhs[nk - 2] + r[nk - 2] * dz * 3.5 * hint[nk - 1] * fe / tek0[nk - 1];
+            r[nk - 2] = 0.;
+        }
+        /* heating (:157-186) */
+        for (k = 0; k < nk; ++k)
+            qtot[k] = omax(F->qo2p[o + k] + F->qop[o + k] + F->qn2p[o + k] + F->qnop[o + k] + F->qnp[o + k] +
+                               F->qop2d[o + k] + F->qop2p[o + k],
+                           1.e-20);
+        for (k = 0; k < nk - 1; ++k) qtot[k] = sqrt(qtot[k] * qtot[k + 1]);
+        qtot[nk - 1] = 0.;
+        for (k = 0; k < nk - 1; ++k) rne[k] = ne[k] * ne[k + 1];
+        rne[nk - 1] = ne[nk - 1] * ne[nk - 1] * ne[nk - 1] / ne[nk - 2];
+        for (k = 0; k < nk; ++k) {
+            rne[k] = sqrt(omax(rne[k], 1.e4));
+            o2n[k] = xnmbar[k] * o2[k] * C->rmassinv_o2;
+            o1n[k] = xnmbar[k] * o1[k] * C->rmassinv_o1;
+            hen[k] = xnmbar[k] * he[k] * C->rmassinv_he;
+            n2n[k] = xnmbar[k] * n2[k] * C->rmassinv_n2;
+            double qe;
+            if (C->electron_heating == 6) {
+                qe = log(rne[k] / (o2n[k] + n2n[k] + o1n[k]));
+                qe = exp(((((((-1.249e-5 * qe - 5.755e-4) * qe - 9.346e-3) * qe - 5.900e-2) * qe - 4.392e-2) * qe +
+                           1.056) * qe + 5.342));
+            } else {
+                qe = log(rne[k] / (o2n[k] + n2n[k] + 0.1 * o1n[k]));
+                qe = exp(-((((0.001996 * qe + 0.08034) * qe + 1.166) * qe + 6.941) * qe + 12.75));
+            }
+            rhs[k] = rhs[k] - qe * qtot[k] * ev;
+            if (C->et) rhs[k] = rhs[k] - (F->Q1[o + k] + F->Q2[o + k]) * 10.0;
+        }
+        /* electron cooling, electron-ion and ion-neutral exchange (:188-246) */
+        for (k = 0; k < nk; ++k) {
+            const double tek = te[k], tnk = tn[k], rt = sqrt(tek);
+            double coll, l2v, leo2, leo1, lehe, len2, len, lxen;
+            const double leo1d = 0.;
+            if (tek >= 1000.) coll = 2.e-7 * exp(-4605.2 / tek);
+            else coll = 5.71e-8 * exp(-3352.6 / tek);
+            if (tek > 2000.) coll = 2.53e-6 * rt * exp(-17620. / tek);
+            if (fabs(tek - tnk) < del) l2v = 3200. / (tnk * tnk);
+            else l2v = 1. / (tek - tnk) * (1. - exp(-3200. * (tek - tnk) / (tek * tnk)));
+            l2v = 1.3e-4 * l2v * coll;
+            leo2 = o2n[k] * (1.21e-18 * (1. + 3.6e-2 * rt) * rt + 6.9e-14 / rt + 3.125e-21 * (tek * tek));
+            leo1 = o1n[k] * (7.9e-19 * (1. + 5.7e-4 * tek) * rt + 3.4e-12 * (1. - 7.e-5 * tek) / tnk * (150. / tek + 0.4));
+            lehe = hen[k] * 2.46e-17 * rt;
+            len2 = n2n[k] * (1.77E-19 * (1. - 1.21E-4 * tek) * tek + 2.9e-14 / rt + l2v);
+            len = leo2 + leo1 + lehe + len2;
+            if (C->et && tek > 500.0 && F->Q2[o + k] > 0.0) len = len * exp(-7.54E-4 * (tek - 500.0));
+            lxen = (len + o1n[k] * (1. - alam / (ad + sd * n2n[k])) * leo1d) * rne[k] * ev;
+            len = (len + o1n[k] * leo1d) * rne[k] * ev;
+            loss_ei[k] = 3.2e-8 * rne[k] / (rt * tek) * 15. * ev * C->rmass_o1 *
+                         (F->op[o + k] * C->rmassinv_o1 + F->o2p[o + k] * C->rmassinv_o2 +
+                          F->nplus[o + k] * C->rmassinv_n4s + F->n2p[o + k] * C->rmassinv_n2 +
+                          F->nop[o + k] * C->rmassinv_no);
+            const double rtn = sqrt(2 * tnk);
+            loss_in[k] = 1e-14 * ev *
+                         (F->op[o + k] * (5.8 * o2n[k] + 0.21 * o1n[k] * rtn + 2.8 * hen[k] + 6.6 * n2n[k]) +
+                          F->o2p[o + k] * (0.14 * o2n[k] * rtn + 4.36 * o1n[k] + 1.63 * hen[k] + 5.81 * n2n[k]) +
+                          F->nplus[o + k] * (5.84 * o2n[k] + 5.84 * o1n[k] + 3.05 * hen[k] + 6.56 * n2n[k]) +
+                          F->n2p[o + k] * (5.54 * o2n[k] + 4.65 * o1n[k] + 1.82 * hen[k] + 0.27 * n2n[k] * rtn) +
+                          F->nop[o + k] * (5.45 * o2n[k] + 4.5 * o1n[k] + 1.72 * hen[k] + 5.92 * n2n[k]));
+            q[k] = q[k] - (len + loss_ei[k]) / pow(tek, 2.5);
+            rhs[k] = rhs[k] - len * tnk - loss_ei[k] * ti[k];
+            q_eni[k] = loss_ei[k] * omax(tek - ti[k], 0.);
+            q_eni[k] = (lxen * (tek - tnk) + q_eni[k]) * C->avo / xnmbar[k];
+        }
+        /* qtotal += q_eni at interfaces (:248-254) */
+        for (k = 1; k < nk - 1; ++k) qtotal[o + k] = qtotal[o + k] + .5 * (q_eni[k - 1] + q_eni[k]);
+        {
+            const double q0 = 1.5 * q_eni[0] - 0.5 * q_eni[1], qn = 1.5 * q_eni[nk - 2] - 0.5 * q_eni[nk - 3];
+            qtotal[o] = qtotal[o] + q0;
+            qtotal[o + nk - 1] = qtotal[o + nk - 1] + qn;
+        }
+        if (p_out)
+            for (k = 0; k < nk; ++k) {
+                p_out[o + k] = p[k];
+                q_out[o + k] = q[k];
+                r_out[o + k] = r[k];
+                rhs_out[o + k] = rhs[k];
+            }
+        /* solve rows 1..nk-1, Te = (Te^3.5)^(2/7), top level, Ti (:256-261) */
+        thomas_column(p, q, r, rhs, x, nk - 1, ws);
+        for (k = 0; k < nk - 1; ++k) x[k] = pow(x[k], 2. / 7.);
+        x[nk - 1] = x[nk - 2] * x[nk - 2] / x[nk - 3];
+        for (k = 0; k < nk; ++k) {
+            const double t = omax(x[k], tn[k]);
+            te_out[o + k] = t;
+            ti_out[o + k] = omax((F->qji_ti[o + k] * xnmbar[k] / C->avo + loss_ei[k] * t + loss_in[k] * tn[k]) /
+                                     (loss_ei[k] + loss_in[k]),
+                                 tn[k]);
+        }
+    }
+    free(w);
+}

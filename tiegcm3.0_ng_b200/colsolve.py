@@ -37,9 +37,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
-EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
+EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor_ng_dev", "tg_comp_ng",
+           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
-           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_plan_sweep_histogram", "tg_plan_destroy",
+           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
 
 
@@ -105,6 +106,30 @@ def minor_consts(c):
                        (ctypes.c_double * 9)(*np.ravel(c["b"], order="F")), (ctypes.c_double * 3)(*c["fb"]))
 
 
+COMP_FIELDS = ("tn", "o2", "o1", "he", "w", "mbar", "o2nm_smooth", "o1nm_smooth", "henm_smooth", "o2_advec",
+               "o1_advec", "he_advec", "hdo2", "hdo1", "hdhe", "fs", "tlbc", "flx_he", "dfactor", "expz", "difk")
+COMP_CONSTS = ("dz", "dtx2inv", "expzmid", "expzmid_inv", "rmassinv_o2", "rmassinv_o1", "rmassinv_he",
+               "rmassinv_n2", "rmass_o2", "rmass_o1", "rmass_he", "p0", "grav")
+
+
+class CompFields(ctypes.Structure):
+    """tg_comp_fields of include/tg_colsolve.h."""
+    _fields_ = [(n, ctypes.c_void_p) for n in COMP_FIELDS]
+
+
+class CompConsts(ctypes.Structure):
+    """tg_comp_consts of include/tg_colsolve.h."""
+    _fields_ = ([(n, ctypes.c_double) for n in COMP_CONSTS] +
+                [("b", ctypes.c_double * 9), ("fb", ctypes.c_double * 3), ("pshelb", ctypes.c_double),
+                 ("calc_helium", ctypes.c_int)])
+
+
+def comp_consts(c):
+    return CompConsts(*[float(c[n]) for n in COMP_CONSTS], (ctypes.c_double * 9)(*np.ravel(c["b"], order="F")),
+                      (ctypes.c_double * 3)(*c["fb"]), float(c.get("pshelb", 0.1154e-5)),
+                      int(c.get("calc_helium", 1)))
+
+
 _lib = None
 
 
@@ -122,6 +147,9 @@ def lib():
             "tg_dt_ng": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I],
             "tg_solve_host": [ctypes.POINTER(HostSystem), I],
             "tg_minor_ng": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, I, I],
+            "tg_comp_ng": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, P, P, I, I],
+            "tg_comp_ng_dev": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, I, I, Lg, P, P, P],
+            "tg_comp_post_ng": [P] * 8 + [D, D, D, I, I] + [P] * 6,
             "tg_minor_ng_dev": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, I, I, Lg, P, P, P],
             "tg_dt_ng_dev": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I, Lg, P, P, P],
             "tg_trsolv_ng": [P, P, P, P, P, I, I, I],
@@ -137,6 +165,7 @@ def lib():
             "tg_plan_status": [P, P],
             "tg_plan_launches": [P],
             "tg_plan_describe": [P, ctypes.c_char_p, I],
+            "tg_set_cache_hints": [I],
             "tg_plan_sweep_histogram": [P, ctypes.POINTER(Lg), I],
             "tg_plan_destroy": [P],
             "tg_set_refine": [I, D],
@@ -305,6 +334,48 @@ def minor_ng(fields, consts, fcomp_out):
     return _check(rc, "tg_minor_ng")
 
 
+def comp_ng(fields, consts, o2_upd, o1_upd, he_upd):
+    """comp_ng's column step (src/comp_ng.F90:74-332) on host arrays: fields
+    COMP_FIELDS ((nk, ncol) Fortran order, fs (12, ncol, nk) C order = the
+    reference's fs(nk, ncol, 3, 0:3)); outputs (nk, ncol) O2, O, He."""
+    nk = o2_upd.shape[0]
+    ncol = o2_upd.size // nk
+    if np.asarray(fields["fs"]).size != 12 * nk * ncol:
+        raise ValueError("fs must hold 12 slabs of nk*ncol")
+    arrs = {n: np.ascontiguousarray(fields[n], dtype=np.float64).reshape(-1) if n == "fs" else fields[n]
+            for n in COMP_FIELDS}
+    F = CompFields(*[_host(arrs[n], n) for n in COMP_FIELDS])
+    C = comp_consts(consts)
+    rc = lib().tg_comp_ng(ctypes.byref(F), ctypes.byref(C), _out(o2_upd, "o2_upd"), _out(o1_upd, "o1_upd"),
+                          _out(he_upd, "he_upd"), nk, ncol)
+    return _check(rc, "tg_comp_ng")
+
+
+def comp_ng_dev(fields, consts, out, nk, ncol, ld, system_out=None, status=None, stream=None):
+    F = CompFields(*[_dptr(fields[n]) for n in COMP_FIELDS])
+    C = comp_consts(consts)
+    rc = lib().tg_comp_ng_dev(ctypes.byref(F), ctypes.byref(C), _dptr(out), nk, ncol, ld, _dptr(system_out),
+                              None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_comp_ng_dev", numeric_ok=False)
+
+
+POST_INPUTS = ("o2", "o1", "he", "o2_nm", "o1_nm", "he_nm", "xnmbar")
+
+
+def comp_post_ng(fields, consts, upd, nm_out):
+    """comp_ng's post-solve steps (src/comp_ng.F90:415-457): upd = [o2, o1, he]
+    (nk, ncol) updated in place, nm_out = [o2nm, o1nm, henm] receive the
+    filtered fields."""
+    nk = upd[0].shape[0]
+    ncol = upd[0].size // nk
+    ins = [_host(fields[n], n) for n in POST_INPUTS]
+    zp = np.ascontiguousarray(fields["zpmid"], dtype=np.float64)
+    rc = lib().tg_comp_post_ng(*ins, zp.ctypes.data, float(consts["dz"]), float(consts["dtsmooth"]),
+                               float(consts["dtsmooth_div2"]), nk, ncol,
+                               *[_out(u, "upd") for u in upd], *[_out(u, "nm_out") for u in nm_out])
+    return _check(rc, "tg_comp_post_ng")
+
+
 def minor_ng_dev(fields, consts, out, nk, ncol, ld, system_out=None, status=None, stream=None):
     F = MinorFields(*[_dptr(fields[n]) for n in MINOR_FIELDS])
     C = minor_consts(consts)
@@ -416,6 +487,11 @@ def selftest_division(a, b, q, stream=None):
     """q = a/b on the device through the kernels' division routine."""
     return _check(lib().tg_selftest_division(_dptr(a), _dptr(b), _dptr(q), int(q.numel()), _stream(stream)),
                   "tg_selftest_division", numeric_ok=False)
+
+
+def set_cache_hints(on):
+    """L2 eviction-priority hints of the ring kernels (1 on, 0 off, -1 default)."""
+    return _check(lib().tg_set_cache_hints(int(on)), "tg_set_cache_hints")
 
 
 def release_buffers():

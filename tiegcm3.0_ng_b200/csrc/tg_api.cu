@@ -799,6 +799,149 @@ __attribute__((visibility("default"))) int tg_minor_ng(const tg_minor_fields *F,
     return flags_to_status(c->flags_host[0]);
 }
 
+static bool comp_fields_ok(const tg_comp_fields *F)
+{
+    const double *const p[] = {F->tn, F->o2, F->o1, F->he, F->w, F->mbar, F->o2nm_smooth, F->o1nm_smooth,
+                               F->henm_smooth, F->o2_advec, F->o1_advec, F->he_advec, F->hdo2, F->hdo1, F->hdhe,
+                               F->fs, F->tlbc, F->flx_he, F->dfactor, F->expz, F->difk};
+    for (const double *q : p)
+        if (!q) return false;
+    return true;
+}
+
+__attribute__((visibility("default"))) int tg_comp_ng_dev(const tg_comp_fields *F, const tg_comp_consts *C,
+                                                          double *out, int nk, int ncol, long ld, double *system_out,
+                                                          int *status_dev, void *stream)
+{
+    if (!F || !C || !out || nk < 3 || ncol < 0 || ld < ncol || !comp_fields_ok(F)) {
+        set_err("tg_comp_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = grow(cx->scratch[0], sizeof(double) * 12 * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
+    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_comp_ng(*F, *C, out, (double *)cx->scratch[0].p, nk, ncol, ld, system_out, cx->flags, st));
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_comp_ng(const tg_comp_fields *F, const tg_comp_consts *C,
+                                                      double *o2_upd, double *o1_upd, double *he_upd, int nk,
+                                                      int ncol)
+{
+    if (!F || !C || !o2_upd || !o1_upd || !he_upd || nk < 3 || ncol < 0 || !comp_fields_ok(F)) {
+        set_err("tg_comp_ng: bad arguments (nk=%d ncol=%d)", nk, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ld = round_up(ncol, 32);
+    const size_t lvl = (size_t)nk * ld, colsz = (size_t)nk * ncol;
+    // 15 fields + 12 fs slabs + 3 outputs, level-major; 3 2-D rows; 2 level profiles
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (30 * lvl + 3 * (size_t)ld + 2 * (size_t)nk)))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * colsz))) return rc;
+    if ((rc = grow(c->scratch[0], sizeof(double) * 12 * lvl))) return rc;
+    double *base = (double *)c->lvlbuf[0][0].p, *stage = (double *)c->colbuf[0][0].p;
+    cudaStream_t st = c->st[0];
+    tg_comp_fields D;
+    const double *src3[15] = {F->tn, F->o2, F->o1, F->he, F->w, F->mbar, F->o2nm_smooth, F->o1nm_smooth,
+                              F->henm_smooth, F->o2_advec, F->o1_advec, F->he_advec, F->hdo2, F->hdo1, F->hdhe};
+    const double **dst3[15] = {&D.tn, &D.o2, &D.o1, &D.he, &D.w, &D.mbar, &D.o2nm_smooth, &D.o1nm_smooth,
+                               &D.henm_smooth, &D.o2_advec, &D.o1_advec, &D.he_advec, &D.hdo2, &D.hdo1, &D.hdhe};
+    for (int i = 0; i < 27; ++i) {
+        const double *h = i < 15 ? src3[i] : F->fs + (size_t)(i - 15) * colsz;
+        double *d = base + i * lvl;
+        TG_CUDA(cudaMemcpyAsync(stage, h, sizeof(double) * colsz, cudaMemcpyHostToDevice, st));
+        TG_CUDA(launch_col_to_level(stage, nk, d, ld, nk, ncol, st));
+        if (i < 15) *dst3[i] = d;
+    }
+    D.fs = base + 15 * lvl;
+    double *out_l = base + 27 * lvl, *two = base + 30 * lvl, *one = two + 3 * ld;
+    const double *src2[3] = {F->tlbc, F->flx_he, F->dfactor};
+    const double **dst2[3] = {&D.tlbc, &D.flx_he, &D.dfactor};
+    for (int i = 0; i < 3; ++i) {
+        TG_CUDA(cudaMemcpyAsync(two + i * ld, src2[i], sizeof(double) * ncol, cudaMemcpyHostToDevice, st));
+        *dst2[i] = two + i * ld;
+    }
+    TG_CUDA(cudaMemcpyAsync(one, F->expz, sizeof(double) * nk, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(one + nk, F->difk, sizeof(double) * nk, cudaMemcpyHostToDevice, st));
+    D.expz = one;
+    D.difk = one + nk;
+    TG_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_comp_ng(D, *C, out_l, (double *)c->scratch[0].p, nk, ncol, ld, nullptr, c->flags, st));
+    double *hout[3] = {o2_upd, o1_upd, he_upd};
+    for (int i = 0; i < 3; ++i) {
+        TG_CUDA(launch_level_to_col(out_l + i * lvl, ld, stage, nk, nk, ncol, st));
+        TG_CUDA(cudaMemcpyAsync(hout[i], stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
+        // the staging buffer is reused by the next species
+        TG_CUDA(cudaStreamSynchronize(st));
+    }
+    TG_CUDA(cudaMemcpy(c->flags_host, c->flags, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    return flags_to_status(c->flags_host[0]);
+}
+
+__attribute__((visibility("default"))) int tg_comp_post_ng(const double *o2, const double *o1, const double *he,
+                                                           const double *o2_nm, const double *o1_nm,
+                                                           const double *he_nm, const double *xnmbar,
+                                                           const double *zpmid, double dz, double dtsmooth,
+                                                           double dtsmooth_div2, int nk, int ncol, double *o2_upd,
+                                                           double *o1_upd, double *he_upd, double *o2nm_upd,
+                                                           double *o1nm_upd, double *henm_upd)
+{
+    const double *in7[7] = {o2, o1, he, o2_nm, o1_nm, he_nm, xnmbar};
+    double *io6[6] = {o2_upd, o1_upd, he_upd, o2nm_upd, o1nm_upd, henm_upd};
+    bool ok = zpmid && nk >= 1 && ncol >= 0;
+    for (const double *p : in7) ok = ok && p;
+    for (double *p : io6) ok = ok && p;
+    if (!ok) {
+        set_err("tg_comp_post_ng: bad arguments (nk=%d ncol=%d)", nk, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ld = round_up(ncol, 32);
+    const size_t lvl = (size_t)nk * ld, colsz = (size_t)nk * ncol;
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (13 * lvl + (size_t)nk)))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * colsz))) return rc;
+    double *base = (double *)c->lvlbuf[0][0].p, *stage = (double *)c->colbuf[0][0].p;
+    cudaStream_t st = c->st[0];
+    const double *din[7];
+    double *dio[6];
+    for (int i = 0; i < 10; ++i) {
+        const double *h = i < 7 ? in7[i] : io6[i - 7];
+        double *d = base + i * lvl;
+        TG_CUDA(cudaMemcpyAsync(stage, h, sizeof(double) * colsz, cudaMemcpyHostToDevice, st));
+        TG_CUDA(launch_col_to_level(stage, nk, d, ld, nk, ncol, st));
+        if (i < 7) din[i] = d;
+        else dio[i - 7] = d;
+    }
+    for (int i = 3; i < 6; ++i) dio[i] = base + (10 + i - 3) * lvl;
+    double *zp = base + 13 * lvl;
+    TG_CUDA(cudaMemcpyAsync(zp, zpmid, sizeof(double) * nk, cudaMemcpyHostToDevice, st));
+    TG_CUDA(launch_comp_post_ng(din, zp, dz, dtsmooth, dtsmooth_div2, nk, ncol, ld, dio, st));
+    for (int i = 0; i < 6; ++i) {
+        TG_CUDA(launch_level_to_col(dio[i], ld, stage, nk, nk, ncol, st));
+        TG_CUDA(cudaMemcpyAsync(io6[i], stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaStreamSynchronize(st));
+    }
+    return TG_OK;
+}
+
 __attribute__((visibility("default"))) int tg_trsolv_dev(const double *a, const double *b, const double *c,
                                                          const double *f, double *x, int nk, int k2, int ncol,
                                                          int layout, long ld, int precision, int *status_dev,
@@ -1086,6 +1229,12 @@ __attribute__((visibility("default"))) int tg_plan_status(tg_plan *p, int *per_s
 }
 
 __attribute__((visibility("default"))) int tg_plan_launches(const tg_plan *p) { return p ? p->launches : 0; }
+
+__attribute__((visibility("default"))) int tg_set_cache_hints(int on)
+{
+    tg::set_cache_hints(on);
+    return TG_OK;
+}
 
 __attribute__((visibility("default"))) int tg_plan_describe(const tg_plan *p, char *buf, int n)
 {

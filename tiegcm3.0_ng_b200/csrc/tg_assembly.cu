@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
     const int K = nk - 1;   // rows 0..K-1 are solved
 
     // window: level k-1, k, k+1 values
-    double tn_m = 0.0, tn_0 = at(F.tn, 0), tn_p = at(F.tn, 1);
+    double tn_0 = at(F.tn, 0), tn_p = at(F.tn, 1);
     double un_m = 0.0, un_0 = at(F.un, 0), un_p = at(F.un, 1);
     double vn_m = 0.0, vn_0 = at(F.vn, 0), vn_p = at(F.vn, 1);
     double w_0 = at(F.w, 0), w_p = at(F.w, 1);
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
         dvdz_prev = dvdz;
         gf0 = gfp;
         v0_0 = v0_p;
-        tn_m = tn_0; tn_0 = tn_p;
+        tn_0 = tn_p;
         un_m = un_0; un_0 = un_p;
         vn_m = vn_0; vn_0 = vn_p;
         w_0 = w_p; cp_0 = cp_p; km_0 = km_p; qt_0 = qt_p;
@@ -166,7 +166,6 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
             qt_p = at(F.qtotal, k + 2);
         }
     }
-    (void)tn_m;
     // back sweep (trsolv_ng.F90:23-26), then tn(nk) = tn(nk-1)**2/tn(nk-2)
     double xn = w3, xprev = w3;
     bool fin = fabs(xn) <= DBL_MAX;
@@ -348,7 +347,7 @@ __global__ void __launch_bounds__(128) k_minor_ng(MinorFields F, MinorConsts C, 
     const double dfac = __ldg(F.dfactor + col);
     const double rdz = xd(1.0, dzp);
     bool ok = true;
-    double w1 = 0.0, w3 = 0.0, rprev = 0.0, y0 = 0.0;
+    double w1 = 0.0, w3 = 0.0, rprev = 0.0;
     for (int k = 0; k < nk; ++k) {
         double p, q, r, f;
         const double expz = __ldg(F.expz + k);
@@ -422,7 +421,6 @@ __global__ void __launch_bounds__(128) k_minor_ng(MinorFields F, MinorConsts C, 
         rprev = r;
         L0 = L1;
     }
-    (void)y0;
     (void)tn_a;
     (void)tni_m;
     double xn = w3;
@@ -457,4 +455,346 @@ cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *
     return cudaGetLastError();
 }
 
+}  // namespace tg
+
+// ===========================================================================
+// comp_ng (O2, O, He): src/comp_ng.F90:74-332, assembly fused with the 3x3
+// block solve.  Row k needs ep and ak = inv(alpha)*wks1 of levels k and k+1
+// and the interface averages of level k+1; a thread carries level k from the
+// previous row.  The forward sweep keeps Gamma_{k+1} (9) and z_{k+1} (3) of
+// every row in a level-major global scratch (L2-resident for the back sweep).
+// The fractional powers use the device pow, as in minor_ng: the kernel agrees
+// with the CPU restatement to a stated tolerance.
+// ===========================================================================
+namespace tg {
+namespace {
+struct CompLevel {
+    double ep[3], ak[9], wks4, a22, a33, a23, a32;
+};
+
+// ep, alpha, ak and wks4 of one level (comp_ng.F90:128-166, 176-211)
+__device__ __forceinline__ void comp_level(const CompConsts &C, double o2i, double o1i, double hei, double embari,
+                                           double tni, double dembardz, double dtndz, bool thermal, CompLevel &L)
+{
+    const double tau = 1.86e+3, thdiffalpha = -0.38, t00 = 273.;
+    double df[3];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) df[n] = pow(xd(tni, t00), xs(1.75, kMSs[n]));
+    const double rinv = xd(1.0, embari);
+    L.ep[0] = xs(1.0, xm(rinv, xa(C.rmass_o2, dembardz)));
+    L.ep[1] = xs(1.0, xm(rinv, xa(C.rmass_o1, dembardz)));
+    L.ep[2] = xs(1.0, xm(rinv, xa(C.rmass_he, dembardz)));
+    if (thermal) L.ep[2] = xs(L.ep[2], xd(xm(thdiffalpha, dtndz), tni));
+#define PH(i, j) kMPhi[(i) - 1][(j) - 1]
+    double A[9], W[9];
+    A[0] = -xa(xa(PH(1, 4), xm(xs(PH(1, 2), PH(1, 4)), o1i)), xm(xs(xm(df[0], PH(1, 3)), PH(1, 4)), hei));
+    A[4] = -xa(xa(PH(2, 4), xm(xs(PH(2, 1), PH(2, 4)), o2i)), xm(xs(xm(df[1], PH(2, 3)), PH(2, 4)), hei));
+    A[8] = -xa(xa(xm(df[2], PH(3, 4)), xm(xs(xm(df[0], PH(3, 1)), xm(df[2], PH(3, 4))), o2i)),
+               xm(xs(xm(df[1], PH(3, 2)), xm(df[2], PH(3, 4))), o1i));
+    A[3] = xm(xs(PH(1, 2), PH(1, 4)), o2i);                          // (1,2)
+    A[6] = xm(xs(xm(df[0], PH(1, 3)), PH(1, 4)), o2i);               // (1,3)
+    A[1] = xm(xs(PH(2, 1), PH(2, 4)), o1i);                          // (2,1)
+    A[7] = xm(xs(xm(df[1], PH(2, 3)), PH(2, 4)), o1i);               // (2,3)
+    A[2] = xm(xs(xm(df[0], PH(3, 1)), xm(df[2], PH(3, 4))), hei);     // (3,1)
+    A[5] = xm(xs(xm(df[1], PH(3, 2)), xm(df[2], PH(3, 4))), hei);     // (3,2)
+#undef PH
+    L.a22 = A[4];
+    L.a33 = A[8];
+    L.a23 = A[7];
+    L.a32 = A[5];
+    inv3_ieee(A, W);
+    const double wks1 = xd(xm(xm(embari, C.rmassinv_n2), pow(xd(t00, tni), 0.25)), tau);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) L.ak[e] = xm(W[e], wks1);
+    L.wks4 = xd(dembardz, xm(embari, 2.0));
+}
+}  // namespace
+}  // namespace tg
+
+namespace tg {
+__global__ void __launch_bounds__(128) k_comp_ng(CompFields F, CompConsts C, double *out, double *scr, int nk, int ncol,
+                                                 long ld, double *sys_out, unsigned *status)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+    const long slab = (long)nk * ld;
+    const double tau = 1.86e+3, t00 = 273.;
+    const double dz = C.dz, rdz = xd(1.0, dz);
+    const double tlbc = __ldg(F.tlbc + col), dfac = __ldg(F.dfactor + col);
+    const double flx_he = C.calc_helium ? __ldg(F.flx_he + col) : 0.0;
+    const double *nms[3] = {F.o2nm_smooth, F.o1nm_smooth, F.henm_smooth};
+    const double *adv[3] = {F.o2_advec, F.o1_advec, F.he_advec};
+    const double *hd[3] = {F.hdo2, F.hdo1, F.hdhe};
+    // lower-boundary mixing ratios and level 1 (comp_ng.F90:74-96, 128-166)
+    double o2_0 = at(F.o2, 0), o1_0 = at(F.o1, 0), he_0 = at(F.he, 0), mb_0 = at(F.mbar, 0), tn_0 = at(F.tn, 0),
+           w_0 = at(F.w, 0);
+    double ps0[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        ps0[i] = xa(xa(xa(xm(C.b[i], o2_0), xm(C.b[i + 3], o1_0)), xm(C.b[i + 6], he_0)), C.fb[i]);
+    const double embar0 =
+        xd(1.0, xa(xa(xa(xm(ps0[0], C.rmassinv_o2), xm(ps0[1], C.rmassinv_o1)), xm(ps0[2], C.rmassinv_he)),
+                   xm(xs(xs(xs(1.0, ps0[0]), ps0[1]), ps0[2]), C.rmassinv_n2)));
+    double embari_k = xm(0.5, xa(embar0, mb_0));
+    CompLevel Lk, Lp;
+    comp_level(C, xm(0.5, xa(ps0[0], o2_0)), xm(0.5, xa(ps0[1], o1_0)), xm(0.5, xa(ps0[2], he_0)), embari_k, tlbc,
+               xd(xs(mb_0, embar0), dz), xd(xm(xs(tn_0, tlbc), 2.0), dz), true, Lp);
+    double G[9], z[3];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) G[e] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) z[i] = 0.0;
+    bool ok = true;
+    double flx00 = 1.0;
+    for (int k = 0; k < nk - 1; ++k) {
+        const double o2_1 = at(F.o2, k + 1), o1_1 = at(F.o1, k + 1), he_1 = at(F.he, k + 1),
+                     mb_1 = at(F.mbar, k + 1), tn_1 = at(F.tn, k + 1), w_1 = at(F.w, k + 1);
+        Lk = Lp;
+        const double embari_1 = xm(0.5, xa(mb_0, mb_1));
+        comp_level(C, xm(0.5, xa(o2_0, o2_1)), xm(0.5, xa(o1_0, o1_1)), xm(0.5, xa(he_0, he_1)), embari_1,
+                   xm(0.5, xa(tn_0, tn_1)), xd(xs(mb_1, mb_0), dz), xd(xs(tn_1, tn_0), dz), k + 1 != nk - 1, Lp);
+        const double wi = xm(0.5, xa(w_0, w_1));
+        const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1), ez = __ldg(F.expz + k);
+        // mol / eddy coefficients and the rows (comp_ng.F90:213-244)
+        const double eddyp = xm(xm(C.expzmid_inv, difk0), xs(rdz, Lk.wks4));
+        const double eddyr = xm(xm(C.expzmid, difk1), xa(rdz, Lp.wks4));
+        const double eddyq =
+            xa(xm(xm(C.expzmid_inv, difk0), xa(rdz, Lk.wks4)), xm(xm(C.expzmid, difk1), xs(rdz, Lp.wks4)));
+        const double ezdz = xd(ez, dz);
+        const double tp = xm(ezdz, xa(xm(eddyp, dfac), xm(0.5, wi)));
+        const double tr = xm(ezdz, xs(xm(eddyr, dfac), xm(0.5, wi)));
+        const double tq = xm(ez, xa(xd(xm(eddyq, dfac), dz), C.dtx2inv));
+        double P[9], Q[9], R[9], f[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const double hk = xd(Lk.ep[m], 2.0), hp = xd(Lp.ep[m], 2.0);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int e = i + 3 * m;
+                const double molp = xm(Lk.ak[e], xa(rdz, hk));
+                const double molr = xm(Lp.ak[e], xs(rdz, hp));
+                const double molq = xa(xm(Lk.ak[e], xs(rdz, hk)), xm(Lp.ak[e], xa(rdz, hp)));
+                const double fsl = xm(ez, at(F.fs + (long)((m + 1) * 3 + i) * slab, k));
+                P[e] = i == m ? xs(xd(molp, dz), tp) : xd(molp, dz);
+                R[e] = i == m ? xs(xd(molr, dz), tr) : xd(molr, dz);
+                Q[e] = i == m ? xs(xa(-xd(molq, dz), tq), fsl) : xs(-xd(molq, dz), fsl);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            f[i] = xm(ez, xa(xs(xm(at(nms[i], k), C.dtx2inv), xs(at(adv[i], k), at(F.fs + (long)i * slab, k))),
+                             at(hd[i], k)));
+        if (k == 0) {
+            // lower boundary b(3,3), fb(3) (comp_ng.F90:246-258)
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+#pragma unroll
+                for (int n = 0; n < 3; ++n)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) Q[i + 3 * m] = xa(Q[i + 3 * m], xm(P[i + 3 * n], C.b[n + 3 * m]));
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) f[i] = xs(f[i], xm(P[i + 3 * m], C.fb[m]));
+#pragma unroll
+            for (int e = 0; e < 9; ++e) P[e] = 0.0;
+        } else if (k == nk - 2) {
+            // upper boundary with the He escape flux (comp_ng.F90:259-279)
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                const double h = xm(xm(0.5, Lp.ep[m]), dz);
+                const double ratio = xd(xa(1.0, h), xs(1.0, h));
+#pragma unroll
+                for (int i = 0; i < 3; ++i) Q[i + 3 * m] = xa(Q[i + 3 * m], xm(ratio, R[i + 3 * m]));
+            }
+            flx00 = xd(xm(xm(xm(embari_k, C.rmassinv_n2), C.p0), pow(xd(t00, tn_0), 0.25)), xm(tau, C.grav));
+            const double d2 = xm(flx00, xs(rdz, xm(0.5, Lp.ep[1]))), d3 = xm(flx00, xs(rdz, xm(0.5, Lp.ep[2])));
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                f[i] = xs(xs(f[i], xd(xm(xm(R[i + 3], xs(Lp.a23, Lp.a22)), flx_he), d2)),
+                          xd(xm(xm(R[i + 6], xs(Lp.a33, Lp.a32)), flx_he), d3));
+#pragma unroll
+            for (int e = 0; e < 9; ++e) R[e] = 0.0;
+        }
+        if (sys_out) {
+            double *so = sys_out + (long)k * ld + col;
+#pragma unroll
+            for (int e = 0; e < 9; ++e) {
+                so[(long)e * slab] = P[e];
+                so[(long)(9 + e) * slab] = Q[e];
+                so[(long)(18 + e) * slab] = R[e];
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) so[(long)(27 + i) * slab] = f[i];
+        }
+        // block forward step (comp_ng.F90:280-314)
+        double W[9], v[3];
+        if (k > 0) {
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+#pragma unroll
+                for (int n = 0; n < 3; ++n)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) Q[i + 3 * m] = xs(Q[i + 3 * m], xm(P[i + 3 * n], G[n + 3 * m]));
+        }
+        inv3_ieee(Q, W);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) ok = ok && fabs(W[e]) <= DBL_MAX;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) v[i] = f[i];
+        if (k > 0) {
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) v[i] = xs(v[i], xm(P[i + 3 * m], z[m]));
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) z[i] = xa(xa(xm(W[i], v[0]), xm(W[i + 3], v[1])), xm(W[i + 6], v[2]));
+        if (k < nk - 2) {
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    G[i + 3 * m] = xa(xa(xm(W[i], R[3 * m]), xm(W[i + 3], R[1 + 3 * m])), xm(W[i + 6], R[2 + 3 * m]));
+            double *sg = scr + (long)(k + 1) * 12 * ld + col;
+#pragma unroll
+            for (int e = 0; e < 9; ++e) sg[(long)e * ld] = G[e];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) sg[(long)(9 + i) * ld] = z[i];
+        }
+        o2_0 = o2_1;
+        o1_0 = o1_1;
+        he_0 = he_1;
+        mb_0 = mb_1;
+        tn_0 = tn_1;
+        w_0 = w_1;
+        embari_k = embari_1;
+    }
+    // back sweep (comp_ng.F90:317-324); x(nk-1) = z_{nk-1}
+    bool fin = true;
+    double x[3], xb[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        x[i] = z[i];
+        xb[i] = z[i];
+        out[(long)i * slab + (long)(nk - 2) * ld + col] = x[i];
+        fin = fin && fabs(x[i]) <= DBL_MAX;
+    }
+    for (int k = nk - 3; k >= 0; --k) {
+        const double *sg = scr + (long)(k + 1) * 12 * ld + col;
+        double g[9], zk[3];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) g[e] = sg[(long)e * ld];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) zk[i] = sg[(long)(9 + i) * ld];
+        double xn[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            xn[i] = xs(xs(xs(zk[i], xm(g[i], x[0])), xm(g[i + 3], x[1])), xm(g[i + 6], x[2]));
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            x[i] = xn[i];
+            fin = fin && fabs(x[i]) <= DBL_MAX;
+            out[(long)i * slab + (long)k * ld + col] = x[i];
+        }
+    }
+    // top level (comp_ng.F90:326-332)
+    double top[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const double h = xm(xm(0.5, Lp.ep[i]), dz);
+        top[i] = xm(xd(xa(1.0, h), xs(1.0, h)), xb[i]);
+    }
+    top[1] = xa(top[1], xd(xm(xs(Lp.a23, Lp.a22), flx_he), xm(flx00, xs(rdz, xm(0.5, Lp.ep[1])))));
+    top[2] = xa(top[2], xd(xm(xs(Lp.a33, Lp.a32), flx_he), xm(flx00, xs(rdz, xm(0.5, Lp.ep[2])))));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        fin = fin && fabs(top[i]) <= DBL_MAX;
+        out[(long)i * slab + (long)(nk - 1) * ld + col] = top[i];
+    }
+    if (!C.calc_helium)
+        for (int k = 0; k < nk; ++k) out[2 * slab + (long)k * ld + col] = C.pshelb;
+    if (!ok || !fin) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+}
+
+cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out, double *scratch, int nk, int ncol,
+                           long ld, double *sys_out, unsigned *status, cudaStream_t st)
+{
+    if (ncol <= 0) return cudaSuccess;
+    if (nk < 3) return cudaErrorInvalidValue;
+    const int T = 128;
+    k_comp_ng<<<(ncol + T - 1) / T, T, 0, st>>>(F, C, out, scratch, nk, ncol, ld, sys_out, status);
+    return cudaGetLastError();
+}
+}  // namespace tg
+
+// comp_ng post-solve steps (src/comp_ng.F90:415-457), one thread per column.
+// The N2 extrapolation uses the device log/exp, so it agrees with the CPU
+// restatement to a tolerance in the extrapolated levels.
+namespace tg {
+__global__ void __launch_bounds__(128) k_comp_post_ng(const double *o2, const double *o1, const double *he,
+                                                      const double *o2_nm, const double *o1_nm, const double *he_nm,
+                                                      const double *xnmbar, const double *zpmid, double dz,
+                                                      double ds, double ds2, int nk, int ncol, long ld, double *o2u,
+                                                      double *o1u, double *heu, double *o2n, double *o1n,
+                                                      double *hen)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const double small = 1.e-9;
+    // first level with N2 < 0.01 (comp_ng.F90:425-429)
+    int ktop = nk;
+    for (int k = 0; k < nk; ++k) {
+        const long o = (long)k * ld + col;
+        const double n2 = xs(xs(xs(1.0, o2u[o]), o1u[o]), heu[o]);
+        if (n2 < 0.01) {
+            ktop = k;
+            break;
+        }
+    }
+    double n2top = 0.0, dn2dz = 0.0, zmtop = 0.0;
+    const bool extrap = ktop > 0 && ktop < nk - 1;
+    if (extrap) {
+        const long o = (long)ktop * ld + col, om = o - ld;
+        zmtop = zpmid[ktop];
+        n2top = log(xm(xs(xs(xs(1.0, o2u[o]), o1u[o]), heu[o]), xnmbar[o]));
+        const double n2top1 = log(xm(xs(xs(xs(1.0, o2u[om]), o1u[om]), heu[om]), xnmbar[om]));
+        dn2dz = xd(xs(n2top, n2top1), dz);
+    }
+    for (int k = 0; k < nk; ++k) {
+        const long o = (long)k * ld + col;
+        const double a0 = o2u[o], b0 = o1u[o], c0 = heu[o];
+        const double an = xa(xm(ds2, xa(o2_nm[o], a0)), xm(ds, o2[o]));
+        const double bn = xa(xm(ds2, xa(o1_nm[o], b0)), xm(ds, o1[o]));
+        const double cn = xa(xm(ds2, xa(he_nm[o], c0)), xm(ds, he[o]));
+        double n2 = xs(xs(xs(1.0, a0), b0), c0);
+        if (extrap && k > ktop) n2 = xd(exp(xa(n2top, xm(dn2dz, xs(zpmid[k], zmtop)))), xnmbar[o]);
+        const double n2nm = xs(xs(xs(1.0, an), bn), cn);
+        double a = fmax(a0, small), b = fmax(b0, small), c = fmax(c0, small), d = fmax(n2, small);
+        double s = xa(xa(xa(a, b), c), d);
+        o2u[o] = xd(a, s);
+        o1u[o] = xd(b, s);
+        heu[o] = xd(c, s);
+        a = fmax(an, small);
+        b = fmax(bn, small);
+        c = fmax(cn, small);
+        d = fmax(n2nm, small);
+        s = xa(xa(xa(a, b), c), d);
+        o2n[o] = xd(a, s);
+        o1n[o] = xd(b, s);
+        hen[o] = xd(c, s);
+    }
+}
+
+cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, double dz, double dtsmooth,
+                                double dtsmooth_div2, int nk, int ncol, long ld, double *const *upd6, cudaStream_t st)
+{
+    if (ncol <= 0) return cudaSuccess;
+    const int T = 128;
+    k_comp_post_ng<<<(ncol + T - 1) / T, T, 0, st>>>(in7[0], in7[1], in7[2], in7[3], in7[4], in7[5], in7[6], zpmid,
+                                                     dz, dtsmooth, dtsmooth_div2, nk, ncol, ld, upd6[0], upd6[1],
+                                                     upd6[2], upd6[3], upd6[4], upd6[5]);
+    return cudaGetLastError();
+}
 }  // namespace tg

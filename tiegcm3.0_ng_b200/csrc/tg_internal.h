@@ -42,6 +42,7 @@ struct SegTable {
     int ntiles;
     int k2max;        // largest k2 of any segment (sizes per-thread scratch)
     Seg one;
+    int hints;        // L2 policy hints: inputs evict-first, sweep scratch evict-last
 };
 
 struct Refine {
@@ -132,6 +133,18 @@ typedef tg_minor_fields MinorFields;
 typedef tg_minor_consts MinorConsts;
 cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *out, int nk, int ncol, long ld,
                             double *sys_out, unsigned *status, cudaStream_t st);
+
+typedef tg_comp_fields CompFields;
+typedef tg_comp_consts CompConsts;
+cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out, double *scratch, int nk, int ncol,
+                           long ld, double *sys_out, unsigned *status, cudaStream_t st);
+cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, double dz, double dtsmooth,
+                                double dtsmooth_div2, int nk, int ncol, long ld, double *const *upd6,
+                                cudaStream_t st);
+
+// L2 cache-policy hints of the bulk-copy ring kernels (tg_set_cache_hints).
+int cache_hints();
+void set_cache_hints(int on);
 
 // Records the message tg_last_error() returns on this thread.
 void record_error(const char *msg);

@@ -13,6 +13,7 @@
 // src/matutil.F90:25-27,63-71,116).
 #include <cfloat>
 #include <cstdio>
+#include <atomic>
 #include <mutex>
 
 #include "tg_internal.h"
@@ -166,6 +167,40 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
                  "l"(src), "r"(bytes), "r"(smem_addr(bar))
                  : "memory");
 }
+// L2 eviction-priority policies (createpolicy): the coefficient streams are
+// read once (evict-first); the sweep's own scratch (w2, and w3 parked in x)
+// is re-read by the back sweep and should stay in L2 (evict-last).  With
+// hints off both are evict-normal.
+__device__ __forceinline__ unsigned long long l2_policy(int hints, bool keep)
+{
+    unsigned long long p;
+    if (!hints)
+        asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    else if (keep)
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ void bulk_load_hint(void *dst, const void *src, uint32_t bytes, unsigned long long *bar,
+                                               unsigned long long pol)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
+        : "memory");
+}
+__device__ __forceinline__ void st_hint(double *p, double v, unsigned long long pol)
+{
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ double ld_hint(const double *p, unsigned long long pol)
+{
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol) : "memory");
+    return v;
+}
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity)
 {
     uint32_t ok;
@@ -191,6 +226,7 @@ template <int NE, int D>
 struct Ring {
     double *buf;                 // D * NE * 32 doubles
     unsigned long long *bar;     // D mbarriers
+    unsigned long long pol;      // L2 policy of the fills
     __device__ __forceinline__ void init(int lane)
     {
         if (lane == 0) {
@@ -206,7 +242,7 @@ struct Ring {
         const int st = (int)(q % D);
         if (lane == 0) mbar_expect(&bar[st], NE * 256u);
         __syncwarp();
-        if (lane < NE) bulk_load(buf + (st * NE + lane) * 32, src_e, 256u, &bar[st]);
+        if (lane < NE) bulk_load_hint(buf + (st * NE + lane) * 32, src_e, 256u, &bar[st], pol);
     }
     __device__ __forceinline__ bool wait(unsigned q) { return mbar_wait_warp(&bar[q % D], (q / D) & 1u); }
     __device__ __forceinline__ double at(unsigned q, int e, int lane) const
@@ -400,7 +436,8 @@ __global__ void __launch_bounds__(256) k_scalar_f64_ring(SegTable tab, double *s
     // each warp of the CTA is independent: its own ring, barriers and tiles
     const long per_warp = (long)D * NE * 32 + (W2G ? 0 : (long)32 * (tab.k2max > 1 ? tab.k2max - 1 : 1));
     double *mine = smem_r + warp * per_warp;
-    Ring<NE, D> ring{mine, bars + warp * D};
+    Ring<NE, D> ring{mine, bars + warp * D, l2_policy(tab.hints, false)};
+    const unsigned long long keep = l2_policy(tab.hints, true);
     const long ws = W2G ? (long)gridDim.x * blockDim.x : 32;
     double *w2s = W2G ? scratch + (long)blockIdx.x * blockDim.x + threadIdx.x : mine + D * NE * 32 + lane;
     ring.init(lane);
@@ -436,14 +473,15 @@ __global__ void __launch_bounds__(256) k_scalar_f64_ring(SegTable tab, double *s
                     w3 = qdiv(fk, w1, y1);
                 } else {
                     const double w2 = qdiv(cprev, w1, y1);
-                    w2s[(k - 1) * ws] = w2;
+                    if (W2G) st_hint(&w2s[(k - 1) * ws], w2, keep);
+                    else w2s[(k - 1) * ws] = w2;
                     w1 = xsub(bk, xmul(ak, w2));
                     y1 = __drcp_rn(w1);
                     w3 = qdiv(xsub(fk, xmul(ak, w3)), w1, y1);
                 }
                 ok = ok && finite_nz(w1);
                 cprev = ck;
-                px[k * ld] = w3;
+                st_hint(&px[k * ld], w3, keep);
             }
         }
         q += k2;
@@ -937,7 +975,8 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
     __shared__ __align__(8) unsigned long long bars[8 * D];
     extern __shared__ __align__(128) double smem_b[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    Ring<NE, D> ring{smem_b + (long)warp * D * NE * 32, bars + warp * D};
+    Ring<NE, D> ring{smem_b + (long)warp * D * NE * 32, bars + warp * D, l2_policy(tab.hints, false)};
+    const unsigned long long keep = l2_policy(tab.hints, true);
     ring.init(lane);
     const long gs = (long)gridDim.x * blockDim.x;
     double *gam = scratch + (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1020,7 +1059,7 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
 #pragma unroll
                 for (int m = 1; m < B; ++m) tv = xadd(tv, xmul(W[i + B * m], v[m]));
                 z[i] = tv;
-                pU[((long)k * B + i) * ld] = tv;
+                st_hint(&pU[((long)k * B + i) * ld], tv, keep);
             }
             if (k < k2 - 1) {
 #pragma unroll
@@ -1031,7 +1070,7 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
 #pragma unroll
                         for (int n = 1; n < B; ++n) g = xadd(g, xmul(W[i + B * n], R[n + B * m]));
                         G[i + B * m] = g;
-                        gam[((long)k * BB + i + B * m) * gs] = g;
+                        st_hint(&gam[((long)k * BB + i + B * m) * gs], g, keep);
                     }
             }
         }
@@ -1776,14 +1815,20 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     return cudaSuccess;
 }
 
+static std::atomic<int> g_cache_hints{1};
+int cache_hints() { return g_cache_hints.load(); }
+void set_cache_hints(int on) { g_cache_hints.store(on < 0 ? 1 : (on ? 1 : 0)); }
+
 cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, Refine rf, double *scratch,
                           unsigned *status, unsigned long long *hist, cudaStream_t st)
 {
     if (tab.ntiles <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     if (precision == TG_PREC_F64 && sh.stages > 0) {
+        SegTable t = tab;
+        t.hints = cache_hints();
         e = with_scalar_ring(sh.stages, sh.w2g, [&](auto k) {
-            k<<<sh.blocks, sh.threads, sh.smem, st>>>(tab, scratch, status);
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, scratch, status);
             return cudaSuccess;
         });
     } else if (precision == TG_PREC_F64 && sh.w2g) {
@@ -1811,8 +1856,10 @@ cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape 
 {
     if (tab.ntiles <= 0) return cudaSuccess;
     if (precision == TG_PREC_F64 && sh.stages > 0) {
+        SegTable t = tab;
+        t.hints = cache_hints();
         cudaError_t e = with_block_ring(B, sh.stages, [&](auto k) {
-            k<<<sh.blocks, sh.threads, sh.smem, st>>>(tab, scratch, status);
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, scratch, status);
             return cudaSuccess;
         });
         if (e != cudaSuccess) return e;

@@ -404,3 +404,60 @@ def comp_post_inputs(nk, ncol, dz, seed, zibot=-7.0):
         f[k] = np.asfortranarray(f[k])
     f["zpmid"] = zibot + (np.arange(nk) + 0.5) * dz
     return f, dict(dz=dz, dtsmooth=0.95, dtsmooth_div2=0.5 * (1.0 - 0.95))
+
+
+SETTEI_FIELDS = ("tn", "o2", "o1", "he", "n2", "ne", "te", "ti", "op", "o2p", "nplus", "n2p", "nop", "xnmbar",
+                 "xnmbari", "scht", "schti", "qji_ti", "qop2p", "qop2d", "qo2p", "qop", "qn2p", "qnp", "qnop",
+                 "Q1", "Q2")
+SETTEI_2D = ("t_lbc", "chi", "rlatm", "dipmag", "qteaur")
+
+
+def settei_inputs(nk, ncol, dz, seed, et=0, electron_heating=0):
+    """Seeded fields of the settei_ng column step (CGS): neutral, electron and
+    ion temperatures (Te >= Tn, a few columns with Te = Tn), species mixing
+    ratios, ion and electron densities, ionisation rates and the solar zenith
+    and magnetic latitude / dip angles spanning the branches of the
+    upper-boundary flux.  Returns (fields dict, constants dict, qtotal)."""
+    rng = _rng(seed)
+    z = np.linspace(0.0, 1.0, nk)[:, None]
+    U = lambda lo, hi, shape=(nk, ncol): rng.uniform(lo, hi, size=shape)
+    f = {}
+    tn = 200.0 + 800.0 * z ** 0.7 * U(0.9, 1.1)
+    f["tn"] = tn
+    te = tn + 2500.0 * z ** 1.5 * U(0.5, 1.5)
+    te[:, :3] = tn[:, :3]                     # Te = Tn columns take the |Te-Tn| < del branch
+    f["te"] = te
+    f["ti"] = tn + 0.5 * (te - tn) * U(0.5, 1.0)
+    f["o2"] = (0.22 - 0.21 * z) * U(0.9, 1.1)
+    f["o1"] = (0.05 + 0.75 * z) * U(0.9, 1.1)
+    f["he"] = (1e-5 + 0.05 * z ** 2) * U(0.9, 1.1)
+    f["n2"] = np.maximum(1.0 - f["o2"] - f["o1"] - f["he"], 0.0)
+    f["xnmbar"] = 1e13 * np.exp(-10.0 * z) * U(0.5, 1.5)
+    f["xnmbari"] = f["xnmbar"] * U(0.95, 1.05)
+    f["ne"] = 1e3 + 1e6 * np.exp(-((z - 0.6) / 0.25) ** 2) * U(0.5, 1.5)
+    f["op"] = 0.8 * f["ne"] * z * U(0.9, 1.1)
+    f["o2p"] = 0.1 * f["ne"] * (1.0 - z) * U(0.9, 1.1)
+    f["nplus"] = 0.02 * f["ne"] * U(0.5, 1.5)
+    f["n2p"] = 0.01 * f["ne"] * U(0.5, 1.5)
+    f["nop"] = 0.1 * f["ne"] * (1.0 - z) * U(0.9, 1.1)
+    f["scht"] = 1e6 + 5e6 * z * U(0.9, 1.1)
+    f["schti"] = f["scht"] * U(0.95, 1.05)
+    f["qji_ti"] = U(0.0, 1e-3)
+    for k in ("qop2p", "qop2d", "qo2p", "qop", "qn2p", "qnp", "qnop"):
+        f[k] = U(0.0, 1.0) * np.exp(-((z - 0.5) / 0.3) ** 2)
+    f["Q1"] = U(0.0, 1e-11)
+    f["Q2"] = U(-2e-12, 1e-11)
+    for k in SETTEI_FIELDS:
+        f[k] = np.asfortranarray(f[k])
+    f["t_lbc"] = rng.uniform(190.0, 210.0, ncol)
+    f["chi"] = rng.uniform(0.0, np.pi, ncol)               # crosses 80-100 deg and pi/2
+    f["rlatm"] = rng.uniform(-np.pi / 2, np.pi / 2, ncol)  # all three branches of a
+    f["dipmag"] = rng.uniform(-np.pi / 2, np.pi / 2, ncol)
+    f["qteaur"] = rng.uniform(-1e8, 0.0, ncol)
+    b = np.eye(3) * rng.uniform(0.6, 0.9, 3) + rng.uniform(-0.05, 0.05, (3, 3))
+    c = dict(f107=rng.uniform(70.0, 300.0), dipmin=0.17, dz=dz, evergs=1.602e-12, avo=6.023e23, rmass_o1=16.0,
+             rmassinv_o2=1.0 / 32.0, rmassinv_o1=1.0 / 16.0, rmassinv_he=1.0 / 4.0, rmassinv_n2=1.0 / 28.0,
+             rmassinv_n4s=1.0 / 14.0, rmassinv_no=1.0 / 30.0, b=b, fb=rng.uniform(0.0, 0.02, 3), et=et,
+             electron_heating=electron_heating)
+    qtotal = np.asfortranarray(rng.uniform(0.0, 5e-2, (nk, ncol)))
+    return f, c, qtotal
