@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--profile", default=None,
                    help="run only one kind's plan for a profiler: KIND:PREC[:VARIANT], KIND scalar|block, "
                         "PREC f64|refine, VARIANT reg:CPB:CPT[:PF], regg:CPB:1[:PF], ring[g]:DEPTH[:WARPS] "
-                        "(default: library default); or 'dt' / 'minor' / 'comp' for the fused assembly+solve kernels")
+                        "(default: library default); or 'dt' / 'minor' / 'comp' / 'settei' for the fused assembly+solve kernels")
     p.add_argument("--skip-assembly", action="store_true")
     return p.parse_args()
 
@@ -232,9 +232,14 @@ def assembly_setup(pkg, wl, which, dev, replicas=ASSEMBLY_REPLICAS):
     elif which == "minor":
         F, C = pkg.synth.minor_inputs(nk, ncol, dz, 103)
         one_d, n2d, n3d = ("expz", "difk"), len(pkg.synth.MINOR_2D), len(pkg.synth.MINOR_FIELDS)
-    else:
+    elif which == "comp":
         F, C = pkg.synth.comp_inputs(nk, ncol, dz, 107)
         one_d, n2d, n3d = ("expz", "difk"), len(pkg.synth.COMP_2D), len(pkg.synth.COMP_FIELDS) + 12
+        nout = 3
+    else:
+        F, C, qt = pkg.synth.settei_inputs(nk, ncol, dz, 109)
+        # 27 fields and qtotal read; te, ti and qtotal written
+        one_d, n2d, n3d = (), len(pkg.synth.SETTEI_2D), len(pkg.synth.SETTEI_FIELDS) + 1
         nout = 3
     ld = pkg.batch.pad_ld(ncol)
     d = {}
@@ -254,9 +259,15 @@ def assembly_setup(pkg, wl, which, dev, replicas=ASSEMBLY_REPLICAS):
             t[:ncol] = torch.from_numpy(v)
             d[k] = t
     out = torch.zeros((nout, nk, ld), dtype=torch.float64, device=dev)
-    fn = {"dt": pkg.dt_ng_dev, "minor": pkg.minor_ng_dev, "comp": pkg.comp_ng_dev}[which]
     # 3-D fields read + the solution written, 2-D and 1-D inputs read
-    nbytes = 8 * ((n3d + nout) * nk * ncol + n2d * ncol + 2 * nk)
+    nbytes = 8 * ((n3d + nout) * nk * ncol + n2d * ncol + len(one_d) * nk)
+    if which == "settei":
+        qtd = pkg.batch.level_scalar(qt, ld, dev)
+
+        def launch(stream):
+            pkg.settei_ng_dev(d, C, out[0], out[1], qtd, nk, ncol, ld, stream=stream)
+        return launch, ncol, nbytes
+    fn = {"dt": pkg.dt_ng_dev, "minor": pkg.minor_ng_dev, "comp": pkg.comp_ng_dev}[which]
 
     def launch(stream):
         fn(d, C, out, nk, ncol, ld, stream=stream)
@@ -267,7 +278,7 @@ def run_profile(args):
     """Executes one kind's plan --warmup + --steps times (for ncu captures)."""
     import torch
     pkg = ge.load_package()
-    if args.profile in ("dt", "minor", "comp"):
+    if args.profile in ("dt", "minor", "comp", "settei"):
         wl = pkg.synth.workload(args.config)
         launch, ncol, nbytes = assembly_setup(pkg, wl, args.profile, "cuda")
         stream = torch.cuda.Stream()
@@ -426,7 +437,8 @@ def main():
     assembly = None
     if not args.skip_assembly:
         assembly = {}
-        for which, kern in (("dt", "k_dt_ng"), ("minor", "k_minor_ng"), ("comp", "k_comp_ng")):
+        for which, kern in (("dt", "k_dt_ng"), ("minor", "k_minor_ng"), ("comp", "k_comp_ng"),
+                            ("settei", "k_settei_ng")):
             launch, ncol_a, nbytes = assembly_setup(pkg, wl, which, dev)
             for _ in range(args.warmup):
                 launch(stream)

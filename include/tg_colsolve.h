@@ -277,6 +277,34 @@ int tg_comp_post_ng(const double *o2, const double *o1, const double *he, const 
                     double dtsmooth_div2, int nk, int ncol, double *o2_upd, double *o1_upd, double *he_upd,
                     double *o2nm_upd, double *o1nm_upd, double *henm_upd);
 
+/* settei_ng's electron and ion temperature step (src/settei_ng.F90:60-261):
+ * the whole routine is column-local, so it is one fused kernel: the heat-flux
+ * boundary fe, thermal conductivity, the conduction rows in Te^3.5, heating,
+ * cooling and exchange rates, the solve of rows 1..nk-1, Te = x^(2/7) with the
+ * top level, and Ti.  qtotal is read and updated (qtotal += q_eni at the
+ * interfaces, :248-254).  3-D fields (nk, ncol), 2-D (ncol).  b, fb: the lbc
+ * module's lower-boundary relation; et and electron_heating: the input
+ * switches of the reference; dipmin the grid's minimum dip. */
+typedef struct {
+    const double *tn, *o2, *o1, *he, *n2, *ne, *te, *ti, *op, *o2p, *nplus, *n2p, *nop, *xnmbar, *xnmbari, *scht;
+    const double *schti, *qji_ti, *qop2p, *qop2d, *qo2p, *qop, *qn2p, *qnp, *qnop, *Q1, *Q2;
+    const double *t_lbc, *chi, *rlatm, *dipmag, *qteaur;
+} tg_settei_fields;
+
+typedef struct {
+    double f107, dipmin, dz, evergs, avo, rmass_o1;
+    double rmassinv_o2, rmassinv_o1, rmassinv_he, rmassinv_n2, rmassinv_n4s, rmassinv_no;
+    double b[9], fb[3];
+    int et, electron_heating;
+} tg_settei_consts;
+
+int tg_settei_ng(const tg_settei_fields *F, const tg_settei_consts *C, double *te_out, double *ti_out,
+                 double *qtotal, int nk, int ncol);
+/* Device form: level-major (k*ld + col) arrays; system_out (may be NULL)
+ * 4 slabs (p, q, r, rhs) of nk*ld, rows 1..nk-1. */
+int tg_settei_ng_dev(const tg_settei_fields *F, const tg_settei_consts *C, double *te_out, double *ti_out,
+                     double *qtotal, int nk, int ncol, long ld, double *system_out, int *status_dev, void *stream);
+
 /* ---- batched, GPU-resident plans ---------------------------------------------
  * A plan solves many independent systems ("segments": any mix of grids, nest
  * levels, sub-steps and species) in one persistent launch per system kind,

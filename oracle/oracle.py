@@ -316,3 +316,43 @@ def settei_ng(fields, consts, qtotal, with_system=False):
     L.oracle_settei_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, _p(te_out), _p(ti_out), _p(qt),
                        *[_p(s) for s in sysarr])
     return ((te_out, ti_out, qt), tuple(sysarr)) if with_system else (te_out, ti_out, qt)
+
+
+OPLUS_FIELD_ORDER = ("tn", "te", "ti", "o2", "o1", "n2", "he", "n2d", "ne", "u", "v", "w", "wi", "xnmbar", "scht",
+                     "qop2p", "qop2d", "qop", "rk1", "rk2", "rk19", "rk20", "rk25", "op", "optm1_smooth2",
+                     "explicit_h", "bdotdh_djbz", "bx", "by", "bz", "dvb", "rlatm", "chi", "dipmag", "sndec", "csdec",
+                     "zpint")
+OPLUS_CONST_ORDER = ("rmass_op", "gask", "grav", "re", "rmassinv_o2", "rmassinv_o1", "rmassinv_n2", "rmassinv_n2d",
+                     "rmassinv_he", "rk10", "rk16", "rk17", "rk18", "rk21", "rk22", "rk23", "rk24", "rk26", "rk27",
+                     "colfac", "opdiffcap", "dtx2inv", "dz", "dlev")
+
+
+class OplusFields(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in OPLUS_FIELD_ORDER]
+
+
+class OplusConsts(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in OPLUS_CONST_ORDER] + [("nstep_sub", ctypes.c_int)]
+
+
+def oplus_consts(c, cls=OplusConsts):
+    return cls(*[float(c[k]) for k in OPLUS_CONST_ORDER], int(c["nstep_sub"]))
+
+
+def oplus_ng(fields, consts, with_system=False):
+    """oplus_ng vertical column step (src/oplus_ng.F90:125-307); returns
+    (opout, xiop2p, xiop2d, Fe, Fn) and, if with_system, (p, q, r, explicit)."""
+    L = lib()
+    if not hasattr(L, "_oplus_bound"):
+        L.oracle_oplus_ng.argtypes = [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), ctypes.c_int,
+                                      ctypes.c_long] + [ctypes.c_void_p] * 9
+        L.oracle_oplus_ng.restype = None
+        L._oplus_bound = True
+    arrs = {k: _fcopy(fields[k]) for k in OPLUS_FIELD_ORDER}
+    nk, ncol = arrs["tn"].shape[0], arrs["tn"].size // arrs["tn"].shape[0]
+    F = OplusFields(*[arrs[k].ctypes.data for k in OPLUS_FIELD_ORDER])
+    C = oplus_consts(consts)
+    outs = [np.zeros((nk, ncol), order="F") for _ in range(5)]
+    sysarr = [np.zeros((nk, ncol), order="F") for _ in range(4)] if with_system else [None] * 4
+    L.oracle_oplus_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(a) for a in outs], *[_p(s) for s in sysarr])
+    return (tuple(outs), tuple(sysarr)) if with_system else tuple(outs)

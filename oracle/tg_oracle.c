@@ -1165,3 +1165,191 @@ ORACLE_API void oracle_settei_ng(const oracle_settei_fields *F, const oracle_set
     }
     free(w);
 }
+
+/* ------------------------------------------------------------------------ */
+/* oplus_ng O+ column step, vertical part (src/oplus_ng.F90:125-303).       */
+/* The terms that need horizontal derivatives are inputs, computed by the   */
+/* host model as the reference does: explicit_h = -explic*diffexp +         */
+/* vdotn_h + bdotdh_bvel (:178-207), bdotdh_djbz = bdotdh(dj*bz) (:234),    */
+/* dvb = (div b + 2 bz)/re before its division by bz (:101-107), and        */
+/* optm1_smooth2 = smooth_ng(optm1) (:162).  Fields (nk, ncol); 2-D (ncol); */
+/* zpint (nk).  Outputs: opout rows 1..nk (the top from :307), xiop2p,      */
+/* xiop2d (:285-288); Fe, Fn (:164-169) and the system p,q,r,explicit rows   */
+/* 1..nk-1 may be NULL.  opout is before the lateral-boundary overwrite,    */
+/* the time filter and the max(.,0) of :326-331, which the caller applies.  */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    const double *tn, *te, *ti, *o2, *o1, *n2, *he, *n2d, *ne, *u, *v, *w, *wi, *xnmbar, *scht, *qop2p, *qop2d,
+        *qop, *rk1, *rk2, *rk19, *rk20, *rk25, *op, *optm1_smooth2, *explicit_h, *bdotdh_djbz;
+    const double *bx, *by, *bz, *dvb, *rlatm, *chi, *dipmag, *sndec, *csdec;
+    const double *zpint;
+} oracle_oplus_fields;
+
+typedef struct {
+    double rmass_op, gask, grav, re, rmassinv_o2, rmassinv_o1, rmassinv_n2, rmassinv_n2d, rmassinv_he;
+    double rk10, rk16, rk17, rk18, rk21, rk22, rk23, rk24, rk26, rk27;
+    double colfac, opdiffcap, dtx2inv, dz, dlev;
+    int nstep_sub;
+} oracle_oplus_consts;
+
+ORACLE_API void oracle_oplus_ng(const oracle_oplus_fields *F, const oracle_oplus_consts *C, int nk, long ncol,
+                                double *opout, double *xiop2p, double *xiop2d, double *Fe, double *Fn,
+                                double *p_out, double *q_out, double *r_out, double *f_out)
+{
+    const double explic = 1., phid = 2.0e8, phin = -2.0e8, ppolar = 0.;
+    const double pi = 4.0 * atan(1.0), rtd = 180.0 / pi, dz = C->dz;
+    double *w = (double *)malloc(sizeof(double) * 24 * (size_t)nk);
+    long col;
+    (void)explic;
+    if (nk < 3) { free(w); return; }
+    for (col = 0; col < ncol; ++col) {
+        const size_t o = (size_t)nk * col;
+#define FL(name) (F->name + o)
+        const double *tn = FL(tn), *te = FL(te), *ti = FL(ti), *o2 = FL(o2), *o1 = FL(o1), *n2 = FL(n2),
+                     *he = FL(he), *n2d = FL(n2d), *ne = FL(ne), *uu = FL(u), *vv = FL(v), *ww = FL(w),
+                     *wiw = FL(wi), *xnmbar = FL(xnmbar), *hj = FL(scht), *qop = FL(qop), *op = FL(op);
+        double *dj = w, *bdotu = w + nk, *hdz = w + 2 * nk, *hdzi = w + 3 * nk, *tp1 = w + 4 * nk,
+               *tph1 = w + 5 * nk, *tph0 = w + 6 * nk, *djint = w + 7 * nk, *hdzm = w + 8 * nk, *hdzp = w + 9 * nk,
+               *p = w + 10 * nk, *q = w + 11 * nk, *r = w + 12 * nk, *ex = w + 13 * nk, *ol = w + 14 * nk,
+               *wni = w + 15 * nk, *wii = w + 16 * nk, *vni = w + 17 * nk, *tpop = w + 18 * nk, *ws = w + 19 * nk,
+               *x = w + 22 * nk;
+        const double bx = F->bx[col], by = F->by[col], bz = F->bz[col];
+        int k;
+        /* oplus_flux (:88-99) */
+        const double arl = fabs(F->rlatm[col]), chi = F->chi[col];
+        double a = 0., opflux;
+        if (arl >= pi / 4.5) a = 1.;
+        if (arl < pi / 4.5 && arl > pi / 18) a = .5 * (1. + cos(arl * 6. - pi * 4. / 3.));
+        if (arl <= pi / 18) a = 0.;
+        {
+            const double fed = phid * a, fen = phin * a;
+            opflux = chi >= 0.5 * pi ? fen : fed;
+            if ((chi * rtd - 80.) * (chi * rtd - 100.) < 0.)
+                opflux = .5 * (fed + fen) + .5 * (fed - fen) * cos(pi * (chi * rtd - 80.) / 20.);
+            if (arl >= pi / 3.) opflux = opflux + ppolar;
+        }
+        /* interface winds (:112-123) */
+        for (k = 0; k < nk - 1; ++k) {
+            wni[k] = .5 * (ww[k] + ww[k + 1]);
+            wii[k] = .5 * (wiw[k] + wiw[k + 1]);
+        }
+        wni[nk - 1] = 1.5 * ww[nk - 1] - .5 * ww[nk - 2];
+        wii[nk - 1] = 1.5 * wiw[nk - 1] - .5 * wiw[nk - 2];
+        /* rrk: collision frequency and diffusion coefficient (:125-135) */
+        for (k = 0; k < nk; ++k) {
+            const double tr = 0.5 * (tn[k] + ti[k]);
+            const double lg = 1. - 0.064 * log10(tr);
+            vni[k] = 18.1 * o2[k] * C->rmassinv_o2 + o1[k] * C->rmassinv_o1 * sqrt(tr) * (lg * lg) * C->colfac +
+                     3.6 * he[k] * C->rmassinv_he + 18.6 * n2[k] * C->rmassinv_n2;
+            dj[k] = 1.42E17 / (xnmbar[k] * vni[k]);
+            vni[k] = 16 * 3.53E-11 * vni[k];
+            if (!(fabs(C->opdiffcap - 0.) < 1e-9)) {
+                const double cap = C->opdiffcap / (1 + pow(2., F->zpint[k] - 6));
+                dj[k] = dj[k] < cap ? dj[k] : cap;
+            }
+            bdotu[k] = bx * uu[k] + by * vv[k] + hj[k] * bz * wni[k];
+            tpop[k] = (te[k] + ti[k]) * op[k];
+        }
+        /* Fe, Fn (:151-169) */
+        if (Fe) {
+            const double sncs = sin(F->dipmag[col]) * cos(F->dipmag[col]);
+            for (k = 0; k < nk; ++k) {
+                double d;
+                if (k == 0) d = tpop[1] - tpop[0];
+                else if (k == nk - 1) d = tpop[nk - 1] - tpop[nk - 2];
+                else if (k == nk - 2) d = tpop[nk - 2] - tpop[nk - 3];
+                else d = (tpop[k + 1] - tpop[k - 1]) / 2.;
+                const double diffj = 1. / (hj[k] * C->dlev) * d + C->rmass_op * C->grav / C->gask * op[k];
+                const double wd = vni[k] * diffj * dj[k];
+                Fe[o + k] = wd * sncs * F->sndec[col];
+                Fn[o + k] = wd * sncs * F->csdec[col];
+            }
+        }
+        /* vertical coefficients (:209-262) */
+        const double dvbz = F->dvb[col] / bz;
+        const double gmr = C->grav * C->rmass_op / (2. * C->gask);
+        for (k = 0; k < nk; ++k) {
+            hdz[k] = 1. / (hj[k] * dz);
+            tp1[k] = 0.5 * (ti[k] + te[k]);
+        }
+        for (k = 1; k < nk - 1; ++k) hdzi[k] = 0.5 * (hdz[k - 1] + hdz[k]);
+        hdzi[0] = 1.5 * hdz[0] - 0.5 * hdz[1];
+        hdzi[nk - 1] = 1.5 * hdz[nk - 2] - 0.5 * hdz[nk - 3];
+        for (k = 0; k < nk; ++k) tph1[k] = 2. * tp1[k] * hdzi[k] + gmr;
+        for (k = 1; k < nk; ++k) tph0[k] = 2. * tp1[k - 1] * hdzi[k] - gmr;
+        tph1[nk - 1] = 2. * (2. * tp1[nk - 2] - tp1[nk - 3]) * hdzi[nk - 1] + gmr;
+        tph0[0] = 2. * (2. * tp1[0] - tp1[1]) * hdzi[0] - gmr;
+        for (k = 1; k < nk - 1; ++k) djint[k] = 0.5 * (dj[k - 1] + dj[k]);
+        djint[0] = 1.5 * dj[0] - 0.5 * dj[1];
+        djint[nk - 1] = 1.5 * dj[nk - 2] - 0.5 * dj[nk - 3];
+        for (k = 0; k < nk; ++k) {
+            const double divbz = dvbz + F->bdotdh_djbz[o + k] / (dj[k] * (bz * bz));
+            hdzm[k] = (hdz[k] - 0.5 * divbz) * (bz * bz);
+            hdzp[k] = (hdz[k] + 0.5 * divbz) * (bz * bz);
+            ex[k] = F->explicit_h[o + k] - F->optm1_smooth2[o + k] * C->dtx2inv * C->nstep_sub;
+        }
+        for (k = 0; k < nk - 1; ++k) {
+            const double diffp = hdzm[k] * djint[k] * tph0[k];
+            const double diffq = -(hdzp[k] * djint[k + 1] * tph0[k + 1] + hdzm[k] * djint[k] * tph1[k]);
+            const double diffr = hdzp[k] * djint[k + 1] * tph1[k + 1];
+            const double driftp = wii[k] * 0.5 * hdz[k], driftq = -wii[k] * 6. / C->re, driftr = -wii[k] * 0.5 * hdz[k];
+            double windp, windq, windr;
+            if (k == 0) windp = bz * (2. * bdotu[0] - bdotu[1]) * 0.5 * hdz[0];
+            else windp = bz * bdotu[k - 1] * 0.5 * hdz[k];
+            windq = -bdotu[k] * dvbz * bz;
+            if (k == nk - 2) windr = bz * (2. * bdotu[nk - 2] - bdotu[nk - 3]) * 0.5 * hdz[nk - 2];
+            else windr = -bz * bdotu[k + 1] * 0.5 * hdz[k];
+            p[k] = diffp + driftp + windp;
+            q[k] = diffq + driftq + windq - C->dtx2inv * C->nstep_sub;
+            r[k] = diffr + driftr + windr;
+        }
+        {
+            const double ubcb = -(bz * bz) * djint[nk - 1] * tph0[nk - 1];
+            const double ubca = -(bz * bz) * djint[nk - 1] * tph1[nk - 1];
+            q[nk - 2] = q[nk - 2] + ubcb / ubca * r[nk - 2];
+            ex[nk - 2] = ex[nk - 2] - opflux * r[nk - 2] / ubca;
+            r[nk - 2] = 0.;
+        }
+        /* chemistry (:285-299) */
+        for (k = 0; k < nk; ++k) {
+            const double q2pi = k < nk - 1 ? .5 * (F->qop2p[o + k] + F->qop2p[o + k + 1])
+                                           : 1.5 * F->qop2p[o + nk - 1] - .5 * F->qop2p[o + nk - 2];
+            const double q2di = k < nk - 1 ? .5 * (F->qop2d[o + k] + F->qop2d[o + k + 1])
+                                           : 1.5 * F->qop2d[o + nk - 1] - .5 * F->qop2d[o + nk - 2];
+            const double qopi = k < nk - 1 ? .5 * (qop[k] + qop[k + 1]) : 1.5 * qop[nk - 1] - .5 * qop[nk - 2];
+            const double rk19 = F->rk19[o + k], rk20 = F->rk20[o + k], rk25 = F->rk25[o + k];
+            const double x2p = q2pi / (xnmbar[k] * ((C->rk16 + C->rk17) * n2[k] * C->rmassinv_n2 +
+                                                   C->rk18 * o1[k] * C->rmassinv_o1) +
+                                       (rk19 + rk20) * ne[k] + C->rk21 + C->rk22);
+            const double x2d = (q2di + (rk20 * ne[k] + C->rk22) * x2p) /
+                               (xnmbar[k] * (C->rk23 * n2[k] * C->rmassinv_n2 + C->rk24 * o1[k] * C->rmassinv_o1 +
+                                             C->rk26 * o2[k] * C->rmassinv_o2) +
+                                rk25 * ne[k] + C->rk27);
+            xiop2p[o + k] = x2p;
+            xiop2d[o + k] = x2d;
+            ol[k] = xnmbar[k] * (F->rk1[o + k] * o2[k] * C->rmassinv_o2 + F->rk2[o + k] * n2[k] * C->rmassinv_n2 +
+                                 C->rk10 * n2d[k] * C->rmassinv_n2d);
+            if (k < nk - 1) q[k] = q[k] - ol[k];
+            const double prod = qopi + (rk19 * ne[k] + C->rk21) * x2p + (rk25 * ne[k] + C->rk27) * x2d +
+                                (C->rk18 * x2p + C->rk24 * x2d) * o1[k] * C->rmassinv_o1 * xnmbar[k];
+            ex[k] = ex[k] - prod;
+        }
+        /* lower boundary (:301-303) */
+        q[0] = q[0] - p[0];
+        ex[0] = ex[0] - 2. * p[0] * qop[0] / (1.5 * ol[0] - 0.5 * ol[1]);
+        p[0] = 0.;
+        if (p_out)
+            for (k = 0; k < nk - 1; ++k) {
+                p_out[o + k] = p[k];
+                q_out[o + k] = q[k];
+                r_out[o + k] = r[k];
+                f_out[o + k] = ex[k];
+            }
+        /* solve rows 1..nk-1 and the top level (:305-307) */
+        thomas_column(p, q, r, ex, x, nk - 1, ws);
+        for (k = 0; k < nk - 1; ++k) opout[o + k] = x[k];
+        opout[o + nk - 1] = x[nk - 2] * x[nk - 2] / x[nk - 3];
+#undef FL
+    }
+    free(w);
+}

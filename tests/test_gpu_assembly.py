@@ -156,3 +156,50 @@ def test_comp_post_ng_host(cuda, pkg, orc, nk, dz, ncol):
     ref = orc.comp_post_ng(F, C)
     for got, want in zip(upd + nm, ref):
         assert _rel(got, want) <= 1e-13
+
+
+# settei_ng: device exp/log/pow/sin/cos differ from the C library's in the
+# last bits; Te, Ti and qtotal agree with the oracle to this relative level.
+SETTEI_TOL = 1e-11
+
+
+@pytest.mark.parametrize("nk,dz,ncol,et,eh", [(57, 0.25, 3001, 0, 0), (29, 0.5, 2592, 1, 6), (113, 0.125, 400, 0, 6),
+                                              (3, 0.5, 33, 1, 0)])
+def test_settei_ng_host(cuda, pkg, orc, nk, dz, ncol, et, eh):
+    F, C, qt = pkg.synth.settei_inputs(nk, ncol, dz, 31 + nk, et=et, electron_heating=eh)
+    te, ti = np.zeros((nk, ncol), order="F"), np.zeros((nk, ncol), order="F")
+    q2 = qt.copy(order="F")
+    assert pkg.settei_ng(F, C, te, ti, q2) == pkg.TG_OK
+    te_r, ti_r, q2_r = orc.settei_ng(F, C, qt)
+    assert _rel(te, te_r) <= SETTEI_TOL
+    assert _rel(ti, ti_r) <= SETTEI_TOL
+    assert _rel(q2, q2_r) <= SETTEI_TOL
+
+
+def test_settei_ng_device_system(cuda, pkg, orc):
+    torch = cuda
+    nk, ncol, dz = 57, 1000, 0.25
+    F, C, qt = pkg.synth.settei_inputs(nk, ncol, dz, 5, et=1, electron_heating=0)
+    (te_r, ti_r, q2_r), sysref = orc.settei_ng(F, C, qt, with_system=True)
+    ld = pkg.batch.pad_ld(ncol)
+    dev = {}
+    for k, v in F.items():
+        if v.ndim == 2:
+            dev[k] = pkg.batch.level_scalar(v, ld, "cuda")
+        else:
+            t = torch.zeros(ld, dtype=torch.float64, device="cuda")
+            t[:ncol] = torch.from_numpy(v)
+            dev[k] = t
+    te = torch.zeros((nk, ld), dtype=torch.float64, device="cuda")
+    ti = torch.zeros((nk, ld), dtype=torch.float64, device="cuda")
+    q2 = pkg.batch.level_scalar(qt, ld, "cuda")
+    sysout = torch.zeros((4, nk, ld), dtype=torch.float64, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pkg.settei_ng_dev(dev, C, te, ti, q2, nk, ncol, ld, system_out=sysout, status=st)
+    torch.cuda.synchronize()
+    assert int(st.item()) == pkg.TG_OK
+    assert _rel(pkg.batch.from_level_scalar(te, ncol), te_r) <= SETTEI_TOL
+    assert _rel(pkg.batch.from_level_scalar(ti, ncol), ti_r) <= SETTEI_TOL
+    assert _rel(pkg.batch.from_level_scalar(q2, ncol), q2_r) <= SETTEI_TOL
+    for i, want in enumerate(sysref):
+        assert _rel(pkg.batch.from_level_scalar(sysout[i], ncol)[:nk - 1], want[:nk - 1]) <= SETTEI_TOL

@@ -38,7 +38,7 @@ LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
 EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor_ng_dev", "tg_comp_ng",
-           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
+           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_settei_ng", "tg_settei_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
@@ -130,6 +130,30 @@ def comp_consts(c):
                       int(c.get("calc_helium", 1)))
 
 
+SETTEI_FIELDS = ("tn", "o2", "o1", "he", "n2", "ne", "te", "ti", "op", "o2p", "nplus", "n2p", "nop", "xnmbar",
+                 "xnmbari", "scht", "schti", "qji_ti", "qop2p", "qop2d", "qo2p", "qop", "qn2p", "qnp", "qnop",
+                 "Q1", "Q2", "t_lbc", "chi", "rlatm", "dipmag", "qteaur")
+SETTEI_CONSTS = ("f107", "dipmin", "dz", "evergs", "avo", "rmass_o1", "rmassinv_o2", "rmassinv_o1",
+                 "rmassinv_he", "rmassinv_n2", "rmassinv_n4s", "rmassinv_no")
+
+
+class SetteiFields(ctypes.Structure):
+    """tg_settei_fields of include/tg_colsolve.h."""
+    _fields_ = [(n, ctypes.c_void_p) for n in SETTEI_FIELDS]
+
+
+class SetteiConsts(ctypes.Structure):
+    """tg_settei_consts of include/tg_colsolve.h."""
+    _fields_ = ([(n, ctypes.c_double) for n in SETTEI_CONSTS] +
+                [("b", ctypes.c_double * 9), ("fb", ctypes.c_double * 3), ("et", ctypes.c_int),
+                 ("electron_heating", ctypes.c_int)])
+
+
+def settei_consts(c):
+    return SetteiConsts(*[float(c[n]) for n in SETTEI_CONSTS], (ctypes.c_double * 9)(*np.ravel(c["b"], order="F")),
+                        (ctypes.c_double * 3)(*c["fb"]), int(c.get("et", 0)), int(c.get("electron_heating", 0)))
+
+
 _lib = None
 
 
@@ -148,6 +172,9 @@ def lib():
             "tg_solve_host": [ctypes.POINTER(HostSystem), I],
             "tg_minor_ng": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, I, I],
             "tg_comp_ng": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, P, P, I, I],
+            "tg_settei_ng": [ctypes.POINTER(SetteiFields), ctypes.POINTER(SetteiConsts), P, P, P, I, I],
+            "tg_settei_ng_dev": [ctypes.POINTER(SetteiFields), ctypes.POINTER(SetteiConsts), P, P, P, I, I, Lg, P, P,
+                                 P],
             "tg_comp_ng_dev": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, I, I, Lg, P, P, P],
             "tg_comp_post_ng": [P] * 8 + [D, D, D, I, I] + [P] * 6,
             "tg_minor_ng_dev": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, I, I, Lg, P, P, P],
@@ -349,6 +376,28 @@ def comp_ng(fields, consts, o2_upd, o1_upd, he_upd):
     rc = lib().tg_comp_ng(ctypes.byref(F), ctypes.byref(C), _out(o2_upd, "o2_upd"), _out(o1_upd, "o1_upd"),
                           _out(he_upd, "he_upd"), nk, ncol)
     return _check(rc, "tg_comp_ng")
+
+
+def settei_ng(fields, consts, te_out, ti_out, qtotal):
+    """settei_ng's column step (src/settei_ng.F90:60-261) on host arrays:
+    fields SETTEI_FIELDS ((nk, ncol) Fortran order, 2-D (ncol)); te_out and
+    ti_out receive Te and Ti; qtotal (nk, ncol) is updated in place."""
+    nk = te_out.shape[0]
+    ncol = te_out.size // nk
+    F = SetteiFields(*[_host(fields[n], n) for n in SETTEI_FIELDS])
+    C = settei_consts(consts)
+    rc = lib().tg_settei_ng(ctypes.byref(F), ctypes.byref(C), _out(te_out, "te_out"), _out(ti_out, "ti_out"),
+                            _out(qtotal, "qtotal"), nk, ncol)
+    return _check(rc, "tg_settei_ng")
+
+
+def settei_ng_dev(fields, consts, te_out, ti_out, qtotal, nk, ncol, ld, system_out=None, status=None, stream=None):
+    F = SetteiFields(*[_dptr(fields[n]) for n in SETTEI_FIELDS])
+    C = settei_consts(consts)
+    rc = lib().tg_settei_ng_dev(ctypes.byref(F), ctypes.byref(C), _dptr(te_out), _dptr(ti_out), _dptr(qtotal), nk,
+                                ncol, ld, _dptr(system_out), None if status is None else _int_dptr(status),
+                                _stream(stream))
+    return _check(rc, "tg_settei_ng_dev", numeric_ok=False)
 
 
 def comp_ng_dev(fields, consts, out, nk, ncol, ld, system_out=None, status=None, stream=None):

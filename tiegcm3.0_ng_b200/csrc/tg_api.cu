@@ -942,6 +942,86 @@ __attribute__((visibility("default"))) int tg_comp_post_ng(const double *o2, con
     return TG_OK;
 }
 
+static bool settei_fields_ok(const tg_settei_fields *F)
+{
+    const double *const *p = &F->tn;
+    for (int i = 0; i < 32; ++i)
+        if (!p[i]) return false;
+    return true;
+}
+
+__attribute__((visibility("default"))) int tg_settei_ng_dev(const tg_settei_fields *F, const tg_settei_consts *C,
+                                                            double *te_out, double *ti_out, double *qtotal, int nk,
+                                                            int ncol, long ld, double *system_out, int *status_dev,
+                                                            void *stream)
+{
+    if (!F || !C || !te_out || !ti_out || !qtotal || nk < 3 || ncol < 0 || ld < ncol || !settei_fields_ok(F)) {
+        set_err("tg_settei_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_settei_ng(*F, *C, te_out, ti_out, qtotal, nk, ncol, ld, system_out, cx->flags, st));
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_settei_ng(const tg_settei_fields *F, const tg_settei_consts *C,
+                                                        double *te_out, double *ti_out, double *qtotal, int nk,
+                                                        int ncol)
+{
+    if (!F || !C || !te_out || !ti_out || !qtotal || nk < 3 || ncol < 0 || !settei_fields_ok(F)) {
+        set_err("tg_settei_ng: bad arguments (nk=%d ncol=%d)", nk, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ld = round_up(ncol, 32);
+    const size_t lvl = (size_t)nk * ld, colsz = (size_t)nk * ncol;
+    // 27 fields + qtotal + te_out + ti_out level-major; 5 2-D rows
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (30 * lvl + 5 * (size_t)ld)))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * colsz))) return rc;
+    double *base = (double *)c->lvlbuf[0][0].p, *stage = (double *)c->colbuf[0][0].p;
+    cudaStream_t st = c->st[0];
+    tg_settei_fields D;
+    const double *const *src = &F->tn;
+    const double **dst = &D.tn;
+    for (int i = 0; i < 28; ++i) {
+        const double *h = i < 27 ? src[i] : qtotal;
+        double *d = base + i * lvl;
+        TG_CUDA(cudaMemcpyAsync(stage, h, sizeof(double) * colsz, cudaMemcpyHostToDevice, st));
+        TG_CUDA(launch_col_to_level(stage, nk, d, ld, nk, ncol, st));
+        if (i < 27) dst[i] = d;
+    }
+    double *qt = base + 27 * lvl, *te_l = base + 28 * lvl, *ti_l = base + 29 * lvl, *two = base + 30 * lvl;
+    for (int i = 0; i < 5; ++i) {
+        TG_CUDA(cudaMemcpyAsync(two + i * ld, src[27 + i], sizeof(double) * ncol, cudaMemcpyHostToDevice, st));
+        dst[27 + i] = two + i * ld;
+    }
+    TG_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_settei_ng(D, *C, te_l, ti_l, qt, nk, ncol, ld, nullptr, c->flags, st));
+    double *hout[3] = {te_out, ti_out, qtotal};
+    double *dout[3] = {te_l, ti_l, qt};
+    for (int i = 0; i < 3; ++i) {
+        TG_CUDA(launch_level_to_col(dout[i], ld, stage, nk, nk, ncol, st));
+        TG_CUDA(cudaMemcpyAsync(hout[i], stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaStreamSynchronize(st));
+    }
+    TG_CUDA(cudaMemcpy(c->flags_host, c->flags, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    return flags_to_status(c->flags_host[0]);
+}
+
 __attribute__((visibility("default"))) int tg_trsolv_dev(const double *a, const double *b, const double *c,
                                                          const double *f, double *x, int nk, int k2, int ncol,
                                                          int layout, long ld, int precision, int *status_dev,

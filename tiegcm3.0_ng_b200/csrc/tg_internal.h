@@ -142,6 +142,12 @@ cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, d
                                 double dtsmooth_div2, int nk, int ncol, long ld, double *const *upd6,
                                 cudaStream_t st);
 
+typedef tg_settei_fields SetteiFields;
+typedef tg_settei_consts SetteiConsts;
+cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, double *te_out, double *ti_out,
+                             double *qtotal, int nk, int ncol, long ld, double *sys_out, unsigned *status,
+                             cudaStream_t st);
+
 // L2 cache-policy hints of the bulk-copy ring kernels (tg_set_cache_hints).
 int cache_hints();
 void set_cache_hints(int on);

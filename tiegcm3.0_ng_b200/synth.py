@@ -461,3 +461,56 @@ def settei_inputs(nk, ncol, dz, seed, et=0, electron_heating=0):
              electron_heating=electron_heating)
     qtotal = np.asfortranarray(rng.uniform(0.0, 5e-2, (nk, ncol)))
     return f, c, qtotal
+
+
+OPLUS_FIELDS = ("tn", "te", "ti", "o2", "o1", "n2", "he", "n2d", "ne", "u", "v", "w", "wi", "xnmbar", "scht",
+                "qop2p", "qop2d", "qop", "rk1", "rk2", "rk19", "rk20", "rk25", "op", "optm1_smooth2", "explicit_h",
+                "bdotdh_djbz")
+OPLUS_2D = ("bx", "by", "bz", "dvb", "rlatm", "chi", "dipmag", "sndec", "csdec")
+
+
+def oplus_inputs(nk, ncol, dz, seed, step=60.0, nstep_sub=10, opdiffcap=0.0):
+    """Seeded fields of the oplus_ng vertical column step (CGS): neutral /
+    ion / electron temperatures, composition, winds and ion drifts, O+ and
+    its production, the temperature-dependent rate fields, the horizontal
+    terms the host model supplies (explicit_h, bdotdh_djbz, dvb) and a
+    magnetic field with |bz| >= 0.2.  Returns (fields dict, constants dict)."""
+    rng = _rng(seed)
+    z = np.linspace(0.0, 1.0, nk)[:, None]
+    U = lambda lo, hi, shape=(nk, ncol): rng.uniform(lo, hi, size=shape)
+    f = {}
+    f["tn"] = 200.0 + 800.0 * z ** 0.7 * U(0.9, 1.1)
+    f["te"] = f["tn"] + 2000.0 * z * U(0.5, 1.5)
+    f["ti"] = f["tn"] + 0.5 * (f["te"] - f["tn"]) * U(0.5, 1.0)
+    f["o2"] = (0.22 - 0.21 * z) * U(0.9, 1.1)
+    f["o1"] = (0.05 + 0.75 * z) * U(0.9, 1.1)
+    f["he"] = (1e-5 + 0.05 * z ** 2) * U(0.9, 1.1)
+    f["n2"] = np.maximum(1.0 - f["o2"] - f["o1"] - f["he"], 1e-3)
+    f["n2d"] = 1e-6 * U(0.5, 1.5)
+    f["ne"] = 1e3 + 1e6 * np.exp(-((z - 0.6) / 0.25) ** 2) * U(0.5, 1.5)
+    f["u"], f["v"] = U(-1e4, 1e4), U(-1e4, 1e4)
+    f["w"], f["wi"] = U(-1e-4, 1e-4), U(-1e-4, 1e-4)
+    f["xnmbar"] = 1e13 * np.exp(-10.0 * z) * U(0.5, 1.5)
+    f["scht"] = 1e6 + 5e6 * z * U(0.9, 1.1)
+    f["qop2p"], f["qop2d"], f["qop"] = (U(0.0, 10.0) * np.exp(-((z - 0.5) / 0.3) ** 2) + 1e-3 for _ in range(3))
+    f["rk1"], f["rk2"] = U(1e-11, 3e-11), U(1e-12, 2e-12)
+    f["rk19"], f["rk20"], f["rk25"] = U(1e-7, 2e-7), U(1e-7, 2e-7), U(1e-7, 2e-7)
+    f["op"] = 0.8 * f["ne"] * z * U(0.9, 1.1) + 1.0
+    f["optm1_smooth2"] = f["op"] * U(0.99, 1.01)
+    f["explicit_h"] = f["op"] * U(-1e-4, 1e-4)
+    f["bdotdh_djbz"] = U(-1e3, 1e3)
+    for k in OPLUS_FIELDS:
+        f[k] = np.asfortranarray(f[k])
+    f["bx"], f["by"] = rng.uniform(-0.5, 0.5, ncol), rng.uniform(-0.5, 0.5, ncol)
+    f["bz"] = rng.choice([-1.0, 1.0], ncol) * rng.uniform(0.2, 1.0, ncol)
+    f["dvb"] = rng.uniform(-1e-9, 1e-9, ncol)
+    f["rlatm"] = rng.uniform(-np.pi / 2, np.pi / 2, ncol)
+    f["chi"] = rng.uniform(0.0, np.pi, ncol)
+    f["dipmag"] = rng.uniform(-np.pi / 2, np.pi / 2, ncol)
+    f["sndec"], f["csdec"] = rng.uniform(-0.2, 0.2, ncol), rng.uniform(0.9, 1.0, ncol)
+    f["zpint"] = -7.0 + np.arange(nk) * dz
+    c = dict(rmass_op=16.0, gask=8.314e7, grav=870.0, re=6.37122e8, rmassinv_o2=1 / 32., rmassinv_o1=1 / 16.,
+             rmassinv_n2=1 / 28., rmassinv_n2d=1 / 14., rmassinv_he=1 / 4., rk10=1.3E-10, rk16=4.8E-10, rk17=1.0E-10,
+             rk18=4.0E-10, rk21=0.047, rk22=0.171, rk23=8.E-10, rk24=5.0E-12, rk26=7.E-10, rk27=7.7E-5, colfac=1.5,
+             opdiffcap=opdiffcap, dtx2inv=1.0 / (2.0 * step), dz=dz, dlev=dz, nstep_sub=nstep_sub)
+    return f, c
