@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--profile", default=None,
                    help="run only one kind's plan for a profiler: KIND:PREC[:VARIANT], KIND scalar|block, "
                         "PREC f64|refine, VARIANT reg:CPB:CPT[:PF], regg:CPB:1[:PF], ring[g]:DEPTH[:WARPS] "
-                        "(default: library default); or 'dt' / 'minor' / 'comp' / 'settei' for the fused assembly+solve kernels")
+                        "(default: library default); or dt / minor / comp / settei / oplus for the fused assembly+solve kernels")
     p.add_argument("--skip-assembly", action="store_true")
     return p.parse_args()
 
@@ -236,6 +236,11 @@ def assembly_setup(pkg, wl, which, dev, replicas=ASSEMBLY_REPLICAS):
         F, C = pkg.synth.comp_inputs(nk, ncol, dz, 107)
         one_d, n2d, n3d = ("expz", "difk"), len(pkg.synth.COMP_2D), len(pkg.synth.COMP_FIELDS) + 12
         nout = 3
+    elif which == "oplus":
+        F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 113)
+        # 27 fields read; opout, xiop2p, xiop2d written (Fe, Fn not requested)
+        one_d, n2d, n3d = ("zpint",), len(pkg.synth.OPLUS_2D), len(pkg.synth.OPLUS_FIELDS)
+        nout = 3
     else:
         F, C, qt = pkg.synth.settei_inputs(nk, ncol, dz, 109)
         # 27 fields and qtotal read; te, ti and qtotal written
@@ -261,6 +266,10 @@ def assembly_setup(pkg, wl, which, dev, replicas=ASSEMBLY_REPLICAS):
     out = torch.zeros((nout, nk, ld), dtype=torch.float64, device=dev)
     # 3-D fields read + the solution written, 2-D and 1-D inputs read
     nbytes = 8 * ((n3d + nout) * nk * ncol + n2d * ncol + len(one_d) * nk)
+    if which == "oplus":
+        def launch(stream):
+            pkg.oplus_ng_dev(d, C, out[0], out[1], out[2], nk, ncol, ld, stream=stream)
+        return launch, ncol, nbytes
     if which == "settei":
         qtd = pkg.batch.level_scalar(qt, ld, dev)
 
@@ -278,7 +287,7 @@ def run_profile(args):
     """Executes one kind's plan --warmup + --steps times (for ncu captures)."""
     import torch
     pkg = ge.load_package()
-    if args.profile in ("dt", "minor", "comp", "settei"):
+    if args.profile in ("dt", "minor", "comp", "settei", "oplus"):
         wl = pkg.synth.workload(args.config)
         launch, ncol, nbytes = assembly_setup(pkg, wl, args.profile, "cuda")
         stream = torch.cuda.Stream()
@@ -438,7 +447,7 @@ def main():
     if not args.skip_assembly:
         assembly = {}
         for which, kern in (("dt", "k_dt_ng"), ("minor", "k_minor_ng"), ("comp", "k_comp_ng"),
-                            ("settei", "k_settei_ng")):
+                            ("settei", "k_settei_ng"), ("oplus", "k_oplus_ng")):
             launch, ncol_a, nbytes = assembly_setup(pkg, wl, which, dev)
             for _ in range(args.warmup):
                 launch(stream)

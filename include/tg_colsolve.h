@@ -305,6 +305,39 @@ int tg_settei_ng(const tg_settei_fields *F, const tg_settei_consts *C, double *t
 int tg_settei_ng_dev(const tg_settei_fields *F, const tg_settei_consts *C, double *te_out, double *ti_out,
                      double *qtotal, int nk, int ncol, long ld, double *system_out, int *status_dev, void *stream);
 
+/* oplus_ng's O+ column step, vertical part (src/oplus_ng.F90:88-307): the
+ * diffusion, drift and wind rows, chemistry, both boundaries, the solve of
+ * rows 1..nk-1 and the top level.  The terms built from horizontal
+ * derivatives come from the host model as inputs, exactly as the reference
+ * computes them: explicit_h = -explic*diffexp + vdotn_h + bdotdh_bvel
+ * (:178-207), bdotdh_djbz = bdotdh(dj*bz) (:234), dvb = (div b + 2 bz)/re
+ * before its division by bz (:101-107), optm1_smooth2 = smooth_ng(optm1)
+ * (:162).  Outputs opout (before the lateral-boundary overwrite, the time
+ * filter and the clamp of :326-331, which stay with the caller), xiop2p,
+ * xiop2d (:285-288); Fe, Fn (:164-169) may be NULL.  The diffusion cap
+ * applies when |opdiffcap| >= 1e-9 (isclose of src/util.F:1384). */
+typedef struct {
+    const double *tn, *te, *ti, *o2, *o1, *n2, *he, *n2d, *ne, *u, *v, *w, *wi, *xnmbar, *scht, *qop2p, *qop2d;
+    const double *qop, *rk1, *rk2, *rk19, *rk20, *rk25, *op, *optm1_smooth2, *explicit_h, *bdotdh_djbz;
+    const double *bx, *by, *bz, *dvb, *rlatm, *chi, *dipmag, *sndec, *csdec;
+    const double *zpint;
+} tg_oplus_fields;
+
+typedef struct {
+    double rmass_op, gask, grav, re, rmassinv_o2, rmassinv_o1, rmassinv_n2, rmassinv_n2d, rmassinv_he;
+    double rk10, rk16, rk17, rk18, rk21, rk22, rk23, rk24, rk26, rk27;
+    double colfac, opdiffcap, dtx2inv, dz, dlev;
+    int nstep_sub;
+} tg_oplus_consts;
+
+int tg_oplus_ng(const tg_oplus_fields *F, const tg_oplus_consts *C, double *opout, double *xiop2p, double *xiop2d,
+                double *Fe, double *Fn, int nk, int ncol);
+/* Device form: level-major (k*ld + col) arrays, zpint (nk); system_out (may
+ * be NULL) 4 slabs (p, q, r, explicit) of nk*ld, rows 1..nk-1. */
+int tg_oplus_ng_dev(const tg_oplus_fields *F, const tg_oplus_consts *C, double *opout, double *xiop2p,
+                    double *xiop2d, double *Fe, double *Fn, int nk, int ncol, long ld, double *system_out,
+                    int *status_dev, void *stream);
+
 /* ---- batched, GPU-resident plans ---------------------------------------------
  * A plan solves many independent systems ("segments": any mix of grids, nest
  * levels, sub-steps and species) in one persistent launch per system kind,

@@ -203,3 +203,52 @@ def test_settei_ng_device_system(cuda, pkg, orc):
     assert _rel(pkg.batch.from_level_scalar(q2, ncol), q2_r) <= SETTEI_TOL
     for i, want in enumerate(sysref):
         assert _rel(pkg.batch.from_level_scalar(sysout[i], ncol)[:nk - 1], want[:nk - 1]) <= SETTEI_TOL
+
+
+# oplus_ng: the device log10 / pow / cos differ from the C library's in the
+# last bits; the system (condition ~1e4 on these inputs) carries that into the
+# solution.  Coefficients, rates and fluxes agree to OPLUS_TOL_COEF.
+OPLUS_TOL = 1e-10
+OPLUS_TOL_COEF = 1e-12
+
+
+@pytest.mark.parametrize("nk,dz,ncol,cap", [(57, 0.25, 3001, 0.0), (29, 0.5, 2592, 1e7), (113, 0.125, 300, 0.0),
+                                            (3, 0.5, 33, 1e5)])
+def test_oplus_ng_host(cuda, pkg, orc, nk, dz, ncol, cap):
+    F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 41 + nk, opdiffcap=cap)
+    outs = [np.zeros((nk, ncol), order="F") for _ in range(5)]
+    assert pkg.oplus_ng(F, C, *outs) == pkg.TG_OK
+    ref = orc.oplus_ng(F, C)
+    assert _rel(outs[0], ref[0]) <= OPLUS_TOL
+    for got, want in zip(outs[1:], ref[1:]):
+        assert _rel(got, want) <= OPLUS_TOL_COEF
+
+
+def test_oplus_ng_device_system(cuda, pkg, orc):
+    torch = cuda
+    nk, ncol, dz = 57, 1000, 0.25
+    F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 6)
+    ref, sysref = orc.oplus_ng(F, C, with_system=True)
+    ld = pkg.batch.pad_ld(ncol)
+    dev = {}
+    for k, v in F.items():
+        if v.ndim == 2:
+            dev[k] = pkg.batch.level_scalar(v, ld, "cuda")
+        elif k == "zpint":
+            dev[k] = torch.from_numpy(np.ascontiguousarray(v)).cuda()
+        else:
+            t = torch.zeros(ld, dtype=torch.float64, device="cuda")
+            t[:ncol] = torch.from_numpy(v)
+            dev[k] = t
+    outs = [torch.zeros((nk, ld), dtype=torch.float64, device="cuda") for _ in range(5)]
+    sysout = torch.zeros((4, nk, ld), dtype=torch.float64, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pkg.oplus_ng_dev(dev, C, outs[0], outs[1], outs[2], nk, ncol, ld, Fe=outs[3], Fn=outs[4], system_out=sysout,
+                     status=st)
+    torch.cuda.synchronize()
+    assert int(st.item()) == pkg.TG_OK
+    assert _rel(pkg.batch.from_level_scalar(outs[0], ncol), ref[0]) <= OPLUS_TOL
+    for o, want in zip(outs[1:], ref[1:]):
+        assert _rel(pkg.batch.from_level_scalar(o, ncol), want) <= OPLUS_TOL_COEF
+    for i, want in enumerate(sysref):
+        assert _rel(pkg.batch.from_level_scalar(sysout[i], ncol)[:nk - 1], want[:nk - 1]) <= OPLUS_TOL_COEF

@@ -38,7 +38,8 @@ LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
 EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor_ng_dev", "tg_comp_ng",
-           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_settei_ng", "tg_settei_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
+           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
+           "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
@@ -154,6 +155,28 @@ def settei_consts(c):
                         (ctypes.c_double * 3)(*c["fb"]), int(c.get("et", 0)), int(c.get("electron_heating", 0)))
 
 
+OPLUS_FIELDS = ("tn", "te", "ti", "o2", "o1", "n2", "he", "n2d", "ne", "u", "v", "w", "wi", "xnmbar", "scht",
+                "qop2p", "qop2d", "qop", "rk1", "rk2", "rk19", "rk20", "rk25", "op", "optm1_smooth2", "explicit_h",
+                "bdotdh_djbz", "bx", "by", "bz", "dvb", "rlatm", "chi", "dipmag", "sndec", "csdec", "zpint")
+OPLUS_CONSTS = ("rmass_op", "gask", "grav", "re", "rmassinv_o2", "rmassinv_o1", "rmassinv_n2", "rmassinv_n2d",
+                "rmassinv_he", "rk10", "rk16", "rk17", "rk18", "rk21", "rk22", "rk23", "rk24", "rk26", "rk27",
+                "colfac", "opdiffcap", "dtx2inv", "dz", "dlev")
+
+
+class OplusFields(ctypes.Structure):
+    """tg_oplus_fields of include/tg_colsolve.h."""
+    _fields_ = [(n, ctypes.c_void_p) for n in OPLUS_FIELDS]
+
+
+class OplusConsts(ctypes.Structure):
+    """tg_oplus_consts of include/tg_colsolve.h."""
+    _fields_ = [(n, ctypes.c_double) for n in OPLUS_CONSTS] + [("nstep_sub", ctypes.c_int)]
+
+
+def oplus_consts(c):
+    return OplusConsts(*[float(c[n]) for n in OPLUS_CONSTS], int(c["nstep_sub"]))
+
+
 _lib = None
 
 
@@ -173,6 +196,9 @@ def lib():
             "tg_minor_ng": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, I, I],
             "tg_comp_ng": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, P, P, I, I],
             "tg_settei_ng": [ctypes.POINTER(SetteiFields), ctypes.POINTER(SetteiConsts), P, P, P, I, I],
+            "tg_oplus_ng": [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), P, P, P, P, P, I, I],
+            "tg_oplus_ng_dev": [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), P, P, P, P, P, I, I, Lg, P,
+                                P, P],
             "tg_settei_ng_dev": [ctypes.POINTER(SetteiFields), ctypes.POINTER(SetteiConsts), P, P, P, I, I, Lg, P, P,
                                  P],
             "tg_comp_ng_dev": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, I, I, Lg, P, P, P],
@@ -389,6 +415,30 @@ def settei_ng(fields, consts, te_out, ti_out, qtotal):
     rc = lib().tg_settei_ng(ctypes.byref(F), ctypes.byref(C), _out(te_out, "te_out"), _out(ti_out, "ti_out"),
                             _out(qtotal, "qtotal"), nk, ncol)
     return _check(rc, "tg_settei_ng")
+
+
+def oplus_ng(fields, consts, opout, xiop2p, xiop2d, Fe=None, Fn=None):
+    """oplus_ng's vertical column step (src/oplus_ng.F90:88-307) on host
+    arrays: fields OPLUS_FIELDS ((nk, ncol) Fortran order, 2-D (ncol), zpint
+    (nk)); outputs (nk, ncol)."""
+    nk = opout.shape[0]
+    ncol = opout.size // nk
+    F = OplusFields(*[_host(fields[n], n) for n in OPLUS_FIELDS])
+    C = oplus_consts(consts)
+    rc = lib().tg_oplus_ng(ctypes.byref(F), ctypes.byref(C), _out(opout, "opout"), _out(xiop2p, "xiop2p"),
+                           _out(xiop2d, "xiop2d"), None if Fe is None else _out(Fe, "Fe"),
+                           None if Fn is None else _out(Fn, "Fn"), nk, ncol)
+    return _check(rc, "tg_oplus_ng")
+
+
+def oplus_ng_dev(fields, consts, opout, xiop2p, xiop2d, nk, ncol, ld, Fe=None, Fn=None, system_out=None,
+                 status=None, stream=None):
+    F = OplusFields(*[_dptr(fields[n]) for n in OPLUS_FIELDS])
+    C = oplus_consts(consts)
+    rc = lib().tg_oplus_ng_dev(ctypes.byref(F), ctypes.byref(C), _dptr(opout), _dptr(xiop2p), _dptr(xiop2d),
+                               _dptr(Fe), _dptr(Fn), nk, ncol, ld, _dptr(system_out),
+                               None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_oplus_ng_dev", numeric_ok=False)
 
 
 def settei_ng_dev(fields, consts, te_out, ti_out, qtotal, nk, ncol, ld, system_out=None, status=None, stream=None):

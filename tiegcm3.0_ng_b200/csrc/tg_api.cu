@@ -1022,6 +1022,95 @@ __attribute__((visibility("default"))) int tg_settei_ng(const tg_settei_fields *
     return flags_to_status(c->flags_host[0]);
 }
 
+static bool oplus_fields_ok(const tg_oplus_fields *F)
+{
+    const double *const *p = &F->tn;
+    for (int i = 0; i < 37; ++i)
+        if (!p[i]) return false;
+    return true;
+}
+
+__attribute__((visibility("default"))) int tg_oplus_ng_dev(const tg_oplus_fields *F, const tg_oplus_consts *C,
+                                                           double *opout, double *xiop2p, double *xiop2d, double *Fe,
+                                                           double *Fn, int nk, int ncol, long ld, double *system_out,
+                                                           int *status_dev, void *stream)
+{
+    if (!F || !C || !opout || !xiop2p || !xiop2d || (!Fe) != (!Fn) || nk < 3 || ncol < 0 || ld < ncol ||
+        !oplus_fields_ok(F)) {
+        set_err("tg_oplus_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t sbytes = sizeof(double) * oplus_scratch_planes() * (size_t)nk * (size_t)(ld > 0 ? ld : 1);
+    if ((rc = grow(cx->scratch[0], sbytes))) return rc;
+    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_oplus_ng(*F, *C, opout, xiop2p, xiop2d, Fe, Fn, (double *)cx->scratch[0].p, nk, ncol, ld,
+                            system_out, cx->flags, st));
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_oplus_ng(const tg_oplus_fields *F, const tg_oplus_consts *C,
+                                                       double *opout, double *xiop2p, double *xiop2d, double *Fe,
+                                                       double *Fn, int nk, int ncol)
+{
+    if (!F || !C || !opout || !xiop2p || !xiop2d || (!Fe) != (!Fn) || nk < 3 || ncol < 0 || !oplus_fields_ok(F)) {
+        set_err("tg_oplus_ng: bad arguments (nk=%d ncol=%d)", nk, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ld = round_up(ncol, 32);
+    const size_t lvl = (size_t)nk * ld, colsz = (size_t)nk * ncol;
+    const int nout = Fe ? 5 : 3;
+    // 27 fields + outputs level-major; 9 2-D rows; zpint
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * ((27 + nout) * lvl + 9 * (size_t)ld + (size_t)nk)))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * colsz))) return rc;
+    if ((rc = grow(c->scratch[0], sizeof(double) * oplus_scratch_planes() * lvl))) return rc;
+    double *base = (double *)c->lvlbuf[0][0].p, *stage = (double *)c->colbuf[0][0].p;
+    cudaStream_t st = c->st[0];
+    tg_oplus_fields D;
+    const double *const *src = &F->tn;
+    const double **dst = &D.tn;
+    for (int i = 0; i < 27; ++i) {
+        double *d = base + i * lvl;
+        TG_CUDA(cudaMemcpyAsync(stage, src[i], sizeof(double) * colsz, cudaMemcpyHostToDevice, st));
+        TG_CUDA(launch_col_to_level(stage, nk, d, ld, nk, ncol, st));
+        dst[i] = d;
+    }
+    double *outs = base + 27 * lvl, *two = outs + nout * lvl, *zp = two + 9 * ld;
+    for (int i = 0; i < 9; ++i) {
+        TG_CUDA(cudaMemcpyAsync(two + i * ld, src[27 + i], sizeof(double) * ncol, cudaMemcpyHostToDevice, st));
+        dst[27 + i] = two + i * ld;
+    }
+    TG_CUDA(cudaMemcpyAsync(zp, F->zpint, sizeof(double) * nk, cudaMemcpyHostToDevice, st));
+    D.zpint = zp;
+    double *dout[5];
+    for (int i = 0; i < nout; ++i) dout[i] = outs + i * lvl;
+    TG_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_oplus_ng(D, *C, dout[0], dout[1], dout[2], Fe ? dout[3] : nullptr, Fe ? dout[4] : nullptr,
+                            (double *)c->scratch[0].p, nk, ncol, ld, nullptr, c->flags, st));
+    double *hout[5] = {opout, xiop2p, xiop2d, Fe, Fn};
+    for (int i = 0; i < nout; ++i) {
+        TG_CUDA(launch_level_to_col(dout[i], ld, stage, nk, nk, ncol, st));
+        TG_CUDA(cudaMemcpyAsync(hout[i], stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaStreamSynchronize(st));
+    }
+    TG_CUDA(cudaMemcpy(c->flags_host, c->flags, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    return flags_to_status(c->flags_host[0]);
+}
+
 __attribute__((visibility("default"))) int tg_trsolv_dev(const double *a, const double *b, const double *c,
                                                          const double *f, double *x, int nk, int k2, int ncol,
                                                          int layout, long ld, int precision, int *status_dev,

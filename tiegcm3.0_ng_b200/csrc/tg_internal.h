@@ -148,6 +148,13 @@ cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, doubl
                              double *qtotal, int nk, int ncol, long ld, double *sys_out, unsigned *status,
                              cudaStream_t st);
 
+typedef tg_oplus_fields OplusFields;
+typedef tg_oplus_consts OplusConsts;
+cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *opout, double *xiop2p,
+                            double *xiop2d, double *Fe, double *Fn, double *scratch, int nk, int ncol, long ld,
+                            double *sys_out, unsigned *status, cudaStream_t st);
+int oplus_scratch_planes();   // level-major scratch planes of launch_oplus_ng (each nk*ld doubles)
+
 // L2 cache-policy hints of the bulk-copy ring kernels (tg_set_cache_hints).
 int cache_hints();
 void set_cache_hints(int on);
