@@ -313,7 +313,7 @@ int tg_settei_ng_dev(const tg_settei_fields *F, const tg_settei_consts *C, doubl
  * (:178-207), bdotdh_djbz = bdotdh(dj*bz) (:234), dvb = (div b + 2 bz)/re
  * before its division by bz (:101-107), optm1_smooth2 = smooth_ng(optm1)
  * (:162).  Outputs opout (before the lateral-boundary overwrite, the time
- * filter and the clamp of :326-331, which stay with the caller), xiop2p,
+ * filter and the clamp of :332-340, which stay with the caller), xiop2p,
  * xiop2d (:285-288); Fe, Fn (:164-169) may be NULL.  The diffusion cap
  * applies when |opdiffcap| >= 1e-9 (isclose of src/util.F:1384). */
 typedef struct {
@@ -418,6 +418,12 @@ int tg_set_scratch_global(int kind, int precision, int on);
  * streams evict-first, the sweep's scratch and parked w3 evict-last.
  * on: 1 (default), 0 off, -1 back to the default. */
 int tg_set_cache_hints(int on);
+
+/* Runs the ring kernels' bounded mbarrier wait on a barrier that nothing
+ * completes, giving up after `polls` polls (1..2^22): *status_dev receives
+ * TG_ETIMEOUT, as a solve does when a bulk copy never lands.  Tests the
+ * timeout path without a stuck copy or a fault. */
+int tg_selftest_wait(unsigned polls, int *status_dev, void *stream);
 /* Test entry: q[i] = a[i]/b[i] (device arrays, n elements) computed by the
  * kernels' division routine (Markstein's correction of the correctly rounded
  * reciprocal, IEEE division outside its safe range); must equal IEEE a/b. */

@@ -1176,7 +1176,7 @@ ORACLE_API void oracle_settei_ng(const oracle_settei_fields *F, const oracle_set
 /* zpint (nk).  Outputs: opout rows 1..nk (the top from :307), xiop2p,      */
 /* xiop2d (:285-288); Fe, Fn (:164-169) and the system p,q,r,explicit rows   */
 /* 1..nk-1 may be NULL.  opout is before the lateral-boundary overwrite,    */
-/* the time filter and the max(.,0) of :326-331, which the caller applies.  */
+/* the time filter and the max(.,0) of :332-340, which the caller applies.   */
 /* ------------------------------------------------------------------------ */
 typedef struct {
     const double *tn, *te, *ti, *o2, *o1, *n2, *he, *n2d, *ne, *u, *v, *w, *wi, *xnmbar, *scht, *qop2p, *qop2d,

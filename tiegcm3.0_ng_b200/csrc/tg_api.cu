@@ -1399,6 +1399,24 @@ __attribute__((visibility("default"))) int tg_plan_status(tg_plan *p, int *per_s
 
 __attribute__((visibility("default"))) int tg_plan_launches(const tg_plan *p) { return p ? p->launches : 0; }
 
+__attribute__((visibility("default"))) int tg_selftest_wait(unsigned polls, int *status_dev, void *stream)
+{
+    if (!status_dev || polls < 1 || polls > (1u << 22)) {
+        set_err("tg_selftest_wait: bad arguments (polls=%u)", polls);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_selftest_wait(polls, cx->flags, st));
+    k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+    TG_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
 __attribute__((visibility("default"))) int tg_set_cache_hints(int on)
 {
     tg::set_cache_hints(on);

@@ -155,6 +155,8 @@ cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *
                             double *sys_out, unsigned *status, cudaStream_t st);
 int oplus_scratch_planes();   // level-major scratch planes of launch_oplus_ng (each nk*ld doubles)
 
+cudaError_t launch_selftest_wait(unsigned polls, unsigned *status, cudaStream_t st);
+
 // L2 cache-policy hints of the bulk-copy ring kernels (tg_set_cache_hints).
 int cache_hints();
 void set_cache_hints(int on);

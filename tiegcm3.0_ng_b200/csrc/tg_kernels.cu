@@ -212,11 +212,11 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t 
     return ok != 0;
 }
 // Bounded wait of the whole warp; true when every lane saw the phase complete.
-__device__ __forceinline__ bool mbar_wait_warp(unsigned long long *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait_warp(unsigned long long *bar, uint32_t parity, unsigned limit = kWaitLimit)
 {
     bool done = false;
 #pragma unroll 1
-    for (unsigned i = 0; i < kWaitLimit && !done; ++i) done = mbar_try_wait(bar, parity);
+    for (unsigned i = 0; i < limit && !done; ++i) done = mbar_try_wait(bar, parity);
     return __all_sync(0xffffffffu, done);
 }
 
@@ -1495,6 +1495,29 @@ __global__ void k_selftest_division(const double *a, const double *b, double *q,
 {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         q[i] = qdiv(a[i], b[i], __drcp_rn(b[i]));
+}
+
+// The ring kernels' bounded wait, run on an mbarrier that nothing arrives
+// at: after `polls` polls the warp gives up and reports FLAG_TIMEOUT, as a
+// ring kernel does when a bulk copy never lands.  Exercises the timeout path
+// without a stuck copy.
+__global__ void __launch_bounds__(32) k_selftest_wait(unsigned polls, unsigned *status)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    const bool ok = mbar_wait_warp(&bar, 0u, polls);
+    if (lane == 0 && !ok) atomicOr(status, FLAG_TIMEOUT);
+}
+
+cudaError_t launch_selftest_wait(unsigned polls, unsigned *status, cudaStream_t st)
+{
+    k_selftest_wait<<<1, 32, 0, st>>>(polls, status);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_selftest_division(const double *a, const double *b, double *q, long n, cudaStream_t st)
