@@ -13,6 +13,84 @@ module tg_colsolve_mod
     TG_ENOCONV = 4, TG_ETIMEOUT = 5, TG_ECUDA = 6, TG_ENOMEM = 7, TG_ENODEV = 8
   integer(c_int), parameter :: TG_PREC_F64 = 0, TG_PREC_F32_REFINE = 1
 
+  ! Field tables of the fused assembly + solve entries: c_loc() of each
+  ! Fortran array (3-D fields (nk, ncol), 2-D (ncol), level profiles (nk)),
+  ! in the order of the C structs in include/tg_colsolve.h.
+  type, bind(C) :: tg_dt_fields
+    type(c_ptr) :: tn, tnsmooth, horadv, un, vn, o1
+    type(c_ptr) :: mbar, xnmbar, scht, schti, cp, kt
+    type(c_ptr) :: km, hdt, qji_tn, cool_imp, cool_exp, w
+    type(c_ptr) :: qtotal, rkm12, tlbc, t_lbc, ulbc, vlbc
+    type(c_ptr) :: expz, dift
+  end type tg_dt_fields
+
+  type, bind(C) :: tg_dt_consts
+    real(c_double) :: dz, dtx2inv, expzmid_inv, grav, p0, avo, gask, tsurplus, rmassinv_o1
+  end type tg_dt_consts
+
+  type, bind(C) :: tg_minor_fields
+    type(c_ptr) :: tn, o2, o1, he, mbar, barm
+    type(c_ptr) :: xnmbar, w, ftm1_smooth, hadvec, sloss, sprod
+    type(c_ptr) :: tlbc, flbc1, flbc2, flbc3, fubc, dfactor
+    type(c_ptr) :: expz, difk
+  end type tg_minor_fields
+
+  type, bind(C) :: tg_minor_consts
+    real(c_double) :: rmx, alfax, phix(4), dzp, dtx2inv, expzmid, expzmid_inv
+    real(c_double) :: rmassinv_o2, rmassinv_o1, rmassinv_n2, rmassinv_he
+    real(c_double) :: rmass_o2, rmass_o1, rmass_he, rmass_n2, p0, grav, avo
+    real(c_double) :: b(9), fb(3)
+  end type tg_minor_consts
+
+  type, bind(C) :: tg_comp_fields
+    type(c_ptr) :: tn, o2, o1, he, w, mbar
+    type(c_ptr) :: o2nm_smooth, o1nm_smooth, henm_smooth, o2_advec, o1_advec, he_advec
+    type(c_ptr) :: hdo2, hdo1, hdhe, fs, tlbc, flx_he
+    type(c_ptr) :: dfactor, expz, difk
+  end type tg_comp_fields
+
+  type, bind(C) :: tg_comp_consts
+    real(c_double) :: dz, dtx2inv, expzmid, expzmid_inv
+    real(c_double) :: rmassinv_o2, rmassinv_o1, rmassinv_he, rmassinv_n2
+    real(c_double) :: rmass_o2, rmass_o1, rmass_he, p0, grav
+    real(c_double) :: b(9), fb(3)
+    real(c_double) :: pshelb
+    integer(c_int) :: calc_helium
+  end type tg_comp_consts
+
+  type, bind(C) :: tg_settei_fields
+    type(c_ptr) :: tn, o2, o1, he, n2, ne
+    type(c_ptr) :: te, ti, op, o2p, nplus, n2p
+    type(c_ptr) :: nop, xnmbar, xnmbari, scht, schti, qji_ti
+    type(c_ptr) :: qop2p, qop2d, qo2p, qop, qn2p, qnp
+    type(c_ptr) :: qnop, Q1, Q2, t_lbc, chi, rlatm
+    type(c_ptr) :: dipmag, qteaur
+  end type tg_settei_fields
+
+  type, bind(C) :: tg_settei_consts
+    real(c_double) :: f107, dipmin, dz, evergs, avo, rmass_o1
+    real(c_double) :: rmassinv_o2, rmassinv_o1, rmassinv_he, rmassinv_n2, rmassinv_n4s, rmassinv_no
+    real(c_double) :: b(9), fb(3)
+    integer(c_int) :: et, electron_heating
+  end type tg_settei_consts
+
+  type, bind(C) :: tg_oplus_fields
+    type(c_ptr) :: tn, te, ti, o2, o1, n2
+    type(c_ptr) :: he, n2d, ne, u, v, w
+    type(c_ptr) :: wi, xnmbar, scht, qop2p, qop2d, qop
+    type(c_ptr) :: rk1, rk2, rk19, rk20, rk25, op
+    type(c_ptr) :: optm1_smooth2, explicit_h, bdotdh_djbz, bx, by, bz
+    type(c_ptr) :: dvb, rlatm, chi, dipmag, sndec, csdec
+    type(c_ptr) :: zpint
+  end type tg_oplus_fields
+
+  type, bind(C) :: tg_oplus_consts
+    real(c_double) :: rmass_op, gask, grav, re, rmassinv_o2, rmassinv_o1, rmassinv_n2, rmassinv_n2d, rmassinv_he
+    real(c_double) :: rk10, rk16, rk17, rk18, rk21, rk22, rk23, rk24, rk26, rk27
+    real(c_double) :: colfac, opdiffcap, dtx2inv, dz, dlev
+    integer(c_int) :: nstep_sub
+  end type tg_oplus_consts
+
   interface
     ! trsolv (src/trsolv.F:2): one latitude slab (lev0:lev1, lon0:lon1)
     integer(c_int) function tg_trsolv(a, b, c, f, x, lev0, lev1, k1, k2, lon0, lon1, lonmax) &
@@ -58,5 +136,56 @@ module tg_colsolve_mod
     integer(c_int) function tg_release_buffers() bind(C, name="tg_release_buffers")
       import :: c_int
     end function tg_release_buffers
+    ! fused column assembly + solve (host arrays, Fortran layout)
+    integer(c_int) function tg_dt_ng(fl, cn, tn_upd, nk, ncol) bind(C, name="tg_dt_ng")
+      import :: c_int, c_double, tg_dt_fields, tg_dt_consts
+      type(tg_dt_fields), intent(in) :: fl
+      type(tg_dt_consts), intent(in) :: cn
+      real(c_double), intent(inout) :: tn_upd(*)
+      integer(c_int), value :: nk, ncol
+    end function tg_dt_ng
+
+    integer(c_int) function tg_minor_ng(fl, cn, fcomp_out, nk, ncol) bind(C, name="tg_minor_ng")
+      import :: c_int, c_double, tg_minor_fields, tg_minor_consts
+      type(tg_minor_fields), intent(in) :: fl
+      type(tg_minor_consts), intent(in) :: cn
+      real(c_double), intent(inout) :: fcomp_out(*)
+      integer(c_int), value :: nk, ncol
+    end function tg_minor_ng
+
+    integer(c_int) function tg_comp_ng(fl, cn, o2_upd, o1_upd, he_upd, nk, ncol) bind(C, name="tg_comp_ng")
+      import :: c_int, c_double, tg_comp_fields, tg_comp_consts
+      type(tg_comp_fields), intent(in) :: fl
+      type(tg_comp_consts), intent(in) :: cn
+      real(c_double), intent(inout) :: o2_upd(*), o1_upd(*), he_upd(*)
+      integer(c_int), value :: nk, ncol
+    end function tg_comp_ng
+
+    integer(c_int) function tg_comp_post_ng(o2, o1, he, o2_nm, o1_nm, he_nm, xnmbar, zpmid, dz, dtsmooth, &
+        dtsmooth_div2, nk, ncol, o2_upd, o1_upd, he_upd, o2nm_upd, o1nm_upd, henm_upd) bind(C, name="tg_comp_post_ng")
+      import :: c_int, c_double
+      real(c_double), intent(in) :: o2(*), o1(*), he(*), o2_nm(*), o1_nm(*), he_nm(*), xnmbar(*), zpmid(*)
+      real(c_double), value :: dz, dtsmooth, dtsmooth_div2
+      integer(c_int), value :: nk, ncol
+      real(c_double), intent(inout) :: o2_upd(*), o1_upd(*), he_upd(*), o2nm_upd(*), o1nm_upd(*), henm_upd(*)
+    end function tg_comp_post_ng
+
+    integer(c_int) function tg_settei_ng(fl, cn, te_out, ti_out, qtotal, nk, ncol) bind(C, name="tg_settei_ng")
+      import :: c_int, c_double, tg_settei_fields, tg_settei_consts
+      type(tg_settei_fields), intent(in) :: fl
+      type(tg_settei_consts), intent(in) :: cn
+      real(c_double), intent(inout) :: te_out(*), ti_out(*), qtotal(*)
+      integer(c_int), value :: nk, ncol
+    end function tg_settei_ng
+
+    ! Fe and Fn may be c_null_ptr (both or neither)
+    integer(c_int) function tg_oplus_ng(fl, cn, opout, xiop2p, xiop2d, fe, fn, nk, ncol) bind(C, name="tg_oplus_ng")
+      import :: c_int, c_double, c_ptr, tg_oplus_fields, tg_oplus_consts
+      type(tg_oplus_fields), intent(in) :: fl
+      type(tg_oplus_consts), intent(in) :: cn
+      real(c_double), intent(inout) :: opout(*), xiop2p(*), xiop2d(*)
+      type(c_ptr), value :: fe, fn
+      integer(c_int), value :: nk, ncol
+    end function tg_oplus_ng
   end interface
 end module tg_colsolve_mod
