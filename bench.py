@@ -314,7 +314,7 @@ def run_profile(args):
     prec = cs.TG_PREC_F64 if parts[1] == "f64" else cs.TG_PREC_F32_REFINE
     if len(parts) > 2:
         v = parts[2]
-        cand = (v, int(parts[3]), int(parts[4]) if len(parts) > 4 else 4, 4) if v in ("ring", "ringg") else \
+        cand = (v, int(parts[3]), int(parts[4]) if len(parts) > 4 else 4, 4) if v in ("ring", "ringg", "rows") else \
             (v, int(parts[3]), int(parts[4]), int(parts[5]) if len(parts) > 5 else 4)
         autotune.apply(kind, prec, cand)
     dw = pkg.batch.DeviceWorkload(wl, "cuda", max_sub=args.max_sub)

@@ -419,6 +419,11 @@ int tg_set_scratch_global(int kind, int precision, int on);
  * on: 1 (default), 0 off, -1 back to the default. */
 int tg_set_cache_hints(int on);
 
+/* FP64 block kinds with a bulk-copy ring: one lane per block row (B lanes per
+ * column, whole blocks exchanged by warp shuffles) instead of one lane per
+ * column.  Same arithmetic, bit-identical results.  on: 1, 0, -1 default. */
+int tg_set_block_rows(int kind, int on);
+
 /* Runs the ring kernels' bounded mbarrier wait on a barrier that nothing
  * completes, giving up after `polls` polls (1..2^22): *status_dev receives
  * TG_ETIMEOUT, as a solve does when a bulk copy never lands.  Tests the

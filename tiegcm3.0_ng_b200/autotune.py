@@ -8,7 +8,8 @@ from a CUDA graph, CUDA-event timed) and keeps the fastest:
             prefetch depth, w2 scratch in shared memory ("reg") or global
             memory ("regg")
             bulk-copy ring kernel: staging depth 4, 8 or 16 levels, w2 in shared
-            ("ring") or global ("ringg") memory
+            ("ring") or global ("ringg") memory; for block kinds also one lane
+            per block row ("rows", depth 4 or 8)
   FP32+ref  columns per block x prefetch depth
 
 Results are cached in a JSON file keyed by GPU name, kind, precision, level
@@ -30,7 +31,8 @@ SCALAR_F64 = [("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg"
               ("ringg", 4, 1, 4), ("ringg", 8, 1, 4), ("ringg", 4, 2, 4), ("ringg", 4, 4, 4), ("ringg", 4, 8, 4)]
 BLOCK_F64 = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 96, 1, 4),
              ("ring", 4, 4, 4), ("ring", 8, 4, 4), ("ring", 4, 2, 4), ("ring", 8, 2, 4), ("ring", 16, 2, 4),
-             ("ring", 4, 1, 4)]
+             ("ring", 4, 1, 4), ("rows", 4, 1, 4), ("rows", 4, 2, 4), ("rows", 4, 4, 4), ("rows", 8, 1, 4),
+             ("rows", 8, 2, 4)]
 SCALAR_REF = [("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg", 64, 1, 8)]
 BLOCK_REF = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4)]
 
@@ -47,7 +49,9 @@ def apply(kind, precision, cand):
     scalar64 = kind == cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64
     if kind == cs.TG_KIND_SCALAR:
         cs.set_prefetch(kind, precision, pf)
-    if v in ("ring", "ringg"):
+    elif precision == cs.TG_PREC_F64:
+        cs.set_block_rows(kind, 1 if v == "rows" else 0)
+    if v in ("ring", "ringg", "rows"):
         cs.set_pipeline(kind, precision, p1, p2)    # ring depth, warps per CTA
     else:
         if precision == cs.TG_PREC_F64:
@@ -64,6 +68,8 @@ def reset(kind, precision):
         cs.set_prefetch(kind, precision, -1)
     if kind == cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64:
         cs.set_scratch_global(kind, precision, -1)
+    if kind != cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64:
+        cs.set_block_rows(kind, -1)
 
 
 def key(gpu, kind, precision, nk, ncol):

@@ -41,7 +41,7 @@ EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor
            "tg_comp_ng_dev", "tg_comp_post_ng", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
-           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
+           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
 
 
@@ -219,6 +219,7 @@ def lib():
             "tg_plan_launches": [P],
             "tg_plan_describe": [P, ctypes.c_char_p, I],
             "tg_set_cache_hints": [I],
+            "tg_set_block_rows": [I, I],
             "tg_selftest_wait": [ctypes.c_uint, P, P],
             "tg_plan_sweep_histogram": [P, ctypes.POINTER(Lg), I],
             "tg_plan_destroy": [P],
@@ -592,6 +593,11 @@ def selftest_division(a, b, q, stream=None):
 def set_cache_hints(on):
     """L2 eviction-priority hints of the ring kernels (1 on, 0 off, -1 default)."""
     return _check(lib().tg_set_cache_hints(int(on)), "tg_set_cache_hints")
+
+
+def set_block_rows(kind, on):
+    """FP64 block ring kernel with one lane per block row (1 on, 0 off, -1 default)."""
+    return _check(lib().tg_set_block_rows(int(kind), int(on)), "tg_set_block_rows")
 
 
 def selftest_wait(polls, status, stream=None):

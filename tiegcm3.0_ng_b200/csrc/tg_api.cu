@@ -1417,6 +1417,16 @@ __attribute__((visibility("default"))) int tg_selftest_wait(unsigned polls, int 
     return TG_OK;
 }
 
+__attribute__((visibility("default"))) int tg_set_block_rows(int kind, int on)
+{
+    if (kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) {
+        set_err("tg_set_block_rows: kind must be TG_KIND_BLOCK2 or TG_KIND_BLOCK3");
+        return TG_EINVAL;
+    }
+    tg::set_block_rows(kind, on);
+    return TG_OK;
+}
+
 __attribute__((visibility("default"))) int tg_set_cache_hints(int on)
 {
     tg::set_cache_hints(on);

@@ -59,6 +59,7 @@ struct Shape {
     int w2g;            // scalar register kernel with w2 in global scratch
     int pf;             // scalar register kernels: prefetch depth in levels
     size_t smem;        // dynamic shared memory bytes
+    int rows;           // block ring kernel with one lane per block row
 };
 
 // Register-prefetch kernel shape of a kind/precision (tg_set_tile).
@@ -85,7 +86,7 @@ size_t scalar_scratch_bytes(long slots, int k2max);
 
 // Shared memory / scratch needs of a kernel for the largest k2 it will see.
 size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g);
-size_t block_smem_bytes(int B, int stages, int threads);
+size_t block_smem_bytes(int B, int stages, int threads, int rows);
 // Global scratch (bytes) of a block kernel with `slots` resident threads.
 size_t block_scratch_bytes(int B, int precision, long slots, int k2max);
 
@@ -156,6 +157,10 @@ cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *
 int oplus_scratch_planes();   // level-major scratch planes of launch_oplus_ng (each nk*ld doubles)
 
 cudaError_t launch_selftest_wait(unsigned polls, unsigned *status, cudaStream_t st);
+
+// Block kinds: the bulk-copy ring kernel with one lane per block row
+// (tg_set_block_rows); 1 on, 0 off, -1 default.
+void set_block_rows(int kind, int on);
 
 // L2 cache-policy hints of the bulk-copy ring kernels (tg_set_cache_hints).
 int cache_hints();

@@ -220,11 +220,11 @@ __device__ __forceinline__ bool mbar_wait_warp(unsigned long long *bar, uint32_t
     return __all_sync(0xffffffffu, done);
 }
 
-// Stage ring of a single-warp CTA: level k of NE arrays (32 columns x 8 B =
-// 256 B each) lands in stage (q % D), q the running level counter of the CTA.
-template <int NE, int D>
+// Stage ring of a single-warp CTA: level k of NE arrays (W columns x 8 B
+// each) lands in stage (q % D), q the running level counter of the CTA.
+template <int NE, int D, int W = 32>
 struct Ring {
-    double *buf;                 // D * NE * 32 doubles
+    double *buf;                 // D * NE * W doubles
     unsigned long long *bar;     // D mbarriers
     unsigned long long pol;      // L2 policy of the fills
     __device__ __forceinline__ void init(int lane)
@@ -240,14 +240,14 @@ struct Ring {
     __device__ __forceinline__ void issue(unsigned q, const double *src_e, int lane)
     {
         const int st = (int)(q % D);
-        if (lane == 0) mbar_expect(&bar[st], NE * 256u);
+        if (lane == 0) mbar_expect(&bar[st], NE * W * 8u);
         __syncwarp();
-        if (lane < NE) bulk_load_hint(buf + (st * NE + lane) * 32, src_e, 256u, &bar[st], pol);
+        if (lane < NE) bulk_load_hint(buf + (st * NE + lane) * W, src_e, W * 8u, &bar[st], pol);
     }
     __device__ __forceinline__ bool wait(unsigned q) { return mbar_wait_warp(&bar[q % D], (q / D) & 1u); }
-    __device__ __forceinline__ double at(unsigned q, int e, int lane) const
+    __device__ __forceinline__ double at(unsigned q, int e, int c) const
     {
-        return buf[((int)(q % D) * NE + e) * 32 + lane];
+        return buf[((int)(q % D) * NE + e) * W + c];
     }
     // After a timeout: bounded wait for the fills still in flight (q0..q1-1).
     __device__ __forceinline__ void drain(unsigned q0, unsigned q1)
@@ -1099,6 +1099,224 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
 }
 
 // ---------------------------------------------------------------------------
+// Block-tridiagonal Thomas, FP64, bit-exact, one lane per block row.  The
+// block recurrence of a single column is a long chain of dependent FP64
+// operations (about 400 warp instructions per level for B = 2 with one lane
+// per column), and a 2.5 deg grid has only ~2 such warps per SM, so the
+// single-lane kernel runs at the latency of that chain.  Here the B rows of a
+// column go to B lanes of a group of G lanes (G = 2 for B = 2, 4 for B = 3
+// with one helper lane), a warp covers 32/G columns, and each lane computes
+// its row of Q' = Q - P Gamma, of W = inv(Q') (the determinant and cofactors
+// redundantly, its own B divisions), of z and of Gamma; whole rows, blocks
+// and vectors are exchanged by shuffles within the group.  Every element is
+// formed by the same operations in the same order as blk_f64_col, so the
+// result is bit-identical.  Coefficients arrive through the bulk-copy ring
+// (entries of 32/G columns), Gamma goes to the column's L2 scratch slot, z is
+// parked in u.
+// ---------------------------------------------------------------------------
+template <int B, int D>
+__global__ void __launch_bounds__(256) k_block_f64_rows(SegTable tab, double *scratch, unsigned *status)
+{
+    constexpr int BB = B * B, NE = 3 * BB + B, G = B == 2 ? 2 : 4, W = 32 / G;
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ __align__(8) unsigned long long bars[8 * D];
+    extern __shared__ __align__(128) double smem_b[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int c = lane / G, ri = lane % G, base = lane - ri;
+    const int i = ri < B ? ri : B - 1;       // the helper lane of B = 3 mirrors row B-1
+    const bool row_lane = ri < B;
+    const unsigned gmask = ((1u << G) - 1u) << base;
+    Ring<NE, D, W> ring{smem_b + (long)warp * D * NE * W, bars + warp * D, l2_policy(tab.hints, false)};
+    const unsigned long long keep = l2_policy(tab.hints, true);
+    ring.init(lane);
+    const long gs = (long)gridDim.x * nwarps * W;
+    double *gam = scratch + ((long)blockIdx.x * nwarps + warp) * W + c;
+    unsigned q = 0;
+    const int nvt = tab.ntiles * G;          // sub-tiles of W columns
+    for (int vt = blockIdx.x * nwarps + warp; vt < nvt; vt += gridDim.x * nwarps) {
+        const int t = vt / G, sub = vt % G;
+        const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
+        const long col0 = (long)(t - s.tile0) * 32 + (long)sub * W;
+        if (col0 >= s.ncol) continue;        // uniform across the warp
+        const long ld = s.ld;
+        const int k2 = s.k2;
+        const bool valid = col0 + c < s.ncol;
+        const double *src = s.a + col0;
+        long lstride = 0;
+        if (lane < BB) {
+            src = s.a + col0 + lane * ld;
+            lstride = BB * ld;
+        } else if (lane < 2 * BB) {
+            src = s.b + col0 + (lane - BB) * ld;
+            lstride = BB * ld;
+        } else if (lane < 3 * BB) {
+            src = s.c + col0 + (lane - 2 * BB) * ld;
+            lstride = BB * ld;
+        } else if (lane < NE) {
+            src = s.f + col0 + (lane - 3 * BB) * ld;
+            lstride = B * ld;
+        }
+        double *pU = s.x + col0 + c;
+        const int pre = k2 < D ? k2 : D;
+        for (int j = 0; j < pre; ++j) ring.issue(q + j, src + j * lstride, lane);
+        bool ok = true;
+        double Gf[BB], z[B];
+        for (int k = 0; k < k2; ++k) {
+            const unsigned qk = q + k;
+            if (!ring.wait(qk)) {
+                ring.drain(qk, q + (k + D < k2 ? k + D : k2));
+                if (lane == 0) report(status, s.status_idx, FLAG_TIMEOUT);
+                return;
+            }
+            double P[B], Qr[B], R[BB], fi;
+#pragma unroll
+            for (int n = 0; n < B; ++n) {
+                P[n] = ring.at(qk, i + B * n, c);
+                Qr[n] = ring.at(qk, BB + i + B * n, c);
+            }
+#pragma unroll
+            for (int e = 0; e < BB; ++e) R[e] = ring.at(qk, 2 * BB + e, c);
+            fi = ring.at(qk, 3 * BB + i, c);
+            __syncwarp();
+            fence_proxy_async();
+            if (k + D < k2) ring.issue(qk + D, src + (k + D) * lstride, lane);
+            // row i of Q' = Q - P Gamma, then the whole Q' of the column
+            double Qp[B];
+#pragma unroll
+            for (int m = 0; m < B; ++m) {
+                double qv = Qr[m];
+                if (k > 0) {
+#pragma unroll
+                    for (int n = 0; n < B; ++n) qv = xsub(qv, xmul(P[n], Gf[n + B * m]));
+                }
+                Qp[m] = qv;
+            }
+            double A[BB];
+#pragma unroll
+            for (int n = 0; n < B; ++n)
+#pragma unroll
+                for (int m = 0; m < B; ++m) A[n + B * m] = __shfl_sync(FULL, Qp[m], base + n);
+            // row i of W = inv(Q') (inv_exact's operations)
+            double d, Wn[B];
+            if (B == 2) {
+                d = xsub(xmul(A[0], A[3]), xmul(A[2], A[1]));
+                Wn[0] = i == 0 ? A[3] : -A[1];
+                Wn[1] = i == 0 ? -A[2] : A[0];
+            } else {
+#define a_(r, q2) A[((r) - 1) + 3 * ((q2) - 1)]
+                d = xmul(xmul(a_(1, 1), a_(2, 2)), a_(3, 3));
+                d = xsub(d, xmul(xmul(a_(1, 1), a_(2, 3)), a_(3, 2)));
+                d = xsub(d, xmul(xmul(a_(1, 2), a_(2, 1)), a_(3, 3)));
+                d = xadd(d, xmul(xmul(a_(1, 2), a_(2, 3)), a_(3, 1)));
+                d = xadd(d, xmul(xmul(a_(1, 3), a_(2, 1)), a_(3, 2)));
+                d = xsub(d, xmul(xmul(a_(1, 3), a_(2, 2)), a_(3, 1)));
+                double w[9];
+                w[0] = xsub(xmul(a_(2, 2), a_(3, 3)), xmul(a_(2, 3), a_(3, 2)));
+                w[1] = -xsub(xmul(a_(2, 1), a_(3, 3)), xmul(a_(2, 3), a_(3, 1)));
+                w[2] = xsub(xmul(a_(2, 1), a_(3, 2)), xmul(a_(2, 2), a_(3, 1)));
+                w[3] = -xsub(xmul(a_(1, 2), a_(3, 3)), xmul(a_(1, 3), a_(3, 2)));
+                w[4] = xsub(xmul(a_(1, 1), a_(3, 3)), xmul(a_(1, 3), a_(3, 1)));
+                w[5] = -xsub(xmul(a_(1, 1), a_(3, 2)), xmul(a_(1, 2), a_(3, 1)));
+                w[6] = xsub(xmul(a_(1, 2), a_(2, 3)), xmul(a_(1, 3), a_(2, 2)));
+                w[7] = -xsub(xmul(a_(1, 1), a_(2, 3)), xmul(a_(1, 3), a_(2, 1)));
+                w[8] = xsub(xmul(a_(1, 1), a_(2, 2)), xmul(a_(1, 2), a_(2, 1)));
+#undef a_
+#pragma unroll
+                for (int m = 0; m < B; ++m) Wn[m] = i == 0 ? w[3 * m] : (i == 1 ? w[1 + 3 * m] : w[2 + 3 * m]);
+            }
+            const double y = __drcp_rn(d);
+            double Wr[B];
+#pragma unroll
+            for (int m = 0; m < B; ++m) Wr[m] = qdiv(Wn[m], d, y);
+            ok = finite_nz(d) && ok;
+            // v = f - P z (row i), z' = W v (row i), then the whole z'
+            double vi = fi;
+            if (k > 0) {
+#pragma unroll
+                for (int m = 0; m < B; ++m) vi = xsub(vi, xmul(P[m], z[m]));
+            }
+            double v[B];
+#pragma unroll
+            for (int n = 0; n < B; ++n) v[n] = __shfl_sync(FULL, vi, base + n);
+            double zi = xmul(Wr[0], v[0]);
+#pragma unroll
+            for (int m = 1; m < B; ++m) zi = xadd(zi, xmul(Wr[m], v[m]));
+#pragma unroll
+            for (int n = 0; n < B; ++n) z[n] = __shfl_sync(FULL, zi, base + n);
+            if (valid && row_lane) st_hint(&pU[((long)k * B + i) * ld], zi, keep);
+            if (k < k2 - 1) {
+                double Gr[B];
+#pragma unroll
+                for (int m = 0; m < B; ++m) {
+                    double g = xmul(Wr[0], R[B * m]);
+#pragma unroll
+                    for (int n = 1; n < B; ++n) g = xadd(g, xmul(Wr[n], R[n + B * m]));
+                    Gr[m] = g;
+                    if (valid && row_lane) st_hint(&gam[((long)k * BB + i + B * m) * gs], g, keep);
+                }
+#pragma unroll
+                for (int n = 0; n < B; ++n)
+#pragma unroll
+                    for (int m = 0; m < B; ++m) Gf[n + B * m] = __shfl_sync(FULL, Gr[m], base + n);
+            }
+        }
+        q += k2;
+        // back sweep u_k = z_{k+1} - Gamma_{k+1} u_{k+1}, row i per lane;
+        // the loads of the next BPF levels stay in flight
+        constexpr int BPF = 4;
+        bool fin = true;
+        double un[B];
+#pragma unroll
+        for (int m = 0; m < B; ++m) un[m] = z[m];
+        const double top = z[i];
+        fin = fabs(top) <= DBL_MAX;
+        double rz[BPF], rg[BPF][B];
+#pragma unroll
+        for (int u = 0; u < BPF; ++u) {
+            const int k = k2 - 2 - u;
+            if (k >= 0 && valid) {
+                rz[u] = pU[((long)k * B + i) * ld];
+#pragma unroll
+                for (int m = 0; m < B; ++m) rg[u][m] = gam[((long)k * BB + i + B * m) * gs];
+            } else {
+                rz[u] = 0.0;
+#pragma unroll
+                for (int m = 0; m < B; ++m) rg[u][m] = 0.0;
+            }
+        }
+        for (int kb = k2 - 2; kb >= 0; kb -= BPF) {
+#pragma unroll
+            for (int u = 0; u < BPF; ++u) {
+                const int k = kb - u;
+                if (k >= 0) {
+                    double t = rz[u];
+#pragma unroll
+                    for (int m = 0; m < B; ++m) t = xsub(t, xmul(rg[u][m], un[m]));
+                    fin = fin && fabs(t) <= DBL_MAX;
+                    const int kn = k - BPF;
+                    if (kn >= 0 && valid) {
+                        rz[u] = pU[((long)kn * B + i) * ld];
+#pragma unroll
+                        for (int m = 0; m < B; ++m) rg[u][m] = gam[((long)kn * BB + i + B * m) * gs];
+                    }
+#pragma unroll
+                    for (int n = 0; n < B; ++n) un[n] = __shfl_sync(FULL, t, base + n);
+                    if (valid && row_lane) pU[((long)k * B + i) * ld] = t;
+                }
+            }
+        }
+        if (s.ubc_ratio && valid) {
+            double tv = xmul(__ldg(s.ubc_ratio + i * ld + col0 + c), top);
+            if (s.ubc_add) tv = xadd(tv, __ldg(s.ubc_add + i * ld + col0 + c));
+            fin = fin && fabs(tv) <= DBL_MAX;
+            if (row_lane) pU[((long)k2 * B + i) * ld] = tv;
+        }
+        const unsigned bad = __ballot_sync(FULL, !(fin || !row_lane)) & gmask;
+        if (valid && ri == 0) report(status, s.status_idx, (ok ? 0u : FLAG_PIVOT) | (bad ? FLAG_NONFINITE : 0u));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Block-tridiagonal, FP32 Gamma/z sweeps + FP64 iterative refinement.
 // Pivot blocks Q' = Q - P G and their inverses W stay in FP64; W and
 // G_{k+1} = W R are kept in FP32 in the thread's scratch slots together with
@@ -1536,6 +1754,7 @@ struct TileCfg {
     int w2g;               // scalar register kernel: w2 in global scratch instead of shared memory
     int pf;                // scalar register kernels: levels of coefficient loads in flight per column
     int wpb;               // ring kernels: independent warps (32-column tiles) per CTA
+    int rows;              // block ring kernels: one lane per block row (k_block_f64_rows)
 };
 // [kind index: scalar, block2, block3][precision]
 // Defaults: the fastest shapes on the 2.5 deg column step (10368 x 57) on a
@@ -1543,12 +1762,12 @@ struct TileCfg {
 // per CTA, w2 in global scratch; 2x2 block ring of depth 4, one warp per CTA;
 // 3x3 block register kernel of 128 threads; refinement kernels 64 threads
 // (scalar, prefetch 8), 64 (2x2) and 128 (3x3).
-const TileCfg kDefaultTile[3][2] = {{{256, 1, 4, 1, 4, 1}, {64, 1, 0, 0, 8, 4}},
-                                     {{64, 1, 4, 0, 4, 1}, {64, 1, 0, 0, 4, 4}},
-                                     {{128, 1, 0, 0, 4, 4}, {128, 1, 0, 0, 4, 4}}};
-TileCfg g_tile[3][2] = {{{256, 1, 4, 1, 4, 1}, {64, 1, 0, 0, 8, 4}},
-                        {{64, 1, 4, 0, 4, 1}, {64, 1, 0, 0, 4, 4}},
-                        {{128, 1, 0, 0, 4, 4}, {128, 1, 0, 0, 4, 4}}};
+const TileCfg kDefaultTile[3][2] = {{{256, 1, 4, 1, 4, 1, 0}, {64, 1, 0, 0, 8, 4, 0}},
+                                     {{64, 1, 4, 0, 4, 1, 0}, {64, 1, 0, 0, 4, 4, 0}},
+                                     {{128, 1, 0, 0, 4, 4, 0}, {128, 1, 0, 0, 4, 4, 0}}};
+TileCfg g_tile[3][2] = {{{256, 1, 4, 1, 4, 1, 0}, {64, 1, 0, 0, 8, 4, 0}},
+                        {{64, 1, 4, 0, 4, 1, 0}, {64, 1, 0, 0, 4, 4, 0}},
+                        {{128, 1, 0, 0, 4, 4, 0}, {128, 1, 0, 0, 4, 4, 0}}};
 int kind_index(int kind) { return kind == TG_KIND_SCALAR ? 0 : (kind == TG_KIND_BLOCK2 ? 1 : 2); }
 int g_num_sms = -1;
 int g_smem_optin = -1;
@@ -1629,6 +1848,23 @@ cudaError_t with_block_ring(int B, int D, F f)
     }
 }
 
+template <typename F>
+cudaError_t with_block_rows(int B, int D, F f)
+{
+    if (B == 2) {
+        switch (D) {
+        case 4: return f(k_block_f64_rows<2, 4>);
+        case 8: return f(k_block_f64_rows<2, 8>);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (D) {
+    case 4: return f(k_block_f64_rows<3, 4>);
+    case 8: return f(k_block_f64_rows<3, 8>);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 template <typename K>
 void allow_smem(K k, int lim)
 {
@@ -1658,6 +1894,8 @@ int num_sms()
         allow_smem(k_block_f64_ring<3, 4>, lim);
         allow_smem(k_block_f64_ring<3, 8>, lim);
         allow_smem(k_block_f64_ring<3, 16>, lim);
+        for (int d : {4, 8})
+            for (int b : {2, 3}) with_block_rows(b, d, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
     }
     return g_num_sms;
 }
@@ -1754,6 +1992,18 @@ void set_stages(int kind, int precision, int stages, int wpb)
     t.wpb = wpb > 0 ? wpb : d.wpb;
 }
 int ring_warps(int kind, int precision) { return g_tile[kind_index(kind)][precision ? 1 : 0].wpb; }
+void set_block_rows(int kind, int on)
+{
+    if (kind == TG_KIND_SCALAR) return;
+    TileCfg &t = g_tile[kind_index(kind)][0];
+    t.rows = on < 0 ? kDefaultTile[kind_index(kind)][0].rows : (on ? 1 : 0);
+}
+static int block_rows(int kind, int precision)
+{
+    return kind != TG_KIND_SCALAR && precision == TG_PREC_F64 && g_tile[kind_index(kind)][0].rows;
+}
+// lanes per column of the row kernel
+static int rows_group(int B) { return B == 2 ? 2 : 4; }
 
 size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g)
 {
@@ -1764,9 +2014,10 @@ size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int sta
     return (size_t)threads * 3 * (size_t)k2max * 4;
 }
 
-size_t block_smem_bytes(int B, int stages, int threads)
+size_t block_smem_bytes(int B, int stages, int threads, int rows)
 {
-    return stages > 0 ? (size_t)threads / 32 * stages * (3 * B * B + B) * 32 * 8 : 0;
+    const int w = rows ? 32 / rows_group(B) : 32;
+    return stages > 0 ? (size_t)threads / 32 * stages * (3 * B * B + B) * w * 8 : 0;
 }
 
 size_t block_scratch_bytes(int B, int precision, long slots, int k2max)
@@ -1786,17 +2037,20 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     sh->stages = stages;
     sh->w2g = w2g;
     sh->pf = prefetch_depth(kind, precision);
+    sh->rows = stages > 0 ? block_rows(kind, precision) : 0;
+    if (sh->rows && stages > 8) stages = sh->stages = 8;
     if (kind == TG_KIND_SCALAR && sh->cpt == 2 && sh->pf > 8) sh->pf = 8;
     if (stages > 0) {
         // a ring that does not fit in shared memory falls back to the
         // register-prefetch kernel with the same 32-column tile
         const size_t need = kind == TG_KIND_SCALAR ? scalar_smem_bytes(precision, sh->threads, 1, k2max, stages, w2g)
-                                                   : block_smem_bytes(kind, stages, sh->threads);
+                                                   : block_smem_bytes(kind, stages, sh->threads, sh->rows);
         if (need > (size_t)(g_smem_optin - 1024)) {
             stages = 0;
             sh->stages = 0;
             sh->threads = 32;
             sh->cpt = 1;
+            sh->rows = 0;
         }
     }
     if (kind == TG_KIND_SCALAR) {
@@ -1813,9 +2067,11 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
             e = with_scalar_refine(sh->pf, occ);
     } else {
         const int B = kind;
-        sh->smem = block_smem_bytes(B, stages, sh->threads);
+        sh->smem = block_smem_bytes(B, stages, sh->threads, sh->rows);
         if (sh->smem > (size_t)(g_smem_optin - 1024)) return cudaErrorInvalidConfiguration;
-        if (stages > 0)
+        if (stages > 0 && sh->rows)
+            e = with_block_rows(B, stages, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
+        else if (stages > 0)
             e = with_block_ring(B, stages, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
         else if (precision == TG_PREC_F64)
             e = B == 2 ? occupancy(k_block_f64<2>, sh->threads, 0, &per_sm)
@@ -1832,7 +2088,8 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     long blocks = (long)per_sm * nsm;
-    const long units = stages > 0 ? (ntiles + sh->threads / 32 - 1) / (sh->threads / 32) : ntiles;
+    const long vt = sh->rows ? (long)ntiles * rows_group(kind) : ntiles;   // warp tiles
+    const long units = stages > 0 ? (vt + sh->threads / 32 - 1) / (sh->threads / 32) : ntiles;
     if (blocks > units) blocks = units;
     sh->blocks = (int)(blocks > 0 ? blocks : 1);
     return cudaSuccess;
@@ -1878,7 +2135,15 @@ cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape 
                          double *scratch, unsigned *status, unsigned long long *hist, cudaStream_t st)
 {
     if (tab.ntiles <= 0) return cudaSuccess;
-    if (precision == TG_PREC_F64 && sh.stages > 0) {
+    if (precision == TG_PREC_F64 && sh.stages > 0 && sh.rows) {
+        SegTable t = tab;
+        t.hints = cache_hints();
+        cudaError_t e = with_block_rows(B, sh.stages, [&](auto k) {
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, scratch, status);
+            return cudaSuccess;
+        });
+        if (e != cudaSuccess) return e;
+    } else if (precision == TG_PREC_F64 && sh.stages > 0) {
         SegTable t = tab;
         t.hints = cache_hints();
         cudaError_t e = with_block_ring(B, sh.stages, [&](auto k) {
