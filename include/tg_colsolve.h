@@ -424,6 +424,28 @@ int tg_set_cache_hints(int on);
  * column.  Same arithmetic, bit-identical results.  on: 1, 0, -1 default. */
 int tg_set_block_rows(int kind, int on);
 
+/* FP64 block kinds with a bulk-copy ring: columns per warp, 32 (default), 16
+ * or 8 (other values restore the default).  Fewer columns per warp means more
+ * warps for the same columns, which helps when a grid has too few columns to
+ * hide the latency of the block recurrence.  Same arithmetic, same bits. */
+int tg_set_block_width(int kind, int width);
+
+/* Scalar FP64 bulk-copy ring with w2 in global scratch: levels per ring stage
+ * (1, 2, 4 or 8; other values restore the default).  With L > 1 one mbarrier
+ * wait and one round of copies serve L levels; the ring depth set by
+ * tg_set_pipeline then counts stages of L levels (2, 3 or 4). */
+int tg_set_stage_levels(int kind, int precision, int levels);
+
+/* Fused assembly routines: 1 (default) two passes where built, the level
+ * quantities with one thread per (level, column) then the column walk; 0 one
+ * fused column walk.  Same operations, same results. */
+int tg_set_assembly_mode(int mode);
+
+/* Block kinds: the L2 budget for the Gamma scratch of all resident warps of
+ * the block kernels, in MB (default 96; <= 0 restores it).  It caps how many
+ * columns are in flight at once on large batches. */
+int tg_set_block_scratch_budget(double megabytes);
+
 /* Runs the ring kernels' bounded mbarrier wait on a barrier that nothing
  * completes, giving up after `polls` polls (1..2^22): *status_dev receives
  * TG_ETIMEOUT, as a solve does when a bulk copy never lands.  Tests the

@@ -51,16 +51,23 @@ def _rel(got, want):
 MINOR_TOL = 1e-12
 
 
+@pytest.fixture(params=[1, 0], ids=["two_pass", "fused"])
+def assembly_mode(request, pkg):
+    pkg.set_assembly_mode(request.param)
+    yield request.param
+    pkg.set_assembly_mode(-1)
+
+
 @pytest.mark.parametrize("nk,dz,ncol", [(57, 0.25, 3001), (29, 0.5, 2592), (113, 0.125, 500), (3, 0.5, 33),
                                         (300, 0.05, 70)])
-def test_minor_ng_host(cuda, pkg, orc, nk, dz, ncol):
+def test_minor_ng_host(cuda, pkg, orc, nk, dz, ncol, assembly_mode):
     F, C = pkg.synth.minor_inputs(nk, ncol, dz, 9 + nk)
     out = np.zeros((nk, ncol), order="F")
     assert pkg.minor_ng(F, C, out) == pkg.TG_OK
     assert _rel(out, orc.minor_ng(F, C)) <= MINOR_TOL
 
 
-def test_minor_ng_device_system_and_solution(cuda, pkg, orc):
+def test_minor_ng_device_system_and_solution(cuda, pkg, orc, assembly_mode):
     torch = cuda
     nk, ncol, dz = 57, 1000, 0.25
     F, C = pkg.synth.minor_inputs(nk, ncol, dz, 4)

@@ -9,7 +9,9 @@ from a CUDA graph, CUDA-event timed) and keeps the fastest:
             memory ("regg")
             bulk-copy ring kernel: staging depth 4, 8 or 16 levels, w2 in shared
             ("ring") or global ("ringg") memory; for block kinds also one lane
-            per block row ("rows", depth 4 or 8)
+            per block row ("rows", depth 4 or 8) and 16 or 8 columns per warp
+            ("ring16", "ring8"); for the scalar kind a ring of stages holding 2, 4
+            or 8 levels each ("chunk2", "chunk4", "chunk8")
   FP32+ref  columns per block x prefetch depth
 
 Results are cached in a JSON file keyed by GPU name, kind, precision, level
@@ -28,11 +30,13 @@ SCALAR_F64 = [("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg"
               ("reg", 128, 1, 16), ("reg", 128, 2, 4), ("reg", 256, 2, 4), ("reg", 128, 2, 8),
               ("regg", 256, 1, 4), ("regg", 128, 1, 8), ("regg", 128, 1, 16),
               ("ring", 4, 4, 4), ("ring", 8, 4, 4), ("ring", 4, 2, 4),
-              ("ringg", 4, 1, 4), ("ringg", 8, 1, 4), ("ringg", 4, 2, 4), ("ringg", 4, 4, 4), ("ringg", 4, 8, 4)]
+              ("ringg", 4, 1, 4), ("ringg", 8, 1, 4), ("ringg", 4, 2, 4), ("ringg", 4, 4, 4), ("ringg", 4, 8, 4),
+              ("chunk2", 4, 1, 4), ("chunk4", 2, 1, 4), ("chunk4", 3, 1, 4), ("chunk4", 4, 1, 4), ("chunk8", 2, 1, 4),
+              ("chunk4", 2, 2, 4)]
 BLOCK_F64 = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 96, 1, 4),
              ("ring", 4, 4, 4), ("ring", 8, 4, 4), ("ring", 4, 2, 4), ("ring", 8, 2, 4), ("ring", 16, 2, 4),
-             ("ring", 4, 1, 4), ("rows", 4, 1, 4), ("rows", 4, 2, 4), ("rows", 4, 4, 4), ("rows", 8, 1, 4),
-             ("rows", 8, 2, 4)]
+             ("ring", 4, 1, 4), ("ring16", 4, 1, 4), ("ring16", 8, 1, 4), ("ring16", 4, 2, 4), ("ring8", 4, 1, 4),
+             ("ring8", 8, 1, 4), ("ring8", 4, 2, 4), ("rows", 4, 1, 4), ("rows", 4, 2, 4), ("rows", 8, 1, 4)]
 SCALAR_REF = [("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg", 64, 1, 8)]
 BLOCK_REF = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4)]
 
@@ -49,16 +53,19 @@ def apply(kind, precision, cand):
     scalar64 = kind == cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64
     if kind == cs.TG_KIND_SCALAR:
         cs.set_prefetch(kind, precision, pf)
+        if precision == cs.TG_PREC_F64:
+            cs.set_stage_levels(kind, precision, int(v[5:]) if v.startswith("chunk") else 1)
     elif precision == cs.TG_PREC_F64:
         cs.set_block_rows(kind, 1 if v == "rows" else 0)
-    if v in ("ring", "ringg", "rows"):
+        cs.set_block_width(kind, {"ring16": 16, "ring8": 8}.get(v, 32))
+    if v in ("ring", "ringg", "rows", "ring16", "ring8") or v.startswith("chunk"):
         cs.set_pipeline(kind, precision, p1, p2)    # ring depth, warps per CTA
     else:
         if precision == cs.TG_PREC_F64:
             cs.set_pipeline(kind, precision, 0)
         cs.set_tile(kind, precision, p1, p2)
     if scalar64:
-        cs.set_scratch_global(kind, precision, 1 if v in ("regg", "ringg") else 0)
+        cs.set_scratch_global(kind, precision, 1 if v in ("regg", "ringg") or v.startswith("chunk") else 0)
 
 
 def reset(kind, precision):
@@ -68,8 +75,10 @@ def reset(kind, precision):
         cs.set_prefetch(kind, precision, -1)
     if kind == cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64:
         cs.set_scratch_global(kind, precision, -1)
+        cs.set_stage_levels(kind, precision, 0)
     if kind != cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64:
         cs.set_block_rows(kind, -1)
+        cs.set_block_width(kind, 0)
 
 
 def key(gpu, kind, precision, nk, ncol):

@@ -41,7 +41,7 @@ EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor
            "tg_comp_ng_dev", "tg_comp_post_ng", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
-           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
+           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
 
 
@@ -220,6 +220,10 @@ def lib():
             "tg_plan_describe": [P, ctypes.c_char_p, I],
             "tg_set_cache_hints": [I],
             "tg_set_block_rows": [I, I],
+            "tg_set_block_width": [I, I],
+            "tg_set_stage_levels": [I, I, I],
+            "tg_set_assembly_mode": [I],
+            "tg_set_block_scratch_budget": [D],
             "tg_selftest_wait": [ctypes.c_uint, P, P],
             "tg_plan_sweep_histogram": [P, ctypes.POINTER(Lg), I],
             "tg_plan_destroy": [P],
@@ -598,6 +602,26 @@ def set_cache_hints(on):
 def set_block_rows(kind, on):
     """FP64 block ring kernel with one lane per block row (1 on, 0 off, -1 default)."""
     return _check(lib().tg_set_block_rows(int(kind), int(on)), "tg_set_block_rows")
+
+
+def set_block_width(kind, width):
+    """Columns per warp of the FP64 block ring kernel (32, 16 or 8; other values: default)."""
+    return _check(lib().tg_set_block_width(int(kind), int(width)), "tg_set_block_width")
+
+
+def set_stage_levels(kind, precision, levels):
+    """Levels per ring stage of the scalar FP64 ring with w2 in global scratch (1, 2, 4, 8)."""
+    return _check(lib().tg_set_stage_levels(int(kind), int(precision), int(levels)), "tg_set_stage_levels")
+
+
+def set_assembly_mode(mode):
+    """Assembly kernels: 1 two passes (default), 0 one fused column walk, -1 default."""
+    return _check(lib().tg_set_assembly_mode(int(mode)), "tg_set_assembly_mode")
+
+
+def set_block_scratch_budget(megabytes):
+    """L2 budget (MB) of the block kernels' Gamma scratch (<= 0: default 96)."""
+    return _check(lib().tg_set_block_scratch_budget(float(megabytes)), "tg_set_block_scratch_budget")
 
 
 def selftest_wait(polls, status, stream=None):

@@ -388,9 +388,9 @@ __attribute__((visibility("default"))) int tg_set_refine(int max_sweeps, double 
 __attribute__((visibility("default"))) int tg_set_pipeline(int kind, int precision, int stages, int warps)
 {
     if ((kind != TG_KIND_SCALAR && kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) || bad_prec(precision) ||
-        (stages != -1 && stages != 0 && stages != 4 && stages != 8 && stages != 16) ||
+        (stages != -1 && stages != 0 && stages != 2 && stages != 3 && stages != 4 && stages != 8 && stages != 16) ||
         (stages > 0 && precision != TG_PREC_F64) || warps < 0 || warps > 8) {
-        set_err("tg_set_pipeline: stages must be 0, 4, 8 or 16 (FP64 only) or -1; warps 0..8");
+        set_err("tg_set_pipeline: stages must be 0, 2, 3, 4, 8 or 16 (FP64 only) or -1; warps 0..8");
         return TG_EINVAL;
     }
     set_stages(kind, precision, stages, warps);
@@ -735,8 +735,9 @@ __attribute__((visibility("default"))) int tg_minor_ng_dev(const tg_minor_fields
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = grow(cx->scratch[0], sizeof(double) * 3 * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
     TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_minor_ng(*F, *C, out, nk, ncol, ld, system_out, cx->flags, st));
+    TG_CUDA(launch_minor_ng(*F, *C, out, nk, ncol, ld, system_out, cx->flags, st, (double *)cx->scratch[0].p));
     if (status_dev) {
         k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
         TG_CUDA(cudaGetLastError());
@@ -791,7 +792,8 @@ __attribute__((visibility("default"))) int tg_minor_ng(const tg_minor_fields *F,
     D.expz = one;
     D.difk = one + nk;
     TG_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_minor_ng(D, *C, out_l, nk, ncol, ld, nullptr, c->flags, st));
+    if ((rc = grow(c->scratch[0], sizeof(double) * 3 * lvl))) return rc;
+    TG_CUDA(launch_minor_ng(D, *C, out_l, nk, ncol, ld, nullptr, c->flags, st, (double *)c->scratch[0].p));
     TG_CUDA(launch_level_to_col(out_l, ld, stage, nk, nk, ncol, st));
     TG_CUDA(cudaMemcpyAsync(out, stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaStreamSynchronize(st));
@@ -1427,6 +1429,42 @@ __attribute__((visibility("default"))) int tg_set_block_rows(int kind, int on)
     return TG_OK;
 }
 
+__attribute__((visibility("default"))) int tg_set_block_width(int kind, int width)
+{
+    if (kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) {
+        set_err("tg_set_block_width: kind must be TG_KIND_BLOCK2 or TG_KIND_BLOCK3");
+        return TG_EINVAL;
+    }
+    tg::set_block_width(kind, width);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_stage_levels(int kind, int precision, int levels)
+{
+    if (kind != TG_KIND_SCALAR || precision != TG_PREC_F64) {
+        set_err("tg_set_stage_levels: applies to TG_KIND_SCALAR, TG_PREC_F64");
+        return TG_EINVAL;
+    }
+    tg::set_stage_levels(kind, precision, levels);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_block_scratch_budget(double megabytes)
+{
+    tg::set_block_scratch_budget(megabytes);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_assembly_mode(int mode)
+{
+    if (mode < -1 || mode > 1) {
+        set_err("tg_set_assembly_mode: mode must be 0, 1 or -1");
+        return TG_EINVAL;
+    }
+    tg::set_assembly_mode(mode);
+    return TG_OK;
+}
+
 __attribute__((visibility("default"))) int tg_set_cache_hints(int on)
 {
     tg::set_cache_hints(on);
@@ -1447,12 +1485,14 @@ __attribute__((visibility("default"))) int tg_plan_describe(const tg_plan *p, ch
         char name[96];
         if (g.kind == TG_KIND_SCALAR) {
             if (!f64) snprintf(name, sizeof name, "k_scalar_refine<%d>", h.pf);
+            else if (h.stages && h.lps > 1) snprintf(name, sizeof name, "k_scalar_f64_chunk<%d,%d>", h.stages, h.lps);
             else if (h.stages) snprintf(name, sizeof name, "k_scalar_f64_ring<%d,%d>", h.stages, h.w2g);
             else if (h.w2g) snprintf(name, sizeof name, "k_scalar_f64_g<%d>", h.pf);
             else snprintf(name, sizeof name, "k_scalar_f64<%d,%d>", h.cpt, h.pf);
         } else {
             if (!f64) snprintf(name, sizeof name, "k_block_refine<%d>", g.kind);
-            else if (h.stages) snprintf(name, sizeof name, "k_block_f64_ring<%d,%d>", g.kind, h.stages);
+            else if (h.stages && h.rows) snprintf(name, sizeof name, "k_block_f64_rows<%d,%d>", g.kind, h.stages);
+            else if (h.stages) snprintf(name, sizeof name, "k_block_f64_ring<%d,%d,%d>", g.kind, h.stages, h.bw);
             else snprintf(name, sizeof name, "k_block_f64<%d>", g.kind);
         }
         char line[256];

@@ -1,0 +1,47 @@
+// Exact FP64 arithmetic helpers shared by the solver and assembly kernels.
+#pragma once
+#include <cfloat>
+#include <cuda_runtime.h>
+
+namespace tg {
+
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ bool finite_nz(double w) { return fabs(w) <= DBL_MAX && w != 0.0; }
+__device__ __forceinline__ bool finite(double w) { return fabs(w) <= DBL_MAX; }
+
+// Correctly rounded quotients that share a divisor.  y = __drcp_rn(b) is the
+// correctly rounded reciprocal; q0 = RN(a*y) is within ~2 ulp of a/b, one
+// FMA correction q1 = RN(q0 + RN(a - b*q0)*y) brings it within 1 ulp, and
+// Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1), 1990; Muller et
+// al., Handbook of Floating-Point Arithmetic, Thm. 5.8) makes the second
+// correction RN(q1 + (a - b*q1)*y) equal to RN(a/b), provided nothing
+// underflows or overflows.  div_safe() keeps a, b (and hence a/b and the
+// residuals) well inside the normal range; other operands, zeros included
+// (whose quotient's sign the correction steps would not keep), take IEEE
+// division.
+// The result is therefore bit-identical to a/b; tg_selftest_division checks
+// it against the hardware division.
+__device__ __forceinline__ bool div_safe(double a, double b)
+{
+    const double lo = 0x1p-500, hi = 0x1p500;
+    const double fa = fabs(a), fb = fabs(b);
+    return fb >= lo && fb <= hi && fa >= lo && fa <= hi;
+}
+__device__ __forceinline__ double div_markstein(double a, double b, double y)
+{
+    double q = __dmul_rn(a, y);
+    double r = __fma_rn(-b, q, a);
+    q = __fma_rn(r, y, q);
+    r = __fma_rn(-b, q, a);
+    return __fma_rn(r, y, q);
+}
+// a/b, correctly rounded, given y = __drcp_rn(b).
+__device__ __forceinline__ double qdiv(double a, double b, double y)
+{
+    return div_safe(a, b) ? div_markstein(a, b, y) : __ddiv_rn(a, b);
+}
+
+}  // namespace tg

@@ -12,9 +12,11 @@
 //
 // Layout: level-major, field(k, col) at k*ld + col; 2-D fields at col; the
 // level constants expz and dift at k.
+#include <atomic>
 #include <cfloat>
 
 #include "tg_internal.h"
+#include "tg_arith.cuh"
 
 namespace tg {
 
@@ -219,7 +221,7 @@ __device__ __constant__ double kMSs[3] = {1.710, 1.749, 1.718};
 
 __device__ __forceinline__ void inv3_ieee(const double (&A)[9], double (&W)[9])
 {
-    // matdet3 / matadj3 / matinv3 (src/matutil.F90), IEEE division
+    // matdet3 / matadj3 / matinv3 (src/matutil.F90)
 #define a_(i, j) A[((i) - 1) + 3 * ((j) - 1)]
 #define w_(i, j) W[((i) - 1) + 3 * ((j) - 1)]
     double d = xm(xm(a_(1, 1), a_(2, 2)), a_(3, 3));
@@ -239,8 +241,11 @@ __device__ __forceinline__ void inv3_ieee(const double (&A)[9], double (&W)[9])
     w_(3, 3) = xs(xm(a_(1, 1), a_(2, 2)), xm(a_(1, 2), a_(2, 1)));
 #undef a_
 #undef w_
+    // the nine quotients share the divisor: correctly rounded, bit-identical
+    // to IEEE division (qdiv)
+    const double y = __drcp_rn(d);
 #pragma unroll
-    for (int e = 0; e < 9; ++e) W[e] = xd(W[e], d);
+    for (int e = 0; e < 9; ++e) W[e] = qdiv(W[e], d, y);
 }
 
 struct MinorLevel {
@@ -433,8 +438,153 @@ __global__ void __launch_bounds__(128) k_minor_ng(MinorFields F, MinorConsts C, 
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
+// ---------------------------------------------------------------------------
+// minor_ng in two passes.  The level quantities (ax, thdiff, dmdz/barm: four
+// fractional powers and a 3x3 inverse per level) are independent across
+// levels, so the first kernel computes them with one thread per (level,
+// column), i.e. nk times the parallelism of the column walk, into a 3-plane
+// level-major buffer; the second walks each column once, forming the rows
+// from those planes and solving.  Same operations as k_minor_ng.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double minor_tni(const MinorFields &F, int j, int nk, long ld, long col, double tlbc)
+{
+    if (j == 0) return tlbc;
+    if (j == nk - 1) return __ldg(F.tn + (long)(nk - 2) * ld + col);
+    return xm(0.5, xa(__ldg(F.tn + (long)j * ld + col), __ldg(F.tn + (long)(j - 1) * ld + col)));
+}
+
+__global__ void __launch_bounds__(128) k_minor_levels(MinorFields F, MinorConsts C, double *lv, int nk, int ncol,
+                                                      long ld)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (col >= ncol) return;
+    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+    const double dzp = C.dzp, tlbc = __ldg(F.tlbc + col);
+    MinorIface I;
+    if (j == 0) {
+        const double o2_0 = at(F.o2, 0), o1_0 = at(F.o1, 0), he_0 = at(F.he, 0), mb_0 = at(F.mbar, 0);
+        const double bo2 = xa(xa(xa(xm(C.b[0], o2_0), xm(C.b[3], o1_0)), xm(C.b[6], he_0)), C.fb[0]);
+        const double bo1 = xa(xa(xa(xm(C.b[1], o2_0), xm(C.b[4], o1_0)), xm(C.b[7], he_0)), C.fb[1]);
+        const double bhe = xa(xa(xa(xm(C.b[2], o2_0), xm(C.b[5], o1_0)), xm(C.b[8], he_0)), C.fb[2]);
+        const double xmbari =
+            xd(1.0, xa(xa(xa(xm(bo2, C.rmassinv_o2), xm(bo1, C.rmassinv_o1)),
+                          xm(xs(xs(xs(1.0, bo2), bo1), bhe), C.rmassinv_n2)),
+                       xm(bhe, C.rmassinv_he)));
+        I.dmdz = xd(xs(mb_0, xmbari), dzp);
+        I.pso1 = xm(0.5, xa(bo1, o1_0));
+        I.pso2 = xm(0.5, xa(bo2, o2_0));
+        I.pshe = xm(0.5, xa(bhe, he_0));
+        I.do1dz = xd(xs(o1_0, bo1), dzp);
+        I.do2dz = xd(xs(o2_0, bo2), dzp);
+        I.dhedz = xd(xs(he_0, bhe), dzp);
+    } else {
+        I = minor_iface(C, at(F.o1, j), at(F.o1, j - 1), at(F.o2, j), at(F.o2, j - 1), at(F.he, j), at(F.he, j - 1),
+                        at(F.mbar, j), at(F.mbar, j - 1));
+    }
+    const double t0 = minor_tni(F, j, nk, ld, col, tlbc);
+    double dt;
+    if (j == 0) dt = xs(minor_tni(F, 1, nk, ld, col, tlbc), t0);
+    else if (j == nk - 1) dt = xs(t0, minor_tni(F, nk - 2, nk, ld, col, tlbc));
+    else dt = xd(xs(minor_tni(F, j + 1, nk, ld, col, tlbc), minor_tni(F, j - 1, nk, ld, col, tlbc)), 2.0);
+    const MinorLevel L = minor_level(C, I, at(F.barm, j), t0, dt);
+    const long slab = (long)nk * ld;
+    lv[(long)j * ld + col] = L.ax;
+    lv[slab + (long)j * ld + col] = L.thdiff;
+    lv[2 * slab + (long)j * ld + col] = L.dmdzs;
+}
+
+__global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C, const double *lv, double *out,
+                                                    int nk, int ncol, long ld, double *sys_out, unsigned *status)
+{
+    extern __shared__ double smem_mr[];
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    double *w2s = smem_mr + threadIdx.x;
+    const int T = blockDim.x;
+    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+    const long slab = (long)nk * ld;
+    auto lev = [&](int k) {
+        MinorLevel L;
+        L.ax = __ldg(lv + (long)k * ld + col);
+        L.thdiff = __ldg(lv + slab + (long)k * ld + col);
+        L.dmdzs = __ldg(lv + 2 * slab + (long)k * ld + col);
+        return L;
+    };
+    const double dzp = C.dzp, rdz = xd(1.0, dzp), dfac = __ldg(F.dfactor + col);
+    MinorLevel L0 = lev(0);
+    bool ok = true;
+    double w1 = 0.0, w3 = 0.0, rprev = 0.0;
+    for (int k = 0; k < nk; ++k) {
+        double p, q, r, f;
+        const double expz = __ldg(F.expz + k);
+        const double sp = xd(xm(at(F.sprod, k), C.rmx), at(F.xnmbar, k));
+        f = xa(xs(xm(at(F.ftm1_smooth, k), C.dtx2inv), at(F.hadvec, k)), sp);
+        f = xm(f, expz);
+        MinorLevel L1 = L0;
+        if (k < nk - 1) {
+            L1 = lev(k + 1);
+            const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1);
+            const double molp = xm(L0.ax, xa(rdz, xm(0.5, L0.thdiff)));
+            const double molr = xm(L1.ax, xs(rdz, xm(0.5, L1.thdiff)));
+            const double molq = xa(xm(L0.ax, xs(rdz, xm(0.5, L0.thdiff))), xm(L1.ax, xa(rdz, xm(0.5, L1.thdiff))));
+            const double eddyp = xm(xm(C.expzmid_inv, difk0), xs(rdz, xm(0.5, L0.dmdzs)));
+            const double eddyr = xm(xm(C.expzmid, difk1), xa(rdz, xm(0.5, L1.dmdzs)));
+            const double eddyq = xa(xm(xm(C.expzmid_inv, difk0), xa(rdz, xm(0.5, L0.dmdzs))),
+                                    xm(xm(C.expzmid, difk1), xs(rdz, xm(0.5, L1.dmdzs))));
+            const double wi = xm(0.5, xa(at(F.w, k), at(F.w, k + 1)));
+            p = xs(xd(molp, dzp), xd(xm(expz, xa(xm(eddyp, dfac), xm(0.5, wi))), dzp));
+            r = xs(xd(molr, dzp), xd(xm(expz, xs(xm(eddyr, dfac), xm(0.5, wi))), dzp));
+            q = xa(-xd(molq, dzp), xm(expz, xs(xa(xd(xm(eddyq, dfac), dzp), C.dtx2inv), at(F.sloss, k))));
+            if (k == 0) {
+                const double l1 = __ldg(F.flbc1 + col), l2 = __ldg(F.flbc2 + col), l3 = __ldg(F.flbc3 + col);
+                const double den = xs(l1, xm(xm(0.5, l2), dzp));
+                q = xa(q, xd(xm(p, xa(l1, xm(xm(0.5, l2), dzp))), den));
+                f = xs(f, xd(xm(xm(p, l3), dzp), den));
+                p = 0.0;
+            }
+        } else {
+            p = xa(1.0, xm(xm(0.5, dzp), L0.thdiff));
+            q = xs(p, 2.0);
+            r = 0.0;
+            f = -xd(xm(xm(xm(C.grav, C.rmx), __ldg(F.fubc + col)), dzp), xm(xm(C.p0, L0.ax), C.avo));
+        }
+        if (sys_out) {
+            sys_out[k * ld + col] = p;
+            sys_out[slab + k * ld + col] = q;
+            sys_out[2 * slab + k * ld + col] = r;
+            sys_out[3 * slab + k * ld + col] = f;
+        }
+        if (k == 0) {
+            w1 = q;
+            w3 = xd(f, w1);
+        } else {
+            const double w2 = xd(rprev, w1);
+            w2s[(k - 1) * T] = w2;
+            w1 = xs(q, xm(p, w2));
+            w3 = xd(xs(f, xm(p, w3)), w1);
+        }
+        ok = ok && fin_nz(w1);
+        out[k * ld + col] = w3;
+        rprev = r;
+        L0 = L1;
+    }
+    double xn = w3;
+    bool fin = fabs(xn) <= DBL_MAX;
+    for (int k = nk - 2; k >= 0; --k) {
+        xn = xs(out[k * ld + col], xm(w2s[k * T], xn));
+        fin = fin && fabs(xn) <= DBL_MAX;
+        out[k * ld + col] = xn;
+    }
+    if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+}
+
+static std::atomic<int> g_assembly_mode{1};
+int assembly_mode() { return g_assembly_mode.load(); }
+void set_assembly_mode(int m) { g_assembly_mode.store(m < 0 ? 1 : (m ? 1 : 0)); }
+
 cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *out, int nk, int ncol, long ld,
-                            double *sys_out, unsigned *status, cudaStream_t st)
+                            double *sys_out, unsigned *status, cudaStream_t st, double *scratch)
 {
     if (ncol <= 0) return cudaSuccess;
     static int optin = 0;
@@ -451,6 +601,16 @@ cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *
     while (T > 32 && (size_t)T * (nk - 1) * sizeof(double) > (size_t)optin) T /= 2;
     const size_t smem = (size_t)T * (nk - 1 > 0 ? nk - 1 : 1) * sizeof(double);
     if (smem > (size_t)optin) return cudaErrorInvalidValue;
+    if (scratch && assembly_mode() == 1) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_minor_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+            attr = true;
+        }
+        k_minor_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch, nk, ncol, ld);
+        k_minor_rows<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, scratch, out, nk, ncol, ld, sys_out, status);
+        return cudaGetLastError();
+    }
     k_minor_ng<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, out, nk, ncol, ld, sys_out, status);
     return cudaGetLastError();
 }

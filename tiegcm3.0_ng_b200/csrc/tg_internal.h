@@ -60,6 +60,8 @@ struct Shape {
     int pf;             // scalar register kernels: prefetch depth in levels
     size_t smem;        // dynamic shared memory bytes
     int rows;           // block ring kernel with one lane per block row
+    int bw;             // block ring kernel: columns per warp (32, 16, 8)
+    int lps;            // scalar FP64 ring: levels per stage (>1: chunked ring kernel)
 };
 
 // Register-prefetch kernel shape of a kind/precision (tg_set_tile).
@@ -85,8 +87,8 @@ void set_w2g(int kind, int precision, int on);
 size_t scalar_scratch_bytes(long slots, int k2max);
 
 // Shared memory / scratch needs of a kernel for the largest k2 it will see.
-size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g);
-size_t block_smem_bytes(int B, int stages, int threads, int rows);
+size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g, int lps);
+size_t block_smem_bytes(int B, int stages, int threads, int rows, int bw);
 // Global scratch (bytes) of a block kernel with `slots` resident threads.
 size_t block_scratch_bytes(int B, int precision, long slots, int k2max);
 
@@ -132,8 +134,14 @@ cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, i
 
 typedef tg_minor_fields MinorFields;
 typedef tg_minor_consts MinorConsts;
+// scratch (3 * nk * ld doubles, may be NULL): the level-quantity planes of the
+// two-pass form, used when assembly_mode() is 1
 cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *out, int nk, int ncol, long ld,
-                            double *sys_out, unsigned *status, cudaStream_t st);
+                            double *sys_out, unsigned *status, cudaStream_t st, double *scratch);
+// Assembly kernels: 1 (default) two-pass (level-parallel level quantities,
+// then the column walk) where built, 0 the single fused column walk.
+int assembly_mode();
+void set_assembly_mode(int m);
 
 typedef tg_comp_fields CompFields;
 typedef tg_comp_consts CompConsts;
@@ -161,6 +169,15 @@ cudaError_t launch_selftest_wait(unsigned polls, unsigned *status, cudaStream_t 
 // Block kinds: the bulk-copy ring kernel with one lane per block row
 // (tg_set_block_rows); 1 on, 0 off, -1 default.
 void set_block_rows(int kind, int on);
+// Block kinds: columns per warp of the bulk-copy ring kernel (32, 16 or 8;
+// other values restore the default).
+void set_block_width(int kind, int w);
+// Scalar FP64 ring with w2 in global scratch: levels per ring stage (1, 2, 4,
+// 8; other values restore the default).
+void set_stage_levels(int kind, int precision, int l);
+// L2 budget (MB) for the Gamma scratch of all resident block-kernel warps;
+// <= 0 restores the default 96 MB.
+void set_block_scratch_budget(double mb);
 
 // L2 cache-policy hints of the bulk-copy ring kernels (tg_set_cache_hints).
 int cache_hints();

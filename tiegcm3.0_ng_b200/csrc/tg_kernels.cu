@@ -17,51 +17,13 @@
 #include <mutex>
 
 #include "tg_internal.h"
+#include "tg_arith.cuh"
 
 namespace tg {
 
 // ---------------------------------------------------------------------------
 // Arithmetic and memory helpers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
-__device__ __forceinline__ bool finite_nz(double w) { return fabs(w) <= DBL_MAX && w != 0.0; }
-__device__ __forceinline__ bool finite(double w) { return fabs(w) <= DBL_MAX; }
-
-// Correctly rounded quotients that share a divisor.  y = __drcp_rn(b) is the
-// correctly rounded reciprocal; q0 = RN(a*y) is within ~2 ulp of a/b, one
-// FMA correction q1 = RN(q0 + RN(a - b*q0)*y) brings it within 1 ulp, and
-// Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1), 1990; Muller et
-// al., Handbook of Floating-Point Arithmetic, Thm. 5.8) makes the second
-// correction RN(q1 + (a - b*q1)*y) equal to RN(a/b), provided nothing
-// underflows or overflows.  div_safe() keeps a, b (and hence a/b and the
-// residuals) well inside the normal range; other operands, zeros included
-// (whose quotient's sign the correction steps would not keep), take IEEE
-// division.
-// The result is therefore bit-identical to a/b; tg_selftest_division checks
-// it against the hardware division.
-__device__ __forceinline__ bool div_safe(double a, double b)
-{
-    const double lo = 0x1p-500, hi = 0x1p500;
-    const double fa = fabs(a), fb = fabs(b);
-    return fb >= lo && fb <= hi && fa >= lo && fa <= hi;
-}
-__device__ __forceinline__ double div_markstein(double a, double b, double y)
-{
-    double q = __dmul_rn(a, y);
-    double r = __fma_rn(-b, q, a);
-    q = __fma_rn(r, y, q);
-    r = __fma_rn(-b, q, a);
-    return __fma_rn(r, y, q);
-}
-// a/b, correctly rounded, given y = __drcp_rn(b).
-__device__ __forceinline__ double qdiv(double a, double b, double y)
-{
-    return div_safe(a, b) ? div_markstein(a, b, y) : __ddiv_rn(a, b);
-}
-
 // Streaming read of coefficients used once (evict-first in L1/L2).
 template <int N>
 __device__ __forceinline__ void ld_stream(const double *p, double (&v)[N]);
@@ -487,6 +449,130 @@ __global__ void __launch_bounds__(256) k_scalar_f64_ring(SegTable tab, double *s
         q += k2;
         if (valid) {
             // back sweep; w3 (in x) and w2 of the next 4 levels in flight
+            double xn = w3;
+            fin = finite(xn);
+            double rw[4], r2[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k2 - 2 - u >= 0) {
+                    rw[u] = px[(k2 - 2 - u) * ld];
+                    r2[u] = w2s[(k2 - 2 - u) * ws];
+                }
+            for (int kb = k2 - 2; kb >= 0; kb -= 4) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = kb - u;
+                    if (k >= 0) {
+                        xn = xsub(rw[u], xmul(r2[u], xn));
+                        fin = fin && finite(xn);
+                        if (k - 4 >= 0) {
+                            rw[u] = px[(k - 4) * ld];
+                            r2[u] = w2s[(k - 4) * ws];
+                        }
+                        px[k * ld] = xn;
+                    }
+                }
+            }
+            report(status, s.status_idx, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Scalar Thomas, FP64, bulk-copy ring of chunks: each of C stages holds L
+// consecutive levels of the four coefficient arrays (4L copies of 256 B), so
+// the mbarrier wait, proxy fence and copy issue happen once per L levels
+// instead of once per level.  w2 in the L2 scratch slot of the lane, w3
+// parked in x, as in k_scalar_f64_ring; same arithmetic, same bits.
+// ---------------------------------------------------------------------------
+template <int C, int L>
+__global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *scratch, unsigned *status)
+{
+    constexpr int NE = 4 * L;
+    static_assert(NE <= 32, "one copy per lane");
+    __shared__ __align__(8) unsigned long long bars[8 * C];
+    extern __shared__ __align__(128) double smem_r[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    double *buf = smem_r + (long)warp * C * NE * 32;
+    unsigned long long *bar = bars + warp * C;
+    const unsigned long long pol = l2_policy(tab.hints, false), keep = l2_policy(tab.hints, true);
+    const long ws = (long)gridDim.x * blockDim.x;
+    double *w2s = scratch + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (lane == 0) {
+#pragma unroll 1
+        for (int i = 0; i < C; ++i) mbar_init(&bar[i], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    unsigned q = 0;
+    for (int t = blockIdx.x * nwarps + warp; t < tab.ntiles; t += gridDim.x * nwarps) {
+        const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
+        const long col0 = (long)(t - s.tile0) * 32;
+        const long ld = s.ld;
+        const int k2 = s.k2;
+        const bool valid = col0 + lane < s.ncol;
+        const int arr = lane & 3;
+        const double *src = (arr == 0 ? s.a : arr == 1 ? s.b : arr == 2 ? s.c : s.f) + col0 + (long)(lane >> 2) * ld;
+        double *px = s.x + col0 + lane;
+        const int nch = (k2 + L - 1) / L;
+        // chunk j: levels j*L .. j*L+L-1 (those < k2) into stage (q + j) % C
+        auto issue = [&](unsigned qc, int j) {
+            const int st = (int)(qc % C), l0 = j * L;
+            const int nl = k2 - l0 < L ? k2 - l0 : L;
+            if (lane == 0) mbar_expect(&bar[st], (uint32_t)(4 * nl * 256));
+            __syncwarp();
+            if (lane < 4 * nl) bulk_load_hint(buf + (st * NE + lane) * 32, src + (long)l0 * ld, 256u, &bar[st], pol);
+        };
+        const int pre = nch < C ? nch : C;
+        for (int j = 0; j < pre; ++j) issue(q + j, j);
+        bool ok = true, fin = true;
+        double w1 = 0.0, y1 = 0.0, w3 = 0.0, cprev = 0.0;
+        for (int j = 0; j < nch; ++j) {
+            const unsigned qc = q + j;
+            if (!mbar_wait_warp(&bar[qc % C], (qc / C) & 1u)) {
+                const unsigned qe = q + (j + C < nch ? j + C : nch);
+#pragma unroll 1
+                for (unsigned r = qc; r < qe; ++r) mbar_wait_warp(&bar[r % C], (r / C) & 1u);
+                if (lane == 0) report(status, s.status_idx, FLAG_TIMEOUT);
+                return;
+            }
+            const double *stg = buf + (int)(qc % C) * NE * 32 + lane;
+            double va[L], vb[L], vc[L], vf[L];
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                va[l] = stg[(4 * l + 0) * 32];
+                vb[l] = stg[(4 * l + 1) * 32];
+                vc[l] = stg[(4 * l + 2) * 32];
+                vf[l] = stg[(4 * l + 3) * 32];
+            }
+            __syncwarp();
+            fence_proxy_async();
+            if (j + C < nch) issue(qc + C, j + C);
+            if (valid) {
+#pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    const int k = j * L + l;
+                    if (k < k2) {
+                        if (k == 0) {
+                            w1 = vb[l];
+                            y1 = __drcp_rn(w1);
+                            w3 = qdiv(vf[l], w1, y1);
+                        } else {
+                            const double w2 = qdiv(cprev, w1, y1);
+                            st_hint(&w2s[(k - 1) * ws], w2, keep);
+                            w1 = xsub(vb[l], xmul(va[l], w2));
+                            y1 = __drcp_rn(w1);
+                            w3 = qdiv(xsub(vf[l], xmul(va[l], w3)), w1, y1);
+                        }
+                        ok = ok && finite_nz(w1);
+                        cprev = vc[l];
+                        st_hint(&px[k * ld], w3, keep);
+                    }
+                }
+            }
+        }
+        q += nch;
+        if (valid) {
             double xn = w3;
             fin = finite(xn);
             double rw[4], r2[4];
@@ -968,25 +1054,30 @@ __global__ void __launch_bounds__(128) k_block_f64(SegTable tab, double *scratch
 // (P, Q, R, f) arrive in a D-stage shared-memory ring, one 256-byte copy per
 // entry issued by one lane.  Same arithmetic as blk_f64_col.
 // ---------------------------------------------------------------------------
-template <int B, int D>
+template <int B, int D, int W>
 __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *scratch, unsigned *status)
 {
-    constexpr int BB = B * B, NE = 3 * BB + B;
+    // W < 32: a warp covers W columns (lanes >= W idle), so that more warps
+    // share the SM's issue slots when there are few columns
+    constexpr int BB = B * B, NE = 3 * BB + B, NSUB = 32 / W;
     __shared__ __align__(8) unsigned long long bars[8 * D];
     extern __shared__ __align__(128) double smem_b[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    Ring<NE, D> ring{smem_b + (long)warp * D * NE * 32, bars + warp * D, l2_policy(tab.hints, false)};
+    const int cl = lane & (W - 1);            // column of this lane within the tile (idle lanes alias)
+    Ring<NE, D, W> ring{smem_b + (long)warp * D * NE * W, bars + warp * D, l2_policy(tab.hints, false)};
     const unsigned long long keep = l2_policy(tab.hints, true);
     ring.init(lane);
-    const long gs = (long)gridDim.x * blockDim.x;
-    double *gam = scratch + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long gs = (long)gridDim.x * nwarps * W;
+    double *gam = scratch + ((long)blockIdx.x * nwarps + warp) * W + cl;
     unsigned q = 0;
-    for (int t = blockIdx.x * nwarps + warp; t < tab.ntiles; t += gridDim.x * nwarps) {
+    for (int vt = blockIdx.x * nwarps + warp; vt < tab.ntiles * NSUB; vt += gridDim.x * nwarps) {
+        const int t = vt / NSUB;
         const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
-        const long col0 = (long)(t - s.tile0) * 32;
+        const long col0 = (long)(t - s.tile0) * 32 + (long)(vt % NSUB) * W;
+        if (col0 >= s.ncol) continue;        // uniform across the warp
         const long ld = s.ld;
         const int k2 = s.k2;
-        const bool valid = col0 + lane < s.ncol;
+        const bool valid = lane < W && col0 + lane < s.ncol;
         // entry e of level k: P/Q/R element e at (k*BB + e)*ld, f component at (k*B + i)*ld
         const double *src = s.a + col0;
         long lstride = 0;
@@ -1003,7 +1094,7 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
             src = s.f + col0 + (lane - 3 * BB) * ld;
             lstride = B * ld;
         }
-        double *pU = s.x + col0 + lane;
+        double *pU = s.x + col0 + cl;
         const int pre = k2 < D ? k2 : D;
         for (int j = 0; j < pre; ++j) ring.issue(q + j, src + j * lstride, lane);
         bool ok = true;
@@ -1018,12 +1109,12 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
             double P[BB], Q[BB], R[BB], F[B];
 #pragma unroll
             for (int e = 0; e < BB; ++e) {
-                P[e] = ring.at(qk, e, lane);
-                Q[e] = ring.at(qk, BB + e, lane);
-                R[e] = ring.at(qk, 2 * BB + e, lane);
+                P[e] = ring.at(qk, e, cl);
+                Q[e] = ring.at(qk, BB + e, cl);
+                R[e] = ring.at(qk, 2 * BB + e, cl);
             }
 #pragma unroll
-            for (int i = 0; i < B; ++i) F[i] = ring.at(qk, 3 * BB + i, lane);
+            for (int i = 0; i < B; ++i) F[i] = ring.at(qk, 3 * BB + i, cl);
             __syncwarp();
             fence_proxy_async();
             if (k + D < k2) ring.issue(qk + D, src + (k + D) * lstride, lane);
@@ -1088,8 +1179,8 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
         if (s.ubc_ratio) {
 #pragma unroll
             for (int i = 0; i < B; ++i) {
-                double tv = xmul(__ldg(s.ubc_ratio + i * ld + col0 + lane), top[i]);
-                if (s.ubc_add) tv = xadd(tv, __ldg(s.ubc_add + i * ld + col0 + lane));
+                double tv = xmul(__ldg(s.ubc_ratio + i * ld + col0 + cl), top[i]);
+                if (s.ubc_add) tv = xadd(tv, __ldg(s.ubc_add + i * ld + col0 + cl));
                 fin = fin && finite(tv);
                 pU[((long)k2 * B + i) * ld] = tv;
             }
@@ -1755,19 +1846,21 @@ struct TileCfg {
     int pf;                // scalar register kernels: levels of coefficient loads in flight per column
     int wpb;               // ring kernels: independent warps (32-column tiles) per CTA
     int rows;              // block ring kernels: one lane per block row (k_block_f64_rows)
+    int bw;                // block ring kernels: columns per warp (32, 16 or 8)
+    int lps;               // scalar FP64 ring: levels per stage (1: k_scalar_f64_ring, >1: k_scalar_f64_chunk)
 };
 // [kind index: scalar, block2, block3][precision]
 // Defaults: the fastest shapes on the 2.5 deg column step (10368 x 57) on a
-// B200 (autotune.py sweep): scalar FP64 bulk-copy ring of depth 4, one warp
-// per CTA, w2 in global scratch; 2x2 block ring of depth 4, one warp per CTA;
+// B200 (autotune.py sweep): scalar FP64 chunked bulk-copy ring of 2 stages x
+// 4 levels, one warp per CTA, w2 in global scratch; 2x2 block ring of depth 4, one warp per CTA;
 // 3x3 block register kernel of 128 threads; refinement kernels 64 threads
 // (scalar, prefetch 8), 64 (2x2) and 128 (3x3).
-const TileCfg kDefaultTile[3][2] = {{{256, 1, 4, 1, 4, 1, 0}, {64, 1, 0, 0, 8, 4, 0}},
-                                     {{64, 1, 4, 0, 4, 1, 0}, {64, 1, 0, 0, 4, 4, 0}},
-                                     {{128, 1, 0, 0, 4, 4, 0}, {128, 1, 0, 0, 4, 4, 0}}};
-TileCfg g_tile[3][2] = {{{256, 1, 4, 1, 4, 1, 0}, {64, 1, 0, 0, 8, 4, 0}},
-                        {{64, 1, 4, 0, 4, 1, 0}, {64, 1, 0, 0, 4, 4, 0}},
-                        {{128, 1, 0, 0, 4, 4, 0}, {128, 1, 0, 0, 4, 4, 0}}};
+const TileCfg kDefaultTile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 0, 0, 8, 4, 0, 32, 1}},
+                                     {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 0, 0, 4, 4, 0, 32, 1}},
+                                     {{128, 1, 0, 0, 4, 4, 0, 32, 1}, {128, 1, 0, 0, 4, 4, 0, 32, 1}}};
+TileCfg g_tile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 0, 0, 8, 4, 0, 32, 1}},
+                        {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 0, 0, 4, 4, 0, 32, 1}},
+                        {{128, 1, 0, 0, 4, 4, 0, 32, 1}, {128, 1, 0, 0, 4, 4, 0, 32, 1}}};
 int kind_index(int kind) { return kind == TG_KIND_SCALAR ? 0 : (kind == TG_KIND_BLOCK2 ? 1 : 2); }
 int g_num_sms = -1;
 int g_smem_optin = -1;
@@ -1830,22 +1923,24 @@ cudaError_t with_scalar_ring(int D, int w2g, F f)
     }
 }
 template <typename F>
-cudaError_t with_block_ring(int B, int D, F f)
+cudaError_t with_scalar_chunk(int C, int L, F f)
 {
-    if (B == 2) {
-        switch (D) {
-        case 4: return f(k_block_f64_ring<2, 4>);
-        case 8: return f(k_block_f64_ring<2, 8>);
-        case 16: return f(k_block_f64_ring<2, 16>);
-        default: return cudaErrorInvalidValue;
-        }
-    }
-    switch (D) {
-    case 4: return f(k_block_f64_ring<3, 4>);
-    case 8: return f(k_block_f64_ring<3, 8>);
-    case 16: return f(k_block_f64_ring<3, 16>);
-    default: return cudaErrorInvalidValue;
-    }
+#define TG_CHUNK(c, l) \
+    if (C == c && L == l) return f(k_scalar_f64_chunk<c, l>);
+    TG_CHUNK(2, 2) TG_CHUNK(3, 2) TG_CHUNK(4, 2) TG_CHUNK(2, 4) TG_CHUNK(3, 4) TG_CHUNK(4, 4) TG_CHUNK(2, 8)
+#undef TG_CHUNK
+    return cudaErrorInvalidValue;
+}
+template <typename F>
+cudaError_t with_block_ring(int B, int D, int W, F f)
+{
+#define TG_RING(b, d, w) \
+    if (B == b && D == d && W == w) return f(k_block_f64_ring<b, d, w>);
+    TG_RING(2, 4, 32) TG_RING(2, 8, 32) TG_RING(2, 16, 32) TG_RING(2, 4, 16) TG_RING(2, 8, 16) TG_RING(2, 4, 8)
+    TG_RING(2, 8, 8) TG_RING(3, 4, 32) TG_RING(3, 8, 32) TG_RING(3, 16, 32) TG_RING(3, 4, 16) TG_RING(3, 8, 16)
+    TG_RING(3, 4, 8) TG_RING(3, 8, 8)
+#undef TG_RING
+    return cudaErrorInvalidValue;
 }
 
 template <typename F>
@@ -1888,12 +1983,12 @@ int num_sms()
         }
         for (int d : {4, 8, 16})
             for (int g : {0, 1}) with_scalar_ring(d, g, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
-        allow_smem(k_block_f64_ring<2, 4>, lim);
-        allow_smem(k_block_f64_ring<2, 8>, lim);
-        allow_smem(k_block_f64_ring<2, 16>, lim);
-        allow_smem(k_block_f64_ring<3, 4>, lim);
-        allow_smem(k_block_f64_ring<3, 8>, lim);
-        allow_smem(k_block_f64_ring<3, 16>, lim);
+        for (int c : {2, 3, 4})
+            for (int l : {2, 4, 8}) with_scalar_chunk(c, l, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+        for (int b : {2, 3})
+            for (int d : {4, 8, 16})
+                for (int w : {32, 16, 8})
+                    with_block_ring(b, d, w, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int d : {4, 8})
             for (int b : {2, 3}) with_block_rows(b, d, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
     }
@@ -1935,7 +2030,7 @@ cudaError_t occupancy(K kernel, int threads, size_t smem, int *per_sm)
 
 // Resident threads per SM allowed for the block kernels: their Gamma scratch
 // (k2 * B*B doubles per resident thread) should stay well inside L2.
-constexpr double kBlockScratchBudget = 48.0 * 1024 * 1024;
+double g_block_scratch_budget = 96.0 * 1024 * 1024;
 }  // namespace
 
 int prefetch_depth(int kind, int precision) { return g_tile[kind_index(kind)][precision ? 1 : 0].pf; }
@@ -1998,6 +2093,23 @@ void set_block_rows(int kind, int on)
     TileCfg &t = g_tile[kind_index(kind)][0];
     t.rows = on < 0 ? kDefaultTile[kind_index(kind)][0].rows : (on ? 1 : 0);
 }
+void set_block_scratch_budget(double mb) { g_block_scratch_budget = (mb > 0 ? mb : 96.0) * 1024 * 1024; }
+void set_stage_levels(int kind, int precision, int l)
+{
+    if (kind != TG_KIND_SCALAR || precision != TG_PREC_F64) return;
+    TileCfg &t = g_tile[0][0];
+    t.lps = (l == 1 || l == 2 || l == 4 || l == 8) ? l : kDefaultTile[0][0].lps;
+}
+void set_block_width(int kind, int w)
+{
+    if (kind == TG_KIND_SCALAR) return;
+    TileCfg &t = g_tile[kind_index(kind)][0];
+    t.bw = (w == 8 || w == 16 || w == 32) ? w : kDefaultTile[kind_index(kind)][0].bw;
+}
+static int block_width(int kind, int precision)
+{
+    return kind != TG_KIND_SCALAR && precision == TG_PREC_F64 ? g_tile[kind_index(kind)][0].bw : 32;
+}
 static int block_rows(int kind, int precision)
 {
     return kind != TG_KIND_SCALAR && precision == TG_PREC_F64 && g_tile[kind_index(kind)][0].rows;
@@ -2005,18 +2117,19 @@ static int block_rows(int kind, int precision)
 // lanes per column of the row kernel
 static int rows_group(int B) { return B == 2 ? 2 : 4; }
 
-size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g)
+size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g, int lps)
 {
     const size_t lev = (size_t)(k2max > 1 ? k2max - 1 : 1);
+    if (stages > 0 && lps > 1) return (size_t)threads / 32 * stages * 4 * lps * 32 * 8;
     if (stages > 0) return (size_t)threads / 32 * ((size_t)stages * 4 * 32 * 8 + (w2g ? 0 : 32 * lev * 8));
     if (w2g) return 0;
     if (precision == TG_PREC_F64) return (size_t)threads * cpt * lev * 8;
     return (size_t)threads * 3 * (size_t)k2max * 4;
 }
 
-size_t block_smem_bytes(int B, int stages, int threads, int rows)
+size_t block_smem_bytes(int B, int stages, int threads, int rows, int bw)
 {
-    const int w = rows ? 32 / rows_group(B) : 32;
+    const int w = rows ? 32 / rows_group(B) : bw;
     return stages > 0 ? (size_t)threads / 32 * stages * (3 * B * B + B) * w * 8 : 0;
 }
 
@@ -2038,26 +2151,37 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     sh->w2g = w2g;
     sh->pf = prefetch_depth(kind, precision);
     sh->rows = stages > 0 ? block_rows(kind, precision) : 0;
+    sh->bw = stages > 0 && kind != TG_KIND_SCALAR && !sh->rows ? block_width(kind, precision) : 32;
+    // chunked scalar ring: w2 in global scratch, C = stages chunks of lps levels
+    sh->lps = stages > 0 && kind == TG_KIND_SCALAR && precision == TG_PREC_F64 && w2g ? g_tile[0][0].lps : 1;
+    if (sh->lps > 1 && stages > 4) stages = sh->stages = 4;
+    if (sh->lps > 1 && sh->lps * stages > 16) stages = sh->stages = 2;
+    if (sh->lps == 1 && stages > 0 && stages < 4) stages = sh->stages = 4;   // per-level rings: depth 4, 8, 16
+    if (sh->bw < 32 && stages > 8) stages = sh->stages = 8;
     if (sh->rows && stages > 8) stages = sh->stages = 8;
     if (kind == TG_KIND_SCALAR && sh->cpt == 2 && sh->pf > 8) sh->pf = 8;
     if (stages > 0) {
         // a ring that does not fit in shared memory falls back to the
         // register-prefetch kernel with the same 32-column tile
-        const size_t need = kind == TG_KIND_SCALAR ? scalar_smem_bytes(precision, sh->threads, 1, k2max, stages, w2g)
-                                                   : block_smem_bytes(kind, stages, sh->threads, sh->rows);
+        const size_t need = kind == TG_KIND_SCALAR ? scalar_smem_bytes(precision, sh->threads, 1, k2max, stages, w2g, sh->lps)
+                                                   : block_smem_bytes(kind, stages, sh->threads, sh->rows, sh->bw);
         if (need > (size_t)(g_smem_optin - 1024)) {
             stages = 0;
             sh->stages = 0;
             sh->threads = 32;
             sh->cpt = 1;
             sh->rows = 0;
+            sh->bw = 32;
+            sh->lps = 1;
         }
     }
     if (kind == TG_KIND_SCALAR) {
-        sh->smem = scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max, stages, w2g);
+        sh->smem = scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max, stages, w2g, sh->lps);
         if (sh->smem > (size_t)(g_smem_optin - 1024)) return cudaErrorInvalidConfiguration;
         auto occ = [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); };
-        if (stages > 0)
+        if (stages > 0 && sh->lps > 1)
+            e = with_scalar_chunk(stages, sh->lps, occ);
+        else if (stages > 0)
             e = with_scalar_ring(stages, w2g, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
         else if (w2g)
             e = with_scalar_g(sh->pf, occ);
@@ -2067,28 +2191,33 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
             e = with_scalar_refine(sh->pf, occ);
     } else {
         const int B = kind;
-        sh->smem = block_smem_bytes(B, stages, sh->threads, sh->rows);
+        sh->smem = block_smem_bytes(B, stages, sh->threads, sh->rows, sh->bw);
         if (sh->smem > (size_t)(g_smem_optin - 1024)) return cudaErrorInvalidConfiguration;
         if (stages > 0 && sh->rows)
             e = with_block_rows(B, stages, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
         else if (stages > 0)
-            e = with_block_ring(B, stages, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
+            e = with_block_ring(B, stages, sh->bw,
+                                [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
         else if (precision == TG_PREC_F64)
             e = B == 2 ? occupancy(k_block_f64<2>, sh->threads, 0, &per_sm)
                        : occupancy(k_block_f64<3>, sh->threads, 0, &per_sm);
         else
             e = B == 2 ? occupancy(k_block_refine<2>, sh->threads, 0, &per_sm)
                        : occupancy(k_block_refine<3>, sh->threads, 0, &per_sm);
-        if (e == cudaSuccess) {
-            const double per_thread = (double)block_scratch_bytes(B, precision, 1, k2max);
-            const int cap = (int)(kBlockScratchBudget / (per_thread * sh->threads * nsm));
-            per_sm = per_sm < cap ? per_sm : (cap > 0 ? cap : 1);
-        }
     }
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     long blocks = (long)per_sm * nsm;
-    const long vt = sh->rows ? (long)ntiles * rows_group(kind) : ntiles;   // warp tiles
+    if (kind != TG_KIND_SCALAR) {
+        // keep the Gamma scratch of all resident blocks within the L2 budget
+        // (a cap on the total, not per SM, so that a grid that fits in one
+        // wave is not split into two)
+        const double per_thread = (double)block_scratch_bytes(kind, precision, 1, k2max);
+        const long cap = (long)(g_block_scratch_budget / (per_thread * sh->threads));
+        if (blocks > cap) blocks = cap > 0 ? cap : 1;
+    }
+    const long vt = sh->rows ? (long)ntiles * rows_group(kind)
+                             : (kind != TG_KIND_SCALAR ? (long)ntiles * (32 / sh->bw) : ntiles);   // warp tiles
     const long units = stages > 0 ? (vt + sh->threads / 32 - 1) / (sh->threads / 32) : ntiles;
     if (blocks > units) blocks = units;
     sh->blocks = (int)(blocks > 0 ? blocks : 1);
@@ -2104,7 +2233,14 @@ cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, R
 {
     if (tab.ntiles <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
-    if (precision == TG_PREC_F64 && sh.stages > 0) {
+    if (precision == TG_PREC_F64 && sh.stages > 0 && sh.lps > 1) {
+        SegTable t = tab;
+        t.hints = cache_hints();
+        e = with_scalar_chunk(sh.stages, sh.lps, [&](auto k) {
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, scratch, status);
+            return cudaSuccess;
+        });
+    } else if (precision == TG_PREC_F64 && sh.stages > 0) {
         SegTable t = tab;
         t.hints = cache_hints();
         e = with_scalar_ring(sh.stages, sh.w2g, [&](auto k) {
@@ -2146,7 +2282,7 @@ cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape 
     } else if (precision == TG_PREC_F64 && sh.stages > 0) {
         SegTable t = tab;
         t.hints = cache_hints();
-        cudaError_t e = with_block_ring(B, sh.stages, [&](auto k) {
+        cudaError_t e = with_block_ring(B, sh.stages, sh.bw, [&](auto k) {
             k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, scratch, status);
             return cudaSuccess;
         });
