@@ -121,7 +121,7 @@ def _comp_dev_inputs(pkg, torch, F, nk, ncol):
 
 @pytest.mark.parametrize("nk,dz,ncol,calc_helium", [(57, 0.25, 3001, 1), (29, 0.5, 2592, 1), (113, 0.125, 300, 1),
                                                     (3, 0.5, 33, 1), (57, 0.25, 500, 0)])
-def test_comp_ng_host(cuda, pkg, orc, nk, dz, ncol, calc_helium):
+def test_comp_ng_host(cuda, pkg, orc, nk, dz, ncol, calc_helium, assembly_mode):
     F, C = pkg.synth.comp_inputs(nk, ncol, dz, 21 + nk, calc_helium=calc_helium)
     out = [np.zeros((nk, ncol), order="F") for _ in range(3)]
     assert pkg.comp_ng(F, C, *out) == pkg.TG_OK
@@ -130,7 +130,7 @@ def test_comp_ng_host(cuda, pkg, orc, nk, dz, ncol, calc_helium):
         assert _rel(got, want) <= COMP_TOL
 
 
-def test_comp_ng_device_system_and_solution(cuda, pkg, orc):
+def test_comp_ng_device_system_and_solution(cuda, pkg, orc, assembly_mode):
     torch = cuda
     nk, ncol, dz = 57, 1000, 0.25
     F, C = pkg.synth.comp_inputs(nk, ncol, dz, 8)

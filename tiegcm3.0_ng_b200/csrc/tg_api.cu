@@ -824,7 +824,7 @@ __attribute__((visibility("default"))) int tg_comp_ng_dev(const tg_comp_fields *
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
-    if ((rc = grow(cx->scratch[0], sizeof(double) * 12 * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
+    if ((rc = grow(cx->scratch[0], sizeof(double) * comp_scratch_doubles(nk, ld > 0 ? ld : 1)))) return rc;
     TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
     TG_CUDA(launch_comp_ng(*F, *C, out, (double *)cx->scratch[0].p, nk, ncol, ld, system_out, cx->flags, st));
     if (status_dev) {
@@ -853,7 +853,7 @@ __attribute__((visibility("default"))) int tg_comp_ng(const tg_comp_fields *F, c
     // 15 fields + 12 fs slabs + 3 outputs, level-major; 3 2-D rows; 2 level profiles
     if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (30 * lvl + 3 * (size_t)ld + 2 * (size_t)nk)))) return rc;
     if ((rc = grow(c->colbuf[0][0], sizeof(double) * colsz))) return rc;
-    if ((rc = grow(c->scratch[0], sizeof(double) * 12 * lvl))) return rc;
+    if ((rc = grow(c->scratch[0], sizeof(double) * comp_scratch_doubles(nk, ld)))) return rc;
     double *base = (double *)c->lvlbuf[0][0].p, *stage = (double *)c->colbuf[0][0].p;
     cudaStream_t st = c->st[0];
     tg_comp_fields D;

@@ -672,34 +672,26 @@ __device__ __forceinline__ void comp_level(const CompConsts &C, double o2i, doub
 }  // namespace tg
 
 namespace tg {
-__global__ void __launch_bounds__(128) k_comp_ng(CompFields F, CompConsts C, double *out, double *scr, int nk, int ncol,
-                                                 long ld, double *sys_out, unsigned *status)
+// One column of comp_ng's rows and block solve (comp_ng.F90:170-332).  The
+// level quantities (ep, ak, wks4 and, at the top, the alpha entries of the
+// He-flux condition) come from Src: computed on the fly from the fields
+// (CompFusedSrc) or read from planes a level-parallel kernel wrote
+// (CompPlaneSrc).  first(L) gives level 0, next(k, L) level k+1, in order.
+template <class Src>
+__device__ __forceinline__ void comp_walk(const CompFields &F, const CompConsts &C, Src &src, double *out,
+                                          double *scr, int nk, long ld, long col, double *sys_out, unsigned *status)
 {
-    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
     auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
     const long slab = (long)nk * ld;
     const double tau = 1.86e+3, t00 = 273.;
     const double dz = C.dz, rdz = xd(1.0, dz);
-    const double tlbc = __ldg(F.tlbc + col), dfac = __ldg(F.dfactor + col);
+    const double dfac = __ldg(F.dfactor + col);
     const double flx_he = C.calc_helium ? __ldg(F.flx_he + col) : 0.0;
     const double *nms[3] = {F.o2nm_smooth, F.o1nm_smooth, F.henm_smooth};
     const double *adv[3] = {F.o2_advec, F.o1_advec, F.he_advec};
     const double *hd[3] = {F.hdo2, F.hdo1, F.hdhe};
-    // lower-boundary mixing ratios and level 1 (comp_ng.F90:74-96, 128-166)
-    double o2_0 = at(F.o2, 0), o1_0 = at(F.o1, 0), he_0 = at(F.he, 0), mb_0 = at(F.mbar, 0), tn_0 = at(F.tn, 0),
-           w_0 = at(F.w, 0);
-    double ps0[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-        ps0[i] = xa(xa(xa(xm(C.b[i], o2_0), xm(C.b[i + 3], o1_0)), xm(C.b[i + 6], he_0)), C.fb[i]);
-    const double embar0 =
-        xd(1.0, xa(xa(xa(xm(ps0[0], C.rmassinv_o2), xm(ps0[1], C.rmassinv_o1)), xm(ps0[2], C.rmassinv_he)),
-                   xm(xs(xs(xs(1.0, ps0[0]), ps0[1]), ps0[2]), C.rmassinv_n2)));
-    double embari_k = xm(0.5, xa(embar0, mb_0));
     CompLevel Lk, Lp;
-    comp_level(C, xm(0.5, xa(ps0[0], o2_0)), xm(0.5, xa(ps0[1], o1_0)), xm(0.5, xa(ps0[2], he_0)), embari_k, tlbc,
-               xd(xs(mb_0, embar0), dz), xd(xm(xs(tn_0, tlbc), 2.0), dz), true, Lp);
+    src.first(Lp);
     double G[9], z[3];
 #pragma unroll
     for (int e = 0; e < 9; ++e) G[e] = 0.0;
@@ -708,13 +700,9 @@ __global__ void __launch_bounds__(128) k_comp_ng(CompFields F, CompConsts C, dou
     bool ok = true;
     double flx00 = 1.0;
     for (int k = 0; k < nk - 1; ++k) {
-        const double o2_1 = at(F.o2, k + 1), o1_1 = at(F.o1, k + 1), he_1 = at(F.he, k + 1),
-                     mb_1 = at(F.mbar, k + 1), tn_1 = at(F.tn, k + 1), w_1 = at(F.w, k + 1);
         Lk = Lp;
-        const double embari_1 = xm(0.5, xa(mb_0, mb_1));
-        comp_level(C, xm(0.5, xa(o2_0, o2_1)), xm(0.5, xa(o1_0, o1_1)), xm(0.5, xa(he_0, he_1)), embari_1,
-                   xm(0.5, xa(tn_0, tn_1)), xd(xs(mb_1, mb_0), dz), xd(xs(tn_1, tn_0), dz), k + 1 != nk - 1, Lp);
-        const double wi = xm(0.5, xa(w_0, w_1));
+        src.next(k, Lp);
+        const double wi = xm(0.5, xa(at(F.w, k), at(F.w, k + 1)));
         const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1), ez = __ldg(F.expz + k);
         // mol / eddy coefficients and the rows (comp_ng.F90:213-244)
         const double eddyp = xm(xm(C.expzmid_inv, difk0), xs(rdz, Lk.wks4));
@@ -768,7 +756,9 @@ __global__ void __launch_bounds__(128) k_comp_ng(CompFields F, CompConsts C, dou
 #pragma unroll
                 for (int i = 0; i < 3; ++i) Q[i + 3 * m] = xa(Q[i + 3 * m], xm(ratio, R[i + 3 * m]));
             }
-            flx00 = xd(xm(xm(xm(embari_k, C.rmassinv_n2), C.p0), pow(xd(t00, tn_0), 0.25)), xm(tau, C.grav));
+            // embari and tn of level k (k = nk-2 >= 1)
+            const double embari_k = xm(0.5, xa(at(F.mbar, k - 1), at(F.mbar, k)));
+            flx00 = xd(xm(xm(xm(embari_k, C.rmassinv_n2), C.p0), pow(xd(t00, at(F.tn, k)), 0.25)), xm(tau, C.grav));
             const double d2 = xm(flx00, xs(rdz, xm(0.5, Lp.ep[1]))), d3 = xm(flx00, xs(rdz, xm(0.5, Lp.ep[2])));
 #pragma unroll
             for (int i = 0; i < 3; ++i)
@@ -823,13 +813,6 @@ __global__ void __launch_bounds__(128) k_comp_ng(CompFields F, CompConsts C, dou
 #pragma unroll
             for (int i = 0; i < 3; ++i) sg[(long)(9 + i) * ld] = z[i];
         }
-        o2_0 = o2_1;
-        o1_0 = o1_1;
-        he_0 = he_1;
-        mb_0 = mb_1;
-        tn_0 = tn_1;
-        w_0 = w_1;
-        embari_k = embari_1;
     }
     // back sweep (comp_ng.F90:317-324); x(nk-1) = z_{nk-1}
     bool fin = true;
@@ -878,15 +861,148 @@ __global__ void __launch_bounds__(128) k_comp_ng(CompFields F, CompConsts C, dou
     if (!ok || !fin) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
+// Level quantities computed from the fields with a window of two levels.
+struct CompFusedSrc {
+    const CompFields &F;
+    const CompConsts &C;
+    long ld, col;
+    int nk;
+    double o2_0, o1_0, he_0, mb_0, tn_0;
+    __device__ __forceinline__ double at(const double *p, int k) const { return __ldg(p + k * ld + col); }
+    __device__ __forceinline__ void first(CompLevel &L)
+    {
+        // lower-boundary mixing ratios and level 1 (comp_ng.F90:74-96, 128-166)
+        const double dz = C.dz, tlbc = __ldg(F.tlbc + col);
+        o2_0 = at(F.o2, 0);
+        o1_0 = at(F.o1, 0);
+        he_0 = at(F.he, 0);
+        mb_0 = at(F.mbar, 0);
+        tn_0 = at(F.tn, 0);
+        double ps0[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            ps0[i] = xa(xa(xa(xm(C.b[i], o2_0), xm(C.b[i + 3], o1_0)), xm(C.b[i + 6], he_0)), C.fb[i]);
+        const double embar0 =
+            xd(1.0, xa(xa(xa(xm(ps0[0], C.rmassinv_o2), xm(ps0[1], C.rmassinv_o1)), xm(ps0[2], C.rmassinv_he)),
+                       xm(xs(xs(xs(1.0, ps0[0]), ps0[1]), ps0[2]), C.rmassinv_n2)));
+        comp_level(C, xm(0.5, xa(ps0[0], o2_0)), xm(0.5, xa(ps0[1], o1_0)), xm(0.5, xa(ps0[2], he_0)),
+                   xm(0.5, xa(embar0, mb_0)), tlbc, xd(xs(mb_0, embar0), dz), xd(xm(xs(tn_0, tlbc), 2.0), dz), true, L);
+    }
+    __device__ __forceinline__ void next(int k, CompLevel &L)
+    {
+        const double dz = C.dz;
+        const double o2_1 = at(F.o2, k + 1), o1_1 = at(F.o1, k + 1), he_1 = at(F.he, k + 1), mb_1 = at(F.mbar, k + 1),
+                     tn_1 = at(F.tn, k + 1);
+        comp_level(C, xm(0.5, xa(o2_0, o2_1)), xm(0.5, xa(o1_0, o1_1)), xm(0.5, xa(he_0, he_1)),
+                   xm(0.5, xa(mb_0, mb_1)), xm(0.5, xa(tn_0, tn_1)), xd(xs(mb_1, mb_0), dz), xd(xs(tn_1, tn_0), dz),
+                   k + 1 != nk - 1, L);
+        o2_0 = o2_1;
+        o1_0 = o1_1;
+        he_0 = he_1;
+        mb_0 = mb_1;
+        tn_0 = tn_1;
+    }
+};
+
+__global__ void __launch_bounds__(128) k_comp_ng(CompFields F, CompConsts C, double *out, double *scr, int nk, int ncol,
+                                                 long ld, double *sys_out, unsigned *status)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    CompFusedSrc src{F, C, ld, col, nk};
+    comp_walk(F, C, src, out, scr, nk, ld, col, sys_out, status);
+}
+
+// Planes of the level-parallel pass: ep (3), ak (9), wks4 at (e*nk + j)*ld +
+// col; the top level's a22, a33, a23, a32 in 4 rows of ld after them.
+constexpr int kCompPlanes = 13;
+
+__global__ void __launch_bounds__(128) k_comp_levels(CompFields F, CompConsts C, double *lv, int nk, int ncol, long ld)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (col >= ncol) return;
+    CompLevel L;
+    if (j == 0) {
+        CompFusedSrc src{F, C, ld, col, nk};
+        src.first(L);
+    } else {
+        auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+        const double dz = C.dz;
+        const double mb0 = at(F.mbar, j - 1), mb1 = at(F.mbar, j), tn0 = at(F.tn, j - 1), tn1 = at(F.tn, j);
+        comp_level(C, xm(0.5, xa(at(F.o2, j - 1), at(F.o2, j))), xm(0.5, xa(at(F.o1, j - 1), at(F.o1, j))),
+                   xm(0.5, xa(at(F.he, j - 1), at(F.he, j))), xm(0.5, xa(mb0, mb1)), xm(0.5, xa(tn0, tn1)),
+                   xd(xs(mb1, mb0), dz), xd(xs(tn1, tn0), dz), j != nk - 1, L);
+    }
+    const long slab = (long)nk * ld, o = (long)j * ld + col;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) lv[i * slab + o] = L.ep[i];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) lv[(3 + e) * slab + o] = L.ak[e];
+    lv[12 * slab + o] = L.wks4;
+    if (j == nk - 1) {
+        double *top = lv + kCompPlanes * slab;
+        top[col] = L.a22;
+        top[ld + col] = L.a33;
+        top[2 * ld + col] = L.a23;
+        top[3 * ld + col] = L.a32;
+    }
+}
+
+// Level quantities read back from the planes.
+struct CompPlaneSrc {
+    const double *lv;
+    long ld, col;
+    int nk;
+    __device__ __forceinline__ void load(int j, CompLevel &L) const
+    {
+        const long slab = (long)nk * ld, o = (long)j * ld + col;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) L.ep[i] = __ldg(lv + i * slab + o);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) L.ak[e] = __ldg(lv + (3 + e) * slab + o);
+        L.wks4 = __ldg(lv + 12 * slab + o);
+        if (j == nk - 1) {
+            const double *top = lv + kCompPlanes * slab;
+            L.a22 = __ldg(top + col);
+            L.a33 = __ldg(top + ld + col);
+            L.a23 = __ldg(top + 2 * ld + col);
+            L.a32 = __ldg(top + 3 * ld + col);
+        } else {
+            L.a22 = L.a33 = L.a23 = L.a32 = 0.0;
+        }
+    }
+    __device__ __forceinline__ void first(CompLevel &L) { load(0, L); }
+    __device__ __forceinline__ void next(int k, CompLevel &L) { load(k + 1, L); }
+};
+
+__global__ void __launch_bounds__(128) k_comp_rows(CompFields F, CompConsts C, const double *lv, double *out,
+                                                   double *scr, int nk, int ncol, long ld, double *sys_out,
+                                                   unsigned *status)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    CompPlaneSrc src{lv, ld, col, nk};
+    comp_walk(F, C, src, out, scr, nk, ld, col, sys_out, status);
+}
+
 cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out, double *scratch, int nk, int ncol,
                            long ld, double *sys_out, unsigned *status, cudaStream_t st)
 {
     if (ncol <= 0) return cudaSuccess;
     if (nk < 3) return cudaErrorInvalidValue;
     const int T = 128;
+    if (assembly_mode() == 1) {
+        double *lv = scratch + 12 * (long)nk * ld;   // after the Gamma/z scratch
+        k_comp_levels<<<dim3((ncol + T - 1) / T, nk), T, 0, st>>>(F, C, lv, nk, ncol, ld);
+        k_comp_rows<<<(ncol + T - 1) / T, T, 0, st>>>(F, C, lv, out, scratch, nk, ncol, ld, sys_out, status);
+        return cudaGetLastError();
+    }
     k_comp_ng<<<(ncol + T - 1) / T, T, 0, st>>>(F, C, out, scratch, nk, ncol, ld, sys_out, status);
     return cudaGetLastError();
 }
+
+size_t comp_scratch_doubles(int nk, long ld) { return (size_t)(12 + kCompPlanes) * nk * ld + 4 * (size_t)ld; }
 }  // namespace tg
 
 // comp_ng post-solve steps (src/comp_ng.F90:415-457), one thread per column.

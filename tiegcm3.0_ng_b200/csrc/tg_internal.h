@@ -145,8 +145,11 @@ void set_assembly_mode(int m);
 
 typedef tg_comp_fields CompFields;
 typedef tg_comp_consts CompConsts;
+// scratch: comp_scratch_doubles(nk, ld) doubles (the block solve's Gamma/z and,
+// in the two-pass form, the level planes)
 cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out, double *scratch, int nk, int ncol,
                            long ld, double *sys_out, unsigned *status, cudaStream_t st);
+size_t comp_scratch_doubles(int nk, long ld);
 cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, double dz, double dtsmooth,
                                 double dtsmooth_div2, int nk, int ncol, long ld, double *const *upd6,
                                 cudaStream_t st);
