@@ -456,8 +456,9 @@ def main():
     assembly = None
     if not args.skip_assembly:
         assembly = {}
-        for which, kern in (("dt", "k_dt_ng"), ("minor", "k_minor_ng"), ("comp", "k_comp_ng"),
-                            ("settei", "k_settei_ng"), ("oplus", "k_oplus_ng")):
+        for which, kern in (("dt", "k_dt_ng"), ("minor", "k_minor_levels+k_minor_rows"),
+                            ("comp", "k_comp_levels+k_comp_rows"), ("settei", "k_settei_levels+k_settei_rows"),
+                            ("oplus", "k_oplus_levels+k_oplus_rows")):
             launch, ncol_a, nbytes = assembly_setup(pkg, wl, which, dev)
             for _ in range(args.warmup):
                 launch(stream)

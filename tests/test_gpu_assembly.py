@@ -172,7 +172,7 @@ SETTEI_TOL = 1e-11
 
 @pytest.mark.parametrize("nk,dz,ncol,et,eh", [(57, 0.25, 3001, 0, 0), (29, 0.5, 2592, 1, 6), (113, 0.125, 400, 0, 6),
                                               (3, 0.5, 33, 1, 0)])
-def test_settei_ng_host(cuda, pkg, orc, nk, dz, ncol, et, eh):
+def test_settei_ng_host(cuda, pkg, orc, nk, dz, ncol, et, eh, assembly_mode):
     F, C, qt = pkg.synth.settei_inputs(nk, ncol, dz, 31 + nk, et=et, electron_heating=eh)
     te, ti = np.zeros((nk, ncol), order="F"), np.zeros((nk, ncol), order="F")
     q2 = qt.copy(order="F")
@@ -183,7 +183,7 @@ def test_settei_ng_host(cuda, pkg, orc, nk, dz, ncol, et, eh):
     assert _rel(q2, q2_r) <= SETTEI_TOL
 
 
-def test_settei_ng_device_system(cuda, pkg, orc):
+def test_settei_ng_device_system(cuda, pkg, orc, assembly_mode):
     torch = cuda
     nk, ncol, dz = 57, 1000, 0.25
     F, C, qt = pkg.synth.settei_inputs(nk, ncol, dz, 5, et=1, electron_heating=0)
@@ -221,7 +221,7 @@ OPLUS_TOL_COEF = 1e-12
 
 @pytest.mark.parametrize("nk,dz,ncol,cap", [(57, 0.25, 3001, 0.0), (29, 0.5, 2592, 1e7), (113, 0.125, 300, 0.0),
                                             (3, 0.5, 33, 1e5)])
-def test_oplus_ng_host(cuda, pkg, orc, nk, dz, ncol, cap):
+def test_oplus_ng_host(cuda, pkg, orc, nk, dz, ncol, cap, assembly_mode):
     F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 41 + nk, opdiffcap=cap)
     outs = [np.zeros((nk, ncol), order="F") for _ in range(5)]
     assert pkg.oplus_ng(F, C, *outs) == pkg.TG_OK
@@ -231,7 +231,7 @@ def test_oplus_ng_host(cuda, pkg, orc, nk, dz, ncol, cap):
         assert _rel(got, want) <= OPLUS_TOL_COEF
 
 
-def test_oplus_ng_device_system(cuda, pkg, orc):
+def test_oplus_ng_device_system(cuda, pkg, orc, assembly_mode):
     torch = cuda
     nk, ncol, dz = 57, 1000, 0.25
     F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 6)

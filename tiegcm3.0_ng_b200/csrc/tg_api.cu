@@ -966,8 +966,10 @@ __attribute__((visibility("default"))) int tg_settei_ng_dev(const tg_settei_fiel
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = grow(cx->scratch[0], sizeof(double) * settei_scratch_doubles(nk, ld > 0 ? ld : 1)))) return rc;
     TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_settei_ng(*F, *C, te_out, ti_out, qtotal, nk, ncol, ld, system_out, cx->flags, st));
+    TG_CUDA(launch_settei_ng(*F, *C, te_out, ti_out, qtotal, nk, ncol, ld, system_out, cx->flags, st,
+                             (double *)cx->scratch[0].p));
     if (status_dev) {
         k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
         TG_CUDA(cudaGetLastError());
@@ -1012,7 +1014,8 @@ __attribute__((visibility("default"))) int tg_settei_ng(const tg_settei_fields *
         dst[27 + i] = two + i * ld;
     }
     TG_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_settei_ng(D, *C, te_l, ti_l, qt, nk, ncol, ld, nullptr, c->flags, st));
+    if ((rc = grow(c->scratch[0], sizeof(double) * settei_scratch_doubles(nk, ld)))) return rc;
+    TG_CUDA(launch_settei_ng(D, *C, te_l, ti_l, qt, nk, ncol, ld, nullptr, c->flags, st, (double *)c->scratch[0].p));
     double *hout[3] = {te_out, ti_out, qtotal};
     double *dout[3] = {te_l, ti_l, qt};
     for (int i = 0; i < 3; ++i) {

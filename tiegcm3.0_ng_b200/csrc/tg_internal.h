@@ -156,9 +156,12 @@ cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, d
 
 typedef tg_settei_fields SetteiFields;
 typedef tg_settei_consts SetteiConsts;
+// scratch (settei_scratch_doubles(nk, ld) doubles, may be NULL): the level
+// planes of the two-pass form, used when assembly_mode() is 1
 cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, double *te_out, double *ti_out,
                              double *qtotal, int nk, int ncol, long ld, double *sys_out, unsigned *status,
-                             cudaStream_t st);
+                             cudaStream_t st, double *scratch);
+size_t settei_scratch_doubles(int nk, long ld);
 
 typedef tg_oplus_fields OplusFields;
 typedef tg_oplus_consts OplusConsts;

@@ -38,22 +38,89 @@ __device__ __forceinline__ double up(const double *p, int j, int nk, long ld, lo
 }
 }  // namespace
 
-__global__ void __launch_bounds__(128) k_oplus_ng(OplusFields F, OplusConsts C, double *opout, double *xiop2p,
-                                                  double *xiop2d, double *Fe, double *Fn, double *scr, int nk,
-                                                  int ncol, long ld, double *sys_out, unsigned *status)
+// Level quantities of level j of one column (oplus_ng.F90:112-169, 285-299):
+// dj, hdz, tp1, b.u, op_loss and op_prod into the scratch planes, xiop2p,
+// xiop2d and (if requested) Fe, Fn into the outputs.
+__device__ __forceinline__ void oplus_level(const OplusFields &F, const OplusConsts &C, double *scr, double *xiop2p,
+                                            double *xiop2d, double *Fe, double *Fn, int nk, long ld, long col, int j)
 {
-    extern __shared__ double smem_op[];
-    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
-    const int T = blockDim.x;
-    double *w2s = smem_op + threadIdx.x;
+    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+    auto S = [&](int e, int k) -> double & { return scr[(long)e * nk * ld + (long)k * ld + col]; };
+    const double dz = C.dz;
+    const double bx = __ldg(F.bx + col), by = __ldg(F.by + col), bz = __ldg(F.bz + col);
+    const bool capped = !(fabs(xs(C.opdiffcap, 0.)) < 1e-9);
+    const double sncs = Fe ? xm(sin(__ldg(F.dipmag + col)), cos(__ldg(F.dipmag + col))) : 0.;
+    const double ogg = xd(xm(C.rmass_op, C.grav), C.gask);
+
+    const double tn = at(F.tn, j), te = at(F.te, j), ti = at(F.ti, j), o2 = at(F.o2, j), o1 = at(F.o1, j),
+                 n2 = at(F.n2, j), he = at(F.he, j), xn = at(F.xnmbar, j), hj = at(F.scht, j),
+                 ne = at(F.ne, j);
+    const double tr = xm(0.5, xa(tn, ti));
+    const double lg = xs(1., xm(0.064, log10(tr)));
+    double vni = xm(xm(18.1, o2), C.rmassinv_o2);
+    vni = xa(vni, xm(xm(xm(xm(o1, C.rmassinv_o1), sqrt(tr)), xm(lg, lg)), C.colfac));
+    vni = xa(vni, xm(xm(3.6, he), C.rmassinv_he));
+    vni = xa(vni, xm(xm(18.6, n2), C.rmassinv_n2));
+    double dj = xd(1.42E17, xm(xn, vni));
+    vni = xm(xm(16., 3.53E-11), vni);
+    if (capped) {
+        const double cap = xd(C.opdiffcap, xa(1., pow(2., xs(__ldg(F.zpint + j), 6.))));
+        dj = dj < cap ? dj : cap;
+    }
+    const double wni = up(F.w, j, nk, ld, col);
+    S(S_DJ, j) = dj;
+    S(S_HDZ, j) = xd(1., xm(hj, dz));
+    S(S_TP1, j) = xm(0.5, xa(ti, te));
+    S(S_BDOTU, j) = xa(xa(xm(bx, at(F.u, j)), xm(by, at(F.v, j))), xm(xm(hj, bz), wni));
+    if (Fe) {
+        auto tpop = [&](int i) { return xm(xa(at(F.te, i), at(F.ti, i)), at(F.op, i)); };
+        double d;
+        if (j == 0) d = xs(tpop(1), tpop(0));
+        else if (j == nk - 1) d = xs(tpop(nk - 1), tpop(nk - 2));
+        else if (j == nk - 2) d = xs(tpop(nk - 2), tpop(nk - 3));
+        else d = xd(xs(tpop(j + 1), tpop(j - 1)), 2.);
+        const double diffj = xa(xm(xd(1., xm(hj, C.dlev)), d), xm(ogg, at(F.op, j)));
+        const double wd = xm(xm(vni, diffj), dj);
+        Fe[j * ld + col] = xm(xm(wd, sncs), __ldg(F.sndec + col));
+        Fn[j * ld + col] = xm(xm(wd, sncs), __ldg(F.csdec + col));
+    }
+    // chemistry (oplus_ng.F90:285-299)
+    const double rk19 = at(F.rk19, j), rk20 = at(F.rk20, j), rk25 = at(F.rk25, j);
+    const double den2p = xa(xa(xa(xm(xn, xa(xm(xm(xa(C.rk16, C.rk17), n2), C.rmassinv_n2),
+                                            xm(xm(C.rk18, o1), C.rmassinv_o1))),
+                                  xm(xa(rk19, rk20), ne)),
+                               C.rk21),
+                            C.rk22);
+    const double x2p = xd(up(F.qop2p, j, nk, ld, col), den2p);
+    const double den2d =
+        xa(xa(xm(xn, xa(xa(xm(xm(C.rk23, n2), C.rmassinv_n2), xm(xm(C.rk24, o1), C.rmassinv_o1)),
+                        xm(xm(C.rk26, o2), C.rmassinv_o2))),
+              xm(rk25, ne)),
+           C.rk27);
+    const double x2d = xd(xa(up(F.qop2d, j, nk, ld, col), xm(xa(xm(rk20, ne), C.rk22), x2p)), den2d);
+    xiop2p[j * ld + col] = x2p;
+    xiop2d[j * ld + col] = x2d;
+    S(S_OL, j) = xm(xn, xa(xa(xm(xm(at(F.rk1, j), o2), C.rmassinv_o2), xm(xm(at(F.rk2, j), n2), C.rmassinv_n2)),
+                            xm(xm(C.rk10, at(F.n2d, j)), C.rmassinv_n2d)));
+    double prod = xa(up(F.qop, j, nk, ld, col), xm(xa(xm(rk19, ne), C.rk21), x2p));
+    prod = xa(prod, xm(xa(xm(rk25, ne), C.rk27), x2d));
+    prod = xa(prod, xm(xm(xm(xa(xm(C.rk18, x2p), xm(C.rk24, x2d)), o1), C.rmassinv_o1), xn));
+    S(S_PROD, j) = prod;
+}
+
+// Rows k = 0..nk-2 from the level planes, the forward sweep and the back
+// sweep of one column (oplus_ng.F90:88-99, 209-307).
+__device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusConsts &C, double *opout, const double *scr,
+                                           double *w2s, int T, int nk, long ld, long col, double *sys_out,
+                                           unsigned *status)
+{
     const long slab = (long)nk * ld;
     auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
-    auto S = [&](int e, int k) -> double & { return scr[(long)e * slab + (long)k * ld + col]; };
+    auto S = [&](int e, int k) { return scr[(long)e * slab + (long)k * ld + col]; };
     // pi = 4*atan(1) of the reference, correctly rounded
-    const double pi = 3.141592653589793, rtd = 180. / pi, dz = C.dz;
+    const double pi = 3.141592653589793, rtd = 180. / pi;
     const double phid = 2.0e8, phin = -2.0e8, ppolar = 0.;
-    const double bx = __ldg(F.bx + col), by = __ldg(F.by + col), bz = __ldg(F.bz + col);
+    const double bz = __ldg(F.bz + col);
     // oplus_flux (oplus_ng.F90:88-99)
     double opflux;
     {
@@ -68,66 +135,6 @@ __global__ void __launch_bounds__(128) k_oplus_ng(OplusFields F, OplusConsts C, 
         if (xm(xs(cd, 80.), xs(cd, 100.)) < 0.)
             opflux = xa(xm(.5, xa(fed, fen)), xm(xm(.5, xs(fed, fen)), cos(xd(xm(pi, xs(cd, 80.)), 20.))));
         if (arl >= xd(pi, 3.)) opflux = xa(opflux, ppolar);
-    }
-    const bool capped = !(fabs(xs(C.opdiffcap, 0.)) < 1e-9);
-    const double sncs = Fe ? xm(sin(__ldg(F.dipmag + col)), cos(__ldg(F.dipmag + col))) : 0.;
-    const double ogg = xd(xm(C.rmass_op, C.grav), C.gask);
-    // ---- pass 1: level quantities (oplus_ng.F90:112-169, 285-299)
-    for (int j = 0; j < nk; ++j) {
-        const double tn = at(F.tn, j), te = at(F.te, j), ti = at(F.ti, j), o2 = at(F.o2, j), o1 = at(F.o1, j),
-                     n2 = at(F.n2, j), he = at(F.he, j), xn = at(F.xnmbar, j), hj = at(F.scht, j),
-                     ne = at(F.ne, j);
-        const double tr = xm(0.5, xa(tn, ti));
-        const double lg = xs(1., xm(0.064, log10(tr)));
-        double vni = xm(xm(18.1, o2), C.rmassinv_o2);
-        vni = xa(vni, xm(xm(xm(xm(o1, C.rmassinv_o1), sqrt(tr)), xm(lg, lg)), C.colfac));
-        vni = xa(vni, xm(xm(3.6, he), C.rmassinv_he));
-        vni = xa(vni, xm(xm(18.6, n2), C.rmassinv_n2));
-        double dj = xd(1.42E17, xm(xn, vni));
-        vni = xm(xm(16., 3.53E-11), vni);
-        if (capped) {
-            const double cap = xd(C.opdiffcap, xa(1., pow(2., xs(__ldg(F.zpint + j), 6.))));
-            dj = dj < cap ? dj : cap;
-        }
-        const double wni = up(F.w, j, nk, ld, col);
-        S(S_DJ, j) = dj;
-        S(S_HDZ, j) = xd(1., xm(hj, dz));
-        S(S_TP1, j) = xm(0.5, xa(ti, te));
-        S(S_BDOTU, j) = xa(xa(xm(bx, at(F.u, j)), xm(by, at(F.v, j))), xm(xm(hj, bz), wni));
-        if (Fe) {
-            auto tpop = [&](int i) { return xm(xa(at(F.te, i), at(F.ti, i)), at(F.op, i)); };
-            double d;
-            if (j == 0) d = xs(tpop(1), tpop(0));
-            else if (j == nk - 1) d = xs(tpop(nk - 1), tpop(nk - 2));
-            else if (j == nk - 2) d = xs(tpop(nk - 2), tpop(nk - 3));
-            else d = xd(xs(tpop(j + 1), tpop(j - 1)), 2.);
-            const double diffj = xa(xm(xd(1., xm(hj, C.dlev)), d), xm(ogg, at(F.op, j)));
-            const double wd = xm(xm(vni, diffj), dj);
-            Fe[j * ld + col] = xm(xm(wd, sncs), __ldg(F.sndec + col));
-            Fn[j * ld + col] = xm(xm(wd, sncs), __ldg(F.csdec + col));
-        }
-        // chemistry (oplus_ng.F90:285-299)
-        const double rk19 = at(F.rk19, j), rk20 = at(F.rk20, j), rk25 = at(F.rk25, j);
-        const double den2p = xa(xa(xa(xm(xn, xa(xm(xm(xa(C.rk16, C.rk17), n2), C.rmassinv_n2),
-                                                xm(xm(C.rk18, o1), C.rmassinv_o1))),
-                                      xm(xa(rk19, rk20), ne)),
-                                   C.rk21),
-                                C.rk22);
-        const double x2p = xd(up(F.qop2p, j, nk, ld, col), den2p);
-        const double den2d =
-            xa(xa(xm(xn, xa(xa(xm(xm(C.rk23, n2), C.rmassinv_n2), xm(xm(C.rk24, o1), C.rmassinv_o1)),
-                            xm(xm(C.rk26, o2), C.rmassinv_o2))),
-                  xm(rk25, ne)),
-               C.rk27);
-        const double x2d = xd(xa(up(F.qop2d, j, nk, ld, col), xm(xa(xm(rk20, ne), C.rk22), x2p)), den2d);
-        xiop2p[j * ld + col] = x2p;
-        xiop2d[j * ld + col] = x2d;
-        S(S_OL, j) = xm(xn, xa(xa(xm(xm(at(F.rk1, j), o2), C.rmassinv_o2), xm(xm(at(F.rk2, j), n2), C.rmassinv_n2)),
-                                xm(xm(C.rk10, at(F.n2d, j)), C.rmassinv_n2d)));
-        double prod = xa(up(F.qop, j, nk, ld, col), xm(xa(xm(rk19, ne), C.rk21), x2p));
-        prod = xa(prod, xm(xa(xm(rk25, ne), C.rk27), x2d));
-        prod = xa(prod, xm(xm(xm(xa(xm(C.rk18, x2p), xm(C.rk24, x2d)), o1), C.rmassinv_o1), xn));
-        S(S_PROD, j) = prod;
     }
     // ---- pass 2: rows and the forward sweep (oplus_ng.F90:209-303)
     const double dvbz = xd(__ldg(F.dvb + col), bz), bz2 = xm(bz, bz);
@@ -227,6 +234,36 @@ __global__ void __launch_bounds__(128) k_oplus_ng(OplusFields F, OplusConsts C, 
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
+__global__ void __launch_bounds__(128) k_oplus_ng(OplusFields F, OplusConsts C, double *opout, double *xiop2p,
+                                                  double *xiop2d, double *Fe, double *Fn, double *scr, int nk,
+                                                  int ncol, long ld, double *sys_out, unsigned *status)
+{
+    extern __shared__ double smem_op[];
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    for (int j = 0; j < nk; ++j) oplus_level(F, C, scr, xiop2p, xiop2d, Fe, Fn, nk, ld, col, j);
+    oplus_walk(F, C, opout, scr, smem_op + threadIdx.x, blockDim.x, nk, ld, col, sys_out, status);
+}
+
+// Two-pass form: the level quantities with one thread per (level, column),
+// then the column walk.
+__global__ void __launch_bounds__(128) k_oplus_levels(OplusFields F, OplusConsts C, double *xiop2p, double *xiop2d,
+                                                      double *Fe, double *Fn, double *scr, int nk, int ncol, long ld)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    oplus_level(F, C, scr, xiop2p, xiop2d, Fe, Fn, nk, ld, col, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(128) k_oplus_rows(OplusFields F, OplusConsts C, double *opout, const double *scr,
+                                                    int nk, int ncol, long ld, double *sys_out, unsigned *status)
+{
+    extern __shared__ double smem_or[];
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    oplus_walk(F, C, opout, scr, smem_or + threadIdx.x, blockDim.x, nk, ld, col, sys_out, status);
+}
+
 cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *opout, double *xiop2p,
                             double *xiop2d, double *Fe, double *Fn, double *scratch, int nk, int ncol, long ld,
                             double *sys_out, unsigned *status, cudaStream_t st)
@@ -245,6 +282,18 @@ cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *
     const size_t per = (size_t)(nk - 1) * sizeof(double);
     while (T > 32 && (size_t)T * per > (size_t)optin) T /= 2;
     if ((size_t)T * per > (size_t)optin) return cudaErrorInvalidValue;
+    if (assembly_mode() == 1) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_oplus_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+            attr = true;
+        }
+        k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, xiop2p, xiop2d, Fe, Fn, scratch, nk, ncol,
+                                                                     ld);
+        k_oplus_rows<<<(ncol + T - 1) / T, T, (size_t)T * per, st>>>(F, C, opout, scratch, nk, ncol, ld, sys_out,
+                                                                     status);
+        return cudaGetLastError();
+    }
     k_oplus_ng<<<(ncol + T - 1) / T, T, (size_t)T * per, st>>>(F, C, opout, xiop2p, xiop2d, Fe, Fn, scratch, nk, ncol,
                                                                ld, sys_out, status);
     return cudaGetLastError();

@@ -341,9 +341,205 @@ __global__ void __launch_bounds__(128) k_settei_ng(SetteiFields F, SetteiConsts 
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
+// ---------------------------------------------------------------------------
+// settei_ng in two passes.  Everything expensive (the conductivity tek0 of
+// each interface and the heating / cooling / exchange rates of each level,
+// with their exp, log and pow) is independent across levels: the first
+// kernel computes it with one thread per (level, column) into 10 level-major
+// planes; the second walks each column once, forming the rows from the
+// planes, solving and finishing Te, Ti and qtotal.  Same operations as
+// k_settei_ng.
+// ---------------------------------------------------------------------------
+namespace {
+enum { P_TEK0 = 0, P_TH, P_DQ, P_QE, P_ET, P_LENTN, P_LEITI, P_LEI, P_LIN, P_QENI, P_N };
+
+__device__ __forceinline__ double settei_fe(const SetteiFields &F, const SetteiConsts &C, long col)
+{
+    const double pi = 3.141592653589793, rtd = 180.0 / pi, ev = C.evergs, fpolar = -3.0e+9;
+    const double f107te = C.f107 < 235. ? C.f107 : 235.;
+    const double arl = fabs(__ldg(F.rlatm + col)), chi = __ldg(F.chi + col), qa = __ldg(F.qteaur + col);
+    double a = 0.;
+    if (arl >= xd(pi, 4.5)) a = 1.;
+    if (arl < xd(pi, 4.5) && arl > xd(pi, 18.)) a = xm(.5, xa(1., cos(xs(xm(arl, 6.), xd(xm(pi, 4.), 3.)))));
+    if (arl <= xd(pi, 18.)) a = 0.;
+    double fed = xm(xm(-9.0e+7, f107te), a);
+    double fen = xd(fed, 2.);
+    fed = xa(fed, qa);
+    fen = xa(fen, qa);
+    double fe = chi >= xm(.5, pi) ? fen : fed;
+    const double cd = xm(chi, rtd);
+    if (xm(xs(cd, 80.), xs(cd, 100.)) >= 0.) fe = xm(fe, ev);
+    else fe = xm(xa(xm(.5, xa(fed, fen)), xm(xm(.5, xs(fed, fen)), cos(xd(xm(pi, xs(cd, 80.)), 20.)))), ev);
+    if (arl >= xd(pi, 3.)) fe = xa(fe, xm(fpolar, ev));
+    return fe;
+}
+}  // namespace
+
+__global__ void __launch_bounds__(128) k_settei_levels(SetteiFields F, SetteiConsts C, double *lv, int nk, int ncol,
+                                                       long ld)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (col >= ncol) return;
+    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+    const long o = (long)j * ld + col;
+    const Lev L = load_lev(F, o);
+    // interface j (settei_ng.F90:89-139)
+    Iface I;
+    if (j == 0) {
+        const double *b = C.b, *fb = C.fb, t_lbc = __ldg(F.t_lbc + col);
+        const Lev L1 = load_lev(F, ld + col);
+        const double te_int = dmax(xs(xm(1.5, L.te), xm(.5, L1.te)), t_lbc);
+        const double o2n = xm(.5, xa(xa(xa(fb[0], xm(xa(b[0], 1.), L.o2)), xm(b[3], L.o1)), xm(b[6], L.he)));
+        const double o1n = xm(.5, xa(xa(xa(fb[0], xm(b[0], L.o2)), xm(xa(b[3], 1.), L.o1)), xm(b[6], L.he)));
+        const double hen = xm(.5, xa(xa(xa(fb[0], xm(b[0], L.o2)), xm(b[3], L.o1)), xm(xa(b[6], 1.), L.he)));
+        const double n2n = dmax(xs(xs(xs(1., o2n), o1n), hen), 0.);
+        I = iface(C, te_int, o2n, o1n, hen, n2n, t_lbc, at(F.xnmbari, 0), at(F.ne, 0), at(F.schti, 0));
+    } else {
+        const Lev Lm = load_lev(F, o - ld);
+        double te_int, tn_int;
+        if (j == nk - 1) {
+            const Lev Lmm = load_lev(F, o - 2 * ld);
+            te_int = xs(xm(1.5, Lm.te), xm(.5, Lmm.te));
+            tn_int = xs(xm(1.5, Lm.tn), xm(.5, Lmm.tn));
+        } else {
+            te_int = xm(.5, xa(L.te, Lm.te));
+            tn_int = xm(.5, xa(L.tn, Lm.tn));
+        }
+        I = iface(C, te_int, xm(.5, xa(L.o2, Lm.o2)), xm(.5, xa(L.o1, Lm.o1)), xm(.5, xa(L.he, Lm.he)),
+                  xm(.5, xa(L.n2, Lm.n2)), tn_int, at(F.xnmbari, j), at(F.ne, j), at(F.schti, j));
+    }
+    // heating, cooling and exchange of level j (settei_ng.F90:157-246)
+    const double ne0 = at(F.ne, j);
+    double qtot, rne_raw;
+    if (j < nk - 1) {
+        qtot = sqrt(xm(qsum(F, o), qsum(F, o + ld)));
+        rne_raw = xm(ne0, at(F.ne, j + 1));
+    } else {
+        qtot = 0.;
+        rne_raw = xd(xm(xm(ne0, ne0), ne0), at(F.ne, nk - 2));
+    }
+    const Loss R = level_loss(F, C, o, L, rne_raw, qtot);
+    const long slab = (long)nk * ld;
+    lv[P_TEK0 * slab + o] = I.tek0;
+    lv[P_TH * slab + o] = I.th;
+    lv[P_DQ * slab + o] = R.dq;
+    lv[P_QE * slab + o] = R.qe_h;
+    lv[P_ET * slab + o] = R.et_h;
+    lv[P_LENTN * slab + o] = R.len_tn;
+    lv[P_LEITI * slab + o] = R.lei_ti;
+    lv[P_LEI * slab + o] = R.lei;
+    lv[P_LIN * slab + o] = R.lin;
+    lv[P_QENI * slab + o] = R.q_eni;
+}
+
+__global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConsts C, const double *lv, double *te_out,
+                                                     double *ti_out, double *qtotal, int nk, int ncol, long ld,
+                                                     double *sys_out, unsigned *status)
+{
+    extern __shared__ double smem_tr[];
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int T = blockDim.x;
+    double *w2s = smem_tr + threadIdx.x;
+    const long slab = (long)nk * ld;
+    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+    auto pl = [&](int e, int k) { return __ldg(lv + e * slab + (long)k * ld + col); };
+    const double dz = C.dz, fe = settei_fe(F, C, col);
+    double sindip;
+    {
+        const double dm = fabs(__ldg(F.dipmag + col));
+        const double sn = sin(dm > C.dipmin ? dm : C.dipmin);
+        sindip = dmax(xm(sn, sn), .10);
+    }
+    const double t_lbc = __ldg(F.t_lbc + col);
+    double qe_m1 = 0., w1 = 0., w3 = 0., rprev = 0.;
+    double th_k = pl(P_TH, 0);
+    bool ok = true;
+    for (int k = 0; k < nk; ++k) {
+        const long o = (long)k * ld + col;
+        const double q_eni = pl(P_QENI, k);
+        // qtotal += q_eni at the interfaces (settei_ng.F90:248-254)
+        if (k == 1) qtotal[col] = xa(qtotal[col], xs(xm(1.5, qe_m1), xm(0.5, q_eni)));
+        if (k >= 1 && k <= nk - 2) qtotal[o] = xa(qtotal[o], xm(.5, xa(qe_m1, q_eni)));
+        if (k == nk - 2) {
+            const double qe_prev = k >= 1 ? qe_m1 : 0.;
+            qtotal[(long)(nk - 1) * ld + col] = xa(qtotal[(long)(nk - 1) * ld + col], xs(xm(1.5, q_eni), xm(0.5, qe_prev)));
+        }
+        if (k <= nk - 2) {
+            const double th_1 = pl(P_TH, k + 1);
+            const double pb = xm(xd(xd(2., 7.), xm(at(F.scht, k), xm(dz, dz))), sindip);
+            double r = xm(pb, th_1);
+            double p = xm(pb, th_k);
+            double q = -xa(p, r);
+            double rhs = 0.;
+            if (k == 0) {
+                q = xs(q, p);
+                rhs = xs(rhs, xm(xm(2., p), pow(t_lbc, 3.5)));
+                p = 0.;
+            }
+            if (k == nk - 2) {
+                q = xa(q, r);
+                rhs = xa(rhs, xd(xm(xm(xm(xm(r, dz), 3.5), at(F.schti, nk - 1)), fe), pl(P_TEK0, nk - 1)));
+                r = 0.;
+            }
+            rhs = xs(rhs, pl(P_QE, k));
+            if (C.et) rhs = xs(rhs, pl(P_ET, k));
+            q = xs(q, pl(P_DQ, k));
+            rhs = xs(xs(rhs, pl(P_LENTN, k)), pl(P_LEITI, k));
+            if (sys_out) {
+                sys_out[o] = p;
+                sys_out[slab + o] = q;
+                sys_out[2 * slab + o] = r;
+                sys_out[3 * slab + o] = rhs;
+            }
+            if (k == 0) {
+                w1 = q;
+                w3 = xd(rhs, w1);
+            } else {
+                const double w2 = xd(rprev, w1);
+                w2s[(long)(k - 1) * T] = w2;
+                w1 = xs(q, xm(p, w2));
+                w3 = xd(xs(rhs, xm(p, w3)), w1);
+            }
+            ok = ok && fabs(w1) <= DBL_MAX && w1 != 0.0;
+            te_out[o] = w3;
+            rprev = r;
+            th_k = th_1;
+        }
+        qe_m1 = q_eni;
+    }
+    const int K = nk - 1;
+    double xn = w3;
+    double tk = pow(xn, xd(2., 7.));
+    double t_top1 = tk, t_top2 = 0.;
+    bool fin = fabs(xn) <= DBL_MAX;
+    auto finish = [&](int k, double t) {
+        const long o = (long)k * ld + col;
+        const double tn = at(F.tn, k);
+        const double te = dmax(t, tn);
+        const double lei = pl(P_LEI, k), lin = pl(P_LIN, k);
+        te_out[o] = te;
+        const double num = xa(xa(xd(xm(at(F.qji_ti, k), at(F.xnmbar, k)), C.avo), xm(lei, te)), xm(lin, tn));
+        ti_out[o] = dmax(xd(num, xa(lei, lin)), tn);
+    };
+    finish(K - 1, tk);
+    for (int k = K - 2; k >= 0; --k) {
+        xn = xs(te_out[(long)k * ld + col], xm(w2s[(long)k * T], xn));
+        fin = fin && fabs(xn) <= DBL_MAX;
+        tk = pow(xn, xd(2., 7.));
+        if (k == K - 2) t_top2 = tk;
+        finish(k, tk);
+    }
+    finish(K, xd(xm(t_top1, t_top1), t_top2));
+    if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+}
+
+size_t settei_scratch_doubles(int nk, long ld) { return (size_t)P_N * nk * ld; }
+
 cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, double *te_out, double *ti_out,
                              double *qtotal, int nk, int ncol, long ld, double *sys_out, unsigned *status,
-                             cudaStream_t st)
+                             cudaStream_t st, double *scratch)
 {
     if (ncol <= 0) return cudaSuccess;
     if (nk < 3) return cudaErrorInvalidValue;
@@ -360,6 +556,20 @@ cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, doubl
     const size_t per = (size_t)(2 * nk - 1) * sizeof(double);
     while (T > 32 && (size_t)T * per > (size_t)optin) T /= 2;
     if ((size_t)T * per > (size_t)optin) return cudaErrorInvalidValue;
+    if (scratch && assembly_mode() == 1) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_settei_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+            attr = true;
+        }
+        int T2 = 128;
+        const size_t per2 = (size_t)(nk - 1) * sizeof(double);
+        while (T2 > 32 && (size_t)T2 * per2 > (size_t)optin) T2 /= 2;
+        k_settei_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch, nk, ncol, ld);
+        k_settei_rows<<<(ncol + T2 - 1) / T2, T2, (size_t)T2 * per2, st>>>(F, C, scratch, te_out, ti_out, qtotal, nk,
+                                                                           ncol, ld, sys_out, status);
+        return cudaGetLastError();
+    }
     k_settei_ng<<<(ncol + T - 1) / T, T, (size_t)T * per, st>>>(F, C, te_out, ti_out, qtotal, nk, ncol, ld, sys_out,
                                                                 status);
     return cudaGetLastError();
