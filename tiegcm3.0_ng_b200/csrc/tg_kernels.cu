@@ -536,40 +536,36 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
                 if (lane == 0) report(status, s.status_idx, FLAG_TIMEOUT);
                 return;
             }
+            // the stage is read in place and handed back to the copy engine
+            // after the L levels are done (registers stay low: more warps/SM)
             const double *stg = buf + (int)(qc % C) * NE * 32 + lane;
-            double va[L], vb[L], vc[L], vf[L];
-#pragma unroll
-            for (int l = 0; l < L; ++l) {
-                va[l] = stg[(4 * l + 0) * 32];
-                vb[l] = stg[(4 * l + 1) * 32];
-                vc[l] = stg[(4 * l + 2) * 32];
-                vf[l] = stg[(4 * l + 3) * 32];
-            }
-            __syncwarp();
-            fence_proxy_async();
-            if (j + C < nch) issue(qc + C, j + C);
             if (valid) {
 #pragma unroll
                 for (int l = 0; l < L; ++l) {
                     const int k = j * L + l;
                     if (k < k2) {
+                        const double ak = stg[(4 * l + 0) * 32], bk = stg[(4 * l + 1) * 32],
+                                     fk = stg[(4 * l + 3) * 32];
                         if (k == 0) {
-                            w1 = vb[l];
+                            w1 = bk;
                             y1 = __drcp_rn(w1);
-                            w3 = qdiv(vf[l], w1, y1);
+                            w3 = qdiv(fk, w1, y1);
                         } else {
                             const double w2 = qdiv(cprev, w1, y1);
                             st_hint(&w2s[(k - 1) * ws], w2, keep);
-                            w1 = xsub(vb[l], xmul(va[l], w2));
+                            w1 = xsub(bk, xmul(ak, w2));
                             y1 = __drcp_rn(w1);
-                            w3 = qdiv(xsub(vf[l], xmul(va[l], w3)), w1, y1);
+                            w3 = qdiv(xsub(fk, xmul(ak, w3)), w1, y1);
                         }
                         ok = ok && finite_nz(w1);
-                        cprev = vc[l];
+                        cprev = stg[(4 * l + 2) * 32];
                         st_hint(&px[k * ld], w3, keep);
                     }
                 }
             }
+            __syncwarp();
+            fence_proxy_async();
+            if (j + C < nch) issue(qc + C, j + C);
         }
         q += nch;
         if (valid) {
@@ -1863,6 +1859,7 @@ TileCfg g_tile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 0, 0, 8, 4, 0, 
                         {{128, 1, 0, 0, 4, 4, 0, 32, 1}, {128, 1, 0, 0, 4, 4, 0, 32, 1}}};
 int kind_index(int kind) { return kind == TG_KIND_SCALAR ? 0 : (kind == TG_KIND_BLOCK2 ? 1 : 2); }
 int g_num_sms = -1;
+int g_carveout = cudaSharedmemCarveoutMaxShared;   // percent of the unified L1/shared store
 int g_smem_optin = -1;
 
 // Register-prefetch scalar kernels by (columns per thread, prefetch depth).
@@ -1964,6 +1961,9 @@ template <typename K>
 void allow_smem(K k, int lim)
 {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    // the rings live in shared memory and the coefficient streams bypass L1:
+    // prefer the largest shared-memory carveout so that more warps fit per SM
+    cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, g_carveout);
 }
 
 int num_sms()
