@@ -446,6 +446,18 @@ int tg_set_assembly_mode(int mode);
  * columns are in flight at once on large batches. */
 int tg_set_block_scratch_budget(double megabytes);
 
+/* Scalar kind, FP64 ring kernels: the L2 budget for the w2 scratch and the
+ * parked forward-sweep results (16 B per level and column) of all resident
+ * columns, in MB (default 128; <= 0 restores it).  It caps how many columns
+ * are in flight at once on large batches. */
+int tg_set_scalar_scratch_budget(double megabytes);
+
+/* How the kinds of one plan share the GPU: 1 the block kinds run on a side
+ * stream beside the scalar kind, 0 one kind after the other, any other
+ * value (default) side by side only when every kind's tiles fit in one
+ * resident wave.  Same results either way. */
+int tg_set_kind_overlap(int mode);
+
 /* Runs the ring kernels' bounded mbarrier wait on a barrier that nothing
  * completes, giving up after `polls` polls (1..2^22): *status_dev receives
  * TG_ETIMEOUT, as a solve does when a bulk copy never lands.  Tests the

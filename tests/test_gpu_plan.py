@@ -162,3 +162,28 @@ def test_ring_kernel_with_unaligned_stride_falls_back(cuda, pkg, orc):
     pkg.trsolv_dev(*t, x, 57, 57, 1000, pkg.TG_LAYOUT_LEVEL, ld)
     torch.cuda.synchronize()
     assert np.array_equal(pkg.batch.from_level_scalar(x, 1000), orc.trsolv_ng(a, b, c, f, 57))
+
+
+def test_kind_overlap_and_l2_budgets_keep_bits(cuda, pkg, orc):
+    """The kinds of a plan side by side or one after the other, and grids cut
+    down by tiny L2 budgets (several waves of tiles per warp), all give the
+    oracle's bits."""
+    torch = cuda
+    segs, refs_in = make_segments(pkg, torch, SPECS, seed=411)
+    try:
+        for overlap, scalar_mb, block_mb in [(1, 0, 0), (0, 0, 0), (-1, 0.05, 0.05), (0, 0.05, 0.05), (-1, 0, 0)]:
+            pkg.set_kind_overlap(overlap)
+            pkg.set_scalar_scratch_budget(scalar_mb)
+            pkg.set_block_scratch_budget(block_mb)
+            for s in segs:
+                s["x"].fill_(3.5)
+            plan = pkg.Plan(segs, pkg.TG_PREC_F64)
+            plan.execute()
+            rc, per = plan.status()
+            plan.close()
+            assert rc == pkg.TG_OK and per == [0] * len(SPECS), (overlap, scalar_mb, block_mb)
+            check(pkg, orc, segs, refs_in)
+    finally:
+        pkg.set_kind_overlap(-1)
+        pkg.set_scalar_scratch_budget(0)
+        pkg.set_block_scratch_budget(0)

@@ -41,7 +41,7 @@ EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor
            "tg_comp_ng_dev", "tg_comp_post_ng", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
-           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
+           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
 
 
@@ -224,6 +224,8 @@ def lib():
             "tg_set_stage_levels": [I, I, I],
             "tg_set_assembly_mode": [I],
             "tg_set_block_scratch_budget": [D],
+            "tg_set_scalar_scratch_budget": [D],
+            "tg_set_kind_overlap": [I],
             "tg_selftest_wait": [ctypes.c_uint, P, P],
             "tg_plan_sweep_histogram": [P, ctypes.POINTER(Lg), I],
             "tg_plan_destroy": [P],
@@ -617,6 +619,16 @@ def set_stage_levels(kind, precision, levels):
 def set_assembly_mode(mode):
     """Assembly kernels: 1 two passes (default), 0 one fused column walk, -1 default."""
     return _check(lib().tg_set_assembly_mode(int(mode)), "tg_set_assembly_mode")
+
+
+def set_scalar_scratch_budget(megabytes):
+    """L2 budget (MB) of the scalar ring kernels' w2 scratch and parked results (<= 0: default)."""
+    return _check(lib().tg_set_scalar_scratch_budget(float(megabytes)), "tg_set_scalar_scratch_budget")
+
+
+def set_kind_overlap(mode):
+    """Kinds of a plan: 1 side by side, 0 one after the other, -1 side by side when each fits in one wave."""
+    return _check(lib().tg_set_kind_overlap(int(mode)), "tg_set_kind_overlap")
 
 
 def set_block_scratch_budget(megabytes):

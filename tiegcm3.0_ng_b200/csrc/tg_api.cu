@@ -1184,16 +1184,23 @@ int plan_launch_group(tg_plan *p, tg_plan::Group &g, cudaStream_t st)
     return TG_OK;
 }
 
-// The scalar kind is bandwidth-bound and the block kinds are latency-bound
-// (few columns, long per-level dependency chains), so the block groups run on
-// a side stream forked from st and joined back: in a captured graph they are
-// parallel branches and the two kernels share the GPU.
+// When every kind's tiles fit in one resident wave the kernels are latency-
+// bound (few columns, long per-level dependency chains), so the block groups
+// run on a side stream forked from st and joined back: in a captured graph
+// they are parallel branches and the kernels share the GPU.  Larger batches
+// run the kinds one after the other: each kind's grid is sized so that its
+// sweep scratch fits in L2, and two such grids side by side would not.
 int plan_enqueue(tg_plan *p, cudaStream_t st)
 {
     TG_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(unsigned) * p->nseg, st));
     if (p->precision != TG_PREC_F64)
         TG_CUDA(cudaMemsetAsync(p->d_hist, 0, kMaxSweepBins * sizeof(unsigned long long), st));
-    const bool split = p->groups[0].nseg > 0 && (p->groups[1].nseg > 0 || p->groups[2].nseg > 0);
+    bool split = p->groups[0].nseg > 0 && (p->groups[1].nseg > 0 || p->groups[2].nseg > 0);
+    const int overlap = kind_overlap();
+    if (overlap == 0) split = false;
+    if (overlap < 0)
+        for (const auto &g : p->groups)
+            if (g.nseg > 0 && !g.shape.one_wave) split = false;
     int rc;
     if (!split) {
         for (auto &g : p->groups)
@@ -1449,6 +1456,18 @@ __attribute__((visibility("default"))) int tg_set_stage_levels(int kind, int pre
         return TG_EINVAL;
     }
     tg::set_stage_levels(kind, precision, levels);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_scalar_scratch_budget(double megabytes)
+{
+    tg::set_scalar_scratch_budget(megabytes);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_kind_overlap(int mode)
+{
+    tg::set_kind_overlap(mode);
     return TG_OK;
 }
 

@@ -62,6 +62,7 @@ struct Shape {
     int rows;           // block ring kernel with one lane per block row
     int bw;             // block ring kernel: columns per warp (32, 16, 8)
     int lps;            // scalar FP64 ring: levels per stage (>1: chunked ring kernel)
+    int one_wave;       // the grid holds every tile at once (no grid-stride second pass)
 };
 
 // Register-prefetch kernel shape of a kind/precision (tg_set_tile).
@@ -184,6 +185,11 @@ void set_stage_levels(int kind, int precision, int l);
 // L2 budget (MB) for the Gamma scratch of all resident block-kernel warps;
 // <= 0 restores the default 96 MB.
 void set_block_scratch_budget(double mb);
+void set_scalar_scratch_budget(double mb);
+// Kinds of one plan: 1 concurrently (block kinds on a side stream), 0 one
+// after the other, -1 concurrently only when every kind fits in one wave.
+void set_kind_overlap(int mode);
+int kind_overlap();
 
 // L2 cache-policy hints of the bulk-copy ring kernels (tg_set_cache_hints).
 int cache_hints();

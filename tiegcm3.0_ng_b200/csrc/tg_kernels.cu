@@ -1115,7 +1115,7 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
             fence_proxy_async();
             if (k + D < k2) ring.issue(qk + D, src + (k + D) * lstride, lane);
             if (!valid) continue;
-            double Qp[BB], W[BB], v[B];
+            double Qp[BB], Wi[BB], v[B];
             if (k == 0) {
 #pragma unroll
                 for (int e = 0; e < BB; ++e) Qp[e] = Q[e];
@@ -1139,12 +1139,12 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
                     v[i] = tv;
                 }
             }
-            ok = inv_exact<B>(Qp, W) && ok;
+            ok = inv_exact<B>(Qp, Wi) && ok;
 #pragma unroll
             for (int i = 0; i < B; ++i) {
-                double tv = xmul(W[i], v[0]);
+                double tv = xmul(Wi[i], v[0]);
 #pragma unroll
-                for (int m = 1; m < B; ++m) tv = xadd(tv, xmul(W[i + B * m], v[m]));
+                for (int m = 1; m < B; ++m) tv = xadd(tv, xmul(Wi[i + B * m], v[m]));
                 z[i] = tv;
                 st_hint(&pU[((long)k * B + i) * ld], tv, keep);
             }
@@ -1153,9 +1153,9 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
                 for (int m = 0; m < B; ++m)
 #pragma unroll
                     for (int i = 0; i < B; ++i) {
-                        double g = xmul(W[i], R[B * m]);
+                        double g = xmul(Wi[i], R[B * m]);
 #pragma unroll
-                        for (int n = 1; n < B; ++n) g = xadd(g, xmul(W[i + B * n], R[n + B * m]));
+                        for (int n = 1; n < B; ++n) g = xadd(g, xmul(Wi[i + B * n], R[n + B * m]));
                         G[i + B * m] = g;
                         st_hint(&gam[((long)k * BB + i + B * m) * gs], g, keep);
                     }
@@ -2031,6 +2031,11 @@ cudaError_t occupancy(K kernel, int threads, size_t smem, int *per_sm)
 // Resident threads per SM allowed for the block kernels: their Gamma scratch
 // (k2 * B*B doubles per resident thread) should stay well inside L2.
 double g_block_scratch_budget = 96.0 * 1024 * 1024;
+// Scalar ring kernels: L2 bytes of w2 scratch and parked w3 of all resident
+// columns.  Past the L2's capacity the back sweep's re-reads go to DRAM.
+constexpr double kScalarBudgetMB = 128.0;
+double g_scalar_scratch_budget = kScalarBudgetMB * 1024 * 1024;
+std::atomic<int> g_kind_overlap{-1};
 }  // namespace
 
 int prefetch_depth(int kind, int precision) { return g_tile[kind_index(kind)][precision ? 1 : 0].pf; }
@@ -2094,6 +2099,12 @@ void set_block_rows(int kind, int on)
     t.rows = on < 0 ? kDefaultTile[kind_index(kind)][0].rows : (on ? 1 : 0);
 }
 void set_block_scratch_budget(double mb) { g_block_scratch_budget = (mb > 0 ? mb : 96.0) * 1024 * 1024; }
+void set_scalar_scratch_budget(double mb)
+{
+    g_scalar_scratch_budget = (mb > 0 ? mb : kScalarBudgetMB) * 1024 * 1024;
+}
+void set_kind_overlap(int mode) { g_kind_overlap.store(mode == 0 || mode == 1 ? mode : -1); }
+int kind_overlap() { return g_kind_overlap.load(); }
 void set_stage_levels(int kind, int precision, int l)
 {
     if (kind != TG_KIND_SCALAR || precision != TG_PREC_F64) return;
@@ -2215,10 +2226,17 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         const double per_thread = (double)block_scratch_bytes(kind, precision, 1, k2max);
         const long cap = (long)(g_block_scratch_budget / (per_thread * sh->threads));
         if (blocks > cap) blocks = cap > 0 ? cap : 1;
+    } else if (stages > 0) {
+        // ring kernels: w2 scratch plus the w3 parked in x, 8 B each per level
+        // and column, of every resident column within the L2 budget
+        const double per_col = (double)(2 * k2max - 1) * 8.0;
+        const long cap = (long)(g_scalar_scratch_budget / (per_col * sh->threads * sh->cpt));
+        if (blocks > cap) blocks = cap > 0 ? cap : 1;
     }
     const long vt = sh->rows ? (long)ntiles * rows_group(kind)
                              : (kind != TG_KIND_SCALAR ? (long)ntiles * (32 / sh->bw) : ntiles);   // warp tiles
     const long units = stages > 0 ? (vt + sh->threads / 32 - 1) / (sh->threads / 32) : ntiles;
+    sh->one_wave = blocks >= units;
     if (blocks > units) blocks = units;
     sh->blocks = (int)(blocks > 0 ? blocks : 1);
     return cudaSuccess;
