@@ -398,10 +398,12 @@ int tg_set_tile(int kind, int precision, int cols_per_block, int cols_per_thread
 /* Coefficient staging of the FP64 kernels of a kind: 0 = register-prefetch
  * kernel (shape from tg_set_tile); 4, 8 or 16 = depth in levels of the
  * shared-memory ring that bulk asynchronous copies fill ahead of the sweep
- * (one warp per 32 columns, `warps` independent warps per CTA, 1..8, 0 keeps
- * the current count; used when the level-major column stride is a multiple
+ * (one warp per 32 columns, `warps` independent warps per CTA, 1..8, 0 the
+ * default count; used when the level-major column stride is a multiple
  * of 32 and the arrays are 16-byte aligned, otherwise the register-prefetch
- * kernel runs); -1 restores the default. */
+ * kernel runs); -1 restores the default.  Scalar kind, TG_PREC_F32_REFINE:
+ * 2..4 = stages of 4 levels of the refinement ring (x 16-byte aligned too),
+ * 0 = register-prefetch refinement kernel. */
 int tg_set_pipeline(int kind, int precision, int stages, int warps);
 /* Depth (levels) of the register prefetch of the scalar kernels' coefficient
  * loads: 4, 8 or 16 (kind TG_KIND_SCALAR, either precision); -1 restores the

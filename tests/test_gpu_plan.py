@@ -187,3 +187,64 @@ def test_kind_overlap_and_l2_budgets_keep_bits(cuda, pkg, orc):
         pkg.set_kind_overlap(-1)
         pkg.set_scalar_scratch_budget(0)
         pkg.set_block_scratch_budget(0)
+
+
+def test_refine_sweeps_follow_conditioning(cuda, pkg, orc):
+    """Well-conditioned columns stop after one correction sweep (the FP32
+    sweep-0 solution seeds the contraction estimate); weakly dominant columns,
+    whose FP32 factors are poorer, take more sweeps.  All reach 1e-10."""
+    torch = cuda
+    nk, ncol = 113, 512
+    rng = np.random.default_rng(5)
+    eps = np.where(np.arange(ncol) < ncol // 2, 1.0, 1e-9)
+    a = np.asfortranarray(-np.ones((nk, ncol)) * rng.uniform(0.9, 1.0, (nk, ncol)))
+    c = np.asfortranarray(-np.ones((nk, ncol)) * rng.uniform(0.9, 1.0, (nk, ncol)))
+    b = np.asfortranarray(-(a + c) + eps[None, :])
+    f = np.asfortranarray(rng.uniform(-1.0, 1.0, (nk, ncol)))
+    ld = pkg.batch.pad_ld(ncol)
+    t = [pkg.batch.level_scalar(v, ld, "cuda") for v in (a, b, c, f)]
+    x = torch.zeros((nk, ld), dtype=torch.float64, device="cuda")
+    seg = dict(kind=pkg.TG_KIND_SCALAR, nk=nk, k2=nk, ncol=ncol, ld=ld, a=t[0], b=t[1], c=t[2], f=t[3], x=x)
+    plan = pkg.Plan([seg], pkg.TG_PREC_F32_REFINE)
+    plan.execute()
+    rc, _ = plan.status()
+    hist = plan.sweep_histogram(8)
+    plan.close()
+    assert rc in (pkg.TG_OK, pkg.TG_ENOCONV)
+    got = pkg.batch.from_level_scalar(x, ncol)
+    want = orc.trsolv_ng(a, b, c, f, nk)
+    for half in (slice(0, ncol // 2), slice(ncol // 2, ncol)):
+        assert np.max(np.abs(got[:, half] - want[:, half])) / np.max(np.abs(want[:, half])) <= 1e-10
+    assert hist[1] >= ncol // 2 and sum(hist[2:]) >= ncol // 4, hist
+
+
+@pytest.mark.parametrize("kind", [0, 2])
+def test_every_refine_variant_within_tolerance(cuda, pkg, orc, kind):
+    """Each refinement launch shape the autotuner may choose (register
+    prefetch, bulk-copy refinement ring of 2..4 stages) reaches 1e-10 and
+    counts every column in the sweep histogram."""
+    torch = cuda
+    from tiegcm_ng_b200 import autotune
+    specs = [(kind, 57, 57, 1000), (kind, 29, 28, 77), (kind, 113, 113, 40), (kind, 57, 56, 31), (kind, 3, 1, 50)]
+    segs, refs_in = make_segments(pkg, torch, specs, seed=500 + kind)
+    try:
+        for cand in autotune.candidates(kind, pkg.TG_PREC_F32_REFINE):
+            autotune.apply(kind, pkg.TG_PREC_F32_REFINE, cand)
+            for s in segs:
+                s["x"].fill_(3.5)
+            try:
+                plan = pkg.Plan(segs, pkg.TG_PREC_F32_REFINE)
+            except pkg.TgError:
+                # a register kernel whose per-thread planes of 113 levels
+                # exceed shared memory at this block size has no shape
+                assert cand[0] == "reg" and cand[1] >= 256, cand
+                continue
+            plan.execute()
+            rc, per = plan.status()
+            hist = plan.sweep_histogram(8)
+            plan.close()
+            assert rc in (pkg.TG_OK, pkg.TG_ENOCONV), cand
+            assert sum(hist) == sum(s["ncol"] for s in segs), (cand, hist)
+            check(pkg, orc, segs, refs_in, exact=False)
+    finally:
+        autotune.reset(kind, pkg.TG_PREC_F32_REFINE)

@@ -12,7 +12,8 @@ from a CUDA graph, CUDA-event timed) and keeps the fastest:
             per block row ("rows", depth 4 or 8) and 16 or 8 columns per warp
             ("ring16", "ring8"); for the scalar kind a ring of stages holding 2, 4
             or 8 levels each ("chunk2", "chunk4", "chunk8")
-  FP32+ref  columns per block x prefetch depth
+  FP32+ref  columns per block x prefetch depth; scalar kind also the
+            bulk-copy refinement ring of 2, 3 or 4 stages ("ring")
 
 Results are cached in a JSON file keyed by GPU name, kind, precision, level
 count and a column-count bucket, and applied with tg_set_tile /
@@ -37,7 +38,8 @@ BLOCK_F64 = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 9
              ("ring", 4, 4, 4), ("ring", 8, 4, 4), ("ring", 4, 2, 4), ("ring", 8, 2, 4), ("ring", 16, 2, 4),
              ("ring", 4, 1, 4), ("ring16", 4, 1, 4), ("ring16", 8, 1, 4), ("ring16", 4, 2, 4), ("ring8", 4, 1, 4),
              ("ring8", 8, 1, 4), ("ring8", 4, 2, 4), ("rows", 4, 1, 4), ("rows", 4, 2, 4), ("rows", 8, 1, 4)]
-SCALAR_REF = [("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg", 64, 1, 8)]
+SCALAR_REF = [("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg", 64, 1, 8),
+              ("ring", 2, 1, 4), ("ring", 3, 1, 4), ("ring", 4, 1, 4), ("ring", 2, 2, 4)]
 BLOCK_REF = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4)]
 
 
@@ -61,8 +63,7 @@ def apply(kind, precision, cand):
     if v in ("ring", "ringg", "rows", "ring16", "ring8") or v.startswith("chunk"):
         cs.set_pipeline(kind, precision, p1, p2)    # ring depth, warps per CTA
     else:
-        if precision == cs.TG_PREC_F64:
-            cs.set_pipeline(kind, precision, 0)
+        cs.set_pipeline(kind, precision, 0)
         cs.set_tile(kind, precision, p1, p2)
     if scalar64:
         cs.set_scratch_global(kind, precision, 1 if v in ("regg", "ringg") or v.startswith("chunk") else 0)
@@ -70,7 +71,7 @@ def apply(kind, precision, cand):
 
 def reset(kind, precision):
     cs.set_tile(kind, precision, 0, 0)
-    cs.set_pipeline(kind, precision, -1, 4)
+    cs.set_pipeline(kind, precision, -1, 0)
     if kind == cs.TG_KIND_SCALAR:
         cs.set_prefetch(kind, precision, -1)
     if kind == cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64:

@@ -576,7 +576,7 @@ def set_tile(kind, precision, cols_per_block=0, cols_per_thread=0):
 
 def set_pipeline(kind, precision, stages=-1, warps=0):
     """Ring depth of the bulk-copy staged FP64 kernels (0: register prefetch,
-    -1: default) and their warps per CTA (0: keep)."""
+    -1: default) and their warps per CTA (0: default)."""
     return _check(lib().tg_set_pipeline(kind, precision, stages, warps), "tg_set_pipeline", numeric_ok=False)
 
 

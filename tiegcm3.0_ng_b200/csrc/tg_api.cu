@@ -148,6 +148,11 @@ bool ring_ok_seg(const Seg &s)
 {
     return s.ld % 32 == 0 && aligned16(s.a) && aligned16(s.b) && aligned16(s.c) && aligned16(s.f);
 }
+// The refinement ring also reads x rows by bulk copies.
+bool ring_ok_for(const Seg &s, int precision)
+{
+    return ring_ok_seg(s) && (precision == TG_PREC_F64 || aligned16(s.x));
+}
 bool cpt2_ok_seg(const Seg &s)
 {
     return s.ld % 2 == 0 && aligned16(s.a) && aligned16(s.b) && aligned16(s.c) && aligned16(s.f) && aligned16(s.x);
@@ -157,7 +162,7 @@ int solve_level(DevCtx *c, int slot, int kind, int precision, Seg seg, unsigned 
 {
     const int B = kind == TG_KIND_SCALAR ? 1 : kind;
     int cpb = 0, cpt = 1, stages = 0, w2g = 0;
-    tile_for(kind, precision, ring_ok_seg(seg), &cpb, &cpt, &stages, &w2g);
+    tile_for(kind, precision, ring_ok_for(seg, precision), &cpb, &cpt, &stages, &w2g);
     if (cpt == 2 && !cpt2_ok_seg(seg)) {
         cpb /= 2;
         cpt = 1;
@@ -389,8 +394,8 @@ __attribute__((visibility("default"))) int tg_set_pipeline(int kind, int precisi
 {
     if ((kind != TG_KIND_SCALAR && kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) || bad_prec(precision) ||
         (stages != -1 && stages != 0 && stages != 2 && stages != 3 && stages != 4 && stages != 8 && stages != 16) ||
-        (stages > 0 && precision != TG_PREC_F64) || warps < 0 || warps > 8) {
-        set_err("tg_set_pipeline: stages must be 0, 2, 3, 4, 8 or 16 (FP64 only) or -1; warps 0..8");
+        (stages > 0 && precision != TG_PREC_F64 && (kind != TG_KIND_SCALAR || stages > 4)) || warps < 0 || warps > 8) {
+        set_err("tg_set_pipeline: stages must be 0, 2, 3, 4, 8 or 16 (FP64; scalar refinement 2..4) or -1; warps 0..8");
         return TG_EINVAL;
     }
     set_stages(kind, precision, stages, warps);
@@ -1278,7 +1283,7 @@ __attribute__((visibility("default"))) int tg_plan_create(const tg_segment *segs
             d.ubc_add = d.ubc_ratio ? s.ubc_add : nullptr;
             d.ld = s.ld; d.nk = s.nk; d.k2 = s.k2; d.ncol = s.ncol; d.kind = s.kind;
             d.status_idx = i;
-            ring_ok = ring_ok && ring_ok_seg(d);
+            ring_ok = ring_ok && ring_ok_for(d, precision);
             cpt2_ok = cpt2_ok && cpt2_ok_seg(d);
             hs.push_back(d);
             g.k2max = std::max(g.k2max, s.k2);
@@ -1506,7 +1511,8 @@ __attribute__((visibility("default"))) int tg_plan_describe(const tg_plan *p, ch
         const Shape &h = g.shape;
         char name[96];
         if (g.kind == TG_KIND_SCALAR) {
-            if (!f64) snprintf(name, sizeof name, "k_scalar_refine<%d>", h.pf);
+            if (!f64 && h.stages) snprintf(name, sizeof name, "k_scalar_refine_ring<%d>", h.stages);
+            else if (!f64) snprintf(name, sizeof name, "k_scalar_refine<%d>", h.pf);
             else if (h.stages && h.lps > 1) snprintf(name, sizeof name, "k_scalar_f64_chunk<%d,%d>", h.stages, h.lps);
             else if (h.stages) snprintf(name, sizeof name, "k_scalar_f64_ring<%d,%d>", h.stages, h.w2g);
             else if (h.w2g) snprintf(name, sizeof name, "k_scalar_f64_g<%d>", h.pf);

@@ -610,17 +610,22 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
 // Shared memory per thread: three float planes (w2, 1/w1, y) of k2 levels.
 // ---------------------------------------------------------------------------
 // Stopping rule of the refinement sweeps.  dmax = max|d| of this sweep's
-// correction, xmax = max|x| after it, dprev = max|d| of the previous sweep
-// (0 before the second sweep).  Each sweep shrinks the error by a factor rho,
-// estimated as dmax/dprev; the error left after applying d is then about
-// dmax*rho/(1-rho).  A column stops when that estimate, or the correction
-// itself, is below rel_tol*xmax.
-__device__ __forceinline__ bool refine_done(double dmax, double xmax, double dprev, double tol)
+// correction, xmax = max|x| after it, dprev = max|d| of the previous
+// correction; for the first correction, max|x| of the FP32 sweep-0 solution
+// (sweep 0 is the correction from x = 0).  Each sweep shrinks the error by a
+// factor rho, estimated as dmax/dprev; the error left after applying d is
+// then about dmax*rho/(1-rho).  A column stops when that estimate, or the
+// correction itself, is below rel_tol*xmax.  The first estimate (from the
+// sweep-0 solution rather than a correction) is the coarser one and must
+// clear the tolerance by a factor 16.  With well-conditioned columns (rho
+// near the FP32 rounding level) one correction suffices.
+__device__ __forceinline__ bool refine_done(double dmax, double xmax, double dprev, double tol, bool first)
 {
     if (dmax <= tol * xmax) return true;
     if (dprev > 0.0) {
         const double rho = dmax / dprev;
-        if (rho < 0.5 && dmax * rho <= (1.0 - rho) * tol * xmax) return true;
+        const double margin = first ? 16.0 : 1.0;
+        if (rho < 0.5 && margin * dmax * rho <= (1.0 - rho) * tol * xmax) return true;
     }
     return false;
 }
@@ -637,6 +642,7 @@ __device__ __forceinline__ unsigned thomas_refine_col(const Seg &s, long col, fl
     const double *__restrict__ pf = s.f + col;
     double *__restrict__ px = s.x + col;
     bool ok = true;
+    double xmax0 = 0.0;
 
     // ---- sweep 0: FP32 factor + solve
     {
@@ -681,18 +687,20 @@ __device__ __forceinline__ unsigned thomas_refine_col(const Seg &s, long col, fl
                 }
             }
         }
-        float xk = y;
+        float xk = y, xm = fabsf(y);
         px[(k2 - 1) * ld] = (double)xk;
         for (int k = k2 - 2; k >= 0; --k) {
             xk = sy[k * T] - sw2[k * T] * xk;
+            xm = fmaxf(xm, fabsf(xk));
             px[k * ld] = (double)xk;
         }
+        xmax0 = (double)xm;
     }
 
     // ---- refinement sweeps
     bool conv = false;
     int sw = 0;
-    double dprev = 0.0;
+    double dprev = xmax0;
     if (ok) {
         for (sw = 1; sw <= rf.max_sweeps; ++sw) {
             double xm1 = 0.0, x0 = px[0];
@@ -742,7 +750,7 @@ __device__ __forceinline__ unsigned thomas_refine_col(const Seg &s, long col, fl
                 xmax = fmax(xmax, fabs(xv));
             }
             if (!(xmax <= DBL_MAX) || !(dmax <= DBL_MAX)) break;
-            if (refine_done(dmax, xmax, dprev, rf.rel_tol)) {
+            if (refine_done(dmax, xmax, dprev, rf.rel_tol, sw == 1)) {
                 conv = true;
                 break;
             }
@@ -807,6 +815,256 @@ __global__ void __launch_bounds__(256) k_scalar_refine(SegTable tab, Refine rf, 
     __syncthreads();
     if (hist && threadIdx.x < kMaxSweepBins && shist[threadIdx.x])
         atomicAdd(hist + threadIdx.x, shist[threadIdx.x]);
+}
+
+// ---------------------------------------------------------------------------
+// Scalar Thomas, FP32 sweeps + FP64 refinement, coefficients staged by the
+// bulk-copy ring (one warp per 32 columns, its own ring and barriers).
+//
+// Sweep 0 reads a, b, c, f rows through the ring (4L copies of 256 B per
+// stage of L levels), factors in FP32 and solves; the FP32 factors (w2,
+// 1/w1) and the forward result y live in three shared-memory float planes
+// [level][lane].  Each correction sweep streams a, b, c, f and the x rows
+// one level above (5L copies per stage), forms the FP64 residual, eliminates
+// with the FP32 factors and back-substitutes x += d.  Stopping rule, cap,
+// bit-exact FP64 fallback and flags as in k_scalar_refine.
+// x rows written by this warp's generic stores are read back by bulk copies:
+// a proxy fence orders the two before each correction sweep.
+// Requires ld % 32 == 0 and 16-byte aligned a, b, c, f, x.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void fence_proxy_async_global()
+{
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+constexpr int kRefineStageLevels = 4;   // levels per ring stage of the refinement ring
+
+template <int C>
+__global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine rf, unsigned *status,
+                                                            unsigned long long *hist)
+{
+    constexpr int L = kRefineStageLevels, NC = 4 * L, NE = 5 * L;
+    static_assert(NE <= 32, "one copy per lane");
+    __shared__ __align__(8) unsigned long long bars[8 * C];
+    extern __shared__ __align__(128) double smem_r[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int K = tab.k2max;
+    double *buf = smem_r + (long)warp * ((long)C * NE * 32 + 48L * K);
+    float *pw2 = reinterpret_cast<float *>(buf + C * NE * 32) + lane;   // [k][32] planes
+    float *pri = pw2 + K * 32;
+    float *py = pri + K * 32;
+    unsigned long long *bar = bars + warp * C;
+    const unsigned long long pol = l2_policy(tab.hints, false);
+    if (lane == 0) {
+#pragma unroll 1
+        for (int i = 0; i < C; ++i) mbar_init(&bar[i], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    unsigned long long hl[kMaxSweepBins];
+#pragma unroll
+    for (int i = 0; i < kMaxSweepBins; ++i) hl[i] = 0ull;
+    unsigned q = 0;
+    for (int t = blockIdx.x * nwarps + warp; t < tab.ntiles; t += gridDim.x * nwarps) {
+        const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
+        const long col0 = (long)(t - s.tile0) * 32;
+        const long ld = s.ld;
+        const int k2 = s.k2;
+        const bool valid = col0 + lane < s.ncol;
+        double *px = s.x + col0 + lane;
+        const int nch = (k2 + L - 1) / L;
+        // lanes 0..4L-1: row (level lane/4) of array lane%4; lanes 4L..5L-1:
+        // x row (lane - 4L + 1) above the chunk's first level
+        const int arr = lane & 3;
+        const double *src = lane < NC ? (arr == 0 ? s.a : arr == 1 ? s.b : arr == 2 ? s.c : s.f) + col0 +
+                                            (long)(lane >> 2) * ld
+                                      : s.x + col0 + (long)(lane - NC + 1) * ld;
+        auto issue = [&](unsigned qc, int j, bool withx) {
+            const int st = (int)(qc % C), l0 = j * L;
+            const int nl = k2 - l0 < L ? k2 - l0 : L;
+            const int nx = withx ? (k2 - 1 - l0 < L ? k2 - 1 - l0 : L) : 0;
+            if (lane == 0) mbar_expect(&bar[st], (uint32_t)(4 * nl + nx) * 256u);
+            __syncwarp();
+            const bool go = lane < NC ? (lane >> 2) < nl : lane < NE && lane - NC < nx;
+            if (go) bulk_load_hint(buf + (st * NE + lane) * 32, src + (long)l0 * ld, 256u, &bar[st], pol);
+        };
+        // bounded wait for chunk qc; on timeout drain the fills in flight
+        auto wait = [&](unsigned q0, int j, int n) -> bool {
+            const unsigned qc = q0 + j;
+            if (mbar_wait_warp(&bar[qc % C], (qc / C) & 1u)) return true;
+            const unsigned qe = q0 + (j + C < n ? j + C : n);
+#pragma unroll 1
+            for (unsigned r = qc; r < qe; ++r) mbar_wait_warp(&bar[r % C], (r / C) & 1u);
+            if (lane == 0) report(status, s.status_idx, FLAG_TIMEOUT);
+            return false;
+        };
+
+        // ---- sweep 0: FP32 factor + solve
+        bool ok = true;
+        float xm0 = 0.f;
+        {
+            const int pre = nch < C ? nch : C;
+            for (int j = 0; j < pre; ++j) issue(q + j, j, false);
+            float w1 = 0.f, ri = 0.f, y = 0.f, cprev = 0.f;
+            for (int j = 0; j < nch; ++j) {
+                if (!wait(q, j, nch)) return;
+                const double *stg = buf + (int)((q + j) % C) * NE * 32 + lane;
+                if (valid) {
+#pragma unroll
+                    for (int l = 0; l < L; ++l) {
+                        const int k = j * L + l;
+                        if (k < k2) {
+                            const float af = (float)stg[(4 * l) * 32], bf = (float)stg[(4 * l + 1) * 32],
+                                        ff = (float)stg[(4 * l + 3) * 32];
+                            if (k == 0) {
+                                w1 = bf;
+                                ri = __frcp_rn(w1);
+                                y = ff * ri;
+                            } else {
+                                const float w2 = cprev * ri;
+                                pw2[(k - 1) * 32] = w2;
+                                w1 = bf - af * w2;
+                                ri = __frcp_rn(w1);
+                                y = (ff - af * y) * ri;
+                            }
+                            ok = ok && (fabsf(w1) <= FLT_MAX) && (w1 != 0.f);
+                            pri[k * 32] = ri;
+                            py[k * 32] = y;
+                            cprev = (float)stg[(4 * l + 2) * 32];
+                        }
+                    }
+                }
+                __syncwarp();
+                fence_proxy_async();
+                if (j + C < nch) issue(q + j + C, j + C, false);
+            }
+            q += nch;
+            if (valid) {
+                float xk = y;
+                xm0 = fabsf(y);
+                px[(k2 - 1) * ld] = (double)xk;
+                for (int k = k2 - 2; k >= 0; --k) {
+                    xk = py[k * 32] - pw2[k * 32] * xk;
+                    xm0 = fmaxf(xm0, fabsf(xk));
+                    px[k * ld] = (double)xk;
+                }
+            }
+        }
+
+        // ---- correction sweeps (the warp streams while any lane is active)
+        bool active = valid && ok, conv = false;
+        int sw = 0, taken = rf.max_sweeps + 1;   // sweep of convergence, else cap + 1
+        double dprev = (double)xm0;
+        for (sw = 1; sw <= rf.max_sweeps && __any_sync(0xffffffffu, active); ++sw) {
+            fence_proxy_async_global();
+            __syncwarp();
+            const int pre = nch < C ? nch : C;
+            for (int j = 0; j < pre; ++j) issue(q + j, j, true);
+            double xm1 = 0.0, x0 = active ? px[0] : 0.0;
+            float y = 0.f;
+            for (int j = 0; j < nch; ++j) {
+                if (!wait(q, j, nch)) return;
+                const double *stg = buf + (int)((q + j) % C) * NE * 32 + lane;
+#pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    const int k = j * L + l;
+                    if (k < k2) {
+                        const double xp1 = k + 1 < k2 ? stg[(NC + l) * 32] : 0.0;
+                        if (active) {
+                            const double ak = stg[(4 * l) * 32];
+                            double r = fma(-stg[(4 * l + 1) * 32], x0, stg[(4 * l + 3) * 32]);
+                            if (k > 0) r = fma(-ak, xm1, r);
+                            if (k + 1 < k2) r = fma(-stg[(4 * l + 2) * 32], xp1, r);
+                            const float rr = (float)r;
+                            y = k == 0 ? rr * pri[0] : (rr - (float)ak * y) * pri[k * 32];
+                            py[k * 32] = y;
+                        }
+                        xm1 = x0;
+                        x0 = xp1;
+                    }
+                }
+                __syncwarp();
+                fence_proxy_async();
+                if (j + C < nch) issue(q + j + C, j + C, true);
+            }
+            q += nch;
+            if (active) {
+                // back substitution, x += d; x(k2-1) is in xm1, the rest is
+                // re-read 4 levels ahead
+                float d = y;
+                double xv = xm1 + (double)d;
+                px[(k2 - 1) * ld] = xv;
+                double dmax = fabs((double)d), xmax = fabs(xv);
+                double rx[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (k2 - 2 - u >= 0) rx[u] = px[(k2 - 2 - u) * ld];
+                for (int kb = k2 - 2; kb >= 0; kb -= 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = kb - u;
+                        if (k >= 0) {
+                            d = py[k * 32] - pw2[k * 32] * d;
+                            xv = rx[u] + (double)d;
+                            if (k - 4 >= 0) rx[u] = px[(k - 4) * ld];
+                            px[k * ld] = xv;
+                            dmax = fmax(dmax, fabs((double)d));
+                            xmax = fmax(xmax, fabs(xv));
+                        }
+                    }
+                }
+                if (!(xmax <= DBL_MAX) || !(dmax <= DBL_MAX)) {
+                    active = false;
+                } else if (refine_done(dmax, xmax, dprev, rf.rel_tol, sw == 1)) {
+                    conv = true;
+                    active = false;
+                    taken = sw;
+                } else {
+                    dprev = dmax;
+                }
+            }
+        }
+        unsigned flags = 0u;
+        if (valid && !conv) {
+            // ---- fallback: bit-exact FP64 re-solve; w2 as two 32-bit halves
+            // in this lane's (w2, 1/w1) plane slots, w3 parked in x
+            const double *pa = s.a + col0 + lane, *pb = s.b + col0 + lane, *pc = s.c + col0 + lane,
+                         *pf = s.f + col0 + lane;
+            bool okd = true, fin = true;
+            double w1 = pb[0], w3 = xdiv(pf[0], w1);
+            okd = finite_nz(w1);
+            px[0] = w3;
+            double cprev = pc[0];
+            for (int k = 1; k < k2; ++k) {
+                const double ak = pa[k * ld], bk = pb[k * ld], fk = pf[k * ld];
+                const double w2 = xdiv(cprev, w1);
+                pw2[(k - 1) * 32] = __int_as_float(__double2hiint(w2));
+                pri[(k - 1) * 32] = __int_as_float(__double2loint(w2));
+                w1 = xsub(bk, xmul(ak, w2));
+                w3 = xdiv(xsub(fk, xmul(ak, w3)), w1);
+                okd = okd && finite_nz(w1);
+                px[k * ld] = w3;
+                cprev = pc[k * ld];
+            }
+            double xn = w3;
+            fin = finite(xn);
+            for (int k = k2 - 2; k >= 0; --k) {
+                const double w2 = __hiloint2double(__float_as_int(pw2[k * 32]), __float_as_int(pri[k * 32]));
+                xn = xsub(px[k * ld], xmul(w2, xn));
+                fin = fin && finite(xn);
+                px[k * ld] = xn;
+            }
+            flags = FLAG_NOCONV | (okd ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE);
+        }
+        if (valid) report(status, s.status_idx, flags);
+        const int bin = taken < kMaxSweepBins - 1 ? taken : kMaxSweepBins - 1;
+#pragma unroll
+        for (int i = 0; i < kMaxSweepBins; ++i) hl[i] += __popc(__ballot_sync(0xffffffffu, valid && bin == i));
+    }
+    if (hist && lane == 0)
+#pragma unroll
+        for (int i = 0; i < kMaxSweepBins; ++i)
+            if (hl[i]) atomicAdd(hist + i, hl[i]);
 }
 
 // ---------------------------------------------------------------------------
@@ -1425,6 +1683,7 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
     auto S = [&](int k, int e) -> float & { return scr[((long)k * NS + e) * gs]; };
 
     bool ok = true;
+    double xmax0 = 0.0;
     // ---- sweep 0
     {
         float G[BB], z[B];
@@ -1485,10 +1744,11 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
                     S(k, BB + i + B * m) = g;
                 }
         }
-        float un[B];
+        float un[B], xm = 0.f;
 #pragma unroll
         for (int i = 0; i < B; ++i) {
             un[i] = z[i];
+            xm = fmaxf(xm, fabsf(z[i]));
             pU[((long)(k2 - 1) * B + i) * ld] = (double)z[i];
         }
         for (int k = k2 - 2; k >= 0; --k) {
@@ -1503,15 +1763,17 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
 #pragma unroll
             for (int i = 0; i < B; ++i) {
                 un[i] = nu[i];
+                xm = fmaxf(xm, fabsf(nu[i]));
                 pU[((long)k * B + i) * ld] = (double)nu[i];
             }
         }
+        xmax0 = (double)xm;
     }
 
     // ---- refinement sweeps
     bool conv = false;
     int sw = 0;
-    double dprev = 0.0;
+    double dprev = xmax0;
     if (ok) {
         for (sw = 1; sw <= rf.max_sweeps; ++sw) {
             double um[B], u0[B];
@@ -1597,7 +1859,7 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
                 }
             }
             if (!(xmax <= DBL_MAX) || !(dmax <= DBL_MAX)) break;
-            if (refine_done(dmax, xmax, dprev, rf.rel_tol)) {
+            if (refine_done(dmax, xmax, dprev, rf.rel_tol, sw == 1)) {
                 conv = true;
                 break;
             }
@@ -1846,15 +2108,16 @@ struct TileCfg {
     int lps;               // scalar FP64 ring: levels per stage (1: k_scalar_f64_ring, >1: k_scalar_f64_chunk)
 };
 // [kind index: scalar, block2, block3][precision]
-// Defaults: the fastest shapes on the 2.5 deg column step (10368 x 57) on a
-// B200 (autotune.py sweep): scalar FP64 chunked bulk-copy ring of 2 stages x
-// 4 levels, one warp per CTA, w2 in global scratch; 2x2 block ring of depth 4, one warp per CTA;
-// 3x3 block register kernel of 128 threads; refinement kernels 64 threads
-// (scalar, prefetch 8), 64 (2x2) and 128 (3x3).
-const TileCfg kDefaultTile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 0, 0, 8, 4, 0, 32, 1}},
+// Defaults: the fastest shapes on a B200 (autotune.py sweeps of the 2.5 deg
+// column step, 10368 x 57, and of the nested 2.5 deg + 3-nest batch): scalar
+// FP64 chunked bulk-copy ring of 2 stages x 4 levels, one warp per CTA, w2 in
+// global scratch; 2x2 block ring of depth 4, one warp per CTA; 3x3 block
+// register kernel of 128 threads; scalar refinement ring of 2 stages, one
+// warp per CTA; block refinement kernels of 64 (2x2) and 128 (3x3) threads.
+const TileCfg kDefaultTile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 2, 0, 8, 1, 0, 32, 1}},
                                      {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 0, 0, 4, 4, 0, 32, 1}},
                                      {{128, 1, 0, 0, 4, 4, 0, 32, 1}, {128, 1, 0, 0, 4, 4, 0, 32, 1}}};
-TileCfg g_tile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 0, 0, 8, 4, 0, 32, 1}},
+TileCfg g_tile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 2, 0, 8, 1, 0, 32, 1}},
                         {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 0, 0, 4, 4, 0, 32, 1}},
                         {{128, 1, 0, 0, 4, 4, 0, 32, 1}, {128, 1, 0, 0, 4, 4, 0, 32, 1}}};
 int kind_index(int kind) { return kind == TG_KIND_SCALAR ? 0 : (kind == TG_KIND_BLOCK2 ? 1 : 2); }
@@ -1897,6 +2160,18 @@ cudaError_t with_scalar_refine(int pf, F f)
     case 4: return f(k_scalar_refine<4>);
     case 8: return f(k_scalar_refine<8>);
     case 16: return f(k_scalar_refine<16>);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// Scalar refinement ring kernels by stage count.
+template <typename F>
+cudaError_t with_scalar_refine_ring(int C, F f)
+{
+    switch (C) {
+    case 2: return f(k_scalar_refine_ring<2>);
+    case 3: return f(k_scalar_refine_ring<3>);
+    case 4: return f(k_scalar_refine_ring<4>);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1983,6 +2258,7 @@ int num_sms()
         }
         for (int d : {4, 8, 16})
             for (int g : {0, 1}) with_scalar_ring(d, g, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+        for (int c : {2, 3, 4}) with_scalar_refine_ring(c, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int c : {2, 3, 4})
             for (int l : {2, 4, 8}) with_scalar_chunk(c, l, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int b : {2, 3})
@@ -2049,7 +2325,7 @@ void tile_for(int kind, int precision, bool ring_ok, int *cpb, int *cpt, int *st
 {
     const TileCfg &t = g_tile[kind_index(kind)][precision ? 1 : 0];
     *w2g = 0;
-    if (precision == TG_PREC_F64 && t.stages > 0 && ring_ok) {
+    if ((precision == TG_PREC_F64 || kind == TG_KIND_SCALAR) && t.stages > 0 && ring_ok) {
         *cpb = 32;
         *cpt = 1;
         *stages = t.stages;
@@ -2131,6 +2407,8 @@ static int rows_group(int B) { return B == 2 ? 2 : 4; }
 size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g, int lps)
 {
     const size_t lev = (size_t)(k2max > 1 ? k2max - 1 : 1);
+    if (stages > 0 && precision != TG_PREC_F64)   // refinement ring: 5L-row stages + 3 float planes
+        return (size_t)threads / 32 * ((size_t)stages * 5 * kRefineStageLevels * 32 * 8 + (size_t)48 * k2max * 8);
     if (stages > 0 && lps > 1) return (size_t)threads / 32 * stages * 4 * lps * 32 * 8;
     if (stages > 0) return (size_t)threads / 32 * ((size_t)stages * 4 * 32 * 8 + (w2g ? 0 : 32 * lev * 8));
     if (w2g) return 0;
@@ -2165,9 +2443,12 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     sh->bw = stages > 0 && kind != TG_KIND_SCALAR && !sh->rows ? block_width(kind, precision) : 32;
     // chunked scalar ring: w2 in global scratch, C = stages chunks of lps levels
     sh->lps = stages > 0 && kind == TG_KIND_SCALAR && precision == TG_PREC_F64 && w2g ? g_tile[0][0].lps : 1;
+    if (kind == TG_KIND_SCALAR && precision != TG_PREC_F64 && stages > 0)   // refinement ring: 2..4 stages
+        stages = sh->stages = stages < 2 ? 2 : (stages > 4 ? 4 : stages);
     if (sh->lps > 1 && stages > 4) stages = sh->stages = 4;
     if (sh->lps > 1 && sh->lps * stages > 16) stages = sh->stages = 2;
-    if (sh->lps == 1 && stages > 0 && stages < 4) stages = sh->stages = 4;   // per-level rings: depth 4, 8, 16
+    if (sh->lps == 1 && stages > 0 && stages < 4 && precision == TG_PREC_F64)
+        stages = sh->stages = 4;   // per-level rings: depth 4, 8, 16
     if (sh->bw < 32 && stages > 8) stages = sh->stages = 8;
     if (sh->rows && stages > 8) stages = sh->stages = 8;
     if (kind == TG_KIND_SCALAR && sh->cpt == 2 && sh->pf > 8) sh->pf = 8;
@@ -2190,7 +2471,9 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         sh->smem = scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max, stages, w2g, sh->lps);
         if (sh->smem > (size_t)(g_smem_optin - 1024)) return cudaErrorInvalidConfiguration;
         auto occ = [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); };
-        if (stages > 0 && sh->lps > 1)
+        if (stages > 0 && precision != TG_PREC_F64)
+            e = with_scalar_refine_ring(stages, occ);
+        else if (stages > 0 && sh->lps > 1)
             e = with_scalar_chunk(stages, sh->lps, occ);
         else if (stages > 0)
             e = with_scalar_ring(stages, w2g, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
@@ -2226,7 +2509,7 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         const double per_thread = (double)block_scratch_bytes(kind, precision, 1, k2max);
         const long cap = (long)(g_block_scratch_budget / (per_thread * sh->threads));
         if (blocks > cap) blocks = cap > 0 ? cap : 1;
-    } else if (stages > 0) {
+    } else if (stages > 0 && precision == TG_PREC_F64) {
         // ring kernels: w2 scratch plus the w3 parked in x, 8 B each per level
         // and column, of every resident column within the L2 budget
         const double per_col = (double)(2 * k2max - 1) * 8.0;
@@ -2251,7 +2534,14 @@ cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, R
 {
     if (tab.ntiles <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
-    if (precision == TG_PREC_F64 && sh.stages > 0 && sh.lps > 1) {
+    if (precision != TG_PREC_F64 && sh.stages > 0) {
+        SegTable t = tab;
+        t.hints = cache_hints();
+        e = with_scalar_refine_ring(sh.stages, [&](auto k) {
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, rf, status, hist);
+            return cudaSuccess;
+        });
+    } else if (precision == TG_PREC_F64 && sh.stages > 0 && sh.lps > 1) {
         SegTable t = tab;
         t.hints = cache_hints();
         e = with_scalar_chunk(sh.stages, sh.lps, [&](auto k) {
