@@ -183,8 +183,11 @@ int solve_level(DevCtx *c, int slot, int kind, int precision, Seg seg, unsigned 
     }
     if (kind == TG_KIND_SCALAR) {
         double *scr = nullptr;
-        if (sh.w2g) {
-            int rc = grow(c->scratch[slot], scalar_scratch_bytes((long)sh.blocks * sh.threads, seg.k2));
+        const bool ring_refine = precision != TG_PREC_F64 && sh.stages > 0;
+        if (sh.w2g || ring_refine) {
+            const long slots = (long)sh.blocks * sh.threads;
+            int rc = grow(c->scratch[slot], ring_refine ? refine_scratch_bytes(slots, seg.k2)
+                                                        : scalar_scratch_bytes(slots, seg.k2));
             if (rc) return rc;
             scr = (double *)c->scratch[slot].p;
         }
@@ -1320,10 +1323,12 @@ __attribute__((visibility("default"))) int tg_plan_create(const tg_segment *segs
             set_err("tg_plan_create: segment table upload failed");
             return TG_ENOMEM;
         }
-        if (g.kind != TG_KIND_SCALAR || g.shape.w2g) {
+        const bool ring_refine = g.kind == TG_KIND_SCALAR && precision != TG_PREC_F64 && g.shape.stages > 0;
+        if (g.kind != TG_KIND_SCALAR || g.shape.w2g || ring_refine) {
             const long slots = (long)g.shape.blocks * g.shape.threads;
-            const size_t need = g.kind == TG_KIND_SCALAR ? scalar_scratch_bytes(slots, g.k2max)
-                                                         : block_scratch_bytes(g.kind, precision, slots, g.k2max);
+            const size_t need = ring_refine ? refine_scratch_bytes(slots, g.k2max)
+                                : g.kind == TG_KIND_SCALAR ? scalar_scratch_bytes(slots, g.k2max)
+                                                           : block_scratch_bytes(g.kind, precision, slots, g.k2max);
             if (cudaMalloc(&g.scratch, need) != cudaSuccess) {
                 cudaGetLastError();
                 plan_free(p);

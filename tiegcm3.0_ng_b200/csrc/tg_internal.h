@@ -86,6 +86,8 @@ void set_prefetch(int kind, int precision, int pf);
 void set_w2g(int kind, int precision, int on);
 // Global scratch (bytes) of the scalar kernel with w2 in global memory.
 size_t scalar_scratch_bytes(long slots, int k2max);
+// Global scratch (bytes) of the scalar refinement ring: three float planes.
+size_t refine_scratch_bytes(long slots, int k2max);
 
 // Shared memory / scratch needs of a kernel for the largest k2 it will see.
 size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g, int lps);

@@ -822,39 +822,49 @@ __global__ void __launch_bounds__(256) k_scalar_refine(SegTable tab, Refine rf, 
 // bulk-copy ring (one warp per 32 columns, its own ring and barriers).
 //
 // Sweep 0 reads a, b, c, f rows through the ring (4L copies of 256 B per
-// stage of L levels), factors in FP32 and solves; the FP32 factors (w2,
-// 1/w1) and the forward result y live in three shared-memory float planes
-// [level][lane].  Each correction sweep streams a, b, c, f and the x rows
-// one level above (5L copies per stage), forms the FP64 residual, eliminates
-// with the FP32 factors and back-substitutes x += d.  Stopping rule, cap,
-// bit-exact FP64 fallback and flags as in k_scalar_refine.
-// x rows written by this warp's generic stores are read back by bulk copies:
-// a proxy fence orders the two before each correction sweep.
+// stage of L levels), factors in FP32 and solves.  The FP32 factors (w2,
+// 1/w1) and the forward result y go to three float planes of a global
+// scratch slot per resident lane ([plane][level][slot], kept in L2 by
+// eviction hints), so shared memory holds only the ring.  Each correction
+// sweep streams a, b, c, f, the x rows one level above and the 1/w1 rows
+// (5L copies of 256 B and L of 128 B per stage), forms the FP64 residual,
+// eliminates with the FP32 factors and back-substitutes x += d.  Stopping
+// rule, cap, bit-exact FP64 fallback and flags as in k_scalar_refine.
+// x and 1/w1 rows written by this warp's generic stores are read back by bulk
+// copies: a proxy fence orders the two before each correction sweep.
 // Requires ld % 32 == 0 and 16-byte aligned a, b, c, f, x.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void fence_proxy_async_global()
 {
     asm volatile("fence.proxy.async.global;" ::: "memory");
 }
+__device__ __forceinline__ void st_hint_f(float *p, float v, unsigned long long pol)
+{
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
+}
 
 constexpr int kRefineStageLevels = 4;   // levels per ring stage of the refinement ring
 
 template <int C>
-__global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine rf, unsigned *status,
+__global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine rf, float *scratch, unsigned *status,
                                                             unsigned long long *hist)
 {
     constexpr int L = kRefineStageLevels, NC = 4 * L, NE = 5 * L;
-    static_assert(NE <= 32, "one copy per lane");
+    constexpr int SD = NE * 32 + L * 16;   // doubles per stage: NE double rows, L float rows
+    static_assert(NE + L <= 32, "one copy per lane");
     __shared__ __align__(8) unsigned long long bars[8 * C];
     extern __shared__ __align__(128) double smem_r[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int K = tab.k2max;
-    double *buf = smem_r + (long)warp * ((long)C * NE * 32 + 48L * K);
-    float *pw2 = reinterpret_cast<float *>(buf + C * NE * 32) + lane;   // [k][32] planes
-    float *pri = pw2 + K * 32;
-    float *py = pri + K * 32;
+    const long K = tab.k2max;
+    double *buf = smem_r + (long)warp * C * SD;
+    const long S = (long)gridDim.x * blockDim.x;            // slots: level stride of a plane
+    const long slot0 = (long)blockIdx.x * blockDim.x + warp * 32;
+    float *gw2 = scratch + slot0 + lane;                    // plane 0: w2(k)
+    float *gri = gw2 + K * S;                               // plane 1: 1/w1(k)
+    float *gy = gri + K * S;                                // plane 2: y(k)
+    const float *rirow = scratch + K * S + slot0;           // row k of plane 1 for this warp
     unsigned long long *bar = bars + warp * C;
-    const unsigned long long pol = l2_policy(tab.hints, false);
+    const unsigned long long pol = l2_policy(tab.hints, false), keep = l2_policy(tab.hints, true);
     if (lane == 0) {
 #pragma unroll 1
         for (int i = 0; i < C; ++i) mbar_init(&bar[i], 1);
@@ -874,21 +884,30 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
         double *px = s.x + col0 + lane;
         const int nch = (k2 + L - 1) / L;
         // lanes 0..4L-1: row (level lane/4) of array lane%4; lanes 4L..5L-1:
-        // x row (lane - 4L + 1) above the chunk's first level
+        // x row (lane - 4L + 1) above the chunk's first level; lanes
+        // 5L..6L-1: 1/w1 row (lane - 5L)
         const int arr = lane & 3;
         const double *src = lane < NC ? (arr == 0 ? s.a : arr == 1 ? s.b : arr == 2 ? s.c : s.f) + col0 +
                                             (long)(lane >> 2) * ld
                                       : s.x + col0 + (long)(lane - NC + 1) * ld;
-        auto issue = [&](unsigned qc, int j, bool withx) {
+        auto issue = [&](unsigned qc, int j, bool corr) {
             const int st = (int)(qc % C), l0 = j * L;
             const int nl = k2 - l0 < L ? k2 - l0 : L;
-            const int nx = withx ? (k2 - 1 - l0 < L ? k2 - 1 - l0 : L) : 0;
-            if (lane == 0) mbar_expect(&bar[st], (uint32_t)(4 * nl + nx) * 256u);
+            const int nx = corr ? (k2 - 1 - l0 < L ? k2 - 1 - l0 : L) : 0;
+            if (lane == 0) mbar_expect(&bar[st], (uint32_t)(4 * nl + nx) * 256u + (corr ? (uint32_t)nl * 128u : 0u));
             __syncwarp();
-            const bool go = lane < NC ? (lane >> 2) < nl : lane < NE && lane - NC < nx;
-            if (go) bulk_load_hint(buf + (st * NE + lane) * 32, src + (long)l0 * ld, 256u, &bar[st], pol);
+            double *stg = buf + (long)st * SD;
+            if (lane < NC) {
+                if ((lane >> 2) < nl) bulk_load_hint(stg + lane * 32, src + (long)l0 * ld, 256u, &bar[st], pol);
+            } else if (lane < NE) {
+                if (lane - NC < nx) bulk_load_hint(stg + lane * 32, src + (long)l0 * ld, 256u, &bar[st], pol);
+            } else if (lane < NE + L) {
+                const int i = lane - NE;
+                if (corr && i < nl)
+                    bulk_load_hint(stg + NE * 32 + i * 16, rirow + (long)(l0 + i) * S, 128u, &bar[st], keep);
+            }
         };
-        // bounded wait for chunk qc; on timeout drain the fills in flight
+        // bounded wait for chunk j; on timeout drain the fills in flight
         auto wait = [&](unsigned q0, int j, int n) -> bool {
             const unsigned qc = q0 + j;
             if (mbar_wait_warp(&bar[qc % C], (qc / C) & 1u)) return true;
@@ -908,7 +927,7 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
             float w1 = 0.f, ri = 0.f, y = 0.f, cprev = 0.f;
             for (int j = 0; j < nch; ++j) {
                 if (!wait(q, j, nch)) return;
-                const double *stg = buf + (int)((q + j) % C) * NE * 32 + lane;
+                const double *stg = buf + (long)((q + j) % C) * SD + lane;
                 if (valid) {
 #pragma unroll
                     for (int l = 0; l < L; ++l) {
@@ -922,14 +941,14 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
                                 y = ff * ri;
                             } else {
                                 const float w2 = cprev * ri;
-                                pw2[(k - 1) * 32] = w2;
+                                st_hint_f(&gw2[(k - 1) * S], w2, keep);
                                 w1 = bf - af * w2;
                                 ri = __frcp_rn(w1);
                                 y = (ff - af * y) * ri;
                             }
                             ok = ok && (fabsf(w1) <= FLT_MAX) && (w1 != 0.f);
-                            pri[k * 32] = ri;
-                            py[k * 32] = y;
+                            st_hint_f(&gri[k * S], ri, keep);
+                            st_hint_f(&gy[k * S], y, keep);
                             cprev = (float)stg[(4 * l + 2) * 32];
                         }
                     }
@@ -940,13 +959,31 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
             }
             q += nch;
             if (valid) {
+                // back substitution; y and w2 re-read 4 levels ahead
                 float xk = y;
                 xm0 = fabsf(y);
                 px[(k2 - 1) * ld] = (double)xk;
-                for (int k = k2 - 2; k >= 0; --k) {
-                    xk = py[k * 32] - pw2[k * 32] * xk;
-                    xm0 = fmaxf(xm0, fabsf(xk));
-                    px[k * ld] = (double)xk;
+                float ry[4], rw[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (k2 - 2 - u >= 0) {
+                        ry[u] = gy[(k2 - 2 - u) * S];
+                        rw[u] = gw2[(k2 - 2 - u) * S];
+                    }
+                for (int kb = k2 - 2; kb >= 0; kb -= 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = kb - u;
+                        if (k >= 0) {
+                            xk = ry[u] - rw[u] * xk;
+                            if (k - 4 >= 0) {
+                                ry[u] = gy[(k - 4) * S];
+                                rw[u] = gw2[(k - 4) * S];
+                            }
+                            xm0 = fmaxf(xm0, fabsf(xk));
+                            st_hint(&px[k * ld], (double)xk, keep);
+                        }
+                    }
                 }
             }
         }
@@ -964,7 +1001,8 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
             float y = 0.f;
             for (int j = 0; j < nch; ++j) {
                 if (!wait(q, j, nch)) return;
-                const double *stg = buf + (int)((q + j) % C) * NE * 32 + lane;
+                const double *stg = buf + (long)((q + j) % C) * SD + lane;
+                const float *stf = reinterpret_cast<const float *>(buf + (long)((q + j) % C) * SD + NE * 32) + lane;
 #pragma unroll
                 for (int l = 0; l < L; ++l) {
                     const int k = j * L + l;
@@ -975,9 +1013,9 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
                             double r = fma(-stg[(4 * l + 1) * 32], x0, stg[(4 * l + 3) * 32]);
                             if (k > 0) r = fma(-ak, xm1, r);
                             if (k + 1 < k2) r = fma(-stg[(4 * l + 2) * 32], xp1, r);
-                            const float rr = (float)r;
-                            y = k == 0 ? rr * pri[0] : (rr - (float)ak * y) * pri[k * 32];
-                            py[k * 32] = y;
+                            const float rr = (float)r, rik = stf[l * 32];
+                            y = k == 0 ? rr * rik : (rr - (float)ak * y) * rik;
+                            st_hint_f(&gy[k * S], y, keep);
                         }
                         xm1 = x0;
                         x0 = xp1;
@@ -989,25 +1027,34 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
             }
             q += nch;
             if (active) {
-                // back substitution, x += d; x(k2-1) is in xm1, the rest is
-                // re-read 4 levels ahead
+                // back substitution, x += d; x(k2-1) is in xm1; x, y and w2
+                // of lower levels re-read 4 levels ahead
                 float d = y;
                 double xv = xm1 + (double)d;
-                px[(k2 - 1) * ld] = xv;
+                st_hint(&px[(k2 - 1) * ld], xv, keep);
                 double dmax = fabs((double)d), xmax = fabs(xv);
                 double rx[4];
+                float ry[4], rw[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    if (k2 - 2 - u >= 0) rx[u] = px[(k2 - 2 - u) * ld];
+                    if (k2 - 2 - u >= 0) {
+                        rx[u] = px[(k2 - 2 - u) * ld];
+                        ry[u] = gy[(k2 - 2 - u) * S];
+                        rw[u] = gw2[(k2 - 2 - u) * S];
+                    }
                 for (int kb = k2 - 2; kb >= 0; kb -= 4) {
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const int k = kb - u;
                         if (k >= 0) {
-                            d = py[k * 32] - pw2[k * 32] * d;
+                            d = ry[u] - rw[u] * d;
                             xv = rx[u] + (double)d;
-                            if (k - 4 >= 0) rx[u] = px[(k - 4) * ld];
-                            px[k * ld] = xv;
+                            if (k - 4 >= 0) {
+                                rx[u] = px[(k - 4) * ld];
+                                ry[u] = gy[(k - 4) * S];
+                                rw[u] = gw2[(k - 4) * S];
+                            }
+                            st_hint(&px[k * ld], xv, keep);
                             dmax = fmax(dmax, fabs((double)d));
                             xmax = fmax(xmax, fabs(xv));
                         }
@@ -1027,7 +1074,7 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
         unsigned flags = 0u;
         if (valid && !conv) {
             // ---- fallback: bit-exact FP64 re-solve; w2 as two 32-bit halves
-            // in this lane's (w2, 1/w1) plane slots, w3 parked in x
+            // in this lane's w2 and 1/w1 plane slots, w3 parked in x
             const double *pa = s.a + col0 + lane, *pb = s.b + col0 + lane, *pc = s.c + col0 + lane,
                          *pf = s.f + col0 + lane;
             bool okd = true, fin = true;
@@ -1038,8 +1085,8 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
             for (int k = 1; k < k2; ++k) {
                 const double ak = pa[k * ld], bk = pb[k * ld], fk = pf[k * ld];
                 const double w2 = xdiv(cprev, w1);
-                pw2[(k - 1) * 32] = __int_as_float(__double2hiint(w2));
-                pri[(k - 1) * 32] = __int_as_float(__double2loint(w2));
+                gw2[(k - 1) * S] = __int_as_float(__double2hiint(w2));
+                gri[(k - 1) * S] = __int_as_float(__double2loint(w2));
                 w1 = xsub(bk, xmul(ak, w2));
                 w3 = xdiv(xsub(fk, xmul(ak, w3)), w1);
                 okd = okd && finite_nz(w1);
@@ -1049,7 +1096,7 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
             double xn = w3;
             fin = finite(xn);
             for (int k = k2 - 2; k >= 0; --k) {
-                const double w2 = __hiloint2double(__float_as_int(pw2[k * 32]), __float_as_int(pri[k * 32]));
+                const double w2 = __hiloint2double(__float_as_int(gw2[k * S]), __float_as_int(gri[k * S]));
                 xn = xsub(px[k * ld], xmul(w2, xn));
                 fin = fin && finite(xn);
                 px[k * ld] = xn;
@@ -2349,6 +2396,7 @@ void set_w2g(int kind, int precision, int on)
 }
 
 size_t scalar_scratch_bytes(long slots, int k2max) { return (size_t)slots * (size_t)(k2max > 1 ? k2max - 1 : 1) * 8; }
+size_t refine_scratch_bytes(long slots, int k2max) { return (size_t)slots * 3 * (size_t)k2max * 4; }
 
 int cols_per_block(int kind, int precision) { return g_tile[kind_index(kind)][precision ? 1 : 0].cpb; }
 int cols_per_thread(int kind, int precision) { return g_tile[kind_index(kind)][precision ? 1 : 0].cpt; }
@@ -2407,8 +2455,8 @@ static int rows_group(int B) { return B == 2 ? 2 : 4; }
 size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g, int lps)
 {
     const size_t lev = (size_t)(k2max > 1 ? k2max - 1 : 1);
-    if (stages > 0 && precision != TG_PREC_F64)   // refinement ring: 5L-row stages + 3 float planes
-        return (size_t)threads / 32 * ((size_t)stages * 5 * kRefineStageLevels * 32 * 8 + (size_t)48 * k2max * 8);
+    if (stages > 0 && precision != TG_PREC_F64)   // refinement ring: 5L double rows + L float rows per stage
+        return (size_t)threads / 32 * stages * (5 * kRefineStageLevels * 32 + kRefineStageLevels * 16) * 8;
     if (stages > 0 && lps > 1) return (size_t)threads / 32 * stages * 4 * lps * 32 * 8;
     if (stages > 0) return (size_t)threads / 32 * ((size_t)stages * 4 * 32 * 8 + (w2g ? 0 : 32 * lev * 8));
     if (w2g) return 0;
@@ -2509,10 +2557,11 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         const double per_thread = (double)block_scratch_bytes(kind, precision, 1, k2max);
         const long cap = (long)(g_block_scratch_budget / (per_thread * sh->threads));
         if (blocks > cap) blocks = cap > 0 ? cap : 1;
-    } else if (stages > 0 && precision == TG_PREC_F64) {
+    } else if (stages > 0) {
         // ring kernels: w2 scratch plus the w3 parked in x, 8 B each per level
-        // and column, of every resident column within the L2 budget
-        const double per_col = (double)(2 * k2max - 1) * 8.0;
+        // and column (refinement: three float planes plus x), of every
+        // resident column within the L2 budget
+        const double per_col = precision == TG_PREC_F64 ? (double)(2 * k2max - 1) * 8.0 : (double)k2max * 20.0;
         const long cap = (long)(g_scalar_scratch_budget / (per_col * sh->threads * sh->cpt));
         if (blocks > cap) blocks = cap > 0 ? cap : 1;
     }
@@ -2538,7 +2587,7 @@ cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, R
         SegTable t = tab;
         t.hints = cache_hints();
         e = with_scalar_refine_ring(sh.stages, [&](auto k) {
-            k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, rf, status, hist);
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, rf, reinterpret_cast<float *>(scratch), status, hist);
             return cudaSuccess;
         });
     } else if (precision == TG_PREC_F64 && sh.stages > 0 && sh.lps > 1) {
