@@ -687,9 +687,6 @@ __device__ __forceinline__ void comp_walk(const CompFields &F, const CompConsts 
     const double dz = C.dz, rdz = xd(1.0, dz);
     const double dfac = __ldg(F.dfactor + col);
     const double flx_he = C.calc_helium ? __ldg(F.flx_he + col) : 0.0;
-    const double *nms[3] = {F.o2nm_smooth, F.o1nm_smooth, F.henm_smooth};
-    const double *adv[3] = {F.o2_advec, F.o1_advec, F.he_advec};
-    const double *hd[3] = {F.hdo2, F.hdo1, F.hdhe};
     CompLevel Lk, Lp;
     src.first(Lp);
     double G[9], z[3];
@@ -700,9 +697,10 @@ __device__ __forceinline__ void comp_walk(const CompFields &F, const CompConsts 
     bool ok = true;
     double flx00 = 1.0;
     for (int k = 0; k < nk - 1; ++k) {
+        src.begin(k);
         Lk = Lp;
         src.next(k, Lp);
-        const double wi = xm(0.5, xa(at(F.w, k), at(F.w, k + 1)));
+        const double wi = xm(0.5, xa(src.w(k), src.w1(k)));
         const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1), ez = __ldg(F.expz + k);
         // mol / eddy coefficients and the rows (comp_ng.F90:213-244)
         const double eddyp = xm(xm(C.expzmid_inv, difk0), xs(rdz, Lk.wks4));
@@ -723,7 +721,7 @@ __device__ __forceinline__ void comp_walk(const CompFields &F, const CompConsts 
                 const double molp = xm(Lk.ak[e], xa(rdz, hk));
                 const double molr = xm(Lp.ak[e], xs(rdz, hp));
                 const double molq = xa(xm(Lk.ak[e], xs(rdz, hk)), xm(Lp.ak[e], xa(rdz, hp)));
-                const double fsl = xm(ez, at(F.fs + (long)((m + 1) * 3 + i) * slab, k));
+                const double fsl = xm(ez, src.fs((m + 1) * 3 + i, k));
                 P[e] = i == m ? xs(xd(molp, dz), tp) : xd(molp, dz);
                 R[e] = i == m ? xs(xd(molr, dz), tr) : xd(molr, dz);
                 Q[e] = i == m ? xs(xa(-xd(molq, dz), tq), fsl) : xs(-xd(molq, dz), fsl);
@@ -731,8 +729,7 @@ __device__ __forceinline__ void comp_walk(const CompFields &F, const CompConsts 
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i)
-            f[i] = xm(ez, xa(xs(xm(at(nms[i], k), C.dtx2inv), xs(at(adv[i], k), at(F.fs + (long)i * slab, k))),
-                             at(hd[i], k)));
+            f[i] = xm(ez, xa(xs(xm(src.nms(i, k), C.dtx2inv), xs(src.adv(i, k), src.fs(i, k))), src.hd(i, k)));
         if (k == 0) {
             // lower boundary b(3,3), fb(3) (comp_ng.F90:246-258)
 #pragma unroll
@@ -861,12 +858,30 @@ __device__ __forceinline__ void comp_walk(const CompFields &F, const CompConsts 
     if (!ok || !fin) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
-// Level quantities computed from the fields with a window of two levels.
-struct CompFusedSrc {
+// Per-level field reads of comp_walk straight from global memory.
+struct CompFieldReads {
     const CompFields &F;
-    const CompConsts &C;
     long ld, col;
     int nk;
+    __device__ __forceinline__ double fat(const double *p, int k) const { return __ldg(p + k * ld + col); }
+    __device__ __forceinline__ void begin(int) {}
+    __device__ __forceinline__ double w(int k) const { return fat(F.w, k); }
+    __device__ __forceinline__ double w1(int k) const { return fat(F.w, k + 1); }
+    __device__ __forceinline__ double fs(int r, int k) const { return fat(F.fs + (long)r * nk * ld, k); }
+    __device__ __forceinline__ double nms(int i, int k) const
+    {
+        return fat(i == 0 ? F.o2nm_smooth : i == 1 ? F.o1nm_smooth : F.henm_smooth, k);
+    }
+    __device__ __forceinline__ double adv(int i, int k) const
+    {
+        return fat(i == 0 ? F.o2_advec : i == 1 ? F.o1_advec : F.he_advec, k);
+    }
+    __device__ __forceinline__ double hd(int i, int k) const { return fat(i == 0 ? F.hdo2 : i == 1 ? F.hdo1 : F.hdhe, k); }
+};
+
+// Level quantities computed from the fields with a window of two levels.
+struct CompFusedSrc : CompFieldReads {
+    const CompConsts &C;
     double o2_0, o1_0, he_0, mb_0, tn_0;
     __device__ __forceinline__ double at(const double *p, int k) const { return __ldg(p + k * ld + col); }
     __device__ __forceinline__ void first(CompLevel &L)
@@ -909,7 +924,7 @@ __global__ void __launch_bounds__(128) k_comp_ng(CompFields F, CompConsts C, dou
 {
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
-    CompFusedSrc src{F, C, ld, col, nk};
+    CompFusedSrc src{{F, ld, col, nk}, C};
     comp_walk(F, C, src, out, scr, nk, ld, col, sys_out, status);
 }
 
@@ -924,7 +939,7 @@ __global__ void __launch_bounds__(128) k_comp_levels(CompFields F, CompConsts C,
     if (col >= ncol) return;
     CompLevel L;
     if (j == 0) {
-        CompFusedSrc src{F, C, ld, col, nk};
+        CompFusedSrc src{{F, ld, col, nk}, C};
         src.first(L);
     } else {
         auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
@@ -950,10 +965,8 @@ __global__ void __launch_bounds__(128) k_comp_levels(CompFields F, CompConsts C,
 }
 
 // Level quantities read back from the planes.
-struct CompPlaneSrc {
+struct CompPlaneSrc : CompFieldReads {
     const double *lv;
-    long ld, col;
-    int nk;
     __device__ __forceinline__ void load(int j, CompLevel &L) const
     {
         const long slab = (long)nk * ld, o = (long)j * ld + col;
@@ -976,13 +989,95 @@ struct CompPlaneSrc {
     __device__ __forceinline__ void next(int k, CompLevel &L) { load(k + 1, L); }
 };
 
-__global__ void __launch_bounds__(128) k_comp_rows(CompFields F, CompConsts C, const double *lv, double *out,
-                                                   double *scr, int nk, int ncol, long ld, double *sys_out,
-                                                   unsigned *status)
+__device__ __forceinline__ void cp_async8(double *dst, const double *src)
 {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// The plane source with every per-level read of the walk staged one
+// iteration ahead: while iteration k computes, asynchronous 8-byte copies
+// bring the 36 values iteration k+1 reads (the 13 planes of level k+2, w at
+// k+1 and k+2, the 12 fs rows, nm, advec and hd of the three species at k+1)
+// into a two-buffer shared-memory array [buffer][value][thread].  Each thread
+// reads only what it copied itself, so no block barrier is needed.
+struct CompStagedSrc : CompPlaneSrc {
+    static constexpr int NS = 36;
+    double *sm;   // this thread's column of the block's slot array
+    int T;        // threads per block (row stride of the slot array)
+    int cur;
+    __device__ __forceinline__ double &slot(int b, int v) const { return sm[(long)(b * NS + v) * T]; }
+    __device__ __forceinline__ void issue(int k, int b)
+    {
+        const long slab = (long)nk * ld, o = (long)k * ld + col;
+#pragma unroll
+        for (int v = 0; v < kCompPlanes; ++v) cp_async8(&slot(b, v), lv + v * slab + o + ld);
+        cp_async8(&slot(b, 13), F.w + o);
+        cp_async8(&slot(b, 14), F.w + o + ld);
+#pragma unroll
+        for (int r = 0; r < 12; ++r) cp_async8(&slot(b, 15 + r), F.fs + r * slab + o);
+        cp_async8(&slot(b, 27), F.o2nm_smooth + o);
+        cp_async8(&slot(b, 28), F.o1nm_smooth + o);
+        cp_async8(&slot(b, 29), F.henm_smooth + o);
+        cp_async8(&slot(b, 30), F.o2_advec + o);
+        cp_async8(&slot(b, 31), F.o1_advec + o);
+        cp_async8(&slot(b, 32), F.he_advec + o);
+        cp_async8(&slot(b, 33), F.hdo2 + o);
+        cp_async8(&slot(b, 34), F.hdo1 + o);
+        cp_async8(&slot(b, 35), F.hdhe + o);
+    }
+    __device__ __forceinline__ void first(CompLevel &L)
+    {
+        load(0, L);
+        issue(0, 0);
+        cp_async_commit();
+    }
+    // iteration k: start the copies of iteration k+1, wait for those of k
+    __device__ __forceinline__ void begin(int k)
+    {
+        if (k + 1 < nk - 1) issue(k + 1, (k + 1) & 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        cur = k & 1;
+    }
+    __device__ __forceinline__ void next(int k, CompLevel &L) const
+    {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) L.ep[i] = slot(cur, i);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) L.ak[e] = slot(cur, 3 + e);
+        L.wks4 = slot(cur, 12);
+        if (k + 1 == nk - 1) {
+            const double *top = lv + kCompPlanes * (long)nk * ld;
+            L.a22 = __ldg(top + col);
+            L.a33 = __ldg(top + ld + col);
+            L.a23 = __ldg(top + 2 * ld + col);
+            L.a32 = __ldg(top + 3 * ld + col);
+        } else {
+            L.a22 = L.a33 = L.a23 = L.a32 = 0.0;
+        }
+    }
+    __device__ __forceinline__ double w(int) const { return slot(cur, 13); }
+    __device__ __forceinline__ double w1(int) const { return slot(cur, 14); }
+    __device__ __forceinline__ double fs(int r, int) const { return slot(cur, 15 + r); }
+    __device__ __forceinline__ double nms(int i, int) const { return slot(cur, 27 + i); }
+    __device__ __forceinline__ double adv(int i, int) const { return slot(cur, 30 + i); }
+    __device__ __forceinline__ double hd(int i, int) const { return slot(cur, 33 + i); }
+};
+
+constexpr int kCompRowThreads = 64;
+
+__global__ void __launch_bounds__(kCompRowThreads, 5) k_comp_rows(CompFields F, CompConsts C, const double *lv,
+                                                               double *out, double *scr, int nk, int ncol, long ld,
+                                                               double *sys_out, unsigned *status)
+{
+    extern __shared__ double comp_slots[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
-    CompPlaneSrc src{lv, ld, col, nk};
+    CompStagedSrc src{{{F, ld, col, nk}, lv}, comp_slots + threadIdx.x, (int)blockDim.x, 0};
     comp_walk(F, C, src, out, scr, nk, ld, col, sys_out, status);
 }
 
@@ -995,7 +1090,9 @@ cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out
     if (assembly_mode() == 1) {
         double *lv = scratch + 12 * (long)nk * ld;   // after the Gamma/z scratch
         k_comp_levels<<<dim3((ncol + T - 1) / T, nk), T, 0, st>>>(F, C, lv, nk, ncol, ld);
-        k_comp_rows<<<(ncol + T - 1) / T, T, 0, st>>>(F, C, lv, out, scratch, nk, ncol, ld, sys_out, status);
+        const int TR = kCompRowThreads;
+        k_comp_rows<<<(ncol + TR - 1) / TR, TR, 2 * CompStagedSrc::NS * TR * sizeof(double), st>>>(
+            F, C, lv, out, scratch, nk, ncol, ld, sys_out, status);
         return cudaGetLastError();
     }
     k_comp_ng<<<(ncol + T - 1) / T, T, 0, st>>>(F, C, out, scratch, nk, ncol, ld, sys_out, status);
