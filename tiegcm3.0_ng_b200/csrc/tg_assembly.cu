@@ -17,6 +17,7 @@
 
 #include "tg_internal.h"
 #include "tg_arith.cuh"
+#include "tg_stage.cuh"
 
 namespace tg {
 
@@ -494,6 +495,11 @@ __global__ void __launch_bounds__(128) k_minor_levels(MinorFields F, MinorConsts
     lv[2 * slab + (long)j * ld + col] = L.dmdzs;
 }
 
+// The column walk over the level planes.  Its eleven per-level reads are
+// staged one iteration ahead (Stage); the back sweep re-reads the parked w3
+// one level ahead.  The two divisions of a level share the divisor w1
+// (qdiv: one correctly rounded reciprocal, the same bits as IEEE a/b).
+constexpr int kMinorStaged = 11;
 __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C, const double *lv, double *out,
                                                     int nk, int ncol, long ld, double *sys_out, unsigned *status)
 {
@@ -502,28 +508,49 @@ __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C
     if (col >= ncol) return;
     double *w2s = smem_mr + threadIdx.x;
     const int T = blockDim.x;
-    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+    Stage<kMinorStaged> sg{smem_mr + (long)(nk > 1 ? nk - 1 : 1) * T + threadIdx.x, T};
     const long slab = (long)nk * ld;
-    auto lev = [&](int k) {
-        MinorLevel L;
-        L.ax = __ldg(lv + (long)k * ld + col);
-        L.thdiff = __ldg(lv + slab + (long)k * ld + col);
-        L.dmdzs = __ldg(lv + 2 * slab + (long)k * ld + col);
-        return L;
+    // reads of level k into buffer b: 0 sprod, 1 xnmbar, 2 ftm1_smooth,
+    // 3 hadvec, 4 sloss, 5 w(k), 6 w(k+1), 7..9 planes of level k+1
+    auto issue = [&](int k, int b) {
+        const long o = (long)k * ld + col;
+        sg.copy(b, 0, F.sprod + o);
+        sg.copy(b, 1, F.xnmbar + o);
+        sg.copy(b, 2, F.ftm1_smooth + o);
+        sg.copy(b, 3, F.hadvec + o);
+        if (k < nk - 1) {
+            sg.copy(b, 4, F.sloss + o);
+            sg.copy(b, 5, F.w + o);
+            sg.copy(b, 6, F.w + o + ld);
+            sg.copy(b, 7, lv + o + ld);
+            sg.copy(b, 8, lv + slab + o + ld);
+            sg.copy(b, 9, lv + 2 * slab + o + ld);
+        }
     };
     const double dzp = C.dzp, rdz = xd(1.0, dzp), dfac = __ldg(F.dfactor + col);
-    MinorLevel L0 = lev(0);
+    MinorLevel L0;
+    L0.ax = __ldg(lv + col);
+    L0.thdiff = __ldg(lv + slab + col);
+    L0.dmdzs = __ldg(lv + 2 * slab + col);
     bool ok = true;
-    double w1 = 0.0, w3 = 0.0, rprev = 0.0;
+    double w1 = 0.0, y1 = 0.0, w3 = 0.0, rprev = 0.0;
+    issue(0, 0);
+    sg.commit();
     for (int k = 0; k < nk; ++k) {
+        if (k + 1 < nk) issue(k + 1, (k + 1) & 1);
+        sg.commit();
+        sg.wait_prev();
+        const int b = k & 1;
         double p, q, r, f;
         const double expz = __ldg(F.expz + k);
-        const double sp = xd(xm(at(F.sprod, k), C.rmx), at(F.xnmbar, k));
-        f = xa(xs(xm(at(F.ftm1_smooth, k), C.dtx2inv), at(F.hadvec, k)), sp);
+        const double sp = xd(xm(sg.at(b, 0), C.rmx), sg.at(b, 1));
+        f = xa(xs(xm(sg.at(b, 2), C.dtx2inv), sg.at(b, 3)), sp);
         f = xm(f, expz);
         MinorLevel L1 = L0;
         if (k < nk - 1) {
-            L1 = lev(k + 1);
+            L1.ax = sg.at(b, 7);
+            L1.thdiff = sg.at(b, 8);
+            L1.dmdzs = sg.at(b, 9);
             const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1);
             const double molp = xm(L0.ax, xa(rdz, xm(0.5, L0.thdiff)));
             const double molr = xm(L1.ax, xs(rdz, xm(0.5, L1.thdiff)));
@@ -532,10 +559,10 @@ __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C
             const double eddyr = xm(xm(C.expzmid, difk1), xa(rdz, xm(0.5, L1.dmdzs)));
             const double eddyq = xa(xm(xm(C.expzmid_inv, difk0), xa(rdz, xm(0.5, L0.dmdzs))),
                                     xm(xm(C.expzmid, difk1), xs(rdz, xm(0.5, L1.dmdzs))));
-            const double wi = xm(0.5, xa(at(F.w, k), at(F.w, k + 1)));
+            const double wi = xm(0.5, xa(sg.at(b, 5), sg.at(b, 6)));
             p = xs(xd(molp, dzp), xd(xm(expz, xa(xm(eddyp, dfac), xm(0.5, wi))), dzp));
             r = xs(xd(molr, dzp), xd(xm(expz, xs(xm(eddyr, dfac), xm(0.5, wi))), dzp));
-            q = xa(-xd(molq, dzp), xm(expz, xs(xa(xd(xm(eddyq, dfac), dzp), C.dtx2inv), at(F.sloss, k))));
+            q = xa(-xd(molq, dzp), xm(expz, xs(xa(xd(xm(eddyq, dfac), dzp), C.dtx2inv), sg.at(b, 4))));
             if (k == 0) {
                 const double l1 = __ldg(F.flbc1 + col), l2 = __ldg(F.flbc2 + col), l3 = __ldg(F.flbc3 + col);
                 const double den = xs(l1, xm(xm(0.5, l2), dzp));
@@ -557,12 +584,14 @@ __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C
         }
         if (k == 0) {
             w1 = q;
-            w3 = xd(f, w1);
+            y1 = __drcp_rn(w1);
+            w3 = qdiv(f, w1, y1);
         } else {
-            const double w2 = xd(rprev, w1);
+            const double w2 = qdiv(rprev, w1, y1);
             w2s[(k - 1) * T] = w2;
             w1 = xs(q, xm(p, w2));
-            w3 = xd(xs(f, xm(p, w3)), w1);
+            y1 = __drcp_rn(w1);
+            w3 = qdiv(xs(f, xm(p, w3)), w1, y1);
         }
         ok = ok && fin_nz(w1);
         out[k * ld + col] = w3;
@@ -571,8 +600,11 @@ __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C
     }
     double xn = w3;
     bool fin = fabs(xn) <= DBL_MAX;
+    double park = nk >= 2 ? out[(nk - 2) * ld + col] : 0.0;
     for (int k = nk - 2; k >= 0; --k) {
-        xn = xs(out[k * ld + col], xm(w2s[k * T], xn));
+        const double wk = park;
+        if (k >= 1) park = out[(k - 1) * ld + col];
+        xn = xs(wk, xm(w2s[k * T], xn));
         fin = fin && fabs(xn) <= DBL_MAX;
         out[k * ld + col] = xn;
     }
@@ -607,8 +639,14 @@ cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *
             cudaFuncSetAttribute(k_minor_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
             attr = true;
         }
+        // the row walk also holds its staged reads in shared memory
+        const size_t per_r = (size_t)(nk - 1 > 0 ? nk - 1 : 1) * sizeof(double) + Stage<kMinorStaged>::bytes_per_thread;
+        int TR = 128;
+        while (TR > 32 && (size_t)TR * per_r > (size_t)optin) TR /= 2;
+        if ((size_t)TR * per_r > (size_t)optin) return cudaErrorInvalidValue;
         k_minor_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch, nk, ncol, ld);
-        k_minor_rows<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, scratch, out, nk, ncol, ld, sys_out, status);
+        k_minor_rows<<<(ncol + TR - 1) / TR, TR, (size_t)TR * per_r, st>>>(F, C, scratch, out, nk, ncol, ld, sys_out,
+                                                                          status);
         return cudaGetLastError();
     }
     k_minor_ng<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, out, nk, ncol, ld, sys_out, status);

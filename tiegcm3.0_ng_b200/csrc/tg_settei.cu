@@ -19,6 +19,8 @@
 #include <cfloat>
 
 #include "tg_internal.h"
+#include "tg_arith.cuh"
+#include "tg_stage.cuh"
 
 namespace tg {
 namespace {
@@ -352,6 +354,7 @@ __global__ void __launch_bounds__(128) k_settei_ng(SetteiFields F, SetteiConsts 
 // ---------------------------------------------------------------------------
 namespace {
 enum { P_TEK0 = 0, P_TH, P_DQ, P_QE, P_ET, P_LENTN, P_LEITI, P_LEI, P_LIN, P_QENI, P_N };
+constexpr int kSetteiStaged = 9;   // values per level staged by the row walk
 
 __device__ __forceinline__ double settei_fe(const SetteiFields &F, const SetteiConsts &C, long col)
 {
@@ -433,6 +436,11 @@ __global__ void __launch_bounds__(128) k_settei_levels(SetteiFields F, SetteiCon
     lv[P_QENI * slab + o] = R.q_eni;
 }
 
+// The column walk over the level planes.  Its per-level reads are staged
+// one iteration ahead (Stage): the forward sweep's nine values of level k+1
+// while level k computes, then the post steps' five values likewise.  The
+// two divisions of a level share the divisor w1: one correctly rounded
+// reciprocal and Markstein's correction (qdiv), the same bits as IEEE a/b.
 __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConsts C, const double *lv, double *te_out,
                                                      double *ti_out, double *qtotal, int nk, int ncol, long ld,
                                                      double *sys_out, unsigned *status)
@@ -442,6 +450,7 @@ __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConst
     if (col >= ncol) return;
     const int T = blockDim.x;
     double *w2s = smem_tr + threadIdx.x;
+    Stage<kSetteiStaged> sg{smem_tr + (long)(nk - 1) * T + threadIdx.x, T};
     const long slab = (long)nk * ld;
     auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
     auto pl = [&](int e, int k) { return __ldg(lv + e * slab + (long)k * ld + col); };
@@ -453,22 +462,44 @@ __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConst
         sindip = dmax(xm(sn, sn), .10);
     }
     const double t_lbc = __ldg(F.t_lbc + col);
-    double qe_m1 = 0., w1 = 0., w3 = 0., rprev = 0.;
+    // forward reads of level k into buffer b: 0 q_eni, 1 qtotal, 2 th(k+1),
+    // 3 scht, 4 qe, 5 et, 6 dq, 7 len_tn, 8 lei_ti
+    auto issue = [&](int k, int b) {
+        const long o = (long)k * ld + col;
+        sg.copy(b, 0, lv + P_QENI * slab + o);
+        if (k >= 1 && k <= nk - 2) sg.copy(b, 1, qtotal + o);
+        if (k <= nk - 2) {
+            sg.copy(b, 2, lv + P_TH * slab + o + ld);
+            sg.copy(b, 3, F.scht + o);
+            sg.copy(b, 4, lv + P_QE * slab + o);
+            if (C.et) sg.copy(b, 5, lv + P_ET * slab + o);
+            sg.copy(b, 6, lv + P_DQ * slab + o);
+            sg.copy(b, 7, lv + P_LENTN * slab + o);
+            sg.copy(b, 8, lv + P_LEITI * slab + o);
+        }
+    };
+    double qe_m1 = 0., w1 = 0., y1 = 0., w3 = 0., rprev = 0.;
     double th_k = pl(P_TH, 0);
     bool ok = true;
+    issue(0, 0);
+    sg.commit();
     for (int k = 0; k < nk; ++k) {
+        if (k + 1 < nk) issue(k + 1, (k + 1) & 1);
+        sg.commit();
+        sg.wait_prev();
+        const int b = k & 1;
         const long o = (long)k * ld + col;
-        const double q_eni = pl(P_QENI, k);
+        const double q_eni = sg.at(b, 0);
         // qtotal += q_eni at the interfaces (settei_ng.F90:248-254)
         if (k == 1) qtotal[col] = xa(qtotal[col], xs(xm(1.5, qe_m1), xm(0.5, q_eni)));
-        if (k >= 1 && k <= nk - 2) qtotal[o] = xa(qtotal[o], xm(.5, xa(qe_m1, q_eni)));
+        if (k >= 1 && k <= nk - 2) qtotal[o] = xa(sg.at(b, 1), xm(.5, xa(qe_m1, q_eni)));
         if (k == nk - 2) {
             const double qe_prev = k >= 1 ? qe_m1 : 0.;
             qtotal[(long)(nk - 1) * ld + col] = xa(qtotal[(long)(nk - 1) * ld + col], xs(xm(1.5, q_eni), xm(0.5, qe_prev)));
         }
         if (k <= nk - 2) {
-            const double th_1 = pl(P_TH, k + 1);
-            const double pb = xm(xd(xd(2., 7.), xm(at(F.scht, k), xm(dz, dz))), sindip);
+            const double th_1 = sg.at(b, 2);
+            const double pb = xm(xd(xd(2., 7.), xm(sg.at(b, 3), xm(dz, dz))), sindip);
             double r = xm(pb, th_1);
             double p = xm(pb, th_k);
             double q = -xa(p, r);
@@ -483,10 +514,10 @@ __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConst
                 rhs = xa(rhs, xd(xm(xm(xm(xm(r, dz), 3.5), at(F.schti, nk - 1)), fe), pl(P_TEK0, nk - 1)));
                 r = 0.;
             }
-            rhs = xs(rhs, pl(P_QE, k));
-            if (C.et) rhs = xs(rhs, pl(P_ET, k));
-            q = xs(q, pl(P_DQ, k));
-            rhs = xs(xs(rhs, pl(P_LENTN, k)), pl(P_LEITI, k));
+            rhs = xs(rhs, sg.at(b, 4));
+            if (C.et) rhs = xs(rhs, sg.at(b, 5));
+            q = xs(q, sg.at(b, 6));
+            rhs = xs(xs(rhs, sg.at(b, 7)), sg.at(b, 8));
             if (sys_out) {
                 sys_out[o] = p;
                 sys_out[slab + o] = q;
@@ -495,12 +526,14 @@ __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConst
             }
             if (k == 0) {
                 w1 = q;
-                w3 = xd(rhs, w1);
+                y1 = __drcp_rn(w1);
+                w3 = qdiv(rhs, w1, y1);
             } else {
-                const double w2 = xd(rprev, w1);
+                const double w2 = qdiv(rprev, w1, y1);
                 w2s[(long)(k - 1) * T] = w2;
                 w1 = xs(q, xm(p, w2));
-                w3 = xd(xs(rhs, xm(p, w3)), w1);
+                y1 = __drcp_rn(w1);
+                w3 = qdiv(xs(rhs, xm(p, w3)), w1, y1);
             }
             ok = ok && fabs(w1) <= DBL_MAX && w1 != 0.0;
             te_out[o] = w3;
@@ -509,29 +542,52 @@ __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConst
         }
         qe_m1 = q_eni;
     }
+    // back substitution and post steps over the levels K-1, K-2, ..., 0, K
+    // (call i treats level lev(i)); te_out holds w3 until a level is final
     const int K = nk - 1;
+    auto lev = [&](int i) { return i < K ? K - 1 - i : K; };
+    auto issue_b = [&](int i, int b) {
+        const long o = (long)lev(i) * ld + col;
+        sg.copy(b, 0, F.tn + o);
+        sg.copy(b, 1, lv + P_LEI * slab + o);
+        sg.copy(b, 2, lv + P_LIN * slab + o);
+        sg.copy(b, 3, F.qji_ti + o);
+        sg.copy(b, 4, F.xnmbar + o);
+    };
     double xn = w3;
     double tk = pow(xn, xd(2., 7.));
     double t_top1 = tk, t_top2 = 0.;
     bool fin = fabs(xn) <= DBL_MAX;
-    auto finish = [&](int k, double t) {
+    double park = K >= 2 ? te_out[(long)(K - 2) * ld + col] : 0.;
+    issue_b(0, 0);
+    sg.commit();
+    for (int i = 0; i <= K; ++i) {
+        if (i + 1 <= K) issue_b(i + 1, (i + 1) & 1);
+        sg.commit();
+        sg.wait_prev();
+        const int b = i & 1, k = lev(i);
+        double t;
+        if (i == 0) {
+            t = tk;
+        } else if (i < K) {
+            const double wk = park;
+            if (k >= 1) park = te_out[(long)(k - 1) * ld + col];
+            xn = xs(wk, xm(w2s[(long)k * T], xn));
+            fin = fin && fabs(xn) <= DBL_MAX;
+            tk = pow(xn, xd(2., 7.));
+            if (k == K - 2) t_top2 = tk;
+            t = tk;
+        } else {
+            t = xd(xm(t_top1, t_top1), t_top2);
+        }
         const long o = (long)k * ld + col;
-        const double tn = at(F.tn, k);
+        const double tn = sg.at(b, 0);
         const double te = dmax(t, tn);
-        const double lei = pl(P_LEI, k), lin = pl(P_LIN, k);
+        const double lei = sg.at(b, 1), lin = sg.at(b, 2);
         te_out[o] = te;
-        const double num = xa(xa(xd(xm(at(F.qji_ti, k), at(F.xnmbar, k)), C.avo), xm(lei, te)), xm(lin, tn));
+        const double num = xa(xa(xd(xm(sg.at(b, 3), sg.at(b, 4)), C.avo), xm(lei, te)), xm(lin, tn));
         ti_out[o] = dmax(xd(num, xa(lei, lin)), tn);
-    };
-    finish(K - 1, tk);
-    for (int k = K - 2; k >= 0; --k) {
-        xn = xs(te_out[(long)k * ld + col], xm(w2s[(long)k * T], xn));
-        fin = fin && fabs(xn) <= DBL_MAX;
-        tk = pow(xn, xd(2., 7.));
-        if (k == K - 2) t_top2 = tk;
-        finish(k, tk);
     }
-    finish(K, xd(xm(t_top1, t_top1), t_top2));
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
@@ -563,7 +619,7 @@ cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, doubl
             attr = true;
         }
         int T2 = 128;
-        const size_t per2 = (size_t)(nk - 1) * sizeof(double);
+        const size_t per2 = (size_t)(nk - 1) * sizeof(double) + Stage<kSetteiStaged>::bytes_per_thread;
         while (T2 > 32 && (size_t)T2 * per2 > (size_t)optin) T2 /= 2;
         k_settei_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch, nk, ncol, ld);
         k_settei_rows<<<(ncol + T2 - 1) / T2, T2, (size_t)T2 * per2, st>>>(F, C, scratch, te_out, ti_out, qtotal, nk,
