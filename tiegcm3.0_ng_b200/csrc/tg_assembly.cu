@@ -47,6 +47,11 @@ __device__ __forceinline__ GF dt_gf(const DtConsts &C, double h, double cp, doub
 }
 }  // namespace
 
+// Per-level reads are staged one iteration ahead (Stage): the 13 fields of
+// row k and the level-(k+2) window while row k-1 computes.  The two divisions
+// of a row share the divisor w1 (qdiv: one correctly rounded reciprocal, the
+// same bits as IEEE a/b).
+constexpr int kDtStaged = 20;
 __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *tn_upd, int nk, int ncol, long ld,
                                                double *sys_out, unsigned *status)
 {
@@ -55,6 +60,7 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
     if (col >= ncol) return;
     double *w2s = smem_dt + threadIdx.x;
     const int T = blockDim.x;
+    Stage<kDtStaged> sg{smem_dt + (long)(nk - 2 > 0 ? nk - 2 : 1) * T + threadIdx.x, T};
     auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
     const double dz = C.dz;
     const double tlbc_prev = __ldg(F.tlbc + col), tlbc_cur = __ldg(F.t_lbc + col);
@@ -75,14 +81,49 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
     GF gf0 = dt_gf(C, at(F.schti, 0), cp_0, at(F.kt, 0), tlbc_prev, __ldg(F.expz), __ldg(F.dift));
     double dudz_prev = 0.0, dvdz_prev = 0.0;
 
+    // reads of row k into buffer b: 0 schti(k+1), 1 kt(k+1), 2 horadv, 3
+    // tnsmooth, 4 mbar, 5 xnmbar, 6 o1, 7 rkm12, 8 scht, 9 hdt, 10 qji_tn, 11
+    // cool_exp, 12 cool_imp; 13..19 tn, un, vn, w, cp, km, qtotal of level k+2
+    auto issue = [&](int k, int b) {
+        const long o = (long)k * ld + col;
+        sg.copy(b, 0, F.schti + o + ld);
+        sg.copy(b, 1, F.kt + o + ld);
+        sg.copy(b, 2, F.horadv + o);
+        sg.copy(b, 3, F.tnsmooth + o);
+        sg.copy(b, 4, F.mbar + o);
+        sg.copy(b, 5, F.xnmbar + o);
+        sg.copy(b, 6, F.o1 + o);
+        sg.copy(b, 7, F.rkm12 + o);
+        sg.copy(b, 8, F.scht + o);
+        sg.copy(b, 9, F.hdt + o);
+        sg.copy(b, 10, F.qji_tn + o);
+        sg.copy(b, 11, F.cool_exp + o);
+        sg.copy(b, 12, F.cool_imp + o);
+        if (k + 2 < nk) {
+            const long o2 = o + 2 * ld;
+            sg.copy(b, 13, F.tn + o2);
+            sg.copy(b, 14, F.un + o2);
+            sg.copy(b, 15, F.vn + o2);
+            sg.copy(b, 16, F.w + o2);
+            sg.copy(b, 17, F.cp + o2);
+            sg.copy(b, 18, F.km + o2);
+            sg.copy(b, 19, F.qtotal + o2);
+        }
+    };
     bool ok = true;
-    double w1 = 0.0, w3 = 0.0, rprev = 0.0;
+    double w1 = 0.0, y1 = 0.0, w3 = 0.0, rprev = 0.0;
+    issue(0, 0);
+    sg.commit();
     for (int k = 0; k < K; ++k) {
+        if (k + 1 < K) issue(k + 1, (k + 1) & 1);
+        sg.commit();
+        sg.wait_prev();
+        const int b = k & 1;
         const double expz = __ldg(F.expz + k), expz_p = __ldg(F.expz + k + 1);
         // level k+1 quantities
         const double v0_p = (k + 1 <= nk - 2) ? xm(xs(tn_p, tn_0), w_p) : 0.0;
         const double tni_p = (k + 1 <= nk - 2) ? xm(0.5, xa(tn_0, tn_p)) : tn_0;
-        const GF gfp = dt_gf(C, at(F.schti, k + 1), cp_p, at(F.kt, k + 1), tni_p, expz_p, __ldg(F.dift + k + 1));
+        const GF gfp = dt_gf(C, sg.at(b, 0), cp_p, sg.at(b, 1), tni_p, expz_p, __ldg(F.dift + k + 1));
         // tridiagonal row (dt_ng.F90:141-148)
         double p = xs(gf0.g, gf0.f);
         double q, r;
@@ -112,18 +153,18 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
         }
         const double qsolar = xm(0.5, xa(qt_0, qt_p));
         // heating and right-hand side (:81-84, :97-118, :150-157)
-        const double advec = xa(at(F.horadv, k), vad);
-        double cptn = xm(cpi, xs(advec, xm(C.dtx2inv, at(F.tnsmooth, k))));
+        const double advec = xa(sg.at(b, 2), vad);
+        double cptn = xm(cpi, xs(advec, xm(C.dtx2inv, sg.at(b, 3))));
         cptn = xm(cptn, expz);
-        const double mbar = at(F.mbar, k);
-        const double xo = xm(xm(at(F.xnmbar, k), at(F.o1, k)), C.rmassinv_o1);
-        const double qrecomb = xd(xm(xm(xm(C.tsurplus, at(F.rkm12, k)), xm(xo, xo)), C.avo), mbar);
-        double qm = xm(xd(xm(C.grav, kmi), xm(C.p0, at(F.scht, k))), xa(xm(dudz, dudz), xm(dvdz, dvdz)));
+        const double mbar = sg.at(b, 4);
+        const double xo = xm(xm(sg.at(b, 5), sg.at(b, 6)), C.rmassinv_o1);
+        const double qrecomb = xd(xm(xm(xm(C.tsurplus, sg.at(b, 7)), xm(xo, xo)), C.avo), mbar);
+        double qm = xm(xd(xm(C.grav, kmi), xm(C.p0, sg.at(b, 8))), xa(xm(dudz, dudz), xm(dvdz, dvdz)));
         qm = xd(qm, expz);
-        const double th = xa(xa(xa(xa(qsolar, at(F.hdt, k)), qrecomb), at(F.qji_tn, k)), qm);
+        const double th = xa(xa(xa(xa(qsolar, sg.at(b, 9)), qrecomb), sg.at(b, 10)), qm);
         cptn = xs(cptn, xm(th, expz));
-        double rhs = xa(cptn, at(F.cool_exp, k));
-        const double qpart = xa(xm(cpi, xa(C.dtx2inv, at(F.cool_imp, k))), xd(xm(wi, C.gask), mbar));
+        double rhs = xa(cptn, sg.at(b, 11));
+        const double qpart = xa(xm(cpi, xa(C.dtx2inv, sg.at(b, 12))), xd(xm(wi, C.gask), mbar));
         q = xs(q, xm(qpart, expz));
         if (k == 0) {   // lower boundary fold (:159-163)
             q = xs(q, p);
@@ -140,12 +181,14 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
         // Thomas forward step (trsolv_ng.F90:14-22), a=p, b=q, c(k-1)=r(k-1), f=rhs
         if (k == 0) {
             w1 = q;
-            w3 = xd(rhs, w1);
+            y1 = __drcp_rn(w1);
+            w3 = qdiv(rhs, w1, y1);
         } else {
-            const double w2 = xd(rprev, w1);
+            const double w2 = qdiv(rprev, w1, y1);
             w2s[(k - 1) * T] = w2;
             w1 = xs(q, xm(p, w2));
-            w3 = xd(xs(rhs, xm(p, w3)), w1);
+            y1 = __drcp_rn(w1);
+            w3 = qdiv(xs(rhs, xm(p, w3)), w1, y1);
         }
         ok = ok && fin_nz(w1);
         tn_upd[k * ld + col] = w3;
@@ -160,21 +203,24 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
         vn_m = vn_0; vn_0 = vn_p;
         w_0 = w_p; cp_0 = cp_p; km_0 = km_p; qt_0 = qt_p;
         if (k + 2 < nk) {
-            tn_p = at(F.tn, k + 2);
-            un_p = at(F.un, k + 2);
-            vn_p = at(F.vn, k + 2);
-            w_p = at(F.w, k + 2);
-            cp_p = at(F.cp, k + 2);
-            km_p = at(F.km, k + 2);
-            qt_p = at(F.qtotal, k + 2);
+            tn_p = sg.at(b, 13);
+            un_p = sg.at(b, 14);
+            vn_p = sg.at(b, 15);
+            w_p = sg.at(b, 16);
+            cp_p = sg.at(b, 17);
+            km_p = sg.at(b, 18);
+            qt_p = sg.at(b, 19);
         }
     }
     // back sweep (trsolv_ng.F90:23-26), then tn(nk) = tn(nk-1)**2/tn(nk-2)
     double xn = w3, xprev = w3;
     bool fin = fabs(xn) <= DBL_MAX;
+    double park = K >= 2 ? tn_upd[(K - 2) * ld + col] : 0.0;
     for (int k = K - 2; k >= 0; --k) {
         xprev = xn;
-        xn = xs(tn_upd[k * ld + col], xm(w2s[k * T], xn));
+        const double wk = park;
+        if (k >= 1) park = tn_upd[(k - 1) * ld + col];
+        xn = xs(wk, xm(w2s[k * T], xn));
         fin = fin && fabs(xn) <= DBL_MAX;
         tn_upd[k * ld + col] = xn;
         if (k == K - 2) {
@@ -189,8 +235,10 @@ cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, i
                          double *sys_out, unsigned *status, cudaStream_t st)
 {
     if (ncol <= 0) return cudaSuccess;
-    const int T = 128;
-    const size_t smem = (size_t)T * (nk - 2 > 0 ? nk - 2 : 1) * sizeof(double);
+    // one warp per block keeps a wave of small blocks resident despite the
+    // per-thread shared memory (w2 column + staged reads)
+    const int T = 32;
+    const size_t smem = (size_t)T * ((nk - 2 > 0 ? nk - 2 : 1) * sizeof(double) + Stage<kDtStaged>::bytes_per_thread);
     static bool attr = false;
     if (!attr) {
         int dev = 0, optin = 0;
