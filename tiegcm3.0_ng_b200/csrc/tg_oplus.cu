@@ -18,6 +18,7 @@
 #include <cfloat>
 
 #include "tg_internal.h"
+#include "tg_arith.cuh"
 
 namespace tg {
 namespace {
@@ -166,8 +167,24 @@ __device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusCons
     const double ubca = xm(xm(-bz2, djint(nk - 1)), tph1(nk - 1));
     const double ubcb = xm(xm(-bz2, djint(nk - 1)), tph0(nk - 1));
     bool ok = true;
-    double w1 = 0., w3 = 0., rprev = 0.;
+    double w1 = 0., y1 = 0., w3 = 0., rprev = 0.;
+    // bring the lines row k+1 touches first (the planes at level k+2, the
+    // fields at k+1) into L1 while row k computes
+    auto pf = [&](const double *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); };
     for (int k = 0; k < nk - 1; ++k) {
+        if (k + 1 < nk - 1) {
+            const long o1 = (long)(k + 1) * ld + col;
+            if (k + 2 < nk) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) pf(scr + (long)e * slab + o1 + ld);
+                pf(F.wi + o1 + ld);
+            }
+            pf(F.bdotdh_djbz + o1);
+            pf(F.explicit_h + o1);
+            pf(F.optm1_smooth2 + o1);
+            pf(scr + (long)S_OL * slab + o1);
+            pf(scr + (long)S_PROD * slab + o1);
+        }
         const double hdzm_k = hdzmp(k, -1.), hdzp_k = hdzmp(k, 1.);
         const double dji_k = djint(k), dji_1 = djint(k + 1);
         const double t0k = tph0(k), t1k = tph1(k), t01 = tph0(k + 1), t11 = tph1(k + 1);
@@ -210,12 +227,14 @@ __device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusCons
         }
         if (k == 0) {
             w1 = q;
-            w3 = xd(ex, w1);
+            y1 = __drcp_rn(w1);
+            w3 = qdiv(ex, w1, y1);
         } else {
-            const double w2 = xd(rprev, w1);
+            const double w2 = qdiv(rprev, w1, y1);
             w2s[(long)(k - 1) * T] = w2;
             w1 = xs(q, xm(p, w2));
-            w3 = xd(xs(ex, xm(p, w3)), w1);
+            y1 = __drcp_rn(w1);
+            w3 = qdiv(xs(ex, xm(p, w3)), w1, y1);
         }
         ok = ok && fabs(w1) <= DBL_MAX && w1 != 0.0;
         opout[(long)k * ld + col] = w3;
@@ -225,8 +244,11 @@ __device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusCons
     const int K = nk - 1;
     double xn = w3, xtop = w3;
     bool fin = fabs(xn) <= DBL_MAX;
+    double park = K >= 2 ? opout[(long)(K - 2) * ld + col] : 0.;
     for (int k = K - 2; k >= 0; --k) {
-        xn = xs(opout[(long)k * ld + col], xm(w2s[(long)k * T], xn));
+        const double wk = park;
+        if (k >= 1) park = opout[(long)(k - 1) * ld + col];
+        xn = xs(wk, xm(w2s[(long)k * T], xn));
         fin = fin && fabs(xn) <= DBL_MAX;
         opout[(long)k * ld + col] = xn;
         if (k == K - 2) opout[(long)K * ld + col] = xd(xm(xtop, xtop), xn);
