@@ -460,6 +460,12 @@ int tg_set_scalar_scratch_budget(double megabytes);
  * resident wave.  Same results either way. */
 int tg_set_kind_overlap(int mode);
 
+/* Host-array entries (tg_solve_host and the per-routine drop-ins): the input
+ * bytes per pipelined column chunk, in KiB, and the number of streams the
+ * chunks rotate over (1..8); <= 0 restores the defaults (streams 3; chunks of
+ * a sixth of the call's input bytes, kept within 4..64 MiB). */
+int tg_set_host_pipeline(int chunk_kb, int streams);
+
 /* Runs the ring kernels' bounded mbarrier wait on a barrier that nothing
  * completes, giving up after `polls` polls (1..2^22): *status_dev receives
  * TG_ETIMEOUT, as a solve does when a bulk copy never lands.  Tests the

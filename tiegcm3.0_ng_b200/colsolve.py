@@ -41,7 +41,7 @@ EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor
            "tg_comp_ng_dev", "tg_comp_post_ng", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
-           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
+           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
 
 
@@ -226,6 +226,7 @@ def lib():
             "tg_set_block_scratch_budget": [D],
             "tg_set_scalar_scratch_budget": [D],
             "tg_set_kind_overlap": [I],
+            "tg_set_host_pipeline": [I, I],
             "tg_selftest_wait": [ctypes.c_uint, P, P],
             "tg_plan_sweep_histogram": [P, ctypes.POINTER(Lg), I],
             "tg_plan_destroy": [P],
@@ -629,6 +630,11 @@ def set_scalar_scratch_budget(megabytes):
 def set_kind_overlap(mode):
     """Kinds of a plan: 1 side by side, 0 one after the other, -1 side by side when each fits in one wave."""
     return _check(lib().tg_set_kind_overlap(int(mode)), "tg_set_kind_overlap")
+
+
+def set_host_pipeline(chunk_kb=0, streams=0):
+    """Host-array entries: input KiB per pipelined column chunk and streams (<= 0: defaults)."""
+    return _check(lib().tg_set_host_pipeline(int(chunk_kb), int(streams)), "tg_set_host_pipeline")
 
 
 def set_block_scratch_budget(megabytes):

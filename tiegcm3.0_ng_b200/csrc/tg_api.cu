@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <new>
@@ -51,9 +52,11 @@ struct Buf {
 };
 
 // Per-device work buffers and streams, created on first use.  The host
-// drop-ins pipeline column chunks over kSlots streams, each with its own
-// buffers.
-constexpr int kSlots = 3;
+// drop-ins pipeline column chunks over up to kSlots streams (g_host_slots in
+// use, 3 by default), each with its own buffers.
+constexpr int kSlots = 8;
+std::atomic<int> g_host_slots{3};
+std::atomic<long> g_host_chunk_bytes{0};   // 0: chosen per call
 struct DevCtx {
     int dev = -1;
     std::mutex mu;
@@ -225,7 +228,27 @@ struct HostPlan {
     long mrows, vrows, orows, mstride, chunk;
 };
 
-HostPlan host_plan(const HostSys &h)
+// Input bytes of one system in the host (Fortran) layout.
+long host_bytes(const HostSys &h)
+{
+    const long B = h.kind == TG_KIND_SCALAR ? 1 : h.kind;
+    return (3 * B * B + B) * (long)h.k2 * h.ncol * 8;
+}
+
+// Column chunk size of a call: every chunk costs a fixed few tens of
+// microseconds (copies, relayouts, a solve launch whose columns are too few
+// to fill the GPU), so large calls use large chunks; about six chunks per
+// call keep the copy-in of the next chunk overlapping the solve of this one.
+long host_chunk_bytes(const HostSys *sys, int nsys)
+{
+    const long set = g_host_chunk_bytes.load();
+    if (set > 0) return set;
+    long total = 0;
+    for (int i = 0; i < nsys; ++i) total += host_bytes(sys[i]);
+    return std::max(4l << 20, std::min(64l << 20, total / 6));
+}
+
+HostPlan host_plan(const HostSys &h, long chunk_bytes)
 {
     HostPlan p;
     p.B = h.kind == TG_KIND_SCALAR ? 1 : h.kind;
@@ -234,7 +257,7 @@ HostPlan host_plan(const HostSys &h)
     p.orows = (long)p.B * (h.k2 + (h.ubc_ratio ? 1 : 0));
     p.mstride = (long)p.B * h.colstride;
     const long in_per_col = (3 * p.mrows + p.vrows) * 8;
-    long nchunks = (in_per_col * h.ncol + (4l << 20) - 1) / (4l << 20);
+    long nchunks = (in_per_col * h.ncol + chunk_bytes - 1) / chunk_bytes;
     nchunks = std::max<long>(1, std::min<long>(nchunks, 64));
     p.chunk = round_up((h.ncol + nchunks - 1) / nchunks, 32);
     return p;
@@ -249,8 +272,9 @@ int host_solve_many(const HostSys *sys, int nsys, int precision)
     TG_CUDA(cudaSetDevice(c->dev));
     std::vector<HostPlan> plans(nsys);
     long need_m = 0, need_v = 0, need_o = 0, need_u = 0, total_chunks = 0;
+    const long chunk_bytes = host_chunk_bytes(sys, nsys);
     for (int i = 0; i < nsys; ++i) {
-        plans[i] = host_plan(sys[i]);
+        plans[i] = host_plan(sys[i], chunk_bytes);
         const HostPlan &p = plans[i];
         need_m = std::max(need_m, p.mrows * p.chunk);
         need_v = std::max(need_v, p.vrows * p.chunk);
@@ -259,7 +283,7 @@ int host_solve_many(const HostSys *sys, int nsys, int precision)
         total_chunks += (sys[i].ncol + p.chunk - 1) / p.chunk;
     }
     if (total_chunks == 0) return TG_OK;
-    const int nslots = (int)std::min<long>(kSlots, total_chunks);
+    const int nslots = (int)std::min<long>(g_host_slots.load(), total_chunks);
     for (int s = 0; s < nslots; ++s) {
         for (int i = 0; i < 3; ++i)
             if ((rc = grow(c->colbuf[s][i], sizeof(double) * need_m))) return rc;
@@ -1478,6 +1502,17 @@ __attribute__((visibility("default"))) int tg_set_scalar_scratch_budget(double m
 __attribute__((visibility("default"))) int tg_set_kind_overlap(int mode)
 {
     tg::set_kind_overlap(mode);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_host_pipeline(int chunk_kb, int streams)
+{
+    if (streams > kSlots) {
+        set_err("tg_set_host_pipeline: at most %d streams", kSlots);
+        return TG_EINVAL;
+    }
+    g_host_chunk_bytes.store(chunk_kb > 0 ? (long)chunk_kb << 10 : 0);
+    g_host_slots.store(streams > 0 ? streams : 3);
     return TG_OK;
 }
 
