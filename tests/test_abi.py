@@ -67,3 +67,18 @@ def test_bad_arguments_rejected_without_device(pkg):
     assert L.tg_trsolv_ng(p, p, p, p, p, 5, 6, 3) == pkg.TG_EINVAL
     assert L.tg_comp_blksolve_ng(4, p, p, p, p, None, None, p, 5, 1) == pkg.TG_EINVAL
     assert L.tg_plan_create(None, 1, 0, None) == pkg.TG_EINVAL
+
+
+def test_tuning_entries_validate_without_device(pkg):
+    """Tuning entries reject out-of-range values and accept their resets
+    without touching CUDA."""
+    L = pkg.colsolve.lib()
+    assert L.tg_set_host_pipeline(0, 9) == pkg.TG_EINVAL   # at most 8 streams
+    assert L.tg_set_host_pipeline(2048, 4) == pkg.TG_OK
+    assert L.tg_set_host_pipeline(0, 0) == pkg.TG_OK       # defaults back
+    assert L.tg_set_kind_overlap(0) == pkg.TG_OK
+    assert L.tg_set_kind_overlap(-1) == pkg.TG_OK
+    assert L.tg_set_scalar_scratch_budget(0.0) == pkg.TG_OK
+    assert L.tg_set_pipeline(pkg.TG_KIND_SCALAR, pkg.TG_PREC_F32_REFINE, 8, 1) == pkg.TG_EINVAL
+    assert L.tg_set_pipeline(pkg.TG_KIND_BLOCK2, pkg.TG_PREC_F32_REFINE, 4, 1) == pkg.TG_EINVAL
+    assert L.tg_set_pipeline(pkg.TG_KIND_SCALAR, pkg.TG_PREC_F32_REFINE, -1, 0) == pkg.TG_OK

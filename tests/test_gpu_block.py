@@ -107,3 +107,26 @@ def test_solve_host_mixed_batch(cuda, pkg, orc):
             assert np.array_equal(q["x"][:k2], ref[:k2])
         else:
             assert np.array_equal(q["x"][:, :k2 + 1], ref[:, :k2 + 1])
+
+
+@pytest.mark.parametrize("chunk_kb,streams", [(1024, 1), (4096, 3), (65536, 8)])
+def test_solve_host_chunking_keeps_bits(cuda, pkg, orc, chunk_kb, streams):
+    """Any column-chunk size and stream count of the host pipeline gives the
+    oracle's bits (the chunks are independent column batches)."""
+    systems, refs = [], []
+    for i, (nk, ncol) in enumerate(((57, 5000), (29, 777))):
+        a, b, c, f = pkg.synth.scalar_system(nk, ncol, 14.0 / (nk - 1), 700 + i)
+        x = np.zeros_like(a, order="F")
+        systems.append(dict(kind=pkg.TG_KIND_SCALAR, a=a, b=b, c=c, f=f, x=x, k2=nk))
+        refs.append(orc.trsolv_ng(a, b, c, f, nk))
+    P, Q, R, f = pkg.synth.block_system(2, 57, 1500, 0.25, 702)
+    u = np.zeros_like(f, order="F")
+    systems.append(dict(kind=2, a=P, b=Q, c=R, f=f, x=u, k2=57))
+    refs.append(orc.blksolve(P, Q, R, f, 57))
+    pkg.set_host_pipeline(chunk_kb, streams)
+    try:
+        assert pkg.solve_host(systems) == pkg.TG_OK
+    finally:
+        pkg.set_host_pipeline(0, 0)
+    for q, ref in zip(systems, refs):
+        assert np.array_equal(q["x"], ref)

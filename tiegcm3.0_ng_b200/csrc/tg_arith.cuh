@@ -44,4 +44,18 @@ __device__ __forceinline__ double qdiv(double a, double b, double y)
     return div_safe(a, b) ? div_markstein(a, b, y) : __ddiv_rn(a, b);
 }
 
+// |v| in [2^-500, 2^500) from the exponent bits alone (biased exponent
+// 523..1522): integer operations, a subset of div_safe's range.
+__device__ __forceinline__ bool exp_safe(double v)
+{
+    const unsigned e2 = (unsigned)__double2hiint(v) * 2u - (523u << 21);   // sign bit shifted out
+    return e2 < (1000u << 21);
+}
+// a/b, correctly rounded, given y = __drcp_rn(b) and b_safe = exp_safe(b),
+// which a recurrence computes once for the two divisions by the same pivot.
+__device__ __forceinline__ double qdiv_pivot(double a, double b, double y, bool b_safe)
+{
+    return b_safe && exp_safe(a) ? div_markstein(a, b, y) : __ddiv_rn(a, b);
+}
+
 }  // namespace tg

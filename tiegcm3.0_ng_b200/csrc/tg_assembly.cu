@@ -293,8 +293,9 @@ __device__ __forceinline__ void inv3_ieee(const double (&A)[9], double (&W)[9])
     // the nine quotients share the divisor: correctly rounded, bit-identical
     // to IEEE division (qdiv)
     const double y = __drcp_rn(d);
+    const bool ds = exp_safe(d);
 #pragma unroll
-    for (int e = 0; e < 9; ++e) W[e] = qdiv(W[e], d, y);
+    for (int e = 0; e < 9; ++e) W[e] = qdiv_pivot(W[e], d, y, ds);
 }
 
 struct MinorLevel {

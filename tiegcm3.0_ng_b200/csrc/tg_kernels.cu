@@ -527,6 +527,7 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
         for (int j = 0; j < pre; ++j) issue(q + j, j);
         bool ok = true, fin = true;
         double w1 = 0.0, y1 = 0.0, w3 = 0.0, cprev = 0.0;
+        bool w1s = false;   // exp_safe(w1): the pivot's range test, shared by its two divisions
         for (int j = 0; j < nch; ++j) {
             const unsigned qc = q + j;
             if (!mbar_wait_warp(&bar[qc % C], (qc / C) & 1u)) {
@@ -549,15 +550,18 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
                         if (k == 0) {
                             w1 = bk;
                             y1 = __drcp_rn(w1);
-                            w3 = qdiv(fk, w1, y1);
+                            w1s = exp_safe(w1);
+                            w3 = qdiv_pivot(fk, w1, y1, w1s);
                         } else {
-                            const double w2 = qdiv(cprev, w1, y1);
+                            const double w2 = qdiv_pivot(cprev, w1, y1, w1s);
                             st_hint(&w2s[(k - 1) * ws], w2, keep);
                             w1 = xsub(bk, xmul(ak, w2));
                             y1 = __drcp_rn(w1);
-                            w3 = qdiv(xsub(fk, xmul(ak, w3)), w1, y1);
+                            w1s = exp_safe(w1);
+                            w3 = qdiv_pivot(xsub(fk, xmul(ak, w3)), w1, y1, w1s);
                         }
-                        ok = ok && finite_nz(w1);
+                        // a pivot in the safe range is finite and nonzero
+                        if (!w1s) ok = ok && finite_nz(w1);
                         cprev = stg[(4 * l + 2) * 32];
                         st_hint(&px[k * ld], w3, keep);
                     }
@@ -1128,11 +1132,12 @@ __device__ __forceinline__ bool inv_exact<2>(const double (&A)[4], double (&W)[4
 {
     const double d = xsub(xmul(A[0], A[3]), xmul(A[2], A[1]));
     const double y = __drcp_rn(d);
-    W[0] = qdiv(A[3], d, y);
-    W[1] = qdiv(-A[1], d, y);
-    W[2] = qdiv(-A[2], d, y);
-    W[3] = qdiv(A[0], d, y);
-    return finite_nz(d);
+    const bool ds = exp_safe(d);
+    W[0] = qdiv_pivot(A[3], d, y, ds);
+    W[1] = qdiv_pivot(-A[1], d, y, ds);
+    W[2] = qdiv_pivot(-A[2], d, y, ds);
+    W[3] = qdiv_pivot(A[0], d, y, ds);
+    return ds || finite_nz(d);
 }
 
 template <>
@@ -1158,9 +1163,10 @@ __device__ __forceinline__ bool inv_exact<3>(const double (&A)[9], double (&W)[9
 #undef a_
 #undef w_
     const double y = __drcp_rn(d);
+    const bool ds = exp_safe(d);
 #pragma unroll
-    for (int e = 0; e < 9; ++e) W[e] = qdiv(W[e], d, y);
-    return finite_nz(d);
+    for (int e = 0; e < 9; ++e) W[e] = qdiv_pivot(W[e], d, y, ds);
+    return ds || finite_nz(d);
 }
 
 // Loads the blocks of level k: P (if wantP), Q, R (if wantR), f.
