@@ -540,31 +540,35 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
             // the stage is read in place and handed back to the copy engine
             // after the L levels are done (registers stay low: more warps/SM)
             const double *stg = buf + (int)(qc % C) * NE * 32 + lane;
+            // level k from stage row l; `first` only for level 0
+            auto step = [&](int l, int k, bool first) {
+                const double ak = stg[(4 * l + 0) * 32], bk = stg[(4 * l + 1) * 32], fk = stg[(4 * l + 3) * 32];
+                if (first) {
+                    w1 = bk;
+                    y1 = __drcp_rn(w1);
+                    w1s = exp_safe(w1);
+                    w3 = qdiv_pivot(fk, w1, y1, w1s);
+                } else {
+                    const double w2 = qdiv_pivot(cprev, w1, y1, w1s);
+                    st_hint(&w2s[(k - 1) * ws], w2, keep);
+                    w1 = xsub(bk, xmul(ak, w2));
+                    y1 = __drcp_rn(w1);
+                    w1s = exp_safe(w1);
+                    w3 = qdiv_pivot(xsub(fk, xmul(ak, w3)), w1, y1, w1s);
+                }
+                // a pivot in the safe range is finite and nonzero
+                if (!w1s) ok = ok && finite_nz(w1);
+                cprev = stg[(4 * l + 2) * 32];
+                st_hint(&px[k * ld], w3, keep);
+            };
             if (valid) {
+                if (j > 0 && (j + 1) * L <= k2) {   // a full chunk past level 0: no per-level tests
 #pragma unroll
-                for (int l = 0; l < L; ++l) {
-                    const int k = j * L + l;
-                    if (k < k2) {
-                        const double ak = stg[(4 * l + 0) * 32], bk = stg[(4 * l + 1) * 32],
-                                     fk = stg[(4 * l + 3) * 32];
-                        if (k == 0) {
-                            w1 = bk;
-                            y1 = __drcp_rn(w1);
-                            w1s = exp_safe(w1);
-                            w3 = qdiv_pivot(fk, w1, y1, w1s);
-                        } else {
-                            const double w2 = qdiv_pivot(cprev, w1, y1, w1s);
-                            st_hint(&w2s[(k - 1) * ws], w2, keep);
-                            w1 = xsub(bk, xmul(ak, w2));
-                            y1 = __drcp_rn(w1);
-                            w1s = exp_safe(w1);
-                            w3 = qdiv_pivot(xsub(fk, xmul(ak, w3)), w1, y1, w1s);
-                        }
-                        // a pivot in the safe range is finite and nonzero
-                        if (!w1s) ok = ok && finite_nz(w1);
-                        cprev = stg[(4 * l + 2) * 32];
-                        st_hint(&px[k * ld], w3, keep);
-                    }
+                    for (int l = 0; l < L; ++l) step(l, j * L + l, false);
+                } else {
+#pragma unroll
+                    for (int l = 0; l < L; ++l)
+                        if (j * L + l < k2) step(l, j * L + l, j * L + l == 0);
                 }
             }
             __syncwarp();
