@@ -66,6 +66,25 @@ def test_trsolv_slab(cuda, pkg, orc, lon0, lon1, k1, k2):
     assert np.array_equal(x, ref)
 
 
+def test_nonfinite_solution_status_and_values(cuda, pkg, orc):
+    """Finite pivots but an inf or NaN right-hand side: the columns' x turn
+    non-finite from that level down (also through a zero w2), the call
+    reports TG_ENONFINITE and the values match the oracle's."""
+    (a, b, c, f), nk = system(pkg, 0, 96)
+    c = c.copy(order="F")
+    f = f.copy(order="F")
+    f[5, 7] = np.inf
+    f[15, 12] = np.nan
+    f[20, 33] = -np.inf
+    c[19, 33] = 0.0        # w2 = 0 just below the inf level of column 33
+    x = np.zeros_like(a, order="F")
+    assert pkg.trsolv_ng(a, b, c, f, x, nk) == pkg.TG_ENONFINITE
+    ref = orc.trsolv_ng(a, b, c, f, nk)
+    assert np.array_equal(x, ref, equal_nan=True)
+    assert not np.isfinite(x[0, [7, 12, 33]]).any()
+    assert np.isfinite(np.delete(x, [7, 12, 33], axis=1)).all()
+
+
 def test_zero_pivot_status_and_values(cuda, pkg, orc):
     (a, b, c, f), nk = system(pkg, 0, 64)
     b = b.copy(order="F")

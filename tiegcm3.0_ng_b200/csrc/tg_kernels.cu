@@ -577,8 +577,9 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
         }
         q += nch;
         if (valid) {
+            // A non-finite x(k+1) makes x(k) = w3 - w2*x(k+1) non-finite (inf
+            // or NaN), down to x(0): x(0) finite <=> every x finite.
             double xn = w3;
-            fin = finite(xn);
             double rw[4], r2[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u)
@@ -586,13 +587,23 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
                     rw[u] = px[(k2 - 2 - u) * ld];
                     r2[u] = w2s[(k2 - 2 - u) * ws];
                 }
-            for (int kb = k2 - 2; kb >= 0; kb -= 4) {
+            int kb = k2 - 2;
+            for (; kb - 7 >= 0; kb -= 4) {   // four levels and their refills all in range
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = kb - u;
+                    xn = xsub(rw[u], xmul(r2[u], xn));
+                    rw[u] = px[(k - 4) * ld];
+                    r2[u] = w2s[(k - 4) * ws];
+                    px[k * ld] = xn;
+                }
+            }
+            for (; kb >= 0; kb -= 4) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int k = kb - u;
                     if (k >= 0) {
                         xn = xsub(rw[u], xmul(r2[u], xn));
-                        fin = fin && finite(xn);
                         if (k - 4 >= 0) {
                             rw[u] = px[(k - 4) * ld];
                             r2[u] = w2s[(k - 4) * ws];
@@ -601,6 +612,7 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
                     }
                 }
             }
+            fin = finite(xn);
             report(status, s.status_idx, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
         }
     }
