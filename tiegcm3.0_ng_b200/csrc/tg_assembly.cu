@@ -239,14 +239,7 @@ cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, i
     // per-thread shared memory (w2 column + staged reads)
     const int T = 32;
     const size_t smem = (size_t)T * ((nk - 2 > 0 ? nk - 2 : 1) * sizeof(double) + Stage<kDtStaged>::bytes_per_thread);
-    static bool attr = false;
-    if (!attr) {
-        int dev = 0, optin = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        cudaFuncSetAttribute(k_dt_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024);
-        attr = true;
-    }
+    once_per_device([] { cudaFuncSetAttribute(k_dt_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin() - 1024); });
     k_dt_ng<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, tn_upd, nk, ncol, ld, sys_out, status);
     return cudaGetLastError();
 }
@@ -668,14 +661,11 @@ cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *
                             double *sys_out, unsigned *status, cudaStream_t st, double *scratch)
 {
     if (ncol <= 0) return cudaSuccess;
-    static int optin = 0;
-    if (!optin) {
-        int dev = 0, v = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        cudaFuncSetAttribute(k_minor_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-        optin = v;
-    }
+    const int optin = smem_optin();
+    once_per_device([optin] {
+        cudaFuncSetAttribute(k_minor_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+        cudaFuncSetAttribute(k_minor_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    });
     // w2 of the forward sweep lives in shared memory, one column per thread:
     // shrink the block until the column fits (nk <= ~220 at 128 threads).
     int T = 128;
@@ -683,11 +673,6 @@ cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *
     const size_t smem = (size_t)T * (nk - 1 > 0 ? nk - 1 : 1) * sizeof(double);
     if (smem > (size_t)optin) return cudaErrorInvalidValue;
     if (scratch && assembly_mode() == 1) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_minor_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-            attr = true;
-        }
         // the row walk also holds its staged reads in shared memory
         const size_t per_r = (size_t)(nk - 1 > 0 ? nk - 1 : 1) * sizeof(double) + Stage<kMinorStaged>::bytes_per_thread;
         int TR = 128;

@@ -5,9 +5,33 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "tg_colsolve.h"
 
 namespace tg {
+
+// Kernel attributes (the dynamic shared-memory opt-in) belong to the device
+// context: runs f the first time it is reached with device d current, once
+// per device and call site, safe against concurrent first calls.
+template <class F>
+inline void once_per_device(F &&f)
+{
+    static std::mutex mu;
+    static bool done[64] = {};
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) {
+        f();
+        return;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done[d]) {
+        f();
+        done[d] = true;
+    }
+}
+// Opt-in shared memory per block of the current device (bytes).
+int smem_optin();
 
 // Per-segment status bits written by the kernels (atomicOr into a device word).
 enum : unsigned {

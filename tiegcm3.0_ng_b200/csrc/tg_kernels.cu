@@ -2190,9 +2190,10 @@ TileCfg g_tile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 2, 0, 8, 1, 0, 
                         {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 0, 0, 4, 4, 0, 32, 1}},
                         {{128, 1, 0, 0, 4, 4, 0, 32, 1}, {128, 1, 0, 0, 4, 4, 0, 32, 1}}};
 int kind_index(int kind) { return kind == TG_KIND_SCALAR ? 0 : (kind == TG_KIND_BLOCK2 ? 1 : 2); }
-int g_num_sms = -1;
+constexpr int kMaxDevIdx = 64;
+int g_num_sms[kMaxDevIdx] = {};
 int g_carveout = cudaSharedmemCarveoutMaxShared;   // percent of the unified L1/shared store
-int g_smem_optin = -1;
+int g_smem_optin[kMaxDevIdx] = {};
 
 // Register-prefetch scalar kernels by (columns per thread, prefetch depth).
 template <typename F>
@@ -2310,16 +2311,22 @@ void allow_smem(K k, int lim)
     cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, g_carveout);
 }
 
-int num_sms()
+// SM count and opt-in shared memory per device; the first call on a device
+// also lets every kernel that takes dynamic shared memory use up to the
+// opt-in limit (minus its static shared memory).
+int device_index()
 {
-    if (g_num_sms < 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        // every kernel that takes dynamic shared memory may use up to the
-        // opt-in limit (minus its static shared memory)
-        const int lim = g_smem_optin - 1024;
+    int d = 0;
+    cudaGetDevice(&d);
+    return d >= 0 && d < kMaxDevIdx ? d : 0;
+}
+void device_init()
+{
+    once_per_device([] {
+        const int d = device_index();
+        cudaDeviceGetAttribute(&g_num_sms[d], cudaDevAttrMultiProcessorCount, d);
+        cudaDeviceGetAttribute(&g_smem_optin[d], cudaDevAttrMaxSharedMemoryPerBlockOptin, d);
+        const int lim = g_smem_optin[d] - 1024;
         for (int pf : {4, 8, 16}) {
             with_scalar_reg(1, pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
             with_scalar_reg(2, pf, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
@@ -2336,9 +2343,20 @@ int num_sms()
                     with_block_ring(b, d, w, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int d : {4, 8})
             for (int b : {2, 3}) with_block_rows(b, d, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
-    }
-    return g_num_sms;
+    });
 }
+int num_sms()
+{
+    device_init();
+    return g_num_sms[device_index()];
+}
+}  // namespace
+int smem_optin()
+{
+    device_init();
+    return g_smem_optin[device_index()];
+}
+namespace {
 
 // Occupancy queries are cached per (kernel, threads, shared memory): the host
 // drop-ins shape one launch per column chunk, and the query is host time on
@@ -2527,7 +2545,7 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         // register-prefetch kernel with the same 32-column tile
         const size_t need = kind == TG_KIND_SCALAR ? scalar_smem_bytes(precision, sh->threads, 1, k2max, stages, w2g, sh->lps)
                                                    : block_smem_bytes(kind, stages, sh->threads, sh->rows, sh->bw);
-        if (need > (size_t)(g_smem_optin - 1024)) {
+        if (need > (size_t)(smem_optin() - 1024)) {
             stages = 0;
             sh->stages = 0;
             sh->threads = 32;
@@ -2539,7 +2557,7 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     }
     if (kind == TG_KIND_SCALAR) {
         sh->smem = scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max, stages, w2g, sh->lps);
-        if (sh->smem > (size_t)(g_smem_optin - 1024)) return cudaErrorInvalidConfiguration;
+        if (sh->smem > (size_t)(smem_optin() - 1024)) return cudaErrorInvalidConfiguration;
         auto occ = [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); };
         if (stages > 0 && precision != TG_PREC_F64)
             e = with_scalar_refine_ring(stages, occ);
@@ -2556,7 +2574,7 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     } else {
         const int B = kind;
         sh->smem = block_smem_bytes(B, stages, sh->threads, sh->rows, sh->bw);
-        if (sh->smem > (size_t)(g_smem_optin - 1024)) return cudaErrorInvalidConfiguration;
+        if (sh->smem > (size_t)(smem_optin() - 1024)) return cudaErrorInvalidConfiguration;
         if (stages > 0 && sh->rows)
             e = with_block_rows(B, stages, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
         else if (stages > 0)

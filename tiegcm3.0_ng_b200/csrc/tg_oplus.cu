@@ -292,24 +292,16 @@ cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *
 {
     if (ncol <= 0) return cudaSuccess;
     if (nk < 3) return cudaErrorInvalidValue;
-    static int optin = 0;
-    if (!optin) {
-        int dev = 0, v = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        cudaFuncSetAttribute(k_oplus_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-        optin = v;
-    }
+    const int optin = smem_optin();
+    once_per_device([optin] {
+        cudaFuncSetAttribute(k_oplus_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+        cudaFuncSetAttribute(k_oplus_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    });
     int T = 128;
     const size_t per = (size_t)(nk - 1) * sizeof(double);
     while (T > 32 && (size_t)T * per > (size_t)optin) T /= 2;
     if ((size_t)T * per > (size_t)optin) return cudaErrorInvalidValue;
     if (assembly_mode() == 1) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_oplus_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-            attr = true;
-        }
         k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, xiop2p, xiop2d, Fe, Fn, scratch, nk, ncol,
                                                                      ld);
         k_oplus_rows<<<(ncol + T - 1) / T, T, (size_t)T * per, st>>>(F, C, opout, scratch, nk, ncol, ld, sys_out,

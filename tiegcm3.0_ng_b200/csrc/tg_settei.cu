@@ -599,25 +599,17 @@ cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, doubl
 {
     if (ncol <= 0) return cudaSuccess;
     if (nk < 3) return cudaErrorInvalidValue;
-    static int optin = 0;
-    if (!optin) {
-        int dev = 0, v = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        cudaFuncSetAttribute(k_settei_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-        optin = v;
-    }
+    const int optin = smem_optin();
+    once_per_device([optin] {
+        cudaFuncSetAttribute(k_settei_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+        cudaFuncSetAttribute(k_settei_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    });
     // w2 (nk-1) and loss_in (nk) per column in shared memory
     int T = 128;
     const size_t per = (size_t)(2 * nk - 1) * sizeof(double);
     while (T > 32 && (size_t)T * per > (size_t)optin) T /= 2;
     if ((size_t)T * per > (size_t)optin) return cudaErrorInvalidValue;
     if (scratch && assembly_mode() == 1) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_settei_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-            attr = true;
-        }
         int T2 = 128;
         const size_t per2 = (size_t)(nk - 1) * sizeof(double) + Stage<kSetteiStaged>::bytes_per_thread;
         while (T2 > 32 && (size_t)T2 * per2 > (size_t)optin) T2 /= 2;
