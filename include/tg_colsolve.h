@@ -385,8 +385,15 @@ int tg_plan_destroy(tg_plan *plan);
 
 /* ---- tuning, configuration, housekeeping ------------------------------------ */
 
-/* Mixed-precision refinement: at most max_sweeps FP64 residual sweeps per
- * column, stopping when max|dx| <= rel_tol * max|x| (defaults 3 and 1e-12). */
+/* Tuning entries (tg_set_*) change process-wide settings that plans and
+ * calls read when they are created or launched: set them before other threads
+ * create plans or call the solvers.
+ *
+ * Mixed-precision refinement: at most max_sweeps FP64 residual sweeps per
+ * column (defaults 3 and 1e-11).  A column stops when its correction, or the
+ * error left after it as estimated from the contraction of successive
+ * corrections (the FP32 sweep-0 solution counting as the first, with a
+ * 16-fold margin), is below rel_tol * max|x|. */
 int tg_set_refine(int max_sweeps, double rel_tol);
 /* Precision of the host-pointer drop-ins (tg_trsolv, tg_trsolv_ng, tg_blktri,
  * tg_comp_blksolve_ng, tg_blksolve), which keep the reference's signatures
