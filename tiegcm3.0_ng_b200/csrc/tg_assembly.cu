@@ -314,14 +314,26 @@ __device__ __forceinline__ MinorIface minor_iface(const MinorConsts &C, double o
     return r;
 }
 
+// The diffusion powers of a level from one logarithm: (tni/t00)**(1.75-ss)
+// of the three species and (t00/tni)**0.25, as exp(y*ln(tni/t00)).  With
+// |y*ln(tni/t00)| below 1 the argument's rounding adds about 2 ulp to exp's
+// own error, within the tolerance the device pow already needs against the
+// host library (the reference writes these as ** powers).
+__device__ __forceinline__ void diffusion_powers(double tni, double (&df)[3], double &p25)
+{
+    const double lx = log(xd(tni, 273.0));
+#pragma unroll
+    for (int n = 0; n < 3; ++n) df[n] = exp(xm(xs(1.75, kMSs[n]), lx));
+    p25 = exp(xm(-0.25, lx));
+}
+
 // ax, thdiff, dmdz/barm of level j (minor_ng.F90:100-153).
 __device__ __forceinline__ MinorLevel minor_level(const MinorConsts &C, const MinorIface &I, double barm, double tni,
                                                   double dtnidz)
 {
-    const double t00 = 273.0, tau = 1.86e+3;
-    double df[3];
-#pragma unroll
-    for (int n = 0; n < 3; ++n) df[n] = pow(xd(tni, t00), xs(1.75, kMSs[n]));
+    const double tau = 1.86e+3;
+    double df[3], p25;
+    diffusion_powers(tni, df, p25);
 #define PH(i, j) kMPhi[(i) - 1][(j) - 1]
     double A[9], W[9];
     A[0] = -xa(xa(PH(1, 4), xm(xs(PH(1, 2), PH(1, 4)), I.pso1)), xm(xs(xm(df[0], PH(1, 3)), PH(1, 4)), I.pshe));
@@ -348,7 +360,7 @@ __device__ __forceinline__ MinorLevel minor_level(const MinorConsts &C, const Mi
     MinorLevel L;
     L.dmdzs = xd(I.dmdz, barm);
     const double den = xa(xa(xa(C.phix[2], xm(s0, I.pso2)), xm(s1, I.pso1)), xm(s2, I.pshe));
-    L.ax = -xd(xm(xd(barm, xm(tau, C.rmass_n2)), pow(xd(t00, tni), 0.25)), den);
+    L.ax = -xd(xm(xd(barm, xm(tau, C.rmass_n2)), p25), den);
     L.thdiff = xs(ex, xd(xm(C.alfax, dtnidz), xm(C.dzp, tni)));
     return L;
 }
@@ -708,10 +720,9 @@ struct CompLevel {
 __device__ __forceinline__ void comp_level(const CompConsts &C, double o2i, double o1i, double hei, double embari,
                                            double tni, double dembardz, double dtndz, bool thermal, CompLevel &L)
 {
-    const double tau = 1.86e+3, thdiffalpha = -0.38, t00 = 273.;
-    double df[3];
-#pragma unroll
-    for (int n = 0; n < 3; ++n) df[n] = pow(xd(tni, t00), xs(1.75, kMSs[n]));
+    const double tau = 1.86e+3, thdiffalpha = -0.38;
+    double df[3], p25;
+    diffusion_powers(tni, df, p25);
     const double rinv = xd(1.0, embari);
     L.ep[0] = xs(1.0, xm(rinv, xa(C.rmass_o2, dembardz)));
     L.ep[1] = xs(1.0, xm(rinv, xa(C.rmass_o1, dembardz)));
@@ -735,7 +746,7 @@ __device__ __forceinline__ void comp_level(const CompConsts &C, double o2i, doub
     L.a23 = A[7];
     L.a32 = A[5];
     inv3_ieee(A, W);
-    const double wks1 = xd(xm(xm(embari, C.rmassinv_n2), pow(xd(t00, tni), 0.25)), tau);
+    const double wks1 = xd(xm(xm(embari, C.rmassinv_n2), p25), tau);
 #pragma unroll
     for (int e = 0; e < 9; ++e) L.ak[e] = xm(W[e], wks1);
     L.wks4 = xd(dembardz, xm(embari, 2.0));
