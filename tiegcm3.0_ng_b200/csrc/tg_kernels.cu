@@ -1742,7 +1742,7 @@ __global__ void __launch_bounds__(256) k_block_f64_rows(SegTable tab, double *sc
 // ---------------------------------------------------------------------------
 template <int B>
 __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float *scr, long gs,
-                                                   Refine rf, int &sweeps)
+                                                   Refine rf, int &sweeps, unsigned long long keep)
 {
     constexpr int BB = B * B, NS = 2 * BB + B;
     const long ld = s.ld;
@@ -1783,7 +1783,7 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
 #pragma unroll
             for (int e = 0; e < BB; ++e) {
                 W32[e] = (float)W[e];
-                S(k, e) = W32[e];
+                st_hint_f(&S(k, e), W32[e], keep);
             }
 #pragma unroll
             for (int i = 0; i < B; ++i) {
@@ -1799,7 +1799,7 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
 #pragma unroll
                 for (int m = 0; m < B; ++m) t = fmaf(W32[i + B * m], v[m], t);
                 z[i] = t;
-                S(k, 2 * BB + i) = t;
+                st_hint_f(&S(k, 2 * BB + i), t, keep);
             }
 #pragma unroll
             for (int m = 0; m < B; ++m)
@@ -1810,7 +1810,7 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
 #pragma unroll
                         for (int n = 0; n < B; ++n) g = fmaf(W32[i + B * n], (float)R[n + B * m], g);
                     G[i + B * m] = g;
-                    S(k, BB + i + B * m) = g;
+                    st_hint_f(&S(k, BB + i + B * m), g, keep);
                 }
         }
         float un[B], xm = 0.f;
@@ -1818,7 +1818,7 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
         for (int i = 0; i < B; ++i) {
             un[i] = z[i];
             xm = fmaxf(xm, fabsf(z[i]));
-            pU[((long)(k2 - 1) * B + i) * ld] = (double)z[i];
+            st_hint(&pU[((long)(k2 - 1) * B + i) * ld], (double)z[i], keep);
         }
         for (int k = k2 - 2; k >= 0; --k) {
             float nu[B];
@@ -1833,7 +1833,7 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
             for (int i = 0; i < B; ++i) {
                 un[i] = nu[i];
                 xm = fmaxf(xm, fabsf(nu[i]));
-                pU[((long)k * B + i) * ld] = (double)nu[i];
+                st_hint(&pU[((long)k * B + i) * ld], (double)nu[i], keep);
             }
         }
         xmax0 = (double)xm;
@@ -1889,7 +1889,7 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
 #pragma unroll
                     for (int m = 0; m < B; ++m) t = fmaf(S(k, i + B * m), v[m], t);
                     zc[i] = t;
-                    S(k, 2 * BB + i) = t;
+                    st_hint_f(&S(k, 2 * BB + i), t, keep);
                 }
 #pragma unroll
                 for (int i = 0; i < B; ++i) {
@@ -2041,12 +2041,14 @@ __global__ void __launch_bounds__(128) k_block_refine(SegTable tab, Refine rf, f
     __syncthreads();
     const long gs = (long)gridDim.x * blockDim.x;
     float *scr = scratch + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    // the FP32 planes and u are re-read by the next sweep: keep them in L2
+    const unsigned long long keep = l2_policy(tab.hints, true);
     for (int t = blockIdx.x; t < tab.ntiles; t += gridDim.x) {
         const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
         const long col = (long)(t - s.tile0) * blockDim.x + threadIdx.x;
         if (col < s.ncol) {
             int sweeps = 0;
-            report(status, s.status_idx, blk_refine_col<B>(s, col, scr, gs, rf, sweeps));
+            report(status, s.status_idx, blk_refine_col<B>(s, col, scr, gs, rf, sweeps, keep));
             atomicAdd(&shist[min(sweeps, kMaxSweepBins - 1)], 1ull);
         }
     }
@@ -2691,10 +2693,12 @@ cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape 
             k_block_f64<3><<<sh.blocks, sh.threads, 0, st>>>(tab, scratch, status);
     } else {
         float *fs = reinterpret_cast<float *>(scratch);
+        SegTable t = tab;
+        t.hints = cache_hints();
         if (B == 2)
-            k_block_refine<2><<<sh.blocks, sh.threads, 0, st>>>(tab, rf, fs, status, hist);
+            k_block_refine<2><<<sh.blocks, sh.threads, 0, st>>>(t, rf, fs, status, hist);
         else
-            k_block_refine<3><<<sh.blocks, sh.threads, 0, st>>>(tab, rf, fs, status, hist);
+            k_block_refine<3><<<sh.blocks, sh.threads, 0, st>>>(t, rf, fs, status, hist);
     }
     return cudaGetLastError();
 }
