@@ -450,9 +450,10 @@ int tg_set_stage_levels(int kind, int precision, int levels);
  * fused column walk.  Same operations, same results. */
 int tg_set_assembly_mode(int mode);
 
-/* Block kinds: the L2 budget for the Gamma scratch of all resident warps of
- * the block kernels, in MB (default 96; <= 0 restores it).  It caps how many
- * columns are in flight at once on large batches. */
+/* Block kinds, FP64: the L2 budget for the Gamma scratch of all resident
+ * warps of the block kernels, in MB (default 96; <= 0 restores it).  It caps
+ * how many columns are in flight at once on large batches (the refinement
+ * kernel is not capped). */
 int tg_set_block_scratch_budget(double megabytes);
 
 /* Scalar kind, FP64 ring kernels: the L2 budget for the w2 scratch and the
