@@ -80,5 +80,5 @@ def test_tuning_entries_validate_without_device(pkg):
     assert L.tg_set_kind_overlap(-1) == pkg.TG_OK
     assert L.tg_set_scalar_scratch_budget(0.0) == pkg.TG_OK
     assert L.tg_set_pipeline(pkg.TG_KIND_SCALAR, pkg.TG_PREC_F32_REFINE, 8, 1) == pkg.TG_EINVAL
-    assert L.tg_set_pipeline(pkg.TG_KIND_BLOCK2, pkg.TG_PREC_F32_REFINE, 4, 1) == pkg.TG_EINVAL
+    assert L.tg_set_pipeline(pkg.TG_KIND_BLOCK2, pkg.TG_PREC_F32_REFINE, 3, 1) == pkg.TG_EINVAL
     assert L.tg_set_pipeline(pkg.TG_KIND_SCALAR, pkg.TG_PREC_F32_REFINE, -1, 0) == pkg.TG_OK

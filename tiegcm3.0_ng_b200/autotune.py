@@ -40,7 +40,8 @@ BLOCK_F64 = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 9
              ("ring8", 8, 1, 4), ("ring8", 4, 2, 4), ("rows", 4, 1, 4), ("rows", 4, 2, 4), ("rows", 8, 1, 4)]
 SCALAR_REF = [("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg", 64, 1, 8),
               ("ring", 2, 1, 4), ("ring", 3, 1, 4), ("ring", 4, 1, 4), ("ring", 2, 2, 4)]
-BLOCK_REF = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4)]
+BLOCK_REF = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("ring", 4, 1, 4), ("ring", 8, 1, 4),
+             ("ring", 4, 2, 4)]
 
 
 def candidates(kind, precision):

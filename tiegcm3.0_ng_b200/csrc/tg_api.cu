@@ -421,8 +421,11 @@ __attribute__((visibility("default"))) int tg_set_pipeline(int kind, int precisi
 {
     if ((kind != TG_KIND_SCALAR && kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) || bad_prec(precision) ||
         (stages != -1 && stages != 0 && stages != 2 && stages != 3 && stages != 4 && stages != 8 && stages != 16) ||
-        (stages > 0 && precision != TG_PREC_F64 && (kind != TG_KIND_SCALAR || stages > 4)) || warps < 0 || warps > 8) {
-        set_err("tg_set_pipeline: stages must be 0, 2, 3, 4, 8 or 16 (FP64; scalar refinement 2..4) or -1; warps 0..8");
+        (stages > 0 && precision != TG_PREC_F64 &&
+         !(kind == TG_KIND_SCALAR && stages <= 4) && !(kind == TG_KIND_BLOCK2 && (stages == 4 || stages == 8))) ||
+        warps < 0 || warps > 8) {
+        set_err("tg_set_pipeline: stages must be 0, 2, 3, 4, 8 or 16 (FP64; refinement: scalar 2..4, 2x2 4 or 8) or -1; "
+                "warps 0..8");
         return TG_EINVAL;
     }
     set_stages(kind, precision, stages, warps);
@@ -1558,7 +1561,8 @@ __attribute__((visibility("default"))) int tg_plan_describe(const tg_plan *p, ch
             else if (h.w2g) snprintf(name, sizeof name, "k_scalar_f64_g<%d>", h.pf);
             else snprintf(name, sizeof name, "k_scalar_f64<%d,%d>", h.cpt, h.pf);
         } else {
-            if (!f64) snprintf(name, sizeof name, "k_block_refine<%d>", g.kind);
+            if (!f64 && h.stages) snprintf(name, sizeof name, "k_block_refine_ring<%d,%d>", g.kind, h.stages);
+            else if (!f64) snprintf(name, sizeof name, "k_block_refine<%d>", g.kind);
             else if (h.stages && h.rows) snprintf(name, sizeof name, "k_block_f64_rows<%d,%d>", g.kind, h.stages);
             else if (h.stages) snprintf(name, sizeof name, "k_block_f64_ring<%d,%d,%d>", g.kind, h.stages, h.bw);
             else snprintf(name, sizeof name, "k_block_f64<%d>", g.kind);

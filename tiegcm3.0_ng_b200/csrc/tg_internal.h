@@ -115,7 +115,7 @@ size_t refine_scratch_bytes(long slots, int k2max);
 
 // Shared memory / scratch needs of a kernel for the largest k2 it will see.
 size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int stages, int w2g, int lps);
-size_t block_smem_bytes(int B, int stages, int threads, int rows, int bw);
+size_t block_smem_bytes(int B, int stages, int threads, int rows, int bw, int precision);
 // Global scratch (bytes) of a block kernel with `slots` resident threads.
 size_t block_scratch_bytes(int B, int precision, long slots, int k2max);
 

@@ -2032,6 +2032,403 @@ __device__ __forceinline__ unsigned blk_refine_col(const Seg &s, long col, float
     return flags;
 }
 
+// ---------------------------------------------------------------------------
+// Block-tridiagonal FP32 sweeps + FP64 refinement with the coefficients
+// staged by the bulk-copy ring: one warp per 32 columns, a D-level ring of
+// the 3*B*B + B coefficient rows per level (and, in the correction sweeps,
+// the B rows of u one level above), one 256-byte copy per row.  Same
+// arithmetic, planes, stopping rule, fallback and flags as blk_refine_col;
+// the FP32 planes W | G | z of level k sit at (k*NS + e)*gs of the lane's
+// scratch slot.  u rows written by this warp's generic stores are read back
+// by bulk copies: a proxy fence orders the two before each correction sweep.
+// Requires ld % 32 == 0 and 16-byte aligned P, Q, R, f, u.
+// ---------------------------------------------------------------------------
+template <int B, int D>
+__global__ void __launch_bounds__(256) k_block_refine_ring(SegTable tab, Refine rf, float *scratch, unsigned *status,
+                                                           unsigned long long *hist)
+{
+    constexpr int BB = B * B, NE = 3 * BB + B, NX = NE + B, NS = 2 * BB + B;
+    static_assert(NX <= 32, "one copy per lane");
+    __shared__ __align__(8) unsigned long long bars[8 * D];
+    extern __shared__ __align__(128) double smem_b[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    double *buf = smem_b + (long)warp * D * NX * 32;
+    unsigned long long *bar = bars + warp * D;
+    const unsigned long long pol = l2_policy(tab.hints, false), keep = l2_policy(tab.hints, true);
+    const long gs = (long)gridDim.x * blockDim.x;
+    float *scr = scratch + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    auto S = [&](int k, int e) -> float & { return scr[((long)k * NS + e) * gs]; };
+    if (lane == 0) {
+#pragma unroll 1
+        for (int i = 0; i < D; ++i) mbar_init(&bar[i], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    unsigned long long hl[kMaxSweepBins];
+#pragma unroll
+    for (int i = 0; i < kMaxSweepBins; ++i) hl[i] = 0ull;
+    unsigned q = 0;
+    for (int t = blockIdx.x * nwarps + warp; t < tab.ntiles; t += gridDim.x * nwarps) {
+        const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
+        const long col0 = (long)(t - s.tile0) * 32;
+        const long ld = s.ld;
+        const int k2 = s.k2;
+        const bool valid = col0 + lane < s.ncol;
+        // row e of level k: P/Q/R element e at (k*BB + e)*ld, f and u
+        // component i at (k*B + i)*ld; lanes NE.. copy u of level k+1
+        const double *src = s.a + col0;
+        long lstride = 0;
+        if (lane < BB) {
+            src = s.a + col0 + lane * ld;
+            lstride = BB * ld;
+        } else if (lane < 2 * BB) {
+            src = s.b + col0 + (lane - BB) * ld;
+            lstride = BB * ld;
+        } else if (lane < 3 * BB) {
+            src = s.c + col0 + (lane - 2 * BB) * ld;
+            lstride = BB * ld;
+        } else if (lane < NE) {
+            src = s.f + col0 + (lane - 3 * BB) * ld;
+            lstride = B * ld;
+        } else if (lane < NX) {
+            src = s.x + col0 + (lane - NE + B) * ld;
+            lstride = B * ld;
+        }
+        double *pU = s.x + col0 + lane;
+        auto issue = [&](unsigned qk, int k, bool withu) {
+            const int st = (int)(qk % D);
+            const bool u = withu && k + 1 < k2;
+            if (lane == 0) mbar_expect(&bar[st], (uint32_t)(NE + (u ? B : 0)) * 256u);
+            __syncwarp();
+            if (lane < NE || (u && lane < NX))
+                bulk_load_hint(buf + (st * NX + lane) * 32, src + (long)k * lstride, 256u, &bar[st], pol);
+        };
+        auto wait = [&](unsigned q0, int k) -> bool {
+            const unsigned qk = q0 + k;
+            if (mbar_wait_warp(&bar[qk % D], (qk / D) & 1u)) return true;
+            const unsigned qe = q0 + (k + D < k2 ? k + D : k2);
+#pragma unroll 1
+            for (unsigned r = qk; r < qe; ++r) mbar_wait_warp(&bar[r % D], (r / D) & 1u);
+            if (lane == 0) report(status, s.status_idx, FLAG_TIMEOUT);
+            return false;
+        };
+        auto at = [&](unsigned qk, int e) { return buf[((int)(qk % D) * NX + e) * 32 + lane]; };
+
+        // ---- sweep 0: FP64 pivots and inverses, FP32 planes and sweeps
+        bool ok = true;
+        float xm = 0.f;
+        {
+            const int pre = k2 < D ? k2 : D;
+            for (int j = 0; j < pre; ++j) issue(q + j, j, false);
+            float G[BB], z[B];
+#pragma unroll
+            for (int e = 0; e < BB; ++e) G[e] = 0.f;
+#pragma unroll
+            for (int i = 0; i < B; ++i) z[i] = 0.f;
+            for (int k = 0; k < k2; ++k) {
+                const unsigned qk = q + k;
+                if (!wait(q, k)) return;
+                double P[BB], Q[BB], R[BB], F[B];
+#pragma unroll
+                for (int e = 0; e < BB; ++e) {
+                    P[e] = k > 0 ? at(qk, e) : 0.0;
+                    Q[e] = at(qk, BB + e);
+                    R[e] = k < k2 - 1 ? at(qk, 2 * BB + e) : 0.0;
+                }
+#pragma unroll
+                for (int i = 0; i < B; ++i) F[i] = at(qk, 3 * BB + i);
+                __syncwarp();
+                fence_proxy_async();
+                if (k + D < k2) issue(qk + D, k + D, false);
+                if (!valid) continue;
+                double Qp[BB], W[BB];
+#pragma unroll
+                for (int m = 0; m < B; ++m)
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        double qv = Q[i + B * m];
+                        if (k > 0)
+#pragma unroll
+                            for (int n = 0; n < B; ++n) qv = fma(-P[i + B * n], (double)G[n + B * m], qv);
+                        Qp[i + B * m] = qv;
+                    }
+                ok = inv_exact<B>(Qp, W) && ok;
+                float W32[BB], v[B];
+#pragma unroll
+                for (int e = 0; e < BB; ++e) {
+                    W32[e] = (float)W[e];
+                    st_hint_f(&S(k, e), W32[e], keep);
+                }
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    float tv = (float)F[i];
+                    if (k > 0)
+#pragma unroll
+                        for (int m = 0; m < B; ++m) tv = fmaf(-(float)P[i + B * m], z[m], tv);
+                    v[i] = tv;
+                }
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    float tv = 0.f;
+#pragma unroll
+                    for (int m = 0; m < B; ++m) tv = fmaf(W32[i + B * m], v[m], tv);
+                    z[i] = tv;
+                    st_hint_f(&S(k, 2 * BB + i), tv, keep);
+                }
+#pragma unroll
+                for (int m = 0; m < B; ++m)
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        float g = 0.f;
+                        if (k < k2 - 1)
+#pragma unroll
+                            for (int n = 0; n < B; ++n) g = fmaf(W32[i + B * n], (float)R[n + B * m], g);
+                        G[i + B * m] = g;
+                        st_hint_f(&S(k, BB + i + B * m), g, keep);
+                    }
+            }
+            q += k2;
+            if (valid) {
+                float un[B];
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    un[i] = z[i];
+                    xm = fmaxf(xm, fabsf(z[i]));
+                    st_hint(&pU[((long)(k2 - 1) * B + i) * ld], (double)z[i], keep);
+                }
+                for (int k = k2 - 2; k >= 0; --k) {
+                    float nu[B];
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        float tv = S(k, 2 * BB + i);
+#pragma unroll
+                        for (int m = 0; m < B; ++m) tv = fmaf(-S(k, BB + i + B * m), un[m], tv);
+                        nu[i] = tv;
+                    }
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        un[i] = nu[i];
+                        xm = fmaxf(xm, fabsf(nu[i]));
+                        st_hint(&pU[((long)k * B + i) * ld], (double)nu[i], keep);
+                    }
+                }
+            }
+        }
+
+        // ---- correction sweeps (the warp streams while any lane is active)
+        bool active = valid && ok, conv = false;
+        int sw = 0, taken = rf.max_sweeps + 1;
+        double dprev = (double)xm;
+        for (sw = 1; sw <= rf.max_sweeps && __any_sync(0xffffffffu, active); ++sw) {
+            fence_proxy_async_global();
+            __syncwarp();
+            const int pre = k2 < D ? k2 : D;
+            for (int j = 0; j < pre; ++j) issue(q + j, j, true);
+            double um[B], u0[B];
+            float zc[B];
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                um[i] = 0.0;
+                u0[i] = active ? pU[i * ld] : 0.0;
+                zc[i] = 0.f;
+            }
+            for (int k = 0; k < k2; ++k) {
+                const unsigned qk = q + k;
+                if (!wait(q, k)) return;
+                double up[B], r[B];
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    up[i] = k + 1 < k2 ? at(qk, NE + i) : 0.0;
+                    r[i] = at(qk, 3 * BB + i);
+                }
+                float P32[BB];
+#pragma unroll
+                for (int e = 0; e < BB; ++e) {
+                    const int i = e % B, m = e / B;
+                    r[i] = fma(-at(qk, BB + e), u0[m], r[i]);
+                    double p = 0.0;
+                    if (k > 0) {
+                        p = at(qk, e);
+                        r[i] = fma(-p, um[m], r[i]);
+                    }
+                    P32[e] = (float)p;
+                    if (k + 1 < k2) r[i] = fma(-at(qk, 2 * BB + e), up[m], r[i]);
+                }
+                __syncwarp();
+                fence_proxy_async();
+                if (k + D < k2) issue(qk + D, k + D, true);
+                if (active) {
+                    float v[B];
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        float tv = (float)r[i];
+#pragma unroll
+                        for (int m = 0; m < B; ++m) tv = fmaf(-P32[i + B * m], zc[m], tv);
+                        v[i] = tv;
+                    }
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        float tv = 0.f;
+#pragma unroll
+                        for (int m = 0; m < B; ++m) tv = fmaf(S(k, i + B * m), v[m], tv);
+                        zc[i] = tv;
+                        st_hint_f(&S(k, 2 * BB + i), tv, keep);
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    um[i] = u0[i];
+                    u0[i] = up[i];
+                }
+            }
+            q += k2;
+            if (active) {
+                double dmax = 0.0, xmax = 0.0;
+                float dn[B];
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    dn[i] = zc[i];
+                    const double xv = um[i] + (double)dn[i];   // um holds u(k2-1)
+                    st_hint(&pU[((long)(k2 - 1) * B + i) * ld], xv, keep);
+                    dmax = fmax(dmax, fabs((double)dn[i]));
+                    xmax = fmax(xmax, fabs(xv));
+                }
+                for (int k = k2 - 2; k >= 0; --k) {
+                    float nd[B];
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        float tv = S(k, 2 * BB + i);
+#pragma unroll
+                        for (int m = 0; m < B; ++m) tv = fmaf(-S(k, BB + i + B * m), dn[m], tv);
+                        nd[i] = tv;
+                    }
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        dn[i] = nd[i];
+                        double *p = pU + ((long)k * B + i) * ld;
+                        const double xv = *p + (double)nd[i];
+                        st_hint(p, xv, keep);
+                        dmax = fmax(dmax, fabs((double)nd[i]));
+                        xmax = fmax(xmax, fabs(xv));
+                    }
+                }
+                if (!(xmax <= DBL_MAX) || !(dmax <= DBL_MAX)) {
+                    active = false;
+                } else if (refine_done(dmax, xmax, dprev, rf.rel_tol, sw == 1)) {
+                    conv = true;
+                    active = false;
+                    taken = sw;
+                } else {
+                    dprev = dmax;
+                }
+            }
+        }
+        unsigned flags = 0u;
+        if (valid && !conv) {
+            // ---- fallback: bit-exact FP64 solve, G kept as (hi, lo) float pairs
+            const double *pP = s.a + col0 + lane, *pQ = s.b + col0 + lane, *pR = s.c + col0 + lane,
+                         *pF = s.f + col0 + lane;
+            flags |= FLAG_NOCONV;
+            bool okd = true, fin = true;
+            double G[BB], z[B];
+            for (int k = 0; k < k2; ++k) {
+                double P[BB], Q[BB], R[BB], F[B];
+                blk_load<B>(pP, pQ, pR, pF, ld, k, k > 0, k < k2 - 1, P, Q, R, F);
+                double Qp[BB], W[BB], v[B];
+#pragma unroll
+                for (int m = 0; m < B; ++m)
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        double qv = Q[i + B * m];
+                        if (k > 0)
+#pragma unroll
+                            for (int n = 0; n < B; ++n) qv = xsub(qv, xmul(P[i + B * n], G[n + B * m]));
+                        Qp[i + B * m] = qv;
+                    }
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    double tv = F[i];
+                    if (k > 0)
+#pragma unroll
+                        for (int m = 0; m < B; ++m) tv = xsub(tv, xmul(P[i + B * m], z[m]));
+                    v[i] = tv;
+                }
+                okd = inv_exact<B>(Qp, W) && okd;
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    double tv = xmul(W[i], v[0]);
+#pragma unroll
+                    for (int m = 1; m < B; ++m) tv = xadd(tv, xmul(W[i + B * m], v[m]));
+                    z[i] = tv;
+                    pU[((long)k * B + i) * ld] = tv;
+                }
+                if (k < k2 - 1) {
+#pragma unroll
+                    for (int m = 0; m < B; ++m)
+#pragma unroll
+                        for (int i = 0; i < B; ++i) {
+                            double g = xmul(W[i], R[B * m]);
+#pragma unroll
+                            for (int n = 1; n < B; ++n) g = xadd(g, xmul(W[i + B * n], R[n + B * m]));
+                            G[i + B * m] = g;
+                            S(k, 2 * (i + B * m)) = __int_as_float(__double2hiint(g));
+                            S(k, 2 * (i + B * m) + 1) = __int_as_float(__double2loint(g));
+                        }
+                }
+            }
+            double un[B];
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                un[i] = z[i];
+                fin = fin && finite(z[i]);
+            }
+            for (int k = k2 - 2; k >= 0; --k) {
+                double nu[B];
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    double tv = pU[((long)k * B + i) * ld];
+#pragma unroll
+                    for (int m = 0; m < B; ++m) {
+                        const int e = i + B * m;
+                        const double g = __hiloint2double(__float_as_int(S(k, 2 * e)), __float_as_int(S(k, 2 * e + 1)));
+                        tv = xsub(tv, xmul(g, un[m]));
+                    }
+                    nu[i] = tv;
+                    fin = fin && finite(tv);
+                }
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    un[i] = nu[i];
+                    pU[((long)k * B + i) * ld] = nu[i];
+                }
+            }
+            flags |= (okd ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE);
+        } else if (valid && !ok) {
+            flags |= FLAG_PIVOT;
+        }
+        if (valid && s.ubc_ratio) {
+            bool fin = true;
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                const double top = pU[((long)(k2 - 1) * B + i) * ld];
+                double tv = xmul(__ldg(s.ubc_ratio + i * ld + col0 + lane), top);
+                if (s.ubc_add) tv = xadd(tv, __ldg(s.ubc_add + i * ld + col0 + lane));
+                fin = fin && finite(tv);
+                pU[((long)k2 * B + i) * ld] = tv;
+            }
+            if (!fin) flags |= FLAG_NONFINITE;
+        }
+        if (valid) report(status, s.status_idx, flags);
+        const int bin = taken < kMaxSweepBins - 1 ? taken : kMaxSweepBins - 1;
+#pragma unroll
+        for (int i = 0; i < kMaxSweepBins; ++i) hl[i] += __popc(__ballot_sync(0xffffffffu, valid && bin == i));
+    }
+    if (hist && lane == 0)
+#pragma unroll
+        for (int i = 0; i < kMaxSweepBins; ++i)
+            if (hl[i]) atomicAdd(hist + i, hl[i]);
+}
+
 template <int B>
 __global__ void __launch_bounds__(128) k_block_refine(SegTable tab, Refine rf, float *scratch,
                                                       unsigned *status, unsigned long long *hist)
@@ -2183,13 +2580,14 @@ struct TileCfg {
 // column step, 10368 x 57, and of the nested 2.5 deg + 3-nest batch): scalar
 // FP64 chunked bulk-copy ring of 2 stages x 4 levels, one warp per CTA, w2 in
 // global scratch; 2x2 block ring of depth 4, one warp per CTA; 3x3 block
-// register kernel of 128 threads; scalar refinement ring of 2 stages, one
-// warp per CTA; block refinement kernels of 64 (2x2) and 128 (3x3) threads.
+// register kernel of 128 threads; scalar refinement ring of 2 stages and 2x2
+// block refinement ring of depth 4, one warp per CTA each; 3x3 block
+// refinement register kernel of 128 threads.
 const TileCfg kDefaultTile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 2, 0, 8, 1, 0, 32, 1}},
-                                     {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 0, 0, 4, 4, 0, 32, 1}},
+                                     {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 4, 0, 4, 1, 0, 32, 1}},
                                      {{128, 1, 0, 0, 4, 4, 0, 32, 1}, {128, 1, 0, 0, 4, 4, 0, 32, 1}}};
 TileCfg g_tile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 2, 0, 8, 1, 0, 32, 1}},
-                        {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 0, 0, 4, 4, 0, 32, 1}},
+                        {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 4, 0, 4, 1, 0, 32, 1}},
                         {{128, 1, 0, 0, 4, 4, 0, 32, 1}, {128, 1, 0, 0, 4, 4, 0, 32, 1}}};
 int kind_index(int kind) { return kind == TG_KIND_SCALAR ? 0 : (kind == TG_KIND_BLOCK2 ? 1 : 2); }
 constexpr int kMaxDevIdx = 64;
@@ -2287,6 +2685,18 @@ cudaError_t with_block_ring(int B, int D, int W, F f)
     return cudaErrorInvalidValue;
 }
 
+// Block refinement ring kernels (2x2 blocks) by ring depth.
+template <typename F>
+cudaError_t with_block_refine_ring(int B, int D, F f)
+{
+    if (B != 2) return cudaErrorInvalidValue;
+    switch (D) {
+    case 4: return f(k_block_refine_ring<2, 4>);
+    case 8: return f(k_block_refine_ring<2, 8>);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 template <typename F>
 cudaError_t with_block_rows(int B, int D, F f)
 {
@@ -2337,6 +2747,7 @@ void device_init()
         for (int d : {4, 8, 16})
             for (int g : {0, 1}) with_scalar_ring(d, g, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int c : {2, 3, 4}) with_scalar_refine_ring(c, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+        for (int dd : {4, 8}) with_block_refine_ring(2, dd, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int c : {2, 3, 4})
             for (int l : {2, 4, 8}) with_scalar_chunk(c, l, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int b : {2, 3})
@@ -2414,7 +2825,7 @@ void tile_for(int kind, int precision, bool ring_ok, int *cpb, int *cpt, int *st
 {
     const TileCfg &t = g_tile[kind_index(kind)][precision ? 1 : 0];
     *w2g = 0;
-    if ((precision == TG_PREC_F64 || kind == TG_KIND_SCALAR) && t.stages > 0 && ring_ok) {
+    if ((precision == TG_PREC_F64 || kind != TG_KIND_BLOCK3) && t.stages > 0 && ring_ok) {
         *cpb = 32;
         *cpt = 1;
         *stages = t.stages;
@@ -2506,8 +2917,10 @@ size_t scalar_smem_bytes(int precision, int threads, int cpt, int k2max, int sta
     return (size_t)threads * 3 * (size_t)k2max * 4;
 }
 
-size_t block_smem_bytes(int B, int stages, int threads, int rows, int bw)
+size_t block_smem_bytes(int B, int stages, int threads, int rows, int bw, int precision)
 {
+    if (precision != TG_PREC_F64)   // refinement ring: P, Q, R, f and u rows per level
+        return stages > 0 ? (size_t)threads / 32 * stages * (3 * B * B + 2 * B) * 32 * 8 : 0;
     const int w = rows ? 32 / rows_group(B) : bw;
     return stages > 0 ? (size_t)threads / 32 * stages * (3 * B * B + B) * w * 8 : 0;
 }
@@ -2535,6 +2948,8 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     sh->lps = stages > 0 && kind == TG_KIND_SCALAR && precision == TG_PREC_F64 && w2g ? g_tile[0][0].lps : 1;
     if (kind == TG_KIND_SCALAR && precision != TG_PREC_F64 && stages > 0)   // refinement ring: 2..4 stages
         stages = sh->stages = stages < 2 ? 2 : (stages > 4 ? 4 : stages);
+    if (kind == TG_KIND_BLOCK2 && precision != TG_PREC_F64 && stages > 0)   // block refinement ring: 4 or 8 levels
+        stages = sh->stages = stages > 4 ? 8 : 4;
     if (sh->lps > 1 && stages > 4) stages = sh->stages = 4;
     if (sh->lps > 1 && sh->lps * stages > 16) stages = sh->stages = 2;
     if (sh->lps == 1 && stages > 0 && stages < 4 && precision == TG_PREC_F64)
@@ -2546,7 +2961,7 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         // a ring that does not fit in shared memory falls back to the
         // register-prefetch kernel with the same 32-column tile
         const size_t need = kind == TG_KIND_SCALAR ? scalar_smem_bytes(precision, sh->threads, 1, k2max, stages, w2g, sh->lps)
-                                                   : block_smem_bytes(kind, stages, sh->threads, sh->rows, sh->bw);
+                                                   : block_smem_bytes(kind, stages, sh->threads, sh->rows, sh->bw, precision);
         if (need > (size_t)(smem_optin() - 1024)) {
             stages = 0;
             sh->stages = 0;
@@ -2575,9 +2990,11 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
             e = with_scalar_refine(sh->pf, occ);
     } else {
         const int B = kind;
-        sh->smem = block_smem_bytes(B, stages, sh->threads, sh->rows, sh->bw);
+        sh->smem = block_smem_bytes(B, stages, sh->threads, sh->rows, sh->bw, precision);
         if (sh->smem > (size_t)(smem_optin() - 1024)) return cudaErrorInvalidConfiguration;
-        if (stages > 0 && sh->rows)
+        if (stages > 0 && precision != TG_PREC_F64)
+            e = with_block_refine_ring(B, stages, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
+        else if (stages > 0 && sh->rows)
             e = with_block_rows(B, stages, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
         else if (stages > 0)
             e = with_block_ring(B, stages, sh->bw,
@@ -2672,7 +3089,15 @@ cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape 
                          double *scratch, unsigned *status, unsigned long long *hist, cudaStream_t st)
 {
     if (tab.ntiles <= 0) return cudaSuccess;
-    if (precision == TG_PREC_F64 && sh.stages > 0 && sh.rows) {
+    if (precision != TG_PREC_F64 && sh.stages > 0) {
+        SegTable t = tab;
+        t.hints = cache_hints();
+        cudaError_t e = with_block_refine_ring(B, sh.stages, [&](auto k) {
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, rf, reinterpret_cast<float *>(scratch), status, hist);
+            return cudaSuccess;
+        });
+        if (e != cudaSuccess) return e;
+    } else if (precision == TG_PREC_F64 && sh.stages > 0 && sh.rows) {
         SegTable t = tab;
         t.hints = cache_hints();
         cudaError_t e = with_block_rows(B, sh.stages, [&](auto k) {
