@@ -462,10 +462,11 @@ int tg_set_block_scratch_budget(double megabytes);
  * are in flight at once on large batches. */
 int tg_set_scalar_scratch_budget(double megabytes);
 
-/* How the kinds of one plan share the GPU: 1 the block kinds run on a side
- * stream beside the scalar kind, 0 one kind after the other, any other
- * value (default) side by side only when every kind's tiles fit in one
- * resident wave.  Same results either way. */
+/* How the kinds of one plan share the GPU, read when a plan is created: 1 the
+ * block kinds run on a side stream beside the scalar kind (whose FP64 grid is
+ * then halved, leaving the block warps, the long pole, more issue slots), 0
+ * one kind after the other, any other value (default) side by side only when
+ * every kind's tiles fit in one resident wave.  Same results either way. */
 int tg_set_kind_overlap(int mode);
 
 /* Host-array entries (tg_solve_host and the per-routine drop-ins): the input

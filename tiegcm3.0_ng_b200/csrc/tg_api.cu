@@ -1201,6 +1201,7 @@ struct tg_plan {
     cudaStream_t side = nullptr;            // block kinds run here, beside the scalar kind
     cudaEvent_t fork = nullptr, join = nullptr;
     int launches = 0;
+    bool side_by_side = false;              // block kinds on `side` beside the scalar kind
 };
 
 namespace {
@@ -1230,14 +1231,8 @@ int plan_enqueue(tg_plan *p, cudaStream_t st)
     TG_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(unsigned) * p->nseg, st));
     if (p->precision != TG_PREC_F64)
         TG_CUDA(cudaMemsetAsync(p->d_hist, 0, kMaxSweepBins * sizeof(unsigned long long), st));
-    bool split = p->groups[0].nseg > 0 && (p->groups[1].nseg > 0 || p->groups[2].nseg > 0);
-    const int overlap = kind_overlap();
-    if (overlap == 0) split = false;
-    if (overlap < 0)
-        for (const auto &g : p->groups)
-            if (g.nseg > 0 && !g.shape.one_wave) split = false;
     int rc;
-    if (!split) {
+    if (!p->side_by_side) {
         for (auto &g : p->groups)
             if (g.nseg > 0 && (rc = plan_launch_group(p, g, st))) return rc;
         return TG_OK;
@@ -1350,6 +1345,28 @@ __attribute__((visibility("default"))) int tg_plan_create(const tg_segment *segs
             set_err("tg_plan_create: segment table upload failed");
             return TG_ENOMEM;
         }
+        p->launches += 1;
+    }
+    // Kinds side by side (the latency-bound regime, every kind in one wave):
+    // the FP64 scalar grid is halved, each warp taking two tiles.  The scalar kind
+    // then still finishes inside the block kinds' time, and the block warps,
+    // the long pole, get more of the SMs' issue slots (2.5 deg grid, 10368
+    // columns: 84 -> 78 us).  Decided here, with the overlap setting of the
+    // plan's creation.
+    {
+        auto &g0 = p->groups[0];
+        bool split = g0.nseg > 0 && (p->groups[1].nseg > 0 || p->groups[2].nseg > 0);
+        const int overlap = kind_overlap();
+        if (overlap == 0) split = false;
+        if (overlap < 0)
+            for (const auto &g : p->groups)
+                if (g.nseg > 0 && !g.shape.one_wave) split = false;
+        p->side_by_side = split;
+        if (split && precision == TG_PREC_F64 && g0.shape.stages > 0 && g0.shape.blocks > 1)
+            g0.shape.blocks = (g0.shape.blocks + 1) / 2;
+    }
+    for (auto &g : p->groups) {
+        if (!g.nseg) continue;
         const bool ring_refine = g.kind == TG_KIND_SCALAR && precision != TG_PREC_F64 && g.shape.stages > 0;
         if (g.kind != TG_KIND_SCALAR || g.shape.w2g || ring_refine) {
             const long slots = (long)g.shape.blocks * g.shape.threads;
@@ -1363,7 +1380,6 @@ __attribute__((visibility("default"))) int tg_plan_create(const tg_segment *segs
                 return TG_ENOMEM;
             }
         }
-        p->launches += 1;
     }
     if (cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess ||
