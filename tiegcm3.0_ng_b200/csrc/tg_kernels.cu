@@ -948,29 +948,33 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
             for (int j = 0; j < nch; ++j) {
                 if (!wait(q, j, nch)) return;
                 const double *stg = buf + (long)((q + j) % C) * SD + lane;
+                auto step0 = [&](int l, int k, bool first) {
+                    const float af = (float)stg[(4 * l) * 32], bf = (float)stg[(4 * l + 1) * 32],
+                                ff = (float)stg[(4 * l + 3) * 32];
+                    if (first) {
+                        w1 = bf;
+                        ri = __frcp_rn(w1);
+                        y = ff * ri;
+                    } else {
+                        const float w2 = cprev * ri;
+                        st_hint_f(&gw2[(k - 1) * S], w2, keep);
+                        w1 = bf - af * w2;
+                        ri = __frcp_rn(w1);
+                        y = (ff - af * y) * ri;
+                    }
+                    ok = ok && (fabsf(w1) <= FLT_MAX) && (w1 != 0.f);
+                    st_hint_f(&gri[k * S], ri, keep);
+                    st_hint_f(&gy[k * S], y, keep);
+                    cprev = (float)stg[(4 * l + 2) * 32];
+                };
                 if (valid) {
+                    if (j > 0 && (j + 1) * L <= k2) {   // a full chunk past level 0: no per-level tests
 #pragma unroll
-                    for (int l = 0; l < L; ++l) {
-                        const int k = j * L + l;
-                        if (k < k2) {
-                            const float af = (float)stg[(4 * l) * 32], bf = (float)stg[(4 * l + 1) * 32],
-                                        ff = (float)stg[(4 * l + 3) * 32];
-                            if (k == 0) {
-                                w1 = bf;
-                                ri = __frcp_rn(w1);
-                                y = ff * ri;
-                            } else {
-                                const float w2 = cprev * ri;
-                                st_hint_f(&gw2[(k - 1) * S], w2, keep);
-                                w1 = bf - af * w2;
-                                ri = __frcp_rn(w1);
-                                y = (ff - af * y) * ri;
-                            }
-                            ok = ok && (fabsf(w1) <= FLT_MAX) && (w1 != 0.f);
-                            st_hint_f(&gri[k * S], ri, keep);
-                            st_hint_f(&gy[k * S], y, keep);
-                            cprev = (float)stg[(4 * l + 2) * 32];
-                        }
+                        for (int l = 0; l < L; ++l) step0(l, j * L + l, false);
+                    } else {
+#pragma unroll
+                        for (int l = 0; l < L; ++l)
+                            if (j * L + l < k2) step0(l, j * L + l, j * L + l == 0);
                     }
                 }
                 __syncwarp();
@@ -1023,22 +1027,29 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
                 if (!wait(q, j, nch)) return;
                 const double *stg = buf + (long)((q + j) % C) * SD + lane;
                 const float *stf = reinterpret_cast<const float *>(buf + (long)((q + j) % C) * SD + NE * 32) + lane;
+                // level k from stage row l; `first` for level 0, `last` for k2-1
+                auto step = [&](int l, int k, bool first, bool last) {
+                    const double xp1 = last ? 0.0 : stg[(NC + l) * 32];
+                    if (active) {
+                        const double ak = stg[(4 * l) * 32];
+                        double r = fma(-stg[(4 * l + 1) * 32], x0, stg[(4 * l + 3) * 32]);
+                        if (!first) r = fma(-ak, xm1, r);
+                        if (!last) r = fma(-stg[(4 * l + 2) * 32], xp1, r);
+                        const float rr = (float)r, rik = stf[l * 32];
+                        y = first ? rr * rik : (rr - (float)ak * y) * rik;
+                        st_hint_f(&gy[k * S], y, keep);
+                    }
+                    xm1 = x0;
+                    x0 = xp1;
+                };
+                if (j > 0 && (j + 1) * L < k2) {   // a full chunk, neither level 0 nor the top
 #pragma unroll
-                for (int l = 0; l < L; ++l) {
-                    const int k = j * L + l;
-                    if (k < k2) {
-                        const double xp1 = k + 1 < k2 ? stg[(NC + l) * 32] : 0.0;
-                        if (active) {
-                            const double ak = stg[(4 * l) * 32];
-                            double r = fma(-stg[(4 * l + 1) * 32], x0, stg[(4 * l + 3) * 32]);
-                            if (k > 0) r = fma(-ak, xm1, r);
-                            if (k + 1 < k2) r = fma(-stg[(4 * l + 2) * 32], xp1, r);
-                            const float rr = (float)r, rik = stf[l * 32];
-                            y = k == 0 ? rr * rik : (rr - (float)ak * y) * rik;
-                            st_hint_f(&gy[k * S], y, keep);
-                        }
-                        xm1 = x0;
-                        x0 = xp1;
+                    for (int l = 0; l < L; ++l) step(l, j * L + l, false, false);
+                } else {
+#pragma unroll
+                    for (int l = 0; l < L; ++l) {
+                        const int k = j * L + l;
+                        if (k < k2) step(l, k, k == 0, k + 1 == k2);
                     }
                 }
                 __syncwarp();
