@@ -1233,16 +1233,20 @@ __device__ __forceinline__ bool blk_back(double *pU, long ld, const double *gam,
     constexpr int BB = B * B, BPF = B == 2 ? 4 : 2;
     bool fin = true;
     double rz[BPF][B], rg[BPF][BB];
+    // level k of u (z parked there) and of Gamma; rows BPF levels apart
+    const long su = (long)B * ld, sg = (long)BB * gs;
 #pragma unroll
     for (int u = 0; u < BPF; ++u) {
         const int k = k2 - 2 - u;
         if (k >= 0) {
 #pragma unroll
-            for (int i = 0; i < B; ++i) rz[u][i] = pU[((long)k * B + i) * ld];
+            for (int i = 0; i < B; ++i) rz[u][i] = pU[k * su + i * ld];
 #pragma unroll
-            for (int e = 0; e < BB; ++e) rg[u][e] = gam[((long)k * BB + e) * gs];
+            for (int e = 0; e < BB; ++e) rg[u][e] = gam[k * sg + e * gs];
         }
     }
+    double *uk = pU + (long)(k2 - 2) * su;
+    const double *gn = gam + (long)(k2 - 2 - BPF) * sg;   // refill rows: level k - BPF
     for (int kb = k2 - 2; kb >= 0; kb -= BPF) {
 #pragma unroll
         for (int u = 0; u < BPF; ++u) {
@@ -1257,18 +1261,20 @@ __device__ __forceinline__ bool blk_back(double *pU, long ld, const double *gam,
                     nu[i] = t;
                     fin = fin && finite(t);
                 }
-                const int kn = k - BPF;
-                if (kn >= 0) {
+                if (k - BPF >= 0) {
+                    const double *un_src = uk - BPF * su;
 #pragma unroll
-                    for (int i = 0; i < B; ++i) rz[u][i] = pU[((long)kn * B + i) * ld];
+                    for (int i = 0; i < B; ++i) rz[u][i] = un_src[i * ld];
 #pragma unroll
-                    for (int e = 0; e < BB; ++e) rg[u][e] = gam[((long)kn * BB + e) * gs];
+                    for (int e = 0; e < BB; ++e) rg[u][e] = gn[e * gs];
                 }
 #pragma unroll
                 for (int i = 0; i < B; ++i) {
                     un[i] = nu[i];
-                    pU[((long)k * B + i) * ld] = nu[i];
+                    uk[i * ld] = nu[i];
                 }
+                uk -= su;
+                gn -= sg;
             }
         }
     }
@@ -1433,7 +1439,8 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
         for (int j = 0; j < pre; ++j) ring.issue(q + j, src + j * lstride, lane);
         bool ok = true;
         double G[BB], z[B];
-        for (int k = 0; k < k2; ++k) {
+        double *pUk = pU, *gk = gam;   // level k of the parked z and of Gamma
+        for (int k = 0; k < k2; ++k, pUk += B * ld, gk += BB * gs) {
             const unsigned qk = q + k;
             if (!ring.wait(qk)) {
                 ring.drain(qk, q + (k + D < k2 ? k + D : k2));
@@ -1484,7 +1491,7 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
 #pragma unroll
                 for (int m = 1; m < B; ++m) tv = xadd(tv, xmul(Wi[i + B * m], v[m]));
                 z[i] = tv;
-                st_hint(&pU[((long)k * B + i) * ld], tv, keep);
+                st_hint(&pUk[(long)i * ld], tv, keep);
             }
             if (k < k2 - 1) {
 #pragma unroll
@@ -1495,7 +1502,7 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
 #pragma unroll
                         for (int n = 1; n < B; ++n) g = xadd(g, xmul(Wi[i + B * n], R[n + B * m]));
                         G[i + B * m] = g;
-                        st_hint(&gam[((long)k * BB + i + B * m) * gs], g, keep);
+                        st_hint(&gk[(long)(i + B * m) * gs], g, keep);
                     }
             }
         }
