@@ -51,6 +51,10 @@ __device__ __forceinline__ bool exp_safe(double v)
     const unsigned e2 = (unsigned)__double2hiint(v) * 2u - (523u << 21);   // sign bit shifted out
     return e2 < (1000u << 21);
 }
+// exp_safe's biased-exponent distance, combined over several values with max:
+// all are safe when the maximum is below kExpSpan.
+constexpr unsigned kExpSpan = 1000u << 21;
+__device__ __forceinline__ unsigned exp_dist(double v) { return (unsigned)__double2hiint(v) * 2u - (523u << 21); }
 // a/b, correctly rounded, given y = __drcp_rn(b) and b_safe = exp_safe(b),
 // which a recurrence computes once for the two divisions by the same pivot.
 __device__ __forceinline__ double qdiv_pivot(double a, double b, double y, bool b_safe)

@@ -1160,6 +1160,15 @@ __device__ __forceinline__ bool inv_exact<2>(const double (&A)[4], double (&W)[4
     const double d = xsub(xmul(A[0], A[3]), xmul(A[2], A[1]));
     const double y = __drcp_rn(d);
     const bool ds = exp_safe(d);
+    // one range test for the pivot and all four numerators (a sign does not
+    // change the exponent); any out of range: each division on its own
+    if (max(max(exp_dist(d), exp_dist(A[0])), max(max(exp_dist(A[1]), exp_dist(A[2])), exp_dist(A[3]))) < kExpSpan) {
+        W[0] = div_markstein(A[3], d, y);
+        W[1] = div_markstein(-A[1], d, y);
+        W[2] = div_markstein(-A[2], d, y);
+        W[3] = div_markstein(A[0], d, y);
+        return true;
+    }
     W[0] = qdiv_pivot(A[3], d, y, ds);
     W[1] = qdiv_pivot(-A[1], d, y, ds);
     W[2] = qdiv_pivot(-A[2], d, y, ds);
@@ -1191,6 +1200,14 @@ __device__ __forceinline__ bool inv_exact<3>(const double (&A)[9], double (&W)[9
 #undef w_
     const double y = __drcp_rn(d);
     const bool ds = exp_safe(d);
+    unsigned dm = exp_dist(d);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) dm = max(dm, exp_dist(W[e]));
+    if (dm < kExpSpan) {   // pivot and all nine numerators in range: one test
+#pragma unroll
+        for (int e = 0; e < 9; ++e) W[e] = div_markstein(W[e], d, y);
+        return true;
+    }
 #pragma unroll
     for (int e = 0; e < 9; ++e) W[e] = qdiv_pivot(W[e], d, y, ds);
     return ds || finite_nz(d);
