@@ -287,6 +287,14 @@ __device__ __forceinline__ void inv3_ieee(const double (&A)[9], double (&W)[9])
     // to IEEE division (qdiv)
     const double y = __drcp_rn(d);
     const bool ds = exp_safe(d);
+    unsigned dm = exp_dist(d);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) dm = max(dm, exp_dist(W[e]));
+    if (dm < kExpSpan) {   // pivot and all nine numerators in range: one test
+#pragma unroll
+        for (int e = 0; e < 9; ++e) W[e] = div_markstein(W[e], d, y);
+        return;
+    }
 #pragma unroll
     for (int e = 0; e < 9; ++e) W[e] = qdiv_pivot(W[e], d, y, ds);
 }
