@@ -526,8 +526,7 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
         const int pre = nch < C ? nch : C;
         for (int j = 0; j < pre; ++j) issue(q + j, j);
         bool ok = true, fin = true;
-        double w1 = 0.0, y1 = 0.0, w3 = 0.0, cprev = 0.0;
-        bool w1s = false;   // exp_safe(w1): the pivot's range test, shared by its two divisions
+        double w1 = 0.0, y1 = 0.0, w3 = 0.0, w2 = 0.0;   // w2: the next level's, from this pivot
         for (int j = 0; j < nch; ++j) {
             const unsigned qc = q + j;
             if (!mbar_wait_warp(&bar[qc % C], (qc / C) & 1u)) {
@@ -540,35 +539,39 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
             // the stage is read in place and handed back to the copy engine
             // after the L levels are done (registers stay low: more warps/SM)
             const double *stg = buf + (int)(qc % C) * NE * 32 + lane;
-            // level k from stage row l; `first` only for level 0
-            auto step = [&](int l, int k, bool first) {
-                const double ak = stg[(4 * l + 0) * 32], bk = stg[(4 * l + 1) * 32], fk = stg[(4 * l + 3) * 32];
-                if (first) {
-                    w1 = bk;
-                    y1 = __drcp_rn(w1);
-                    w1s = exp_safe(w1);
-                    w3 = qdiv_pivot(fk, w1, y1, w1s);
+            // Level k from stage row l.  Both divisions by the pivot w1(k) are
+            // done here: w3(k) = (f - a*w3(k-1))/w1(k) and the next level's
+            // w2 = c(k)/w1(k) (the same operands as the reference's, so the
+            // same correctly rounded quotients), under one range test.
+            auto step = [&](int l, int k, bool first, bool last) {
+                const double ak = stg[(4 * l + 0) * 32], bk = stg[(4 * l + 1) * 32], fk = stg[(4 * l + 3) * 32],
+                             ck = stg[(4 * l + 2) * 32];
+                w1 = first ? bk : xsub(bk, xmul(ak, w2));
+                y1 = __drcp_rn(w1);
+                const double num = first ? fk : xsub(fk, xmul(ak, w3));
+                if (max(exp_dist(w1), max(exp_dist(num), exp_dist(ck))) < kExpSpan) {
+                    w3 = div_markstein(num, w1, y1);
+                    w2 = div_markstein(ck, w1, y1);
                 } else {
-                    const double w2 = qdiv_pivot(cprev, w1, y1, w1s);
-                    st_hint(&w2s[(k - 1) * ws], w2, keep);
-                    w1 = xsub(bk, xmul(ak, w2));
-                    y1 = __drcp_rn(w1);
-                    w1s = exp_safe(w1);
-                    w3 = qdiv_pivot(xsub(fk, xmul(ak, w3)), w1, y1, w1s);
+                    const bool w1s = exp_safe(w1);
+                    w3 = qdiv_pivot(num, w1, y1, w1s);
+                    w2 = qdiv_pivot(ck, w1, y1, w1s);
+                    // a pivot in the safe range is finite and nonzero
+                    if (!w1s) ok = ok && finite_nz(w1);
                 }
-                // a pivot in the safe range is finite and nonzero
-                if (!w1s) ok = ok && finite_nz(w1);
-                cprev = stg[(4 * l + 2) * 32];
+                if (!last) st_hint(&w2s[k * ws], w2, keep);
                 st_hint(&px[k * ld], w3, keep);
             };
             if (valid) {
-                if (j > 0 && (j + 1) * L <= k2) {   // a full chunk past level 0: no per-level tests
+                if (j > 0 && (j + 1) * L < k2) {   // a full chunk, neither level 0 nor the top
 #pragma unroll
-                    for (int l = 0; l < L; ++l) step(l, j * L + l, false);
+                    for (int l = 0; l < L; ++l) step(l, j * L + l, false, false);
                 } else {
 #pragma unroll
-                    for (int l = 0; l < L; ++l)
-                        if (j * L + l < k2) step(l, j * L + l, j * L + l == 0);
+                    for (int l = 0; l < L; ++l) {
+                        const int k = j * L + l;
+                        if (k < k2) step(l, k, k == 0, k + 1 == k2);
+                    }
                 }
             }
             __syncwarp();
