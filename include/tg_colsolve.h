@@ -277,6 +277,31 @@ int tg_comp_post_ng(const double *o2, const double *o1, const double *he, const 
                     double dtsmooth_div2, int nk, int ncol, double *o2_upd, double *o1_upd, double *he_upd,
                     double *o2nm_upd, double *o1nm_upd, double *henm_upd);
 
+/* The post-solve time filter and floor of the scalar routines, applied after
+ * the caller has written its lateral-boundary columns:
+ *   TG_FILTER_DT    src/dt_ng.F90:208-213     tn_nm_upd = dtsmooth_div2*(tn_nm+tn_upd) + dtsmooth*tn,
+ *                                             tn_upd = max(tn_upd, 100.)
+ *   TG_FILTER_MINOR src/minor_ng.F90:234-237  fcomp_tm1_out = dtsmooth*fcomp + dtsmooth_div2*(fcomp_tm1+fcomp_out),
+ *                                             both floored at 1e-12
+ *   TG_FILTER_OPLUS src/oplus_ng.F90:337-340  optm1out = dtsmooth*op + dtsmooth_div2*(optm1+opout),
+ *                                             both floored at 0
+ * cur is the field at the current step (tn, fcomp, op), prev the previous
+ * step (tn_nm, fcomp_tm1, optm1); upd (tn_upd, fcomp_out, opout) is read and
+ * floored in place and nm_upd receives the filtered field.  nm_upd may be
+ * the same array as prev or cur.  A floor keeps x when x > floor and gives
+ * the floor otherwise (NaN included, as tg_comp_post_ng does).  Results are
+ * bit-identical to the reference's FP64 arithmetic (no fused multiply-add).
+ * Host arrays (nk, ncol), synchronous. */
+#define TG_FILTER_DT 0
+#define TG_FILTER_MINOR 1
+#define TG_FILTER_OPLUS 2
+int tg_time_filter_ng(int which, const double *cur, const double *prev, double dtsmooth, double dtsmooth_div2,
+                      int nk, int ncol, double *upd, double *nm_upd);
+/* Device arrays, level-major (k*ld + col), stream-ordered; nk <= 65535. */
+int tg_time_filter_ng_dev(int which, const double *cur, const double *prev, double dtsmooth,
+                          double dtsmooth_div2, int nk, int ncol, long ld, double *upd, double *nm_upd,
+                          void *stream);
+
 /* settei_ng's electron and ion temperature step (src/settei_ng.F90:60-261):
  * the whole routine is column-local, so it is one fused kernel: the heat-flux
  * boundary fe, thermal conductivity, the conduction rows in Te^3.5, heating,

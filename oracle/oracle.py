@@ -275,6 +275,26 @@ def comp_post_ng(fields, consts):
     return tuple(upd) + tuple(nm)
 
 
+FILTER_DT, FILTER_MINOR, FILTER_OPLUS = 0, 1, 2
+
+
+def time_filter_ng(which, cur, prev, upd, dtsmooth, dtsmooth_div2):
+    """Post-solve time filter and floor of dt_ng (src/dt_ng.F90:208-213),
+    minor_ng (src/minor_ng.F90:234-237) or oplus_ng (src/oplus_ng.F90:337-340);
+    returns (upd floored, nm) as new (nk, ncol) arrays."""
+    L = lib()
+    if not hasattr(L, "_filter_bound"):
+        L.oracle_time_filter_ng.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_time_filter_ng.restype = None
+        L._filter_bound = True
+    c, p = _fcopy(cur), _fcopy(prev)
+    u = _fcopy(upd).copy(order="F")
+    nm = np.zeros_like(u, order="F")
+    L.oracle_time_filter_ng(int(which), _p(c), _p(p), float(dtsmooth), float(dtsmooth_div2), u.size, _p(u), _p(nm))
+    return u, nm
+
+
 SETTEI_FIELD_ORDER = ("tn", "o2", "o1", "he", "n2", "ne", "te", "ti", "op", "o2p", "nplus", "n2p", "nop", "xnmbar",
                       "xnmbari", "scht", "schti", "qji_ti", "qop2p", "qop2d", "qo2p", "qop", "qn2p", "qnp", "qnop",
                       "Q1", "Q2", "t_lbc", "chi", "rlatm", "dipmag", "qteaur")

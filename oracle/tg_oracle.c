@@ -959,6 +959,30 @@ ORACLE_API void oracle_comp_post_ng(const double *o2, const double *o1, const do
     free(n2);
 }
 
+/* Post-solve time filter and floor of dt_ng (src/dt_ng.F90:208-213,        */
+/* which 0: floor 100 on upd only), minor_ng (src/minor_ng.F90:234-237,     */
+/* which 1: floor small = 1e-12 on both) and oplus_ng                        */
+/* (src/oplus_ng.F90:337-340, which 2: floor 0 on both).  upd is read and   */
+/* floored in place, nm receives the filtered field.  Element-wise, so n =  */
+/* nk*ncol elements in any layout.  The floor keeps x when x > fl, as the   */
+/* comp_ng restatement above does.                                           */
+ORACLE_API void oracle_time_filter_ng(int which, const double *cur, const double *prev, double dtsmooth,
+                                      double dtsmooth_div2, long n, double *upd, double *nm)
+{
+    const double fl = which == 0 ? 100. : which == 1 ? 1.e-12 : 0.;
+    long i;
+    for (i = 0; i < n; ++i) {
+        const double u = upd[i];
+        /* dt_ng writes dtsmooth_div2*(tn_nm+tn_upd)+dtsmooth*tn, the other two */
+        /* dtsmooth*cur+dtsmooth_div2*(prev+upd): the same two rounded terms    */
+        /* summed, and IEEE addition is commutative.                            */
+        const double v = which == 0 ? dtsmooth_div2 * (prev[i] + u) + dtsmooth * cur[i]
+                                    : dtsmooth * cur[i] + dtsmooth_div2 * (prev[i] + u);
+        upd[i] = u > fl ? u : fl;
+        nm[i] = (which == 0 || v > fl) ? v : fl;
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* settei_ng electron / ion temperature column step (src/settei_ng.F90:     */
 /* 60-261): the whole routine is column-local.  Fields (nk, ncol), 2-D      */

@@ -31,6 +31,7 @@ STATUS_NAMES = {0: "TG_OK", 1: "TG_EINVAL", 2: "TG_EPIVOT", 3: "TG_ENONFINITE", 
 TG_PREC_F64, TG_PREC_F32_REFINE = 0, 1
 TG_LAYOUT_COLUMN, TG_LAYOUT_LEVEL = 0, 1
 TG_KIND_SCALAR, TG_KIND_BLOCK2, TG_KIND_BLOCK3 = 0, 2, 3
+TG_FILTER_DT, TG_FILTER_MINOR, TG_FILTER_OPLUS = 0, 1, 2
 NUMERIC_STATUS = (TG_OK, TG_EPIVOT, TG_ENONFINITE, TG_ENOCONV)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -38,7 +39,7 @@ LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
 EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor_ng_dev", "tg_comp_ng",
-           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
+           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
@@ -203,6 +204,8 @@ def lib():
                                  P],
             "tg_comp_ng_dev": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, I, I, Lg, P, P, P],
             "tg_comp_post_ng": [P] * 8 + [D, D, D, I, I] + [P] * 6,
+            "tg_time_filter_ng": [I, P, P, D, D, I, I, P, P],
+            "tg_time_filter_ng_dev": [I, P, P, D, D, I, I, Lg, P, P, P],
             "tg_minor_ng_dev": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, I, I, Lg, P, P, P],
             "tg_dt_ng_dev": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I, Lg, P, P, P],
             "tg_trsolv_ng": [P, P, P, P, P, I, I, I],
@@ -482,6 +485,25 @@ def comp_post_ng(fields, consts, upd, nm_out):
                                float(consts["dtsmooth_div2"]), nk, ncol,
                                *[_out(u, "upd") for u in upd], *[_out(u, "nm_out") for u in nm_out])
     return _check(rc, "tg_comp_post_ng")
+
+
+def time_filter_ng(which, cur, prev, dtsmooth, dtsmooth_div2, upd, nm_out):
+    """Post-solve time filter and floor (which = TG_FILTER_DT: src/dt_ng.F90:208-213,
+    TG_FILTER_MINOR: src/minor_ng.F90:234-237, TG_FILTER_OPLUS:
+    src/oplus_ng.F90:337-340) on host (nk, ncol) arrays: upd is floored in
+    place and nm_out receives the filtered field."""
+    nk = upd.shape[0]
+    ncol = upd.size // nk
+    rc = lib().tg_time_filter_ng(int(which), _host(cur, "cur"), _host(prev, "prev"), float(dtsmooth),
+                                 float(dtsmooth_div2), nk, ncol, _out(upd, "upd"), _out(nm_out, "nm_out"))
+    return _check(rc, "tg_time_filter_ng", numeric_ok=False)
+
+
+def time_filter_ng_dev(which, cur, prev, dtsmooth, dtsmooth_div2, upd, nm_out, nk, ncol, ld, stream=None):
+    """Device form of time_filter_ng on level-major (nk, ld) fields."""
+    rc = lib().tg_time_filter_ng_dev(int(which), _dptr(cur), _dptr(prev), float(dtsmooth), float(dtsmooth_div2), nk,
+                                     ncol, ld, _dptr(upd), _dptr(nm_out), _stream(stream))
+    return _check(rc, "tg_time_filter_ng_dev", numeric_ok=False)
 
 
 def minor_ng_dev(fields, consts, out, nk, ncol, ld, system_out=None, status=None, stream=None):

@@ -979,6 +979,57 @@ __attribute__((visibility("default"))) int tg_comp_post_ng(const double *o2, con
     return TG_OK;
 }
 
+static bool time_filter_args_ok(const char *who, int which, const double *cur, const double *prev, int nk, int ncol,
+                                const double *upd, const double *nm)
+{
+    const bool ok = which >= TG_FILTER_DT && which <= TG_FILTER_OPLUS && cur && prev && upd && nm && upd != nm &&
+                    upd != cur && upd != prev && nk >= 1 && ncol >= 0;
+    if (!ok) set_err("%s: bad arguments (which=%d nk=%d ncol=%d)", who, which, nk, ncol);
+    return ok;
+}
+
+__attribute__((visibility("default"))) int tg_time_filter_ng_dev(int which, const double *cur, const double *prev,
+                                                                 double dtsmooth, double dtsmooth_div2, int nk,
+                                                                 int ncol, long ld, double *upd, double *nm_upd,
+                                                                 void *stream)
+{
+    if (!time_filter_args_ok("tg_time_filter_ng_dev", which, cur, prev, nk, ncol, upd, nm_upd)) return TG_EINVAL;
+    if (ld < ncol || nk > 65535) {
+        set_err("tg_time_filter_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    TG_CUDA(launch_time_filter(which, cur, prev, dtsmooth, dtsmooth_div2, nk, ncol, ld, upd, nm_upd,
+                               (cudaStream_t)stream));
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_time_filter_ng(int which, const double *cur, const double *prev,
+                                                             double dtsmooth, double dtsmooth_div2, int nk, int ncol,
+                                                             double *upd, double *nm_upd)
+{
+    if (!time_filter_args_ok("tg_time_filter_ng", which, cur, prev, nk, ncol, upd, nm_upd)) return TG_EINVAL;
+    if (ncol == 0) return TG_OK;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    // element-wise, so the Fortran (nk, ncol) arrays are one row of nk*ncol
+    const size_t n = (size_t)nk * ncol, bytes = sizeof(double) * n;
+    if ((rc = grow(c->lvlbuf[0][0], 4 * bytes))) return rc;
+    double *d = (double *)c->lvlbuf[0][0].p;
+    cudaStream_t st = c->st[0];
+    TG_CUDA(cudaMemcpyAsync(d, cur, bytes, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(d + n, prev, bytes, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(d + 2 * n, upd, bytes, cudaMemcpyHostToDevice, st));
+    TG_CUDA(launch_time_filter(which, d, d + n, dtsmooth, dtsmooth_div2, 1, (long)n, (long)n, d + 2 * n, d + 3 * n,
+                               st));
+    TG_CUDA(cudaMemcpyAsync(upd, d + 2 * n, bytes, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaMemcpyAsync(nm_upd, d + 3 * n, bytes, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    return TG_OK;
+}
+
 static bool settei_fields_ok(const tg_settei_fields *F)
 {
     const double *const *p = &F->tn;

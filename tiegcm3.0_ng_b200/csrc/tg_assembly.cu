@@ -1261,4 +1261,40 @@ cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, d
                                                      upd6[2], upd6[3], upd6[4], upd6[5]);
     return cudaGetLastError();
 }
+
+// The post-solve time filter and floor that dt_ng (src/dt_ng.F90:208-213),
+// minor_ng (src/minor_ng.F90:234-237) and oplus_ng (src/oplus_ng.F90:337-340)
+// apply once the lateral-boundary columns are written:
+//   nm = dtsmooth_div2*(prev + upd) + dtsmooth*cur,  upd = max(upd, fl)
+// and, for minor_ng and oplus_ng, nm = max(nm, fl).  Element-wise, so one
+// thread per element of rows of len elements at stride ld; nm may alias prev
+// or cur (each element is read before it is written by the same thread).
+// A floor keeps x when x > fl and gives fl otherwise, NaN included.
+template <bool FloorNm>
+__global__ void __launch_bounds__(256) k_time_filter(const double *cur, const double *prev, double ds, double ds2,
+                                                     double fl, long len, long ld, double *upd, double *nm)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= len) return;
+    const long o = (long)blockIdx.y * ld + i;
+    const double u = upd[o];
+    const double n = xa(xm(ds2, xa(prev[o], u)), xm(ds, cur[o]));
+    upd[o] = u > fl ? u : fl;
+    nm[o] = (!FloorNm || n > fl) ? n : fl;
+}
+
+cudaError_t launch_time_filter(int which, const double *cur, const double *prev, double dtsmooth,
+                               double dtsmooth_div2, int rows, long len, long ld, double *upd, double *nm,
+                               cudaStream_t st)
+{
+    if (rows <= 0 || len <= 0) return cudaSuccess;
+    const int T = 256;
+    const dim3 grid((unsigned)((len + T - 1) / T), (unsigned)rows);
+    if (which == TG_FILTER_DT)
+        k_time_filter<false><<<grid, T, 0, st>>>(cur, prev, dtsmooth, dtsmooth_div2, 100.0, len, ld, upd, nm);
+    else
+        k_time_filter<true><<<grid, T, 0, st>>>(cur, prev, dtsmooth, dtsmooth_div2,
+                                                which == TG_FILTER_MINOR ? 1.e-12 : 0.0, len, ld, upd, nm);
+    return cudaGetLastError();
+}
 }  // namespace tg

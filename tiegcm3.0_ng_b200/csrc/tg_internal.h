@@ -180,6 +180,11 @@ size_t comp_scratch_doubles(int nk, long ld);
 cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, double dz, double dtsmooth,
                                 double dtsmooth_div2, int nk, int ncol, long ld, double *const *upd6,
                                 cudaStream_t st);
+// post-solve time filter and floor of dt_ng / minor_ng / oplus_ng (which =
+// TG_FILTER_*) over rows of len elements at stride ld
+cudaError_t launch_time_filter(int which, const double *cur, const double *prev, double dtsmooth,
+                               double dtsmooth_div2, int rows, long len, long ld, double *upd, double *nm,
+                               cudaStream_t st);
 
 typedef tg_settei_fields SetteiFields;
 typedef tg_settei_consts SetteiConsts;

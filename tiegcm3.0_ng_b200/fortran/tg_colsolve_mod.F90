@@ -12,6 +12,7 @@ module tg_colsolve_mod
   integer(c_int), parameter :: TG_OK = 0, TG_EINVAL = 1, TG_EPIVOT = 2, TG_ENONFINITE = 3, &
     TG_ENOCONV = 4, TG_ETIMEOUT = 5, TG_ECUDA = 6, TG_ENOMEM = 7, TG_ENODEV = 8
   integer(c_int), parameter :: TG_PREC_F64 = 0, TG_PREC_F32_REFINE = 1
+  integer(c_int), parameter :: TG_FILTER_DT = 0, TG_FILTER_MINOR = 1, TG_FILTER_OPLUS = 2
 
   ! Field tables of the fused assembly + solve entries: c_loc() of each
   ! Fortran array (3-D fields (nk, ncol), 2-D (ncol), level profiles (nk)),
@@ -169,6 +170,18 @@ module tg_colsolve_mod
       integer(c_int), value :: nk, ncol
       real(c_double), intent(inout) :: o2_upd(*), o1_upd(*), he_upd(*), o2nm_upd(*), o1nm_upd(*), henm_upd(*)
     end function tg_comp_post_ng
+
+    ! which = TG_FILTER_DT / _MINOR / _OPLUS: the time filter and floor after
+    ! the lateral-boundary hook (dt_ng.F90:208-213, minor_ng.F90:234-237,
+    ! oplus_ng.F90:337-340); upd floored in place, nm_upd the filtered field
+    integer(c_int) function tg_time_filter_ng(which, cur, prev, dtsmooth, dtsmooth_div2, nk, ncol, upd, nm_upd) &
+        bind(C, name="tg_time_filter_ng")
+      import :: c_int, c_double
+      integer(c_int), value :: which, nk, ncol
+      real(c_double), intent(in) :: cur(*), prev(*)
+      real(c_double), value :: dtsmooth, dtsmooth_div2
+      real(c_double), intent(inout) :: upd(*), nm_upd(*)
+    end function tg_time_filter_ng
 
     integer(c_int) function tg_settei_ng(fl, cn, te_out, ti_out, qtotal, nk, ncol) bind(C, name="tg_settei_ng")
       import :: c_int, c_double, tg_settei_fields, tg_settei_consts
