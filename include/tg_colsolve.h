@@ -297,6 +297,31 @@ int tg_comp_post_ng(const double *o2, const double *o1, const double *he, const 
 #define TG_FILTER_OPLUS 2
 int tg_time_filter_ng(int which, const double *cur, const double *prev, double dtsmooth, double dtsmooth_div2,
                       int nk, int ncol, double *upd, double *nm_upd);
+/* ---- horizontal operators feeding the assembly -------------------------------
+ * advec_ng (src/advec_ng.F90:1-52) and smooth_ng (src/smooth_ng.F90:1-42)
+ * with their difference and mean helpers (src/dffm_ng.F90), for a nest held
+ * as one subdomain: arrays (nk, nlon+4, nlat+4) over the ghost-inclusive
+ * lond0:lond1 x latd0:latd1, every lateral edge a boundary (is_bndry all
+ * true, the one-task decomposition of src/fields_ng.F90:143-147), so the
+ * halo exchanges of src/sync_ng.F90 have nothing to exchange.
+ *   tg_advec_ng:  hadvec from f, the winds un, vn (the itp level of the
+ *                 model's fields), racs (nlat+4) per latitude, dlamda, dphi
+ *                 and re_inv = 1/re.
+ *   tg_smooth_ng: fout = the Shapiro filter of fin, in lat then lon.
+ * Results are bit-identical to the reference's FP64 arithmetic.  Outputs
+ * must not alias inputs.  nk <= 65535, nlat <= 500000. */
+int tg_advec_ng(const double *f, const double *un, const double *vn, const double *racs, double dlamda,
+                double dphi, double re_inv, int nk, int nlon, int nlat, double *hadvec);
+int tg_smooth_ng(const double *fin, double shapiro, int nk, int nlon, int nlat, double *fout);
+/* Device forms: level-major planes, (k, i, j) at k*ld + i + (nlon+4)*j with
+ * ld >= (nlon+4)*(nlat+4) (the column index of the other device entries);
+ * racs a device array (nlat+4); stream-ordered. */
+int tg_advec_ng_dev(const double *f, const double *un, const double *vn, const double *racs, double dlamda,
+                    double dphi, double re_inv, double *hadvec, int nk, int nlon, int nlat, long ld,
+                    void *stream);
+int tg_smooth_ng_dev(const double *fin, double shapiro, double *fout, int nk, int nlon, int nlat, long ld,
+                     void *stream);
+
 /* Device arrays, level-major (k*ld + col), stream-ordered; nk <= 65535. */
 int tg_time_filter_ng_dev(int which, const double *cur, const double *prev, double dtsmooth,
                           double dtsmooth_div2, int nk, int ncol, long ld, double *upd, double *nm_upd,

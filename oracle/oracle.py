@@ -376,3 +376,38 @@ def oplus_ng(fields, consts, with_system=False):
     sysarr = [np.zeros((nk, ncol), order="F") for _ in range(4)] if with_system else [None] * 4
     L.oracle_oplus_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(a) for a in outs], *[_p(s) for s in sysarr])
     return (tuple(outs), tuple(sysarr)) if with_system else tuple(outs)
+
+
+def _bind_horiz(L):
+    if not hasattr(L, "_horiz_bound"):
+        P, D, I = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+        L.oracle_advec_ng.argtypes = [P, P, P, P, D, D, D, I, I, I, P]
+        L.oracle_advec_ng.restype = None
+        L.oracle_smooth_ng.argtypes = [P, D, I, I, I, P]
+        L.oracle_smooth_ng.restype = None
+        L._horiz_bound = True
+    return L
+
+
+def advec_ng(f, un, vn, racs, dlamda, dphi, re_inv):
+    """advec_ng (src/advec_ng.F90:1-52) on one nest held as a single
+    subdomain; f, un, vn (nk, nlon+4, nlat+4), racs (nlat+4).  Returns hadvec."""
+    L = _bind_horiz(lib())
+    a = [_fcopy(x) for x in (f, un, vn)]
+    r = np.ascontiguousarray(racs, dtype=np.float64)
+    nk, nlond, nlatd = a[0].shape
+    out = np.zeros_like(a[0], order="F")
+    L.oracle_advec_ng(*[_p(x) for x in a], r.ctypes.data, float(dlamda), float(dphi), float(re_inv), nk,
+                      nlond - 4, nlatd - 4, _p(out))
+    return out
+
+
+def smooth_ng(fin, shapiro):
+    """smooth_ng (src/smooth_ng.F90:1-42) on one nest held as a single
+    subdomain; fin (nk, nlon+4, nlat+4).  Returns fout."""
+    L = _bind_horiz(lib())
+    a = _fcopy(fin)
+    nk, nlond, nlatd = a.shape
+    out = np.zeros_like(a, order="F")
+    L.oracle_smooth_ng(_p(a), float(shapiro), nk, nlond - 4, nlatd - 4, _p(out))
+    return out

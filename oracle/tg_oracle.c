@@ -1377,3 +1377,123 @@ ORACLE_API void oracle_oplus_ng(const oracle_oplus_fields *F, const oracle_oplus
     }
     free(w);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Horizontal operators of one nest held as a single subdomain: arrays       */
+/* (nk, nlon+4, nlat+4) over the ghost-inclusive lond0:lond1 x latd0:latd1, */
+/* every lateral edge a boundary (is_bndry all true, the one-task           */
+/* decomposition of src/fields_ng.F90:143-147), so the halo syncs of        */
+/* src/sync_ng.F90 exchange nothing.                                         */
+/* ------------------------------------------------------------------------ */
+
+/* df_3d (src/dffm_ng.F90:66-110) along lon (dir 0) or lat (dir 1), order   */
+/* 1 or 2: centred differences over 2*order spacings, one-sided at the      */
+/* edges.                                                                    */
+static void hz_df(const double *f, double *df, int order, int dir, int nk, int nlond, int nlatd)
+{
+    const long s = dir == 0 ? nk : (long)nk * nlond;
+    const int n = dir == 0 ? nlond : nlatd;
+    int k, i, j;
+    for (j = 0; j < nlatd; ++j)
+        for (i = 0; i < nlond; ++i)
+            for (k = 0; k < nk; ++k) {
+                const long o = k + (long)nk * (i + (long)nlond * j);
+                const int t = dir == 0 ? i : j;
+                if (t == 0) df[o] = f[o + s] - f[o];
+                else if (t == n - 1) df[o] = f[o] - f[o - s];
+                else if (order == 2 && (t == 1 || t == n - 2)) df[o] = (f[o + s] - f[o - s]) / 2.;
+                else df[o] = (f[o + order * s] - f[o - order * s]) / (double)(order * 2);
+            }
+}
+
+/* fm_3d (src/dffm_ng.F90:166-205): centred means, the input at the edges. */
+static void hz_fm(const double *f, double *fm, int order, int dir, int nk, int nlond, int nlatd)
+{
+    const long s = dir == 0 ? nk : (long)nk * nlond;
+    const int n = dir == 0 ? nlond : nlatd;
+    int k, i, j;
+    for (j = 0; j < nlatd; ++j)
+        for (i = 0; i < nlond; ++i)
+            for (k = 0; k < nk; ++k) {
+                const long o = k + (long)nk * (i + (long)nlond * j);
+                const int t = dir == 0 ? i : j;
+                if (t == 0 || t == n - 1) fm[o] = f[o];
+                else if (order == 2 && (t == 1 || t == n - 2)) fm[o] = (f[o + s] + f[o - s]) / 2.;
+                else fm[o] = (f[o + order * s] + f[o - order * s]) / 2.;
+            }
+}
+
+/* advec_ng (src/advec_ng.F90:1-52): hadvec = wk1/dlamda + wk2*re_inv/dphi  */
+/* with the fourth-order lon and lat advection terms; on the two ghost rows */
+/* of each boundary side the second-order term alone (:36-37, :47-48).      */
+/* racs (nlat+4) per latitude.                                              */
+ORACLE_API void oracle_advec_ng(const double *f, const double *un, const double *vn, const double *racs,
+                                double dlamda, double dphi, double re_inv, int nk, int nlon, int nlat,
+                                double *hadvec)
+{
+    const int nlond = nlon + 4, nlatd = nlat + 4;
+    const size_t n = (size_t)nk * nlond * nlatd;
+    double *w = (double *)malloc(sizeof(double) * 4 * n);
+    double *m1 = w, *m2 = w + n, *d1 = w + 2 * n, *d2 = w + 3 * n;
+    int k, i, j;
+    /* wk1 into hadvec */
+    hz_fm(un, m1, 1, 0, nk, nlond, nlatd);
+    hz_fm(un, m2, 2, 0, nk, nlond, nlatd);
+    hz_df(f, d1, 1, 0, nk, nlond, nlatd);
+    hz_df(f, d2, 2, 0, nk, nlond, nlatd);
+    for (j = 0; j < nlatd; ++j)
+        for (i = 0; i < nlond; ++i)
+            for (k = 0; k < nk; ++k) {
+                const long o = k + (long)nk * (i + (long)nlond * j);
+                double v = d1[o] * 2. * 2. / 3. * m1[o] - d2[o] * 4. / 12. * m2[o];
+                if (i <= 1 || i >= nlond - 2) v = d1[o] * m1[o];
+                hadvec[o] = v * racs[j];
+            }
+    /* wk2, combined */
+    hz_fm(vn, m1, 1, 1, nk, nlond, nlatd);
+    hz_fm(vn, m2, 2, 1, nk, nlond, nlatd);
+    hz_df(f, d1, 1, 1, nk, nlond, nlatd);
+    hz_df(f, d2, 2, 1, nk, nlond, nlatd);
+    for (j = 0; j < nlatd; ++j)
+        for (i = 0; i < nlond; ++i)
+            for (k = 0; k < nk; ++k) {
+                const long o = k + (long)nk * (i + (long)nlond * j);
+                double v = d1[o] * 2. * 2. / 3. * m1[o] - d2[o] * 4. / 12. * m2[o];
+                if (j <= 1 || j >= nlatd - 2) v = d1[o] * m1[o];
+                hadvec[o] = hadvec[o] / dlamda + v * re_inv / dphi;
+            }
+    free(w);
+}
+
+/* smooth_ng (src/smooth_ng.F90:1-42): the Shapiro filter in lat, then in   */
+/* lon, each with the 3-point form one row in from a boundary and the input */
+/* kept on the outermost ghost row.                                          */
+ORACLE_API void oracle_smooth_ng(const double *fin, double shapiro, int nk, int nlon, int nlat, double *fout)
+{
+    const int nlond = nlon + 4, nlatd = nlat + 4;
+    const size_t n = (size_t)nk * nlond * nlatd;
+    double *w = (double *)malloc(sizeof(double) * 3 * n);
+    double *m1 = w, *m2 = w + n, *ft = w + 2 * n;
+    int k, i, j;
+    hz_fm(fin, m1, 1, 1, nk, nlond, nlatd);
+    hz_fm(fin, m2, 2, 1, nk, nlond, nlatd);
+    for (j = 0; j < nlatd; ++j)
+        for (i = 0; i < nlond; ++i)
+            for (k = 0; k < nk; ++k) {
+                const long o = k + (long)nk * (i + (long)nlond * j);
+                if (j == 0 || j == nlatd - 1) ft[o] = fin[o];
+                else if (j == 1 || j == nlatd - 2) ft[o] = fin[o] - shapiro * (-8. * m1[o] + 8. * fin[o]);
+                else ft[o] = fin[o] - shapiro * (2. * m2[o] - 8. * m1[o] + 6. * fin[o]);
+            }
+    hz_fm(ft, m1, 1, 0, nk, nlond, nlatd);
+    hz_fm(ft, m2, 2, 0, nk, nlond, nlatd);
+    for (j = 0; j < nlatd; ++j)
+        for (i = 0; i < nlond; ++i)
+            for (k = 0; k < nk; ++k) {
+                const long o = k + (long)nk * (i + (long)nlond * j);
+                if (i == 0 || i == nlond - 1) fout[o] = ft[o];
+                else if (i == 1 || i == nlond - 2) fout[o] = ft[o] - shapiro * (-8. * m1[o] + 8. * ft[o]);
+                else fout[o] = ft[o] - shapiro * (2. * m2[o] - 8. * m1[o] + 6. * ft[o]);
+            }
+    free(w);
+}

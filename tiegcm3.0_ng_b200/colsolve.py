@@ -39,7 +39,7 @@ LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
 EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor_ng_dev", "tg_comp_ng",
-           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
+           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_advec_ng", "tg_advec_ng_dev", "tg_smooth_ng", "tg_smooth_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
@@ -206,6 +206,10 @@ def lib():
             "tg_comp_post_ng": [P] * 8 + [D, D, D, I, I] + [P] * 6,
             "tg_time_filter_ng": [I, P, P, D, D, I, I, P, P],
             "tg_time_filter_ng_dev": [I, P, P, D, D, I, I, Lg, P, P, P],
+            "tg_advec_ng": [P, P, P, P, D, D, D, I, I, I, P],
+            "tg_advec_ng_dev": [P, P, P, P, D, D, D, P, I, I, I, Lg, P],
+            "tg_smooth_ng": [P, D, I, I, I, P],
+            "tg_smooth_ng_dev": [P, D, P, I, I, I, Lg, P],
             "tg_minor_ng_dev": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, I, I, Lg, P, P, P],
             "tg_dt_ng_dev": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I, Lg, P, P, P],
             "tg_trsolv_ng": [P, P, P, P, P, I, I, I],
@@ -504,6 +508,37 @@ def time_filter_ng_dev(which, cur, prev, dtsmooth, dtsmooth_div2, upd, nm_out, n
     rc = lib().tg_time_filter_ng_dev(int(which), _dptr(cur), _dptr(prev), float(dtsmooth), float(dtsmooth_div2), nk,
                                      ncol, ld, _dptr(upd), _dptr(nm_out), _stream(stream))
     return _check(rc, "tg_time_filter_ng_dev", numeric_ok=False)
+
+
+def advec_ng(f, un, vn, racs, dlamda, dphi, re_inv, hadvec):
+    """advec_ng (src/advec_ng.F90) for a nest held as one subdomain: f, un, vn
+    and hadvec are (nk, nlon+4, nlat+4) Fortran arrays, racs (nlat+4)."""
+    nk, nlond, nlatd = f.shape
+    r = np.ascontiguousarray(racs, dtype=np.float64)
+    rc = lib().tg_advec_ng(_host(f, "f"), _host(un, "un"), _host(vn, "vn"), r.ctypes.data, float(dlamda),
+                           float(dphi), float(re_inv), nk, nlond - 4, nlatd - 4, _out(hadvec, "hadvec"))
+    return _check(rc, "tg_advec_ng", numeric_ok=False)
+
+
+def smooth_ng(fin, shapiro, fout):
+    """smooth_ng (src/smooth_ng.F90) for a nest held as one subdomain; fin and
+    fout are (nk, nlon+4, nlat+4) Fortran arrays."""
+    nk, nlond, nlatd = fin.shape
+    rc = lib().tg_smooth_ng(_host(fin, "fin"), float(shapiro), nk, nlond - 4, nlatd - 4, _out(fout, "fout"))
+    return _check(rc, "tg_smooth_ng", numeric_ok=False)
+
+
+def advec_ng_dev(f, un, vn, racs, dlamda, dphi, re_inv, hadvec, nk, nlon, nlat, ld, stream=None):
+    """Device form of advec_ng on level-major planes (k*ld + i + (nlon+4)*j)."""
+    rc = lib().tg_advec_ng_dev(_dptr(f), _dptr(un), _dptr(vn), _dptr(racs), float(dlamda), float(dphi),
+                               float(re_inv), _dptr(hadvec), nk, nlon, nlat, ld, _stream(stream))
+    return _check(rc, "tg_advec_ng_dev", numeric_ok=False)
+
+
+def smooth_ng_dev(fin, shapiro, fout, nk, nlon, nlat, ld, stream=None):
+    """Device form of smooth_ng on level-major planes (k*ld + i + (nlon+4)*j)."""
+    rc = lib().tg_smooth_ng_dev(_dptr(fin), float(shapiro), _dptr(fout), nk, nlon, nlat, ld, _stream(stream))
+    return _check(rc, "tg_smooth_ng_dev", numeric_ok=False)
 
 
 def minor_ng_dev(fields, consts, out, nk, ncol, ld, system_out=None, status=None, stream=None):

@@ -979,6 +979,106 @@ __attribute__((visibility("default"))) int tg_comp_post_ng(const double *o2, con
     return TG_OK;
 }
 
+static bool horiz_args_ok(const char *who, int nk, int nlon, int nlat, long ld, bool ld_given)
+{
+    const long ncol = (long)(nlon + 4) * (nlat + 4);
+    const bool ok = nk >= 1 && nk <= 65535 && nlon >= 1 && nlat >= 1 && nlon <= (1 << 24) && nlat <= 500000 &&
+                    (!ld_given || ld >= ncol);
+    if (!ok) set_err("%s: bad arguments (nk=%d nlon=%d nlat=%d ld=%ld)", who, nk, nlon, nlat, ld);
+    return ok;
+}
+
+__attribute__((visibility("default"))) int tg_advec_ng_dev(const double *f, const double *un, const double *vn,
+                                                           const double *racs, double dlamda, double dphi,
+                                                           double re_inv, double *hadvec, int nk, int nlon,
+                                                           int nlat, long ld, void *stream)
+{
+    if (!f || !un || !vn || !racs || !hadvec || hadvec == f || hadvec == un || hadvec == vn) {
+        set_err("tg_advec_ng_dev: a pointer is NULL or hadvec aliases an input");
+        return TG_EINVAL;
+    }
+    if (!horiz_args_ok("tg_advec_ng_dev", nk, nlon, nlat, ld, true)) return TG_EINVAL;
+    TG_CUDA(launch_advec_ng(f, un, vn, racs, dlamda, dphi, re_inv, nk, nlon, nlat, ld, hadvec,
+                            (cudaStream_t)stream));
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_smooth_ng_dev(const double *fin, double shapiro, double *fout, int nk,
+                                                            int nlon, int nlat, long ld, void *stream)
+{
+    if (!fin || !fout || fin == fout) {
+        set_err("tg_smooth_ng_dev: a pointer is NULL or fout is fin");
+        return TG_EINVAL;
+    }
+    if (!horiz_args_ok("tg_smooth_ng_dev", nk, nlon, nlat, ld, true)) return TG_EINVAL;
+    TG_CUDA(launch_smooth_ng(fin, shapiro, nk, nlon, nlat, ld, fout, (cudaStream_t)stream));
+    return TG_OK;
+}
+
+// Host forms: the (nk, nlon+4, nlat+4) Fortran arrays are (nk, ncol) column
+// arrays, relaid out to level-major planes for the kernels and back.
+__attribute__((visibility("default"))) int tg_advec_ng(const double *f, const double *un, const double *vn,
+                                                       const double *racs, double dlamda, double dphi,
+                                                       double re_inv, int nk, int nlon, int nlat, double *hadvec)
+{
+    if (!f || !un || !vn || !racs || !hadvec || hadvec == f || hadvec == un || hadvec == vn) {
+        set_err("tg_advec_ng: a pointer is NULL or hadvec aliases an input");
+        return TG_EINVAL;
+    }
+    if (!horiz_args_ok("tg_advec_ng", nk, nlon, nlat, 0, false)) return TG_EINVAL;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ncol = (long)(nlon + 4) * (nlat + 4), ld = round_up(ncol, 32);
+    const size_t lvl = (size_t)nk * ld, colsz = (size_t)nk * ncol;
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (4 * lvl + (size_t)(nlat + 4))))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * colsz))) return rc;
+    double *base = (double *)c->lvlbuf[0][0].p, *stage = (double *)c->colbuf[0][0].p;
+    cudaStream_t st = c->st[0];
+    const double *in3[3] = {f, un, vn};
+    for (int i = 0; i < 3; ++i) {
+        TG_CUDA(cudaMemcpyAsync(stage, in3[i], sizeof(double) * colsz, cudaMemcpyHostToDevice, st));
+        TG_CUDA(launch_col_to_level(stage, nk, base + i * lvl, ld, nk, ncol, st));
+    }
+    double *out = base + 3 * lvl, *dr = base + 4 * lvl;
+    TG_CUDA(cudaMemcpyAsync(dr, racs, sizeof(double) * (nlat + 4), cudaMemcpyHostToDevice, st));
+    TG_CUDA(launch_advec_ng(base, base + lvl, base + 2 * lvl, dr, dlamda, dphi, re_inv, nk, nlon, nlat, ld, out, st));
+    TG_CUDA(launch_level_to_col(out, ld, stage, nk, nk, ncol, st));
+    TG_CUDA(cudaMemcpyAsync(hadvec, stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_smooth_ng(const double *fin, double shapiro, int nk, int nlon, int nlat,
+                                                        double *fout)
+{
+    if (!fin || !fout || fin == fout) {
+        set_err("tg_smooth_ng: a pointer is NULL or fout is fin");
+        return TG_EINVAL;
+    }
+    if (!horiz_args_ok("tg_smooth_ng", nk, nlon, nlat, 0, false)) return TG_EINVAL;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ncol = (long)(nlon + 4) * (nlat + 4), ld = round_up(ncol, 32);
+    const size_t lvl = (size_t)nk * ld, colsz = (size_t)nk * ncol;
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * 2 * lvl))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * colsz))) return rc;
+    double *base = (double *)c->lvlbuf[0][0].p, *stage = (double *)c->colbuf[0][0].p;
+    cudaStream_t st = c->st[0];
+    TG_CUDA(cudaMemcpyAsync(stage, fin, sizeof(double) * colsz, cudaMemcpyHostToDevice, st));
+    TG_CUDA(launch_col_to_level(stage, nk, base, ld, nk, ncol, st));
+    TG_CUDA(launch_smooth_ng(base, shapiro, nk, nlon, nlat, ld, base + lvl, st));
+    TG_CUDA(launch_level_to_col(base + lvl, ld, stage, nk, nk, ncol, st));
+    TG_CUDA(cudaMemcpyAsync(fout, stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    return TG_OK;
+}
+
 static bool time_filter_args_ok(const char *who, int which, const double *cur, const double *prev, int nk, int ncol,
                                 const double *upd, const double *nm)
 {

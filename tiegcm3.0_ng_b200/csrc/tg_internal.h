@@ -180,6 +180,13 @@ size_t comp_scratch_doubles(int nk, long ld);
 cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, double dz, double dtsmooth,
                                 double dtsmooth_div2, int nk, int ncol, long ld, double *const *upd6,
                                 cudaStream_t st);
+// advec_ng / smooth_ng on one nest held as a single subdomain (tg_horiz.cu):
+// level-major planes (k, i, j) at k*ld + i + (nlon+4)*j
+cudaError_t launch_advec_ng(const double *f, const double *un, const double *vn, const double *racs, double dlamda,
+                            double dphi, double re_inv, int nk, int nlon, int nlat, long ld, double *hadvec,
+                            cudaStream_t st);
+cudaError_t launch_smooth_ng(const double *fin, double shapiro, int nk, int nlon, int nlat, long ld, double *fout,
+                             cudaStream_t st);
 // post-solve time filter and floor of dt_ng / minor_ng / oplus_ng (which =
 // TG_FILTER_*) over rows of len elements at stride ld
 cudaError_t launch_time_filter(int which, const double *cur, const double *prev, double dtsmooth,

@@ -183,6 +183,26 @@ module tg_colsolve_mod
       real(c_double), intent(inout) :: upd(*), nm_upd(*)
     end function tg_time_filter_ng
 
+    ! advec_ng / smooth_ng (src/advec_ng.F90, src/smooth_ng.F90) for a nest
+    ! held as one subdomain: f, un, vn, hadvec, fin, fout (nk, lond0:lond1,
+    ! latd0:latd1), racs (latd0:latd1)
+    integer(c_int) function tg_advec_ng(f, un, vn, racs, dlamda, dphi, re_inv, nk, nlon, nlat, hadvec) &
+        bind(C, name="tg_advec_ng")
+      import :: c_int, c_double
+      real(c_double), intent(in) :: f(*), un(*), vn(*), racs(*)
+      real(c_double), value :: dlamda, dphi, re_inv
+      integer(c_int), value :: nk, nlon, nlat
+      real(c_double), intent(inout) :: hadvec(*)
+    end function tg_advec_ng
+
+    integer(c_int) function tg_smooth_ng(fin, shapiro, nk, nlon, nlat, fout) bind(C, name="tg_smooth_ng")
+      import :: c_int, c_double
+      real(c_double), intent(in) :: fin(*)
+      real(c_double), value :: shapiro
+      integer(c_int), value :: nk, nlon, nlat
+      real(c_double), intent(inout) :: fout(*)
+    end function tg_smooth_ng
+
     integer(c_int) function tg_settei_ng(fl, cn, te_out, ti_out, qtotal, nk, ncol) bind(C, name="tg_settei_ng")
       import :: c_int, c_double, tg_settei_fields, tg_settei_consts
       type(tg_settei_fields), intent(in) :: fl
