@@ -15,6 +15,8 @@
 // operations.  Divisions by 2 and 4 are written as multiplications by 0.5
 // and 0.25 (the same correctly rounded number); divisions by 3, 12, dlamda
 // and dphi are correctly rounded (qdiv with the reciprocal from the host).
+#include <cmath>
+
 #include "tg_internal.h"
 #include "tg_arith.cuh"
 
@@ -23,47 +25,40 @@ namespace {
 
 constexpr int kTx = 32, kTy = 8;
 
-// a point's index along one axis, the axis extent and the element stride
-struct Axis {
-    int t, n;
-    long s;
-};
-
-// fm_3d (src/dffm_ng.F90:166-205): the centred mean over +-O points, the
-// input itself on the edge rows, the +-1 mean on the rows next to them (O=2).
-template <int O>
-__device__ __forceinline__ double fm_at(const double *p, Axis a)
-{
-    if (a.t == 0 || a.t == a.n - 1) return __ldg(p);
-    const long d = (O == 2 && (a.t == 1 || a.t == a.n - 2)) ? a.s : O * a.s;
-    return xmul(xadd(__ldg(p + d), __ldg(p - d)), 0.5);
-}
-
-// df_3d (src/dffm_ng.F90:66-110): the centred difference over 2*O spacings,
-// one-sided on the edge rows, over 2 spacings on the rows next to them (O=2).
-template <int O>
-__device__ __forceinline__ double df_at(const double *p, Axis a)
-{
-    if (a.t == 0) return xsub(__ldg(p + a.s), __ldg(p));
-    if (a.t == a.n - 1) return xsub(__ldg(p), __ldg(p - a.s));
-    if (O == 2 && (a.t == 1 || a.t == a.n - 2)) return xmul(xsub(__ldg(p + a.s), __ldg(p - a.s)), 0.5);
-    return xmul(xsub(__ldg(p + O * a.s), __ldg(p - O * a.s)), O == 1 ? 0.5 : 0.25);
-}
-
 struct AdvecRcp {
     double r3, r12, rlam, rphi;  // correctly rounded 1/3, 1/12, 1/dlamda, 1/dphi
+    int lam_safe, phi_safe;      // dlamda, dphi inside the Markstein range
 };
 
-// One direction of advec_ng (:33-37 lon, :44-48 lat): the fourth-order term
-// dfdx1*2*2/3*ubar1 - dfdx2*4/12*ubar2, and dfdx1*ubar1 on the two ghost
-// rows of a boundary side.  (d*2)*2 is d*4 exactly.
-__device__ __forceinline__ double advec_dir(const double *f, const double *u, Axis a, const AdvecRcp &rc)
+// a/b correctly rounded, y the reciprocal of b, b known to be in range
+__device__ __forceinline__ double qdiv_by(double a, double b, double y, bool b_safe)
 {
-    const double d1 = df_at<1>(f, a), m1 = fm_at<1>(u, a);
-    if (a.t <= 1 || a.t >= a.n - 2) return xmul(d1, m1);
-    const double d2 = df_at<2>(f, a), m2 = fm_at<2>(u, a);
-    const double lhs = xmul(qdiv(xmul(d1, 4.0), 3.0, rc.r3), m1);
-    const double rhs = xmul(qdiv(xmul(d2, 4.0), 12.0, rc.r12), m2);
+    return b_safe && exp_safe(a) ? div_markstein(a, b, y) : __ddiv_rn(a, b);
+}
+
+// One direction of advec_ng (:33-37 lon, :44-48 lat) at index t of an axis
+// of n points with element stride s (p: the field, u: the wind, both at the
+// point).  df_3d and fm_3d (src/dffm_ng.F90:66-110, :166-205) of order 1 are
+// (p[+1]-p[-1])/2 and (u[+1]+u[-1])/2 inside, and on the edge rows the
+// one-sided difference and the value itself; with the neighbour indices
+// clamped into the axis, p[+1]-p[-1] is the one-sided difference there.  The
+// term is dfdx1*2*2/3*ubar1 - dfdx2*4/12*ubar2 on rows 2..n-3 (where the
+// order-2 helpers take their centred form) and dfdx1*ubar1 on the two ghost
+// rows of each boundary side.  (d*2)*2 is d*4 exactly; x/2 and x/4 are the
+// same numbers as x*0.5 and x*0.25.
+__device__ __forceinline__ double advec_dir(const double *p, const double *u, int t, int n, int s,
+                                            const AdvecRcp &rc)
+{
+    const int dm = t > 0 ? -s : 0, dp = t < n - 1 ? s : 0;
+    const bool edge = t == 0 || t == n - 1;
+    const double dif = xsub(__ldg(p + dp), __ldg(p + dm));
+    const double d1 = edge ? dif : xmul(dif, 0.5);
+    const double m1 = edge ? __ldg(u) : xmul(xadd(__ldg(u + dp), __ldg(u + dm)), 0.5);
+    if (t <= 1 || t >= n - 2) return xmul(d1, m1);
+    const double d2 = xmul(xsub(__ldg(p + 2 * s), __ldg(p - 2 * s)), 0.25);
+    const double m2 = xmul(xadd(__ldg(u + 2 * s), __ldg(u - 2 * s)), 0.5);
+    const double lhs = xmul(qdiv_by(xmul(d1, 4.0), 3.0, rc.r3, true), m1);
+    const double rhs = xmul(qdiv_by(xmul(d2, 4.0), 12.0, rc.r12, true), m2);
     return xsub(lhs, rhs);
 }
 
@@ -75,48 +70,49 @@ __global__ void __launch_bounds__(kTx * kTy) k_advec_ng(const double *f, const d
     const int i = blockIdx.x * kTx + threadIdx.x, j = blockIdx.y * kTy + threadIdx.y;
     if (i >= nlond || j >= nlatd) return;
     const long o = (long)blockIdx.z * ld + i + (long)nlond * j;
-    const double wk1 = xmul(advec_dir(f + o, un + o, Axis{i, nlond, 1}, rc), __ldg(racs + j));
-    const double wk2 = advec_dir(f + o, vn + o, Axis{j, nlatd, nlond}, rc);
+    const double wk1 = xmul(advec_dir(f + o, un + o, i, nlond, 1, rc), __ldg(racs + j));
+    const double wk2 = advec_dir(f + o, vn + o, j, nlatd, nlond, rc);
     // hadvec = wk1/dlamda + wk2*re_inv/dphi (:50)
-    hadvec[o] = xadd(qdiv(wk1, dlamda, rc.rlam), qdiv(xmul(wk2, re_inv), dphi, rc.rphi));
+    hadvec[o] = xadd(qdiv_by(wk1, dlamda, rc.rlam, rc.lam_safe), qdiv_by(xmul(wk2, re_inv), dphi, rc.rphi, rc.phi_safe));
 }
 
-// One Shapiro pass of smooth_ng along an axis (lat :18-29, lon :31-42):
-// x - sh*(2*fm2 - 8*fm1 + 6*x) inside, x - sh*(-8*fm1 + 8*x) one row in from
-// a boundary (written 8*x - 8*fm1, the same rounded number), x on the
-// outermost ghost row.
-template <class Load>
-__device__ __forceinline__ double shapiro_at(Load ld, int t, int n, double sh)
+// One Shapiro pass of smooth_ng along an axis (lat :18-29, lon :31-42) at
+// index t of n points, stride s: x - sh*(2*fm2 - 8*fm1 + 6*x) inside,
+// x - sh*(-8*fm1 + 8*x) one row in from a boundary (written 8*x - 8*fm1,
+// the same rounded number), x on the outermost ghost row.  Where they are
+// used, fm1 and fm2 are the plain +-1 and +-2 means.
+__device__ __forceinline__ double shapiro_at(const double *p, int t, int n, int s, double sh)
 {
-    const double x = ld(0);
+    const double x = p[0];
     if (t == 0 || t == n - 1) return x;
-    const double m1 = xmul(xadd(ld(1), ld(-1)), 0.5);
+    const double m1 = xmul(xadd(p[s], p[-s]), 0.5);
     if (t == 1 || t == n - 2) return xsub(x, xmul(sh, xsub(xmul(8.0, x), xmul(8.0, m1))));
-    const double m2 = xmul(xadd(ld(2), ld(-2)), 0.5);
+    const double m2 = xmul(xadd(p[2 * s], p[-2 * s]), 0.5);
     return xsub(x, xmul(sh, xadd(xsub(xmul(2.0, m2), xmul(8.0, m1)), xmul(6.0, x))));
 }
 
 // The lat pass lands in a shared tile of the block's 8 rows x (32 + 4)
-// longitudes (the lon pass needs +-2 neighbours), then the lon pass reads it.
+// longitudes (the lon pass needs +-2 neighbours): its 288 points are dealt
+// to the 256 threads in order, so only one warp takes a second point.  Then
+// the lon pass reads the tile.
 __global__ void __launch_bounds__(kTx * kTy) k_smooth_ng(const double *fin, double sh, int nlond, int nlatd,
                                                         long ld, double *fout)
 {
-    __shared__ double ft[kTy][kTx + 4 + 1];
-    const int i0 = blockIdx.x * kTx, j = blockIdx.y * kTy + threadIdx.y;
+    constexpr int W = kTx + 4;
+    __shared__ double ft[kTy][W + 1];
+    const int i0 = blockIdx.x * kTx, j0 = blockIdx.y * kTy;
     const double *plane = fin + (long)blockIdx.z * ld;
-    if (j < nlatd) {
-        for (int c = threadIdx.x; c < kTx + 4; c += kTx) {
-            const int i = i0 - 2 + c;
-            if (i < 0 || i >= nlond) continue;
-            const double *p = plane + i + (long)nlond * j;
-            ft[threadIdx.y][c] = shapiro_at([&](int d) { return __ldg(p + (long)d * nlond); }, j, nlatd, sh);
-        }
+    for (int q = threadIdx.y * kTx + threadIdx.x; q < W * kTy; q += kTx * kTy) {
+        const int r = q / W, c = q - r * W;
+        const int i = i0 - 2 + c, j = j0 + r;
+        if (i < 0 || i >= nlond || j >= nlatd) continue;
+        ft[r][c] = shapiro_at(plane + i + (long)nlond * j, j, nlatd, nlond, sh);
     }
     __syncthreads();
-    const int i = i0 + threadIdx.x;
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
     if (i >= nlond || j >= nlatd) return;
-    const double *row = &ft[threadIdx.y][threadIdx.x + 2];
-    fout[(long)blockIdx.z * ld + i + (long)nlond * j] = shapiro_at([&](int d) { return row[d]; }, i, nlond, sh);
+    // every longitude the lon pass reads (i-2..i+2 where used) is in the tile
+    fout[(long)blockIdx.z * ld + i + (long)nlond * j] = shapiro_at(&ft[threadIdx.y][threadIdx.x + 2], i, nlond, 1, sh);
 }
 
 dim3 plane_grid(int nk, int nlond, int nlatd)
@@ -132,7 +128,8 @@ cudaError_t launch_advec_ng(const double *f, const double *un, const double *vn,
 {
     const int nlond = nlon + 4, nlatd = nlat + 4;
     // host IEEE division: the correctly rounded reciprocals the Markstein step needs
-    const AdvecRcp rc{1.0 / 3.0, 1.0 / 12.0, 1.0 / dlamda, 1.0 / dphi};
+    auto in_range = [](double b) { return std::fabs(b) >= 0x1p-500 && std::fabs(b) < 0x1p500; };
+    const AdvecRcp rc{1.0 / 3.0, 1.0 / 12.0, 1.0 / dlamda, 1.0 / dphi, in_range(dlamda), in_range(dphi)};
     k_advec_ng<<<plane_grid(nk, nlond, nlatd), dim3(kTx, kTy), 0, st>>>(f, un, vn, racs, dlamda, dphi, re_inv, rc,
                                                                         nlond, nlatd, ld, hadvec);
     return cudaGetLastError();
