@@ -26,6 +26,8 @@ L2 flush is needed between steps.  --config 1 selects the global grid alone.
           bandwidth, algorithmic bytes = 40 B per scalar unknown.
   assembly  the fused assembly + solve kernels (dt_ng, minor_ng, comp_ng,
           settei_ng, oplus_ng) on 4 copies of the global grid.
+  horizontal  advec_ng, smooth_ng and the dt_ng post-solve time filter on the
+          576 x 288 x 113 grid held as one subdomain.
   cpu_baseline  the oracle port (C, OpenMP, all host threads) on full steps of
           the global grid.
 
@@ -67,7 +69,8 @@ def parse():
     p.add_argument("--profile", default=None,
                    help="run only one kind's plan for a profiler: KIND:PREC[:VARIANT], KIND scalar|block, "
                         "PREC f64|refine, VARIANT reg:CPB:CPT[:PF], regg:CPB:1[:PF], ring[g]:DEPTH[:WARPS] "
-                        "(default: library default); or dt / minor / comp / settei / oplus for the fused assembly+solve kernels")
+                        "(default: library default); or dt / minor / comp / settei / oplus for the fused assembly+solve kernels, "
+                        "advec / smooth / filter for the horizontal operators and the time filter")
     p.add_argument("--skip-assembly", action="store_true")
     return p.parse_args()
 
@@ -293,13 +296,61 @@ def assembly_setup(pkg, wl, which, dev, replicas=ASSEMBLY_REPLICAS):
     return launch, ncol, nbytes
 
 
+HORIZ_GRID = (113, 576, 288)   # levels, lon, lat: the 0.625-degree global grid, inputs > L2
+HORIZ_TAG = "576x288x113"
+EARTH_RADIUS_CM = 6.37122e8
+
+
+def horizontal_setup(pkg, which, dev):
+    """Device inputs of advec_ng, smooth_ng or the dt_ng time filter on the
+    576x288x113 grid held as one subdomain (level-major planes).  Returns
+    (launch(stream), points, algorithmic bytes per launch)."""
+    import torch
+    nk, nlon, nlat = HORIZ_GRID
+    ncol = (nlon + 4) * (nlat + 4)
+    ld = pkg.batch.pad_ld(ncol)
+    g = torch.Generator(device=dev).manual_seed(211)
+
+    def field(lo, hi):
+        return torch.rand((nk, ld), dtype=torch.float64, device=dev, generator=g) * (hi - lo) + lo
+
+    dlat = np.radians(180.0 / nlat)
+    dlon = np.radians(360.0 / nlon)
+    if which == "advec":
+        f, un, vn = field(150.0, 2000.0), field(-1.0e4, 1.0e4), field(-1.0e4, 1.0e4)
+        lat = -np.pi / 2 + dlat * (np.arange(nlat + 4) - 1.5)
+        racs = torch.from_numpy(1.0 / (EARTH_RADIUS_CM * np.maximum(np.cos(lat), 1e-3))).to(dev)
+        out = torch.empty_like(f)
+
+        def launch(stream):
+            pkg.advec_ng_dev(f, un, vn, racs, dlon, dlat, 1.0 / EARTH_RADIUS_CM, out, nk, nlon, nlat, ld,
+                             stream=stream)
+        return launch, nk * ncol, 8 * (4 * nk * ncol + nlat + 4)
+    if which == "smooth":
+        fin = field(150.0, 2000.0)
+        out = torch.empty_like(fin)
+
+        def launch(stream):
+            pkg.smooth_ng_dev(fin, 0.03, out, nk, nlon, nlat, ld, stream=stream)
+        return launch, nk * ncol, 16 * nk * ncol
+    cur, prev, upd = field(150.0, 2000.0), field(150.0, 2000.0), field(50.0, 2000.0)
+    nm = torch.empty_like(cur)
+
+    def launch(stream):
+        pkg.time_filter_ng_dev(pkg.TG_FILTER_DT, cur, prev, 0.95, 0.025, upd, nm, nk, ncol, ld, stream=stream)
+    return launch, nk * ncol, 40 * nk * ncol
+
+
 def run_profile(args):
     """Executes one kind's plan --warmup + --steps times (for ncu captures)."""
     import torch
     pkg = ge.load_package()
-    if args.profile in ("dt", "minor", "comp", "settei", "oplus"):
+    if args.profile in ("dt", "minor", "comp", "settei", "oplus", "advec", "smooth", "filter"):
         wl = pkg.synth.workload(args.config)
-        launch, ncol, nbytes = assembly_setup(pkg, wl, args.profile, "cuda")
+        if args.profile in ("advec", "smooth", "filter"):
+            launch, ncol, nbytes = horizontal_setup(pkg, args.profile, "cuda")
+        else:
+            launch, ncol, nbytes = assembly_setup(pkg, wl, args.profile, "cuda")
         stream = torch.cuda.Stream()
         for _ in range(args.warmup):
             launch(stream)
@@ -482,6 +533,35 @@ def main():
             del launch
         torch.cuda.empty_cache()
 
+    # ---- horizontal operators and the post-solve time filter, device-resident
+    horizontal = None
+    if not args.skip_assembly:
+        horizontal = {}
+        for which, name, kern in (("advec", "advec_ng", "k_advec_ng"), ("smooth", "smooth_ng", "k_smooth_ng"),
+                                  ("filter", "time_filter_ng", "k_time_filter")):
+            launch, npts, nbytes = horizontal_setup(pkg, which, dev)
+            for _ in range(args.warmup):
+                launch(stream)
+            stream.synchronize()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                launch(stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+            pk, _ = measured_peak()
+            ach = nbytes / (ms * 1e-3) / 1e9
+            horizontal[name] = {
+                "kernel": kern, "points": npts, "ms_per_launch": ms, "points_per_s": world * npts / (ms * 1e-3),
+                "algorithmic_bytes_per_launch": nbytes,
+                "roofline": {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
+                             "traffic": traffic_from_profiles(kern, HORIZ_TAG)},
+                "inputs": f"the {HORIZ_TAG} grid held as one subdomain, {nbytes / 1e6:.0f} MB > L2"}
+            del launch
+        torch.cuda.empty_cache()
+
     peak, peak_kind = measured_peak()
     bytes_scalar = dw.algorithmic_bytes((cs.TG_KIND_SCALAR,))
     wl_tag = f"{wl.name}_B{wl.block}"
@@ -612,6 +692,7 @@ def main():
                        "roofline": roofline("refine", "k_scalar_refine")},
             "kernel_ms": {k: v for k, v in results.items()},
             "assembly": assembly,
+            "horizontal": horizontal,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk,
