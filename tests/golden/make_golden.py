@@ -6,9 +6,17 @@ kat_*.npz    known-answer tests: integer-valued, diagonally dominant systems
              solver (the reference ships no golden vectors for this path).
 pin_*.npz    bitwise pins of the oracle on small seeded synthetic inputs, so a
              change of the oracle's arithmetic is noticed.
+kat_horizontal.npz  known answers of advec_ng and smooth_ng (src/advec_ng.F90,
+             src/smooth_ng.F90, src/dffm_ng.F90) on a small nest: fields that
+             are multiples of 3, integer winds and power-of-two
+             spacings and factors keep every intermediate an exactly
+             representable dyadic rational, so the answers are computed in
+             exact rational arithmetic, independently of floating point.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [name ...]
+(no names: every fixture; otherwise only the named files, e.g. kat_horizontal).
 """
+from fractions import Fraction
 import os
 import sys
 
@@ -49,7 +57,84 @@ def kat_block(rng, B, nk, ncol):
     return {k: np.asfortranarray(v.astype(np.float64)) for k, v in dict(P=P, Q=Q, R=R, f=f, u=u).items()}
 
 
-def main():
+def _fm(v, t, n, order):
+    """fm_3d along one axis in exact arithmetic; v(d) is the value d points away."""
+    if t == 0 or t == n - 1:
+        return v(0)
+    d = 1 if (order == 2 and t in (1, n - 2)) else order
+    return (v(d) + v(-d)) / 2
+
+
+def _df(v, t, n, order):
+    """df_3d along one axis in exact arithmetic."""
+    if t == 0:
+        return v(1) - v(0)
+    if t == n - 1:
+        return v(0) - v(-1)
+    if order == 2 and t in (1, n - 2):
+        return (v(1) - v(-1)) / 2
+    return (v(order) - v(-order)) / (2 * order)
+
+
+def kat_horizontal(rng, nk=3, nlon=7, nlat=5):
+    """advec_ng and smooth_ng on a single-subdomain nest, exact answers."""
+    nx, ny = nlon + 4, nlat + 4
+    f = 3 * rng.integers(-40, 41, size=(nk, nx, ny))
+    un = rng.integers(-9, 10, size=(nk, nx, ny))
+    vn = rng.integers(-9, 10, size=(nk, nx, ny))
+    racs = rng.integers(1, 16, size=ny)
+    racs_q = [Fraction(int(r), 1024) for r in racs]
+    dlamda, dphi, re_inv, shapiro = Fraction(1, 64), Fraction(1, 32), Fraction(1, 1024), Fraction(1, 32)
+    F = lambda a: [[[Fraction(int(a[k, i, j])) for j in range(ny)] for i in range(nx)] for k in range(nk)]  # noqa: E731
+    fq, uq, vq = F(f), F(un), F(vn)
+    had = np.zeros((nk, nx, ny))
+    fout = np.zeros((nk, nx, ny))
+
+    def exact(x):
+        y = float(x)
+        assert Fraction(y) == x, "a known answer is not representable"
+        return y
+
+    for k in range(nk):
+        for i in range(nx):
+            for j in range(ny):
+                def term(a, b, t, n, along_lon):
+                    va = (lambda d: a[k][i + d][j]) if along_lon else (lambda d: a[k][i][j + d])
+                    vb = (lambda d: b[k][i + d][j]) if along_lon else (lambda d: b[k][i][j + d])
+                    d1, m1 = _df(va, t, n, 1), _fm(vb, t, n, 1)
+                    if t <= 1 or t >= n - 2:
+                        return d1 * m1
+                    d2, m2 = _df(va, t, n, 2), _fm(vb, t, n, 2)
+                    return d1 * 2 * 2 / 3 * m1 - d2 * 4 / 12 * m2
+                wk1 = term(fq, uq, i, nx, True) * racs_q[j]
+                wk2 = term(fq, vq, j, ny, False)
+                had[k, i, j] = exact(wk1 / dlamda + wk2 * re_inv / dphi)
+        # smooth_ng: the lat pass, then the lon pass on its result
+        def shap(v, t, n):
+            x = v(0)
+            if t == 0 or t == n - 1:
+                return x
+            m1 = _fm(v, t, n, 1)
+            if t in (1, n - 2):
+                return x - shapiro * (-8 * m1 + 8 * x)
+            return x - shapiro * (2 * _fm(v, t, n, 2) - 8 * m1 + 6 * x)
+        tmp = [[shap(lambda d: fq[k][i][j + d], j, ny) for j in range(ny)] for i in range(nx)]
+        for i in range(nx):
+            for j in range(ny):
+                fout[k, i, j] = exact(shap(lambda d: tmp[i + d][j], i, nx))
+    return dict(f=np.asfortranarray(f.astype(np.float64)), un=np.asfortranarray(un.astype(np.float64)),
+                vn=np.asfortranarray(vn.astype(np.float64)), racs=racs.astype(np.float64) / 1024,
+                dlamda=float(dlamda), dphi=float(dphi), re_inv=float(re_inv), shapiro=float(shapiro),
+                hadvec=np.asfortranarray(had), fout=np.asfortranarray(fout))
+
+
+def main(names=()):
+    if names:
+        if "kat_horizontal" in names:
+            np.savez_compressed(os.path.join(HERE, "kat_horizontal.npz"),
+                                **kat_horizontal(np.random.default_rng(20261204)))
+        return
+    np.savez_compressed(os.path.join(HERE, "kat_horizontal.npz"), **kat_horizontal(np.random.default_rng(20261204)))
     rng = np.random.default_rng(20261203)
     out = {}
     for nk in (2, 3, 5, 29, 57):
@@ -79,4 +164,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

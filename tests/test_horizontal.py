@@ -5,6 +5,8 @@ independent numpy transcription and analytic properties, and the CUDA entries
 import numpy as np
 import pytest
 
+from conftest import golden
+
 RE_INV = 1.0 / 6.37122e8   # 1/re, re in cm
 SHAPIRO = 3.0e-2
 
@@ -175,3 +177,28 @@ def test_horizontal_rejects_bad_arguments(pkg):
     assert L.tg_smooth_ng_dev(8, SHAPIRO, 16, 3, 0, 1, 64, None) == pkg.TG_EINVAL       # nlon < 1
     assert L.tg_smooth_ng_dev(8, SHAPIRO, 16, 3, 1, 1, 20, None) == pkg.TG_EINVAL       # ld < 25 columns
     assert L.tg_advec_ng_dev(8, 16, 24, 32, 0.01, 0.01, RE_INV, 40, 70000, 1, 1, 64, None) == pkg.TG_EINVAL
+
+
+def _kat():
+    g = golden("kat_horizontal.npz")
+    return {k: g[k] for k in g.files}
+
+
+def test_oracle_known_answers(orc):
+    """Exact answers computed in rational arithmetic (tests/golden/make_golden.py)."""
+    g = _kat()
+    h = orc.advec_ng(g["f"], g["un"], g["vn"], g["racs"], float(g["dlamda"]), float(g["dphi"]), float(g["re_inv"]))
+    assert np.array_equal(h, g["hadvec"])
+    assert np.array_equal(orc.smooth_ng(g["f"], float(g["shapiro"])), g["fout"])
+
+
+@pytest.mark.gpu
+def test_known_answers_on_gpu(cuda, pkg):
+    g = _kat()
+    h = np.zeros_like(g["f"], order="F")
+    assert pkg.advec_ng(g["f"], g["un"], g["vn"], g["racs"], float(g["dlamda"]), float(g["dphi"]),
+                        float(g["re_inv"]), h) == pkg.TG_OK
+    assert np.array_equal(h, g["hadvec"])
+    s = np.zeros_like(g["f"], order="F")
+    assert pkg.smooth_ng(g["f"], float(g["shapiro"]), s) == pkg.TG_OK
+    assert np.array_equal(s, g["fout"])
