@@ -82,3 +82,30 @@ def test_tuning_entries_validate_without_device(pkg):
     assert L.tg_set_pipeline(pkg.TG_KIND_SCALAR, pkg.TG_PREC_F32_REFINE, 8, 1) == pkg.TG_EINVAL
     assert L.tg_set_pipeline(pkg.TG_KIND_BLOCK2, pkg.TG_PREC_F32_REFINE, 3, 1) == pkg.TG_EINVAL
     assert L.tg_set_pipeline(pkg.TG_KIND_SCALAR, pkg.TG_PREC_F32_REFINE, -1, 0) == pkg.TG_OK
+
+
+def header_arity():
+    """Number of parameters of each declared entry point."""
+    txt = open(os.path.join(ROOT, "include", "tg_colsolve.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    out = {}
+    for m in re.finditer(r"^\s*(?:int|const char \*)\s*(tg_\w+)\s*\(([^;]*?)\)\s*;", txt, re.M | re.S):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_fortran_binding_matches_header():
+    """The ISO_C_BINDING module (not compilable here: no Fortran compiler)
+    binds only exported names, each with the header's parameter count."""
+    src = open(os.path.join(ROOT, "tiegcm3.0_ng_b200", "fortran", "tg_colsolve_mod.F90")).read()
+    src = re.sub(r"!.*", "", src)
+    src = re.sub(r"&\s*\n\s*", " ", src)
+    arity = header_arity()
+    found = re.findall(r"function\s+(\w+)\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)", src, re.I)
+    assert len(found) >= 15
+    for fname, args, cname in found:
+        assert fname == cname, (fname, cname)
+        assert cname in arity, cname
+        nargs = 0 if not args.strip() else args.count(",") + 1
+        assert nargs == arity[cname], (cname, nargs, arity[cname])
