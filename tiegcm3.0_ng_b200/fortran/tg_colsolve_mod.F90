@@ -13,6 +13,25 @@ module tg_colsolve_mod
     TG_ENOCONV = 4, TG_ETIMEOUT = 5, TG_ECUDA = 6, TG_ENOMEM = 7, TG_ENODEV = 8
   integer(c_int), parameter :: TG_PREC_F64 = 0, TG_PREC_F32_REFINE = 1
   integer(c_int), parameter :: TG_FILTER_DT = 0, TG_FILTER_MINOR = 1, TG_FILTER_OPLUS = 2
+  integer(c_int), parameter :: TG_LAYOUT_COLUMN = 0, TG_LAYOUT_LEVEL = 1
+  integer(c_int), parameter :: TG_KIND_SCALAR = 0, TG_KIND_BLOCK2 = 2, TG_KIND_BLOCK3 = 3
+
+  ! One system of a batched host call (tg_solve_host): c_loc() of the
+  ! Fortran arrays, block systems with P, Q, R in a, b, c and u in x.
+  type, bind(C) :: tg_host_system
+    integer(c_int) :: kind, nk, k2, ncol
+    type(c_ptr) :: a = c_null_ptr, b = c_null_ptr, c = c_null_ptr, f = c_null_ptr, x = c_null_ptr
+    type(c_ptr) :: ubc_ratio = c_null_ptr, ubc_add = c_null_ptr
+  end type tg_host_system
+
+  ! One segment of a GPU-resident plan: device pointers (CUDA Fortran
+  ! c_devloc, OpenACC host_data use_device), level-major with stride ld.
+  type, bind(C) :: tg_segment
+    integer(c_int) :: kind, nk, k2, ncol
+    integer(c_long) :: ld
+    type(c_ptr) :: a = c_null_ptr, b = c_null_ptr, c = c_null_ptr, f = c_null_ptr, x = c_null_ptr
+    type(c_ptr) :: ubc_ratio = c_null_ptr, ubc_add = c_null_ptr
+  end type tg_segment
 
   ! Field tables of the fused assembly + solve entries: c_loc() of each
   ! Fortran array (3-D fields (nk, ncol), 2-D (ncol), level profiles (nk)),
@@ -137,6 +156,65 @@ module tg_colsolve_mod
     integer(c_int) function tg_release_buffers() bind(C, name="tg_release_buffers")
       import :: c_int
     end function tg_release_buffers
+
+    ! every system of a step in one call (host arrays, pipelined copies)
+    integer(c_int) function tg_solve_host(sys, nsys) bind(C, name="tg_solve_host")
+      import :: c_int, tg_host_system
+      type(tg_host_system), intent(in) :: sys(*)
+      integer(c_int), value :: nsys
+    end function tg_solve_host
+
+    ! device pointers, stream-ordered; status_dev and stream may be c_null_ptr
+    integer(c_int) function tg_trsolv_dev(a, b, c, f, x, nk, k2, ncol, layout, ld, precision, status_dev, &
+        stream) bind(C, name="tg_trsolv_dev")
+      import :: c_int, c_long, c_ptr
+      type(c_ptr), value :: a, b, c, f, x, status_dev, stream
+      integer(c_int), value :: nk, k2, ncol, layout, precision
+      integer(c_long), value :: ld
+    end function tg_trsolv_dev
+
+    integer(c_int) function tg_blksolve_dev(nb, p, q, r, f, ubc_ratio, ubc_add, u, nk, k2, ncol, layout, ld, &
+        precision, status_dev, stream) bind(C, name="tg_blksolve_dev")
+      import :: c_int, c_long, c_ptr
+      integer(c_int), value :: nb, nk, k2, ncol, layout, precision
+      type(c_ptr), value :: p, q, r, f, ubc_ratio, ubc_add, u, status_dev, stream
+      integer(c_long), value :: ld
+    end function tg_blksolve_dev
+
+    ! GPU-resident plans over many segments (one persistent launch per kind)
+    integer(c_int) function tg_plan_create(segs, nseg, precision, plan) bind(C, name="tg_plan_create")
+      import :: c_int, c_ptr, tg_segment
+      type(tg_segment), intent(in) :: segs(*)
+      integer(c_int), value :: nseg, precision
+      type(c_ptr), intent(out) :: plan
+    end function tg_plan_create
+
+    integer(c_int) function tg_plan_execute(plan, stream) bind(C, name="tg_plan_execute")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: plan, stream
+    end function tg_plan_execute
+
+    integer(c_int) function tg_plan_capture_graph(plan, stream) bind(C, name="tg_plan_capture_graph")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: plan, stream
+    end function tg_plan_capture_graph
+
+    integer(c_int) function tg_plan_status(plan, per_segment_status) bind(C, name="tg_plan_status")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: plan
+      integer(c_int), intent(out) :: per_segment_status(*)
+    end function tg_plan_status
+
+    integer(c_int) function tg_plan_destroy(plan) bind(C, name="tg_plan_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: plan
+    end function tg_plan_destroy
+
+    integer(c_int) function tg_set_refine(max_sweeps, rel_tol) bind(C, name="tg_set_refine")
+      import :: c_int, c_double
+      integer(c_int), value :: max_sweeps
+      real(c_double), value :: rel_tol
+    end function tg_set_refine
     ! fused column assembly + solve (host arrays, Fortran layout)
     integer(c_int) function tg_dt_ng(fl, cn, tn_upd, nk, ncol) bind(C, name="tg_dt_ng")
       import :: c_int, c_double, tg_dt_fields, tg_dt_consts
