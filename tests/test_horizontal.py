@@ -202,3 +202,17 @@ def test_known_answers_on_gpu(cuda, pkg):
     s = np.zeros_like(g["f"], order="F")
     assert pkg.smooth_ng(g["f"], float(g["shapiro"]), s) == pkg.TG_OK
     assert np.array_equal(s, g["fout"])
+
+
+def test_python_shape_checks(pkg):
+    a = np.zeros((3, 5, 5), order="F")
+    with pytest.raises(ValueError):
+        pkg.advec_ng(a, a, np.zeros((3, 5, 6), order="F"), np.zeros(5), 0.01, 0.01, RE_INV,
+                     np.zeros((3, 5, 5), order="F"))
+    with pytest.raises(ValueError):
+        pkg.advec_ng(a, a, a, np.zeros(4), 0.01, 0.01, RE_INV, np.zeros((3, 5, 5), order="F"))
+    with pytest.raises(ValueError):
+        pkg.smooth_ng(a, SHAPIRO, np.zeros((3, 5, 4), order="F"))
+    with pytest.raises(ValueError):
+        pkg.time_filter_ng(0, a, np.zeros((3, 5), order="F"), 0.95, 0.025, np.zeros((3, 5, 5), order="F"),
+                           np.zeros((3, 5, 5), order="F"))

@@ -496,6 +496,9 @@ def time_filter_ng(which, cur, prev, dtsmooth, dtsmooth_div2, upd, nm_out):
     TG_FILTER_MINOR: src/minor_ng.F90:234-237, TG_FILTER_OPLUS:
     src/oplus_ng.F90:337-340) on host (nk, ncol) arrays: upd is floored in
     place and nm_out receives the filtered field."""
+    for n, x in (("cur", cur), ("prev", prev), ("nm_out", nm_out)):
+        if np.shape(x) != np.shape(upd):
+            raise ValueError(f"time_filter_ng: {n} must have the shape of upd {upd.shape}")
     nk = upd.shape[0]
     ncol = upd.size // nk
     rc = lib().tg_time_filter_ng(int(which), _host(cur, "cur"), _host(prev, "prev"), float(dtsmooth),
@@ -513,8 +516,15 @@ def time_filter_ng_dev(which, cur, prev, dtsmooth, dtsmooth_div2, upd, nm_out, n
 def advec_ng(f, un, vn, racs, dlamda, dphi, re_inv, hadvec):
     """advec_ng (src/advec_ng.F90) for a nest held as one subdomain: f, un, vn
     and hadvec are (nk, nlon+4, nlat+4) Fortran arrays, racs (nlat+4)."""
+    if np.ndim(f) != 3:
+        raise ValueError("advec_ng: f must be (nk, nlon+4, nlat+4)")
+    for n, x in (("un", un), ("vn", vn), ("hadvec", hadvec)):
+        if np.shape(x) != f.shape:
+            raise ValueError(f"advec_ng: {n} must have the shape of f {f.shape}")
     nk, nlond, nlatd = f.shape
     r = np.ascontiguousarray(racs, dtype=np.float64)
+    if r.shape != (nlatd,):
+        raise ValueError(f"advec_ng: racs must have {nlatd} values")
     rc = lib().tg_advec_ng(_host(f, "f"), _host(un, "un"), _host(vn, "vn"), r.ctypes.data, float(dlamda),
                            float(dphi), float(re_inv), nk, nlond - 4, nlatd - 4, _out(hadvec, "hadvec"))
     return _check(rc, "tg_advec_ng", numeric_ok=False)
@@ -523,6 +533,8 @@ def advec_ng(f, un, vn, racs, dlamda, dphi, re_inv, hadvec):
 def smooth_ng(fin, shapiro, fout):
     """smooth_ng (src/smooth_ng.F90) for a nest held as one subdomain; fin and
     fout are (nk, nlon+4, nlat+4) Fortran arrays."""
+    if np.ndim(fin) != 3 or np.shape(fout) != np.shape(fin):
+        raise ValueError("smooth_ng: fin and fout must both be (nk, nlon+4, nlat+4)")
     nk, nlond, nlatd = fin.shape
     rc = lib().tg_smooth_ng(_host(fin, "fin"), float(shapiro), nk, nlond - 4, nlatd - 4, _out(fout, "fout"))
     return _check(rc, "tg_smooth_ng", numeric_ok=False)
