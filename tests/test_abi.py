@@ -109,3 +109,34 @@ def test_fortran_binding_matches_header():
         assert cname in arity, cname
         nargs = 0 if not args.strip() else args.count(",") + 1
         assert nargs == arity[cname], (cname, nargs, arity[cname])
+
+
+def test_host_wrappers_check_field_sizes(pkg):
+    """The fused host wrappers accept the benchmark's field shapes (the call
+    then stops at the missing device) and reject a short field before any C
+    call reads it."""
+    import numpy as np
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("checks the no-device path")
+    nk, ncol, dz = 5, 12, 0.5
+    z = lambda: np.zeros((nk, ncol), order="F")  # noqa: E731
+    calls = {
+        "dt": (pkg.synth.dt_inputs(nk, ncol, dz, 1), lambda F, C: pkg.dt_ng(F, C, z()), "tlbc"),
+        "minor": (pkg.synth.minor_inputs(nk, ncol, dz, 1), lambda F, C: pkg.minor_ng(F, C, z()), "fubc"),
+        "comp": (pkg.synth.comp_inputs(nk, ncol, dz, 1), lambda F, C: pkg.comp_ng(F, C, z(), z(), z()), "difk"),
+        "oplus": (pkg.synth.oplus_inputs(nk, ncol, dz, 1), lambda F, C: pkg.oplus_ng(F, C, z(), z(), z()), "zpint"),
+    }
+    for name, ((F, C), call, short) in calls.items():
+        with pytest.raises(pkg.TgError) as e:
+            call(F, C)
+        assert e.value.status == pkg.TG_ENODEV, name
+        F = dict(F)
+        F[short] = np.asarray(F[short])[:-1].copy()
+        with pytest.raises(ValueError):
+            call(F, C)
+    F, C, qt = pkg.synth.settei_inputs(nk, ncol, dz, 1)
+    with pytest.raises(pkg.TgError):
+        pkg.settei_ng(F, C, z(), z(), qt.copy(order="F"))
+    with pytest.raises(ValueError):
+        pkg.settei_ng(F, C, z(), z(), np.zeros((nk, ncol - 1), order="F"))

@@ -281,6 +281,18 @@ def _out(x, name):
     return p
 
 
+def _check_sizes(where, fields, names, nk, ncol, two_d=(), one_d=(), outs=()):
+    """Every field holds the values the C entry reads: 3-D fields nk*ncol,
+    2-D fields ncol, level profiles nk (a short array would be over-read)."""
+    for n in names:
+        want = nk if n in one_d else ncol if n in two_d else 12 * nk * ncol if n == "fs" else nk * ncol
+        if np.size(fields[n]) != want:
+            raise ValueError(f"{where}: {n} has {np.size(fields[n])} values, expected {want}")
+    for n, x in outs:
+        if np.size(x) != nk * ncol:
+            raise ValueError(f"{where}: {n} must hold nk*ncol = {nk * ncol} values")
+
+
 # ---------------------------------------------------------------------------
 # Drop-ins (host arrays, synchronous)
 # ---------------------------------------------------------------------------
@@ -385,6 +397,8 @@ def dt_ng(fields, consts, tn_upd):
     (nk, ...) receives the solution."""
     nk = tn_upd.shape[0]
     ncol = tn_upd.size // nk
+    _check_sizes("dt_ng", fields, DT_FIELDS, nk, ncol, two_d=("tlbc", "t_lbc", "ulbc", "vlbc"),
+                 one_d=("expz", "dift"))
     F = DtFields(*[_host(fields[n], n) for n in DT_FIELDS])
     C = DtConsts(*[float(consts[n]) for n in DT_CONSTS])
     rc = lib().tg_dt_ng(ctypes.byref(F), ctypes.byref(C), _out(tn_upd, "tn_upd"), nk, ncol)
@@ -397,6 +411,8 @@ def minor_ng(fields, consts, fcomp_out):
     and the MINOR_CONSTS2 constants); fcomp_out (nk, ...) receives the solution."""
     nk = fcomp_out.shape[0]
     ncol = fcomp_out.size // nk
+    _check_sizes("minor_ng", fields, MINOR_FIELDS, nk, ncol,
+                 two_d=("tlbc", "flbc1", "flbc2", "flbc3", "fubc", "dfactor"), one_d=("expz", "difk"))
     F = MinorFields(*[_host(fields[n], n) for n in MINOR_FIELDS])
     C = minor_consts(consts)
     rc = lib().tg_minor_ng(ctypes.byref(F), ctypes.byref(C), _out(fcomp_out, "fcomp_out"), nk, ncol)
@@ -411,6 +427,8 @@ def comp_ng(fields, consts, o2_upd, o1_upd, he_upd):
     ncol = o2_upd.size // nk
     if np.asarray(fields["fs"]).size != 12 * nk * ncol:
         raise ValueError("fs must hold 12 slabs of nk*ncol")
+    _check_sizes("comp_ng", fields, COMP_FIELDS, nk, ncol, two_d=("tlbc", "flx_he", "dfactor"),
+                 one_d=("expz", "difk"), outs=(("o1_upd", o1_upd), ("he_upd", he_upd)))
     arrs = {n: np.ascontiguousarray(fields[n], dtype=np.float64).reshape(-1) if n == "fs" else fields[n]
             for n in COMP_FIELDS}
     F = CompFields(*[_host(arrs[n], n) for n in COMP_FIELDS])
@@ -426,6 +444,8 @@ def settei_ng(fields, consts, te_out, ti_out, qtotal):
     ti_out receive Te and Ti; qtotal (nk, ncol) is updated in place."""
     nk = te_out.shape[0]
     ncol = te_out.size // nk
+    _check_sizes("settei_ng", fields, SETTEI_FIELDS, nk, ncol,
+                 two_d=("t_lbc", "chi", "rlatm", "dipmag", "qteaur"), outs=(("ti_out", ti_out), ("qtotal", qtotal)))
     F = SetteiFields(*[_host(fields[n], n) for n in SETTEI_FIELDS])
     C = settei_consts(consts)
     rc = lib().tg_settei_ng(ctypes.byref(F), ctypes.byref(C), _out(te_out, "te_out"), _out(ti_out, "ti_out"),
@@ -439,6 +459,9 @@ def oplus_ng(fields, consts, opout, xiop2p, xiop2d, Fe=None, Fn=None):
     (nk)); outputs (nk, ncol)."""
     nk = opout.shape[0]
     ncol = opout.size // nk
+    _check_sizes("oplus_ng", fields, OPLUS_FIELDS, nk, ncol,
+                 two_d=("bx", "by", "bz", "dvb", "rlatm", "chi", "dipmag", "sndec", "csdec"), one_d=("zpint",),
+                 outs=(("xiop2p", xiop2p), ("xiop2d", xiop2d)))
     F = OplusFields(*[_host(fields[n], n) for n in OPLUS_FIELDS])
     C = oplus_consts(consts)
     rc = lib().tg_oplus_ng(ctypes.byref(F), ctypes.byref(C), _out(opout, "opout"), _out(xiop2p, "xiop2p"),
