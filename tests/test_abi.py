@@ -140,3 +140,20 @@ def test_host_wrappers_check_field_sizes(pkg):
         pkg.settei_ng(F, C, z(), z(), qt.copy(order="F"))
     with pytest.raises(ValueError):
         pkg.settei_ng(F, C, z(), z(), np.zeros((nk, ncol - 1), order="F"))
+
+
+def test_plain_c_caller(pkg, tmp_path):
+    """tests/c/abi_check.c: the header and library used from C alone."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    libdir = os.path.dirname(pkg.colsolve.LIB_PATH)
+    exe = str(tmp_path / "abi_check")
+    subprocess.run([cc, "-O0", "-std=c11", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c", "abi_check.c"), "-o", exe, "-L", libdir, "-ltg_colsolve",
+                    f"-Wl,-rpath,{libdir}", "-lm"], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.startswith("abi_check: ok")
