@@ -166,6 +166,29 @@ def dt_ng(fields, consts, with_system=False):
     return (tn_upd, tuple(sysarr)) if with_system else tn_upd
 
 
+DT_DIAG_NAMES = ("DTDT", "DT_SOLAR", "DT_HORDIF", "DT_RECOMB", "DT_JOULE", "DT_MOLDIF", "DT_COOL", "DT_HORADV",
+                 "DT_VERADV", "DT_ADIA", "DT_CONDUCT", "DEN")
+
+
+def dt_diag_ng(fields, consts, tn_upd):
+    """dt_ng's history diagnostics (src/dt_ng.F90:169-191, DEN :133) from the
+    fields and the solution tn_upd (nk, ncol); returns a dict name -> (nk, ncol)."""
+    L = lib()
+    if not hasattr(L, "_dt_diag_bound"):
+        L.oracle_dt_diag_ng.argtypes = [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), ctypes.c_int,
+                                        ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_dt_diag_ng.restype = None
+        L._dt_diag_bound = True
+    arrs = {k: _fcopy(fields[k]) for k in DT_FIELD_ORDER}
+    nk, ncol = arrs["tn"].shape[0], arrs["tn"].size // arrs["tn"].shape[0]
+    F = DtFields(*[arrs[k].ctypes.data for k in DT_FIELD_ORDER])
+    C = DtConsts(*[float(consts[k]) for k in DT_CONST_ORDER])
+    x = _fcopy(tn_upd)
+    out = np.zeros((nk, ncol, len(DT_DIAG_NAMES)), order="F")
+    L.oracle_dt_diag_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, _p(x), _p(out))
+    return {n: out[:, :, i] for i, n in enumerate(DT_DIAG_NAMES)}
+
+
 MINOR_FIELD_ORDER = ("tn", "o2", "o1", "he", "mbar", "barm", "xnmbar", "w", "ftm1_smooth", "hadvec", "sloss",
                      "sprod", "tlbc", "flbc1", "flbc2", "flbc3", "fubc", "dfactor", "expz", "difk")
 MINOR_CONST_ORDER = ("dzp", "dtx2inv", "expzmid", "expzmid_inv", "rmassinv_o2", "rmassinv_o1", "rmassinv_n2",

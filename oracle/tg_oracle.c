@@ -525,6 +525,102 @@ ORACLE_API void oracle_dt_ng(const oracle_dt_fields *F, const oracle_dt_consts *
 }
 
 /* ------------------------------------------------------------------------ */
+/* dt_ng's history diagnostics (src/dt_ng.F90:169-191 and DEN at :133), from */
+/* the fields of oracle_dt_ng and its solution tn_upd (rows 1..nk, before   */
+/* the lateral-boundary overwrite, as the reference writes them).  diag     */
+/* receives 12 slabs of (nk, ncol): DTDT, DT_SOLAR, DT_HORDIF, DT_RECOMB,    */
+/* DT_JOULE, DT_MOLDIF, DT_COOL, DT_HORADV, DT_VERADV, DT_ADIA, DT_CONDUCT,  */
+/* DEN.  DT_CONDUCT rows 1 and nk are left unset by the reference (a local   */
+/* array); they are 0 here.                                                  */
+/* ------------------------------------------------------------------------ */
+ORACLE_API void oracle_dt_diag_ng(const oracle_dt_fields *F, const oracle_dt_consts *C, int nk, long ncol,
+                                  const double *tn_upd, double *diag)
+{
+    double *w = (double *)malloc(sizeof(double) * 10 * (size_t)nk);
+    double *vad = w, *cpi = w + nk, *kmi = w + 2 * nk, *wi = w + 3 * nk, *dudz = w + 4 * nk,
+           *dvdz = w + 5 * nk, *qsolar = w + 6 * nk, *tni = w + 7 * nk, *g = w + 8 * nk, *f = w + 9 * nk;
+    const double dz = C->dz;
+    const size_t slab = (size_t)nk * ncol;
+    long col;
+    int k;
+    for (col = 0; col < ncol; ++col) {
+        const size_t o = (size_t)nk * col;
+        const double *tn = F->tn + o, *ww = F->w + o, *cp = F->cp + o, *km = F->km + o, *un = F->un + o,
+                     *vn = F->vn + o, *qt = F->qtotal + o, *x = tn_upd + o;
+        double *d[12];
+        for (k = 0; k < 12; ++k) d[k] = diag + k * slab + o;
+        /* the intermediates, as oracle_dt_ng forms them (:57-148) */
+        vad[0] = (tn[0] - F->t_lbc[col]) * ww[0] * 2.;
+        vad[nk - 1] = 0.;
+        for (k = 1; k < nk - 1; ++k) vad[k] = (tn[k] - tn[k - 1]) * ww[k];
+        for (k = 0; k < nk - 1; ++k) vad[k] = (vad[k] + vad[k + 1]) * .5;
+        for (k = 0; k < nk; ++k) vad[k] = vad[k] / dz;
+        for (k = 0; k < nk - 1; ++k) {
+            cpi[k] = .5 * (cp[k] + cp[k + 1]);
+            kmi[k] = .5 * (km[k] + km[k + 1]);
+            wi[k] = .5 * (ww[k] + ww[k + 1]);
+        }
+        cpi[nk - 1] = 1.5 * cp[nk - 1] - .5 * cp[nk - 2];
+        kmi[nk - 1] = 1.5 * km[nk - 1] - .5 * km[nk - 2];
+        wi[nk - 1] = 1.5 * ww[nk - 1] - .5 * ww[nk - 2];
+        for (k = 1; k < nk - 2; ++k) {
+            dudz[k] = (un[k + 1] - un[k - 1]) / (2. * dz);
+            dvdz[k] = (vn[k + 1] - vn[k - 1]) / (2. * dz);
+        }
+        dudz[0] = (un[0] + 1. / 3. * un[1] - 4. / 3. * F->ulbc[col]) / dz;
+        dvdz[0] = (vn[0] + 1. / 3. * vn[1] - 4. / 3. * F->vlbc[col]) / dz;
+        dudz[nk - 2] = dudz[nk - 3] / 3.;
+        dvdz[nk - 2] = dvdz[nk - 3] / 3.;
+        dudz[nk - 1] = dudz[nk - 2] / 3.;
+        dvdz[nk - 1] = dvdz[nk - 2] / 3.;
+        for (k = 0; k < nk - 1; ++k) qsolar[k] = .5 * (qt[k] + qt[k + 1]);
+        qsolar[nk - 1] = 1.5 * qt[nk - 1] - .5 * qt[nk - 2];
+        for (k = 1; k < nk - 1; ++k) tni[k] = .5 * (tn[k - 1] + tn[k]);
+        tni[0] = F->tlbc[col];
+        tni[nk - 1] = tn[nk - 2];
+        for (k = 0; k < nk; ++k) {
+            const size_t i = o + k;
+            const double h = F->schti[i];
+            double rho = C->p0 * C->expzmid_inv / (h * C->grav);
+            rho = rho * F->expz[k];
+            double gpart = h * h * rho * cp[k];
+            gpart = gpart * F->dift[k];
+            g[k] = C->grav * (F->kt[i] + gpart) / (C->p0 * h * (dz * dz));
+            double ff = C->grav * C->grav * (h * h) * rho / (tni[k] * C->p0 * 2. * dz);
+            f[k] = ff * F->dift[k];
+            const double xo = F->xnmbar[i] * F->o1[i] * C->rmassinv_o1;
+            const double qrecomb = C->tsurplus * F->rkm12[i] * (xo * xo) * C->avo / F->mbar[i];
+            double qm = C->grav * kmi[k] / (C->p0 * F->scht[i]) * (dudz[k] * dudz[k] + dvdz[k] * dvdz[k]);
+            qm = qm / F->expz[k];
+            /* :169-180 */
+            d[0][k] = C->dtx2inv * (x[k] - F->tnsmooth[i]);
+            d[1][k] = qsolar[k] / cpi[k];
+            d[2][k] = F->hdt[i] / cpi[k];
+            d[3][k] = qrecomb / cpi[k];
+            d[4][k] = F->qji_tn[i] / cpi[k];
+            d[5][k] = qm / cpi[k];
+            double cool_exp = F->cool_exp[i] / cpi[k];
+            cool_exp = cool_exp / F->expz[k];
+            d[6][k] = -cool_exp - F->cool_imp[i] * x[k];
+            d[7][k] = -F->horadv[i];
+            d[8][k] = -vad[k];
+            d[9][k] = -(wi[k] * C->gask / (cpi[k] * F->mbar[i]) * x[k]);
+            d[11][k] = rho;
+        }
+        /* DT_CONDUCT (:181-186) */
+        d[10][0] = 0.;
+        d[10][nk - 1] = 0.;
+        for (k = 1; k < nk - 1; ++k) {
+            const double t = (g[k] - f[k]) * x[k - 1] - (g[k + 1] - f[k + 1] + g[k] + f[k]) * x[k] +
+                             (g[k + 1] + f[k + 1]) * x[k + 1];
+            d[10][k] = 1. / F->expz[k] * t;
+        }
+        for (k = 0; k < nk; ++k) d[10][k] = d[10][k] / cpi[k];
+    }
+    free(w);
+}
+
+/* ------------------------------------------------------------------------ */
 /* minor_ng minor-species column assembly + solve (src/minor_ng.F90:60-200), */
 /* used for N4S, NO, N2D and Ar.  Fields (nk, ncol); 2-D (ncol); expz, difk  */
 /* (nk).  hadvec = advec_ng(fcomp) and ftm1_smooth = smooth_ng(fcomp_tm1)    */

@@ -5,7 +5,8 @@ import numpy as np
 import pytest
 
 
-def dt_numpy(F, C):
+def dt_numpy(F, C, keep=None):
+    """The assembled rows; keep (a dict), if given, receives the intermediates."""
     nk = F["tn"].shape[0]
     tn, w, cp, km, un, vn, qt = (F[k] for k in ("tn", "w", "cp", "km", "un", "vn", "qtotal"))
     expz, dift = F["expz"][:, None], F["dift"][:, None]
@@ -65,7 +66,34 @@ def dt_numpy(F, C):
     q[0] = q[0] - p[0]
     rhs[0] = rhs[0] - 2. * p[0] * F["t_lbc"]
     p[0] = 0.
+    if keep is not None:
+        keep.update(vad=vad, cpi=cpi, wi=wi, qsolar=qsolar, qrecomb=qrecomb, qm=qm, g=g, f=f, rho=rho)
     return p, q, r, rhs
+
+
+def dt_diag_numpy(F, C, tn_upd):
+    """dt_ng.F90:169-191 (and DEN, :133) as the Fortran array statements."""
+    m = {}
+    dt_numpy(F, C, keep=m)
+    nk = F["tn"].shape[0]
+    expz = F["expz"][:, None]
+    cpi, g, f, x = m["cpi"], m["g"], m["f"], tn_upd
+    out = {"DTDT": C["dtx2inv"] * (x - F["tnsmooth"]), "DT_SOLAR": m["qsolar"] / cpi, "DT_HORDIF": F["hdt"] / cpi,
+           "DT_RECOMB": m["qrecomb"] / cpi, "DT_JOULE": F["qji_tn"] / cpi, "DT_MOLDIF": m["qm"] / cpi}
+    dt_cool_exp = F["cool_exp"] / cpi
+    dt_cool_exp = dt_cool_exp / expz
+    out["DT_COOL"] = -dt_cool_exp - F["cool_imp"] * x
+    out["DT_HORADV"] = -F["horadv"]
+    out["DT_VERADV"] = -m["vad"]
+    out["DT_ADIA"] = -m["wi"] * C["gask"] / (cpi * F["mbar"]) * x
+    cond = np.zeros_like(x)
+    k = slice(1, nk - 1)
+    km1, kp1 = slice(0, nk - 2), slice(2, nk)
+    cond[k] = 1 / expz[k] * ((g[k] - f[k]) * x[km1] - (g[kp1] - f[kp1] + g[k] + f[k]) * x[k] +
+                             (g[kp1] + f[kp1]) * x[kp1])
+    out["DT_CONDUCT"] = cond / cpi
+    out["DEN"] = m["rho"] * np.ones_like(x)
+    return out
 
 
 @pytest.mark.parametrize("nk,dz", [(29, 0.5), (57, 0.25), (3, 0.5)])
@@ -80,3 +108,16 @@ def test_dt_assembly_matches_independent_transcription(pkg, orc, nk, dz):
     assert np.array_equal(tn_upd[:nk - 1], x[:nk - 1])
     assert np.array_equal(tn_upd[nk - 1], x[nk - 2] ** 2 / x[nk - 3])
     assert np.all(np.isfinite(tn_upd))
+
+
+@pytest.mark.parametrize("nk,dz", [(29, 0.5), (57, 0.25), (3, 0.5)])
+def test_dt_diagnostics_match_independent_transcription(pkg, orc, nk, dz):
+    F, C = pkg.synth.dt_inputs(nk, 47, dz, 13 + nk)
+    tn_upd = orc.dt_ng(F, C)
+    got = orc.dt_diag_ng(F, C, tn_upd)
+    want = dt_diag_numpy(F, C, tn_upd)
+    assert set(got) == set(want)
+    for name in got:
+        # -x and (-1)*x differ only in the sign of zero; compare values
+        assert np.array_equal(got[name], want[name]), name
+    assert np.all(got["DT_CONDUCT"][[0, nk - 1]] == 0.0)
