@@ -205,6 +205,35 @@ class MinorConsts(ctypes.Structure):
                 [("b", ctypes.c_double * 9), ("fb", ctypes.c_double * 3)])
 
 
+def _minor_consts(consts):
+    return MinorConsts(consts["rmx"], consts["alfax"], (ctypes.c_double * 4)(*consts["phix"]),
+                       *[float(consts[k]) for k in MINOR_CONST_ORDER],
+                       (ctypes.c_double * 9)(*np.ravel(consts["b"], order="F")), (ctypes.c_double * 3)(*consts["fb"]))
+
+
+MINOR_DIAG_NAMES = ("DPDT", "PROD", "LOSS", "MOLDIF", "EDDYDIF", "VERADV", "HORADV")
+
+
+def minor_diag_ng(fields, consts, fcomp_out):
+    """minor_ng's history diagnostics (src/minor_ng.F90:202-224) from the
+    fields and the solution; returns a dict name -> (nk, ncol) holding the
+    values passed to addfld (VERADV and HORADV with the reference's sign)."""
+    L = lib()
+    if not hasattr(L, "_minor_diag_bound"):
+        L.oracle_minor_diag_ng.argtypes = [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), ctypes.c_int,
+                                           ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_minor_diag_ng.restype = None
+        L._minor_diag_bound = True
+    arrs = {k: _fcopy(fields[k]) for k in MINOR_FIELD_ORDER}
+    nk, ncol = arrs["tn"].shape[0], arrs["tn"].size // arrs["tn"].shape[0]
+    F = MinorFields(*[arrs[k].ctypes.data for k in MINOR_FIELD_ORDER])
+    C = _minor_consts(consts)
+    x = _fcopy(fcomp_out)
+    out = np.zeros((nk, ncol, len(MINOR_DIAG_NAMES)), order="F")
+    L.oracle_minor_diag_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, _p(x), _p(out))
+    return {n: out[:, :, i] for i, n in enumerate(MINOR_DIAG_NAMES)}
+
+
 def minor_ng(fields, consts, with_system=False):
     """minor_ng assembly + solve (src/minor_ng.F90:60-200); returns fcomp_out
     (before the max(.,small) clamp) and, if with_system, (p, q, r, f) rows 1..nk."""
@@ -217,9 +246,7 @@ def minor_ng(fields, consts, with_system=False):
     arrs = {k: _fcopy(fields[k]) for k in MINOR_FIELD_ORDER}
     nk, ncol = arrs["tn"].shape[0], arrs["tn"].size // arrs["tn"].shape[0]
     F = MinorFields(*[arrs[k].ctypes.data for k in MINOR_FIELD_ORDER])
-    C = MinorConsts(consts["rmx"], consts["alfax"], (ctypes.c_double * 4)(*consts["phix"]),
-                    *[float(consts[k]) for k in MINOR_CONST_ORDER],
-                    (ctypes.c_double * 9)(*np.ravel(consts["b"], order="F")), (ctypes.c_double * 3)(*consts["fb"]))
+    C = _minor_consts(consts)
     out = np.zeros((nk, ncol), order="F")
     sysarr = [np.zeros((nk, ncol), order="F") for _ in range(4)] if with_system else [None] * 4
     L.oracle_minor_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(s) for s in sysarr], _p(out))

@@ -648,89 +648,149 @@ typedef struct {
 static const double MPHI[3][4] = {{0., 1.35, 2.16, 1.11}, {0.673, 0., 1.616, 0.769}, {0.270, 0.404, 0., 0.322}};
 static const double MSS[3] = {1.710, 1.749, 1.718};
 
-ORACLE_API void oracle_minor_ng(const oracle_minor_fields *F, const oracle_minor_consts *C, int nk, long ncol,
-                                double *p_out, double *q_out, double *r_out, double *f_out, double *fcomp_out)
+/* Per-column terms of minor_ng's rows (:72-159): after the call ax, thdiff,
+ * dmdz (divided by barm) and wi hold their values for levels 0..nk-1.  w
+ * holds 15*nk doubles of work, the first four blocks being those arrays. */
+static void minor_terms(const oracle_minor_fields *F, const oracle_minor_consts *C, int nk, long col,
+                        const double *salfax, double *w)
 {
     const double tau = 1.86e+3, t00 = 273.;
     const double dzp = C->dzp;
+    double *ax = w, *thdiff = w + nk, *dmdz = w + 2 * nk, *wi = w + 3 * nk, *pso1 = w + 4 * nk,
+           *pso2 = w + 5 * nk, *pshe = w + 6 * nk, *do1dz = w + 7 * nk, *do2dz = w + 8 * nk, *dhedz = w + 9 * nk,
+           *tni = w + 10 * nk, *sa1 = w + 11 * nk, *sa2 = w + 12 * nk, *sa3 = w + 13 * nk, *ex = w + 14 * nk;
+    const size_t o = (size_t)nk * col;
+    const double *tn = F->tn + o, *o2 = F->o2 + o, *o1 = F->o1 + o, *he = F->he + o, *mbar = F->mbar + o,
+                 *barm = F->barm + o, *ww = F->w + o;
+    int k, n;
+    /* lower-boundary mixing ratios (:72-75) */
+    const double bo2 = C->b[0] * o2[0] + C->b[3] * o1[0] + C->b[6] * he[0] + C->fb[0];
+    const double bo1 = C->b[1] * o2[0] + C->b[4] * o1[0] + C->b[7] * he[0] + C->fb[1];
+    const double bhe = C->b[2] * o2[0] + C->b[5] * o1[0] + C->b[8] * he[0] + C->fb[2];
+    const double xmbari = 1. / (bo2 * C->rmassinv_o2 + bo1 * C->rmassinv_o1 +
+                                (1. - bo2 - bo1 - bhe) * C->rmassinv_n2 + bhe * C->rmassinv_he);
+    /* interface quantities (:77-96) */
+    dmdz[0] = (mbar[0] - xmbari) / dzp;
+    pso1[0] = .5 * (bo1 + o1[0]);
+    pso2[0] = .5 * (bo2 + o2[0]);
+    pshe[0] = .5 * (bhe + he[0]);
+    do1dz[0] = (o1[0] - bo1) / dzp;
+    do2dz[0] = (o2[0] - bo2) / dzp;
+    dhedz[0] = (he[0] - bhe) / dzp;
+    for (k = 1; k < nk; ++k) {
+        dmdz[k] = (mbar[k] - mbar[k - 1]) / dzp;
+        pso1[k] = .5 * (o1[k] + o1[k - 1]);
+        pso2[k] = .5 * (o2[k] + o2[k - 1]);
+        pshe[k] = .5 * (he[k] + he[k - 1]);
+        do1dz[k] = (o1[k] - o1[k - 1]) / dzp;
+        do2dz[k] = (o2[k] - o2[k - 1]) / dzp;
+        dhedz[k] = (he[k] - he[k - 1]) / dzp;
+    }
+    tni[0] = F->tlbc[col];
+    tni[nk - 1] = tn[nk - 2];
+    for (k = 1; k < nk - 1; ++k) tni[k] = .5 * (tn[k] + tn[k - 1]);
+    /* alfa matrix, its inverse, salfax . invalfa(:,n) (:100-133) */
+    for (k = 0; k < nk; ++k) {
+        double df[3], A[9], Ai[9];
+        for (n = 0; n < 3; ++n) df[n] = pow(tni[k] / t00, 1.75 - MSS[n]);
+#define PH(i, j) MPHI[(i) - 1][(j) - 1]
+        M3(A, 1, 1) = -(PH(1, 4) + (PH(1, 2) - PH(1, 4)) * pso1[k] + (df[0] * PH(1, 3) - PH(1, 4)) * pshe[k]);
+        M3(A, 2, 2) = -(PH(2, 4) + (PH(2, 1) - PH(2, 4)) * pso2[k] + (df[1] * PH(2, 3) - PH(2, 4)) * pshe[k]);
+        M3(A, 3, 3) = -(df[2] * PH(3, 4) + (df[0] * PH(3, 1) - df[2] * PH(3, 4)) * pso2[k] +
+                       (df[1] * PH(3, 2) - df[2] * PH(3, 4)) * pso1[k]);
+        M3(A, 1, 2) = (PH(1, 2) - PH(1, 4)) * pso2[k];
+        M3(A, 1, 3) = (df[0] * PH(1, 3) - PH(1, 4)) * pso2[k];
+        M3(A, 2, 1) = (PH(2, 1) - PH(2, 4)) * pso1[k];
+        M3(A, 2, 3) = (df[1] * PH(2, 3) - PH(2, 4)) * pso1[k];
+        M3(A, 3, 1) = (df[0] * PH(3, 1) - df[2] * PH(3, 4)) * pshe[k];
+        M3(A, 3, 2) = (df[1] * PH(3, 2) - df[2] * PH(3, 4)) * pshe[k];
+        oracle_matinv3(A, Ai);
+        sa1[k] = salfax[0] * M3(Ai, 1, 1) + salfax[1] * M3(Ai, 2, 1) + salfax[2] * M3(Ai, 3, 1);
+        sa2[k] = salfax[0] * M3(Ai, 1, 2) + salfax[1] * M3(Ai, 2, 2) + salfax[2] * M3(Ai, 3, 2);
+        sa3[k] = salfax[0] * M3(Ai, 1, 3) + salfax[1] * M3(Ai, 2, 3) + salfax[2] * M3(Ai, 3, 3);
+    }
+    /* ex, ax, thdiff (:135-153) */
+    for (k = 0; k < nk; ++k) {
+        ex[k] = 1. - (C->rmx + dmdz[k]) / barm[k] +
+                sa1[k] * (do2dz[k] - (1. - (C->rmass_o2 + dmdz[k]) / barm[k]) * pso2[k]) +
+                sa2[k] * (do1dz[k] - (1. - (C->rmass_o1 + dmdz[k]) / barm[k]) * pso1[k]) +
+                sa3[k] * (dhedz[k] - (1. - (C->rmass_he + dmdz[k]) / barm[k]) * pshe[k]);
+        dmdz[k] = dmdz[k] / barm[k];
+        ax[k] = -(barm[k] / (tau * C->rmass_n2) * pow(t00 / tni[k], 0.25) /
+                  (C->phix[2] + salfax[0] * pso2[k] + salfax[1] * pso1[k] + salfax[2] * pshe[k]));
+    }
+    for (k = 0; k < nk; ++k) {
+        double dt;
+        if (k == 0) dt = tni[1] - tni[0];
+        else if (k == nk - 1) dt = tni[nk - 1] - tni[nk - 2];
+        else dt = (tni[k + 1] - tni[k - 1]) / 2.;
+        thdiff[k] = ex[k] - C->alfax * dt / (dzp * tni[k]);
+    }
+    for (k = 0; k < nk - 1; ++k) wi[k] = .5 * (ww[k] + ww[k + 1]);
+    wi[nk - 1] = 1.5 * ww[nk - 1] - .5 * ww[nk - 2];
+}
+
+/* minor_ng's history diagnostics (src/minor_ng.F90:202-224) from the      */
+/* fields of oracle_minor_ng and its solution fcomp_out (before the lateral */
+/* overwrite).  diag receives 7 slabs of (nk, ncol): DPDT, PROD (s0prod),   */
+/* LOSS, MOLDIF, EDDYDIF (times dfactor), -VERADV and -HORADV, the values    */
+/* the reference passes to addfld.  MOLDIF, EDDYDIF and VERADV rows 1 and nk */
+/* are left unset by the reference (local arrays); they are 0 here.          */
+ORACLE_API void oracle_minor_diag_ng(const oracle_minor_fields *F, const oracle_minor_consts *C, int nk, long ncol,
+                                     const double *fcomp_out, double *diag)
+{
+    const double dzp = C->dzp;
     double salfax[3];
-    double *w = (double *)malloc(sizeof(double) * 24 * (size_t)nk);
-    double *dmdz = w, *pso1 = w + nk, *pso2 = w + 2 * nk, *pshe = w + 3 * nk, *do1dz = w + 4 * nk,
-           *do2dz = w + 5 * nk, *dhedz = w + 6 * nk, *tni = w + 7 * nk, *sa1 = w + 8 * nk, *sa2 = w + 9 * nk,
-           *sa3 = w + 10 * nk, *ex = w + 11 * nk, *ax = w + 12 * nk, *thdiff = w + 13 * nk, *wi = w + 14 * nk,
-           *p = w + 15 * nk, *q = w + 16 * nk, *r = w + 17 * nk, *f = w + 18 * nk, *ws = w + 19 * nk;
+    double *w = (double *)malloc(sizeof(double) * 15 * (size_t)nk);
+    const double *ax = w, *thdiff = w + nk, *dmdz = w + 2 * nk, *wi = w + 3 * nk;
+    const size_t slab = (size_t)nk * ncol;
     long col;
     int k, n;
     for (n = 0; n < 3; ++n) salfax[n] = C->phix[n] - C->phix[3];
     for (col = 0; col < ncol; ++col) {
         const size_t o = (size_t)nk * col;
-        const double *tn = F->tn + o, *o2 = F->o2 + o, *o1 = F->o1 + o, *he = F->he + o, *mbar = F->mbar + o,
-                     *barm = F->barm + o, *ww = F->w + o;
-        /* lower-boundary mixing ratios (:72-75) */
-        const double bo2 = C->b[0] * o2[0] + C->b[3] * o1[0] + C->b[6] * he[0] + C->fb[0];
-        const double bo1 = C->b[1] * o2[0] + C->b[4] * o1[0] + C->b[7] * he[0] + C->fb[1];
-        const double bhe = C->b[2] * o2[0] + C->b[5] * o1[0] + C->b[8] * he[0] + C->fb[2];
-        const double xmbari = 1. / (bo2 * C->rmassinv_o2 + bo1 * C->rmassinv_o1 +
-                                    (1. - bo2 - bo1 - bhe) * C->rmassinv_n2 + bhe * C->rmassinv_he);
-        /* interface quantities (:77-96) */
-        dmdz[0] = (mbar[0] - xmbari) / dzp;
-        pso1[0] = .5 * (bo1 + o1[0]);
-        pso2[0] = .5 * (bo2 + o2[0]);
-        pshe[0] = .5 * (bhe + he[0]);
-        do1dz[0] = (o1[0] - bo1) / dzp;
-        do2dz[0] = (o2[0] - bo2) / dzp;
-        dhedz[0] = (he[0] - bhe) / dzp;
-        for (k = 1; k < nk; ++k) {
-            dmdz[k] = (mbar[k] - mbar[k - 1]) / dzp;
-            pso1[k] = .5 * (o1[k] + o1[k - 1]);
-            pso2[k] = .5 * (o2[k] + o2[k - 1]);
-            pshe[k] = .5 * (he[k] + he[k - 1]);
-            do1dz[k] = (o1[k] - o1[k - 1]) / dzp;
-            do2dz[k] = (o2[k] - o2[k - 1]) / dzp;
-            dhedz[k] = (he[k] - he[k - 1]) / dzp;
-        }
-        tni[0] = F->tlbc[col];
-        tni[nk - 1] = tn[nk - 2];
-        for (k = 1; k < nk - 1; ++k) tni[k] = .5 * (tn[k] + tn[k - 1]);
-        /* alfa matrix, its inverse, salfax . invalfa(:,n) (:100-133) */
+        const double *x = fcomp_out + o;
+        double *d[7];
+        for (n = 0; n < 7; ++n) d[n] = diag + n * slab + o;
+        minor_terms(F, C, nk, col, salfax, w);
         for (k = 0; k < nk; ++k) {
-            double df[3], A[9], Ai[9];
-            for (n = 0; n < 3; ++n) df[n] = pow(tni[k] / t00, 1.75 - MSS[n]);
-#define PH(i, j) MPHI[(i) - 1][(j) - 1]
-            M3(A, 1, 1) = -(PH(1, 4) + (PH(1, 2) - PH(1, 4)) * pso1[k] + (df[0] * PH(1, 3) - PH(1, 4)) * pshe[k]);
-            M3(A, 2, 2) = -(PH(2, 4) + (PH(2, 1) - PH(2, 4)) * pso2[k] + (df[1] * PH(2, 3) - PH(2, 4)) * pshe[k]);
-            M3(A, 3, 3) = -(df[2] * PH(3, 4) + (df[0] * PH(3, 1) - df[2] * PH(3, 4)) * pso2[k] +
-                           (df[1] * PH(3, 2) - df[2] * PH(3, 4)) * pso1[k]);
-            M3(A, 1, 2) = (PH(1, 2) - PH(1, 4)) * pso2[k];
-            M3(A, 1, 3) = (df[0] * PH(1, 3) - PH(1, 4)) * pso2[k];
-            M3(A, 2, 1) = (PH(2, 1) - PH(2, 4)) * pso1[k];
-            M3(A, 2, 3) = (df[1] * PH(2, 3) - PH(2, 4)) * pso1[k];
-            M3(A, 3, 1) = (df[0] * PH(3, 1) - df[2] * PH(3, 4)) * pshe[k];
-            M3(A, 3, 2) = (df[1] * PH(3, 2) - df[2] * PH(3, 4)) * pshe[k];
-            oracle_matinv3(A, Ai);
-            sa1[k] = salfax[0] * M3(Ai, 1, 1) + salfax[1] * M3(Ai, 2, 1) + salfax[2] * M3(Ai, 3, 1);
-            sa2[k] = salfax[0] * M3(Ai, 1, 2) + salfax[1] * M3(Ai, 2, 2) + salfax[2] * M3(Ai, 3, 2);
-            sa3[k] = salfax[0] * M3(Ai, 1, 3) + salfax[1] * M3(Ai, 2, 3) + salfax[2] * M3(Ai, 3, 3);
+            d[0][k] = C->dtx2inv * (x[k] - F->ftm1_smooth[o + k]);
+            d[1][k] = F->sprod[o + k] * C->rmx / F->xnmbar[o + k];
+            d[2][k] = F->sloss[o + k] * x[k];
+            d[3][k] = d[4][k] = d[5][k] = 0.;
+            d[6][k] = -F->hadvec[o + k];
         }
-        /* ex, ax, thdiff (:135-153) */
-        for (k = 0; k < nk; ++k) {
-            ex[k] = 1. - (C->rmx + dmdz[k]) / barm[k] +
-                    sa1[k] * (do2dz[k] - (1. - (C->rmass_o2 + dmdz[k]) / barm[k]) * pso2[k]) +
-                    sa2[k] * (do1dz[k] - (1. - (C->rmass_o1 + dmdz[k]) / barm[k]) * pso1[k]) +
-                    sa3[k] * (dhedz[k] - (1. - (C->rmass_he + dmdz[k]) / barm[k]) * pshe[k]);
-            dmdz[k] = dmdz[k] / barm[k];
-            ax[k] = -(barm[k] / (tau * C->rmass_n2) * pow(t00 / tni[k], 0.25) /
-                      (C->phix[2] + salfax[0] * pso2[k] + salfax[1] * pso1[k] + salfax[2] * pshe[k]));
+        for (k = 1; k < nk - 1; ++k) {
+            const double molp = ax[k] * (1. / dzp + .5 * thdiff[k]);
+            const double molr = ax[k + 1] * (1. / dzp - .5 * thdiff[k + 1]);
+            const double molq = ax[k] * (1. / dzp - .5 * thdiff[k]) + ax[k + 1] * (1. / dzp + .5 * thdiff[k + 1]);
+            const double eddyp = C->expzmid_inv * F->difk[k] * (1. / dzp - .5 * dmdz[k]);
+            const double eddyr = C->expzmid * F->difk[k + 1] * (1. / dzp + .5 * dmdz[k + 1]);
+            const double eddyq = C->expzmid_inv * F->difk[k] * (1. / dzp + .5 * dmdz[k]) +
+                                 C->expzmid * F->difk[k + 1] * (1. / dzp - .5 * dmdz[k + 1]);
+            d[3][k] = -(1. / F->expz[k] / dzp * (molp * x[k - 1] - molq * x[k] + molr * x[k + 1]));
+            d[4][k] = 1. / dzp * (eddyp * x[k - 1] - eddyq * x[k] + eddyr * x[k + 1]);
+            d[5][k] = -(wi[k] / (2. * dzp) * (x[k + 1] - x[k - 1]));
         }
-        for (k = 0; k < nk; ++k) {
-            double dt;
-            if (k == 0) dt = tni[1] - tni[0];
-            else if (k == nk - 1) dt = tni[nk - 1] - tni[nk - 2];
-            else dt = (tni[k + 1] - tni[k - 1]) / 2.;
-            thdiff[k] = ex[k] - C->alfax * dt / (dzp * tni[k]);
-        }
-        for (k = 0; k < nk - 1; ++k) wi[k] = .5 * (ww[k] + ww[k + 1]);
-        wi[nk - 1] = 1.5 * ww[nk - 1] - .5 * ww[nk - 2];
+        for (k = 0; k < nk; ++k) d[4][k] = d[4][k] * F->dfactor[col];
+    }
+    free(w);
+}
+
+ORACLE_API void oracle_minor_ng(const oracle_minor_fields *F, const oracle_minor_consts *C, int nk, long ncol,
+                                double *p_out, double *q_out, double *r_out, double *f_out, double *fcomp_out)
+{
+    const double dzp = C->dzp;
+    double salfax[3];
+    double *w = (double *)malloc(sizeof(double) * 24 * (size_t)nk);
+    double *ax = w, *thdiff = w + nk, *dmdz = w + 2 * nk, *wi = w + 3 * nk, *p = w + 15 * nk, *q = w + 16 * nk,
+           *r = w + 17 * nk, *f = w + 18 * nk, *ws = w + 19 * nk;
+    long col;
+    int k, n;
+    for (n = 0; n < 3; ++n) salfax[n] = C->phix[n] - C->phix[3];
+    for (col = 0; col < ncol; ++col) {
+        const size_t o = (size_t)nk * col;
+        minor_terms(F, C, nk, col, salfax, w);
         /* p, q, r, f (:161-198) */
         const double dfac = F->dfactor[col];
         for (k = 0; k < nk - 1; ++k) {

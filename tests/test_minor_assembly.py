@@ -30,7 +30,7 @@ def matinv3(a):
     return adj / d
 
 
-def minor_numpy(F, C):
+def minor_numpy(F, C, keep=None):
     nk = F["tn"].shape[0]
     tn, o2, o1, he, mbar, barm, w = (F[k] for k in ("tn", "o2", "o1", "he", "mbar", "barm", "w"))
     b, fb, dzp, rmx = C["b"], C["fb"], C["dzp"], C["rmx"]
@@ -114,7 +114,26 @@ def minor_numpy(F, C):
     q[nk - 1] = p[nk - 1] - 2.
     r[nk - 1] = 0.
     f[nk - 1] = -C["grav"] * rmx * F["fubc"] * dzp / (C["p0"] * ax[nk - 1] * C["avo"])
+    if keep is not None:
+        keep.update(molp=molp, molq=molq, molr=molr, eddyp=eddyp, eddyq=eddyq, eddyr=eddyr, wi=wi, s0prod=s0prod)
     return p, q, r, f
+
+
+def minor_diag_numpy(F, C, x):
+    """minor_ng.F90:202-224: the values the reference passes to addfld."""
+    m = {}
+    minor_numpy(F, C, keep=m)
+    nk = x.shape[0]
+    dzp, expz = C["dzp"], F["expz"][:, None]
+    k, km1, kp1 = slice(1, nk - 1), slice(0, nk - 2), slice(2, nk)
+    moldif, eddydif, veradv = (np.zeros_like(x) for _ in range(3))
+    # molp(k) etc. are the rows k of the k = 1..nk-1 arrays
+    moldif[k] = -1 / expz[k] / dzp * (m["molp"][k] * x[km1] - m["molq"][k] * x[k] + m["molr"][k] * x[kp1])
+    eddydif[k] = 1 / dzp * (m["eddyp"][k] * x[km1] - m["eddyq"][k] * x[k] + m["eddyr"][k] * x[kp1])
+    veradv[k] = m["wi"][k] / (2 * dzp) * (x[kp1] - x[km1])
+    eddydif = eddydif * F["dfactor"]
+    return {"DPDT": C["dtx2inv"] * (x - F["ftm1_smooth"]), "PROD": m["s0prod"] * np.ones_like(x),
+            "LOSS": F["sloss"] * x, "MOLDIF": moldif, "EDDYDIF": eddydif, "VERADV": -veradv, "HORADV": -F["hadvec"]}
 
 
 @pytest.mark.parametrize("nk,dz", [(29, 0.5), (57, 0.25), (3, 0.5)])
@@ -133,3 +152,14 @@ def test_minor_inputs_give_a_well_posed_system(pkg, orc):
     x = orc.minor_ng(F, C)
     # the column solution stays at the species' mixing-ratio scale
     assert np.all(np.isfinite(x)) and np.max(np.abs(x)) < 1e-3
+
+
+@pytest.mark.parametrize("nk,dz", [(29, 0.5), (57, 0.25), (3, 0.5)])
+def test_minor_diagnostics_match_independent_transcription(pkg, orc, nk, dz):
+    F, C = pkg.synth.minor_inputs(nk, 41, dz, 7 + nk)
+    x = orc.minor_ng(F, C)
+    got = orc.minor_diag_ng(F, C, x)
+    want = minor_diag_numpy(F, C, x)
+    assert set(got) == set(want)
+    for name in got:
+        assert np.array_equal(got[name], want[name]), name
