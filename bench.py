@@ -159,34 +159,123 @@ def dist_setup(args):
     return world, rank, local
 
 
+METRIC = "column unknowns/s (FP64 path; FP32+FP64-refine path beside it, <=1e-10 rel err)"
+
+
 def host_inputs(pkg, wl, grid, seed_offset=0):
     """numpy (Fortran layout) inputs of one column step of one grid."""
     scal, blk = pkg.synth.column_step(wl, grid, sub=seed_offset)
     return scal, blk
 
 
-def cpu_step(orc, scal, blk, nthreads):
-    for (a, b, c, f) in scal:
-        orc.trsolv_ng(a, b, c, f, a.shape[0], nthreads=nthreads)
-    if blk is not None:
-        P, Q, R, f = blk
-        orc.blksolve(P, Q, R, f, f.shape[1], nthreads=nthreads)
+def nsub_of(g, max_sub):
+    return g.nsub if max_sub is None else min(g.nsub, max_sub)
 
 
-def cpu_unknowns(scal, blk):
-    n = sum(a.size for (a, _, _, _) in scal)
-    if blk is not None:
-        n += blk[3].size
-    return n
+def workload_config(pkg, wl, max_sub):
+    """The `config` object of both arms' JSON lines: the workload's grids,
+    systems and sizes, computed from its definition alone, so that the two
+    arms describe the same work identically."""
+    B = wl.block
+    nsys = wl.n_scalar + (1 if B else 0)
+    unknowns = segments = nbytes = 0
+    for g in wl.grids:
+        n = nsub_of(g, max_sub)
+        unknowns += n * g.ncol * g.nk * (wl.n_scalar + (B or 0))
+        segments += n * nsys
+        nbytes += n * pkg.batch.pad_ld(g.ncol) * g.nk * 8 * (4 * wl.n_scalar + ((3 * B * B + B) if B else 0))
+    return {"workload": wl.name, "grids": [(g.name, g.nlon, g.nlat, g.nk, nsub_of(g, max_sub)) for g in wl.grids],
+            "systems_per_column": nsys, "block": B, "unknowns_per_step": unknowns, "segments": segments,
+            "l2": f"inputs {nbytes / 1e9:.3f} GB per step > 126 MB L2 (no flush needed)",
+            "parallelism": "columns sharded over the ranks (contiguous column ranges, balanced by unknowns)"}
 
 
-def time_cpu(orc, scal, blk, nthreads, steps=None, seconds=None, warmup=1):
+def job_shapes(wl, g):
+    """Fortran-layout shapes of the arrays of one grid sub-step: per scalar
+    system a, b, c, f, x (nk, ncol); the block system P, Q, R (B, B, nk, ncol)
+    and f, u (B, nk, ncol)."""
+    shp = [[(g.nk, g.ncol)] * 5 for _ in range(wl.n_scalar)]
+    if wl.block:
+        B = wl.block
+        shp.append([(B, B, g.nk, g.ncol)] * 3 + [(B, g.nk, g.ncol)] * 2)
+    return shp
+
+
+class HostWorkload:
+    """Every system of one outer step of a workload (or of the given grid
+    sub-steps) in host memory, in the reference's Fortran layout, with
+    preallocated solutions.  Generated by the same seeded law as the device
+    workload (synth.column_step per grid and sub-step), in parallel host
+    threads.  With pinned=True all arrays live in one page-locked arena, as a
+    host model's buffers registered for fast copies would."""
+
+    def __init__(self, pkg, wl, max_sub=None, threads=8, jobs=None, pinned=False):
+        from concurrent.futures import ThreadPoolExecutor
+        if jobs is None:
+            jobs = [(g, sub) for g in wl.grids for sub in range(nsub_of(g, max_sub))]
+        self.jobs = [(g.name, sub) for g, sub in jobs]
+        self.arena = None
+        offs, off = [], 0
+        for g, _ in jobs:
+            o = []
+            for sysshp in job_shapes(wl, g):
+                oo = []
+                for shp in sysshp:
+                    oo.append(off)
+                    off += (int(np.prod(shp)) * 8 + 255) // 256 * 256
+                o.append(oo)
+            offs.append(o)
+        if pinned:
+            import torch
+            self.arena = torch.empty(max(off, 1), dtype=torch.uint8, pin_memory=True)
+            buf = self.arena.numpy()
+        else:
+            buf = np.empty(max(off, 1), dtype=np.uint8)
+
+        def view(o, shp):
+            return np.ndarray(shp, dtype=np.float64, buffer=buf, offset=o, order="F")
+
+        def make(i):
+            g, sub = jobs[i]
+            scal, blk = pkg.synth.column_step(wl, g, sub=sub)
+            out = []
+            for arrs, shps, oo in zip(list(scal) + ([blk] if blk is not None else []), job_shapes(wl, g), offs[i]):
+                vs = [view(o, shp) for o, shp in zip(oo, shps)]
+                for v, a in zip(vs, arrs):
+                    np.copyto(v, a)
+                vs[4][...] = 0.0
+                out.append(tuple(vs))
+            return out
+
+        with ThreadPoolExecutor(max(1, threads)) as ex:
+            per_job = list(ex.map(make, range(len(jobs))))
+        self.scal, self.blk = [], []
+        for systems in per_job:
+            for t in systems:
+                (self.scal if t[0].ndim == 2 else self.blk).append(t)
+
+    def unknowns(self):
+        return sum(a.size for (a, *_r) in self.scal) + sum(t[3].size for t in self.blk)
+
+    def input_bytes(self):
+        return sum(sum(v.nbytes for v in t[:4]) for t in self.scal + self.blk)
+
+    def step(self, orc, nthreads):
+        """One outer step through the oracle port (the reference's FP64
+        arithmetic), OpenMP over the columns of each system."""
+        for (a, b, c, f, x) in self.scal:
+            orc.trsolv_ng(a, b, c, f, a.shape[0], x=x, nthreads=nthreads)
+        for (P, Q, R, f, u) in self.blk:
+            orc.blksolve(P, Q, R, f, f.shape[1], u=u, nthreads=nthreads)
+
+
+def time_host_steps(orc, hw, nthreads, steps=None, seconds=None, warmup=1):
     for _ in range(warmup):
-        cpu_step(orc, scal, blk, nthreads)
+        hw.step(orc, nthreads)
     t0 = time.perf_counter()
     n = 0
     while True:
-        cpu_step(orc, scal, blk, nthreads)
+        hw.step(orc, nthreads)
         n += 1
         el = time.perf_counter() - t0
         if steps is not None and n >= steps:
@@ -196,7 +285,19 @@ def time_cpu(orc, scal, blk, nthreads, steps=None, seconds=None, warmup=1):
     return el / n, n
 
 
+def host_memory_available():
+    try:
+        import psutil
+        return psutil.virtual_memory().available
+    except Exception:
+        return None
+
+
 def run_reference(args):
+    """The reference's CPU implementation of the path on this host's cores:
+    the oracle port (the reference is Fortran and no Fortran compiler exists
+    here), timed on every system of the same workload and config as the
+    GPU arm, rank 0 alone."""
     world, rank, _ = dist_setup(args)
     if rank != 0:
         return 0
@@ -205,24 +306,32 @@ def run_reference(args):
     wl = pkg.synth.workload(args.config)
     if wl.block:
         wl.block = args.block
-    grid = wl.grids[0]
-    scal, blk = host_inputs(pkg, wl, grid)
     nthreads = orc.max_threads()
-    dt, n = time_cpu(orc, scal, blk, nthreads, steps=args.steps, warmup=args.warmup)
-    unk = cpu_unknowns(scal, blk)
-    value = unk / dt
-    sample = f"{grid.name}: {grid.ncol} columns x {grid.nk} levels, {len(scal)} scalar + {1 if blk else 0} block(B={wl.block}) systems per step"
+    cfg = workload_config(pkg, wl, args.max_sub)
+    need = 1.3 * sum(nsub_of(g, args.max_sub) * g.ncol * g.nk * 8 * (5 * wl.n_scalar + ((3 * wl.block ** 2 + 2 * wl.block) if wl.block else 0))
+                     for g in wl.grids)
+    avail = host_memory_available()
+    if avail is None or need < 0.6 * avail:
+        hw = HostWorkload(pkg, wl, args.max_sub, threads=nthreads)
+        sample = (f"every system of every grid and sub-step of the workload ({len(hw.jobs)} grid sub-steps, "
+                  f"{hw.unknowns()} unknowns, {hw.input_bytes() / 1e9:.1f} GB of coefficients) per step")
+    else:
+        # not enough host memory for the whole step: one sub-step of each grid
+        hw = HostWorkload(pkg, wl, threads=nthreads, jobs=[(g, 0) for g in wl.grids])
+        sample = (f"one sub-step of each grid per step ({hw.unknowns()} unknowns; the whole step needs "
+                  f"{need / 1e9:.0f} GB of host memory, {avail / 1e9:.0f} GB available)")
+    dt, n = time_host_steps(orc, hw, nthreads, steps=args.steps, warmup=args.warmup)
+    value = hw.unknowns() / dt
     out = {
-        "impl": "reference", "metric": "column unknowns/s (FP64 path; FP32+FP64-refine path beside it, <=1e-10 rel err)",
-        "value": value, "unit": "unknowns/s",
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "unknowns/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wl.name, "columns": grid.ncol, "levels": grid.nk, "systems": len(scal) + (1 if blk else 0),
-                   "block": wl.block, "parallelism": "host threads"},
-        "cpu_baseline": {"value": value, "unit": "unknowns/s", "cores": nthreads, "kind": "port", "sample": sample},
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded, generated on the host)", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "unknowns/s", "cores": nthreads, "kind": "port",
+                         "sample": sample + ", oracle C port (-O2 -ffp-contract=off), OpenMP over columns"},
         "e2e": {"value": value, "unit": "unknowns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "reference algorithm restated in C (oracle port, -O2 -ffp-contract=off, OpenMP over columns); "
-                "the reference is Fortran and no Fortran compiler is available",
+        "note": "reference algorithm restated in C (oracle port); the reference is Fortran and no Fortran "
+                "compiler is available",
     }
     print(json.dumps(out))
     return 0
@@ -375,7 +484,7 @@ def run_profile(args):
     prec = cs.TG_PREC_F64 if parts[1] == "f64" else cs.TG_PREC_F32_REFINE
     if len(parts) > 2:
         v = parts[2]
-        cand = (v, int(parts[3]), int(parts[4]) if len(parts) > 4 else 4, 4) if v in ("ring", "ringg", "rows", "ring16", "ring8") or v.startswith("chunk") else \
+        cand = (v, int(parts[3]), int(parts[4]) if len(parts) > 4 else 4, 4) if v in ("ring", "ringg", "rows", "ring16", "ring8") or v.startswith(("chunk", "res")) else \
             (v, int(parts[3]), int(parts[4]), int(parts[5]) if len(parts) > 5 else 4)
         autotune.apply(kind, prec, cand)
     dw = pkg.batch.DeviceWorkload(wl, "cuda", max_sub=args.max_sub)
@@ -422,11 +531,14 @@ def main():
     if wl.block:
         wl.block = args.block
 
-    dw = pkg.batch.DeviceWorkload(wl, dev, seed=pkg.synth.SEED_BASE + 7919 * rank, max_sub=args.max_sub)
-    segs = dw.segments()
-    scal_segs = dw.segments((cs.TG_KIND_SCALAR,))
+    # one workload, the same on every rank; each rank solves its share of the
+    # columns (contiguous ranges of the flattened column space, balanced by
+    # unknowns, cut on 32-column tiles): no data-path collective
+    dw = pkg.batch.DeviceWorkload(wl, dev, seed=pkg.synth.SEED_BASE, max_sub=args.max_sub)
+    segs = pkg.batch.shard_segments(dw.segments(), world, rank)
+    scal_segs = [s for s in segs if s["kind"] == cs.TG_KIND_SCALAR]
     blk_segs = [s for s in segs if s["kind"] != cs.TG_KIND_SCALAR]
-    unknowns = dw.unknowns()
+    unknowns = dw.unknowns()                       # the whole job's, over all ranks
     stream = torch.cuda.Stream(device=dev)
 
     def make(seglist, prec):
@@ -563,7 +675,7 @@ def main():
         torch.cuda.empty_cache()
 
     peak, peak_kind = measured_peak()
-    bytes_scalar = dw.algorithmic_bytes((cs.TG_KIND_SCALAR,))
+    bytes_scalar = pkg.batch.segment_bytes(scal_segs)          # this rank's share
     wl_tag = f"{wl.name}_B{wl.block}"
 
     def roofline(name, kernel):
@@ -575,70 +687,95 @@ def main():
                 "traffic": tr, "algorithmic_bytes_per_launch": bytes_scalar, "ms_per_launch": ms,
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s"}
 
-    vref = world * unknowns / (results["refine"] * 1e-3)
-    value = world * unknowns / (results["fp64"] * 1e-3)
+    # the whole job's unknowns over the slowest rank's time
+    vref = unknowns / (results["refine"] * 1e-3)
+    value = unknowns / (results["fp64"] * 1e-3)
     launches_per_step = plans["refine"].launches
 
-    # ---- end to end through the host-pointer C ABI (rank-local, pinned buffers)
+    # ---- end to end through the host-pointer C ABI: this rank's share of the
+    # workload's systems in pinned host memory (Fortran layout), one
+    # tg_solve_host call per step, copies in and out inside the timed region
     e2e = None
     cpu = None
-    if not args.skip_e2e or (rank == 0 and not args.skip_cpu):
-        grid = wl.grids[0]
-        scal_np, blk_np = host_inputs(pkg, wl, grid, seed_offset=rank)
+    jobs_all = [(g, sub) for g in wl.grids for sub in range(nsub_of(g, args.max_sub))]
+    nsys = wl.n_scalar + (1 if wl.block else 0)
     if not args.skip_e2e:
-        def pinned_like(a):
-            t = torch.empty(a.shape[::-1], dtype=torch.float64, pin_memory=True)
-            v = t.numpy().T
-            v[...] = a
-            return t, v
-        keep = []
-        hs = []
-        for (a, b, c, f) in scal_np:
-            arrs = []
-            for v in (a, b, c, f, np.zeros_like(a, order="F")):
-                t, nv = pinned_like(v)
-                keep.append(t)
-                arrs.append(nv)
-            hs.append(arrs)
-        hb = None
-        if blk_np is not None:
-            hb = []
-            for v in (*blk_np, np.zeros_like(blk_np[3], order="F")):
-                t, nv = pinned_like(v)
-                keep.append(t)
-                hb.append(nv)
-        h2d = sum(4 * a.nbytes for (a, *_r) in hs) + (sum(v.nbytes for v in hb[:4]) if hb else 0)
-        d2h = sum(arr[4].nbytes for arr in hs) + (hb[4].nbytes if hb else 0)
-        systems = [dict(kind=cs.TG_KIND_SCALAR, a=a, b=b, c=c, f=f, x=x, k2=a.shape[0]) for (a, b, c, f, x) in hs]
-        if hb:
-            P, Q, R, f, u = hb
-            systems.append(dict(kind=wl.block, a=P, b=Q, c=R, f=f, x=u, k2=f.shape[1]))
+        seg_all = dw.segments()
+        mine = pkg.batch.shard_columns([t["ncol"] for t in seg_all],
+                                       [(1 if t["kind"] == cs.TG_KIND_SCALAR else t["kind"]) * t["k2"] for t in seg_all],
+                                       world, rank, 32)
+        need = sum(sum(int(np.prod(shp)) * 8 for sysshp in job_shapes(wl, g) for shp in sysshp) for g, _ in jobs_all)
+        avail = host_memory_available()
+        whole = avail is None or need * world < 0.5 * avail
+        if whole:
+            jidx = sorted({i // nsys for i, _, _ in mine})
+            hw = HostWorkload(pkg, wl, jobs=[jobs_all[j] for j in jidx], threads=os.cpu_count() or 8, pinned=True)
+            pos = {j: n for n, j in enumerate(jidx)}
+            flat = []
+            for n in range(len(jidx)):   # systems of each job in segment order
+                flat += hw.scal[n * wl.n_scalar:(n + 1) * wl.n_scalar] + ([hw.blk[n]] if wl.block else [])
+            shares = [(flat[pos[i // nsys] * nsys + i % nsys], c0, c1) for i, c0, c1 in mine]
+            what = "this rank's share of every system of the workload"
+        else:
+            # not enough host memory: one sub-step of each grid, whole columns
+            hw = HostWorkload(pkg, wl, jobs=[(g, 0) for g in wl.grids], threads=os.cpu_count() or 8, pinned=True)
+            flat = []
+            for n in range(len(wl.grids)):
+                flat += hw.scal[n * wl.n_scalar:(n + 1) * wl.n_scalar] + ([hw.blk[n]] if wl.block else [])
+            shares = [(t, 0, t[0].shape[-1]) for t in flat]
+            what = (f"one sub-step of each grid (the whole step needs {need * world / 1e9:.0f} GB of pinned host "
+                    f"memory, {avail / 1e9:.0f} GB available)")
+        systems = []
+        h2d = d2h = e2e_unk = 0
+        for t, c0, c1 in shares:
+            v = [a[..., c0:c1] for a in t]
+            if v[0].ndim == 2:
+                systems.append(dict(kind=cs.TG_KIND_SCALAR, a=v[0], b=v[1], c=v[2], f=v[3], x=v[4], k2=v[0].shape[0]))
+            else:
+                systems.append(dict(kind=wl.block, a=v[0], b=v[1], c=v[2], f=v[3], x=v[4], k2=v[3].shape[1]))
+            h2d += sum(a.nbytes for a in v[:4])
+            d2h += v[4].nbytes
+            e2e_unk += v[4].size
 
         def e2e_step():            # one pipelined C-ABI call for the whole step
             cs.solve_host(systems)
 
-        def e2e_percall():         # the per-routine drop-ins, one call per system
-            for (a, b, c, f, x) in hs:
-                cs.trsolv_ng(a, b, c, f, x, a.shape[0])
-            if hb:
-                P, Q, R, f, u = hb
-                cs.blksolve(P, Q, R, f, u, f.shape[1])
-
-        def time_host(fn):
-            for _ in range(max(1, min(args.warmup, 3))):
+        def time_host(fn, steps):
+            for _ in range(max(1, min(args.warmup, 2))):
                 fn()
             torch.cuda.synchronize()
             barrier()
             t0 = time.perf_counter()
-            for _ in range(args.e2e_steps):
+            for _ in range(steps):
                 fn()
             torch.cuda.synchronize()
-            return max_over_ranks((time.perf_counter() - t0) / args.e2e_steps)
-        dt = time_host(e2e_step)
-        dt_pc = time_host(e2e_percall)
+            return max_over_ranks((time.perf_counter() - t0) / steps)
+        dt = time_host(e2e_step, args.e2e_steps)
+        e2e = {"value": (unknowns if whole else world * e2e_unk) / dt, "unit": "unknowns/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3,
+               "steps": args.e2e_steps, "systems_per_call": len(systems),
+               "path": f"tg_solve_host, {what} in one call per step, pinned host Fortran-layout arrays, FP64",
+               "timer": "host wall clock around synchronous C-ABI calls, max over ranks"}
+        # the per-routine drop-ins on the global grid (tg_trsolv_ng per scalar
+        # system, tg_blksolve for the block system), one call per system
+        if world == 1:
+            g0 = flat[:nsys]
+
+            def e2e_percall():
+                for t in g0:
+                    if t[0].ndim == 2:
+                        cs.trsolv_ng(t[0], t[1], t[2], t[3], t[4], t[0].shape[0])
+                    else:
+                        cs.blksolve(t[0], t[1], t[2], t[3], t[4], t[3].shape[1])
+            dt_pc = time_host(e2e_percall, 5)
+            unk_pc = sum(t[4].size for t in g0)
+            e2e["per_call_drop_ins"] = {"value": unk_pc / dt_pc, "ms_per_step": dt_pc * 1e3,
+                                        "path": f"tg_trsolv_ng x{wl.n_scalar} + tg_blksolve on one sub-step of "
+                                                f"{wl.grids[0].name}"}
         # the link this path is bound by: pinned host<->device copy bandwidth
-        hbuf = torch.empty(h2d // 8, dtype=torch.float64, pin_memory=True)
-        dbuf = torch.empty(h2d // 8, dtype=torch.float64, device=dev)
+        nb = min(h2d, 1 << 30) // 8
+        hbuf = torch.empty(nb, dtype=torch.float64, pin_memory=True)
+        dbuf = torch.empty(nb, dtype=torch.float64, device=dev)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         cstream = torch.cuda.Stream(device=dev)
         with torch.cuda.stream(cstream):
@@ -649,40 +786,30 @@ def main():
             hbuf.copy_(dbuf, non_blocking=True)
             ev[2].record(cstream)
         cstream.synchronize()
-        h2d_gbs = h2d / (ev[0].elapsed_time(ev[1]) * 1e-3) / 1e9
-        d2h_gbs = h2d / (ev[1].elapsed_time(ev[2]) * 1e-3) / 1e9
-        del hbuf, dbuf
-        e2e_unk = cpu_unknowns([tuple(h[:4]) for h in hs], tuple(hb[:4]) if hb else None)
-        e2e = {"value": world * e2e_unk / dt, "unit": "unknowns/s", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3, "steps": args.e2e_steps,
-               "path": "tg_solve_host (all systems of one sub-step of the global grid in one call), pinned host "
-                       "Fortran-layout arrays, FP64",
-               "timer": "host wall clock around synchronous C-ABI calls",
-               "per_call_drop_ins": {"value": world * e2e_unk / dt_pc, "ms_per_step": dt_pc * 1e3,
-                                     "path": "tg_trsolv_ng x7 + tg_blksolve"},
-               "link": {"h2d_GBps": h2d_gbs, "d2h_GBps": d2h_gbs,
-                        "h2d_bound_ms_per_step": h2d / h2d_gbs / 1e6}}
-        del keep
+        h2d_gbs = nb * 8 / (ev[0].elapsed_time(ev[1]) * 1e-3) / 1e9
+        d2h_gbs = nb * 8 / (ev[1].elapsed_time(ev[2]) * 1e-3) / 1e9
+        e2e["link"] = {"h2d_GBps": h2d_gbs, "d2h_GBps": d2h_gbs, "h2d_bound_ms_per_step": h2d / h2d_gbs / 1e6}
+        del hbuf, dbuf, systems, shares, flat, hw
 
     if rank == 0 and not args.skip_cpu and world == 1:
+        # the oracle port on a bounded sample of the same workload: one
+        # sub-step of each grid, repeated for --cpu-seconds
         orc = ge.load_oracle()
         nthr = orc.max_threads()
-        dt, n = time_cpu(orc, scal_np, blk_np, nthr, seconds=args.cpu_seconds)
-        cpu = {"value": cpu_unknowns(scal_np, blk_np) / dt, "unit": "unknowns/s", "cores": nthr, "kind": "port",
-               "sample": f"{n} full column steps ({grid.ncol} columns x {grid.nk} levels, {len(scal_np)} scalar + "
-                         f"{1 if blk_np else 0} block systems), oracle C port, OpenMP"}
+        hs = HostWorkload(pkg, wl, jobs=[(g, 0) for g in wl.grids], threads=nthr)
+        dt, n = time_host_steps(orc, hs, nthr, seconds=args.cpu_seconds)
+        cpu = {"value": hs.unknowns() / dt, "unit": "unknowns/s", "cores": nthr, "kind": "port",
+               "sample": f"{n} passes over one sub-step of each grid of the workload ({hs.unknowns()} unknowns, "
+                         f"{len(wl.grids)} grids x {nsys} systems), oracle C port (-O2 -ffp-contract=off), OpenMP"}
+        del hs
 
     if rank == 0:
         out = {
-            "metric": "column unknowns/s (FP64 path; FP32+FP64-refine path beside it, <=1e-10 rel err)",
+            "metric": METRIC,
             "value": value, "unit": "unknowns/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": results["fp64"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": results["fp64"], "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded, generated on device)",
-            "config": {"workload": wl.name, "grids": [(g.name, g.nlon, g.nlat, g.nk, g.nsub if args.max_sub is None else min(g.nsub, args.max_sub)) for g in wl.grids],
-                       "systems_per_column": wl.n_scalar + (1 if wl.block else 0), "block": wl.block,
-                       "unknowns_per_step_per_gpu": unknowns, "segments": len(segs),
-                       "l2": f"inputs {dw.input_bytes() / 1e9:.3f} GB per step > 126 MB L2 (no flush needed)",
-                       "parallelism": f"{world} GPU(s), independent column batches per GPU"},
+            "config": workload_config(pkg, wl, args.max_sub),
             "roofline": roofline("fp64", "k_scalar_f64"),
             "kernels": {k: plans[k].describe() for k in ("fp64", "refine")},
             "fp64": {"value": value, "ms_per_step": results["fp64"], "status": cs.STATUS_NAMES[rc64]},

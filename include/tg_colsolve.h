@@ -99,6 +99,24 @@ int tg_trsolv_ng(const double *a, const double *b, const double *c, const double
  * rows lev0..lev1-1, skipping the periodic columns as duv.F:102-105 does with
  * nlonp4.  The reference's beta, gamma and y arguments are work arrays its
  * callers never read; they are not produced. */
+/* Deferred form of tg_trsolv for the global grid's latitude scans
+ * (src/dt.F:126-330, src/minor.F:491, src/oplus.F:840, src/settei.F:651),
+ * which call trsolv once per latitude slab of ~nlon columns: too few to pay
+ * for a host->device copy, a launch and a device->host copy each.
+ * tg_trsolv_defer takes tg_trsolv's arguments and semantics (rows k1..k2,
+ * periodic columns skipped) but only queues the slab: it copies the solved
+ * rows and columns of a, b, c, f at once (the caller may reuse them for the
+ * next latitude) and remembers x.  tg_trsolv_flush solves every queued slab
+ * in one batched host call (runs of slabs with equal k2-k1+1 form one system)
+ * and writes each slab's rows k1..k2 into its x; x must stay valid and
+ * unread until then.  Same bits as tg_trsolv.  The flush returns the first
+ * status; on a numerical status the x values are written as the reference
+ * would compute them.  One queue per process, safe from several threads; the
+ * flush runs on the calling thread's current device. */
+int tg_trsolv_defer(const double *a, const double *b, const double *c, const double *f, double *x,
+                    int lev0, int lev1, int k1, int k2, int lon0, int lon1, int lonmax);
+int tg_trsolv_flush(void);
+
 int tg_blktri(const double *a, const double *b, const double *c, const double *f,
               double *x, int lev0, int lev1, int lon0, int lon1, int nlonp4);
 
@@ -159,15 +177,16 @@ int tg_blksolve_dev(int B, const double *P, const double *Q, const double *R,
  * whole device-memory budget up front, or a time loop that must not be
  * stalled by the device synchronisation cudaFree implies.  FP64 only,
  * TG_LAYOUT_LEVEL only; results are bit-identical to tg_blksolve_dev.
- * The scratch is a fixed 16 MiB array in the library's device image, held by
- * every GPU that loads the library until the process exits.  Limit: each
- * resident thread needs B*B*k2 doubles and one thread block of the block
- * kernel (64 threads by default) must fit, so k2 <= 3640 for B = 3 and
- * k2 <= 8192 for B = 2; larger k2 returns TG_EINVAL.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (e.g. on two streams) race and must not be
- * issued concurrently. */
+ * The scratch is a fixed 16 MiB array (2^21 doubles) in the library's device
+ * image, held by every GPU that loads the library until the process exits.
+ * Limit: each resident thread needs B*B*k2 doubles and one 64-column thread
+ * block (a fixed tile, whatever tg_set_tile says) must fit:
+ * B*B*k2*64 <= 2^21, so k2 <= 3640 for B = 3 and k2 <= 8192 for B = 2;
+ * larger k2 returns TG_EINVAL.  The first call on a device (and the first
+ * after a device reset) looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (e.g. on two
+ * streams) race and must not be issued concurrently. */
 int tg_blksolve_dev_noalloc(int B, const double *P, const double *Q, const double *R,
                             const double *f, const double *ubc_ratio, const double *ubc_add,
                             double *u, int nk, int k2, int ncol, long ld, int *status_dev,
@@ -327,6 +346,31 @@ int tg_time_filter_ng_dev(int which, const double *cur, const double *prev, doub
                           double dtsmooth_div2, int nk, int ncol, long ld, double *upd, double *nm_upd,
                           void *stream);
 
+/* ---- polar ring filter ------------------------------------------------------
+ * ringfilter (src/ringfilter.F:1-111) over every latitude of a global field
+ * held whole on one device, as filter_o2o (src/comp.F:1065-1145) and the
+ * global dt, oplus, minor and duv filters apply it once the longitudes are
+ * gathered (here no gather is needed).  f is (nk, nlon+4, nlat) in the
+ * reference's layout, longitude index 1..nlon+4 with the interior at
+ * 3..nlon+2 and two periodic points each side, filtered in place.
+ * Latitudes within nlat_filter rows of a pole take chunk_array's chunk count
+ * (cons_module's chunk_array, src/cons.F:331-355); the others are unchanged.
+ * order: Fourier modes kept as the mean, 1..15 and below nlon (filter_o2o 1,
+ * the others 3); poly: 1 for OPLUS's piecewise polynomial reconstruction, 0
+ * the piecewise linear one.  Bit-identical to the reference arithmetic with
+ * sums in longitude order.  The first call with a given (nlon, order,
+ * dlamda) on a device uploads a cos/sin table (synchronously). */
+int tg_ringfilter(double *f, int nk, int nlon, int nlat, int order, int poly, const int *chunk_array,
+                  int nlat_filter, double dlamda);
+/* filter_o2o's filter of one species (src/comp.F:1065-1145): tg_ringfilter
+ * with order 1, linear reconstruction. */
+int tg_filter_o2o(double *fout, int nk, int nlon, int nlat, const int *chunk_array, int nlat_filter,
+                  double dlamda);
+/* Device form: level-major planes, element (k, i, j) at k*ld + i + (nlon+4)*j
+ * (i, j 0-based), on the caller's stream. */
+int tg_ringfilter_dev(double *f, int nk, int nlon, int nlat, int order, int poly, const int *chunk_array,
+                      int nlat_filter, double dlamda, long ld, void *stream);
+
 /* settei_ng's electron and ion temperature step (src/settei_ng.F90:60-261):
  * the whole routine is column-local, so it is one fused kernel: the heat-flux
  * boundary fe, thermal conductivity, the conduction rows in Te^3.5, heating,
@@ -475,7 +519,9 @@ int tg_set_prefetch(int kind, int precision, int levels);
 int tg_set_scratch_global(int kind, int precision, int on);
 /* L2 eviction-priority hints of the bulk-copy (ring) kernels: coefficient
  * streams evict-first, the sweep's scratch and parked w3 evict-last.
- * on: 1 (default), 0 off, -1 back to the default. */
+ * on: 1 (default), 0 off, -1 back to the default; 2 and 3 as 1, except that
+ * the refinement kernels' coefficient fills, which every sweep reads again,
+ * are evict-normal (2) or evict-last (3). */
 int tg_set_cache_hints(int on);
 
 /* FP64 block kinds with a bulk-copy ring: one lane per block row (B lanes per
@@ -494,6 +540,15 @@ int tg_set_block_width(int kind, int width);
  * wait and one round of copies serve L levels; the ring depth set by
  * tg_set_pipeline then counts stages of L levels (2, 3 or 4). */
 int tg_set_stage_levels(int kind, int precision, int levels);
+
+/* Scalar FP64 chunked bulk-copy ring: where the forward sweep keeps w2 and w3
+ * until the back sweep reads them.  0: w2 in an L2 scratch slot per resident
+ * lane, w3 parked in x (k_scalar_f64_chunk); 1: w2 in the warp's shared
+ * memory, w3 parked in x; 2: both in shared memory, so DRAM sees the
+ * coefficients read once and x written once (k_scalar_f64_res).  -1 restores
+ * the default.  Columns too tall for shared memory take mode 0.  Same
+ * arithmetic, same bits. */
+int tg_set_column_residency(int kind, int precision, int mode);
 
 /* Fused assembly routines: 1 (default) two passes where built, the level
  * quantities with one thread per (level, column) then the column walk; 0 one
@@ -538,6 +593,9 @@ int tg_selftest_division(const double *a, const double *b, double *q, long n, vo
 int tg_release_buffers(void);
 /* Library version, e.g. "tg_colsolve 0.1.0 sm_100a". */
 const char *tg_version(void);
+/* The SASS target the library's kernels run as on the current device, as
+ * major*10 + minor (100 for sm_100a); TG_ENODEV without a device. */
+int tg_kernel_arch(int *arch);
 /* Message of the last failing call on this thread. */
 const char *tg_last_error(void);
 

@@ -461,3 +461,22 @@ def smooth_ng(fin, shapiro):
     out = np.zeros_like(a, order="F")
     L.oracle_smooth_ng(_p(a), float(shapiro), nk, nlond - 4, nlatd - 4, _p(out))
     return out
+
+
+def ringfilter(f, order, poly, chunk_array, dlamda):
+    """ringfilter (src/ringfilter.F:1-111) over every latitude of a global
+    field f (nk, nlon+4, nlat); returns the filtered copy."""
+    L = lib()
+    if not hasattr(L, "_ring_bound"):
+        P, D, I = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+        L.oracle_ringfilter.argtypes = [P, I, I, I, I, I, P, I, D]
+        L.oracle_ringfilter.restype = I
+        L._ring_bound = True
+    out = np.array(f, dtype=np.float64, order="F", copy=True)
+    nk, nlonp4, nlat = out.shape
+    ch = np.ascontiguousarray(chunk_array, dtype=np.int32)
+    rc = L.oracle_ringfilter(_p(out), nk, nlonp4 - 4, nlat, int(order), int(poly), ch.ctypes.data, ch.size,
+                             float(dlamda))
+    if rc:
+        raise ValueError("ringfilter: order >= nlon")
+    return out

@@ -1653,3 +1653,98 @@ ORACLE_API void oracle_smooth_ng(const double *fin, double shapiro, int nk, int 
             }
     free(w);
 }
+
+/* ------------------------------------------------------------------------ */
+/* ringfilter (src/ringfilter.F:1-111) over every latitude of a global      */
+/* field held whole, as filter_o2o (src/comp.F:1065-1145) runs it once the  */
+/* longitudes are gathered, without the MPI gather and scatter.  f is       */
+/* (nk, nlon+4, nlat), longitude index 1..nlon+4 with the interior at       */
+/* 3..nlon+2 and two periodic points on each side, filtered in place.       */
+/* Latitude lat (1..nlat) within nlat_filter rows of a pole takes           */
+/* chunk_array's chunk count (src/cons.F:331-355, :25-29 of ringfilter.F);  */
+/* the others are left as they are.  order: Fourier modes kept as the mean  */
+/* (1 for O2O, 3 for TN and the others); poly: 1 for the piecewise          */
+/* polynomial reconstruction of OPLUS (:84-89), 0 the piecewise linear one  */
+/* (:91-94).  Returns 1 (and filters nothing) when order >= nlon, where the */
+/* reference shuts down.  Sums run in index order, as a loop does.          */
+/* ------------------------------------------------------------------------ */
+ORACLE_API int oracle_ringfilter(double *f, int nk, int nlon, int nlat, int order, int poly,
+                                 const int *chunk_array, int nlat_filter, double dlamda)
+{
+    const int nlonp4 = nlon + 4;
+    int lat, k, i, m, ichnk;
+    if (order >= nlon) return 1;
+    double *w = (double *)malloc(sizeof(double) * (size_t)(4 * nlon + 2 * order + 2));
+    double *wm = w + nlon, *fx = wm + nlon, *avg = fx + nlon, *a = avg + nlon, *b = a + order;
+    for (lat = 1; lat <= nlat; ++lat) {
+        int nchnk = 0;
+        if (lat <= nlat_filter) nchnk = chunk_array[lat - 1];
+        else if (lat >= nlat - nlat_filter + 1) nchnk = chunk_array[nlat - lat];
+        if (nchnk == 0) continue;
+        for (k = 0; k < nk; ++k) {
+            /* f(k, i, lat) for the 1-based longitude index i */
+            double *row = f + k + (size_t)nk * (size_t)nlonp4 * (size_t)(lat - 1);
+#define RF(i) row[(size_t)nk * (size_t)((i) - 1)]
+            for (i = 1; i <= nlon; ++i) w[i - 1] = RF(i + 2);
+            /* Fourier series to order `order` (:41-52) */
+            double a0 = 0.;
+            for (i = 0; i < nlon; ++i) a0 = a0 + w[i];
+            a0 = a0 / nlon;
+            for (m = 0; m < order; ++m) a[m] = b[m] = 0.;
+            for (i = 1; i <= nlon; ++i) {
+                const double ang = i * dlamda;
+                for (m = 1; m <= order; ++m) {
+                    a[m - 1] = a[m - 1] + w[i - 1] * cos(m * ang);
+                    b[m - 1] = b[m - 1] + w[i - 1] * sin(m * ang);
+                }
+            }
+            for (m = 0; m < order; ++m) {
+                a[m] = 2. * a[m] / nlon;
+                b[m] = 2. * b[m] / nlon;
+            }
+            /* the series as the mean (:55-61), the deviation (:64) */
+            for (i = 1; i <= nlon; ++i) {
+                const double ang = i * dlamda;
+                double v = a0;
+                for (m = 1; m <= order; ++m) v = v + a[m - 1] * cos(m * ang) + b[m - 1] * sin(m * ang);
+                wm[i - 1] = v;
+                fx[i - 1] = w[i - 1] - v;
+            }
+            /* chunk means (:67-71) and the reconstruction (:73-96) */
+            const int n = nlon / nchnk;
+            for (ichnk = 1; ichnk <= nchnk; ++ichnk) {
+                double s = 0.;
+                for (i = (ichnk - 1) * n; i < ichnk * n; ++i) s = s + fx[i];
+                avg[ichnk - 1] = s / n;
+            }
+            for (ichnk = 1; ichnk <= nchnk; ++ichnk) {
+                int im2 = ichnk - 2, im1 = ichnk - 1, ip1 = ichnk + 1, ip2 = ichnk + 2;
+                if (im2 <= 0) im2 += nchnk;
+                if (im1 <= 0) im1 += nchnk;
+                if (ip1 >= nchnk + 1) ip1 -= nchnk;
+                if (ip2 >= nchnk + 1) ip2 -= nchnk;
+                const double av = avg[ichnk - 1];
+                const double left = (-avg[im2 - 1] + 7. * avg[im1 - 1] + 7. * av - avg[ip1 - 1]) / 12.;
+                const double right = (-avg[im1 - 1] + 7. * av + 7. * avg[ip1 - 1] - avg[ip2 - 1]) / 12.;
+                const double fa = (left + right - 2. * av) / (double)(n * n);
+                const double fb = (3. * av - 2. * left - right) / n;
+                for (m = 1; m <= n; ++m) {
+                    double *x = fx + (ichnk - 1) * n + m - 1;
+                    if (poly)
+                        *x = fa * (3. * (double)(m * m) - 3. * m + 1.) + fb * (2. * m - 1.) + left;
+                    else
+                        *x = (left * (n - m) + right * m) / n;
+                }
+            }
+            /* the full field and its periodic points (:99-104) */
+            for (i = 1; i <= nlon; ++i) RF(i + 2) = fx[i - 1] + wm[i - 1];
+            RF(1) = RF(nlon + 1);
+            RF(2) = RF(nlon + 2);
+            RF(nlon + 3) = RF(3);
+            RF(nlon + 4) = RF(4);
+#undef RF
+        }
+    }
+    free(w);
+    return 0;
+}

@@ -23,12 +23,20 @@ def test_library_exports_all_symbols(pkg):
         assert hasattr(L, name), name
 
 
-def test_library_has_sm100a_code(pkg):
-    import subprocess
-    out = subprocess.run(["cuobjdump", "--list-elf", pkg.colsolve.LIB_PATH], capture_output=True, text=True)
-    if out.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    assert "sm_100a" in out.stdout
+def test_kernel_arch_without_device(pkg):
+    """The architecture query needs a device; without one it says so."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("checks the no-device path")
+    with pytest.raises(pkg.TgError) as e:
+        pkg.colsolve.kernel_arch()
+    assert e.value.status == pkg.TG_ENODEV
+
+
+@pytest.mark.gpu
+def test_library_runs_sm100a_code(cuda, pkg):
+    """The kernels the device loads are the library's sm_100a build."""
+    assert pkg.colsolve.kernel_arch() == 100
 
 
 def test_version_and_host_validation(pkg):

@@ -183,3 +183,35 @@ def test_division_routine_matches_ieee(cuda, pkg):
         ref = a / b
     same = (q.view(np.int64) == ref.view(np.int64)) | (np.isnan(q) & np.isnan(ref))
     assert same.all(), (a[~same][:5], b[~same][:5], q[~same][:5], ref[~same][:5])
+
+
+def test_trsolv_deferred_latitude_scan_bit_exact(cuda, pkg, orc):
+    """The global grid's latitude scan as dt.F runs it (one work array per
+    latitude, reused for the next), with every trsolv call deferred and one
+    flush: each latitude's x equals tg_trsolv's and the oracle's bit for bit.
+    Slabs of two row counts (k2 = lev1-1 and lev1) and a partial-longitude
+    slab make three runs in the flush."""
+    nlev, lonmax, nlat = 57, 148, 72
+    tn_upd = np.full((nlev, lonmax, nlat), -9.0, order="F")
+    refs = {}
+    work = [np.zeros((nlev, lonmax), order="F") for _ in range(4)]
+    for lat in range(nlat):
+        (a, b, c, f), _ = system(pkg, 1, lonmax, seed=500 + lat)
+        for w, v in zip(work, (a, b, c, f)):
+            w[...] = v                    # the scan's reused work arrays
+        k2 = nlev - 1 if lat % 3 else nlev
+        lon0, lon1 = (1, lonmax) if lat != 5 else (3, 80)
+        x = tn_upd[:, lon0 - 1:lon1, lat]
+        args = (1, nlev, 1, k2, lon0, lon1, lonmax)
+        sl = [w[:, lon0 - 1:lon1] for w in work]
+        sl = [np.asfortranarray(v) for v in sl]
+        pkg.trsolv_defer(*sl, x, *args)
+        refs[lat] = orc.trsolv(*sl, np.full(x.shape, -9.0, order="F"), *args)
+        for w in work:
+            w[...] = np.nan               # the caller reuses its arrays at once
+    assert pkg.trsolv_flush() == pkg.TG_OK
+    for lat, ref in refs.items():
+        lon0, lon1 = (1, lonmax) if lat != 5 else (3, 80)
+        assert np.array_equal(tn_upd[:, lon0 - 1:lon1, lat], ref), lat
+    # an empty flush is a no-op
+    assert pkg.trsolv_flush() == pkg.TG_OK

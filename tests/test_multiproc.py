@@ -28,6 +28,26 @@ def test_shard_columns_cover_exactly_once(pkg):
         assert max(loads) - min(loads) <= 2 * max(weights)
 
 
+def test_aligned_shards_start_on_tiles(pkg):
+    """With align=32 every cut inside a segment falls on a 32-column tile
+    boundary; still every column exactly once and the loads balanced to
+    within one aligned block of columns."""
+    sc = pkg.batch.shard_columns
+    ncols, weights = [10368, 6969, 2072, 333, 1], [57, 57, 114, 56, 113]
+    for world in (1, 2, 3, 4, 8):
+        seen = [np.zeros(n, int) for n in ncols]
+        loads = []
+        for r in range(world):
+            load = 0
+            for i, c0, c1 in sc(ncols, weights, world, r, align=32):
+                assert c0 % 32 == 0 and (c1 % 32 == 0 or c1 == ncols[i])
+                seen[i][c0:c1] += 1
+                load += (c1 - c0) * weights[i]
+            loads.append(load)
+        assert all(np.all(s == 1) for s in seen)
+        assert max(loads) - min(loads) <= 2 * 32 * max(weights)
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))

@@ -63,3 +63,53 @@ def test_noalloc_rejects_oversized_columns(cuda, pkg):
     buf = torch.zeros(8, dtype=torch.float64, device="cuda")
     with pytest.raises(cs.TgError, match="exceeds the fixed scratch"):
         cs.blksolve_dev_noalloc(3, buf, buf, buf, buf, buf, nk, nk, 1, ld=1)
+
+
+NO_ALLOC_PROBE = r"""
+import sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+import __graft_entry__ as ge
+torch.cuda.set_device(0)
+pkg = ge.load_package()
+cs = pkg.colsolve
+
+
+def inputs(B, nk, ncol, seed):
+    P, Q, R, f = pkg.synth.block_system(B, nk, ncol, 14.0 / (nk - 1), seed)
+    ld = pkg.batch.pad_ld(ncol)
+    t = [pkg.batch.level_matrix(v, ld, "cuda") for v in (P, Q, R)] + [pkg.batch.level_vector(f, ld, "cuda")]
+    return t, torch.zeros_like(t[3]), ld
+
+
+small, u0, ld0 = inputs(3, 57, 500, 1)
+big, u1, ld1 = inputs(3, 113, 60000, 2)
+st = torch.zeros(2, dtype=torch.int32, device="cuda")
+torch.cuda.synchronize()
+# the first call loads the library's kernels and its fixed array
+cs.blksolve_dev_noalloc(3, *small, u0, 57, 57, 500, ld=ld0, status=st[0:1])
+torch.cuda.synchronize()
+free0 = torch.cuda.mem_get_info()[0]
+# a larger second call: the regular entry would grow its scratch here
+cs.blksolve_dev_noalloc(3, *big, u1, 113, 113, 60000, ld=ld1, status=st[1:2])
+torch.cuda.synchronize()
+free1 = torch.cuda.mem_get_info()[0]
+print("free", free0, free1, "status", st.tolist())
+assert st.tolist() == [0, 0]
+assert free1 == free0, (free0, free1)
+"""
+
+
+def test_noalloc_leaves_free_device_memory_unchanged(cuda, pkg):
+    """In a fresh process whose first library call is this entry: a second,
+    larger call leaves the device's free memory exactly as it was (the
+    regular entry would have grown its scratch buffer for it)."""
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    r = subprocess.run([sys.executable, "-c", NO_ALLOC_PROBE, ROOT], capture_output=True, text=True, timeout=600,
+                       env=dict(os.environ, CUDA_MODULE_LOADING="LAZY"))
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "free" in r.stdout

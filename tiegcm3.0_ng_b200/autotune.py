@@ -11,7 +11,9 @@ from a CUDA graph, CUDA-event timed) and keeps the fastest:
             ("ring") or global ("ringg") memory; for block kinds also one lane
             per block row ("rows", depth 4 or 8) and 16 or 8 columns per warp
             ("ring16", "ring8"); for the scalar kind a ring of stages holding 2, 4
-            or 8 levels each ("chunk2", "chunk4", "chunk8")
+            or 8 levels each ("chunk2", "chunk4", "chunk8"), and the same ring with
+            the sweep's w2 ("res1cL") or w2 and w3 ("res2cL") resident in
+            shared memory, L levels per stage
   FP32+ref  columns per block x prefetch depth; scalar kind also the
             bulk-copy refinement ring of 2, 3 or 4 stages ("ring")
 
@@ -33,7 +35,9 @@ SCALAR_F64 = [("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg"
               ("ring", 4, 4, 4), ("ring", 8, 4, 4), ("ring", 4, 2, 4),
               ("ringg", 4, 1, 4), ("ringg", 8, 1, 4), ("ringg", 4, 2, 4), ("ringg", 4, 4, 4), ("ringg", 4, 8, 4),
               ("chunk2", 4, 1, 4), ("chunk4", 2, 1, 4), ("chunk4", 3, 1, 4), ("chunk4", 4, 1, 4), ("chunk8", 2, 1, 4),
-              ("chunk4", 2, 2, 4)]
+              ("chunk4", 2, 2, 4),
+              ("res1c4", 2, 1, 4), ("res1c4", 3, 1, 4), ("res1c4", 4, 1, 4), ("res1c2", 4, 1, 4),
+              ("res2c4", 2, 1, 4), ("res2c4", 3, 1, 4), ("res2c4", 4, 1, 4), ("res2c2", 4, 1, 4), ("res2c4", 2, 2, 4)]
 BLOCK_F64 = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 96, 1, 4),
              ("ring", 4, 4, 4), ("ring", 8, 4, 4), ("ring", 4, 2, 4), ("ring", 8, 2, 4), ("ring", 16, 2, 4),
              ("ring", 4, 1, 4), ("ring16", 4, 1, 4), ("ring16", 8, 1, 4), ("ring16", 4, 2, 4), ("ring8", 4, 1, 4),
@@ -57,17 +61,19 @@ def apply(kind, precision, cand):
     if kind == cs.TG_KIND_SCALAR:
         cs.set_prefetch(kind, precision, pf)
         if precision == cs.TG_PREC_F64:
-            cs.set_stage_levels(kind, precision, int(v[5:]) if v.startswith("chunk") else 1)
+            levels = int(v[5:]) if v.startswith("chunk") else int(v[5:]) if v.startswith("res") else 1
+            cs.set_stage_levels(kind, precision, levels)
+            cs.set_column_residency(kind, precision, int(v[3]) if v.startswith("res") else 0)
     elif precision == cs.TG_PREC_F64:
         cs.set_block_rows(kind, 1 if v == "rows" else 0)
         cs.set_block_width(kind, {"ring16": 16, "ring8": 8}.get(v, 32))
-    if v in ("ring", "ringg", "rows", "ring16", "ring8") or v.startswith("chunk"):
+    if v in ("ring", "ringg", "rows", "ring16", "ring8") or v.startswith(("chunk", "res")):
         cs.set_pipeline(kind, precision, p1, p2)    # ring depth, warps per CTA
     else:
         cs.set_pipeline(kind, precision, 0)
         cs.set_tile(kind, precision, p1, p2)
     if scalar64:
-        cs.set_scratch_global(kind, precision, 1 if v in ("regg", "ringg") or v.startswith("chunk") else 0)
+        cs.set_scratch_global(kind, precision, 1 if v in ("regg", "ringg") or v.startswith(("chunk", "res")) else 0)
 
 
 def reset(kind, precision):
@@ -78,6 +84,7 @@ def reset(kind, precision):
     if kind == cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64:
         cs.set_scratch_global(kind, precision, -1)
         cs.set_stage_levels(kind, precision, 0)
+        cs.set_column_residency(kind, precision, -1)
     if kind != cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64:
         cs.set_block_rows(kind, -1)
         cs.set_block_width(kind, 0)

@@ -161,23 +161,10 @@ class DeviceWorkload:
         return [it for it in self.items if kinds is None or it["kind"] in kinds]
 
     def unknowns(self, kinds=None):
-        n = 0
-        for it in self.segments(kinds):
-            B = 1 if it["kind"] == TG_KIND_SCALAR else it["kind"]
-            n += B * it["k2"] * it["ncol"]
-        return n
+        return segment_unknowns(self.segments(kinds))
 
     def algorithmic_bytes(self, kinds=None):
-        """FP64 I/O contract bytes: 40 B per scalar unknown; (3B^2+2B)*8 B per
-        B x B block row."""
-        n = 0
-        for it in self.segments(kinds):
-            if it["kind"] == TG_KIND_SCALAR:
-                n += 40 * it["k2"] * it["ncol"]
-            else:
-                B = it["kind"]
-                n += (3 * B * B + 2 * B) * 8 * it["k2"] * it["ncol"]
-        return n
+        return segment_bytes(self.segments(kinds))
 
     def input_bytes(self):
         n = 0
@@ -187,38 +174,72 @@ class DeviceWorkload:
         return n
 
 
+def segment_unknowns(segs):
+    """Unknowns solved by a list of plan segments: B*k2 per column."""
+    n = 0
+    for it in segs:
+        B = 1 if it["kind"] == TG_KIND_SCALAR else it["kind"]
+        n += B * it["k2"] * it["ncol"]
+    return n
+
+
+def segment_bytes(segs):
+    """FP64 I/O contract bytes of a list of plan segments: 40 B per scalar
+    unknown; (3B^2+2B)*8 B per B x B block row."""
+    n = 0
+    for it in segs:
+        if it["kind"] == TG_KIND_SCALAR:
+            n += 40 * it["k2"] * it["ncol"]
+        else:
+            B = it["kind"]
+            n += (3 * B * B + 2 * B) * 8 * it["k2"] * it["ncol"]
+    return n
+
+
 # ---- sharding across GPUs -------------------------------------------------------
-def shard_columns(ncols, weights, world, rank):
+def shard_columns(ncols, weights, world, rank, align=1):
     """Contiguous share of the flattened column space for one rank.
 
     Segment i has ncols[i] columns of weight weights[i] (unknowns per column:
     B*k2).  The concatenated columns are cut at multiples of total/world in
     weight, so every column goes to exactly one rank and the ranks' unknowns
-    differ by at most one column's weight.  Returns [(segment, c0, c1), ...]."""
+    differ by at most one column's weight (align columns' weight when a cut
+    inside a segment is rounded up to a multiple of align columns, which
+    keeps each share's first column on a tile boundary).  Returns
+    [(segment, c0, c1), ...]."""
     total = sum(n * w for n, w in zip(ncols, weights))
     lo = total * rank // world
     hi = total * (rank + 1) // world
     out = []
     start = 0
+
+    def cut(pos, seg_lo, n, w):
+        # a column belongs to the rank whose range holds its first unknown;
+        # both neighbours of a cut compute it from the same position
+        c = -(-(pos - seg_lo) // w)
+        return min(n, -(-c // align) * align)
+
     for i, (n, w) in enumerate(zip(ncols, weights)):
         seg_lo, seg_hi = start, start + n * w
         a, b = max(lo, seg_lo), min(hi, seg_hi)
         if a < b:
-            # a column belongs to the rank whose range holds its first unknown
-            c0 = -(-(a - seg_lo) // w)
-            c1 = -(-(b - seg_lo) // w)
+            c0 = cut(a, seg_lo, n, w)
+            c1 = cut(b, seg_lo, n, w)
             if c1 > c0:
                 out.append((i, c0, c1))
         start = seg_hi
     return out
 
 
-def shard_segments(segments, world, rank):
-    """Plan segments restricted to this rank's columns (views, no copies)."""
+def shard_segments(segments, world, rank, align=32):
+    """Plan segments restricted to this rank's columns (views, no copies).
+    Cuts inside a segment fall on multiples of `align` columns, so a share
+    starts on a 32-column tile with 16-byte aligned rows and keeps the
+    bulk-copy kernels."""
     ncols = [s["ncol"] for s in segments]
     weights = [(1 if s["kind"] == TG_KIND_SCALAR else s["kind"]) * s["k2"] for s in segments]
     out = []
-    for i, c0, c1 in shard_columns(ncols, weights, world, rank):
+    for i, c0, c1 in shard_columns(ncols, weights, world, rank, align):
         s = dict(segments[i])
         for k in ("a", "b", "c", "f", "x", "ubc_ratio", "ubc_add"):
             if s.get(k) is not None:

@@ -42,8 +42,8 @@ EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor
            "tg_comp_ng_dev", "tg_comp_post_ng", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_advec_ng", "tg_advec_ng_dev", "tg_smooth_ng", "tg_smooth_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
-           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
-           "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_last_error")
+           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_column_residency", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
+           "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_kernel_arch", "tg_ringfilter", "tg_ringfilter_dev", "tg_filter_o2o", "tg_trsolv_defer", "tg_trsolv_flush", "tg_last_error")
 
 
 class TgError(RuntimeError):
@@ -229,6 +229,13 @@ def lib():
             "tg_set_block_rows": [I, I],
             "tg_set_block_width": [I, I],
             "tg_set_stage_levels": [I, I, I],
+            "tg_set_column_residency": [I, I, I],
+            "tg_kernel_arch": [ctypes.POINTER(I)],
+            "tg_ringfilter": [P, I, I, I, I, I, P, I, D],
+            "tg_trsolv_defer": [P, P, P, P, P, I, I, I, I, I, I, I],
+            "tg_trsolv_flush": [],
+            "tg_filter_o2o": [P, I, I, I, P, I, D],
+            "tg_ringfilter_dev": [P, I, I, I, I, I, P, I, D, Lg, P],
             "tg_set_assembly_mode": [I],
             "tg_set_block_scratch_budget": [D],
             "tg_set_scalar_scratch_budget": [D],
@@ -260,6 +267,46 @@ def lib():
 
 def version():
     return lib().tg_version().decode()
+
+
+def _chunks(chunk_array):
+    ch = np.ascontiguousarray(chunk_array, dtype=np.int32)
+    return ch, ch.ctypes.data, int(ch.size)
+
+
+def ringfilter(f, order, poly, chunk_array, dlamda):
+    """ringfilter (src/ringfilter.F) over every latitude of the global field
+    f (nk, nlon+4, nlat), Fortran-ordered float64, filtered in place."""
+    if f.ndim != 3:
+        raise ValueError("ringfilter: f must be (nk, nlon+4, nlat)")
+    nk, nlonp4, nlat = f.shape
+    ch, cp, nf = _chunks(chunk_array)
+    return _check(lib().tg_ringfilter(_host(f, "f"), nk, nlonp4 - 4, nlat, int(order), int(poly), cp, nf,
+                                      float(dlamda)), "tg_ringfilter", numeric_ok=False)
+
+
+def filter_o2o(fout, chunk_array, dlamda):
+    """filter_o2o (src/comp.F:1065-1145): the order-1 ring filter of one species, in place."""
+    if fout.ndim != 3:
+        raise ValueError("filter_o2o: fout must be (nk, nlon+4, nlat)")
+    nk, nlonp4, nlat = fout.shape
+    ch, cp, nf = _chunks(chunk_array)
+    return _check(lib().tg_filter_o2o(_host(fout, "fout"), nk, nlonp4 - 4, nlat, cp, nf, float(dlamda)),
+                  "tg_filter_o2o", numeric_ok=False)
+
+
+def ringfilter_dev(f, nk, nlon, nlat, order, poly, chunk_array, dlamda, ld, stream=None):
+    """Device form on level-major planes (k, i + (nlon+4)*j) at stride ld."""
+    ch, cp, nf = _chunks(chunk_array)
+    return _check(lib().tg_ringfilter_dev(_dptr(f), nk, nlon, nlat, int(order), int(poly), cp, nf, float(dlamda),
+                                          int(ld), _stream(stream)), "tg_ringfilter_dev", numeric_ok=False)
+
+
+def kernel_arch():
+    """SASS target of the library's kernels on the current device (100 for sm_100a)."""
+    v = ctypes.c_int(0)
+    _check(lib().tg_kernel_arch(ctypes.byref(v)), "tg_kernel_arch", numeric_ok=False)
+    return v.value
 
 
 def _check(rc, where, numeric_ok=True):
@@ -306,6 +353,31 @@ def trsolv(a, b, c, f, x, lev0, lev1, k1, k2, lon0, lon1, lonmax, lat=None, ideb
     rc = lib().tg_trsolv(_host(a, "a"), _host(b, "b"), _host(c, "c"), _host(f, "f"), _out(x, "x"),
                          lev0, lev1, k1, k2, lon0, lon1, lonmax)
     return _check(rc, "tg_trsolv")
+
+
+_deferred_x = []   # the x arrays of queued slabs, kept alive until the flush
+
+
+def trsolv_defer(a, b, c, f, x, lev0, lev1, k1, k2, lon0, lon1, lonmax, lat=None, idebug=0):
+    """tg_trsolv_defer: queue one latitude slab (arguments as trsolv); a, b,
+    c, f are copied now and may be reused; x is written by trsolv_flush()."""
+    nlev, nlon = lev1 - lev0 + 1, lon1 - lon0 + 1
+    for v, n in ((a, "a"), (b, "b"), (c, "c"), (f, "f"), (x, "x")):
+        if v.shape != (nlev, nlon):
+            raise ValueError(f"trsolv_defer: {n} must have shape {(nlev, nlon)}")
+    rc = lib().tg_trsolv_defer(_host(a, "a"), _host(b, "b"), _host(c, "c"), _host(f, "f"), _out(x, "x"),
+                               lev0, lev1, k1, k2, lon0, lon1, lonmax)
+    _check(rc, "tg_trsolv_defer", numeric_ok=False)
+    _deferred_x.append(x)
+    return rc
+
+
+def trsolv_flush():
+    """tg_trsolv_flush: solve every queued slab and write their x."""
+    try:
+        return _check(lib().tg_trsolv_flush(), "tg_trsolv_flush")
+    finally:
+        _deferred_x.clear()
 
 
 def trsolv_ng(a, b, c, f, x, k2, i_ng=None):
@@ -707,6 +779,11 @@ def set_block_width(kind, width):
 def set_stage_levels(kind, precision, levels):
     """Levels per ring stage of the scalar FP64 ring with w2 in global scratch (1, 2, 4, 8)."""
     return _check(lib().tg_set_stage_levels(int(kind), int(precision), int(levels)), "tg_set_stage_levels")
+
+
+def set_column_residency(kind, precision, mode):
+    """Scalar FP64 chunked ring: 0 w2 in L2 scratch, 1 w2 in shared memory, 2 w2 and w3 in shared memory, -1 default."""
+    return _check(lib().tg_set_column_residency(int(kind), int(precision), int(mode)), "tg_set_column_residency")
 
 
 def set_assembly_mode(mode):

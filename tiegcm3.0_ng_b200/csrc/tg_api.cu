@@ -404,6 +404,22 @@ extern "C" {
 
 __attribute__((visibility("default"))) const char *tg_version(void) { return "tg_colsolve 0.1.0 sm_100a"; }
 
+__attribute__((visibility("default"))) int tg_kernel_arch(int *arch)
+{
+    if (!arch) {
+        set_err("tg_kernel_arch: null argument");
+        return TG_EINVAL;
+    }
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        set_err("no CUDA device available");
+        return TG_ENODEV;
+    }
+    TG_CUDA(kernel_binary_version(arch));
+    return TG_OK;
+}
+
 __attribute__((visibility("default"))) const char *tg_last_error(void) { return g_err; }
 
 __attribute__((visibility("default"))) int tg_set_refine(int max_sweeps, double rel_tol)
@@ -547,6 +563,118 @@ __attribute__((visibility("default"))) int tg_trsolv(const double *a, const doub
     const double *m[3] = {a + off, b + off, c + off};
     return host_solve(TG_KIND_SCALAR, m, f + off, x + off, nlev, k2 - k1 + 1, lonend - lonbeg + 1, nullptr,
                       nullptr, g_host_precision);
+}
+
+}  // extern "C"
+
+// Deferred latitude slabs (tg_trsolv_defer, tg_trsolv_flush).  The global
+// callers of trsolv assemble each latitude into work arrays they reuse for
+// the next one, so a slab is copied when it is queued: rows k1..k2 of the
+// solved columns of a, b, c, f go to page-locked staging, one region per
+// array, slab after slab; each slab's columns are then nrows-long contiguous
+// columns, and consecutive slabs of equal nrows form one (nrows, sum ncol)
+// system.  The flush solves every run in one batched host call and copies the
+// solutions to each slab's x.  One queue per process, guarded by a mutex.
+namespace {
+struct DeferSlab {
+    double *x;        // row k1 of the first solved column of the caller's x
+    long xstride;     // elements between the caller's columns (lev1-lev0+1)
+    int nrows;        // k2-k1+1
+    long ncol;
+    size_t off;       // first element in each staging region
+};
+struct DeferQueue {
+    std::mutex mu;
+    std::vector<DeferSlab> slabs;
+    double *in = nullptr;    // page-locked: regions a, b, c, f of cap elements each
+    double *out = nullptr;   // page-locked: cap elements
+    size_t cap = 0, used = 0;
+};
+DeferQueue g_defer;
+
+int defer_reserve(DeferQueue &q, size_t need)
+{
+    if (need <= q.cap) return TG_OK;
+    size_t cap = std::max(need, std::max(2 * q.cap, (size_t)1 << 20));
+    double *in = nullptr, *out = nullptr;
+    if (cudaHostAlloc((void **)&in, sizeof(double) * 4 * cap, cudaHostAllocPortable) != cudaSuccess ||
+        cudaHostAlloc((void **)&out, sizeof(double) * cap, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        if (in) cudaFreeHost(in);
+        set_err("tg_trsolv_defer: page-locked staging of %zu MB not available", sizeof(double) * 5 * cap >> 20);
+        return TG_ENOMEM;
+    }
+    for (int r = 0; r < 4 && q.used; ++r) memcpy(in + r * cap, q.in + r * q.cap, sizeof(double) * q.used);
+    if (q.in) cudaFreeHost(q.in);
+    if (q.out) cudaFreeHost(q.out);
+    q.in = in;
+    q.out = out;
+    q.cap = cap;
+    return TG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+__attribute__((visibility("default"))) int tg_trsolv_defer(const double *a, const double *b, const double *c,
+                                                           const double *f, double *x, int lev0, int lev1, int k1,
+                                                           int k2, int lon0, int lon1, int lonmax)
+{
+    const int nlev = lev1 - lev0 + 1;
+    if (!a || !b || !c || !f || !x || nlev < 1 || k1 < lev0 || k2 > lev1 || k2 < k1 || lon1 < lon0) {
+        set_err("tg_trsolv_defer: bad arguments");
+        return TG_EINVAL;
+    }
+    const int lonbeg = lon0 == 1 ? 3 : lon0;
+    const int lonend = lon1 == lonmax ? lon1 - 2 : lon1;
+    if (lonend < lonbeg) return TG_OK;
+    const int nrows = k2 - k1 + 1;
+    const long ncol = lonend - lonbeg + 1;
+    const size_t off0 = (size_t)nlev * (lonbeg - lon0) + (k1 - lev0);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        set_err("no CUDA device available");
+        return TG_ENODEV;
+    }
+    std::lock_guard<std::mutex> lk(g_defer.mu);
+    int rc = defer_reserve(g_defer, g_defer.used + (size_t)nrows * ncol);
+    if (rc) return rc;
+    const double *src[4] = {a, b, c, f};
+    for (int r = 0; r < 4; ++r) {
+        double *dst = g_defer.in + r * g_defer.cap + g_defer.used;
+        for (long i = 0; i < ncol; ++i)
+            memcpy(dst + i * nrows, src[r] + off0 + (size_t)nlev * i, sizeof(double) * nrows);
+    }
+    g_defer.slabs.push_back(DeferSlab{x + off0, nlev, nrows, ncol, g_defer.used});
+    g_defer.used += (size_t)nrows * ncol;
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_trsolv_flush(void)
+{
+    std::lock_guard<std::mutex> lk(g_defer.mu);
+    DeferQueue &q = g_defer;
+    if (q.slabs.empty()) return TG_OK;
+    std::vector<HostSys> hs;
+    for (size_t i = 0; i < q.slabs.size();) {
+        size_t j = i;
+        long ncol = 0;
+        while (j < q.slabs.size() && q.slabs[j].nrows == q.slabs[i].nrows) ncol += q.slabs[j++].ncol;
+        const size_t o = q.slabs[i].off;
+        hs.push_back(HostSys{TG_KIND_SCALAR, {q.in + o, q.in + q.cap + o, q.in + 2 * q.cap + o}, q.in + 3 * q.cap + o,
+                             q.out + o, (long)q.slabs[i].nrows, q.slabs[i].nrows, ncol, nullptr, nullptr});
+        i = j;
+    }
+    const int rc = host_solve_many(hs.data(), (int)hs.size(), g_host_precision);
+    const bool numeric = rc == TG_OK || rc == TG_EPIVOT || rc == TG_ENONFINITE || rc == TG_ENOCONV;
+    if (numeric)
+        for (const DeferSlab &d : q.slabs)
+            for (long i = 0; i < d.ncol; ++i)
+                memcpy(d.x + d.xstride * i, q.out + d.off + (size_t)d.nrows * i, sizeof(double) * d.nrows);
+    q.slabs.clear();
+    q.used = 0;
+    return rc;
 }
 
 __attribute__((visibility("default"))) int tg_blktri(const double *a, const double *b, const double *c,
@@ -1013,6 +1141,83 @@ __attribute__((visibility("default"))) int tg_smooth_ng_dev(const double *fin, d
     if (!horiz_args_ok("tg_smooth_ng_dev", nk, nlon, nlat, ld, true)) return TG_EINVAL;
     TG_CUDA(launch_smooth_ng(fin, shapiro, nk, nlon, nlat, ld, fout, (cudaStream_t)stream));
     return TG_OK;
+}
+
+// The polar ring filter: the latitudes it changes and their chunk counts
+// (src/ringfilter.F:24-33), checked against the filter's limits.
+static bool ring_rows(const char *who, int nk, int nlon, int nlat, int order, const int *chunk_array,
+                      int nlat_filter, RingRows *rows)
+{
+    if (nk < 1 || nk > 65535 || nlon < 1 || nlon > (1 << 20) || nlat < 1 || nlat > 500000 || order < 1 ||
+        order > kMaxRingOrder || order >= nlon || nlat_filter < 0 || (nlat_filter > 0 && !chunk_array) ||
+        ringfilter_smem_bytes(nlon) > (size_t)(200 * 1024)) {
+        set_err("%s: bad arguments (nk=%d nlon=%d nlat=%d order=%d nlat_filter=%d; order must be 1..%d and below "
+                "nlon)", who, nk, nlon, nlat, order, nlat_filter, kMaxRingOrder);
+        return false;
+    }
+    rows->n = 0;
+    for (int lat = 1; lat <= nlat; ++lat) {
+        int nchnk = 0;
+        if (lat <= nlat_filter) nchnk = chunk_array[lat - 1];
+        else if (lat >= nlat - nlat_filter + 1) nchnk = chunk_array[nlat - lat];
+        if (nchnk == 0) continue;
+        if (nchnk < 3 || nchnk > nlon || rows->n == kMaxRingRows) {
+            set_err("%s: latitude %d: %d chunks (3..nlon allowed, at most %d filtered latitudes)", who, lat, nchnk,
+                    kMaxRingRows);
+            return false;
+        }
+        rows->lat[rows->n] = lat - 1;
+        rows->nchnk[rows->n] = nchnk;
+        ++rows->n;
+    }
+    return true;
+}
+
+__attribute__((visibility("default"))) int tg_ringfilter_dev(double *f, int nk, int nlon, int nlat, int order,
+                                                             int poly, const int *chunk_array, int nlat_filter,
+                                                             double dlamda, long ld, void *stream)
+{
+    RingRows rows;
+    if (!f || !ring_rows("tg_ringfilter_dev", nk, nlon, nlat, order, chunk_array, nlat_filter, &rows))
+        return TG_EINVAL;
+    if (ld < (long)(nlon + 4) * nlat) {
+        set_err("tg_ringfilter_dev: ld %ld below (nlon+4)*nlat", ld);
+        return TG_EINVAL;
+    }
+    TG_CUDA(launch_ringfilter(rows, f, ld, nk, nlon, order, poly ? 1 : 0, dlamda, (cudaStream_t)stream));
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_ringfilter(double *f, int nk, int nlon, int nlat, int order, int poly,
+                                                         const int *chunk_array, int nlat_filter, double dlamda)
+{
+    RingRows rows;
+    if (!f || !ring_rows("tg_ringfilter", nk, nlon, nlat, order, chunk_array, nlat_filter, &rows)) return TG_EINVAL;
+    if (rows.n == 0) return TG_OK;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ncol = (long)(nlon + 4) * nlat, ld = round_up(ncol, 32);
+    const size_t colsz = (size_t)nk * ncol;
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (size_t)nk * ld))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * colsz))) return rc;
+    double *lvl = (double *)c->lvlbuf[0][0].p, *stage = (double *)c->colbuf[0][0].p;
+    cudaStream_t st = c->st[0];
+    TG_CUDA(cudaMemcpyAsync(stage, f, sizeof(double) * colsz, cudaMemcpyHostToDevice, st));
+    TG_CUDA(launch_col_to_level(stage, nk, lvl, ld, nk, ncol, st));
+    TG_CUDA(launch_ringfilter(rows, lvl, ld, nk, nlon, order, poly ? 1 : 0, dlamda, st));
+    TG_CUDA(launch_level_to_col(lvl, ld, stage, nk, nk, ncol, st));
+    TG_CUDA(cudaMemcpyAsync(f, stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_filter_o2o(double *fout, int nk, int nlon, int nlat,
+                                                         const int *chunk_array, int nlat_filter, double dlamda)
+{
+    return tg_ringfilter(fout, nk, nlon, nlat, 1, 0, chunk_array, nlat_filter, dlamda);
 }
 
 // Host forms: the (nk, nlon+4, nlat+4) Fortran arrays are (nk, ncol) column
@@ -1663,6 +1868,16 @@ __attribute__((visibility("default"))) int tg_set_stage_levels(int kind, int pre
     return TG_OK;
 }
 
+__attribute__((visibility("default"))) int tg_set_column_residency(int kind, int precision, int mode)
+{
+    if (kind != TG_KIND_SCALAR || precision != TG_PREC_F64 || mode > 2) {
+        set_err("tg_set_column_residency: applies to TG_KIND_SCALAR, TG_PREC_F64 with mode 0, 1, 2 or -1");
+        return TG_EINVAL;
+    }
+    tg::set_column_residency(kind, precision, mode);
+    return TG_OK;
+}
+
 __attribute__((visibility("default"))) int tg_set_scalar_scratch_budget(double megabytes)
 {
     tg::set_scalar_scratch_budget(megabytes);
@@ -1723,6 +1938,7 @@ __attribute__((visibility("default"))) int tg_plan_describe(const tg_plan *p, ch
         if (g.kind == TG_KIND_SCALAR) {
             if (!f64 && h.stages) snprintf(name, sizeof name, "k_scalar_refine_ring<%d>", h.stages);
             else if (!f64) snprintf(name, sizeof name, "k_scalar_refine<%d>", h.pf);
+            else if (h.stages && h.res) snprintf(name, sizeof name, "k_scalar_f64_res<%d,%d,%d>", h.stages, h.lps, h.res == 2);
             else if (h.stages && h.lps > 1) snprintf(name, sizeof name, "k_scalar_f64_chunk<%d,%d>", h.stages, h.lps);
             else if (h.stages) snprintf(name, sizeof name, "k_scalar_f64_ring<%d,%d>", h.stages, h.w2g);
             else if (h.w2g) snprintf(name, sizeof name, "k_scalar_f64_g<%d>", h.pf);

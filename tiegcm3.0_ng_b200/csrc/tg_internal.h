@@ -86,6 +86,8 @@ struct Shape {
     int rows;           // block ring kernel with one lane per block row
     int bw;             // block ring kernel: columns per warp (32, 16, 8)
     int lps;            // scalar FP64 ring: levels per stage (>1: chunked ring kernel)
+    int res;            // scalar FP64 chunked ring: 1 w2 in shared memory (w3 parked in x), 2 w2 and w3 in
+                        // shared memory (k_scalar_f64_res); 0 L2 scratch (k_scalar_f64_chunk)
     int one_wave;       // the grid holds every tile at once (no grid-stride second pass)
 };
 
@@ -209,7 +211,23 @@ cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *
                             double *sys_out, unsigned *status, cudaStream_t st);
 int oplus_scratch_planes();   // level-major scratch planes of launch_oplus_ng (each nk*ld doubles)
 
+// Polar ring filter (tg_filter.cu): the latitudes it filters, with their
+// chunk counts; planes (k, i + (nlon+4)*j) at stride ld.
+constexpr int kMaxRingRows = 128;    // filtered latitudes (both polar bands)
+constexpr int kMaxRingOrder = 15;    // Fourier modes kept as the mean
+struct RingRows {
+    int n;
+    int lat[kMaxRingRows];     // 0-based latitude index
+    int nchnk[kMaxRingRows];   // chunks of that latitude
+};
+size_t ringfilter_smem_bytes(int nlon);
+cudaError_t launch_ringfilter(const RingRows &rows, double *f, long ld, int nk, int nlon, int order, int poly,
+                              double dlamda, cudaStream_t st);
+
 cudaError_t launch_selftest_wait(unsigned polls, unsigned *status, cudaStream_t st);
+// binaryVersion of the library's kernels as loaded on the current device
+// (major*10 + minor of the SASS target: 100 for sm_100a).
+cudaError_t kernel_binary_version(int *v);
 
 // Block kinds: the bulk-copy ring kernel with one lane per block row
 // (tg_set_block_rows); 1 on, 0 off, -1 default.
@@ -220,6 +238,11 @@ void set_block_width(int kind, int w);
 // Scalar FP64 ring with w2 in global scratch: levels per ring stage (1, 2, 4,
 // 8; other values restore the default).
 void set_stage_levels(int kind, int precision, int l);
+// Scalar FP64 chunked ring: where the sweep's w2/w3 live between the forward
+// and back sweeps (0 L2 scratch, 1 w2 in shared memory, 2 w2 and w3 in shared
+// memory; other values restore the default).
+void set_column_residency(int kind, int precision, int mode);
+int column_residency();
 // L2 budget (MB) for the Gamma scratch of all resident block-kernel warps;
 // <= 0 restores the default 96 MB.
 void set_block_scratch_budget(double mb);

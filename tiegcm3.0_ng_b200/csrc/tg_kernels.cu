@@ -144,6 +144,20 @@ __device__ __forceinline__ unsigned long long l2_policy(int hints, bool keep)
         asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
     return p;
 }
+// Coefficient fills of the refinement kernels, which read a, b, c, f (P, Q,
+// R, f) once per sweep: hints 2 and 3 keep them in L2 between the sweeps
+// (evict-normal, evict-last) instead of marking them evict-first.
+__device__ __forceinline__ unsigned long long refine_fill_policy(int hints)
+{
+    unsigned long long p;
+    if (hints == 2)
+        asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    else if (hints == 3)
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else
+        p = l2_policy(hints, false);
+    return p;
+}
 __device__ __forceinline__ void bulk_load_hint(void *dst, const void *src, uint32_t bytes, unsigned long long *bar,
                                                unsigned long long pol)
 {
@@ -622,6 +636,188 @@ __global__ void __launch_bounds__(256) k_scalar_f64_chunk(SegTable tab, double *
 }
 
 // ---------------------------------------------------------------------------
+// Scalar Thomas, FP64, chunked bulk-copy ring with the column's sweep
+// quantities resident in shared memory.  w2(k) of the warp's 32 columns for
+// every level (and, with W3S, w3(k) too) stay in this warp's slice of shared
+// memory from the forward sweep to the back sweep, so DRAM sees a, b, c, f
+// read once and x written once; k_scalar_f64_chunk sends w2 to an L2 scratch
+// slot and parks w3 in x, and part of that spills to DRAM when L2 is busy.
+// Without W3S, w3 is still parked in x (an L2 line written and re-read), which
+// halves the shared memory per warp: more warps per SM, more copies in flight.
+// The first chunks of the warp's next tile are requested before its back
+// sweep, so the copy engine keeps streaming while the warp substitutes.
+// Same arithmetic and operation order as k_scalar_f64_chunk: same bits.
+// Shared memory per warp: C*4L ring rows + (k2max-1) w2 rows (+ as many w3
+// rows with W3S; the top level's w3 stays in a register), 256 B each.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr long res_rows(int C, int L, int k2max, bool w3s)
+{
+    return (long)C * 4 * L + (long)(k2max > 1 ? k2max - 1 : 1) * (w3s ? 2 : 1);
+}
+
+template <int C, int L>
+__device__ __forceinline__ void chunk_issue(double *buf, unsigned long long *bar, const double *src, long ld, int k2,
+                                            unsigned qc, int j, int lane, unsigned long long pol)
+{
+    const int st = (int)(qc % C), l0 = j * L;
+    const int nl = k2 - l0 < L ? k2 - l0 : L;
+    if (lane == 0) mbar_expect(&bar[st], (uint32_t)(4 * nl * 256));
+    __syncwarp();
+    if (lane < 4 * nl) bulk_load_hint(buf + (st * 4 * L + lane) * 32, src + (long)l0 * ld, 256u, &bar[st], pol);
+}
+
+template <int C, int L, bool W3S>
+__global__ void __launch_bounds__(256) k_scalar_f64_res(SegTable tab, unsigned *status)
+{
+    constexpr int NE = 4 * L;
+    static_assert(NE <= 32, "one copy per lane");
+    __shared__ __align__(8) unsigned long long bars[8 * C];
+    extern __shared__ __align__(128) double smem_r[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int K = tab.k2max;
+    double *buf = smem_r + (long)warp * res_rows(C, L, K, W3S) * 32;
+    double *w2c = buf + C * NE * 32 + lane;                      // w2(k) at w2c[k*32]
+    double *w3c = w2c + (long)(K > 1 ? K - 1 : 1) * 32;          // w3(k) at w3c[k*32] (W3S)
+    unsigned long long *bar = bars + warp * C;
+    const unsigned long long pol = l2_policy(tab.hints, false), keep = l2_policy(tab.hints, true);
+    if (lane == 0) {
+#pragma unroll 1
+        for (int i = 0; i < C; ++i) mbar_init(&bar[i], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    const int arr = lane & 3;
+    // this lane's copy source (row lane/4 of array lane%4) of tile t of segment s
+    auto source = [&](const Seg &s, int t) -> const double * {
+        return (arr == 0 ? s.a : arr == 1 ? s.b : arr == 2 ? s.c : s.f) + (long)(t - s.tile0) * 32 +
+               (long)(lane >> 2) * s.ld;
+    };
+    const int tstride = gridDim.x * nwarps;
+    unsigned q = 0;
+    int issued = 0;   // chunks of the current tile requested during the previous tile
+    for (int t = blockIdx.x * nwarps + warp; t < tab.ntiles; t += tstride) {
+        const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
+        const long col0 = (long)(t - s.tile0) * 32;
+        const long ld = s.ld;
+        const int k2 = s.k2;
+        const bool valid = col0 + lane < s.ncol;
+        const double *src = source(s, t);
+        double *px = s.x + col0 + lane;
+        const int nch = (k2 + L - 1) / L;
+        const int pre = nch < C ? nch : C;
+        for (int j = issued; j < pre; ++j) chunk_issue<C, L>(buf, bar, src, ld, k2, q + j, j, lane, pol);
+        bool ok = true;
+        double w1 = 0.0, y1 = 0.0, w3 = 0.0, w2 = 0.0;   // w2: the next level's, from this pivot
+        for (int j = 0; j < nch; ++j) {
+            const unsigned qc = q + j;
+            if (!mbar_wait_warp(&bar[qc % C], (qc / C) & 1u)) {
+                const unsigned qe = q + (j + C < nch ? j + C : nch);
+#pragma unroll 1
+                for (unsigned r = qc; r < qe; ++r) mbar_wait_warp(&bar[r % C], (r / C) & 1u);
+                if (lane == 0) report(status, s.status_idx, FLAG_TIMEOUT);
+                return;
+            }
+            const double *stg = buf + (int)(qc % C) * NE * 32 + lane;
+            // level k from stage row l: both divisions by the pivot w1(k)
+            // under one range test, as in k_scalar_f64_chunk
+            auto step = [&](int l, int k, bool first, bool last) {
+                const double ak = stg[(4 * l + 0) * 32], bk = stg[(4 * l + 1) * 32], fk = stg[(4 * l + 3) * 32],
+                             ck = stg[(4 * l + 2) * 32];
+                w1 = first ? bk : xsub(bk, xmul(ak, w2));
+                y1 = __drcp_rn(w1);
+                const double num = first ? fk : xsub(fk, xmul(ak, w3));
+                if (max(exp_dist(w1), max(exp_dist(num), exp_dist(ck))) < kExpSpan) {
+                    w3 = div_markstein(num, w1, y1);
+                    w2 = div_markstein(ck, w1, y1);
+                } else {
+                    const bool w1s = exp_safe(w1);
+                    w3 = qdiv_pivot(num, w1, y1, w1s);
+                    w2 = qdiv_pivot(ck, w1, y1, w1s);
+                    if (!w1s) ok = ok && finite_nz(w1);
+                }
+                if (!last) w2c[k * 32] = w2;
+                if (W3S) {
+                    if (!last) w3c[k * 32] = w3;
+                } else {
+                    st_hint(&px[k * ld], w3, keep);
+                }
+            };
+            if (valid) {
+                if (j > 0 && (j + 1) * L < k2) {   // a full chunk, neither level 0 nor the top
+#pragma unroll
+                    for (int l = 0; l < L; ++l) step(l, j * L + l, false, false);
+                } else {
+#pragma unroll
+                    for (int l = 0; l < L; ++l) {
+                        const int k = j * L + l;
+                        if (k < k2) step(l, k, k == 0, k + 1 == k2);
+                    }
+                }
+            }
+            __syncwarp();
+            fence_proxy_async();
+            if (j + C < nch) chunk_issue<C, L>(buf, bar, src, ld, k2, qc + C, j + C, lane, pol);
+        }
+        q += nch;
+        // the ring is free: request the next tile's first chunks before the
+        // back sweep, which needs only the resident rows
+        issued = 0;
+        {
+            const int tn = t + tstride;
+            if (tn < tab.ntiles) {
+                const Seg sn = tab.segs ? tab.segs[find_seg(tab, tn)] : tab.one;
+                const int nchn = (sn.k2 + L - 1) / L;
+                issued = nchn < C ? nchn : C;
+                const double *srcn = source(sn, tn);
+                for (int j = 0; j < issued; ++j) chunk_issue<C, L>(buf, bar, srcn, sn.ld, sn.k2, q + j, j, lane, pol);
+            }
+        }
+        if (valid) {
+            // x(k2-1) = w3(k2-1); a non-finite x(k+1) makes every lower x
+            // non-finite, so x(0) finite <=> every x finite
+            double xn = w3;
+            if (W3S) {
+                px[(k2 - 1) * ld] = xn;
+#pragma unroll 4
+                for (int k = k2 - 2; k >= 0; --k) {
+                    xn = xsub(w3c[k * 32], xmul(w2c[k * 32], xn));
+                    px[k * ld] = xn;
+                }
+            } else {
+                double rw[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (k2 - 2 - u >= 0) rw[u] = px[(k2 - 2 - u) * ld];
+                int kb = k2 - 2;
+                for (; kb - 7 >= 0; kb -= 4) {   // four levels and their refills all in range
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = kb - u;
+                        xn = xsub(rw[u], xmul(w2c[k * 32], xn));
+                        rw[u] = px[(k - 4) * ld];
+                        px[k * ld] = xn;
+                    }
+                }
+                for (; kb >= 0; kb -= 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = kb - u;
+                        if (k >= 0) {
+                            xn = xsub(rw[u], xmul(w2c[k * 32], xn));
+                            if (k - 4 >= 0) rw[u] = px[(k - 4) * ld];
+                            px[k * ld] = xn;
+                        }
+                    }
+                }
+            }
+            const bool fin = finite(xn);
+            report(status, s.status_idx, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Scalar Thomas, FP32 sweeps + FP64 iterative refinement.
 //
 // Sweep 0 factors A in FP32 (w2 = c/w1 and 1/w1 kept in shared memory) and
@@ -887,7 +1083,7 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
     float *gy = gri + K * S;                                // plane 2: y(k)
     const float *rirow = scratch + K * S + slot0;           // row k of plane 1 for this warp
     unsigned long long *bar = bars + warp * C;
-    const unsigned long long pol = l2_policy(tab.hints, false), keep = l2_policy(tab.hints, true);
+    const unsigned long long pol = refine_fill_policy(tab.hints), keep = l2_policy(tab.hints, true);
     if (lane == 0) {
 #pragma unroll 1
         for (int i = 0; i < C; ++i) mbar_init(&bar[i], 1);
@@ -2092,7 +2288,7 @@ __global__ void __launch_bounds__(256) k_block_refine_ring(SegTable tab, Refine 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     double *buf = smem_b + (long)warp * D * NX * 32;
     unsigned long long *bar = bars + warp * D;
-    const unsigned long long pol = l2_policy(tab.hints, false), keep = l2_policy(tab.hints, true);
+    const unsigned long long pol = refine_fill_policy(tab.hints), keep = l2_policy(tab.hints, true);
     const long gs = (long)gridDim.x * blockDim.x;
     float *scr = scratch + (long)blockIdx.x * blockDim.x + threadIdx.x;
     auto S = [&](int k, int e) -> float & { return scr[((long)k * NS + e) * gs]; };
@@ -2612,6 +2808,8 @@ struct TileCfg {
     int rows;              // block ring kernels: one lane per block row (k_block_f64_rows)
     int bw;                // block ring kernels: columns per warp (32, 16 or 8)
     int lps;               // scalar FP64 ring: levels per stage (1: k_scalar_f64_ring, >1: k_scalar_f64_chunk)
+    int res;               // scalar FP64 chunked ring: 0 scratch in L2 (k_scalar_f64_chunk), 1 w2 resident in
+                           // shared memory, w3 parked in x, 2 w2 and w3 resident (k_scalar_f64_res)
 };
 // [kind index: scalar, block2, block3][precision]
 // Defaults: the fastest shapes on a B200 (autotune.py sweeps of the 2.5 deg
@@ -2621,12 +2819,12 @@ struct TileCfg {
 // register kernel of 128 threads; scalar refinement ring of 2 stages and 2x2
 // block refinement ring of depth 4, one warp per CTA each; 3x3 block
 // refinement register kernel of 128 threads.
-const TileCfg kDefaultTile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 2, 0, 8, 1, 0, 32, 1}},
-                                     {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 4, 0, 4, 1, 0, 32, 1}},
-                                     {{128, 1, 0, 0, 4, 4, 0, 32, 1}, {128, 1, 0, 0, 4, 4, 0, 32, 1}}};
-TileCfg g_tile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4}, {64, 1, 2, 0, 8, 1, 0, 32, 1}},
-                        {{64, 1, 4, 0, 4, 1, 0, 32, 1}, {64, 1, 4, 0, 4, 1, 0, 32, 1}},
-                        {{128, 1, 0, 0, 4, 4, 0, 32, 1}, {128, 1, 0, 0, 4, 4, 0, 32, 1}}};
+const TileCfg kDefaultTile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4, 0}, {64, 1, 2, 0, 8, 1, 0, 32, 1, 0}},
+                                     {{64, 1, 4, 0, 4, 1, 0, 32, 1, 0}, {64, 1, 4, 0, 4, 1, 0, 32, 1, 0}},
+                                     {{128, 1, 0, 0, 4, 4, 0, 32, 1, 0}, {128, 1, 0, 0, 4, 4, 0, 32, 1, 0}}};
+TileCfg g_tile[3][2] = {{{256, 1, 2, 1, 4, 1, 0, 32, 4, 0}, {64, 1, 2, 0, 8, 1, 0, 32, 1, 0}},
+                        {{64, 1, 4, 0, 4, 1, 0, 32, 1, 0}, {64, 1, 4, 0, 4, 1, 0, 32, 1, 0}},
+                        {{128, 1, 0, 0, 4, 4, 0, 32, 1, 0}, {128, 1, 0, 0, 4, 4, 0, 32, 1, 0}}};
 int kind_index(int kind) { return kind == TG_KIND_SCALAR ? 0 : (kind == TG_KIND_BLOCK2 ? 1 : 2); }
 constexpr int kMaxDevIdx = 64;
 int g_num_sms[kMaxDevIdx] = {};
@@ -2711,6 +2909,19 @@ cudaError_t with_scalar_chunk(int C, int L, F f)
 #undef TG_CHUNK
     return cudaErrorInvalidValue;
 }
+// Shared-memory-resident scalar kernels by (stages, levels per stage, w3 resident).
+template <typename F>
+cudaError_t with_scalar_res(int C, int L, int w3s, F f)
+{
+#define TG_RES(c, l)                                                 \
+    if (C == c && L == l) {                                          \
+        if (w3s) return f(k_scalar_f64_res<c, l, true>);             \
+        return f(k_scalar_f64_res<c, l, false>);                     \
+    }
+    TG_RES(2, 2) TG_RES(3, 2) TG_RES(4, 2) TG_RES(2, 4) TG_RES(3, 4) TG_RES(4, 4)
+#undef TG_RES
+    return cudaErrorInvalidValue;
+}
 template <typename F>
 cudaError_t with_block_ring(int B, int D, int W, F f)
 {
@@ -2788,6 +2999,9 @@ void device_init()
         for (int dd : {4, 8}) with_block_refine_ring(2, dd, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int c : {2, 3, 4})
             for (int l : {2, 4, 8}) with_scalar_chunk(c, l, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+        for (int c : {2, 3, 4})
+            for (int l : {2, 4})
+                for (int w : {0, 1}) with_scalar_res(c, l, w, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int b : {2, 3})
             for (int d : {4, 8, 16})
                 for (int w : {32, 16, 8})
@@ -2920,6 +3134,12 @@ void set_scalar_scratch_budget(double mb)
 }
 void set_kind_overlap(int mode) { g_kind_overlap.store(mode == 0 || mode == 1 ? mode : -1); }
 int kind_overlap() { return g_kind_overlap.load(); }
+void set_column_residency(int kind, int precision, int mode)
+{
+    if (kind != TG_KIND_SCALAR || precision != TG_PREC_F64) return;
+    g_tile[0][0].res = mode >= 0 && mode <= 2 ? mode : kDefaultTile[0][0].res;
+}
+int column_residency() { return g_tile[0][0].res; }
 void set_stage_levels(int kind, int precision, int l)
 {
     if (kind != TG_KIND_SCALAR || precision != TG_PREC_F64) return;
@@ -2988,6 +3208,15 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         stages = sh->stages = stages < 2 ? 2 : (stages > 4 ? 4 : stages);
     if (kind == TG_KIND_BLOCK2 && precision != TG_PREC_F64 && stages > 0)   // block refinement ring: 4 or 8 levels
         stages = sh->stages = stages > 4 ? 8 : 4;
+    // shared-memory-resident scalar kernel (k_scalar_f64_res): chunked ring of
+    // 2..4 stages of 2 or 4 levels, w2 (and w3) on chip, no global scratch
+    sh->res = 0;
+    if (kind == TG_KIND_SCALAR && precision == TG_PREC_F64 && stages > 0 && g_tile[0][0].res > 0) {
+        sh->res = g_tile[0][0].res;
+        sh->lps = g_tile[0][0].lps == 2 ? 2 : 4;
+        sh->w2g = 0;
+        stages = sh->stages = stages < 2 ? 2 : (stages > 4 ? 4 : stages);
+    }
     if (sh->lps > 1 && stages > 4) stages = sh->stages = 4;
     if (sh->lps > 1 && sh->lps * stages > 16) stages = sh->stages = 2;
     if (sh->lps == 1 && stages > 0 && stages < 4 && precision == TG_PREC_F64)
@@ -2998,9 +3227,15 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     if (stages > 0) {
         // a ring that does not fit in shared memory falls back to the
         // register-prefetch kernel with the same 32-column tile
+        if (sh->res && (size_t)sh->threads / 32 * res_rows(stages, sh->lps, k2max, sh->res == 2) * 256 >
+                           (size_t)(smem_optin() - 1024)) {
+            // columns too tall to stay on chip: the chunked ring with L2 scratch
+            sh->res = 0;
+            sh->w2g = w2g = 1;
+        }
         const size_t need = kind == TG_KIND_SCALAR ? scalar_smem_bytes(precision, sh->threads, 1, k2max, stages, w2g, sh->lps)
                                                    : block_smem_bytes(kind, stages, sh->threads, sh->rows, sh->bw, precision);
-        if (need > (size_t)(smem_optin() - 1024)) {
+        if (!sh->res && need > (size_t)(smem_optin() - 1024)) {
             stages = 0;
             sh->stages = 0;
             sh->threads = 32;
@@ -3011,10 +3246,13 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         }
     }
     if (kind == TG_KIND_SCALAR) {
-        sh->smem = scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max, stages, w2g, sh->lps);
+        sh->smem = sh->res ? (size_t)sh->threads / 32 * res_rows(stages, sh->lps, k2max, sh->res == 2) * 256
+                           : scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max, stages, w2g, sh->lps);
         if (sh->smem > (size_t)(smem_optin() - 1024)) return cudaErrorInvalidConfiguration;
         auto occ = [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); };
-        if (stages > 0 && precision != TG_PREC_F64)
+        if (sh->res)
+            e = with_scalar_res(stages, sh->lps, sh->res == 2, occ);
+        else if (stages > 0 && precision != TG_PREC_F64)
             e = with_scalar_refine_ring(stages, occ);
         else if (stages > 0 && sh->lps > 1)
             e = with_scalar_chunk(stages, sh->lps, occ);
@@ -3056,11 +3294,12 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         const double per_thread = (double)block_scratch_bytes(kind, precision, 1, k2max);
         const long cap = (long)(g_block_scratch_budget / (per_thread * sh->threads));
         if (blocks > cap) blocks = cap > 0 ? cap : 1;
-    } else if (stages > 0) {
+    } else if (stages > 0 && sh->res != 2) {
         // ring kernels: w2 scratch plus the w3 parked in x, 8 B each per level
-        // and column (refinement: three float planes plus x), of every
-        // resident column within the L2 budget
-        const double per_col = precision == TG_PREC_F64 ? (double)(2 * k2max - 1) * 8.0 : (double)k2max * 20.0;
+        // and column (refinement: three float planes plus x; w2 on chip: the
+        // parked w3 alone), of every resident column within the L2 budget
+        const double per_col = sh->res == 1 ? (double)k2max * 8.0
+                               : precision == TG_PREC_F64 ? (double)(2 * k2max - 1) * 8.0 : (double)k2max * 20.0;
         const long cap = (long)(g_scalar_scratch_budget / (per_col * sh->threads * sh->cpt));
         if (blocks > cap) blocks = cap > 0 ? cap : 1;
     }
@@ -3075,7 +3314,7 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
 
 static std::atomic<int> g_cache_hints{1};
 int cache_hints() { return g_cache_hints.load(); }
-void set_cache_hints(int on) { g_cache_hints.store(on < 0 ? 1 : (on ? 1 : 0)); }
+void set_cache_hints(int on) { g_cache_hints.store(on < 0 || on > 3 ? 1 : on); }
 
 cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, Refine rf, double *scratch,
                           unsigned *status, unsigned long long *hist, cudaStream_t st)
@@ -3087,6 +3326,13 @@ cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, R
         t.hints = cache_hints();
         e = with_scalar_refine_ring(sh.stages, [&](auto k) {
             k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, rf, reinterpret_cast<float *>(scratch), status, hist);
+            return cudaSuccess;
+        });
+    } else if (precision == TG_PREC_F64 && sh.stages > 0 && sh.res > 0) {
+        SegTable t = tab;
+        t.hints = cache_hints();
+        e = with_scalar_res(sh.stages, sh.lps, sh.res == 2, [&](auto k) {
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, status);
             return cudaSuccess;
         });
     } else if (precision == TG_PREC_F64 && sh.stages > 0 && sh.lps > 1) {
@@ -3166,6 +3412,14 @@ cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape 
             k_block_refine<3><<<sh.blocks, sh.threads, 0, st>>>(t, rf, fs, status, hist);
     }
     return cudaGetLastError();
+}
+
+cudaError_t kernel_binary_version(int *v)
+{
+    cudaFuncAttributes attr{};
+    const cudaError_t e = cudaFuncGetAttributes(&attr, k_col_to_level);
+    if (e == cudaSuccess) *v = attr.binaryVersion;
+    return e;
 }
 
 static int relayout_blocks(long nrows, long ncols)

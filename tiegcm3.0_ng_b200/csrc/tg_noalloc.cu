@@ -13,6 +13,7 @@
 // block Thomas sweep, B*B doubles per level per resident thread) lives in the
 // fixed array below, which every GPU that loads the library holds until the
 // process exits.  The caller still passes the inputs and outputs.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -26,17 +27,54 @@ namespace {
 constexpr long kScratchDoubles = (16l << 20) / (long)sizeof(double);
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 static __device__ __align__(256) unsigned g_noalloc_flags[1];
+// Columns per thread block of this entry's launches: fixed, so that its
+// limit (B*B*k2*kTileColumns <= kScratchDoubles) does not depend on the
+// tuning entries.
+constexpr int kTileColumns = 64;
 
-// Device addresses of the two arrays, looked up once per device.  The names
-// above are host-side stand-ins in host code, never device addresses.
+// Device addresses of the two arrays, looked up once per device and context.
+// The names above are host-side stand-ins in host code, never device
+// addresses.  A device reset (cudaDeviceReset) destroys the context and the
+// module; the next context may load the array elsewhere, so the cached
+// addresses are tied to the unique id of the context they were looked up in.
 struct DevPtrs {
     bool ready = false;
+    unsigned long long ctx_id = 0;
     double *scratch = nullptr;
     unsigned *flags = nullptr;
 };
 constexpr int kMaxDev = 64;
 DevPtrs g_ptrs[kMaxDev];
 std::mutex g_mu;
+
+// Unique id of the calling thread's current context (driver entries reached
+// through the runtime, so the library needs no link to libcuda); 0 when none
+// is current or the driver cannot say.
+unsigned long long current_ctx_id()
+{
+    typedef CUresult (*GetCurrent)(CUcontext *);
+    typedef CUresult (*GetId)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (GetCurrent)fn;
+        fn = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (GetId)fn;
+        cudaGetLastError();
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
 
 int device_ptrs(DevPtrs *out)
 {
@@ -48,6 +86,10 @@ int device_ptrs(DevPtrs *out)
     }
     std::lock_guard<std::mutex> lk(g_mu);
     DevPtrs &p = g_ptrs[dev];
+    // a context other than the one of the cached addresses (or none yet,
+    // before the first runtime call on this device): look them up again;
+    // the lookup makes the device's primary context current
+    if (p.ready && (p.ctx_id == 0 || current_ctx_id() != p.ctx_id)) p.ready = false;
     if (!p.ready) {
         e = cudaGetSymbolAddress((void **)&p.scratch, g_noalloc_scratch);
         if (e != cudaSuccess) {
@@ -65,6 +107,7 @@ int device_ptrs(DevPtrs *out)
             tg::record_error(msg);
             return TG_ECUDA;
         }
+        p.ctx_id = current_ctx_id();
         p.ready = true;
     }
     *out = p;
@@ -90,7 +133,7 @@ extern "C" __attribute__((visibility("default"))) int tg_blksolve_dev_noalloc(
     }
     // Each resident thread needs B*B*k2 doubles; at least one thread block
     // must fit in the fixed scratch.
-    const int threads = tg::cols_per_block(B, TG_PREC_F64);
+    const int threads = kTileColumns;
     const long per_thread = (long)B * B * k2;
     const long max_slots = kScratchDoubles / per_thread;
     if (max_slots < threads) {

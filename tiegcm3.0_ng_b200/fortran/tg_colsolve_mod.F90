@@ -1,7 +1,7 @@
 ! ISO_C_BINDING interface to libtg_colsolve.so (include/tg_colsolve.h) for the
 ! TIE-GCM NG Fortran host.  It declares the C entry points; the drop-in
-! wrappers that keep the reference's subroutine names and arguments are shown
-! in INTEGRATION.md (they need the model's params_module / fields_ng_module).
+! wrappers that keep the reference's subroutine names and arguments belong to
+! the model's side, since they need its params_module / fields_ng_module.
 !
 ! No Fortran compiler exists in the build image, so this module is not
 ! compiled here; the C ABI it binds is exercised from C and Python instead.
@@ -298,5 +298,26 @@ module tg_colsolve_mod
       type(c_ptr), value :: fe, fn
       integer(c_int), value :: nk, ncol
     end function tg_oplus_ng
+
+    ! the polar ring filter of a global field held whole, f(nk, nlonp4, nlat):
+    ! filter_o2o's latscan loop over ringfilter (comp.F:1109-1125) becomes
+    !   istat = tg_filter_o2o(fkij, nlevs, nlon, nlat, chunk_array, nlat_filter, dlamda)
+    integer(c_int) function tg_ringfilter(f, nk, nlon, nlat, order, poly, chunk_array, nlat_filter, dlamda) &
+        bind(C, name="tg_ringfilter")
+      import :: c_int, c_double
+      real(c_double), intent(inout) :: f(*)
+      integer(c_int), value :: nk, nlon, nlat, order, poly, nlat_filter
+      integer(c_int), intent(in) :: chunk_array(*)
+      real(c_double), value :: dlamda
+    end function tg_ringfilter
+
+    integer(c_int) function tg_filter_o2o(fout, nk, nlon, nlat, chunk_array, nlat_filter, dlamda) &
+        bind(C, name="tg_filter_o2o")
+      import :: c_int, c_double
+      real(c_double), intent(inout) :: fout(*)
+      integer(c_int), value :: nk, nlon, nlat, nlat_filter
+      integer(c_int), intent(in) :: chunk_array(*)
+      real(c_double), value :: dlamda
+    end function tg_filter_o2o
   end interface
 end module tg_colsolve_mod

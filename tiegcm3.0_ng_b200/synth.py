@@ -514,3 +514,36 @@ def oplus_inputs(nk, ncol, dz, seed, step=60.0, nstep_sub=10, opdiffcap=0.0):
              rk18=4.0E-10, rk21=0.047, rk22=0.171, rk23=8.E-10, rk24=5.0E-12, rk26=7.E-10, rk27=7.7E-5, colfac=1.5,
              opdiffcap=opdiffcap, dtx2inv=1.0 / (2.0 * step), dz=dz, dlev=dz, nstep_sub=nstep_sub)
     return f, c
+
+
+# ---------------------------------------------------------------------------
+# Global fields for the polar ring filter (ringfilter, filter_o2o)
+# ---------------------------------------------------------------------------
+# Chunk counts of the ring filter by latitude row from each pole, per global
+# resolution (nlon, nlat): the model's constants (src/cons.F:331-355).
+RING_CHUNKS = {
+    (72, 36): (3, 9, 18, 36, 36),
+    (144, 72): (3, 3, 9, 9, 18, 18, 36, 36, 72, 72),
+    (288, 144): (3, 3, 3, 9, 9, 9, 18, 18, 18, 36, 36, 36, 72, 72, 72, 72, 144, 144, 144, 144, 144),
+    (576, 288): (3, 3, 3, 3, 3, 9, 9, 9, 9, 9, 18, 18, 18, 18, 18, 18, 36, 36, 36, 36, 36, 36, 72, 72, 72, 72, 72,
+                 72, 144, 144, 144, 144, 144, 144, 288, 288, 288, 288, 288, 288),
+}
+
+
+def ring_field(nk, nlon, nlat, seed, lo=0.05, hi=0.3):
+    """A global mixing-ratio-like field (nk, nlon+4, nlat), Fortran order:
+    a smooth zonal wave pattern plus grid-scale noise, with the two periodic
+    longitude points on each side copied from the interior as the model
+    keeps them."""
+    rng = _rng(seed)
+    lon = 2 * np.pi * np.arange(1, nlon + 1) / nlon
+    lat = np.linspace(-np.pi / 2, np.pi / 2, nlat)
+    k = np.arange(nk)[:, None, None]
+    base = (0.5 * (lo + hi) + 0.25 * (hi - lo) * np.cos(lon)[None, :, None] * np.cos(lat)[None, None, :]
+            * np.exp(-k / max(nk, 1)))
+    noise = 0.1 * (hi - lo) * rng.standard_normal((nk, nlon, nlat))
+    f = np.empty((nk, nlon + 4, nlat))
+    f[:, 2:nlon + 2] = base + noise
+    f[:, 0:2] = f[:, nlon:nlon + 2]
+    f[:, nlon + 2:] = f[:, 2:4]
+    return np.asfortranarray(f)
