@@ -248,6 +248,30 @@ int tg_minor_ng(const tg_minor_fields *F, const tg_minor_consts *C, double *fcom
 int tg_minor_ng_dev(const tg_minor_fields *F, const tg_minor_consts *C, double *fcomp_out, int nk, int ncol,
                     long ld, double *system_out, int *status_dev, void *stream);
 
+/* History diagnostics of dt_ng (src/dt_ng.F90:169-191) and minor_ng
+ * (src/minor_ng.F90:202-224): the fields the reference passes to addfld,
+ * computed from the routine's fields and its solution (tn_upd / fcomp_out
+ * rows 1..nk as the solve returns them, before the lateral-boundary
+ * overwrite).  dt_ng: 12 slabs DTDT, DT_SOLAR, DT_HORDIF, DT_RECOMB,
+ * DT_JOULE, DT_MOLDIF, DT_COOL, DT_HORADV (= -horadv), DT_VERADV (= -the
+ * vertical advection), DT_ADIA, DT_CONDUCT (rows 1 and nk zero), DEN (the
+ * density of :133); bit-identical to the reference arithmetic.  minor_ng: 7
+ * slabs D<name>DT, <name>_PROD, <name>_LOSS, <name>_MOLDIF, <name>_EDDYDIF,
+ * -<name>_VERADV, -<name>_HORADV (MOLDIF, EDDYDIF, VERADV rows 1 and nk
+ * zero); MOLDIF and EDDYDIF use the device's fractional powers like
+ * tg_minor_ng (within ~1e-13 relative), the others are bit-identical.
+ * Host forms: fields as for tg_dt_ng / tg_minor_ng, diag (nk, ncol, nd) in
+ * the Fortran layout.  Device forms: level-major planes, diag nd planes of
+ * nk*ld, on the caller's stream. */
+int tg_dt_diag_ng(const tg_dt_fields *F, const tg_dt_consts *C, const double *tn_upd, double *diag, int nk,
+                  int ncol);
+int tg_dt_diag_ng_dev(const tg_dt_fields *F, const tg_dt_consts *C, const double *tn_upd, double *diag, int nk,
+                      int ncol, long ld, void *stream);
+int tg_minor_diag_ng(const tg_minor_fields *F, const tg_minor_consts *C, const double *fcomp_out, double *diag,
+                     int nk, int ncol);
+int tg_minor_diag_ng_dev(const tg_minor_fields *F, const tg_minor_consts *C, const double *fcomp_out, double *diag,
+                         int nk, int ncol, long ld, void *stream);
+
 /* comp_ng's major-species column step (src/comp_ng.F90:74-332): O2, O and He
  * from the 3x3 block-tridiagonal diffusion system, assembled per column and
  * solved for rows 1..nk-1, with the top level from the upper boundary (He
@@ -346,6 +370,36 @@ int tg_time_filter_ng_dev(int which, const double *cur, const double *prev, doub
                           double dtsmooth_div2, int nk, int ncol, long ld, double *upd, double *nm_upd,
                           void *stream);
 
+/* The same post-solve steps fused into the solve: the fused assembly + solve
+ * of dt_ng, minor_ng or oplus_ng (as tg_*_ng_dev) stores every solution row
+ * through them, so the solution is written once, already filtered.  In the
+ * reference's order: the top row (dt_ng, oplus_ng) from the unfiltered
+ * values; then the lateral-boundary overwrite (src/dt_ng.F90:201-206,
+ * src/minor_ng.F90:226-232, src/oplus_ng.F90:330-335), which here takes the
+ * columns flagged in bnd_mask (ncol bytes, nonzero = a boundary column) from
+ * bnd (level-major, the values the caller's lon_b/lat_b give those columns;
+ * bnd_mask and bnd both NULL when there is none); then the time filter into
+ * nm_upd and the floors of TG_FILTER_DT / MINOR / OPLUS.  nm_upd may alias
+ * prev or cur.  Results are the separate solve, overwrite and
+ * tg_time_filter_ng_dev's, bit for bit (to the routine's tolerance for
+ * minor_ng and oplus_ng, whose solves carry the device's fractional powers).
+ * The history diagnostics (tg_dt_diag_ng_dev, tg_minor_diag_ng_dev) need the
+ * unfiltered solution: callers that write them use the separate steps.
+ * Device arrays, level-major, stream-ordered. */
+typedef struct {
+    const double *cur;              /* tn, fcomp, op: the field at this step        */
+    const double *prev;             /* tn_nm, fcomp_tm1, optm1: the previous step   */
+    double *nm_upd;                 /* tn_nm_upd, fcomp_tm1_out, optm1out            */
+    const unsigned char *bnd_mask;  /* per column: nonzero for a lateral boundary   */
+    const double *bnd;              /* boundary values of the flagged columns       */
+    double dtsmooth, dtsmooth_div2;
+} tg_post_step;
+int tg_dt_ng_post_dev(const tg_dt_fields *F, const tg_dt_consts *C, double *tn_upd, int nk, int ncol, long ld,
+                      const tg_post_step *P, int *status_dev, void *stream);
+int tg_minor_ng_post_dev(const tg_minor_fields *F, const tg_minor_consts *C, double *fcomp_out, int nk, int ncol,
+                         long ld, const tg_post_step *P, int *status_dev, void *stream);
+/* tg_oplus_ng_post_dev follows tg_oplus_ng_dev below. */
+
 /* ---- polar ring filter ------------------------------------------------------
  * ringfilter (src/ringfilter.F:1-111) over every latitude of a global field
  * held whole on one device, as filter_o2o (src/comp.F:1065-1145) and the
@@ -431,6 +485,10 @@ int tg_oplus_ng(const tg_oplus_fields *F, const tg_oplus_consts *C, double *opou
 int tg_oplus_ng_dev(const tg_oplus_fields *F, const tg_oplus_consts *C, double *opout, double *xiop2p,
                     double *xiop2d, double *Fe, double *Fn, int nk, int ncol, long ld, double *system_out,
                     int *status_dev, void *stream);
+/* oplus_ng with the post-solve steps fused (see tg_post_step above). */
+int tg_oplus_ng_post_dev(const tg_oplus_fields *F, const tg_oplus_consts *C, double *opout, double *xiop2p,
+                         double *xiop2d, double *Fe, double *Fn, int nk, int ncol, long ld, const tg_post_step *P,
+                         int *status_dev, void *stream);
 
 /* ---- batched, GPU-resident plans ---------------------------------------------
  * A plan solves many independent systems ("segments": any mix of grids, nest

@@ -43,7 +43,14 @@ EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_column_residency", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
-           "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_kernel_arch", "tg_ringfilter", "tg_ringfilter_dev", "tg_filter_o2o", "tg_trsolv_defer", "tg_trsolv_flush", "tg_last_error")
+           "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_kernel_arch", "tg_ringfilter", "tg_ringfilter_dev", "tg_filter_o2o", "tg_trsolv_defer", "tg_trsolv_flush", "tg_dt_diag_ng", "tg_dt_diag_ng_dev", "tg_minor_diag_ng", "tg_minor_diag_ng_dev", "tg_dt_ng_post_dev", "tg_minor_ng_post_dev", "tg_oplus_ng_post_dev", "tg_last_error")
+
+
+class PostStepArgs(ctypes.Structure):
+    """tg_post_step of include/tg_colsolve.h."""
+    _fields_ = [("cur", ctypes.c_void_p), ("prev", ctypes.c_void_p), ("nm_upd", ctypes.c_void_p),
+                ("bnd_mask", ctypes.c_void_p), ("bnd", ctypes.c_void_p), ("dtsmooth", ctypes.c_double),
+                ("dtsmooth_div2", ctypes.c_double)]
 
 
 class TgError(RuntimeError):
@@ -234,6 +241,16 @@ def lib():
             "tg_ringfilter": [P, I, I, I, I, I, P, I, D],
             "tg_trsolv_defer": [P, P, P, P, P, I, I, I, I, I, I, I],
             "tg_trsolv_flush": [],
+            "tg_dt_ng_post_dev": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, I, I, Lg,
+                                  ctypes.POINTER(PostStepArgs), P, P],
+            "tg_minor_ng_post_dev": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, I, I, Lg,
+                                     ctypes.POINTER(PostStepArgs), P, P],
+            "tg_oplus_ng_post_dev": [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), P, P, P, P, P, I, I,
+                                     Lg, ctypes.POINTER(PostStepArgs), P, P],
+            "tg_dt_diag_ng": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, P, I, I],
+            "tg_dt_diag_ng_dev": [ctypes.POINTER(DtFields), ctypes.POINTER(DtConsts), P, P, I, I, Lg, P],
+            "tg_minor_diag_ng": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, P, I, I],
+            "tg_minor_diag_ng_dev": [ctypes.POINTER(MinorFields), ctypes.POINTER(MinorConsts), P, P, I, I, Lg, P],
             "tg_filter_o2o": [P, I, I, I, P, I, D],
             "tg_ringfilter_dev": [P, I, I, I, I, I, P, I, D, Lg, P],
             "tg_set_assembly_mode": [I],
@@ -491,6 +508,60 @@ def minor_ng(fields, consts, fcomp_out):
     return _check(rc, "tg_minor_ng")
 
 
+DT_DIAG_NAMES = ("DTDT", "DT_SOLAR", "DT_HORDIF", "DT_RECOMB", "DT_JOULE", "DT_MOLDIF", "DT_COOL", "DT_HORADV",
+                 "DT_VERADV", "DT_ADIA", "DT_CONDUCT", "DEN")
+MINOR_DIAG_NAMES = ("DPDT", "PROD", "LOSS", "MOLDIF", "EDDYDIF", "VERADV", "HORADV")
+
+
+def dt_diag_ng(fields, consts, tn_upd):
+    """dt_ng's history diagnostics (src/dt_ng.F90:169-191, DEN :133) from the
+    fields and the solution; returns a dict name -> (nk, ncol) array."""
+    nk = tn_upd.shape[0]
+    ncol = tn_upd.size // nk
+    _check_sizes("dt_diag_ng", fields, DT_FIELDS, nk, ncol, two_d=("tlbc", "t_lbc", "ulbc", "vlbc"),
+                 one_d=("expz", "dift"), outs=(("tn_upd", tn_upd),))
+    F = DtFields(*[_host(fields[n], n) for n in DT_FIELDS])
+    C = DtConsts(*[float(consts[n]) for n in DT_CONSTS])
+    out = np.zeros((nk, ncol, len(DT_DIAG_NAMES)), order="F")
+    _check(lib().tg_dt_diag_ng(ctypes.byref(F), ctypes.byref(C), _host(tn_upd, "tn_upd"), out.ctypes.data, nk, ncol),
+           "tg_dt_diag_ng", numeric_ok=False)
+    return {n: out[:, :, i] for i, n in enumerate(DT_DIAG_NAMES)}
+
+
+def minor_diag_ng(fields, consts, fcomp_out):
+    """minor_ng's history diagnostics (src/minor_ng.F90:202-224) from the
+    fields and the solution; returns a dict name -> (nk, ncol) array."""
+    nk = fcomp_out.shape[0]
+    ncol = fcomp_out.size // nk
+    _check_sizes("minor_diag_ng", fields, MINOR_FIELDS, nk, ncol,
+                 two_d=("tlbc", "flbc1", "flbc2", "flbc3", "fubc", "dfactor"), one_d=("expz", "difk"),
+                 outs=(("fcomp_out", fcomp_out),))
+    F = MinorFields(*[_host(fields[n], n) for n in MINOR_FIELDS])
+    C = minor_consts(consts)
+    out = np.zeros((nk, ncol, len(MINOR_DIAG_NAMES)), order="F")
+    _check(lib().tg_minor_diag_ng(ctypes.byref(F), ctypes.byref(C), _host(fcomp_out, "fcomp_out"), out.ctypes.data,
+                                  nk, ncol), "tg_minor_diag_ng", numeric_ok=False)
+    return {n: out[:, :, i] for i, n in enumerate(MINOR_DIAG_NAMES)}
+
+
+def dt_diag_ng_dev(fields, consts, tn_upd, diag, nk, ncol, ld, stream=None):
+    """Device form: level-major fields, diag 12 planes of nk*ld."""
+    F = DtFields(*[_dptr(fields[n]) for n in DT_FIELDS])
+    C = DtConsts(*[float(consts[n]) for n in DT_CONSTS])
+    rc = lib().tg_dt_diag_ng_dev(ctypes.byref(F), ctypes.byref(C), _dptr(tn_upd), _dptr(diag), nk, ncol, ld,
+                                 _stream(stream))
+    return _check(rc, "tg_dt_diag_ng_dev", numeric_ok=False)
+
+
+def minor_diag_ng_dev(fields, consts, fcomp_out, diag, nk, ncol, ld, stream=None):
+    """Device form: level-major fields, diag 7 planes of nk*ld."""
+    F = MinorFields(*[_dptr(fields[n]) for n in MINOR_FIELDS])
+    C = minor_consts(consts)
+    rc = lib().tg_minor_diag_ng_dev(ctypes.byref(F), ctypes.byref(C), _dptr(fcomp_out), _dptr(diag), nk, ncol, ld,
+                                    _stream(stream))
+    return _check(rc, "tg_minor_diag_ng_dev", numeric_ok=False)
+
+
 def comp_ng(fields, consts, o2_upd, o1_upd, he_upd):
     """comp_ng's column step (src/comp_ng.F90:74-332) on host arrays: fields
     COMP_FIELDS ((nk, ncol) Fortran order, fs (12, ncol, nk) C order = the
@@ -550,6 +621,50 @@ def oplus_ng_dev(fields, consts, opout, xiop2p, xiop2d, nk, ncol, ld, Fe=None, F
                                _dptr(Fe), _dptr(Fn), nk, ncol, ld, _dptr(system_out),
                                None if status is None else _int_dptr(status), _stream(stream))
     return _check(rc, "tg_oplus_ng_dev", numeric_ok=False)
+
+
+def _post(post):
+    """post: dict cur, prev, nm_upd (CUDA tensors or device pointers), optional
+    bnd_mask (uint8 per column) and bnd, dtsmooth, dtsmooth_div2."""
+    m = post.get("bnd_mask")
+    if m is not None and not isinstance(m, int):
+        if not m.is_cuda or str(m.dtype) != "torch.uint8":
+            raise TypeError("bnd_mask must be a uint8 CUDA tensor")
+        m = m.data_ptr()
+    return PostStepArgs(_dptr(post["cur"]), _dptr(post["prev"]), _dptr(post["nm_upd"]), m, _dptr(post.get("bnd")),
+                        float(post["dtsmooth"]), float(post["dtsmooth_div2"]))
+
+
+def dt_ng_post_dev(fields, consts, tn_upd, nk, ncol, ld, post, status=None, stream=None):
+    """dt_ng with the lateral overwrite, time filter and floor fused into its back sweep."""
+    F = DtFields(*[_dptr(fields[n]) for n in DT_FIELDS])
+    C = DtConsts(*[float(consts[n]) for n in DT_CONSTS])
+    Pp = _post(post)
+    rc = lib().tg_dt_ng_post_dev(ctypes.byref(F), ctypes.byref(C), _dptr(tn_upd), nk, ncol, ld, ctypes.byref(Pp),
+                                 None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_dt_ng_post_dev", numeric_ok=False)
+
+
+def minor_ng_post_dev(fields, consts, fcomp_out, nk, ncol, ld, post, status=None, stream=None):
+    """minor_ng with the lateral overwrite, time filter and floors fused into its back sweep."""
+    F = MinorFields(*[_dptr(fields[n]) for n in MINOR_FIELDS])
+    C = minor_consts(consts)
+    Pp = _post(post)
+    rc = lib().tg_minor_ng_post_dev(ctypes.byref(F), ctypes.byref(C), _dptr(fcomp_out), nk, ncol, ld,
+                                    ctypes.byref(Pp), None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_minor_ng_post_dev", numeric_ok=False)
+
+
+def oplus_ng_post_dev(fields, consts, opout, xiop2p, xiop2d, nk, ncol, ld, post, Fe=None, Fn=None, status=None,
+                      stream=None):
+    """oplus_ng with the lateral overwrite, time filter and floors fused into its back sweep."""
+    F = OplusFields(*[_dptr(fields[n]) for n in OPLUS_FIELDS])
+    C = oplus_consts(consts)
+    Pp = _post(post)
+    rc = lib().tg_oplus_ng_post_dev(ctypes.byref(F), ctypes.byref(C), _dptr(opout), _dptr(xiop2p), _dptr(xiop2d),
+                                    _dptr(Fe), _dptr(Fn), nk, ncol, ld, ctypes.byref(Pp),
+                                    None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_oplus_ng_post_dev", numeric_ok=False)
 
 
 def settei_ng_dev(fields, consts, te_out, ti_out, qtotal, nk, ncol, ld, system_out=None, status=None, stream=None):

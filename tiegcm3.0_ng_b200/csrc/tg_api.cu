@@ -964,6 +964,218 @@ __attribute__((visibility("default"))) int tg_minor_ng(const tg_minor_fields *F,
     return flags_to_status(c->flags_host[0]);
 }
 
+// ---- history diagnostics of dt_ng and minor_ng (the addfld fields) --------
+// Host forms: the fields and the solution in the Fortran layout, relaid out to
+// level-major planes; diag receives nd slabs of (nk, ncol).
+namespace {
+struct Upload {
+    double *base, *stage;
+    long ld;
+    size_t lvl, colsz;
+    cudaStream_t st;
+};
+int upload3(const Upload &u, int nk, long ncol, const double *src, int i, const double **dst)
+{
+    double *d = u.base + (size_t)i * u.lvl;
+    TG_CUDA(cudaMemcpyAsync(u.stage, src, sizeof(double) * u.colsz, cudaMemcpyHostToDevice, u.st));
+    TG_CUDA(launch_col_to_level(u.stage, nk, d, u.ld, nk, ncol, u.st));
+    *dst = d;
+    return TG_OK;
+}
+int download3(const Upload &u, int nk, long ncol, const double *planes, int nd, double *diag)
+{
+    for (int i = 0; i < nd; ++i) {
+        TG_CUDA(launch_level_to_col(planes + (size_t)i * u.lvl, u.ld, u.stage, nk, nk, ncol, u.st));
+        TG_CUDA(cudaMemcpyAsync(diag + (size_t)i * u.colsz, u.stage, sizeof(double) * u.colsz, cudaMemcpyDeviceToHost,
+                                u.st));
+    }
+    TG_CUDA(cudaStreamSynchronize(u.st));
+    return TG_OK;
+}
+}  // namespace
+
+__attribute__((visibility("default"))) int tg_dt_diag_ng_dev(const tg_dt_fields *F, const tg_dt_consts *C,
+                                                             const double *tn_upd, double *diag, int nk, int ncol,
+                                                             long ld, void *stream)
+{
+    if (!F || !C || !tn_upd || !diag || nk < 3 || ncol < 0 || ld < ncol) {
+        set_err("tg_dt_diag_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    TG_CUDA(launch_dt_diag_ng(*F, *C, tn_upd, nk, ncol, ld, diag, (cudaStream_t)stream));
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_minor_diag_ng_dev(const tg_minor_fields *F, const tg_minor_consts *C,
+                                                                const double *fcomp_out, double *diag, int nk,
+                                                                int ncol, long ld, void *stream)
+{
+    if (!F || !C || !fcomp_out || !diag || nk < 3 || ncol < 0 || ld < ncol) {
+        set_err("tg_minor_diag_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    TG_CUDA(launch_minor_diag_ng(*F, *C, fcomp_out, nk, ncol, ld, diag, (cudaStream_t)stream));
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_dt_diag_ng(const tg_dt_fields *F, const tg_dt_consts *C,
+                                                         const double *tn_upd, double *diag, int nk, int ncol)
+{
+    if (!F || !C || !tn_upd || !diag || nk < 3 || ncol < 0) {
+        set_err("tg_dt_diag_ng: bad arguments (nk=%d ncol=%d)", nk, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    const double *const f3[21] = {F->tn, F->tnsmooth, F->horadv, F->un, F->vn, F->o1, F->mbar, F->xnmbar,
+                                  F->scht, F->schti, F->cp, F->kt, F->km, F->hdt, F->qji_tn, F->cool_imp,
+                                  F->cool_exp, F->w, F->qtotal, F->rkm12, tn_upd};
+    const double *const f2[4] = {F->tlbc, F->t_lbc, F->ulbc, F->vlbc};
+    for (const double *p : f3)
+        if (!p) return set_err("tg_dt_diag_ng: a field pointer is NULL"), TG_EINVAL;
+    for (const double *p : f2)
+        if (!p) return set_err("tg_dt_diag_ng: a field pointer is NULL"), TG_EINVAL;
+    if (!F->expz || !F->dift) return set_err("tg_dt_diag_ng: expz/dift NULL"), TG_EINVAL;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ld = round_up(ncol, 32);
+    Upload u{nullptr, nullptr, ld, (size_t)nk * ld, (size_t)nk * ncol, c->st[0]};
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (33 * u.lvl + 4 * (size_t)ld + 2 * (size_t)nk)))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * u.colsz))) return rc;
+    u.base = (double *)c->lvlbuf[0][0].p;
+    u.stage = (double *)c->colbuf[0][0].p;
+    tg_dt_fields D;
+    const double *x = nullptr;
+    const double **dst3[21] = {&D.tn, &D.tnsmooth, &D.horadv, &D.un, &D.vn, &D.o1, &D.mbar, &D.xnmbar, &D.scht,
+                               &D.schti, &D.cp, &D.kt, &D.km, &D.hdt, &D.qji_tn, &D.cool_imp, &D.cool_exp, &D.w,
+                               &D.qtotal, &D.rkm12, &x};
+    for (int i = 0; i < 21; ++i)
+        if ((rc = upload3(u, nk, ncol, f3[i], i, dst3[i]))) return rc;
+    double *planes = u.base + 21 * u.lvl, *two = u.base + 33 * u.lvl, *one = two + 4 * ld;
+    const double **dst2[4] = {&D.tlbc, &D.t_lbc, &D.ulbc, &D.vlbc};
+    for (int i = 0; i < 4; ++i) {
+        TG_CUDA(cudaMemcpyAsync(two + i * ld, f2[i], sizeof(double) * ncol, cudaMemcpyHostToDevice, u.st));
+        *dst2[i] = two + i * ld;
+    }
+    TG_CUDA(cudaMemcpyAsync(one, F->expz, sizeof(double) * nk, cudaMemcpyHostToDevice, u.st));
+    TG_CUDA(cudaMemcpyAsync(one + nk, F->dift, sizeof(double) * nk, cudaMemcpyHostToDevice, u.st));
+    D.expz = one;
+    D.dift = one + nk;
+    TG_CUDA(launch_dt_diag_ng(D, *C, x, nk, ncol, ld, planes, u.st));
+    return download3(u, nk, ncol, planes, 12, diag);
+}
+
+__attribute__((visibility("default"))) int tg_minor_diag_ng(const tg_minor_fields *F, const tg_minor_consts *C,
+                                                            const double *fcomp_out, double *diag, int nk, int ncol)
+{
+    if (!F || !C || !fcomp_out || !diag || nk < 3 || ncol < 0) {
+        set_err("tg_minor_diag_ng: bad arguments (nk=%d ncol=%d)", nk, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    const double *const f3[13] = {F->tn, F->o2, F->o1, F->he, F->mbar, F->barm, F->xnmbar, F->w, F->ftm1_smooth,
+                                  F->hadvec, F->sloss, F->sprod, fcomp_out};
+    const double *const f2[6] = {F->tlbc, F->flbc1, F->flbc2, F->flbc3, F->fubc, F->dfactor};
+    for (const double *p : f3)
+        if (!p) return set_err("tg_minor_diag_ng: a field pointer is NULL"), TG_EINVAL;
+    for (const double *p : f2)
+        if (!p) return set_err("tg_minor_diag_ng: a field pointer is NULL"), TG_EINVAL;
+    if (!F->expz || !F->difk) return set_err("tg_minor_diag_ng: expz/difk NULL"), TG_EINVAL;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ld = round_up(ncol, 32);
+    Upload u{nullptr, nullptr, ld, (size_t)nk * ld, (size_t)nk * ncol, c->st[0]};
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (20 * u.lvl + 6 * (size_t)ld + 2 * (size_t)nk)))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * u.colsz))) return rc;
+    u.base = (double *)c->lvlbuf[0][0].p;
+    u.stage = (double *)c->colbuf[0][0].p;
+    tg_minor_fields D;
+    const double *x = nullptr;
+    const double **dst3[13] = {&D.tn, &D.o2, &D.o1, &D.he, &D.mbar, &D.barm, &D.xnmbar, &D.w, &D.ftm1_smooth,
+                               &D.hadvec, &D.sloss, &D.sprod, &x};
+    for (int i = 0; i < 13; ++i)
+        if ((rc = upload3(u, nk, ncol, f3[i], i, dst3[i]))) return rc;
+    double *planes = u.base + 13 * u.lvl, *two = u.base + 20 * u.lvl, *one = two + 6 * ld;
+    const double **dst2[6] = {&D.tlbc, &D.flbc1, &D.flbc2, &D.flbc3, &D.fubc, &D.dfactor};
+    for (int i = 0; i < 6; ++i) {
+        TG_CUDA(cudaMemcpyAsync(two + i * ld, f2[i], sizeof(double) * ncol, cudaMemcpyHostToDevice, u.st));
+        *dst2[i] = two + i * ld;
+    }
+    TG_CUDA(cudaMemcpyAsync(one, F->expz, sizeof(double) * nk, cudaMemcpyHostToDevice, u.st));
+    TG_CUDA(cudaMemcpyAsync(one + nk, F->difk, sizeof(double) * nk, cudaMemcpyHostToDevice, u.st));
+    D.expz = one;
+    D.difk = one + nk;
+    TG_CUDA(launch_minor_diag_ng(D, *C, x, nk, ncol, ld, planes, u.st));
+    return download3(u, nk, ncol, planes, 7, diag);
+}
+
+// ---- the post-solve steps fused into the back sweep -------------------------
+static bool post_ok(const char *who, const tg_post_step *P)
+{
+    if (!P || !P->cur || !P->prev || !P->nm_upd || (!P->bnd_mask) != (!P->bnd)) {
+        set_err("%s: bad post-step arguments (cur, prev, nm_upd needed; bnd_mask and bnd both or neither)", who);
+        return false;
+    }
+    return true;
+}
+static PostStep post_of(const tg_post_step *P, double floor, int floor_nm)
+{
+    return PostStep{P->cur, P->prev, P->nm_upd, P->bnd_mask, P->bnd, P->dtsmooth, P->dtsmooth_div2, floor, floor_nm};
+}
+
+__attribute__((visibility("default"))) int tg_dt_ng_post_dev(const tg_dt_fields *F, const tg_dt_consts *C,
+                                                             double *tn_upd, int nk, int ncol, long ld,
+                                                             const tg_post_step *P, int *status_dev, void *stream)
+{
+    if (!F || !C || !tn_upd || nk < 3 || ncol < 0 || ld < ncol || !post_ok("tg_dt_ng_post_dev", P)) {
+        if (!P || P->cur) set_err("tg_dt_ng_post_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    const PostStep post = post_of(P, 100.0, 0);
+    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_dt_ng(*F, *C, tn_upd, nk, ncol, ld, nullptr, cx->flags, st, &post));
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_minor_ng_post_dev(const tg_minor_fields *F, const tg_minor_consts *C,
+                                                                double *fcomp_out, int nk, int ncol, long ld,
+                                                                const tg_post_step *P, int *status_dev, void *stream)
+{
+    if (!F || !C || !fcomp_out || nk < 3 || ncol < 0 || ld < ncol || !post_ok("tg_minor_ng_post_dev", P)) {
+        if (!P || P->cur) set_err("tg_minor_ng_post_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = grow(cx->scratch[0], sizeof(double) * 3 * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
+    const PostStep post = post_of(P, 1.e-12, 1);
+    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_minor_ng(*F, *C, fcomp_out, nk, ncol, ld, nullptr, cx->flags, st, (double *)cx->scratch[0].p,
+                            &post));
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
 static bool comp_fields_ok(const tg_comp_fields *F)
 {
     const double *const p[] = {F->tn, F->o2, F->o1, F->he, F->w, F->mbar, F->o2nm_smooth, F->o1nm_smooth,
@@ -1446,6 +1658,34 @@ __attribute__((visibility("default"))) int tg_oplus_ng_dev(const tg_oplus_fields
     TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
     TG_CUDA(launch_oplus_ng(*F, *C, opout, xiop2p, xiop2d, Fe, Fn, (double *)cx->scratch[0].p, nk, ncol, ld,
                             system_out, cx->flags, st));
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_oplus_ng_post_dev(const tg_oplus_fields *F, const tg_oplus_consts *C,
+                                                                double *opout, double *xiop2p, double *xiop2d,
+                                                                double *Fe, double *Fn, int nk, int ncol, long ld,
+                                                                const tg_post_step *P, int *status_dev, void *stream)
+{
+    if (!F || !C || !opout || !xiop2p || !xiop2d || (!Fe) != (!Fn) || nk < 3 || ncol < 0 || ld < ncol ||
+        !oplus_fields_ok(F) || !post_ok("tg_oplus_ng_post_dev", P)) {
+        if (!P || P->cur) set_err("tg_oplus_ng_post_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t sbytes = sizeof(double) * oplus_scratch_planes() * (size_t)nk * (size_t)(ld > 0 ? ld : 1);
+    if ((rc = grow(cx->scratch[0], sbytes))) return rc;
+    const PostStep post = post_of(P, 0.0, 1);
+    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_oplus_ng(*F, *C, opout, xiop2p, xiop2d, Fe, Fn, (double *)cx->scratch[0].p, nk, ncol, ld, nullptr,
+                            cx->flags, st, &post));
     if (status_dev) {
         k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
         TG_CUDA(cudaGetLastError());

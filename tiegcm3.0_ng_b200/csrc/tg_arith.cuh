@@ -62,4 +62,23 @@ __device__ __forceinline__ double qdiv_pivot(double a, double b, double y, bool 
     return b_safe && exp_safe(a) ? div_markstein(a, b, y) : __ddiv_rn(a, b);
 }
 
+// The store of solution row o with the post-solve steps when `on`: a flagged
+// lateral-boundary column takes its boundary value, the previous-step field
+// is filtered, nm = ds2*(prev + x) + ds*cur, and both are floored (a floor
+// keeps v when v > floor, NaN included otherwise).  The same operations as
+// the reference's statements and as tg_time_filter_ng.
+template <class P>
+__device__ __forceinline__ void post_store(const P &post, bool on, bool bcol, double *out, long o, double x)
+{
+    if (!on) {
+        out[o] = x;
+        return;
+    }
+    if (bcol) x = __ldg(post.bnd + o);
+    // plain loads: nm may alias prev or cur
+    const double n = __dadd_rn(__dmul_rn(post.ds2, __dadd_rn(post.prev[o], x)), __dmul_rn(post.ds, post.cur[o]));
+    post.nm[o] = (!post.floor_nm || n > post.floor) ? n : post.floor;
+    out[o] = x > post.floor ? x : post.floor;
+}
+
 }  // namespace tg

@@ -53,7 +53,7 @@ __device__ __forceinline__ GF dt_gf(const DtConsts &C, double h, double cp, doub
 // same bits as IEEE a/b).
 constexpr int kDtStaged = 20;
 __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *tn_upd, int nk, int ncol, long ld,
-                                               double *sys_out, unsigned *status)
+                                               double *sys_out, unsigned *status, PostStep post, int has_post)
 {
     extern __shared__ double smem_dt[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -212,7 +212,10 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
             qt_p = sg.at(b, 19);
         }
     }
-    // back sweep (trsolv_ng.F90:23-26), then tn(nk) = tn(nk-1)**2/tn(nk-2)
+    // back sweep (trsolv_ng.F90:23-26), then tn(nk) = tn(nk-1)**2/tn(nk-2);
+    // with has_post every row is stored through the post-solve steps
+    // (:201-213), the top row computed from the unfiltered values first
+    const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
     double xn = w3, xprev = w3;
     bool fin = fabs(xn) <= DBL_MAX;
     double park = K >= 2 ? tn_upd[(K - 2) * ld + col] : 0.0;
@@ -222,17 +225,18 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
         if (k >= 1) park = tn_upd[(k - 1) * ld + col];
         xn = xs(wk, xm(w2s[k * T], xn));
         fin = fin && fabs(xn) <= DBL_MAX;
-        tn_upd[k * ld + col] = xn;
+        post_store(post, has_post, bcol, tn_upd, k * ld + col, xn);
         if (k == K - 2) {
             // xprev = x(K-1), xn = x(K-2): the two top solved rows
-            tn_upd[(long)K * ld + col] = xd(xm(xprev, xprev), xn);
+            post_store(post, has_post, bcol, tn_upd, (long)K * ld + col, xd(xm(xprev, xprev), xn));
+            if (has_post) post_store(post, true, bcol, tn_upd, (long)(K - 1) * ld + col, xprev);
         }
     }
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
 cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, int nk, int ncol, long ld,
-                         double *sys_out, unsigned *status, cudaStream_t st)
+                         double *sys_out, unsigned *status, cudaStream_t st, const PostStep *post)
 {
     if (ncol <= 0) return cudaSuccess;
     // one warp per block keeps a wave of small blocks resident despite the
@@ -240,7 +244,111 @@ cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, i
     const int T = 32;
     const size_t smem = (size_t)T * ((nk - 2 > 0 ? nk - 2 : 1) * sizeof(double) + Stage<kDtStaged>::bytes_per_thread);
     once_per_device([] { cudaFuncSetAttribute(k_dt_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin() - 1024); });
-    k_dt_ng<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, tn_upd, nk, ncol, ld, sys_out, status);
+    k_dt_ng<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, tn_upd, nk, ncol, ld, sys_out, status,
+                                                  post ? *post : PostStep{}, post != nullptr);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// dt_ng's history diagnostics (src/dt_ng.F90:169-191, and the density of
+// :133) from the fields and the solution x (rows 1..nk, before the lateral
+// overwrite): 12 level-major planes DTDT, DT_SOLAR, DT_HORDIF, DT_RECOMB,
+// DT_JOULE, DT_MOLDIF, DT_COOL, DT_HORADV, DT_VERADV, DT_ADIA, DT_CONDUCT,
+// DEN, the values the reference hands to addfld.  One thread per (level,
+// column): every term of level k needs only levels k-1..k+1 (the wind shear
+// of the top two levels comes from level nk-3's), so no column walk is
+// needed.  Same operations in the same order as the reference: bit-identical.
+// ---------------------------------------------------------------------------
+namespace {
+__device__ __forceinline__ double dt_vad0(const DtFields &F, int j, int nk, long ld, long col)
+{
+    if (j == 0) return xm(xm(xs(__ldg(F.tn + col), __ldg(F.t_lbc + col)), __ldg(F.w + col)), 2.0);
+    if (j >= nk - 1) return 0.0;
+    return xm(xs(__ldg(F.tn + (long)j * ld + col), __ldg(F.tn + (long)(j - 1) * ld + col)),
+              __ldg(F.w + (long)j * ld + col));
+}
+// .5*(v(k)+v(k+1)), the top level extrapolated as 1.5*v(nk)-.5*v(nk-1)
+__device__ __forceinline__ double dt_iface(const double *v, int k, int nk, long ld, long col)
+{
+    if (k < nk - 1) return xm(0.5, xa(__ldg(v + (long)k * ld + col), __ldg(v + (long)(k + 1) * ld + col)));
+    return xs(xm(1.5, __ldg(v + (long)(nk - 1) * ld + col)), xm(0.5, __ldg(v + (long)(nk - 2) * ld + col)));
+}
+__device__ __forceinline__ double dt_shear(const double *v, const double *vlbc, const DtConsts &C, int k, int nk,
+                                           long ld, long col)
+{
+    auto at = [&](int j) { return __ldg(v + (long)j * ld + col); };
+    auto base = [&](int j) {   // the levels the reference computes directly
+        if (j == 0) return xd(xs(xa(at(0), xm(1.0 / 3.0, at(1))), xm(4.0 / 3.0, __ldg(vlbc + col))), C.dz);
+        return xd(xs(at(j + 1), at(j - 1)), xm(2.0, C.dz));
+    };
+    if (k <= nk - 3) return base(k);
+    const double d = xd(base(nk - 3), 3.0);   // level nk-2
+    return k == nk - 2 ? d : xd(d, 3.0);
+}
+__device__ __forceinline__ double dt_tni(const DtFields &F, int j, int nk, long ld, long col)
+{
+    if (j == 0) return __ldg(F.tlbc + col);
+    if (j == nk - 1) return __ldg(F.tn + (long)(nk - 2) * ld + col);
+    return xm(0.5, xa(__ldg(F.tn + (long)(j - 1) * ld + col), __ldg(F.tn + (long)j * ld + col)));
+}
+}  // namespace
+
+__global__ void __launch_bounds__(256) k_dt_diag_ng(DtFields F, DtConsts C, const double *x, int nk, int ncol, long ld,
+                                                    double *diag)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (col >= ncol) return;
+    const long o = (long)k * ld + col, slab = (long)nk * ld;
+    auto at = [&](const double *p) { return __ldg(p + o); };
+    const double xk = x[o];
+    const double expz = __ldg(F.expz + k);
+    const double vad = k < nk - 1 ? xd(xm(xa(dt_vad0(F, k, nk, ld, col), dt_vad0(F, k + 1, nk, ld, col)), 0.5), C.dz)
+                                  : xd(0.0, C.dz);
+    const double cpi = dt_iface(F.cp, k, nk, ld, col), kmi = dt_iface(F.km, k, nk, ld, col);
+    const double wi = dt_iface(F.w, k, nk, ld, col), qsolar = dt_iface(F.qtotal, k, nk, ld, col);
+    const double dudz = dt_shear(F.un, F.ulbc, C, k, nk, ld, col), dvdz = dt_shear(F.vn, F.vlbc, C, k, nk, ld, col);
+    // density (:126-133)
+    const double h = at(F.schti);
+    double rho = xd(xm(C.p0, C.expzmid_inv), xm(h, C.grav));
+    rho = xm(rho, expz);
+    const double mbar = at(F.mbar);
+    const double xo = xm(xm(at(F.xnmbar), at(F.o1)), C.rmassinv_o1);
+    const double qrecomb = xd(xm(xm(xm(C.tsurplus, at(F.rkm12)), xm(xo, xo)), C.avo), mbar);
+    double qm = xm(xd(xm(C.grav, kmi), xm(C.p0, at(F.scht))), xa(xm(dudz, dudz), xm(dvdz, dvdz)));
+    qm = xd(qm, expz);
+    double *d = diag + o;
+    d[0] = xm(C.dtx2inv, xs(xk, at(F.tnsmooth)));
+    d[slab] = xd(qsolar, cpi);
+    d[2 * slab] = xd(at(F.hdt), cpi);
+    d[3 * slab] = xd(qrecomb, cpi);
+    d[4 * slab] = xd(at(F.qji_tn), cpi);
+    d[5 * slab] = xd(qm, cpi);
+    const double cool_exp = xd(xd(at(F.cool_exp), cpi), expz);
+    d[6 * slab] = xs(-cool_exp, xm(at(F.cool_imp), xk));
+    d[7 * slab] = -at(F.horadv);
+    d[8 * slab] = -vad;
+    d[9 * slab] = -xm(xd(xm(wi, C.gask), xm(cpi, mbar)), xk);
+    // conductive heating (:181-186), rows 2..nk-1
+    double cond = 0.0;
+    if (k >= 1 && k <= nk - 2) {
+        const GF g0 = dt_gf(C, h, at(F.cp), at(F.kt), dt_tni(F, k, nk, ld, col), expz, __ldg(F.dift + k));
+        const long o1 = o + ld;
+        const GF g1 = dt_gf(C, __ldg(F.schti + o1), __ldg(F.cp + o1), __ldg(F.kt + o1), dt_tni(F, k + 1, nk, ld, col),
+                            __ldg(F.expz + k + 1), __ldg(F.dift + k + 1));
+        const double t = xa(xs(xm(xs(g0.g, g0.f), x[o - ld]), xm(xa(xa(xs(g1.g, g1.f), g0.g), g0.f), xk)),
+                            xm(xa(g1.g, g1.f), x[o1]));
+        cond = xm(xd(1.0, expz), t);
+    }
+    d[10 * slab] = xd(cond, cpi);
+    d[11 * slab] = rho;
+}
+
+cudaError_t launch_dt_diag_ng(const DtFields &F, const DtConsts &C, const double *x, int nk, int ncol, long ld,
+                              double *diag, cudaStream_t st)
+{
+    if (ncol <= 0) return cudaSuccess;
+    k_dt_diag_ng<<<dim3((ncol + 255) / 256, nk), 256, 0, st>>>(F, C, x, nk, ncol, ld, diag);
     return cudaGetLastError();
 }
 
@@ -375,7 +483,7 @@ __device__ __forceinline__ MinorLevel minor_level(const MinorConsts &C, const Mi
 }  // namespace
 
 __global__ void __launch_bounds__(128) k_minor_ng(MinorFields F, MinorConsts C, double *out, int nk, int ncol, long ld,
-                                                  double *sys_out, unsigned *status)
+                                                  double *sys_out, unsigned *status, PostStep post, int has_post)
 {
     extern __shared__ double smem_mn[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -491,12 +599,16 @@ __global__ void __launch_bounds__(128) k_minor_ng(MinorFields F, MinorConsts C, 
     }
     (void)tn_a;
     (void)tni_m;
+    // back sweep; with has_post every row goes through the post-solve steps
+    // (:226-237), the top row's unfiltered value first
+    const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
     double xn = w3;
     bool fin = fabs(xn) <= DBL_MAX;
+    if (has_post) post_store(post, true, bcol, out, (long)(nk - 1) * ld + col, xn);
     for (int k = nk - 2; k >= 0; --k) {
         xn = xs(out[k * ld + col], xm(w2s[k * T], xn));
         fin = fin && fabs(xn) <= DBL_MAX;
-        out[k * ld + col] = xn;
+        post_store(post, has_post, bcol, out, k * ld + col, xn);
     }
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
@@ -516,12 +628,10 @@ __device__ __forceinline__ double minor_tni(const MinorFields &F, int j, int nk,
     return xm(0.5, xa(__ldg(F.tn + (long)j * ld + col), __ldg(F.tn + (long)(j - 1) * ld + col)));
 }
 
-__global__ void __launch_bounds__(128) k_minor_levels(MinorFields F, MinorConsts C, double *lv, int nk, int ncol,
-                                                      long ld)
+// ax, thdiff, dmdz/barm of level j of one column (minor_ng.F90:72-153).
+__device__ __forceinline__ MinorLevel minor_level_at(const MinorFields &F, const MinorConsts &C, int j, int nk, long ld,
+                                                     long col)
 {
-    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (col >= ncol) return;
     auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
     const double dzp = C.dzp, tlbc = __ldg(F.tlbc + col);
     MinorIface I;
@@ -550,7 +660,16 @@ __global__ void __launch_bounds__(128) k_minor_levels(MinorFields F, MinorConsts
     if (j == 0) dt = xs(minor_tni(F, 1, nk, ld, col, tlbc), t0);
     else if (j == nk - 1) dt = xs(t0, minor_tni(F, nk - 2, nk, ld, col, tlbc));
     else dt = xd(xs(minor_tni(F, j + 1, nk, ld, col, tlbc), minor_tni(F, j - 1, nk, ld, col, tlbc)), 2.0);
-    const MinorLevel L = minor_level(C, I, at(F.barm, j), t0, dt);
+    return minor_level(C, I, at(F.barm, j), t0, dt);
+}
+
+__global__ void __launch_bounds__(128) k_minor_levels(MinorFields F, MinorConsts C, double *lv, int nk, int ncol,
+                                                      long ld)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (col >= ncol) return;
+    const MinorLevel L = minor_level_at(F, C, j, nk, ld, col);
     const long slab = (long)nk * ld;
     lv[(long)j * ld + col] = L.ax;
     lv[slab + (long)j * ld + col] = L.thdiff;
@@ -563,7 +682,8 @@ __global__ void __launch_bounds__(128) k_minor_levels(MinorFields F, MinorConsts
 // (qdiv: one correctly rounded reciprocal, the same bits as IEEE a/b).
 constexpr int kMinorStaged = 11;
 __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C, const double *lv, double *out,
-                                                    int nk, int ncol, long ld, double *sys_out, unsigned *status)
+                                                    int nk, int ncol, long ld, double *sys_out, unsigned *status,
+                                                    PostStep post, int has_post)
 {
     extern __shared__ double smem_mr[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -660,15 +780,17 @@ __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C
         rprev = r;
         L0 = L1;
     }
+    const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
     double xn = w3;
     bool fin = fabs(xn) <= DBL_MAX;
     double park = nk >= 2 ? out[(nk - 2) * ld + col] : 0.0;
+    if (has_post) post_store(post, true, bcol, out, (long)(nk - 1) * ld + col, xn);
     for (int k = nk - 2; k >= 0; --k) {
         const double wk = park;
         if (k >= 1) park = out[(k - 1) * ld + col];
         xn = xs(wk, xm(w2s[k * T], xn));
         fin = fin && fabs(xn) <= DBL_MAX;
-        out[k * ld + col] = xn;
+        post_store(post, has_post, bcol, out, k * ld + col, xn);
     }
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
@@ -678,8 +800,10 @@ int assembly_mode() { return g_assembly_mode.load(); }
 void set_assembly_mode(int m) { g_assembly_mode.store(m < 0 ? 1 : (m ? 1 : 0)); }
 
 cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *out, int nk, int ncol, long ld,
-                            double *sys_out, unsigned *status, cudaStream_t st, double *scratch)
+                            double *sys_out, unsigned *status, cudaStream_t st, double *scratch, const PostStep *post)
 {
+    const PostStep pv = post ? *post : PostStep{};
+    const int hp = post != nullptr;
     if (ncol <= 0) return cudaSuccess;
     const int optin = smem_optin();
     once_per_device([optin] {
@@ -700,10 +824,65 @@ cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *
         if ((size_t)TR * per_r > (size_t)optin) return cudaErrorInvalidValue;
         k_minor_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch, nk, ncol, ld);
         k_minor_rows<<<(ncol + TR - 1) / TR, TR, (size_t)TR * per_r, st>>>(F, C, scratch, out, nk, ncol, ld, sys_out,
-                                                                          status);
+                                                                          status, pv, hp);
         return cudaGetLastError();
     }
-    k_minor_ng<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, out, nk, ncol, ld, sys_out, status);
+    k_minor_ng<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, out, nk, ncol, ld, sys_out, status, pv, hp);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// minor_ng's history diagnostics (src/minor_ng.F90:202-224) from the fields
+// and the solution x (before the lateral overwrite and the floor): 7
+// level-major planes D<name>DT, <name>_PROD, <name>_LOSS, <name>_MOLDIF,
+// <name>_EDDYDIF, -<name>_VERADV, -<name>_HORADV, the values the reference
+// hands to addfld (MOLDIF, EDDYDIF and VERADV rows 1 and nk, which the
+// reference leaves unset, are 0).  One thread per (level, column); the level
+// quantities ax, thdiff, dmdz/barm of levels k and k+1 come from the same
+// device code as the solve (its fractional powers within a few ulp of the
+// host library's), everything else is bit-identical.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_minor_diag_ng(MinorFields F, MinorConsts C, const double *x, int nk, int ncol,
+                                                       long ld, double *diag)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (col >= ncol) return;
+    const long o = (long)k * ld + col, slab = (long)nk * ld;
+    const double xk = x[o], dzp = C.dzp;
+    double *d = diag + o;
+    d[0] = xm(C.dtx2inv, xs(xk, __ldg(F.ftm1_smooth + o)));
+    d[slab] = xd(xm(__ldg(F.sprod + o), C.rmx), __ldg(F.xnmbar + o));
+    d[2 * slab] = xm(__ldg(F.sloss + o), xk);
+    d[6 * slab] = -__ldg(F.hadvec + o);
+    double mol = 0.0, eddy = 0.0, vadv = 0.0;
+    if (k >= 1 && k <= nk - 2) {
+        const MinorLevel L0 = minor_level_at(F, C, k, nk, ld, col), L1 = minor_level_at(F, C, k + 1, nk, ld, col);
+        const double rdz = xd(1.0, dzp);
+        const double molp = xm(L0.ax, xa(rdz, xm(0.5, L0.thdiff)));
+        const double molr = xm(L1.ax, xs(rdz, xm(0.5, L1.thdiff)));
+        const double molq = xa(xm(L0.ax, xs(rdz, xm(0.5, L0.thdiff))), xm(L1.ax, xa(rdz, xm(0.5, L1.thdiff))));
+        const double dk = __ldg(F.difk + k), dk1 = __ldg(F.difk + k + 1);
+        const double eddyp = xm(xm(C.expzmid_inv, dk), xs(rdz, xm(0.5, L0.dmdzs)));
+        const double eddyr = xm(xm(C.expzmid, dk1), xa(rdz, xm(0.5, L1.dmdzs)));
+        const double eddyq = xa(xm(xm(C.expzmid_inv, dk), xa(rdz, xm(0.5, L0.dmdzs))),
+                                xm(xm(C.expzmid, dk1), xs(rdz, xm(0.5, L1.dmdzs))));
+        const double xm1 = x[o - ld], xp1 = x[o + ld];
+        mol = -xm(xd(xd(1.0, __ldg(F.expz + k)), dzp), xa(xs(xm(molp, xm1), xm(molq, xk)), xm(molr, xp1)));
+        eddy = xm(rdz, xa(xs(xm(eddyp, xm1), xm(eddyq, xk)), xm(eddyr, xp1)));
+        const double wi = xm(0.5, xa(__ldg(F.w + o), __ldg(F.w + o + ld)));
+        vadv = -xm(xd(wi, xm(2.0, dzp)), xs(xp1, xm1));
+    }
+    d[3 * slab] = mol;
+    d[4 * slab] = xm(eddy, __ldg(F.dfactor + col));
+    d[5 * slab] = vadv;
+}
+
+cudaError_t launch_minor_diag_ng(const MinorFields &F, const MinorConsts &C, const double *x, int nk, int ncol, long ld,
+                                 double *diag, cudaStream_t st)
+{
+    if (ncol <= 0) return cudaSuccess;
+    k_minor_diag_ng<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, x, nk, ncol, ld, diag);
     return cudaGetLastError();
 }
 

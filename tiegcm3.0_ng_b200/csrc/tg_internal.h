@@ -155,22 +155,44 @@ cudaError_t launch_col_to_level_multi(const Relayout &r, cudaStream_t st);
 cudaError_t launch_level_to_col(const double *in, long in_ld, double *out, long out_ld,
                                 long nrows, long ncols, cudaStream_t st);
 
+// The post-solve steps of dt_ng, minor_ng and oplus_ng (src/dt_ng.F90:201-213,
+// src/minor_ng.F90:226-237, src/oplus_ng.F90:330-340) done at the back sweep's
+// stores: the lateral-boundary overwrite of the flagged columns, the time
+// filter of the previous-step field and the floors.  Level-major planes.
+struct PostStep {
+    const double *cur, *prev;        // the field at this step and at the previous one
+    double *nm;                      // receives the filtered previous-step field (may alias prev or cur)
+    const unsigned char *bnd_mask;   // (ncol) nonzero: a lateral-boundary column, or null for none
+    const double *bnd;               // the boundary values of those columns
+    double ds, ds2, floor;           // dtsmooth, dtsmooth_div2, the floor
+    int floor_nm;                    // the filtered field is floored too
+};
+
 // dt_ng fused assembly + solve (tg_assembly.cu).
 typedef tg_dt_fields DtFields;
 typedef tg_dt_consts DtConsts;
 cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, int nk, int ncol, long ld,
-                         double *sys_out, unsigned *status, cudaStream_t st);
+                         double *sys_out, unsigned *status, cudaStream_t st, const PostStep *post = nullptr);
+
+// dt_ng's 12 history diagnostics of a solution x: level-major planes of nk*ld
+cudaError_t launch_dt_diag_ng(const DtFields &F, const DtConsts &C, const double *x, int nk, int ncol, long ld,
+                              double *diag, cudaStream_t st);
 
 typedef tg_minor_fields MinorFields;
 typedef tg_minor_consts MinorConsts;
 // scratch (3 * nk * ld doubles, may be NULL): the level-quantity planes of the
 // two-pass form, used when assembly_mode() is 1
 cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *out, int nk, int ncol, long ld,
-                            double *sys_out, unsigned *status, cudaStream_t st, double *scratch);
+                            double *sys_out, unsigned *status, cudaStream_t st, double *scratch,
+                            const PostStep *post = nullptr);
 // Assembly kernels: 1 (default) two-pass (level-parallel level quantities,
 // then the column walk) where built, 0 the single fused column walk.
 int assembly_mode();
 void set_assembly_mode(int m);
+
+// minor_ng's 7 history diagnostics of a solution x: level-major planes of nk*ld
+cudaError_t launch_minor_diag_ng(const MinorFields &F, const MinorConsts &C, const double *x, int nk, int ncol,
+                                 long ld, double *diag, cudaStream_t st);
 
 typedef tg_comp_fields CompFields;
 typedef tg_comp_consts CompConsts;
@@ -208,7 +230,7 @@ typedef tg_oplus_fields OplusFields;
 typedef tg_oplus_consts OplusConsts;
 cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *opout, double *xiop2p,
                             double *xiop2d, double *Fe, double *Fn, double *scratch, int nk, int ncol, long ld,
-                            double *sys_out, unsigned *status, cudaStream_t st);
+                            double *sys_out, unsigned *status, cudaStream_t st, const PostStep *post = nullptr);
 int oplus_scratch_planes();   // level-major scratch planes of launch_oplus_ng (each nk*ld doubles)
 
 // Polar ring filter (tg_filter.cu): the latitudes it filters, with their

@@ -113,7 +113,7 @@ __device__ __forceinline__ void oplus_level(const OplusFields &F, const OplusCon
 // sweep of one column (oplus_ng.F90:88-99, 209-307).
 __device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusConsts &C, double *opout, const double *scr,
                                            double *w2s, int T, int nk, long ld, long col, double *sys_out,
-                                           unsigned *status)
+                                           unsigned *status, const PostStep &post, int has_post)
 {
     const long slab = (long)nk * ld;
     auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
@@ -241,7 +241,10 @@ __device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusCons
         rprev = r;
     }
     // ---- pass 3: back sweep and the top level (oplus_ng.F90:305-307)
+    // with has_post every row goes through the post-solve steps (:330-340),
+    // the top row computed from the unfiltered values first
     const int K = nk - 1;
+    const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
     double xn = w3, xtop = w3;
     bool fin = fabs(xn) <= DBL_MAX;
     double park = K >= 2 ? opout[(long)(K - 2) * ld + col] : 0.;
@@ -250,21 +253,25 @@ __device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusCons
         if (k >= 1) park = opout[(long)(k - 1) * ld + col];
         xn = xs(wk, xm(w2s[(long)k * T], xn));
         fin = fin && fabs(xn) <= DBL_MAX;
-        opout[(long)k * ld + col] = xn;
-        if (k == K - 2) opout[(long)K * ld + col] = xd(xm(xtop, xtop), xn);
+        post_store(post, has_post, bcol, opout, (long)k * ld + col, xn);
+        if (k == K - 2) {
+            post_store(post, has_post, bcol, opout, (long)K * ld + col, xd(xm(xtop, xtop), xn));
+            if (has_post) post_store(post, true, bcol, opout, (long)(K - 1) * ld + col, xtop);
+        }
     }
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
 __global__ void __launch_bounds__(128) k_oplus_ng(OplusFields F, OplusConsts C, double *opout, double *xiop2p,
                                                   double *xiop2d, double *Fe, double *Fn, double *scr, int nk,
-                                                  int ncol, long ld, double *sys_out, unsigned *status)
+                                                  int ncol, long ld, double *sys_out, unsigned *status,
+                                                  PostStep post, int has_post)
 {
     extern __shared__ double smem_op[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
     for (int j = 0; j < nk; ++j) oplus_level(F, C, scr, xiop2p, xiop2d, Fe, Fn, nk, ld, col, j);
-    oplus_walk(F, C, opout, scr, smem_op + threadIdx.x, blockDim.x, nk, ld, col, sys_out, status);
+    oplus_walk(F, C, opout, scr, smem_op + threadIdx.x, blockDim.x, nk, ld, col, sys_out, status, post, has_post);
 }
 
 // Two-pass form: the level quantities with one thread per (level, column),
@@ -278,18 +285,21 @@ __global__ void __launch_bounds__(128) k_oplus_levels(OplusFields F, OplusConsts
 }
 
 __global__ void __launch_bounds__(128) k_oplus_rows(OplusFields F, OplusConsts C, double *opout, const double *scr,
-                                                    int nk, int ncol, long ld, double *sys_out, unsigned *status)
+                                                    int nk, int ncol, long ld, double *sys_out, unsigned *status,
+                                                    PostStep post, int has_post)
 {
     extern __shared__ double smem_or[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
-    oplus_walk(F, C, opout, scr, smem_or + threadIdx.x, blockDim.x, nk, ld, col, sys_out, status);
+    oplus_walk(F, C, opout, scr, smem_or + threadIdx.x, blockDim.x, nk, ld, col, sys_out, status, post, has_post);
 }
 
 cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *opout, double *xiop2p,
                             double *xiop2d, double *Fe, double *Fn, double *scratch, int nk, int ncol, long ld,
-                            double *sys_out, unsigned *status, cudaStream_t st)
+                            double *sys_out, unsigned *status, cudaStream_t st, const PostStep *post)
 {
+    const PostStep pv = post ? *post : PostStep{};
+    const int hp = post != nullptr;
     if (ncol <= 0) return cudaSuccess;
     if (nk < 3) return cudaErrorInvalidValue;
     const int optin = smem_optin();
@@ -305,11 +315,11 @@ cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *
         k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, xiop2p, xiop2d, Fe, Fn, scratch, nk, ncol,
                                                                      ld);
         k_oplus_rows<<<(ncol + T - 1) / T, T, (size_t)T * per, st>>>(F, C, opout, scratch, nk, ncol, ld, sys_out,
-                                                                     status);
+                                                                     status, pv, hp);
         return cudaGetLastError();
     }
     k_oplus_ng<<<(ncol + T - 1) / T, T, (size_t)T * per, st>>>(F, C, opout, xiop2p, xiop2d, Fe, Fn, scratch, nk, ncol,
-                                                               ld, sys_out, status);
+                                                               ld, sys_out, status, pv, hp);
     return cudaGetLastError();
 }
 
