@@ -51,6 +51,28 @@ int main(void)
     y[3] = w3[3];
     for (int k = 2; k >= 0; --k) y[k] = w3[k] - w2[k] * y[k + 1];
     for (int k = 0; k < 4; ++k) CHECK(x[k] == y[k]);
+    /* the kernels run as the library's sm_100a build */
+    int arch = 0;
+    CHECK(tg_kernel_arch(&arch) == TG_OK && arch == 100);
+    /* the same system as a latitude slab with the periodic columns around it
+     * (lon0 = 1, lon1 = lonmax = 5: columns 1, 2, 4, 5 are skipped), queued
+     * and flushed; the work arrays are overwritten before the flush */
+    double sa[20], sb[20], sc[20], sf[20], sx[20];
+    for (int i = 0; i < 5; ++i)
+        for (int k = 0; k < 4; ++k) {
+            sa[4 * i + k] = a[k];
+            sb[4 * i + k] = b[k];
+            sc[4 * i + k] = c[k];
+            sf[4 * i + k] = f[k];
+            sx[4 * i + k] = -1.0;
+        }
+    CHECK(tg_trsolv_defer(sa, sb, sc, sf, sx, 1, 4, 1, 4, 1, 5, 5) == TG_OK);
+    for (int i = 0; i < 20; ++i) sa[i] = sb[i] = sc[i] = sf[i] = NAN;
+    CHECK(tg_trsolv_flush() == TG_OK);
+    for (int k = 0; k < 4; ++k) CHECK(sx[8 + k] == y[k]);
+    for (int i = 0; i < 5; ++i)
+        if (i != 2)
+            for (int k = 0; k < 4; ++k) CHECK(sx[4 * i + k] == -1.0);
     printf("abi_check: ok (solved on the device)\n");
     return 0;
 }

@@ -42,3 +42,17 @@ def cuda():
 
 def golden(name):
     return np.load(os.path.join(GOLDEN, name))
+
+
+def prec_fn(f, lf):
+    """A transcendental function for the numpy transcriptions: on float64
+    values the C library's (through math, as the oracle calls it), on long
+    double values numpy's long double ufunc, so a transcription fed long
+    double inputs evaluates the same formulas to ~1e-19."""
+    vf = np.vectorize(f, otypes=[float])
+
+    def g(*args):
+        if any(np.asarray(a).dtype == np.longdouble for a in args):
+            return lf(*args)
+        return vf(*args)
+    return g

@@ -150,8 +150,7 @@ def test_host_wrappers_check_field_sizes(pkg):
         pkg.settei_ng(F, C, z(), z(), np.zeros((nk, ncol - 1), order="F"))
 
 
-def test_plain_c_caller(pkg, tmp_path):
-    """tests/c/abi_check.c: the header and library used from C alone."""
+def _run_c_caller(pkg, tmp_path):
     import shutil
     import subprocess
     cc = shutil.which("gcc") or shutil.which("cc")
@@ -163,5 +162,17 @@ def test_plain_c_caller(pkg, tmp_path):
                     os.path.join(ROOT, "tests", "c", "abi_check.c"), "-o", exe, "-L", libdir, "-ltg_colsolve",
                     f"-Wl,-rpath,{libdir}", "-lm"], check=True)
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
-    assert r.returncode == 0, r.stderr
-    assert r.stdout.startswith("abi_check: ok")
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r.stdout
+
+
+def test_plain_c_caller(pkg, tmp_path):
+    """tests/c/abi_check.c: the header and library used from C alone."""
+    assert _run_c_caller(pkg, tmp_path).startswith("abi_check: ok")
+
+
+@pytest.mark.gpu
+def test_plain_c_caller_solves_on_the_device(cuda, pkg, tmp_path):
+    """The C caller's device branch: a solve, the architecture query and a
+    deferred latitude slab, from C with no Python in the process."""
+    assert _run_c_caller(pkg, tmp_path).startswith("abi_check: ok (solved on the device)")

@@ -7,12 +7,13 @@ import math
 import numpy as np
 import pytest
 
+from conftest import prec_fn
 from test_minor_assembly import PHI, SS, matinv3
 
 TAU, T00, THDIFFALPHA = 1.86e3, 273., -0.38
-_pow = np.vectorize(math.pow, otypes=[float])
-_log = np.vectorize(math.log, otypes=[float])
-_exp = np.vectorize(math.exp, otypes=[float])
+_pow = prec_fn(math.pow, np.power)
+_log = prec_fn(math.log, np.log)
+_exp = prec_fn(math.exp, np.exp)
 
 
 def comp_numpy(F, C):
@@ -20,7 +21,8 @@ def comp_numpy(F, C):
     nk, ncol = F["tn"].shape
     tn, o2, o1, he, w, mbar = (F[k] for k in ("tn", "o2", "o1", "he", "w", "mbar"))
     b, fb, dz = C["b"], C["fb"], C["dz"]
-    flx_he = F["flx_he"] if C["calc_helium"] else np.zeros(ncol)
+    dt = F["tn"].dtype
+    flx_he = F["flx_he"] if C["calc_helium"] else np.zeros(ncol, dtype=dt)
     fs = F["fs"].reshape(4, 3, ncol, nk)          # fs(k, col, isp, m) -> [m, isp, col, k]
     ps0 = [b[i, 0] * o2[0] + b[i, 1] * o1[0] + b[i, 2] * he[0] + fb[i] for i in range(3)]
     embar0 = 1. / (ps0[0] * C["rmassinv_o2"] + ps0[1] * C["rmassinv_o1"] + ps0[2] * C["rmassinv_he"] +
@@ -53,7 +55,7 @@ def comp_numpy(F, C):
         ep = [1. - 1. / embari[j] * (rmass[i] + dembardz[j]) for i in range(3)]
         if thermal:
             ep[2] = ep[2] - THDIFFALPHA * dtndz[j] / tni[j]
-        a = np.empty((3, 3, ncol))
+        a = np.empty((3, 3, ncol), dtype=dt)
         a[0, 0] = -(phi(1, 4) + (phi(1, 2) - phi(1, 4)) * o1i[j] + (df[0][j] * phi(1, 3) - phi(1, 4)) * hei[j])
         a[1, 1] = -(phi(2, 4) + (phi(2, 1) - phi(2, 4)) * o2i[j] + (df[1][j] * phi(2, 3) - phi(2, 4)) * hei[j])
         a[2, 2] = -(df[2][j] * phi(3, 4) + (df[0][j] * phi(3, 1) - df[2][j] * phi(3, 4)) * o2i[j] +
@@ -73,10 +75,10 @@ def comp_numpy(F, C):
     adv = (F["o2_advec"], F["o1_advec"], F["he_advec"])
     hd = (F["hdo2"], F["hdo1"], F["hdhe"])
     dfac = F["dfactor"]
-    P, Q, R = (np.zeros((3, 3, nk - 1, ncol)) for _ in range(3))
-    fv = np.zeros((3, nk - 1, ncol))
-    gama = np.zeros((nk, 3, 3, ncol))
-    zz = np.zeros((nk, 3, ncol))
+    P, Q, R = (np.zeros((3, 3, nk - 1, ncol), dtype=dt) for _ in range(3))
+    fv = np.zeros((3, nk - 1, ncol), dtype=dt)
+    gama = np.zeros((nk, 3, 3, ncol), dtype=dt)
+    zz = np.zeros((nk, 3, ncol), dtype=dt)
     for k in range(nk - 1):
         ep_km, ak_km, wks3 = ep_kp, ak_kp, wks4
         ep_kp, a_kp, ak_kp, wks4 = level(k + 1, k + 1 != nk - 1)
@@ -85,7 +87,7 @@ def comp_numpy(F, C):
         eddyq = (C["expzmid_inv"] * F["difk"][k] * (1. / dz + wks3) +
                  C["expzmid"] * F["difk"][k + 1] * (1. / dz - wks4))
         ez = F["expz"][k]
-        pk, qk, rk = (np.empty((3, 3, ncol)) for _ in range(3))
+        pk, qk, rk = (np.empty((3, 3, ncol), dtype=dt) for _ in range(3))
         for isp in range(3):
             for m in range(3):
                 d = 1. if isp == m else 0.
@@ -123,7 +125,7 @@ def comp_numpy(F, C):
                 gama[k + 1, :, m] = gama[k + 1, :, m] + wkm1[:, n] * rk[n, m]
         for m in range(3):
             zz[k + 1] = zz[k + 1] + wkm1[:, m] * wkv1[m]
-    upd = np.zeros((3, nk, ncol))
+    upd = np.zeros((3, nk, ncol), dtype=dt)
     for k in range(nk - 2, -1, -1):
         upd[:, k] = zz[k + 1]
         for isp in range(3):

@@ -248,3 +248,40 @@ def test_every_refine_variant_within_tolerance(cuda, pkg, orc, kind):
             check(pkg, orc, segs, refs_in, exact=False)
     finally:
         autotune.reset(kind, pkg.TG_PREC_F32_REFINE)
+
+
+def test_autotune_tune_and_cache_round_trip(cuda, pkg, orc, tmp_path):
+    """autotune.tune() times every candidate of each kind and precision on a
+    small segment set, applies the fastest and records it in the JSON cache;
+    load() in a fresh state applies the same choices, and the plan built
+    under them still gives the oracle's bits."""
+    torch = cuda
+    import json
+    from tiegcm_ng_b200 import autotune
+    specs = [(0, 57, 57, 700), (0, 57, 56, 130), (2, 57, 57, 300)]
+    segs, refs_in = make_segments(pkg, torch, specs, seed=900)
+    cache = str(tmp_path / "tune.json")
+    try:
+        out = autotune.tune(segs, cache=cache, reps=3)
+        for kind in (0, 2):
+            for prec in (pkg.TG_PREC_F64, pkg.TG_PREC_F32_REFINE):
+                best, ms, times = out[(kind, prec)]
+                assert best in times and ms == times[best] and ms < float("inf")
+        db = json.load(open(cache))
+        assert len([k for k in db if "|kind0|" in k]) == 2 and len([k for k in db if "|kind2|" in k]) == 2
+        for kind in (0, 2):
+            for prec in (pkg.TG_PREC_F64, pkg.TG_PREC_F32_REFINE):
+                autotune.reset(kind, prec)
+        found = autotune.load(segs, cache=cache)
+        assert sorted(found) == sorted([(0, 0), (0, 1), (2, 0), (2, 1)])
+        for s in segs:
+            s["x"].fill_(3.5)
+        plan = pkg.Plan(segs, pkg.TG_PREC_F64)
+        plan.execute()
+        assert plan.status()[0] == pkg.TG_OK
+        plan.close()
+        check(pkg, orc, segs, refs_in)
+    finally:
+        for kind in (0, 2):
+            for prec in (pkg.TG_PREC_F64, pkg.TG_PREC_F32_REFINE):
+                autotune.reset(kind, prec)

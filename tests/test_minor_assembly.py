@@ -10,7 +10,9 @@ import pytest
 TAU, T00 = 1.86e3, 273.
 SS = (1.710, 1.749, 1.718)
 PHI = np.array([0., 0.673, 0.270, 1.35, 0., 0.404, 2.16, 1.616, 0., 1.11, 0.769, 0.322]).reshape((3, 4), order="F")
-_pow = np.vectorize(math.pow, otypes=[float])
+from conftest import prec_fn  # noqa: E402
+
+_pow = prec_fn(math.pow, np.power)
 
 
 def matinv3(a):
@@ -63,7 +65,7 @@ def minor_numpy(F, C, keep=None):
     s0prod = F["sprod"] * rmx / F["xnmbar"]
     df = [_pow(tni / T00, 1.75 - SS[n]) for n in range(3)]
     phi = lambda i, j: PHI[i - 1, j - 1]
-    alfa = np.empty((3, 3) + tn.shape)
+    alfa = np.empty((3, 3) + tn.shape, dtype=tn.dtype)
     alfa[0, 0] = -(phi(1, 4) + (phi(1, 2) - phi(1, 4)) * pso1 + (df[0] * phi(1, 3) - phi(1, 4)) * pshe)
     alfa[1, 1] = -(phi(2, 4) + (phi(2, 1) - phi(2, 4)) * pso2 + (df[1] * phi(2, 3) - phi(2, 4)) * pshe)
     alfa[2, 2] = -(df[2] * phi(3, 4) + (df[0] * phi(3, 1) - df[2] * phi(3, 4)) * pso2 +

@@ -7,8 +7,10 @@ import math
 import numpy as np
 import pytest
 
-_v = lambda f: np.vectorize(f, otypes=[float])
-COS, SIN, LOG10, POW = _v(math.cos), _v(math.sin), _v(math.log10), _v(math.pow)
+from conftest import prec_fn
+
+COS, SIN, LOG10, POW = (prec_fn(math.cos, np.cos), prec_fn(math.sin, np.sin), prec_fn(math.log10, np.log10),
+                        prec_fn(math.pow, np.power))
 
 
 def interp_up(a):
@@ -28,7 +30,7 @@ def oplus_numpy(F, C):
     tn, te, ti, o2, o1, n2, he, n2d, ne = (g(k) for k in ("tn", "te", "ti", "o2", "o1", "n2", "he", "n2d", "ne"))
     xnmbar, op, bx, by, bz = g("xnmbar"), g("op"), g("bx"), g("by"), g("bz")
     arl, chi = np.abs(g("rlatm")), g("chi")
-    a = np.full(ncol, np.nan)
+    a = np.full(ncol, np.nan, dtype=F["tn"].dtype)
     a = np.where(arl >= pi / 4.5, 1., a)
     a = np.where((arl < pi / 4.5) & (arl > pi / 18), .5 * (1. + COS(arl * 6. - pi * 4. / 3.)), a)
     a = np.where(arl <= pi / 18, 0., a)

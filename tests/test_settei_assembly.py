@@ -7,9 +7,11 @@ import math
 import numpy as np
 import pytest
 
-_v = lambda f: np.vectorize(f, otypes=[float])
-EXP, LOG, SQRT, COS, SIN = _v(math.exp), _v(math.log), np.sqrt, _v(math.cos), _v(math.sin)
-POW = _v(math.pow)
+from conftest import prec_fn
+
+EXP, LOG, SQRT, COS, SIN = (prec_fn(math.exp, np.exp), prec_fn(math.log, np.log), np.sqrt,
+                            prec_fn(math.cos, np.cos), prec_fn(math.sin, np.sin))
+POW = prec_fn(math.pow, np.power)
 
 
 def settei_numpy(F, C, qtotal):
@@ -22,7 +24,7 @@ def settei_numpy(F, C, qtotal):
     nk, ncol = tn.shape
     f107te = min(C["f107"], 235.)
     arl, chi = np.abs(F["rlatm"]), F["chi"]
-    a = np.full(ncol, np.nan)
+    a = np.full(ncol, np.nan, dtype=F["tn"].dtype)
     a = np.where(arl >= pi / 4.5, 1., a)
     a = np.where((arl < pi / 4.5) & (arl > pi / 18), .5 * (1. + COS(arl * 6. - pi * 4. / 3.)), a)
     a = np.where(arl <= pi / 18, 0., a)

@@ -1,0 +1,86 @@
+"""The FP64 assembly routines against their long-double evaluation
+(tests/truth.py): the oracle (the reference's FP64 arithmetic) and the GPU
+kernels are each within a stated distance of the exact result of the same
+formulas, and the GPU is no further from it than the oracle is (to within a
+factor 2 and a few ulp).  This separates rounding (device vs C library
+transcendental functions, amplified by the systems' conditioning) from a
+kernel error, which would put the GPU far from both."""
+import numpy as np
+import pytest
+
+import truth
+
+EPS = 2.0 ** -52
+ORACLE_BOUND = 1e-12          # the oracle's own distance from the long-double result
+
+CASES = [(57, 0.25, 300), (29, 0.5, 200), (113, 0.125, 100), (3, 0.5, 33)]
+
+
+def _cases(pkg, name, nk, dz, ncol):
+    if name == "comp":
+        F, C = pkg.synth.comp_inputs(nk, ncol, dz, 21 + nk)
+        return F, C, None
+    if name == "settei":
+        F, C, qt = pkg.synth.settei_inputs(nk, ncol, dz, 31 + nk)
+        return F, C, qt
+    if name == "oplus":
+        F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 41 + nk)
+        return F, C, None
+    F, C = pkg.synth.minor_inputs(nk, ncol, dz, 9 + nk)
+    return F, C, None
+
+
+def _oracle(orc, name, F, C, qt):
+    if name == "comp":
+        return list(orc.comp_ng(F, C)), truth.comp_truth(F, C)
+    if name == "settei":
+        return list(orc.settei_ng(F, C, qt)), truth.settei_truth(F, C, qt)
+    if name == "oplus":
+        return list(orc.oplus_ng(F, C)), truth.oplus_truth(F, C)
+    return [orc.minor_ng(F, C)], [truth.minor_truth(F, C)]
+
+
+def _gpu(pkg, name, F, C, qt, nk, ncol):
+    z = lambda: np.zeros((nk, ncol), order="F")  # noqa: E731
+    if name == "comp":
+        out = [z(), z(), z()]
+        pkg.comp_ng(F, C, *out)
+    elif name == "settei":
+        out = [z(), z(), qt.copy(order="F")]
+        pkg.settei_ng(F, C, out[0], out[1], out[2])
+    elif name == "oplus":
+        out = [z() for _ in range(5)]
+        pkg.oplus_ng(F, C, *out)
+    else:
+        out = [z()]
+        pkg.minor_ng(F, C, out[0])
+    return out
+
+
+@pytest.mark.parametrize("name", ["comp", "settei", "oplus", "minor"])
+@pytest.mark.parametrize("nk,dz,ncol", CASES)
+def test_oracle_close_to_long_double(pkg, orc, name, nk, dz, ncol):
+    if nk < 4 and name != "comp":
+        pytest.skip("the extrapolated top rows need nk >= 4 here")
+    F, C, qt = _cases(pkg, name, nk, dz, ncol)
+    got, want = _oracle(orc, name, F, C, qt)
+    for i, (g, w) in enumerate(zip(got, want)):
+        assert truth.rel(g, w) <= ORACLE_BOUND, (name, i, truth.rel(g, w))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [1, 0], ids=["two_pass", "fused"])
+@pytest.mark.parametrize("name", ["comp", "settei", "oplus", "minor"])
+@pytest.mark.parametrize("nk,dz,ncol", CASES[:3])
+def test_gpu_as_close_to_long_double_as_the_oracle(cuda, pkg, orc, name, nk, dz, ncol, mode):
+    F, C, qt = _cases(pkg, name, nk, dz, ncol)
+    got_o, want = _oracle(orc, name, F, C, qt)
+    pkg.set_assembly_mode(mode)
+    try:
+        got_g = _gpu(pkg, name, F, C, qt, nk, ncol)
+    finally:
+        pkg.set_assembly_mode(-1)
+    for i, (g, o, w) in enumerate(zip(got_g, got_o, want)):
+        eg, eo = truth.rel(g, w), truth.rel(o, w)
+        print(f"{name} nk={nk} field {i}: gpu {eg:.3e} oracle {eo:.3e}")
+        assert eg <= 2.0 * eo + 16 * EPS, (name, i, eg, eo)

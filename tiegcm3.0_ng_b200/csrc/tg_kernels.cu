@@ -3298,8 +3298,11 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         // ring kernels: w2 scratch plus the w3 parked in x, 8 B each per level
         // and column (refinement: three float planes plus x; w2 on chip: the
         // parked w3 alone), of every resident column within the L2 budget
+        // (refinement with hints 2 or 3 keeps its FP64 coefficients in L2
+        // between the sweeps: their 32 B per level count too)
         const double per_col = sh->res == 1 ? (double)k2max * 8.0
-                               : precision == TG_PREC_F64 ? (double)(2 * k2max - 1) * 8.0 : (double)k2max * 20.0;
+                               : precision == TG_PREC_F64 ? (double)(2 * k2max - 1) * 8.0
+                                                          : (double)k2max * (cache_hints() >= 2 ? 52.0 : 20.0);
         const long cap = (long)(g_scalar_scratch_budget / (per_col * sh->threads * sh->cpt));
         if (blocks > cap) blocks = cap > 0 ? cap : 1;
     }
