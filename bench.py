@@ -442,6 +442,20 @@ def horizontal_setup(pkg, which, dev):
         def launch(stream):
             pkg.smooth_ng_dev(fin, 0.03, out, nk, nlon, nlat, ld, stream=stream)
         return launch, nk * ncol, 16 * nk * ncol
+    if which == "ring":
+        # filter_o2o's order-1 ring filter over the 576 x 288 global grid
+        # (the model's 0.625 deg chunk table: 80 polar latitudes filtered)
+        ncg = (nlon + 4) * nlat
+        ldg = pkg.batch.pad_ld(ncg)
+        chunks = pkg.synth.RING_CHUNKS[(nlon, nlat)]
+        f = torch.rand((nk, ldg), dtype=torch.float64, device=dev, generator=g) * 0.25 + 0.05
+        dl = 2.0 * (4.0 * np.arctan(1.0)) / nlon
+        rows = 2 * len(chunks) * nk
+
+        def launch(stream):
+            pkg.ringfilter_dev(f, nk, nlon, nlat, 1, 0, chunks, dl, ldg, stream=stream)
+        # each filtered row: nlon+4 values read and written
+        return launch, rows * (nlon + 4), 16 * rows * (nlon + 4)
     cur, prev, upd = field(150.0, 2000.0), field(150.0, 2000.0), field(50.0, 2000.0)
     nm = torch.empty_like(cur)
 
@@ -454,9 +468,9 @@ def run_profile(args):
     """Executes one kind's plan --warmup + --steps times (for ncu captures)."""
     import torch
     pkg = ge.load_package()
-    if args.profile in ("dt", "minor", "comp", "settei", "oplus", "advec", "smooth", "filter"):
+    if args.profile in ("dt", "minor", "comp", "settei", "oplus", "advec", "smooth", "filter", "ring"):
         wl = pkg.synth.workload(args.config)
-        if args.profile in ("advec", "smooth", "filter"):
+        if args.profile in ("advec", "smooth", "filter", "ring"):
             launch, ncol, nbytes = horizontal_setup(pkg, args.profile, "cuda")
         else:
             launch, ncol, nbytes = assembly_setup(pkg, wl, args.profile, "cuda")
@@ -650,7 +664,7 @@ def main():
     if not args.skip_assembly:
         horizontal = {}
         for which, name, kern in (("advec", "advec_ng", "k_advec_ng"), ("smooth", "smooth_ng", "k_smooth_ng"),
-                                  ("filter", "time_filter_ng", "k_time_filter")):
+                                  ("filter", "time_filter_ng", "k_time_filter"), ("ring", "filter_o2o", "k_ringfilter")):
             launch, npts, nbytes = horizontal_setup(pkg, which, dev)
             for _ in range(args.warmup):
                 launch(stream)
@@ -670,7 +684,9 @@ def main():
                 "algorithmic_bytes_per_launch": nbytes,
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
                              "traffic": traffic_from_profiles(kern, HORIZ_TAG)},
-                "inputs": f"the {HORIZ_TAG} grid held as one subdomain, {nbytes / 1e6:.0f} MB > L2"}
+                "inputs": (f"the {HORIZ_TAG} grid held as one subdomain, {nbytes / 1e6:.0f} MB > L2" if which != "ring"
+                           else f"the polar rows of the 576 x 288 x 113 global grid, {nbytes / 1e6:.0f} MB, filtered "
+                                f"in place launch after launch (L2-resident)")}
             del launch
         torch.cuda.empty_cache()
 

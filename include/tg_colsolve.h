@@ -599,13 +599,15 @@ int tg_set_block_width(int kind, int width);
  * tg_set_pipeline then counts stages of L levels (2, 3 or 4). */
 int tg_set_stage_levels(int kind, int precision, int levels);
 
-/* Scalar FP64 chunked bulk-copy ring: where the forward sweep keeps w2 and w3
- * until the back sweep reads them.  0: w2 in an L2 scratch slot per resident
- * lane, w3 parked in x (k_scalar_f64_chunk); 1: w2 in the warp's shared
- * memory, w3 parked in x; 2: both in shared memory, so DRAM sees the
- * coefficients read once and x written once (k_scalar_f64_res).  -1 restores
- * the default.  Columns too tall for shared memory take mode 0.  Same
- * arithmetic, same bits. */
+/* Where the FP64 bulk-copy ring kernels keep the forward sweep's quantities
+ * until the back sweep reads them.  Scalar kind (chunked ring): 0 w2 in an L2
+ * scratch slot per resident lane, w3 parked in x (k_scalar_f64_chunk); 1 w2
+ * in the warp's shared memory, w3 parked in x; 2 both in shared memory
+ * (k_scalar_f64_res).  Block kinds: 0 Gamma in an L2 scratch slot, 1 or 2
+ * Gamma in the warp's shared memory (k_block_f64_ring<..., 1>).  On chip,
+ * DRAM sees the coefficients read once, at the cost of fewer warps per SM.
+ * -1 restores the default.  Columns too tall for shared memory take mode 0.
+ * Same arithmetic, same bits. */
 int tg_set_column_residency(int kind, int precision, int mode);
 
 /* Fused assembly routines: 1 (default) two passes where built, the level

@@ -11,7 +11,10 @@ import pytest
 import truth
 
 EPS = 2.0 ** -52
-ORACLE_BOUND = 1e-12          # the oracle's own distance from the long-double result
+# the oracle's own distance from the long-double result, per routine: oplus_ng's
+# systems (condition ~1e4) carry its rounding furthest (6.0e-12 on 3001
+# columns at nk = 57; below 1e-12 on these smaller cases)
+ORACLE_BOUND = {"comp": 1e-12, "settei": 1e-13, "oplus": 1e-11, "minor": 1e-13}
 
 CASES = [(57, 0.25, 300), (29, 0.5, 200), (113, 0.125, 100), (3, 0.5, 33)]
 
@@ -65,7 +68,7 @@ def test_oracle_close_to_long_double(pkg, orc, name, nk, dz, ncol):
     F, C, qt = _cases(pkg, name, nk, dz, ncol)
     got, want = _oracle(orc, name, F, C, qt)
     for i, (g, w) in enumerate(zip(got, want)):
-        assert truth.rel(g, w) <= ORACLE_BOUND, (name, i, truth.rel(g, w))
+        assert truth.rel(g, w) <= ORACLE_BOUND[name], (name, i, truth.rel(g, w))
 
 
 @pytest.mark.gpu

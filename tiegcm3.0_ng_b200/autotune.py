@@ -10,7 +10,8 @@ from a CUDA graph, CUDA-event timed) and keeps the fastest:
             bulk-copy ring kernel: staging depth 4, 8 or 16 levels, w2 in shared
             ("ring") or global ("ringg") memory; for block kinds also one lane
             per block row ("rows", depth 4 or 8) and 16 or 8 columns per warp
-            ("ring16", "ring8"); for the scalar kind a ring of stages holding 2, 4
+            ("ring16", "ring8"), and those rings with Gamma resident in shared
+            memory ("ringsm", "ring16sm", "ring8sm"); for the scalar kind a ring of stages holding 2, 4
             or 8 levels each ("chunk2", "chunk4", "chunk8"), and the same ring with
             the sweep's w2 ("res1cL") or w2 and w3 ("res2cL") resident in
             shared memory, L levels per stage
@@ -41,7 +42,9 @@ SCALAR_F64 = [("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg"
 BLOCK_F64 = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 96, 1, 4),
              ("ring", 4, 4, 4), ("ring", 8, 4, 4), ("ring", 4, 2, 4), ("ring", 8, 2, 4), ("ring", 16, 2, 4),
              ("ring", 4, 1, 4), ("ring16", 4, 1, 4), ("ring16", 8, 1, 4), ("ring16", 4, 2, 4), ("ring8", 4, 1, 4),
-             ("ring8", 8, 1, 4), ("ring8", 4, 2, 4), ("rows", 4, 1, 4), ("rows", 4, 2, 4), ("rows", 8, 1, 4)]
+             ("ring8", 8, 1, 4), ("ring8", 4, 2, 4), ("rows", 4, 1, 4), ("rows", 4, 2, 4), ("rows", 8, 1, 4),
+             ("ringsm", 4, 1, 4), ("ring16sm", 4, 1, 4), ("ring16sm", 8, 1, 4), ("ring8sm", 4, 1, 4),
+             ("ring8sm", 8, 1, 4)]
 SCALAR_REF = [("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg", 64, 1, 8),
               ("ring", 2, 1, 4), ("ring", 3, 1, 4), ("ring", 4, 1, 4), ("ring", 2, 2, 4)]
 BLOCK_REF = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("ring", 4, 1, 4), ("ring", 8, 1, 4),
@@ -66,8 +69,9 @@ def apply(kind, precision, cand):
             cs.set_column_residency(kind, precision, int(v[3]) if v.startswith("res") else 0)
     elif precision == cs.TG_PREC_F64:
         cs.set_block_rows(kind, 1 if v == "rows" else 0)
-        cs.set_block_width(kind, {"ring16": 16, "ring8": 8}.get(v, 32))
-    if v in ("ring", "ringg", "rows", "ring16", "ring8") or v.startswith(("chunk", "res")):
+        cs.set_block_width(kind, {"ring16": 16, "ring8": 8, "ring16sm": 16, "ring8sm": 8}.get(v, 32))
+        cs.set_column_residency(kind, precision, 1 if v.endswith("sm") else 0)
+    if v in ("ring", "ringg", "rows", "ring16", "ring8") or v.startswith(("chunk", "res", "ring")):
         cs.set_pipeline(kind, precision, p1, p2)    # ring depth, warps per CTA
     else:
         cs.set_pipeline(kind, precision, 0)
@@ -88,6 +92,7 @@ def reset(kind, precision):
     if kind != cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64:
         cs.set_block_rows(kind, -1)
         cs.set_block_width(kind, 0)
+        cs.set_column_residency(kind, precision, -1)
 
 
 def key(gpu, kind, precision, nk, ncol):

@@ -897,7 +897,8 @@ def set_stage_levels(kind, precision, levels):
 
 
 def set_column_residency(kind, precision, mode):
-    """Scalar FP64 chunked ring: 0 w2 in L2 scratch, 1 w2 in shared memory, 2 w2 and w3 in shared memory, -1 default."""
+    """FP64 ring kernels: scalar 0 w2 in L2 scratch, 1 w2 in shared memory, 2 w2 and w3 in shared memory;
+    block kinds 0 Gamma in L2 scratch, 1 Gamma in shared memory; -1 default."""
     return _check(lib().tg_set_column_residency(int(kind), int(precision), int(mode)), "tg_set_column_residency")
 
 

@@ -2110,8 +2110,9 @@ __attribute__((visibility("default"))) int tg_set_stage_levels(int kind, int pre
 
 __attribute__((visibility("default"))) int tg_set_column_residency(int kind, int precision, int mode)
 {
-    if (kind != TG_KIND_SCALAR || precision != TG_PREC_F64 || mode > 2) {
-        set_err("tg_set_column_residency: applies to TG_KIND_SCALAR, TG_PREC_F64 with mode 0, 1, 2 or -1");
+    if ((kind != TG_KIND_SCALAR && kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) || precision != TG_PREC_F64 ||
+        mode > 2) {
+        set_err("tg_set_column_residency: applies to TG_PREC_F64 with mode 0, 1, 2 or -1");
         return TG_EINVAL;
     }
     tg::set_column_residency(kind, precision, mode);
@@ -2187,6 +2188,7 @@ __attribute__((visibility("default"))) int tg_plan_describe(const tg_plan *p, ch
             if (!f64 && h.stages) snprintf(name, sizeof name, "k_block_refine_ring<%d,%d>", g.kind, h.stages);
             else if (!f64) snprintf(name, sizeof name, "k_block_refine<%d>", g.kind);
             else if (h.stages && h.rows) snprintf(name, sizeof name, "k_block_f64_rows<%d,%d>", g.kind, h.stages);
+            else if (h.stages && h.res) snprintf(name, sizeof name, "k_block_f64_ring<%d,%d,%d,1>", g.kind, h.stages, h.bw);
             else if (h.stages) snprintf(name, sizeof name, "k_block_f64_ring<%d,%d,%d>", g.kind, h.stages, h.bw);
             else snprintf(name, sizeof name, "k_block_f64<%d>", g.kind);
         }

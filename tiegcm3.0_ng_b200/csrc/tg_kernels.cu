@@ -1610,7 +1610,13 @@ __global__ void __launch_bounds__(128) k_block_f64(SegTable tab, double *scratch
 // (P, Q, R, f) arrive in a D-stage shared-memory ring, one 256-byte copy per
 // entry issued by one lane.  Same arithmetic as blk_f64_col.
 // ---------------------------------------------------------------------------
-template <int B, int D, int W>
+// With GSM, Gamma of the warp's columns stays in the warp's slice of shared
+// memory for every level (k2max-1 rows of B*B*W doubles after the ring)
+// instead of an L2 scratch slot, so DRAM sees P, Q, R, f read once and u
+// written once (z is still parked in u, a small L2 footprint); and the next
+// tile's first D levels are requested before the back sweep, which needs only
+// Gamma and the parked z.  Same arithmetic, same bits.
+template <int B, int D, int W, bool GSM = false>
 __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *scratch, unsigned *status)
 {
     // W < 32: a warp covers W columns (lanes >= W idle), so that more warps
@@ -1620,13 +1626,40 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
     extern __shared__ __align__(128) double smem_b[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int cl = lane & (W - 1);            // column of this lane within the tile (idle lanes alias)
-    Ring<NE, D, W> ring{smem_b + (long)warp * D * NE * W, bars + warp * D, l2_policy(tab.hints, false)};
+    const long gsm_rows = GSM ? (long)(tab.k2max > 1 ? tab.k2max - 1 : 1) * BB : 0;
+    double *wbase = smem_b + (long)warp * (D * NE * W + gsm_rows * W);
+    Ring<NE, D, W> ring{wbase, bars + warp * D, l2_policy(tab.hints, false)};
     const unsigned long long keep = l2_policy(tab.hints, true);
     ring.init(lane);
-    const long gs = (long)gridDim.x * nwarps * W;
-    double *gam = scratch + ((long)blockIdx.x * nwarps + warp) * W + cl;
+    const long gs = GSM ? (long)W : (long)gridDim.x * nwarps * W;
+    double *gam = GSM ? wbase + D * NE * W + cl : scratch + ((long)blockIdx.x * nwarps + warp) * W + cl;
+    // this lane's copy source (entry `lane` of level 0) of the tile at col0
+    // of segment s, and its level stride
+    auto source = [&](const Seg &s, long col0, long &lstride) -> const double * {
+        const long ld = s.ld;
+        lstride = 0;
+        if (lane < BB) {
+            lstride = BB * ld;
+            return s.a + col0 + lane * ld;
+        }
+        if (lane < 2 * BB) {
+            lstride = BB * ld;
+            return s.b + col0 + (lane - BB) * ld;
+        }
+        if (lane < 3 * BB) {
+            lstride = BB * ld;
+            return s.c + col0 + (lane - 2 * BB) * ld;
+        }
+        if (lane < NE) {
+            lstride = B * ld;
+            return s.f + col0 + (lane - 3 * BB) * ld;
+        }
+        return s.a + col0;
+    };
+    const int vstride = gridDim.x * nwarps;
     unsigned q = 0;
-    for (int vt = blockIdx.x * nwarps + warp; vt < tab.ntiles * NSUB; vt += gridDim.x * nwarps) {
+    int pref_vt = -1;   // a tile whose first levels were requested during the previous one
+    for (int vt = blockIdx.x * nwarps + warp; vt < tab.ntiles * NSUB; vt += vstride) {
         const int t = vt / NSUB;
         const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
         const long col0 = (long)(t - s.tile0) * 32 + (long)(vt % NSUB) * W;
@@ -1635,24 +1668,13 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
         const int k2 = s.k2;
         const bool valid = lane < W && col0 + lane < s.ncol;
         // entry e of level k: P/Q/R element e at (k*BB + e)*ld, f component at (k*B + i)*ld
-        const double *src = s.a + col0;
         long lstride = 0;
-        if (lane < BB) {
-            src = s.a + col0 + lane * ld;
-            lstride = BB * ld;
-        } else if (lane < 2 * BB) {
-            src = s.b + col0 + (lane - BB) * ld;
-            lstride = BB * ld;
-        } else if (lane < 3 * BB) {
-            src = s.c + col0 + (lane - 2 * BB) * ld;
-            lstride = BB * ld;
-        } else if (lane < NE) {
-            src = s.f + col0 + (lane - 3 * BB) * ld;
-            lstride = B * ld;
-        }
+        const double *src = source(s, col0, lstride);
         double *pU = s.x + col0 + cl;
         const int pre = k2 < D ? k2 : D;
-        for (int j = 0; j < pre; ++j) ring.issue(q + j, src + j * lstride, lane);
+        if (pref_vt != vt)
+            for (int j = 0; j < pre; ++j) ring.issue(q + j, src + j * lstride, lane);
+        pref_vt = -1;
         bool ok = true;
         double G[BB], z[B];
         double *pUk = pU, *gk = gam;   // level k of the parked z and of Gamma
@@ -1718,11 +1740,31 @@ __global__ void __launch_bounds__(256) k_block_f64_ring(SegTable tab, double *sc
 #pragma unroll
                         for (int n = 1; n < B; ++n) g = xadd(g, xmul(Wi[i + B * n], R[n + B * m]));
                         G[i + B * m] = g;
-                        st_hint(&gk[(long)(i + B * m) * gs], g, keep);
+                        if (GSM)
+                            gk[(long)(i + B * m) * gs] = g;
+                        else
+                            st_hint(&gk[(long)(i + B * m) * gs], g, keep);
                     }
             }
         }
         q += k2;
+        if (GSM) {
+            // the ring is free: request the next tile's first levels before
+            // the back sweep (only when that tile is one this warp solves)
+            const int vn = vt + vstride;
+            if (vn < tab.ntiles * NSUB) {
+                const int tn = vn / NSUB;
+                const Seg sn = tab.segs ? tab.segs[find_seg(tab, tn)] : tab.one;
+                const long c0n = (long)(tn - sn.tile0) * 32 + (long)(vn % NSUB) * W;
+                if (c0n < sn.ncol) {
+                    long lsn = 0;
+                    const double *srcn = source(sn, c0n, lsn);
+                    const int pren = sn.k2 < D ? sn.k2 : D;
+                    for (int j = 0; j < pren; ++j) ring.issue(q + j, srcn + j * lsn, lane);
+                    pref_vt = vn;
+                }
+            }
+        }
         if (!valid) continue;
         bool fin = true;
         double un[B], top[B];
@@ -2934,6 +2976,18 @@ cudaError_t with_block_ring(int B, int D, int W, F f)
     return cudaErrorInvalidValue;
 }
 
+// Block ring kernels with Gamma resident in shared memory.
+template <typename F>
+cudaError_t with_block_ring_gsm(int B, int D, int W, F f)
+{
+#define TG_RING_GSM(b, d, w) \
+    if (B == b && D == d && W == w) return f(k_block_f64_ring<b, d, w, true>);
+    TG_RING_GSM(2, 4, 32) TG_RING_GSM(2, 4, 16) TG_RING_GSM(2, 8, 16) TG_RING_GSM(2, 4, 8) TG_RING_GSM(2, 8, 8)
+    TG_RING_GSM(3, 4, 16) TG_RING_GSM(3, 4, 8) TG_RING_GSM(3, 8, 8)
+#undef TG_RING_GSM
+    return cudaErrorInvalidValue;
+}
+
 // Block refinement ring kernels (2x2 blocks) by ring depth.
 template <typename F>
 cudaError_t with_block_refine_ring(int B, int D, F f)
@@ -3004,8 +3058,10 @@ void device_init()
                 for (int w : {0, 1}) with_scalar_res(c, l, w, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int b : {2, 3})
             for (int d : {4, 8, 16})
-                for (int w : {32, 16, 8})
+                for (int w : {32, 16, 8}) {
                     with_block_ring(b, d, w, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+                    with_block_ring_gsm(b, d, w, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+                }
         for (int d : {4, 8})
             for (int b : {2, 3}) with_block_rows(b, d, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
     });
@@ -3136,8 +3192,11 @@ void set_kind_overlap(int mode) { g_kind_overlap.store(mode == 0 || mode == 1 ? 
 int kind_overlap() { return g_kind_overlap.load(); }
 void set_column_residency(int kind, int precision, int mode)
 {
-    if (kind != TG_KIND_SCALAR || precision != TG_PREC_F64) return;
-    g_tile[0][0].res = mode >= 0 && mode <= 2 ? mode : kDefaultTile[0][0].res;
+    if (precision != TG_PREC_F64) return;
+    TileCfg &t = g_tile[kind_index(kind)][0];
+    const int def = kDefaultTile[kind_index(kind)][0].res;
+    if (kind == TG_KIND_SCALAR) t.res = mode >= 0 && mode <= 2 ? mode : def;
+    else t.res = mode >= 0 && mode <= 2 ? (mode ? 1 : 0) : def;
 }
 int column_residency() { return g_tile[0][0].res; }
 void set_stage_levels(int kind, int precision, int l)
@@ -3222,6 +3281,13 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     if (sh->lps == 1 && stages > 0 && stages < 4 && precision == TG_PREC_F64)
         stages = sh->stages = 4;   // per-level rings: depth 4, 8, 16
     if (sh->bw < 32 && stages > 8) stages = sh->stages = 8;
+    // block kinds: Gamma resident in shared memory (k_block_f64_ring<..., true>)
+    if (kind != TG_KIND_SCALAR && precision == TG_PREC_F64 && stages > 0 && !sh->rows &&
+        g_tile[kind_index(kind)][0].res > 0) {
+        sh->res = 1;
+        if (stages > 8) stages = sh->stages = 8;
+        if (with_block_ring_gsm(kind, stages, sh->bw, [](auto) { return cudaSuccess; }) != cudaSuccess) sh->res = 0;
+    }
     if (sh->rows && stages > 8) stages = sh->stages = 8;
     if (kind == TG_KIND_SCALAR && sh->cpt == 2 && sh->pf > 8) sh->pf = 8;
     if (stages > 0) {
@@ -3233,8 +3299,13 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
             sh->res = 0;
             sh->w2g = w2g = 1;
         }
-        const size_t need = kind == TG_KIND_SCALAR ? scalar_smem_bytes(precision, sh->threads, 1, k2max, stages, w2g, sh->lps)
-                                                   : block_smem_bytes(kind, stages, sh->threads, sh->rows, sh->bw, precision);
+        size_t need = kind == TG_KIND_SCALAR ? scalar_smem_bytes(precision, sh->threads, 1, k2max, stages, w2g, sh->lps)
+                                             : block_smem_bytes(kind, stages, sh->threads, sh->rows, sh->bw, precision);
+        if (kind != TG_KIND_SCALAR && sh->res) {
+            const size_t gam = (size_t)sh->threads / 32 * (size_t)(k2max > 1 ? k2max - 1 : 1) * kind * kind * sh->bw * 8;
+            if (need + gam > (size_t)(smem_optin() - 1024)) sh->res = 0;   // too tall: Gamma in L2
+            else need += gam;
+        }
         if (!sh->res && need > (size_t)(smem_optin() - 1024)) {
             stages = 0;
             sh->stages = 0;
@@ -3267,8 +3338,12 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     } else {
         const int B = kind;
         sh->smem = block_smem_bytes(B, stages, sh->threads, sh->rows, sh->bw, precision);
+        if (sh->res)
+            sh->smem += (size_t)sh->threads / 32 * (size_t)(k2max > 1 ? k2max - 1 : 1) * B * B * sh->bw * 8;
         if (sh->smem > (size_t)(smem_optin() - 1024)) return cudaErrorInvalidConfiguration;
-        if (stages > 0 && precision != TG_PREC_F64)
+        if (sh->res)
+            e = with_block_ring_gsm(B, stages, sh->bw, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
+        else if (stages > 0 && precision != TG_PREC_F64)
             e = with_block_refine_ring(B, stages, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
         else if (stages > 0 && sh->rows)
             e = with_block_rows(B, stages, [&](auto k) { return occupancy(k, sh->threads, sh->smem, &per_sm); });
@@ -3285,7 +3360,7 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     long blocks = (long)per_sm * nsm;
-    if (kind != TG_KIND_SCALAR && precision == TG_PREC_F64) {
+    if (kind != TG_KIND_SCALAR && precision == TG_PREC_F64 && !sh->res) {
         // keep the Gamma scratch of all resident blocks within the L2 budget
         // (a cap on the total, not per SM, so that a grid that fits in one
         // wave is not split into two).  The block refinement kernel is not
@@ -3381,6 +3456,14 @@ cudaError_t launch_block(const SegTable &tab, int B, int precision, const Shape 
         t.hints = cache_hints();
         cudaError_t e = with_block_refine_ring(B, sh.stages, [&](auto k) {
             k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, rf, reinterpret_cast<float *>(scratch), status, hist);
+            return cudaSuccess;
+        });
+        if (e != cudaSuccess) return e;
+    } else if (precision == TG_PREC_F64 && sh.stages > 0 && sh.res) {
+        SegTable t = tab;
+        t.hints = cache_hints();
+        cudaError_t e = with_block_ring_gsm(B, sh.stages, sh.bw, [&](auto k) {
+            k<<<sh.blocks, sh.threads, sh.smem, st>>>(t, scratch, status);
             return cudaSuccess;
         });
         if (e != cudaSuccess) return e;
