@@ -72,6 +72,10 @@ def parse():
                         "(default: library default); or dt / minor / comp / settei / oplus for the fused assembly+solve kernels, "
                         "advec / smooth / filter for the horizontal operators and the time filter")
     p.add_argument("--skip-assembly", action="store_true")
+    p.add_argument("--tune", action="store_true",
+                   help="run the autotuner over this workload's segments first and record its choices in the "
+                        "package's tuning cache (tiegcm3.0_ng_b200/tuned_b200.json)")
+    p.add_argument("--no-tuned", action="store_true", help="ignore the package's tuning cache (library defaults)")
     return p.parse_args()
 
 
@@ -554,6 +558,20 @@ def main():
     blk_segs = [s for s in segs if s["kind"] != cs.TG_KIND_SCALAR]
     unknowns = dw.unknowns()                       # the whole job's, over all ranks
     stream = torch.cuda.Stream(device=dev)
+    from tiegcm_ng_b200 import autotune
+    tuning = None
+    if args.tune:
+        res = autotune.tune(segs, cache=autotune.PACKAGED, reps=5)
+        tuning = {"tuned_now": {f"kind{k}_prec{p}": [list(v[0]), v[1]] for (k, p), v in res.items()
+                                if k != "combined"}}
+        for (k, p), (best, ms, times) in sorted((kv for kv in res.items() if kv[0][0] != "combined"),
+                                                key=lambda kv: kv[0]):
+            print(f"autotune kind {k} prec {p}: best {best} {ms:.4f} ms; " +
+                  ", ".join(f"{c}: {t:.4f}" for c, t in sorted(times.items(), key=lambda ct: ct[1])),
+                  file=sys.stderr)
+    elif not args.no_tuned:
+        found = autotune.load(segs, cache=autotune.PACKAGED)
+        tuning = {"applied_from_cache": [list(f) for f in found]} if found else {"applied_from_cache": []}
 
     def make(seglist, prec):
         p = pkg.Plan(seglist, prec)
@@ -828,6 +846,7 @@ def main():
             "config": workload_config(pkg, wl, args.max_sub),
             "roofline": roofline("fp64", "k_scalar_f64"),
             "kernels": {k: plans[k].describe() for k in ("fp64", "refine")},
+            "tuning": tuning,
             "fp64": {"value": value, "ms_per_step": results["fp64"], "status": cs.STATUS_NAMES[rc64]},
             "refine": {"value": vref, "ms_per_step": results["refine"], "refine_over_fp64": vref / value,
                        "max_rel_err_vs_fp64": max_rel, "sweep_histogram": hist, "status": cs.STATUS_NAMES[rc_ref],

@@ -5,7 +5,9 @@ kat_*.npz    known-answer tests: integer-valued, diagonally dominant systems
              arithmetic, so x* is the exact answer independently of any
              solver (the reference ships no golden vectors for this path).
 pin_*.npz    bitwise pins of the oracle on small seeded synthetic inputs, so a
-             change of the oracle's arithmetic is noticed.
+             change of the oracle's arithmetic is noticed (pin_ringfilter:
+             the polar ring filter of ringfilter.F, orders 1 and 3, linear and
+             polynomial reconstruction, on the 5 deg global grid).
 kat_horizontal.npz  known answers of advec_ng and smooth_ng (src/advec_ng.F90,
              src/smooth_ng.F90, src/dffm_ng.F90) on a small nest: fields that
              are multiples of 3, integer winds and power-of-two
@@ -128,12 +130,25 @@ def kat_horizontal(rng, nk=3, nlon=7, nlat=5):
                 hadvec=np.asfortranarray(had), fout=np.asfortranarray(fout))
 
 
+def pin_ringfilter():
+    orc = ge.load_oracle()
+    pkg = ge.load_package()
+    f = pkg.synth.ring_field(2, 72, 36, pkg.synth.SEED_BASE + 7)
+    chunks = np.asarray(pkg.synth.RING_CHUNKS[(72, 36)], dtype=np.int32)
+    dl = 2.0 * (4.0 * np.arctan(1.0)) / 72
+    return dict(f=f, chunks=chunks, dlamda=np.float64(dl), o1=orc.ringfilter(f, 1, 0, chunks, dl),
+                o3=orc.ringfilter(f, 3, 0, chunks, dl), o3poly=orc.ringfilter(f, 3, 1, chunks, dl))
+
+
 def main(names=()):
     if names:
         if "kat_horizontal" in names:
             np.savez_compressed(os.path.join(HERE, "kat_horizontal.npz"),
                                 **kat_horizontal(np.random.default_rng(20261204)))
+        if "pin_ringfilter" in names:
+            np.savez_compressed(os.path.join(HERE, "pin_ringfilter.npz"), **pin_ringfilter())
         return
+    np.savez_compressed(os.path.join(HERE, "pin_ringfilter.npz"), **pin_ringfilter())
     np.savez_compressed(os.path.join(HERE, "kat_horizontal.npz"), **kat_horizontal(np.random.default_rng(20261204)))
     rng = np.random.default_rng(20261203)
     out = {}

@@ -149,3 +149,25 @@ def test_ringfilter_rejects_bad_arguments(pkg):
         pkg.ringfilter(f, 16, 0, ch, 0.1)            # more modes than the kernel keeps
     with pytest.raises(pkg.TgError):
         pkg.ringfilter(f, 1, 0, (3, 2, 18), 0.1)     # fewer than 3 chunks
+
+
+def test_oracle_matches_golden_pin(orc):
+    """The oracle's filter of the committed field, bit for bit
+    (tests/golden/pin_ringfilter.npz, made by tests/golden/make_golden.py)."""
+    from conftest import golden
+    g = golden("pin_ringfilter.npz")
+    dl = float(g["dlamda"])
+    assert np.array_equal(orc.ringfilter(g["f"], 1, 0, g["chunks"], dl), g["o1"])
+    assert np.array_equal(orc.ringfilter(g["f"], 3, 0, g["chunks"], dl), g["o3"])
+    assert np.array_equal(orc.ringfilter(g["f"], 3, 1, g["chunks"], dl), g["o3poly"])
+
+
+@pytest.mark.gpu
+def test_ringfilter_matches_golden_pin(cuda, pkg):
+    from conftest import golden
+    g = golden("pin_ringfilter.npz")
+    dl = float(g["dlamda"])
+    for key, order, poly in (("o1", 1, 0), ("o3", 3, 0), ("o3poly", 3, 1)):
+        got = np.array(g["f"], order="F", copy=True)
+        pkg.ringfilter(got, order, poly, g["chunks"], dl)
+        assert np.array_equal(got, g[key]), key

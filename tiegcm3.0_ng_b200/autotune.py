@@ -29,6 +29,8 @@ import os
 from . import colsolve as cs
 
 CACHE_DEFAULT = os.path.join(os.path.expanduser("~"), ".cache", "tg_colsolve_tune.json")
+# choices tuned on a B200 for the benchmark workloads, shipped with the package
+PACKAGED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_b200.json")
 
 SCALAR_F64 = [("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg", 256, 1, 8), ("reg", 64, 1, 16),
               ("reg", 128, 1, 16), ("reg", 128, 2, 4), ("reg", 256, 2, 4), ("reg", 128, 2, 8),
