@@ -806,6 +806,36 @@ def main():
             e2e["per_call_drop_ins"] = {"value": unk_pc / dt_pc, "ms_per_step": dt_pc * 1e3,
                                         "path": f"tg_trsolv_ng x{wl.n_scalar} + tg_blksolve on one sub-step of "
                                                 f"{wl.grids[0].name}"}
+        # the global grid's latitude scan (src/dt.F:126-330): one trsolv per
+        # latitude slab of nlon+4 columns, as calls and deferred to one flush
+        if world == 1:
+            g = wl.grids[0]
+            lonmax, nlat, nk = g.nlon + 4, g.nlat, g.nk
+            a, b, c, f = pkg.synth.scalar_system(nk, lonmax * nlat, g.dz, 4242, wl.d0_range, wl.loss, wl.d_span)
+            shp = (nk, lonmax, nlat)
+            a, b, c, f = (np.asfortranarray(v.reshape(shp, order="F")) for v in (a, b, c, f))
+            xs = np.zeros(shp, order="F")
+            work = [np.zeros((nk, lonmax), order="F") for _ in range(4)]
+            scan_args = (1, nk, 1, nk - 1, 1, lonmax, lonmax)
+
+            def scan(defer):
+                for lat in range(nlat):
+                    for w, v in zip(work, (a, b, c, f)):
+                        w[...] = v[:, :, lat]          # the scan's per-latitude work arrays
+                    if defer:
+                        cs.trsolv_defer(*work, xs[:, :, lat], *scan_args)
+                    else:
+                        cs.trsolv(*work, xs[:, :, lat], *scan_args)
+                if defer:
+                    cs.trsolv_flush()
+            t_slab = time_host(lambda: scan(False), 5)
+            x_slab = xs.copy()
+            t_defer = time_host(lambda: scan(True), 5)
+            e2e["per_latitude"] = {"per_slab_ms": t_slab * 1e3, "deferred_ms": t_defer * 1e3,
+                                   "same_bits": bool(np.array_equal(x_slab, xs)),
+                                   "scan": f"{nlat} latitude slabs of {lonmax} x {nk} (one scalar system of "
+                                           f"{g.name}), tg_trsolv per slab vs tg_trsolv_defer + one "
+                                           f"tg_trsolv_flush, host wall clock"}
         # the link this path is bound by: pinned host<->device copy bandwidth
         nb = min(h2d, 1 << 30) // 8
         hbuf = torch.empty(nb, dtype=torch.float64, pin_memory=True)

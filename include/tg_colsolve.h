@@ -604,7 +604,10 @@ int tg_set_stage_levels(int kind, int precision, int levels);
  * scratch slot per resident lane, w3 parked in x (k_scalar_f64_chunk); 1 w2
  * in the warp's shared memory, w3 parked in x; 2 both in shared memory
  * (k_scalar_f64_res).  Block kinds: 0 Gamma in an L2 scratch slot, 1 or 2
- * Gamma in the warp's shared memory (k_block_f64_ring<..., 1>).  On chip,
+ * Gamma in the warp's shared memory (k_block_f64_ring<..., 1>).  Scalar
+ * refinement (TG_PREC_F32_REFINE): 1 the warp's whole 32-column tile (FP64
+ * a, b, c, f, x and the FP32 factors) in shared memory, so the coefficients
+ * are read once for all sweeps (k_scalar_refine_tile).  On chip,
  * DRAM sees the coefficients read once, at the cost of fewer warps per SM.
  * -1 restores the default.  Columns too tall for shared memory take mode 0.
  * Same arithmetic, same bits. */

@@ -285,3 +285,29 @@ def test_autotune_tune_and_cache_round_trip(cuda, pkg, orc, tmp_path):
         for kind in (0, 2):
             for prec in (pkg.TG_PREC_F64, pkg.TG_PREC_F32_REFINE):
                 autotune.reset(kind, prec)
+
+
+def test_every_refinement_variant_within_tolerance(cuda, pkg, orc):
+    """Each scalar refinement launch shape the autotuner may choose (register
+    kernels, the bulk-copy ring, the whole tile in shared memory) solves to
+    within 1e-10 of the FP64 oracle, with a sweep histogram over every
+    column."""
+    torch = cuda
+    from tiegcm_ng_b200 import autotune
+    specs = [(0, 57, 57, 1000), (0, 29, 28, 77), (0, 113, 113, 40), (0, 57, 56, 31)]
+    segs, refs_in = make_segments(pkg, torch, specs, seed=700)
+    try:
+        for cand in autotune.candidates(0, pkg.TG_PREC_F32_REFINE):
+            autotune.apply(0, pkg.TG_PREC_F32_REFINE, cand)
+            for s in segs:
+                s["x"].fill_(3.5)
+            plan = pkg.Plan(segs, pkg.TG_PREC_F32_REFINE)
+            plan.execute()
+            rc, _ = plan.status()
+            hist = plan.sweep_histogram(8)
+            plan.close()
+            assert rc in (pkg.TG_OK, pkg.TG_ENOCONV), cand
+            assert sum(hist) == sum(s["ncol"] for s in segs), cand
+            check(pkg, orc, segs, refs_in, exact=False)
+    finally:
+        autotune.reset(0, pkg.TG_PREC_F32_REFINE)

@@ -16,7 +16,8 @@ from a CUDA graph, CUDA-event timed) and keeps the fastest:
             the sweep's w2 ("res1cL") or w2 and w3 ("res2cL") resident in
             shared memory, L levels per stage
   FP32+ref  columns per block x prefetch depth; scalar kind also the
-            bulk-copy refinement ring of 2, 3 or 4 stages ("ring")
+            bulk-copy refinement ring of 2, 3 or 4 stages ("ring") and the
+            whole tile held in shared memory ("tile")
 
 Results are cached in a JSON file keyed by GPU name, kind, precision, level
 count and a column-count bucket, and applied with tg_set_tile /
@@ -48,7 +49,7 @@ BLOCK_F64 = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 9
              ("ringsm", 4, 1, 4), ("ring16sm", 4, 1, 4), ("ring16sm", 8, 1, 4), ("ring8sm", 4, 1, 4),
              ("ring8sm", 8, 1, 4)]
 SCALAR_REF = [("reg", 64, 1, 4), ("reg", 128, 1, 4), ("reg", 256, 1, 4), ("reg", 128, 1, 8), ("reg", 64, 1, 8),
-              ("ring", 2, 1, 4), ("ring", 3, 1, 4), ("ring", 4, 1, 4), ("ring", 2, 2, 4)]
+              ("ring", 2, 1, 4), ("ring", 3, 1, 4), ("ring", 4, 1, 4), ("ring", 2, 2, 4), ("tile", 2, 1, 4)]
 BLOCK_REF = [("reg", 32, 1, 4), ("reg", 64, 1, 4), ("reg", 128, 1, 4), ("ring", 4, 1, 4), ("ring", 8, 1, 4),
              ("ring", 4, 2, 4)]
 
@@ -65,6 +66,8 @@ def apply(kind, precision, cand):
     scalar64 = kind == cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64
     if kind == cs.TG_KIND_SCALAR:
         cs.set_prefetch(kind, precision, pf)
+        if precision != cs.TG_PREC_F64:
+            cs.set_column_residency(kind, precision, 1 if v == "tile" else 0)
         if precision == cs.TG_PREC_F64:
             levels = int(v[5:]) if v.startswith("chunk") else int(v[5:]) if v.startswith("res") else 1
             cs.set_stage_levels(kind, precision, levels)
@@ -73,7 +76,7 @@ def apply(kind, precision, cand):
         cs.set_block_rows(kind, 1 if v == "rows" else 0)
         cs.set_block_width(kind, {"ring16": 16, "ring8": 8, "ring16sm": 16, "ring8sm": 8}.get(v, 32))
         cs.set_column_residency(kind, precision, 1 if v.endswith("sm") else 0)
-    if v in ("ring", "ringg", "rows", "ring16", "ring8") or v.startswith(("chunk", "res", "ring")):
+    if v in ("ring", "ringg", "rows", "ring16", "ring8", "tile") or v.startswith(("chunk", "res", "ring")):
         cs.set_pipeline(kind, precision, p1, p2)    # ring depth, warps per CTA
     else:
         cs.set_pipeline(kind, precision, 0)
@@ -87,6 +90,8 @@ def reset(kind, precision):
     cs.set_pipeline(kind, precision, -1, 0)
     if kind == cs.TG_KIND_SCALAR:
         cs.set_prefetch(kind, precision, -1)
+    if kind == cs.TG_KIND_SCALAR and precision != cs.TG_PREC_F64:
+        cs.set_column_residency(kind, precision, -1)
     if kind == cs.TG_KIND_SCALAR and precision == cs.TG_PREC_F64:
         cs.set_scratch_global(kind, precision, -1)
         cs.set_stage_levels(kind, precision, 0)

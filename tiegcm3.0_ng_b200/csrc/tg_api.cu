@@ -2110,9 +2110,9 @@ __attribute__((visibility("default"))) int tg_set_stage_levels(int kind, int pre
 
 __attribute__((visibility("default"))) int tg_set_column_residency(int kind, int precision, int mode)
 {
-    if ((kind != TG_KIND_SCALAR && kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) || precision != TG_PREC_F64 ||
-        mode > 2) {
-        set_err("tg_set_column_residency: applies to TG_PREC_F64 with mode 0, 1, 2 or -1");
+    if ((kind != TG_KIND_SCALAR && kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) || bad_prec(precision) ||
+        (precision != TG_PREC_F64 && kind != TG_KIND_SCALAR) || mode > 2) {
+        set_err("tg_set_column_residency: FP64 kinds or the scalar refinement, mode 0, 1, 2 or -1");
         return TG_EINVAL;
     }
     tg::set_column_residency(kind, precision, mode);
@@ -2177,7 +2177,8 @@ __attribute__((visibility("default"))) int tg_plan_describe(const tg_plan *p, ch
         const Shape &h = g.shape;
         char name[96];
         if (g.kind == TG_KIND_SCALAR) {
-            if (!f64 && h.stages) snprintf(name, sizeof name, "k_scalar_refine_ring<%d>", h.stages);
+            if (!f64 && h.res == 3) snprintf(name, sizeof name, "k_scalar_refine_tile");
+            else if (!f64 && h.stages) snprintf(name, sizeof name, "k_scalar_refine_ring<%d>", h.stages);
             else if (!f64) snprintf(name, sizeof name, "k_scalar_refine<%d>", h.pf);
             else if (h.stages && h.res) snprintf(name, sizeof name, "k_scalar_f64_res<%d,%d,%d>", h.stages, h.lps, h.res == 2);
             else if (h.stages && h.lps > 1) snprintf(name, sizeof name, "k_scalar_f64_chunk<%d,%d>", h.stages, h.lps);

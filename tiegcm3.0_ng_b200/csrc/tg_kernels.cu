@@ -1345,6 +1345,177 @@ __global__ void __launch_bounds__(256) k_scalar_refine_ring(SegTable tab, Refine
 }
 
 // ---------------------------------------------------------------------------
+// Scalar refinement with the whole tile on chip: the FP64 a, b, c, f of the
+// warp's 32 columns for every level arrive once (one mbarrier transaction of
+// 4*k2 bulk copies), and sweep 0, every residual, every correction and an
+// FP64 fallback run from shared memory, with x (FP64) and the FP32 factors
+// beside them; x goes to HBM once.  DRAM sees 40 B per unknown, at the price
+// of (5 doubles + 3 floats) per level and column of shared memory: 95 KB per
+// warp at 57 levels, two warps per SM.  Same stopping rule and FP64 fallback
+// as k_scalar_refine_ring.
+// ---------------------------------------------------------------------------
+constexpr int kRefineTileBytesPerLevel = 32 * (5 * 8 + 3 * 4);
+
+__global__ void __launch_bounds__(32) k_scalar_refine_tile(SegTable tab, Refine rf, unsigned *status,
+                                                           unsigned long long *hist)
+{
+    extern __shared__ __align__(128) double smem_t[];
+    __shared__ __align__(8) unsigned long long bar;
+    const int lane = threadIdx.x;
+    const long K = tab.k2max;
+    double *A = smem_t;                                  // plane p (a, b, c, f) row k at (p*K + k)*32
+    double *X = A + 4 * K * 32;                          // x(k) at k*32
+    float *W2 = reinterpret_cast<float *>(X + K * 32);   // w2(k), 1/w1(k), y(k) at k*32
+    float *RI = W2 + K * 32;
+    float *Y = RI + K * 32;
+    const unsigned long long pol = l2_policy(tab.hints, false);
+    if (lane == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    unsigned long long hl[kMaxSweepBins];
+#pragma unroll
+    for (int i = 0; i < kMaxSweepBins; ++i) hl[i] = 0ull;
+    unsigned phase = 0;
+    for (int t = blockIdx.x; t < tab.ntiles; t += gridDim.x) {
+        const Seg s = tab.segs ? tab.segs[find_seg(tab, t)] : tab.one;
+        const long col0 = (long)(t - s.tile0) * 32;
+        const long ld = s.ld;
+        const int k2 = s.k2;
+        const bool valid = col0 + lane < s.ncol;
+        // the tile's 4*k2 rows of 256 B, one transaction
+        if (lane == 0) mbar_expect(&bar, (uint32_t)(4 * k2 * 256));
+        __syncwarp();
+        for (int r = lane; r < 4 * k2; r += 32) {
+            const int p = r & 3, k = r >> 2;
+            const double *src = (p == 0 ? s.a : p == 1 ? s.b : p == 2 ? s.c : s.f) + (long)k * ld + col0;
+            bulk_load_hint(A + ((long)p * K + k) * 32, src, 256u, &bar, pol);
+        }
+        if (!mbar_wait_warp(&bar, phase)) {
+            mbar_wait_warp(&bar, phase);
+            if (lane == 0) report(status, s.status_idx, FLAG_TIMEOUT);
+            return;
+        }
+        phase ^= 1u;
+        const double *pa = A + lane, *pb = A + K * 32 + lane, *pc = A + 2 * K * 32 + lane, *pf = A + 3 * K * 32 + lane;
+        double *px = X + lane;
+        float *pw2 = W2 + lane, *pri = RI + lane, *py = Y + lane;
+        // ---- sweep 0: FP32 factor and solve
+        bool ok = true;
+        float xm0 = 0.f;
+        if (valid) {
+            float w1 = (float)pb[0], ri = __frcp_rn(w1), y = (float)pf[0] * ri;
+            ok = (fabsf(w1) <= FLT_MAX) && (w1 != 0.f);
+            pri[0] = ri;
+            py[0] = y;
+            for (int k = 1; k < k2; ++k) {
+                const float af = (float)pa[k * 32];
+                const float w2 = (float)pc[(k - 1) * 32] * ri;
+                pw2[(k - 1) * 32] = w2;
+                w1 = (float)pb[k * 32] - af * w2;
+                ri = __frcp_rn(w1);
+                y = ((float)pf[k * 32] - af * y) * ri;
+                ok = ok && (fabsf(w1) <= FLT_MAX) && (w1 != 0.f);
+                pri[k * 32] = ri;
+                py[k * 32] = y;
+            }
+            float xk = y;
+            xm0 = fabsf(xk);
+            px[(k2 - 1) * 32] = (double)xk;
+            for (int k = k2 - 2; k >= 0; --k) {
+                xk = py[k * 32] - pw2[k * 32] * xk;
+                xm0 = fmaxf(xm0, fabsf(xk));
+                px[k * 32] = (double)xk;
+            }
+        }
+        // ---- corrections: FP64 residual from the tile, FP32 solve, x += d
+        bool active = valid && ok, conv = false;
+        int taken = rf.max_sweeps + 1;
+        double dprev = (double)xm0;
+        for (int sw = 1; sw <= rf.max_sweeps && active; ++sw) {
+            double xm1 = 0.0, x0 = px[0];
+            float y = 0.f;
+            for (int k = 0; k < k2; ++k) {
+                const double xp1 = k + 1 < k2 ? px[(k + 1) * 32] : 0.0;
+                const double ak = pa[k * 32];
+                double r = fma(-pb[k * 32], x0, pf[k * 32]);
+                if (k > 0) r = fma(-ak, xm1, r);
+                if (k + 1 < k2) r = fma(-pc[k * 32], xp1, r);
+                const float rr = (float)r;
+                y = k == 0 ? rr * pri[0] : (rr - (float)ak * y) * pri[k * 32];
+                py[k * 32] = y;
+                xm1 = x0;
+                x0 = xp1;
+            }
+            float d = y;
+            double xv = px[(k2 - 1) * 32] + (double)d;
+            px[(k2 - 1) * 32] = xv;
+            double dmax = fabs((double)d), xmax = fabs(xv);
+            for (int k = k2 - 2; k >= 0; --k) {
+                d = py[k * 32] - pw2[k * 32] * d;
+                xv = px[k * 32] + (double)d;
+                px[k * 32] = xv;
+                dmax = fmax(dmax, fabs((double)d));
+                xmax = fmax(xmax, fabs(xv));
+            }
+            if (!(xmax <= DBL_MAX) || !(dmax <= DBL_MAX)) {
+                active = false;
+            } else if (refine_done(dmax, xmax, dprev, rf.rel_tol, sw == 1)) {
+                conv = true;
+                active = false;
+                taken = sw;
+            } else {
+                dprev = dmax;
+            }
+        }
+        unsigned flags = 0u;
+        if (valid && !conv) {
+            // FP64 re-solve from the tile (bit-exact; w3 in x, w2 in the two
+            // float planes' halves)
+            bool okd = true;
+            double w1 = pb[0], w3 = xdiv(pf[0], w1);
+            okd = finite_nz(w1);
+            px[0] = w3;
+            for (int k = 1; k < k2; ++k) {
+                const double ak = pa[k * 32];
+                const double w2 = xdiv(pc[(k - 1) * 32], w1);
+                pw2[(k - 1) * 32] = __int_as_float(__double2hiint(w2));
+                pri[(k - 1) * 32] = __int_as_float(__double2loint(w2));
+                w1 = xsub(pb[k * 32], xmul(ak, w2));
+                w3 = xdiv(xsub(pf[k * 32], xmul(ak, w3)), w1);
+                okd = okd && finite_nz(w1);
+                px[k * 32] = w3;
+            }
+            double xn = w3;
+            bool fin = finite(xn);
+            for (int k = k2 - 2; k >= 0; --k) {
+                const double w2 = __hiloint2double(__float_as_int(pw2[k * 32]), __float_as_int(pri[k * 32]));
+                xn = xsub(px[k * 32], xmul(w2, xn));
+                fin = fin && finite(xn);
+                px[k * 32] = xn;
+            }
+            flags = FLAG_NOCONV | (okd ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE);
+        }
+        if (valid) {
+            double *gx = s.x + col0 + lane;
+            for (int k = 0; k < k2; ++k) gx[k * ld] = px[k * 32];
+            report(status, s.status_idx, flags);
+        }
+        const int bin = taken < kMaxSweepBins - 1 ? taken : kMaxSweepBins - 1;
+#pragma unroll
+        for (int i = 0; i < kMaxSweepBins; ++i) hl[i] += __popc(__ballot_sync(0xffffffffu, valid && bin == i));
+        // every lane is done with the tile before the next one's copies land
+        __syncwarp();
+        fence_proxy_async();
+    }
+    if (hist && lane == 0)
+#pragma unroll
+        for (int i = 0; i < kMaxSweepBins; ++i)
+            if (hl[i]) atomicAdd(hist + i, hl[i]);
+}
+
+// ---------------------------------------------------------------------------
 // Small-matrix inverse, adjugate / determinant without pivoting, exactly as
 // matdet2/matadj2/matinv2 and matdet3/matadj3/matinv3 (src/matutil.F90).
 // Column-major: A(i,j) = A[(i-1) + B*(j-1)].  Returns false for a zero or
@@ -3050,6 +3221,7 @@ void device_init()
         for (int d : {4, 8, 16})
             for (int g : {0, 1}) with_scalar_ring(d, g, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int c : {2, 3, 4}) with_scalar_refine_ring(c, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
+        allow_smem(k_scalar_refine_tile, lim);
         for (int dd : {4, 8}) with_block_refine_ring(2, dd, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
         for (int c : {2, 3, 4})
             for (int l : {2, 4, 8}) with_scalar_chunk(c, l, [&](auto k) { allow_smem(k, lim); return cudaSuccess; });
@@ -3192,7 +3364,11 @@ void set_kind_overlap(int mode) { g_kind_overlap.store(mode == 0 || mode == 1 ? 
 int kind_overlap() { return g_kind_overlap.load(); }
 void set_column_residency(int kind, int precision, int mode)
 {
-    if (precision != TG_PREC_F64) return;
+    if (precision != TG_PREC_F64) {   // scalar refinement: 1 the whole tile on chip
+        if (kind != TG_KIND_SCALAR) return;
+        g_tile[0][1].res = mode >= 0 && mode <= 2 ? (mode ? 1 : 0) : kDefaultTile[0][1].res;
+        return;
+    }
     TileCfg &t = g_tile[kind_index(kind)][0];
     const int def = kDefaultTile[kind_index(kind)][0].res;
     if (kind == TG_KIND_SCALAR) t.res = mode >= 0 && mode <= 2 ? mode : def;
@@ -3265,6 +3441,9 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
     sh->lps = stages > 0 && kind == TG_KIND_SCALAR && precision == TG_PREC_F64 && w2g ? g_tile[0][0].lps : 1;
     if (kind == TG_KIND_SCALAR && precision != TG_PREC_F64 && stages > 0)   // refinement ring: 2..4 stages
         stages = sh->stages = stages < 2 ? 2 : (stages > 4 ? 4 : stages);
+    // refinement with the whole tile on chip (k_scalar_refine_tile)
+    const bool refine_tile = kind == TG_KIND_SCALAR && precision != TG_PREC_F64 && stages > 0 && g_tile[0][1].res > 0 &&
+                             (size_t)k2max * kRefineTileBytesPerLevel <= (size_t)(smem_optin() - 1024);
     if (kind == TG_KIND_BLOCK2 && precision != TG_PREC_F64 && stages > 0)   // block refinement ring: 4 or 8 levels
         stages = sh->stages = stages > 4 ? 8 : 4;
     // shared-memory-resident scalar kernel (k_scalar_f64_res): chunked ring of
@@ -3316,7 +3495,12 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
             sh->lps = 1;
         }
     }
-    if (kind == TG_KIND_SCALAR) {
+    if (refine_tile) {
+        sh->res = 3;
+        sh->threads = 32;
+        sh->smem = (size_t)k2max * kRefineTileBytesPerLevel;
+        e = occupancy(k_scalar_refine_tile, 32, sh->smem, &per_sm);
+    } else if (kind == TG_KIND_SCALAR) {
         sh->smem = sh->res ? (size_t)sh->threads / 32 * res_rows(stages, sh->lps, k2max, sh->res == 2) * 256
                            : scalar_smem_bytes(precision, sh->threads, sh->cpt, k2max, stages, w2g, sh->lps);
         if (sh->smem > (size_t)(smem_optin() - 1024)) return cudaErrorInvalidConfiguration;
@@ -3369,7 +3553,7 @@ cudaError_t plan_shape(int kind, int precision, int k2max, int ntiles, int cpb, 
         const double per_thread = (double)block_scratch_bytes(kind, precision, 1, k2max);
         const long cap = (long)(g_block_scratch_budget / (per_thread * sh->threads));
         if (blocks > cap) blocks = cap > 0 ? cap : 1;
-    } else if (stages > 0 && sh->res != 2) {
+    } else if (stages > 0 && sh->res != 2 && sh->res != 3) {
         // ring kernels: w2 scratch plus the w3 parked in x, 8 B each per level
         // and column (refinement: three float planes plus x; w2 on chip: the
         // parked w3 alone), of every resident column within the L2 budget
@@ -3399,7 +3583,11 @@ cudaError_t launch_scalar(const SegTable &tab, int precision, const Shape &sh, R
 {
     if (tab.ntiles <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
-    if (precision != TG_PREC_F64 && sh.stages > 0) {
+    if (precision != TG_PREC_F64 && sh.res == 3) {
+        SegTable t = tab;
+        t.hints = cache_hints();
+        k_scalar_refine_tile<<<sh.blocks, 32, sh.smem, st>>>(t, rf, status, hist);
+    } else if (precision != TG_PREC_F64 && sh.stages > 0) {
         SegTable t = tab;
         t.hints = cache_hints();
         e = with_scalar_refine_ring(sh.stages, [&](auto k) {
