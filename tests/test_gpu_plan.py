@@ -301,7 +301,14 @@ def test_every_refinement_variant_within_tolerance(cuda, pkg, orc):
             autotune.apply(0, pkg.TG_PREC_F32_REFINE, cand)
             for s in segs:
                 s["x"].fill_(3.5)
-            plan = pkg.Plan(segs, pkg.TG_PREC_F32_REFINE)
+            try:
+                plan = pkg.Plan(segs, pkg.TG_PREC_F32_REFINE)
+            except pkg.TgError:
+                # the register kernels keep three FP32 planes per thread in
+                # shared memory: 113 levels do not fit the wider blocks, and the
+                # plan says so (the autotuner scores such a shape as infinite)
+                assert cand[0] == "reg" and cand[1] * 3 * 113 * 4 > 200 * 1024, cand
+                continue
             plan.execute()
             rc, _ = plan.status()
             hist = plan.sweep_histogram(8)
