@@ -740,7 +740,9 @@ def main():
                                        world, rank, 32)
         need = sum(sum(int(np.prod(shp)) * 8 for sysshp in job_shapes(wl, g) for shp in sysshp) for g, _ in jobs_all)
         avail = host_memory_available()
-        whole = avail is None or need * world < 0.5 * avail
+        # each rank holds only the grid sub-steps its share touches: about
+        # `need` over all ranks together
+        whole = avail is None or need < 0.5 * avail
         if whole:
             jidx = sorted({i // nsys for i, _, _ in mine})
             hw = HostWorkload(pkg, wl, jobs=[jobs_all[j] for j in jidx], threads=os.cpu_count() or 8, pinned=True)
@@ -757,7 +759,7 @@ def main():
             for n in range(len(wl.grids)):
                 flat += hw.scal[n * wl.n_scalar:(n + 1) * wl.n_scalar] + ([hw.blk[n]] if wl.block else [])
             shares = [(t, 0, t[0].shape[-1]) for t in flat]
-            what = (f"one sub-step of each grid (the whole step needs {need * world / 1e9:.0f} GB of pinned host "
+            what = (f"one sub-step of each grid (the whole step needs {need / 1e9:.0f} GB of pinned host "
                     f"memory, {avail / 1e9:.0f} GB available)")
         systems = []
         h2d = d2h = e2e_unk = 0

@@ -24,10 +24,13 @@ def _check(line, n_gpus):
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
     assert line["config"]["workload"]
+    # the same config object the GPU arm prints: the workload's definition
+    assert line["config"]["segments"] == sum(g[4] for g in line["config"]["grids"]) * line["config"]["systems_per_column"]
 
 
 def test_reference_arm_prints_one_contract_line():
-    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1"],
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1",
+                        "--max-sub", "2"],
                        cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _json_lines(r.stdout)
@@ -39,7 +42,7 @@ def test_reference_arm_two_ranks_rank0_only():
     env = dict(os.environ, OMP_NUM_THREADS="2")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", "29571", "bench.py", "--impl", "reference",
-           "--gpus", "2", "--steps", "1", "--warmup", "1"]
+           "--gpus", "2", "--steps", "1", "--warmup", "1", "--max-sub", "2"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _json_lines(r.stdout)
