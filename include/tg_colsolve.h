@@ -618,8 +618,8 @@ int tg_set_column_residency(int kind, int precision, int mode);
  * fused column walk.  Same operations, same results. */
 int tg_set_assembly_mode(int mode);
 
-/* Block kinds, FP64: the L2 budget for the Gamma scratch of all resident
- * warps of the block kernels, in MB (default 96; <= 0 restores it).  It caps
+/* Block kinds, FP64: the budget for the Gamma scratch of all resident warps
+ * of the block kernels, in MB (default 160; <= 0 restores it).  It caps
  * how many columns are in flight at once on large batches (the refinement
  * kernel is not capped). */
 int tg_set_block_scratch_budget(double megabytes);

@@ -923,7 +923,7 @@ def set_host_pipeline(chunk_kb=0, streams=0):
 
 
 def set_block_scratch_budget(megabytes):
-    """L2 budget (MB) of the block kernels' Gamma scratch (<= 0: default 96)."""
+    """Budget (MB) of the block kernels' Gamma scratch (<= 0: default 160)."""
     return _check(lib().tg_set_block_scratch_budget(float(megabytes)), "tg_set_block_scratch_budget")
 
 

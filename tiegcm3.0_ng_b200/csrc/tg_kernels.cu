@@ -3285,9 +3285,13 @@ cudaError_t occupancy(K kernel, int threads, size_t smem, int *per_sm)
     return e;
 }
 
-// Resident threads per SM allowed for the block kernels: their Gamma scratch
-// (k2 * B*B doubles per resident thread) should stay well inside L2.
-double g_block_scratch_budget = 96.0 * 1024 * 1024;
+// Resident threads allowed for the block kernels: their Gamma scratch (k2 *
+// B*B doubles per resident thread) of all of them within this budget.  160 MB
+// lets more columns into flight than L2 holds, and that wins: 3x3 blocks on
+// the nested batch took 2.15 ms at 96 MB and 1.72 ms at 128 and 192 MB (2x2
+// blocks are occupancy-bound from 128 MB on: 2.19 -> 2.17 ms).
+constexpr double kBlockBudgetMB = 160.0;
+double g_block_scratch_budget = kBlockBudgetMB * 1024 * 1024;
 // Scalar ring kernels: L2 bytes of w2 scratch and parked w3 of all resident
 // columns.  Past the L2's capacity the back sweep's re-reads go to DRAM.
 constexpr double kScalarBudgetMB = 128.0;
@@ -3356,7 +3360,7 @@ void set_block_rows(int kind, int on)
     TileCfg &t = g_tile[kind_index(kind)][0];
     t.rows = on < 0 ? kDefaultTile[kind_index(kind)][0].rows : (on ? 1 : 0);
 }
-void set_block_scratch_budget(double mb) { g_block_scratch_budget = (mb > 0 ? mb : 96.0) * 1024 * 1024; }
+void set_block_scratch_budget(double mb) { g_block_scratch_budget = (mb > 0 ? mb : kBlockBudgetMB) * 1024 * 1024; }
 void set_scalar_scratch_budget(double mb)
 {
     g_scalar_scratch_budget = (mb > 0 ? mb : kScalarBudgetMB) * 1024 * 1024;
