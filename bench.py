@@ -468,6 +468,88 @@ def horizontal_setup(pkg, which, dev):
     return launch, nk * ncol, 40 * nk * ncol
 
 
+def dynamics_leg(pkg, wl, steps, warmup, stream, max_over_ranks, barrier, cpu=True):
+    """One dynamics_ng step of the column routines on each grid of the
+    workload (the global grid with the polar ring filter, each nest held as
+    one subdomain; 10 O+ sub-steps): device-resident, serial on one stream,
+    fanned out over five streams, and as one CUDA graph; the same step through
+    the host-pointer entries routine by routine, and the oracle's routines on
+    one host core.  The model's outer step takes nsub steps of each grid one
+    after the other (each nest step starts from the last), so its column
+    physics costs the sum over grids of nsub x the graph's time."""
+    import torch
+    dyn = pkg.dynamics
+    orc = ge.load_oracle() if cpu else None
+    out = {}
+    model_ms = 0.0
+    for gi, g in enumerate(wl.grids):
+        if (g.nlon + 4) * (g.nlat + 4) * g.nk > 4_000_000:
+            # ~200 level-major fields per step: host generation of the inputs would dominate the run
+            out[g.name] = {"grid": f"{g.name} {g.nlon}x{g.nlat}x{g.nk}", "skipped": "more than 4 M points per field"}
+            continue
+        ring = pkg.synth.RING_CHUNKS.get((g.nlon, g.nlat)) if gi == 0 else None
+        if gi == 0:
+            grid = dyn.Grid(g.nk, g.nlon, g.nlat, g.dz)
+        else:
+            # a regional nest: latitude rows 2.5 deg / 2**gi apart from 20 N
+            grid = dyn.Grid(g.nk, g.nlon, g.nlat, g.dz, lat0_deg=20.0, dlat_deg=2.5 / 2 ** gi,
+                            shapiro=0.03)
+        h = dyn.synthetic_inputs(grid, 17 + gi, nstep_sub=10)
+        rec = {"grid": f"{g.name} {g.nlon}x{g.nlat}x{g.nk}", "columns": grid.ncol, "levels": grid.nk,
+               "nsub_per_outer_step": g.nsub, "o_plus_sub_steps": 10, "ring_filter": ring is not None}
+
+        def timed(fn):
+            for _ in range(warmup):
+                fn()
+            stream.synchronize()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                fn()
+            e1.record(stream)
+            e1.synchronize()
+            return max_over_ranks(e0.elapsed_time(e1) / steps)
+
+        serial = dyn.DynamicsStep(grid, h, ring=ring, fan_out=False)
+        rec["ms_serial"] = timed(lambda: serial.issue(stream))
+        del serial
+        fan = dyn.DynamicsStep(grid, h, ring=ring, fan_out=True)
+        rec["ms_fan_out"] = timed(lambda: fan.issue(stream))
+        fan.capture(stream)
+        rec["ms_graph"] = timed(lambda: fan.replay(stream))
+        nbytes = fan.bytes_per_step()
+        pk, _ = measured_peak()
+        ach = nbytes / (rec["ms_graph"] * 1e-3) / 1e9
+        rec["algorithmic_bytes_per_step"] = nbytes
+        rec["roofline"] = {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk}
+        del fan
+        torch.cuda.synchronize()
+        # the same step through the host-pointer entries (wall clock, synchronous calls)
+        if gi <= 1:
+            host = dyn.HostEntries()
+            dyn.host_step(host, grid, h, ring)
+            n, t0 = 0, time.perf_counter()
+            while n < 2 or (n < 10 and time.perf_counter() - t0 < 2.0):
+                dyn.host_step(host, grid, h, ring)
+                n += 1
+            rec["ms_host_entries"] = (time.perf_counter() - t0) / n * 1e3
+            if orc is not None:
+                n, t0 = 0, time.perf_counter()
+                while n < 1 or (n < 5 and time.perf_counter() - t0 < 3.0):
+                    dyn.host_step(orc, grid, h, ring)
+                    n += 1
+                rec["ms_oracle_one_core"] = (time.perf_counter() - t0) / n * 1e3
+        model_ms += g.nsub * rec["ms_graph"]
+        out[g.name] = rec
+        torch.cuda.empty_cache()
+    if not any("skipped" in r for r in out.values()):
+        out["outer_step_column_physics_ms"] = model_ms
+    out["outer_step_note"] = ("sum over grids of nsub x the graph's time: the column routines of one global step with "
+                              "every nest sub-step in sequence")
+    return out
+
+
 def run_profile(args):
     """Executes one kind's plan --warmup + --steps times (for ncu captures)."""
     import torch
@@ -708,6 +790,12 @@ def main():
             del launch
         torch.cuda.empty_cache()
 
+    # ---- one dynamics_ng step of the column routines per grid, device-resident
+    dynamics = None
+    if not args.skip_assembly and wl.grids[0].nk >= 3 and len(wl.grids) > 1:
+        dynamics = dynamics_leg(pkg, wl, args.steps, args.warmup, stream, max_over_ranks, barrier,
+                                cpu=(rank == 0 and not args.skip_cpu))
+
     peak, peak_kind = measured_peak()
     bytes_scalar = pkg.batch.segment_bytes(scal_segs)          # this rank's share
     wl_tag = f"{wl.name}_B{wl.block}"
@@ -887,6 +975,7 @@ def main():
             "kernel_ms": {k: v for k, v in results.items()},
             "assembly": assembly,
             "horizontal": horizontal,
+            "dynamics": dynamics,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk,

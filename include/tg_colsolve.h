@@ -19,7 +19,13 @@
  *     Row arguments (k1, k2, lev0, lev1 ...) are 1-based, as in the reference.
  *   - Host-pointer entry points are synchronous, like the Fortran routines
  *     they replace.  Device-pointer entry points (suffix _dev) are
- *     stream-ordered and do not synchronise.
+ *     stream-ordered and do not synchronise.  Each caller stream has its own
+ *     device work buffers and status word, so _dev calls on different
+ *     streams may run at the same time (up to 16 streams at once; a 17th
+ *     stream drains the device and takes the least recently used stream's
+ *     buffers).  A stream's first call, and a call that needs larger buffers
+ *     than the stream had, allocate and synchronise: make those calls once
+ *     before capturing the calls into a CUDA graph.
  *   - Every entry point returns a tg_status.  The reference has no error
  *     return (a zero pivot silently yields Inf/NaN); the solves here produce
  *     the same numbers in that case and additionally report TG_EPIVOT.
@@ -319,6 +325,21 @@ int tg_comp_post_ng(const double *o2, const double *o1, const double *he, const 
                     const double *he_nm, const double *xnmbar, const double *zpmid, double dz, double dtsmooth,
                     double dtsmooth_div2, int nk, int ncol, double *o2_upd, double *o1_upd, double *he_upd,
                     double *o2nm_upd, double *o1nm_upd, double *henm_upd);
+/* Device form: level-major (k*ld + col) device arrays, zpmid a device array
+ * (nk), stream-ordered.  o2_upd/o1_upd/he_upd hold comp_ng's solution on
+ * entry (e.g. the three planes tg_comp_ng_dev wrote) and are updated in
+ * place; each nm_upd may be the same array as its species' *_nm or current
+ * field (every value is read before its own index is written).  With
+ * bnd_mask (ncol bytes, nonzero = a lateral-boundary column) the flagged
+ * columns of o2/o1/he_upd first take o2_bnd/o1_bnd/he_bnd (level-major, like
+ * the fields): the Dirichlet hook of src/comp_ng.F90:394-413.  bnd_mask and
+ * the three bnd arrays NULL: no overwrite. */
+int tg_comp_post_ng_dev(const double *o2, const double *o1, const double *he, const double *o2_nm,
+                        const double *o1_nm, const double *he_nm, const double *xnmbar, const double *zpmid,
+                        double dz, double dtsmooth, double dtsmooth_div2, int nk, int ncol, long ld,
+                        double *o2_upd, double *o1_upd, double *he_upd, double *o2nm_upd, double *o1nm_upd,
+                        double *henm_upd, const unsigned char *bnd_mask, const double *o2_bnd,
+                        const double *o1_bnd, const double *he_bnd, void *stream);
 
 /* The post-solve time filter and floor of the scalar routines, applied after
  * the caller has written its lateral-boundary columns:

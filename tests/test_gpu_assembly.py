@@ -167,6 +167,40 @@ def test_comp_post_ng_host(cuda, pkg, orc, nk, dz, ncol):
         assert _rel(got, want) <= 1e-15   # measured: at most 2.6e-16
 
 
+@pytest.mark.parametrize("alias,boundary", [(False, False), (True, False), (False, True)])
+def test_comp_post_ng_device(cuda, pkg, orc, alias, boundary):
+    """The device form on level-major planes gives the host form's bits; with
+    alias, each nm_upd is its species' *_nm array (the model's in-place use);
+    with boundary, the flagged columns first take the boundary values, as the
+    caller's overwrite before the host form does."""
+    torch = cuda
+    nk, ncol, dz = 57, 1111, 0.25
+    F, C = pkg.synth.comp_post_inputs(nk, ncol, dz, 9)
+    ld = pkg.batch.pad_ld(ncol)
+    dev = {k: pkg.batch.level_scalar(F[k], ld, "cuda") for k in pkg.colsolve.POST_INPUTS}
+    upd = [pkg.batch.level_scalar(F[k], ld, "cuda") for k in ("o2_upd", "o1_upd", "he_upd")]
+    nm = ([dev["o2_nm"], dev["o1_nm"], dev["he_nm"]] if alias else
+          [torch.zeros((nk, ld), dtype=torch.float64, device="cuda") for _ in range(3)])
+    zp = torch.from_numpy(np.ascontiguousarray(F["zpmid"], dtype=np.float64)).cuda()
+    hu = [F[k].copy(order="F") for k in ("o2_upd", "o1_upd", "he_upd")]
+    kw = {}
+    if boundary:
+        mask = np.zeros(ncol, dtype=np.uint8)
+        mask[::9] = 1
+        mask[:40] = 1
+        bnd = [F[k].copy(order="F")[:, ::-1].copy(order="F") for k in ("o2", "o1", "he")]
+        for h, b in zip(hu, bnd):
+            h[:, mask.astype(bool)] = b[:, mask.astype(bool)]
+        kw = dict(bnd_mask=torch.from_numpy(np.pad(mask, (0, ld - ncol))).cuda(),
+                  bnd=[pkg.batch.level_scalar(b, ld, "cuda") for b in bnd])
+    pkg.comp_post_ng_dev(dev, zp, C, upd, nm, nk, ncol, ld, **kw)
+    torch.cuda.synchronize()
+    hn = [np.zeros((nk, ncol), order="F") for _ in range(3)]
+    assert pkg.comp_post_ng(F, C, hu, hn) == pkg.TG_OK
+    for got, want in zip(upd + nm, hu + hn):
+        assert np.array_equal(pkg.batch.from_level_scalar(got, ncol), want)
+
+
 # settei_ng: device exp/log/pow/sin/cos differ from the C library's in the
 # last bits; Te, Ti and qtotal agree with the oracle to this relative level
 # (measured on B200: at most 4.6e-15).

@@ -39,7 +39,7 @@ LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
 EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor_ng_dev", "tg_comp_ng",
-           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_advec_ng", "tg_advec_ng_dev", "tg_smooth_ng", "tg_smooth_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
+           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_comp_post_ng_dev", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_advec_ng", "tg_advec_ng_dev", "tg_smooth_ng", "tg_smooth_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_column_residency", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
@@ -211,6 +211,7 @@ def lib():
                                  P],
             "tg_comp_ng_dev": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, I, I, Lg, P, P, P],
             "tg_comp_post_ng": [P] * 8 + [D, D, D, I, I] + [P] * 6,
+            "tg_comp_post_ng_dev": [P] * 8 + [D, D, D, I, I, Lg] + [P] * 11,
             "tg_time_filter_ng": [I, P, P, D, D, I, I, P, P],
             "tg_time_filter_ng_dev": [I, P, P, D, D, I, I, Lg, P, P, P],
             "tg_advec_ng": [P, P, P, P, D, D, D, I, I, I, P],
@@ -699,6 +700,25 @@ def comp_post_ng(fields, consts, upd, nm_out):
                                float(consts["dtsmooth_div2"]), nk, ncol,
                                *[_out(u, "upd") for u in upd], *[_out(u, "nm_out") for u in nm_out])
     return _check(rc, "tg_comp_post_ng")
+
+
+def comp_post_ng_dev(fields, zpmid, consts, upd, nm_out, nk, ncol, ld, bnd_mask=None, bnd=None, stream=None):
+    """Device form of comp_post_ng on level-major (nk, ld) fields: fields holds
+    POST_INPUTS as CUDA tensors, zpmid (nk) on the device, upd = [o2, o1, he]
+    (comp_ng's solution, updated in place), nm_out = [o2nm, o1nm, henm].
+    bnd_mask (uint8 per column) and bnd = [o2, o1, he] boundary values: the
+    lateral-boundary overwrite before the post steps."""
+    ins = [_dptr(fields[n]) for n in POST_INPUTS]
+    if (bnd_mask is None) != (bnd is None):
+        raise ValueError("comp_post_ng_dev: give bnd_mask and bnd together")
+    if bnd_mask is not None and (not bnd_mask.is_cuda or str(bnd_mask.dtype) != "torch.uint8"):
+        raise TypeError("bnd_mask must be a uint8 CUDA tensor")
+    bp = [None] * 3 if bnd is None else [_dptr(b) for b in bnd]
+    rc = lib().tg_comp_post_ng_dev(*ins, _dptr(zpmid), float(consts["dz"]), float(consts["dtsmooth"]),
+                                   float(consts["dtsmooth_div2"]), nk, ncol, ld, *[_dptr(u) for u in upd],
+                                   *[_dptr(u) for u in nm_out], None if bnd_mask is None else bnd_mask.data_ptr(),
+                                   *bp, _stream(stream))
+    return _check(rc, "tg_comp_post_ng_dev", numeric_ok=False)
 
 
 def time_filter_ng(which, cur, prev, dtsmooth, dtsmooth_div2, upd, nm_out):

@@ -57,6 +57,21 @@ struct Buf {
 constexpr int kSlots = 8;
 std::atomic<int> g_host_slots{3};
 std::atomic<long> g_host_chunk_bytes{0};   // 0: chosen per call
+// Device workspace of the stream-ordered (_dev) entries, one per caller
+// stream: entries issued on different streams may run at the same time, so
+// each stream's work gets its own scratch, relayout buffers, status word and
+// sweep histogram.  Work on one stream is ordered, so it can share them.
+struct StreamWs {
+    cudaStream_t key = nullptr;
+    bool used = false;
+    unsigned long long tick = 0;   // last use, for eviction
+    Buf lvl[7];                    // level-major relayout of column-layout solves
+    Buf scratch;                   // kernel scratch (Gamma, planes, w2)
+    unsigned *flags = nullptr;     // device status word
+    unsigned long long *hist = nullptr;   // device, kMaxSweepBins
+};
+constexpr int kStreamWs = 16;
+
 struct DevCtx {
     int dev = -1;
     std::mutex mu;
@@ -67,6 +82,8 @@ struct DevCtx {
     unsigned *flags = nullptr;           // device, one word per slot
     unsigned *flags_host = nullptr;      // pinned, one word per slot
     unsigned long long *hist = nullptr;  // device, kMaxSweepBins
+    StreamWs ws[kStreamWs];              // per caller stream, see StreamWs
+    unsigned long long ws_tick = 0;
 };
 
 constexpr int kMaxDev = 64;
@@ -127,6 +144,46 @@ int grow(Buf &b, size_t bytes)
     return TG_OK;
 }
 
+// The workspace of caller stream st (the caller holds c->mu).  A stream
+// seen for the first time takes a free entry; with all kStreamWs taken, the
+// least recently used one is drained (device synchronised) and reassigned.
+int stream_ws(DevCtx *c, cudaStream_t st, StreamWs **out)
+{
+    StreamWs *hit = nullptr, *free_ws = nullptr, *lru = nullptr;
+    for (StreamWs &w : c->ws) {
+        if (w.used && w.key == st) {
+            hit = &w;
+            break;
+        }
+        if (!w.used && !free_ws) free_ws = &w;
+        if (w.used && (!lru || w.tick < lru->tick)) lru = &w;
+    }
+    if (!hit) {
+        hit = free_ws;
+        if (!hit) {
+            // another stream's queued work may still use these buffers
+            TG_CUDA(cudaDeviceSynchronize());
+            hit = lru;
+            for (Buf &b : hit->lvl)
+                if (b.p) {
+                    TG_CUDA(cudaFree(b.p));
+                    b = Buf{};
+                }
+            if (hit->scratch.p) {
+                TG_CUDA(cudaFree(hit->scratch.p));
+                hit->scratch = Buf{};
+            }
+        }
+        if (!hit->flags) TG_CUDA(cudaMalloc(&hit->flags, sizeof(unsigned)));
+        if (!hit->hist) TG_CUDA(cudaMalloc(&hit->hist, kMaxSweepBins * sizeof(unsigned long long)));
+        hit->key = st;
+        hit->used = true;
+    }
+    hit->tick = ++c->ws_tick;
+    *out = hit;
+    return TG_OK;
+}
+
 int flags_to_status(unsigned f)
 {
     if (f & FLAG_TIMEOUT) return TG_ETIMEOUT;
@@ -161,7 +218,8 @@ bool cpt2_ok_seg(const Seg &s)
     return s.ld % 2 == 0 && aligned16(s.a) && aligned16(s.b) && aligned16(s.c) && aligned16(s.f) && aligned16(s.x);
 }
 
-int solve_level(DevCtx *c, int slot, int kind, int precision, Seg seg, unsigned *flags, cudaStream_t st)
+int solve_level(Buf &scratch, unsigned long long *hist, int kind, int precision, Seg seg, unsigned *flags,
+                cudaStream_t st)
 {
     const int B = kind == TG_KIND_SCALAR ? 1 : kind;
     int cpb = 0, cpt = 1, stages = 0, w2g = 0;
@@ -189,17 +247,16 @@ int solve_level(DevCtx *c, int slot, int kind, int precision, Seg seg, unsigned 
         const bool ring_refine = precision != TG_PREC_F64 && sh.stages > 0;
         if (sh.w2g || ring_refine) {
             const long slots = (long)sh.blocks * sh.threads;
-            int rc = grow(c->scratch[slot], ring_refine ? refine_scratch_bytes(slots, seg.k2)
-                                                        : scalar_scratch_bytes(slots, seg.k2));
+            int rc = grow(scratch, ring_refine ? refine_scratch_bytes(slots, seg.k2) : scalar_scratch_bytes(slots, seg.k2));
             if (rc) return rc;
-            scr = (double *)c->scratch[slot].p;
+            scr = (double *)scratch.p;
         }
-        TG_CUDA(launch_scalar(tab, precision, sh, g_refine, scr, flags, c->hist, st));
+        TG_CUDA(launch_scalar(tab, precision, sh, g_refine, scr, flags, hist, st));
     } else {
         const size_t need = block_scratch_bytes(B, precision, (long)sh.blocks * sh.threads, seg.k2);
-        int rc = grow(c->scratch[slot], need);
+        int rc = grow(scratch, need);
         if (rc) return rc;
-        TG_CUDA(launch_block(tab, B, precision, sh, g_refine, (double *)c->scratch[slot].p, flags, c->hist, st));
+        TG_CUDA(launch_block(tab, B, precision, sh, g_refine, (double *)scratch.p, flags, hist, st));
     }
     return TG_OK;
 }
@@ -365,7 +422,7 @@ int host_solve_many(const HostSys *sys, int nsys, int precision)
             seg.k2 = h.k2;
             seg.ncol = (int)nc;
             seg.kind = h.kind;
-            if ((rc = solve_level(c, s, h.kind, precision, seg, c->flags + s, st))) return rc;
+            if ((rc = solve_level(c->scratch[s], c->hist, h.kind, precision, seg, c->flags + s, st))) return rc;
             double *ob = (double *)c->colbuf[s][4].p;
             TG_CUDA(launch_level_to_col(lv[4], ld, ob, p.orows, p.orows, nc, st));
             if (p.orows == h.colstride)
@@ -738,10 +795,12 @@ static int dev_solve(int kind, const double *a, const double *b, const double *c
     int rc = get_ctx(&cx);
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
-    unsigned *flags = cx->flags;
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    unsigned *flags = ws->flags;
     TG_CUDA(cudaMemsetAsync(flags, 0, sizeof(unsigned), st));
     if (precision != TG_PREC_F64)
-        TG_CUDA(cudaMemsetAsync(cx->hist, 0, kMaxSweepBins * sizeof(unsigned long long), st));
+        TG_CUDA(cudaMemsetAsync(ws->hist, 0, kMaxSweepBins * sizeof(unsigned long long), st));
     if (ncol > 0) {
         Seg seg{};
         seg.nk = nk;
@@ -754,20 +813,20 @@ static int dev_solve(int kind, const double *a, const double *b, const double *c
             seg.ubc_ratio = ubc_ratio;
             seg.ubc_add = ubc_ratio ? ubc_add : nullptr;
             seg.ld = ld;
-            if ((rc = solve_level(cx, 0, kind, precision, seg, flags, st))) return rc;
+            if ((rc = solve_level(ws->scratch, ws->hist, kind, precision, seg, flags, st))) return rc;
         } else {
             const long mrows = (long)B * B * k2, vrows = (long)B * k2;
             const long lld = round_up(ncol, 32);
             for (int i = 0; i < 3; ++i)
-                if ((rc = grow(cx->lvlbuf[0][i], sizeof(double) * mrows * lld))) return rc;
-            if ((rc = grow(cx->lvlbuf[0][3], sizeof(double) * vrows * lld))) return rc;
-            if ((rc = grow(cx->lvlbuf[0][4], sizeof(double) * orows * lld))) return rc;
+                if ((rc = grow(ws->lvl[i], sizeof(double) * mrows * lld))) return rc;
+            if ((rc = grow(ws->lvl[3], sizeof(double) * vrows * lld))) return rc;
+            if ((rc = grow(ws->lvl[4], sizeof(double) * orows * lld))) return rc;
             if (ubc_ratio) {
-                if ((rc = grow(cx->lvlbuf[0][5], sizeof(double) * B * lld))) return rc;
-                if ((rc = grow(cx->lvlbuf[0][6], sizeof(double) * B * lld))) return rc;
+                if ((rc = grow(ws->lvl[5], sizeof(double) * B * lld))) return rc;
+                if ((rc = grow(ws->lvl[6], sizeof(double) * B * lld))) return rc;
             }
             double *lv[7];
-            for (int i = 0; i < 7; ++i) lv[i] = (double *)cx->lvlbuf[0][i].p;
+            for (int i = 0; i < 7; ++i) lv[i] = (double *)ws->lvl[i].p;
             const double *src[3] = {a, b, c};
             for (int i = 0; i < 3; ++i) TG_CUDA(launch_col_to_level(src[i], (long)B * B * nk, lv[i], lld, mrows, ncol, st));
             TG_CUDA(launch_col_to_level(f, (long)B * nk, lv[3], lld, vrows, ncol, st));
@@ -780,7 +839,7 @@ static int dev_solve(int kind, const double *a, const double *b, const double *c
             seg.ubc_add = (ubc_ratio && ubc_add) ? lv[6] : nullptr;
             seg.ld = lld;
             seg.nk = k2 + (ubc_ratio ? 1 : 0);
-            if ((rc = solve_level(cx, 0, kind, precision, seg, flags, st))) return rc;
+            if ((rc = solve_level(ws->scratch, ws->hist, kind, precision, seg, flags, st))) return rc;
             TG_CUDA(launch_level_to_col(lv[4], lld, x, (long)B * nk, orows, ncol, st));
         }
     }
@@ -813,10 +872,12 @@ __attribute__((visibility("default"))) int tg_dt_ng_dev(const tg_dt_fields *F, c
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
-    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_dt_ng(*F, *C, tn_upd, nk, ncol, ld, system_out, cx->flags, st));
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_dt_ng(*F, *C, tn_upd, nk, ncol, ld, system_out, ws->flags, st));
     if (status_dev) {
-        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
         TG_CUDA(cudaGetLastError());
     }
     return TG_OK;
@@ -898,11 +959,13 @@ __attribute__((visibility("default"))) int tg_minor_ng_dev(const tg_minor_fields
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
-    if ((rc = grow(cx->scratch[0], sizeof(double) * 3 * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
-    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_minor_ng(*F, *C, out, nk, ncol, ld, system_out, cx->flags, st, (double *)cx->scratch[0].p));
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    if ((rc = grow(ws->scratch, sizeof(double) * 3 * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_minor_ng(*F, *C, out, nk, ncol, ld, system_out, ws->flags, st, (double *)ws->scratch.p));
     if (status_dev) {
-        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
         TG_CUDA(cudaGetLastError());
     }
     return TG_OK;
@@ -1141,11 +1204,13 @@ __attribute__((visibility("default"))) int tg_dt_ng_post_dev(const tg_dt_fields 
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
     const PostStep post = post_of(P, 100.0, 0);
-    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_dt_ng(*F, *C, tn_upd, nk, ncol, ld, nullptr, cx->flags, st, &post));
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_dt_ng(*F, *C, tn_upd, nk, ncol, ld, nullptr, ws->flags, st, &post));
     if (status_dev) {
-        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
         TG_CUDA(cudaGetLastError());
     }
     return TG_OK;
@@ -1164,13 +1229,15 @@ __attribute__((visibility("default"))) int tg_minor_ng_post_dev(const tg_minor_f
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
-    if ((rc = grow(cx->scratch[0], sizeof(double) * 3 * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    if ((rc = grow(ws->scratch, sizeof(double) * 3 * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
     const PostStep post = post_of(P, 1.e-12, 1);
-    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_minor_ng(*F, *C, fcomp_out, nk, ncol, ld, nullptr, cx->flags, st, (double *)cx->scratch[0].p,
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_minor_ng(*F, *C, fcomp_out, nk, ncol, ld, nullptr, ws->flags, st, (double *)ws->scratch.p,
                             &post));
     if (status_dev) {
-        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
         TG_CUDA(cudaGetLastError());
     }
     return TG_OK;
@@ -1199,11 +1266,13 @@ __attribute__((visibility("default"))) int tg_comp_ng_dev(const tg_comp_fields *
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
-    if ((rc = grow(cx->scratch[0], sizeof(double) * comp_scratch_doubles(nk, ld > 0 ? ld : 1)))) return rc;
-    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_comp_ng(*F, *C, out, (double *)cx->scratch[0].p, nk, ncol, ld, system_out, cx->flags, st));
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    if ((rc = grow(ws->scratch, sizeof(double) * comp_scratch_doubles(nk, ld > 0 ? ld : 1)))) return rc;
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_comp_ng(*F, *C, out, (double *)ws->scratch.p, nk, ncol, ld, system_out, ws->flags, st));
     if (status_dev) {
-        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
         TG_CUDA(cudaGetLastError());
     }
     return TG_OK;
@@ -1316,6 +1385,33 @@ __attribute__((visibility("default"))) int tg_comp_post_ng(const double *o2, con
         TG_CUDA(cudaMemcpyAsync(io6[i], stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
         TG_CUDA(cudaStreamSynchronize(st));
     }
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_comp_post_ng_dev(const double *o2, const double *o1, const double *he,
+                                                               const double *o2_nm, const double *o1_nm,
+                                                               const double *he_nm, const double *xnmbar,
+                                                               const double *zpmid, double dz, double dtsmooth,
+                                                               double dtsmooth_div2, int nk, int ncol, long ld,
+                                                               double *o2_upd, double *o1_upd, double *he_upd,
+                                                               double *o2nm_upd, double *o1nm_upd, double *henm_upd,
+                                                               const unsigned char *bnd_mask, const double *o2_bnd,
+                                                               const double *o1_bnd, const double *he_bnd,
+                                                               void *stream)
+{
+    const double *in7[7] = {o2, o1, he, o2_nm, o1_nm, he_nm, xnmbar};
+    double *io6[6] = {o2_upd, o1_upd, he_upd, o2nm_upd, o1nm_upd, henm_upd};
+    const double *bnd3[3] = {o2_bnd, o1_bnd, he_bnd};
+    bool ok = zpmid && nk >= 1 && nk <= 65535 && ncol >= 0 && ld >= ncol &&
+              (!bnd_mask || (o2_bnd && o1_bnd && he_bnd));
+    for (const double *p : in7) ok = ok && p;
+    for (double *p : io6) ok = ok && p;
+    if (!ok) {
+        set_err("tg_comp_post_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    TG_CUDA(launch_comp_post_ng(in7, zpmid, dz, dtsmooth, dtsmooth_div2, nk, ncol, ld, io6, (cudaStream_t)stream,
+                                bnd_mask, bnd3));
     return TG_OK;
 }
 
@@ -1569,12 +1665,14 @@ __attribute__((visibility("default"))) int tg_settei_ng_dev(const tg_settei_fiel
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
-    if ((rc = grow(cx->scratch[0], sizeof(double) * settei_scratch_doubles(nk, ld > 0 ? ld : 1)))) return rc;
-    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_settei_ng(*F, *C, te_out, ti_out, qtotal, nk, ncol, ld, system_out, cx->flags, st,
-                             (double *)cx->scratch[0].p));
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    if ((rc = grow(ws->scratch, sizeof(double) * settei_scratch_doubles(nk, ld > 0 ? ld : 1)))) return rc;
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_settei_ng(*F, *C, te_out, ti_out, qtotal, nk, ncol, ld, system_out, ws->flags, st,
+                             (double *)ws->scratch.p));
     if (status_dev) {
-        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
         TG_CUDA(cudaGetLastError());
     }
     return TG_OK;
@@ -1653,13 +1751,15 @@ __attribute__((visibility("default"))) int tg_oplus_ng_dev(const tg_oplus_fields
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
     const size_t sbytes = sizeof(double) * oplus_scratch_planes() * (size_t)nk * (size_t)(ld > 0 ? ld : 1);
-    if ((rc = grow(cx->scratch[0], sbytes))) return rc;
-    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_oplus_ng(*F, *C, opout, xiop2p, xiop2d, Fe, Fn, (double *)cx->scratch[0].p, nk, ncol, ld,
-                            system_out, cx->flags, st));
+    if ((rc = grow(ws->scratch, sbytes))) return rc;
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_oplus_ng(*F, *C, opout, xiop2p, xiop2d, Fe, Fn, (double *)ws->scratch.p, nk, ncol, ld,
+                            system_out, ws->flags, st));
     if (status_dev) {
-        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
         TG_CUDA(cudaGetLastError());
     }
     return TG_OK;
@@ -1680,14 +1780,16 @@ __attribute__((visibility("default"))) int tg_oplus_ng_post_dev(const tg_oplus_f
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
     const size_t sbytes = sizeof(double) * oplus_scratch_planes() * (size_t)nk * (size_t)(ld > 0 ? ld : 1);
-    if ((rc = grow(cx->scratch[0], sbytes))) return rc;
+    if ((rc = grow(ws->scratch, sbytes))) return rc;
     const PostStep post = post_of(P, 0.0, 1);
-    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_oplus_ng(*F, *C, opout, xiop2p, xiop2d, Fe, Fn, (double *)cx->scratch[0].p, nk, ncol, ld, nullptr,
-                            cx->flags, st, &post));
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_oplus_ng(*F, *C, opout, xiop2p, xiop2d, Fe, Fn, (double *)ws->scratch.p, nk, ncol, ld, nullptr,
+                            ws->flags, st, &post));
     if (status_dev) {
-        k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+        k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
         TG_CUDA(cudaGetLastError());
     }
     return TG_OK;
@@ -2071,9 +2173,11 @@ __attribute__((visibility("default"))) int tg_selftest_wait(unsigned polls, int 
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(cx->mu);
     cudaStream_t st = (cudaStream_t)stream;
-    TG_CUDA(cudaMemsetAsync(cx->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_selftest_wait(polls, cx->flags, st));
-    k_finish_status<<<1, 1, 0, st>>>(cx->flags, status_dev);
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_selftest_wait(polls, ws->flags, st));
+    k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
     TG_CUDA(cudaGetLastError());
     return TG_OK;
 }
@@ -2246,6 +2350,13 @@ __attribute__((visibility("default"))) int tg_release_buffers(void)
                 if (b.p) cudaFree(b.p);
             if (c->scratch[s].p) cudaFree(c->scratch[s].p);
             if (c->st[s]) cudaStreamDestroy(c->st[s]);
+        }
+        for (StreamWs &w : c->ws) {
+            for (auto &b : w.lvl)
+                if (b.p) cudaFree(b.p);
+            if (w.scratch.p) cudaFree(w.scratch.p);
+            if (w.flags) cudaFree(w.flags);
+            if (w.hist) cudaFree(w.hist);
         }
         if (c->flags) cudaFree(c->flags);
         if (c->flags_host) cudaFreeHost(c->flags_host);

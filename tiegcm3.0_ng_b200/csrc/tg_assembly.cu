@@ -1372,8 +1372,10 @@ cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out
 size_t comp_scratch_doubles(int nk, long ld) { return (size_t)(12 + kCompPlanes) * nk * ld + 4 * (size_t)ld; }
 }  // namespace tg
 
-// comp_ng post-solve steps (src/comp_ng.F90:415-457), one thread per column.
-// The N2 extrapolation uses the device log/exp, so it agrees with the CPU
+// comp_ng post-solve steps (src/comp_ng.F90:394-457), one thread per column:
+// the lateral-boundary overwrite of the columns flagged in bmask (when given),
+// the time filter, the N2 extrapolation, floors and normalisation.  The N2
+// extrapolation uses the device log/exp, so it agrees with the CPU
 // restatement to a tolerance in the extrapolated levels.
 namespace tg {
 __global__ void __launch_bounds__(128) k_comp_post_ng(const double *o2, const double *o1, const double *he,
@@ -1381,11 +1383,20 @@ __global__ void __launch_bounds__(128) k_comp_post_ng(const double *o2, const do
                                                       const double *xnmbar, const double *zpmid, double dz,
                                                       double ds, double ds2, int nk, int ncol, long ld, double *o2u,
                                                       double *o1u, double *heu, double *o2n, double *o1n,
-                                                      double *hen)
+                                                      double *hen, const unsigned char *bmask, const double *b2,
+                                                      const double *b1, const double *bh)
 {
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
     const double small = 1.e-9;
+    // the Dirichlet lateral-boundary hook (comp_ng.F90:394-413)
+    if (bmask && bmask[col])
+        for (int k = 0; k < nk; ++k) {
+            const long o = (long)k * ld + col;
+            o2u[o] = b2[o];
+            o1u[o] = b1[o];
+            heu[o] = bh[o];
+        }
     // first level with N2 < 0.01 (comp_ng.F90:425-429)
     int ktop = nk;
     for (int k = 0; k < nk; ++k) {
@@ -1431,13 +1442,16 @@ __global__ void __launch_bounds__(128) k_comp_post_ng(const double *o2, const do
 }
 
 cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, double dz, double dtsmooth,
-                                double dtsmooth_div2, int nk, int ncol, long ld, double *const *upd6, cudaStream_t st)
+                                double dtsmooth_div2, int nk, int ncol, long ld, double *const *upd6, cudaStream_t st,
+                                const unsigned char *bnd_mask, const double *const *bnd3)
 {
     if (ncol <= 0) return cudaSuccess;
     const int T = 128;
     k_comp_post_ng<<<(ncol + T - 1) / T, T, 0, st>>>(in7[0], in7[1], in7[2], in7[3], in7[4], in7[5], in7[6], zpmid,
                                                      dz, dtsmooth, dtsmooth_div2, nk, ncol, ld, upd6[0], upd6[1],
-                                                     upd6[2], upd6[3], upd6[4], upd6[5]);
+                                                     upd6[2], upd6[3], upd6[4], upd6[5], bnd_mask,
+                                                     bnd_mask ? bnd3[0] : nullptr, bnd_mask ? bnd3[1] : nullptr,
+                                                     bnd_mask ? bnd3[2] : nullptr);
     return cudaGetLastError();
 }
 

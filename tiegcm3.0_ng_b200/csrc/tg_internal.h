@@ -201,9 +201,12 @@ typedef tg_comp_consts CompConsts;
 cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out, double *scratch, int nk, int ncol,
                            long ld, double *sys_out, unsigned *status, cudaStream_t st);
 size_t comp_scratch_doubles(int nk, long ld);
+// bnd_mask (per column, nonzero = lateral boundary) and bnd3 (o2, o1, he
+// boundary values) are optional: the overwrite the caller otherwise makes.
 cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, double dz, double dtsmooth,
                                 double dtsmooth_div2, int nk, int ncol, long ld, double *const *upd6,
-                                cudaStream_t st);
+                                cudaStream_t st, const unsigned char *bnd_mask = nullptr,
+                                const double *const *bnd3 = nullptr);
 // advec_ng / smooth_ng on one nest held as a single subdomain (tg_horiz.cu):
 // level-major planes (k, i, j) at k*ld + i + (nlon+4)*j
 cudaError_t launch_advec_ng(const double *f, const double *un, const double *vn, const double *racs, double dlamda,

@@ -249,6 +249,19 @@ module tg_colsolve_mod
       real(c_double), intent(inout) :: o2_upd(*), o1_upd(*), he_upd(*), o2nm_upd(*), o1nm_upd(*), henm_upd(*)
     end function tg_comp_post_ng
 
+    ! device form: level-major device arrays (stride ld), zpmid on the device
+    integer(c_int) function tg_comp_post_ng_dev(o2, o1, he, o2_nm, o1_nm, he_nm, xnmbar, zpmid, dz, dtsmooth, &
+        dtsmooth_div2, nk, ncol, ld, o2_upd, o1_upd, he_upd, o2nm_upd, o1nm_upd, henm_upd, bnd_mask, o2_bnd, &
+        o1_bnd, he_bnd, stream) bind(C, name="tg_comp_post_ng_dev")
+      import :: c_int, c_long, c_double, c_ptr
+      type(c_ptr), value :: o2, o1, he, o2_nm, o1_nm, he_nm, xnmbar, zpmid
+      real(c_double), value :: dz, dtsmooth, dtsmooth_div2
+      integer(c_int), value :: nk, ncol
+      integer(c_long), value :: ld
+      type(c_ptr), value :: o2_upd, o1_upd, he_upd, o2nm_upd, o1nm_upd, henm_upd
+      type(c_ptr), value :: bnd_mask, o2_bnd, o1_bnd, he_bnd, stream
+    end function tg_comp_post_ng_dev
+
     ! which = TG_FILTER_DT / _MINOR / _OPLUS: the time filter and floor after
     ! the lateral-boundary hook (dt_ng.F90:208-213, minor_ng.F90:234-237,
     ! oplus_ng.F90:337-340); upd floored in place, nm_upd the filtered field
