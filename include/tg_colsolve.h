@@ -634,10 +634,20 @@ int tg_set_stage_levels(int kind, int precision, int levels);
  * Same arithmetic, same bits. */
 int tg_set_column_residency(int kind, int precision, int mode);
 
-/* Fused assembly routines: 1 (default) two passes where built, the level
- * quantities with one thread per (level, column) then the column walk; 0 one
- * fused column walk.  Same operations, same results. */
+/* Fused assembly routines: 2 (default) three passes where built (dt_ng on
+ * launches of up to 16384 columns, minor_ng, oplus_ng): the level quantities
+ * and then the tridiagonal rows with one thread per (level, column), then a
+ * column walk that is the recurrence alone; 1 two passes, the level
+ * quantities then a walk that forms the rows as it goes (comp_ng, settei_ng
+ * and dt_ng above 16384 columns in mode 2 too); 0 one fused column walk.
+ * Same operations, same results. */
 int tg_set_assembly_mode(int mode);
+
+/* Fused assembly routines: how many levels ahead their column walks request
+ * the reads of a level (n >= 1), or -1 (default) for automatic: 8 levels for
+ * launches of up to 16384 columns, where few warps per SM leave every level
+ * waiting on memory otherwise, 1 above.  Same results. */
+int tg_set_walk_prefetch(int levels);
 
 /* Block kinds, FP64: the budget for the Gamma scratch of all resident warps
  * of the block kernels, in MB (default 160; <= 0 restores it).  It caps

@@ -5,15 +5,22 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=[1, 0, 2], ids=["two_pass", "fused", "three_pass"])
+def assembly_mode(request, pkg):
+    pkg.set_assembly_mode(request.param)
+    yield request.param
+    pkg.set_assembly_mode(-1)
+
+
 @pytest.mark.parametrize("nk,dz,ncol", [(57, 0.25, 3001), (29, 0.5, 2592), (113, 0.125, 500), (3, 0.5, 33)])
-def test_dt_ng_host_bit_exact(cuda, pkg, orc, nk, dz, ncol):
+def test_dt_ng_host_bit_exact(cuda, pkg, orc, nk, dz, ncol, assembly_mode):
     F, C = pkg.synth.dt_inputs(nk, ncol, dz, 7 + nk)
     tn_upd = np.zeros((nk, ncol), order="F")
     assert pkg.dt_ng(F, C, tn_upd) == pkg.TG_OK
     assert np.array_equal(tn_upd, orc.dt_ng(F, C))
 
 
-def test_dt_ng_device_system_and_solution(cuda, pkg, orc):
+def test_dt_ng_device_system_and_solution(cuda, pkg, orc, assembly_mode):
     torch = cuda
     nk, ncol, dz = 57, 1000, 0.25
     F, C = pkg.synth.dt_inputs(nk, ncol, dz, 3)
@@ -50,13 +57,6 @@ def _rel(got, want):
 # now and then, so the fused kernel agrees with the oracle to a tolerance
 # (measured on B200: at most 3.3e-14 over these cases).
 MINOR_TOL = 3e-13
-
-
-@pytest.fixture(params=[1, 0], ids=["two_pass", "fused"])
-def assembly_mode(request, pkg):
-    pkg.set_assembly_mode(request.param)
-    yield request.param
-    pkg.set_assembly_mode(-1)
 
 
 @pytest.mark.parametrize("nk,dz,ncol", [(57, 0.25, 3001), (29, 0.5, 2592), (113, 0.125, 500), (3, 0.5, 33),

@@ -118,3 +118,77 @@ def test_oplus_post_fused_without_mask(cuda, pkg):
     assert torch.equal(y[0][:, :ncol], x[:, :ncol])
     assert torch.equal(nm[:, :ncol], nm_want[:, :ncol])
     assert torch.equal(y[1][:, :ncol], outs[1][:, :ncol])
+
+
+@pytest.mark.parametrize("ncol", [1500, 17000], ids=["walk_prefetch_8", "walk_prefetch_1"])
+def test_three_pass_gives_the_two_pass_bits(cuda, pkg, ncol):
+    """Assembly mode 2 (rows formed one thread per level and column, then the
+    recurrence alone) gives the bits of mode 1, with and without the fused
+    post-solve steps, for dt_ng, minor_ng and oplus_ng."""
+    torch = cuda
+    nk, dz = 57, 0.25
+    cases = []
+    F, C = pkg.synth.dt_inputs(nk, ncol, dz, 21)
+    dev, ld = _level(pkg, torch, F, nk, ncol, ("expz", "dift"))
+    cases.append(("dt", dev, C, dev["tn"], pkg.dt_ng_dev, pkg.dt_ng_post_dev, 50.0, 1500.0))
+    F, C = pkg.synth.minor_inputs(nk, ncol, dz, 22)
+    dev, ld = _level(pkg, torch, F, nk, ncol, ("expz", "difk"))
+    cur = pkg.batch.level_scalar(np.asfortranarray(np.abs(F["ftm1_smooth"])), ld, "cuda")
+    cases.append(("minor", dev, C, cur, pkg.minor_ng_dev, pkg.minor_ng_post_dev, -1e-9, 1e-5))
+    F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 23)
+    dev, ld = _level(pkg, torch, F, nk, ncol, ("zpint",))
+    cases.append(("oplus", dev, C, dev["op"], None, None, 0.0, 1e6))
+    z = lambda: torch.zeros((nk, ld), dtype=torch.float64, device="cuda")  # noqa: E731
+    for name, dev, C, cur, plain, fused, lo, hi in cases:
+        prev, bnd, mask, _ = _post_inputs(torch, cur, nk, ncol, ld, 9, lo, hi, False)
+        got = {}
+        for mode in (1, 2):
+            pkg.set_assembly_mode(mode)
+            try:
+                st = torch.zeros(1, dtype=torch.int32, device="cuda")
+                nm = torch.full((nk, ld), -3.0, dtype=torch.float64, device="cuda")
+                post = dict(cur=cur, prev=prev, nm_upd=nm, bnd_mask=mask, bnd=bnd, dtsmooth=0.9, dtsmooth_div2=0.05)
+                if name == "oplus":
+                    a, b = [z() for _ in range(3)], [z() for _ in range(3)]
+                    pkg.oplus_ng_dev(dev, C, a[0], a[1], a[2], nk, ncol, ld, status=st)
+                    pkg.oplus_ng_post_dev(dev, C, b[0], b[1], b[2], nk, ncol, ld, post)
+                    outs = a + b
+                else:
+                    a, b = z(), z()
+                    plain(dev, C, a, nk, ncol, ld, status=st)
+                    fused(dev, C, b, nk, ncol, ld, post)
+                    outs = [a, b]
+                torch.cuda.synchronize()
+                assert int(st.item()) == pkg.TG_OK, (name, mode)
+                got[mode] = [o[:, :ncol].clone() for o in outs] + [nm[:, :ncol].clone()]
+            finally:
+                pkg.set_assembly_mode(-1)
+        for i, (u, v) in enumerate(zip(got[1], got[2])):
+            assert torch.equal(u, v), (name, i)
+
+
+@pytest.mark.parametrize("ncol,calc_helium", [(1500, 1), (1500, 0), (17000, 1)])
+def test_comp_three_pass_gives_the_two_pass_bits(cuda, pkg, ncol, calc_helium):
+    """comp_ng in assembly mode 2 (the 30 row planes formed level-parallel,
+    then the block recurrence alone) gives mode 1's solution and system."""
+    torch = cuda
+    nk, dz = 57, 0.25
+    F, C = pkg.synth.comp_inputs(nk, ncol, dz, 31, calc_helium=calc_helium)
+    ld = pkg.batch.pad_ld(ncol)
+    grid = type("G", (), dict(nk=nk, ncol=ncol, ld=ld))()
+    dev = pkg.dynamics._dev_fields(F, grid, ("expz", "difk"), "cuda")
+    got = {}
+    for mode in (1, 2):
+        pkg.set_assembly_mode(mode)
+        try:
+            out = torch.zeros((3, nk, ld), dtype=torch.float64, device="cuda")
+            so = torch.zeros((30, nk, ld), dtype=torch.float64, device="cuda")
+            st = torch.zeros(1, dtype=torch.int32, device="cuda")
+            pkg.comp_ng_dev(dev, C, out, nk, ncol, ld, system_out=so, status=st)
+            torch.cuda.synchronize()
+            assert int(st.item()) == pkg.TG_OK
+            got[mode] = (out[..., :ncol].clone(), so[:, :nk - 1, :ncol].clone())
+        finally:
+            pkg.set_assembly_mode(-1)
+    assert torch.equal(got[1][0], got[2][0])
+    assert torch.equal(got[1][1], got[2][1])

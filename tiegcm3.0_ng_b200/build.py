@@ -11,7 +11,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libtg_colsolve.so")
-SOURCES = ["tg_kernels.cu", "tg_assembly.cu", "tg_settei.cu", "tg_oplus.cu", "tg_horiz.cu", "tg_filter.cu", "tg_api.cu", "tg_noalloc.cu"]
+SOURCES = ["tg_kernels.cu", "tg_assembly.cu", "tg_settei.cu", "tg_oplus.cu", "tg_walk.cu", "tg_horiz.cu", "tg_filter.cu",
+           "tg_api.cu", "tg_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]

@@ -42,7 +42,7 @@ EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor
            "tg_comp_ng_dev", "tg_comp_post_ng", "tg_comp_post_ng_dev", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_advec_ng", "tg_advec_ng_dev", "tg_smooth_ng", "tg_smooth_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
-           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_column_residency", "tg_set_assembly_mode", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
+           "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_column_residency", "tg_set_assembly_mode", "tg_set_walk_prefetch", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
            "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_kernel_arch", "tg_ringfilter", "tg_ringfilter_dev", "tg_filter_o2o", "tg_trsolv_defer", "tg_trsolv_flush", "tg_dt_diag_ng", "tg_dt_diag_ng_dev", "tg_minor_diag_ng", "tg_minor_diag_ng_dev", "tg_dt_ng_post_dev", "tg_minor_ng_post_dev", "tg_oplus_ng_post_dev", "tg_last_error")
 
 
@@ -255,6 +255,7 @@ def lib():
             "tg_filter_o2o": [P, I, I, I, P, I, D],
             "tg_ringfilter_dev": [P, I, I, I, I, I, P, I, D, Lg, P],
             "tg_set_assembly_mode": [I],
+            "tg_set_walk_prefetch": [I],
             "tg_set_block_scratch_budget": [D],
             "tg_set_scalar_scratch_budget": [D],
             "tg_set_kind_overlap": [I],
@@ -923,8 +924,13 @@ def set_column_residency(kind, precision, mode):
 
 
 def set_assembly_mode(mode):
-    """Assembly kernels: 1 two passes (default), 0 one fused column walk, -1 default."""
+    """Assembly kernels: 2 three passes where built (default), 1 two passes, 0 one fused column walk, -1 default."""
     return _check(lib().tg_set_assembly_mode(int(mode)), "tg_set_assembly_mode")
+
+
+def set_walk_prefetch(levels):
+    """Levels the assembly walks read ahead: 1..32, or -1 automatic (8 up to 16384 columns, else 1)."""
+    return _check(lib().tg_set_walk_prefetch(int(levels)), "tg_set_walk_prefetch")
 
 
 def set_scalar_scratch_budget(megabytes):

@@ -875,7 +875,9 @@ __attribute__((visibility("default"))) int tg_dt_ng_dev(const tg_dt_fields *F, c
     StreamWs *ws = nullptr;
     if ((rc = stream_ws(cx, st, &ws))) return rc;
     TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_dt_ng(*F, *C, tn_upd, nk, ncol, ld, system_out, ws->flags, st));
+    if ((rc = grow(ws->scratch, sizeof(double) * dt_scratch_planes() * (size_t)nk * (size_t)(ld > 0 ? ld : 1))))
+        return rc;
+    TG_CUDA(launch_dt_ng(*F, *C, tn_upd, nk, ncol, ld, system_out, ws->flags, st, nullptr, (double *)ws->scratch.p));
     if (status_dev) {
         k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
         TG_CUDA(cudaGetLastError());
@@ -932,8 +934,9 @@ __attribute__((visibility("default"))) int tg_dt_ng(const tg_dt_fields *F, const
     TG_CUDA(cudaMemcpyAsync(one + nk, F->dift, sizeof(double) * nk, cudaMemcpyHostToDevice, st));
     D.expz = one;
     D.dift = one + nk;
+    if ((rc = grow(c->scratch[0], sizeof(double) * dt_scratch_planes() * lvl))) return rc;
     TG_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_dt_ng(D, *C, out, nk, ncol, ld, nullptr, c->flags, st));
+    TG_CUDA(launch_dt_ng(D, *C, out, nk, ncol, ld, nullptr, c->flags, st, nullptr, (double *)c->scratch[0].p));
     TG_CUDA(launch_level_to_col(out, ld, stage, nk, nk, ncol, st));
     TG_CUDA(cudaMemcpyAsync(tn_upd, stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaStreamSynchronize(st));
@@ -961,7 +964,7 @@ __attribute__((visibility("default"))) int tg_minor_ng_dev(const tg_minor_fields
     cudaStream_t st = (cudaStream_t)stream;
     StreamWs *ws = nullptr;
     if ((rc = stream_ws(cx, st, &ws))) return rc;
-    if ((rc = grow(ws->scratch, sizeof(double) * 3 * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
+    if ((rc = grow(ws->scratch, sizeof(double) * minor_scratch_planes() * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
     TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
     TG_CUDA(launch_minor_ng(*F, *C, out, nk, ncol, ld, system_out, ws->flags, st, (double *)ws->scratch.p));
     if (status_dev) {
@@ -1018,7 +1021,7 @@ __attribute__((visibility("default"))) int tg_minor_ng(const tg_minor_fields *F,
     D.expz = one;
     D.difk = one + nk;
     TG_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(unsigned), st));
-    if ((rc = grow(c->scratch[0], sizeof(double) * 3 * lvl))) return rc;
+    if ((rc = grow(c->scratch[0], sizeof(double) * minor_scratch_planes() * lvl))) return rc;
     TG_CUDA(launch_minor_ng(D, *C, out_l, nk, ncol, ld, nullptr, c->flags, st, (double *)c->scratch[0].p));
     TG_CUDA(launch_level_to_col(out_l, ld, stage, nk, nk, ncol, st));
     TG_CUDA(cudaMemcpyAsync(out, stage, sizeof(double) * colsz, cudaMemcpyDeviceToHost, st));
@@ -1208,7 +1211,9 @@ __attribute__((visibility("default"))) int tg_dt_ng_post_dev(const tg_dt_fields 
     if ((rc = stream_ws(cx, st, &ws))) return rc;
     const PostStep post = post_of(P, 100.0, 0);
     TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
-    TG_CUDA(launch_dt_ng(*F, *C, tn_upd, nk, ncol, ld, nullptr, ws->flags, st, &post));
+    if ((rc = grow(ws->scratch, sizeof(double) * dt_scratch_planes() * (size_t)nk * (size_t)(ld > 0 ? ld : 1))))
+        return rc;
+    TG_CUDA(launch_dt_ng(*F, *C, tn_upd, nk, ncol, ld, nullptr, ws->flags, st, &post, (double *)ws->scratch.p));
     if (status_dev) {
         k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
         TG_CUDA(cudaGetLastError());
@@ -1231,7 +1236,7 @@ __attribute__((visibility("default"))) int tg_minor_ng_post_dev(const tg_minor_f
     cudaStream_t st = (cudaStream_t)stream;
     StreamWs *ws = nullptr;
     if ((rc = stream_ws(cx, st, &ws))) return rc;
-    if ((rc = grow(ws->scratch, sizeof(double) * 3 * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
+    if ((rc = grow(ws->scratch, sizeof(double) * minor_scratch_planes() * (size_t)nk * (size_t)(ld > 0 ? ld : 1)))) return rc;
     const PostStep post = post_of(P, 1.e-12, 1);
     TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
     TG_CUDA(launch_minor_ng(*F, *C, fcomp_out, nk, ncol, ld, nullptr, ws->flags, st, (double *)ws->scratch.p,
@@ -2254,11 +2259,21 @@ __attribute__((visibility("default"))) int tg_set_block_scratch_budget(double me
 
 __attribute__((visibility("default"))) int tg_set_assembly_mode(int mode)
 {
-    if (mode < -1 || mode > 1) {
-        set_err("tg_set_assembly_mode: mode must be 0, 1 or -1");
+    if (mode < -1 || mode > 2) {
+        set_err("tg_set_assembly_mode: mode must be 0, 1, 2 or -1");
         return TG_EINVAL;
     }
     tg::set_assembly_mode(mode);
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_set_walk_prefetch(int levels)
+{
+    if (levels < -1 || levels == 0 || levels > 32) {
+        set_err("tg_set_walk_prefetch: levels must be 1..32 or -1");
+        return TG_EINVAL;
+    }
+    tg::set_walk_prefetch(levels);
     return TG_OK;
 }
 

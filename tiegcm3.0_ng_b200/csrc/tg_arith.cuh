@@ -62,6 +62,20 @@ __device__ __forceinline__ double qdiv_pivot(double a, double b, double y, bool 
     return b_safe && exp_safe(a) ? div_markstein(a, b, y) : __ddiv_rn(a, b);
 }
 
+// A hint that brings the line holding p into L1 (no register, no wait).
+__device__ __forceinline__ void pf_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// The reads of post_store at index o, requested ahead of the store.
+template <class P>
+__device__ __forceinline__ void post_prefetch(const P &post, bool on, bool bcol, const double *out, long o)
+{
+    pf_l1(out + o);
+    if (!on) return;
+    pf_l1(post.prev + o);
+    pf_l1(post.cur + o);
+    if (bcol) pf_l1(post.bnd + o);
+}
+
 // The store of solution row o with the post-solve steps when `on`: a flagged
 // lateral-boundary column takes its boundary value, the previous-step field
 // is filtered, nm = ds2*(prev + x) + ds*cur, and both are floored (a floor

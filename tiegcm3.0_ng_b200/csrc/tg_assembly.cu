@@ -53,7 +53,7 @@ __device__ __forceinline__ GF dt_gf(const DtConsts &C, double h, double cp, doub
 // same bits as IEEE a/b).
 constexpr int kDtStaged = 20;
 __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *tn_upd, int nk, int ncol, long ld,
-                                               double *sys_out, unsigned *status, PostStep post, int has_post)
+                                               double *sys_out, unsigned *status, PostStep post, int has_post, int pd)
 {
     extern __shared__ double smem_dt[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -84,37 +84,41 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
     // reads of row k into buffer b: 0 schti(k+1), 1 kt(k+1), 2 horadv, 3
     // tnsmooth, 4 mbar, 5 xnmbar, 6 o1, 7 rkm12, 8 scht, 9 hdt, 10 qji_tn, 11
     // cool_exp, 12 cool_imp; 13..19 tn, un, vn, w, cp, km, qtotal of level k+2
-    auto issue = [&](int k, int b) {
+    auto reads = [&](int k, auto &&fn) {
         const long o = (long)k * ld + col;
-        sg.copy(b, 0, F.schti + o + ld);
-        sg.copy(b, 1, F.kt + o + ld);
-        sg.copy(b, 2, F.horadv + o);
-        sg.copy(b, 3, F.tnsmooth + o);
-        sg.copy(b, 4, F.mbar + o);
-        sg.copy(b, 5, F.xnmbar + o);
-        sg.copy(b, 6, F.o1 + o);
-        sg.copy(b, 7, F.rkm12 + o);
-        sg.copy(b, 8, F.scht + o);
-        sg.copy(b, 9, F.hdt + o);
-        sg.copy(b, 10, F.qji_tn + o);
-        sg.copy(b, 11, F.cool_exp + o);
-        sg.copy(b, 12, F.cool_imp + o);
+        fn(0, F.schti + o + ld);
+        fn(1, F.kt + o + ld);
+        fn(2, F.horadv + o);
+        fn(3, F.tnsmooth + o);
+        fn(4, F.mbar + o);
+        fn(5, F.xnmbar + o);
+        fn(6, F.o1 + o);
+        fn(7, F.rkm12 + o);
+        fn(8, F.scht + o);
+        fn(9, F.hdt + o);
+        fn(10, F.qji_tn + o);
+        fn(11, F.cool_exp + o);
+        fn(12, F.cool_imp + o);
         if (k + 2 < nk) {
             const long o2 = o + 2 * ld;
-            sg.copy(b, 13, F.tn + o2);
-            sg.copy(b, 14, F.un + o2);
-            sg.copy(b, 15, F.vn + o2);
-            sg.copy(b, 16, F.w + o2);
-            sg.copy(b, 17, F.cp + o2);
-            sg.copy(b, 18, F.km + o2);
-            sg.copy(b, 19, F.qtotal + o2);
+            fn(13, F.tn + o2);
+            fn(14, F.un + o2);
+            fn(15, F.vn + o2);
+            fn(16, F.w + o2);
+            fn(17, F.cp + o2);
+            fn(18, F.km + o2);
+            fn(19, F.qtotal + o2);
         }
     };
+    auto issue = [&](int k, int b) { reads(k, [&](int v, const double *src) { sg.copy(b, v, src); }); };
+    auto prefetch = [&](int k) { reads(k, [](int, const double *src) { pf_l1(src); }); };
     bool ok = true;
     double w1 = 0.0, y1 = 0.0, w3 = 0.0, rprev = 0.0;
     issue(0, 0);
     sg.commit();
+    for (int kk = 2; kk < pd + 1 && kk < K; ++kk) prefetch(kk);
     for (int k = 0; k < K; ++k) {
+        if (pd > 1 && k + 1 + pd < K) prefetch(k + 1 + pd);
         if (k + 1 < K) issue(k + 1, (k + 1) & 1);
         sg.commit();
         sg.wait_prev();
@@ -219,7 +223,9 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
     double xn = w3, xprev = w3;
     bool fin = fabs(xn) <= DBL_MAX;
     double park = K >= 2 ? tn_upd[(K - 2) * ld + col] : 0.0;
+    for (int kk = K - 3; kk > K - 2 - pd && kk >= 0; --kk) post_prefetch(post, has_post, bcol, tn_upd, (long)kk * ld + col);
     for (int k = K - 2; k >= 0; --k) {
+        if (k - pd >= 0) post_prefetch(post, has_post, bcol, tn_upd, (long)(k - pd) * ld + col);
         xprev = xn;
         const double wk = park;
         if (k >= 1) park = tn_upd[(k - 1) * ld + col];
@@ -235,17 +241,130 @@ __global__ void __launch_bounds__(128) k_dt_ng(DtFields F, DtConsts C, double *t
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
+// Three-pass form of dt_ng: row k (0..nk-2) of every column, one thread per
+// (row, column), from the fields of levels k-1..k+1 read directly: the same
+// operations as k_dt_ng's walk, which keeps those levels in a sliding window.
+namespace {
+// g, f of level j: tni(0) is the previous lower boundary, tni(j) the
+// interface mean of tn(j-1), tn(j) up to nk-2 and tn(j-1) above
+__device__ __forceinline__ GF dt_gf_at(const DtFields &F, const DtConsts &C, int j, int nk, long ld, long col)
+{
+    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+    double tni;
+    if (j == 0) tni = __ldg(F.tlbc + col);
+    else if (j <= nk - 2) tni = xm(0.5, xa(at(F.tn, j - 1), at(F.tn, j)));
+    else tni = at(F.tn, j - 1);
+    return dt_gf(C, at(F.schti, j), at(F.cp, j), at(F.kt, j), tni, __ldg(F.expz + j), __ldg(F.dift + j));
+}
+// vertical advection term of level j before averaging (dt_ng.F90:57-61)
+__device__ __forceinline__ double dt_v0(const DtFields &F, int j, int nk, long ld, long col)
+{
+    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
+    if (j == 0) return xm(xm(xs(at(F.tn, 0), __ldg(F.t_lbc + col)), at(F.w, 0)), 2.0);
+    if (j <= nk - 2) return xm(xs(at(F.tn, j), at(F.tn, j - 1)), at(F.w, j));
+    return 0.0;
+}
+// wind shear of row k (dt_ng.F90:86-95); the top rows divide the row below by 3
+__device__ __forceinline__ void dt_shear_at(const DtFields &F, const DtConsts &C, int k, int nk, long ld, long col,
+                                            double &dudz, double &dvdz)
+{
+    auto at = [&](const double *p, int kk) { return __ldg(p + kk * ld + col); };
+    const double dz = C.dz;
+    const int kc = k <= nk - 3 ? k : nk - 3;
+    if (kc <= 0) {
+        dudz = xd(xs(xa(at(F.un, 0), xm(1.0 / 3.0, at(F.un, 1))), xm(4.0 / 3.0, __ldg(F.ulbc + col))), dz);
+        dvdz = xd(xs(xa(at(F.vn, 0), xm(1.0 / 3.0, at(F.vn, 1))), xm(4.0 / 3.0, __ldg(F.vlbc + col))), dz);
+    } else {
+        dudz = xd(xs(at(F.un, kc + 1), at(F.un, kc - 1)), xm(2.0, dz));
+        dvdz = xd(xs(at(F.vn, kc + 1), at(F.vn, kc - 1)), xm(2.0, dz));
+    }
+    for (int kk = kc + 1; kk <= k; ++kk) {
+        dudz = xd(dudz, 3.0);
+        dvdz = xd(dvdz, 3.0);
+    }
+}
+}  // namespace
+
+__global__ void __launch_bounds__(128) k_dt_coefs(DtFields F, DtConsts C, double *pqrf, int nk, int ncol, long ld,
+                                                  double *sys_out)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int k = blockIdx.y, K = nk - 1;
+    auto at = [&](const double *p, int kk) { return __ldg(p + kk * ld + col); };
+    const double dz = C.dz;
+    const double expz = __ldg(F.expz + k);
+    const GF gf0 = dt_gf_at(F, C, k, nk, ld, col), gfp = dt_gf_at(F, C, k + 1, nk, ld, col);
+    double p = xs(gf0.g, gf0.f);
+    double q, r;
+    if (k < K - 1) {
+        q = -xa(xa(xs(gfp.g, gfp.f), gf0.g), gf0.f);
+        r = xa(gfp.g, gfp.f);
+    } else {
+        q = xs(-gf0.g, gf0.f);
+        r = 0.0;
+    }
+    const double vad = xd(xm(xa(dt_v0(F, k, nk, ld, col), dt_v0(F, k + 1, nk, ld, col)), 0.5), dz);
+    const double cp_0 = at(F.cp, k), cp_p = at(F.cp, k + 1);
+    const double cpi = xm(0.5, xa(cp_0, cp_p));
+    const double kmi = xm(0.5, xa(at(F.km, k), at(F.km, k + 1)));
+    const double wi = xm(0.5, xa(at(F.w, k), at(F.w, k + 1)));
+    double dudz, dvdz;
+    dt_shear_at(F, C, k, nk, ld, col, dudz, dvdz);
+    const double qsolar = xm(0.5, xa(at(F.qtotal, k), at(F.qtotal, k + 1)));
+    const double advec = xa(at(F.horadv, k), vad);
+    double cptn = xm(cpi, xs(advec, xm(C.dtx2inv, at(F.tnsmooth, k))));
+    cptn = xm(cptn, expz);
+    const double mbar = at(F.mbar, k);
+    const double xo = xm(xm(at(F.xnmbar, k), at(F.o1, k)), C.rmassinv_o1);
+    const double qrecomb = xd(xm(xm(xm(C.tsurplus, at(F.rkm12, k)), xm(xo, xo)), C.avo), mbar);
+    double qm = xm(xd(xm(C.grav, kmi), xm(C.p0, at(F.scht, k))), xa(xm(dudz, dudz), xm(dvdz, dvdz)));
+    qm = xd(qm, expz);
+    const double th = xa(xa(xa(xa(qsolar, at(F.hdt, k)), qrecomb), at(F.qji_tn, k)), qm);
+    cptn = xs(cptn, xm(th, expz));
+    double rhs = xa(cptn, at(F.cool_exp, k));
+    const double qpart = xa(xm(cpi, xa(C.dtx2inv, at(F.cool_imp, k))), xd(xm(wi, C.gask), mbar));
+    q = xs(q, xm(qpart, expz));
+    if (k == 0) {   // lower boundary fold (:159-163)
+        q = xs(q, p);
+        rhs = xs(rhs, xm(xm(2.0, p), __ldg(F.t_lbc + col)));
+        p = 0.0;
+    }
+    const long slab = (long)nk * ld, o = (long)k * ld + col;
+    pqrf[o] = p;
+    pqrf[slab + o] = q;
+    pqrf[2 * slab + o] = r;
+    pqrf[3 * slab + o] = rhs;
+    if (sys_out) {
+        sys_out[o] = p;
+        sys_out[slab + o] = q;
+        sys_out[2 * slab + o] = r;
+        sys_out[3 * slab + o] = rhs;
+    }
+}
+
+int dt_scratch_planes() { return 4; }
+
 cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, int nk, int ncol, long ld,
-                         double *sys_out, unsigned *status, cudaStream_t st, const PostStep *post)
+                         double *sys_out, unsigned *status, cudaStream_t st, const PostStep *post, double *scratch)
 {
     if (ncol <= 0) return cudaSuccess;
+    // dt_ng's own walk forms its rows from a register window of levels, so the
+    // three-pass form pays off only where few columns leave the walk latency
+    // bound (on 41472 columns it took 157 against 149 us)
+    if (scratch && assembly_mode() == 2 && nk >= 3 && ncol <= kSmallWalkColumns) {
+        const long slab = (long)nk * ld;
+        k_dt_coefs<<<dim3((ncol + 127) / 128, nk - 1), 128, 0, st>>>(F, C, scratch, nk, ncol, ld, sys_out);
+        return launch_thomas_post(scratch, scratch + slab, scratch + 2 * slab, scratch + 3 * slab, tn_upd, nk, nk - 1,
+                                  1, ncol, ld, status, post, st);
+    }
     // one warp per block keeps a wave of small blocks resident despite the
     // per-thread shared memory (w2 column + staged reads)
     const int T = 32;
     const size_t smem = (size_t)T * ((nk - 2 > 0 ? nk - 2 : 1) * sizeof(double) + Stage<kDtStaged>::bytes_per_thread);
     once_per_device([] { cudaFuncSetAttribute(k_dt_ng, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin() - 1024); });
     k_dt_ng<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, tn_upd, nk, ncol, ld, sys_out, status,
-                                                  post ? *post : PostStep{}, post != nullptr);
+                                                  post ? *post : PostStep{}, post != nullptr, walk_prefetch(ncol));
     return cudaGetLastError();
 }
 
@@ -676,6 +795,92 @@ __global__ void __launch_bounds__(128) k_minor_levels(MinorFields F, MinorConsts
     lv[2 * slab + (long)j * ld + col] = L.dmdzs;
 }
 
+// Row k of minor_ng's system (minor_ng.F90:150-198): from the level planes
+// of levels k and k+1 and the fields of level k; the lower-boundary fold at
+// k = 0 and the upper-boundary row at k = nk-1.
+struct MinorRowIn {
+    double sprod, xnmbar, ftm1, hadvec, sloss, w0, w1;
+    MinorLevel L0, L1;
+};
+__device__ __forceinline__ void minor_row(const MinorFields &F, const MinorConsts &C, long col, int k, int nk,
+                                          double dfac, const MinorRowIn &in, double &p, double &q, double &r,
+                                          double &f)
+{
+    const double dzp = C.dzp, rdz = xd(1.0, dzp);
+    const MinorLevel &L0 = in.L0, &L1 = in.L1;
+    const double expz = __ldg(F.expz + k);
+    const double sp = xd(xm(in.sprod, C.rmx), in.xnmbar);
+    f = xa(xs(xm(in.ftm1, C.dtx2inv), in.hadvec), sp);
+    f = xm(f, expz);
+    if (k < nk - 1) {
+        const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1);
+        const double molp = xm(L0.ax, xa(rdz, xm(0.5, L0.thdiff)));
+        const double molr = xm(L1.ax, xs(rdz, xm(0.5, L1.thdiff)));
+        const double molq = xa(xm(L0.ax, xs(rdz, xm(0.5, L0.thdiff))), xm(L1.ax, xa(rdz, xm(0.5, L1.thdiff))));
+        const double eddyp = xm(xm(C.expzmid_inv, difk0), xs(rdz, xm(0.5, L0.dmdzs)));
+        const double eddyr = xm(xm(C.expzmid, difk1), xa(rdz, xm(0.5, L1.dmdzs)));
+        const double eddyq = xa(xm(xm(C.expzmid_inv, difk0), xa(rdz, xm(0.5, L0.dmdzs))),
+                                xm(xm(C.expzmid, difk1), xs(rdz, xm(0.5, L1.dmdzs))));
+        const double wi = xm(0.5, xa(in.w0, in.w1));
+        p = xs(xd(molp, dzp), xd(xm(expz, xa(xm(eddyp, dfac), xm(0.5, wi))), dzp));
+        r = xs(xd(molr, dzp), xd(xm(expz, xs(xm(eddyr, dfac), xm(0.5, wi))), dzp));
+        q = xa(-xd(molq, dzp), xm(expz, xs(xa(xd(xm(eddyq, dfac), dzp), C.dtx2inv), in.sloss)));
+        if (k == 0) {
+            const double l1 = __ldg(F.flbc1 + col), l2 = __ldg(F.flbc2 + col), l3 = __ldg(F.flbc3 + col);
+            const double den = xs(l1, xm(xm(0.5, l2), dzp));
+            q = xa(q, xd(xm(p, xa(l1, xm(xm(0.5, l2), dzp))), den));
+            f = xs(f, xd(xm(xm(p, l3), dzp), den));
+            p = 0.0;
+        }
+    } else {
+        p = xa(1.0, xm(xm(0.5, dzp), L0.thdiff));
+        q = xs(p, 2.0);
+        r = 0.0;
+        f = -xd(xm(xm(xm(C.grav, C.rmx), __ldg(F.fubc + col)), dzp), xm(xm(C.p0, L0.ax), C.avo));
+    }
+}
+
+// Three-pass form, pass 2: row k of every column, one thread per (row,
+// column), into the planes pqrf (p, q, r, f, each nk*ld).
+__global__ void __launch_bounds__(128) k_minor_coefs(MinorFields F, MinorConsts C, const double *lv, double *pqrf,
+                                                     int nk, int ncol, long ld, double *sys_out)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int k = blockIdx.y;
+    const long slab = (long)nk * ld, o = (long)k * ld + col;
+    MinorRowIn in;
+    in.sprod = __ldg(F.sprod + o);
+    in.xnmbar = __ldg(F.xnmbar + o);
+    in.ftm1 = __ldg(F.ftm1_smooth + o);
+    in.hadvec = __ldg(F.hadvec + o);
+    in.L0.ax = __ldg(lv + o);
+    in.L0.thdiff = __ldg(lv + slab + o);
+    in.L0.dmdzs = __ldg(lv + 2 * slab + o);
+    in.L1 = in.L0;
+    in.sloss = in.w0 = in.w1 = 0.0;
+    if (k < nk - 1) {
+        in.sloss = __ldg(F.sloss + o);
+        in.w0 = __ldg(F.w + o);
+        in.w1 = __ldg(F.w + o + ld);
+        in.L1.ax = __ldg(lv + o + ld);
+        in.L1.thdiff = __ldg(lv + slab + o + ld);
+        in.L1.dmdzs = __ldg(lv + 2 * slab + o + ld);
+    }
+    double p, q, r, f;
+    minor_row(F, C, col, k, nk, __ldg(F.dfactor + col), in, p, q, r, f);
+    pqrf[o] = p;
+    pqrf[slab + o] = q;
+    pqrf[2 * slab + o] = r;
+    pqrf[3 * slab + o] = f;
+    if (sys_out) {
+        sys_out[o] = p;
+        sys_out[slab + o] = q;
+        sys_out[2 * slab + o] = r;
+        sys_out[3 * slab + o] = f;
+    }
+}
+
 // The column walk over the level planes.  Its eleven per-level reads are
 // staged one iteration ahead (Stage); the back sweep re-reads the parked w3
 // one level ahead.  The two divisions of a level share the divisor w1
@@ -683,7 +888,7 @@ __global__ void __launch_bounds__(128) k_minor_levels(MinorFields F, MinorConsts
 constexpr int kMinorStaged = 11;
 __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C, const double *lv, double *out,
                                                     int nk, int ncol, long ld, double *sys_out, unsigned *status,
-                                                    PostStep post, int has_post)
+                                                    PostStep post, int has_post, int pd)
 {
     extern __shared__ double smem_mr[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -693,23 +898,26 @@ __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C
     Stage<kMinorStaged> sg{smem_mr + (long)(nk > 1 ? nk - 1 : 1) * T + threadIdx.x, T};
     const long slab = (long)nk * ld;
     // reads of level k into buffer b: 0 sprod, 1 xnmbar, 2 ftm1_smooth,
-    // 3 hadvec, 4 sloss, 5 w(k), 6 w(k+1), 7..9 planes of level k+1
-    auto issue = [&](int k, int b) {
+    // 3 hadvec, 4 sloss, 5 w(k), 6 w(k+1), 7..9 planes of level k+1;
+    // fn(value index, address)
+    auto reads = [&](int k, auto &&fn) {
         const long o = (long)k * ld + col;
-        sg.copy(b, 0, F.sprod + o);
-        sg.copy(b, 1, F.xnmbar + o);
-        sg.copy(b, 2, F.ftm1_smooth + o);
-        sg.copy(b, 3, F.hadvec + o);
+        fn(0, F.sprod + o);
+        fn(1, F.xnmbar + o);
+        fn(2, F.ftm1_smooth + o);
+        fn(3, F.hadvec + o);
         if (k < nk - 1) {
-            sg.copy(b, 4, F.sloss + o);
-            sg.copy(b, 5, F.w + o);
-            sg.copy(b, 6, F.w + o + ld);
-            sg.copy(b, 7, lv + o + ld);
-            sg.copy(b, 8, lv + slab + o + ld);
-            sg.copy(b, 9, lv + 2 * slab + o + ld);
+            fn(4, F.sloss + o);
+            fn(5, F.w + o);
+            fn(6, F.w + o + ld);
+            fn(7, lv + o + ld);
+            fn(8, lv + slab + o + ld);
+            fn(9, lv + 2 * slab + o + ld);
         }
     };
-    const double dzp = C.dzp, rdz = xd(1.0, dzp), dfac = __ldg(F.dfactor + col);
+    auto issue = [&](int k, int b) { reads(k, [&](int v, const double *src) { sg.copy(b, v, src); }); };
+    auto prefetch = [&](int k) { reads(k, [](int, const double *src) { pf_l1(src); }); };
+    const double dfac = __ldg(F.dfactor + col);
     MinorLevel L0;
     L0.ax = __ldg(lv + col);
     L0.thdiff = __ldg(lv + slab + col);
@@ -718,46 +926,32 @@ __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C
     double w1 = 0.0, y1 = 0.0, w3 = 0.0, rprev = 0.0;
     issue(0, 0);
     sg.commit();
+    for (int kk = 2; kk < pd + 1 && kk < nk; ++kk) prefetch(kk);
     for (int k = 0; k < nk; ++k) {
+        if (pd > 1 && k + 1 + pd < nk) prefetch(k + 1 + pd);
         if (k + 1 < nk) issue(k + 1, (k + 1) & 1);
         sg.commit();
         sg.wait_prev();
         const int b = k & 1;
-        double p, q, r, f;
-        const double expz = __ldg(F.expz + k);
-        const double sp = xd(xm(sg.at(b, 0), C.rmx), sg.at(b, 1));
-        f = xa(xs(xm(sg.at(b, 2), C.dtx2inv), sg.at(b, 3)), sp);
-        f = xm(f, expz);
-        MinorLevel L1 = L0;
+        MinorRowIn in;
+        in.sloss = in.w0 = in.w1 = 0.0;
+        in.sprod = sg.at(b, 0);
+        in.xnmbar = sg.at(b, 1);
+        in.ftm1 = sg.at(b, 2);
+        in.hadvec = sg.at(b, 3);
+        in.L0 = L0;
+        in.L1 = L0;
         if (k < nk - 1) {
-            L1.ax = sg.at(b, 7);
-            L1.thdiff = sg.at(b, 8);
-            L1.dmdzs = sg.at(b, 9);
-            const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1);
-            const double molp = xm(L0.ax, xa(rdz, xm(0.5, L0.thdiff)));
-            const double molr = xm(L1.ax, xs(rdz, xm(0.5, L1.thdiff)));
-            const double molq = xa(xm(L0.ax, xs(rdz, xm(0.5, L0.thdiff))), xm(L1.ax, xa(rdz, xm(0.5, L1.thdiff))));
-            const double eddyp = xm(xm(C.expzmid_inv, difk0), xs(rdz, xm(0.5, L0.dmdzs)));
-            const double eddyr = xm(xm(C.expzmid, difk1), xa(rdz, xm(0.5, L1.dmdzs)));
-            const double eddyq = xa(xm(xm(C.expzmid_inv, difk0), xa(rdz, xm(0.5, L0.dmdzs))),
-                                    xm(xm(C.expzmid, difk1), xs(rdz, xm(0.5, L1.dmdzs))));
-            const double wi = xm(0.5, xa(sg.at(b, 5), sg.at(b, 6)));
-            p = xs(xd(molp, dzp), xd(xm(expz, xa(xm(eddyp, dfac), xm(0.5, wi))), dzp));
-            r = xs(xd(molr, dzp), xd(xm(expz, xs(xm(eddyr, dfac), xm(0.5, wi))), dzp));
-            q = xa(-xd(molq, dzp), xm(expz, xs(xa(xd(xm(eddyq, dfac), dzp), C.dtx2inv), sg.at(b, 4))));
-            if (k == 0) {
-                const double l1 = __ldg(F.flbc1 + col), l2 = __ldg(F.flbc2 + col), l3 = __ldg(F.flbc3 + col);
-                const double den = xs(l1, xm(xm(0.5, l2), dzp));
-                q = xa(q, xd(xm(p, xa(l1, xm(xm(0.5, l2), dzp))), den));
-                f = xs(f, xd(xm(xm(p, l3), dzp), den));
-                p = 0.0;
-            }
-        } else {
-            p = xa(1.0, xm(xm(0.5, dzp), L0.thdiff));
-            q = xs(p, 2.0);
-            r = 0.0;
-            f = -xd(xm(xm(xm(C.grav, C.rmx), __ldg(F.fubc + col)), dzp), xm(xm(C.p0, L0.ax), C.avo));
+            in.sloss = sg.at(b, 4);
+            in.w0 = sg.at(b, 5);
+            in.w1 = sg.at(b, 6);
+            in.L1.ax = sg.at(b, 7);
+            in.L1.thdiff = sg.at(b, 8);
+            in.L1.dmdzs = sg.at(b, 9);
         }
+        double p, q, r, f;
+        minor_row(F, C, col, k, nk, dfac, in, p, q, r, f);
+        const MinorLevel L1 = in.L1;
         if (sys_out) {
             sys_out[k * ld + col] = p;
             sys_out[slab + k * ld + col] = q;
@@ -785,7 +979,9 @@ __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C
     bool fin = fabs(xn) <= DBL_MAX;
     double park = nk >= 2 ? out[(nk - 2) * ld + col] : 0.0;
     if (has_post) post_store(post, true, bcol, out, (long)(nk - 1) * ld + col, xn);
+    for (int kk = nk - 3; kk > nk - 2 - pd && kk >= 0; --kk) post_prefetch(post, has_post, bcol, out, (long)kk * ld + col);
     for (int k = nk - 2; k >= 0; --k) {
+        if (k - pd >= 0) post_prefetch(post, has_post, bcol, out, (long)(k - pd) * ld + col);
         const double wk = park;
         if (k >= 1) park = out[(k - 1) * ld + col];
         xn = xs(wk, xm(w2s[k * T], xn));
@@ -795,9 +991,21 @@ __global__ void __launch_bounds__(128) k_minor_rows(MinorFields F, MinorConsts C
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
-static std::atomic<int> g_assembly_mode{1};
+static std::atomic<int> g_assembly_mode{2};
 int assembly_mode() { return g_assembly_mode.load(); }
-void set_assembly_mode(int m) { g_assembly_mode.store(m < 0 ? 1 : (m ? 1 : 0)); }
+void set_assembly_mode(int m) { g_assembly_mode.store(m < 0 ? 2 : (m > 2 ? 2 : m)); }
+
+// level planes (ax, thdiff, dmdz/barm) and the rows p, q, r, f
+int minor_scratch_planes() { return 7; }
+
+static std::atomic<int> g_walk_prefetch{-1};
+int walk_prefetch(long ncol)
+{
+    const int v = g_walk_prefetch.load();
+    if (v >= 1) return v;
+    return ncol <= kSmallWalkColumns ? 8 : 1;
+}
+void set_walk_prefetch(int levels) { g_walk_prefetch.store(levels < 1 ? -1 : (levels > 32 ? 32 : levels)); }
 
 cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *out, int nk, int ncol, long ld,
                             double *sys_out, unsigned *status, cudaStream_t st, double *scratch, const PostStep *post)
@@ -816,7 +1024,15 @@ cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *
     while (T > 32 && (size_t)T * (nk - 1) * sizeof(double) > (size_t)optin) T /= 2;
     const size_t smem = (size_t)T * (nk - 1 > 0 ? nk - 1 : 1) * sizeof(double);
     if (smem > (size_t)optin) return cudaErrorInvalidValue;
-    if (scratch && assembly_mode() == 1) {
+    if (scratch && assembly_mode() == 2) {
+        const long slab = (long)nk * ld;
+        double *pqrf = scratch + 3 * slab;
+        k_minor_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch, nk, ncol, ld);
+        k_minor_coefs<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch, pqrf, nk, ncol, ld, sys_out);
+        return launch_thomas_post(pqrf, pqrf + slab, pqrf + 2 * slab, pqrf + 3 * slab, out, nk, nk, 0, ncol, ld,
+                                  status, post, st);
+    }
+    if (scratch && assembly_mode() >= 1) {
         // the row walk also holds its staged reads in shared memory
         const size_t per_r = (size_t)(nk - 1 > 0 ? nk - 1 : 1) * sizeof(double) + Stage<kMinorStaged>::bytes_per_thread;
         int TR = 128;
@@ -824,7 +1040,7 @@ cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *
         if ((size_t)TR * per_r > (size_t)optin) return cudaErrorInvalidValue;
         k_minor_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch, nk, ncol, ld);
         k_minor_rows<<<(ncol + TR - 1) / TR, TR, (size_t)TR * per_r, st>>>(F, C, scratch, out, nk, ncol, ld, sys_out,
-                                                                          status, pv, hp);
+                                                                          status, pv, hp, walk_prefetch(ncol));
         return cudaGetLastError();
     }
     k_minor_ng<<<(ncol + T - 1) / T, T, smem, st>>>(F, C, out, nk, ncol, ld, sys_out, status, pv, hp);
@@ -942,145 +1158,134 @@ __device__ __forceinline__ void comp_level(const CompConsts &C, double o2i, doub
 }  // namespace tg
 
 namespace tg {
-// One column of comp_ng's rows and block solve (comp_ng.F90:170-332).  The
-// level quantities (ep, ak, wks4 and, at the top, the alpha entries of the
-// He-flux condition) come from Src: computed on the fly from the fields
-// (CompFusedSrc) or read from planes a level-parallel kernel wrote
-// (CompPlaneSrc).  first(L) gives level 0, next(k, L) level k+1, in order.
+// Row k of the comp_ng block system (comp_ng.F90:213-279): P, Q, R and f
+// from the level quantities of levels k (Lk) and k+1 (Lp) and the fields of
+// level k (through Src), with both boundary folds; flx00 is set at the top row.
 template <class Src>
-__device__ __forceinline__ void comp_walk(const CompFields &F, const CompConsts &C, Src &src, double *out,
-                                          double *scr, int nk, long ld, long col, double *sys_out, unsigned *status)
+__device__ __forceinline__ void comp_row(const CompFields &F, const CompConsts &C, const Src &src, const CompLevel &Lk,
+                                         const CompLevel &Lp, int k, int nk, long ld, long col, double dfac,
+                                         double flx_he, double (&P)[9], double (&Q)[9], double (&R)[9],
+                                         double (&f)[3], double &flx00)
 {
-    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
-    const long slab = (long)nk * ld;
+    auto at = [&](const double *p, int kk) { return __ldg(p + kk * ld + col); };
     const double tau = 1.86e+3, t00 = 273.;
     const double dz = C.dz, rdz = xd(1.0, dz);
-    const double dfac = __ldg(F.dfactor + col);
-    const double flx_he = C.calc_helium ? __ldg(F.flx_he + col) : 0.0;
-    CompLevel Lk, Lp;
-    src.first(Lp);
-    double G[9], z[3];
+    const double wi = xm(0.5, xa(src.w(k), src.w1(k)));
+    const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1), ez = __ldg(F.expz + k);
+    // mol / eddy coefficients and the rows (comp_ng.F90:213-244)
+    const double eddyp = xm(xm(C.expzmid_inv, difk0), xs(rdz, Lk.wks4));
+    const double eddyr = xm(xm(C.expzmid, difk1), xa(rdz, Lp.wks4));
+    const double eddyq =
+        xa(xm(xm(C.expzmid_inv, difk0), xa(rdz, Lk.wks4)), xm(xm(C.expzmid, difk1), xs(rdz, Lp.wks4)));
+    const double ezdz = xd(ez, dz);
+    const double tp = xm(ezdz, xa(xm(eddyp, dfac), xm(0.5, wi)));
+    const double tr = xm(ezdz, xs(xm(eddyr, dfac), xm(0.5, wi)));
+    const double tq = xm(ez, xa(xd(xm(eddyq, dfac), dz), C.dtx2inv));
 #pragma unroll
-    for (int e = 0; e < 9; ++e) G[e] = 0.0;
+    for (int m = 0; m < 3; ++m) {
+        const double hk = xd(Lk.ep[m], 2.0), hp = xd(Lp.ep[m], 2.0);
 #pragma unroll
-    for (int i = 0; i < 3; ++i) z[i] = 0.0;
-    bool ok = true;
-    double flx00 = 1.0;
-    for (int k = 0; k < nk - 1; ++k) {
-        src.begin(k);
-        Lk = Lp;
-        src.next(k, Lp);
-        const double wi = xm(0.5, xa(src.w(k), src.w1(k)));
-        const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1), ez = __ldg(F.expz + k);
-        // mol / eddy coefficients and the rows (comp_ng.F90:213-244)
-        const double eddyp = xm(xm(C.expzmid_inv, difk0), xs(rdz, Lk.wks4));
-        const double eddyr = xm(xm(C.expzmid, difk1), xa(rdz, Lp.wks4));
-        const double eddyq =
-            xa(xm(xm(C.expzmid_inv, difk0), xa(rdz, Lk.wks4)), xm(xm(C.expzmid, difk1), xs(rdz, Lp.wks4)));
-        const double ezdz = xd(ez, dz);
-        const double tp = xm(ezdz, xa(xm(eddyp, dfac), xm(0.5, wi)));
-        const double tr = xm(ezdz, xs(xm(eddyr, dfac), xm(0.5, wi)));
-        const double tq = xm(ez, xa(xd(xm(eddyq, dfac), dz), C.dtx2inv));
-        double P[9], Q[9], R[9], f[3];
-#pragma unroll
-        for (int m = 0; m < 3; ++m) {
-            const double hk = xd(Lk.ep[m], 2.0), hp = xd(Lp.ep[m], 2.0);
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const int e = i + 3 * m;
-                const double molp = xm(Lk.ak[e], xa(rdz, hk));
-                const double molr = xm(Lp.ak[e], xs(rdz, hp));
-                const double molq = xa(xm(Lk.ak[e], xs(rdz, hk)), xm(Lp.ak[e], xa(rdz, hp)));
-                const double fsl = xm(ez, src.fs((m + 1) * 3 + i, k));
-                P[e] = i == m ? xs(xd(molp, dz), tp) : xd(molp, dz);
-                R[e] = i == m ? xs(xd(molr, dz), tr) : xd(molr, dz);
-                Q[e] = i == m ? xs(xa(-xd(molq, dz), tq), fsl) : xs(-xd(molq, dz), fsl);
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-            f[i] = xm(ez, xa(xs(xm(src.nms(i, k), C.dtx2inv), xs(src.adv(i, k), src.fs(i, k))), src.hd(i, k)));
-        if (k == 0) {
-            // lower boundary b(3,3), fb(3) (comp_ng.F90:246-258)
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-#pragma unroll
-                for (int n = 0; n < 3; ++n)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) Q[i + 3 * m] = xa(Q[i + 3 * m], xm(P[i + 3 * n], C.b[n + 3 * m]));
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-#pragma unroll
-                for (int i = 0; i < 3; ++i) f[i] = xs(f[i], xm(P[i + 3 * m], C.fb[m]));
-#pragma unroll
-            for (int e = 0; e < 9; ++e) P[e] = 0.0;
-        } else if (k == nk - 2) {
-            // upper boundary with the He escape flux (comp_ng.F90:259-279)
-#pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                const double h = xm(xm(0.5, Lp.ep[m]), dz);
-                const double ratio = xd(xa(1.0, h), xs(1.0, h));
-#pragma unroll
-                for (int i = 0; i < 3; ++i) Q[i + 3 * m] = xa(Q[i + 3 * m], xm(ratio, R[i + 3 * m]));
-            }
-            // embari and tn of level k (k = nk-2 >= 1)
-            const double embari_k = xm(0.5, xa(at(F.mbar, k - 1), at(F.mbar, k)));
-            flx00 = xd(xm(xm(xm(embari_k, C.rmassinv_n2), C.p0), pow(xd(t00, at(F.tn, k)), 0.25)), xm(tau, C.grav));
-            const double d2 = xm(flx00, xs(rdz, xm(0.5, Lp.ep[1]))), d3 = xm(flx00, xs(rdz, xm(0.5, Lp.ep[2])));
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-                f[i] = xs(xs(f[i], xd(xm(xm(R[i + 3], xs(Lp.a23, Lp.a22)), flx_he), d2)),
-                          xd(xm(xm(R[i + 6], xs(Lp.a33, Lp.a32)), flx_he), d3));
-#pragma unroll
-            for (int e = 0; e < 9; ++e) R[e] = 0.0;
-        }
-        if (sys_out) {
-            double *so = sys_out + (long)k * ld + col;
-#pragma unroll
-            for (int e = 0; e < 9; ++e) {
-                so[(long)e * slab] = P[e];
-                so[(long)(9 + e) * slab] = Q[e];
-                so[(long)(18 + e) * slab] = R[e];
-            }
-#pragma unroll
-            for (int i = 0; i < 3; ++i) so[(long)(27 + i) * slab] = f[i];
-        }
-        // block forward step (comp_ng.F90:280-314)
-        double W[9], v[3];
-        if (k > 0) {
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-#pragma unroll
-                for (int n = 0; n < 3; ++n)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) Q[i + 3 * m] = xs(Q[i + 3 * m], xm(P[i + 3 * n], G[n + 3 * m]));
-        }
-        inv3_ieee(Q, W);
-#pragma unroll
-        for (int e = 0; e < 9; ++e) ok = ok && fabs(W[e]) <= DBL_MAX;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) v[i] = f[i];
-        if (k > 0) {
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-#pragma unroll
-                for (int i = 0; i < 3; ++i) v[i] = xs(v[i], xm(P[i + 3 * m], z[m]));
-        }
-#pragma unroll
-        for (int i = 0; i < 3; ++i) z[i] = xa(xa(xm(W[i], v[0]), xm(W[i + 3], v[1])), xm(W[i + 6], v[2]));
-        if (k < nk - 2) {
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-                    G[i + 3 * m] = xa(xa(xm(W[i], R[3 * m]), xm(W[i + 3], R[1 + 3 * m])), xm(W[i + 6], R[2 + 3 * m]));
-            double *sg = scr + (long)(k + 1) * 12 * ld + col;
-#pragma unroll
-            for (int e = 0; e < 9; ++e) sg[(long)e * ld] = G[e];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) sg[(long)(9 + i) * ld] = z[i];
+        for (int i = 0; i < 3; ++i) {
+            const int e = i + 3 * m;
+            const double molp = xm(Lk.ak[e], xa(rdz, hk));
+            const double molr = xm(Lp.ak[e], xs(rdz, hp));
+            const double molq = xa(xm(Lk.ak[e], xs(rdz, hk)), xm(Lp.ak[e], xa(rdz, hp)));
+            const double fsl = xm(ez, src.fs((m + 1) * 3 + i, k));
+            P[e] = i == m ? xs(xd(molp, dz), tp) : xd(molp, dz);
+            R[e] = i == m ? xs(xd(molr, dz), tr) : xd(molr, dz);
+            Q[e] = i == m ? xs(xa(-xd(molq, dz), tq), fsl) : xs(-xd(molq, dz), fsl);
         }
     }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        f[i] = xm(ez, xa(xs(xm(src.nms(i, k), C.dtx2inv), xs(src.adv(i, k), src.fs(i, k))), src.hd(i, k)));
+    if (k == 0) {
+        // lower boundary b(3,3), fb(3) (comp_ng.F90:246-258)
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) Q[i + 3 * m] = xa(Q[i + 3 * m], xm(P[i + 3 * n], C.b[n + 3 * m]));
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) f[i] = xs(f[i], xm(P[i + 3 * m], C.fb[m]));
+#pragma unroll
+        for (int e = 0; e < 9; ++e) P[e] = 0.0;
+    } else if (k == nk - 2) {
+        // upper boundary with the He escape flux (comp_ng.F90:259-279)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const double h = xm(xm(0.5, Lp.ep[m]), dz);
+            const double ratio = xd(xa(1.0, h), xs(1.0, h));
+#pragma unroll
+            for (int i = 0; i < 3; ++i) Q[i + 3 * m] = xa(Q[i + 3 * m], xm(ratio, R[i + 3 * m]));
+        }
+        // embari and tn of level k (k = nk-2 >= 1)
+        const double embari_k = xm(0.5, xa(at(F.mbar, k - 1), at(F.mbar, k)));
+        flx00 = xd(xm(xm(xm(embari_k, C.rmassinv_n2), C.p0), pow(xd(t00, at(F.tn, k)), 0.25)), xm(tau, C.grav));
+        const double d2 = xm(flx00, xs(rdz, xm(0.5, Lp.ep[1]))), d3 = xm(flx00, xs(rdz, xm(0.5, Lp.ep[2])));
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            f[i] = xs(xs(f[i], xd(xm(xm(R[i + 3], xs(Lp.a23, Lp.a22)), flx_he), d2)),
+                      xd(xm(xm(R[i + 6], xs(Lp.a33, Lp.a32)), flx_he), d3));
+#pragma unroll
+        for (int e = 0; e < 9; ++e) R[e] = 0.0;
+    }
+}
+
+// The block forward step of row k (comp_ng.F90:280-314): Q' = Q - P Gamma_k,
+// W = Q'^-1, z_(k+1) = W (f - P z_k), Gamma_(k+1) = W R, the last two into the
+// scratch rows of level k+1.
+__device__ __forceinline__ void comp_forward(const double (&P)[9], double (&Q)[9], const double (&R)[9],
+                                             const double (&f)[3], int k, int nk, long ld, long col, double *scr,
+                                             double (&G)[9], double (&z)[3], bool &ok)
+{
+    double W[9], v[3];
+    if (k > 0) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) Q[i + 3 * m] = xs(Q[i + 3 * m], xm(P[i + 3 * n], G[n + 3 * m]));
+    }
+    inv3_ieee(Q, W);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) ok = ok && fabs(W[e]) <= DBL_MAX;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = f[i];
+    if (k > 0) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) v[i] = xs(v[i], xm(P[i + 3 * m], z[m]));
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) z[i] = xa(xa(xm(W[i], v[0]), xm(W[i + 3], v[1])), xm(W[i + 6], v[2]));
+    if (k < nk - 2) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                G[i + 3 * m] = xa(xa(xm(W[i], R[3 * m]), xm(W[i + 3], R[1 + 3 * m])), xm(W[i + 6], R[2 + 3 * m]));
+        double *sg = scr + (long)(k + 1) * 12 * ld + col;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) sg[(long)e * ld] = G[e];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) sg[(long)(9 + i) * ld] = z[i];
+    }
+}
+
+// The back sweep (comp_ng.F90:317-324) from the scratch rows, the top level
+// with the He escape flux (:326-332) and calc_helium = 0's fixed He.
+__device__ __forceinline__ void comp_back(const CompConsts &C, const CompLevel &Lp, double flx00, double flx_he,
+                                          const double (&z)[3], bool ok, double *out, const double *scr, int nk,
+                                          long ld, long col, unsigned *status, int pd)
+{
+    const long slab = (long)nk * ld;
+    const double dz = C.dz, rdz = xd(1.0, dz);
     // back sweep (comp_ng.F90:317-324); x(nk-1) = z_{nk-1}
     bool fin = true;
     double x[3], xb[3];
@@ -1091,7 +1296,15 @@ __device__ __forceinline__ void comp_walk(const CompFields &F, const CompConsts 
         out[(long)i * slab + (long)(nk - 2) * ld + col] = x[i];
         fin = fin && fabs(x[i]) <= DBL_MAX;
     }
+    // the Gamma/z rows of level kk+1, requested pd levels ahead of their use
+    auto pf_gz = [&](int kk) {
+        const double *sg = scr + (long)(kk + 1) * 12 * ld + col;
+#pragma unroll
+        for (int e = 0; e < 12; ++e) pf_l1(sg + (long)e * ld);
+    };
+    for (int kk = nk - 4; kk > nk - 3 - pd && kk >= 0; --kk) pf_gz(kk);
     for (int k = nk - 3; k >= 0; --k) {
+        if (k - pd >= 0) pf_gz(k - pd);
         const double *sg = scr + (long)(k + 1) * 12 * ld + col;
         double g[9], zk[3];
 #pragma unroll
@@ -1126,6 +1339,50 @@ __device__ __forceinline__ void comp_walk(const CompFields &F, const CompConsts 
     if (!C.calc_helium)
         for (int k = 0; k < nk; ++k) out[2 * slab + (long)k * ld + col] = C.pshelb;
     if (!ok || !fin) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+}
+
+// One column of comp_ng's rows and block solve (comp_ng.F90:170-332).  The
+// level quantities (ep, ak, wks4 and, at the top, the alpha entries of the
+// He-flux condition) come from Src: computed on the fly from the fields
+// (CompFusedSrc) or read from planes a level-parallel kernel wrote
+// (CompPlaneSrc).  first(L) gives level 0, next(k, L) level k+1, in order.
+template <class Src>
+__device__ __forceinline__ void comp_walk(const CompFields &F, const CompConsts &C, Src &src, double *out,
+                                          double *scr, int nk, long ld, long col, double *sys_out, unsigned *status,
+                                          int pd = 1)
+{
+    const long slab = (long)nk * ld;
+    const double dfac = __ldg(F.dfactor + col);
+    const double flx_he = C.calc_helium ? __ldg(F.flx_he + col) : 0.0;
+    CompLevel Lk, Lp;
+    src.first(Lp);
+    double G[9], z[3];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) G[e] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) z[i] = 0.0;
+    bool ok = true;
+    double flx00 = 1.0;
+    for (int k = 0; k < nk - 1; ++k) {
+        src.begin(k);
+        Lk = Lp;
+        src.next(k, Lp);
+        double P[9], Q[9], R[9], f[3];
+        comp_row(F, C, src, Lk, Lp, k, nk, ld, col, dfac, flx_he, P, Q, R, f, flx00);
+        if (sys_out) {
+            double *so = sys_out + (long)k * ld + col;
+#pragma unroll
+            for (int e = 0; e < 9; ++e) {
+                so[(long)e * slab] = P[e];
+                so[(long)(9 + e) * slab] = Q[e];
+                so[(long)(18 + e) * slab] = R[e];
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) so[(long)(27 + i) * slab] = f[i];
+        }
+        comp_forward(P, Q, R, f, k, nk, ld, col, scr, G, z, ok);
+    }
+    comp_back(C, Lp, flx00, flx_he, z, ok, out, scr, nk, ld, col, status, pd);
 }
 
 // Per-level field reads of comp_walk straight from global memory.
@@ -1279,6 +1536,7 @@ struct CompStagedSrc : CompPlaneSrc {
     double *sm;   // this thread's column of the block's slot array
     int T;        // threads per block (row stride of the slot array)
     int cur;
+    int pd;       // levels ahead whose reads are requested into L1
     __device__ __forceinline__ double &slot(int b, int v) const { return sm[(long)(b * NS + v) * T]; }
     __device__ __forceinline__ void issue(int k, int b)
     {
@@ -1299,15 +1557,37 @@ struct CompStagedSrc : CompPlaneSrc {
         cp_async8(&slot(b, 34), F.hdo1 + o);
         cp_async8(&slot(b, 35), F.hdhe + o);
     }
+    // the lines issue(k) copies, requested into L1 ahead of the copies
+    __device__ __forceinline__ void prefetch(int k) const
+    {
+        const long slab = (long)nk * ld, o = (long)k * ld + col;
+#pragma unroll
+        for (int v = 0; v < kCompPlanes; ++v) pf_l1(lv + v * slab + o + ld);
+        pf_l1(F.w + o);
+        pf_l1(F.w + o + ld);
+#pragma unroll
+        for (int r = 0; r < 12; ++r) pf_l1(F.fs + r * slab + o);
+        pf_l1(F.o2nm_smooth + o);
+        pf_l1(F.o1nm_smooth + o);
+        pf_l1(F.henm_smooth + o);
+        pf_l1(F.o2_advec + o);
+        pf_l1(F.o1_advec + o);
+        pf_l1(F.he_advec + o);
+        pf_l1(F.hdo2 + o);
+        pf_l1(F.hdo1 + o);
+        pf_l1(F.hdhe + o);
+    }
     __device__ __forceinline__ void first(CompLevel &L)
     {
         load(0, L);
         issue(0, 0);
         cp_async_commit();
+        for (int kk = 2; kk < pd + 1 && kk < nk - 1; ++kk) prefetch(kk);
     }
     // iteration k: start the copies of iteration k+1, wait for those of k
     __device__ __forceinline__ void begin(int k)
     {
+        if (k + 1 + pd < nk - 1 && pd > 1) prefetch(k + 1 + pd);
         if (k + 1 < nk - 1) issue(k + 1, (k + 1) & 1);
         cp_async_commit();
         cp_async_wait<1>();
@@ -1342,13 +1622,96 @@ constexpr int kCompRowThreads = 64;
 
 __global__ void __launch_bounds__(kCompRowThreads, 5) k_comp_rows(CompFields F, CompConsts C, const double *lv,
                                                                double *out, double *scr, int nk, int ncol, long ld,
-                                                               double *sys_out, unsigned *status)
+                                                               double *sys_out, unsigned *status, int pd)
 {
     extern __shared__ double comp_slots[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
-    CompStagedSrc src{{{F, ld, col, nk}, lv}, comp_slots + threadIdx.x, (int)blockDim.x, 0};
-    comp_walk(F, C, src, out, scr, nk, ld, col, sys_out, status);
+    CompStagedSrc src{{{F, ld, col, nk}, lv}, comp_slots + threadIdx.x, (int)blockDim.x, 0, pd};
+    comp_walk(F, C, src, out, scr, nk, ld, col, sys_out, status, pd);
+}
+
+// Three-pass form, pass 2: row k of every column, one thread per (row,
+// column), into 30 row planes (P, Q, R by entry i + 3m, then f); the top row
+// also leaves flx00 in its column's slot.
+__global__ void __launch_bounds__(128) k_comp_coefs(CompFields F, CompConsts C, const double *lv, double *rows,
+                                                    double *flx00_row, int nk, int ncol, long ld, double *sys_out)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int k = blockIdx.y;
+    const long slab = (long)nk * ld, o = (long)k * ld + col;
+    CompPlaneSrc src{{F, ld, col, nk}, lv};
+    CompLevel Lk, Lp;
+    src.load(k, Lk);
+    src.load(k + 1, Lp);
+    double P[9], Q[9], R[9], f[3], flx00 = 1.0;
+    comp_row(F, C, src, Lk, Lp, k, nk, ld, col, __ldg(F.dfactor + col),
+             C.calc_helium ? __ldg(F.flx_he + col) : 0.0, P, Q, R, f, flx00);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+        rows[(long)e * slab + o] = P[e];
+        rows[(long)(9 + e) * slab + o] = Q[e];
+        rows[(long)(18 + e) * slab + o] = R[e];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) rows[(long)(27 + i) * slab + o] = f[i];
+    if (k == nk - 2) flx00_row[col] = flx00;
+    if (sys_out) {
+        double *so = sys_out + o;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+            so[(long)e * slab] = P[e];
+            so[(long)(9 + e) * slab] = Q[e];
+            so[(long)(18 + e) * slab] = R[e];
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) so[(long)(27 + i) * slab] = f[i];
+    }
+}
+
+// Three-pass form, pass 3: the block recurrence over the row planes, one
+// thread per column, one warp per block (the columns spread over every SM).
+constexpr int kCompWalkThreads = 32;
+__global__ void __launch_bounds__(kCompWalkThreads) k_comp_walk(CompFields F, CompConsts C, const double *lv,
+                                                                const double *rows, const double *flx00_row,
+                                                                double *out, double *scr, int nk, int ncol, long ld,
+                                                                unsigned *status, int pd)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const long slab = (long)nk * ld;
+    auto pf_row = [&](int k) {
+        const double *r = rows + (long)k * ld + col;
+#pragma unroll
+        for (int v = 0; v < 30; ++v) pf_l1(r + (long)v * slab);
+    };
+    for (int kk = 1; kk < pd && kk < nk - 1; ++kk) pf_row(kk);
+    double G[9], z[3];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) G[e] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) z[i] = 0.0;
+    bool ok = true;
+    for (int k = 0; k < nk - 1; ++k) {
+        if (k + pd < nk - 1) pf_row(k + pd);
+        const double *r = rows + (long)k * ld + col;
+        double P[9], Q[9], R[9], f[3];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+            P[e] = r[(long)e * slab];
+            Q[e] = r[(long)(9 + e) * slab];
+            R[e] = r[(long)(18 + e) * slab];
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) f[i] = r[(long)(27 + i) * slab];
+        comp_forward(P, Q, R, f, k, nk, ld, col, scr, G, z, ok);
+    }
+    CompPlaneSrc src{{F, ld, col, nk}, lv};
+    CompLevel Lp;
+    src.load(nk - 1, Lp);
+    comp_back(C, Lp, flx00_row[col], C.calc_helium ? __ldg(F.flx_he + col) : 0.0, z, ok, out, scr, nk, ld, col,
+              status, pd);
 }
 
 cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out, double *scratch, int nk, int ncol,
@@ -1357,66 +1720,101 @@ cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out
     if (ncol <= 0) return cudaSuccess;
     if (nk < 3) return cudaErrorInvalidValue;
     const int T = 128;
-    if (assembly_mode() == 1) {
+    // the 30 row planes cost more traffic than they save above a few thousand
+    // columns per SM-wave (41472 columns: 625 against 449 us)
+    if (assembly_mode() == 2 && ncol <= kSmallWalkColumns) {
+        const long slab = (long)nk * ld;
+        double *lv = scratch + 12 * slab;                   // after the Gamma/z scratch
+        double *flx00_row = lv + kCompPlanes * slab + 4 * ld;
+        double *rows = flx00_row + ld;
+        k_comp_levels<<<dim3((ncol + T - 1) / T, nk), T, 0, st>>>(F, C, lv, nk, ncol, ld);
+        k_comp_coefs<<<dim3((ncol + T - 1) / T, nk - 1), T, 0, st>>>(F, C, lv, rows, flx00_row, nk, ncol, ld, sys_out);
+        const int TW = kCompWalkThreads;
+        k_comp_walk<<<(ncol + TW - 1) / TW, TW, 0, st>>>(F, C, lv, rows, flx00_row, out, scratch, nk, ncol, ld, status,
+                                                         walk_prefetch(ncol));
+        return cudaGetLastError();
+    }
+    if (assembly_mode() >= 1) {
         double *lv = scratch + 12 * (long)nk * ld;   // after the Gamma/z scratch
         k_comp_levels<<<dim3((ncol + T - 1) / T, nk), T, 0, st>>>(F, C, lv, nk, ncol, ld);
         const int TR = kCompRowThreads;
         k_comp_rows<<<(ncol + TR - 1) / TR, TR, 2 * CompStagedSrc::NS * TR * sizeof(double), st>>>(
-            F, C, lv, out, scratch, nk, ncol, ld, sys_out, status);
+            F, C, lv, out, scratch, nk, ncol, ld, sys_out, status, walk_prefetch(ncol));
         return cudaGetLastError();
     }
     k_comp_ng<<<(ncol + T - 1) / T, T, 0, st>>>(F, C, out, scratch, nk, ncol, ld, sys_out, status);
     return cudaGetLastError();
 }
 
-size_t comp_scratch_doubles(int nk, long ld) { return (size_t)(12 + kCompPlanes) * nk * ld + 4 * (size_t)ld; }
+// Gamma/z (12 planes), the level planes and their 4 top rows, then (three-pass
+// form) the flx00 row and the 30 row planes
+size_t comp_scratch_doubles(int nk, long ld) { return (size_t)(12 + kCompPlanes + 30) * nk * ld + 5 * (size_t)ld; }
 }  // namespace tg
 
-// comp_ng post-solve steps (src/comp_ng.F90:394-457), one thread per column:
-// the lateral-boundary overwrite of the columns flagged in bmask (when given),
-// the time filter, the N2 extrapolation, floors and normalisation.  The N2
-// extrapolation uses the device log/exp, so it agrees with the CPU
+// comp_ng post-solve steps (src/comp_ng.F90:394-457): the lateral-boundary
+// overwrite of the columns flagged in bmask (when given), the time filter,
+// the N2 extrapolation, floors and normalisation.  A block takes 32 columns
+// with four warps; a warp works on the 32 columns of one level at a time, so
+// every phase runs over all levels at once: the overwrite, the search for the
+// first level with N2 < 0.01 (the least level any warp finds), the
+// extrapolation constants (one thread per column), then the per-level steps.
+// The N2 extrapolation uses the device log/exp, so it agrees with the CPU
 // restatement to a tolerance in the extrapolated levels.
 namespace tg {
-__global__ void __launch_bounds__(128) k_comp_post_ng(const double *o2, const double *o1, const double *he,
-                                                      const double *o2_nm, const double *o1_nm, const double *he_nm,
-                                                      const double *xnmbar, const double *zpmid, double dz,
-                                                      double ds, double ds2, int nk, int ncol, long ld, double *o2u,
-                                                      double *o1u, double *heu, double *o2n, double *o1n,
-                                                      double *hen, const unsigned char *bmask, const double *b2,
-                                                      const double *b1, const double *bh)
+constexpr int kPostCols = 32, kPostWarps = 4;
+
+__global__ void __launch_bounds__(kPostCols * kPostWarps) k_comp_post_ng(
+    const double *o2, const double *o1, const double *he, const double *o2_nm, const double *o1_nm,
+    const double *he_nm, const double *xnmbar, const double *zpmid, double dz, double ds, double ds2, int nk, int ncol,
+    long ld, double *o2u, double *o1u, double *heu, double *o2n, double *o1n, double *hen, const unsigned char *bmask,
+    const double *b2, const double *b1, const double *bh)
 {
-    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
+    __shared__ int ktop_s[kPostCols];
+    __shared__ double n2top_s[kPostCols], dn2dz_s[kPostCols], zmtop_s[kPostCols];
+    const int c = threadIdx.x % kPostCols, w = threadIdx.x / kPostCols;
+    const long col = (long)blockIdx.x * kPostCols + c;
+    const bool live = col < ncol;
     const double small = 1.e-9;
+    if (w == 0) ktop_s[c] = nk;
     // the Dirichlet lateral-boundary hook (comp_ng.F90:394-413)
-    if (bmask && bmask[col])
-        for (int k = 0; k < nk; ++k) {
+    if (live && bmask && bmask[col])
+        for (int k = w; k < nk; k += kPostWarps) {
             const long o = (long)k * ld + col;
             o2u[o] = b2[o];
             o1u[o] = b1[o];
             heu[o] = bh[o];
         }
+    __syncthreads();
     // first level with N2 < 0.01 (comp_ng.F90:425-429)
-    int ktop = nk;
-    for (int k = 0; k < nk; ++k) {
-        const long o = (long)k * ld + col;
-        const double n2 = xs(xs(xs(1.0, o2u[o]), o1u[o]), heu[o]);
-        if (n2 < 0.01) {
-            ktop = k;
-            break;
+    if (live)
+        for (int k = w; k < nk; k += kPostWarps) {
+            const long o = (long)k * ld + col;
+            if (xs(xs(xs(1.0, o2u[o]), o1u[o]), heu[o]) < 0.01) {
+                atomicMin(&ktop_s[c], k);
+                break;
+            }
         }
+    __syncthreads();
+    if (w == 0 && live) {
+        const int ktop = ktop_s[c];
+        double n2top = 0.0, dn2dz = 0.0, zmtop = 0.0;
+        if (ktop > 0 && ktop < nk - 1) {
+            const long o = (long)ktop * ld + col, om = o - ld;
+            zmtop = zpmid[ktop];
+            n2top = log(xm(xs(xs(xs(1.0, o2u[o]), o1u[o]), heu[o]), xnmbar[o]));
+            const double n2top1 = log(xm(xs(xs(xs(1.0, o2u[om]), o1u[om]), heu[om]), xnmbar[om]));
+            dn2dz = xd(xs(n2top, n2top1), dz);
+        }
+        n2top_s[c] = n2top;
+        dn2dz_s[c] = dn2dz;
+        zmtop_s[c] = zmtop;
     }
-    double n2top = 0.0, dn2dz = 0.0, zmtop = 0.0;
+    __syncthreads();
+    if (!live) return;
+    const int ktop = ktop_s[c];
     const bool extrap = ktop > 0 && ktop < nk - 1;
-    if (extrap) {
-        const long o = (long)ktop * ld + col, om = o - ld;
-        zmtop = zpmid[ktop];
-        n2top = log(xm(xs(xs(xs(1.0, o2u[o]), o1u[o]), heu[o]), xnmbar[o]));
-        const double n2top1 = log(xm(xs(xs(xs(1.0, o2u[om]), o1u[om]), heu[om]), xnmbar[om]));
-        dn2dz = xd(xs(n2top, n2top1), dz);
-    }
-    for (int k = 0; k < nk; ++k) {
+    const double n2top = n2top_s[c], dn2dz = dn2dz_s[c], zmtop = zmtop_s[c];
+    for (int k = w; k < nk; k += kPostWarps) {
         const long o = (long)k * ld + col;
         const double a0 = o2u[o], b0 = o1u[o], c0 = heu[o];
         const double an = xa(xm(ds2, xa(o2_nm[o], a0)), xm(ds, o2[o]));
@@ -1425,19 +1823,19 @@ __global__ void __launch_bounds__(128) k_comp_post_ng(const double *o2, const do
         double n2 = xs(xs(xs(1.0, a0), b0), c0);
         if (extrap && k > ktop) n2 = xd(exp(xa(n2top, xm(dn2dz, xs(zpmid[k], zmtop)))), xnmbar[o]);
         const double n2nm = xs(xs(xs(1.0, an), bn), cn);
-        double a = fmax(a0, small), b = fmax(b0, small), c = fmax(c0, small), d = fmax(n2, small);
-        double s = xa(xa(xa(a, b), c), d);
+        double a = fmax(a0, small), b = fmax(b0, small), cc = fmax(c0, small), d = fmax(n2, small);
+        double s = xa(xa(xa(a, b), cc), d);
         o2u[o] = xd(a, s);
         o1u[o] = xd(b, s);
-        heu[o] = xd(c, s);
+        heu[o] = xd(cc, s);
         a = fmax(an, small);
         b = fmax(bn, small);
-        c = fmax(cn, small);
+        cc = fmax(cn, small);
         d = fmax(n2nm, small);
-        s = xa(xa(xa(a, b), c), d);
+        s = xa(xa(xa(a, b), cc), d);
         o2n[o] = xd(a, s);
         o1n[o] = xd(b, s);
-        hen[o] = xd(c, s);
+        hen[o] = xd(cc, s);
     }
 }
 
@@ -1446,12 +1844,10 @@ cudaError_t launch_comp_post_ng(const double *const *in7, const double *zpmid, d
                                 const unsigned char *bnd_mask, const double *const *bnd3)
 {
     if (ncol <= 0) return cudaSuccess;
-    const int T = 128;
-    k_comp_post_ng<<<(ncol + T - 1) / T, T, 0, st>>>(in7[0], in7[1], in7[2], in7[3], in7[4], in7[5], in7[6], zpmid,
-                                                     dz, dtsmooth, dtsmooth_div2, nk, ncol, ld, upd6[0], upd6[1],
-                                                     upd6[2], upd6[3], upd6[4], upd6[5], bnd_mask,
-                                                     bnd_mask ? bnd3[0] : nullptr, bnd_mask ? bnd3[1] : nullptr,
-                                                     bnd_mask ? bnd3[2] : nullptr);
+    k_comp_post_ng<<<(ncol + kPostCols - 1) / kPostCols, kPostCols * kPostWarps, 0, st>>>(
+        in7[0], in7[1], in7[2], in7[3], in7[4], in7[5], in7[6], zpmid, dz, dtsmooth, dtsmooth_div2, nk, ncol, ld,
+        upd6[0], upd6[1], upd6[2], upd6[3], upd6[4], upd6[5], bnd_mask, bnd_mask ? bnd3[0] : nullptr,
+        bnd_mask ? bnd3[1] : nullptr, bnd_mask ? bnd3[2] : nullptr);
     return cudaGetLastError();
 }
 

@@ -171,8 +171,12 @@ struct PostStep {
 // dt_ng fused assembly + solve (tg_assembly.cu).
 typedef tg_dt_fields DtFields;
 typedef tg_dt_consts DtConsts;
+// scratch (dt_scratch_planes() planes of nk*ld) is used by the three-pass
+// form only; without it the fused walk runs.
 cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, int nk, int ncol, long ld,
-                         double *sys_out, unsigned *status, cudaStream_t st, const PostStep *post = nullptr);
+                         double *sys_out, unsigned *status, cudaStream_t st, const PostStep *post = nullptr,
+                         double *scratch = nullptr);
+int dt_scratch_planes();
 
 // dt_ng's 12 history diagnostics of a solution x: level-major planes of nk*ld
 cudaError_t launch_dt_diag_ng(const DtFields &F, const DtConsts &C, const double *x, int nk, int ncol, long ld,
@@ -187,8 +191,27 @@ cudaError_t launch_minor_ng(const MinorFields &F, const MinorConsts &C, double *
                             const PostStep *post = nullptr);
 // Assembly kernels: 1 (default) two-pass (level-parallel level quantities,
 // then the column walk) where built, 0 the single fused column walk.
+// 0 one fused column walk, 1 two passes (level quantities, then a walk that
+// forms the rows), 2 three passes (the rows too are formed one thread per
+// level and column; the walk is the recurrence alone) where built
 int assembly_mode();
 void set_assembly_mode(int m);
+// The walk of the three-pass form (tg_walk.cu): rows 0..K-1 of the p, q, r, f
+// planes into x; top 0: K = nk; top 1: K = nk-1 and x(nk-1) =
+// x(nk-2)**2/x(nk-3); stored through post when given.
+cudaError_t launch_thomas_post(const double *p, const double *q, const double *r, const double *f, double *x, int nk,
+                               int K, int top, int ncol, long ld, unsigned *status, const PostStep *post,
+                               cudaStream_t st);
+// Levels a column walk of the assembly kernels prefetches ahead of the level
+// it computes, for a launch over ncol columns: few columns leave few warps
+// per SM, and each level of the walk then waits out a memory latency unless
+// its reads were requested several levels earlier.  set_walk_prefetch(n):
+// n >= 1 fixed, -1 automatic (8 up to kSmallWalkColumns columns, else 1).
+constexpr int kSmallWalkColumns = 16384;
+// level-major planes of nk*ld doubles the minor_ng scratch holds
+int minor_scratch_planes();
+int walk_prefetch(long ncol);
+void set_walk_prefetch(int levels);
 
 // minor_ng's 7 history diagnostics of a solution x: level-major planes of nk*ld
 cudaError_t launch_minor_diag_ng(const MinorFields &F, const MinorConsts &C, const double *x, int nk, int ncol,

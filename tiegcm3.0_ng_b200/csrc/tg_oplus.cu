@@ -27,8 +27,9 @@ __device__ __forceinline__ double xa(double a, double b) { return __dadd_rn(a, b
 __device__ __forceinline__ double xs(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double xd(double a, double b) { return __ddiv_rn(a, b); }
 
-// scratch planes, level-major
-enum { S_DJ = 0, S_HDZ, S_TP1, S_BDOTU, S_OL, S_PROD, S_N };
+// scratch planes, level-major: the level quantities, then the rows of the
+// three-pass form
+enum { S_DJ = 0, S_HDZ, S_TP1, S_BDOTU, S_OL, S_PROD, S_P, S_Q, S_R, S_EX, S_N };
 
 // interface value at j of a(j), a(j+1): .5*(a(j)+a(j+1)); at the top
 // 1.5*a(nk)-.5*a(nk-1)
@@ -109,21 +110,53 @@ __device__ __forceinline__ void oplus_level(const OplusFields &F, const OplusCon
     S(S_PROD, j) = prod;
 }
 
-// Rows k = 0..nk-2 from the level planes, the forward sweep and the back
-// sweep of one column (oplus_ng.F90:88-99, 209-307).
-__device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusConsts &C, double *opout, const double *scr,
-                                           double *w2s, int T, int nk, long ld, long col, double *sys_out,
-                                           unsigned *status, const PostStep &post, int has_post)
+// Per-column constants of the rows: the top O+ flux (oplus_flux,
+// oplus_ng.F90:88-99), b_z terms, g*m/(2R), the sub-step time factor and the
+// upper-boundary ratios (:262-266).
+struct OplusCol {
+    double bz, opflux, dvbz, bz2, gmr, dtn, ubca, ubcb;
+};
+
+// Interface and half-level quantities of row j built from the level planes
+// (oplus_ng.F90:209-254), as the reference forms them.
+struct OplusRowsAt {
+    const double *scr;
+    long slab, ld, col;
+    int nk;
+    double gmr, dvbz, bz2;
+    __device__ __forceinline__ double S(int e, int k) const { return scr[(long)e * slab + (long)k * ld + col]; }
+    __device__ __forceinline__ double hdzi(int j) const
+    {
+        if (j == 0) return xs(xm(1.5, S(S_HDZ, 0)), xm(0.5, S(S_HDZ, 1)));
+        if (j == nk - 1) return xs(xm(1.5, S(S_HDZ, nk - 2)), xm(0.5, S(S_HDZ, nk - 3)));
+        return xm(0.5, xa(S(S_HDZ, j - 1), S(S_HDZ, j)));
+    }
+    __device__ __forceinline__ double tph1(int j) const
+    {
+        if (j == nk - 1) return xa(xm(xm(2., xs(xm(2., S(S_TP1, nk - 2)), S(S_TP1, nk - 3))), hdzi(nk - 1)), gmr);
+        return xa(xm(xm(2., S(S_TP1, j)), hdzi(j)), gmr);
+    }
+    __device__ __forceinline__ double tph0(int j) const
+    {
+        if (j == 0) return xs(xm(xm(2., xs(xm(2., S(S_TP1, 0)), S(S_TP1, 1))), hdzi(0)), gmr);
+        return xs(xm(xm(2., S(S_TP1, j - 1)), hdzi(j)), gmr);
+    }
+    __device__ __forceinline__ double djint(int j) const
+    {
+        if (j == 0) return xs(xm(1.5, S(S_DJ, 0)), xm(0.5, S(S_DJ, 1)));
+        if (j == nk - 1) return xs(xm(1.5, S(S_DJ, nk - 2)), xm(0.5, S(S_DJ, nk - 3)));
+        return xm(0.5, xa(S(S_DJ, j - 1), S(S_DJ, j)));
+    }
+};
+
+__device__ __forceinline__ OplusCol oplus_col(const OplusFields &F, const OplusConsts &C, const OplusRowsAt &A)
 {
-    const long slab = (long)nk * ld;
-    auto at = [&](const double *p, int k) { return __ldg(p + k * ld + col); };
-    auto S = [&](int e, int k) { return scr[(long)e * slab + (long)k * ld + col]; };
+    const long col = A.col;
     // pi = 4*atan(1) of the reference, correctly rounded
     const double pi = 3.141592653589793, rtd = 180. / pi;
     const double phid = 2.0e8, phin = -2.0e8, ppolar = 0.;
-    const double bz = __ldg(F.bz + col);
-    // oplus_flux (oplus_ng.F90:88-99)
-    double opflux;
+    OplusCol c;
+    c.bz = __ldg(F.bz + col);
     {
         const double arl = fabs(__ldg(F.rlatm + col)), chi = __ldg(F.chi + col);
         double a = 0.;
@@ -131,93 +164,106 @@ __device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusCons
         if (arl < xd(pi, 4.5) && arl > xd(pi, 18.)) a = xm(.5, xa(1., cos(xs(xm(arl, 6.), xd(xm(pi, 4.), 3.)))));
         if (arl <= xd(pi, 18.)) a = 0.;
         const double fed = xm(phid, a), fen = xm(phin, a);
-        opflux = chi >= xm(0.5, pi) ? fen : fed;
+        double opflux = chi >= xm(0.5, pi) ? fen : fed;
         const double cd = xm(chi, rtd);
         if (xm(xs(cd, 80.), xs(cd, 100.)) < 0.)
             opflux = xa(xm(.5, xa(fed, fen)), xm(xm(.5, xs(fed, fen)), cos(xd(xm(pi, xs(cd, 80.)), 20.))));
         if (arl >= xd(pi, 3.)) opflux = xa(opflux, ppolar);
+        c.opflux = opflux;
     }
-    // ---- pass 2: rows and the forward sweep (oplus_ng.F90:209-303)
-    const double dvbz = xd(__ldg(F.dvb + col), bz), bz2 = xm(bz, bz);
-    const double gmr = xd(xm(C.grav, C.rmass_op), xm(2., C.gask));
-    const double dtn = xm(C.dtx2inv, (double)C.nstep_sub);
-    auto hdzi = [&](int j) {
-        if (j == 0) return xs(xm(1.5, S(S_HDZ, 0)), xm(0.5, S(S_HDZ, 1)));
-        if (j == nk - 1) return xs(xm(1.5, S(S_HDZ, nk - 2)), xm(0.5, S(S_HDZ, nk - 3)));
-        return xm(0.5, xa(S(S_HDZ, j - 1), S(S_HDZ, j)));
-    };
-    auto tph1 = [&](int j) {
-        if (j == nk - 1) return xa(xm(xm(2., xs(xm(2., S(S_TP1, nk - 2)), S(S_TP1, nk - 3))), hdzi(nk - 1)), gmr);
-        return xa(xm(xm(2., S(S_TP1, j)), hdzi(j)), gmr);
-    };
-    auto tph0 = [&](int j) {
-        if (j == 0) return xs(xm(xm(2., xs(xm(2., S(S_TP1, 0)), S(S_TP1, 1))), hdzi(0)), gmr);
-        return xs(xm(xm(2., S(S_TP1, j - 1)), hdzi(j)), gmr);
-    };
-    auto djint = [&](int j) {
-        if (j == 0) return xs(xm(1.5, S(S_DJ, 0)), xm(0.5, S(S_DJ, 1)));
-        if (j == nk - 1) return xs(xm(1.5, S(S_DJ, nk - 2)), xm(0.5, S(S_DJ, nk - 3)));
-        return xm(0.5, xa(S(S_DJ, j - 1), S(S_DJ, j)));
-    };
+    c.dvbz = xd(__ldg(F.dvb + col), c.bz);
+    c.bz2 = xm(c.bz, c.bz);
+    c.gmr = xd(xm(C.grav, C.rmass_op), xm(2., C.gask));
+    c.dtn = xm(C.dtx2inv, (double)C.nstep_sub);
+    OplusRowsAt B = A;
+    B.gmr = c.gmr;
+    const int nk = A.nk;
+    c.ubca = xm(xm(-c.bz2, B.djint(nk - 1)), B.tph1(nk - 1));
+    c.ubcb = xm(xm(-c.bz2, B.djint(nk - 1)), B.tph0(nk - 1));
+    return c;
+}
+
+// Row k (0..nk-2) of the O+ system: p, q, r and the right-hand side, with
+// both boundary folds (oplus_ng.F90:255-303).
+__device__ __forceinline__ void oplus_row(const OplusFields &F, const OplusConsts &C, const OplusRowsAt &A,
+                                          const OplusCol &cc, int k, double &p, double &q, double &r, double &ex)
+{
+    const int nk = A.nk;
+    const long ld = A.ld, col = A.col;
+    auto at = [&](const double *pp, int kk) { return __ldg(pp + kk * ld + col); };
+    const double bz = cc.bz;
     auto hdzmp = [&](int j, double sgn) {
-        const double divbz = xa(dvbz, xd(at(F.bdotdh_djbz, j), xm(S(S_DJ, j), bz2)));
-        const double h = S(S_HDZ, j);
-        return xm(sgn > 0 ? xa(h, xm(0.5, divbz)) : xs(h, xm(0.5, divbz)), bz2);
+        const double divbz = xa(cc.dvbz, xd(at(F.bdotdh_djbz, j), xm(A.S(S_DJ, j), cc.bz2)));
+        const double h = A.S(S_HDZ, j);
+        return xm(sgn > 0 ? xa(h, xm(0.5, divbz)) : xs(h, xm(0.5, divbz)), cc.bz2);
     };
-    const double ubca = xm(xm(-bz2, djint(nk - 1)), tph1(nk - 1));
-    const double ubcb = xm(xm(-bz2, djint(nk - 1)), tph0(nk - 1));
+    const double hdzm_k = hdzmp(k, -1.), hdzp_k = hdzmp(k, 1.);
+    const double dji_k = A.djint(k), dji_1 = A.djint(k + 1);
+    const double t0k = A.tph0(k), t1k = A.tph1(k), t01 = A.tph0(k + 1), t11 = A.tph1(k + 1);
+    const double hdz_k = A.S(S_HDZ, k);
+    const double diffp = xm(xm(hdzm_k, dji_k), t0k);
+    const double diffq = -xa(xm(xm(hdzp_k, dji_1), t01), xm(xm(hdzm_k, dji_k), t1k));
+    const double diffr = xm(xm(hdzp_k, dji_1), t11);
+    const double wii = up(F.wi, k, nk, ld, col);
+    const double driftp = xm(xm(wii, 0.5), hdz_k);
+    const double driftq = xd(xm(-wii, 6.), C.re);
+    const double driftr = xm(xm(-wii, 0.5), hdz_k);
+    const double bu_k = A.S(S_BDOTU, k);
+    const double windp = k == 0 ? xm(xm(xm(bz, xs(xm(2., bu_k), A.S(S_BDOTU, 1))), 0.5), hdz_k)
+                                : xm(xm(xm(bz, A.S(S_BDOTU, k - 1)), 0.5), hdz_k);
+    const double windq = xm(xm(-bu_k, cc.dvbz), bz);
+    const double windr = k == nk - 2 ? xm(xm(xm(bz, xs(xm(2., bu_k), A.S(S_BDOTU, k - 1 >= 0 ? k - 1 : 0))), 0.5), hdz_k)
+                                     : xm(xm(xm(-bz, A.S(S_BDOTU, k + 1)), 0.5), hdz_k);
+    p = xa(xa(diffp, driftp), windp);
+    q = xs(xa(xa(diffq, driftq), windq), cc.dtn);
+    r = xa(xa(diffr, driftr), windr);
+    ex = xs(at(F.explicit_h, k), xm(xm(at(F.optm1_smooth2, k), C.dtx2inv), (double)C.nstep_sub));
+    if (k == nk - 2) {
+        q = xa(q, xm(xd(cc.ubcb, cc.ubca), r));
+        ex = xs(ex, xd(xm(cc.opflux, r), cc.ubca));
+        r = 0.;
+    }
+    q = xs(q, A.S(S_OL, k));
+    ex = xs(ex, A.S(S_PROD, k));
+    if (k == 0) {
+        q = xs(q, p);
+        ex = xs(ex, xd(xm(xm(2., p), at(F.qop, 0)), xs(xm(1.5, A.S(S_OL, 0)), xm(0.5, A.S(S_OL, 1)))));
+        p = 0.;
+    }
+}
+
+// Rows k = 0..nk-2 from the level planes, the forward sweep and the back
+// sweep of one column (oplus_ng.F90:88-99, 209-307).
+__device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusConsts &C, double *opout, const double *scr,
+                                           double *w2s, int T, int nk, long ld, long col, double *sys_out,
+                                           unsigned *status, const PostStep &post, int has_post, int pd)
+{
+    const long slab = (long)nk * ld;
+    OplusRowsAt A{scr, slab, ld, col, nk, 0., 0., 0.};
+    const OplusCol cc = oplus_col(F, C, A);
+    A.gmr = cc.gmr;
     bool ok = true;
     double w1 = 0., y1 = 0., w3 = 0., rprev = 0.;
-    // bring the lines row k+1 touches first (the planes at level k+2, the
-    // fields at k+1) into L1 while row k computes
-    auto pf = [&](const double *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); };
-    for (int k = 0; k < nk - 1; ++k) {
-        if (k + 1 < nk - 1) {
-            const long o1 = (long)(k + 1) * ld + col;
-            if (k + 2 < nk) {
+    // bring the lines row kk touches first (the planes at level kk+1, the
+    // fields at kk) into L1, pd rows ahead of the row that computes
+    auto pf_row = [&](int kk) {
+        const long o1 = (long)kk * ld + col;
+        if (kk + 1 < nk) {
 #pragma unroll
-                for (int e = 0; e < 4; ++e) pf(scr + (long)e * slab + o1 + ld);
-                pf(F.wi + o1 + ld);
-            }
-            pf(F.bdotdh_djbz + o1);
-            pf(F.explicit_h + o1);
-            pf(F.optm1_smooth2 + o1);
-            pf(scr + (long)S_OL * slab + o1);
-            pf(scr + (long)S_PROD * slab + o1);
+            for (int e = 0; e < 4; ++e) pf_l1(scr + (long)e * slab + o1 + ld);
+            pf_l1(F.wi + o1 + ld);
         }
-        const double hdzm_k = hdzmp(k, -1.), hdzp_k = hdzmp(k, 1.);
-        const double dji_k = djint(k), dji_1 = djint(k + 1);
-        const double t0k = tph0(k), t1k = tph1(k), t01 = tph0(k + 1), t11 = tph1(k + 1);
-        const double hdz_k = S(S_HDZ, k);
-        const double diffp = xm(xm(hdzm_k, dji_k), t0k);
-        const double diffq = -xa(xm(xm(hdzp_k, dji_1), t01), xm(xm(hdzm_k, dji_k), t1k));
-        const double diffr = xm(xm(hdzp_k, dji_1), t11);
-        const double wii = up(F.wi, k, nk, ld, col);
-        const double driftp = xm(xm(wii, 0.5), hdz_k);
-        const double driftq = xd(xm(-wii, 6.), C.re);
-        const double driftr = xm(xm(-wii, 0.5), hdz_k);
-        const double bu_k = S(S_BDOTU, k);
-        const double windp = k == 0 ? xm(xm(xm(bz, xs(xm(2., bu_k), S(S_BDOTU, 1))), 0.5), hdz_k)
-                                    : xm(xm(xm(bz, S(S_BDOTU, k - 1)), 0.5), hdz_k);
-        const double windq = xm(xm(-bu_k, dvbz), bz);
-        const double windr = k == nk - 2 ? xm(xm(xm(bz, xs(xm(2., bu_k), S(S_BDOTU, k - 1 >= 0 ? k - 1 : 0))), 0.5), hdz_k)
-                                         : xm(xm(xm(-bz, S(S_BDOTU, k + 1)), 0.5), hdz_k);
-        double p = xa(xa(diffp, driftp), windp);
-        double q = xs(xa(xa(diffq, driftq), windq), dtn);
-        double r = xa(xa(diffr, driftr), windr);
-        double ex = xs(at(F.explicit_h, k), xm(xm(at(F.optm1_smooth2, k), C.dtx2inv), (double)C.nstep_sub));
-        if (k == nk - 2) {
-            q = xa(q, xm(xd(ubcb, ubca), r));
-            ex = xs(ex, xd(xm(opflux, r), ubca));
-            r = 0.;
-        }
-        q = xs(q, S(S_OL, k));
-        ex = xs(ex, S(S_PROD, k));
-        if (k == 0) {
-            q = xs(q, p);
-            ex = xs(ex, xd(xm(xm(2., p), at(F.qop, 0)), xs(xm(1.5, S(S_OL, 0)), xm(0.5, S(S_OL, 1)))));
-            p = 0.;
-        }
+        pf_l1(F.bdotdh_djbz + o1);
+        pf_l1(F.explicit_h + o1);
+        pf_l1(F.optm1_smooth2 + o1);
+        pf_l1(scr + (long)S_OL * slab + o1);
+        pf_l1(scr + (long)S_PROD * slab + o1);
+    };
+    for (int kk = 1; kk < pd && kk < nk - 1; ++kk) pf_row(kk);
+    for (int k = 0; k < nk - 1; ++k) {
+        if (k + pd < nk - 1) pf_row(k + pd);
+        double p, q, r, ex;
+        oplus_row(F, C, A, cc, k, p, q, r, ex);
         if (sys_out) {
             const long o = (long)k * ld + col;
             sys_out[o] = p;
@@ -248,7 +294,9 @@ __device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusCons
     double xn = w3, xtop = w3;
     bool fin = fabs(xn) <= DBL_MAX;
     double park = K >= 2 ? opout[(long)(K - 2) * ld + col] : 0.;
+    for (int kk = K - 3; kk > K - 2 - pd && kk >= 0; --kk) post_prefetch(post, has_post, bcol, opout, (long)kk * ld + col);
     for (int k = K - 2; k >= 0; --k) {
+        if (k - pd >= 0) post_prefetch(post, has_post, bcol, opout, (long)(k - pd) * ld + col);
         const double wk = park;
         if (k >= 1) park = opout[(long)(k - 1) * ld + col];
         xn = xs(wk, xm(w2s[(long)k * T], xn));
@@ -265,13 +313,13 @@ __device__ __forceinline__ void oplus_walk(const OplusFields &F, const OplusCons
 __global__ void __launch_bounds__(128) k_oplus_ng(OplusFields F, OplusConsts C, double *opout, double *xiop2p,
                                                   double *xiop2d, double *Fe, double *Fn, double *scr, int nk,
                                                   int ncol, long ld, double *sys_out, unsigned *status,
-                                                  PostStep post, int has_post)
+                                                  PostStep post, int has_post, int pd)
 {
     extern __shared__ double smem_op[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
     for (int j = 0; j < nk; ++j) oplus_level(F, C, scr, xiop2p, xiop2d, Fe, Fn, nk, ld, col, j);
-    oplus_walk(F, C, opout, scr, smem_op + threadIdx.x, blockDim.x, nk, ld, col, sys_out, status, post, has_post);
+    oplus_walk(F, C, opout, scr, smem_op + threadIdx.x, blockDim.x, nk, ld, col, sys_out, status, post, has_post, pd);
 }
 
 // Two-pass form: the level quantities with one thread per (level, column),
@@ -286,12 +334,37 @@ __global__ void __launch_bounds__(128) k_oplus_levels(OplusFields F, OplusConsts
 
 __global__ void __launch_bounds__(128) k_oplus_rows(OplusFields F, OplusConsts C, double *opout, const double *scr,
                                                     int nk, int ncol, long ld, double *sys_out, unsigned *status,
-                                                    PostStep post, int has_post)
+                                                    PostStep post, int has_post, int pd)
 {
     extern __shared__ double smem_or[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
-    oplus_walk(F, C, opout, scr, smem_or + threadIdx.x, blockDim.x, nk, ld, col, sys_out, status, post, has_post);
+    oplus_walk(F, C, opout, scr, smem_or + threadIdx.x, blockDim.x, nk, ld, col, sys_out, status, post, has_post, pd);
+}
+
+// Three-pass form, pass 2: row k of every column, one thread per (row, column).
+__global__ void __launch_bounds__(128) k_oplus_coefs(OplusFields F, OplusConsts C, double *scr, int nk, int ncol,
+                                                     long ld, double *sys_out)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int k = blockIdx.y;
+    const long slab = (long)nk * ld, o = (long)k * ld + col;
+    OplusRowsAt A{scr, slab, ld, col, nk, 0., 0., 0.};
+    const OplusCol cc = oplus_col(F, C, A);
+    A.gmr = cc.gmr;
+    double p, q, r, ex;
+    oplus_row(F, C, A, cc, k, p, q, r, ex);
+    scr[S_P * slab + o] = p;
+    scr[S_Q * slab + o] = q;
+    scr[S_R * slab + o] = r;
+    scr[S_EX * slab + o] = ex;
+    if (sys_out) {
+        sys_out[o] = p;
+        sys_out[slab + o] = q;
+        sys_out[2 * slab + o] = r;
+        sys_out[3 * slab + o] = ex;
+    }
 }
 
 cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *opout, double *xiop2p,
@@ -311,15 +384,24 @@ cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *
     const size_t per = (size_t)(nk - 1) * sizeof(double);
     while (T > 32 && (size_t)T * per > (size_t)optin) T /= 2;
     if ((size_t)T * per > (size_t)optin) return cudaErrorInvalidValue;
-    if (assembly_mode() == 1) {
+    const int pd = walk_prefetch(ncol);
+    if (assembly_mode() == 2) {
+        const long slab = (long)nk * ld;
+        k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, xiop2p, xiop2d, Fe, Fn, scratch, nk, ncol,
+                                                                     ld);
+        k_oplus_coefs<<<dim3((ncol + 127) / 128, nk - 1), 128, 0, st>>>(F, C, scratch, nk, ncol, ld, sys_out);
+        return launch_thomas_post(scratch + S_P * slab, scratch + S_Q * slab, scratch + S_R * slab,
+                                  scratch + S_EX * slab, opout, nk, nk - 1, 1, ncol, ld, status, post, st);
+    }
+    if (assembly_mode() >= 1) {
         k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, xiop2p, xiop2d, Fe, Fn, scratch, nk, ncol,
                                                                      ld);
         k_oplus_rows<<<(ncol + T - 1) / T, T, (size_t)T * per, st>>>(F, C, opout, scratch, nk, ncol, ld, sys_out,
-                                                                     status, pv, hp);
+                                                                     status, pv, hp, pd);
         return cudaGetLastError();
     }
     k_oplus_ng<<<(ncol + T - 1) / T, T, (size_t)T * per, st>>>(F, C, opout, xiop2p, xiop2d, Fe, Fn, scratch, nk, ncol,
-                                                               ld, sys_out, status, pv, hp);
+                                                               ld, sys_out, status, pv, hp, pd);
     return cudaGetLastError();
 }
 

@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(128) k_settei_levels(SetteiFields F, SetteiCon
 // reciprocal and Markstein's correction (qdiv), the same bits as IEEE a/b.
 __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConsts C, const double *lv, double *te_out,
                                                      double *ti_out, double *qtotal, int nk, int ncol, long ld,
-                                                     double *sys_out, unsigned *status)
+                                                     double *sys_out, unsigned *status, int pd)
 {
     extern __shared__ double smem_tr[];
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -464,26 +464,30 @@ __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConst
     const double t_lbc = __ldg(F.t_lbc + col);
     // forward reads of level k into buffer b: 0 q_eni, 1 qtotal, 2 th(k+1),
     // 3 scht, 4 qe, 5 et, 6 dq, 7 len_tn, 8 lei_ti
-    auto issue = [&](int k, int b) {
+    auto reads = [&](int k, auto &&fn) {
         const long o = (long)k * ld + col;
-        sg.copy(b, 0, lv + P_QENI * slab + o);
-        if (k >= 1 && k <= nk - 2) sg.copy(b, 1, qtotal + o);
+        fn(0, lv + P_QENI * slab + o);
+        if (k >= 1 && k <= nk - 2) fn(1, qtotal + o);
         if (k <= nk - 2) {
-            sg.copy(b, 2, lv + P_TH * slab + o + ld);
-            sg.copy(b, 3, F.scht + o);
-            sg.copy(b, 4, lv + P_QE * slab + o);
-            if (C.et) sg.copy(b, 5, lv + P_ET * slab + o);
-            sg.copy(b, 6, lv + P_DQ * slab + o);
-            sg.copy(b, 7, lv + P_LENTN * slab + o);
-            sg.copy(b, 8, lv + P_LEITI * slab + o);
+            fn(2, lv + P_TH * slab + o + ld);
+            fn(3, F.scht + o);
+            fn(4, lv + P_QE * slab + o);
+            if (C.et) fn(5, lv + P_ET * slab + o);
+            fn(6, lv + P_DQ * slab + o);
+            fn(7, lv + P_LENTN * slab + o);
+            fn(8, lv + P_LEITI * slab + o);
         }
     };
+    auto issue = [&](int k, int b) { reads(k, [&](int v, const double *src) { sg.copy(b, v, src); }); };
+    auto prefetch = [&](int k) { reads(k, [](int, const double *src) { pf_l1(src); }); };
     double qe_m1 = 0., w1 = 0., y1 = 0., w3 = 0., rprev = 0.;
     double th_k = pl(P_TH, 0);
     bool ok = true;
     issue(0, 0);
     sg.commit();
+    for (int kk = 2; kk < pd + 1 && kk < nk; ++kk) prefetch(kk);
     for (int k = 0; k < nk; ++k) {
+        if (pd > 1 && k + 1 + pd < nk) prefetch(k + 1 + pd);
         if (k + 1 < nk) issue(k + 1, (k + 1) & 1);
         sg.commit();
         sg.wait_prev();
@@ -546,13 +550,19 @@ __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConst
     // (call i treats level lev(i)); te_out holds w3 until a level is final
     const int K = nk - 1;
     auto lev = [&](int i) { return i < K ? K - 1 - i : K; };
-    auto issue_b = [&](int i, int b) {
+    auto reads_b = [&](int i, auto &&fn) {
         const long o = (long)lev(i) * ld + col;
-        sg.copy(b, 0, F.tn + o);
-        sg.copy(b, 1, lv + P_LEI * slab + o);
-        sg.copy(b, 2, lv + P_LIN * slab + o);
-        sg.copy(b, 3, F.qji_ti + o);
-        sg.copy(b, 4, F.xnmbar + o);
+        fn(0, F.tn + o);
+        fn(1, lv + P_LEI * slab + o);
+        fn(2, lv + P_LIN * slab + o);
+        fn(3, F.qji_ti + o);
+        fn(4, F.xnmbar + o);
+    };
+    auto issue_b = [&](int i, int b) { reads_b(i, [&](int v, const double *src) { sg.copy(b, v, src); }); };
+    // with the parked forward result of the level after
+    auto prefetch_b = [&](int i) {
+        reads_b(i, [](int, const double *src) { pf_l1(src); });
+        if (lev(i) >= 1 && i < K) pf_l1(te_out + (long)(lev(i) - 1) * ld + col);
     };
     double xn = w3;
     double tk = pow(xn, xd(2., 7.));
@@ -561,7 +571,9 @@ __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConst
     double park = K >= 2 ? te_out[(long)(K - 2) * ld + col] : 0.;
     issue_b(0, 0);
     sg.commit();
+    for (int ii = 2; ii < pd + 1 && ii <= K; ++ii) prefetch_b(ii);
     for (int i = 0; i <= K; ++i) {
+        if (pd > 1 && i + 1 + pd <= K) prefetch_b(i + 1 + pd);
         if (i + 1 <= K) issue_b(i + 1, (i + 1) & 1);
         sg.commit();
         sg.wait_prev();
@@ -609,13 +621,14 @@ cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, doubl
     const size_t per = (size_t)(2 * nk - 1) * sizeof(double);
     while (T > 32 && (size_t)T * per > (size_t)optin) T /= 2;
     if ((size_t)T * per > (size_t)optin) return cudaErrorInvalidValue;
-    if (scratch && assembly_mode() == 1) {
+    if (scratch && assembly_mode() >= 1) {
         int T2 = 128;
         const size_t per2 = (size_t)(nk - 1) * sizeof(double) + Stage<kSetteiStaged>::bytes_per_thread;
         while (T2 > 32 && (size_t)T2 * per2 > (size_t)optin) T2 /= 2;
         k_settei_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch, nk, ncol, ld);
         k_settei_rows<<<(ncol + T2 - 1) / T2, T2, (size_t)T2 * per2, st>>>(F, C, scratch, te_out, ti_out, qtotal, nk,
-                                                                           ncol, ld, sys_out, status);
+                                                                           ncol, ld, sys_out, status,
+                                                                           walk_prefetch(ncol));
         return cudaGetLastError();
     }
     k_settei_ng<<<(ncol + T - 1) / T, T, (size_t)T * per, st>>>(F, C, te_out, ti_out, qtotal, nk, ncol, ld, sys_out,

@@ -1,0 +1,185 @@
+// The column walk of the three-pass assembly routines: the Thomas solve
+// (src/trsolv_ng.F90:14-26) of rows already formed by a level-parallel pass,
+// stored through the routines' post-solve steps.
+//
+// In the two-pass form each walk forms its rows as it goes (hundreds of
+// dependent instructions per level, one thread per column); with few columns
+// per SM every level then waits on its own instruction latencies.  Here the
+// rows come from planes p, q, r, f (level-major, k*ld + col) that one thread
+// per (level, column) wrote, so a walk level is the recurrence alone: two
+// divisions sharing one correctly rounded reciprocal (qdiv), a product and a
+// difference, with the planes requested pd levels ahead.
+//
+//   top = 0 (minor_ng): rows 0..K-1 with K = nk, no extrapolation;
+//   top = 1 (dt_ng, oplus_ng): rows 0..K-1 with K = nk-1 and
+//         x(nk-1) = x(nk-2)**2/x(nk-3) from the unfiltered values
+//         (dt_ng.F90:167, oplus_ng.F90:307).
+// With a PostStep every row is stored through post_store: the lateral
+// boundary overwrite, the time filter and the floors.  Same operations in the
+// same order as the fused walks, so the same bits.
+#include <cfloat>
+
+#include "tg_internal.h"
+#include "tg_arith.cuh"
+
+namespace tg {
+namespace {
+__device__ __forceinline__ double xm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xs(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xd(double a, double b) { return __ddiv_rn(a, b); }
+
+constexpr int kWalkThreads = 32;   // one warp per block: the walk's columns spread over every SM
+
+__global__ void __launch_bounds__(kWalkThreads) k_thomas_post(const double *P, const double *Q, const double *R,
+                                                              const double *Fv, double *x, int nk, int K, int top,
+                                                              int ncol, long ld, unsigned *status, PostStep post,
+                                                              int has_post, int pd)
+{
+    extern __shared__ double w2_walk[];
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int T = blockDim.x;
+    double *w2s = w2_walk + threadIdx.x;
+    auto pf_row = [&](int k) {
+        const long o = (long)k * ld + col;
+        pf_l1(P + o);
+        pf_l1(Q + o);
+        pf_l1(R + o);
+        pf_l1(Fv + o);
+    };
+    for (int kk = 1; kk < pd && kk < K; ++kk) pf_row(kk);
+    bool ok = true;
+    double w1 = 0.0, y1 = 0.0, w3 = 0.0, rprev = 0.0;
+    for (int k = 0; k < K; ++k) {
+        if (k + pd < K) pf_row(k + pd);
+        const long o = (long)k * ld + col;
+        const double p = P[o], q = Q[o], r = R[o], f = Fv[o];
+        if (k == 0) {
+            w1 = q;
+            y1 = __drcp_rn(w1);
+            w3 = qdiv(f, w1, y1);
+        } else {
+            const double w2 = qdiv(rprev, w1, y1);
+            w2s[(long)(k - 1) * T] = w2;
+            w1 = xs(q, xm(p, w2));
+            y1 = __drcp_rn(w1);
+            w3 = qdiv(xs(f, xm(p, w3)), w1, y1);
+        }
+        ok = ok && fabs(w1) <= DBL_MAX && w1 != 0.0;
+        x[o] = w3;
+        rprev = r;
+    }
+    const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
+    double xn = w3;
+    const double xtop = w3;
+    bool fin = fabs(xn) <= DBL_MAX;
+    double park = K >= 2 ? x[(long)(K - 2) * ld + col] : 0.0;
+    if (top == 0 && has_post) post_store(post, true, bcol, x, (long)(K - 1) * ld + col, xn);
+    for (int kk = K - 3; kk > K - 2 - pd && kk >= 0; --kk) post_prefetch(post, has_post, bcol, x, (long)kk * ld + col);
+    for (int k = K - 2; k >= 0; --k) {
+        if (k - pd >= 0) post_prefetch(post, has_post, bcol, x, (long)(k - pd) * ld + col);
+        const double wk = park;
+        if (k >= 1) park = x[(long)(k - 1) * ld + col];
+        xn = xs(wk, xm(w2s[(long)k * T], xn));
+        fin = fin && fabs(xn) <= DBL_MAX;
+        post_store(post, has_post, bcol, x, (long)k * ld + col, xn);
+        if (top == 1 && k == K - 2) {
+            // xtop = x(K-1), xn = x(K-2): the two top solved rows
+            post_store(post, has_post, bcol, x, (long)K * ld + col, xd(xm(xtop, xtop), xn));
+            if (has_post) post_store(post, true, bcol, x, (long)(K - 1) * ld + col, xtop);
+        }
+    }
+    if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+}
+// The same walk with the column tile held in shared memory, for launches of
+// few columns: a warp first copies the p, q, r, f rows of all its levels
+// (cp.async, every copy in flight at once), then runs the recurrence from
+// shared memory, keeping w2 where r(k-1) was and the parked w3 where q(k)
+// was; the back sweep leaves the solution there too, and the post-solve
+// stores, independent of one another, go out last.
+__global__ void __launch_bounds__(kWalkThreads) k_thomas_post_tile(const double *P, const double *Q, const double *R,
+                                                                   const double *Fv, double *x, int nk, int K,
+                                                                   int top, int ncol, long ld, unsigned *status,
+                                                                   PostStep post, int has_post)
+{
+    extern __shared__ double tile_walk[];
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int T = kWalkThreads, t = threadIdx.x;
+    double *sp = tile_walk, *sq = sp + (long)K * T, *sr = sq + (long)K * T, *sf = sr + (long)K * T;
+    auto cp8 = [](double *dst, const double *src) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                     "l"(src)
+                     : "memory");
+    };
+    for (int k = 0; k < K; ++k) {
+        const long o = (long)k * ld + col;
+        const int s = k * T + t;
+        cp8(sp + s, P + o);
+        cp8(sq + s, Q + o);
+        cp8(sr + s, R + o);
+        cp8(sf + s, Fv + o);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    bool ok = true;
+    double w1 = 0.0, y1 = 0.0, w3 = 0.0;
+    for (int k = 0; k < K; ++k) {
+        const int s = k * T + t;
+        const double p = sp[s], q = sq[s], f = sf[s];
+        if (k == 0) {
+            w1 = q;
+            y1 = __drcp_rn(w1);
+            w3 = qdiv(f, w1, y1);
+        } else {
+            const double w2 = qdiv(sr[s - T], w1, y1);
+            sr[s - T] = w2;
+            w1 = xs(q, xm(p, w2));
+            y1 = __drcp_rn(w1);
+            w3 = qdiv(xs(f, xm(p, w3)), w1, y1);
+        }
+        ok = ok && fabs(w1) <= DBL_MAX && w1 != 0.0;
+        sq[s] = w3;
+    }
+    double xn = w3;
+    const double xtop = w3;
+    bool fin = fabs(xn) <= DBL_MAX;
+    for (int k = K - 2; k >= 0; --k) {
+        const int s = k * T + t;
+        xn = xs(sq[s], xm(sr[s], xn));
+        fin = fin && fabs(xn) <= DBL_MAX;
+        sq[s] = xn;
+    }
+    const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
+#pragma unroll 4
+    for (int k = 0; k < K; ++k) post_store(post, has_post, bcol, x, (long)k * ld + col, sq[k * T + t]);
+    // x(nk-1) = x(nk-2)**2/x(nk-3) from the unfiltered values
+    if (top == 1) post_store(post, has_post, bcol, x, (long)K * ld + col, xd(xm(xtop, xtop), sq[(K - 2) * T + t]));
+    if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+}
+}  // namespace
+
+cudaError_t launch_thomas_post(const double *p, const double *q, const double *r, const double *f, double *x, int nk,
+                               int K, int top, int ncol, long ld, unsigned *status, const PostStep *post,
+                               cudaStream_t st)
+{
+    if (ncol <= 0) return cudaSuccess;
+    if (K < 1 || K > nk || (top == 1 && (K != nk - 1 || K < 2))) return cudaErrorInvalidValue;
+    const size_t tile = (size_t)kWalkThreads * 4 * K * sizeof(double);
+    if (ncol <= kSmallWalkColumns && tile <= (size_t)smem_optin()) {
+        once_per_device([] {
+            cudaFuncSetAttribute(k_thomas_post_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
+        });
+        k_thomas_post_tile<<<(ncol + kWalkThreads - 1) / kWalkThreads, kWalkThreads, tile, st>>>(
+            p, q, r, f, x, nk, K, top, ncol, ld, status, post ? *post : PostStep{}, post != nullptr);
+        return cudaGetLastError();
+    }
+    const size_t smem = (size_t)kWalkThreads * (K > 1 ? K - 1 : 1) * sizeof(double);
+    once_per_device([] { cudaFuncSetAttribute(k_thomas_post, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin()); });
+    if (smem > (size_t)smem_optin()) return cudaErrorInvalidValue;
+    k_thomas_post<<<(ncol + kWalkThreads - 1) / kWalkThreads, kWalkThreads, smem, st>>>(
+        p, q, r, f, x, nk, K, top, ncol, ld, status, post ? *post : PostStep{}, post != nullptr,
+        walk_prefetch(ncol));
+    return cudaGetLastError();
+}
+}  // namespace tg
