@@ -511,6 +511,27 @@ int tg_oplus_ng_post_dev(const tg_oplus_fields *F, const tg_oplus_consts *C, dou
                          double *xiop2d, double *Fe, double *Fn, int nk, int ncol, long ld, const tg_post_step *P,
                          int *status_dev, void *stream);
 
+/* The O+ sub-cycle (src/dynamics_ng.F90:103-117): oplus_ng runs nstep_sub
+ * times on the same fields, and only op, optm1 (hence optm1_smooth2) and the
+ * horizontal terms explicit_h change from one sub-step to the next.  They
+ * enter the right-hand side alone, so the rows p, q, r and the forward
+ * elimination's pivots are the same in every sub-step:
+ *   tg_oplus_ng_factor_dev  forms them once per step into `factor` (device
+ *                           memory of tg_oplus_ng_factor_doubles(nk, ld)
+ *                           doubles, owned by the caller), with xiop2p and
+ *                           xiop2d; status TG_EPIVOT for a zero pivot;
+ *   tg_oplus_ng_solve_dev   one sub-step: opout from the factor and F's
+ *                           current explicit_h and optm1_smooth2 (the other
+ *                           fields must be those the factor was formed from),
+ *                           with the post-solve steps when P is not NULL.
+ * Each sub-step's opout is bit-identical to tg_oplus_ng_dev /
+ * tg_oplus_ng_post_dev on the same fields. */
+long tg_oplus_ng_factor_doubles(int nk, long ld);
+int tg_oplus_ng_factor_dev(const tg_oplus_fields *F, const tg_oplus_consts *C, double *xiop2p, double *xiop2d,
+                           double *factor, int nk, int ncol, long ld, int *status_dev, void *stream);
+int tg_oplus_ng_solve_dev(const tg_oplus_fields *F, const tg_oplus_consts *C, const double *factor, double *opout,
+                          int nk, int ncol, long ld, const tg_post_step *P, int *status_dev, void *stream);
+
 /* ---- batched, GPU-resident plans ---------------------------------------------
  * A plan solves many independent systems ("segments": any mix of grids, nest
  * levels, sub-steps and species) in one persistent launch per system kind,

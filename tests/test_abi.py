@@ -10,7 +10,7 @@ from conftest import ROOT
 
 def header_functions():
     txt = open(os.path.join(ROOT, "include", "tg_colsolve.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char \*)\s*(tg_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long|const char \*)\s*(tg_\w+)\s*\(", txt, re.M)))
 
 
 def test_header_lists_every_export(pkg):

@@ -192,3 +192,47 @@ def test_comp_three_pass_gives_the_two_pass_bits(cuda, pkg, ncol, calc_helium):
             pkg.set_assembly_mode(-1)
     assert torch.equal(got[1][0], got[2][0])
     assert torch.equal(got[1][1], got[2][1])
+
+
+@pytest.mark.parametrize("ncol", [1500, 17000], ids=["tile", "global_reads"])
+def test_oplus_factor_and_solve_give_the_full_step_bits(cuda, pkg, ncol):
+    """The O+ sub-cycle: the rows and pivots formed once, then three sub-steps
+    with new explicit_h, optm1_smooth2 and op each, with and without the
+    post-solve steps, give tg_oplus_ng_dev / tg_oplus_ng_post_dev's bits."""
+    torch = cuda
+    nk, dz = 57, 0.25
+    F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 41, nstep_sub=3)
+    dev, ld = _level(pkg, torch, F, nk, ncol, ("zpint",))
+    z = lambda: torch.zeros((nk, ld), dtype=torch.float64, device="cuda")  # noqa: E731
+    factor = torch.zeros(pkg.oplus_ng_factor_doubles(nk, ld), dtype=torch.float64, device="cuda")
+    x2p, x2d = z(), z()
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pkg.oplus_ng_factor_dev(dev, C, x2p, x2d, factor, nk, ncol, ld, status=st)
+    torch.cuda.synchronize()
+    assert int(st.item()) == pkg.TG_OK
+    g = torch.Generator(device="cuda").manual_seed(5)
+    op = dev["op"]
+    for sub in range(3):
+        d = dict(dev, op=op)
+        d["explicit_h"] = dev["explicit_h"] * (1.0 + 0.1 * torch.rand((nk, ld), dtype=torch.float64, device="cuda",
+                                                                          generator=g))
+        d["optm1_smooth2"] = op * (0.99 + 0.02 * torch.rand((nk, ld), dtype=torch.float64, device="cuda", generator=g))
+        prev, bnd, mask, _ = _post_inputs(torch, op, nk, ncol, ld, 10 + sub, 0.0, 1e6, False)
+        want = [z() for _ in range(3)]
+        pkg.oplus_ng_dev(d, C, want[0], want[1], want[2], nk, ncol, ld)
+        got = z()
+        pkg.oplus_ng_solve_dev(d, C, factor, got, nk, ncol, ld, status=st)
+        nm_w, nm_g = z(), z()
+        post_w = dict(cur=op, prev=prev, nm_upd=nm_w, bnd_mask=mask, bnd=bnd, dtsmooth=0.9, dtsmooth_div2=0.05)
+        post_g = dict(post_w, nm_upd=nm_g)
+        want_p = [z() for _ in range(3)]
+        pkg.oplus_ng_post_dev(d, C, want_p[0], want_p[1], want_p[2], nk, ncol, ld, post_w)
+        got_p = z()
+        pkg.oplus_ng_solve_dev(d, C, factor, got_p, nk, ncol, ld, post=post_g, status=st)
+        torch.cuda.synchronize()
+        assert int(st.item()) == pkg.TG_OK
+        assert torch.equal(got[:, :ncol], want[0][:, :ncol]), sub
+        assert torch.equal(got_p[:, :ncol], want_p[0][:, :ncol]), sub
+        assert torch.equal(nm_g[:, :ncol], nm_w[:, :ncol]), sub
+        assert torch.equal(x2p[:, :ncol], want[1][:, :ncol]) and torch.equal(x2d[:, :ncol], want[2][:, :ncol])
+        op = got_p

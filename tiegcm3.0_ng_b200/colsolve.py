@@ -39,7 +39,7 @@ LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
 EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor_ng_dev", "tg_comp_ng",
-           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_comp_post_ng_dev", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_advec_ng", "tg_advec_ng_dev", "tg_smooth_ng", "tg_smooth_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
+           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_comp_post_ng_dev", "tg_oplus_ng_factor_doubles", "tg_oplus_ng_factor_dev", "tg_oplus_ng_solve_dev", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_advec_ng", "tg_advec_ng_dev", "tg_smooth_ng", "tg_smooth_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_column_residency", "tg_set_assembly_mode", "tg_set_walk_prefetch", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
@@ -212,6 +212,11 @@ def lib():
             "tg_comp_ng_dev": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, I, I, Lg, P, P, P],
             "tg_comp_post_ng": [P] * 8 + [D, D, D, I, I] + [P] * 6,
             "tg_comp_post_ng_dev": [P] * 8 + [D, D, D, I, I, Lg] + [P] * 11,
+            "tg_oplus_ng_factor_doubles": [I, Lg],
+            "tg_oplus_ng_factor_dev": [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), P, P, P, I, I, Lg, P,
+                                       P],
+            "tg_oplus_ng_solve_dev": [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), P, P, I, I, Lg,
+                                      ctypes.POINTER(PostStepArgs), P, P],
             "tg_time_filter_ng": [I, P, P, D, D, I, I, P, P],
             "tg_time_filter_ng_dev": [I, P, P, D, D, I, I, Lg, P, P, P],
             "tg_advec_ng": [P, P, P, P, D, D, D, I, I, I, P],
@@ -279,6 +284,7 @@ def lib():
             fn.argtypes = args
             fn.restype = I
         L.tg_version.restype = ctypes.c_char_p
+        L.tg_oplus_ng_factor_doubles.restype = Lg
         L.tg_last_error.restype = ctypes.c_char_p
         _lib = L
     return _lib
@@ -667,6 +673,32 @@ def oplus_ng_post_dev(fields, consts, opout, xiop2p, xiop2d, nk, ncol, ld, post,
                                     _dptr(Fe), _dptr(Fn), nk, ncol, ld, ctypes.byref(Pp),
                                     None if status is None else _int_dptr(status), _stream(stream))
     return _check(rc, "tg_oplus_ng_post_dev", numeric_ok=False)
+
+
+def oplus_ng_factor_doubles(nk, ld):
+    """Doubles of the factor buffer tg_oplus_ng_factor_dev fills."""
+    return int(lib().tg_oplus_ng_factor_doubles(int(nk), int(ld)))
+
+
+def oplus_ng_factor_dev(fields, consts, xiop2p, xiop2d, factor, nk, ncol, ld, status=None, stream=None):
+    """The O+ sub-cycle's rows and pivots, once per step, into factor (a float64
+    CUDA tensor of oplus_ng_factor_doubles(nk, ld) elements)."""
+    F = OplusFields(*[_dptr(fields[n]) for n in OPLUS_FIELDS])
+    C = oplus_consts(consts)
+    rc = lib().tg_oplus_ng_factor_dev(ctypes.byref(F), ctypes.byref(C), _dptr(xiop2p), _dptr(xiop2d), _dptr(factor),
+                                      nk, ncol, ld, None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_oplus_ng_factor_dev", numeric_ok=False)
+
+
+def oplus_ng_solve_dev(fields, consts, factor, opout, nk, ncol, ld, post=None, status=None, stream=None):
+    """One O+ sub-step from the factor with fields' current explicit_h and
+    optm1_smooth2; post (as for oplus_ng_post_dev) fuses the post-solve steps."""
+    F = OplusFields(*[_dptr(fields[n]) for n in OPLUS_FIELDS])
+    C = oplus_consts(consts)
+    Pp = None if post is None else ctypes.byref(_post(post))
+    rc = lib().tg_oplus_ng_solve_dev(ctypes.byref(F), ctypes.byref(C), _dptr(factor), _dptr(opout), nk, ncol, ld,
+                                     Pp, None if status is None else _int_dptr(status), _stream(stream))
+    return _check(rc, "tg_oplus_ng_solve_dev", numeric_ok=False)
 
 
 def settei_ng_dev(fields, consts, te_out, ti_out, qtotal, nk, ncol, ld, system_out=None, status=None, stream=None):

@@ -1800,6 +1800,67 @@ __attribute__((visibility("default"))) int tg_oplus_ng_post_dev(const tg_oplus_f
     return TG_OK;
 }
 
+__attribute__((visibility("default"))) long tg_oplus_ng_factor_doubles(int nk, long ld)
+{
+    return nk < 3 || ld < 1 ? 0 : (long)oplus_scratch_planes() * nk * ld;
+}
+
+__attribute__((visibility("default"))) int tg_oplus_ng_factor_dev(const tg_oplus_fields *F, const tg_oplus_consts *C,
+                                                                  double *xiop2p, double *xiop2d, double *factor,
+                                                                  int nk, int ncol, long ld, int *status_dev,
+                                                                  void *stream)
+{
+    if (!F || !C || !xiop2p || !xiop2d || !factor || nk < 3 || ncol < 0 || ld < ncol || !oplus_fields_ok(F)) {
+        set_err("tg_oplus_ng_factor_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    TG_CUDA(launch_oplus_factor(*F, *C, xiop2p, xiop2d, factor, nk, ncol, ld, ws->flags, st));
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_oplus_ng_solve_dev(const tg_oplus_fields *F, const tg_oplus_consts *C,
+                                                                 const double *factor, double *opout, int nk,
+                                                                 int ncol, long ld, const tg_post_step *P,
+                                                                 int *status_dev, void *stream)
+{
+    if (!F || !C || !factor || !opout || nk < 3 || ncol < 0 || ld < ncol || !oplus_fields_ok(F) ||
+        (P && !post_ok("tg_oplus_ng_solve_dev", P))) {
+        if (!P || P->cur) set_err("tg_oplus_ng_solve_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    if (P) {
+        const PostStep post = post_of(P, 0.0, 1);
+        TG_CUDA(launch_oplus_solve(*F, *C, factor, opout, nk, ncol, ld, ws->flags, st, &post));
+    } else {
+        TG_CUDA(launch_oplus_solve(*F, *C, factor, opout, nk, ncol, ld, ws->flags, st, nullptr));
+    }
+    if (status_dev) {
+        k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
+        TG_CUDA(cudaGetLastError());
+    }
+    return TG_OK;
+}
+
 __attribute__((visibility("default"))) int tg_oplus_ng(const tg_oplus_fields *F, const tg_oplus_consts *C,
                                                        double *opout, double *xiop2p, double *xiop2d, double *Fe,
                                                        double *Fn, int nk, int ncol)

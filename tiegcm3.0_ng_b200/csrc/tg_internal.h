@@ -257,6 +257,13 @@ typedef tg_oplus_consts OplusConsts;
 cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *opout, double *xiop2p,
                             double *xiop2d, double *Fe, double *Fn, double *scratch, int nk, int ncol, long ld,
                             double *sys_out, unsigned *status, cudaStream_t st, const PostStep *post = nullptr);
+// The O+ sub-cycle (tg_oplus.cu): the factorization of one step's rows into
+// `factor` (oplus_scratch_planes() planes of nk*ld), then one sub-step's
+// solve from it with that sub-step's optm1_smooth2 and explicit_h.
+cudaError_t launch_oplus_factor(const OplusFields &F, const OplusConsts &C, double *xiop2p, double *xiop2d,
+                                double *factor, int nk, int ncol, long ld, unsigned *status, cudaStream_t st);
+cudaError_t launch_oplus_solve(const OplusFields &F, const OplusConsts &C, const double *factor, double *opout, int nk,
+                               int ncol, long ld, unsigned *status, cudaStream_t st, const PostStep *post = nullptr);
 int oplus_scratch_planes();   // level-major scratch planes of launch_oplus_ng (each nk*ld doubles)
 
 // Polar ring filter (tg_filter.cu): the latitudes it filters, with their

@@ -29,7 +29,10 @@ __device__ __forceinline__ double xd(double a, double b) { return __ddiv_rn(a, b
 
 // scratch planes, level-major: the level quantities, then the rows of the
 // three-pass form
-enum { S_DJ = 0, S_HDZ, S_TP1, S_BDOTU, S_OL, S_PROD, S_P, S_Q, S_R, S_EX, S_N };
+// three-pass form, then the factorization the sub-step solves reuse (w1,
+// 1/w1, w2 per row; the boundary terms of the right-hand side in rows 0 and 1
+// of S_TB)
+enum { S_DJ = 0, S_HDZ, S_TP1, S_BDOTU, S_OL, S_PROD, S_P, S_Q, S_R, S_EX, S_W1, S_Y1, S_W2, S_TB, S_N };
 
 // interface value at j of a(j), a(j+1): .5*(a(j)+a(j+1)); at the top
 // 1.5*a(nk)-.5*a(nk-1)
@@ -185,8 +188,11 @@ __device__ __forceinline__ OplusCol oplus_col(const OplusFields &F, const OplusC
 
 // Row k (0..nk-2) of the O+ system: p, q, r and the right-hand side, with
 // both boundary folds (oplus_ng.F90:255-303).
+// t_top and t_bot receive the boundary terms the right-hand side takes at
+// k = nk-2 and k = 0 (when given).
 __device__ __forceinline__ void oplus_row(const OplusFields &F, const OplusConsts &C, const OplusRowsAt &A,
-                                          const OplusCol &cc, int k, double &p, double &q, double &r, double &ex)
+                                          const OplusCol &cc, int k, double &p, double &q, double &r, double &ex,
+                                          double *t_top = nullptr, double *t_bot = nullptr)
 {
     const int nk = A.nk;
     const long ld = A.ld, col = A.col;
@@ -220,14 +226,18 @@ __device__ __forceinline__ void oplus_row(const OplusFields &F, const OplusConst
     ex = xs(at(F.explicit_h, k), xm(xm(at(F.optm1_smooth2, k), C.dtx2inv), (double)C.nstep_sub));
     if (k == nk - 2) {
         q = xa(q, xm(xd(cc.ubcb, cc.ubca), r));
-        ex = xs(ex, xd(xm(cc.opflux, r), cc.ubca));
+        const double tt = xd(xm(cc.opflux, r), cc.ubca);
+        if (t_top) *t_top = tt;
+        ex = xs(ex, tt);
         r = 0.;
     }
     q = xs(q, A.S(S_OL, k));
     ex = xs(ex, A.S(S_PROD, k));
     if (k == 0) {
         q = xs(q, p);
-        ex = xs(ex, xd(xm(xm(2., p), at(F.qop, 0)), xs(xm(1.5, A.S(S_OL, 0)), xm(0.5, A.S(S_OL, 1)))));
+        const double tb = xd(xm(xm(2., p), at(F.qop, 0)), xs(xm(1.5, A.S(S_OL, 0)), xm(0.5, A.S(S_OL, 1))));
+        if (t_bot) *t_bot = tb;
+        ex = xs(ex, tb);
         p = 0.;
     }
 }
@@ -353,8 +363,10 @@ __global__ void __launch_bounds__(128) k_oplus_coefs(OplusFields F, OplusConsts 
     OplusRowsAt A{scr, slab, ld, col, nk, 0., 0., 0.};
     const OplusCol cc = oplus_col(F, C, A);
     A.gmr = cc.gmr;
-    double p, q, r, ex;
-    oplus_row(F, C, A, cc, k, p, q, r, ex);
+    double p, q, r, ex, t_top = 0., t_bot = 0.;
+    oplus_row(F, C, A, cc, k, p, q, r, ex, &t_top, &t_bot);
+    if (k == nk - 2) scr[S_TB * slab + col] = t_top;
+    if (k == 0) scr[S_TB * slab + ld + col] = t_bot;
     scr[S_P * slab + o] = p;
     scr[S_Q * slab + o] = q;
     scr[S_R * slab + o] = r;
@@ -365,6 +377,210 @@ __global__ void __launch_bounds__(128) k_oplus_coefs(OplusFields F, OplusConsts 
         sys_out[2 * slab + o] = r;
         sys_out[3 * slab + o] = ex;
     }
+}
+
+// ---- the O+ sub-cycle: factor once, solve every sub-step -------------------
+// Within one model step oplus_ng runs nstep_sub times (dynamics_ng.F90:103-
+// 117) on the same fields; only op, optm1 (smoothed into optm1_smooth2) and
+// the horizontal terms (explicit_h) change, and they enter the right-hand
+// side alone.  The rows p, q, r and the forward elimination's w1, 1/w1 and w2
+// are therefore the same in every sub-step: the factor pass forms them once,
+// and each sub-step's solve runs the remaining recurrence w3 = (ex - p*w3)/w1
+// (qdiv with the stored reciprocal) and the back sweep.  The operations and
+// their order are those of the full walk, so the bits are too.
+
+// Pass 3 of the factorization: w1, 1/w1 and w2 of every row, one column per
+// thread.
+__global__ void __launch_bounds__(32) k_oplus_factor(double *scr, int nk, int ncol, long ld, unsigned *status, int pd)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const long slab = (long)nk * ld;
+    const int K = nk - 1;
+    const double *P = scr + S_P * slab, *Q = scr + S_Q * slab, *R = scr + S_R * slab;
+    double *W1 = scr + S_W1 * slab, *Y1 = scr + S_Y1 * slab, *W2 = scr + S_W2 * slab;
+    auto pf_row = [&](int k) {
+        const long o = (long)k * ld + col;
+        pf_l1(P + o);
+        pf_l1(Q + o);
+        pf_l1(R + o);
+    };
+    for (int kk = 1; kk < pd && kk < K; ++kk) pf_row(kk);
+    bool ok = true;
+    double w1 = 0., y1 = 0., rprev = 0.;
+    for (int k = 0; k < K; ++k) {
+        if (k + pd < K) pf_row(k + pd);
+        const long o = (long)k * ld + col;
+        const double q = Q[o];
+        if (k == 0) {
+            w1 = q;
+        } else {
+            const double w2 = qdiv(rprev, w1, y1);
+            W2[o - ld] = w2;
+            w1 = xs(q, xm(P[o], w2));
+        }
+        y1 = __drcp_rn(w1);
+        ok = ok && fabs(w1) <= DBL_MAX && w1 != 0.0;
+        W1[o] = w1;
+        Y1[o] = y1;
+        rprev = R[o];
+    }
+    if (status && !ok) atomicOr(status, FLAG_PIVOT);
+}
+
+// One sub-step's solve with the column tile in shared memory: p, w1, 1/w1,
+// w2 and the three right-hand-side inputs of every level copied at once
+// (cp.async), ex formed level by level as oplus_row forms it, the forward
+// recurrence, the back sweep, and the post-solve stores last.
+constexpr int kSolveThreads = 32;
+__global__ void __launch_bounds__(kSolveThreads) k_oplus_solve_tile(OplusFields F, OplusConsts C, const double *scr,
+                                                                    double *opout, int nk, int ncol, long ld,
+                                                                    unsigned *status, PostStep post, int has_post)
+{
+    extern __shared__ double solve_tile[];
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int T = kSolveThreads, t = threadIdx.x, K = nk - 1;
+    const long slab = (long)nk * ld;
+    double *sp = solve_tile, *sw1 = sp + (long)K * T, *sy1 = sw1 + (long)K * T, *sw2 = sy1 + (long)K * T;
+    double *sxh = sw2 + (long)K * T, *som = sxh + (long)K * T, *spr = som + (long)K * T;
+    auto cp8 = [](double *dst, const double *src) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                     "l"(src)
+                     : "memory");
+    };
+    for (int k = 0; k < K; ++k) {
+        const long o = (long)k * ld + col;
+        const int s = k * T + t;
+        cp8(sp + s, scr + S_P * slab + o);
+        cp8(sw1 + s, scr + S_W1 * slab + o);
+        cp8(sy1 + s, scr + S_Y1 * slab + o);
+        cp8(sw2 + s, scr + S_W2 * slab + o);
+        cp8(sxh + s, F.explicit_h + o);
+        cp8(som + s, F.optm1_smooth2 + o);
+        cp8(spr + s, scr + S_PROD * slab + o);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    const double t_top = scr[S_TB * slab + col], t_bot = scr[S_TB * slab + ld + col];
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    double w3 = 0.;
+    for (int k = 0; k < K; ++k) {
+        const int s = k * T + t;
+        double ex = xs(sxh[s], xm(xm(som[s], C.dtx2inv), (double)C.nstep_sub));
+        if (k == nk - 2) ex = xs(ex, t_top);
+        ex = xs(ex, spr[s]);
+        if (k == 0) {
+            ex = xs(ex, t_bot);
+            w3 = qdiv(ex, sw1[s], sy1[s]);
+        } else {
+            w3 = qdiv(xs(ex, xm(sp[s], w3)), sw1[s], sy1[s]);
+        }
+        som[s] = w3;
+    }
+    double xn = w3;
+    const double xtop = w3;
+    bool fin = fabs(xn) <= DBL_MAX;
+    for (int k = K - 2; k >= 0; --k) {
+        const int s = k * T + t;
+        xn = xs(som[s], xm(sw2[s], xn));
+        fin = fin && fabs(xn) <= DBL_MAX;
+        som[s] = xn;
+    }
+    const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
+#pragma unroll 4
+    for (int k = 0; k < K; ++k) post_store(post, has_post, bcol, opout, (long)k * ld + col, som[k * T + t]);
+    // opout(nk) = opout(nk-1)**2/opout(nk-2) from the unfiltered values (oplus_ng.F90:307)
+    post_store(post, has_post, bcol, opout, (long)K * ld + col, xd(xm(xtop, xtop), som[(K - 2) * T + t]));
+    if (status && !fin) atomicOr(status, FLAG_NONFINITE);
+}
+
+// The same solve reading the rows from global memory (launches too large for
+// the shared-memory tile), pd levels requested ahead.
+__global__ void __launch_bounds__(kSolveThreads) k_oplus_solve(OplusFields F, OplusConsts C, const double *scr,
+                                                               double *opout, int nk, int ncol, long ld,
+                                                               unsigned *status, PostStep post, int has_post, int pd)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int K = nk - 1;
+    const long slab = (long)nk * ld;
+    auto pf_row = [&](int k) {
+        const long o = (long)k * ld + col;
+        pf_l1(scr + S_P * slab + o);
+        pf_l1(scr + S_W1 * slab + o);
+        pf_l1(scr + S_Y1 * slab + o);
+        pf_l1(F.explicit_h + o);
+        pf_l1(F.optm1_smooth2 + o);
+        pf_l1(scr + S_PROD * slab + o);
+    };
+    for (int kk = 1; kk < pd && kk < K; ++kk) pf_row(kk);
+    const double t_top = scr[S_TB * slab + col], t_bot = scr[S_TB * slab + ld + col];
+    double w3 = 0.;
+    for (int k = 0; k < K; ++k) {
+        if (k + pd < K) pf_row(k + pd);
+        const long o = (long)k * ld + col;
+        double ex = xs(F.explicit_h[o], xm(xm(F.optm1_smooth2[o], C.dtx2inv), (double)C.nstep_sub));
+        if (k == nk - 2) ex = xs(ex, t_top);
+        ex = xs(ex, scr[S_PROD * slab + o]);
+        if (k == 0) {
+            ex = xs(ex, t_bot);
+            w3 = qdiv(ex, scr[S_W1 * slab + o], scr[S_Y1 * slab + o]);
+        } else {
+            w3 = qdiv(xs(ex, xm(scr[S_P * slab + o], w3)), scr[S_W1 * slab + o], scr[S_Y1 * slab + o]);
+        }
+        opout[o] = w3;
+    }
+    const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
+    double xn = w3;
+    const double xtop = w3;
+    bool fin = fabs(xn) <= DBL_MAX;
+    double park = K >= 2 ? opout[(long)(K - 2) * ld + col] : 0.;
+    for (int k = K - 2; k >= 0; --k) {
+        if (k - pd >= 0) post_prefetch(post, has_post, bcol, opout, (long)(k - pd) * ld + col);
+        const double wk = park;
+        if (k >= 1) park = opout[(long)(k - 1) * ld + col];
+        xn = xs(wk, xm(scr[S_W2 * slab + (long)k * ld + col], xn));
+        fin = fin && fabs(xn) <= DBL_MAX;
+        post_store(post, has_post, bcol, opout, (long)k * ld + col, xn);
+        if (k == K - 2) {
+            post_store(post, has_post, bcol, opout, (long)K * ld + col, xd(xm(xtop, xtop), xn));
+            if (has_post) post_store(post, true, bcol, opout, (long)(K - 1) * ld + col, xtop);
+        }
+    }
+    if (status && !fin) atomicOr(status, FLAG_NONFINITE);
+}
+
+cudaError_t launch_oplus_factor(const OplusFields &F, const OplusConsts &C, double *xiop2p, double *xiop2d,
+                                double *factor, int nk, int ncol, long ld, unsigned *status, cudaStream_t st)
+{
+    if (ncol <= 0) return cudaSuccess;
+    if (nk < 3) return cudaErrorInvalidValue;
+    k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, xiop2p, xiop2d, nullptr, nullptr, factor, nk,
+                                                                 ncol, ld);
+    k_oplus_coefs<<<dim3((ncol + 127) / 128, nk - 1), 128, 0, st>>>(F, C, factor, nk, ncol, ld, nullptr);
+    k_oplus_factor<<<(ncol + 31) / 32, 32, 0, st>>>(factor, nk, ncol, ld, status, walk_prefetch(ncol));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_oplus_solve(const OplusFields &F, const OplusConsts &C, const double *factor, double *opout, int nk,
+                               int ncol, long ld, unsigned *status, cudaStream_t st, const PostStep *post)
+{
+    if (ncol <= 0) return cudaSuccess;
+    if (nk < 3) return cudaErrorInvalidValue;
+    const PostStep pv = post ? *post : PostStep{};
+    const int hp = post != nullptr;
+    const size_t tile = (size_t)kSolveThreads * 7 * (nk - 1) * sizeof(double);
+    const int T = kSolveThreads;
+    if (ncol <= kSmallWalkColumns && tile <= (size_t)smem_optin()) {
+        once_per_device([] {
+            cudaFuncSetAttribute(k_oplus_solve_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
+        });
+        k_oplus_solve_tile<<<(ncol + T - 1) / T, T, tile, st>>>(F, C, factor, opout, nk, ncol, ld, status, pv, hp);
+    } else {
+        k_oplus_solve<<<(ncol + T - 1) / T, T, 0, st>>>(F, C, factor, opout, nk, ncol, ld, status, pv, hp,
+                                                        walk_prefetch(ncol));
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *opout, double *xiop2p,

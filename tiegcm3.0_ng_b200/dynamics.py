@@ -6,7 +6,10 @@ inputs it computes itself:
 
   oplus_ng x nstep_sub   smooth_ng(optm1), the O+ column step + lateral
                          hook + time filter (src/oplus_ng.F90:159, 125-340);
-                         sub-step s reads what sub-step s-1 wrote
+                         sub-step s reads what sub-step s-1 wrote; the rows
+                         and pivots, the same in every sub-step, are formed
+                         once (tg_oplus_ng_factor_dev) and each sub-step
+                         solves from them (tg_oplus_ng_solve_dev)
   minor_ng x 4           N2D, N4S, NO, Ar (comp_n2d_ng ... comp_ar_ng):
                          smooth_ng(fcomp_tm1), advec_ng(fcomp), the column
                          step + lateral hook + time filter and floors
@@ -170,7 +173,9 @@ class DynamicsStep:
         self.nstep_sub = int(o["C"]["nstep_sub"])
         Fo = _dev_fields(o["F"], g, ("zpint",), device)
         self.oplus = dict(F=Fo, C=o["C"], op0=Fo["op"], optm10=lvl(o["optm1"]), bnd=lvl(o["bnd"]),
-                          op=[z(), z()], optm1=[z(), z()], xiop2p=z(), xiop2d=z())
+                          op=[z(), z()], optm1=[z(), z()], xiop2p=z(), xiop2d=z(),
+                          factor=torch.zeros(cs.oplus_ng_factor_doubles(nk, ld), dtype=torch.float64,
+                                             device=device))
         # comp_ng + post-solve steps
         c = host["comp"]
         Fc = _dev_fields(c["F"], g, ("expz", "difk"), device)
@@ -199,14 +204,17 @@ class DynamicsStep:
                     dtsmooth_div2=self.ds[1])
 
     def _oplus(self, st):
+        # the rows and pivots once (they do not change between sub-steps),
+        # then each sub-step's smoothing and solve
         g, o = self.grid, self.oplus
         op, optm1 = o["op0"], o["optm10"]
+        cs.oplus_ng_factor_dev(o["F"], o["C"], o["xiop2p"], o["xiop2d"], o["factor"], g.nk, g.ncol, g.ld, stream=st)
         for s in range(self.nstep_sub):
             nxt = s % 2
             self._smooth(optm1, o["F"]["optm1_smooth2"], st, g.shapiro / self.nstep_sub)
             F = dict(o["F"], op=op)
-            cs.oplus_ng_post_dev(F, o["C"], o["op"][nxt], o["xiop2p"], o["xiop2d"], g.nk, g.ncol, g.ld,
-                                 self._post(op, optm1, o["optm1"][nxt], o["bnd"]), stream=st)
+            cs.oplus_ng_solve_dev(F, o["C"], o["factor"], o["op"][nxt], g.nk, g.ncol, g.ld,
+                                  self._post(op, optm1, o["optm1"][nxt], o["bnd"]), stream=st)
             op, optm1 = o["op"][nxt], o["optm1"][nxt]
 
     def _minor(self, m, st):
