@@ -313,6 +313,26 @@ int tg_comp_ng(const tg_comp_fields *F, const tg_comp_consts *C, double *o2_upd,
  * of nk*ld: P(i,m) at slab i+3m, Q at 9+i+3m, R at 18+i+3m, f at 27+i. */
 int tg_comp_ng_dev(const tg_comp_fields *F, const tg_comp_consts *C, double *out, int nk, int ncol, long ld,
                    double *system_out, int *status_dev, void *stream);
+/* comp_ng's history diagnostics (src/comp_ng.F90:334-380): the 24 fields the
+ * reference passes to addfld, from the fields and the solution (o2/o1/he_upd
+ * as tg_comp_ng returns them, before the lateral-boundary overwrite and the
+ * post steps), in the order of the calls: DO2DT, DO1DT, DHEDT, O2/O1/HE_PROD,
+ * O2/O1/HE_LOSS, O2/O1/HE_HORDIF, O2/O1/HE_MOLDIF, O2/O1/HE_EDDYDIF,
+ * -O2/O1/HE_VERADV, -O2/O1/HE_HORADV.  LOSS and MOLDIF are summed over the
+ * fourth index of loss(k,i,j,isp,m) and moldif, the row's species, as the
+ * reference's sum(., dim=4) does; MOLDIF, EDDYDIF and VERADV, which the
+ * reference leaves unset on the first and top levels, are 0 there.  MOLDIF
+ * and EDDYDIF use the device's fractional powers like tg_comp_ng (within
+ * ~1e-13 relative); the others are bit-identical.  With calc_helium = 0
+ * the reference's He planes use the solved He, which tg_comp_ng replaces by
+ * pshelb before returning it: their values here are those of the He passed.
+ * Host form: diag (nk, ncol, 24) in the Fortran layout.  Device form: upd the three level-major
+ * planes (as tg_comp_ng_dev writes them), diag 24 planes of nk*ld, on the
+ * caller's stream. */
+int tg_comp_diag_ng(const tg_comp_fields *F, const tg_comp_consts *C, const double *o2_upd, const double *o1_upd,
+                    const double *he_upd, double *diag, int nk, int ncol);
+int tg_comp_diag_ng_dev(const tg_comp_fields *F, const tg_comp_consts *C, const double *upd, double *diag, int nk,
+                        int ncol, long ld, void *stream);
 
 /* comp_ng's post-solve steps per column (src/comp_ng.F90:415-457): time
  * filter, N2 = 1-O2-O-He with the exponential extrapolation above the first
@@ -527,6 +547,23 @@ int tg_oplus_ng_post_dev(const tg_oplus_fields *F, const tg_oplus_consts *C, dou
  * Each sub-step's opout is bit-identical to tg_oplus_ng_dev /
  * tg_oplus_ng_post_dev on the same fields. */
 long tg_oplus_ng_factor_doubles(int nk, long ld);
+/* oplus_ng's history diagnostics (src/oplus_ng.F90:309-330): 6 fields DOPDT,
+ * OP_PROD, OP_LOSS (= -op_loss*opout), OP_DIFF, OP_DRIFT, OP_WIND of the
+ * solution opout (rows 1..nk, the top level included, before the lateral
+ * overwrite and the post steps).  The three sums add the horizontal terms
+ * the host model computes in the routine's horizontal part (diffexp,
+ * vdotn_h, bdotdh_bvel: each may be NULL, taken as 0, and the sum then holds
+ * the vertical part alone) and are defined on levels 2..nk-1; the reference
+ * leaves the first and top levels unset, here they are 0.  OP_DIFF carries
+ * the device's log10 and pow through dj (within ~1e-13 relative, like
+ * tg_oplus_ng); the others are bit-identical.  Host form: diag (nk, ncol, 6)
+ * in the Fortran layout; device form: 6 planes of nk*ld on the caller's
+ * stream. */
+int tg_oplus_diag_ng(const tg_oplus_fields *F, const tg_oplus_consts *C, const double *opout, const double *diffexp,
+                     const double *vdotn_h, const double *bdotdh_bvel, double *diag, int nk, int ncol);
+int tg_oplus_diag_ng_dev(const tg_oplus_fields *F, const tg_oplus_consts *C, const double *opout,
+                         const double *diffexp, const double *vdotn_h, const double *bdotdh_bvel, double *diag,
+                         int nk, int ncol, long ld, void *stream);
 int tg_oplus_ng_factor_dev(const tg_oplus_fields *F, const tg_oplus_consts *C, double *xiop2p, double *xiop2d,
                            double *factor, int nk, int ncol, long ld, int *status_dev, void *stream);
 int tg_oplus_ng_solve_dev(const tg_oplus_fields *F, const tg_oplus_consts *C, const double *factor, double *opout,

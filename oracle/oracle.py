@@ -283,6 +283,9 @@ def _bind_comp(L):
         L.oracle_comp_post_ng.argtypes = [ctypes.c_void_p] * 8 + [ctypes.c_double] * 3 + \
             [ctypes.c_int, ctypes.c_long] + [ctypes.c_void_p] * 6
         L.oracle_comp_post_ng.restype = None
+        L.oracle_comp_diag_ng.argtypes = [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), ctypes.c_int,
+                                          ctypes.c_long] + [ctypes.c_void_p] * 4
+        L.oracle_comp_diag_ng.restype = None
         L._comp_bound = True
     return L
 
@@ -305,6 +308,28 @@ def comp_ng(fields, consts, with_system=False):
         sysarr = [None] * 5
     L.oracle_comp_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(u) for u in upd], *[_p(s) for s in sysarr])
     return (tuple(upd), tuple(sysarr)) if with_system else tuple(upd)
+
+
+COMP_DIAG_NAMES = ("DO2DT", "DO1DT", "DHEDT", "O2_PROD", "O1_PROD", "HE_PROD", "O2_LOSS", "O1_LOSS", "HE_LOSS",
+                   "O2_HORDIF", "O1_HORDIF", "HE_HORDIF", "O2_MOLDIF", "O1_MOLDIF", "HE_MOLDIF", "O2_EDDYDIF",
+                   "O1_EDDYDIF", "HE_EDDYDIF", "O2_VERADV", "O1_VERADV", "HE_VERADV", "O2_HORADV", "O1_HORADV",
+                   "HE_HORADV")
+
+
+def comp_diag_ng(fields, consts, upd):
+    """comp_ng's history diagnostics (src/comp_ng.F90:334-380) of the solution
+    upd = (o2, o1, he) (nk, ncol): a dict of (nk, ncol) arrays by the names of
+    the addfld calls (VERADV and HORADV negated as they are handed over;
+    MOLDIF, EDDYDIF, VERADV 0 on the first and top levels)."""
+    L = _bind_comp(lib())
+    arrs = {k: (np.ascontiguousarray(fields[k]) if k == "fs" else _fcopy(fields[k])) for k in COMP_FIELD_ORDER}
+    nk, ncol = arrs["tn"].shape[0], arrs["tn"].size // arrs["tn"].shape[0]
+    F = CompFields(*[arrs[k].ctypes.data for k in COMP_FIELD_ORDER])
+    C = comp_consts(consts)
+    x = [_fcopy(u) for u in upd]
+    out = np.zeros((nk, ncol, len(COMP_DIAG_NAMES)), order="F")
+    L.oracle_comp_diag_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(u) for u in x], _p(out))
+    return {n: out[:, :, i] for i, n in enumerate(COMP_DIAG_NAMES)}
 
 
 POST_INPUTS = ("o2", "o1", "he", "o2_nm", "o1_nm", "he_nm", "xnmbar")
@@ -426,6 +451,30 @@ def oplus_ng(fields, consts, with_system=False):
     sysarr = [np.zeros((nk, ncol), order="F") for _ in range(4)] if with_system else [None] * 4
     L.oracle_oplus_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, *[_p(a) for a in outs], *[_p(s) for s in sysarr])
     return (tuple(outs), tuple(sysarr)) if with_system else tuple(outs)
+
+
+OPLUS_DIAG_NAMES = ("DOPDT", "OP_PROD", "OP_LOSS", "OP_DIFF", "OP_DRIFT", "OP_WIND")
+
+
+def oplus_diag_ng(fields, consts, opout, diffexp=None, vdotn_h=None, bdotdh_bvel=None):
+    """oplus_ng's history diagnostics (src/oplus_ng.F90:309-330) of the
+    solution opout (nk, ncol), with the horizontal terms (None: 0); a dict of
+    (nk, ncol) arrays by the names of the addfld calls."""
+    L = lib()
+    if not hasattr(L, "_oplus_diag_bound"):
+        L.oracle_oplus_diag_ng.argtypes = [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), ctypes.c_int,
+                                           ctypes.c_long] + [ctypes.c_void_p] * 5
+        L.oracle_oplus_diag_ng.restype = None
+        L._oplus_diag_bound = True
+    arrs = {k: _fcopy(fields[k]) for k in OPLUS_FIELD_ORDER}
+    nk, ncol = arrs["tn"].shape[0], arrs["tn"].size // arrs["tn"].shape[0]
+    F = OplusFields(*[arrs[k].ctypes.data for k in OPLUS_FIELD_ORDER])
+    C = oplus_consts(consts)
+    x = _fcopy(opout)
+    h = [None if a is None else _fcopy(a) for a in (diffexp, vdotn_h, bdotdh_bvel)]
+    out = np.zeros((nk, ncol, len(OPLUS_DIAG_NAMES)), order="F")
+    L.oracle_oplus_diag_ng(ctypes.byref(F), ctypes.byref(C), nk, ncol, _p(x), *[_p(a) for a in h], _p(out))
+    return {n: out[:, :, i] for i, n in enumerate(OPLUS_DIAG_NAMES)}
 
 
 def _bind_horiz(L):

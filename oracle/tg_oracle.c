@@ -1062,6 +1062,117 @@ ORACLE_API void oracle_comp_ng(const oracle_comp_fields *F, const oracle_comp_co
 /* receive the final mixing ratios, *nm_upd the filtered ones.  A column    */
 /* whose N2 drops below 0.01 at level 1 is left without extrapolation (the  */
 /* reference would read level 0 there).                                      */
+/* comp_ng's history diagnostics (comp_ng.F90:334-380) of a solution upd =
+ * (o2, o1, he) before the lateral overwrite and the post steps: 24 planes
+ * (nk, ncol) in the order of the addfld calls,
+ *   DO2DT DO1DT DHEDT, O2/O1/HE_PROD, _LOSS, _HORDIF, _MOLDIF, _EDDYDIF,
+ *   -_VERADV, -_HORADV.
+ * loss and moldif are summed over their fourth index, the species the row
+ * belongs to (sum(loss, dim=4), sum(moldif, dim=4)), so X_LOSS and X_MOLDIF
+ * are indexed by the species the solution value belongs to.  MOLDIF,
+ * EDDYDIF and VERADV are defined on levels 2..nk-1 (1-based); the reference
+ * leaves the others unset, here they are 0. */
+ORACLE_API void oracle_comp_diag_ng(const oracle_comp_fields *F, const oracle_comp_consts *C, int nk, long ncol,
+                                    const double *o2_upd, const double *o1_upd, const double *he_upd, double *diag)
+{
+    const double dz = C->dz;
+    double *w = (double *)malloc(sizeof(double) * (8 + 14 * 2) * (size_t)nk);
+    long col;
+    if (nk < 3) { free(w); return; }
+    const size_t slab = (size_t)nk * ncol;
+    for (col = 0; col < ncol; ++col) {
+        const size_t o = (size_t)nk * col;
+        const double *tn = F->tn + o, *o2 = F->o2 + o, *o1 = F->o1 + o, *he = F->he + o, *mbar = F->mbar + o,
+                     *ww = F->w + o;
+        const double *nms[3] = {F->o2nm_smooth + o, F->o1nm_smooth + o, F->henm_smooth + o};
+        const double *adv[3] = {F->o2_advec + o, F->o1_advec + o, F->he_advec + o};
+        const double *hd[3] = {F->hdo2 + o, F->hdo1 + o, F->hdhe + o};
+        const double *x[3] = {o2_upd + o, o1_upd + o, he_upd + o};
+        double *o2i = w, *o1i = w + nk, *hei = w + 2 * nk, *embari = w + 3 * nk, *tni = w + 4 * nk,
+               *dembardz = w + 5 * nk, *dtndz = w + 6 * nk, *wi = w + 7 * nk;
+        /* per level: ep (3), ak (9), wks4 */
+        double *lev = w + 8 * nk;
+        double ps0[3], embar0, A[9];
+        double *d[24];
+        int k, i, m, n;
+        for (n = 0; n < 24; ++n) d[n] = diag + n * slab + o;
+        for (i = 0; i < 3; ++i)
+            ps0[i] = C->b[i] * o2[0] + C->b[i + 3] * o1[0] + C->b[i + 6] * he[0] + C->fb[i];
+        embar0 = 1. / (ps0[0] * C->rmassinv_o2 + ps0[1] * C->rmassinv_o1 + ps0[2] * C->rmassinv_he +
+                       (1. - ps0[0] - ps0[1] - ps0[2]) * C->rmassinv_n2);
+        o2i[0] = .5 * (ps0[0] + o2[0]);
+        o1i[0] = .5 * (ps0[1] + o1[0]);
+        hei[0] = .5 * (ps0[2] + he[0]);
+        embari[0] = .5 * (embar0 + mbar[0]);
+        tni[0] = F->tlbc[col];
+        dembardz[0] = mbar[0] - embar0;
+        dtndz[0] = (tn[0] - F->tlbc[col]) * 2;
+        for (k = 1; k < nk; ++k) {
+            o2i[k] = .5 * (o2[k - 1] + o2[k]);
+            o1i[k] = .5 * (o1[k - 1] + o1[k]);
+            hei[k] = .5 * (he[k - 1] + he[k]);
+            embari[k] = .5 * (mbar[k - 1] + mbar[k]);
+            tni[k] = .5 * (tn[k - 1] + tn[k]);
+            dembardz[k] = mbar[k] - mbar[k - 1];
+            dtndz[k] = tn[k] - tn[k - 1];
+        }
+        for (k = 0; k < nk; ++k) {
+            dembardz[k] = dembardz[k] / dz;
+            dtndz[k] = dtndz[k] / dz;
+        }
+        for (k = 0; k < nk - 1; ++k) wi[k] = .5 * (ww[k] + ww[k + 1]);
+        wi[nk - 1] = 1.5 * ww[nk - 1] - .5 * ww[nk - 2];
+        /* level quantities (:128-211); the top level has no thermal diffusion term */
+        for (k = 0; k < nk; ++k) {
+            double *L = lev + 13 * (size_t)k;
+            comp_level(C, o2i[k], o1i[k], hei[k], embari[k], tni[k], dembardz[k], dtndz[k], k != nk - 1, L, A,
+                       L + 3, L + 12);
+        }
+        for (k = 0; k < nk; ++k) {
+            for (i = 0; i < 3; ++i) {
+                d[i][k] = C->dtx2inv * (x[i][k] - nms[i][k]);
+                d[3 + i][k] = F->fs[(size_t)i * slab + o + k];
+                d[9 + i][k] = hd[i][k];
+                d[21 + i][k] = -adv[i][k];
+            }
+            /* loss_sum(m) = sum over isp of fs(isp, m) * upd(m), accumulated from 0 as SUM does */
+            for (m = 0; m < 3; ++m) {
+                double s = 0.;
+                for (i = 0; i < 3; ++i) s = s + F->fs[(size_t)(m + 1) * 3 * slab + (size_t)i * slab + o + k] * x[m][k];
+                d[6 + m][k] = s;
+            }
+            for (i = 0; i < 3; ++i) d[12 + i][k] = d[15 + i][k] = d[18 + i][k] = 0.;
+        }
+        for (k = 1; k < nk - 1; ++k) {
+            /* row k's coefficients: levels k (km) and k+1 (kp) */
+            const double *Lk = lev + 13 * (size_t)k, *Lp = lev + 13 * (size_t)(k + 1);
+            const double wks3 = Lk[12], wks4 = Lp[12];
+            const double eddyp = C->expzmid_inv * F->difk[k] * (1. / dz - wks3);
+            const double eddyr = C->expzmid * F->difk[k + 1] * (1. / dz + wks4);
+            const double eddyq = C->expzmid_inv * F->difk[k] * (1. / dz + wks3) +
+                                 C->expzmid * F->difk[k + 1] * (1. / dz - wks4);
+            for (m = 0; m < 3; ++m) {
+                double s = 0.;
+                for (i = 0; i < 3; ++i) {
+                    const double molp = Lk[3 + i + 3 * m] * (1. / dz + Lk[m] / 2.);
+                    const double molr = Lp[3 + i + 3 * m] * (1. / dz - Lp[m] / 2.);
+                    const double molq = Lk[3 + i + 3 * m] * (1. / dz - Lk[m] / 2.) +
+                                        Lp[3 + i + 3 * m] * (1. / dz + Lp[m] / 2.);
+                    s = s + -(1. / F->expz[k] / dz * (molp * x[m][k - 1] - molq * x[m][k] + molr * x[m][k + 1]));
+                }
+                d[12 + m][k] = s;
+            }
+            for (i = 0; i < 3; ++i) {
+                d[15 + i][k] = 1. / dz * (eddyp * x[i][k - 1] - eddyq * x[i][k] + eddyr * x[i][k + 1]);
+                d[18 + i][k] = -(wi[k] / (2. * dz) * (x[i][k + 1] - x[i][k - 1]));
+            }
+        }
+        for (k = 0; k < nk; ++k)
+            for (i = 0; i < 3; ++i) d[15 + i][k] = d[15 + i][k] * F->dfactor[col];
+    }
+    free(w);
+}
+
 ORACLE_API void oracle_comp_post_ng(const double *o2, const double *o1, const double *he, const double *o2_nm,
                                     const double *o1_nm, const double *he_nm, const double *xnmbar,
                                     const double *zpmid, double dz, double dtsmooth, double dtsmooth_div2,
@@ -1372,13 +1483,16 @@ typedef struct {
     int nstep_sub;
 } oracle_oplus_consts;
 
-ORACLE_API void oracle_oplus_ng(const oracle_oplus_fields *F, const oracle_oplus_consts *C, int nk, long ncol,
-                                double *opout, double *xiop2p, double *xiop2d, double *Fe, double *Fn,
-                                double *p_out, double *q_out, double *r_out, double *f_out)
+/* The O+ column step, and (diag not NULL) instead of the solve the history
+ * diagnostics of a given solution xsol (oplus_ng.F90:309-330) with the
+ * horizontal terms h3 = diffexp, vdotn_h, bdotdh_bvel (each may be NULL: 0). */
+static void oplus_core(const oracle_oplus_fields *F, const oracle_oplus_consts *C, int nk, long ncol, double *opout,
+                       double *xiop2p, double *xiop2d, double *Fe, double *Fn, double *p_out, double *q_out,
+                       double *r_out, double *f_out, const double *xsol, const double *const *h3, double *diag)
 {
     const double explic = 1., phid = 2.0e8, phin = -2.0e8, ppolar = 0.;
     const double pi = 4.0 * atan(1.0), rtd = 180.0 / pi, dz = C->dz;
-    double *w = (double *)malloc(sizeof(double) * 24 * (size_t)nk);
+    double *w = (double *)malloc(sizeof(double) * 34 * (size_t)nk);
     long col;
     (void)explic;
     if (nk < 3) { free(w); return; }
@@ -1392,7 +1506,7 @@ ORACLE_API void oracle_oplus_ng(const oracle_oplus_fields *F, const oracle_oplus
                *tph1 = w + 5 * nk, *tph0 = w + 6 * nk, *djint = w + 7 * nk, *hdzm = w + 8 * nk, *hdzp = w + 9 * nk,
                *p = w + 10 * nk, *q = w + 11 * nk, *r = w + 12 * nk, *ex = w + 13 * nk, *ol = w + 14 * nk,
                *wni = w + 15 * nk, *wii = w + 16 * nk, *vni = w + 17 * nk, *tpop = w + 18 * nk, *ws = w + 19 * nk,
-               *x = w + 22 * nk;
+               *x = w + 22 * nk, *part = w + 24 * nk, *prodv = w + 33 * nk;
         const double bx = F->bx[col], by = F->by[col], bz = F->bz[col];
         int k;
         /* oplus_flux (:88-99) */
@@ -1479,6 +1593,11 @@ ORACLE_API void oracle_oplus_ng(const oracle_oplus_fields *F, const oracle_oplus
             windq = -bdotu[k] * dvbz * bz;
             if (k == nk - 2) windr = bz * (2. * bdotu[nk - 2] - bdotu[nk - 3]) * 0.5 * hdz[nk - 2];
             else windr = -bz * bdotu[k + 1] * 0.5 * hdz[k];
+            {
+                const double pt[9] = {diffp, diffq, diffr, driftp, driftq, driftr, windp, windq, windr};
+                int e;
+                for (e = 0; e < 9; ++e) part[e * nk + k] = pt[e];
+            }
             p[k] = diffp + driftp + windp;
             q[k] = diffq + driftq + windq - C->dtx2inv * C->nstep_sub;
             r[k] = diffr + driftr + windr;
@@ -1505,14 +1624,36 @@ ORACLE_API void oracle_oplus_ng(const oracle_oplus_fields *F, const oracle_oplus
                                (xnmbar[k] * (C->rk23 * n2[k] * C->rmassinv_n2 + C->rk24 * o1[k] * C->rmassinv_o1 +
                                              C->rk26 * o2[k] * C->rmassinv_o2) +
                                 rk25 * ne[k] + C->rk27);
-            xiop2p[o + k] = x2p;
-            xiop2d[o + k] = x2d;
+            if (xiop2p) xiop2p[o + k] = x2p;
+            if (xiop2d) xiop2d[o + k] = x2d;
             ol[k] = xnmbar[k] * (F->rk1[o + k] * o2[k] * C->rmassinv_o2 + F->rk2[o + k] * n2[k] * C->rmassinv_n2 +
                                  C->rk10 * n2d[k] * C->rmassinv_n2d);
             if (k < nk - 1) q[k] = q[k] - ol[k];
             const double prod = qopi + (rk19 * ne[k] + C->rk21) * x2p + (rk25 * ne[k] + C->rk27) * x2d +
                                 (C->rk18 * x2p + C->rk24 * x2d) * o1[k] * C->rmassinv_o1 * xnmbar[k];
             ex[k] = ex[k] - prod;
+            prodv[k] = prod;
+        }
+        if (diag) {
+            /* dopdt, op_prod, -op_loss_out, diffsum, driftsum, windsum (:309-330) */
+            const double *xs = xsol + o;
+            const size_t slab = (size_t)nk * ncol;
+            double *d[6];
+            int n;
+            for (n = 0; n < 6; ++n) d[n] = diag + n * slab + o;
+            for (k = 0; k < nk; ++k) {
+                d[0][k] = (xs[k] - F->optm1_smooth2[o + k]) * C->dtx2inv * C->nstep_sub;
+                d[1][k] = prodv[k];
+                d[2][k] = -(ol[k] * xs[k]);
+                d[3][k] = d[4][k] = d[5][k] = 0.;
+            }
+            for (k = 1; k < nk - 1; ++k)
+                for (n = 0; n < 3; ++n) {
+                    const double hz = h3 && h3[n] ? h3[n][o + k] : 0.;
+                    const double *pt = part + 3 * n * nk;
+                    d[3 + n][k] = (n == 0 ? hz : -hz) + pt[k] * xs[k - 1] + pt[nk + k] * xs[k] + pt[2 * nk + k] * xs[k + 1];
+                }
+            continue;
         }
         /* lower boundary (:301-303) */
         q[0] = q[0] - p[0];
@@ -1532,6 +1673,28 @@ ORACLE_API void oracle_oplus_ng(const oracle_oplus_fields *F, const oracle_oplus
 #undef FL
     }
     free(w);
+}
+
+ORACLE_API void oracle_oplus_ng(const oracle_oplus_fields *F, const oracle_oplus_consts *C, int nk, long ncol,
+                                double *opout, double *xiop2p, double *xiop2d, double *Fe, double *Fn,
+                                double *p_out, double *q_out, double *r_out, double *f_out)
+{
+    oplus_core(F, C, nk, ncol, opout, xiop2p, xiop2d, Fe, Fn, p_out, q_out, r_out, f_out, NULL, NULL, NULL);
+}
+
+/* oplus_ng's history diagnostics (oplus_ng.F90:309-330) of the solution
+ * opout (rows 1..nk, the top included, before the lateral overwrite and the
+ * post steps): 6 planes (nk, ncol) DOPDT, OP_PROD, OP_LOSS (= -op_loss*opout),
+ * OP_DIFF, OP_DRIFT, OP_WIND.  The last three add the horizontal terms
+ * diffexp, -vdotn_h, -bdotdh_bvel the host model computes (NULL: 0) to the
+ * vertical parts, on levels 2..nk-1 (1-based); the reference leaves the
+ * first and top levels unset, here they are 0. */
+ORACLE_API void oracle_oplus_diag_ng(const oracle_oplus_fields *F, const oracle_oplus_consts *C, int nk, long ncol,
+                                     const double *opout, const double *diffexp, const double *vdotn_h,
+                                     const double *bdotdh_bvel, double *diag)
+{
+    const double *h3[3] = {diffexp, vdotn_h, bdotdh_bvel};
+    oplus_core(F, C, nk, ncol, NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL, opout, h3, diag);
 }
 
 /* ------------------------------------------------------------------------ */

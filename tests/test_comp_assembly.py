@@ -16,14 +16,13 @@ _log = prec_fn(math.log, np.log)
 _exp = prec_fn(math.exp, np.exp)
 
 
-def comp_numpy(F, C):
-    """Returns (upd (3, nk, ncol), P, Q, R (3,3,nk-1,ncol), f (3,nk-1,ncol))."""
+def _comp_levels(F, C):
+    """Interface quantities (comp_ng.F90:74-102) and level(j, thermal): ep, the
+    alpha matrix, ak and wks4 of level j (:128-211); also wi."""
     nk, ncol = F["tn"].shape
     tn, o2, o1, he, w, mbar = (F[k] for k in ("tn", "o2", "o1", "he", "w", "mbar"))
     b, fb, dz = C["b"], C["fb"], C["dz"]
     dt = F["tn"].dtype
-    flx_he = F["flx_he"] if C["calc_helium"] else np.zeros(ncol, dtype=dt)
-    fs = F["fs"].reshape(4, 3, ncol, nk)          # fs(k, col, isp, m) -> [m, isp, col, k]
     ps0 = [b[i, 0] * o2[0] + b[i, 1] * o1[0] + b[i, 2] * he[0] + fb[i] for i in range(3)]
     embar0 = 1. / (ps0[0] * C["rmassinv_o2"] + ps0[1] * C["rmassinv_o1"] + ps0[2] * C["rmassinv_he"] +
                    (1. - ps0[0] - ps0[1] - ps0[2]) * C["rmassinv_n2"])
@@ -70,6 +69,18 @@ def comp_numpy(F, C):
         ak = matinv3(a) * wks1
         return ep, a, ak, dembardz[j] / (embari[j] * 2.)
 
+    return level, wi, embari
+
+
+def comp_numpy(F, C):
+    """Returns (upd (3, nk, ncol), P, Q, R (3,3,nk-1,ncol), f (3,nk-1,ncol))."""
+    nk, ncol = F["tn"].shape
+    tn = F["tn"]
+    b, fb, dz = C["b"], C["fb"], C["dz"]
+    dt = F["tn"].dtype
+    flx_he = F["flx_he"] if C["calc_helium"] else np.zeros(ncol, dtype=dt)
+    fs = F["fs"].reshape(4, 3, ncol, nk)          # fs(k, col, isp, m) -> [m, isp, col, k]
+    level, wi, embari = _comp_levels(F, C)
     ep_kp, a_kp, ak_kp, wks4 = level(0, True)
     nms = (F["o2nm_smooth"], F["o1nm_smooth"], F["henm_smooth"])
     adv = (F["o2_advec"], F["o1_advec"], F["he_advec"])
@@ -138,6 +149,70 @@ def comp_numpy(F, C):
     if not C["calc_helium"]:
         upd[2] = C["pshelb"]
     return upd, P, Q, R, fv
+
+
+def comp_diag_numpy(F, C, upd):
+    """comp_ng's addfld diagnostics (comp_ng.F90:334-380) as the array
+    statements write them: sum(loss, dim=4) and sum(moldif, dim=4) add over
+    the row's species, accumulated from 0."""
+    nk, ncol = F["tn"].shape
+    dz = C["dz"]
+    fs = F["fs"].reshape(4, 3, ncol, nk)
+    level, wi, _ = _comp_levels(F, C)
+    L = [level(j, j != nk - 1) for j in range(nk)]
+    nms = (F["o2nm_smooth"], F["o1nm_smooth"], F["henm_smooth"])
+    adv = (F["o2_advec"], F["o1_advec"], F["he_advec"])
+    hd = (F["hdo2"], F["hdo1"], F["hdhe"])
+    names = ("O2", "O1", "HE")
+    out = {}
+    for i, n in enumerate(names):
+        out["D" + n + "DT"] = C["dtx2inv"] * (upd[i] - nms[i])
+        out[n + "_PROD"] = fs[0, i].T.copy()
+        out[n + "_HORDIF"] = hd[i]
+        out[n + "_HORADV"] = -adv[i]
+    for m, n in enumerate(names):
+        s = np.zeros((nk, ncol))
+        for isp in range(3):
+            s = s + fs[m + 1, isp].T * upd[m]
+        out[n + "_LOSS"] = s
+    moldif = np.zeros((3, nk, ncol))
+    eddydif = np.zeros((3, nk, ncol))
+    veradv = np.zeros((3, nk, ncol))
+    for k in range(1, nk - 1):
+        ep_km, _, ak_km, wks3 = L[k]
+        ep_kp, _, ak_kp, wks4 = L[k + 1]
+        eddyp = C["expzmid_inv"] * F["difk"][k] * (1. / dz - wks3)
+        eddyr = C["expzmid"] * F["difk"][k + 1] * (1. / dz + wks4)
+        eddyq = (C["expzmid_inv"] * F["difk"][k] * (1. / dz + wks3) +
+                 C["expzmid"] * F["difk"][k + 1] * (1. / dz - wks4))
+        for m in range(3):
+            s = np.zeros(ncol)
+            for isp in range(3):
+                molp = ak_km[isp, m] * (1. / dz + ep_km[m] / 2.)
+                molr = ak_kp[isp, m] * (1. / dz - ep_kp[m] / 2.)
+                molq = ak_km[isp, m] * (1. / dz - ep_km[m] / 2.) + ak_kp[isp, m] * (1. / dz + ep_kp[m] / 2.)
+                s = s + -(1. / F["expz"][k] / dz * (molp * upd[m, k - 1] - molq * upd[m, k] + molr * upd[m, k + 1]))
+            moldif[m, k] = s
+        for isp in range(3):
+            eddydif[isp, k] = 1. / dz * (eddyp * upd[isp, k - 1] - eddyq * upd[isp, k] + eddyr * upd[isp, k + 1])
+            veradv[isp, k] = wi[k] / (2 * dz) * (upd[isp, k + 1] - upd[isp, k - 1])
+    eddydif = eddydif * F["dfactor"]
+    for i, n in enumerate(names):
+        out[n + "_MOLDIF"] = moldif[i]
+        out[n + "_EDDYDIF"] = eddydif[i]
+        out[n + "_VERADV"] = -veradv[i]
+    return out
+
+
+@pytest.mark.parametrize("nk,dz,calc_helium", [(29, 0.5, 1), (57, 0.25, 1), (3, 0.5, 1), (29, 0.5, 0)])
+def test_comp_diagnostics_match_independent_transcription(pkg, orc, nk, dz, calc_helium):
+    F, C = pkg.synth.comp_inputs(nk, 40, dz, 13 + nk, calc_helium=calc_helium)
+    upd = orc.comp_ng(F, C)
+    got = orc.comp_diag_ng(F, C, upd)
+    want = comp_diag_numpy(F, C, np.array(upd))
+    assert sorted(got) == sorted(orc.COMP_DIAG_NAMES)
+    for name in orc.COMP_DIAG_NAMES:
+        assert np.array_equal(got[name], want[name]), name
 
 
 @pytest.mark.parametrize("nk,dz,calc_helium", [(29, 0.5, 1), (57, 0.25, 1), (3, 0.5, 1), (29, 0.5, 0)])

@@ -91,3 +91,88 @@ def test_minor_diag_device(cuda, pkg, orc):
             assert np.array_equal(got, want[name]), name
         else:
             assert _rel(got, want[name]) <= MINOR_TOL, name
+
+
+# comp_ng: MOLDIF and EDDYDIF carry the level quantities ak, ep, wks4 with the
+# device's fractional powers, and MOLDIF's three-point difference of large
+# terms cancels (measured on B200: 1.02e-12 of the column's largest value);
+# the other 18 planes are bit-identical.
+COMP_TOL = 1e-11
+
+
+def _comp_check(pkg, got, want):
+    for name in pkg.colsolve.COMP_DIAG_NAMES:
+        if name.endswith("_MOLDIF") or name.endswith("_EDDYDIF"):
+            assert _rel(got[name], want[name]) <= COMP_TOL, name
+        else:
+            assert np.array_equal(got[name], want[name]), name
+
+
+@pytest.mark.parametrize("nk,dz,ncol,calc_helium", [(57, 0.25, 2001, 1), (29, 0.5, 777, 0), (113, 0.125, 300, 1),
+                                                    (3, 0.5, 33, 1)])
+def test_comp_diag_host(cuda, pkg, orc, nk, dz, ncol, calc_helium):
+    F, C = pkg.synth.comp_inputs(nk, ncol, dz, 90 + nk, calc_helium=calc_helium)
+    upd = orc.comp_ng(F, C)
+    got = pkg.comp_diag_ng(F, C, *[np.asfortranarray(u) for u in upd])
+    want = orc.comp_diag_ng(F, C, upd)
+    _comp_check(pkg, got, want)
+
+
+def test_comp_diag_device(cuda, pkg, orc):
+    torch = cuda
+    nk, ncol, dz = 57, 1500, 0.25
+    F, C = pkg.synth.comp_inputs(nk, ncol, dz, 19)
+    upd = orc.comp_ng(F, C)
+    ld = pkg.batch.pad_ld(ncol)
+    grid = type("G", (), dict(nk=nk, ncol=ncol, ld=ld))()
+    dev = pkg.dynamics._dev_fields(F, grid, ("expz", "difk"), "cuda")
+    x = torch.stack([pkg.batch.level_scalar(np.asfortranarray(u), ld, "cuda") for u in upd])
+    diag = torch.full((24, nk, ld), 7.0, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    pkg.comp_diag_ng_dev(dev, C, x, diag, nk, ncol, ld, stream=stream)
+    stream.synchronize()
+    got = {n: pkg.batch.from_level_scalar(diag[i], ncol) for i, n in enumerate(pkg.colsolve.COMP_DIAG_NAMES)}
+    _comp_check(pkg, got, orc.comp_diag_ng(F, C, upd))
+
+
+# oplus_ng: OP_DIFF carries dj, whose collision frequency takes the device's
+# log10 (and pow with the diffusion cap); the other five are bit-identical.
+OPLUS_TOL = 1e-12
+
+
+def _oplus_check(pkg, got, want):
+    for name in pkg.colsolve.OPLUS_DIAG_NAMES:
+        if name == "OP_DIFF":
+            assert _rel(got[name], want[name]) <= OPLUS_TOL, name
+        else:
+            assert np.array_equal(got[name], want[name]), name
+
+
+@pytest.mark.parametrize("nk,dz,ncol,cap,horizontal", [(57, 0.25, 2001, 0.0, True), (29, 0.5, 777, 1e7, False),
+                                                       (3, 0.5, 33, 0.0, True)])
+def test_oplus_diag_host(cuda, pkg, orc, nk, dz, ncol, cap, horizontal):
+    F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 95 + nk, opdiffcap=cap)
+    op = orc.oplus_ng(F, C)[0]
+    rng = np.random.default_rng(nk)
+    h3 = [np.asfortranarray(rng.uniform(-1e-3, 1e-3, op.shape)) for _ in range(3)] if horizontal else [None] * 3
+    got = pkg.oplus_diag_ng(F, C, np.asfortranarray(op), *h3)
+    want = orc.oplus_diag_ng(F, C, op, *h3)
+    _oplus_check(pkg, got, want)
+
+
+def test_oplus_diag_device(cuda, pkg, orc):
+    torch = cuda
+    nk, ncol, dz = 57, 1500, 0.25
+    F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 29)
+    op = orc.oplus_ng(F, C)[0]
+    rng = np.random.default_rng(3)
+    h3 = [np.asfortranarray(rng.uniform(-1e-3, 1e-3, op.shape)) for _ in range(3)]
+    dev, ld = _level(pkg, torch, F, nk, ncol, ("zpint",))
+    x = pkg.batch.level_scalar(np.asfortranarray(op), ld, "cuda")
+    hd = [pkg.batch.level_scalar(h, ld, "cuda") for h in h3]
+    diag = torch.full((6, nk, ld), 7.0, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    pkg.oplus_diag_ng_dev(dev, C, x, diag, nk, ncol, ld, *hd, stream=stream)
+    stream.synchronize()
+    got = {n: pkg.batch.from_level_scalar(diag[i], ncol) for i, n in enumerate(pkg.colsolve.OPLUS_DIAG_NAMES)}
+    _oplus_check(pkg, got, orc.oplus_diag_ng(F, C, op, *h3))

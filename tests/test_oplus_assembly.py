@@ -21,7 +21,9 @@ def interp_up(a):
     return out
 
 
-def oplus_numpy(F, C):
+def oplus_numpy(F, C, parts=None):
+    """The system rows, rates and fluxes; parts (a dict) receives the raw
+    diffusion / drift / wind coefficients, op_loss and op_prod."""
     pi = 4.0 * math.atan(1.0)
     rtd = 180. / pi
     phid, phin, ppolar = 2.0e8, -2.0e8, 0.
@@ -100,6 +102,9 @@ def oplus_numpy(F, C):
     windp[0] = bz * (2. * bdotu[0] - bdotu[1]) * 0.5 * hdz[0]
     windq[nk - 2] = -bdotu[nk - 2] * dvb * bz
     windr[nk - 2] = bz * (2. * bdotu[nk - 2] - bdotu[nk - 3]) * 0.5 * hdz[nk - 2]
+    if parts is not None:
+        parts.update(diffp=diffp, diffq=diffq, diffr=diffr, driftp=driftp, driftq=driftq, driftr=driftr,
+                     windp=windp, windq=windq, windr=windr)
     p = diffp + driftp + windp
     q = diffq + driftq + windq - C["dtx2inv"] * C["nstep_sub"]
     r = diffr + driftr + windr
@@ -120,6 +125,8 @@ def oplus_numpy(F, C):
     op_prod = (qopi + (rk19 * ne + C["rk21"]) * xiop2p + (rk25 * ne + C["rk27"]) * xiop2d +
                (C["rk18"] * xiop2p + C["rk24"] * xiop2d) * o1 * C["rmassinv_o1"] * xnmbar)
     explicit = explicit - op_prod
+    if parts is not None:
+        parts.update(op_loss=op_loss, op_prod=op_prod)
     q[0] = q[0] - p[0]
     explicit[0] = explicit[0] - 2. * p[0] * g("qop")[0] / (1.5 * op_loss[0] - 0.5 * op_loss[1])
     p[0] = 0.
@@ -138,3 +145,38 @@ def test_oplus_matches_independent_transcription(pkg, orc, nk, dz, cap):
     x = orc.trsolv_ng(pn, qn, rn, exn, nk - 1)
     assert np.array_equal(op[:nk - 1], x[:nk - 1])
     assert np.array_equal(op[nk - 1], x[nk - 2] * x[nk - 2] / x[nk - 3])
+
+
+def oplus_diag_numpy(F, C, x, h3):
+    """The addfld diagnostics of oplus_ng.F90:309-330 as its array statements
+    write them, on levels 2..nk-1 for the three sums."""
+    parts = {}
+    oplus_numpy(F, C, parts)
+    nk = x.shape[0]
+    out = {"DOPDT": (x - F["optm1_smooth2"]) * C["dtx2inv"] * C["nstep_sub"], "OP_PROD": parts["op_prod"],
+           "OP_LOSS": -(parts["op_loss"] * x)}
+    for name, pre, hz in (("OP_DIFF", "diff", h3[0]), ("OP_DRIFT", "drift", -h3[1]), ("OP_WIND", "wind", -h3[2])):
+        s = np.zeros_like(x)
+        k = slice(1, nk - 1)
+        s[k] = (hz[k] + parts[pre + "p"][k] * x[:nk - 2] + parts[pre + "q"][k] * x[1:nk - 1] +
+                parts[pre + "r"][k] * x[2:])
+        out[name] = s
+    return out
+
+
+@pytest.mark.parametrize("nk,dz,cap", [(29, 0.5, 0.0), (57, 0.25, 1e7), (3, 0.5, 1e5)])
+def test_oplus_diagnostics_match_independent_transcription(pkg, orc, nk, dz, cap):
+    F, C = pkg.synth.oplus_inputs(nk, 61, dz, 23 + nk, opdiffcap=cap)
+    op = orc.oplus_ng(F, C)[0]
+    rng = np.random.default_rng(nk)
+    h3 = [np.asfortranarray(rng.uniform(-1e-3, 1e-3, op.shape)) for _ in range(3)]
+    got = orc.oplus_diag_ng(F, C, op, *h3)
+    want = oplus_diag_numpy(F, C, op, h3)
+    assert sorted(got) == sorted(orc.OPLUS_DIAG_NAMES)
+    for name in orc.OPLUS_DIAG_NAMES:
+        assert np.array_equal(got[name], want[name]), name
+    # without the horizontal terms the sums hold the vertical parts alone
+    zero = orc.oplus_diag_ng(F, C, op)
+    want0 = oplus_diag_numpy(F, C, op, [np.zeros_like(op)] * 3)
+    for name in orc.OPLUS_DIAG_NAMES:
+        assert np.array_equal(zero[name], want0[name]), name

@@ -39,7 +39,7 @@ LIB_PATH = os.path.join(HERE, "libtg_colsolve.so")
 
 # Every symbol include/tg_colsolve.h declares.
 EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor_ng_dev", "tg_comp_ng",
-           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_comp_post_ng_dev", "tg_oplus_ng_factor_doubles", "tg_oplus_ng_factor_dev", "tg_oplus_ng_solve_dev", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_advec_ng", "tg_advec_ng_dev", "tg_smooth_ng", "tg_smooth_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
+           "tg_comp_ng_dev", "tg_comp_post_ng", "tg_comp_post_ng_dev", "tg_comp_diag_ng", "tg_comp_diag_ng_dev", "tg_oplus_ng_factor_doubles", "tg_oplus_diag_ng", "tg_oplus_diag_ng_dev", "tg_oplus_ng_factor_dev", "tg_oplus_ng_solve_dev", "tg_time_filter_ng", "tg_time_filter_ng_dev", "tg_advec_ng", "tg_advec_ng_dev", "tg_smooth_ng", "tg_smooth_ng_dev", "tg_settei_ng", "tg_settei_ng_dev", "tg_oplus_ng",
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_column_residency", "tg_set_assembly_mode", "tg_set_walk_prefetch", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
@@ -210,9 +210,14 @@ def lib():
             "tg_settei_ng_dev": [ctypes.POINTER(SetteiFields), ctypes.POINTER(SetteiConsts), P, P, P, I, I, Lg, P, P,
                                  P],
             "tg_comp_ng_dev": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, I, I, Lg, P, P, P],
+            "tg_comp_diag_ng": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, P, P, P, I, I],
+            "tg_comp_diag_ng_dev": [ctypes.POINTER(CompFields), ctypes.POINTER(CompConsts), P, P, I, I, Lg, P],
             "tg_comp_post_ng": [P] * 8 + [D, D, D, I, I] + [P] * 6,
             "tg_comp_post_ng_dev": [P] * 8 + [D, D, D, I, I, Lg] + [P] * 11,
             "tg_oplus_ng_factor_doubles": [I, Lg],
+            "tg_oplus_diag_ng": [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), P, P, P, P, P, I, I],
+            "tg_oplus_diag_ng_dev": [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), P, P, P, P, P, I, I,
+                                     Lg, P],
             "tg_oplus_ng_factor_dev": [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), P, P, P, I, I, Lg, P,
                                        P],
             "tg_oplus_ng_solve_dev": [ctypes.POINTER(OplusFields), ctypes.POINTER(OplusConsts), P, P, I, I, Lg,
@@ -570,6 +575,41 @@ def minor_diag_ng_dev(fields, consts, fcomp_out, diag, nk, ncol, ld, stream=None
     return _check(rc, "tg_minor_diag_ng_dev", numeric_ok=False)
 
 
+COMP_DIAG_NAMES = ("DO2DT", "DO1DT", "DHEDT", "O2_PROD", "O1_PROD", "HE_PROD", "O2_LOSS", "O1_LOSS", "HE_LOSS",
+                   "O2_HORDIF", "O1_HORDIF", "HE_HORDIF", "O2_MOLDIF", "O1_MOLDIF", "HE_MOLDIF", "O2_EDDYDIF",
+                   "O1_EDDYDIF", "HE_EDDYDIF", "O2_VERADV", "O1_VERADV", "HE_VERADV", "O2_HORADV", "O1_HORADV",
+                   "HE_HORADV")
+
+
+def comp_diag_ng(fields, consts, o2_upd, o1_upd, he_upd):
+    """comp_ng's history diagnostics (src/comp_ng.F90:334-380) from the fields
+    and the solution; returns a dict name -> (nk, ncol) array."""
+    nk = o2_upd.shape[0]
+    ncol = o2_upd.size // nk
+    if np.asarray(fields["fs"]).size != 12 * nk * ncol:
+        raise ValueError("fs must hold 12 slabs of nk*ncol")
+    _check_sizes("comp_diag_ng", fields, COMP_FIELDS, nk, ncol, two_d=("tlbc", "flx_he", "dfactor"),
+                 one_d=("expz", "difk"), outs=(("o1_upd", o1_upd), ("he_upd", he_upd)))
+    arrs = {n: np.ascontiguousarray(fields[n], dtype=np.float64).reshape(-1) if n == "fs" else fields[n]
+            for n in COMP_FIELDS}
+    F = CompFields(*[_host(arrs[n], n) for n in COMP_FIELDS])
+    C = comp_consts(consts)
+    out = np.zeros((nk, ncol, len(COMP_DIAG_NAMES)), order="F")
+    _check(lib().tg_comp_diag_ng(ctypes.byref(F), ctypes.byref(C), _host(o2_upd, "o2_upd"), _host(o1_upd, "o1_upd"),
+                                 _host(he_upd, "he_upd"), out.ctypes.data, nk, ncol), "tg_comp_diag_ng",
+           numeric_ok=False)
+    return {n: out[:, :, i] for i, n in enumerate(COMP_DIAG_NAMES)}
+
+
+def comp_diag_ng_dev(fields, consts, upd, diag, nk, ncol, ld, stream=None):
+    """Device form: level-major fields, upd the (3, nk, ld) solution, diag 24 planes of nk*ld."""
+    F = CompFields(*[_dptr(fields[n]) for n in COMP_FIELDS])
+    C = comp_consts(consts)
+    rc = lib().tg_comp_diag_ng_dev(ctypes.byref(F), ctypes.byref(C), _dptr(upd), _dptr(diag), nk, ncol, ld,
+                                   _stream(stream))
+    return _check(rc, "tg_comp_diag_ng_dev", numeric_ok=False)
+
+
 def comp_ng(fields, consts, o2_upd, o1_upd, he_upd):
     """comp_ng's column step (src/comp_ng.F90:74-332) on host arrays: fields
     COMP_FIELDS ((nk, ncol) Fortran order, fs (12, ncol, nk) C order = the
@@ -673,6 +713,41 @@ def oplus_ng_post_dev(fields, consts, opout, xiop2p, xiop2d, nk, ncol, ld, post,
                                     _dptr(Fe), _dptr(Fn), nk, ncol, ld, ctypes.byref(Pp),
                                     None if status is None else _int_dptr(status), _stream(stream))
     return _check(rc, "tg_oplus_ng_post_dev", numeric_ok=False)
+
+
+OPLUS_DIAG_NAMES = ("DOPDT", "OP_PROD", "OP_LOSS", "OP_DIFF", "OP_DRIFT", "OP_WIND")
+
+
+def oplus_diag_ng(fields, consts, opout, diffexp=None, vdotn_h=None, bdotdh_bvel=None):
+    """oplus_ng's history diagnostics (src/oplus_ng.F90:309-330) of the solution
+    on host arrays, with the horizontal terms (None: 0); returns a dict name ->
+    (nk, ncol) array."""
+    nk = opout.shape[0]
+    ncol = opout.size // nk
+    _check_sizes("oplus_diag_ng", fields, OPLUS_FIELDS, nk, ncol,
+                 two_d=("bx", "by", "bz", "dvb", "rlatm", "chi", "dipmag", "sndec", "csdec"), one_d=("zpint",),
+                 outs=(("opout", opout),))
+    for a, n in ((diffexp, "diffexp"), (vdotn_h, "vdotn_h"), (bdotdh_bvel, "bdotdh_bvel")):
+        if a is not None and np.size(a) != nk * ncol:
+            raise ValueError(f"oplus_diag_ng: {n} must hold nk*ncol values")
+    F = OplusFields(*[_host(fields[n], n) for n in OPLUS_FIELDS])
+    C = oplus_consts(consts)
+    h = [None if a is None else _host(a, n) for a, n in ((diffexp, "diffexp"), (vdotn_h, "vdotn_h"),
+                                                          (bdotdh_bvel, "bdotdh_bvel"))]
+    out = np.zeros((nk, ncol, len(OPLUS_DIAG_NAMES)), order="F")
+    _check(lib().tg_oplus_diag_ng(ctypes.byref(F), ctypes.byref(C), _host(opout, "opout"), *h, out.ctypes.data, nk,
+                                  ncol), "tg_oplus_diag_ng", numeric_ok=False)
+    return {n: out[:, :, i] for i, n in enumerate(OPLUS_DIAG_NAMES)}
+
+
+def oplus_diag_ng_dev(fields, consts, opout, diag, nk, ncol, ld, diffexp=None, vdotn_h=None, bdotdh_bvel=None,
+                      stream=None):
+    """Device form: level-major fields and solution, diag 6 planes of nk*ld."""
+    F = OplusFields(*[_dptr(fields[n]) for n in OPLUS_FIELDS])
+    C = oplus_consts(consts)
+    rc = lib().tg_oplus_diag_ng_dev(ctypes.byref(F), ctypes.byref(C), _dptr(opout), _dptr(diffexp), _dptr(vdotn_h),
+                                    _dptr(bdotdh_bvel), _dptr(diag), nk, ncol, ld, _stream(stream))
+    return _check(rc, "tg_oplus_diag_ng_dev", numeric_ok=False)
 
 
 def oplus_ng_factor_doubles(nk, ld):

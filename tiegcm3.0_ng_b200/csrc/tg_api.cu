@@ -1283,6 +1283,77 @@ __attribute__((visibility("default"))) int tg_comp_ng_dev(const tg_comp_fields *
     return TG_OK;
 }
 
+__attribute__((visibility("default"))) int tg_comp_diag_ng_dev(const tg_comp_fields *F, const tg_comp_consts *C,
+                                                               const double *upd, double *diag, int nk, int ncol,
+                                                               long ld, void *stream)
+{
+    if (!F || !C || !upd || !diag || nk < 3 || ncol < 0 || ld < ncol || !comp_fields_ok(F)) {
+        set_err("tg_comp_diag_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    if ((rc = grow(ws->scratch, sizeof(double) * comp_scratch_doubles(nk, ld > 0 ? ld : 1)))) return rc;
+    TG_CUDA(launch_comp_diag_ng(*F, *C, upd, nk, ncol, ld, diag, (double *)ws->scratch.p, st));
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_comp_diag_ng(const tg_comp_fields *F, const tg_comp_consts *C,
+                                                           const double *o2_upd, const double *o1_upd,
+                                                           const double *he_upd, double *diag, int nk, int ncol)
+{
+    if (!F || !C || !o2_upd || !o1_upd || !he_upd || !diag || nk < 3 || ncol < 0 || !comp_fields_ok(F)) {
+        set_err("tg_comp_diag_ng: bad arguments (nk=%d ncol=%d)", nk, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ld = round_up(ncol, 32);
+    Upload u{nullptr, nullptr, ld, (size_t)nk * ld, (size_t)nk * ncol, c->st[0]};
+    // 15 fields, 12 fs slabs and the 3 solution planes, then 24 diagnostic planes, 3 rows, 2 profiles
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (54 * u.lvl + 3 * (size_t)ld + 2 * (size_t)nk)))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * u.colsz))) return rc;
+    if ((rc = grow(c->scratch[0], sizeof(double) * comp_scratch_doubles(nk, ld)))) return rc;
+    u.base = (double *)c->lvlbuf[0][0].p;
+    u.stage = (double *)c->colbuf[0][0].p;
+    tg_comp_fields D;
+    const double *src3[15] = {F->tn, F->o2, F->o1, F->he, F->w, F->mbar, F->o2nm_smooth, F->o1nm_smooth,
+                              F->henm_smooth, F->o2_advec, F->o1_advec, F->he_advec, F->hdo2, F->hdo1, F->hdhe};
+    const double **dst3[15] = {&D.tn, &D.o2, &D.o1, &D.he, &D.w, &D.mbar, &D.o2nm_smooth, &D.o1nm_smooth,
+                               &D.henm_smooth, &D.o2_advec, &D.o1_advec, &D.he_advec, &D.hdo2, &D.hdo1, &D.hdhe};
+    for (int i = 0; i < 15; ++i)
+        if ((rc = upload3(u, nk, ncol, src3[i], i, dst3[i]))) return rc;
+    const double *ignored = nullptr;
+    for (int i = 0; i < 12; ++i)
+        if ((rc = upload3(u, nk, ncol, F->fs + (size_t)i * u.colsz, 15 + i, &ignored))) return rc;
+    D.fs = u.base + 15 * u.lvl;
+    const double *x3[3] = {o2_upd, o1_upd, he_upd};
+    for (int i = 0; i < 3; ++i)
+        if ((rc = upload3(u, nk, ncol, x3[i], 27 + i, &ignored))) return rc;
+    double *planes = u.base + 30 * u.lvl, *two = u.base + 54 * u.lvl, *one = two + 3 * ld;
+    const double *src2[3] = {F->tlbc, F->flx_he, F->dfactor};
+    const double **dst2[3] = {&D.tlbc, &D.flx_he, &D.dfactor};
+    for (int i = 0; i < 3; ++i) {
+        TG_CUDA(cudaMemcpyAsync(two + i * ld, src2[i], sizeof(double) * ncol, cudaMemcpyHostToDevice, u.st));
+        *dst2[i] = two + i * ld;
+    }
+    TG_CUDA(cudaMemcpyAsync(one, F->expz, sizeof(double) * nk, cudaMemcpyHostToDevice, u.st));
+    TG_CUDA(cudaMemcpyAsync(one + nk, F->difk, sizeof(double) * nk, cudaMemcpyHostToDevice, u.st));
+    D.expz = one;
+    D.difk = one + nk;
+    TG_CUDA(launch_comp_diag_ng(D, *C, u.base + 27 * u.lvl, nk, ncol, ld, planes, (double *)c->scratch[0].p, u.st));
+    return download3(u, nk, ncol, planes, 24, diag);
+}
+
 __attribute__((visibility("default"))) int tg_comp_ng(const tg_comp_fields *F, const tg_comp_consts *C,
                                                       double *o2_upd, double *o1_upd, double *he_upd, int nk,
                                                       int ncol)
@@ -1859,6 +1930,73 @@ __attribute__((visibility("default"))) int tg_oplus_ng_solve_dev(const tg_oplus_
         TG_CUDA(cudaGetLastError());
     }
     return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_oplus_diag_ng_dev(const tg_oplus_fields *F, const tg_oplus_consts *C,
+                                                                const double *opout, const double *diffexp,
+                                                                const double *vdotn_h, const double *bdotdh_bvel,
+                                                                double *diag, int nk, int ncol, long ld, void *stream)
+{
+    if (!F || !C || !opout || !diag || nk < 3 || ncol < 0 || ld < ncol || !oplus_fields_ok(F)) {
+        set_err("tg_oplus_diag_ng_dev: bad arguments (nk=%d ncol=%d ld=%ld)", nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    const size_t sbytes = sizeof(double) * oplus_scratch_planes() * (size_t)nk * (size_t)(ld > 0 ? ld : 1);
+    if ((rc = grow(ws->scratch, sbytes))) return rc;
+    TG_CUDA(launch_oplus_diag_ng(*F, *C, opout, diffexp, vdotn_h, bdotdh_bvel, nk, ncol, ld, diag,
+                                 (double *)ws->scratch.p, st));
+    return TG_OK;
+}
+
+__attribute__((visibility("default"))) int tg_oplus_diag_ng(const tg_oplus_fields *F, const tg_oplus_consts *C,
+                                                            const double *opout, const double *diffexp,
+                                                            const double *vdotn_h, const double *bdotdh_bvel,
+                                                            double *diag, int nk, int ncol)
+{
+    if (!F || !C || !opout || !diag || nk < 3 || ncol < 0 || !oplus_fields_ok(F)) {
+        set_err("tg_oplus_diag_ng: bad arguments (nk=%d ncol=%d)", nk, ncol);
+        return TG_EINVAL;
+    }
+    if (ncol == 0) return TG_OK;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TG_CUDA(cudaSetDevice(c->dev));
+    const long ld = round_up(ncol, 32);
+    Upload u{nullptr, nullptr, ld, (size_t)nk * ld, (size_t)nk * ncol, c->st[0]};
+    // 27 fields, the solution and 3 horizontal terms, then 6 diagnostic planes, 9 rows, zpint
+    if ((rc = grow(c->lvlbuf[0][0], sizeof(double) * (37 * u.lvl + 9 * (size_t)ld + (size_t)nk)))) return rc;
+    if ((rc = grow(c->colbuf[0][0], sizeof(double) * u.colsz))) return rc;
+    if ((rc = grow(c->scratch[0], sizeof(double) * oplus_scratch_planes() * u.lvl))) return rc;
+    u.base = (double *)c->lvlbuf[0][0].p;
+    u.stage = (double *)c->colbuf[0][0].p;
+    tg_oplus_fields D;
+    const double *const *src = &F->tn;
+    const double **dst = &D.tn;
+    for (int i = 0; i < 27; ++i)
+        if ((rc = upload3(u, nk, ncol, src[i], i, &dst[i]))) return rc;
+    const double *x = nullptr, *h[3] = {nullptr, nullptr, nullptr};
+    if ((rc = upload3(u, nk, ncol, opout, 27, &x))) return rc;
+    const double *hin[3] = {diffexp, vdotn_h, bdotdh_bvel};
+    for (int i = 0; i < 3; ++i)
+        if (hin[i] && (rc = upload3(u, nk, ncol, hin[i], 28 + i, &h[i]))) return rc;
+    double *planes = u.base + 31 * u.lvl, *two = u.base + 37 * u.lvl, *zp = two + 9 * ld;
+    for (int i = 0; i < 9; ++i) {
+        TG_CUDA(cudaMemcpyAsync(two + i * ld, src[27 + i], sizeof(double) * ncol, cudaMemcpyHostToDevice, u.st));
+        dst[27 + i] = two + i * ld;
+    }
+    TG_CUDA(cudaMemcpyAsync(zp, F->zpint, sizeof(double) * nk, cudaMemcpyHostToDevice, u.st));
+    D.zpint = zp;
+    TG_CUDA(launch_oplus_diag_ng(D, *C, x, h[0], h[1], h[2], nk, ncol, ld, planes, (double *)c->scratch[0].p, u.st));
+    return download3(u, nk, ncol, planes, 6, diag);
 }
 
 __attribute__((visibility("default"))) int tg_oplus_ng(const tg_oplus_fields *F, const tg_oplus_consts *C,

@@ -1714,6 +1714,105 @@ __global__ void __launch_bounds__(kCompWalkThreads) k_comp_walk(CompFields F, Co
               status, pd);
 }
 
+// ---------------------------------------------------------------------------
+// comp_ng's history diagnostics (src/comp_ng.F90:334-380) from the fields and
+// the solution x (three level-major planes O2, O, He, before the lateral
+// overwrite and the post steps): 24 planes in the order of the addfld calls,
+// D<sp>DT, <sp>_PROD, _LOSS, _HORDIF, _MOLDIF, _EDDYDIF, -_VERADV, -_HORADV
+// for sp = O2, O1, HE.  loss and moldif are summed over their fourth index,
+// the row's species, from 0 (sum(..., dim=4)); MOLDIF, EDDYDIF and VERADV,
+// which the reference leaves unset on the first and top levels, are 0 there.
+// One thread per (level, column); ep, ak and wks4 of levels k and k+1 from
+// the planes k_comp_levels wrote (its fractional powers within a few ulp of
+// the host library's: MOLDIF and EDDYDIF to a tolerance), everything else
+// bit-identical.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_comp_diag_ng(CompFields F, CompConsts C, const double *lv, const double *x,
+                                                      int nk, int ncol, long ld, double *diag)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int k = blockIdx.y;
+    const long slab = (long)nk * ld, o = (long)k * ld + col;
+    const double dz = C.dz, rdz = xd(1.0, dz);
+    auto X = [&](int i, int kk) { return __ldg(x + i * slab + (long)kk * ld + col); };
+    auto D = [&](int n) -> double & { return diag[(long)n * slab + o]; };
+    const double *nms[3] = {F.o2nm_smooth, F.o1nm_smooth, F.henm_smooth};
+    const double *adv[3] = {F.o2_advec, F.o1_advec, F.he_advec};
+    const double *hd[3] = {F.hdo2, F.hdo1, F.hdhe};
+    double xk[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        xk[i] = X(i, k);
+        D(i) = xm(C.dtx2inv, xs(xk[i], __ldg(nms[i] + o)));
+        D(3 + i) = __ldg(F.fs + (long)i * slab + o);
+        D(9 + i) = __ldg(hd[i] + o);
+        D(21 + i) = -__ldg(adv[i] + o);
+    }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        double s = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) s = xa(s, xm(__ldg(F.fs + (long)((m + 1) * 3 + i) * slab + o), xk[m]));
+        D(6 + m) = s;
+    }
+    if (k == 0 || k == nk - 1) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) D(12 + i) = D(15 + i) = D(18 + i) = 0.0;
+        return;
+    }
+    CompPlaneSrc src{{F, ld, col, nk}, lv};
+    CompLevel Lk, Lp;
+    src.load(k, Lk);
+    src.load(k + 1, Lp);
+    const double difk0 = __ldg(F.difk + k), difk1 = __ldg(F.difk + k + 1);
+    const double eddyp = xm(xm(C.expzmid_inv, difk0), xs(rdz, Lk.wks4));
+    const double eddyr = xm(xm(C.expzmid, difk1), xa(rdz, Lp.wks4));
+    const double eddyq =
+        xa(xm(xm(C.expzmid_inv, difk0), xa(rdz, Lk.wks4)), xm(xm(C.expzmid, difk1), xs(rdz, Lp.wks4)));
+    const double emd = xd(xd(1.0, __ldg(F.expz + k)), dz);
+    double xm1[3], xp1[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        xm1[i] = X(i, k - 1);
+        xp1[i] = X(i, k + 1);
+    }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const double hk = xd(Lk.ep[m], 2.0), hp = xd(Lp.ep[m], 2.0);
+        double s = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int e = i + 3 * m;
+            const double molp = xm(Lk.ak[e], xa(rdz, hk));
+            const double molr = xm(Lp.ak[e], xs(rdz, hp));
+            const double molq = xa(xm(Lk.ak[e], xs(rdz, hk)), xm(Lp.ak[e], xa(rdz, hp)));
+            s = xa(s, -xm(emd, xa(xs(xm(molp, xm1[m]), xm(molq, xk[m])), xm(molr, xp1[m]))));
+        }
+        D(12 + m) = s;
+    }
+    const double dfac = __ldg(F.dfactor + col);
+    const double wi = xm(0.5, xa(__ldg(F.w + o), __ldg(F.w + o + ld)));
+    const double wdz = xd(wi, xm(2.0, dz));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        D(15 + i) = xm(xm(rdz, xa(xs(xm(eddyp, xm1[i]), xm(eddyq, xk[i])), xm(eddyr, xp1[i]))), dfac);
+        D(18 + i) = -xm(wdz, xs(xp1[i], xm1[i]));
+    }
+}
+
+cudaError_t launch_comp_diag_ng(const CompFields &F, const CompConsts &C, const double *x, int nk, int ncol, long ld,
+                                double *diag, double *scratch, cudaStream_t st)
+{
+    if (ncol <= 0) return cudaSuccess;
+    if (nk < 3) return cudaErrorInvalidValue;
+    const int T = 128;
+    double *lv = scratch + 12 * (long)nk * ld;
+    k_comp_levels<<<dim3((ncol + T - 1) / T, nk), T, 0, st>>>(F, C, lv, nk, ncol, ld);
+    k_comp_diag_ng<<<dim3((ncol + T - 1) / T, nk), T, 0, st>>>(F, C, lv, x, nk, ncol, ld, diag);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out, double *scratch, int nk, int ncol,
                            long ld, double *sys_out, unsigned *status, cudaStream_t st)
 {

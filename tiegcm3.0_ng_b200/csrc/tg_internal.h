@@ -223,6 +223,10 @@ typedef tg_comp_consts CompConsts;
 // in the two-pass form, the level planes)
 cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out, double *scratch, int nk, int ncol,
                            long ld, double *sys_out, unsigned *status, cudaStream_t st);
+// comp_ng's 24 history diagnostics of the solution x (3 planes); scratch as
+// for launch_comp_ng.
+cudaError_t launch_comp_diag_ng(const CompFields &F, const CompConsts &C, const double *x, int nk, int ncol, long ld,
+                                double *diag, double *scratch, cudaStream_t st);
 size_t comp_scratch_doubles(int nk, long ld);
 // bnd_mask (per column, nonzero = lateral boundary) and bnd3 (o2, o1, he
 // boundary values) are optional: the overwrite the caller otherwise makes.
@@ -262,6 +266,11 @@ cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *
 // solve from it with that sub-step's optm1_smooth2 and explicit_h.
 cudaError_t launch_oplus_factor(const OplusFields &F, const OplusConsts &C, double *xiop2p, double *xiop2d,
                                 double *factor, int nk, int ncol, long ld, unsigned *status, cudaStream_t st);
+// oplus_ng's 6 history diagnostics of the solution x; the horizontal terms
+// may be NULL; scratch of oplus_scratch_planes() planes.
+cudaError_t launch_oplus_diag_ng(const OplusFields &F, const OplusConsts &C, const double *x, const double *diffexp,
+                                 const double *vdotn_h, const double *bdotdh_bvel, int nk, int ncol, long ld,
+                                 double *diag, double *scratch, cudaStream_t st);
 cudaError_t launch_oplus_solve(const OplusFields &F, const OplusConsts &C, const double *factor, double *opout, int nk,
                                int ncol, long ld, unsigned *status, cudaStream_t st, const PostStep *post = nullptr);
 int oplus_scratch_planes();   // level-major scratch planes of launch_oplus_ng (each nk*ld doubles)

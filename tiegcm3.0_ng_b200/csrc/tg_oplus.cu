@@ -186,13 +186,10 @@ __device__ __forceinline__ OplusCol oplus_col(const OplusFields &F, const OplusC
     return c;
 }
 
-// Row k (0..nk-2) of the O+ system: p, q, r and the right-hand side, with
-// both boundary folds (oplus_ng.F90:255-303).
-// t_top and t_bot receive the boundary terms the right-hand side takes at
-// k = nk-2 and k = 0 (when given).
-__device__ __forceinline__ void oplus_row(const OplusFields &F, const OplusConsts &C, const OplusRowsAt &A,
-                                          const OplusCol &cc, int k, double &p, double &q, double &r, double &ex,
-                                          double *t_top = nullptr, double *t_bot = nullptr)
+// The diffusion, drift and wind parts of row k's coefficients (oplus_ng.F90:
+// 255-282): {diffp, diffq, diffr, driftp, driftq, driftr, windp, windq, windr}.
+__device__ __forceinline__ void oplus_parts(const OplusFields &F, const OplusConsts &C, const OplusRowsAt &A,
+                                            const OplusCol &cc, int k, double (&pt)[9])
 {
     const int nk = A.nk;
     const long ld = A.ld, col = A.col;
@@ -207,22 +204,37 @@ __device__ __forceinline__ void oplus_row(const OplusFields &F, const OplusConst
     const double dji_k = A.djint(k), dji_1 = A.djint(k + 1);
     const double t0k = A.tph0(k), t1k = A.tph1(k), t01 = A.tph0(k + 1), t11 = A.tph1(k + 1);
     const double hdz_k = A.S(S_HDZ, k);
-    const double diffp = xm(xm(hdzm_k, dji_k), t0k);
-    const double diffq = -xa(xm(xm(hdzp_k, dji_1), t01), xm(xm(hdzm_k, dji_k), t1k));
-    const double diffr = xm(xm(hdzp_k, dji_1), t11);
+    pt[0] = xm(xm(hdzm_k, dji_k), t0k);
+    pt[1] = -xa(xm(xm(hdzp_k, dji_1), t01), xm(xm(hdzm_k, dji_k), t1k));
+    pt[2] = xm(xm(hdzp_k, dji_1), t11);
     const double wii = up(F.wi, k, nk, ld, col);
-    const double driftp = xm(xm(wii, 0.5), hdz_k);
-    const double driftq = xd(xm(-wii, 6.), C.re);
-    const double driftr = xm(xm(-wii, 0.5), hdz_k);
+    pt[3] = xm(xm(wii, 0.5), hdz_k);
+    pt[4] = xd(xm(-wii, 6.), C.re);
+    pt[5] = xm(xm(-wii, 0.5), hdz_k);
     const double bu_k = A.S(S_BDOTU, k);
-    const double windp = k == 0 ? xm(xm(xm(bz, xs(xm(2., bu_k), A.S(S_BDOTU, 1))), 0.5), hdz_k)
-                                : xm(xm(xm(bz, A.S(S_BDOTU, k - 1)), 0.5), hdz_k);
-    const double windq = xm(xm(-bu_k, cc.dvbz), bz);
-    const double windr = k == nk - 2 ? xm(xm(xm(bz, xs(xm(2., bu_k), A.S(S_BDOTU, k - 1 >= 0 ? k - 1 : 0))), 0.5), hdz_k)
-                                     : xm(xm(xm(-bz, A.S(S_BDOTU, k + 1)), 0.5), hdz_k);
-    p = xa(xa(diffp, driftp), windp);
-    q = xs(xa(xa(diffq, driftq), windq), cc.dtn);
-    r = xa(xa(diffr, driftr), windr);
+    pt[6] = k == 0 ? xm(xm(xm(bz, xs(xm(2., bu_k), A.S(S_BDOTU, 1))), 0.5), hdz_k)
+                   : xm(xm(xm(bz, A.S(S_BDOTU, k - 1)), 0.5), hdz_k);
+    pt[7] = xm(xm(-bu_k, cc.dvbz), bz);
+    pt[8] = k == nk - 2 ? xm(xm(xm(bz, xs(xm(2., bu_k), A.S(S_BDOTU, k - 1 >= 0 ? k - 1 : 0))), 0.5), hdz_k)
+                        : xm(xm(xm(-bz, A.S(S_BDOTU, k + 1)), 0.5), hdz_k);
+}
+
+// Row k (0..nk-2) of the O+ system: p, q, r and the right-hand side, with
+// both boundary folds (oplus_ng.F90:255-303).
+// t_top and t_bot receive the boundary terms the right-hand side takes at
+// k = nk-2 and k = 0 (when given).
+__device__ __forceinline__ void oplus_row(const OplusFields &F, const OplusConsts &C, const OplusRowsAt &A,
+                                          const OplusCol &cc, int k, double &p, double &q, double &r, double &ex,
+                                          double *t_top = nullptr, double *t_bot = nullptr)
+{
+    const int nk = A.nk;
+    const long ld = A.ld, col = A.col;
+    auto at = [&](const double *pp, int kk) { return __ldg(pp + kk * ld + col); };
+    double pt[9];
+    oplus_parts(F, C, A, cc, k, pt);
+    p = xa(xa(pt[0], pt[3]), pt[6]);
+    q = xs(xa(xa(pt[1], pt[4]), pt[7]), cc.dtn);
+    r = xa(xa(pt[2], pt[5]), pt[8]);
     ex = xs(at(F.explicit_h, k), xm(xm(at(F.optm1_smooth2, k), C.dtx2inv), (double)C.nstep_sub));
     if (k == nk - 2) {
         q = xa(q, xm(xd(cc.ubcb, cc.ubca), r));
@@ -548,6 +560,60 @@ __global__ void __launch_bounds__(kSolveThreads) k_oplus_solve(OplusFields F, Op
         }
     }
     if (status && !fin) atomicOr(status, FLAG_NONFINITE);
+}
+
+// ---- oplus_ng's history diagnostics (oplus_ng.F90:309-330) ----------------
+// Of the solution x (rows 1..nk, the top included, before the lateral
+// overwrite and the post steps), one thread per (level, column): DOPDT,
+// OP_PROD, OP_LOSS (= -op_loss*x), and on levels 2..nk-1 (1-based; 0 on the
+// others, which the reference leaves unset) OP_DIFF, OP_DRIFT, OP_WIND: the
+// horizontal term (diffexp, -vdotn_h, -bdotdh_bvel; 0 when not given) plus
+// the vertical part's coefficients times x at k-1, k, k+1.
+__global__ void __launch_bounds__(128) k_oplus_diag_ng(OplusFields F, OplusConsts C, const double *scr,
+                                                       const double *x, const double *diffexp, const double *vdotn_h,
+                                                       const double *bdotdh_bvel, int nk, int ncol, long ld,
+                                                       double *diag)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int k = blockIdx.y;
+    const long slab = (long)nk * ld, o = (long)k * ld + col;
+    auto D = [&](int n) -> double & { return diag[(long)n * slab + o]; };
+    const double xk = __ldg(x + o);
+    D(0) = xm(xm(xs(xk, __ldg(F.optm1_smooth2 + o)), C.dtx2inv), (double)C.nstep_sub);
+    D(1) = scr[S_PROD * slab + o];
+    D(2) = -xm(scr[S_OL * slab + o], xk);
+    if (k == 0 || k == nk - 1) {
+        D(3) = D(4) = D(5) = 0.0;
+        return;
+    }
+    OplusRowsAt A{scr, slab, ld, col, nk, 0., 0., 0.};
+    const OplusCol cc = oplus_col(F, C, A);
+    A.gmr = cc.gmr;
+    double pt[9];
+    oplus_parts(F, C, A, cc, k, pt);
+    const double xm1 = __ldg(x + o - ld), xp1 = __ldg(x + o + ld);
+    const double *h3[3] = {diffexp, vdotn_h, bdotdh_bvel};
+#pragma unroll
+    for (int n = 0; n < 3; ++n) {
+        const double hz = h3[n] ? __ldg(h3[n] + o) : 0.0;
+        D(3 + n) = xa(xa(xa(n == 0 ? hz : -hz, xm(pt[3 * n], xm1)), xm(pt[3 * n + 1], xk)), xm(pt[3 * n + 2], xp1));
+    }
+}
+
+cudaError_t launch_oplus_diag_ng(const OplusFields &F, const OplusConsts &C, const double *x, const double *diffexp,
+                                 const double *vdotn_h, const double *bdotdh_bvel, int nk, int ncol, long ld,
+                                 double *diag, double *scratch, cudaStream_t st)
+{
+    if (ncol <= 0) return cudaSuccess;
+    if (nk < 3) return cudaErrorInvalidValue;
+    const long slab = (long)nk * ld;
+    // the level planes; the ion rates it also writes go to unused scratch planes
+    k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch + S_W1 * slab, scratch + S_Y1 * slab,
+                                                                 nullptr, nullptr, scratch, nk, ncol, ld);
+    k_oplus_diag_ng<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, scratch, x, diffexp, vdotn_h, bdotdh_bvel,
+                                                                  nk, ncol, ld, diag);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_oplus_factor(const OplusFields &F, const OplusConsts &C, double *xiop2p, double *xiop2d,
