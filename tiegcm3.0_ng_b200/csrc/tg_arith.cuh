@@ -81,6 +81,18 @@ __device__ __forceinline__ void post_prefetch(const P &post, bool on, bool bcol,
 // is filtered, nm = ds2*(prev + x) + ds*cur, and both are floored (a floor
 // keeps v when v > floor, NaN included otherwise).  The same operations as
 // the reference's statements and as tg_time_filter_ng.
+// post_store with the previous- and current-step values already read (the
+// shared-memory tile walks copy them in with the rows).
+template <class P>
+__device__ __forceinline__ void post_store_v(const P &post, bool bcol, double *out, long o, double x, double prev,
+                                             double cur)
+{
+    if (bcol) x = __ldg(post.bnd + o);
+    const double n = __dadd_rn(__dmul_rn(post.ds2, __dadd_rn(prev, x)), __dmul_rn(post.ds, cur));
+    post.nm[o] = (!post.floor_nm || n > post.floor) ? n : post.floor;
+    out[o] = x > post.floor ? x : post.floor;
+}
+
 template <class P>
 __device__ __forceinline__ void post_store(const P &post, bool on, bool bcol, double *out, long o, double x)
 {

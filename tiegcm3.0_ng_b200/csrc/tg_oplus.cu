@@ -456,6 +456,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_oplus_solve_tile(OplusFields 
     const long slab = (long)nk * ld;
     double *sp = solve_tile, *sw1 = sp + (long)K * T, *sy1 = sw1 + (long)K * T, *sw2 = sy1 + (long)K * T;
     double *sxh = sw2 + (long)K * T, *som = sxh + (long)K * T, *spr = som + (long)K * T;
+    // with the post-solve steps, prev and cur of the nk stored rows come in too
+    double *sprev = spr + (long)K * T, *scur = sprev + (long)nk * T;
     auto cp8 = [](double *dst, const double *src) {
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
                      "l"(src)
@@ -472,6 +474,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_oplus_solve_tile(OplusFields 
         cp8(som + s, F.optm1_smooth2 + o);
         cp8(spr + s, scr + S_PROD * slab + o);
     }
+    if (has_post)
+        for (int k = 0; k < nk; ++k) {
+            const long o = (long)k * ld + col;
+            cp8(sprev + k * T + t, post.prev + o);
+            cp8(scur + k * T + t, post.cur + o);
+        }
     asm volatile("cp.async.commit_group;" ::: "memory");
     const double t_top = scr[S_TB * slab + col], t_bot = scr[S_TB * slab + ld + col];
     asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -499,10 +507,16 @@ __global__ void __launch_bounds__(kSolveThreads) k_oplus_solve_tile(OplusFields 
         som[s] = xn;
     }
     const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
-#pragma unroll 4
-    for (int k = 0; k < K; ++k) post_store(post, has_post, bcol, opout, (long)k * ld + col, som[k * T + t]);
     // opout(nk) = opout(nk-1)**2/opout(nk-2) from the unfiltered values (oplus_ng.F90:307)
-    post_store(post, has_post, bcol, opout, (long)K * ld + col, xd(xm(xtop, xtop), som[(K - 2) * T + t]));
+    const double xk = xd(xm(xtop, xtop), som[(K - 2) * T + t]);
+    if (has_post) {
+        for (int k = 0; k < K; ++k)
+            post_store_v(post, bcol, opout, (long)k * ld + col, som[k * T + t], sprev[k * T + t], scur[k * T + t]);
+        post_store_v(post, bcol, opout, (long)K * ld + col, xk, sprev[K * T + t], scur[K * T + t]);
+    } else {
+        for (int k = 0; k < K; ++k) opout[(long)k * ld + col] = som[k * T + t];
+        opout[(long)K * ld + col] = xk;
+    }
     if (status && !fin) atomicOr(status, FLAG_NONFINITE);
 }
 
@@ -635,7 +649,7 @@ cudaError_t launch_oplus_solve(const OplusFields &F, const OplusConsts &C, const
     if (nk < 3) return cudaErrorInvalidValue;
     const PostStep pv = post ? *post : PostStep{};
     const int hp = post != nullptr;
-    const size_t tile = (size_t)kSolveThreads * 7 * (nk - 1) * sizeof(double);
+    const size_t tile = (size_t)kSolveThreads * (7 * (nk - 1) + (post ? 2 * nk : 0)) * sizeof(double);
     const int T = kSolveThreads;
     if (ncol <= kSmallWalkColumns && tile <= (size_t)smem_optin()) {
         once_per_device([] {

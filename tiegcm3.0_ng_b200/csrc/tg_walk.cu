@@ -107,6 +107,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_thomas_post_tile(const double 
     if (col >= ncol) return;
     const int T = kWalkThreads, t = threadIdx.x;
     double *sp = tile_walk, *sq = sp + (long)K * T, *sr = sq + (long)K * T, *sf = sr + (long)K * T;
+    // with the post-solve steps, prev and cur of every stored row (K, and the
+    // top row for top = 1) come in with the rows
+    const int KS = top == 1 ? K + 1 : K;
+    double *sprev = sf + (long)K * T, *scur = sprev + (long)KS * T;
     auto cp8 = [](double *dst, const double *src) {
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
                      "l"(src)
@@ -120,6 +124,12 @@ __global__ void __launch_bounds__(kWalkThreads) k_thomas_post_tile(const double 
         cp8(sr + s, R + o);
         cp8(sf + s, Fv + o);
     }
+    if (has_post)
+        for (int k = 0; k < KS; ++k) {
+            const long o = (long)k * ld + col;
+            cp8(sprev + k * T + t, post.prev + o);
+            cp8(scur + k * T + t, post.cur + o);
+        }
     asm volatile("cp.async.commit_group;" ::: "memory");
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     bool ok = true;
@@ -151,10 +161,16 @@ __global__ void __launch_bounds__(kWalkThreads) k_thomas_post_tile(const double 
         sq[s] = xn;
     }
     const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
-#pragma unroll 4
-    for (int k = 0; k < K; ++k) post_store(post, has_post, bcol, x, (long)k * ld + col, sq[k * T + t]);
     // x(nk-1) = x(nk-2)**2/x(nk-3) from the unfiltered values
-    if (top == 1) post_store(post, has_post, bcol, x, (long)K * ld + col, xd(xm(xtop, xtop), sq[(K - 2) * T + t]));
+    const double xk = top == 1 ? xd(xm(xtop, xtop), sq[(K - 2) * T + t]) : 0.0;
+    if (has_post) {
+        for (int k = 0; k < K; ++k)
+            post_store_v(post, bcol, x, (long)k * ld + col, sq[k * T + t], sprev[k * T + t], scur[k * T + t]);
+        if (top == 1) post_store_v(post, bcol, x, (long)K * ld + col, xk, sprev[K * T + t], scur[K * T + t]);
+    } else {
+        for (int k = 0; k < K; ++k) x[(long)k * ld + col] = sq[k * T + t];
+        if (top == 1) x[(long)K * ld + col] = xk;
+    }
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 }  // namespace
@@ -165,7 +181,7 @@ cudaError_t launch_thomas_post(const double *p, const double *q, const double *r
 {
     if (ncol <= 0) return cudaSuccess;
     if (K < 1 || K > nk || (top == 1 && (K != nk - 1 || K < 2))) return cudaErrorInvalidValue;
-    const size_t tile = (size_t)kWalkThreads * 4 * K * sizeof(double);
+    const size_t tile = (size_t)kWalkThreads * (4 * K + (post ? 2 * (top == 1 ? K + 1 : K) : 0)) * sizeof(double);
     if (ncol <= kSmallWalkColumns && tile <= (size_t)smem_optin()) {
         once_per_device([] {
             cudaFuncSetAttribute(k_thomas_post_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());

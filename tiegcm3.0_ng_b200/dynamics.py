@@ -186,7 +186,9 @@ class DynamicsStep:
             bnd=[lvl(c[sp + "_bnd"]) for sp in ("o2", "o1", "he")],
             out=torch.zeros((3, nk, ld), dtype=torch.float64, device=device),
             nm=torch.zeros((3, nk, ld), dtype=torch.float64, device=device))
-        self.streams = [torch.cuda.Stream(device=device) for _ in range(4)] if fan_out else []
+        # the O+ sub-cycle is the step's longest chain: its stream gets the higher priority
+        self.streams = ([torch.cuda.Stream(device=device, priority=-1)] +
+                        [torch.cuda.Stream(device=device) for _ in range(3)]) if fan_out else []
         self.graph = None
 
     # ---- the routines, each on one stream --------------------------------
