@@ -728,8 +728,11 @@ int tg_set_kind_overlap(int mode);
 
 /* Host-array entries (tg_solve_host and the per-routine drop-ins): the input
  * bytes per pipelined column chunk, in KiB, and the number of streams the
- * chunks rotate over (1..8); <= 0 restores the defaults (streams 3; chunks of
- * a sixth of the call's input bytes, kept within 4..64 MiB). */
+ * chunks rotate over (1..8); <= 0 restores the defaults (streams 4; chunks of
+ * a sixth of the call's input bytes, kept within 4..64 MiB).  Consecutive
+ * chunks whose input arrays lie side by side in one page-locked allocation
+ * (gaps at most an eighth of the bytes) cross the link in one copy per run
+ * of up to max(chunk, 8 MiB) bytes instead of one copy per array. */
 int tg_set_host_pipeline(int chunk_kb, int streams);
 
 /* Runs the ring kernels' bounded mbarrier wait on a barrier that nothing

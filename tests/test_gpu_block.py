@@ -130,3 +130,43 @@ def test_solve_host_chunking_keeps_bits(cuda, pkg, orc, chunk_kb, streams):
         pkg.set_host_pipeline(0, 0)
     for q, ref in zip(systems, refs):
         assert np.array_equal(q["x"], ref)
+
+
+@pytest.mark.parametrize("chunk_kb,streams", [(0, 0), (1024, 2)])
+def test_solve_host_arena_keeps_bits(cuda, pkg, orc, chunk_kb, streams):
+    """Systems whose arrays lie side by side in one page-locked arena (the
+    input copies of consecutive chunks then merge into one per run), with
+    small gaps and one system outside the arena, give the oracle's bits."""
+    torch = cuda
+    shapes = [(57, 2072), (57, 2072), (29, 777), (57, 3001)]
+    nbytes = sum(5 * nk * ncol * 8 + 5 * 64 for nk, ncol in shapes) + 4096
+    arena = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+    off = 0
+    systems, refs = [], []
+
+    def take(shape):
+        nonlocal off
+        v = np.ndarray(shape, dtype=np.float64, buffer=arena, offset=off, order="F")
+        off += int(np.prod(shape)) * 8 + 64          # a 64-byte gap after every array
+        return v
+
+    for i, (nk, ncol) in enumerate(shapes):
+        a, b, c, f = pkg.synth.scalar_system(nk, ncol, 14.0 / (nk - 1), 800 + i)
+        if i == 3:            # outside the arena: separate host arrays
+            arrs = [a, b, c, f, np.zeros_like(a, order="F")]
+        else:
+            arrs = [take((nk, ncol)) for _ in range(5)]
+            for v, w in zip(arrs, (a, b, c, f)):
+                np.copyto(v, w)
+            arrs[4][...] = 0.0
+        systems.append(dict(kind=pkg.TG_KIND_SCALAR, a=arrs[0], b=arrs[1], c=arrs[2], f=arrs[3], x=arrs[4],
+                            k2=nk - (i % 2)))
+        refs.append(orc.trsolv_ng(a, b, c, f, nk - (i % 2)))
+    pkg.set_host_pipeline(chunk_kb, streams)
+    try:
+        assert pkg.solve_host(systems) == pkg.TG_OK
+    finally:
+        pkg.set_host_pipeline(0, 0)
+    for q, ref in zip(systems, refs):
+        k2 = q["k2"]
+        assert np.array_equal(q["x"][:k2], ref[:k2])
