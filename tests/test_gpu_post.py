@@ -9,8 +9,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _level(pkg, torch, F, nk, ncol, one_d):
-    ld = pkg.batch.pad_ld(ncol)
+def _level(pkg, torch, F, nk, ncol, one_d, ld=None):
+    ld = pkg.batch.pad_ld(ncol) if ld is None else ld
     dev = {}
     for k, v in F.items():
         if k == "fs":
@@ -120,23 +120,27 @@ def test_oplus_post_fused_without_mask(cuda, pkg):
     assert torch.equal(y[1][:, :ncol], outs[1][:, :ncol])
 
 
-@pytest.mark.parametrize("ncol", [1500, 17000], ids=["walk_prefetch_8", "walk_prefetch_1"])
-def test_three_pass_gives_the_two_pass_bits(cuda, pkg, ncol):
+@pytest.mark.parametrize("ncol,odd_ld", [(1500, False), (1500, True), (17000, False)],
+                         ids=["tile_bulk_rows", "tile_odd_ld", "global_reads"])
+def test_three_pass_gives_the_two_pass_bits(cuda, pkg, ncol, odd_ld):
     """Assembly mode 2 (rows formed one thread per level and column, then the
     recurrence alone) gives the bits of mode 1, with and without the fused
-    post-solve steps, for dt_ng, minor_ng and oplus_ng."""
+    post-solve steps, for dt_ng, minor_ng and oplus_ng: with the column tile
+    in shared memory (bulk row copies, or 8-byte copies when the column stride
+    leaves the rows unaligned) and on larger launches."""
     torch = cuda
     nk, dz = 57, 0.25
+    lds = ncol + 5 if odd_ld else None
     cases = []
     F, C = pkg.synth.dt_inputs(nk, ncol, dz, 21)
-    dev, ld = _level(pkg, torch, F, nk, ncol, ("expz", "dift"))
+    dev, ld = _level(pkg, torch, F, nk, ncol, ("expz", "dift"), lds)
     cases.append(("dt", dev, C, dev["tn"], pkg.dt_ng_dev, pkg.dt_ng_post_dev, 50.0, 1500.0))
     F, C = pkg.synth.minor_inputs(nk, ncol, dz, 22)
-    dev, ld = _level(pkg, torch, F, nk, ncol, ("expz", "difk"))
+    dev, ld = _level(pkg, torch, F, nk, ncol, ("expz", "difk"), lds)
     cur = pkg.batch.level_scalar(np.asfortranarray(np.abs(F["ftm1_smooth"])), ld, "cuda")
     cases.append(("minor", dev, C, cur, pkg.minor_ng_dev, pkg.minor_ng_post_dev, -1e-9, 1e-5))
     F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 23)
-    dev, ld = _level(pkg, torch, F, nk, ncol, ("zpint",))
+    dev, ld = _level(pkg, torch, F, nk, ncol, ("zpint",), lds)
     cases.append(("oplus", dev, C, dev["op"], None, None, 0.0, 1e6))
     z = lambda: torch.zeros((nk, ld), dtype=torch.float64, device="cuda")  # noqa: E731
     for name, dev, C, cur, plain, fused, lo, hi in cases:
@@ -194,15 +198,16 @@ def test_comp_three_pass_gives_the_two_pass_bits(cuda, pkg, ncol, calc_helium):
     assert torch.equal(got[1][1], got[2][1])
 
 
-@pytest.mark.parametrize("ncol", [1500, 17000], ids=["tile", "global_reads"])
-def test_oplus_factor_and_solve_give_the_full_step_bits(cuda, pkg, ncol):
+@pytest.mark.parametrize("ncol,odd_ld", [(1500, False), (1500, True), (17000, False)],
+                         ids=["tile_bulk_rows", "tile_odd_ld", "global_reads"])
+def test_oplus_factor_and_solve_give_the_full_step_bits(cuda, pkg, ncol, odd_ld):
     """The O+ sub-cycle: the rows and pivots formed once, then three sub-steps
     with new explicit_h, optm1_smooth2 and op each, with and without the
     post-solve steps, give tg_oplus_ng_dev / tg_oplus_ng_post_dev's bits."""
     torch = cuda
     nk, dz = 57, 0.25
     F, C = pkg.synth.oplus_inputs(nk, ncol, dz, 41, nstep_sub=3)
-    dev, ld = _level(pkg, torch, F, nk, ncol, ("zpint",))
+    dev, ld = _level(pkg, torch, F, nk, ncol, ("zpint",), ncol + 5 if odd_ld else None)
     z = lambda: torch.zeros((nk, ld), dtype=torch.float64, device="cuda")  # noqa: E731
     factor = torch.zeros(pkg.oplus_ng_factor_doubles(nk, ld), dtype=torch.float64, device="cuda")
     x2p, x2d = z(), z()

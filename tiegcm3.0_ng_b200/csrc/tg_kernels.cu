@@ -18,6 +18,7 @@
 
 #include "tg_internal.h"
 #include "tg_arith.cuh"
+#include "tg_bulk.cuh"
 
 namespace tg {
 
@@ -93,42 +94,6 @@ __device__ __forceinline__ void report(unsigned *status, int idx, unsigned flags
     if (flags && status) atomicOr(status + idx, flags);
 }
 
-// ---------------------------------------------------------------------------
-// Bulk asynchronous copies global -> shared (the TMA engine, 1-D form) with
-// mbarrier completion.  Each CTA copies only into its own shared memory.
-// Waits are bounded: kWaitLimit polls of mbarrier.try_wait (each poll may
-// suspend the thread for a short hardware-defined time) before giving up.
-// ---------------------------------------------------------------------------
-constexpr unsigned kWaitLimit = 1u << 22;
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void fence_proxy_async()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect(unsigned long long *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, unsigned long long *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
 // L2 eviction-priority policies (createpolicy): the coefficient streams are
 // read once (evict-first); the sweep's own scratch (w2, and w3 parked in x)
 // is re-read by the back sweep and should stay in L2 (evict-last).  With
@@ -177,25 +142,6 @@ __device__ __forceinline__ double ld_hint(const double *p, unsigned long long po
     asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol) : "memory");
     return v;
 }
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait of the whole warp; true when every lane saw the phase complete.
-__device__ __forceinline__ bool mbar_wait_warp(unsigned long long *bar, uint32_t parity, unsigned limit = kWaitLimit)
-{
-    bool done = false;
-#pragma unroll 1
-    for (unsigned i = 0; i < limit && !done; ++i) done = mbar_try_wait(bar, parity);
-    return __all_sync(0xffffffffu, done);
-}
-
 // Stage ring of a single-warp CTA: level k of NE arrays (W columns x 8 B
 // each) lands in stage (q % D), q the running level counter of the CTA.
 template <int NE, int D, int W = 32>
