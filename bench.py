@@ -70,7 +70,8 @@ def parse():
                    help="run only one kind's plan for a profiler: KIND:PREC[:VARIANT], KIND scalar|block, "
                         "PREC f64|refine, VARIANT reg:CPB:CPT[:PF], regg:CPB:1[:PF], ring[g]:DEPTH[:WARPS] "
                         "(default: library default); or dt / minor / comp / settei / oplus for the fused assembly+solve kernels, "
-                        "advec / smooth / filter for the horizontal operators and the time filter")
+                        "advec / smooth / filter for the horizontal operators and the time filter; "
+                        "dynamics:N for one dynamics step of grid N, serial on one stream")
     p.add_argument("--skip-assembly", action="store_true")
     p.add_argument("--tune", action="store_true",
                    help="run the autotuner over this workload's segments first and record its choices in the "
@@ -554,6 +555,22 @@ def run_profile(args):
     """Executes one kind's plan --warmup + --steps times (for ncu captures)."""
     import torch
     pkg = ge.load_package()
+    if args.profile.startswith("dynamics:"):
+        # one dynamics step of grid N of the workload, serial on one stream
+        dyn = pkg.dynamics
+        wl = pkg.synth.workload(args.config)
+        gi = int(args.profile.split(":")[1])
+        g = wl.grids[gi]
+        grid = (dyn.Grid(g.nk, g.nlon, g.nlat, g.dz) if gi == 0 else
+                dyn.Grid(g.nk, g.nlon, g.nlat, g.dz, lat0_deg=20.0, dlat_deg=2.5 / 2 ** gi))
+        ring = pkg.synth.RING_CHUNKS.get((g.nlon, g.nlat)) if gi == 0 else None
+        step = dyn.DynamicsStep(grid, dyn.synthetic_inputs(grid, 17 + gi, nstep_sub=10), ring=ring, fan_out=False)
+        stream = torch.cuda.Stream()
+        for _ in range(args.warmup + args.steps):
+            step.issue(stream)
+        stream.synchronize()
+        print(json.dumps({"profile": args.profile, "grid": g.name, "columns": grid.ncol, "steps": args.steps}))
+        return 0
     if args.profile in ("dt", "minor", "comp", "settei", "oplus", "advec", "smooth", "filter", "ring"):
         wl = pkg.synth.workload(args.config)
         if args.profile in ("advec", "smooth", "filter", "ring"):
