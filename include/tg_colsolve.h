@@ -730,9 +730,12 @@ int tg_set_kind_overlap(int mode);
  * bytes per pipelined column chunk, in KiB, and the number of streams the
  * chunks rotate over (1..8); <= 0 restores the defaults (streams 4; chunks of
  * a sixth of the call's input bytes, kept within 4..64 MiB).  Consecutive
- * chunks whose input arrays lie side by side in one page-locked allocation
- * (gaps at most an eighth of the bytes) cross the link in one copy per run
- * of up to max(chunk, 8 MiB) bytes instead of one copy per array. */
+ * chunks whose input arrays lie in one page-locked allocation, within a
+ * region of up to max(chunk, 8 MiB) bytes, form a run whose inputs cross the
+ * link in few copies instead of one per array: inputs that touch (gaps of up
+ * to 4 KiB) in one copy, equal inputs at one pitch (systems of one shape,
+ * each with its solution array between them) in one strided copy; nothing
+ * but inputs and those small gaps is copied. */
 int tg_set_host_pipeline(int chunk_kb, int streams);
 
 /* Runs the ring kernels' bounded mbarrier wait on a barrier that nothing

@@ -170,3 +170,50 @@ def test_solve_host_arena_keeps_bits(cuda, pkg, orc, chunk_kb, streams):
     for q, ref in zip(systems, refs):
         k2 = q["k2"]
         assert np.array_equal(q["x"][:k2], ref[:k2])
+
+
+@pytest.mark.parametrize("chunk_kb,streams", [(0, 0), (1024, 2), (300, 3)])
+def test_solve_host_arena_strided_copies_keep_bits(cuda, pkg, orc, chunk_kb, streams):
+    """Systems of one shape side by side in a page-locked arena, each followed
+    by its solution array (their inputs cross the link as strided copies
+    that skip the solutions), scalar and 2x2 block, give the oracle's bits;
+    the solution arrays between the inputs are left as the solve wrote them."""
+    torch = cuda
+    nk, ncol, B = 57, 1000, 2
+    shapes = [("s", (nk, ncol))] * 6 + [("b", None)] * 3
+    blk = [(B, B, nk, ncol)] * 3 + [(B, nk, ncol)] * 2
+    nbytes = sum(5 * nk * ncol * 8 + 5 * 256 for _ in range(6)) + 3 * sum(int(np.prod(s)) * 8 + 256 for s in blk)
+    arena = torch.empty(nbytes + 4096, dtype=torch.uint8, pin_memory=True).numpy()
+    off = 0
+
+    def take(shape):
+        nonlocal off
+        v = np.ndarray(shape, dtype=np.float64, buffer=arena, offset=off, order="F")
+        off += (int(np.prod(shape)) * 8 + 255) // 256 * 256
+        return v
+
+    systems, refs = [], []
+    for i, (kind, shp) in enumerate(shapes):
+        if kind == "s":
+            src = pkg.synth.scalar_system(nk, ncol, 0.25, 900 + i)
+            arrs = [take(shp) for _ in range(5)]
+        else:
+            src = pkg.synth.block_system(B, nk, ncol, 0.25, 900 + i)
+            arrs = [take(s) for s in blk]
+        for v, w in zip(arrs, src):
+            np.copyto(v, w)
+        arrs[4][...] = np.nan        # the solve overwrites every solution value
+        if kind == "s":
+            systems.append(dict(kind=pkg.TG_KIND_SCALAR, a=arrs[0], b=arrs[1], c=arrs[2], f=arrs[3], x=arrs[4],
+                                k2=nk))
+            refs.append(orc.trsolv_ng(*src, nk))
+        else:
+            systems.append(dict(kind=B, a=arrs[0], b=arrs[1], c=arrs[2], f=arrs[3], x=arrs[4], k2=nk))
+            refs.append(orc.blksolve(*src, nk))
+    pkg.set_host_pipeline(chunk_kb, streams)
+    try:
+        assert pkg.solve_host(systems) == pkg.TG_OK
+    finally:
+        pkg.set_host_pipeline(0, 0)
+    for q, ref in zip(systems, refs):
+        assert np.array_equal(q["x"], ref)

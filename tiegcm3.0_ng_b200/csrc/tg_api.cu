@@ -390,17 +390,25 @@ int host_solve_many(const HostSys *sys, int nsys, int precision)
         }
         TG_CUDA(cudaMemsetAsync(c->flags + s, 0, sizeof(unsigned), c->st[s]));
     }
-    // The chunks in issue order, each with the host region its inputs span.
-    // Consecutive chunks whose inputs lie in one region (a caller that keeps
-    // its systems' arrays side by side, as in one registered arena) form a
-    // run: its inputs cross the link in one copy instead of one per array,
-    // which on this part moves ~20% more bytes per second than ~1 MB copies.
+    // The chunks in issue order, each with the host ranges of its inputs.
+    // Consecutive chunks whose inputs lie in one page-locked region (a caller
+    // that keeps its systems' arrays side by side, as in one registered
+    // arena) form a run: a device buffer mirrors the region, and the inputs
+    // cross the link in few large copies instead of one per array (~1 MB
+    // copies move ~20% fewer bytes per second on this part).  Only the
+    // inputs are copied: ranges that touch merge into one copy, and equal
+    // ranges at a fixed pitch (systems of one shape, each followed by its
+    // solution array) into one strided copy.
+    struct Piece {
+        const char *lo, *hi;
+    };
     struct ChunkRef {
         int si;
         long c0, nc;
         const char *lo, *hi;   // region of the chunk's inputs (flat: each a single range)
-        long in_bytes;         // bytes of those ranges
         bool flat;
+        int npc;
+        Piece pc[6];
     };
     std::vector<ChunkRef> chunks;
     chunks.reserve(total_chunks);
@@ -409,7 +417,7 @@ int host_solve_many(const HostSys *sys, int nsys, int precision)
         const HostPlan &p = plans[si];
         for (long c0 = 0; c0 < h.ncol; c0 += p.chunk) {
             const long nc = std::min(p.chunk, h.ncol - c0);
-            ChunkRef ch{si, c0, nc, nullptr, nullptr, 0, true};
+            ChunkRef ch{si, c0, nc, nullptr, nullptr, true, 0, {}};
             auto add = [&](const double *base, long rows, long stride) {
                 if (rows != stride) {
                     ch.flat = false;
@@ -418,7 +426,7 @@ int host_solve_many(const HostSys *sys, int nsys, int precision)
                 const char *a = (const char *)(base + c0 * stride), *b = a + sizeof(double) * rows * nc;
                 ch.lo = ch.lo && ch.lo < a ? ch.lo : a;
                 ch.hi = ch.hi && ch.hi > b ? ch.hi : b;
-                ch.in_bytes += b - a;
+                ch.pc[ch.npc++] = Piece{a, b};
             };
             for (int i = 0; i < 3; ++i) add(h.m[i], p.mrows, p.mstride);
             add(h.v, p.vrows, h.colstride);
@@ -430,7 +438,7 @@ int host_solve_many(const HostSys *sys, int nsys, int precision)
     struct Run {
         size_t j0, j1;
         const char *lo;
-        long bytes;
+        long bytes;   // the region the device buffer mirrors (0: per-array copies)
     };
     std::vector<Run> runs;
     long max_span = 0;
@@ -439,19 +447,15 @@ int host_solve_many(const HostSys *sys, int nsys, int precision)
         Run r{j, j + 1, chunks[j].lo, 0};
         if (chunks[j].flat) {
             const char *lo = chunks[j].lo, *hi = chunks[j].hi;
-            long used = chunks[j].in_bytes;
             while (r.j1 < chunks.size() && chunks[r.j1].flat) {
                 const ChunkRef &n = chunks[r.j1];
                 const char *l2 = std::min(lo, n.lo), *h2 = std::max(hi, n.hi);
-                const long span = h2 - l2, u2 = used + n.in_bytes;
-                // at most an eighth of the copied bytes outside the inputs
-                if (span > run_cap || 8 * (span - u2) > span) break;
+                if (h2 - l2 > run_cap) break;
                 lo = l2;
                 hi = h2;
-                used = u2;
                 ++r.j1;
             }
-            if ((r.j1 - r.j0 > 1 || 8 * ((hi - lo) - used) <= hi - lo) && pinned_region(lo, hi)) {
+            if (hi - lo <= run_cap && pinned_region(lo, hi)) {
                 r.lo = lo;
                 r.bytes = hi - lo;
                 max_span = std::max(max_span, r.bytes);
@@ -460,6 +464,37 @@ int host_solve_many(const HostSys *sys, int nsys, int precision)
         runs.push_back(r);
         j = r.j1;
     }
+    // The copies of a run's inputs: the pieces in address order, merged where
+    // they touch (gaps of alignment padding included), then equal pieces at
+    // one pitch grouped into a strided copy.
+    std::vector<Piece> pieces;
+    auto copy_run = [&](const Run &run, char *dspan, cudaStream_t st) -> cudaError_t {
+        pieces.clear();
+        for (size_t jj = run.j0; jj < run.j1; ++jj)
+            for (int i = 0; i < chunks[jj].npc; ++i) pieces.push_back(chunks[jj].pc[i]);
+        std::sort(pieces.begin(), pieces.end(), [](const Piece &a, const Piece &b) { return a.lo < b.lo; });
+        size_t n = 0;
+        for (const Piece &q : pieces) {
+            if (n > 0 && q.lo <= pieces[n - 1].hi + 4096) {
+                pieces[n - 1].hi = std::max(pieces[n - 1].hi, q.hi);
+            } else {
+                pieces[n++] = q;
+            }
+        }
+        for (size_t i = 0; i < n;) {
+            const long w = pieces[i].hi - pieces[i].lo;
+            size_t e = i + 1;
+            const long pitch = e < n ? pieces[e].lo - pieces[i].lo : 0;
+            while (e < n && pieces[e].hi - pieces[e].lo == w && pieces[e].lo - pieces[e - 1].lo == pitch) ++e;
+            char *d = dspan + (pieces[i].lo - run.lo);
+            cudaError_t err = e - i > 1 ? cudaMemcpy2DAsync(d, pitch, pieces[i].lo, pitch, w, e - i,
+                                                            cudaMemcpyHostToDevice, st)
+                                        : cudaMemcpyAsync(d, pieces[i].lo, w, cudaMemcpyHostToDevice, st);
+            if (err != cudaSuccess) return err;
+            i = e;
+        }
+        return cudaSuccess;
+    };
     if (max_span > 0)
         for (int s = 0; s < nslots; ++s)
             if ((rc = grow(c->span[s], (size_t)max_span))) return rc;
@@ -468,8 +503,7 @@ int host_solve_many(const HostSys *sys, int nsys, int precision)
         const int s = (int)(ri % nslots);
         cudaStream_t st = c->st[s];
         const char *dspan = (const char *)c->span[s].p;
-        if (run.bytes > 0)
-            TG_CUDA(cudaMemcpyAsync(c->span[s].p, run.lo, run.bytes, cudaMemcpyHostToDevice, st));
+        if (run.bytes > 0) TG_CUDA(copy_run(run, (char *)c->span[s].p, st));
         // where a run's host array landed on the device
         auto in_span = [&](const double *host) { return (const double *)(dspan + ((const char *)host - run.lo)); };
         for (size_t jj = run.j0; jj < run.j1; ++jj) {

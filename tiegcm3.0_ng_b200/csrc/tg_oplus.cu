@@ -440,6 +440,54 @@ __global__ void __launch_bounds__(32) k_oplus_factor(double *scr, int nk, int nc
     if (status && !ok) atomicOr(status, FLAG_PIVOT);
 }
 
+// One asynchronous 8-byte copy global -> shared (cp.async).
+__device__ __forceinline__ void cp_async8(double *dst, const double *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+
+// The same pass for launches of few columns: the column tile's p, q, r rows
+// of every level are copied into shared memory at once (cp.async, every copy
+// in flight), then the recurrence runs from there.
+__global__ void __launch_bounds__(32) k_oplus_factor_tile(double *scr, int nk, int ncol, long ld, unsigned *status)
+{
+    extern __shared__ double factor_tile[];
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int T = 32, t = threadIdx.x, K = nk - 1;
+    const long slab = (long)nk * ld;
+    double *sp = factor_tile, *sq = sp + (long)K * T, *sr = sq + (long)K * T;
+    for (int k = 0; k < K; ++k) {
+        const long o = (long)k * ld + col;
+        const int s = k * T + t;
+        cp_async8(sp + s, scr + S_P * slab + o);
+        cp_async8(sq + s, scr + S_Q * slab + o);
+        cp_async8(sr + s, scr + S_R * slab + o);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    double *W1 = scr + S_W1 * slab, *Y1 = scr + S_Y1 * slab, *W2 = scr + S_W2 * slab;
+    bool ok = true;
+    double w1 = 0., y1 = 0.;
+    for (int k = 0; k < K; ++k) {
+        const long o = (long)k * ld + col;
+        const int s = k * T + t;
+        if (k == 0) {
+            w1 = sq[s];
+        } else {
+            const double w2 = qdiv(sr[s - T], w1, y1);
+            W2[o - ld] = w2;
+            w1 = xs(sq[s], xm(sp[s], w2));
+        }
+        y1 = __drcp_rn(w1);
+        ok = ok && fabs(w1) <= DBL_MAX && w1 != 0.0;
+        W1[o] = w1;
+        Y1[o] = y1;
+    }
+    if (status && !ok) atomicOr(status, FLAG_PIVOT);
+}
+
 // One sub-step's solve with the column tile in shared memory: p, w1, 1/w1,
 // w2 and the three right-hand-side inputs of every level copied at once
 // (cp.async), ex formed level by level as oplus_row forms it, the forward
@@ -458,11 +506,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_oplus_solve_tile(OplusFields 
     double *sxh = sw2 + (long)K * T, *som = sxh + (long)K * T, *spr = som + (long)K * T;
     // with the post-solve steps, prev and cur of the nk stored rows come in too
     double *sprev = spr + (long)K * T, *scur = sprev + (long)nk * T;
-    auto cp8 = [](double *dst, const double *src) {
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-                     "l"(src)
-                     : "memory");
-    };
+    const auto cp8 = cp_async8;
     for (int k = 0; k < K; ++k) {
         const long o = (long)k * ld + col;
         const int s = k * T + t;
@@ -638,7 +682,15 @@ cudaError_t launch_oplus_factor(const OplusFields &F, const OplusConsts &C, doub
     k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, xiop2p, xiop2d, nullptr, nullptr, factor, nk,
                                                                  ncol, ld);
     k_oplus_coefs<<<dim3((ncol + 127) / 128, nk - 1), 128, 0, st>>>(F, C, factor, nk, ncol, ld, nullptr);
-    k_oplus_factor<<<(ncol + 31) / 32, 32, 0, st>>>(factor, nk, ncol, ld, status, walk_prefetch(ncol));
+    const size_t tile = (size_t)32 * 3 * (nk - 1) * sizeof(double);
+    if (ncol <= kSmallWalkColumns && tile <= (size_t)smem_optin()) {
+        once_per_device([] {
+            cudaFuncSetAttribute(k_oplus_factor_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
+        });
+        k_oplus_factor_tile<<<(ncol + 31) / 32, 32, tile, st>>>(factor, nk, ncol, ld, status);
+    } else {
+        k_oplus_factor<<<(ncol + 31) / 32, 32, 0, st>>>(factor, nk, ncol, ld, status, walk_prefetch(ncol));
+    }
     return cudaGetLastError();
 }
 
