@@ -747,6 +747,21 @@ int tg_selftest_wait(unsigned polls, int *status_dev, void *stream);
  * kernels' division routine (Markstein's correction of the correctly rounded
  * reciprocal, IEEE division outside its safe range); must equal IEEE a/b. */
 int tg_selftest_division(const double *a, const double *b, double *q, long n, void *stream);
+/* Test entry: one column walk of the assembly routines on rows the caller
+ * formed, level-major (k*ld + col) device planes of nk*ld doubles.
+ *   which 0: the Thomas walk of the three-pass routines: buf holds five
+ *            planes p, q, r, f, x; rows 0..K-1 are solved into x (top = 1:
+ *            K = nk-1 and x(nk-1) = x(nk-2)**2/x(nk-3)).
+ *   which 1: oplus_ng's factor pass: buf is a factor buffer of
+ *            tg_oplus_ng_factor_doubles(nk, ld) doubles whose p, q, r planes
+ *            (planes 6, 7, 8 of nk*ld; rows 0..nk-2) the caller filled; the
+ *            pass writes w1 (plane 10), 1/w1 (plane 11) and w2 (plane 12,
+ *            rows 0..nk-3).
+ * Launches of up to 16384 columns take the shared-memory tile walks, larger
+ * ones the walks that read global memory; both give the same bits.
+ * *status_dev receives the walk's status (TG_EPIVOT, TG_ENONFINITE). */
+int tg_selftest_walk(int which, double *buf, int nk, int K, int top, int ncol, long ld, int *status_dev,
+                     void *stream);
 /* Frees the per-device mirrors, work buffers and streams. */
 int tg_release_buffers(void);
 /* Library version, e.g. "tg_colsolve 0.1.0 sm_100a". */

@@ -43,7 +43,7 @@ EXPORTS = ("tg_solve_host", "tg_dt_ng", "tg_dt_ng_dev", "tg_minor_ng", "tg_minor
            "tg_oplus_ng_dev", "tg_trsolv", "tg_trsolv_ng", "tg_blktri", "tg_comp_blksolve_ng", "tg_blksolve", "tg_trsolv_dev",
            "tg_blksolve_dev", "tg_blksolve_dev_noalloc", "tg_plan_create", "tg_plan_execute", "tg_plan_capture_graph",
            "tg_plan_status", "tg_plan_launches", "tg_plan_describe", "tg_set_cache_hints", "tg_set_block_rows", "tg_set_block_width", "tg_set_stage_levels", "tg_set_column_residency", "tg_set_assembly_mode", "tg_set_walk_prefetch", "tg_set_block_scratch_budget", "tg_set_scalar_scratch_budget", "tg_set_kind_overlap", "tg_set_host_pipeline", "tg_selftest_wait", "tg_plan_sweep_histogram", "tg_plan_destroy",
-           "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_release_buffers", "tg_version", "tg_kernel_arch", "tg_ringfilter", "tg_ringfilter_dev", "tg_filter_o2o", "tg_trsolv_defer", "tg_trsolv_flush", "tg_dt_diag_ng", "tg_dt_diag_ng_dev", "tg_minor_diag_ng", "tg_minor_diag_ng_dev", "tg_dt_ng_post_dev", "tg_minor_ng_post_dev", "tg_oplus_ng_post_dev", "tg_last_error")
+           "tg_set_refine", "tg_set_host_precision", "tg_set_tile", "tg_set_pipeline", "tg_set_prefetch", "tg_set_scratch_global", "tg_selftest_division", "tg_selftest_walk", "tg_release_buffers", "tg_version", "tg_kernel_arch", "tg_ringfilter", "tg_ringfilter_dev", "tg_filter_o2o", "tg_trsolv_defer", "tg_trsolv_flush", "tg_dt_diag_ng", "tg_dt_diag_ng_dev", "tg_minor_diag_ng", "tg_minor_diag_ng_dev", "tg_dt_ng_post_dev", "tg_minor_ng_post_dev", "tg_oplus_ng_post_dev", "tg_last_error")
 
 
 class PostStepArgs(ctypes.Structure):
@@ -280,6 +280,7 @@ def lib():
             "tg_set_scratch_global": [I, I, I],
             "tg_set_prefetch": [I, I, I],
             "tg_selftest_division": [P, P, P, Lg, P],
+            "tg_selftest_walk": [I, P, I, I, I, I, Lg, P, P],
             "tg_release_buffers": [],
             "tg_version": [],
             "tg_last_error": [],
@@ -1002,6 +1003,20 @@ def selftest_division(a, b, q, stream=None):
     """q = a/b on the device through the kernels' division routine."""
     return _check(lib().tg_selftest_division(_dptr(a), _dptr(b), _dptr(q), int(q.numel()), _stream(stream)),
                   "tg_selftest_division", numeric_ok=False)
+
+
+def selftest_walk(which, buf, nk, K, top, ncol, ld, status, stream=None):
+    """One column walk of the assembly routines on caller-formed level-major
+    rows (which 0: the Thomas walk over planes p, q, r, f, x of buf; which 1:
+    oplus_ng's factor pass over a factor buffer); the walk's status goes to
+    the device int `status`."""
+    need = (5 if which == 0 else 1) * nk * ld
+    if which == 1:
+        need = oplus_ng_factor_doubles(nk, ld)
+    if buf.numel() < need:
+        raise ValueError(f"selftest_walk: buf holds {buf.numel()} doubles, expected {need}")
+    return _check(lib().tg_selftest_walk(int(which), _dptr(buf), int(nk), int(K), int(top), int(ncol), int(ld),
+                                         _int_dptr(status), _stream(stream)), "tg_selftest_walk", numeric_ok=False)
 
 
 def set_cache_hints(on):

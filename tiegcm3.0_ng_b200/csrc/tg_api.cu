@@ -2546,6 +2546,36 @@ __attribute__((visibility("default"))) int tg_selftest_wait(unsigned polls, int 
     return TG_OK;
 }
 
+__attribute__((visibility("default"))) int tg_selftest_walk(int which, double *buf, int nk, int K, int top, int ncol,
+                                                            long ld, int *status_dev, void *stream)
+{
+    if (!buf || !status_dev || (which != 0 && which != 1) || nk < 1 || ncol < 0 || ld < ncol ||
+        (which == 1 && nk < 3)) {
+        set_err("tg_selftest_walk: bad arguments (which=%d nk=%d ncol=%d ld=%ld)", which, nk, ncol, ld);
+        return TG_EINVAL;
+    }
+    DevCtx *cx = nullptr;
+    int rc = get_ctx(&cx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(cx->mu);
+    cudaStream_t st = (cudaStream_t)stream;
+    StreamWs *ws = nullptr;
+    if ((rc = stream_ws(cx, st, &ws))) return rc;
+    TG_CUDA(cudaMemsetAsync(ws->flags, 0, sizeof(unsigned), st));
+    const long slab = (long)nk * ld;
+    cudaError_t e = which == 0 ? launch_thomas_post(buf, buf + slab, buf + 2 * slab, buf + 3 * slab, buf + 4 * slab,
+                                                    nk, K, top, ncol, ld, ws->flags, nullptr, st)
+                               : launch_oplus_factor_pass(buf, nk, ncol, ld, ws->flags, st);
+    if (e == cudaErrorInvalidValue) {
+        set_err("tg_selftest_walk: unsupported rows (K=%d top=%d nk=%d)", K, top, nk);
+        return TG_EINVAL;
+    }
+    TG_CUDA(e);
+    k_finish_status<<<1, 1, 0, st>>>(ws->flags, status_dev);
+    TG_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
 __attribute__((visibility("default"))) int tg_set_block_rows(int kind, int on)
 {
     if (kind != TG_KIND_BLOCK2 && kind != TG_KIND_BLOCK3) {

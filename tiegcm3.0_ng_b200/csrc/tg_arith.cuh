@@ -62,6 +62,27 @@ __device__ __forceinline__ double qdiv_pivot(double a, double b, double y, bool 
     return b_safe && exp_safe(a) ? div_markstein(a, b, y) : __ddiv_rn(a, b);
 }
 
+// a/b, correctly rounded, given y = __drcp_rn(b): one exponent-range test
+// (integer operations) for both operands, a subset of div_safe's range.
+__device__ __forceinline__ double qdiv1(double a, double b, double y)
+{
+    return max(exp_dist(a), exp_dist(b)) < kExpSpan ? div_markstein(a, b, y) : __ddiv_rn(a, b);
+}
+// Both quotients by one pivot, qa = a/b and qc = c/b, correctly rounded,
+// given y = __drcp_rn(b), under one exponent-range test for the three
+// operands (a recurrence's w3 and next w2).
+__device__ __forceinline__ void qdiv2(double a, double c, double b, double y, double &qa, double &qc)
+{
+    if (max(exp_dist(b), max(exp_dist(a), exp_dist(c))) < kExpSpan) {
+        qa = div_markstein(a, b, y);
+        qc = div_markstein(c, b, y);
+    } else {
+        const bool bs = exp_safe(b);
+        qa = qdiv_pivot(a, b, y, bs);
+        qc = qdiv_pivot(c, b, y, bs);
+    }
+}
+
 // A hint that brings the line holding p into L1 (no register, no wait).
 __device__ __forceinline__ void pf_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 

@@ -1516,15 +1516,6 @@ struct CompPlaneSrc : CompFieldReads {
     __device__ __forceinline__ void next(int k, CompLevel &L) { load(k + 1, L); }
 };
 
-__device__ __forceinline__ void cp_async8(double *dst, const double *src)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
 // The plane source with every per-level read of the walk staged one
 // iteration ahead: while iteration k computes, asynchronous 8-byte copies
 // bring the 36 values iteration k+1 reads (the 13 planes of level k+2, w at

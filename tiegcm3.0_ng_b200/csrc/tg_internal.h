@@ -271,6 +271,9 @@ cudaError_t launch_oplus_factor(const OplusFields &F, const OplusConsts &C, doub
 cudaError_t launch_oplus_diag_ng(const OplusFields &F, const OplusConsts &C, const double *x, const double *diffexp,
                                  const double *vdotn_h, const double *bdotdh_bvel, int nk, int ncol, long ld,
                                  double *diag, double *scratch, cudaStream_t st);
+// The factor pass alone (w1, 1/w1, w2 from the p, q, r planes of a factor
+// buffer the level and row passes filled).
+cudaError_t launch_oplus_factor_pass(double *factor, int nk, int ncol, long ld, unsigned *status, cudaStream_t st);
 cudaError_t launch_oplus_solve(const OplusFields &F, const OplusConsts &C, const double *factor, double *opout, int nk,
                                int ncol, long ld, unsigned *status, cudaStream_t st, const PostStep *post = nullptr);
 int oplus_scratch_planes();   // level-major scratch planes of launch_oplus_ng (each nk*ld doubles)

@@ -19,6 +19,7 @@
 
 #include "tg_internal.h"
 #include "tg_arith.cuh"
+#include "tg_stage.cuh"
 
 namespace tg {
 namespace {
@@ -440,130 +441,200 @@ __global__ void __launch_bounds__(32) k_oplus_factor(double *scr, int nk, int nc
     if (status && !ok) atomicOr(status, FLAG_PIVOT);
 }
 
-// One asynchronous 8-byte copy global -> shared (cp.async).
-__device__ __forceinline__ void cp_async8(double *dst, const double *src)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
-}
-
-// The same pass for launches of few columns: the column tile's p, q, r rows
-// of every level are copied into shared memory at once (cp.async, every copy
-// in flight), then the recurrence runs from there.
-__global__ void __launch_bounds__(32) k_oplus_factor_tile(double *scr, int nk, int ncol, long ld, unsigned *status)
+// The same pass for launches of few columns.  The kTileWarps warps of a
+// block share one 32-column tile: together they copy the p, q, r rows of
+// every level into shared memory (cp.async, every copy in flight, each warp
+// a quarter of the levels); warp 0 alone runs the recurrence there, leaving
+// 1/w1 where p(k) was, w1 where q(k) was and w2 where r(k-1) was; then all
+// warps store the three planes, each its quarter of the levels.
+constexpr int kTileWarps = 4;
+__global__ void __launch_bounds__(32 * kTileWarps) k_oplus_factor_tile(double *scr, int nk, int ncol, long ld,
+                                                                       unsigned *status)
 {
     extern __shared__ double factor_tile[];
-    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
-    const int T = 32, t = threadIdx.x, K = nk - 1;
-    const long slab = (long)nk * ld;
+    const int T = 32, t = threadIdx.x & 31, w = threadIdx.x >> 5, NW = kTileWarps, K = nk - 1;
+    const long col = (long)blockIdx.x * T + t, slab = (long)nk * ld;
+    const bool live = col < ncol;
     double *sp = factor_tile, *sq = sp + (long)K * T, *sr = sq + (long)K * T;
-    for (int k = 0; k < K; ++k) {
-        const long o = (long)k * ld + col;
-        const int s = k * T + t;
-        cp_async8(sp + s, scr + S_P * slab + o);
-        cp_async8(sq + s, scr + S_Q * slab + o);
-        cp_async8(sr + s, scr + S_R * slab + o);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    double *W1 = scr + S_W1 * slab, *Y1 = scr + S_Y1 * slab, *W2 = scr + S_W2 * slab;
-    bool ok = true;
-    double w1 = 0., y1 = 0.;
-    for (int k = 0; k < K; ++k) {
-        const long o = (long)k * ld + col;
-        const int s = k * T + t;
-        if (k == 0) {
-            w1 = sq[s];
-        } else {
-            const double w2 = qdiv(sr[s - T], w1, y1);
-            W2[o - ld] = w2;
-            w1 = xs(sq[s], xm(sp[s], w2));
+    if (live)
+        for (int k = w; k < K; k += NW) {
+            const long o = (long)k * ld + col;
+            const int s = k * T + t;
+            cp_async8(sp + s, scr + S_P * slab + o);
+            cp_async8(sq + s, scr + S_Q * slab + o);
+            cp_async8(sr + s, scr + S_R * slab + o);
         }
-        y1 = __drcp_rn(w1);
-        ok = ok && fabs(w1) <= DBL_MAX && w1 != 0.0;
-        W1[o] = w1;
-        Y1[o] = y1;
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    if (w == 0 && live) {
+        // Level k forms the next level's w2 = r(k)/w1(k) and keeps it where
+        // r(k) was.  The chain is the recurrence alone: quotients by
+        // Markstein's sequence without a branch, operands read one level
+        // ahead; from the first level whose operands leave the sequence's
+        // safe range (stores stop there) the levels are walked again with
+        // the IEEE fallback (qdiv1).
+        bool ok = true;
+        int bad = K;
+        double w1 = 0., y1 = 0., w2 = 0.;
+        auto level = [&](int k, double p, double q, double r, bool top_level) {
+            w1 = k == 0 ? q : xs(q, xm(p, w2));
+            y1 = __drcp_rn(w1);
+            ok = ok && (bad < K || finite_nz(w1));
+            const unsigned d = max(exp_dist(w1), top_level ? 0u : exp_dist(r));
+            bad = d >= kExpSpan && bad == K ? k : bad;
+            w2 = div_markstein(r, w1, y1);
+            if (bad > k) {
+                sq[k * T + t] = w1;
+                sp[k * T + t] = y1;
+                sr[k * T + t] = w2;
+            }
+        };
+        double pn = sp[t], qn = sq[t], rn = sr[t];
+        for (int k = 0; k < K - 1; ++k) {
+            const int s = k * T + t;
+            const double p = pn, q = qn, r = rn;
+            pn = sp[s + T];
+            qn = sq[s + T];
+            rn = sr[s + T];
+            level(k, p, q, r, false);
+        }
+        level(K - 1, pn, qn, rn, true);
+        if (bad < K) {
+            w2 = bad > 0 ? sr[(bad - 1) * T + t] : 0.;
+            for (int k = bad; k < K; ++k) {
+                const int s = k * T + t;
+                w1 = k == 0 ? sq[s] : xs(sq[s], xm(sp[s], w2));
+                y1 = __drcp_rn(w1);
+                w2 = k + 1 < K ? qdiv1(sr[s], w1, y1) : 0.;
+                ok = ok && finite_nz(w1);
+                sq[s] = w1;
+                sp[s] = y1;
+                sr[s] = w2;
+            }
+        }
+        if (status && !ok) atomicOr(status, FLAG_PIVOT);
     }
-    if (status && !ok) atomicOr(status, FLAG_PIVOT);
+    __syncthreads();
+    if (!live) return;
+    double *W1 = scr + S_W1 * slab, *Y1 = scr + S_Y1 * slab, *W2 = scr + S_W2 * slab;
+    for (int k = w; k < K; k += NW) {
+        const long o = (long)k * ld + col;
+        const int s = k * T + t;
+        W1[o] = sq[s];
+        Y1[o] = sp[s];
+        if (k < K - 1) W2[o] = sr[s];
+    }
 }
 
-// One sub-step's solve with the column tile in shared memory: p, w1, 1/w1,
-// w2 and the three right-hand-side inputs of every level copied at once
-// (cp.async), ex formed level by level as oplus_row forms it, the forward
-// recurrence, the back sweep, and the post-solve stores last.
-constexpr int kSolveThreads = 32;
-__global__ void __launch_bounds__(kSolveThreads) k_oplus_solve_tile(OplusFields F, OplusConsts C, const double *scr,
-                                                                    double *opout, int nk, int ncol, long ld,
-                                                                    unsigned *status, PostStep post, int has_post)
+// One sub-step's solve with the column tile in shared memory, the
+// kTileWarps warps of a block on one 32-column tile: together they copy p,
+// w1, 1/w1, w2 and the three right-hand-side inputs of every level (and the
+// post-step inputs) at once (cp.async); warp 0 alone forms each level's ex
+// as oplus_row forms it and runs the forward recurrence and the back sweep;
+// all warps store the rows through the post-solve steps.
+__global__ void __launch_bounds__(32 * kTileWarps) k_oplus_solve_tile(OplusFields F, OplusConsts C, const double *scr,
+                                                                      double *opout, int nk, int ncol, long ld,
+                                                                      unsigned *status, PostStep post, int has_post)
 {
     extern __shared__ double solve_tile[];
-    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
-    const int T = kSolveThreads, t = threadIdx.x, K = nk - 1;
-    const long slab = (long)nk * ld;
+    const int T = 32, t = threadIdx.x & 31, w = threadIdx.x >> 5, NW = kTileWarps, K = nk - 1;
+    const long col = (long)blockIdx.x * T + t, slab = (long)nk * ld;
+    const bool live = col < ncol;
+    // ex, then the solution, in som: nk rows (the top row's extrapolation too)
     double *sp = solve_tile, *sw1 = sp + (long)K * T, *sy1 = sw1 + (long)K * T, *sw2 = sy1 + (long)K * T;
-    double *sxh = sw2 + (long)K * T, *som = sxh + (long)K * T, *spr = som + (long)K * T;
+    double *sxh = sw2 + (long)K * T, *som = sxh + (long)K * T, *spr = som + (long)nk * T;
     // with the post-solve steps, prev and cur of the nk stored rows come in too
     double *sprev = spr + (long)K * T, *scur = sprev + (long)nk * T;
-    const auto cp8 = cp_async8;
-    for (int k = 0; k < K; ++k) {
-        const long o = (long)k * ld + col;
-        const int s = k * T + t;
-        cp8(sp + s, scr + S_P * slab + o);
-        cp8(sw1 + s, scr + S_W1 * slab + o);
-        cp8(sy1 + s, scr + S_Y1 * slab + o);
-        cp8(sw2 + s, scr + S_W2 * slab + o);
-        cp8(sxh + s, F.explicit_h + o);
-        cp8(som + s, F.optm1_smooth2 + o);
-        cp8(spr + s, scr + S_PROD * slab + o);
-    }
-    if (has_post)
-        for (int k = 0; k < nk; ++k) {
+    if (live) {
+        for (int k = w; k < K; k += NW) {
             const long o = (long)k * ld + col;
-            cp8(sprev + k * T + t, post.prev + o);
-            cp8(scur + k * T + t, post.cur + o);
+            const int s = k * T + t;
+            cp_async8(sp + s, scr + S_P * slab + o);
+            cp_async8(sw1 + s, scr + S_W1 * slab + o);
+            cp_async8(sy1 + s, scr + S_Y1 * slab + o);
+            cp_async8(sw2 + s, scr + S_W2 * slab + o);
+            cp_async8(sxh + s, F.explicit_h + o);
+            cp_async8(som + s, F.optm1_smooth2 + o);
+            cp_async8(spr + s, scr + S_PROD * slab + o);
         }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    const double t_top = scr[S_TB * slab + col], t_bot = scr[S_TB * slab + ld + col];
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    double w3 = 0.;
-    for (int k = 0; k < K; ++k) {
-        const int s = k * T + t;
-        double ex = xs(sxh[s], xm(xm(som[s], C.dtx2inv), (double)C.nstep_sub));
-        if (k == nk - 2) ex = xs(ex, t_top);
-        ex = xs(ex, spr[s]);
-        if (k == 0) {
-            ex = xs(ex, t_bot);
-            w3 = qdiv(ex, sw1[s], sy1[s]);
-        } else {
-            w3 = qdiv(xs(ex, xm(sp[s], w3)), sw1[s], sy1[s]);
+        if (has_post)
+            for (int k = w; k < nk; k += NW) {
+                const long o = (long)k * ld + col;
+                cp_async8(sprev + k * T + t, post.prev + o);
+                cp_async8(scur + k * T + t, post.cur + o);
+            }
+    }
+    const double t_top = w == 0 && live ? scr[S_TB * slab + col] : 0.;
+    const double t_bot = w == 0 && live ? scr[S_TB * slab + ld + col] : 0.;
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    if (w == 0 && live) {
+        // ex formed as oplus_row forms it, then the recurrence; each level's
+        // operands read one level ahead, so the ex arithmetic stays off the
+        // recurrence's chain
+        // quotients by Markstein's sequence without a branch; from the first
+        // level whose operands leave its safe range (stores stop there) the
+        // levels are walked again with the IEEE fallback (qdiv1)
+        double w3 = 0.;
+        int bad = K;
+        auto ex_of = [&](int k, double xh, double om, double pr) {
+            double ex = xs(xh, xm(xm(om, C.dtx2inv), (double)C.nstep_sub));
+            if (k == nk - 2) ex = xs(ex, t_top);
+            ex = xs(ex, pr);
+            if (k == 0) ex = xs(ex, t_bot);
+            return ex;
+        };
+        auto level = [&](int k, double ex, double p, double w1, double y1) {
+            const double num = k == 0 ? ex : xs(ex, xm(p, w3));
+            const unsigned d = max(exp_dist(num), exp_dist(w1));
+            bad = d >= kExpSpan && bad == K ? k : bad;
+            w3 = div_markstein(num, w1, y1);
+            if (bad > k) som[k * T + t] = w3;
+        };
+        double xhn = sxh[t], omn = som[t], prn = spr[t], pn = sp[t], w1n = sw1[t], y1n = sy1[t];
+        for (int k = 0; k < K - 1; ++k) {
+            const int s = k * T + t;
+            const double xh = xhn, om = omn, pr = prn, p = pn, w1 = w1n, y1 = y1n;
+            xhn = sxh[s + T];
+            omn = som[s + T];
+            prn = spr[s + T];
+            pn = sp[s + T];
+            w1n = sw1[s + T];
+            y1n = sy1[s + T];
+            level(k, ex_of(k, xh, om, pr), p, w1, y1);
         }
-        som[s] = w3;
+        level(K - 1, ex_of(K - 1, xhn, omn, prn), pn, w1n, y1n);
+        if (bad < K) {
+            w3 = bad > 0 ? som[(bad - 1) * T + t] : 0.;
+            for (int k = bad; k < K; ++k) {
+                const int s = k * T + t;
+                const double ex = ex_of(k, sxh[s], som[s], spr[s]);
+                w3 = qdiv1(k == 0 ? ex : xs(ex, xm(sp[s], w3)), sw1[s], sy1[s]);
+                som[s] = w3;
+            }
+        }
+        const double xtop = w3;
+        back_sweep(som, sw2, K, t, w3);
+        // x(k) = w3 - w2*x(k+1) carries a non-finite value down to x(0)
+        const bool fin = finite(som[t]) && finite(xtop);
+        // opout(nk) = opout(nk-1)**2/opout(nk-2) from the unfiltered values (oplus_ng.F90:307)
+        som[K * T + t] = xd(xm(xtop, xtop), som[(K - 2) * T + t]);
+        if (status && !fin) atomicOr(status, FLAG_NONFINITE);
     }
-    double xn = w3;
-    const double xtop = w3;
-    bool fin = fabs(xn) <= DBL_MAX;
-    for (int k = K - 2; k >= 0; --k) {
-        const int s = k * T + t;
-        xn = xs(som[s], xm(sw2[s], xn));
-        fin = fin && fabs(xn) <= DBL_MAX;
-        som[s] = xn;
-    }
-    const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
-    // opout(nk) = opout(nk-1)**2/opout(nk-2) from the unfiltered values (oplus_ng.F90:307)
-    const double xk = xd(xm(xtop, xtop), som[(K - 2) * T + t]);
+    __syncthreads();
+    if (!live) return;
     if (has_post) {
-        for (int k = 0; k < K; ++k)
+        const bool bcol = post.bnd_mask && post.bnd_mask[col];
+        for (int k = w; k < nk; k += NW)
             post_store_v(post, bcol, opout, (long)k * ld + col, som[k * T + t], sprev[k * T + t], scur[k * T + t]);
-        post_store_v(post, bcol, opout, (long)K * ld + col, xk, sprev[K * T + t], scur[K * T + t]);
     } else {
-        for (int k = 0; k < K; ++k) opout[(long)k * ld + col] = som[k * T + t];
-        opout[(long)K * ld + col] = xk;
+        for (int k = w; k < nk; k += NW) opout[(long)k * ld + col] = som[k * T + t];
     }
-    if (status && !fin) atomicOr(status, FLAG_NONFINITE);
 }
 
+constexpr int kSolveThreads = 32;
 // The same solve reading the rows from global memory (launches too large for
 // the shared-memory tile), pd levels requested ahead.
 __global__ void __launch_bounds__(kSolveThreads) k_oplus_solve(OplusFields F, OplusConsts C, const double *scr,
@@ -682,12 +753,19 @@ cudaError_t launch_oplus_factor(const OplusFields &F, const OplusConsts &C, doub
     k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, xiop2p, xiop2d, nullptr, nullptr, factor, nk,
                                                                  ncol, ld);
     k_oplus_coefs<<<dim3((ncol + 127) / 128, nk - 1), 128, 0, st>>>(F, C, factor, nk, ncol, ld, nullptr);
+    return launch_oplus_factor_pass(factor, nk, ncol, ld, status, st);
+}
+
+cudaError_t launch_oplus_factor_pass(double *factor, int nk, int ncol, long ld, unsigned *status, cudaStream_t st)
+{
+    if (ncol <= 0) return cudaSuccess;
+    if (nk < 3) return cudaErrorInvalidValue;
     const size_t tile = (size_t)32 * 3 * (nk - 1) * sizeof(double);
     if (ncol <= kSmallWalkColumns && tile <= (size_t)smem_optin()) {
         once_per_device([] {
             cudaFuncSetAttribute(k_oplus_factor_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
         });
-        k_oplus_factor_tile<<<(ncol + 31) / 32, 32, tile, st>>>(factor, nk, ncol, ld, status);
+        k_oplus_factor_tile<<<(ncol + 31) / 32, 32 * kTileWarps, tile, st>>>(factor, nk, ncol, ld, status);
     } else {
         k_oplus_factor<<<(ncol + 31) / 32, 32, 0, st>>>(factor, nk, ncol, ld, status, walk_prefetch(ncol));
     }
@@ -701,13 +779,14 @@ cudaError_t launch_oplus_solve(const OplusFields &F, const OplusConsts &C, const
     if (nk < 3) return cudaErrorInvalidValue;
     const PostStep pv = post ? *post : PostStep{};
     const int hp = post != nullptr;
-    const size_t tile = (size_t)kSolveThreads * (7 * (nk - 1) + (post ? 2 * nk : 0)) * sizeof(double);
+    const size_t tile = (size_t)32 * (7 * (nk - 1) + 1 + (post ? 2 * nk : 0)) * sizeof(double);
     const int T = kSolveThreads;
     if (ncol <= kSmallWalkColumns && tile <= (size_t)smem_optin()) {
         once_per_device([] {
             cudaFuncSetAttribute(k_oplus_solve_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
         });
-        k_oplus_solve_tile<<<(ncol + T - 1) / T, T, tile, st>>>(F, C, factor, opout, nk, ncol, ld, status, pv, hp);
+        k_oplus_solve_tile<<<(ncol + 31) / 32, 32 * kTileWarps, tile, st>>>(F, C, factor, opout, nk, ncol, ld, status,
+                                                                            pv, hp);
     } else {
         k_oplus_solve<<<(ncol + T - 1) / T, T, 0, st>>>(F, C, factor, opout, nk, ncol, ld, status, pv, hp,
                                                         walk_prefetch(ncol));

@@ -21,6 +21,7 @@
 
 #include "tg_internal.h"
 #include "tg_arith.cuh"
+#include "tg_stage.cuh"
 
 namespace tg {
 namespace {
@@ -92,86 +93,120 @@ __global__ void __launch_bounds__(kWalkThreads) k_thomas_post(const double *P, c
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 // The same walk with the column tile held in shared memory, for launches of
-// few columns: a warp first copies the p, q, r, f rows of all its levels
-// (cp.async, every copy in flight at once), then runs the recurrence from
-// shared memory, keeping w2 where r(k-1) was and the parked w3 where q(k)
-// was; the back sweep leaves the solution there too, and the post-solve
-// stores, independent of one another, go out last.
-__global__ void __launch_bounds__(kWalkThreads) k_thomas_post_tile(const double *P, const double *Q, const double *R,
-                                                                   const double *Fv, double *x, int nk, int K,
-                                                                   int top, int ncol, long ld, unsigned *status,
-                                                                   PostStep post, int has_post)
+// few columns.  The kTileWarps warps of a block share one 32-column tile:
+// together they copy the p, q, r, f rows of every level (cp.async, every
+// copy in flight at once, each warp a quarter of the levels), then warp 0
+// alone runs the recurrence from shared memory, keeping w2 where r(k-1) was
+// and the parked w3, then the solution, where q(k) was; finally all warps
+// store the rows through the post-solve steps, each its quarter of the
+// levels.  The per-column serial part is the recurrence alone.
+constexpr int kTileWarps = 4;
+__global__ void __launch_bounds__(32 * kTileWarps) k_thomas_post_tile(const double *P, const double *Q,
+                                                                      const double *R, const double *Fv, double *x,
+                                                                      int nk, int K, int top, int ncol, long ld,
+                                                                      unsigned *status, PostStep post, int has_post)
 {
     extern __shared__ double tile_walk[];
-    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
-    const int T = kWalkThreads, t = threadIdx.x;
-    double *sp = tile_walk, *sq = sp + (long)K * T, *sr = sq + (long)K * T, *sf = sr + (long)K * T;
+    const int T = 32, t = threadIdx.x & 31, w = threadIdx.x >> 5, NW = kTileWarps;
+    const long col = (long)blockIdx.x * T + t;
+    const bool live = col < ncol;
     // with the post-solve steps, prev and cur of every stored row (K, and the
-    // top row for top = 1) come in with the rows
+    // top row for top = 1) come in with the rows; q holds the KS solved rows
     const int KS = top == 1 ? K + 1 : K;
+    double *sp = tile_walk, *sq = sp + (long)K * T, *sr = sq + (long)KS * T, *sf = sr + (long)K * T;
     double *sprev = sf + (long)K * T, *scur = sprev + (long)KS * T;
-    auto cp8 = [](double *dst, const double *src) {
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-                     "l"(src)
-                     : "memory");
-    };
-    for (int k = 0; k < K; ++k) {
-        const long o = (long)k * ld + col;
-        const int s = k * T + t;
-        cp8(sp + s, P + o);
-        cp8(sq + s, Q + o);
-        cp8(sr + s, R + o);
-        cp8(sf + s, Fv + o);
-    }
-    if (has_post)
-        for (int k = 0; k < KS; ++k) {
+    if (live) {
+        for (int k = w; k < K; k += NW) {
             const long o = (long)k * ld + col;
-            cp8(sprev + k * T + t, post.prev + o);
-            cp8(scur + k * T + t, post.cur + o);
+            const int s = k * T + t;
+            cp_async8(sp + s, P + o);
+            cp_async8(sq + s, Q + o);
+            cp_async8(sr + s, R + o);
+            cp_async8(sf + s, Fv + o);
         }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    bool ok = true;
-    double w1 = 0.0, y1 = 0.0, w3 = 0.0;
-    for (int k = 0; k < K; ++k) {
-        const int s = k * T + t;
-        const double p = sp[s], q = sq[s], f = sf[s];
-        if (k == 0) {
-            w1 = q;
+        if (has_post)
+            for (int k = w; k < KS; k += NW) {
+                const long o = (long)k * ld + col;
+                cp_async8(sprev + k * T + t, post.prev + o);
+                cp_async8(scur + k * T + t, post.cur + o);
+            }
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    if (w == 0 && live) {
+        // Level k divides by its pivot w1(k) twice: w3(k) and the next
+        // level's w2 = r(k)/w1(k) (the reference's operands, so the same
+        // quotients), kept where r(k) was.  The walk's chain is the
+        // recurrence alone: every quotient by Markstein's sequence, no
+        // branch, each level's operands read one level ahead.  A level whose
+        // operands leave the sequence's safe range (zeros, non-finite or
+        // extreme values) stops the stores; the levels from the first such
+        // one are then walked again with the IEEE fallback (qdiv2, qdiv1).
+        bool ok = true;
+        int bad = K;
+        double w1 = 0.0, y1 = 0.0, w2 = 0.0, w3 = 0.0;
+        auto level = [&](int k, double p, double q, double r, double f, bool top_level) {
+            w1 = k == 0 ? q : xs(q, xm(p, w2));
             y1 = __drcp_rn(w1);
-            w3 = qdiv(f, w1, y1);
-        } else {
-            const double w2 = qdiv(sr[s - T], w1, y1);
-            sr[s - T] = w2;
-            w1 = xs(q, xm(p, w2));
-            y1 = __drcp_rn(w1);
-            w3 = qdiv(xs(f, xm(p, w3)), w1, y1);
+            const double num = k == 0 ? f : xs(f, xm(p, w3));
+            ok = ok && (bad < K || finite_nz(w1));
+            const unsigned d = max(exp_dist(w1), max(exp_dist(num), top_level ? 0u : exp_dist(r)));
+            bad = d >= kExpSpan && bad == K ? k : bad;
+            w3 = div_markstein(num, w1, y1);
+            w2 = div_markstein(r, w1, y1);
+            if (bad > k) {
+                sr[k * T + t] = w2;
+                sq[k * T + t] = w3;
+            }
+        };
+        double pn = sp[t], qn = sq[t], rn = sr[t], fn = sf[t];
+        for (int k = 0; k < K - 1; ++k) {
+            const int s = k * T + t;
+            const double p = pn, q = qn, r = rn, f = fn;
+            pn = sp[s + T];
+            qn = sq[s + T];
+            rn = sr[s + T];
+            fn = sf[s + T];
+            level(k, p, q, r, f, false);
         }
-        ok = ok && fabs(w1) <= DBL_MAX && w1 != 0.0;
-        sq[s] = w3;
+        level(K - 1, pn, qn, rn, fn, true);
+        if (bad < K) {
+            w2 = bad > 0 ? sr[(bad - 1) * T + t] : 0.0;
+            w3 = bad > 0 ? sq[(bad - 1) * T + t] : 0.0;
+            for (int k = bad; k < K; ++k) {
+                const int s = k * T + t;
+                const double p = sp[s], q = sq[s], f = sf[s];
+                w1 = k == 0 ? q : xs(q, xm(p, w2));
+                y1 = __drcp_rn(w1);
+                const double num = k == 0 ? f : xs(f, xm(p, w3));
+                if (k + 1 < K) {
+                    qdiv2(num, sr[s], w1, y1, w3, w2);
+                    sr[s] = w2;
+                } else {
+                    w3 = qdiv1(num, w1, y1);
+                }
+                ok = ok && finite_nz(w1);
+                sq[s] = w3;
+            }
+        }
+        const double xtop = w3;
+        back_sweep(sq, sr, K, t, w3);
+        // x(k) = w3 - w2*x(k+1) carries a non-finite value down to x(0)
+        const bool fin = finite(sq[t]) && finite(xtop);
+        // x(nk-1) = x(nk-2)**2/x(nk-3) from the unfiltered values
+        if (top == 1) sq[K * T + t] = xd(xm(xtop, xtop), sq[(K - 2) * T + t]);
+        if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
     }
-    double xn = w3;
-    const double xtop = w3;
-    bool fin = fabs(xn) <= DBL_MAX;
-    for (int k = K - 2; k >= 0; --k) {
-        const int s = k * T + t;
-        xn = xs(sq[s], xm(sr[s], xn));
-        fin = fin && fabs(xn) <= DBL_MAX;
-        sq[s] = xn;
-    }
-    const bool bcol = has_post && post.bnd_mask && post.bnd_mask[col];
-    // x(nk-1) = x(nk-2)**2/x(nk-3) from the unfiltered values
-    const double xk = top == 1 ? xd(xm(xtop, xtop), sq[(K - 2) * T + t]) : 0.0;
+    __syncthreads();
+    if (!live) return;
     if (has_post) {
-        for (int k = 0; k < K; ++k)
+        const bool bcol = post.bnd_mask && post.bnd_mask[col];
+        for (int k = w; k < KS; k += NW)
             post_store_v(post, bcol, x, (long)k * ld + col, sq[k * T + t], sprev[k * T + t], scur[k * T + t]);
-        if (top == 1) post_store_v(post, bcol, x, (long)K * ld + col, xk, sprev[K * T + t], scur[K * T + t]);
     } else {
-        for (int k = 0; k < K; ++k) x[(long)k * ld + col] = sq[k * T + t];
-        if (top == 1) x[(long)K * ld + col] = xk;
+        for (int k = w; k < KS; k += NW) x[(long)k * ld + col] = sq[k * T + t];
     }
-    if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 }  // namespace
 
@@ -181,12 +216,13 @@ cudaError_t launch_thomas_post(const double *p, const double *q, const double *r
 {
     if (ncol <= 0) return cudaSuccess;
     if (K < 1 || K > nk || (top == 1 && (K != nk - 1 || K < 2))) return cudaErrorInvalidValue;
-    const size_t tile = (size_t)kWalkThreads * (4 * K + (post ? 2 * (top == 1 ? K + 1 : K) : 0)) * sizeof(double);
+    const int KS = top == 1 ? K + 1 : K;
+    const size_t tile = (size_t)32 * (3 * K + KS + (post ? 2 * KS : 0)) * sizeof(double);
     if (ncol <= kSmallWalkColumns && tile <= (size_t)smem_optin()) {
         once_per_device([] {
             cudaFuncSetAttribute(k_thomas_post_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
         });
-        k_thomas_post_tile<<<(ncol + kWalkThreads - 1) / kWalkThreads, kWalkThreads, tile, st>>>(
+        k_thomas_post_tile<<<(ncol + 31) / 32, 32 * kTileWarps, tile, st>>>(
             p, q, r, f, x, nk, K, top, ncol, ld, status, post ? *post : PostStep{}, post != nullptr);
         return cudaGetLastError();
     }
