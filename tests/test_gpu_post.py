@@ -241,3 +241,41 @@ def test_oplus_factor_and_solve_give_the_full_step_bits(cuda, pkg, ncol, odd_ld)
         assert torch.equal(nm_g[:, :ncol], nm_w[:, :ncol]), sub
         assert torch.equal(x2p[:, :ncol], want[1][:, :ncol]) and torch.equal(x2d[:, :ncol], want[2][:, :ncol])
         op = got_p
+
+
+@pytest.mark.parametrize("ncol,pad,et,eh", [(1500, 0, 1, 0), (1500, 5, 0, 6), (17000, 0, 1, 6)],
+                         ids=["tile", "tile_odd_ld", "above_tile_limit"])
+def test_settei_three_pass_gives_the_two_pass_bits(cuda, pkg, ncol, pad, et, eh):
+    """settei_ng in assembly mode 2 (rows formed one thread per level and
+    column, the Thomas walk alone, Te and Ti formed level-parallel) gives
+    mode 1's Te, Ti, qtotal and system bit for bit."""
+    torch = cuda
+    nk, dz = 57, 0.25
+    F, C, qt = pkg.synth.settei_inputs(nk, ncol, dz, 61, et=et, electron_heating=eh)
+    ld = ncol + pad
+    dev = {}
+    for k, v in F.items():
+        t = torch.zeros((nk, ld) if v.ndim == 2 else (ld,), dtype=torch.float64, device="cuda")
+        if v.ndim == 2:
+            t[:, :ncol] = torch.from_numpy(np.ascontiguousarray(v))
+        else:
+            t[:ncol] = torch.from_numpy(v)
+        dev[k] = t
+    q0 = torch.zeros((nk, ld), dtype=torch.float64, device="cuda")
+    q0[:, :ncol] = torch.from_numpy(np.ascontiguousarray(qt))
+    got = {}
+    for mode in (1, 2):
+        pkg.set_assembly_mode(mode)
+        try:
+            te, ti = (torch.full((nk, ld), -1.0, dtype=torch.float64, device="cuda") for _ in range(2))
+            q2 = q0.clone()
+            so = torch.zeros((4, nk, ld), dtype=torch.float64, device="cuda")
+            st = torch.zeros(1, dtype=torch.int32, device="cuda")
+            pkg.settei_ng_dev(dev, C, te, ti, q2, nk, ncol, ld, system_out=so, status=st)
+            torch.cuda.synchronize()
+            assert int(st.item()) == pkg.TG_OK
+            got[mode] = [v[..., :ncol].clone() for v in (te, ti, q2)] + [so[:, :nk - 1, :ncol].clone()]
+        finally:
+            pkg.set_assembly_mode(-1)
+    for i, (u, v) in enumerate(zip(got[1], got[2])):
+        assert torch.equal(u, v), i

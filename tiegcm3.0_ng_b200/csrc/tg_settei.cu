@@ -603,7 +603,103 @@ __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConst
     if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
 }
 
-size_t settei_scratch_doubles(int nk, long ld) { return (size_t)P_N * nk * ld; }
+// ---------------------------------------------------------------------------
+// settei_ng in three passes, for launches of few columns, where a walk that
+// forms its rows and raises every solved level to the 2/7 power waits on
+// those instructions level by level.  After k_settei_levels:
+//   k_settei_coefs: one thread per (level, column) forms row k (p, q, r and
+//     rhs, as the walk forms them) into four planes and adds q_eni to qtotal
+//     at the interfaces;
+//   the Thomas walk of the assembly routines (launch_thomas_post) solves the
+//     rows 0..nk-2 for x = Te^3.5 into a scratch plane;
+//   k_settei_post: one thread per (level, column) turns x into Te, the top
+//     level from its two neighbours, and forms Ti.
+// The same operations on the same operands as k_settei_rows: the same bits.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_settei_coefs(SetteiFields F, SetteiConsts C, const double *lv,
+                                                      double *rows, double *qtotal, int nk, int ncol, long ld,
+                                                      double *sys_out)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int k = blockIdx.y;
+    const long slab = (long)nk * ld, o = (long)k * ld + col;
+    auto pl = [&](int e, int kk) { return __ldg(lv + e * slab + (long)kk * ld + col); };
+    // qtotal += q_eni at the interfaces (settei_ng.F90:248-254); level k
+    // reads and writes only its own qtotal
+    const double qe_k = pl(P_QENI, k);
+    if (k == 0)
+        qtotal[o] = xa(qtotal[o], xs(xm(1.5, qe_k), xm(0.5, pl(P_QENI, 1))));
+    else if (k <= nk - 2)
+        qtotal[o] = xa(qtotal[o], xm(.5, xa(pl(P_QENI, k - 1), qe_k)));
+    else
+        qtotal[o] = xa(qtotal[o], xs(xm(1.5, pl(P_QENI, nk - 2)), xm(0.5, nk >= 3 ? pl(P_QENI, nk - 3) : 0.)));
+    if (k > nk - 2) return;
+    const double dz = C.dz;
+    double sindip;
+    {
+        const double dm = fabs(__ldg(F.dipmag + col));
+        const double sn = sin(dm > C.dipmin ? dm : C.dipmin);
+        sindip = dmax(xm(sn, sn), .10);
+    }
+    const double pb = xm(xd(xd(2., 7.), xm(__ldg(F.scht + o), xm(dz, dz))), sindip);
+    double r = xm(pb, pl(P_TH, k + 1));
+    double p = xm(pb, pl(P_TH, k));
+    double q = -xa(p, r);
+    double rhs = 0.;
+    if (k == 0) {
+        q = xs(q, p);
+        rhs = xs(rhs, xm(xm(2., p), pow(__ldg(F.t_lbc + col), 3.5)));
+        p = 0.;
+    }
+    if (k == nk - 2) {
+        q = xa(q, r);
+        rhs = xa(rhs, xd(xm(xm(xm(xm(r, dz), 3.5), __ldg(F.schti + (long)(nk - 1) * ld + col)), settei_fe(F, C, col)),
+                         pl(P_TEK0, nk - 1)));
+        r = 0.;
+    }
+    rhs = xs(rhs, pl(P_QE, k));
+    if (C.et) rhs = xs(rhs, pl(P_ET, k));
+    q = xs(q, pl(P_DQ, k));
+    rhs = xs(xs(rhs, pl(P_LENTN, k)), pl(P_LEITI, k));
+    rows[o] = p;
+    rows[slab + o] = q;
+    rows[2 * slab + o] = r;
+    rows[3 * slab + o] = rhs;
+    if (sys_out) {
+        sys_out[o] = p;
+        sys_out[slab + o] = q;
+        sys_out[2 * slab + o] = r;
+        sys_out[3 * slab + o] = rhs;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_settei_post(SetteiFields F, SetteiConsts C, const double *lv, const double *x,
+                                                     double *te_out, double *ti_out, int nk, int ncol, long ld)
+{
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int k = blockIdx.y, K = nk - 1;
+    const long slab = (long)nk * ld, o = (long)k * ld + col;
+    const double e27 = xd(2., 7.);
+    double t;
+    if (k < K) {
+        t = pow(x[o], e27);
+    } else {
+        // te(nk) = te(nk-1)**2/te(nk-2) from the unfloored values
+        const double t1 = pow(x[(long)(K - 1) * ld + col], e27), t2 = pow(x[(long)(K - 2) * ld + col], e27);
+        t = xd(xm(t1, t1), t2);
+    }
+    const double tn = __ldg(F.tn + o);
+    const double te = dmax(t, tn);
+    const double lei = __ldg(lv + P_LEI * slab + o), lin = __ldg(lv + P_LIN * slab + o);
+    te_out[o] = te;
+    const double num = xa(xa(xd(xm(__ldg(F.qji_ti + o), __ldg(F.xnmbar + o)), C.avo), xm(lei, te)), xm(lin, tn));
+    ti_out[o] = dmax(xd(num, xa(lei, lin)), tn);
+}
+
+// the level planes, then (three-pass form) the four row planes and x
+size_t settei_scratch_doubles(int nk, long ld) { return (size_t)(P_N + 5) * nk * ld; }
 
 cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, double *te_out, double *ti_out,
                              double *qtotal, int nk, int ncol, long ld, double *sys_out, unsigned *status,
@@ -621,6 +717,18 @@ cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, doubl
     const size_t per = (size_t)(2 * nk - 1) * sizeof(double);
     while (T > 32 && (size_t)T * per > (size_t)optin) T /= 2;
     if ((size_t)T * per > (size_t)optin) return cudaErrorInvalidValue;
+    if (scratch && assembly_mode() == 2 && ncol <= kSmallWalkColumns) {
+        const long slab = (long)nk * ld;
+        double *rows = scratch + P_N * slab, *x = rows + 4 * slab;
+        const dim3 grid((ncol + 127) / 128, nk);
+        k_settei_levels<<<grid, 128, 0, st>>>(F, C, scratch, nk, ncol, ld);
+        k_settei_coefs<<<grid, 128, 0, st>>>(F, C, scratch, rows, qtotal, nk, ncol, ld, sys_out);
+        cudaError_t e = launch_thomas_post(rows, rows + slab, rows + 2 * slab, rows + 3 * slab, x, nk, nk - 1, 0, ncol,
+                                           ld, status, nullptr, st);
+        if (e != cudaSuccess) return e;
+        k_settei_post<<<grid, 128, 0, st>>>(F, C, scratch, x, te_out, ti_out, nk, ncol, ld);
+        return cudaGetLastError();
+    }
     if (scratch && assembly_mode() >= 1) {
         int T2 = 128;
         const size_t per2 = (size_t)(nk - 1) * sizeof(double) + Stage<kSetteiStaged>::bytes_per_thread;
