@@ -1280,12 +1280,52 @@ __device__ __forceinline__ void comp_forward(const double (&P)[9], double (&Q)[9
 
 // The back sweep (comp_ng.F90:317-324) from the scratch rows, the top level
 // with the He escape flux (:326-332) and calc_helium = 0's fixed He.
+// One level of the back sweep: x(k) = z(k+1) - Gamma(k+1) x(k+1), stored.
+__device__ __forceinline__ void comp_back_level(const double (&g)[9], const double (&zk)[3], double (&x)[3], bool &fin,
+                                                double *out, long slab, long o)
+{
+    double xn[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) xn[i] = xs(xs(xs(zk[i], xm(g[i], x[0])), xm(g[i + 3], x[1])), xm(g[i + 6], x[2]));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        x[i] = xn[i];
+        fin = fin && fabs(x[i]) <= DBL_MAX;
+        out[(long)i * slab + o] = x[i];
+    }
+}
+
+// The top level (comp_ng.F90:326-332) from xb = x(nk-2), calc_helium = 0's
+// fixed He, and the status.
+__device__ __forceinline__ void comp_top(const CompConsts &C, const CompLevel &Lp, double flx00, double flx_he,
+                                         const double (&xb)[3], bool ok, bool fin, double *out, int nk, long ld,
+                                         long col, unsigned *status)
+{
+    const long slab = (long)nk * ld;
+    const double dz = C.dz, rdz = xd(1.0, dz);
+    double top[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const double h = xm(xm(0.5, Lp.ep[i]), dz);
+        top[i] = xm(xd(xa(1.0, h), xs(1.0, h)), xb[i]);
+    }
+    top[1] = xa(top[1], xd(xm(xs(Lp.a23, Lp.a22), flx_he), xm(flx00, xs(rdz, xm(0.5, Lp.ep[1])))));
+    top[2] = xa(top[2], xd(xm(xs(Lp.a33, Lp.a32), flx_he), xm(flx00, xs(rdz, xm(0.5, Lp.ep[2])))));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        fin = fin && fabs(top[i]) <= DBL_MAX;
+        out[(long)i * slab + (long)(nk - 1) * ld + col] = top[i];
+    }
+    if (!C.calc_helium)
+        for (int k = 0; k < nk; ++k) out[2 * slab + (long)k * ld + col] = C.pshelb;
+    if (!ok || !fin) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+}
+
 __device__ __forceinline__ void comp_back(const CompConsts &C, const CompLevel &Lp, double flx00, double flx_he,
                                           const double (&z)[3], bool ok, double *out, const double *scr, int nk,
                                           long ld, long col, unsigned *status, int pd)
 {
     const long slab = (long)nk * ld;
-    const double dz = C.dz, rdz = xd(1.0, dz);
     // back sweep (comp_ng.F90:317-324); x(nk-1) = z_{nk-1}
     bool fin = true;
     double x[3], xb[3];
@@ -1311,34 +1351,9 @@ __device__ __forceinline__ void comp_back(const CompConsts &C, const CompLevel &
         for (int e = 0; e < 9; ++e) g[e] = sg[(long)e * ld];
 #pragma unroll
         for (int i = 0; i < 3; ++i) zk[i] = sg[(long)(9 + i) * ld];
-        double xn[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-            xn[i] = xs(xs(xs(zk[i], xm(g[i], x[0])), xm(g[i + 3], x[1])), xm(g[i + 6], x[2]));
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            x[i] = xn[i];
-            fin = fin && fabs(x[i]) <= DBL_MAX;
-            out[(long)i * slab + (long)k * ld + col] = x[i];
-        }
+        comp_back_level(g, zk, x, fin, out, slab, (long)k * ld + col);
     }
-    // top level (comp_ng.F90:326-332)
-    double top[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        const double h = xm(xm(0.5, Lp.ep[i]), dz);
-        top[i] = xm(xd(xa(1.0, h), xs(1.0, h)), xb[i]);
-    }
-    top[1] = xa(top[1], xd(xm(xs(Lp.a23, Lp.a22), flx_he), xm(flx00, xs(rdz, xm(0.5, Lp.ep[1])))));
-    top[2] = xa(top[2], xd(xm(xs(Lp.a33, Lp.a32), flx_he), xm(flx00, xs(rdz, xm(0.5, Lp.ep[2])))));
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        fin = fin && fabs(top[i]) <= DBL_MAX;
-        out[(long)i * slab + (long)(nk - 1) * ld + col] = top[i];
-    }
-    if (!C.calc_helium)
-        for (int k = 0; k < nk; ++k) out[2 * slab + (long)k * ld + col] = C.pshelb;
-    if (!ok || !fin) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+    comp_top(C, Lp, flx00, flx_he, xb, ok, fin, out, nk, ld, col, status);
 }
 
 // One column of comp_ng's rows and block solve (comp_ng.F90:170-332).  The
@@ -1705,6 +1720,119 @@ __global__ void __launch_bounds__(kCompWalkThreads) k_comp_walk(CompFields F, Co
               status, pd);
 }
 
+// The same pass for launches of few columns, on a 16-column tile per block
+// of kCompTileWarps warps.  The 30 row planes stream through a two-buffer
+// shared-memory ring, kCompChunk levels per buffer: all warps copy the next
+// chunk (cp.async) while warp 0 runs the recurrence over this one.  Gamma
+// and z of every level go to the global scratch (L2) and come back through
+// the same ring, top down, for the back sweep.  Same arithmetic
+// (comp_forward, comp_back_level, comp_top), same bits.
+constexpr int kCompTileCols = 16, kCompChunk = 8, kCompTileWarps = 4;
+constexpr size_t kCompTileBytes = sizeof(double) * 2 * kCompChunk * 30 * kCompTileCols;
+__global__ void __launch_bounds__(32 * kCompTileWarps) k_comp_walk_tile(CompFields F, CompConsts C, const double *lv,
+                                                                        const double *rows, const double *flx00_row,
+                                                                        double *out, double *scr, int nk, int ncol,
+                                                                        long ld, unsigned *status)
+{
+    extern __shared__ double comp_tile[];
+    constexpr int TC = kCompTileCols, L = kCompChunk, NT = 32 * kCompTileWarps;
+    double *ring = comp_tile;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    const long col0 = (long)blockIdx.x * TC, col = col0 + lane;
+    const long slab = (long)nk * ld;
+    const int K = nk - 1, nch = (K + L - 1) / L;
+    // chunk c (levels c*L .. c*L+L-1 below K) into buffer c & 1, laid out
+    // [level][plane][column]
+    auto load = [&](int c) {
+        const int k0 = c * L, nl = K - k0 < L ? K - k0 : L;
+        double *buf = ring + (c & 1) * L * 30 * TC;
+        for (int i = tid; i < nl * 30 * TC; i += NT) {
+            const int j = i % TC, lv30 = i / TC, l = lv30 / 30, v = lv30 - 30 * l;
+            if (col0 + j < ncol) cp_async8(buf + i, rows + (long)v * slab + (long)(k0 + l) * ld + col0 + j);
+        }
+        cp_async_commit();
+    };
+    const bool walker = w == 0 && lane < TC && col < ncol;
+    double G[9], z[3];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) G[e] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) z[i] = 0.0;
+    bool ok = true;
+    load(0);
+    for (int c = 0; c < nch; ++c) {
+        if (c + 1 < nch) load(c + 1);
+        else cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        if (walker) {
+            const double *buf = ring + (c & 1) * L * 30 * TC + lane;
+            const int k0 = c * L, nl = K - k0 < L ? K - k0 : L;
+            for (int l = 0; l < nl; ++l) {
+                const double *r = buf + l * 30 * TC;
+                double P[9], Q[9], R[9], f[3];
+#pragma unroll
+                for (int e = 0; e < 9; ++e) {
+                    P[e] = r[e * TC];
+                    Q[e] = r[(9 + e) * TC];
+                    R[e] = r[(18 + e) * TC];
+                }
+#pragma unroll
+                for (int i = 0; i < 3; ++i) f[i] = r[(27 + i) * TC];
+                comp_forward(P, Q, R, f, k0 + l, nk, ld, col, scr, G, z, ok);
+            }
+        }
+        __syncthreads();
+    }
+    // back sweep (comp_ng.F90:317-324): level k from the Gamma/z row k+1,
+    // k = nk-3 .. 0, chunk d holding levels kh(d) - l, l < L
+    const int KB = nk - 2, nb = (KB + L - 1) / L;
+    auto load_b = [&](int d) {
+        const int kh = nk - 3 - d * L, nl = KB - d * L < L ? KB - d * L : L;
+        double *buf = ring + (d & 1) * L * 30 * TC;
+        for (int i = tid; i < nl * 12 * TC; i += NT) {
+            const int j = i % TC, le = i / TC, l = le / 12, e = le - 12 * l;
+            if (col0 + j < ncol) cp_async8(buf + i, scr + (long)(kh - l + 1) * 12 * ld + (long)e * ld + col0 + j);
+        }
+        cp_async_commit();
+    };
+    bool fin = true;
+    double x[3], xb[3];
+    if (walker)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            x[i] = xb[i] = z[i];
+            out[(long)i * slab + (long)(nk - 2) * ld + col] = x[i];
+            fin = fin && fabs(x[i]) <= DBL_MAX;
+        }
+    load_b(0);
+    for (int d = 0; d < nb; ++d) {
+        if (d + 1 < nb) load_b(d + 1);
+        else cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        if (walker) {
+            const double *buf = ring + (d & 1) * L * 30 * TC + lane;
+            const int kh = nk - 3 - d * L, nl = KB - d * L < L ? KB - d * L : L;
+            for (int l = 0; l < nl; ++l) {
+                double g[9], zk[3];
+#pragma unroll
+                for (int e = 0; e < 9; ++e) g[e] = buf[(l * 12 + e) * TC];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) zk[i] = buf[(l * 12 + 9 + i) * TC];
+                comp_back_level(g, zk, x, fin, out, slab, (long)(kh - l) * ld + col);
+            }
+        }
+        __syncthreads();
+    }
+    if (!walker) return;
+    CompPlaneSrc src{{F, ld, col, nk}, lv};
+    CompLevel Lp;
+    src.load(nk - 1, Lp);
+    comp_top(C, Lp, flx00_row[col], C.calc_helium ? __ldg(F.flx_he + col) : 0.0, xb, ok, fin, out, nk, ld, col,
+             status);
+}
+
 // ---------------------------------------------------------------------------
 // comp_ng's history diagnostics (src/comp_ng.F90:334-380) from the fields and
 // the solution x (three level-major planes O2, O, He, before the lateral
@@ -1819,9 +1947,11 @@ cudaError_t launch_comp_ng(const CompFields &F, const CompConsts &C, double *out
         double *rows = flx00_row + ld;
         k_comp_levels<<<dim3((ncol + T - 1) / T, nk), T, 0, st>>>(F, C, lv, nk, ncol, ld);
         k_comp_coefs<<<dim3((ncol + T - 1) / T, nk - 1), T, 0, st>>>(F, C, lv, rows, flx00_row, nk, ncol, ld, sys_out);
-        const int TW = kCompWalkThreads;
-        k_comp_walk<<<(ncol + TW - 1) / TW, TW, 0, st>>>(F, C, lv, rows, flx00_row, out, scratch, nk, ncol, ld, status,
-                                                         walk_prefetch(ncol));
+        once_per_device([] {
+            cudaFuncSetAttribute(k_comp_walk_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCompTileBytes);
+        });
+        k_comp_walk_tile<<<(ncol + kCompTileCols - 1) / kCompTileCols, 32 * kCompTileWarps, kCompTileBytes, st>>>(
+            F, C, lv, rows, flx00_row, out, scratch, nk, ncol, ld, status);
         return cudaGetLastError();
     }
     if (assembly_mode() >= 1) {

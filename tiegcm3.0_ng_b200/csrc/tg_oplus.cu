@@ -366,15 +366,41 @@ __global__ void __launch_bounds__(128) k_oplus_rows(OplusFields F, OplusConsts C
 }
 
 // Three-pass form, pass 2: row k of every column, one thread per (row, column).
-__global__ void __launch_bounds__(128) k_oplus_coefs(OplusFields F, OplusConsts C, double *scr, int nk, int ncol,
-                                                     long ld, double *sys_out)
+// A block covers kCoefCols columns x kCoefRows rows; the column quantities
+// (oplus_col: the O+ flux boundary with its cosine, the upper-boundary
+// coefficients, several divisions) are formed once per column and block by
+// the block's first row of threads and shared.
+constexpr int kCoefCols = 32, kCoefRows = 8;
+dim3 coef_grid(int nk, int ncol)
 {
-    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
-    const int k = blockIdx.y;
+    return dim3((unsigned)((ncol + kCoefCols - 1) / kCoefCols), (unsigned)((nk - 1 + kCoefRows - 1) / kCoefRows));
+}
+__global__ void __launch_bounds__(kCoefCols * kCoefRows) k_oplus_coefs(OplusFields F, OplusConsts C, double *scr,
+                                                                       int nk, int ncol, long ld, double *sys_out)
+{
+    __shared__ OplusCol col_q[kCoefCols];
+    const long col = (long)blockIdx.x * kCoefCols + threadIdx.x;
+    const int k = blockIdx.y * kCoefRows + threadIdx.y;
     const long slab = (long)nk * ld, o = (long)k * ld + col;
     OplusRowsAt A{scr, slab, ld, col, nk, 0., 0., 0.};
-    const OplusCol cc = oplus_col(F, C, A);
+    // every line row k reads, requested into L1 at once: the loads below
+    // sit between divisions and would otherwise wait one at a time
+    if (col < ncol && k < nk - 1) {
+        const int km = k > 0 ? k - 1 : 0;
+        for (int e = S_DJ; e <= S_PROD; ++e)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) pf_l1(scr + (long)e * slab + (long)(km + j) * ld + col);
+        pf_l1(F.bdotdh_djbz + o);
+        pf_l1(F.bdotdh_djbz + o + ld);
+        pf_l1(F.wi + o);
+        pf_l1(F.wi + o + ld);
+        pf_l1(F.explicit_h + o);
+        pf_l1(F.optm1_smooth2 + o);
+    }
+    if (threadIdx.y == 0 && col < ncol) col_q[threadIdx.x] = oplus_col(F, C, A);
+    __syncthreads();
+    if (col >= ncol || k >= nk - 1) return;
+    const OplusCol cc = col_q[threadIdx.x];
     A.gmr = cc.gmr;
     double p, q, r, ex, t_top = 0., t_bot = 0.;
     oplus_row(F, C, A, cc, k, p, q, r, ex, &t_top, &t_bot);
@@ -752,7 +778,7 @@ cudaError_t launch_oplus_factor(const OplusFields &F, const OplusConsts &C, doub
     if (nk < 3) return cudaErrorInvalidValue;
     k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, xiop2p, xiop2d, nullptr, nullptr, factor, nk,
                                                                  ncol, ld);
-    k_oplus_coefs<<<dim3((ncol + 127) / 128, nk - 1), 128, 0, st>>>(F, C, factor, nk, ncol, ld, nullptr);
+    k_oplus_coefs<<<coef_grid(nk, ncol), dim3(kCoefCols, kCoefRows), 0, st>>>(F, C, factor, nk, ncol, ld, nullptr);
     return launch_oplus_factor_pass(factor, nk, ncol, ld, status, st);
 }
 
@@ -816,7 +842,8 @@ cudaError_t launch_oplus_ng(const OplusFields &F, const OplusConsts &C, double *
         const long slab = (long)nk * ld;
         k_oplus_levels<<<dim3((ncol + 127) / 128, nk), 128, 0, st>>>(F, C, xiop2p, xiop2d, Fe, Fn, scratch, nk, ncol,
                                                                      ld);
-        k_oplus_coefs<<<dim3((ncol + 127) / 128, nk - 1), 128, 0, st>>>(F, C, scratch, nk, ncol, ld, sys_out);
+        k_oplus_coefs<<<coef_grid(nk, ncol), dim3(kCoefCols, kCoefRows), 0, st>>>(F, C, scratch, nk, ncol, ld,
+                                                                                  sys_out);
         return launch_thomas_post(scratch + S_P * slab, scratch + S_Q * slab, scratch + S_R * slab,
                                   scratch + S_EX * slab, opout, nk, nk - 1, 1, ncol, ld, status, post, st);
     }

@@ -208,6 +208,123 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_thomas_post_tile(const doub
         for (int k = w; k < KS; k += NW) x[(long)k * ld + col] = sq[k * T + t];
     }
 }
+
+// The walk for launches above the tile limit, one warp per 32-column block:
+// each lane's rows of p, q, r, f stream through a two-buffer shared-memory
+// ring of kRingLevels levels, the copies of the next chunk in flight while
+// this one is walked (a lane reads only what it copied itself: no barrier).
+// w2 of every level stays in shared memory, w3 is parked in x; the main loop
+// is branch-free Markstein with the IEEE re-walk from the first out-of-range
+// level (from the planes in global memory), as in the tile walk.  The back
+// sweep leaves the solution in shared memory where w2 was, and the stores
+// through the post steps go out last.
+constexpr int kRingLevels = 4;
+__global__ void __launch_bounds__(32) k_thomas_post_ring(const double *P, const double *Q, const double *R,
+                                                         const double *Fv, double *x, int nk, int K, int top,
+                                                         int ncol, long ld, unsigned *status, PostStep post,
+                                                         int has_post)
+{
+    extern __shared__ double ring_walk[];
+    const int T = 32, t = threadIdx.x, L = kRingLevels;
+    const long col = (long)blockIdx.x * T + t;
+    if (col >= ncol) return;
+    const int KS = top == 1 ? K + 1 : K, nch = (K + L - 1) / L;
+    double *rb = ring_walk, *sw = ring_walk + 2 * L * 4 * T;   // ring [2][L][4][32]; w2, then x: KS rows
+    const double *src[4] = {P, Q, R, Fv};
+    auto load = [&](int c) {
+        const int k0 = c * L, nl = K - k0 < L ? K - k0 : L;
+        double *buf = rb + (c & 1) * L * 4 * T + t;
+        for (int l = 0; l < nl; ++l)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) cp_async8(buf + (l * 4 + v) * T, src[v] + (long)(k0 + l) * ld + col);
+        cp_async_commit();
+    };
+    bool ok = true;
+    int bad = K;
+    double w1 = 0.0, y1 = 0.0, w2 = 0.0, w3 = 0.0;
+    load(0);
+    for (int c = 0; c < nch; ++c) {
+        if (c + 1 < nch) load(c + 1);
+        else cp_async_commit();
+        cp_async_wait<1>();
+        const double *buf = rb + (c & 1) * L * 4 * T + t;
+        const int k0 = c * L, nl = K - k0 < L ? K - k0 : L;
+        for (int l = 0; l < nl; ++l) {
+            const int k = k0 + l;
+            const double p = buf[(l * 4) * T], q = buf[(l * 4 + 1) * T], r = buf[(l * 4 + 2) * T],
+                         f = buf[(l * 4 + 3) * T];
+            w1 = k == 0 ? q : xs(q, xm(p, w2));
+            y1 = __drcp_rn(w1);
+            const double num = k == 0 ? f : xs(f, xm(p, w3));
+            ok = ok && (bad < K || finite_nz(w1));
+            const unsigned d = max(exp_dist(w1), max(exp_dist(num), k + 1 == K ? 0u : exp_dist(r)));
+            bad = d >= kExpSpan && bad == K ? k : bad;
+            w3 = div_markstein(num, w1, y1);
+            w2 = div_markstein(r, w1, y1);
+            if (bad > k) {
+                sw[k * T + t] = w2;
+                x[(long)k * ld + col] = w3;
+            }
+        }
+    }
+    if (bad < K) {
+        // from the first out-of-range level, the divisions with their IEEE
+        // fallback, the rows read again from the planes
+        w2 = bad > 0 ? sw[(bad - 1) * T + t] : 0.0;
+        w3 = bad > 0 ? x[(long)(bad - 1) * ld + col] : 0.0;
+        for (int k = bad; k < K; ++k) {
+            const long o = (long)k * ld + col;
+            const double p = P[o], q = Q[o], f = Fv[o];
+            w1 = k == 0 ? q : xs(q, xm(p, w2));
+            y1 = __drcp_rn(w1);
+            const double num = k == 0 ? f : xs(f, xm(p, w3));
+            if (k + 1 < K) qdiv2(num, R[o], w1, y1, w3, w2);
+            else w3 = qdiv1(num, w1, y1);
+            ok = ok && finite_nz(w1);
+            sw[k * T + t] = w2;
+            x[o] = w3;
+        }
+    }
+    // back sweep: x(k) = w3(k) - w2(k)*x(k+1), w3 from x four levels ahead
+    const double xtop = w3;
+    double xn = xtop, rw[4] = {0., 0., 0., 0.};
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if (K - 2 - u >= 0) rw[u] = x[(long)(K - 2 - u) * ld + col];
+    sw[(K - 1) * T + t] = xtop;
+    int kb = K - 2;
+    for (; kb - 7 >= 0; kb -= 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = kb - u;
+            xn = xs(rw[u], xm(sw[k * T + t], xn));
+            rw[u] = x[(long)(k - 4) * ld + col];
+            sw[k * T + t] = xn;
+        }
+    }
+    for (; kb >= 0; kb -= 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = kb - u;
+            if (k >= 0) {
+                xn = xs(rw[u], xm(sw[k * T + t], xn));
+                if (k - 4 >= 0) rw[u] = x[(long)(k - 4) * ld + col];
+                sw[k * T + t] = xn;
+            }
+        }
+    }
+    // x(k) = w3 - w2*x(k+1) carries a non-finite value down to x(0)
+    const bool fin = finite(sw[t]) && finite(xtop);
+    // x(nk-1) = x(nk-2)**2/x(nk-3) from the unfiltered values
+    if (top == 1) sw[K * T + t] = xd(xm(xtop, xtop), sw[(K - 2) * T + t]);
+    if (status && (!ok || !fin)) atomicOr(status, (ok ? 0u : FLAG_PIVOT) | (fin ? 0u : FLAG_NONFINITE));
+    if (has_post) {
+        const bool bcol = post.bnd_mask && post.bnd_mask[col];
+        for (int k = 0; k < KS; ++k) post_store(post, true, bcol, x, (long)k * ld + col, sw[k * T + t]);
+    } else {
+        for (int k = 0; k < KS; ++k) x[(long)k * ld + col] = sw[k * T + t];
+    }
+}
 }  // namespace
 
 cudaError_t launch_thomas_post(const double *p, const double *q, const double *r, const double *f, double *x, int nk,
@@ -224,6 +341,15 @@ cudaError_t launch_thomas_post(const double *p, const double *q, const double *r
         });
         k_thomas_post_tile<<<(ncol + 31) / 32, 32 * kTileWarps, tile, st>>>(
             p, q, r, f, x, nk, K, top, ncol, ld, status, post ? *post : PostStep{}, post != nullptr);
+        return cudaGetLastError();
+    }
+    const size_t ring = (size_t)32 * (2 * kRingLevels * 4 + KS) * sizeof(double);
+    if (ring <= (size_t)smem_optin()) {
+        once_per_device([] {
+            cudaFuncSetAttribute(k_thomas_post_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
+        });
+        k_thomas_post_ring<<<(ncol + 31) / 32, 32, ring, st>>>(p, q, r, f, x, nk, K, top, ncol, ld, status,
+                                                               post ? *post : PostStep{}, post != nullptr);
         return cudaGetLastError();
     }
     const size_t smem = (size_t)kWalkThreads * (K > 1 ? K - 1 : 1) * sizeof(double);
