@@ -692,13 +692,14 @@ int tg_set_stage_levels(int kind, int precision, int levels);
  * Same arithmetic, same bits. */
 int tg_set_column_residency(int kind, int precision, int mode);
 
-/* Fused assembly routines: 2 (default) three passes where built (dt_ng on
- * launches of up to 16384 columns, minor_ng, oplus_ng): the level quantities
- * and then the tridiagonal rows with one thread per (level, column), then a
- * column walk that is the recurrence alone; 1 two passes, the level
- * quantities then a walk that forms the rows as it goes (comp_ng, settei_ng
- * and dt_ng above 16384 columns in mode 2 too); 0 one fused column walk.
- * Same operations, same results. */
+/* Fused assembly routines: 2 (default) three passes where built (dt_ng,
+ * minor_ng, oplus_ng, settei_ng, and comp_ng on launches of up to 16384
+ * columns): the level quantities and then the rows with one thread per
+ * (level, column), then a column walk that is the recurrence alone (and
+ * settei_ng's Te, Ti level-parallel again); 1 two passes, the level
+ * quantities then a walk that forms the rows as it goes (comp_ng above
+ * 16384 columns in mode 2 too); 0 one fused column walk.  Same operations,
+ * same results. */
 int tg_set_assembly_mode(int mode);
 
 /* Fused assembly routines: how many levels ahead their column walks request

@@ -349,10 +349,9 @@ cudaError_t launch_dt_ng(const DtFields &F, const DtConsts &C, double *tn_upd, i
                          double *sys_out, unsigned *status, cudaStream_t st, const PostStep *post, double *scratch)
 {
     if (ncol <= 0) return cudaSuccess;
-    // dt_ng's own walk forms its rows from a register window of levels, so the
-    // three-pass form pays off only where few columns leave the walk latency
-    // bound (on 41472 columns it took 157 against 149 us)
-    if (scratch && assembly_mode() == 2 && nk >= 3 && ncol <= kSmallWalkColumns) {
+    // three-pass: the rows level-parallel, then the Thomas walk alone (on
+    // 41472 columns 143 against 151 us for the fused walk)
+    if (scratch && assembly_mode() == 2 && nk >= 3) {
         const long slab = (long)nk * ld;
         k_dt_coefs<<<dim3((ncol + 127) / 128, nk - 1), 128, 0, st>>>(F, C, scratch, nk, ncol, ld, sys_out);
         return launch_thomas_post(scratch, scratch + slab, scratch + 2 * slab, scratch + 3 * slab, tn_upd, nk, nk - 1,

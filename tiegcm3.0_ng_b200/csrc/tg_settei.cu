@@ -604,9 +604,9 @@ __global__ void __launch_bounds__(128) k_settei_rows(SetteiFields F, SetteiConst
 }
 
 // ---------------------------------------------------------------------------
-// settei_ng in three passes, for launches of few columns, where a walk that
-// forms its rows and raises every solved level to the 2/7 power waits on
-// those instructions level by level.  After k_settei_levels:
+// settei_ng in three passes (the default), so that the column walk is the
+// recurrence alone instead of forming its rows and raising every solved
+// level to the 2/7 power level by level.  After k_settei_levels:
 //   k_settei_coefs: one thread per (level, column) forms row k (p, q, r and
 //     rhs, as the walk forms them) into four planes and adds q_eni to qtotal
 //     at the interfaces;
@@ -717,7 +717,8 @@ cudaError_t launch_settei_ng(const SetteiFields &F, const SetteiConsts &C, doubl
     const size_t per = (size_t)(2 * nk - 1) * sizeof(double);
     while (T > 32 && (size_t)T * per > (size_t)optin) T /= 2;
     if ((size_t)T * per > (size_t)optin) return cudaErrorInvalidValue;
-    if (scratch && assembly_mode() == 2 && ncol <= kSmallWalkColumns) {
+    // three-pass (on 41472 columns 271 against 280 us for the two-pass walk)
+    if (scratch && assembly_mode() == 2) {
         const long slab = (long)nk * ld;
         double *rows = scratch + P_N * slab, *x = rows + 4 * slab;
         const dim3 grid((ncol + 127) / 128, nk);
