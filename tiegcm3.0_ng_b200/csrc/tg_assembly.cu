@@ -1973,14 +1973,16 @@ size_t comp_scratch_doubles(int nk, long ld) { return (size_t)(12 + kCompPlanes 
 // comp_ng post-solve steps (src/comp_ng.F90:394-457): the lateral-boundary
 // overwrite of the columns flagged in bmask (when given), the time filter,
 // the N2 extrapolation, floors and normalisation.  A block takes 32 columns
-// with four warps; a warp works on the 32 columns of one level at a time, so
+// with sixteen warps (about four levels each, so that few-column launches
+// do not wait on a long run of levels per warp); a warp works on the 32
+// columns of one level at a time, so
 // every phase runs over all levels at once: the overwrite, the search for the
 // first level with N2 < 0.01 (the least level any warp finds), the
 // extrapolation constants (one thread per column), then the per-level steps.
 // The N2 extrapolation uses the device log/exp, so it agrees with the CPU
 // restatement to a tolerance in the extrapolated levels.
 namespace tg {
-constexpr int kPostCols = 32, kPostWarps = 4;
+constexpr int kPostCols = 32, kPostWarps = 16;
 
 __global__ void __launch_bounds__(kPostCols * kPostWarps) k_comp_post_ng(
     const double *o2, const double *o1, const double *he, const double *o2_nm, const double *o1_nm,
@@ -2043,18 +2045,20 @@ __global__ void __launch_bounds__(kPostCols * kPostWarps) k_comp_post_ng(
         if (extrap && k > ktop) n2 = xd(exp(xa(n2top, xm(dn2dz, xs(zpmid[k], zmtop)))), xnmbar[o]);
         const double n2nm = xs(xs(xs(1.0, an), bn), cn);
         double a = fmax(a0, small), b = fmax(b0, small), cc = fmax(c0, small), d = fmax(n2, small);
-        double s = xa(xa(xa(a, b), cc), d);
-        o2u[o] = xd(a, s);
-        o1u[o] = xd(b, s);
-        heu[o] = xd(cc, s);
+        // the three quotients by one sum share a correctly rounded reciprocal
+        double s = xa(xa(xa(a, b), cc), d), y = __drcp_rn(s);
+        o2u[o] = qdiv(a, s, y);
+        o1u[o] = qdiv(b, s, y);
+        heu[o] = qdiv(cc, s, y);
         a = fmax(an, small);
         b = fmax(bn, small);
         cc = fmax(cn, small);
         d = fmax(n2nm, small);
         s = xa(xa(xa(a, b), cc), d);
-        o2n[o] = xd(a, s);
-        o1n[o] = xd(b, s);
-        hen[o] = xd(cc, s);
+        y = __drcp_rn(s);
+        o2n[o] = qdiv(a, s, y);
+        o1n[o] = qdiv(b, s, y);
+        hen[o] = qdiv(cc, s, y);
     }
 }
 
