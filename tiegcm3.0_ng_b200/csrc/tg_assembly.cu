@@ -292,6 +292,28 @@ __global__ void __launch_bounds__(128) k_dt_coefs(DtFields F, DtConsts C, double
     if (col >= ncol) return;
     const int k = blockIdx.y, K = nk - 1;
     auto at = [&](const double *p, int kk) { return __ldg(p + kk * ld + col); };
+    {
+        // every line the row reads, requested into L1 at once: the reads
+        // below sit between divisions and would otherwise wait one at a time
+        const int km = k > 0 ? k - 1 : 0;
+        const long o = (long)k * ld + col;
+        for (int j = km; j <= k + 1; ++j) {
+            const long oj = (long)j * ld + col;
+            pf_l1(F.tn + oj);
+            pf_l1(F.un + oj);
+            pf_l1(F.vn + oj);
+        }
+        const double *pair[] = {F.schti, F.cp, F.kt, F.w, F.km, F.qtotal};
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            pf_l1(pair[i] + o);
+            pf_l1(pair[i] + o + ld);
+        }
+        const double *one[] = {F.horadv, F.tnsmooth, F.mbar, F.xnmbar, F.o1, F.rkm12, F.scht, F.hdt, F.qji_tn,
+                               F.cool_exp, F.cool_imp};
+#pragma unroll
+        for (int i = 0; i < 11; ++i) pf_l1(one[i] + o);
+    }
     const double dz = C.dz;
     const double expz = __ldg(F.expz + k);
     const GF gf0 = dt_gf_at(F, C, k, nk, ld, col), gfp = dt_gf_at(F, C, k + 1, nk, ld, col);
