@@ -352,7 +352,24 @@ __global__ void __launch_bounds__(128) k_oplus_levels(OplusFields F, OplusConsts
 {
     const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
-    oplus_level(F, C, scr, xiop2p, xiop2d, Fe, Fn, nk, ld, col, blockIdx.y);
+    const int j = blockIdx.y;
+    {
+        // every line level j reads, requested into L1 at once: the reads sit
+        // between log10, sqrt, pow and divisions and would otherwise wait
+        // one at a time
+        const long o = (long)j * ld + col;
+        const double *lvl[] = {F.tn, F.te, F.ti, F.o2, F.o1, F.n2, F.he, F.xnmbar, F.scht, F.ne, F.u, F.v,
+                               F.rk19, F.rk20, F.rk25, F.rk1, F.rk2, F.n2d, F.w, F.qop2p, F.qop2d, F.qop};
+#pragma unroll
+        for (int i = 0; i < 22; ++i) pf_l1(lvl[i] + o);
+        if (j + 1 < nk) {
+            pf_l1(F.w + o + ld);
+            pf_l1(F.qop2p + o + ld);
+            pf_l1(F.qop2d + o + ld);
+            pf_l1(F.qop + o + ld);
+        }
+    }
+    oplus_level(F, C, scr, xiop2p, xiop2d, Fe, Fn, nk, ld, col, j);
 }
 
 __global__ void __launch_bounds__(128) k_oplus_rows(OplusFields F, OplusConsts C, double *opout, const double *scr,
