@@ -1697,53 +1697,10 @@ __global__ void __launch_bounds__(128) k_comp_coefs(CompFields F, CompConsts C, 
     }
 }
 
-// Three-pass form, pass 3: the block recurrence over the row planes, one
-// thread per column, one warp per block (the columns spread over every SM).
-constexpr int kCompWalkThreads = 32;
-__global__ void __launch_bounds__(kCompWalkThreads) k_comp_walk(CompFields F, CompConsts C, const double *lv,
-                                                                const double *rows, const double *flx00_row,
-                                                                double *out, double *scr, int nk, int ncol, long ld,
-                                                                unsigned *status, int pd)
-{
-    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
-    const long slab = (long)nk * ld;
-    auto pf_row = [&](int k) {
-        const double *r = rows + (long)k * ld + col;
-#pragma unroll
-        for (int v = 0; v < 30; ++v) pf_l1(r + (long)v * slab);
-    };
-    for (int kk = 1; kk < pd && kk < nk - 1; ++kk) pf_row(kk);
-    double G[9], z[3];
-#pragma unroll
-    for (int e = 0; e < 9; ++e) G[e] = 0.0;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) z[i] = 0.0;
-    bool ok = true;
-    for (int k = 0; k < nk - 1; ++k) {
-        if (k + pd < nk - 1) pf_row(k + pd);
-        const double *r = rows + (long)k * ld + col;
-        double P[9], Q[9], R[9], f[3];
-#pragma unroll
-        for (int e = 0; e < 9; ++e) {
-            P[e] = r[(long)e * slab];
-            Q[e] = r[(long)(9 + e) * slab];
-            R[e] = r[(long)(18 + e) * slab];
-        }
-#pragma unroll
-        for (int i = 0; i < 3; ++i) f[i] = r[(long)(27 + i) * slab];
-        comp_forward(P, Q, R, f, k, nk, ld, col, scr, G, z, ok);
-    }
-    CompPlaneSrc src{{F, ld, col, nk}, lv};
-    CompLevel Lp;
-    src.load(nk - 1, Lp);
-    comp_back(C, Lp, flx00_row[col], C.calc_helium ? __ldg(F.flx_he + col) : 0.0, z, ok, out, scr, nk, ld, col,
-              status, pd);
-}
-
-// The same pass for launches of few columns, on a 16-column tile per block
-// of kCompTileWarps warps.  The 30 row planes stream through a two-buffer
-// shared-memory ring, kCompChunk levels per buffer: all warps copy the next
+// Three-pass form, pass 3: the block recurrence over the row planes, on a
+// 16-column tile per block of kCompTileWarps warps.  The 30 row planes
+// stream through a two-buffer shared-memory ring, kCompChunk levels per
+// buffer: all warps copy the next
 // chunk (cp.async) while warp 0 runs the recurrence over this one.  Gamma
 // and z of every level go to the global scratch (L2) and come back through
 // the same ring, top down, for the back sweep.  Same arithmetic
