@@ -750,9 +750,13 @@ def main():
     assembly = None
     if not args.skip_assembly:
         assembly = {}
-        for which, kern in (("dt", "k_dt_ng"), ("minor", "k_minor_levels+k_minor_rows"),
-                            ("comp", "k_comp_levels+k_comp_rows"), ("settei", "k_settei_levels+k_settei_rows"),
-                            ("oplus", "k_oplus_levels+k_oplus_rows")):
+        # the kernels each routine runs at this size (41472 columns) in the
+        # default assembly form: three passes, comp_ng two above 16384 columns
+        for which, kern in (("dt", "k_dt_coefs+k_thomas_post_ring"),
+                            ("minor", "k_minor_levels+k_minor_coefs+k_thomas_post_ring"),
+                            ("comp", "k_comp_levels+k_comp_rows"),
+                            ("settei", "k_settei_levels+k_settei_coefs+k_thomas_post_ring+k_settei_post"),
+                            ("oplus", "k_oplus_levels+k_oplus_coefs+k_thomas_post_ring")):
             launch, ncol_a, nbytes = assembly_setup(pkg, wl, which, dev)
             for _ in range(args.warmup):
                 launch(stream)
