@@ -870,6 +870,19 @@ __global__ void __launch_bounds__(128) k_minor_coefs(MinorFields F, MinorConsts 
     if (col >= ncol) return;
     const int k = blockIdx.y;
     const long slab = (long)nk * ld, o = (long)k * ld + col;
+    {
+        // every line the row reads, requested into L1 at once
+        const long op = k < nk - 1 ? o + ld : o;
+        const double *one[] = {F.sprod, F.xnmbar, F.ftm1_smooth, F.hadvec, F.sloss, F.w};
+#pragma unroll
+        for (int i = 0; i < 6; ++i) pf_l1(one[i] + o);
+        pf_l1(F.w + op);
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            pf_l1(lv + e * slab + o);
+            pf_l1(lv + e * slab + op);
+        }
+    }
     MinorRowIn in;
     in.sprod = __ldg(F.sprod + o);
     in.xnmbar = __ldg(F.xnmbar + o);

@@ -625,6 +625,18 @@ __global__ void __launch_bounds__(128) k_settei_coefs(SetteiFields F, SetteiCons
     const int k = blockIdx.y;
     const long slab = (long)nk * ld, o = (long)k * ld + col;
     auto pl = [&](int e, int kk) { return __ldg(lv + e * slab + (long)kk * ld + col); };
+    {
+        // every line the row reads, requested into L1 at once
+        const int km = k > 0 ? k - 1 : 0, kp = k + 1 < nk ? k + 1 : nk - 1;
+        pf_l1(lv + P_QENI * slab + (long)km * ld + col);
+        pf_l1(lv + P_QENI * slab + o);
+        pf_l1(lv + P_QENI * slab + (long)kp * ld + col);
+        pf_l1(lv + P_TH * slab + (long)kp * ld + col);
+#pragma unroll
+        for (int e = P_TH; e <= P_LEITI; ++e) pf_l1(lv + e * slab + o);
+        pf_l1(qtotal + o);
+        pf_l1(F.scht + o);
+    }
     // qtotal += q_eni at the interfaces (settei_ng.F90:248-254); level k
     // reads and writes only its own qtotal
     const double qe_k = pl(P_QENI, k);
