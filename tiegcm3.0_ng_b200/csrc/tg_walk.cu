@@ -96,8 +96,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_thomas_post(const double *P, c
 // few columns.  The kTileWarps warps of a block share one 32-column tile:
 // together they copy the p, q, r, f rows of every level (cp.async, every
 // copy in flight at once, each warp a quarter of the levels), then warp 0
-// alone runs the recurrence from shared memory, keeping w2 where r(k-1) was
-// and the parked w3, then the solution, where q(k) was; finally all warps
+// alone runs the recurrence from shared memory, keeping the next level's
+// w2 = r(k)/w1(k) where r(k) was and the parked w3, then the solution, where
+// q(k) was; finally all warps
 // store the rows through the post-solve steps, each its quarter of the
 // levels.  The per-column serial part is the recurrence alone.
 constexpr int kTileWarps = 4;
