@@ -75,6 +75,13 @@ def test_bad_arguments_rejected_without_device(pkg):
     assert L.tg_trsolv_ng(p, p, p, p, p, 5, 6, 3) == pkg.TG_EINVAL
     assert L.tg_comp_blksolve_ng(4, p, p, p, p, None, None, p, 5, 1) == pkg.TG_EINVAL
     assert L.tg_plan_create(None, 1, 0, None) == pkg.TG_EINVAL
+    # the walk test entry: an unknown walk, a stride below the columns, a
+    # missing status word, an O+ factor pass on fewer than 3 levels
+    st = ctypes.cast((ctypes.c_int * 1)(), ctypes.c_void_p)
+    assert L.tg_selftest_walk(2, p, 3, 3, 0, 2, 2, st, None) == pkg.TG_EINVAL
+    assert L.tg_selftest_walk(0, p, 3, 3, 0, 4, 2, st, None) == pkg.TG_EINVAL
+    assert L.tg_selftest_walk(0, p, 3, 3, 0, 2, 2, None, None) == pkg.TG_EINVAL
+    assert L.tg_selftest_walk(1, p, 2, 1, 1, 2, 2, st, None) == pkg.TG_EINVAL
 
 
 def test_tuning_entries_validate_without_device(pkg):
